@@ -1,0 +1,396 @@
+"""Benchmark of the volumetric path-tracing hot path on B200.
+
+Workload (the dense multi-tracker configuration): 512^3 fp32 fBm Perlin cloud (seed 2, 6 octaves,
+lacunarity 2, gain 0.5, ~35% empty), unit cube, extinction 1000, albedo 0.99, HG g = 0.85, sun 5
+plus constant sky 0.2, pinhole camera 60 deg at distance 2, 1024x1024, max 128 bounces.  One step =
+one render_frame of SPP_PER_STEP 1-spp frames (1024^2 * SPP_PER_STEP camera paths) with delta
+tracking; the other trackers are timed for a few steps each (per_tracker).  The grid (512 MiB) is
+larger than L2, so no flush is needed between steps.
+
+`python bench.py --gpus N --steps K --warmup W` prints one JSON line (rank 0).  Under torchrun each
+rank renders its own frames (disjoint seeds; weak scaling, no collective on the data path).
+`--impl reference` times the CPU oracle on this host (bounded sample of the same workload).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "path samples/s per tracker"
+UNIT = "path samples/s"
+GRID = 512
+RES = 1024
+SPP_PER_STEP = 16
+MAX_BOUNCES = 128
+EXTINCTION = 1000.0
+SEED = 2
+TRACKERS = {"delta": 0, "ratio": 2, "decomposition": 3, "residual_ratio": 4, "nee": 5}
+BYTES_PER_LOOKUP = 32  # one 32-byte sector per uncoalesced density gather
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def workload_config(n_gpus):
+    return {"workload": f"dense {GRID}^3 fBm cloud, {RES}x{RES}, {SPP_PER_STEP} spp/step, delta tracking "
+                        f"(+ratio/decomposition/residual-ratio/NEE timed separately)",
+            "grid": GRID, "image": RES, "spp_per_step": SPP_PER_STEP, "max_bounces": MAX_BOUNCES,
+            "extinction": EXTINCTION, "albedo": 0.99, "g": 0.85, "interpolation": "stochastic",
+            "l2": "grid 512 MiB > L2 126 MB: inputs larger than L2, no flush",
+            "parallelism": f"spp-sharded x{n_gpus}" if n_gpus > 1 else "single GPU"}
+
+
+def sun_dir(seed):
+    rng = np.random.default_rng(seed)
+    v = rng.normal(size=3)
+    v[1] = abs(v[1]) + 0.5
+    return (v / np.linalg.norm(v)).tolist()
+
+
+def camera_pos(seed):
+    rng = np.random.default_rng(seed + 1000)
+    a = rng.uniform(0, 2 * math.pi)
+    return [2.0 * math.sin(a), 0.4, 2.0 * math.cos(a)]
+
+
+class Clocks:
+    """Samples nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def setup_scene(vpt, rank):
+    vpt.set_max_grid_extent(0.5)
+    vpt.generate_fbm_cloud(GRID, seed=SEED)
+    vpt.set_extinction_scale(EXTINCTION)
+    vpt.set_scattering_albedo([0.99, 0.99, 0.99])
+    vpt.set_phase_g(0.85)
+    vpt.set_use_builtin_environment_map("Constant Sky + Sun")
+    vpt.set_sky_color([0.2, 0.2, 0.2])
+    vpt.set_sun(sun_dir(SEED), [5.0, 5.0, 5.0])
+    vpt.set_camera_position(camera_pos(SEED))
+    vpt.set_camera_target([0.0, 0.0, 0.0])
+    vpt.set_camera_fovy(60.0)
+    vpt.set_max_bounces(MAX_BOUNCES)
+    vpt.set_grid_interpolation("Stochastic")
+    vpt.set_denoiser("None")
+    # disjoint frame seeds per rank: the whole job renders rank-strided spp of one image
+    vpt.set_seed_offset((rank * 0x9E3779B1) & 0xFFFFFFFF)
+
+
+def run_ours(args):
+    import torch
+    from cloudrendering_b200 import vpt, _lib
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    lib = _lib.load()
+    vpt.initialize()
+    ctx = vpt.context_handle()
+    setup_scene(vpt, rank)
+    stream = torch.cuda.current_stream()
+    ctypes_stream = __import__("ctypes").c_void_p(stream.cuda_stream)
+    img = torch.zeros((4, RES, RES), dtype=torch.float32, device="cuda")
+
+    def render_step():
+        _lib.check(lib.vpt_render_frames(ctx, SPP_PER_STEP, ctypes_stream), "render", ctx)
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(v):
+        if world == 1:
+            return v
+        import torch.distributed as dist
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    vpt.set_vpt_mode_from_name("Delta Tracking")
+    vpt.render_frame(img, 1)
+    for _ in range(args.warmup):
+        render_step()
+    barrier()
+    vpt.reset_stats()
+    launches0 = lib.vpt_kernel_launch_count()
+    clocks = Clocks(local)
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        render_step()
+    ev1.record(stream)
+    barrier()
+    clock_info = clocks.stop()
+    ms_total = max_over_ranks(ev0.elapsed_time(ev1))
+    launches = lib.vpt_kernel_launch_count() - launches0
+    st = vpt.get_stats()
+    _lib.check(lib.vpt_synchronize(ctx, ctypes_stream), "sync", ctx)
+    paths_per_rank = RES * RES * SPP_PER_STEP * args.steps
+    total_paths = paths_per_rank * world
+    value = total_paths / (ms_total / 1e3)
+    lookups = st["density_lookups"]
+    ms_per_launch = ms_total / args.steps
+    achieved = (lookups / args.steps) * BYTES_PER_LOOKUP / (ms_per_launch / 1e3) / 1e9
+    peak, peak_kind = peaks()
+
+    # per tracker (2 steps each after 1 warm-up step)
+    per_tracker = {}
+    for name, mode in TRACKERS.items():
+        vpt.set_vpt_mode(mode)
+        vpt.render_frame(img, 1)
+        barrier()
+        vpt.reset_stats()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(2):
+            render_step()
+        e1.record(stream)
+        barrier()
+        ms = max_over_ranks(e0.elapsed_time(e1))
+        s2 = vpt.get_stats()
+        per_tracker[name] = {"path_samples_per_s": RES * RES * SPP_PER_STEP * 2 * world / (ms / 1e3),
+                             "lookups_per_path": s2["density_lookups"] / max(1, s2["paths"]),
+                             "ms_per_step": ms / 2}
+
+    # end to end through the public API: host grid -> device, render, result -> host
+    vpt.set_vpt_mode_from_name("Delta Tracking")
+    grid_host = torch.empty((GRID, GRID, GRID), dtype=torch.float32).pin_memory()
+    _lib.check(lib.vpt_get_dense_grid(ctx, __import__("ctypes").c_void_p(grid_host.data_ptr()), 0), "get grid", ctx)
+    out_cpu = torch.zeros((4, RES, RES), dtype=torch.float32)
+    e2e_steps = max(1, min(args.steps, 3))
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        vpt.set_density_field(grid_host)
+        res = vpt.render_frame(out_cpu, SPP_PER_STEP)
+    barrier()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    e2e = {"value": RES * RES * SPP_PER_STEP * e2e_steps * world / e2e_s, "unit": UNIT,
+           "h2d_bytes_per_step": GRID ** 3 * 4, "d2h_bytes_per_step": int(res.numel() * 4),
+           "path": "vpt.set_density_field(pinned host grid) + vpt.render_frame(cpu tensor)"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(lib, ctx, vpt)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_total / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded fBm Perlin cloud)",
+            "config": workload_config(world),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "note": f"algorithmic bytes = density lookups x {BYTES_PER_LOOKUP} B sector; peak {peak_kind}"},
+            "lookups_per_s": lookups / (ms_total / 1e3) * world,
+            "lookups_per_path": lookups / max(1, st["paths"]),
+            "per_tracker": per_tracker, "e2e": e2e, "gpu_launches": int(launches), "clocks": clock_info,
+        }
+        if cpu is not None:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    vpt.cleanup()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def cpu_baseline(lib, ctx, vpt, target_s=12.0):
+    """CPU oracle on a band of rows of the same workload (1 spp), all host cores."""
+    import ctypes
+    from oracle import bridge
+
+    n = GRID ** 3
+    grid = np.empty((GRID, GRID, GRID), np.float32)
+    _lib_check = vpt._lib.check
+    _lib_check(lib.vpt_get_dense_grid(ctx, grid.ctypes.data_as(ctypes.c_void_p), 0), "get grid", ctx)
+    inv = (ctypes.c_float * 16)()
+    vp = (ctypes.c_float * 16)()
+    vpt.set_vpt_mode_from_name("Delta Tracking")
+    _lib_check(lib.vpt_get_camera_matrices(ctx, inv, vp), "camera", ctx)
+    vmin, vmax = bridge.minmax(grid)
+    dens = bridge.normalize(grid, vmin, vmax)
+    bmin, bmax = bridge.grid_bounds(GRID, GRID, GRID, 0.5)
+    f32 = np.float32
+    vpu = [float(f32(GRID / (float(f32(b1)) - float(f32(b0))))) for b0, b1 in zip(bmin, bmax)]
+    sd = np.array(sun_dir(SEED), np.float32)
+    dl = np.sqrt(f32(f32(sd[0] * sd[0]) + f32(sd[1] * sd[1])) + f32(sd[2] * sd[2]), dtype=np.float32)
+    sc = bridge.Scene(inv_view_proj=list(inv), width=RES, height=RES, frame_count=0, num_frames=1, seed_offset=0,
+                      mode=0, interp=1, max_bounces=MAX_BOUNCES, use_ess=0, box_min=bmin, box_max=bmax, nx=GRID,
+                      ny=GRID, nz=GRID, vox_per_unit=vpu,
+                      border_density=float((f32(0.0) - f32(vmin)) / (f32(vmax) - f32(vmin))), extinction=EXTINCTION,
+                      albedo=0.99,
+                      g=0.85, env_kind=3, use_linear_rgb=1, env_image_linear=1,
+                      sun_dir=[float(f32(sd[i] / dl)) for i in range(3)], sun_intensity=[5.0] * 3,
+                      sky_color=[0.2] * 3, env_intensity=[1.0] * 3, density=dens)
+    threads = os.cpu_count() or 1
+    rows, elapsed, lookups = 4, 0.0, 0
+    row0 = RES // 2
+    while True:
+        t0 = time.perf_counter()
+        _, lookups = sc.render_rows(row0, row0 + rows, threads)
+        elapsed = time.perf_counter() - t0
+        if elapsed >= target_s / 4 or rows >= RES // 2:
+            break
+        rows *= 2
+    if elapsed < target_s and rows < RES // 2:
+        rows = min(RES // 2, max(rows, int(rows * target_s / max(elapsed, 1e-3))))
+        t0 = time.perf_counter()
+        _, lookups = sc.render_rows(row0 - rows // 2, row0 - rows // 2 + rows, threads)
+        elapsed = time.perf_counter() - t0
+    paths = rows * RES
+    return {"value": paths / elapsed, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"delta tracking, rows {row0 - rows // 2}..{row0 - rows // 2 + rows} of the {RES}x{RES} image "
+                      f"at 1 spp ({paths} paths, {elapsed:.1f} s, {lookups / elapsed:.3g} lookups/s)",
+            "lookups_per_path": lookups / paths}
+
+
+def run_reference(args):
+    """CPU reference arm: the oracle restatement of the reference shaders on this host's cores."""
+    import ctypes
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    from oracle import bridge
+    grid = bridge.fbm(GRID, SEED, base_frequency=3.0, contrast=3.5)
+    vmin, vmax = bridge.minmax(grid)
+    dens = bridge.normalize(grid, vmin, vmax)
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from tests.harness import SceneSpec, camera_inv_view_proj
+    sp = SceneSpec(cam_pos=camera_pos(SEED), fovy=math.radians(60.0), near=1.0 / 512.0, far=80.0, width=RES,
+                   height=RES)
+    inv = camera_inv_view_proj(sp)
+    bmin, bmax = bridge.grid_bounds(GRID, GRID, GRID, 0.5)
+    f32 = np.float32
+    vpu = [float(f32(GRID / (float(f32(b1)) - float(f32(b0))))) for b0, b1 in zip(bmin, bmax)]
+    sd = np.array(sun_dir(SEED), np.float32)
+    sd = sd / np.linalg.norm(sd)
+    sc = bridge.Scene(inv_view_proj=inv, width=RES, height=RES, frame_count=0, num_frames=1, seed_offset=0, mode=0,
+                      interp=1, max_bounces=MAX_BOUNCES, use_ess=0, box_min=bmin, box_max=bmax, nx=GRID, ny=GRID,
+                      nz=GRID, vox_per_unit=vpu, border_density=0.0, extinction=EXTINCTION, albedo=0.99, g=0.85,
+                      env_kind=3, use_linear_rgb=1, env_image_linear=1, sun_dir=sd.tolist(), sun_intensity=[5.0] * 3,
+                      sky_color=[0.2] * 3, env_intensity=[1.0] * 3, density=dens)
+    threads = os.cpu_count() or 1
+    rows = 8
+    row0 = RES // 2 - rows // 2
+    for _ in range(args.warmup):
+        sc.render_rows(row0, row0 + 2, threads)
+    times = []
+    lookups = 0
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        _, lookups = sc.render_rows(row0, row0 + rows, threads)
+        times.append(time.perf_counter() - t0)
+    total = sum(times)
+    paths = rows * RES * args.steps
+    value = paths / total
+    sample = f"delta tracking, {rows} rows x {RES} px at 1 spp per step (center band), {threads} threads"
+    print(json.dumps({
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total / args.steps * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded fBm Perlin cloud)", "config": workload_config(world),
+        "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "lookups_per_path": lookups / (rows * RES),
+    }), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,127 @@
+"""ctypes binding of ``libvpt_b200.so`` (the C ABI declared in include/vpt_b200.h).
+
+The library is loaded from this package directory.  There is no fallback: if the shared library is
+missing the import of the rendering entry points raises, naming the build command.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from ctypes import POINTER, c_char_p, c_double, c_float, c_int, c_uint32, c_uint64, c_void_p
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libvpt_b200.so")
+
+
+class VptStats(ctypes.Structure):
+    _fields_ = [
+        ("paths", c_uint64),
+        ("density_lookups", c_uint64),
+        ("frames", c_uint64),
+        ("error_flags", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+    ]
+
+
+VptCtxP = c_void_p
+F3 = POINTER(c_float)
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "vpt_status_string": (c_char_p, [c_int]),
+    "vpt_abi_version": (c_int, []),
+    "vpt_kernel_launch_count": (c_uint64, []),
+    "vpt_create": (c_int, [POINTER(c_void_p), c_int]),
+    "vpt_destroy": (None, [VptCtxP]),
+    "vpt_last_error": (c_char_p, [VptCtxP]),
+    "vpt_set_dense_grid": (c_int, [VptCtxP, c_void_p, c_int, c_int, c_int, c_int]),
+    "vpt_generate_fbm_grid": (c_int, [VptCtxP, c_int, c_int, c_int, c_uint32, c_int, c_float, c_float, c_float, c_float]),
+    "vpt_get_dense_grid": (c_int, [VptCtxP, c_void_p, c_int]),
+    "vpt_set_voxel_size": (c_int, [VptCtxP, c_double, c_double, c_double]),
+    "vpt_set_max_grid_extent": (c_int, [VptCtxP, c_float]),
+    "vpt_get_render_bounding_box": (c_int, [VptCtxP, F3]),
+    "vpt_set_vpt_mode": (c_int, [VptCtxP, c_int]),
+    "vpt_set_grid_interpolation": (c_int, [VptCtxP, c_int]),
+    "vpt_set_extinction_scale": (c_int, [VptCtxP, c_float]),
+    "vpt_set_extinction_base": (c_int, [VptCtxP, F3]),
+    "vpt_set_scattering_albedo": (c_int, [VptCtxP, F3]),
+    "vpt_set_phase_g": (c_int, [VptCtxP, c_float]),
+    "vpt_set_seed_offset": (c_int, [VptCtxP, c_uint32]),
+    "vpt_set_use_linear_rgb": (c_int, [VptCtxP, c_int]),
+    "vpt_set_max_bounces": (c_int, [VptCtxP, c_int]),
+    "vpt_set_builtin_environment_map": (c_int, [VptCtxP, c_int]),
+    "vpt_set_environment_map_intensity_rgb": (c_int, [VptCtxP, F3]),
+    "vpt_set_sun": (c_int, [VptCtxP, F3, F3]),
+    "vpt_set_sky_color": (c_int, [VptCtxP, F3]),
+    "vpt_load_environment_map_rgba": (c_int, [VptCtxP, c_void_p, c_int, c_int, c_int, c_int]),
+    "vpt_set_camera": (c_int, [VptCtxP, F3, F3, F3, c_float, c_float, c_float]),
+    "vpt_set_view_matrix": (c_int, [VptCtxP, F3]),
+    "vpt_get_camera_matrices": (c_int, [VptCtxP, F3, F3]),
+    "vpt_set_resolution": (c_int, [VptCtxP, c_int, c_int]),
+    "vpt_reset_accumulation": (c_int, [VptCtxP]),
+    "vpt_render_frames": (c_int, [VptCtxP, c_int, c_void_p]),
+    "vpt_read_result": (c_int, [VptCtxP, c_void_p, c_int, c_int, c_void_p]),
+    "vpt_render_frame": (c_int, [VptCtxP, c_int, c_void_p, c_int, c_int, c_void_p]),
+    "vpt_set_collect_statistics": (c_int, [VptCtxP, c_int]),
+    "vpt_read_statistics": (c_int, [VptCtxP, c_void_p, c_void_p, c_int, c_void_p]),
+    "vpt_set_use_feature_maps": (c_int, [VptCtxP, POINTER(c_int), c_int]),
+    "vpt_get_feature_map": (c_int, [VptCtxP, c_int, c_void_p, c_int, c_int, c_void_p]),
+    "vpt_get_stats": (c_int, [VptCtxP, POINTER(VptStats)]),
+    "vpt_reset_stats": (c_int, [VptCtxP]),
+    "vpt_synchronize": (c_int, [VptCtxP, c_void_p]),
+    "vpt_set_use_empty_space_skipping": (c_int, [VptCtxP, c_int]),
+    "vpt_set_option": (c_int, [VptCtxP, c_char_p, c_double]),
+    "vpt_set_denoiser": (c_int, [VptCtxP, c_int]),
+    "vpt_set_denoiser_property": (c_int, [VptCtxP, c_char_p, c_char_p]),
+    "vpt_build_supervoxel_grid": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_int, c_void_p, c_void_p,
+                                          c_void_p, c_void_p, c_void_p]),
+    "vpt_build_rrt_params": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_float, c_int, c_void_p, c_void_p]),
+    "vpt_build_occupancy_grid": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_int, c_float, c_void_p,
+                                         c_void_p]),
+    "vpt_build_environment_pyramid": (c_int, [c_void_p, c_int, c_int, c_int, c_void_p, c_void_p]),
+    "vpt_eaw_denoise_rgba": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_float, c_float, c_float,
+                                     c_int, c_void_p, c_void_p]),
+}
+
+_lib = None
+
+
+def load() -> ctypes.CDLL:
+    """Loads the library (once) and installs the argument types."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"{LIB_PATH} is missing: build the CUDA core first (python -m cloudrendering_b200.build)"
+        )
+    lib = ctypes.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def farr(values) -> ctypes.Array:
+    vals = [float(v) for v in values]
+    return (c_float * len(vals))(*vals)
+
+
+class VptError(RuntimeError):
+    """A call into the CUDA core returned a non-zero VptStatus."""
+
+    def __init__(self, status: int, where: str, message: str):
+        super().__init__(f"{where}: {message} (status {status})")
+        self.status = status
+
+
+def check(status: int, where: str, ctx=None) -> None:
+    if status == 0:
+        return
+    lib = load()
+    msg = lib.vpt_last_error(ctx).decode() if ctx else ""
+    if not msg:
+        msg = lib.vpt_status_string(status).decode()
+    raise VptError(status, where, msg)

@@ -1,0 +1,1169 @@
+// vpt_context.cu - the C ABI (include/vpt_b200.h): context life cycle, settings, scene data,
+// camera, film and launches.  The context plays the role of the reference's
+// VolumetricPathTracingModuleRenderer + VolumetricPathTracingPass pair
+// (src/PyTorch/VolumetricPathTracingModuleRenderer.cpp, src/PathTracer/VolumetricPathTracingPass.cpp):
+// it owns every device buffer and fills the launch parameter block before each render.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "../../include/vpt_b200.h"
+#include "vpt_kernels.h"
+#include "vpt_params.h"
+#include "vpt_denoise.h"
+
+using vpt::F3;
+
+namespace {
+
+F3 mk(float x, float y, float z) {
+    F3 r;
+    r.x = x;
+    r.y = y;
+    r.z = z;
+    return r;
+}
+
+template <class T>
+struct DevBuf {
+    T* ptr = nullptr;
+    size_t count = 0;
+    cudaError_t alloc(size_t n) {
+        if (n == count && ptr) return cudaSuccess;
+        release();
+        if (n == 0) return cudaSuccess;
+        cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&ptr), n * sizeof(T));
+        if (e != cudaSuccess) {
+            ptr = nullptr;
+            return e;
+        }
+        count = n;
+        return cudaSuccess;
+    }
+    void release() {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        count = 0;
+    }
+};
+
+// 32-bit PCG (RXS-M-XS output) used to shuffle the Perlin permutation.
+uint32_t pcg_next(uint32_t& state) {
+    state = state * 747796405u + 2891336453u;
+    uint32_t word = ((state >> ((state >> 28u) + 4u)) ^ state) * 277803737u;
+    return (word >> 22u) ^ word;
+}
+
+void make_permutation(uint32_t seed, int out512[512]) {
+    int p[256];
+    for (int i = 0; i < 256; i++) p[i] = i;
+    uint32_t st = seed;
+    for (int i = 255; i > 0; i--) {
+        uint32_t j = pcg_next(st) % (uint32_t)(i + 1);
+        std::swap(p[i], p[j]);
+    }
+    for (int i = 0; i < 512; i++) out512[i] = p[i & 255];
+}
+
+// 4x4 helpers, column-major (m[col * 4 + row]) like glm, computed in double.
+void mat_mul(const double* a, const double* b, double* out) {
+    double r[16];
+    for (int c = 0; c < 4; c++)
+        for (int rr = 0; rr < 4; rr++) {
+            double s = 0.0;
+            for (int k = 0; k < 4; k++) s += a[k * 4 + rr] * b[c * 4 + k];
+            r[c * 4 + rr] = s;
+        }
+    memcpy(out, r, sizeof(r));
+}
+
+bool mat_inverse(const double* m, double* out) {
+    double a[4][8];
+    for (int r = 0; r < 4; r++) {
+        for (int c = 0; c < 4; c++) a[r][c] = m[c * 4 + r];
+        for (int c = 0; c < 4; c++) a[r][4 + c] = (r == c) ? 1.0 : 0.0;
+    }
+    for (int col = 0; col < 4; col++) {
+        int piv = col;
+        for (int r = col + 1; r < 4; r++)
+            if (fabs(a[r][col]) > fabs(a[piv][col])) piv = r;
+        if (fabs(a[piv][col]) < 1e-300) return false;
+        if (piv != col)
+            for (int c = 0; c < 8; c++) std::swap(a[piv][c], a[col][c]);
+        double inv = 1.0 / a[col][col];
+        for (int c = 0; c < 8; c++) a[col][c] *= inv;
+        for (int r = 0; r < 4; r++) {
+            if (r == col) continue;
+            double f = a[r][col];
+            for (int c = 0; c < 8; c++) a[r][c] -= f * a[col][c];
+        }
+    }
+    for (int r = 0; r < 4; r++)
+        for (int c = 0; c < 4; c++) out[c * 4 + r] = a[r][4 + c];
+    return true;
+}
+
+}  // namespace
+
+struct VptContext {
+    int device = 0;
+    std::string last_error;
+
+    // settings (defaults of VolumetricPathTracingPass.hpp:247-345 and Module.cpp:797-798)
+    int mode = VPT_MODE_DELTA_TRACKING;
+    int interp = VPT_INTERP_STOCHASTIC;
+    float extinction_scale = 1024.0f;
+    float extinction_base[3] = {1.0f, 1.0f, 1.0f};
+    float albedo[3] = {0.9f, 0.9f, 0.9f};
+    float g = 0.5f;
+    uint32_t seed_offset = 0;
+    int use_linear_rgb = 1;
+    int max_bounces = 0;
+    int env_kind = VPT_ENV_DEFAULT;
+    int env_image_loaded = 0;
+    int env_image_linear = 1;
+    int env_image_black = 0;
+    float env_intensity[3] = {1.0f, 1.0f, 1.0f};
+    float sun_dir[3] = {0.0f, 0.0f, 0.0f};
+    float sun_intensity[3] = {2.6f * 1.0f, 2.6f * 0.961538462f, 2.6f * 0.884615385f};
+    float sky_color[3] = {1.0f, 1.0f, 1.0f};
+    float max_grid_extent = 0.25f;
+    float voxel_size[3] = {1.0f, 1.0f, 1.0f};          // spacing of the current grid
+    float pending_voxel_size[3] = {1.0f, 1.0f, 1.0f};  // spacing for the next grid
+    int use_ess = 0;
+    int ess_ref_compat = 0;
+    int schedule = vpt::kSchedulePersistent;
+    int persistent_blocks_per_sm = 0;  // 0 = occupancy calculator (one resident wave)
+    uint32_t max_steps = vpt::kMaxStepsPerPath;
+
+    // dense grid
+    int nx = 0, ny = 0, nz = 0;
+    float vmin = 0.0f, vmax = 1.0f;
+    float box_min[3] = {0, 0, 0}, box_max[3] = {0, 0, 0};
+    DevBuf<float> raw, norm;
+    DevBuf<float> minmax;
+
+    // acceleration structures (rebuilt lazily)
+    int sv_size = 8, svx = 0, svy = 0, svz = 0;
+    int sv_kind = -1;            // tracker they were built for
+    int sv_interp = -1;
+    float sv_extinction = -1.0f;
+    DevBuf<float> sv_min, sv_max, sv_avg, sv_pairs;
+    DevBuf<uint8_t> sv_occ;
+    bool occ_valid = false;
+    int occ_interp = -1;
+    DevBuf<uint8_t> occupancy;
+
+    // environment image
+    int env_w = 0, env_h = 0;
+    int env_levels = 12;
+    DevBuf<float> env_rgba, env_pyramid;
+    DevBuf<uint64_t> env_offsets;
+    std::vector<uint64_t> env_offsets_host;
+
+    // camera (VolumetricPathTracingModuleRenderer.cpp:124-131)
+    float cam_pos[3] = {0.0f, 0.0f, 0.8f};
+    float cam_target[3] = {0.0f, 0.0f, 0.0f};
+    float cam_up[3] = {0.0f, 1.0f, 0.0f};
+    float fovy = 2.0f * atanf(0.5f);
+    float near_dist = 1.0f / 512.0f, far_dist = 80.0f;
+    bool view_overridden = false;
+    double view[16];
+
+    // film
+    int width = 0, height = 0;
+    uint32_t frame_count = 0;      // FrameInfo::frameCount: seeds and accumulation
+    uint32_t film_frames = 0;      // frames held in the film (1 for SVGF, which wants 1-spp input)
+    DevBuf<double> film, film_sq;
+    bool collect_stats = false;
+    bool features_on = false;
+    DevBuf<float> feat;
+    DevBuf<float> rgba_src, rgba_a, rgba_b;  // denoiser input and ping-pong buffers
+    DevBuf<float> eaw_maps;                  // position + normal RGBA for EAW
+    double prev_view_proj[16];
+    bool has_prev_view_proj = false;
+    DevBuf<float> staging;         // CHW staging for host outputs
+
+    DevBuf<unsigned long long> counters;
+    DevBuf<int> error_flags;
+    DevBuf<unsigned int> work_counter;
+    uint64_t frames_total = 0;
+
+    // denoiser
+    int denoiser = VPT_DENOISER_EAW;
+    vpt::EawSettings eaw;
+    vpt::SvgfSettings svgf;
+    vpt::SvgfState svgf_state;
+
+    int num_sms = 148;
+};
+
+namespace {
+
+VptStatus fail(VptContext* ctx, VptStatus st, const std::string& msg) {
+    if (ctx) ctx->last_error = msg;
+    return st;
+}
+
+VptStatus cuda_fail(VptContext* ctx, cudaError_t e, const char* where) {
+    std::string m = std::string(where) + ": " + cudaGetErrorString(e);
+    return fail(ctx, e == cudaErrorMemoryAllocation ? VPT_ERR_OOM : VPT_ERR_CUDA, m);
+}
+
+#define VPT_CHECK_CUDA(ctx, expr)                                   \
+    do {                                                            \
+        cudaError_t _e = (expr);                                    \
+        if (_e != cudaSuccess) return cuda_fail((ctx), _e, #expr);  \
+    } while (0)
+
+#define VPT_CHECK_CTX(ctx) \
+    do {                   \
+        if (!(ctx)) return VPT_ERR_ARG; \
+    } while (0)
+
+cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+bool features_needed(const VptContext* ctx);
+
+void reset_film_state(VptContext* ctx) {
+    ctx->frame_count = 0;
+    ctx->film_frames = 0;
+}
+
+// CloudData::computeGridBounds (CloudData.cpp:63-78) with voxel size 1.
+void compute_bounds(VptContext* ctx) {
+    float sx = float(ctx->nx) * ctx->voxel_size[0], sy = float(ctx->ny) * ctx->voxel_size[1];
+    float sz = float(ctx->nz) * ctx->voxel_size[2];
+    float ms = std::max(sx, std::max(sy, sz));
+    ctx->box_max[0] = sx * ctx->max_grid_extent / ms;
+    ctx->box_max[1] = sy * ctx->max_grid_extent / ms;
+    ctx->box_max[2] = sz * ctx->max_grid_extent / ms;
+    for (int i = 0; i < 3; i++) ctx->box_min[i] = -ctx->box_max[i];
+}
+
+void invalidate_accel(VptContext* ctx) {
+    ctx->sv_kind = -1;
+    ctx->occ_valid = false;
+}
+
+VptStatus finish_grid(VptContext* ctx, cudaStream_t s) {
+    size_t n = (size_t)ctx->nx * ctx->ny * ctx->nz;
+    for (int i = 0; i < 3; i++) {
+        ctx->voxel_size[i] = ctx->pending_voxel_size[i];
+        ctx->pending_voxel_size[i] = 1.0f;
+    }
+    VPT_CHECK_CUDA(ctx, ctx->minmax.alloc(2));
+    VPT_CHECK_CUDA(ctx, vpt::launch_minmax(ctx->raw.ptr, n, ctx->minmax.ptr, s));
+    float mm[2];
+    VPT_CHECK_CUDA(ctx, cudaMemcpyAsync(mm, ctx->minmax.ptr, sizeof(mm), cudaMemcpyDeviceToHost, s));
+    VPT_CHECK_CUDA(ctx, cudaStreamSynchronize(s));
+    ctx->vmin = mm[0];
+    ctx->vmax = mm[1];
+    if (ctx->vmin == ctx->vmax) ctx->vmin = 0.0f;  // DensityField.cpp:146-150
+    VPT_CHECK_CUDA(ctx, ctx->norm.alloc(n));
+    VPT_CHECK_CUDA(ctx, vpt::launch_normalize(ctx->raw.ptr, ctx->norm.ptr, n, ctx->vmin, ctx->vmax, s));
+    VPT_CHECK_CUDA(ctx, cudaStreamSynchronize(s));
+    compute_bounds(ctx);
+    invalidate_accel(ctx);
+    reset_film_state(ctx);
+    return VPT_OK;
+}
+
+int tracker_of(int mode) {
+    switch (mode) {
+        case VPT_MODE_DELTA_TRACKING: return vpt::kDelta;
+        case VPT_MODE_RATIO_TRACKING: return vpt::kRatio;
+        case VPT_MODE_DECOMPOSITION_TRACKING: return vpt::kDecomposition;
+        case VPT_MODE_RESIDUAL_RATIO_TRACKING: return vpt::kResidualRatio;
+        case VPT_MODE_NEXT_EVENT_TRACKING: return vpt::kNextEvent;
+        default: return -1;
+    }
+}
+
+// SuperVoxelGrid constructors (SuperVoxelGrid.cpp:46-65, 275-294): halve the supervoxel size until
+// it divides the grid when the grid is smaller than one supervoxel.
+void supervoxel_dims(VptContext* ctx) {
+    int s = 8;
+    if (ctx->nx < s || ctx->ny < s || ctx->nz < s) {
+        while (!(ctx->nx % s == 0 && ctx->ny % s == 0 && ctx->nz % s == 0)) s /= 2;
+    }
+    ctx->sv_size = s;
+    ctx->svx = (ctx->nx + s - 1) / s;
+    ctx->svy = (ctx->ny + s - 1) / s;
+    ctx->svz = (ctx->nz + s - 1) / s;
+}
+
+float extinction_x(const VptContext* ctx) { return ctx->extinction_base[0] * ctx->extinction_scale; }
+
+VptStatus ensure_accel(VptContext* ctx, int tracker, cudaStream_t s) {
+    const bool need_sv = tracker == vpt::kDecomposition || tracker == vpt::kResidualRatio;
+    const bool need_occ = tracker == vpt::kNextEvent && ctx->use_ess;
+    if (need_sv) {
+        // setExtinctionScale does not rebuild the RRT grid in the reference
+        // (VolumetricPathTracingPass.cpp:1289-1291); here the grid follows the current extinction.
+        bool stale = ctx->sv_kind != tracker || ctx->sv_interp != ctx->interp ||
+                     (tracker == vpt::kResidualRatio && ctx->sv_extinction != extinction_x(ctx));
+        if (stale) {
+            supervoxel_dims(ctx);
+            int total = ctx->svx * ctx->svy * ctx->svz;
+            VPT_CHECK_CUDA(ctx, ctx->sv_min.alloc(total));
+            VPT_CHECK_CUDA(ctx, ctx->sv_max.alloc(total));
+            VPT_CHECK_CUDA(ctx, ctx->sv_avg.alloc(total));
+            VPT_CHECK_CUDA(ctx, ctx->sv_occ.alloc(total));
+            VPT_CHECK_CUDA(ctx, ctx->sv_pairs.alloc((size_t)total * 2));
+            int halo = ctx->interp == VPT_INTERP_NEAREST ? 0 : 1;
+            VPT_CHECK_CUDA(ctx, vpt::launch_supervoxel_stats(ctx->norm.ptr, ctx->nx, ctx->ny, ctx->nz, ctx->sv_size,
+                                                             ctx->svx, ctx->svy, ctx->svz, halo, ctx->sv_min.ptr,
+                                                             ctx->sv_max.ptr, ctx->sv_avg.ptr, ctx->sv_occ.ptr, s));
+            if (tracker == vpt::kResidualRatio) {
+                float D = sqrtf(3.0f) * float(ctx->sv_size);
+                VPT_CHECK_CUDA(ctx, vpt::launch_rrt_params(ctx->sv_min.ptr, ctx->sv_max.ptr, ctx->sv_avg.ptr, total,
+                                                           extinction_x(ctx), D, ctx->sv_pairs.ptr, s));
+            } else {
+                VPT_CHECK_CUDA(ctx, vpt::launch_interleave(ctx->sv_min.ptr, ctx->sv_max.ptr, total, ctx->sv_pairs.ptr, s));
+            }
+            ctx->sv_kind = tracker;
+            ctx->sv_interp = ctx->interp;
+            ctx->sv_extinction = extinction_x(ctx);
+        }
+    }
+    if (need_occ && (!ctx->occ_valid || ctx->occ_interp != ctx->interp)) {
+        int bs = 8;
+        ctx->sv_size = bs;
+        int gx = (ctx->nx + bs - 1) / bs, gy = (ctx->ny + bs - 1) / bs, gz = (ctx->nz + bs - 1) / bs;
+        VPT_CHECK_CUDA(ctx, ctx->occupancy.alloc((size_t)gx * gy * gz));
+        int halo = ctx->interp == VPT_INTERP_NEAREST ? 0 : 1;
+        VPT_CHECK_CUDA(ctx, vpt::launch_occupancy(ctx->norm.ptr, ctx->nx, ctx->ny, ctx->nz, bs, gx, gy, gz, halo, 0.0f,
+                                                  ctx->ess_ref_compat, ctx->occupancy.ptr, s));
+        ctx->occ_valid = true;
+        ctx->occ_interp = ctx->interp;
+        ctx->sv_kind = -1;  // sv_size now refers to the occupancy grid
+    }
+    return VPT_OK;
+}
+
+void compute_view(const VptContext* ctx, double* view) {
+    if (ctx->view_overridden) {
+        memcpy(view, ctx->view, sizeof(ctx->view));
+    } else {
+        double e[3] = {ctx->cam_pos[0], ctx->cam_pos[1], ctx->cam_pos[2]};
+        double f[3] = {ctx->cam_target[0] - e[0], ctx->cam_target[1] - e[1], ctx->cam_target[2] - e[2]};
+        double fl = sqrt(f[0] * f[0] + f[1] * f[1] + f[2] * f[2]);
+        for (double& v : f) v /= fl;
+        double u0[3] = {ctx->cam_up[0], ctx->cam_up[1], ctx->cam_up[2]};
+        double s[3] = {f[1] * u0[2] - f[2] * u0[1], f[2] * u0[0] - f[0] * u0[2], f[0] * u0[1] - f[1] * u0[0]};
+        double sl = sqrt(s[0] * s[0] + s[1] * s[1] + s[2] * s[2]);
+        for (double& v : s) v /= sl;
+        double u[3] = {s[1] * f[2] - s[2] * f[1], s[2] * f[0] - s[0] * f[2], s[0] * f[1] - s[1] * f[0]};
+        double m[16] = {s[0], u[0], -f[0], 0.0, s[1], u[1], -f[1], 0.0, s[2], u[2], -f[2], 0.0,
+                        -(s[0] * e[0] + s[1] * e[1] + s[2] * e[2]), -(u[0] * e[0] + u[1] * e[1] + u[2] * e[2]),
+                        (f[0] * e[0] + f[1] * e[1] + f[2] * e[2]), 1.0};
+        memcpy(view, m, sizeof(m));
+    }
+}
+
+void compute_camera(const VptContext* ctx, double* vp_out, double* inv_out) {
+    double view[16];
+    compute_view(ctx, view);
+    double aspect = (ctx->width > 0 && ctx->height > 0) ? double(ctx->width) / double(ctx->height) : 1.0;
+    double th = tan(double(ctx->fovy) / 2.0);
+    double n = ctx->near_dist, fa = ctx->far_dist;
+    double proj[16] = {0};
+    proj[0] = 1.0 / (aspect * th);
+    proj[5] = -1.0 / th;  // y flipped: image row 0 is the top of the picture
+    proj[10] = fa / (n - fa);
+    proj[11] = -1.0;
+    proj[14] = -(fa * n) / (fa - n);
+    mat_mul(proj, view, vp_out);
+    mat_inverse(vp_out, inv_out);
+}
+
+VptStatus fill_params(VptContext* ctx, int tracker, int frames, vpt::TraceParams& P) {
+    memset(&P, 0, sizeof(P));
+    double vp[16], inv[16];
+    compute_camera(ctx, vp, inv);
+    for (int i = 0; i < 16; i++) {
+        P.inv_view_proj[i] = float(inv[i]);
+        P.prev_view_proj[i] = float(vp[i]);
+    }
+    P.width = ctx->width;
+    P.height = ctx->height;
+    P.frame_count = ctx->frame_count;
+    P.global_frame = ctx->frame_count;
+    P.num_frames = (uint32_t)frames;
+    P.seed_offset = ctx->seed_offset;
+    P.num_paths = (uint64_t)ctx->width * ctx->height * (uint64_t)frames;
+    P.box_min = mk(ctx->box_min[0], ctx->box_min[1], ctx->box_min[2]);
+    P.box_max = mk(ctx->box_max[0], ctx->box_max[1], ctx->box_max[2]);
+    P.nx = ctx->nx;
+    P.ny = ctx->ny;
+    P.nz = ctx->nz;
+    P.vox_per_unit = mk(float(double(ctx->nx) / (double(ctx->box_max[0]) - double(ctx->box_min[0]))),
+                        float(double(ctx->ny) / (double(ctx->box_max[1]) - double(ctx->box_min[1]))),
+                        float(double(ctx->nz) / (double(ctx->box_max[2]) - double(ctx->box_min[2]))));
+    P.border_density = (0.0f - ctx->vmin) / (ctx->vmax - ctx->vmin);
+    P.extinction = extinction_x(ctx);
+    P.inv_extinction = 1.0f / P.extinction;
+    P.albedo = ctx->albedo[0];
+    P.absorb_albedo = 1.0f - ctx->albedo[0];
+    P.g = ctx->g;
+    P.interp = ctx->interp;
+    P.max_bounces = ctx->max_bounces;
+    P.max_steps = ctx->max_steps;
+    P.ess_ref_compat = ctx->ess_ref_compat;
+    P.sv_size = ctx->sv_size;
+    P.svx = (ctx->nx + ctx->sv_size - 1) / ctx->sv_size;
+    P.svy = (ctx->ny + ctx->sv_size - 1) / ctx->sv_size;
+    P.svz = (ctx->nz + ctx->sv_size - 1) / ctx->sv_size;
+    for (int a = 0; a < 3; a++) {
+        float delta = ctx->box_max[a] - ctx->box_min[a];
+        int n = a == 0 ? ctx->nx : (a == 1 ? ctx->ny : ctx->nz);
+        float v = (float(ctx->sv_size) * delta) / float(n);
+        if (a == 0) P.sv_world.x = v;
+        if (a == 1) P.sv_world.y = v;
+        if (a == 2) P.sv_world.z = v;
+    }
+    P.env_kind = ctx->env_kind;
+    P.use_linear_rgb = ctx->use_linear_rgb;
+    P.env_image_linear = ctx->env_image_linear;
+    P.sun_dir = mk(ctx->sun_dir[0], ctx->sun_dir[1], ctx->sun_dir[2]);
+    P.sun_intensity = mk(ctx->sun_intensity[0], ctx->sun_intensity[1], ctx->sun_intensity[2]);
+    P.sky_color = mk(ctx->sky_color[0], ctx->sky_color[1], ctx->sky_color[2]);
+    P.env_intensity = mk(ctx->env_intensity[0], ctx->env_intensity[1], ctx->env_intensity[2]);
+    P.env_is_black = ctx->env_kind == VPT_ENV_BLACK || (ctx->env_kind == VPT_ENV_IMAGE && ctx->env_image_black);
+    P.env_w = ctx->env_w;
+    P.env_h = ctx->env_h;
+    P.env_levels = ctx->env_levels;
+    P.env_base_res = 1 << ctx->env_levels;
+    P.density = ctx->norm.ptr;
+    P.sv_data = ctx->sv_pairs.ptr;
+    P.occupancy = ctx->occupancy.ptr;
+    P.env_rgba = ctx->env_rgba.ptr;
+    P.env_pyramid = ctx->env_pyramid.ptr;
+    P.env_level_offset = ctx->env_offsets.ptr;
+    P.film = ctx->film.ptr;
+    P.film_sq = ctx->collect_stats ? ctx->film_sq.ptr : nullptr;
+    P.feat = features_needed(ctx) ? ctx->feat.ptr : nullptr;
+    P.counters = ctx->counters.ptr;
+    P.error_flags = ctx->error_flags.ptr;
+    P.work_counter = ctx->work_counter.ptr;
+    (void)tracker;
+    return VPT_OK;
+}
+
+// Feature accumulators are written when the user asked for feature maps or a denoiser needs them
+// (the reference creates the maps a denoiser requests, VolumetricPathTracingPass.cpp:231-293).
+bool features_needed(const VptContext* ctx) {
+    return ctx->features_on || ctx->denoiser == VPT_DENOISER_SVGF ||
+           (ctx->denoiser == VPT_DENOISER_EAW && ctx->eaw.iterations > 0);
+}
+
+VptStatus ensure_film(VptContext* ctx, cudaStream_t s) {
+    size_t n = (size_t)ctx->width * ctx->height;
+    if (ctx->film.count != n * 3) {
+        VPT_CHECK_CUDA(ctx, ctx->film.alloc(n * 3));
+        reset_film_state(ctx);
+    }
+    if (ctx->collect_stats && ctx->film_sq.count != n * 3) {
+        VPT_CHECK_CUDA(ctx, ctx->film_sq.alloc(n * 3));
+        reset_film_state(ctx);
+    }
+    if (features_needed(ctx) && ctx->feat.count != n * vpt::kFeatStride) {
+        VPT_CHECK_CUDA(ctx, ctx->feat.alloc(n * vpt::kFeatStride));
+        reset_film_state(ctx);
+    }
+    if (ctx->film_frames == 0) {
+        VPT_CHECK_CUDA(ctx, cudaMemsetAsync(ctx->film.ptr, 0, n * 3 * sizeof(double), s));
+        if (ctx->collect_stats) VPT_CHECK_CUDA(ctx, cudaMemsetAsync(ctx->film_sq.ptr, 0, n * 3 * sizeof(double), s));
+        if (features_needed(ctx))
+            VPT_CHECK_CUDA(ctx, cudaMemsetAsync(ctx->feat.ptr, 0, n * vpt::kFeatStride * sizeof(float), s));
+    }
+    return VPT_OK;
+}
+
+bool parse_float(const char* v, float& out) {
+    char* end = nullptr;
+    out = strtof(v, &end);
+    return end && end != v;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* vpt_status_string(int status) {
+    switch (status) {
+        case VPT_OK: return "ok";
+        case VPT_ERR_ARG: return "invalid argument";
+        case VPT_ERR_CUDA: return "CUDA error";
+        case VPT_ERR_OOM: return "out of device memory";
+        case VPT_ERR_ITER_LIMIT: return "iteration guard reached";
+        case VPT_ERR_STATE: return "invalid state";
+        case VPT_ERR_UNSUPPORTED: return "unsupported";
+        default: return "unknown status";
+    }
+}
+
+int vpt_abi_version(void) { return VPT_B200_ABI_VERSION; }
+
+uint64_t vpt_kernel_launch_count(void) { return vpt::launch_count(); }
+
+VptStatus vpt_create(VptContext** out_ctx, int cuda_device) {
+    if (!out_ctx) return VPT_ERR_ARG;
+    *out_ctx = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) return VPT_ERR_CUDA;
+    if (cuda_device < 0 || cuda_device >= count) return VPT_ERR_ARG;
+    if (cudaSetDevice(cuda_device) != cudaSuccess) return VPT_ERR_CUDA;
+    VptContext* ctx = new VptContext();
+    ctx->device = cuda_device;
+    cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, cuda_device);
+    // sunlightDirection = normalize(0.5826, 0.7660, 0.2717) (VolumetricPathTracingPass.hpp:319)
+    float d[3] = {0.5826f, 0.7660f, 0.2717f};
+    float l = sqrtf(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+    for (int i = 0; i < 3; i++) ctx->sun_dir[i] = d[i] / l;
+    if (ctx->counters.alloc(4) != cudaSuccess || ctx->error_flags.alloc(1) != cudaSuccess ||
+        ctx->work_counter.alloc(2) != cudaSuccess) {
+        delete ctx;
+        return VPT_ERR_OOM;
+    }
+    cudaMemset(ctx->counters.ptr, 0, 4 * sizeof(unsigned long long));
+    cudaMemset(ctx->error_flags.ptr, 0, sizeof(int));
+    *out_ctx = ctx;
+    return VPT_OK;
+}
+
+void vpt_destroy(VptContext* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    cudaDeviceSynchronize();
+    ctx->raw.release();
+    ctx->norm.release();
+    ctx->minmax.release();
+    ctx->sv_min.release();
+    ctx->sv_max.release();
+    ctx->sv_avg.release();
+    ctx->sv_pairs.release();
+    ctx->sv_occ.release();
+    ctx->occupancy.release();
+    ctx->env_rgba.release();
+    ctx->env_pyramid.release();
+    ctx->env_offsets.release();
+    ctx->film.release();
+    ctx->film_sq.release();
+    ctx->feat.release();
+    ctx->rgba_src.release();
+    ctx->eaw_maps.release();
+    ctx->rgba_a.release();
+    ctx->rgba_b.release();
+    ctx->staging.release();
+    ctx->counters.release();
+    ctx->error_flags.release();
+    ctx->work_counter.release();
+    vpt::svgf_release(ctx->svgf_state);
+    delete ctx;
+}
+
+const char* vpt_last_error(const VptContext* ctx) { return ctx ? ctx->last_error.c_str() : "null context"; }
+
+VptStatus vpt_set_dense_grid(VptContext* ctx, const float* data, int nx, int ny, int nz, int data_on_device) {
+    VPT_CHECK_CTX(ctx);
+    if (!data || nx <= 0 || ny <= 0 || nz <= 0) return fail(ctx, VPT_ERR_ARG, "vpt_set_dense_grid: bad grid");
+    cudaSetDevice(ctx->device);
+    size_t n = (size_t)nx * ny * nz;
+    VPT_CHECK_CUDA(ctx, ctx->raw.alloc(n));
+    VPT_CHECK_CUDA(ctx, cudaMemcpy(ctx->raw.ptr, data, n * sizeof(float),
+                                   data_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice));
+    ctx->nx = nx;
+    ctx->ny = ny;
+    ctx->nz = nz;
+    return finish_grid(ctx, 0);
+}
+
+VptStatus vpt_generate_fbm_grid(VptContext* ctx, int nx, int ny, int nz, uint32_t seed, int octaves, float lacunarity,
+                                float gain, float base_frequency, float threshold) {
+    VPT_CHECK_CTX(ctx);
+    if (nx <= 0 || ny <= 0 || nz <= 0 || octaves <= 0 || octaves > 16)
+        return fail(ctx, VPT_ERR_ARG, "vpt_generate_fbm_grid: bad size or octave count");
+    cudaSetDevice(ctx->device);
+    size_t n = (size_t)nx * ny * nz;
+    VPT_CHECK_CUDA(ctx, ctx->raw.alloc(n));
+    int perm[512];
+    make_permutation(seed, perm);
+    vpt::FbmParams fp;
+    fp.octaves = octaves;
+    fp.lacunarity = lacunarity;
+    fp.gain = gain;
+    fp.base_frequency = base_frequency;
+    fp.threshold = threshold;
+    fp.contrast = 3.5f;  // 0.5 + 3.5 * fbm, clamped: ~35% of voxels below 0.3 at base frequency 3
+    fp.inv_max_dim = 1.0f / float(std::max(nx, std::max(ny, nz)));
+    VPT_CHECK_CUDA(ctx, vpt::launch_fbm(ctx->raw.ptr, nx, ny, nz, perm, fp, 0));
+    ctx->nx = nx;
+    ctx->ny = ny;
+    ctx->nz = nz;
+    return finish_grid(ctx, 0);
+}
+
+VptStatus vpt_get_dense_grid(VptContext* ctx, float* out, int out_on_device) {
+    VPT_CHECK_CTX(ctx);
+    if (!ctx->raw.ptr) return fail(ctx, VPT_ERR_STATE, "no dense grid");
+    if (!out) return fail(ctx, VPT_ERR_ARG, "null output");
+    size_t n = (size_t)ctx->nx * ctx->ny * ctx->nz;
+    VPT_CHECK_CUDA(ctx, cudaMemcpy(out, ctx->raw.ptr, n * sizeof(float),
+                                   out_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost));
+    return VPT_OK;
+}
+
+VptStatus vpt_set_voxel_size(VptContext* ctx, double sx, double sy, double sz) {
+    VPT_CHECK_CTX(ctx);
+    if (!(sx > 0.0 && sy > 0.0 && sz > 0.0)) return fail(ctx, VPT_ERR_ARG, "voxel sizes must be > 0");
+    ctx->pending_voxel_size[0] = float(sx);
+    ctx->pending_voxel_size[1] = float(sy);
+    ctx->pending_voxel_size[2] = float(sz);
+    return VPT_OK;
+}
+
+VptStatus vpt_set_max_grid_extent(VptContext* ctx, float e) {
+    VPT_CHECK_CTX(ctx);
+    if (!(e > 0.0f)) return fail(ctx, VPT_ERR_ARG, "max grid extent must be > 0");
+    ctx->max_grid_extent = e;
+    return VPT_OK;
+}
+
+VptStatus vpt_get_render_bounding_box(VptContext* ctx, float out[6]) {
+    VPT_CHECK_CTX(ctx);
+    if (!out) return VPT_ERR_ARG;
+    for (int i = 0; i < 3; i++) {
+        out[i] = ctx->box_min[i];
+        out[3 + i] = ctx->box_max[i];
+    }
+    return VPT_OK;
+}
+
+VptStatus vpt_set_vpt_mode(VptContext* ctx, int mode) {
+    VPT_CHECK_CTX(ctx);
+    if (mode < 0 || mode > VPT_MODE_RAY_MARCHING_EMISSION_ABSORPTION)
+        return fail(ctx, VPT_ERR_ARG, "unknown VptMode");
+    if (tracker_of(mode) < 0) return fail(ctx, VPT_ERR_UNSUPPORTED, "VptMode not built in this core");
+    if (mode != ctx->mode) reset_film_state(ctx);
+    ctx->mode = mode;
+    return VPT_OK;
+}
+
+VptStatus vpt_set_grid_interpolation(VptContext* ctx, int interpolation) {
+    VPT_CHECK_CTX(ctx);
+    if (interpolation < 0 || interpolation > 2) return fail(ctx, VPT_ERR_ARG, "unknown interpolation");
+    if (interpolation != ctx->interp) reset_film_state(ctx);
+    ctx->interp = interpolation;
+    return VPT_OK;
+}
+
+VptStatus vpt_set_extinction_scale(VptContext* ctx, float scale) {
+    VPT_CHECK_CTX(ctx);
+    ctx->extinction_scale = scale;
+    reset_film_state(ctx);
+    return VPT_OK;
+}
+
+VptStatus vpt_set_extinction_base(VptContext* ctx, const float rgb[3]) {
+    VPT_CHECK_CTX(ctx);
+    if (!rgb) return VPT_ERR_ARG;
+    memcpy(ctx->extinction_base, rgb, sizeof(float) * 3);
+    reset_film_state(ctx);
+    return VPT_OK;
+}
+
+VptStatus vpt_set_scattering_albedo(VptContext* ctx, const float rgb[3]) {
+    VPT_CHECK_CTX(ctx);
+    if (!rgb) return VPT_ERR_ARG;
+    memcpy(ctx->albedo, rgb, sizeof(float) * 3);
+    reset_film_state(ctx);
+    return VPT_OK;
+}
+
+VptStatus vpt_set_phase_g(VptContext* ctx, float g) {
+    VPT_CHECK_CTX(ctx);
+    ctx->g = g;
+    reset_film_state(ctx);
+    return VPT_OK;
+}
+
+VptStatus vpt_set_seed_offset(VptContext* ctx, uint32_t offset) {
+    VPT_CHECK_CTX(ctx);
+    ctx->seed_offset = offset;
+    reset_film_state(ctx);
+    return VPT_OK;
+}
+
+VptStatus vpt_set_use_linear_rgb(VptContext* ctx, int v) {
+    VPT_CHECK_CTX(ctx);
+    ctx->use_linear_rgb = v ? 1 : 0;
+    reset_film_state(ctx);
+    return VPT_OK;
+}
+
+VptStatus vpt_set_max_bounces(VptContext* ctx, int max_bounces) {
+    VPT_CHECK_CTX(ctx);
+    if (max_bounces < 0) return fail(ctx, VPT_ERR_ARG, "max_bounces must be >= 0");
+    ctx->max_bounces = max_bounces;
+    reset_film_state(ctx);
+    return VPT_OK;
+}
+
+VptStatus vpt_set_builtin_environment_map(VptContext* ctx, int env_kind) {
+    VPT_CHECK_CTX(ctx);
+    if (env_kind < 0 || env_kind > VPT_ENV_CONSTANT_SUN) return fail(ctx, VPT_ERR_ARG, "unknown builtin environment map");
+    ctx->env_kind = env_kind;
+    reset_film_state(ctx);
+    return VPT_OK;
+}
+
+VptStatus vpt_set_environment_map_intensity_rgb(VptContext* ctx, const float rgb[3]) {
+    VPT_CHECK_CTX(ctx);
+    if (!rgb) return VPT_ERR_ARG;
+    memcpy(ctx->env_intensity, rgb, sizeof(float) * 3);
+    reset_film_state(ctx);
+    return VPT_OK;
+}
+
+VptStatus vpt_set_sun(VptContext* ctx, const float direction[3], const float intensity_rgb[3]) {
+    VPT_CHECK_CTX(ctx);
+    if (direction) {
+        float l = sqrtf(direction[0] * direction[0] + direction[1] * direction[1] + direction[2] * direction[2]);
+        if (!(l > 0.0f)) return fail(ctx, VPT_ERR_ARG, "sun direction must be non-zero");
+        for (int i = 0; i < 3; i++) ctx->sun_dir[i] = direction[i] / l;
+    }
+    if (intensity_rgb) memcpy(ctx->sun_intensity, intensity_rgb, sizeof(float) * 3);
+    reset_film_state(ctx);
+    return VPT_OK;
+}
+
+VptStatus vpt_set_sky_color(VptContext* ctx, const float rgb[3]) {
+    VPT_CHECK_CTX(ctx);
+    if (!rgb) return VPT_ERR_ARG;
+    memcpy(ctx->sky_color, rgb, sizeof(float) * 3);
+    reset_film_state(ctx);
+    return VPT_OK;
+}
+
+VptStatus vpt_load_environment_map_rgba(VptContext* ctx, const float* rgba, int width, int height, int is_linear_rgb,
+                                        int data_on_device) {
+    VPT_CHECK_CTX(ctx);
+    if (!rgba || width <= 0 || height <= 0) return fail(ctx, VPT_ERR_ARG, "bad environment image");
+    cudaSetDevice(ctx->device);
+    size_t n = (size_t)width * height * 4;
+    VPT_CHECK_CUDA(ctx, ctx->env_rgba.alloc(n));
+    VPT_CHECK_CUDA(ctx, cudaMemcpy(ctx->env_rgba.ptr, rgba, n * sizeof(float),
+                                   data_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice));
+    // computeIsImageBlack (VolumetricPathTracingPass.cpp:1358-1374)
+    std::vector<float> host(n);
+    VPT_CHECK_CUDA(ctx, cudaMemcpy(host.data(), ctx->env_rgba.ptr, n * sizeof(float), cudaMemcpyDeviceToHost));
+    bool black = true;
+    for (size_t i = 0; i < (size_t)width * height && black; i++)
+        if (host[i * 4] != 0.0f || host[i * 4 + 1] != 0.0f || host[i * 4 + 2] != 0.0f) black = false;
+    ctx->env_image_black = black ? 1 : 0;
+    ctx->env_w = width;
+    ctx->env_h = height;
+    ctx->env_image_linear = is_linear_rgb ? 1 : 0;
+    const int levels = ctx->env_levels;  // createEnvironmentMapOctahedralTexture(12)
+    ctx->env_offsets_host.assign(levels, 0);
+    uint64_t off = 0;
+    for (int l = 0; l < levels; l++) {
+        ctx->env_offsets_host[l] = off;
+        uint64_t r = (uint64_t)1 << (levels - l);
+        off += r * r;
+    }
+    VPT_CHECK_CUDA(ctx, ctx->env_pyramid.alloc(off));
+    VPT_CHECK_CUDA(ctx, ctx->env_offsets.alloc(levels));
+    VPT_CHECK_CUDA(ctx, cudaMemcpy(ctx->env_offsets.ptr, ctx->env_offsets_host.data(), levels * sizeof(uint64_t),
+                                   cudaMemcpyHostToDevice));
+    ctx->env_kind = VPT_ENV_IMAGE;
+    vpt::TraceParams P;
+    fill_params(ctx, 0, 1, P);
+    VPT_CHECK_CUDA(ctx, vpt::launch_env_pyramid(P, ctx->env_pyramid.ptr, ctx->env_offsets_host.data(), levels, 0));
+    VPT_CHECK_CUDA(ctx, cudaDeviceSynchronize());
+    reset_film_state(ctx);
+    return VPT_OK;
+}
+
+VptStatus vpt_set_camera(VptContext* ctx, const float position[3], const float target[3], const float up[3],
+                         float fovy_radians, float near_dist, float far_dist) {
+    VPT_CHECK_CTX(ctx);
+    if (!position || !target || !up || !(fovy_radians > 0.0f) || !(near_dist > 0.0f) || !(far_dist > near_dist))
+        return fail(ctx, VPT_ERR_ARG, "bad camera");
+    memcpy(ctx->cam_pos, position, sizeof(float) * 3);
+    memcpy(ctx->cam_target, target, sizeof(float) * 3);
+    memcpy(ctx->cam_up, up, sizeof(float) * 3);
+    ctx->fovy = fovy_radians;
+    ctx->near_dist = near_dist;
+    ctx->far_dist = far_dist;
+    ctx->view_overridden = false;
+    reset_film_state(ctx);
+    return VPT_OK;
+}
+
+VptStatus vpt_set_view_matrix(VptContext* ctx, const float view[16]) {
+    VPT_CHECK_CTX(ctx);
+    if (!view) return VPT_ERR_ARG;
+    for (int i = 0; i < 16; i++) ctx->view[i] = view[i];
+    ctx->view_overridden = true;
+    reset_film_state(ctx);
+    return VPT_OK;
+}
+
+VptStatus vpt_get_camera_matrices(VptContext* ctx, float inv_view_proj[16], float view_proj[16]) {
+    VPT_CHECK_CTX(ctx);
+    double vp[16], inv[16];
+    compute_camera(ctx, vp, inv);
+    for (int i = 0; i < 16; i++) {
+        if (inv_view_proj) inv_view_proj[i] = float(inv[i]);
+        if (view_proj) view_proj[i] = float(vp[i]);
+    }
+    return VPT_OK;
+}
+
+VptStatus vpt_set_resolution(VptContext* ctx, int width, int height) {
+    VPT_CHECK_CTX(ctx);
+    if (width <= 0 || height <= 0 || width > 16384 || height > 16384)
+        return fail(ctx, VPT_ERR_ARG, "resolution out of range");
+    if (width != ctx->width || height != ctx->height) {
+        ctx->width = width;
+        ctx->height = height;
+        reset_film_state(ctx);
+        vpt::svgf_release(ctx->svgf_state);
+    }
+    return VPT_OK;
+}
+
+VptStatus vpt_reset_accumulation(VptContext* ctx) {
+    VPT_CHECK_CTX(ctx);
+    reset_film_state(ctx);
+    return VPT_OK;
+}
+
+VptStatus vpt_render_frames(VptContext* ctx, int frames, void* stream) {
+    VPT_CHECK_CTX(ctx);
+    if (frames <= 0) return fail(ctx, VPT_ERR_ARG, "frames must be > 0");
+    if (!ctx->norm.ptr) return fail(ctx, VPT_ERR_STATE, "no volume loaded");
+    if (ctx->width <= 0) return fail(ctx, VPT_ERR_STATE, "resolution not set");
+    int tracker = tracker_of(ctx->mode);
+    if (tracker < 0) return fail(ctx, VPT_ERR_UNSUPPORTED, "VptMode not built in this core");
+    if (ctx->env_kind == VPT_ENV_IMAGE && !ctx->env_pyramid.ptr)
+        return fail(ctx, VPT_ERR_STATE, "environment image not loaded");
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = as_stream(stream);
+    VptStatus st = ensure_accel(ctx, tracker, s);
+    if (st != VPT_OK) return st;
+    // SVGF wants the last 1-spp frame (DISABLE_ACCUMULATION, VolumetricPathTracingPass.cpp:1665-1667):
+    // earlier frames of the call only advance the frame counter, so only the last one is traced.
+    const bool single = ctx->denoiser == VPT_DENOISER_SVGF;
+    if (single) ctx->film_frames = 0;
+    st = ensure_film(ctx, s);
+    if (st != VPT_OK) return st;
+    vpt::TraceParams P;
+    fill_params(ctx, tracker, single ? 1 : frames, P);
+    if (single) {
+        P.frame_count = ctx->frame_count + (uint32_t)frames - 1u;
+        P.global_frame = P.frame_count;
+    }
+    if (tracker == vpt::kDecomposition || tracker == vpt::kResidualRatio) {
+        P.sv_size = ctx->sv_size;
+        P.svx = ctx->svx;
+        P.svy = ctx->svy;
+        P.svz = ctx->svz;
+    }
+    int pb = 0;  // 0: persistent grid sized by the occupancy calculator
+    if (ctx->schedule == vpt::kSchedulePersistent && ctx->persistent_blocks_per_sm > 0) {
+        pb = ctx->persistent_blocks_per_sm * ctx->num_sms;
+    }
+    VPT_CHECK_CUDA(ctx, vpt::launch_trace(P, tracker, ctx->use_ess, ctx->schedule, P.feat ? 1 : 0, pb, s));
+    ctx->frame_count += (uint32_t)frames;
+    ctx->film_frames += single ? 1u : (uint32_t)frames;
+    ctx->frames_total += (uint64_t)frames;
+    return VPT_OK;
+}
+
+VptStatus vpt_read_result(VptContext* ctx, float* out, int channels, int out_on_device, void* stream) {
+    VPT_CHECK_CTX(ctx);
+    if (!out || (channels != 3 && channels != 4)) return fail(ctx, VPT_ERR_ARG, "channels must be 3 or 4");
+    if (ctx->film_frames == 0 || !ctx->film.ptr) return fail(ctx, VPT_ERR_STATE, "nothing rendered yet");
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = as_stream(stream);
+    int n = ctx->width * ctx->height;
+    float* dst = out;
+    if (!out_on_device) {
+        VPT_CHECK_CUDA(ctx, ctx->staging.alloc((size_t)n * 4));
+        dst = ctx->staging.ptr;
+    }
+    double inv = 1.0 / double(ctx->film_frames);
+    bool denoise = (ctx->denoiser == VPT_DENOISER_EAW && ctx->eaw.iterations > 0) ||
+                   ctx->denoiser == VPT_DENOISER_SVGF;
+    if (!denoise) {
+        VPT_CHECK_CUDA(ctx, vpt::launch_film_to_chw(ctx->film.ptr, ctx->width, ctx->height, inv, channels, dst, s));
+    } else {
+        VPT_CHECK_CUDA(ctx, ctx->rgba_src.alloc((size_t)n * 4));
+        VPT_CHECK_CUDA(ctx, ctx->rgba_a.alloc((size_t)n * 4));
+        VPT_CHECK_CUDA(ctx, ctx->rgba_b.alloc((size_t)n * 4));
+        VPT_CHECK_CUDA(ctx, vpt::launch_film_to_rgba(ctx->film.ptr, n, inv, ctx->rgba_src.ptr, s));
+        const float* feat = ctx->feat.count ? ctx->feat.ptr : nullptr;
+        float* result = nullptr;
+        cudaError_t e;
+        if (ctx->denoiser == VPT_DENOISER_EAW) {
+            VPT_CHECK_CUDA(ctx, ctx->eaw_maps.alloc((size_t)n * 8));
+            e = vpt::eaw_denoise_features(ctx->rgba_src.ptr, feat, ctx->film_frames, ctx->width, ctx->height, ctx->eaw,
+                                          ctx->eaw_maps.ptr, ctx->rgba_a.ptr, ctx->rgba_b.ptr, &result, s);
+        } else {
+            double vp[16], inv_vp[16];
+            compute_camera(ctx, vp, inv_vp);
+            double view[16], iv[16];
+            compute_view(ctx, view);
+            mat_inverse(view, iv);
+            for (int r = 0; r < 4; r++)
+                for (int c = 0; c < 4; c++) ctx->svgf.inv_transposed_view[c * 4 + r] = float(iv[r * 4 + c]);
+            for (int i = 0; i < 16; i++)
+                ctx->svgf.prev_view_proj[i] = float(ctx->has_prev_view_proj ? ctx->prev_view_proj[i] : vp[i]);
+            ctx->svgf.far_dist = ctx->far_dist;
+            e = vpt::svgf_denoise_features(ctx->rgba_src.ptr, feat, ctx->film_frames, ctx->width, ctx->height, ctx->svgf,
+                                           ctx->svgf_state, ctx->rgba_b.ptr, &result, s);
+            // setPreviousViewProjMatrix(current) at the end of _render (VolumetricPathTracingPass.cpp:2421)
+            memcpy(ctx->prev_view_proj, vp, sizeof(vp));
+            ctx->has_prev_view_proj = true;
+        }
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "denoise");
+        VPT_CHECK_CUDA(ctx, vpt::launch_rgba_to_chw(result, n, channels, dst, s));
+    }
+    if (!out_on_device) {
+        VPT_CHECK_CUDA(ctx, cudaMemcpyAsync(out, dst, (size_t)n * channels * sizeof(float), cudaMemcpyDeviceToHost, s));
+        VPT_CHECK_CUDA(ctx, cudaStreamSynchronize(s));
+    }
+    return VPT_OK;
+}
+
+VptStatus vpt_render_frame(VptContext* ctx, int frames, float* out, int channels, int out_on_device, void* stream) {
+    VptStatus st = vpt_render_frames(ctx, frames, stream);
+    if (st != VPT_OK) return st;
+    return vpt_read_result(ctx, out, channels, out_on_device, stream);
+}
+
+VptStatus vpt_set_collect_statistics(VptContext* ctx, int enabled) {
+    VPT_CHECK_CTX(ctx);
+    bool e = enabled != 0;
+    if (e != ctx->collect_stats) reset_film_state(ctx);
+    ctx->collect_stats = e;
+    return VPT_OK;
+}
+
+VptStatus vpt_read_statistics(VptContext* ctx, double* out_sum, double* out_sum_sq, int out_on_device, void* stream) {
+    VPT_CHECK_CTX(ctx);
+    if (!ctx->film.ptr || ctx->film_frames == 0) return fail(ctx, VPT_ERR_STATE, "nothing rendered yet");
+    cudaStream_t s = as_stream(stream);
+    size_t n = (size_t)ctx->width * ctx->height * 3;
+    cudaMemcpyKind k = out_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    if (out_sum) VPT_CHECK_CUDA(ctx, cudaMemcpyAsync(out_sum, ctx->film.ptr, n * sizeof(double), k, s));
+    if (out_sum_sq) {
+        if (!ctx->collect_stats) return fail(ctx, VPT_ERR_STATE, "statistics collection is off");
+        VPT_CHECK_CUDA(ctx, cudaMemcpyAsync(out_sum_sq, ctx->film_sq.ptr, n * sizeof(double), k, s));
+    }
+    VPT_CHECK_CUDA(ctx, cudaStreamSynchronize(s));
+    return VPT_OK;
+}
+
+VptStatus vpt_set_use_feature_maps(VptContext* ctx, const int* features, int count) {
+    VPT_CHECK_CTX(ctx);
+    bool on = false;
+    for (int i = 0; i < count; i++)
+        if (features && features[i] != VPT_FEATURE_RESULT) on = true;
+    if (on != ctx->features_on) reset_film_state(ctx);
+    ctx->features_on = on;
+    return VPT_OK;
+}
+
+VptStatus vpt_get_feature_map(VptContext* ctx, int feature, float* out, int channels, int out_on_device, void* stream) {
+    VPT_CHECK_CTX(ctx);
+    if (feature == VPT_FEATURE_RESULT) return vpt_read_result(ctx, out, channels, out_on_device, stream);
+    if (!features_needed(ctx) || !ctx->feat.ptr || ctx->film_frames == 0)
+        return fail(ctx, VPT_ERR_STATE, "feature maps are not enabled or nothing rendered");
+    if (!out || channels < 1 || channels > 4) return fail(ctx, VPT_ERR_ARG, "bad output");
+    cudaStream_t s = as_stream(stream);
+    int n = ctx->width * ctx->height;
+    float* dst = out;
+    if (!out_on_device) {
+        VPT_CHECK_CUDA(ctx, ctx->staging.alloc((size_t)n * 4));
+        dst = ctx->staging.ptr;
+    }
+    cudaError_t e = vpt::feature_to_chw(ctx->feat.ptr, n, ctx->film_frames, feature, channels, ctx->albedo, dst, s);
+    if (e == cudaErrorInvalidValue) return fail(ctx, VPT_ERR_ARG, "feature map not supported");
+    VPT_CHECK_CUDA(ctx, e);
+    if (!out_on_device) {
+        VPT_CHECK_CUDA(ctx, cudaMemcpyAsync(out, dst, (size_t)n * channels * sizeof(float), cudaMemcpyDeviceToHost, s));
+        VPT_CHECK_CUDA(ctx, cudaStreamSynchronize(s));
+    }
+    return VPT_OK;
+}
+
+VptStatus vpt_get_stats(VptContext* ctx, VptStats* stats) {
+    VPT_CHECK_CTX(ctx);
+    if (!stats) return VPT_ERR_ARG;
+    unsigned long long c[4];
+    int flags = 0;
+    VPT_CHECK_CUDA(ctx, cudaMemcpy(c, ctx->counters.ptr, sizeof(c), cudaMemcpyDeviceToHost));
+    VPT_CHECK_CUDA(ctx, cudaMemcpy(&flags, ctx->error_flags.ptr, sizeof(int), cudaMemcpyDeviceToHost));
+    stats->paths = c[0];
+    stats->density_lookups = c[1];
+    stats->frames = ctx->film_frames;
+    stats->error_flags = flags;
+    stats->reserved = 0;
+    return VPT_OK;
+}
+
+VptStatus vpt_reset_stats(VptContext* ctx) {
+    VPT_CHECK_CTX(ctx);
+    VPT_CHECK_CUDA(ctx, cudaMemset(ctx->counters.ptr, 0, 4 * sizeof(unsigned long long)));
+    VPT_CHECK_CUDA(ctx, cudaMemset(ctx->error_flags.ptr, 0, sizeof(int)));
+    return VPT_OK;
+}
+
+VptStatus vpt_synchronize(VptContext* ctx, void* stream) {
+    VPT_CHECK_CTX(ctx);
+    VPT_CHECK_CUDA(ctx, cudaStreamSynchronize(as_stream(stream)));
+    int flags = 0;
+    VPT_CHECK_CUDA(ctx, cudaMemcpy(&flags, ctx->error_flags.ptr, sizeof(int), cudaMemcpyDeviceToHost));
+    if (flags & vpt::kErrIterLimit) return fail(ctx, VPT_ERR_ITER_LIMIT, "a path reached the iteration guard");
+    return VPT_OK;
+}
+
+VptStatus vpt_set_denoiser(VptContext* ctx, int denoiser_type) {
+    VPT_CHECK_CTX(ctx);
+    if (denoiser_type < VPT_DENOISER_NONE || denoiser_type > VPT_DENOISER_SVGF)
+        return fail(ctx, VPT_ERR_ARG, "unknown denoiser");
+    ctx->denoiser = denoiser_type;
+    // setDenoiserType clears the settings (VolumetricPathTracingModuleRenderer.cpp:255-261).
+    ctx->eaw = vpt::EawSettings();
+    ctx->svgf = vpt::SvgfSettings();
+    vpt::svgf_release(ctx->svgf_state);
+    return VPT_OK;
+}
+
+VptStatus vpt_set_denoiser_property(VptContext* ctx, const char* key, const char* value) {
+    VPT_CHECK_CTX(ctx);
+    if (!key || !value) return VPT_ERR_ARG;
+    float f;
+    if (!parse_float(value, f)) return fail(ctx, VPT_ERR_ARG, std::string("not a number: ") + value);
+    std::string k(key);
+    if (k == "iterations" || k == "maxNumIterations") ctx->eaw.iterations = int(f);
+    else if (k == "phi_color" || k == "phiColor") ctx->eaw.phi_color = f;
+    else if (k == "phi_position" || k == "phiPosition") ctx->eaw.phi_position = f;
+    else if (k == "phi_normal" || k == "phiNormal") ctx->eaw.phi_normal = f;
+    else if (k == "ref_compute_quirk") ctx->eaw.ref_compute_quirk = int(f);
+    else if (k == "z_threshold") ctx->svgf.z_threshold = f;
+    else if (k == "normal_threshold") ctx->svgf.normal_threshold = f;
+    else return fail(ctx, VPT_ERR_ARG, std::string("unknown denoiser property: ") + key);
+    return VPT_OK;
+}
+
+VptStatus vpt_set_use_empty_space_skipping(VptContext* ctx, int enabled) {
+    VPT_CHECK_CTX(ctx);
+    ctx->use_ess = enabled ? 1 : 0;
+    reset_film_state(ctx);
+    return VPT_OK;
+}
+
+VptStatus vpt_set_option(VptContext* ctx, const char* key, double value) {
+    VPT_CHECK_CTX(ctx);
+    if (!key) return VPT_ERR_ARG;
+    std::string k(key);
+    if (k == "schedule") {
+        ctx->schedule = int(value) ? vpt::kSchedulePersistent : vpt::kScheduleTiles;
+    } else if (k == "persistent_blocks_per_sm") {
+        if (value < 0 || value > 64) return fail(ctx, VPT_ERR_ARG, "persistent_blocks_per_sm out of range");
+        ctx->persistent_blocks_per_sm = int(value);
+    } else if (k == "max_steps_per_path") {
+        if (value < 1 || value > 4294967295.0) return fail(ctx, VPT_ERR_ARG, "max_steps_per_path out of range");
+        ctx->max_steps = (uint32_t)value;
+    } else if (k == "ess_ref_compat") {
+        ctx->ess_ref_compat = int(value) ? 1 : 0;
+        ctx->occ_valid = false;
+        reset_film_state(ctx);
+    } else {
+        return fail(ctx, VPT_ERR_ARG, std::string("unknown option: ") + key);
+    }
+    return VPT_OK;
+}
+
+VptStatus vpt_build_supervoxel_grid(const float* density, int nx, int ny, int nz, int sv, int halo, float* out_min,
+                                    float* out_max, float* out_avg, uint8_t* out_occ, void* stream) {
+    if (!density || !out_min || !out_max || nx <= 0 || ny <= 0 || nz <= 0 || sv <= 0) return VPT_ERR_ARG;
+    int gx = (nx + sv - 1) / sv, gy = (ny + sv - 1) / sv, gz = (nz + sv - 1) / sv;
+    cudaError_t e = vpt::launch_supervoxel_stats(density, nx, ny, nz, sv, gx, gy, gz, halo ? 1 : 0, out_min, out_max,
+                                                 out_avg, out_occ, as_stream(stream));
+    return e == cudaSuccess ? VPT_OK : VPT_ERR_CUDA;
+}
+
+VptStatus vpt_build_rrt_params(const float* sv_min, const float* sv_max, const float* sv_avg, int count,
+                               float extinction, int sv, float* out_pairs, void* stream) {
+    if (!sv_min || !sv_max || !sv_avg || !out_pairs || count <= 0 || sv <= 0) return VPT_ERR_ARG;
+    float D = sqrtf(3.0f) * float(sv);
+    cudaError_t e = vpt::launch_rrt_params(sv_min, sv_max, sv_avg, count, extinction, D, out_pairs, as_stream(stream));
+    return e == cudaSuccess ? VPT_OK : VPT_ERR_CUDA;
+}
+
+VptStatus vpt_build_occupancy_grid(const float* density, int nx, int ny, int nz, int block, int halo, float threshold,
+                                   uint8_t* out, void* stream) {
+    if (!density || !out || nx <= 0 || ny <= 0 || nz <= 0 || block <= 0 || halo < 0) return VPT_ERR_ARG;
+    int gx = (nx + block - 1) / block, gy = (ny + block - 1) / block, gz = (nz + block - 1) / block;
+    cudaError_t e =
+        vpt::launch_occupancy(density, nx, ny, nz, block, gx, gy, gz, halo, threshold, 0, out, as_stream(stream));
+    return e == cudaSuccess ? VPT_OK : VPT_ERR_CUDA;
+}
+
+VptStatus vpt_build_environment_pyramid(const float* rgba, int width, int height, int levels, float* out_pyramid,
+                                        void* stream) {
+    if (!rgba || !out_pyramid || width <= 0 || height <= 0 || levels <= 0 || levels > 14) return VPT_ERR_ARG;
+    std::vector<uint64_t> off(levels);
+    uint64_t o = 0;
+    for (int l = 0; l < levels; l++) {
+        off[l] = o;
+        uint64_t r = (uint64_t)1 << (levels - l);
+        o += r * r;
+    }
+    vpt::TraceParams P;
+    memset(&P, 0, sizeof(P));
+    P.env_rgba = rgba;
+    P.env_w = width;
+    P.env_h = height;
+    cudaError_t e = vpt::launch_env_pyramid(P, out_pyramid, off.data(), levels, as_stream(stream));
+    return e == cudaSuccess ? VPT_OK : VPT_ERR_CUDA;
+}
+
+VptStatus vpt_eaw_denoise_rgba(const float* color, const float* position, const float* normal, int width, int height,
+                               int iterations, float phi_color, float phi_position, float phi_normal,
+                               int ref_compute_quirk, float* out, void* stream) {
+    if (!color || !out || width <= 0 || height <= 0 || iterations < 0) return VPT_ERR_ARG;
+    cudaStream_t s = as_stream(stream);
+    size_t bytes = (size_t)width * height * 4 * sizeof(float);
+    if (iterations == 0) {
+        return cudaMemcpyAsync(out, color, bytes, cudaMemcpyDeviceToDevice, s) == cudaSuccess ? VPT_OK : VPT_ERR_CUDA;
+    }
+    float* scratch = nullptr;
+    if (cudaMallocAsync(reinterpret_cast<void**>(&scratch), bytes, s) != cudaSuccess) return VPT_ERR_OOM;
+    vpt::EawSettings st;
+    st.iterations = iterations;
+    st.phi_color = phi_color;
+    st.phi_position = phi_position;
+    st.phi_normal = phi_normal;
+    st.ref_compute_quirk = ref_compute_quirk;
+    // Ping-pong between `out` and the scratch image so that the last iteration lands in `out`.
+    float* ping = (iterations % 2 == 1) ? out : scratch;
+    float* pong = (iterations % 2 == 1) ? scratch : out;
+    float* result = nullptr;
+    cudaError_t e = vpt::eaw_denoise(color, position, normal, width, height, st, ping, pong, &result, s);
+    cudaFreeAsync(scratch, s);
+    return e == cudaSuccess ? VPT_OK : VPT_ERR_CUDA;
+}
+
+}  // extern "C"

@@ -1,0 +1,410 @@
+// vpt_device.cuh - device-side building blocks of the tracer: RNG, camera rays, box clipping,
+// Henyey-Greenstein sampling, sky/sun models and dense-grid density lookups.
+//
+// Arithmetic conventions (identical in the CPU oracle, so that paths can be compared one by one):
+//  * this translation unit is compiled with --fmad=false: a*b+c is two IEEE-rounded operations;
+//  * divisions and square roots are IEEE-rounded (-prec-div/-prec-sqrt default true);
+//  * the reference's per-step ratios are written in closed form: with majorant == extinction.x,
+//    Pa = (1 - albedo) * density and 1 - Pn = density (DeltaTracking.glsl:262-268);
+//  * world -> voxel coordinates use one multiply by voxels-per-unit, (pos - boxMin) * (N / extent),
+//    and the stochastic jitter is added in voxel units (VptUtils.glsl:585-591 does the same in
+//    texture units).
+#pragma once
+#include <stdint.h>
+#include <math.h>
+#include "vpt_params.h"
+
+namespace vpt {
+
+#define VPT_DEV __device__ __forceinline__
+
+constexpr float kPi = 3.14159265359f;        // VptUtils.glsl:27
+constexpr float kTwoPi = 2.0f * 3.14159265359f;
+
+VPT_DEV F3 f3(float x, float y, float z) { F3 r; r.x = x; r.y = y; r.z = z; return r; }
+VPT_DEV F3 operator+(F3 a, F3 b) { return f3(a.x + b.x, a.y + b.y, a.z + b.z); }
+VPT_DEV F3 operator-(F3 a, F3 b) { return f3(a.x - b.x, a.y - b.y, a.z - b.z); }
+VPT_DEV F3 operator-(F3 a) { return f3(-a.x, -a.y, -a.z); }
+VPT_DEV F3 operator*(F3 a, float s) { return f3(a.x * s, a.y * s, a.z * s); }
+VPT_DEV F3 operator*(float s, F3 a) { return f3(s * a.x, s * a.y, s * a.z); }
+VPT_DEV F3 operator*(F3 a, F3 b) { return f3(a.x * b.x, a.y * b.y, a.z * b.z); }
+VPT_DEV F3 operator/(F3 a, F3 b) { return f3(a.x / b.x, a.y / b.y, a.z / b.z); }
+VPT_DEV float dot3(F3 a, F3 b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
+VPT_DEV F3 cross3(F3 a, F3 b) {
+    return f3(a.y * b.z - b.y * a.z, a.z * b.x - b.z * a.x, a.x * b.y - b.x * a.y);
+}
+VPT_DEV float length3(F3 a) { return sqrtf(dot3(a, a)); }
+VPT_DEV F3 normalize3(F3 a) {
+    float l = length3(a);
+    return f3(a.x / l, a.y / l, a.z / l);
+}
+VPT_DEV float mixf(float a, float b, float t) { return a * (1.0f - t) + b * t; }
+VPT_DEV float clampf(float v, float lo, float hi) { return fminf(fmaxf(v, lo), hi); }
+VPT_DEV float smoothstepf(float e0, float e1, float x) {
+    float t = clampf((x - e0) / (e1 - e0), 0.0f, 1.0f);
+    return t * t * (3.0f - 2.0f * t);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Hybrid Tausworthe generator: three Tausworthe steps and one LCG step combined by XOR
+// (VptUtils.glsl:48-65).  Integer part is bit-exact; the float is float(u32) * 2^-32 rounded.
+struct Rng {
+    uint32_t x, y, z, w;
+};
+
+VPT_DEV uint32_t taus_step(uint32_t z, int s1, int s2, int s3, uint32_t m) {
+    uint32_t b = ((z << s1) ^ z) >> s2;
+    return ((z & m) << s3) ^ b;
+}
+
+VPT_DEV float rng_next(Rng& r) {
+    r.x = taus_step(r.x, 13, 19, 12, 4294967294u);
+    r.y = taus_step(r.y, 2, 25, 4, 4294967288u);
+    r.z = taus_step(r.z, 3, 11, 17, 4294967280u);
+    r.w = 1664525u * r.w + 1013904223u;
+    return 2.3283064365387e-10f * __uint2float_rn(r.x ^ r.y ^ r.z ^ r.w);
+}
+
+VPT_DEV Rng rng_init(uint32_t seed) {
+    Rng r;
+    r.x = r.y = r.z = r.w = seed;
+    uint32_t n = seed % 7u + 2u;
+    for (uint32_t i = 0; i < n; i++) rng_next(r);
+    return r;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Camera ray through NDC (x, y): near-plane point and direction to the far-plane point
+// (createCameraRay, VptUtils.glsl:750-761).
+VPT_DEV void mat4_mul_point(const float* m, float x, float y, float z, float w, float out[4]) {
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+        out[r] = ((m[0 * 4 + r] * x + m[1 * 4 + r] * y) + m[2 * 4 + r] * z) + m[3 * 4 + r] * w;
+    }
+}
+
+VPT_DEV void camera_ray(const TraceParams& P, float sx, float sy, F3& x, F3& w) {
+    float p[4], t[4];
+    mat4_mul_point(P.inv_view_proj, sx, sy, 0.0f, 1.0f, p);
+    mat4_mul_point(P.inv_view_proj, sx, sy, 1.0f, 1.0f, t);
+    F3 vp = f3(p[0] / p[3], p[1] / p[3], p[2] / p[3]);
+    F3 vt = f3(t[0] / t[3], t[1] / t[3], t[2] / t[3]);
+    x = vp;
+    w = normalize3(vt - vp);
+}
+
+// Slab test with a 1e-6 clamp of near-zero direction components (rayBoxIntersect,
+// VptUtils.glsl:763-801; the clip plane is not supported).
+VPT_DEV bool ray_box(F3 bmin, F3 bmax, F3 p, F3 d, float& tmin, float& tmax) {
+    d.x = fabsf(d.x) <= 0.000001f ? 0.000001f : d.x;
+    d.y = fabsf(d.y) <= 0.000001f ? 0.000001f : d.y;
+    d.z = fabsf(d.z) <= 0.000001f ? 0.000001f : d.z;
+    F3 cmin = (bmin - p) / d;
+    F3 cmax = (bmax - p) / d;
+    tmin = fmaxf(fmaxf(fminf(cmin.x, cmax.x), fminf(cmin.y, cmax.y)), fminf(cmin.z, cmax.z));
+    tmin = fmaxf(0.0f, tmin);
+    tmax = fminf(fminf(fmaxf(cmin.x, cmax.x), fmaxf(cmin.y, cmax.y)), fmaxf(cmin.z, cmax.z));
+    return !(tmax <= tmin || tmax <= 0.0f);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Direction sampling (VptUtils.glsl:67-123).
+VPT_DEV void orthonormal_basis(F3 d, F3& b, F3& t) {
+    F3 other = fabsf(d.z) >= 0.9999f ? f3(1.0f, 0.0f, 0.0f) : f3(0.0f, 0.0f, 1.0f);
+    b = normalize3(cross3(other, d));
+    t = normalize3(cross3(d, b));
+}
+
+VPT_DEV F3 random_direction(Rng& rng, F3 d) {
+    float r1 = rng_next(rng);
+    float r2 = rng_next(rng) * 2.0f - 1.0f;
+    float sq = r2 * r2;
+    float a = kTwoPi * r1;
+    float s = sqrtf(1.0f - sq);
+    float x = cosf(a) * s;
+    float y = sinf(a) * s;
+    F3 t0, t1;
+    orthonormal_basis(d, t0, t1);
+    return (t0 * x + t1 * y) + d * r2;
+}
+
+VPT_DEV float hg_invert_cdf(float g, float xi) {
+    float t = (1.0f - g * g) / (1.0f - g + 2.0f * g * xi);
+    return (0.5f / g) * ((1.0f + g * g) - t * t);
+}
+
+// importanceSamplePhase without the pdf (only evaluatePhase's pdf feeds the estimators).
+VPT_DEV F3 sample_phase(Rng& rng, float g, F3 d) {
+    if (fabsf(g) < 0.001f) {
+        return random_direction(rng, -d);
+    }
+    float phi = rng_next(rng) * 2.0f * kPi;
+    float cos_t = hg_invert_cdf(g, rng_next(rng));
+    float sin_t = sqrtf(fmaxf(0.0f, 1.0f - cos_t * cos_t));
+    F3 t0, t1;
+    orthonormal_basis(d, t0, t1);
+    return (t0 * (sin_t * sinf(phi)) + t1 * (sin_t * cosf(phi))) + d * cos_t;
+}
+
+VPT_DEV float evaluate_phase(float g, F3 a, F3 b) {
+    float c = dot3(normalize3(a), normalize3(b));
+    return ((0.25f / kPi) * (1.0f - g * g)) / powf((1.0f + g * g) - 2.0f * g * c, 1.5f);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Sky and sun (VptUtils.glsl:288-389).
+VPT_DEV float srgb_to_linear(float c) {
+    return c <= 0.04045f ? c / 12.92f : powf((c + 0.055f) / 1.055f, 2.4f);
+}
+
+VPT_DEV float linear_to_srgb(float c) {
+    return c <= 0.0031308f ? c * 12.92f : 1.055f * powf(c, 1.0f / 2.4f) - 0.055f;
+}
+
+VPT_DEV F3 sky_default(F3 dir, int linear_rgb) {
+    const float cr[5] = {0.1f, 0.01f, 0.8f, 0.1f, 0.01f};
+    const float cg[5] = {0.05f, 0.05f, 0.9f, 0.3f, 0.1f};
+    const float cb[5] = {0.01f, 0.2f, 1.0f, 1.0f, 0.7f};
+    const float dists[5] = {-1.0f, -0.1f, 0.0f, 0.4f, 1.0f};
+    float r = cr[0], g = cg[0], b = cb[0];
+#pragma unroll
+    for (int i = 1; i < 5; i++) {
+        float s = smoothstepf(dists[i - 1], dists[i], dir.y);
+        r = mixf(r, cr[i], s);
+        g = mixf(g, cg[i], s);
+        b = mixf(b, cb[i], s);
+    }
+    if (linear_rgb) {
+        r = srgb_to_linear(r);
+        g = srgb_to_linear(g);
+        b = srgb_to_linear(b);
+    }
+    return f3(r, g, b);
+}
+
+// Phong lobe with exponent 10 around the sun direction, normalised by (N+1)/(2*3.14159)
+// (sampleLight, VptUtils.glsl:370-374).
+VPT_DEV F3 sun_lobe(const TraceParams& P, F3 dir) {
+    const float norm = 11.0f / (2.0f * 3.14159f);
+    float p = powf(fmaxf(0.0f, dot3(dir, P.sun_dir)), 10.0f);
+    return f3((P.sun_intensity.x * p) * norm, (P.sun_intensity.y * p) * norm, (P.sun_intensity.z * p) * norm);
+}
+
+// Bilinear fetch of the equirectangular image with REPEAT addressing.
+VPT_DEV F3 env_image_fetch(const TraceParams& P, float u, float v) {
+    float fx = u * (float)P.env_w - 0.5f;
+    float fy = v * (float)P.env_h - 0.5f;
+    float x0f = floorf(fx), y0f = floorf(fy);
+    float ax = fx - x0f, ay = fy - y0f;
+    int x0 = (int)x0f, y0 = (int)y0f;
+    int w = P.env_w, h = P.env_h;
+    int xa = ((x0 % w) + w) % w, xb = (((x0 + 1) % w) + w) % w;
+    int ya = ((y0 % h) + h) % h, yb = (((y0 + 1) % h) + h) % h;
+    const float4* img = reinterpret_cast<const float4*>(P.env_rgba);
+    float4 c00 = __ldg(img + (size_t)ya * w + xa), c10 = __ldg(img + (size_t)ya * w + xb);
+    float4 c01 = __ldg(img + (size_t)yb * w + xa), c11 = __ldg(img + (size_t)yb * w + xb);
+    F3 r;
+    r.x = mixf(mixf(c00.x, c10.x, ax), mixf(c01.x, c11.x, ax), ay);
+    r.y = mixf(mixf(c00.y, c10.y, ax), mixf(c01.y, c11.y, ax), ay);
+    r.z = mixf(mixf(c00.z, c10.z, ax), mixf(c01.z, c11.z, ax), ay);
+    return r;
+}
+
+// sampleSkybox for an environment image (VptUtils.glsl:303-328; no rotation).
+VPT_DEV F3 sky_image(const TraceParams& P, F3 dir) {
+    float u = atan2f(dir.z, dir.x) / kTwoPi + 0.5f;
+    float v = -asinf(dir.y) / kPi + 0.5f;
+    F3 c = env_image_fetch(P, u, v);
+    c.x = fminf(c.x, 100000.0f);
+    c.y = fminf(c.y, 100000.0f);
+    c.z = fminf(c.z, 100000.0f);
+    if (!P.env_image_linear && P.use_linear_rgb) {
+        c = f3(srgb_to_linear(c.x), srgb_to_linear(c.y), srgb_to_linear(c.z));
+    } else if (P.env_image_linear && !P.use_linear_rgb) {
+        c = f3(linear_to_srgb(c.x), linear_to_srgb(c.y), linear_to_srgb(c.z));
+    }
+    return P.env_intensity * c;
+}
+
+// sampleSkybox(dir) + sampleLight(dir) for the configured environment.
+VPT_DEV F3 sky_and_sun(const TraceParams& P, F3 dir) {
+    switch (P.env_kind) {
+        case kEnvDefault: return sky_default(dir, P.use_linear_rgb) + sun_lobe(P, dir);
+        case kEnvBlack: return f3(0.0f, 0.0f, 0.0f);
+        case kEnvSingleColor: return P.sun_intensity;
+        case kEnvConstantSun: return P.sky_color + sun_lobe(P, dir);
+        default: return sky_image(P, dir);
+    }
+}
+
+// sampleSkybox(dir) only (background feature map).
+VPT_DEV F3 sky_only(const TraceParams& P, F3 dir) {
+    switch (P.env_kind) {
+        case kEnvDefault: return sky_default(dir, P.use_linear_rgb);
+        case kEnvBlack: return f3(0.0f, 0.0f, 0.0f);
+        case kEnvSingleColor: return P.sun_intensity;
+        case kEnvConstantSun: return P.sky_color;
+        default: return sky_image(P, dir);
+    }
+}
+
+// Octahedral map helpers (VptUtils.glsl:127-170; no rotation).
+VPT_DEV float signf(float v) { return v > 0.0f ? 1.0f : (v < 0.0f ? -1.0f : 0.0f); }
+
+VPT_DEV F3 octahedral_uv_to_world(float u, float v) {
+    u = u * 2.0f - 1.0f;
+    v = v * 2.0f - 1.0f;
+    float sx = signf(u), sy = signf(v);
+    u = fabsf(u);
+    v = fabsf(v);
+    float r = 1.0f - fabsf(1.0f - u - v);
+    float phi = 0.25f * kPi * ((v - u) / r + 1.0f);
+    if (r == 0.0f) phi = 0.0f;
+    float r2 = r * r;
+    float s = sqrtf(2.0f - r2);
+    float x = sx * cosf(phi) * r * s;
+    float y = sy * sinf(phi) * r * s;
+    float z = signf(1.0f - u - v) * (1.0f - r2);
+    return f3(x, y, z);
+}
+
+VPT_DEV void world_to_octahedral_uv(F3 dir, float& u, float& v) {
+    dir = normalize3(dir);
+    float sx = signf(dir.x), sy = signf(dir.y), sz = signf(dir.z);
+    dir = f3(fabsf(dir.x), fabsf(dir.y), fabsf(dir.z));
+    float phi = atan2f(dir.y, dir.x);
+    float r = sqrtf(1.0f - dir.z);
+    float vv = r * 2.0f / kPi * phi;
+    float uu = r - vv;
+    if (sz < 0.0f) {
+        float t = uu;
+        uu = 1.0f - vv;
+        vv = 1.0f - t;
+    }
+    u = uu * sx * 0.5f + 0.5f;
+    v = vv * sy * 0.5f + 0.5f;
+}
+
+VPT_DEV float pyr_fetch(const TraceParams& P, int level, int x, int y) {
+    int res = P.env_base_res >> level;
+    return __ldg(P.env_pyramid + P.env_level_offset[level] + (size_t)y * res + x) + 0.001f;
+}
+
+// Hierarchical sample of the octahedral max-luminance pyramid (importanceSampleSkybox,
+// VptUtils.glsl:172-220).
+VPT_DEV F3 importance_sample_env_image(const TraceParams& P, Rng& rng, float& pdf) {
+    float rx = rng_next(rng);
+    float ry = rng_next(rng);
+    int px = 0, py = 0;
+    pdf = 0.25f / kPi;
+    for (int mip = P.env_levels - 1; mip >= 0; mip--) {
+        px *= 2;
+        py *= 2;
+        pdf *= 4.0f;
+        float ul = pyr_fetch(P, mip, px, py), ur = pyr_fetch(P, mip, px + 1, py);
+        float dl = pyr_fetch(P, mip, px, py + 1), dr = pyr_fetch(P, mip, px + 1, py + 1);
+        float l = ul + dl, r = ur + dr, total = l + r;
+        float hs = l / total, vs;
+        if (rx < hs) {
+            rx = rx / hs;
+            vs = ul / l;
+            pdf *= hs;
+        } else {
+            px += 1;
+            rx = (rx - hs) / (1.0f - hs);
+            vs = ur / r;
+            pdf *= (1.0f - hs);
+        }
+        if (ry < vs) {
+            ry = ry / vs;
+            pdf *= vs;
+        } else {
+            py += 1;
+            ry = (ry - vs) / (1.0f - vs);
+            pdf *= (1.0f - vs);
+        }
+    }
+    float inv = 1.0f / (float)P.env_base_res;
+    return octahedral_uv_to_world(((float)px + rx) * inv, ((float)py + ry) * inv);
+}
+
+// Light sample for NEE: environment image -> pyramid, builtin -> uniform sphere.
+VPT_DEV F3 importance_sample_sky(const TraceParams& P, Rng& rng, float& pdf) {
+    if (P.env_kind == kEnvImage) return importance_sample_env_image(P, rng, pdf);
+    pdf = 1.0f / (4.0f * kPi);
+    return random_direction(rng, f3(1.0f, 0.0f, 0.0f));
+}
+
+// ---------------------------------------------------------------------------------------------
+// Dense density lookup with CLAMP_TO_BORDER semantics (sampleCloud/sampleCloudRaw,
+// VptUtils.glsl:583-591, 674-683).  Values in `density` are already normalised.
+VPT_DEV float dense_texel(const TraceParams& P, int ix, int iy, int iz) {
+    if ((unsigned)ix >= (unsigned)P.nx || (unsigned)iy >= (unsigned)P.ny || (unsigned)iz >= (unsigned)P.nz) {
+        return P.border_density;
+    }
+    return __ldg(P.density + ((size_t)iz * (size_t)P.ny + (size_t)iy) * (size_t)P.nx + (size_t)ix);
+}
+
+// Lookup at continuous voxel coordinates u (texel i covers [i, i+1)).
+template <int INTERP>
+VPT_DEV float sample_dense_vox(const TraceParams& P, float ux, float uy, float uz) {
+    if (INTERP != kTrilinear) {
+        return dense_texel(P, (int)floorf(ux), (int)floorf(uy), (int)floorf(uz));
+    }
+    ux = ux - 0.5f;
+    uy = uy - 0.5f;
+    uz = uz - 0.5f;
+    float fx0 = floorf(ux), fy0 = floorf(uy), fz0 = floorf(uz);
+    float ax = ux - fx0, ay = uy - fy0, az = uz - fz0;
+    int x0 = (int)fx0, y0 = (int)fy0, z0 = (int)fz0;
+    float f000 = dense_texel(P, x0, y0, z0), f100 = dense_texel(P, x0 + 1, y0, z0);
+    float f010 = dense_texel(P, x0, y0 + 1, z0), f110 = dense_texel(P, x0 + 1, y0 + 1, z0);
+    float f001 = dense_texel(P, x0, y0, z0 + 1), f101 = dense_texel(P, x0 + 1, y0, z0 + 1);
+    float f011 = dense_texel(P, x0, y0 + 1, z0 + 1), f111 = dense_texel(P, x0 + 1, y0 + 1, z0 + 1);
+    float f0 = mixf(mixf(f000, f100, ax), mixf(f010, f110, ax), ay);
+    float f1 = mixf(mixf(f001, f101, ax), mixf(f011, f111, ax), ay);
+    return mixf(f0, f1, az);
+}
+
+template <int INTERP>
+VPT_DEV float sample_dense(const TraceParams& P, F3 pos, Rng& rng) {
+    float ux = (pos.x - P.box_min.x) * P.vox_per_unit.x;
+    float uy = (pos.y - P.box_min.y) * P.vox_per_unit.y;
+    float uz = (pos.z - P.box_min.z) * P.vox_per_unit.z;
+    if (INTERP == kStochastic) {
+        float jx = rng_next(rng) - 0.5f;
+        float jy = rng_next(rng) - 0.5f;
+        float jz = rng_next(rng) - 0.5f;
+        ux = ux + jx;
+        uy = uy + jy;
+        uz = uz + jz;
+    }
+    return sample_dense_vox<INTERP>(P, ux, uy, uz);
+}
+
+// Normal feature: central differences of the density one voxel apart, scaled by 100/dim and
+// normalised when longer than 1e-5 (getCloudFiniteDifference, VptUtils.glsl:726-748).
+template <int INTERP>
+VPT_DEV F3 density_normal(const TraceParams& P, F3 pos, Rng& rng) {
+    float ux = (pos.x - P.box_min.x) * P.vox_per_unit.x;
+    float uy = (pos.y - P.box_min.y) * P.vox_per_unit.y;
+    float uz = (pos.z - P.box_min.z) * P.vox_per_unit.z;
+    if (INTERP == kStochastic) {
+        float jx = rng_next(rng) - 0.5f;
+        float jy = rng_next(rng) - 0.5f;
+        float jz = rng_next(rng) - 0.5f;
+        ux = ux + jx;
+        uy = uy + jy;
+        uz = uz + jz;
+    }
+    F3 d;
+    d.x = sample_dense_vox<INTERP>(P, ux - 1.0f, uy, uz) - sample_dense_vox<INTERP>(P, ux + 1.0f, uy, uz);
+    d.y = sample_dense_vox<INTERP>(P, ux, uy - 1.0f, uz) - sample_dense_vox<INTERP>(P, ux, uy + 1.0f, uz);
+    d.z = sample_dense_vox<INTERP>(P, ux, uy, uz - 1.0f) - sample_dense_vox<INTERP>(P, ux, uy, uz + 1.0f);
+    d = f3((d.x / (float)P.nx) * 100.0f, (d.y / (float)P.ny) * 100.0f, (d.z / (float)P.nz) * 100.0f);
+    float l = length3(d);
+    if (l > 1e-5f) d = f3(d.x / l, d.y / l, d.z / l);
+    return d;
+}
+
+}  // namespace vpt

@@ -1,0 +1,611 @@
+// vpt_kernels.cu - CUDA kernels of the tracing path and their launchers.
+//
+//  * trace kernels: one camera path per thread; TRACKER x INTERP x FEATURES are template
+//    parameters (the reference selects them with shader #defines, VolumetricPathTracingPass.cpp:
+//    1558-1782).  Two schedules: a plain grid over 16x16 pixel tiles and a persistent grid whose
+//    warps pull 32-path batches from a global counter (no block waits on its slowest warp).
+//  * grid preparation: min/max reduction and normalisation (DensityField.cpp:136-154, 262-267),
+//    seeded fBm scene generator, supervoxel and occupancy builders (SuperVoxelGrid.cpp,
+//    ComputeOccupancyGrid.glsl), octahedral environment pyramid (OctahedralMapper.glsl).
+//  * film readout: FP64 sums -> fp32 mean, channels x H x W.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "vpt_device.cuh"
+#include "vpt_trackers.cuh"
+#include "vpt_kernels.h"
+
+namespace vpt {
+
+// Number of kernels this library has launched (all launch sites below and in vpt_denoise.cu).
+static unsigned long long g_launches = 0;
+void count_launches(unsigned n) { __atomic_fetch_add(&g_launches, (unsigned long long)n, __ATOMIC_RELAXED); }
+unsigned long long launch_count() { return __atomic_load_n(&g_launches, __ATOMIC_RELAXED); }
+
+template <int INTERP>
+struct DenseSampler {
+    const TraceParams& P;
+    VPT_DEV float operator()(F3 pos, Rng& rng) const { return sample_dense<INTERP>(P, pos, rng); }
+    VPT_DEV F3 normal(F3 pos, Rng& rng) const { return density_normal<INTERP>(P, pos, rng); }
+};
+
+// Per-path feature accumulation (Clouds.glsl:195-256): position of the first event, depth,
+// density, albedo-weighted hit flag, primary-ray transmittance proxy.
+template <class S>
+VPT_DEV void accumulate_features(const TraceParams& P, S& sample, Rng& rng, size_t pix, const FirstEvent& fe,
+                                 F3 result) {
+    float* f = P.feat + pix * kFeatStride;
+    if (fe.has) {
+        F3 n = sample.normal(fe.x, rng);
+        atomicAdd(f + kFeatNormal + 0, n.x);
+        atomicAdd(f + kFeatNormal + 1, n.y);
+        atomicAdd(f + kFeatNormal + 2, n.z);
+        atomicAdd(f + kFeatPos + 0, fe.x.x);
+        atomicAdd(f + kFeatPos + 1, fe.x.y);
+        atomicAdd(f + kFeatPos + 2, fe.x.z);
+        atomicAdd(f + kFeatPos + 3, 1.0f);
+        atomicAdd(f + kFeatDepth + 0, fe.depth);
+        atomicAdd(f + kFeatDepth + 1, fe.depth * fe.depth);
+        atomicAdd(f + kFeatDensity + 0, fe.density * 0.001f);
+        atomicAdd(f + kFeatDensity + 1, (fe.density * fe.density * 0.001f) * 0.001f);
+        atomicAdd(f + kFeatCloudOnly + 0, result.x);
+        atomicAdd(f + kFeatCloudOnly + 1, result.y);
+        atomicAdd(f + kFeatCloudOnly + 2, result.z);
+    } else {
+        atomicAdd(f + kFeatTrans, 1.0f);
+    }
+}
+
+template <int TRACKER, class S>
+VPT_DEV F3 run_tracker(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, FirstEvent& fe, PathCtx& pc) {
+    if (TRACKER == kDelta) return track_delta(P, sample, rng, x, w, fe, pc);
+    if (TRACKER == kRatio) return track_ratio(P, sample, rng, x, w, fe, pc);
+    if (TRACKER == kDecomposition) return track_decomposition(P, sample, rng, x, w, fe, pc);
+    if (TRACKER == kResidualRatio) return track_residual_ratio(P, sample, rng, x, w, fe, pc);
+    if (TRACKER == kNextEvent + 100) return track_nee<true>(P, sample, rng, x, w, fe, pc);
+    return track_nee<false>(P, sample, rng, x, w, fe, pc);
+}
+
+// Maps a path index to (frame, x, y): 16x16 pixel tiles, tiles row-major, frames outermost, so a
+// warp traces a 16x2 pixel strip of one frame (coherent primary rays).
+VPT_DEV bool decode_path(const TraceParams& P, uint64_t p, uint32_t& frame, int& x, int& y) {
+    const uint32_t tiles_x = (uint32_t)(P.width + 15) >> 4;
+    const uint32_t tiles_y = (uint32_t)(P.height + 15) >> 4;
+    const uint64_t per_frame = (uint64_t)tiles_x * tiles_y * 256u;
+    frame = (uint32_t)(p / per_frame);
+    uint32_t q = (uint32_t)(p - (uint64_t)frame * per_frame);
+    uint32_t tile = q >> 8, within = q & 255u;
+    x = (int)((tile % tiles_x) * 16u + (within & 15u));
+    y = (int)((tile / tiles_x) * 16u + (within >> 4));
+    return frame < P.num_frames && x < P.width && y < P.height;
+}
+
+// One camera path: seed (Clouds.glsl:80-84), jittered NDC (Clouds.glsl:86), tracker, film.
+template <int TRACKER, class S>
+VPT_DEV void trace_one(const TraceParams& P, S& sample, uint32_t frame, int px, int py, bool features,
+                       uint32_t& lookups, bool& guard_hit) {
+    const uint32_t w_u = (uint32_t)P.width, h_u = (uint32_t)P.height;
+    uint32_t seed = (P.global_frame + frame) * w_u * h_u + (uint32_t)px + (uint32_t)py * w_u;
+    seed += P.seed_offset;
+    Rng rng = rng_init(seed);
+    float rx = rng_next(rng);
+    float ry = rng_next(rng);
+    float sx = (2.0f * ((float)px + rx)) / (float)P.width - 1.0f;
+    float sy = (2.0f * ((float)py + ry)) / (float)P.height - 1.0f;
+    F3 x, w;
+    camera_ray(P, sx, sy, x, w);
+    FirstEvent fe;
+    fe.has = false;
+    PathCtx pc;
+    pc.steps = 0;
+    pc.max_steps = P.max_steps;
+    pc.lookups = 0;
+    pc.guard_hit = false;
+    F3 L = run_tracker<TRACKER>(P, sample, rng, x, w, fe, pc);
+    const size_t pix = (size_t)py * P.width + px;
+    atomicAdd(P.film + pix * 3 + 0, (double)L.x);
+    atomicAdd(P.film + pix * 3 + 1, (double)L.y);
+    atomicAdd(P.film + pix * 3 + 2, (double)L.z);
+    if (P.film_sq) {
+        atomicAdd(P.film_sq + pix * 3 + 0, (double)L.x * (double)L.x);
+        atomicAdd(P.film_sq + pix * 3 + 1, (double)L.y * (double)L.y);
+        atomicAdd(P.film_sq + pix * 3 + 2, (double)L.z * (double)L.z);
+    }
+    if (features) accumulate_features(P, sample, rng, pix, fe, L);
+    lookups += pc.lookups;
+    guard_hit |= pc.guard_hit;
+}
+
+VPT_DEV void flush_counters(const TraceParams& P, uint32_t paths, uint32_t lookups, bool guard_hit) {
+    unsigned long long l = lookups;
+    unsigned long long n = paths;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        l += __shfl_xor_sync(0xffffffffu, l, o);
+        n += __shfl_xor_sync(0xffffffffu, n, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(P.counters + 0, n);
+        atomicAdd(P.counters + 1, l);
+    }
+    if (guard_hit) atomicOr(P.error_flags, kErrIterLimit);
+}
+
+template <int TRACKER, int INTERP>
+__global__ void __launch_bounds__(kTraceBlock) trace_tiles_kernel(const __grid_constant__ TraceParams P, int features) {
+    DenseSampler<INTERP> sample{P};
+    uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t frame;
+    int px, py;
+    uint32_t lookups = 0, paths = 0;
+    bool guard_hit = false;
+    if (decode_path(P, p, frame, px, py)) {
+        trace_one<TRACKER>(P, sample, frame, px, py, features != 0, lookups, guard_hit);
+        paths = 1;
+    }
+    __syncwarp();
+    flush_counters(P, paths, lookups, guard_hit);
+}
+
+template <int TRACKER, int INTERP>
+__global__ void __launch_bounds__(kTraceBlock) trace_persistent_kernel(const __grid_constant__ TraceParams P,
+                                                                       int features, uint64_t total) {
+    DenseSampler<INTERP> sample{P};
+    const int lane = threadIdx.x & 31;
+    uint32_t lookups = 0, paths = 0;
+    bool guard_hit = false;
+    while (true) {
+        unsigned long long base = 0;
+        if (lane == 0) base = atomicAdd(reinterpret_cast<unsigned long long*>(P.work_counter), 32ull);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= total) break;
+        uint64_t p = base + lane;
+        uint32_t frame;
+        int px, py;
+        if (p < total && decode_path(P, p, frame, px, py)) {
+            trace_one<TRACKER>(P, sample, frame, px, py, features != 0, lookups, guard_hit);
+            paths++;
+        }
+        __syncwarp();
+    }
+    flush_counters(P, paths, lookups, guard_hit);
+}
+
+uint64_t padded_paths(int width, int height, uint32_t frames) {
+    uint64_t tiles = (uint64_t)((width + 15) / 16) * (uint64_t)((height + 15) / 16);
+    return tiles * 256ull * frames;
+}
+
+template <int TRACKER, int INTERP>
+static cudaError_t launch_trace_t(const TraceParams& P, int schedule, int features, int persistent_blocks,
+                                  cudaStream_t stream) {
+    uint64_t total = padded_paths(P.width, P.height, P.num_frames);
+    if (schedule == kScheduleTiles) {
+        uint64_t blocks = (total + kTraceBlock - 1) / kTraceBlock;
+        trace_tiles_kernel<TRACKER, INTERP><<<(unsigned)blocks, kTraceBlock, 0, stream>>>(P, features);
+        count_launches(1);
+    } else {
+        if (persistent_blocks <= 0) {
+            // one wave of resident blocks: SMs x blocks per SM from the occupancy calculator
+            static int per_sm = 0;
+            if (per_sm == 0) {
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_persistent_kernel<TRACKER, INTERP>,
+                                                              kTraceBlock, 0);
+                if (per_sm <= 0) per_sm = 1;
+            }
+            int dev = 0, sms = 148;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            persistent_blocks = per_sm * sms;
+        }
+        cudaMemsetAsync(P.work_counter, 0, sizeof(unsigned long long), stream);
+        trace_persistent_kernel<TRACKER, INTERP><<<persistent_blocks, kTraceBlock, 0, stream>>>(P, features, total);
+        count_launches(1);
+    }
+    return cudaGetLastError();
+}
+
+template <int TRACKER>
+static cudaError_t launch_interp(const TraceParams& P, int schedule, int features, int pb, cudaStream_t s) {
+    switch (P.interp) {
+        case kNearest: return launch_trace_t<TRACKER, kNearest>(P, schedule, features, pb, s);
+        case kStochastic: return launch_trace_t<TRACKER, kStochastic>(P, schedule, features, pb, s);
+        default: return launch_trace_t<TRACKER, kTrilinear>(P, schedule, features, pb, s);
+    }
+}
+
+cudaError_t launch_trace(const TraceParams& P, int tracker, int use_ess, int schedule, int features,
+                         int persistent_blocks, cudaStream_t stream) {
+    switch (tracker) {
+        case kDelta: return launch_interp<kDelta>(P, schedule, features, persistent_blocks, stream);
+        case kRatio: return launch_interp<kRatio>(P, schedule, features, persistent_blocks, stream);
+        case kDecomposition: return launch_interp<kDecomposition>(P, schedule, features, persistent_blocks, stream);
+        case kResidualRatio: return launch_interp<kResidualRatio>(P, schedule, features, persistent_blocks, stream);
+        case kNextEvent:
+            if (use_ess) return launch_interp<kNextEvent + 100>(P, schedule, features, persistent_blocks, stream);
+            return launch_interp<kNextEvent>(P, schedule, features, persistent_blocks, stream);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Grid preparation.
+
+__device__ __forceinline__ void atomic_min_float(float* addr, float v) {
+    int* a = reinterpret_cast<int*>(addr);
+    int old = *a;
+    while (__int_as_float(old) > v) {
+        int assumed = old;
+        old = atomicCAS(a, assumed, __float_as_int(v));
+        if (old == assumed) break;
+    }
+}
+__device__ __forceinline__ void atomic_max_float(float* addr, float v) {
+    int* a = reinterpret_cast<int*>(addr);
+    int old = *a;
+    while (__int_as_float(old) < v) {
+        int assumed = old;
+        old = atomicCAS(a, assumed, __float_as_int(v));
+        if (old == assumed) break;
+    }
+}
+
+// min/max over the raw grid (sgl::reduceFloatArrayMinMax semantics; order-independent, exact).
+__global__ void minmax_kernel(const float* __restrict__ v, size_t n, float* out_minmax) {
+    float lo = INFINITY, hi = -INFINITY;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        float x = v[i];
+        lo = fminf(lo, x);
+        hi = fmaxf(hi, x);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        lo = fminf(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+        hi = fmaxf(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    }
+    __shared__ float slo[32], shi[32];
+    int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) {
+        slo[warp] = lo;
+        shi[warp] = hi;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        int nw = blockDim.x >> 5;
+        lo = lane < nw ? slo[lane] : INFINITY;
+        hi = lane < nw ? shi[lane] : -INFINITY;
+        for (int o = 16; o > 0; o >>= 1) {
+            lo = fminf(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+            hi = fmaxf(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+        }
+        if (lane == 0) {
+            atomic_min_float(out_minmax + 0, lo);
+            atomic_max_float(out_minmax + 1, hi);
+        }
+    }
+}
+
+// (v - min) / (max - min), IEEE division as in DensityField::getDataFloatAtNorm.
+__global__ void normalize_kernel(const float* __restrict__ in, float* __restrict__ out, size_t n, float vmin,
+                                 float vmax) {
+    const float range = vmax - vmin;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        out[i] = (in[i] - vmin) / range;
+    }
+}
+
+// Improved Perlin noise (K. Perlin, "Improving Noise", SIGGRAPH 2002) with a seeded permutation;
+// only +, -, *, floor, so the CPU oracle reproduces every value bit for bit.
+struct PermTable {
+    int p[512];
+};
+
+__device__ __forceinline__ float fade(float t) { return t * t * t * (t * (t * 6.0f - 15.0f) + 10.0f); }
+__device__ __forceinline__ float lerpf(float t, float a, float b) { return a + t * (b - a); }
+__device__ __forceinline__ float grad(int h, float x, float y, float z) {
+    h &= 15;
+    float u = h < 8 ? x : y;
+    float v = h < 4 ? y : ((h == 12 || h == 14) ? x : z);
+    return ((h & 1) ? -u : u) + ((h & 2) ? -v : v);
+}
+
+__device__ float perlin3(const int* __restrict__ p, float x, float y, float z) {
+    float fx = floorf(x), fy = floorf(y), fz = floorf(z);
+    int X = (int)fx & 255, Y = (int)fy & 255, Z = (int)fz & 255;
+    x -= fx;
+    y -= fy;
+    z -= fz;
+    float u = fade(x), v = fade(y), w = fade(z);
+    int A = p[X] + Y, AA = p[A] + Z, AB = p[A + 1] + Z;
+    int B = p[X + 1] + Y, BA = p[B] + Z, BB = p[B + 1] + Z;
+    float r0 = lerpf(v, lerpf(u, grad(p[AA], x, y, z), grad(p[BA], x - 1.0f, y, z)),
+                     lerpf(u, grad(p[AB], x, y - 1.0f, z), grad(p[BB], x - 1.0f, y - 1.0f, z)));
+    float r1 = lerpf(v, lerpf(u, grad(p[AA + 1], x, y, z - 1.0f), grad(p[BA + 1], x - 1.0f, y, z - 1.0f)),
+                     lerpf(u, grad(p[AB + 1], x, y - 1.0f, z - 1.0f), grad(p[BB + 1], x - 1.0f, y - 1.0f, z - 1.0f)));
+    return lerpf(w, r0, r1);
+}
+
+__global__ void fbm_kernel(float* __restrict__ out, int nx, int ny, int nz, const __grid_constant__ PermTable perm,
+                           FbmParams fp) {
+    __shared__ int p[512];
+    for (int i = threadIdx.x; i < 512; i += blockDim.x) p[i] = perm.p[i];
+    __syncthreads();
+    const size_t n = (size_t)nx * ny * nz;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        int ix = (int)(i % (size_t)nx);
+        int iy = (int)((i / (size_t)nx) % (size_t)ny);
+        int iz = (int)(i / ((size_t)nx * ny));
+        float px = ((float)ix + 0.5f) * fp.inv_max_dim;
+        float py = ((float)iy + 0.5f) * fp.inv_max_dim;
+        float pz = ((float)iz + 0.5f) * fp.inv_max_dim;
+        float sum = 0.0f, amp = 1.0f, freq = fp.base_frequency, norm = 0.0f;
+        for (int o = 0; o < fp.octaves; o++) {
+            sum += amp * perlin3(p, px * freq, py * freq, pz * freq);
+            norm += amp;
+            amp *= fp.gain;
+            freq *= fp.lacunarity;
+        }
+        float v = sum / norm;
+        v = fminf(fmaxf(0.5f + fp.contrast * v, 0.0f), 1.0f);
+        out[i] = v < fp.threshold ? 0.0f : v;
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Supervoxel grid: min / max / mean of the normalised density over each sv^3 block, with a one
+// voxel halo unless the interpolation is NEAREST; voxels outside the grid count as 0 and a
+// partial boundary supervoxel has min := 0 (SuperVoxelGrid.cpp:101-211, 316-396).  One thread
+// per supervoxel accumulates the mean in the reference's z-y-x loop order, so the sum is
+// bit-identical; min/max are order-independent.
+__global__ void supervoxel_stats_kernel(const float* __restrict__ dens, int nx, int ny, int nz, int sv, int svx,
+                                        int svy, int svz, int halo, float* __restrict__ out_min,
+                                        float* __restrict__ out_max, float* __restrict__ out_avg,
+                                        uint8_t* __restrict__ out_occ) {
+    int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    int total = svx * svy * svz;
+    if (idx >= total) return;
+    int bx = idx % svx, by = (idx / svx) % svy, bz = idx / (svx * svy);
+    float lo = 3.402823466e+38f, hi = -3.402823466e+38f, sum = 0.0f;
+    int cnt = 0;
+    int o0 = halo ? -1 : 0, o1 = halo ? sv : sv - 1;
+    for (int oz = o0; oz <= o1; oz++) {
+        int z = bz * sv + oz;
+        for (int oy = o0; oy <= o1; oy++) {
+            int y = by * sv + oy;
+            for (int ox = o0; ox <= o1; ox++) {
+                int x = bx * sv + ox;
+                float v = 0.0f;
+                if (x >= 0 && y >= 0 && z >= 0 && x < nx && y < ny && z < nz) {
+                    v = __ldg(dens + ((size_t)z * ny + y) * nx + x);
+                }
+                lo = fminf(lo, v);
+                hi = fmaxf(hi, v);
+                sum += v;
+                cnt++;
+            }
+        }
+    }
+    float avg = sum / (float)cnt;
+    if ((nx % sv != 0 && bx == svx - 1) || (ny % sv != 0 && by == svy - 1) || (nz % sv != 0 && bz == svz - 1)) {
+        lo = 0.0f;
+    }
+    out_min[idx] = lo;
+    out_max[idx] = hi;
+    if (out_avg) out_avg[idx] = avg;
+    if (out_occ) out_occ[idx] = hi < 1e-5f ? 0 : 1;
+}
+
+// Residual-ratio-tracking control and residual extinctions (SuperVoxelGrid.cpp:218-256):
+// mu_r_bar = max(mu_max - mu_min, 0.1), mu_c = clamp(mu_min + mu_r_bar * gamma^(1/(D mu_r_bar) - 1),
+// mu_min, mu_avg) with gamma = 2, D = sqrt(3) * sv.
+__global__ void rrt_params_kernel(const float* __restrict__ mn, const float* __restrict__ mx,
+                                  const float* __restrict__ avg, int total, float extinction, float D,
+                                  float* __restrict__ out_pairs) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= total) return;
+    float mu_min = mn[i] * extinction, mu_max = mx[i] * extinction, mu_avg = avg[i] * extinction;
+    float mu_r = fmaxf(mu_max - mu_min, 0.1f);
+    float mu_c = mu_min + mu_r * powf(2.0f, (1.0f / (D * mu_r)) - 1.0f);
+    mu_c = fminf(fmaxf(mu_c, mu_min), mu_avg);
+    out_pairs[2 * i + 0] = mu_c;
+    out_pairs[2 * i + 1] = mu_r;
+}
+
+__global__ void interleave_kernel(const float* __restrict__ a, const float* __restrict__ b, int total,
+                                  float* __restrict__ out_pairs) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= total) return;
+    out_pairs[2 * i + 0] = a[i];
+    out_pairs[2 * i + 1] = b[i];
+}
+
+// Occupancy grid for NEE empty-space skipping.  The reference shader's loop never executes
+// (ComputeOccupancyGrid.glsl:108-109) so every block is marked occupied; `ref_compat` reproduces
+// that.  Otherwise one warp per block votes whether any voxel of the block (plus a one-voxel halo
+// for stochastic / trilinear lookups) exceeds `threshold`.
+__global__ void occupancy_kernel(const float* __restrict__ dens, int nx, int ny, int nz, int bs, int gx, int gy,
+                                 int gz, int halo, float threshold, int ref_compat, uint8_t* __restrict__ out) {
+    int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int lane = threadIdx.x & 31;
+    int total = gx * gy * gz;
+    if (warp >= total) return;
+    if (ref_compat) {
+        if (lane == 0) out[warp] = 1;
+        return;
+    }
+    int bx = warp % gx, by = (warp / gx) % gy, bz = warp / (gx * gy);
+    int ext = bs + 2 * halo;
+    int n = ext * ext * ext;
+    bool occ = false;
+    for (int i = lane; i < n && !__any_sync(__activemask(), occ); i += 32) {
+        int ox = i % ext - halo, oy = (i / ext) % ext - halo, oz = i / (ext * ext) - halo;
+        int x = bx * bs + ox, y = by * bs + oy, z = bz * bs + oz;
+        if (x >= 0 && y >= 0 && z >= 0 && x < nx && y < ny && z < nz) {
+            occ |= __ldg(dens + ((size_t)z * ny + y) * nx + x) > threshold;
+        }
+    }
+    occ = __any_sync(0xffffffffu, occ);
+    if (lane == 0) out[warp] = occ ? 1 : 0;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Octahedral max-luminance pyramid of the environment image (OctahedralMapper.glsl:65-85, then a
+// 2x2 box reduction per level like vkCmdBlitImage mip generation).
+__global__ void env_octahedral_level0_kernel(const __grid_constant__ TraceParams P, float* __restrict__ out, int res) {
+    int x = blockIdx.x * blockDim.x + threadIdx.x;
+    int y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= res || y >= res) return;
+    float best = -1.0f;
+    for (int i = 0; i < 5; i++) {
+        float sxo = 0.1f + 0.2f * (float)i;
+        for (int j = 0; j < 5; j++) {
+            float syo = 0.1f + 0.2f * (float)j;
+            float u = ((float)x + sxo) / (float)res;
+            float v = ((float)y + syo) / (float)res;
+            F3 dir = octahedral_uv_to_world(u, v);
+            float tu = atan2f(dir.z, dir.x) / (2.0f * kPi) + 0.5f;
+            float tv = -asinf(dir.y) / kPi + 0.5f;
+            F3 c = env_image_fetch(P, tu, tv);
+            c = f3(fminf(c.x, 100000.0f), fminf(c.y, 100000.0f), fminf(c.z, 100000.0f));
+            best = fmaxf(best, length3(c));
+        }
+    }
+    out[(size_t)y * res + x] = best;
+}
+
+__global__ void env_downsample_kernel(const float* __restrict__ in, float* __restrict__ out, int res_out) {
+    int x = blockIdx.x * blockDim.x + threadIdx.x;
+    int y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= res_out || y >= res_out) return;
+    int ri = res_out * 2;
+    float a = in[(size_t)(2 * y) * ri + 2 * x], b = in[(size_t)(2 * y) * ri + 2 * x + 1];
+    float c = in[(size_t)(2 * y + 1) * ri + 2 * x], d = in[(size_t)(2 * y + 1) * ri + 2 * x + 1];
+    out[(size_t)y * res_out + x] = ((a + b) + (c + d)) * 0.25f;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Film readout: mean = sum / frames as channels x H x W (alpha = 1 for 4 channels).
+__global__ void film_to_chw_kernel(const double* __restrict__ film, int width, int height, double inv_frames,
+                                   int channels, float* __restrict__ out) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int n = width * height;
+    if (i >= n) return;
+    for (int c = 0; c < 3; c++) out[(size_t)c * n + i] = (float)(film[(size_t)i * 3 + c] * inv_frames);
+    if (channels == 4) out[(size_t)3 * n + i] = 1.0f;
+}
+
+__global__ void film_to_rgba_kernel(const double* __restrict__ film, int n, double inv_frames, float4* __restrict__ out) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    out[i] = make_float4((float)(film[(size_t)i * 3 + 0] * inv_frames), (float)(film[(size_t)i * 3 + 1] * inv_frames),
+                         (float)(film[(size_t)i * 3 + 2] * inv_frames), 1.0f);
+}
+
+__global__ void rgba_to_chw_kernel(const float4* __restrict__ in, int n, int channels, float* __restrict__ out) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float4 v = in[i];
+    out[i] = v.x;
+    out[(size_t)n + i] = v.y;
+    out[(size_t)2 * n + i] = v.z;
+    if (channels == 4) out[(size_t)3 * n + i] = v.w;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Launchers (declared in vpt_kernels.h).
+
+static unsigned grid_for(size_t n, int block, unsigned cap = 148u * 32u) {
+    size_t g = (n + block - 1) / block;
+    if (g > cap) g = cap;
+    if (g == 0) g = 1;
+    return (unsigned)g;
+}
+
+cudaError_t launch_minmax(const float* v, size_t n, float* out_minmax, cudaStream_t s) {
+    float init[2] = {INFINITY, -INFINITY};
+    cudaMemcpyAsync(out_minmax, init, sizeof(init), cudaMemcpyHostToDevice, s);
+    minmax_kernel<<<grid_for(n, 256), 256, 0, s>>>(v, n, out_minmax);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_normalize(const float* in, float* out, size_t n, float vmin, float vmax, cudaStream_t s) {
+    normalize_kernel<<<grid_for(n, 256), 256, 0, s>>>(in, out, n, vmin, vmax);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fbm(float* out, int nx, int ny, int nz, const int* perm512, const FbmParams& fp, cudaStream_t s) {
+    PermTable t;
+    for (int i = 0; i < 512; i++) t.p[i] = perm512[i];
+    size_t n = (size_t)nx * ny * nz;
+    fbm_kernel<<<grid_for(n, 256), 256, 0, s>>>(out, nx, ny, nz, t, fp);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_supervoxel_stats(const float* dens, int nx, int ny, int nz, int sv, int svx, int svy, int svz,
+                                    int halo, float* mn, float* mx, float* avg, uint8_t* occ, cudaStream_t s) {
+    int total = svx * svy * svz;
+    supervoxel_stats_kernel<<<(total + 127) / 128, 128, 0, s>>>(dens, nx, ny, nz, sv, svx, svy, svz, halo, mn, mx,
+                                                                avg, occ);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_rrt_params(const float* mn, const float* mx, const float* avg, int total, float extinction,
+                              float D, float* out_pairs, cudaStream_t s) {
+    rrt_params_kernel<<<(total + 255) / 256, 256, 0, s>>>(mn, mx, avg, total, extinction, D, out_pairs);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_interleave(const float* a, const float* b, int total, float* out_pairs, cudaStream_t s) {
+    interleave_kernel<<<(total + 255) / 256, 256, 0, s>>>(a, b, total, out_pairs);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_occupancy(const float* dens, int nx, int ny, int nz, int bs, int gx, int gy, int gz, int halo,
+                             float threshold, int ref_compat, uint8_t* out, cudaStream_t s) {
+    int total = gx * gy * gz;
+    size_t threads = (size_t)total * 32;
+    occupancy_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(dens, nx, ny, nz, bs, gx, gy, gz, halo,
+                                                                       threshold, ref_compat, out);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_env_pyramid(const TraceParams& P, float* pyramid, const uint64_t* level_offsets_host, int levels,
+                               cudaStream_t s) {
+    int res = 1 << levels;
+    dim3 b(16, 16);
+    env_octahedral_level0_kernel<<<dim3((res + 15) / 16, (res + 15) / 16), b, 0, s>>>(P, pyramid, res);
+    count_launches((unsigned)levels);
+    for (int l = 1; l < levels; l++) {
+        int r = res >> l;
+        env_downsample_kernel<<<dim3((r + 15) / 16, (r + 15) / 16), b, 0, s>>>(
+            pyramid + level_offsets_host[l - 1], pyramid + level_offsets_host[l], r);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_film_to_chw(const double* film, int width, int height, double inv_frames, int channels,
+                               float* out, cudaStream_t s) {
+    int n = width * height;
+    film_to_chw_kernel<<<(n + 255) / 256, 256, 0, s>>>(film, width, height, inv_frames, channels, out);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_film_to_rgba(const double* film, int n, double inv_frames, float* out_rgba, cudaStream_t s) {
+    film_to_rgba_kernel<<<(n + 255) / 256, 256, 0, s>>>(film, n, inv_frames, reinterpret_cast<float4*>(out_rgba));
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_rgba_to_chw(const float* rgba, int n, int channels, float* out, cudaStream_t s) {
+    rgba_to_chw_kernel<<<(n + 255) / 256, 256, 0, s>>>(reinterpret_cast<const float4*>(rgba), n, channels, out);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+}  // namespace vpt

@@ -1,0 +1,46 @@
+// vpt_kernels.h - host-side declarations of the kernel launchers in vpt_kernels.cu.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "vpt_params.h"
+
+namespace vpt {
+
+constexpr int kTraceBlock = 128;
+
+enum Schedule : int { kScheduleTiles = 0, kSchedulePersistent = 1 };
+
+struct FbmParams {
+    int octaves;
+    float lacunarity;
+    float gain;
+    float base_frequency;
+    float threshold;
+    float contrast;
+    float inv_max_dim;
+};
+
+uint64_t padded_paths(int width, int height, uint32_t frames);
+void count_launches(unsigned n);
+unsigned long long launch_count();
+
+cudaError_t launch_trace(const TraceParams& P, int tracker, int use_ess, int schedule, int features,
+                         int persistent_blocks, cudaStream_t stream);
+cudaError_t launch_minmax(const float* v, size_t n, float* out_minmax, cudaStream_t s);
+cudaError_t launch_normalize(const float* in, float* out, size_t n, float vmin, float vmax, cudaStream_t s);
+cudaError_t launch_fbm(float* out, int nx, int ny, int nz, const int* perm512, const FbmParams& fp, cudaStream_t s);
+cudaError_t launch_supervoxel_stats(const float* dens, int nx, int ny, int nz, int sv, int svx, int svy, int svz,
+                                    int halo, float* mn, float* mx, float* avg, uint8_t* occ, cudaStream_t s);
+cudaError_t launch_rrt_params(const float* mn, const float* mx, const float* avg, int total, float extinction,
+                              float D, float* out_pairs, cudaStream_t s);
+cudaError_t launch_interleave(const float* a, const float* b, int total, float* out_pairs, cudaStream_t s);
+cudaError_t launch_occupancy(const float* dens, int nx, int ny, int nz, int bs, int gx, int gy, int gz, int halo,
+                             float threshold, int ref_compat, uint8_t* out, cudaStream_t s);
+cudaError_t launch_env_pyramid(const TraceParams& P, float* pyramid, const uint64_t* level_offsets_host, int levels,
+                               cudaStream_t s);
+cudaError_t launch_film_to_chw(const double* film, int width, int height, double inv_frames, int channels,
+                               float* out, cudaStream_t s);
+cudaError_t launch_film_to_rgba(const double* film, int n, double inv_frames, float* out_rgba, cudaStream_t s);
+cudaError_t launch_rgba_to_chw(const float* rgba, int n, int channels, float* out, cudaStream_t s);
+
+}  // namespace vpt

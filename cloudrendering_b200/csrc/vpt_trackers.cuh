@@ -1,0 +1,476 @@
+// vpt_trackers.cuh - free-path samplers of the tracer, one device function per VptMode.
+//
+// Each function follows one reference shader (cited per function) and consumes random numbers in
+// exactly the same order, so a path traced here and the same path traced by the CPU oracle take
+// the same decisions.  Grid access goes through a sampler object `S` with
+//     float operator()(F3 world_pos, Rng& rng)   -> normalised density at world_pos
+// so the dense texture and the NanoVDB tree share the trackers.
+#pragma once
+#include "vpt_device.cuh"
+
+namespace vpt {
+
+struct FirstEvent {
+    bool has;
+    F3 x;
+    float depth;
+    float density;
+};
+
+struct PathCtx {
+    uint32_t steps;      // tentative collisions + supervoxel steps of this path (guard)
+    uint32_t max_steps;  // TraceParams::max_steps
+    uint32_t lookups;    // density lookups of this path
+    bool guard_hit;
+};
+
+VPT_DEV bool guard(PathCtx& pc) {
+    if (++pc.steps > pc.max_steps) {
+        pc.guard_hit = true;
+        return true;
+    }
+    return false;
+}
+
+VPT_DEV float free_path(Rng& rng, float inv_majorant) {
+    return -logf(fmaxf(0.0000000001f, 1.0f - rng_next(rng))) * inv_majorant;
+}
+
+VPT_DEV void record_event(FirstEvent& fe, F3 x, float density, float extinction, float depth) {
+    if (!fe.has) {
+        fe.has = true;
+        fe.x = x;
+        fe.density = density * extinction;
+        fe.depth = depth;
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Analog delta (Woodcock) tracking: absorb with P_a, scatter with P_s, null collision otherwise;
+// escape radiance = sky + sun lobe (deltaTracking, DeltaTracking.glsl:168-344).
+template <class S>
+VPT_DEV F3 track_delta(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, FirstEvent& fe, PathCtx& pc) {
+    float tmin, tmax;
+    if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
+        x = x + w * tmin;
+        float d = tmax - tmin;
+        int bounces = 0;
+        while (true) {
+            if (guard(pc)) return f3(0.0f, 0.0f, 0.0f);
+            float t = free_path(rng, P.inv_extinction);
+            if (t > d) break;
+            F3 xn = x + w * t;
+            float density = sample(xn, rng);
+            pc.lookups++;
+            x = xn;
+            float xi = rng_next(rng);
+            if (xi < P.absorb_albedo * density) {
+                record_event(fe, x, density, P.extinction, tmax - d + t);
+                return f3(0.0f, 0.0f, 0.0f);
+            }
+            if (xi < density) {
+                if (P.max_bounces > 0 && ++bounces > P.max_bounces) return f3(0.0f, 0.0f, 0.0f);
+                w = sample_phase(rng, P.g, w);
+                record_event(fe, x, density, P.extinction, tmax - d + t);
+                if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
+                    x = x + w * tmin;
+                    d = tmax - tmin;
+                }
+            } else {
+                d -= t;
+            }
+        }
+    }
+    return sky_and_sun(P, w);
+}
+
+// VptMode::RATIO_TRACKING: delta tracking that never absorbs and weights each real collision by
+// the single-scattering albedo (ratioTracking, RatioTracking.glsl:26-95).
+template <class S>
+VPT_DEV F3 track_ratio(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, FirstEvent& fe, PathCtx& pc) {
+    float trans = 1.0f;
+    float tmin, tmax;
+    if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
+        x = x + w * tmin;
+        float d = tmax - tmin;
+        int bounces = 0;
+        while (true) {
+            if (guard(pc)) return f3(0.0f, 0.0f, 0.0f);
+            float t = free_path(rng, P.inv_extinction);
+            if (t > d) break;
+            x = x + w * t;
+            float density = sample(x, rng);
+            pc.lookups++;
+            float xi = rng_next(rng);
+            if (xi < density) {
+                if (P.max_bounces > 0 && ++bounces > P.max_bounces) return f3(0.0f, 0.0f, 0.0f);
+                float pa = P.absorb_albedo * density;
+                float ps = P.albedo * density;
+                trans *= 1.0f - pa / (pa + ps);
+                w = sample_phase(rng, P.g, w);
+                if (!fe.has) {
+                    fe.has = true;
+                    fe.x = x;
+                    fe.density = 0.0f;
+                    fe.depth = 0.0f;
+                }
+                if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
+                    x = x + w * tmin;
+                    d = tmax - tmin;
+                }
+            } else {
+                d -= t;
+            }
+        }
+    }
+    return sky_and_sun(P, w) * trans;
+}
+
+// Ratio-tracking transmittance toward the light (calculateTransmittance without occupancy grid,
+// NeeTransmittance.glsl:5-119; T *= P_n = 1 - density per tentative collision).
+template <class S>
+VPT_DEV float shadow_transmittance(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, PathCtx& pc) {
+    float trans = 1.0f;
+    float tmin, tmax;
+    if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
+        x = x + w * tmin;
+        float d = tmax - tmin;
+        while (true) {
+            if (guard(pc)) return 0.0f;
+            float t = free_path(rng, P.inv_extinction);
+            if (t > d) break;
+            F3 xn = x + w * t;
+            float density = sample(xn, rng);
+            pc.lookups++;
+            x = xn;
+            trans *= 1.0f - density;
+            d -= t;
+        }
+    }
+    return trans;
+}
+
+// Ratio-tracking transmittance with empty-space skipping over the occupancy grid
+// (calculateTransmittance with USE_OCCUPANCY_GRID, NeeTransmittance.glsl:121-259).
+template <class S>
+VPT_DEV float shadow_transmittance_ess(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, PathCtx& pc) {
+    float trans = 1.0f;
+    const F3 eps = f3(1e-6f, 1e-6f, 1e-6f);
+    float tmin_val, tmax_val;
+    if (!ray_box(P.box_min + eps, P.box_max - eps, x, w, tmin_val, tmax_val)) return trans;
+    F3 delta = P.box_max - P.box_min;
+    x = x + w * tmin_val;
+    F3 sp = (((x - P.box_min) / delta) * f3((float)P.nx, (float)P.ny, (float)P.nz)) /
+            f3((float)P.sv_size, (float)P.sv_size, (float)P.sv_size);
+    int ix = (int)floorf(sp.x), iy = (int)floorf(sp.y), iz = (int)floorf(sp.z);
+    int cx = ix, cy = iy, cz = iz;
+    bool empty = false;
+    while (ix >= 0 && iy >= 0 && iz >= 0 && ix < P.svx && iy < P.svy && iz < P.svz) {
+        if (guard(pc)) return 0.0f;
+        F3 smin = P.box_min + f3((float)ix, (float)iy, (float)iz) * P.sv_world;
+        F3 smax = smin + P.sv_world;
+        float tmin_sv = 0.0f, tmax_sv = 0.0f;
+        ray_box(smin, smax, x, w, tmin_sv, tmax_sv);
+        float d_max = tmax_sv - tmin_sv;
+        x = x + w * tmin_sv;
+        if (cx != ix || cy != iy || cz != iz) {
+            empty = __ldg(P.occupancy + ((size_t)iz * P.svy + iy) * P.svx + ix) == 0;
+            cx = ix;
+            cy = iy;
+            cz = iz;
+        }
+        if (empty) {
+            x = x + w * d_max;
+        } else {
+            // The reference advances x to each sample while t keeps counting from the supervoxel
+            // entry, so its samples overshoot (NeeTransmittance.glsl:173-228); ess_ref_compat keeps
+            // that behaviour, the default measures t from the entry point.
+            const F3 x0 = x;
+            float t = 0.0f;
+            while (true) {
+                if (guard(pc)) return 0.0f;
+                t -= logf(fmaxf(0.0000000001f, 1.0f - rng_next(rng))) * P.inv_extinction;
+                if (t >= d_max) {
+                    x = (P.ess_ref_compat ? x : x0) + w * d_max;
+                    break;
+                }
+                F3 xn = (P.ess_ref_compat ? x : x0) + w * t;
+                float density = sample(xn, rng);
+                pc.lookups++;
+                x = xn;
+                trans *= 1.0f - density;
+            }
+        }
+        F3 center = (smin + smax) * 0.5f;
+        F3 mov = (x + w * 0.00001f) - center;
+        float sx = signf(mov.x), sy = signf(mov.y), sz = signf(mov.z);
+        mov = f3(mov.x * sx, mov.y * sy, mov.z * sz);
+        int dx = (mov.x >= mov.y && mov.x >= mov.z) ? 1 : 0;
+        int dy = (mov.y >= mov.x && mov.y >= mov.z) ? 1 : 0;
+        int dz = (mov.z >= mov.x && mov.z >= mov.y) ? 1 : 0;
+        ix += dx * (int)sx;
+        iy += dy * (int)sy;
+        iz += dz * (int)sz;
+    }
+    return trans;
+}
+
+// Next-event tracking: delta-tracked path; at each scatter one light sample toward the sky / sun
+// with ratio-tracked transmittance; escape radiance only if no event happened
+// (nextEventTracking, NextEventTracking.glsl:224-393; lights are not supported).
+template <bool ESS, class S>
+VPT_DEV F3 track_nee(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, FirstEvent& fe, PathCtx& pc) {
+    F3 color = f3(0.0f, 0.0f, 0.0f);
+    float tmin, tmax;
+    if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
+        x = x + w * tmin;
+        float d = tmax - tmin;
+        int bounces = 0;
+        while (true) {
+            if (guard(pc)) return color;
+            float t = free_path(rng, P.inv_extinction);
+            if (t > d) break;
+            F3 xn = x + w * t;
+            float density = sample(xn, rng);
+            pc.lookups++;
+            x = xn;
+            float xi = rng_next(rng);
+            if (xi < P.absorb_albedo * density) {
+                record_event(fe, x, density, P.extinction, tmax - d + t);
+                return color;
+            }
+            if (xi < density) {
+                if (P.max_bounces > 0 && ++bounces > P.max_bounces) return color;
+                F3 next_w = sample_phase(rng, P.g, w);
+                record_event(fe, x, density, P.extinction, tmax - d + t);
+                float pdf_light;
+                F3 dir_light = importance_sample_sky(P, rng, pdf_light);
+                float pdf_phase = evaluate_phase(P.g, w, dir_light);
+                w = next_w;
+                float tr = ESS ? shadow_transmittance_ess(P, sample, rng, x, dir_light, pc)
+                               : shadow_transmittance(P, sample, rng, x, dir_light, pc);
+                float f = (pdf_phase / pdf_light) * tr;
+                F3 l = sky_and_sun(P, dir_light);
+                color = color + f3(f * l.x, f * l.y, f * l.z);
+                if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
+                    x = x + w * tmin;
+                    d = tmax - tmin;
+                }
+            } else {
+                d -= t;
+            }
+        }
+    }
+    if (!fe.has) color = color + sky_and_sun(P, w);
+    return color;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Supervoxel stepping shared by decomposition tracking and the occupancy-grid shadow ray: after a
+// supervoxel is left, move to the neighbour along the dominant axis of (x + 1e-5 w - centre)
+// (DecompositionTracking.glsl:112-118).
+VPT_DEV void sv_step(F3 smin, F3 smax, F3 x, F3 w, int& ix, int& iy, int& iz) {
+    F3 center = (smin + smax) * 0.5f;
+    F3 mov = (x + w * 0.00001f) - center;
+    float sx = signf(mov.x), sy = signf(mov.y), sz = signf(mov.z);
+    mov = f3(mov.x * sx, mov.y * sy, mov.z * sz);
+    int dx = (mov.x >= mov.y && mov.x >= mov.z) ? 1 : 0;
+    int dy = (mov.y >= mov.x && mov.y >= mov.z) ? 1 : 0;
+    int dz = (mov.z >= mov.x && mov.z >= mov.y) ? 1 : 0;
+    ix += dx * (int)sx;
+    iy += dy * (int)sy;
+    iz += dz * (int)sz;
+}
+
+// Analog decomposition tracking over the dense supervoxel grid: per supervoxel a control
+// extinction mu_c = majorant * min and a residual majorant majorant * max - mu_c; competing
+// exponential samples t_c, t_r; residual collisions accepted with (mu(x) - mu_c) / mu_r
+// (analogDecompositionTracking, DecompositionTracking.glsl:35-123).
+template <class S>
+VPT_DEV F3 track_decomposition(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, FirstEvent& fe,
+                               PathCtx& pc) {
+    const F3 eps = f3(1e-6f, 1e-6f, 1e-6f);
+    float tmin_val, tmax_val;
+    if (ray_box(P.box_min + eps, P.box_max - eps, x, w, tmin_val, tmax_val)) {
+        const float majorant = P.extinction;
+        F3 delta = P.box_max - P.box_min;
+        x = x + w * tmin_val;
+        F3 sp = (((x - P.box_min) / delta) * f3((float)P.nx, (float)P.ny, (float)P.nz)) /
+                f3((float)P.sv_size, (float)P.sv_size, (float)P.sv_size);
+        int ix = (int)floorf(sp.x), iy = (int)floorf(sp.y), iz = (int)floorf(sp.z);
+        int cx = -1, cy = -1, cz = -1;
+        float smin_d = 0.0f, smax_d = 0.0f;
+        int bounces = 0;
+        while (ix >= 0 && iy >= 0 && iz >= 0 && ix < P.svx && iy < P.svy && iz < P.svz) {
+            if (guard(pc)) return f3(0.0f, 0.0f, 0.0f);
+            F3 smin = P.box_min + f3((float)ix, (float)iy, (float)iz) * P.sv_world;
+            F3 smax = smin + P.sv_world;
+            float tmin_sv = 0.0f, tmax_sv = 0.0f;
+            ray_box(smin, smax, x, w, tmin_sv, tmax_sv);
+            float d_max = tmax_sv - tmin_sv;
+            x = x + w * tmin_sv;
+            if (cx != ix || cy != iy || cz != iz) {
+                const float2 mm = __ldg(reinterpret_cast<const float2*>(P.sv_data) + ((size_t)iz * P.svy + iy) * P.svx + ix);
+                smin_d = mm.x;
+                smax_d = mm.y;
+                cx = ix;
+                cy = iy;
+                cz = iz;
+            }
+            if (smax_d < 1e-5f) {
+                x = x + w * d_max;
+            } else {
+                float mu_c = fmaxf(0.0000000001f, majorant * smin_d);
+                float mu_r = fmaxf(0.0000000001f, majorant * smax_d - mu_c);
+                float t_c = -logf(fmaxf(0.0000000001f, 1.0f - rng_next(rng))) / mu_c;
+                float t_r = 0.0f;
+                while (true) {
+                    if (guard(pc)) return f3(0.0f, 0.0f, 0.0f);
+                    t_r -= logf(fmaxf(0.0000000001f, 1.0f - rng_next(rng))) / mu_r;
+                    if (t_c >= d_max && t_r >= d_max) {
+                        x = x + w * d_max;
+                        break;
+                    }
+                    F3 xs = x + w * fminf(t_c, t_r);
+                    bool collision;
+                    if (t_c <= t_r) {
+                        collision = true;
+                    } else {
+                        float density = sample(xs, rng);
+                        pc.lookups++;
+                        collision = rng_next(rng) * mu_r < P.extinction * density - mu_c;
+                    }
+                    if (collision) {
+                        x = xs;
+                        if (rng_next(rng) < P.absorb_albedo) return f3(0.0f, 0.0f, 0.0f);
+                        if (P.max_bounces > 0 && ++bounces > P.max_bounces) return f3(0.0f, 0.0f, 0.0f);
+                        w = sample_phase(rng, P.g, w);
+                        t_r = 0.0f;
+                        t_c = -logf(fmaxf(0.0000000001f, 1.0f - rng_next(rng))) / mu_c;
+                        ray_box(smin, smax, x, w, tmin_sv, tmax_sv);
+                        d_max = tmax_sv - tmin_sv;
+                    }
+                }
+            }
+            sv_step(smin, smax, x, w, ix, iy, iz);
+        }
+    }
+    return sky_and_sun(P, w);
+}
+
+// Per-supervoxel residual ratio tracking estimator with reservoir selection of the next
+// in-scattering distance (residualRatioTrackingEstimator, ResidualRatioTracking.glsl:34-76).
+template <class S>
+VPT_DEV float rrt_estimator(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, float d_start, float d_end,
+                            float T, float& wsum, float& res_t, float& res_dist, float mu_c, float mu_r,
+                            PathCtx& pc) {
+    float t_c = expf(-mu_c * (d_end - d_start));
+    float t_r = 1.0f;
+    float d_trav = d_start;
+    while (true) {
+        if (guard(pc)) break;
+        float t = -logf(fmaxf(0.0000000001f, 1.0f - rng_next(rng))) / mu_r;
+        x = x + w * t;
+        d_trav += t;
+        if (d_trav >= d_end) break;
+        float density = sample(x, rng);
+        pc.lookups++;
+        float mu = P.extinction * density;
+        t_r *= 1.0f - (mu - mu_c) / mu_r;
+        float t_c_local = expf(-mu_c * (d_trav - d_start));
+        float t_local = (T * t_r) * t_c_local;
+        wsum += t_local;
+        float xi = rng_next(rng);
+        if (xi < t_local / wsum) {
+            res_t = t_local;
+            res_dist = d_trav;
+        }
+    }
+    return t_c * t_r;
+}
+
+VPT_DEV float fractf(float v) { return v - floorf(v); }
+
+// Residual ratio tracking over the supervoxel (mu_c, mu_r_bar) grid with an Amanatides-Woo DDA and
+// up to 10 reservoir-sampled in-scattering rays (residualRatioTracking,
+// ResidualRatioTracking.glsl:78-223; the reference marks this estimator "work in progress").
+template <class S>
+VPT_DEV F3 track_residual_ratio(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, FirstEvent& fe,
+                                PathCtx& pc) {
+    float wsum = 0.0f, res_t = 0.0f, res_dist = 0.0f;
+    float T = 1.0f;
+    F3 acc = f3(0.0f, 0.0f, 0.0f);
+    const F3 eps = f3(1e-6f, 1e-6f, 1e-6f);
+    const F3 n = f3((float)P.nx, (float)P.ny, (float)P.nz);
+    const F3 sv = f3((float)P.sv_size, (float)P.sv_size, (float)P.sv_size);
+    F3 delta = P.box_max - P.box_min;
+    F3 old_x = x;
+    int iteration = 0;
+    while (true) {
+        float tmin_val, tmax_val;
+        if (!ray_box(P.box_min + eps, P.box_max - eps, x, w, tmin_val, tmax_val)) break;
+        x = x + w * tmin_val;
+        old_x = x;
+        float d_total = tmax_val - tmin_val;
+        F3 sp = (((x - P.box_min) / delta) * n) / sv;
+        F3 ep = ((((x + w * d_total) - P.box_min) / delta) * n) / sv;
+        float spv[3] = {sp.x, sp.y, sp.z};
+        float epv[3] = {ep.x, ep.y, ep.z};
+        int step[3], idx[3];
+        float tdel[3], tmx[3];
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            float diff = epv[a] - spv[a];
+            step[a] = (int)signf(diff);
+            tdel[a] = step[a] != 0 ? fminf((float)step[a] / diff, 1e7f) : 1e7f;
+            tmx[a] = step[a] > 0 ? tdel[a] * (1.0f - fractf(spv[a])) : tdel[a] * fractf(spv[a]);
+            idx[a] = (int)floorf(spv[a]);
+        }
+        if (step[0] == 0 && step[1] == 0 && step[2] == 0) break;
+        while (idx[0] >= 0 && idx[1] >= 0 && idx[2] >= 0 && idx[0] < P.svx && idx[1] < P.svy && idx[2] < P.svz) {
+            if (guard(pc)) return acc;
+            const float2 sv_val =
+                __ldg(reinterpret_cast<const float2*>(P.sv_data) + ((size_t)idx[2] * P.svy + idx[1]) * P.svx + idx[0]);
+            F3 vmin = f3((float)(idx[0] * P.sv_size), (float)(idx[1] * P.sv_size), (float)(idx[2] * P.sv_size));
+            F3 vmax = f3((float)(idx[0] * P.sv_size + P.sv_size), (float)(idx[1] * P.sv_size + P.sv_size),
+                         (float)(idx[2] * P.sv_size + P.sv_size));
+            vmin = (vmin / n) * delta + P.box_min;
+            vmax = (vmax / n) * delta + P.box_min;
+            float tmin_v = 0.0f, tmax_v = 0.0f;
+            ray_box(vmin, vmax, old_x, w, tmin_v, tmax_v);
+            x = old_x + w * tmin_v;
+            T *= rrt_estimator(P, sample, rng, x, w, tmin_v, tmax_v, T, wsum, res_t, res_dist, sv_val.x, sv_val.y, pc);
+            if (tmx[0] < tmx[1]) {
+                if (tmx[0] < tmx[2]) {
+                    idx[0] += step[0];
+                    tmx[0] += tdel[0];
+                } else {
+                    idx[2] += step[2];
+                    tmx[2] += tdel[2];
+                }
+            } else {
+                if (tmx[1] < tmx[2]) {
+                    idx[1] += step[1];
+                    tmx[1] += tdel[1];
+                } else {
+                    idx[2] += step[2];
+                    tmx[2] += tdel[2];
+                }
+            }
+        }
+        float xi = rng_next(rng);
+        if (xi > wsum || iteration >= 10) break;
+        acc = acc + sky_and_sun(P, w) * T;
+        iteration++;
+        T = res_t;
+        x = old_x + w * res_dist;
+        w = sample_phase(rng, P.g, w);
+        wsum = 0.0f;
+        res_t = 0.0f;
+        res_dist = 0.0f;
+    }
+    acc = acc + sky_and_sun(P, w) * T;
+    return acc;
+}
+
+}  // namespace vpt

@@ -1,0 +1,438 @@
+"""Drop-in mirror of the reference's ``vpt`` PyTorch module for the path-tracing hot path.
+
+Same function names, argument meanings and error behaviour as ``src/PyTorch/vpt.pyi`` /
+``src/PyTorch/Module.cpp`` of chrismile/CloudRendering for the functions on the tracing path; every
+call goes to the CUDA core through its C ABI (include/vpt_b200.h).  torch is used only for tensors
+and the current CUDA stream.
+
+Differences, all documented supersets:
+* ``render_frame`` on CUDA returns a fresh tensor instead of a view of an internal buffer that the
+  next call overwrites (Module.cpp:687-692).
+* extra entry points: ``set_density_field`` (CloudData::setDensityField), ``generate_fbm_cloud``,
+  ``set_grid_interpolation``, ``set_max_bounces``, ``set_sun``, ``set_sky_color``, ``get_stats``.
+* the builtin environment map list gains "Constant Sky + Sun" (constant sky plus the reference's
+  Phong sun lobe, visible to every tracker).
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+import struct
+from typing import List, Optional
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import check, farr
+
+# RenderSettings.hpp:37-41
+VPT_MODE_NAMES = [
+    "Delta Tracking", "Delta Tracking (Spectral)", "Ratio Tracking", "Decomposition Tracking",
+    "Residual Ratio Tracking", "Next Event Tracking", "Next Event Tracking (Spectral)", "Isosurfaces",
+    "Ray Marching (Emission/Absorption)",
+]
+# RenderSettings.hpp:56-58
+GRID_INTERPOLATION_TYPE_NAMES = ["Nearest", "Stochastic", "Trilinear"]
+# RenderSettings.hpp:123-125 (+ one addition)
+BUILTIN_ENV_MAP_NAMES = ["Default", "Black", "Single Color", "Constant Sky + Sun"]
+# Denoiser.hpp:63-79 (names of the denoisers built here)
+DENOISER_NAMES = {"None": 0, "Edge-Avoiding À-Trous Wavelet Transform": 1, "SVGF": 2}
+# VolumetricPathTracingPass.hpp:74-80 (+ the new 2D transmittance feature)
+VPT_FEATURE_MAP_NAMES = [
+    "Result", "First X", "First W", "Normal", "Normal (Length 1)", "Cloud Only", "Depth", "Depth Far",
+    "Flow", "Flow Reverse", "Depth (nabla)", "Depth (fwidth)", "Density", "Background", "Reprojected UV",
+    "Depth Blended", "Depth Nearest Opaque", "Albedo", "Transmittance Volume",
+    "Primary Ray Absorption Moments", "Scatter Ray Absorption Moments",
+]
+FEATURE_TRANSMITTANCE = 32
+_FEATURE_BY_NAME = {n: i for i, n in enumerate(VPT_FEATURE_MAP_NAMES)}
+_FEATURE_BY_NAME["Transmittance"] = FEATURE_TRANSMITTANCE
+
+
+class _State:
+    ctx: Optional[int] = None
+    refcount: int = 0
+    device: int = 0
+    cam_pos = [0.0, 0.0, 0.8]
+    cam_target = [0.0, 0.0, 0.0]
+    cam_up = [0.0, 1.0, 0.0]
+    fovy = 2.0 * math.atan(0.5)
+    near = 1.0 / 512.0
+    far = 80.0
+    view_override: Optional[List[float]] = None
+    grid_size = (0, 0, 0)
+    env_intensity = 1.0
+
+
+S = _State()
+
+
+def _ctx():
+    if S.ctx is None:
+        raise RuntimeError("vpt is not initialized: call initialize() first")
+    return S.ctx
+
+
+def _c(name: str, *args):
+    lib = _lib.load()
+    check(getattr(lib, name)(_ctx(), *args), name, _ctx())
+
+
+def _apply_camera():
+    if S.view_override is not None:
+        _c("vpt_set_view_matrix", farr(S.view_override))
+    else:
+        _c("vpt_set_camera", farr(S.cam_pos), farr(S.cam_target), farr(S.cam_up), S.fovy, S.near, S.far)
+
+
+def _fog_sphere(radius=0.25, voxel_size=0.01, half_width=3.0):
+    """Dense counterpart of nanovdb::createFogVolumeSphere (the reference's default scene,
+    Module.cpp:792-796): 1 inside, a linear ramp over `half_width` voxels at the surface."""
+    n = int(math.ceil(2.0 * (radius + half_width * voxel_size) / voxel_size))
+    c = (np.arange(n, dtype=np.float64) + 0.5) * voxel_size - n * voxel_size / 2.0
+    z, y, x = np.meshgrid(c, c, c, indexing="ij")
+    sdf = np.sqrt(x * x + y * y + z * z) - radius
+    fog = np.clip(-sdf / (half_width * voxel_size), 0.0, 1.0).astype(np.float32)
+    return np.ascontiguousarray(fog)
+
+
+# ---- life cycle (Module.cpp:732-813) ----
+def initialize() -> None:
+    if S.refcount == 0:
+        lib = _lib.load()
+        ctx = ctypes.c_void_p()
+        dev = torch.cuda.current_device() if torch.cuda.is_available() else 0
+        st = lib.vpt_create(ctypes.byref(ctx), dev)
+        if st != 0:
+            raise RuntimeError(f"vpt_create failed: {lib.vpt_status_string(st).decode()}")
+        S.ctx = ctx.value
+        S.device = dev
+        fog = _fog_sphere()
+        set_density_field(torch.from_numpy(fog))
+        _c("vpt_set_vpt_mode", 0)
+        _c("vpt_set_use_linear_rgb", 1)
+        _apply_camera()
+    S.refcount += 1
+
+
+def cleanup() -> None:
+    if S.refcount <= 0:
+        return
+    S.refcount -= 1
+    if S.refcount == 0:
+        _lib.load().vpt_destroy(S.ctx)
+        S.ctx = None
+
+
+# ---- volume data ----
+def set_density_field(density: torch.Tensor) -> None:
+    """CloudData::setDensityField for a [Z, Y, X] (x fastest) float32 tensor on any device."""
+    if density.dim() != 3:
+        raise RuntimeError("Error in set_density_field: expected a 3D tensor [Z, Y, X].")
+    d = density.detach().to(torch.float32).contiguous()
+    nz, ny, nx = d.shape
+    on_dev = 1 if d.is_cuda else 0
+    _c("vpt_set_dense_grid", ctypes.c_void_p(d.data_ptr()), nx, ny, nz, on_dev)
+    if on_dev:
+        torch.cuda.synchronize(d.device)
+    S.grid_size = (nx, ny, nz)
+
+
+def generate_fbm_cloud(size, seed: int = 1, octaves: int = 6, lacunarity: float = 2.0, gain: float = 0.5,
+                       base_frequency: float = 3.0, threshold: float = 0.3) -> None:
+    """Seeded fBm Perlin cloud generated on the GPU (no reference counterpart)."""
+    nx, ny, nz = (size, size, size) if isinstance(size, int) else size
+    _c("vpt_generate_fbm_grid", nx, ny, nz, seed, octaves, lacunarity, gain, base_frequency, threshold)
+    S.grid_size = (nx, ny, nz)
+
+
+def load_cloud_file(filename: str) -> None:
+    """Loads a dense .xyz grid (CloudData::loadFromXyzFile, CloudData.cpp:236-317)."""
+    if not os.path.exists(filename):
+        raise RuntimeError(f"Error in CloudData::loadFromFile: The file \"{filename}\" does not exist.")
+    if not filename.endswith(".xyz"):
+        raise RuntimeError(f"Error in CloudData::loadFromFile: unsupported file format \"{filename}\".")
+    with open(filename, "rb") as f:
+        buf = f.read()
+    xs, ys, zs = struct.unpack_from("<3I", buf, 0)
+    vx, vy, vz = struct.unpack_from("<3d", buf, 12)
+    n = xs * ys * zs
+    data = np.frombuffer(buf, dtype="<f4", count=n, offset=36).astype(np.float32)
+    grid = data.reshape(xs, ys, zs).transpose(2, 1, 0).copy()  # z-fastest file -> x-fastest
+    lo = min(0.0, float(grid.min()))
+    hi = float(grid.max())
+    if hi - lo > 1e-6:
+        grid = (grid - np.float32(lo)) / np.float32(hi - lo)
+    _c("vpt_set_voxel_size", vx, vy, vz)
+    set_density_field(torch.from_numpy(np.ascontiguousarray(grid, dtype=np.float32)))
+
+
+load_volume_file = load_cloud_file
+
+
+def set_max_grid_extent(max_grid_extent: float) -> None:
+    _c("vpt_set_max_grid_extent", float(max_grid_extent))
+
+
+def get_render_bounding_box() -> List[float]:
+    out = (ctypes.c_float * 6)()
+    _c("vpt_get_render_bounding_box", out)
+    return [out[0], out[3], out[1], out[4], out[2], out[5]]
+
+
+def get_volume_voxel_size() -> List[int]:
+    nx, ny, nz = S.grid_size
+    return [nz, ny, nx]
+
+
+# ---- medium ----
+def set_scattering_albedo(albedo: List[float]) -> None:
+    _c("vpt_set_scattering_albedo", farr(_vec3(albedo, "setScatteringAlbedo")))
+
+
+def set_extinction_scale(extinction_scale: float) -> None:
+    _c("vpt_set_extinction_scale", float(extinction_scale))
+
+
+def set_extinction_base(extinction_base: List[float]) -> None:
+    _c("vpt_set_extinction_base", farr(_vec3(extinction_base, "setExtinctionBase")))
+
+
+def set_phase_g(phase_g: float) -> None:
+    _c("vpt_set_phase_g", float(phase_g))
+
+
+def _vec3(v, where):
+    if len(v) != 3:
+        raise RuntimeError(f"Error in parseVector3: Expected vector of size 3 ({where}).")
+    return [float(x) for x in v]
+
+
+# ---- mode and sampling ----
+def set_vpt_mode(mode: int) -> None:
+    _c("vpt_set_vpt_mode", int(mode))
+
+
+def set_vpt_mode_from_name(mode_name: str) -> None:
+    if mode_name in VPT_MODE_NAMES:
+        set_vpt_mode(VPT_MODE_NAMES.index(mode_name))
+
+
+def set_grid_interpolation(name: str) -> None:
+    if name not in GRID_INTERPOLATION_TYPE_NAMES:
+        raise RuntimeError(f"Unknown grid interpolation type \"{name}\".")
+    _c("vpt_set_grid_interpolation", GRID_INTERPOLATION_TYPE_NAMES.index(name))
+
+
+def set_seed_offset(offset: int) -> None:
+    _c("vpt_set_seed_offset", int(offset) & 0xFFFFFFFF)
+
+
+def set_max_bounces(max_bounces: int) -> None:
+    _c("vpt_set_max_bounces", int(max_bounces))
+
+
+def set_use_empty_space_skipping(use: bool) -> None:
+    _c("vpt_set_use_empty_space_skipping", 1 if use else 0)
+
+
+# ---- lighting ----
+def set_use_builtin_environment_map(env_map_name: str) -> None:
+    if env_map_name in BUILTIN_ENV_MAP_NAMES:
+        _c("vpt_set_builtin_environment_map", BUILTIN_ENV_MAP_NAMES.index(env_map_name))
+
+
+def set_environment_map_intensity(intensity_factor: float) -> None:
+    S.env_intensity = float(intensity_factor)
+    _c("vpt_set_environment_map_intensity_rgb", farr([intensity_factor] * 3))
+
+
+def set_environment_map_intensity_rgb(intensity_factor: List[float]) -> None:
+    _c("vpt_set_environment_map_intensity_rgb", farr(_vec3(intensity_factor, "setEnvironmentMapIntensityFactorRgb")))
+
+
+def set_sun(direction: List[float], intensity_rgb: List[float]) -> None:
+    _c("vpt_set_sun", farr(_vec3(direction, "setSun")), farr(_vec3(intensity_rgb, "setSun")))
+
+
+def set_sky_color(rgb: List[float]) -> None:
+    _c("vpt_set_sky_color", farr(_vec3(rgb, "setSkyColor")))
+
+
+def load_environment_map_from_tensor(env_map_tensor: torch.Tensor) -> None:
+    """loadEnvironmentMapFromTensor (Module.cpp:898-963): CPU tensor [C, H, W] (C = 3 or 4) of uint8
+    (sRGB), float16 or float32 (linear RGB), equirectangular."""
+    if env_map_tensor.device.type != "cpu":
+        raise RuntimeError("Error in loadEnvironmentMapFromTensor: Expected tensor using CPU memory.")
+    c, h, w = env_map_tensor.shape
+    if c not in (3, 4):
+        raise RuntimeError("Error in loadEnvironmentMapFromTensor: Number of channels must be 3 or 4.")
+    t = env_map_tensor.permute(1, 2, 0).contiguous()
+    if t.dtype == torch.uint8:
+        rgb = t.to(torch.float32) / 255.0
+        linear = 0
+    elif t.dtype in (torch.float16, torch.float32):
+        rgb = t.to(torch.float32)
+        linear = 1
+    else:
+        raise RuntimeError("Error in loadEnvironmentMapFromTensor: Unsupported pixel format.")
+    rgba = torch.ones((h, w, 4), dtype=torch.float32)
+    rgba[..., : min(c, 4)] = rgb[..., : min(c, 4)]
+    rgba = rgba.contiguous()
+    _c("vpt_load_environment_map_rgba", ctypes.c_void_p(rgba.data_ptr()), w, h, linear, 0)
+
+
+def load_environment_map(filename: str) -> None:
+    """Loads an equirectangular environment map stored as .npy (H, W, 3|4) float32 linear RGB.
+    (.exr/.png need OpenEXR/libpng, which this build does not bundle.)"""
+    if not filename.endswith(".npy"):
+        raise RuntimeError(f"Error in loadEnvironmentMapImage: unsupported file format \"{filename}\".")
+    arr = np.load(filename).astype(np.float32)
+    load_environment_map_from_tensor(torch.from_numpy(arr).permute(2, 0, 1).contiguous())
+
+
+# ---- camera (VolumetricPathTracingModuleRenderer.cpp:303-324, Module.cpp:1282-1328) ----
+def get_camera_position() -> List[float]:
+    return list(S.cam_pos)
+
+
+def get_camera_fovy() -> float:
+    return S.fovy
+
+
+def get_camera_view_matrix() -> List[float]:
+    inv = (ctypes.c_float * 16)()
+    vp = (ctypes.c_float * 16)()
+    _c("vpt_get_camera_matrices", inv, vp)
+    if S.view_override is not None:
+        return list(S.view_override)
+    e = np.array(S.cam_pos, np.float64)
+    f = np.array(S.cam_target, np.float64) - e
+    f /= np.linalg.norm(f)
+    s = np.cross(f, np.array(S.cam_up, np.float64))
+    s /= np.linalg.norm(s)
+    u = np.cross(s, f)
+    m = [s[0], u[0], -f[0], 0.0, s[1], u[1], -f[1], 0.0, s[2], u[2], -f[2], 0.0,
+         -s.dot(e), -u.dot(e), f.dot(e), 1.0]
+    return [float(x) for x in m]
+
+
+def set_camera_position(camera_position: List[float]) -> None:
+    S.cam_pos = _vec3(camera_position, "setCameraPosition")
+    S.view_override = None
+    _apply_camera()
+
+
+def set_camera_target(camera_target: List[float]) -> None:
+    S.cam_target = _vec3(camera_target, "setCameraTarget")
+    S.view_override = None
+    _apply_camera()
+
+
+def set_camera_fovy(fovy: float) -> None:
+    """Degrees, like the reference (Module.cpp:1325-1328)."""
+    S.fovy = float(fovy) * math.pi / 180.0
+    _apply_camera()
+
+
+def overwrite_camera_view_matrix(view_matrix_data: List[float]) -> None:
+    if len(view_matrix_data) != 16:
+        raise RuntimeError("Error in overwriteCameraViewMatrix: expected 16 values.")
+    S.view_override = [float(x) for x in view_matrix_data]
+    _apply_camera()
+
+
+def set_view_projection_matrix_as_previous() -> None:
+    """The SVGF history uses the view-projection of the previous render automatically."""
+
+
+# ---- denoising ----
+def set_denoiser(denoiser_name: str) -> None:
+    if denoiser_name not in DENOISER_NAMES:
+        raise RuntimeError(f"Error in setDenoiser: Invalid denoiser name \"{denoiser_name}\".")
+    _c("vpt_set_denoiser", DENOISER_NAMES[denoiser_name])
+
+
+def set_denoiser_property(key: str, value: str) -> None:
+    _c("vpt_set_denoiser_property", key.encode(), str(value).encode())
+
+
+# ---- feature maps ----
+def set_use_feature_maps(feature_map_names: List[str]) -> None:
+    ids = [_FEATURE_BY_NAME[n] for n in feature_map_names if n in _FEATURE_BY_NAME]
+    arr = (ctypes.c_int * max(1, len(ids)))(*ids)
+    _c("vpt_set_use_feature_maps", arr, len(ids))
+
+
+_FEATURE_CHANNELS = {1: 4, 3: 4, 5: 4, 6: 2, 12: 2, 17: 4, FEATURE_TRANSMITTANCE: 1}
+
+
+def get_feature_map(input_tensor: torch.Tensor, feature_map: int) -> torch.Tensor:
+    if feature_map == 0:
+        return _read(input_tensor, input_tensor.size(0), "vpt_read_result")
+    if feature_map not in _FEATURE_CHANNELS:
+        raise RuntimeError(f"Error in getFeatureMap: feature map {feature_map} is not supported.")
+    return _read(input_tensor, _FEATURE_CHANNELS[feature_map], "vpt_get_feature_map", feature_map)
+
+
+def get_feature_map_from_string(input_tensor: torch.Tensor, feature_map: str) -> torch.Tensor:
+    if feature_map not in _FEATURE_BY_NAME:
+        raise RuntimeError(f"Error in getFeatureMapFromString: unknown feature map \"{feature_map}\".")
+    return get_feature_map(input_tensor, _FEATURE_BY_NAME[feature_map])
+
+
+# ---- rendering (Module.cpp:286-317) ----
+def _validate(input_tensor: torch.Tensor):
+    if input_tensor.dim() != 3:
+        raise RuntimeError("Error in renderFrame: inputTensor.sizes().size() != 3.")
+    if input_tensor.size(0) not in (3, 4):
+        raise RuntimeError("Error in renderFrame: The number of image channels is not equal to 3 or 4.")
+    if input_tensor.dtype != torch.float32:
+        raise RuntimeError("Error in renderFrame: The only data type currently supported is 32-bit float.")
+    if input_tensor.device.type not in ("cpu", "cuda"):
+        raise RuntimeError("Unsupported PyTorch device type.")
+
+
+def _stream_of(t: torch.Tensor):
+    if t.is_cuda:
+        return ctypes.c_void_p(torch.cuda.current_stream(t.device).cuda_stream)
+    return ctypes.c_void_p(0)
+
+
+def _read(input_tensor: torch.Tensor, channels: int, fn: str, feature: Optional[int] = None) -> torch.Tensor:
+    h, w = input_tensor.size(1), input_tensor.size(2)
+    out = torch.empty((channels, h, w), dtype=torch.float32, device=input_tensor.device)
+    on_dev = 1 if out.is_cuda else 0
+    ptr = ctypes.c_void_p(out.data_ptr())
+    if feature is None:
+        _c(fn, ptr, channels, on_dev, _stream_of(input_tensor))
+    else:
+        _c(fn, feature, ptr, channels, on_dev, _stream_of(input_tensor))
+    return out
+
+
+def render_frame(input_tensor: torch.Tensor, frame_count: int) -> torch.Tensor:
+    """Renders `frame_count` 1-spp frames into the running mean and returns it as [C, H, W]."""
+    _validate(input_tensor)
+    c, h, w = input_tensor.shape
+    _c("vpt_set_resolution", int(w), int(h))
+    _c("vpt_render_frames", int(frame_count), _stream_of(input_tensor))
+    return _read(input_tensor, c, "vpt_read_result")
+
+
+def get_stats() -> dict:
+    st = _lib.VptStats()
+    _c("vpt_get_stats", ctypes.byref(st))
+    return {"paths": st.paths, "density_lookups": st.density_lookups, "frames": st.frames,
+            "error_flags": st.error_flags}
+
+
+def reset_stats() -> None:
+    _c("vpt_reset_stats")
+
+
+def context_handle() -> int:
+    """Raw VptContext* of the module's renderer (for C-ABI level tooling)."""
+    return _ctx()

@@ -1,0 +1,226 @@
+/*
+ * vpt_b200.h - C ABI of the B200-native volumetric path-tracing core.
+ *
+ * Plain C, plain pointers and sizes.  No CUDA or torch types appear in the signatures: a CUDA
+ * stream is passed as `void*` (a cudaStream_t, or NULL for the legacy default stream).  Every entry
+ * point returns a VptStatus; no C++ exception crosses this boundary.  A context is not
+ * thread-safe: use one context per host thread.
+ *
+ * Each declaration names the reference interface it replaces (paths inside chrismile/CloudRendering).
+ * The reference reaches its tracer through the pybind11/TORCH_LIBRARY module `vpt`
+ * (src/PyTorch/Module.cpp:85-182, 186+) and, below it, the VolumetricPathTracingPass setters
+ * (src/PathTracer/VolumetricPathTracingPass.hpp:137-212).
+ */
+#ifndef VPT_B200_H
+#define VPT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VPT_B200_ABI_VERSION 1
+
+typedef struct VptContext VptContext;
+
+typedef enum VptStatus {
+    VPT_OK = 0,
+    VPT_ERR_ARG = 1,          /* bad argument (shape, range, null pointer, unknown name) */
+    VPT_ERR_CUDA = 2,         /* a CUDA runtime call failed */
+    VPT_ERR_OOM = 3,          /* device allocation failed */
+    VPT_ERR_ITER_LIMIT = 4,   /* a device loop hit its iteration guard (result is incomplete) */
+    VPT_ERR_STATE = 5,        /* call not valid in the current state (e.g. no volume loaded) */
+    VPT_ERR_UNSUPPORTED = 6   /* combination of settings not supported */
+} VptStatus;
+
+/* VptMode, same numbering as the reference enum (src/PathTracer/RenderSettings.hpp:32-36). */
+enum {
+    VPT_MODE_DELTA_TRACKING = 0,
+    VPT_MODE_SPECTRAL_DELTA_TRACKING = 1,
+    VPT_MODE_RATIO_TRACKING = 2,
+    VPT_MODE_DECOMPOSITION_TRACKING = 3,
+    VPT_MODE_RESIDUAL_RATIO_TRACKING = 4,
+    VPT_MODE_NEXT_EVENT_TRACKING = 5,
+    VPT_MODE_NEXT_EVENT_TRACKING_SPECTRAL = 6,
+    VPT_MODE_ISOSURFACE_RENDERING = 7,
+    VPT_MODE_RAY_MARCHING_EMISSION_ABSORPTION = 8
+};
+
+/* GridInterpolationType (RenderSettings.hpp:51-55). */
+enum { VPT_INTERP_NEAREST = 0, VPT_INTERP_STOCHASTIC = 1, VPT_INTERP_TRILINEAR = 2 };
+
+/* BuiltinEnvMap (RenderSettings.hpp:120-122) plus one addition: a constant sky with the
+ * reference's Phong sun lobe, so that every tracker sees the sun (value 3). */
+enum {
+    VPT_ENV_DEFAULT = 0,
+    VPT_ENV_BLACK = 1,
+    VPT_ENV_SINGLE_COLOR = 2,
+    VPT_ENV_CONSTANT_SUN = 3,
+    VPT_ENV_IMAGE = 4          /* set by vpt_load_environment_map_rgba */
+};
+
+/* Feature maps (FeatureMapTypeVpt, VolumetricPathTracingPass.hpp:67-73) that this core writes. */
+enum {
+    VPT_FEATURE_RESULT = 0,
+    VPT_FEATURE_FIRST_X = 1,
+    VPT_FEATURE_NORMAL = 3,
+    VPT_FEATURE_CLOUD_ONLY = 5,
+    VPT_FEATURE_DEPTH = 6,
+    VPT_FEATURE_DENSITY = 12,
+    VPT_FEATURE_BACKGROUND = 13,
+    VPT_FEATURE_ALBEDO = 17,
+    VPT_FEATURE_TRANSMITTANCE = 32 /* new: primary-ray transmittance (no reference counterpart) */
+};
+
+/* Denoiser types (DenoiserType, src/Denoiser/Denoiser.hpp:63-79; only these are built here). */
+enum { VPT_DENOISER_NONE = 0, VPT_DENOISER_EAW = 1, VPT_DENOISER_SVGF = 2 };
+
+typedef struct VptStats {
+    uint64_t paths;            /* camera paths traced since the last reset of the counters */
+    uint64_t density_lookups;  /* sampleCloud calls (trilinear = 1 call = 8 texels) */
+    uint64_t frames;           /* frames accumulated in the film since the last reset */
+    int32_t error_flags;       /* sticky device error bits (1 = iteration guard) */
+    int32_t reserved;
+} VptStats;
+
+/* ---- life cycle: replaces vpt.initialize()/cleanup() (Module.cpp:732-813) ---- */
+const char* vpt_status_string(int status);
+int         vpt_abi_version(void);
+/* Number of CUDA kernels this library has launched in this process (all contexts). */
+uint64_t    vpt_kernel_launch_count(void);
+VptStatus   vpt_create(VptContext** out_ctx, int cuda_device);
+void        vpt_destroy(VptContext* ctx);
+const char* vpt_last_error(const VptContext* ctx);
+
+/* ---- volume data ----
+ * Dense grid in x-fastest order (CloudData::setDensityField, src/CloudData.cpp:147-167; note the
+ * reference sizes the buffer as X*Z*Z there, this core uses X*Y*Z).  The world box follows
+ * CloudData::computeGridBounds (CloudData.cpp:63-78): largest side spans [-maxGridExtent, maxGridExtent].
+ * Values are normalised on the device by (v - min)/(max - min) (DensityField::getDataFloatAtNorm,
+ * src/DensityField.cpp:262-267; min := 0 when min == max, DensityField.cpp:146-150). */
+VptStatus vpt_set_dense_grid(VptContext* ctx, const float* data, int nx, int ny, int nz, int data_on_device);
+/* Synthetic scene on the device: seeded fBm of improved Perlin noise, remapped to [0, 1], values
+ * below `threshold` set to 0.  No reference counterpart (the reference loads files). */
+VptStatus vpt_generate_fbm_grid(VptContext* ctx, int nx, int ny, int nz, uint32_t seed, int octaves,
+                                float lacunarity, float gain, float base_frequency, float threshold);
+/* Copies the device grid (raw, un-normalised values) to `out` (x-fastest, nx*ny*nz floats). */
+VptStatus vpt_get_dense_grid(VptContext* ctx, float* out, int out_on_device);
+/* Voxel spacing of the next grid set by vpt_set_dense_grid (CloudData voxelSizeX/Y/Z, read from
+ * .xyz headers in CloudData::loadFromXyzFile, CloudData.cpp:248-258); reset to 1 after that call. */
+VptStatus vpt_set_voxel_size(VptContext* ctx, double sx, double sy, double sz);
+/* vpt.set_max_grid_extent (Module.cpp setMaxGridExtent); applies to the next grid that is set. */
+VptStatus vpt_set_max_grid_extent(VptContext* ctx, float max_grid_extent);
+/* Returns boxMin (3 floats) then boxMax (3 floats) in world space (vpt.get_render_bounding_box). */
+VptStatus vpt_get_render_bounding_box(VptContext* ctx, float out_min_max[6]);
+
+/* ---- settings (VolumetricPathTracingPass setters, .hpp:137-212) ---- */
+VptStatus vpt_set_vpt_mode(VptContext* ctx, int mode);                     /* setVptMode */
+VptStatus vpt_set_grid_interpolation(VptContext* ctx, int interpolation);  /* setSparseGridInterpolationType */
+VptStatus vpt_set_extinction_scale(VptContext* ctx, float scale);          /* setExtinctionScale */
+VptStatus vpt_set_extinction_base(VptContext* ctx, const float rgb[3]);    /* setExtinctionBase */
+VptStatus vpt_set_scattering_albedo(VptContext* ctx, const float rgb[3]);  /* setScatteringAlbedo */
+VptStatus vpt_set_phase_g(VptContext* ctx, float g);                       /* setPhaseG */
+VptStatus vpt_set_seed_offset(VptContext* ctx, uint32_t offset);           /* setCustomSeedOffset */
+VptStatus vpt_set_use_linear_rgb(VptContext* ctx, int use_linear_rgb);     /* setUseLinearRGB */
+/* Scatter events after which a path counts as absorbed; 0 = unlimited (the reference has no cap). */
+VptStatus vpt_set_max_bounces(VptContext* ctx, int max_bounces);
+/* setUseBuiltinEnvironmentMap (VolumetricPathTracingPass.cpp:1194-1202) by enum value. */
+VptStatus vpt_set_builtin_environment_map(VptContext* ctx, int env_kind);
+VptStatus vpt_set_environment_map_intensity_rgb(VptContext* ctx, const float rgb[3]);
+/* Sun direction (normalised here) and sun intensity (rgb, = sunlightIntensity * sunlightColor in
+ * VolumetricPathTracingPass.cpp:2063-2064).  For VPT_ENV_SINGLE_COLOR the sky is `intensity`. */
+VptStatus vpt_set_sun(VptContext* ctx, const float direction[3], const float intensity_rgb[3]);
+/* Sky radiance of VPT_ENV_CONSTANT_SUN. */
+VptStatus vpt_set_sky_color(VptContext* ctx, const float rgb[3]);
+/* loadEnvironmentMapImageFromLinearBuffer (VolumetricPathTracingPass.cpp:1489-1556) for fp32 RGBA,
+ * equirectangular, row-major; builds the 4096^2 octahedral importance pyramid on the device. */
+VptStatus vpt_load_environment_map_rgba(VptContext* ctx, const float* rgba, int width, int height,
+                                        int is_linear_rgb, int data_on_device);
+
+/* ---- camera (VolumetricPathTracingModuleRenderer.cpp:124-131, 303-324) ----
+ * Right-handed look-at view, perspective projection with depth in [0, 1] and y flipped so that
+ * image row 0 is the top of the picture.  fovy in radians. */
+VptStatus vpt_set_camera(VptContext* ctx, const float position[3], const float target[3],
+                         const float up[3], float fovy_radians, float near_dist, float far_dist);
+/* Overwrites the view matrix (16 floats, column-major) (overwrite_camera_view_matrix). */
+VptStatus vpt_set_view_matrix(VptContext* ctx, const float view[16]);
+/* 16 floats each, column-major: inverse(proj * view) for the current resolution, and proj * view. */
+VptStatus vpt_get_camera_matrices(VptContext* ctx, float inv_view_proj[16], float view_proj[16]);
+
+/* ---- rendering: replaces vpt.render_frame (Module.cpp:286-317, 589-693) ---- */
+VptStatus vpt_set_resolution(VptContext* ctx, int width, int height);
+/* Clears the film: next frame index is 0 (onHasMoved, VolumetricPathTracingPass.cpp:1150-1162). */
+VptStatus vpt_reset_accumulation(VptContext* ctx);
+/* Traces `frames` 1-spp frames into the FP64 film on `stream` (enqueued, not synchronised). */
+VptStatus vpt_render_frames(VptContext* ctx, int frames, void* stream);
+/* Writes the accumulated mean (denoised when a denoiser is set) as channels x H x W fp32
+ * (channels 3 or 4; alpha = 1).  `out` is a device pointer when out_on_device, else host
+ * memory (the copy is synchronous then). */
+VptStatus vpt_read_result(VptContext* ctx, float* out, int channels, int out_on_device, void* stream);
+/* render_frames + read_result in one call: the reference render_frame. */
+VptStatus vpt_render_frame(VptContext* ctx, int frames, float* out, int channels, int out_on_device,
+                           void* stream);
+/* Per-pixel sample variance of the mean (channels x H x W) when statistics are enabled. */
+VptStatus vpt_set_collect_statistics(VptContext* ctx, int enabled);
+VptStatus vpt_read_statistics(VptContext* ctx, double* out_sum, double* out_sum_sq, int out_on_device,
+                              void* stream);
+/* vpt.set_use_feature_maps / get_feature_map (Module.cpp setUseFeatureMaps, getFeatureMap). */
+VptStatus vpt_set_use_feature_maps(VptContext* ctx, const int* features, int count);
+VptStatus vpt_get_feature_map(VptContext* ctx, int feature, float* out, int channels, int out_on_device,
+                              void* stream);
+VptStatus vpt_get_stats(VptContext* ctx, VptStats* stats);
+VptStatus vpt_reset_stats(VptContext* ctx);
+/* Waits for the context's work on `stream`, then reports sticky device errors. */
+VptStatus vpt_synchronize(VptContext* ctx, void* stream);
+
+/* vpt.set_use_empty_space_skipping (VolumetricPathTracingPass::setUseEmptySpaceSkipping): NEE shadow
+ * rays skip empty 8^3 blocks of the occupancy grid. */
+VptStatus vpt_set_use_empty_space_skipping(VptContext* ctx, int enabled);
+/* Tuning knobs without a reference counterpart: "schedule" (0 = tiles, 1 = persistent),
+ * "persistent_blocks_per_sm", "max_steps_per_path" (guard on tentative collisions of one path,
+ * default 2^24; a path that reaches it stops and vpt_synchronize reports VPT_ERR_ITER_LIMIT),
+ * "ess_ref_compat" (1 = empty-space skipping exactly as the reference runs it: every block marked
+ * occupied, ComputeOccupancyGrid.glsl:108-109, and shadow samples stepped from the moving point,
+ * NeeTransmittance.glsl:173-228). */
+VptStatus vpt_set_option(VptContext* ctx, const char* key, double value);
+
+/* ---- denoisers (VolumetricPathTracingPass.cpp:2287-2311) ---- */
+VptStatus vpt_set_denoiser(VptContext* ctx, int denoiser_type);
+/* EAW keys: "iterations", "phi_color", "phi_position", "phi_normal", "ref_compute_quirk";
+ * SVGF keys: "z_threshold", "normal_threshold" (set_denoiser_property). */
+VptStatus vpt_set_denoiser_property(VptContext* ctx, const char* key, const char* value);
+
+/* ---- stateless kernels on caller-owned device buffers (all pointers are device pointers) ---- */
+/* Supervoxel min / max / mean of a normalised x-fastest grid with optional one-voxel halo and the
+ * occupancy byte (max >= 1e-5) (SuperVoxelGridResidualRatioTracking::computeSuperVoxels and
+ * SuperVoxelGridDecompositionTracking, src/PathTracer/SuperVoxelGrid.cpp:101-211, 316-396).
+ * Outputs hold ceil(nx/sv)*ceil(ny/sv)*ceil(nz/sv) entries; avg/occ may be NULL. */
+VptStatus vpt_build_supervoxel_grid(const float* density, int nx, int ny, int nz, int sv, int halo,
+                                    float* out_min, float* out_max, float* out_avg, uint8_t* out_occupancy,
+                                    void* stream);
+/* Residual ratio tracking (mu_c, mu_r_bar) pairs from supervoxel min/max/mean and the extinction
+ * (SuperVoxelGridResidualRatioTracking::recomputeSuperVoxels, SuperVoxelGrid.cpp:218-256). */
+VptStatus vpt_build_rrt_params(const float* sv_min, const float* sv_max, const float* sv_avg, int count,
+                               float extinction, int sv, float* out_pairs, void* stream);
+/* Occupancy of block^3 blocks: 1 if any voxel (plus `halo` voxels around) exceeds `threshold`
+ * (intent of OccupancyGridPass / ComputeOccupancyGrid.glsl:91-143, whose loop never runs). */
+VptStatus vpt_build_occupancy_grid(const float* density, int nx, int ny, int nz, int block, int halo,
+                                   float threshold, uint8_t* out, void* stream);
+/* Octahedral max-luminance importance pyramid (2^levels square at level 0, levels concatenated)
+ * of an equirectangular RGBA image (OctahedralMapper.glsl:65-85 + mip reduction). */
+VptStatus vpt_build_environment_pyramid(const float* rgba, int width, int height, int levels, float* out_pyramid,
+                                        void* stream);
+/* EAW a-trous chain (EAWBlitPass::_renderCompute, src/Denoiser/EAWDenoiser.cpp:345-391; weights of
+ * EAWDenoise.glsl) on RGBA images; position/normal may be NULL.  Allocates its ping-pong images
+ * on `stream` with the stream-ordered allocator and frees them before returning. */
+VptStatus vpt_eaw_denoise_rgba(const float* color, const float* position, const float* normal, int width,
+                               int height, int iterations, float phi_color, float phi_position, float phi_normal,
+                               int ref_compute_quirk, float* out, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VPT_B200_H */

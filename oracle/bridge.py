@@ -1,0 +1,190 @@
+"""ctypes bridge to the CPU oracle (TEST INFRASTRUCTURE ONLY).
+
+Used by tests/, bench.py's cpu_baseline leg and __graft_entry__.smoke() as the checker.  The product
+package never imports this module.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from ctypes import POINTER, c_float, c_int, c_uint8, c_uint32, c_uint64, c_void_p
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle_vpt.so")
+
+
+class OracleScene(ctypes.Structure):
+    _fields_ = [
+        ("inv_view_proj", c_float * 16),
+        ("width", c_int), ("height", c_int),
+        ("frame_count", c_uint32), ("num_frames", c_uint32), ("seed_offset", c_uint32),
+        ("mode", c_int), ("interp", c_int), ("max_bounces", c_int), ("use_ess", c_int), ("ess_ref_compat", c_int),
+        ("box_min", c_float * 3), ("box_max", c_float * 3),
+        ("nx", c_int), ("ny", c_int), ("nz", c_int),
+        ("vox_per_unit", c_float * 3),
+        ("border_density", c_float),
+        ("extinction", c_float), ("albedo", c_float), ("g", c_float),
+        ("sv_size", c_int), ("svx", c_int), ("svy", c_int), ("svz", c_int),
+        ("sv_world", c_float * 3),
+        ("env_kind", c_int), ("use_linear_rgb", c_int), ("env_image_linear", c_int),
+        ("sun_dir", c_float * 3), ("sun_intensity", c_float * 3), ("sky_color", c_float * 3),
+        ("env_intensity", c_float * 3),
+        ("env_w", c_int), ("env_h", c_int), ("env_levels", c_int),
+        ("density", c_void_p), ("sv_data", c_void_p), ("occupancy", c_void_p),
+        ("env_rgba", c_void_p), ("env_pyramid", c_void_p),
+    ]
+
+
+_lib = None
+
+
+def load():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            from . import build_oracle
+            build_oracle.build()
+        lib = ctypes.CDLL(LIB_PATH)
+        P = POINTER
+        lib.oracle_render.argtypes = [P(OracleScene), c_void_p, c_void_p, P(c_uint64), c_int]
+        lib.oracle_render_rows.argtypes = [P(OracleScene), c_int, c_int, c_void_p, P(c_uint64), c_int]
+        lib.oracle_trace_paths.argtypes = [P(OracleScene), c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_int]
+        lib.oracle_fbm.argtypes = [c_void_p, c_int, c_int, c_int, c_uint32, c_int, c_float, c_float, c_float,
+                                   c_float, c_float]
+        lib.oracle_minmax.argtypes = [c_void_p, c_uint64, P(c_float), P(c_float)]
+        lib.oracle_normalize.argtypes = [c_void_p, c_void_p, c_uint64, c_float, c_float]
+        lib.oracle_grid_bounds.argtypes = [c_int, c_int, c_int, c_float, P(c_float), P(c_float)]
+        lib.oracle_supervoxel_stats.argtypes = [c_void_p, c_int, c_int, c_int, c_int, c_int, c_void_p, c_void_p,
+                                                c_void_p, c_void_p]
+        lib.oracle_rrt_params.argtypes = [c_void_p, c_void_p, c_void_p, c_int, c_float, c_int, c_void_p]
+        lib.oracle_occupancy.argtypes = [c_void_p, c_int, c_int, c_int, c_int, c_int, c_float, c_void_p]
+        lib.oracle_env_pyramid.argtypes = [c_void_p, c_int, c_int, c_int, c_void_p]
+        lib.oracle_eaw.argtypes = [c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_float, c_float, c_float,
+                                   c_int, c_void_p]
+        lib.oracle_rng_stream.argtypes = [c_uint32, c_int, c_void_p, c_void_p]
+        _lib = lib
+    return _lib
+
+
+def _p(a: np.ndarray | None):
+    return None if a is None else a.ctypes.data_as(c_void_p)
+
+
+def fbm(n, seed, octaves=6, lacunarity=2.0, gain=0.5, base_frequency=4.0, threshold=0.3, contrast=2.0):
+    nx, ny, nz = (n, n, n) if isinstance(n, int) else n
+    out = np.empty((nz, ny, nx), np.float32)
+    load().oracle_fbm(_p(out), nx, ny, nz, seed, octaves, lacunarity, gain, base_frequency, threshold, contrast)
+    return out
+
+
+def minmax(v: np.ndarray):
+    lo, hi = c_float(), c_float()
+    load().oracle_minmax(_p(np.ascontiguousarray(v, np.float32)), v.size, ctypes.byref(lo), ctypes.byref(hi))
+    return lo.value, hi.value
+
+
+def normalize(v: np.ndarray, vmin: float, vmax: float) -> np.ndarray:
+    v = np.ascontiguousarray(v, np.float32)
+    out = np.empty_like(v)
+    load().oracle_normalize(_p(v), _p(out), v.size, vmin, vmax)
+    return out
+
+
+def grid_bounds(nx, ny, nz, extent):
+    bmin, bmax = (c_float * 3)(), (c_float * 3)()
+    load().oracle_grid_bounds(nx, ny, nz, extent, bmin, bmax)
+    return list(bmin), list(bmax)
+
+
+def supervoxel_stats(dens: np.ndarray, sv: int, halo: int):
+    nz, ny, nx = dens.shape
+    gx, gy, gz = -(-nx // sv), -(-ny // sv), -(-nz // sv)
+    mn = np.empty(gx * gy * gz, np.float32)
+    mx = np.empty_like(mn)
+    avg = np.empty_like(mn)
+    occ = np.empty(gx * gy * gz, np.uint8)
+    load().oracle_supervoxel_stats(_p(np.ascontiguousarray(dens, np.float32)), nx, ny, nz, sv, halo, _p(mn),
+                                   _p(mx), _p(avg), _p(occ))
+    return mn, mx, avg, occ
+
+
+def rrt_params(mn, mx, avg, extinction, sv):
+    out = np.empty(mn.size * 2, np.float32)
+    load().oracle_rrt_params(_p(mn), _p(mx), _p(avg), mn.size, extinction, sv, _p(out))
+    return out
+
+
+def occupancy(dens, bs=8, halo=0, threshold=0.0):
+    nz, ny, nx = dens.shape
+    gx, gy, gz = -(-nx // bs), -(-ny // bs), -(-nz // bs)
+    out = np.empty(gx * gy * gz, np.uint8)
+    load().oracle_occupancy(_p(np.ascontiguousarray(dens, np.float32)), nx, ny, nz, bs, halo, threshold, _p(out))
+    return out
+
+
+def env_pyramid(rgba: np.ndarray, levels: int = 12) -> np.ndarray:
+    h, w, _ = rgba.shape
+    total = sum((1 << (levels - l)) ** 2 for l in range(levels))
+    out = np.empty(total, np.float32)
+    load().oracle_env_pyramid(_p(np.ascontiguousarray(rgba, np.float32)), w, h, levels, _p(out))
+    return out
+
+
+def eaw(color, pos, nrm, iterations, phi_c=5.0, phi_p=0.1, phi_n=0.1, quirk=0):
+    h, w, _ = color.shape
+    out = np.empty_like(color)
+    load().oracle_eaw(_p(color), _p(pos), _p(nrm), w, h, iterations, phi_c, phi_p, phi_n, quirk, _p(out))
+    return out
+
+
+def rng_stream(seed: int, n: int):
+    out = np.empty(n, np.float32)
+    st = np.empty(4, np.uint32)
+    load().oracle_rng_stream(seed, n, _p(out), _p(st))
+    return out, st
+
+
+class Scene:
+    """Holds an OracleScene plus the numpy buffers it points to."""
+
+    def __init__(self, **kw):
+        self.s = OracleScene()
+        self._keep = {}
+        for k, v in kw.items():
+            self.set(k, v)
+
+    def set(self, k, v):
+        if k in ("density", "sv_data", "occupancy", "env_rgba", "env_pyramid"):
+            arr = None if v is None else np.ascontiguousarray(v)
+            self._keep[k] = arr
+            setattr(self.s, k, None if arr is None else arr.ctypes.data_as(c_void_p).value)
+        elif isinstance(v, (list, tuple, np.ndarray)):
+            arr = getattr(self.s, k)
+            for i, x in enumerate(v):
+                arr[i] = float(x)
+        else:
+            setattr(self.s, k, v)
+
+    def render(self, threads=0, with_sq=False):
+        n = self.s.width * self.s.height * 3
+        film = np.zeros(n, np.float64)
+        sq = np.zeros(n, np.float64) if with_sq else None
+        lk = c_uint64(0)
+        load().oracle_render(ctypes.byref(self.s), _p(film), _p(sq), ctypes.byref(lk), threads)
+        return film, sq, lk.value
+
+    def render_rows(self, row0, row1, threads=0):
+        film = np.zeros(self.s.width * self.s.height * 3, np.float64)
+        lk = c_uint64(0)
+        load().oracle_render_rows(ctypes.byref(self.s), row0, row1, _p(film), ctypes.byref(lk), threads)
+        return film, lk.value
+
+    def trace_paths(self, xs, ys, frames, threads=0):
+        xs = np.ascontiguousarray(xs, np.int32)
+        ys = np.ascontiguousarray(ys, np.int32)
+        fr = np.ascontiguousarray(frames, np.uint32)
+        out = np.empty((xs.size, 3), np.float32)
+        load().oracle_trace_paths(ctypes.byref(self.s), _p(xs), _p(ys), _p(fr), xs.size, _p(out), threads)
+        return out

@@ -1,0 +1,1046 @@
+// vpt_oracle.cpp - CPU oracle (TEST INFRASTRUCTURE ONLY): a restatement of the reference's
+// volumetric path-tracing shaders for checking the CUDA core and for the timed CPU baseline.
+// Each function cites the reference file:line it follows (paths inside chrismile/CloudRendering).
+// Build: oracle/build_oracle.py (g++ -O3 -fopenmp -ffp-contract=off).
+#include "vpt_oracle.h"
+
+#include <math.h>
+#include <string.h>
+#include <algorithm>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+const float PI = 3.14159265359f;  // VptUtils.glsl:27
+const float TWO_PI = 2.0f * 3.14159265359f;
+
+struct V3 {
+    float x, y, z;
+};
+inline V3 v3(float x, float y, float z) { return V3{x, y, z}; }
+inline V3 add(V3 a, V3 b) { return v3(a.x + b.x, a.y + b.y, a.z + b.z); }
+inline V3 sub(V3 a, V3 b) { return v3(a.x - b.x, a.y - b.y, a.z - b.z); }
+inline V3 mul(V3 a, float s) { return v3(a.x * s, a.y * s, a.z * s); }
+inline V3 mulv(V3 a, V3 b) { return v3(a.x * b.x, a.y * b.y, a.z * b.z); }
+inline V3 divv(V3 a, V3 b) { return v3(a.x / b.x, a.y / b.y, a.z / b.z); }
+inline V3 neg(V3 a) { return v3(-a.x, -a.y, -a.z); }
+inline float dot(V3 a, V3 b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
+inline V3 cross(V3 a, V3 b) { return v3(a.y * b.z - b.y * a.z, a.z * b.x - b.z * a.x, a.x * b.y - b.x * a.y); }
+inline float length(V3 a) { return sqrtf(dot(a, a)); }
+inline V3 normalize(V3 a) {
+    float l = length(a);
+    return v3(a.x / l, a.y / l, a.z / l);
+}
+inline float mixf(float a, float b, float t) { return a * (1.0f - t) + b * t; }
+inline float clampf(float v, float lo, float hi) { return std::min(std::max(v, lo), hi); }
+inline float smoothstepf(float e0, float e1, float x) {
+    float t = clampf((x - e0) / (e1 - e0), 0.0f, 1.0f);
+    return t * t * (3.0f - 2.0f * t);
+}
+inline float signf(float v) { return v > 0.0f ? 1.0f : (v < 0.0f ? -1.0f : 0.0f); }
+
+// ---- RNG (VptUtils.glsl:48-65) ----
+struct Rng {
+    uint32_t x, y, z, w;
+};
+inline uint32_t taus(uint32_t z, int s1, int s2, int s3, uint32_t m) {
+    uint32_t b = ((z << s1) ^ z) >> s2;
+    return ((z & m) << s3) ^ b;
+}
+inline float rnd(Rng& r) {
+    r.x = taus(r.x, 13, 19, 12, 4294967294u);
+    r.y = taus(r.y, 2, 25, 4, 4294967288u);
+    r.z = taus(r.z, 3, 11, 17, 4294967280u);
+    r.w = 1664525u * r.w + 1013904223u;
+    return 2.3283064365387e-10f * (float)(r.x ^ r.y ^ r.z ^ r.w);
+}
+inline Rng rng_init(uint32_t seed) {
+    Rng r{seed, seed, seed, seed};
+    for (uint32_t i = 0; i < seed % 7u + 2u; i++) rnd(r);
+    return r;
+}
+
+// ---- camera ray (VptUtils.glsl:750-761) ----
+void mat_point(const float* m, float x, float y, float z, float w, float o[4]) {
+    for (int r = 0; r < 4; r++) o[r] = ((m[r] * x + m[4 + r] * y) + m[8 + r] * z) + m[12 + r] * w;
+}
+void camera_ray(const OracleScene& S, float sx, float sy, V3& x, V3& w) {
+    float p[4], t[4];
+    mat_point(S.inv_view_proj, sx, sy, 0.0f, 1.0f, p);
+    mat_point(S.inv_view_proj, sx, sy, 1.0f, 1.0f, t);
+    V3 vp = v3(p[0] / p[3], p[1] / p[3], p[2] / p[3]);
+    V3 vt = v3(t[0] / t[3], t[1] / t[3], t[2] / t[3]);
+    x = vp;
+    w = normalize(sub(vt, vp));
+}
+
+// ---- rayBoxIntersect (VptUtils.glsl:763-801) ----
+bool ray_box(V3 bmin, V3 bmax, V3 p, V3 d, float& tmin, float& tmax) {
+    d.x = fabsf(d.x) <= 0.000001f ? 0.000001f : d.x;
+    d.y = fabsf(d.y) <= 0.000001f ? 0.000001f : d.y;
+    d.z = fabsf(d.z) <= 0.000001f ? 0.000001f : d.z;
+    V3 cmin = divv(sub(bmin, p), d), cmax = divv(sub(bmax, p), d);
+    tmin = std::max(std::max(std::min(cmin.x, cmax.x), std::min(cmin.y, cmax.y)), std::min(cmin.z, cmax.z));
+    tmin = std::max(0.0f, tmin);
+    tmax = std::min(std::min(std::max(cmin.x, cmax.x), std::max(cmin.y, cmax.y)), std::max(cmin.z, cmax.z));
+    return !(tmax <= tmin || tmax <= 0.0f);
+}
+
+// ---- directions (VptUtils.glsl:67-123) ----
+void basis(V3 d, V3& b, V3& t) {
+    V3 other = fabsf(d.z) >= 0.9999f ? v3(1, 0, 0) : v3(0, 0, 1);
+    b = normalize(cross(other, d));
+    t = normalize(cross(d, b));
+}
+V3 random_direction(Rng& r, V3 d) {
+    float r1 = rnd(r);
+    float r2 = rnd(r) * 2.0f - 1.0f;
+    float s = sqrtf(1.0f - r2 * r2);
+    float a = TWO_PI * r1;
+    float x = cosf(a) * s, y = sinf(a) * s;
+    V3 t0, t1;
+    basis(d, t0, t1);
+    return add(add(mul(t0, x), mul(t1, y)), mul(d, r2));
+}
+V3 sample_phase(Rng& r, float g, V3 d) {
+    if (fabsf(g) < 0.001f) return random_direction(r, neg(d));
+    float phi = rnd(r) * 2.0f * PI;
+    float xi = rnd(r);
+    float t = (1.0f - g * g) / (1.0f - g + 2.0f * g * xi);
+    float cos_t = (0.5f / g) * ((1.0f + g * g) - t * t);
+    float sin_t = sqrtf(std::max(0.0f, 1.0f - cos_t * cos_t));
+    V3 t0, t1;
+    basis(d, t0, t1);
+    return add(add(mul(t0, sin_t * sinf(phi)), mul(t1, sin_t * cosf(phi))), mul(d, cos_t));
+}
+float eval_phase(float g, V3 a, V3 b) {
+    float c = dot(normalize(a), normalize(b));
+    return ((0.25f / PI) * (1.0f - g * g)) / powf((1.0f + g * g) - 2.0f * g * c, 1.5f);
+}
+
+// ---- sky and sun (VptUtils.glsl:288-389, 125-267) ----
+float srgb_to_lin(float c) { return c <= 0.04045f ? c / 12.92f : powf((c + 0.055f) / 1.055f, 2.4f); }
+float lin_to_srgb(float c) { return c <= 0.0031308f ? c * 12.92f : 1.055f * powf(c, 1.0f / 2.4f) - 0.055f; }
+
+V3 sky_default(V3 dir, int lin) {
+    const float cr[5] = {0.1f, 0.01f, 0.8f, 0.1f, 0.01f};
+    const float cg[5] = {0.05f, 0.05f, 0.9f, 0.3f, 0.1f};
+    const float cb[5] = {0.01f, 0.2f, 1.0f, 1.0f, 0.7f};
+    const float ds[5] = {-1.0f, -0.1f, 0.0f, 0.4f, 1.0f};
+    float r = cr[0], g = cg[0], b = cb[0];
+    for (int i = 1; i < 5; i++) {
+        float s = smoothstepf(ds[i - 1], ds[i], dir.y);
+        r = mixf(r, cr[i], s);
+        g = mixf(g, cg[i], s);
+        b = mixf(b, cb[i], s);
+    }
+    if (lin) return v3(srgb_to_lin(r), srgb_to_lin(g), srgb_to_lin(b));
+    return v3(r, g, b);
+}
+V3 sun_lobe(const OracleScene& S, V3 dir) {
+    const float norm = 11.0f / (2.0f * 3.14159f);
+    float p = powf(std::max(0.0f, dot(dir, v3(S.sun_dir[0], S.sun_dir[1], S.sun_dir[2]))), 10.0f);
+    return v3((S.sun_intensity[0] * p) * norm, (S.sun_intensity[1] * p) * norm, (S.sun_intensity[2] * p) * norm);
+}
+V3 env_fetch(const OracleScene& S, float u, float v) {
+    float fx = u * (float)S.env_w - 0.5f, fy = v * (float)S.env_h - 0.5f;
+    float x0f = floorf(fx), y0f = floorf(fy);
+    float ax = fx - x0f, ay = fy - y0f;
+    int x0 = (int)x0f, y0 = (int)y0f, w = S.env_w, h = S.env_h;
+    int xa = ((x0 % w) + w) % w, xb = (((x0 + 1) % w) + w) % w;
+    int ya = ((y0 % h) + h) % h, yb = (((y0 + 1) % h) + h) % h;
+    const float* c00 = S.env_rgba + ((size_t)ya * w + xa) * 4;
+    const float* c10 = S.env_rgba + ((size_t)ya * w + xb) * 4;
+    const float* c01 = S.env_rgba + ((size_t)yb * w + xa) * 4;
+    const float* c11 = S.env_rgba + ((size_t)yb * w + xb) * 4;
+    float o[3];
+    for (int c = 0; c < 3; c++) o[c] = mixf(mixf(c00[c], c10[c], ax), mixf(c01[c], c11[c], ax), ay);
+    return v3(o[0], o[1], o[2]);
+}
+V3 sky_image(const OracleScene& S, V3 dir) {
+    float u = atan2f(dir.z, dir.x) / TWO_PI + 0.5f;
+    float v = -asinf(dir.y) / PI + 0.5f;
+    V3 c = env_fetch(S, u, v);
+    c = v3(std::min(c.x, 100000.0f), std::min(c.y, 100000.0f), std::min(c.z, 100000.0f));
+    if (!S.env_image_linear && S.use_linear_rgb) c = v3(srgb_to_lin(c.x), srgb_to_lin(c.y), srgb_to_lin(c.z));
+    else if (S.env_image_linear && !S.use_linear_rgb) c = v3(lin_to_srgb(c.x), lin_to_srgb(c.y), lin_to_srgb(c.z));
+    return mulv(v3(S.env_intensity[0], S.env_intensity[1], S.env_intensity[2]), c);
+}
+V3 sky_and_sun(const OracleScene& S, V3 dir) {
+    switch (S.env_kind) {
+        case 0: return add(sky_default(dir, S.use_linear_rgb), sun_lobe(S, dir));
+        case 1: return v3(0, 0, 0);
+        case 2: return v3(S.sun_intensity[0], S.sun_intensity[1], S.sun_intensity[2]);
+        case 3: return add(v3(S.sky_color[0], S.sky_color[1], S.sky_color[2]), sun_lobe(S, dir));
+        default: return sky_image(S, dir);
+    }
+}
+
+V3 oct_to_world(float u, float v) {
+    u = u * 2.0f - 1.0f;
+    v = v * 2.0f - 1.0f;
+    float sx = signf(u), sy = signf(v);
+    u = fabsf(u);
+    v = fabsf(v);
+    float r = 1.0f - fabsf(1.0f - u - v);
+    float phi = 0.25f * PI * ((v - u) / r + 1.0f);
+    if (r == 0.0f) phi = 0.0f;
+    float r2 = r * r, s = sqrtf(2.0f - r2);
+    return v3(sx * cosf(phi) * r * s, sy * sinf(phi) * r * s, signf(1.0f - u - v) * (1.0f - r2));
+}
+
+struct Pyramid {
+    std::vector<size_t> off;
+};
+float pyr(const OracleScene& S, const size_t* off, int level, int x, int y) {
+    int res = (1 << S.env_levels) >> level;
+    return S.env_pyramid[off[level] + (size_t)y * res + x] + 0.001f;
+}
+V3 sample_env_image(const OracleScene& S, const size_t* off, Rng& r, float& pdf) {
+    float rx = rnd(r), ry = rnd(r);
+    int px = 0, py = 0;
+    pdf = 0.25f / PI;
+    for (int mip = S.env_levels - 1; mip >= 0; mip--) {
+        px *= 2;
+        py *= 2;
+        pdf *= 4.0f;
+        float ul = pyr(S, off, mip, px, py), ur = pyr(S, off, mip, px + 1, py);
+        float dl = pyr(S, off, mip, px, py + 1), dr = pyr(S, off, mip, px + 1, py + 1);
+        float l = ul + dl, rr = ur + dr, total = l + rr;
+        float hs = l / total, vs;
+        if (rx < hs) {
+            rx = rx / hs;
+            vs = ul / l;
+            pdf *= hs;
+        } else {
+            px += 1;
+            rx = (rx - hs) / (1.0f - hs);
+            vs = ur / rr;
+            pdf *= (1.0f - hs);
+        }
+        if (ry < vs) {
+            ry = ry / vs;
+            pdf *= vs;
+        } else {
+            py += 1;
+            ry = (ry - vs) / (1.0f - vs);
+            pdf *= (1.0f - vs);
+        }
+    }
+    float inv = 1.0f / (float)(1 << S.env_levels);
+    return oct_to_world(((float)px + rx) * inv, ((float)py + ry) * inv);
+}
+
+// ---- density lookup (VptUtils.glsl:583-591, 674-683; CLAMP_TO_BORDER) ----
+struct Tracer {
+    const OracleScene& S;
+    std::vector<size_t> env_off;
+    uint64_t lookups = 0;
+    uint32_t steps = 0;
+
+    explicit Tracer(const OracleScene& s) : S(s) {
+        if (S.env_kind == 4) {
+            size_t o = 0;
+            for (int l = 0; l < S.env_levels; l++) {
+                env_off.push_back(o);
+                size_t r = (size_t)1 << (S.env_levels - l);
+                o += r * r;
+            }
+        }
+    }
+    V3 bmin() const { return v3(S.box_min[0], S.box_min[1], S.box_min[2]); }
+    V3 bmax() const { return v3(S.box_max[0], S.box_max[1], S.box_max[2]); }
+
+    float texel(int x, int y, int z) const {
+        if (x < 0 || y < 0 || z < 0 || x >= S.nx || y >= S.ny || z >= S.nz) return S.border_density;
+        return S.density[((size_t)z * S.ny + y) * S.nx + x];
+    }
+    float at_vox(float ux, float uy, float uz) const {
+        if (S.interp != 2) return texel((int)floorf(ux), (int)floorf(uy), (int)floorf(uz));
+        ux = ux - 0.5f;
+        uy = uy - 0.5f;
+        uz = uz - 0.5f;
+        float fx = floorf(ux), fy = floorf(uy), fz = floorf(uz);
+        float ax = ux - fx, ay = uy - fy, az = uz - fz;
+        int x0 = (int)fx, y0 = (int)fy, z0 = (int)fz;
+        float f0 = mixf(mixf(texel(x0, y0, z0), texel(x0 + 1, y0, z0), ax),
+                        mixf(texel(x0, y0 + 1, z0), texel(x0 + 1, y0 + 1, z0), ax), ay);
+        float f1 = mixf(mixf(texel(x0, y0, z0 + 1), texel(x0 + 1, y0, z0 + 1), ax),
+                        mixf(texel(x0, y0 + 1, z0 + 1), texel(x0 + 1, y0 + 1, z0 + 1), ax), ay);
+        return mixf(f0, f1, az);
+    }
+    float sample(V3 pos, Rng& r) {
+        lookups++;
+        float ux = (pos.x - S.box_min[0]) * S.vox_per_unit[0];
+        float uy = (pos.y - S.box_min[1]) * S.vox_per_unit[1];
+        float uz = (pos.z - S.box_min[2]) * S.vox_per_unit[2];
+        if (S.interp == 1) {
+            float jx = rnd(r) - 0.5f, jy = rnd(r) - 0.5f, jz = rnd(r) - 0.5f;
+            ux = ux + jx;
+            uy = uy + jy;
+            uz = uz + jz;
+        }
+        return at_vox(ux, uy, uz);
+    }
+    float free_path(Rng& r) const { return -logf(std::max(0.0000000001f, 1.0f - rnd(r))) * (1.0f / S.extinction); }
+    bool guard() { return ++steps > (1u << 24); }
+    V3 sky(V3 d) const { return sky_and_sun(S, d); }
+
+    // deltaTracking (DeltaTracking.glsl:168-344)
+    V3 delta(V3 x, V3 w, Rng& r, bool& ev) {
+        float tmin, tmax;
+        const float absorb = 1.0f - S.albedo;
+        if (ray_box(bmin(), bmax(), x, w, tmin, tmax)) {
+            x = add(x, mul(w, tmin));
+            float d = tmax - tmin;
+            int bounces = 0;
+            while (true) {
+                if (guard()) return v3(0, 0, 0);
+                float t = free_path(r);
+                if (t > d) break;
+                V3 xn = add(x, mul(w, t));
+                float dens = sample(xn, r);
+                x = xn;
+                float xi = rnd(r);
+                if (xi < absorb * dens) {
+                    ev = true;
+                    return v3(0, 0, 0);
+                }
+                if (xi < dens) {
+                    if (S.max_bounces > 0 && ++bounces > S.max_bounces) return v3(0, 0, 0);
+                    w = sample_phase(r, S.g, w);
+                    ev = true;
+                    if (ray_box(bmin(), bmax(), x, w, tmin, tmax)) {
+                        x = add(x, mul(w, tmin));
+                        d = tmax - tmin;
+                    }
+                } else {
+                    d -= t;
+                }
+            }
+        }
+        return sky(w);
+    }
+
+    // ratioTracking (RatioTracking.glsl:26-95)
+    V3 ratio(V3 x, V3 w, Rng& r, bool& ev) {
+        float trans = 1.0f, tmin, tmax;
+        if (ray_box(bmin(), bmax(), x, w, tmin, tmax)) {
+            x = add(x, mul(w, tmin));
+            float d = tmax - tmin;
+            int bounces = 0;
+            while (true) {
+                if (guard()) return v3(0, 0, 0);
+                float t = free_path(r);
+                if (t > d) break;
+                x = add(x, mul(w, t));
+                float dens = sample(x, r);
+                float xi = rnd(r);
+                if (xi < dens) {
+                    if (S.max_bounces > 0 && ++bounces > S.max_bounces) return v3(0, 0, 0);
+                    float pa = (1.0f - S.albedo) * dens, ps = S.albedo * dens;
+                    trans *= 1.0f - pa / (pa + ps);
+                    w = sample_phase(r, S.g, w);
+                    ev = true;
+                    if (ray_box(bmin(), bmax(), x, w, tmin, tmax)) {
+                        x = add(x, mul(w, tmin));
+                        d = tmax - tmin;
+                    }
+                } else {
+                    d -= t;
+                }
+            }
+        }
+        V3 l = sky(w);
+        return v3(l.x * trans, l.y * trans, l.z * trans);
+    }
+
+    // calculateTransmittance (NeeTransmittance.glsl:5-119), ratio tracking T *= P_n
+    float transmittance(V3 x, V3 w, Rng& r) {
+        float trans = 1.0f, tmin, tmax;
+        if (ray_box(bmin(), bmax(), x, w, tmin, tmax)) {
+            x = add(x, mul(w, tmin));
+            float d = tmax - tmin;
+            while (true) {
+                if (guard()) return 0.0f;
+                float t = free_path(r);
+                if (t > d) break;
+                V3 xn = add(x, mul(w, t));
+                float dens = sample(xn, r);
+                x = xn;
+                trans *= 1.0f - dens;
+                d -= t;
+            }
+        }
+        return trans;
+    }
+
+    void sv_step(V3 smin, V3 smax, V3 x, V3 w, int& ix, int& iy, int& iz) const {
+        V3 c = mul(add(smin, smax), 0.5f);
+        V3 mov = sub(add(x, mul(w, 0.00001f)), c);
+        float sx = signf(mov.x), sy = signf(mov.y), sz = signf(mov.z);
+        mov = v3(mov.x * sx, mov.y * sy, mov.z * sz);
+        ix += (mov.x >= mov.y && mov.x >= mov.z ? 1 : 0) * (int)sx;
+        iy += (mov.y >= mov.x && mov.y >= mov.z ? 1 : 0) * (int)sy;
+        iz += (mov.z >= mov.x && mov.z >= mov.y ? 1 : 0) * (int)sz;
+    }
+    V3 grid_f() const { return v3((float)S.nx, (float)S.ny, (float)S.nz); }
+    V3 svs_f() const { return v3((float)S.sv_size, (float)S.sv_size, (float)S.sv_size); }
+    V3 svw() const { return v3(S.sv_world[0], S.sv_world[1], S.sv_world[2]); }
+
+    // calculateTransmittance with USE_OCCUPANCY_GRID (NeeTransmittance.glsl:121-259)
+    float transmittance_ess(V3 x, V3 w, Rng& r) {
+        float trans = 1.0f;
+        V3 eps = v3(1e-6f, 1e-6f, 1e-6f);
+        float tminv, tmaxv;
+        if (!ray_box(add(bmin(), eps), sub(bmax(), eps), x, w, tminv, tmaxv)) return trans;
+        V3 delta = sub(bmax(), bmin());
+        x = add(x, mul(w, tminv));
+        V3 sp = divv(mulv(divv(sub(x, bmin()), delta), grid_f()), svs_f());
+        int ix = (int)floorf(sp.x), iy = (int)floorf(sp.y), iz = (int)floorf(sp.z);
+        int cx = ix, cy = iy, cz = iz;
+        bool empty = false;
+        while (ix >= 0 && iy >= 0 && iz >= 0 && ix < S.svx && iy < S.svy && iz < S.svz) {
+            if (guard()) return 0.0f;
+            V3 smin = add(bmin(), mulv(v3((float)ix, (float)iy, (float)iz), svw()));
+            V3 smax = add(smin, svw());
+            float ts0 = 0.0f, ts1 = 0.0f;
+            ray_box(smin, smax, x, w, ts0, ts1);
+            float dmax = ts1 - ts0;
+            x = add(x, mul(w, ts0));
+            if (cx != ix || cy != iy || cz != iz) {
+                empty = S.occupancy[((size_t)iz * S.svy + iy) * S.svx + ix] == 0;
+                cx = ix;
+                cy = iy;
+                cz = iz;
+            }
+            if (empty) {
+                x = add(x, mul(w, dmax));
+            } else {
+                // t counts from the supervoxel entry x0 (the reference steps from the moving x,
+                // NeeTransmittance.glsl:173-228, which overshoots; ess_ref_compat keeps that)
+                const V3 x0 = x;
+                float t = 0.0f;
+                while (true) {
+                    if (guard()) return 0.0f;
+                    t -= logf(std::max(0.0000000001f, 1.0f - rnd(r))) * (1.0f / S.extinction);
+                    if (t >= dmax) {
+                        x = add(S.ess_ref_compat ? x : x0, mul(w, dmax));
+                        break;
+                    }
+                    V3 xn = add(S.ess_ref_compat ? x : x0, mul(w, t));
+                    float dens = sample(xn, r);
+                    x = xn;
+                    trans *= 1.0f - dens;
+                }
+            }
+            sv_step(smin, smax, x, w, ix, iy, iz);
+        }
+        return trans;
+    }
+
+    V3 importance_sky(Rng& r, float& pdf) {
+        if (S.env_kind == 4) return sample_env_image(S, env_off.data(), r, pdf);
+        pdf = 1.0f / (4.0f * PI);
+        return random_direction(r, v3(1, 0, 0));
+    }
+
+    // nextEventTracking (NextEventTracking.glsl:224-393)
+    V3 nee(V3 x, V3 w, Rng& r, bool& ev) {
+        V3 color = v3(0, 0, 0);
+        float tmin, tmax;
+        const float absorb = 1.0f - S.albedo;
+        if (ray_box(bmin(), bmax(), x, w, tmin, tmax)) {
+            x = add(x, mul(w, tmin));
+            float d = tmax - tmin;
+            int bounces = 0;
+            while (true) {
+                if (guard()) return color;
+                float t = free_path(r);
+                if (t > d) break;
+                V3 xn = add(x, mul(w, t));
+                float dens = sample(xn, r);
+                x = xn;
+                float xi = rnd(r);
+                if (xi < absorb * dens) {
+                    ev = true;
+                    return color;
+                }
+                if (xi < dens) {
+                    if (S.max_bounces > 0 && ++bounces > S.max_bounces) return color;
+                    V3 nw = sample_phase(r, S.g, w);
+                    ev = true;
+                    float pdf_l;
+                    V3 dl = importance_sky(r, pdf_l);
+                    float pdf_p = eval_phase(S.g, w, dl);
+                    w = nw;
+                    float tr = S.use_ess ? transmittance_ess(x, dl, r) : transmittance(x, dl, r);
+                    float f = (pdf_p / pdf_l) * tr;
+                    V3 l = sky(dl);
+                    color = add(color, v3(f * l.x, f * l.y, f * l.z));
+                    if (ray_box(bmin(), bmax(), x, w, tmin, tmax)) {
+                        x = add(x, mul(w, tmin));
+                        d = tmax - tmin;
+                    }
+                } else {
+                    d -= t;
+                }
+            }
+        }
+        if (!ev) color = add(color, sky(w));
+        return color;
+    }
+
+    // analogDecompositionTracking, dense (DecompositionTracking.glsl:35-123)
+    V3 decomposition(V3 x, V3 w, Rng& r) {
+        V3 eps = v3(1e-6f, 1e-6f, 1e-6f);
+        float tminv, tmaxv;
+        if (ray_box(add(bmin(), eps), sub(bmax(), eps), x, w, tminv, tmaxv)) {
+            const float maj = S.extinction, absorb = 1.0f - S.albedo;
+            V3 delta = sub(bmax(), bmin());
+            x = add(x, mul(w, tminv));
+            V3 sp = divv(mulv(divv(sub(x, bmin()), delta), grid_f()), svs_f());
+            int ix = (int)floorf(sp.x), iy = (int)floorf(sp.y), iz = (int)floorf(sp.z);
+            int cx = -1, cy = -1, cz = -1;
+            float mn = 0.0f, mx = 0.0f;
+            int bounces = 0;
+            while (ix >= 0 && iy >= 0 && iz >= 0 && ix < S.svx && iy < S.svy && iz < S.svz) {
+                if (guard()) return v3(0, 0, 0);
+                V3 smin = add(bmin(), mulv(v3((float)ix, (float)iy, (float)iz), svw()));
+                V3 smax = add(smin, svw());
+                float ts0 = 0.0f, ts1 = 0.0f;
+                ray_box(smin, smax, x, w, ts0, ts1);
+                float dmax = ts1 - ts0;
+                x = add(x, mul(w, ts0));
+                if (cx != ix || cy != iy || cz != iz) {
+                    size_t k = ((size_t)iz * S.svy + iy) * S.svx + ix;
+                    mn = S.sv_data[2 * k];
+                    mx = S.sv_data[2 * k + 1];
+                    cx = ix;
+                    cy = iy;
+                    cz = iz;
+                }
+                if (mx < 1e-5f) {
+                    x = add(x, mul(w, dmax));
+                } else {
+                    float mu_c = std::max(0.0000000001f, maj * mn);
+                    float mu_r = std::max(0.0000000001f, maj * mx - mu_c);
+                    float t_c = -logf(std::max(0.0000000001f, 1.0f - rnd(r))) / mu_c;
+                    float t_r = 0.0f;
+                    while (true) {
+                        if (guard()) return v3(0, 0, 0);
+                        t_r -= logf(std::max(0.0000000001f, 1.0f - rnd(r))) / mu_r;
+                        if (t_c >= dmax && t_r >= dmax) {
+                            x = add(x, mul(w, dmax));
+                            break;
+                        }
+                        V3 xs = add(x, mul(w, std::min(t_c, t_r)));
+                        bool coll;
+                        if (t_c <= t_r) {
+                            coll = true;
+                        } else {
+                            float dens = sample(xs, r);
+                            coll = rnd(r) * mu_r < S.extinction * dens - mu_c;
+                        }
+                        if (coll) {
+                            x = xs;
+                            if (rnd(r) < absorb) return v3(0, 0, 0);
+                            if (S.max_bounces > 0 && ++bounces > S.max_bounces) return v3(0, 0, 0);
+                            w = sample_phase(r, S.g, w);
+                            t_r = 0.0f;
+                            t_c = -logf(std::max(0.0000000001f, 1.0f - rnd(r))) / mu_c;
+                            ray_box(smin, smax, x, w, ts0, ts1);
+                            dmax = ts1 - ts0;
+                        }
+                    }
+                }
+                sv_step(smin, smax, x, w, ix, iy, iz);
+            }
+        }
+        return sky(w);
+    }
+
+    // residualRatioTrackingEstimator (ResidualRatioTracking.glsl:34-76)
+    float rrt_est(V3 x, V3 w, float d0, float d1, float T, float& wsum, float& res_t, float& res_d, float mu_c,
+                  float mu_r, Rng& r) {
+        float tc = expf(-mu_c * (d1 - d0));
+        float tr = 1.0f;
+        float dt = d0;
+        while (true) {
+            if (guard()) break;
+            float t = -logf(std::max(0.0000000001f, 1.0f - rnd(r))) / mu_r;
+            x = add(x, mul(w, t));
+            dt += t;
+            if (dt >= d1) break;
+            float dens = sample(x, r);
+            float mu = S.extinction * dens;
+            tr *= 1.0f - (mu - mu_c) / mu_r;
+            float tcl = expf(-mu_c * (dt - d0));
+            float tl = (T * tr) * tcl;
+            wsum += tl;
+            float xi = rnd(r);
+            if (xi < tl / wsum) {
+                res_t = tl;
+                res_d = dt;
+            }
+        }
+        return tc * tr;
+    }
+
+    // residualRatioTracking (ResidualRatioTracking.glsl:78-223)
+    V3 rrt(V3 x, V3 w, Rng& r) {
+        float wsum = 0.0f, res_t = 0.0f, res_d = 0.0f, T = 1.0f;
+        V3 acc = v3(0, 0, 0);
+        V3 eps = v3(1e-6f, 1e-6f, 1e-6f);
+        V3 n = grid_f(), sv = svs_f(), delta = sub(bmax(), bmin());
+        V3 old_x = x;
+        int iteration = 0;
+        while (true) {
+            float tminv, tmaxv;
+            if (!ray_box(add(bmin(), eps), sub(bmax(), eps), x, w, tminv, tmaxv)) break;
+            x = add(x, mul(w, tminv));
+            old_x = x;
+            float dtot = tmaxv - tminv;
+            V3 sp = divv(mulv(divv(sub(x, bmin()), delta), n), sv);
+            V3 ep = divv(mulv(divv(sub(add(x, mul(w, dtot)), bmin()), delta), n), sv);
+            float spv[3] = {sp.x, sp.y, sp.z}, epv[3] = {ep.x, ep.y, ep.z};
+            int step[3], idx[3];
+            float tdel[3], tmx[3];
+            for (int a = 0; a < 3; a++) {
+                float diff = epv[a] - spv[a];
+                step[a] = (int)signf(diff);
+                tdel[a] = step[a] != 0 ? std::min((float)step[a] / diff, 1e7f) : 1e7f;
+                float fr = spv[a] - floorf(spv[a]);
+                tmx[a] = step[a] > 0 ? tdel[a] * (1.0f - fr) : tdel[a] * fr;
+                idx[a] = (int)floorf(spv[a]);
+            }
+            if (step[0] == 0 && step[1] == 0 && step[2] == 0) break;
+            while (idx[0] >= 0 && idx[1] >= 0 && idx[2] >= 0 && idx[0] < S.svx && idx[1] < S.svy && idx[2] < S.svz) {
+                if (guard()) return acc;
+                size_t k = ((size_t)idx[2] * S.svy + idx[1]) * S.svx + idx[0];
+                float mu_c = S.sv_data[2 * k], mu_r = S.sv_data[2 * k + 1];
+                V3 vmin = v3((float)(idx[0] * S.sv_size), (float)(idx[1] * S.sv_size), (float)(idx[2] * S.sv_size));
+                V3 vmax = v3((float)(idx[0] * S.sv_size + S.sv_size), (float)(idx[1] * S.sv_size + S.sv_size),
+                             (float)(idx[2] * S.sv_size + S.sv_size));
+                vmin = add(mulv(divv(vmin, n), delta), bmin());
+                vmax = add(mulv(divv(vmax, n), delta), bmin());
+                float tv0 = 0.0f, tv1 = 0.0f;
+                ray_box(vmin, vmax, old_x, w, tv0, tv1);
+                x = add(old_x, mul(w, tv0));
+                T *= rrt_est(x, w, tv0, tv1, T, wsum, res_t, res_d, mu_c, mu_r, r);
+                if (tmx[0] < tmx[1]) {
+                    if (tmx[0] < tmx[2]) {
+                        idx[0] += step[0];
+                        tmx[0] += tdel[0];
+                    } else {
+                        idx[2] += step[2];
+                        tmx[2] += tdel[2];
+                    }
+                } else {
+                    if (tmx[1] < tmx[2]) {
+                        idx[1] += step[1];
+                        tmx[1] += tdel[1];
+                    } else {
+                        idx[2] += step[2];
+                        tmx[2] += tdel[2];
+                    }
+                }
+            }
+            float xi = rnd(r);
+            if (xi > wsum || iteration >= 10) break;
+            V3 l = sky(w);
+            acc = add(acc, v3(l.x * T, l.y * T, l.z * T));
+            iteration++;
+            T = res_t;
+            x = add(old_x, mul(w, res_d));
+            w = sample_phase(r, S.g, w);
+            wsum = 0.0f;
+            res_t = 0.0f;
+            res_d = 0.0f;
+        }
+        V3 l = sky(w);
+        return add(acc, v3(l.x * T, l.y * T, l.z * T));
+    }
+
+    // pathTraceSample (Clouds.glsl:73-141): seed, jittered camera ray, tracker
+    V3 path(int px, int py, uint32_t frame) {
+        steps = 0;
+        uint32_t W = (uint32_t)S.width, H = (uint32_t)S.height;
+        uint32_t seed = (S.frame_count + frame) * W * H + (uint32_t)px + (uint32_t)py * W;
+        seed += S.seed_offset;
+        Rng r = rng_init(seed);
+        float rx = rnd(r), ry = rnd(r);
+        float sx = (2.0f * ((float)px + rx)) / (float)S.width - 1.0f;
+        float sy = (2.0f * ((float)py + ry)) / (float)S.height - 1.0f;
+        V3 x, w;
+        camera_ray(S, sx, sy, x, w);
+        bool ev = false;
+        switch (S.mode) {
+            case 0: return delta(x, w, r, ev);
+            case 2: return ratio(x, w, r, ev);
+            case 3: return decomposition(x, w, r);
+            case 4: return rrt(x, w, r);
+            default: return nee(x, w, r, ev);
+        }
+    }
+};
+
+int threads_or_default(int t) {
+#ifdef _OPENMP
+    return t > 0 ? t : omp_get_max_threads();
+#else
+    (void)t;
+    return 1;
+#endif
+}
+
+}  // namespace
+
+extern "C" {
+
+int oracle_render_rows(const OracleScene* s, int row0, int row1, double* film, uint64_t* lookups, int threads) {
+    const OracleScene& S = *s;
+    uint64_t total_lookups = 0;
+    int nt = threads_or_default(threads);
+    const int rows = row1 - row0;
+#pragma omp parallel num_threads(nt) reduction(+ : total_lookups)
+    {
+        Tracer T(S);
+#pragma omp for schedule(dynamic, 1)
+        for (int yy = 0; yy < rows; yy++) {
+            int y = row0 + yy;
+            for (int x = 0; x < S.width; x++) {
+                double acc[3] = {0, 0, 0};
+                for (uint32_t f = 0; f < S.num_frames; f++) {
+                    V3 L = T.path(x, y, f);
+                    acc[0] += L.x;
+                    acc[1] += L.y;
+                    acc[2] += L.z;
+                }
+                size_t p = (size_t)y * S.width + x;
+                film[p * 3 + 0] += acc[0];
+                film[p * 3 + 1] += acc[1];
+                film[p * 3 + 2] += acc[2];
+            }
+        }
+        total_lookups += T.lookups;
+    }
+    if (lookups) *lookups += total_lookups;
+    return 0;
+}
+
+int oracle_render(const OracleScene* s, double* film, double* film_sq, uint64_t* lookups, int threads) {
+    const OracleScene& S = *s;
+    uint64_t total_lookups = 0;
+    int nt = threads_or_default(threads);
+#pragma omp parallel num_threads(nt) reduction(+ : total_lookups)
+    {
+        Tracer T(S);
+#pragma omp for schedule(dynamic, 1)
+        for (int y = 0; y < S.height; y++) {
+            for (int x = 0; x < S.width; x++) {
+                double acc[3] = {0, 0, 0}, acc2[3] = {0, 0, 0};
+                for (uint32_t f = 0; f < S.num_frames; f++) {
+                    V3 L = T.path(x, y, f);
+                    acc[0] += L.x;
+                    acc[1] += L.y;
+                    acc[2] += L.z;
+                    acc2[0] += (double)L.x * L.x;
+                    acc2[1] += (double)L.y * L.y;
+                    acc2[2] += (double)L.z * L.z;
+                }
+                size_t p = (size_t)y * S.width + x;
+                for (int c = 0; c < 3; c++) {
+                    film[p * 3 + c] += acc[c];
+                    if (film_sq) film_sq[p * 3 + c] += acc2[c];
+                }
+            }
+        }
+        total_lookups += T.lookups;
+    }
+    if (lookups) *lookups += total_lookups;
+    return 0;
+}
+
+int oracle_trace_paths(const OracleScene* s, const int* xs, const int* ys, const uint32_t* frames, int n,
+                       float* out_rgb, int threads) {
+    int nt = threads_or_default(threads);
+#pragma omp parallel num_threads(nt)
+    {
+        Tracer T(*s);
+#pragma omp for schedule(dynamic, 64)
+        for (int i = 0; i < n; i++) {
+            V3 L = T.path(xs[i], ys[i], frames[i]);
+            out_rgb[3 * i + 0] = L.x;
+            out_rgb[3 * i + 1] = L.y;
+            out_rgb[3 * i + 2] = L.z;
+        }
+    }
+    return 0;
+}
+
+// ---- scene generation: improved Perlin noise (Perlin 2002), seeded permutation ----
+static uint32_t pcg(uint32_t& st) {
+    st = st * 747796405u + 2891336453u;
+    uint32_t word = ((st >> ((st >> 28u) + 4u)) ^ st) * 277803737u;
+    return (word >> 22u) ^ word;
+}
+static float fade(float t) { return t * t * t * (t * (t * 6.0f - 15.0f) + 10.0f); }
+static float lerpf(float t, float a, float b) { return a + t * (b - a); }
+static float grad(int h, float x, float y, float z) {
+    h &= 15;
+    float u = h < 8 ? x : y;
+    float v = h < 4 ? y : ((h == 12 || h == 14) ? x : z);
+    return ((h & 1) ? -u : u) + ((h & 2) ? -v : v);
+}
+static float perlin(const int* p, float x, float y, float z) {
+    float fx = floorf(x), fy = floorf(y), fz = floorf(z);
+    int X = (int)fx & 255, Y = (int)fy & 255, Z = (int)fz & 255;
+    x -= fx;
+    y -= fy;
+    z -= fz;
+    float u = fade(x), v = fade(y), w = fade(z);
+    int A = p[X] + Y, AA = p[A] + Z, AB = p[A + 1] + Z, B = p[X + 1] + Y, BA = p[B] + Z, BB = p[B + 1] + Z;
+    float r0 = lerpf(v, lerpf(u, grad(p[AA], x, y, z), grad(p[BA], x - 1.0f, y, z)),
+                     lerpf(u, grad(p[AB], x, y - 1.0f, z), grad(p[BB], x - 1.0f, y - 1.0f, z)));
+    float r1 = lerpf(v, lerpf(u, grad(p[AA + 1], x, y, z - 1.0f), grad(p[BA + 1], x - 1.0f, y, z - 1.0f)),
+                     lerpf(u, grad(p[AB + 1], x, y - 1.0f, z - 1.0f), grad(p[BB + 1], x - 1.0f, y - 1.0f, z - 1.0f)));
+    return lerpf(w, r0, r1);
+}
+
+void oracle_fbm(float* out, int nx, int ny, int nz, uint32_t seed, int octaves, float lacunarity, float gain,
+                float base_frequency, float threshold, float contrast) {
+    int perm[256], p[512];
+    for (int i = 0; i < 256; i++) perm[i] = i;
+    uint32_t st = seed;
+    for (int i = 255; i > 0; i--) {
+        uint32_t j = pcg(st) % (uint32_t)(i + 1);
+        std::swap(perm[i], perm[j]);
+    }
+    for (int i = 0; i < 512; i++) p[i] = perm[i & 255];
+    const float inv = 1.0f / (float)std::max(nx, std::max(ny, nz));
+#pragma omp parallel for schedule(static)
+    for (int z = 0; z < nz; z++)
+        for (int y = 0; y < ny; y++)
+            for (int x = 0; x < nx; x++) {
+                float px = ((float)x + 0.5f) * inv, py = ((float)y + 0.5f) * inv, pz = ((float)z + 0.5f) * inv;
+                float sum = 0.0f, amp = 1.0f, freq = base_frequency, norm = 0.0f;
+                for (int o = 0; o < octaves; o++) {
+                    sum += amp * perlin(p, px * freq, py * freq, pz * freq);
+                    norm += amp;
+                    amp *= gain;
+                    freq *= lacunarity;
+                }
+                float v = sum / norm;
+                v = std::min(std::max(0.5f + contrast * v, 0.0f), 1.0f);
+                out[((size_t)z * ny + y) * nx + x] = v < threshold ? 0.0f : v;
+            }
+}
+
+void oracle_minmax(const float* v, uint64_t n, float* out_min, float* out_max) {
+    float lo = INFINITY, hi = -INFINITY;
+    for (uint64_t i = 0; i < n; i++) {
+        lo = std::min(lo, v[i]);
+        hi = std::max(hi, v[i]);
+    }
+    if (lo == hi) lo = 0.0f;  // DensityField.cpp:146-150
+    *out_min = lo;
+    *out_max = hi;
+}
+
+void oracle_normalize(const float* in, float* out, uint64_t n, float vmin, float vmax) {
+    const float range = vmax - vmin;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < (int64_t)n; i++) out[i] = (in[i] - vmin) / range;
+}
+
+// CloudData::computeGridBounds (CloudData.cpp:63-78) with voxel size 1
+void oracle_grid_bounds(int nx, int ny, int nz, float e, float* bmin, float* bmax) {
+    float sx = (float)nx, sy = (float)ny, sz = (float)nz;
+    float ms = std::max(sx, std::max(sy, sz));
+    bmax[0] = sx * e / ms;
+    bmax[1] = sy * e / ms;
+    bmax[2] = sz * e / ms;
+    for (int i = 0; i < 3; i++) bmin[i] = -bmax[i];
+}
+
+// SuperVoxelGridResidualRatioTracking::computeSuperVoxels / SuperVoxelGridDecompositionTracking
+// (SuperVoxelGrid.cpp:101-211, 316-396)
+void oracle_supervoxel_stats(const float* dens, int nx, int ny, int nz, int sv, int halo, float* out_min,
+                             float* out_max, float* out_avg, uint8_t* out_occ) {
+    int gx = (nx + sv - 1) / sv, gy = (ny + sv - 1) / sv, gz = (nz + sv - 1) / sv;
+    int total = gx * gy * gz;
+#pragma omp parallel for schedule(static)
+    for (int idx = 0; idx < total; idx++) {
+        int bx = idx % gx, by = (idx / gx) % gy, bz = idx / (gx * gy);
+        float lo = 3.402823466e+38f, hi = -3.402823466e+38f, sum = 0.0f;
+        int cnt = 0;
+        int o0 = halo ? -1 : 0, o1 = halo ? sv : sv - 1;
+        for (int oz = o0; oz <= o1; oz++)
+            for (int oy = o0; oy <= o1; oy++)
+                for (int ox = o0; ox <= o1; ox++) {
+                    int x = bx * sv + ox, y = by * sv + oy, z = bz * sv + oz;
+                    float v = 0.0f;
+                    if (x >= 0 && y >= 0 && z >= 0 && x < nx && y < ny && z < nz) v = dens[((size_t)z * ny + y) * nx + x];
+                    lo = std::min(lo, v);
+                    hi = std::max(hi, v);
+                    sum += v;
+                    cnt++;
+                }
+        float avg = sum / (float)cnt;
+        if ((nx % sv != 0 && bx == gx - 1) || (ny % sv != 0 && by == gy - 1) || (nz % sv != 0 && bz == gz - 1)) lo = 0.0f;
+        out_min[idx] = lo;
+        out_max[idx] = hi;
+        if (out_avg) out_avg[idx] = avg;
+        if (out_occ) out_occ[idx] = hi < 1e-5f ? 0 : 1;
+    }
+}
+
+// SuperVoxelGridResidualRatioTracking::recomputeSuperVoxels (SuperVoxelGrid.cpp:218-256)
+void oracle_rrt_params(const float* mn, const float* mx, const float* avg, int total, float extinction, int sv,
+                       float* out_pairs) {
+    const float gamma = 2.0f;
+    const float D = sqrtf(3.0f) * (float)sv;
+    for (int i = 0; i < total; i++) {
+        float mu_min = mn[i] * extinction, mu_max = mx[i] * extinction, mu_avg = avg[i] * extinction;
+        float mu_r = std::max(mu_max - mu_min, 0.1f);
+        float mu_c = mu_min + mu_r * powf(gamma, (1.0f / (D * mu_r)) - 1.0f);
+        mu_c = std::min(std::max(mu_c, mu_min), mu_avg);
+        out_pairs[2 * i] = mu_c;
+        out_pairs[2 * i + 1] = mu_r;
+    }
+}
+
+// Occupancy of bs^3 blocks: any voxel (plus halo) above `threshold` (intent of
+// ComputeOccupancyGrid.glsl:91-143).
+void oracle_occupancy(const float* dens, int nx, int ny, int nz, int bs, int halo, float threshold, uint8_t* out) {
+    int gx = (nx + bs - 1) / bs, gy = (ny + bs - 1) / bs, gz = (nz + bs - 1) / bs;
+    for (int bz = 0; bz < gz; bz++)
+        for (int by = 0; by < gy; by++)
+            for (int bx = 0; bx < gx; bx++) {
+                bool occ = false;
+                for (int z = bz * bs - halo; z < bz * bs + bs + halo && !occ; z++)
+                    for (int y = by * bs - halo; y < by * bs + bs + halo && !occ; y++)
+                        for (int x = bx * bs - halo; x < bx * bs + bs + halo && !occ; x++)
+                            if (x >= 0 && y >= 0 && z >= 0 && x < nx && y < ny && z < nz &&
+                                dens[((size_t)z * ny + y) * nx + x] > threshold)
+                                occ = true;
+                out[((size_t)bz * gy + by) * gx + bx] = occ ? 1 : 0;
+            }
+}
+
+// OctahedralMapper.glsl:65-85 + 2x2 mip reduction
+void oracle_env_pyramid(const float* rgba, int w, int h, int levels, float* pyramid) {
+    OracleScene S;
+    memset(&S, 0, sizeof(S));
+    S.env_rgba = rgba;
+    S.env_w = w;
+    S.env_h = h;
+    int res = 1 << levels;
+#pragma omp parallel for schedule(static)
+    for (int y = 0; y < res; y++)
+        for (int x = 0; x < res; x++) {
+            float best = -1.0f;
+            for (int i = 0; i < 5; i++) {
+                float sxo = 0.1f + 0.2f * (float)i;
+                for (int j = 0; j < 5; j++) {
+                    float syo = 0.1f + 0.2f * (float)j;
+                    V3 dir = oct_to_world(((float)x + sxo) / (float)res, ((float)y + syo) / (float)res);
+                    float tu = atan2f(dir.z, dir.x) / (2.0f * PI) + 0.5f;
+                    float tv = -asinf(dir.y) / PI + 0.5f;
+                    V3 c = env_fetch(S, tu, tv);
+                    c = v3(std::min(c.x, 100000.0f), std::min(c.y, 100000.0f), std::min(c.z, 100000.0f));
+                    best = std::max(best, length(c));
+                }
+            }
+            pyramid[(size_t)y * res + x] = best;
+        }
+    size_t off_in = 0, off_out = (size_t)res * res;
+    for (int l = 1; l < levels; l++) {
+        int r = res >> l, ri = r * 2;
+        for (int y = 0; y < r; y++)
+            for (int x = 0; x < r; x++) {
+                const float* in = pyramid + off_in;
+                float a = in[(size_t)(2 * y) * ri + 2 * x], b = in[(size_t)(2 * y) * ri + 2 * x + 1];
+                float c = in[(size_t)(2 * y + 1) * ri + 2 * x], d = in[(size_t)(2 * y + 1) * ri + 2 * x + 1];
+                pyramid[off_out + (size_t)y * r + x] = ((a + b) + (c + d)) * 0.25f;
+            }
+        off_in = off_out;
+        off_out += (size_t)r * r;
+    }
+}
+
+// EAWDenoise.glsl:216-314 (compute path) / 92-158 (fragment path colour weight)
+void oracle_eaw(const float* color, const float* pos, const float* nrm, int w, int h, int iterations, float phi_c,
+                float phi_p, float phi_n, int quirk, float* out) {
+    std::vector<float> a(color, color + (size_t)w * h * 4), b((size_t)w * h * 4);
+    float kern[25];
+    for (int i = 0; i < 25; i++) {
+        int x = i % 5 - 2, y = i / 5 - 2;
+        kern[i] = expf(-float(x * x + y * y) / 2.0f);
+    }
+    auto ld = [&](const float* img, int x, int y, int c) {
+        x = std::min(std::max(x, 0), w - 1);
+        y = std::min(std::max(y, 0), h - 1);
+        return img[((size_t)y * w + x) * 4 + c];
+    };
+    int step = 1;
+    for (int it = 0; it < iterations; it++) {
+        const float* src = a.data();
+#pragma omp parallel for schedule(static)
+        for (int y = 0; y < h; y++)
+            for (int x = 0; x < w; x++) {
+                float cc[4], cp[4] = {0, 0, 0, 0}, cn[4] = {0, 0, 0, 0};
+                for (int c = 0; c < 4; c++) {
+                    cc[c] = ld(src, x, y, c);
+                    if (pos) cp[c] = ld(pos, x, y, c);
+                    if (nrm) cn[c] = ld(nrm, x, y, c);
+                }
+                float sum[4] = {0, 0, 0, 0}, acc = 0.0f;
+                const float qwc = std::min(expf(-1.0f / phi_c), 1.0f);
+                for (int i = 0; i < 25; i++) {
+                    int sx = x + (i % 5 - 2) * step, sy = y + (i / 5 - 2) * step;
+                    float oc[4];
+                    for (int c = 0; c < 4; c++) oc[c] = ld(src, sx, sy, c);
+                    float weight = 1.0f;
+                    float d[4];
+                    for (int c = 0; c < 4; c++) d[c] = cc[c] - oc[c];
+                    float dist = ((d[0] * d[0] + d[1] * d[1]) + d[2] * d[2]) + d[3] * d[3];
+                    weight *= quirk ? qwc : std::min(expf(-dist / phi_c), 1.0f);
+                    if (pos) {
+                        for (int c = 0; c < 4; c++) d[c] = cp[c] - ld(pos, sx, sy, c);
+                        dist = ((d[0] * d[0] + d[1] * d[1]) + d[2] * d[2]) + d[3] * d[3];
+                        weight *= std::min(expf(-dist / phi_p), 1.0f);
+                    }
+                    if (nrm) {
+                        for (int c = 0; c < 4; c++) d[c] = cn[c] - ld(nrm, sx, sy, c);
+                        dist = ((d[0] * d[0] + d[1] * d[1]) + d[2] * d[2]) + d[3] * d[3];
+                        weight *= std::min(expf(-dist / phi_n), 1.0f);
+                    }
+                    float wk = weight * kern[i];
+                    for (int c = 0; c < 4; c++) sum[c] += oc[c] * wk;
+                    acc += wk;
+                }
+                for (int c = 0; c < 4; c++) b[((size_t)y * w + x) * 4 + c] = sum[c] / acc;
+            }
+        std::swap(a, b);
+        step *= 2;
+    }
+    memcpy(out, a.data(), a.size() * sizeof(float));
+}
+
+void oracle_rng_stream(uint32_t seed, int n, float* out, uint32_t* st4) {
+    Rng r = rng_init(seed);
+    for (int i = 0; i < n; i++) out[i] = rnd(r);
+    if (st4) {
+        st4[0] = r.x;
+        st4[1] = r.y;
+        st4[2] = r.z;
+        st4[3] = r.w;
+    }
+}
+
+}  // extern "C"

@@ -1,0 +1,79 @@
+/*
+ * vpt_oracle.h - CPU oracle of the volumetric path-tracing hot path (TEST INFRASTRUCTURE).
+ *
+ * A plain C++17 + OpenMP restatement of the reference's shader math (Data/Shaders/VPT/*.glsl,
+ * src/PathTracer/SuperVoxelGrid.cpp, Data/Shaders/Denoiser/EAWDenoise.glsl).  It is the checker of
+ * the CUDA core and the timed CPU baseline; nothing in the product links or calls it.
+ *
+ * Arithmetic follows the same conventions as the CUDA core: no FMA contraction
+ * (-ffp-contract=off), IEEE division and sqrt, libm transcendentals (which may differ from CUDA's
+ * by an ulp, the only source of path divergence).
+ */
+#ifndef VPT_ORACLE_H
+#define VPT_ORACLE_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct OracleScene {
+    float inv_view_proj[16];  /* column-major */
+    int width, height;
+    uint32_t frame_count;     /* first frame index (seed frame) */
+    uint32_t num_frames;
+    uint32_t seed_offset;
+    int mode;                 /* VptMode numbering */
+    int interp;               /* 0 nearest, 1 stochastic, 2 trilinear */
+    int max_bounces;
+    int use_ess;              /* NEE: occupancy-grid empty-space skipping */
+    int ess_ref_compat;       /* reference stepping of the skipping shadow loop */
+    float box_min[3], box_max[3];
+    int nx, ny, nz;
+    float vox_per_unit[3];
+    float border_density;
+    float extinction, albedo, g;
+    int sv_size, svx, svy, svz;
+    float sv_world[3];
+    int env_kind, use_linear_rgb, env_image_linear;
+    float sun_dir[3], sun_intensity[3], sky_color[3], env_intensity[3];
+    int env_w, env_h, env_levels;
+    const float* density;     /* normalised, x-fastest */
+    const float* sv_data;     /* 2 floats per supervoxel */
+    const uint8_t* occupancy;
+    const float* env_rgba;
+    const float* env_pyramid; /* levels concatenated, level 0 first */
+} OracleScene;
+
+/* Renders width*height*num_frames paths; adds radiance (and its square) per pixel (3 doubles). */
+int oracle_render(const OracleScene* s, double* film, double* film_sq, uint64_t* lookups, int threads);
+/* One path per (x, y, frame) triple; writes rgb radiance per path. */
+int oracle_trace_paths(const OracleScene* s, const int* xs, const int* ys, const uint32_t* frames, int n,
+                       float* out_rgb, int threads);
+/* Rows [row0, row1) of every frame (bounded CPU-baseline samples). */
+int oracle_render_rows(const OracleScene* s, int row0, int row1, double* film, uint64_t* lookups, int threads);
+
+/* Scene preparation (same definitions as the CUDA core). */
+void oracle_fbm(float* out, int nx, int ny, int nz, uint32_t seed, int octaves, float lacunarity, float gain,
+                float base_frequency, float threshold, float contrast);
+void oracle_minmax(const float* v, uint64_t n, float* out_min, float* out_max);
+void oracle_normalize(const float* in, float* out, uint64_t n, float vmin, float vmax);
+void oracle_grid_bounds(int nx, int ny, int nz, float max_grid_extent, float* box_min, float* box_max);
+void oracle_supervoxel_stats(const float* dens, int nx, int ny, int nz, int sv, int halo, float* out_min,
+                             float* out_max, float* out_avg, uint8_t* out_occ);
+void oracle_rrt_params(const float* mn, const float* mx, const float* avg, int total, float extinction, int sv,
+                       float* out_pairs);
+void oracle_occupancy(const float* dens, int nx, int ny, int nz, int bs, int halo, float threshold, uint8_t* out);
+void oracle_env_pyramid(const float* rgba, int w, int h, int levels, float* pyramid);
+
+/* EAW a-trous chain on RGBA images (position/normal may be NULL). */
+void oracle_eaw(const float* color, const float* pos, const float* nrm, int w, int h, int iterations,
+                float phi_c, float phi_p, float phi_n, int quirk, float* out);
+
+/* Hybrid Tausworthe stream: n floats after seeding with `seed`. */
+void oracle_rng_stream(uint32_t seed, int n, float* out, uint32_t* out_state4);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

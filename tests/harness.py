@@ -1,0 +1,211 @@
+"""Test harness: drives the CUDA core through its C ABI and sets up the same scene in the CPU oracle.
+
+The oracle side recomputes everything from the raw grid with its own code (bounds, normalisation,
+supervoxels, occupancy, environment pyramid); only the camera matrix is taken from the core so that
+both sides start every path from the same float matrix.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+
+import numpy as np
+
+from cloudrendering_b200 import _lib
+from cloudrendering_b200._lib import check, farr
+from oracle import bridge
+
+MODE = {"delta": 0, "ratio": 2, "decomposition": 3, "rrt": 4, "nee": 5}
+INTERP = {"nearest": 0, "stochastic": 1, "trilinear": 2}
+ENV = {"default": 0, "black": 1, "single": 2, "constant_sun": 3, "image": 4}
+
+
+def cloud_block(xs, ys, zs, value=1.0, empty_boundary=False):
+    """createCloudBlock (test/VolumetricPathTracingTestData.cpp:32-61)."""
+    g = np.full((zs, ys, xs), value, np.float32)
+    if empty_boundary and xs >= 3 and ys >= 3 and zs >= 3:
+        g[:] = 0.0
+        g[1:zs - 1, 1:ys - 1, 1:xs - 1] = value
+    return g
+
+
+def supervoxel_size(nx, ny, nz, s=8):
+    """SuperVoxelGrid constructors (SuperVoxelGrid.cpp:46-58)."""
+    if nx < s or ny < s or nz < s:
+        while not (nx % s == 0 and ny % s == 0 and nz % s == 0):
+            s //= 2
+    return s
+
+
+class Core:
+    """One VptContext."""
+
+    def __init__(self, device=0):
+        self.lib = _lib.load()
+        c = ctypes.c_void_p()
+        st = self.lib.vpt_create(ctypes.byref(c), device)
+        if st != 0:
+            raise RuntimeError(f"vpt_create failed: {st}")
+        self.ctx = c.value
+
+    def __call__(self, name, *args):
+        check(getattr(self.lib, name)(self.ctx, *args), name, self.ctx)
+
+    def close(self):
+        if self.ctx:
+            self.lib.vpt_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        self.close()
+
+
+class SceneSpec:
+    def __init__(self, grid=None, mode="delta", interp="stochastic", extinction=1024.0, albedo=0.9, g=0.5,
+                 width=64, height=64, seed_offset=0, max_bounces=0, env="default", linear_rgb=0,
+                 sun_dir=(0.5826, 0.7660, 0.2717), sun_intensity=(2.6, 2.6 * 0.961538462, 2.6 * 0.884615385),
+                 sky_color=(1.0, 1.0, 1.0), cam_pos=(0.0, 0.0, 0.8), cam_target=(0.0, 0.0, 0.0),
+                 fovy=2.0 * math.atan(0.5), near=0.01, far=100.0, max_grid_extent=0.25, env_rgba=None,
+                 use_ess=False, env_intensity=(1.0, 1.0, 1.0)):
+        self.__dict__.update(locals())
+        del self.__dict__["self"]
+
+
+def setup_core(core: Core, sp: SceneSpec):
+    core("vpt_set_max_grid_extent", sp.max_grid_extent)
+    g = np.ascontiguousarray(sp.grid, np.float32)
+    nz, ny, nx = g.shape
+    core("vpt_set_dense_grid", g.ctypes.data_as(ctypes.c_void_p), nx, ny, nz, 0)
+    core("vpt_set_vpt_mode", MODE[sp.mode])
+    core("vpt_set_grid_interpolation", INTERP[sp.interp])
+    core("vpt_set_extinction_scale", sp.extinction)
+    core("vpt_set_extinction_base", farr([1, 1, 1]))
+    core("vpt_set_scattering_albedo", farr([sp.albedo] * 3))
+    core("vpt_set_phase_g", sp.g)
+    core("vpt_set_seed_offset", sp.seed_offset)
+    core("vpt_set_use_linear_rgb", sp.linear_rgb)
+    core("vpt_set_max_bounces", sp.max_bounces)
+    core("vpt_set_sun", farr(sp.sun_dir), farr(sp.sun_intensity))
+    core("vpt_set_sky_color", farr(sp.sky_color))
+    core("vpt_set_environment_map_intensity_rgb", farr(sp.env_intensity))
+    if sp.env == "image":
+        rgba = np.ascontiguousarray(sp.env_rgba, np.float32)
+        core("vpt_load_environment_map_rgba", rgba.ctypes.data_as(ctypes.c_void_p), rgba.shape[1], rgba.shape[0], 1, 0)
+    else:
+        core("vpt_set_builtin_environment_map", ENV[sp.env])
+    core("vpt_set_use_empty_space_skipping", 1 if sp.use_ess else 0)
+    core("vpt_set_camera", farr(sp.cam_pos), farr(sp.cam_target), farr([0, 1, 0]), sp.fovy, sp.near, sp.far)
+    core("vpt_set_resolution", sp.width, sp.height)
+    core("vpt_set_denoiser", 0)
+
+
+def gpu_render(core: Core, sp: SceneSpec, frames: int, stats=True):
+    """Renders `frames` frames from a reset film; returns (sum, sum_sq) as [H, W, 3] float64."""
+    core("vpt_set_collect_statistics", 1 if stats else 0)
+    core("vpt_reset_accumulation")
+    core("vpt_render_frames", frames, None)
+    core("vpt_synchronize", None)
+    n = sp.width * sp.height * 3
+    s = np.zeros(n, np.float64)
+    sq = np.zeros(n, np.float64) if stats else None
+    core("vpt_read_statistics", s.ctypes.data_as(ctypes.c_void_p),
+         sq.ctypes.data_as(ctypes.c_void_p) if stats else None, 0, None)
+    s = s.reshape(sp.height, sp.width, 3)
+    if stats:
+        sq = sq.reshape(sp.height, sp.width, 3)
+    return s, sq
+
+
+def camera_inv_view_proj(sp: SceneSpec):
+    """Same camera model as the core (vpt_set_camera): look-at view, perspective with depth in
+    [0, 1] and y flipped, computed in double, inverse rounded to float."""
+    e = np.array(sp.cam_pos, np.float64)
+    f = np.array(sp.cam_target, np.float64) - e
+    f /= np.linalg.norm(f)
+    s = np.cross(f, np.array([0.0, 1.0, 0.0]))
+    s /= np.linalg.norm(s)
+    u = np.cross(s, f)
+    view = np.array([[s[0], s[1], s[2], -s.dot(e)], [u[0], u[1], u[2], -u.dot(e)],
+                     [-f[0], -f[1], -f[2], f.dot(e)], [0, 0, 0, 1.0]])
+    th = math.tan(sp.fovy / 2.0)
+    aspect = sp.width / sp.height
+    n, fa = sp.near, sp.far
+    proj = np.zeros((4, 4))
+    proj[0, 0] = 1.0 / (aspect * th)
+    proj[1, 1] = -1.0 / th
+    proj[2, 2] = fa / (n - fa)
+    proj[3, 2] = -1.0
+    proj[2, 3] = -(fa * n) / (fa - n)
+    inv = np.linalg.inv(proj @ view)
+    return [float(np.float32(v)) for v in inv.T.reshape(-1)]  # column-major
+
+
+def oracle_scene(core, sp: SceneSpec, frames: int, frame_count: int = 0) -> bridge.Scene:
+    if core is not None:
+        inv = (ctypes.c_float * 16)()
+        vp = (ctypes.c_float * 16)()
+        core("vpt_get_camera_matrices", inv, vp)
+    else:
+        inv = camera_inv_view_proj(sp)
+    g = np.ascontiguousarray(sp.grid, np.float32)
+    nz, ny, nx = g.shape
+    vmin, vmax = bridge.minmax(g)
+    dens = bridge.normalize(g, vmin, vmax)
+    bmin, bmax = bridge.grid_bounds(nx, ny, nz, sp.max_grid_extent)
+    f32 = np.float32
+    vpu = [f32(n / (float(f32(b1)) - float(f32(b0)))) for n, b0, b1 in zip((nx, ny, nz), bmin, bmax)]
+    border = (f32(0.0) - f32(vmin)) / (f32(vmax) - f32(vmin))
+    sc = bridge.Scene(
+        inv_view_proj=list(inv), width=sp.width, height=sp.height, frame_count=frame_count, num_frames=frames,
+        seed_offset=sp.seed_offset, mode=MODE[sp.mode], interp=INTERP[sp.interp], max_bounces=sp.max_bounces,
+        use_ess=1 if sp.use_ess else 0, box_min=bmin, box_max=bmax, nx=nx, ny=ny, nz=nz, vox_per_unit=vpu,
+        border_density=float(border), extinction=float(f32(sp.extinction)), albedo=float(f32(sp.albedo)),
+        g=float(f32(sp.g)), env_kind=ENV[sp.env], use_linear_rgb=sp.linear_rgb, env_image_linear=1,
+        sun_intensity=sp.sun_intensity, sky_color=sp.sky_color, env_intensity=sp.env_intensity, density=dens)
+    # sun direction normalised exactly like vpt_set_sun (float ops in order)
+    d = np.array(sp.sun_dir, np.float32)
+    dl = np.sqrt(np.float32(np.float32(d[0] * d[0]) + np.float32(d[1] * d[1])) + np.float32(d[2] * d[2]), dtype=np.float32)
+    sc.set("sun_dir", [float(np.float32(d[i] / dl)) for i in range(3)])
+    ext = f32(sp.extinction)
+    if sp.mode in ("decomposition", "rrt") or sp.use_ess:
+        svs = 8 if sp.use_ess and sp.mode == "nee" else supervoxel_size(nx, ny, nz)
+        svx, svy, svz = -(-nx // svs), -(-ny // svs), -(-nz // svs)
+        delta = [f32(b1) - f32(b0) for b0, b1 in zip(bmin, bmax)]
+        svw = [(f32(svs) * dlt) / f32(n) for dlt, n in zip(delta, (nx, ny, nz))]
+        sc.set("sv_size", svs)
+        sc.set("svx", svx)
+        sc.set("svy", svy)
+        sc.set("svz", svz)
+        sc.set("sv_world", [float(v) for v in svw])
+        halo = 0 if sp.interp == "nearest" else 1
+        if sp.mode == "nee":
+            sc.set("occupancy", bridge.occupancy(dens, 8, halo, 0.0))
+        else:
+            mn, mx, avg, occ = bridge.supervoxel_stats(dens, svs, halo)
+            if sp.mode == "rrt":
+                sc.set("sv_data", bridge.rrt_params(mn, mx, avg, float(ext), svs))
+            else:
+                sc.set("sv_data", np.stack([mn, mx], axis=1).reshape(-1).copy())
+    if sp.env == "image":
+        rgba = np.ascontiguousarray(sp.env_rgba, np.float32)
+        sc.set("env_rgba", rgba)
+        sc.set("env_w", rgba.shape[1])
+        sc.set("env_h", rgba.shape[0])
+        sc.set("env_levels", 12)
+        sc.set("env_pyramid", bridge.env_pyramid(rgba, 12))
+    return sc
+
+
+def path_agreement(a: np.ndarray, b: np.ndarray, rtol=1e-4, atol=1e-5) -> float:
+    """Fraction of paths whose rgb radiance agrees within rtol/atol on every channel."""
+    ok = np.all(np.abs(a - b) <= atol + rtol * np.abs(b), axis=-1)
+    return float(ok.mean())
+
+
+def z_scores(sum_a, sq_a, n_a, sum_b, sq_b, n_b):
+    ma, mb = sum_a / n_a, sum_b / n_b
+    va = np.maximum(sq_a / n_a - ma * ma, 0.0) * n_a / max(n_a - 1, 1)
+    vb = np.maximum(sq_b / n_b - mb * mb, 0.0) * n_b / max(n_b - 1, 1)
+    se = np.sqrt(va / n_a + vb / n_b)
+    z = np.where(se > 0, (ma - mb) / np.where(se > 0, se, 1.0), np.where(np.abs(ma - mb) > 1e-7, np.inf, 0.0))
+    return z

@@ -1,0 +1,100 @@
+"""The drop-in module surface (initialize / render_frame / cleanup and the setters) on the GPU, with
+the reference's error behaviour (Module.cpp:286-317)."""
+import numpy as np
+import pytest
+import torch
+
+from cloudrendering_b200 import vpt
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module", autouse=True)
+def module():
+    vpt.initialize()
+    yield
+    vpt.cleanup()
+
+
+def test_render_frame_cpu_and_cuda_shapes():
+    for dev in ("cpu", "cuda"):
+        for c in (3, 4):
+            t = torch.zeros((c, 40, 56), dtype=torch.float32, device=dev)
+            out = vpt.render_frame(t, 2)
+            assert out.shape == (c, 40, 56) and out.dtype == torch.float32 and out.device == t.device
+            assert torch.isfinite(out).all()
+            if c == 4:
+                assert torch.all(out[3] == 1.0)
+
+
+def test_accumulation_continues_across_calls():
+    vpt.set_vpt_mode_from_name("Delta Tracking")
+    t = torch.zeros((3, 32, 32), dtype=torch.float32, device="cuda")
+    vpt.set_seed_offset(0)  # resets accumulation
+    a = vpt.render_frame(t, 4)
+    b = vpt.render_frame(t, 4)  # mean over 8 frames
+    vpt.set_seed_offset(0)
+    c = vpt.render_frame(t, 8)
+    assert torch.allclose(b, c, rtol=1e-5, atol=1e-6)
+    assert not torch.equal(a, b)
+
+
+def test_errors_match_reference():
+    with pytest.raises(RuntimeError, match="sizes"):
+        vpt.render_frame(torch.zeros((32, 32)), 1)
+    with pytest.raises(RuntimeError, match="channels"):
+        vpt.render_frame(torch.zeros((2, 32, 32)), 1)
+    with pytest.raises(RuntimeError, match="32-bit float"):
+        vpt.render_frame(torch.zeros((3, 32, 32), dtype=torch.float64), 1)
+    with pytest.raises(RuntimeError):
+        vpt.set_denoiser("OptiX Denoiser")
+
+
+def test_settings_surface_and_fbm_scene():
+    vpt.set_max_grid_extent(0.5)
+    vpt.generate_fbm_cloud(64, seed=1)
+    bb = vpt.get_render_bounding_box()
+    assert np.allclose(bb, [-0.5, 0.5, -0.5, 0.5, -0.5, 0.5])
+    vpt.set_extinction_scale(200.0)
+    vpt.set_scattering_albedo([0.99, 0.99, 0.99])
+    vpt.set_phase_g(0.85)
+    vpt.set_use_builtin_environment_map("Constant Sky + Sun")
+    vpt.set_sky_color([0.2, 0.2, 0.2])
+    vpt.set_sun([0.3, 0.8, 0.5], [5.0, 5.0, 5.0])
+    vpt.set_camera_position([0.0, 0.3, 2.0])
+    vpt.set_camera_target([0.0, 0.0, 0.0])
+    vpt.set_camera_fovy(60.0)
+    vpt.set_max_bounces(64)
+    t = torch.zeros((4, 64, 64), dtype=torch.float32, device="cuda")
+    for name in vpt.VPT_MODE_NAMES[:6]:
+        if name == "Delta Tracking (Spectral)":
+            with pytest.raises(RuntimeError):
+                vpt.set_vpt_mode_from_name(name)
+            continue
+        vpt.set_vpt_mode_from_name(name)
+        img = vpt.render_frame(t, 4)
+        assert torch.isfinite(img).all() and img[:3].mean() > 0.0
+    st = vpt.get_stats()
+    assert st["paths"] > 0 and st["density_lookups"] > 0
+
+
+def test_feature_maps_and_eaw():
+    vpt.set_vpt_mode_from_name("Next Event Tracking")
+    vpt.set_use_feature_maps(["Result", "First X", "Normal", "Depth", "Albedo", "Transmittance"])
+    t = torch.zeros((3, 48, 48), dtype=torch.float32, device="cuda")
+    img = vpt.render_frame(t, 8)
+    pos = vpt.get_feature_map_from_string(t, "First X")
+    assert pos.shape == (4, 48, 48)
+    hit = pos[3]
+    assert 0.0 < float(hit.mean()) <= 1.0
+    tr = vpt.get_feature_map_from_string(t, "Transmittance")
+    assert torch.allclose(tr[0] + hit, torch.ones_like(hit), atol=1e-5)
+    vpt.set_denoiser("Edge-Avoiding À-Trous Wavelet Transform")
+    vpt.set_denoiser_property("iterations", "3")
+    den = vpt.render_frame(t, 8)
+    assert den.shape == img.shape and torch.isfinite(den).all()
+    assert float(den.std()) <= float(img.std()) * 1.05
+    vpt.set_denoiser("SVGF")
+    s = vpt.render_frame(t, 1)
+    assert torch.isfinite(s).all()
+    vpt.set_denoiser("None")

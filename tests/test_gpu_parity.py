@@ -1,0 +1,211 @@
+"""GPU parity tests: the CUDA core (through its C ABI) against the CPU oracle on the same inputs.
+
+* integer / builder work is bit-exact: fBm grid, supervoxel min/max/mean/occupancy, occupancy grid;
+* paths: every camera path of a 1-spp frame is traced by both sides from the same seed and camera
+  matrix; they take the same random decisions, so the radiance agrees to float rounding except for
+  paths where a libm / CUDA transcendental differs by an ulp and flips a later comparison.  The test
+  requires >= 99% of paths to agree to rtol 1e-4 (measured agreement is printed);
+* images: per-pixel z-test (Bonferroni, |z| < 6) and image-mean agreement at 64 frames.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import bridge
+from tests.harness import (Core, SceneSpec, cloud_block, gpu_render, oracle_scene, path_agreement, setup_core,
+                           z_scores)
+
+pytestmark = pytest.mark.gpu
+
+AGREE_MIN = 0.99
+
+
+@pytest.fixture(scope="module")
+def core():
+    c = Core(0)
+    yield c
+    c.close()
+
+
+def dptr(t: torch.Tensor):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def test_fbm_grid_bit_exact(core):
+    for (nx, ny, nz), seed in [((64, 64, 64), 1), ((40, 24, 33), 7)]:
+        core("vpt_generate_fbm_grid", nx, ny, nz, seed, 6, 2.0, 0.5, 3.0, 0.3)
+        out = np.empty((nz, ny, nx), np.float32)
+        core("vpt_get_dense_grid", out.ctypes.data_as(ctypes.c_void_p), 0)
+        ref = bridge.fbm((nx, ny, nz), seed, base_frequency=3.0, contrast=3.5)
+        assert np.array_equal(out.view(np.uint32), ref.view(np.uint32))
+
+
+@pytest.mark.parametrize("shape,sv,halo", [((64, 64, 64), 8, 0), ((64, 64, 64), 8, 1), ((37, 20, 29), 8, 1),
+                                           ((6, 6, 6), 2, 0)])
+def test_supervoxel_grid_bit_exact(core, shape, sv, halo):
+    nz, ny, nx = shape
+    g = bridge.fbm((nx, ny, nz), 11, base_frequency=3.0, contrast=3.5)
+    d = torch.from_numpy(g).cuda()
+    gx, gy, gz = -(-nx // sv), -(-ny // sv), -(-nz // sv)
+    n = gx * gy * gz
+    mn, mx, avg = (torch.empty(n, device="cuda") for _ in range(3))
+    occ = torch.empty(n, dtype=torch.uint8, device="cuda")
+    lib = core.lib
+    assert lib.vpt_build_supervoxel_grid(dptr(d), nx, ny, nz, sv, halo, dptr(mn), dptr(mx), dptr(avg), dptr(occ),
+                                         None) == 0
+    torch.cuda.synchronize()
+    rmn, rmx, ravg, rocc = bridge.supervoxel_stats(g, sv, halo)
+    assert np.array_equal(mn.cpu().numpy().view(np.uint32), rmn.view(np.uint32))
+    assert np.array_equal(mx.cpu().numpy().view(np.uint32), rmx.view(np.uint32))
+    assert np.array_equal(avg.cpu().numpy().view(np.uint32), ravg.view(np.uint32))
+    assert np.array_equal(occ.cpu().numpy(), rocc)
+    pairs = torch.empty(2 * n, device="cuda")
+    assert lib.vpt_build_rrt_params(dptr(mn), dptr(mx), dptr(avg), n, 1000.0, sv, dptr(pairs), None) == 0
+    torch.cuda.synchronize()
+    ref = bridge.rrt_params(rmn, rmx, ravg, 1000.0, sv)
+    # mu_c uses powf (CUDA vs libm may differ by one ulp); mu_r_bar is exact
+    got = pairs.cpu().numpy()
+    assert np.array_equal(got[1::2], ref[1::2])
+    assert np.allclose(got[0::2], ref[0::2], rtol=2e-7, atol=0)
+
+
+@pytest.mark.parametrize("halo", [0, 1])
+def test_occupancy_grid_bit_exact(core, halo):
+    g = bridge.fbm((48, 40, 56), 3, base_frequency=3.0, contrast=3.5)
+    g[g < 0.6] = 0.0
+    nz, ny, nx = g.shape
+    d = torch.from_numpy(g).cuda()
+    n = 6 * 5 * 7
+    out = torch.empty(n, dtype=torch.uint8, device="cuda")
+    assert core.lib.vpt_build_occupancy_grid(dptr(d), nx, ny, nz, 8, halo, 0.0, dptr(out), None) == 0
+    torch.cuda.synchronize()
+    assert np.array_equal(out.cpu().numpy(), bridge.occupancy(g, 8, halo, 0.0))
+
+
+def test_environment_pyramid_matches_oracle(core):
+    rng = np.random.default_rng(4)
+    rgba = np.ones((32, 64, 4), np.float32)
+    rgba[..., :3] = rng.random((32, 64, 3)).astype(np.float32) * 3.0
+    levels = 8
+    total = sum((1 << (levels - l)) ** 2 for l in range(levels))
+    d = torch.from_numpy(rgba).cuda()
+    out = torch.empty(total, device="cuda")
+    assert core.lib.vpt_build_environment_pyramid(dptr(d), 64, 32, levels, dptr(out), None) == 0
+    torch.cuda.synchronize()
+    ref = bridge.env_pyramid(rgba, levels)
+    assert np.allclose(out.cpu().numpy(), ref, rtol=1e-5, atol=1e-6)
+
+
+@pytest.mark.parametrize("quirk", [0, 1])
+def test_eaw_matches_oracle(core, quirk):
+    rng = np.random.default_rng(5)
+    h, w = 48, 64
+    color = rng.random((h, w, 4)).astype(np.float32)
+    pos = rng.random((h, w, 4)).astype(np.float32) * 0.2
+    nrm = rng.random((h, w, 4)).astype(np.float32)
+    dc, dp, dn = (torch.from_numpy(a).cuda() for a in (color, pos, nrm))
+    out = torch.empty_like(dc)
+    assert core.lib.vpt_eaw_denoise_rgba(dptr(dc), dptr(dp), dptr(dn), w, h, 3, 5.0, 0.1, 0.1, quirk, dptr(out),
+                                         None) == 0
+    torch.cuda.synchronize()
+    ref = bridge.eaw(color, pos, nrm, 3, 5.0, 0.1, 0.1, quirk)
+    assert np.allclose(out.cpu().numpy(), ref, rtol=1e-5, atol=1e-6)
+
+
+def fbm_scene(**kw):
+    g = bridge.fbm(48, 2, base_frequency=3.0, contrast=3.5)
+    base = dict(grid=g, extinction=150.0, albedo=0.99, g=0.85, width=64, height=64, env="constant_sun",
+                sky_color=(0.2, 0.2, 0.2), sun_dir=(0.3, 0.8, 0.5), sun_intensity=(5.0, 5.0, 5.0),
+                cam_pos=(0.3, 0.4, 1.4), max_grid_extent=0.5, linear_rgb=1, max_bounces=64)
+    base.update(kw)
+    return SceneSpec(**base)
+
+
+PATH_CASES = {
+    "delta_stochastic": dict(mode="delta"),
+    "delta_nearest": dict(mode="delta", interp="nearest"),
+    "delta_trilinear": dict(mode="delta", interp="trilinear"),
+    "ratio": dict(mode="ratio"),
+    "nee": dict(mode="nee"),
+    "nee_ess": dict(mode="nee", use_ess=True),
+    "decomposition": dict(mode="decomposition"),
+    "decomposition_trilinear": dict(mode="decomposition", interp="trilinear"),
+    "rrt": dict(mode="rrt"),
+    "delta_default_sky": dict(mode="delta", env="default", linear_rgb=0),
+    "nee_default_sky_g0": dict(mode="nee", env="default", g=0.0),
+}
+
+
+@pytest.mark.parametrize("case", sorted(PATH_CASES))
+def test_path_parity(core, case):
+    sp = fbm_scene(**PATH_CASES[case])
+    setup_core(core, sp)
+    s, _ = gpu_render(core, sp, 1, stats=False)
+    sc = oracle_scene(core, sp, 1)
+    ys, xs = np.mgrid[0:sp.height, 0:sp.width]
+    ref = sc.trace_paths(xs.reshape(-1), ys.reshape(-1), np.zeros(xs.size, np.uint32)).reshape(sp.height, sp.width, 3)
+    agree = path_agreement(s.astype(np.float32), ref)
+    print(f"{case}: path agreement {agree:.5f}")
+    assert agree >= AGREE_MIN
+
+
+def test_path_parity_environment_image(core):
+    rng = np.random.default_rng(9)
+    rgba = np.ones((64, 128, 4), np.float32)
+    rgba[..., :3] = 0.2
+    rgba[10:14, 40:46, :3] = 50.0  # a small bright "sun" patch
+    rgba[..., :3] += rng.random((64, 128, 3)).astype(np.float32) * 0.05
+    sp = fbm_scene(mode="nee", env="image", env_rgba=rgba)
+    setup_core(core, sp)
+    s, _ = gpu_render(core, sp, 1, stats=False)
+    sc = oracle_scene(core, sp, 1)
+    ys, xs = np.mgrid[0:sp.height, 0:sp.width]
+    ref = sc.trace_paths(xs.reshape(-1), ys.reshape(-1), np.zeros(xs.size, np.uint32)).reshape(sp.height, sp.width, 3)
+    agree = path_agreement(s.astype(np.float32), ref)
+    print(f"env image nee: path agreement {agree:.5f}")
+    assert agree >= AGREE_MIN
+
+
+@pytest.mark.parametrize("case", ["delta_stochastic", "nee", "decomposition", "rrt"])
+def test_image_statistics_match_oracle(core, case):
+    sp = fbm_scene(**PATH_CASES[case], width=48, height=48)
+    frames = 64
+    setup_core(core, sp)
+    s, sq = gpu_render(core, sp, frames)
+    sc = oracle_scene(core, sp, frames)
+    rs, rsq, _ = sc.render(with_sq=True)
+    rs = rs.reshape(s.shape)
+    rsq = rsq.reshape(s.shape)
+    z = z_scores(s, sq, frames, rs, rsq, frames)
+    assert np.nanmax(np.abs(z)) < 6.0
+    assert np.all(np.abs(s.mean(axis=(0, 1)) - rs.mean(axis=(0, 1))) / frames <= 1e-3)
+
+
+def test_lookup_counter_matches_oracle(core):
+    sp = fbm_scene(mode="delta", width=32, height=32)
+    setup_core(core, sp)
+    core("vpt_reset_stats")
+    gpu_render(core, sp, 4, stats=False)
+    from cloudrendering_b200._lib import VptStats
+    st = VptStats()
+    core("vpt_get_stats", ctypes.byref(st))
+    sc = oracle_scene(core, sp, 4)
+    _, _, lookups = sc.render()
+    assert st.paths == 32 * 32 * 4
+    assert abs(st.density_lookups - lookups) <= 0.01 * lookups
+
+
+def test_iteration_guard_reports_error_without_hanging(core):
+    sp = SceneSpec(grid=cloud_block(8, 8, 8), mode="delta", width=16, height=16)
+    setup_core(core, sp)
+    core("vpt_reset_stats")
+    core("vpt_set_option", b"max_steps_per_path", 8.0)
+    core("vpt_render_frames", 1, None)
+    st = core.lib.vpt_synchronize(core.ctx, None)
+    assert st == 4  # VPT_ERR_ITER_LIMIT
+    core("vpt_set_option", b"max_steps_per_path", float(1 << 24))
+    core("vpt_reset_stats")
+    core("vpt_render_frames", 1, None)
+    core("vpt_synchronize", None)

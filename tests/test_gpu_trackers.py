@@ -1,0 +1,95 @@
+"""The reference's tracker-agreement tests (test/TestVolumetricPathTracing.cpp:156-281) on the CUDA
+core, 1:1: 128x128, 64 spp, |mean0 - mean1| <= 1e-3 per RGB channel, the reference's default
+medium (extinction 1024, albedo 0.9, g 0.5), default sky with sun lobe, sRGB output, camera at
+(0, 0, 0.8), fovy 2 atan(1/2).  Plus the cases the reference does not test (residual ratio
+tracking, trilinear, empty-space skipping, the 64-scene-style fBm cloud)."""
+import numpy as np
+import pytest
+
+from oracle import bridge
+from tests.harness import Core, SceneSpec, cloud_block, gpu_render, setup_core, z_scores
+
+pytestmark = pytest.mark.gpu
+
+EPS = 1e-3
+RES = 128
+SPP = 64
+
+
+@pytest.fixture(scope="module")
+def core():
+    c = Core(0)
+    yield c
+    c.close()
+
+
+def mean_image(core, sp, frames=SPP):
+    setup_core(core, sp)
+    s, sq = gpu_render(core, sp, frames)
+    return s, sq
+
+
+def assert_equal_mean(core, sp0, sp1, eps=EPS, frames=SPP):
+    s0, _ = mean_image(core, sp0, frames)
+    s1, _ = mean_image(core, sp1, frames)
+    m0 = (s0 / frames).mean(axis=(0, 1))
+    m1 = (s1 / frames).mean(axis=(0, 1))
+    print("means", m0, m1)
+    assert np.all(np.abs(m0 - m1) <= eps), (m0, m1)
+
+
+def spec(grid, mode, **kw):
+    return SceneSpec(grid=grid, mode=mode, width=RES, height=RES, **kw)
+
+
+def test_delta_ratio_equal_mean(core):
+    g = cloud_block(1, 1, 1)
+    assert_equal_mean(core, spec(g, "delta"), spec(g, "ratio"))
+
+
+def test_delta_seed_independent_equal_mean(core):
+    g = cloud_block(1, 1, 1)
+    assert_equal_mean(core, spec(g, "delta"), spec(g, "delta", seed_offset=268435456))
+
+
+@pytest.mark.parametrize("interp", ["nearest", "stochastic"])
+def test_delta_decomposition_equal_mean(core, interp):
+    g = cloud_block(8, 8, 8)
+    assert_equal_mean(core, spec(g, "delta", interp=interp), spec(g, "decomposition", interp=interp))
+
+
+def test_delta_decomposition_equal_mean_boundary_layer(core):
+    g = cloud_block(8, 8, 8, empty_boundary=True)
+    assert_equal_mean(core, spec(g, "delta"), spec(g, "decomposition"))
+
+
+def test_delta_nee_equal_mean(core):
+    g = cloud_block(8, 8, 8, empty_boundary=True)
+    assert_equal_mean(core, spec(g, "delta"), spec(g, "nee"))
+
+
+# ---- beyond the reference's suite ----
+
+def fbm_spec(mode, **kw):
+    g = bridge.fbm(64, 1, base_frequency=3.0, contrast=3.5)
+    base = dict(extinction=200.0, albedo=0.99, g=0.85, env="constant_sun", sky_color=(0.2, 0.2, 0.2),
+                sun_dir=(0.3, 0.8, 0.5), sun_intensity=(5.0, 5.0, 5.0), cam_pos=(0.0, 0.3, 2.0),
+                max_grid_extent=0.5, linear_rgb=1, fovy=np.radians(60.0), width=96, height=96)
+    base.update(kw)
+    return SceneSpec(grid=g, mode=mode, **base)
+
+
+@pytest.mark.parametrize("mode,kw", [("ratio", {}), ("decomposition", {}), ("nee", {}), ("nee", {"use_ess": True}),
+                                     ("rrt", {}), ("decomposition", {"interp": "trilinear"})])
+def test_trackers_agree_with_delta_per_pixel(core, mode, kw):
+    """Every tracker agrees with delta tracking on the fBm cloud under a per-pixel z-test."""
+    frames = 128
+    base_kw = {k: v for k, v in kw.items() if k == "interp"}
+    s0, q0 = mean_image(core, fbm_spec("delta", **base_kw), frames)
+    s1, q1 = mean_image(core, fbm_spec(mode, **kw), frames)
+    z = z_scores(s0, q0, frames, s1, q1, frames)
+    zmax = float(np.nanmax(np.abs(z)))
+    print(mode, kw, "max |z|", zmax, "mean diff", (s0 - s1).mean(axis=(0, 1)) / frames)
+    assert zmax < 6.0
+    m0, m1 = (s0 / frames).mean(axis=(0, 1)), (s1 / frames).mean(axis=(0, 1))
+    assert np.all(np.abs(m0 - m1) <= 5e-3 * np.maximum(1.0, np.abs(m0)))
