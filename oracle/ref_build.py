@@ -1,0 +1,162 @@
+"""Builds the reference's own code for the CPU (TEST INFRASTRUCTURE ONLY; outputs in oracle/_ref/).
+
+1. ``libref_vpt.so``: the reference tracer shaders (Data/Shaders/VPT/Clouds.glsl and everything it
+   includes) compiled as C++ on top of ``ref_shim.h``.  The GLSL text is rewritten mechanically
+   (comments dropped, ``in/out/inout`` parameter qualifiers -> C++ values/references, float
+   literals -> ``f`` suffix, the RNG state made thread-local, ``main`` renamed); nothing else is
+   changed.  One variant per (tracker, interpolation, environment, colour space) define set, as the
+   reference's loadShader() would select (VolumetricPathTracingPass.cpp:1558-1782).
+2. ``libref_svgrid.so``: src/PathTracer/SuperVoxelGrid.cpp compiled against stub headers for the
+   GPU-upload parts (the CPU loops are the reference's).
+3. ``libref_pnanovdb.so``: Data/Shaders/VPT/PNanoVDB.glsl compiled as C99 (-DPNANOVDB_C).
+
+The reference tree is read from $VPT_REFERENCE_ROOT or /root/reference; when it is absent the build
+is skipped (the prebuilt libraries under oracle/_ref are used as they are).
+"""
+from __future__ import annotations
+
+import os
+import re
+import subprocess
+import sys
+from concurrent.futures import ThreadPoolExecutor
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+OUT = os.path.join(HERE, "_ref")
+GEN = os.path.join(OUT, "gen")
+REF = os.environ.get("VPT_REFERENCE_ROOT", "/root/reference")
+SHADERS = os.path.join(REF, "Data", "Shaders", "VPT")
+
+# (name, defines) of the tracer variants; the C driver indexes them in this order.
+TRACKERS = {
+    "delta": ["USE_DELTA_TRACKING"],
+    "ratio": ["USE_RATIO_TRACKING"],
+    "decomposition": ["USE_DECOMPOSITION_TRACKING"],
+    "rrt": ["USE_RESIDUAL_RATIO_TRACKING"],
+    "nee": ["USE_NEXT_EVENT_TRACKING"],
+    "nee_ess": ["USE_NEXT_EVENT_TRACKING", "USE_OCCUPANCY_GRID"],
+}
+INTERPS = {"nearest": "GRID_INTERPOLATION_NEAREST", "stochastic": "GRID_INTERPOLATION_STOCHASTIC",
+           "trilinear": "GRID_INTERPOLATION_TRILINEAR"}
+# environment x colour space combinations that are built
+ENVS = {
+    "default__srgb": ["USE_ENVIRONMENT_MAP_DEFAULT"],
+    "default__linear": ["USE_ENVIRONMENT_MAP_DEFAULT", "USE_LINEAR_RGB"],
+    "black__linear": ["USE_ENVIRONMENT_MAP_BLACK", "USE_LINEAR_RGB"],
+    "single__linear": ["USE_ENVIRONMENT_MAP_SINGLE_COLOR", "USE_LINEAR_RGB"],
+    "image__linear": ["USE_ENVIRONMENT_MAP_IMAGE", "ENV_MAP_IMAGE_USES_LINEAR_RGB", "USE_LINEAR_RGB"],
+}
+
+
+def variants():
+    out = []
+    for t, tdefs in TRACKERS.items():
+        for i, idef in INTERPS.items():
+            for e, edefs in ENVS.items():
+                out.append((f"{t}__{i}__{e}", tdefs + [idef] + edefs))
+    return out
+
+
+FLOAT_LIT = re.compile(r"(?<![\w.])((?:\d+\.\d*|\.\d+)(?:[eE][+-]?\d+)?|\d+[eE][+-]?\d+)(?![\w.])")
+QUAL_REF = re.compile(r"\b(?:inout|out)\s+(\w+)\s+(\w+)")
+QUAL_IN = re.compile(r"\bin\s+(\w+)\s+(\w+)")
+MULTI_RANDOM = re.compile(r"\b(vec[234])\(((?:[^()]|\(\))*random\(\)(?:[^()]|\(\))*random\(\)(?:[^()]|\(\))*)\)")
+
+
+def strip_comments(text: str) -> str:
+    text = re.sub(r"/\*.*?\*/", lambda m: "\n" * m.group(0).count("\n"), text, flags=re.S)
+    return re.sub(r"//[^\n]*", "", text)
+
+
+def transform(text: str) -> str:
+    text = strip_comments(text)
+    lines = []
+    for ln in text.split("\n"):
+        s = ln.strip()
+        if s.startswith("--") or s.startswith("#version") or s.startswith("#extension"):
+            lines.append("")
+            continue
+        m = re.match(r'\s*#include\s+"([\w.]+)"', ln)
+        if m:
+            name = m.group(1)
+            lines.append(f'#include "{name}.inc"' if name != "VptHeader.glsl" else "")
+            continue
+        if s.startswith("#define"):
+            lines.append(FLOAT_LIT.sub(lambda m: m.group(1) + "f", ln))
+            continue
+        if s.startswith("#"):
+            lines.append(ln)
+            continue
+        ln = QUAL_REF.sub(r"\1& \2", ln)
+        ln = QUAL_IN.sub(r"\1 \2", ln)
+        ln = FLOAT_LIT.sub(lambda m: m.group(1) + "f", ln)
+        ln = re.sub(r"^uvec4 rngState", "thread_local uvec4 rngState", ln)
+        # GLSL evaluates constructor arguments left to right; C++ does so only in braced lists.
+        ln = MULTI_RANDOM.sub(lambda m: m.group(1) + "{" + m.group(2) + "}", ln)
+        lines.append(ln)
+    return "\n".join(lines)
+
+
+def generate() -> None:
+    os.makedirs(GEN, exist_ok=True)
+    for f in os.listdir(SHADERS):
+        if f.endswith(".glsl"):
+            with open(os.path.join(SHADERS, f), encoding="utf-8") as fh:
+                text = fh.read()
+            with open(os.path.join(GEN, f + ".inc"), "w") as fh:
+                fh.write(transform(text))
+
+
+def _run(cmd, verbose):
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"reference build failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr[-6000:]}")
+
+
+def build_tracer(force=False, verbose=False) -> str:
+    lib = os.path.join(OUT, "libref_vpt.so")
+    driver = os.path.join(HERE, "ref_driver.cpp")
+    shim = os.path.join(HERE, "ref_shim.h")
+    if not force and os.path.exists(lib) and os.path.getmtime(lib) > max(os.path.getmtime(driver),
+                                                                         os.path.getmtime(shim),
+                                                                         os.path.getmtime(__file__)):
+        return lib
+    generate()
+    objs, jobs = [], []
+    vs = variants()
+    flags = ["g++", "-O2", "-std=c++20", "-fPIC", "-fopenmp", "-ffp-contract=off", "-w", "-I", GEN, "-I", HERE]
+    for idx, (name, defs) in enumerate(vs):
+        obj = os.path.join(GEN, f"v_{name}.o")
+        objs.append(obj)
+        dflags = [f"-D{d}" for d in defs] + [f"-DREF_VARIANT_NS=v_{name}", "-DNUM_LIGHTS=0",
+                                             "-DCUSTOM_SEED_OFFSET=ref_seed_offset", "-DREF_VARIANT_BODY"]
+        jobs.append(flags + dflags + ["-c", driver, "-o", obj])
+    reg = os.path.join(GEN, "registry.cpp")
+    with open(reg, "w") as fh:
+        fh.write('#include "ref_shim.h"\n#include "ref_driver_api.h"\n')
+        for name, _ in vs:
+            fh.write(f"namespace glslref {{ namespace v_{name} {{ void run_pixel(int x, int y); }} }}\n")
+        fh.write("const RefVariant ref_variants[] = {\n")
+        for name, _ in vs:
+            fh.write(f'    {{"{name}", &glslref::v_{name}::run_pixel}},\n')
+        fh.write("};\nconst int ref_num_variants = %d;\n" % len(vs))
+    jobs.append(flags + ["-c", reg, "-o", os.path.join(GEN, "registry.o")])
+    jobs.append(flags + ["-DREF_DRIVER_COMMON", "-c", driver, "-o", os.path.join(GEN, "driver_common.o")])
+    objs += [os.path.join(GEN, "registry.o"), os.path.join(GEN, "driver_common.o")]
+    with ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:
+        list(ex.map(lambda c: _run(c, verbose), jobs))
+    _run(["g++", "-shared", "-fopenmp", "-o", lib] + objs, verbose)
+    return lib
+
+
+def build(force=False, verbose=False) -> None:
+    if not os.path.isdir(SHADERS):
+        return
+    os.makedirs(OUT, exist_ok=True)
+    build_tracer(force, verbose)
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose="-v" in sys.argv)

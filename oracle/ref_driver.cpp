@@ -1,0 +1,177 @@
+// ref_driver.cpp - runs the reference's tracer shader (Clouds.glsl compiled as C++) on the CPU
+// (TEST INFRASTRUCTURE ONLY).  Compiled once per define set (REF_VARIANT_BODY: one namespace per
+// variant holding the shader) and once as the common part (REF_DRIVER_COMMON: shared state and the
+// C entry points).  Per frame the driver sets FrameInfo and invokes the shader's main() for every
+// pixel, exactly like one compute dispatch; accImage keeps the reference's fp32 running mean.
+#include <stdint.h>
+#include <string.h>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+#include "ref_driver_api.h"
+
+#ifdef REF_VARIANT_BODY
+namespace glslref {
+namespace REF_VARIANT_NS {
+static Parameters& parameters = g_ref.params;
+static FrameInfo& frameInfo = g_ref.frame;
+static sampler3D& gridImage = g_ref.grid;
+static sampler3D& superVoxelGridImage = g_ref.sv;
+static usampler3D& superVoxelGridOccupancyImage = g_ref.svocc;
+static sampler2D& environmentMapTexture = g_ref.env;
+static sampler2D& environmentMapOctahedralTexture = g_ref.envocta;
+static uimage3D& occupancyGridImage = g_ref.occ;
+static image2D& resultImage = g_ref.result;
+static image2D& accImage = g_ref.acc;
+#define gl_GlobalInvocationID gl_global_invocation_id
+#define main glsl_main
+#include "Clouds.glsl.inc"
+#undef main
+void run_pixel(int x, int y) {
+    gl_global_invocation_id = uvec3((uint)x, (uint)y, 0u);
+    glsl_main();
+}
+}  // namespace REF_VARIANT_NS
+}  // namespace glslref
+#endif
+
+#ifdef REF_DRIVER_COMMON
+namespace glslref {
+RefState g_ref;
+thread_local uvec3 gl_global_invocation_id;
+uint ref_seed_offset = 0;
+}  // namespace glslref
+
+using namespace glslref;
+
+extern "C" {
+
+typedef struct RefScene {
+    float inv_view_proj[16];
+    int width, height;
+    uint32_t frame_start, num_frames, seed_offset;
+    float box_min[3], box_max[3];
+    const float* grid;
+    int nx, ny, nz;
+    int linear_filter;
+    float voxel_value_min, voxel_value_max;
+    float extinction[3], albedo[3], g;
+    float sun_dir[3], sun_intensity[3], env_intensity[3];
+    const float* sv_data;
+    int svx, svy, svz, sv_size;
+    const uint8_t* occupancy;
+    int ox, oy, oz, occ_block;
+    const float* env_rgba;
+    int env_w, env_h;
+    const float* env_pyramid;
+    int env_levels;
+    int is_env_black;
+    float far_dist;
+} RefScene;
+
+int ref_variant_count(void) { return ref_num_variants; }
+const char* ref_variant_name(int i) { return (i >= 0 && i < ref_num_variants) ? ref_variants[i].name : ""; }
+int ref_find_variant(const char* name) {
+    for (int i = 0; i < ref_num_variants; i++)
+        if (strcmp(ref_variants[i].name, name) == 0) return i;
+    return -1;
+}
+
+// Renders num_frames frames from a cleared accumulation image; out_rgba gets accImage (W*H*4).
+int ref_render(int variant, const RefScene* s, float* out_rgba, int threads) {
+    if (variant < 0 || variant >= ref_num_variants || !s || !out_rgba) return 1;
+    Parameters& p = g_ref.params;
+    memset(&p, 0, sizeof(p));
+    for (int c = 0; c < 4; c++)
+        p.inverseViewProjMatrix.c[c] = vec4(s->inv_view_proj[c * 4 + 0], s->inv_view_proj[c * 4 + 1],
+                                            s->inv_view_proj[c * 4 + 2], s->inv_view_proj[c * 4 + 3]);
+    p.boxMin = vec3(s->box_min[0], s->box_min[1], s->box_min[2]);
+    p.boxMax = vec3(s->box_max[0], s->box_max[1], s->box_max[2]);
+    p.voxelValueMin = s->voxel_value_min;
+    p.voxelValueMax = s->voxel_value_max;
+    p.gridMin = vec3(0.0f);
+    p.gridMax = vec3(1.0f);
+    p.extinction = vec3(s->extinction[0], s->extinction[1], s->extinction[2]);
+    p.scatteringAlbedo = vec3(s->albedo[0], s->albedo[1], s->albedo[2]);
+    p.phaseG = s->g;
+    p.sunDirection = vec3(s->sun_dir[0], s->sun_dir[1], s->sun_dir[2]);
+    p.sunIntensity = vec3(s->sun_intensity[0], s->sun_intensity[1], s->sun_intensity[2]);
+    p.environmentMapIntensityFactor = vec3(s->env_intensity[0], s->env_intensity[1], s->env_intensity[2]);
+    p.numFeatureMapSamplesPerFrame = 1;
+    p.useLinearRGB = 1;
+    if (s->occupancy) {
+        p.superVoxelSize = ivec3(s->occ_block);
+        p.superVoxelGridSize = ivec3(s->ox, s->oy, s->oz);
+    } else {
+        p.superVoxelSize = ivec3(s->sv_size);
+        p.superVoxelGridSize = ivec3(s->svx, s->svy, s->svz);
+    }
+    p.gridResolution = ivec3(s->nx, s->ny, s->nz);
+    p.isEnvMapBlack = (uint)s->is_env_black;
+    p.voxelTexelSize = vec3(1.0f / float(s->nx - 1), 1.0f / float(s->ny - 1), 1.0f / float(s->nz - 1));
+    p.farDistance = s->far_dist;
+
+    g_ref.grid.data = s->grid;
+    g_ref.grid.w = s->nx;
+    g_ref.grid.h = s->ny;
+    g_ref.grid.d = s->nz;
+    g_ref.grid.channels = 1;
+    g_ref.grid.filter = s->linear_filter ? FILTER_LINEAR : FILTER_NEAREST;
+    g_ref.sv.data = s->sv_data;
+    g_ref.sv.w = s->svx;
+    g_ref.sv.h = s->svy;
+    g_ref.sv.d = s->svz;
+    g_ref.sv.channels = 2;
+    g_ref.sv.filter = FILTER_NEAREST;
+    g_ref.occ.data = s->occupancy;
+    g_ref.occ.w = s->ox;
+    g_ref.occ.h = s->oy;
+    g_ref.occ.d = s->oz;
+    g_ref.env.levels.clear();
+    g_ref.envocta.levels.clear();
+    if (s->env_rgba) {
+        g_ref.env.levels.push_back(s->env_rgba);
+        g_ref.env.w = s->env_w;
+        g_ref.env.h = s->env_h;
+        g_ref.env.channels = 4;
+        g_ref.env.filter = FILTER_LINEAR;
+        g_ref.env.address = ADDRESS_REPEAT;
+        size_t off = 0;
+        for (int l = 0; l < s->env_levels; l++) {
+            g_ref.envocta.levels.push_back(s->env_pyramid + off);
+            size_t r = (size_t)1 << (s->env_levels - l);
+            off += r * r;
+        }
+        g_ref.envocta.w = g_ref.envocta.h = 1 << s->env_levels;
+        g_ref.envocta.channels = 1;
+        g_ref.envocta.address = ADDRESS_CLAMP_TO_EDGE;
+    }
+    std::vector<float> result((size_t)s->width * s->height * 4, 0.0f), acc((size_t)s->width * s->height * 4, 0.0f);
+    g_ref.result.data = result.data();
+    g_ref.result.w = s->width;
+    g_ref.result.h = s->height;
+    g_ref.acc.data = acc.data();
+    g_ref.acc.w = s->width;
+    g_ref.acc.h = s->height;
+    ref_seed_offset = s->seed_offset;
+    int nt = threads;
+#ifdef _OPENMP
+    if (nt <= 0) nt = omp_get_max_threads();
+#else
+    nt = 1;
+#endif
+    void (*run)(int, int) = ref_variants[variant].run_pixel;
+    for (uint32_t f = 0; f < s->num_frames; f++) {
+        g_ref.frame.frameCount = s->frame_start + f;
+        g_ref.frame.globalFrameNumber = s->frame_start + f;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nt)
+        for (int y = 0; y < s->height; y++)
+            for (int x = 0; x < s->width; x++) run(x, y);
+    }
+    memcpy(out_rgba, acc.data(), acc.size() * sizeof(float));
+    return 0;
+}
+
+}  // extern "C"
+#endif

@@ -1,0 +1,27 @@
+// ref_driver_api.h - state shared by the reference-shader variants (TEST INFRASTRUCTURE ONLY).
+#pragma once
+#include "ref_shim.h"
+
+namespace glslref {
+struct RefState {
+    Parameters params;
+    FrameInfo frame;
+    sampler3D grid;       // gridImage
+    sampler3D sv;         // superVoxelGridImage (RG32F)
+    usampler3D svocc;     // superVoxelGridOccupancyImage
+    sampler2D env;        // environmentMapTexture
+    sampler2D envocta;    // environmentMapOctahedralTexture (mip chain)
+    uimage3D occ;         // occupancyGridImage
+    image2D result, acc;  // resultImage, accImage
+};
+extern RefState g_ref;
+extern thread_local uvec3 gl_global_invocation_id;
+extern uint ref_seed_offset;
+}  // namespace glslref
+
+struct RefVariant {
+    const char* name;
+    void (*run_pixel)(int x, int y);
+};
+extern const RefVariant ref_variants[];
+extern const int ref_num_variants;

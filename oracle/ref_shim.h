@@ -136,13 +136,17 @@ struct uvec2 {
     uvec2() : x(0), y(0) {}
     uvec2(uint a, uint b) : x(a), y(b) {}
 };
+struct USw2 {
+    uint v[3];
+    operator uvec2() const { return uvec2(v[0], v[1]); }
+};
 struct uvec3 {
     union {
         struct { uint x, y, z; };
+        USw2 xy;
     };
     uvec3() : x(0), y(0), z(0) {}
     uvec3(uint a, uint b, uint c) : x(a), y(b), z(c) {}
-    uvec2 xy_() const { return uvec2(x, y); }
 };
 struct uvec4 {
     uint x, y, z, w;
@@ -194,6 +198,7 @@ inline ivec2 operator+(const ivec2& a, const ivec2& b) { return ivec2(a.x + b.x,
 inline ivec2 operator*(const ivec2& a, int s) { return ivec2(a.x * s, a.y * s); }
 inline vec3 operator-(const vec3& a) { return vec3(-a.x, -a.y, -a.z); }
 inline vec2 operator-(const vec2& a) { return vec2(-a.x, -a.y); }
+inline vec2 operator+(const USw2& a, const vec2& b) { return vec2(uvec2(a)) + b; }
 inline vec3& operator+=(vec3& a, const vec3& b) { return a = a + b; }
 inline vec3& operator-=(vec3& a, const vec3& b) { return a = a - b; }
 inline vec3& operator*=(vec3& a, const vec3& b) { return a = a * b; }
@@ -251,6 +256,10 @@ inline float max(float a, float b) { return a < b ? b : a; }
 inline int min(int a, int b) { return b < a ? b : a; }
 inline int max(int a, int b) { return a < b ? b : a; }
 inline uint min(uint a, uint b) { return b < a ? b : a; }
+inline float max(int a, float b) { return max((float)a, b); }
+inline float max(float a, int b) { return max(a, (float)b); }
+inline float min(int a, float b) { return min((float)a, b); }
+inline float min(float a, int b) { return min(a, (float)b); }
 inline vec3 min(const vec3& a, const vec3& b) { return vec3(min(a.x, b.x), min(a.y, b.y), min(a.z, b.z)); }
 inline vec3 max(const vec3& a, const vec3& b) { return vec3(max(a.x, b.x), max(a.y, b.y), max(a.z, b.z)); }
 inline vec3 max(const vec3& a, float b) { return vec3(max(a.x, b), max(a.y, b), max(a.z, b)); }

@@ -1,0 +1,94 @@
+"""Generates tests/golden/ref_paths.npz from the reference's own tracer shaders
+(Data/Shaders/VPT/Clouds.glsl and the tracker includes, compiled for the CPU by oracle/ref_build.py).
+
+For every case the fixture stores the inputs (grid, scene parameters, camera matrix) and the
+reference's output: the radiance of each camera path of frame 0 (1 spp; accImage after one frame is
+the path radiance itself) and the reference's fp32 running mean after 8 frames.
+
+Run in a container that has the reference tree:  python tests/golden/make_golden.py
+"""
+import json
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+from oracle import bridge, ref_build  # noqa: E402
+from tests.harness import SceneSpec, camera_inv_view_proj, cloud_block, reference_scene  # noqa: E402
+
+W = H = 32
+
+
+def env_image():
+    rng = np.random.default_rng(9)
+    rgba = np.ones((32, 64, 4), np.float32)
+    rgba[..., :3] = 0.2 + rng.random((32, 64, 3)).astype(np.float32) * 0.05
+    rgba[5:8, 20:24, :3] = 40.0
+    return rgba
+
+
+def cases():
+    fbm = bridge.fbm(24, 2, base_frequency=3.0, contrast=3.5)
+    base = dict(extinction=120.0, albedo=0.99, g=0.85, width=W, height=H, env="default", linear_rgb=1,
+                cam_pos=(0.3, 0.4, 1.4), max_grid_extent=0.5)
+    out = {
+        # the reference test suite's fixtures (test/VolumetricPathTracingTestData.cpp) and settings
+        "block1_delta": SceneSpec(grid=cloud_block(1, 1, 1), mode="delta", width=W, height=H),
+        "block1_ratio": SceneSpec(grid=cloud_block(1, 1, 1), mode="ratio", width=W, height=H),
+        "block8_decomposition_nearest": SceneSpec(grid=cloud_block(8, 8, 8), mode="decomposition",
+                                                  interp="nearest", width=W, height=H),
+        "block8b_nee": SceneSpec(grid=cloud_block(8, 8, 8, empty_boundary=True), mode="nee", width=W, height=H),
+    }
+    for name, kw in {"delta_stochastic": dict(mode="delta"), "delta_nearest": dict(mode="delta", interp="nearest"),
+                     "delta_trilinear": dict(mode="delta", interp="trilinear"), "ratio": dict(mode="ratio"),
+                     "nee": dict(mode="nee"), "nee_ess": dict(mode="nee", use_ess=True),
+                     "decomposition": dict(mode="decomposition"), "rrt": dict(mode="rrt"),
+                     "nee_env_image": dict(mode="nee", env="image", env_rgba=env_image()),
+                     "delta_black": dict(mode="delta", env="black"),
+                     "delta_single_color": dict(mode="delta", env="single")}.items():
+        kw2 = dict(base)
+        kw2.update(kw)
+        out["fbm_" + name] = SceneSpec(grid=fbm, **kw2)
+    return out
+
+
+FIELDS = ["mode", "interp", "extinction", "albedo", "g", "width", "height", "seed_offset", "env", "linear_rgb",
+          "sun_dir", "sun_intensity", "cam_pos", "cam_target", "fovy", "near", "far", "max_grid_extent", "use_ess",
+          "env_intensity", "max_bounces"]
+
+
+def main():
+    ref_build.build()
+    data = {}
+    meta = {}
+    grids = []
+    for name, sp in cases().items():
+        inv = camera_inv_view_proj(sp)
+        sc, variant = reference_scene(sp, 1, inv=inv)
+        paths = sc.render(variant)[..., :3].copy()
+        sc.set("num_frames", 8)
+        mean8 = sc.render(variant)[..., :3].copy()
+        g = np.ascontiguousarray(sp.grid, np.float32)
+        key = next((k for k, a in grids if a.shape == g.shape and np.array_equal(a, g)), None)
+        if key is None:
+            key = f"grid{len(grids)}"
+            grids.append((key, g))
+            data[key] = g
+        data[name + "__paths"] = paths
+        data[name + "__mean8"] = mean8
+        data[name + "__inv_view_proj"] = np.array(inv, np.float32)
+        if sp.env == "image":
+            data[name + "__env_rgba"] = np.ascontiguousarray(sp.env_rgba, np.float32)
+        meta[name] = {"variant": variant, "grid": key, **{f: (list(getattr(sp, f)) if isinstance(getattr(sp, f), tuple)
+                                                 else getattr(sp, f)) for f in FIELDS}}
+        print(name, variant, float(paths.mean()))
+    out = os.path.join(os.path.dirname(os.path.abspath(__file__)), "ref_paths.npz")
+    np.savez_compressed(out, meta=json.dumps(meta), **data)
+    print("wrote", out, os.path.getsize(out), "bytes")
+
+
+if __name__ == "__main__":
+    main()

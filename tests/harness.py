@@ -209,3 +209,75 @@ def z_scores(sum_a, sq_a, n_a, sum_b, sq_b, n_b):
     se = np.sqrt(va / n_a + vb / n_b)
     z = np.where(se > 0, (ma - mb) / np.where(se > 0, se, 1.0), np.where(np.abs(ma - mb) > 1e-7, np.inf, 0.0))
     return z
+
+
+def reference_scene(sp: SceneSpec, frames: int, frame_start: int = 0, inv=None):
+    """The same scene for the reference's own shader code compiled for the CPU (oracle/_ref)."""
+    from oracle import ref_bridge
+
+    if inv is None:
+        inv = camera_inv_view_proj(sp)
+    g = np.ascontiguousarray(sp.grid, np.float32)
+    nz, ny, nx = g.shape
+    vmin, vmax = bridge.minmax(g)
+    dens = bridge.normalize(g, vmin, vmax)
+    bmin, bmax = bridge.grid_bounds(nx, ny, nz, sp.max_grid_extent)
+    d = np.array(sp.sun_dir, np.float32)
+    dl = np.sqrt(np.float32(np.float32(d[0] * d[0]) + np.float32(d[1] * d[1])) + np.float32(d[2] * d[2]),
+                 dtype=np.float32)
+    sc = ref_bridge.Scene(
+        inv_view_proj=list(inv), width=sp.width, height=sp.height, frame_start=frame_start, num_frames=frames,
+        seed_offset=sp.seed_offset, box_min=bmin, box_max=bmax, grid=g, nx=nx, ny=ny, nz=nz,
+        linear_filter=1 if sp.interp == "trilinear" else 0, voxel_value_min=vmin, voxel_value_max=vmax,
+        extinction=[sp.extinction] * 3, albedo=[sp.albedo] * 3, g=sp.g,
+        sun_dir=[float(np.float32(d[i] / dl)) for i in range(3)], sun_intensity=sp.sun_intensity,
+        env_intensity=sp.env_intensity, is_env_black=1 if sp.env == "black" else 0, far_dist=sp.far)
+    if sp.mode in ("decomposition", "rrt"):
+        svs = supervoxel_size(nx, ny, nz)
+        halo = 0 if sp.interp == "nearest" else 1
+        mn, mx, avg, occ = bridge.supervoxel_stats(dens, svs, halo)
+        data = bridge.rrt_params(mn, mx, avg, float(np.float32(sp.extinction)), svs) if sp.mode == "rrt" else \
+            np.stack([mn, mx], axis=1).reshape(-1).copy()
+        sc.set("sv_data", data)
+        for k, v in zip(("svx", "svy", "svz", "sv_size"), (-(-nx // svs), -(-ny // svs), -(-nz // svs), svs)):
+            sc.set(k, v)
+    if sp.use_ess:
+        halo = 0 if sp.interp == "nearest" else 1
+        occ = bridge.occupancy(dens, 8, halo, 0.0) if not getattr(sp, "ess_ref_compat", False) else None
+        sc.set("occupancy", occ)
+        for k, v in zip(("ox", "oy", "oz", "occ_block"), (-(-nx // 8), -(-ny // 8), -(-nz // 8), 8)):
+            sc.set(k, v)
+    if sp.env == "image":
+        rgba = np.ascontiguousarray(sp.env_rgba, np.float32)
+        sc.set("env_rgba", rgba)
+        sc.set("env_w", rgba.shape[1])
+        sc.set("env_h", rgba.shape[0])
+        sc.set("env_levels", 12)
+        sc.set("env_pyramid", bridge.env_pyramid(rgba, 12))
+    tracker = {"delta": "delta", "ratio": "ratio", "decomposition": "decomposition", "rrt": "rrt",
+               "nee": "nee_ess" if sp.use_ess else "nee"}[sp.mode]
+    env = {"default": "default", "black": "black", "single": "single", "image": "image"}[sp.env]
+    colour = "linear" if (sp.linear_rgb or env != "default") else "srgb"
+    return sc, f"{tracker}__{sp.interp}__{env}__{colour}"
+
+
+GOLDEN = __import__("os").path.join(__import__("os").path.dirname(__import__("os").path.abspath(__file__)),
+                                    "golden", "ref_paths.npz")
+
+
+def golden_cases():
+    """Cases of tests/golden/ref_paths.npz (outputs of the reference's own shader code):
+    name -> (SceneSpec, inv_view_proj, paths [H, W, 3], mean8 [H, W, 3])."""
+    import json
+
+    z = np.load(GOLDEN)
+    meta = json.loads(str(z["meta"]))
+    out = {}
+    for name, m in meta.items():
+        kw = {k: (tuple(v) if isinstance(v, list) else v) for k, v in m.items() if k not in ("variant", "grid")}
+        kw["grid"] = z[m["grid"]]
+        if name + "__env_rgba" in z:
+            kw["env_rgba"] = z[name + "__env_rgba"]
+        sp = SceneSpec(**kw)
+        out[name] = (sp, list(z[name + "__inv_view_proj"]), z[name + "__paths"], z[name + "__mean8"])
+    return out
