@@ -44,7 +44,7 @@ def cases():
     }
     for name, kw in {"delta_stochastic": dict(mode="delta"), "delta_nearest": dict(mode="delta", interp="nearest"),
                      "delta_trilinear": dict(mode="delta", interp="trilinear"), "ratio": dict(mode="ratio"),
-                     "nee": dict(mode="nee"), "nee_ess": dict(mode="nee", use_ess=True),
+                     "nee": dict(mode="nee"), "nee_ess": dict(mode="nee", use_ess=True, ess_ref_compat=True),
                      "decomposition": dict(mode="decomposition"), "rrt": dict(mode="rrt"),
                      "nee_env_image": dict(mode="nee", env="image", env_rgba=env_image()),
                      "delta_black": dict(mode="delta", env="black"),
@@ -57,7 +57,7 @@ def cases():
 
 FIELDS = ["mode", "interp", "extinction", "albedo", "g", "width", "height", "seed_offset", "env", "linear_rgb",
           "sun_dir", "sun_intensity", "cam_pos", "cam_target", "fovy", "near", "far", "max_grid_extent", "use_ess",
-          "env_intensity", "max_bounces"]
+          "env_intensity", "max_bounces", "ess_ref_compat"]
 
 
 def main():

@@ -66,7 +66,7 @@ class SceneSpec:
                  sun_dir=(0.5826, 0.7660, 0.2717), sun_intensity=(2.6, 2.6 * 0.961538462, 2.6 * 0.884615385),
                  sky_color=(1.0, 1.0, 1.0), cam_pos=(0.0, 0.0, 0.8), cam_target=(0.0, 0.0, 0.0),
                  fovy=2.0 * math.atan(0.5), near=0.01, far=100.0, max_grid_extent=0.25, env_rgba=None,
-                 use_ess=False, env_intensity=(1.0, 1.0, 1.0)):
+                 use_ess=False, env_intensity=(1.0, 1.0, 1.0), ess_ref_compat=False):
         self.__dict__.update(locals())
         del self.__dict__["self"]
 
@@ -179,7 +179,11 @@ def oracle_scene(core, sp: SceneSpec, frames: int, frame_count: int = 0) -> brid
         sc.set("sv_world", [float(v) for v in svw])
         halo = 0 if sp.interp == "nearest" else 1
         if sp.mode == "nee":
-            sc.set("occupancy", bridge.occupancy(dens, 8, halo, 0.0))
+            if sp.ess_ref_compat:  # the reference marks every block occupied (ComputeOccupancyGrid.glsl:108-109)
+                sc.set("occupancy", np.ones(svx * svy * svz, np.uint8))
+                sc.set("ess_ref_compat", 1)
+            else:
+                sc.set("occupancy", bridge.occupancy(dens, 8, halo, 0.0))
         else:
             mn, mx, avg, occ = bridge.supervoxel_stats(dens, svs, halo)
             if sp.mode == "rrt":
@@ -242,9 +246,8 @@ def reference_scene(sp: SceneSpec, frames: int, frame_start: int = 0, inv=None):
         for k, v in zip(("svx", "svy", "svz", "sv_size"), (-(-nx // svs), -(-ny // svs), -(-nz // svs), svs)):
             sc.set(k, v)
     if sp.use_ess:
-        halo = 0 if sp.interp == "nearest" else 1
-        occ = bridge.occupancy(dens, 8, halo, 0.0) if not getattr(sp, "ess_ref_compat", False) else None
-        sc.set("occupancy", occ)
+        # the reference's occupancy pass marks every block occupied (ComputeOccupancyGrid.glsl:108-109)
+        sc.set("occupancy", np.ones((-(-nx // 8)) * (-(-ny // 8)) * (-(-nz // 8)), np.uint8))
         for k, v in zip(("ox", "oy", "oz", "occ_block"), (-(-nx // 8), -(-ny // 8), -(-nz // 8), 8)):
             sc.set(k, v)
     if sp.env == "image":

@@ -13,10 +13,8 @@ CASES = golden_cases()
 @pytest.mark.parametrize("name", sorted(CASES))
 def test_oracle_matches_reference_shader_paths(name):
     sp, inv, paths, mean8 = CASES[name]
-    sc = oracle_scene(None, sp, 1)
+    sc = oracle_scene(None, sp, 1)  # nee_ess runs with ess_ref_compat (the reference's behaviour)
     sc.set("inv_view_proj", inv)
-    if sp.use_ess:
-        sc.set("ess_ref_compat", 1)  # the reference's skipping shadow loop, as compiled
     ys, xs = np.mgrid[0:sp.height, 0:sp.width]
     got = sc.trace_paths(xs.reshape(-1), ys.reshape(-1), np.zeros(xs.size, np.uint32)).reshape(paths.shape)
     agree = path_agreement(got, paths, rtol=1e-5, atol=1e-6)
