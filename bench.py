@@ -234,6 +234,22 @@ def run_ours(args):
                              "lookups_per_s": s2["density_lookups"] * world / (ms / 1e3),
                              "ms_per_step": ms / 2, "spp_per_step": TRACKER_SPP}
 
+    # schedule comparison for delta tracking (the reason the refill schedule is the default)
+    schedules = {}
+    vpt.set_vpt_mode_from_name("Delta Tracking")
+    for sched, label in ((0, "tiles"), (1, "persistent_warp_batches"), (2, "per_lane_refill")):
+        _lib.check(lib.vpt_set_option(ctx, b"schedule", float(sched)), "schedule", ctx)
+        vpt.render_frame(img, 1)
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        _lib.check(lib.vpt_render_frames(ctx, TRACKER_SPP, ctypes_stream), "render", ctx)
+        e1.record(stream)
+        barrier()
+        ms = max_over_ranks(e0.elapsed_time(e1))
+        schedules[label] = RES * RES * TRACKER_SPP * world / (ms / 1e3)
+    _lib.check(lib.vpt_set_option(ctx, b"schedule", 2.0), "schedule", ctx)
+
     # end to end through the public API: host grid -> device, render, result -> host
     vpt.set_vpt_mode_from_name("Delta Tracking")
     grid_host = torch.empty((GRID, GRID, GRID), dtype=torch.float32).pin_memory()
@@ -266,7 +282,7 @@ def run_ours(args):
                          "note": f"algorithmic bytes = density lookups x {BYTES_PER_LOOKUP} B sector; peak {peak_kind}"},
             "lookups_per_s": lookups / (ms_total / 1e3) * world,
             "lookups_per_path": lookups / max(1, st["paths"]),
-            "per_tracker": per_tracker, "e2e": e2e, "gpu_launches": int(launches), "clocks": clock_info,
+            "per_tracker": per_tracker, "schedules_delta": schedules, "e2e": e2e, "gpu_launches": int(launches), "clocks": clock_info,
         }
         if cpu is not None:
             line["cpu_baseline"] = cpu

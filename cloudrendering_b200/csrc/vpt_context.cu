@@ -136,7 +136,7 @@ struct VptContext {
     float pending_voxel_size[3] = {1.0f, 1.0f, 1.0f};  // spacing for the next grid
     int use_ess = 0;
     int ess_ref_compat = 0;
-    int schedule = vpt::kSchedulePersistent;
+    int schedule = vpt::kScheduleRefill;
     int persistent_blocks_per_sm = 0;  // 0 = occupancy calculator (one resident wave)
     uint32_t max_steps = vpt::kMaxStepsPerPath;
 
@@ -878,7 +878,7 @@ VptStatus vpt_render_frames(VptContext* ctx, int frames, void* stream) {
         P.svz = ctx->svz;
     }
     int pb = 0;  // 0: persistent grid sized by the occupancy calculator
-    if (ctx->schedule == vpt::kSchedulePersistent && ctx->persistent_blocks_per_sm > 0) {
+    if (ctx->schedule != vpt::kScheduleTiles && ctx->persistent_blocks_per_sm > 0) {
         pb = ctx->persistent_blocks_per_sm * ctx->num_sms;
     }
     VPT_CHECK_CUDA(ctx, vpt::launch_trace(P, tracker, ctx->use_ess, ctx->schedule, P.feat ? 1 : 0, pb, s));
@@ -1078,7 +1078,9 @@ VptStatus vpt_set_option(VptContext* ctx, const char* key, double value) {
     if (!key) return VPT_ERR_ARG;
     std::string k(key);
     if (k == "schedule") {
-        ctx->schedule = int(value) ? vpt::kSchedulePersistent : vpt::kScheduleTiles;
+        int v = int(value);
+        if (v < 0 || v > 2) return fail(ctx, VPT_ERR_ARG, "schedule must be 0 (tiles), 1 (persistent) or 2 (refill)");
+        ctx->schedule = v;
     } else if (k == "persistent_blocks_per_sm") {
         if (value < 0 || value > 64) return fail(ctx, VPT_ERR_ARG, "persistent_blocks_per_sm out of range");
         ctx->persistent_blocks_per_sm = int(value);

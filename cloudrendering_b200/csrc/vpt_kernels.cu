@@ -170,15 +170,252 @@ __global__ void __launch_bounds__(kTraceBlock) trace_persistent_kernel(const __g
     flush_counters(P, paths, lookups, guard_hit);
 }
 
+
+// ---------------------------------------------------------------------------------------------
+// Per-lane path refill schedule (delta, ratio and NEE trackers).
+//
+// Each loop iteration advances every live lane by ONE tentative collision.  A lane whose path ends
+// (escape, absorption, bounce cap) writes the film and takes the next path id at the top of the
+// next iteration, so the 32 lanes of a warp keep executing the same step code instead of waiting
+// for the warp's longest path.  NEE shadow rays are a second mode of the same step: the free-path
+// sample and the density lookup are shared code for primary and shadow lanes.  Random numbers are
+// drawn in exactly the order of the recursive trackers (vpt_trackers.cuh), so every path is the same
+// path.  Path ids come from a global counter in warp batches of 64 (one atomic per 64 paths).
+enum : int { kModePrimary = 0, kModeShadow = 1 };
+constexpr int kRefillBatch = 64;
+
+template <int TRACKER>
+VPT_DEV void refill_finish(const TraceParams& P, size_t pix, F3 L, bool& has) {
+    atomicAdd(P.film + pix * 3 + 0, (double)L.x);
+    atomicAdd(P.film + pix * 3 + 1, (double)L.y);
+    atomicAdd(P.film + pix * 3 + 2, (double)L.z);
+    if (P.film_sq) {
+        atomicAdd(P.film_sq + pix * 3 + 0, (double)L.x * (double)L.x);
+        atomicAdd(P.film_sq + pix * 3 + 1, (double)L.y * (double)L.y);
+        atomicAdd(P.film_sq + pix * 3 + 2, (double)L.z * (double)L.z);
+    }
+    has = false;
+}
+
+// Shadow ray done: add the light sample (f = pdf_phase / pdf_light * T, NextEventTracking.glsl:367-369)
+// and resume the primary path at the scatter point with the sampled direction.
+VPT_DEV void end_shadow(const TraceParams& P, F3& color, F3& x, F3& w, float& d, F3 xp, F3 nw, float dp,
+                        float weight, float ts, int& mode) {
+    const float f = weight * ts;
+    const F3 l = sky_and_sun(P, w);
+    color = color + f3(f * l.x, f * l.y, f * l.z);
+    x = xp;
+    w = nw;
+    d = dp;
+    mode = kModePrimary;
+    float tmin, tmax;
+    if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
+        x = x + w * tmin;
+        d = tmax - tmin;
+    }
+}
+
+template <int TRACKER, int INTERP>
+__global__ void __launch_bounds__(kTraceBlock) trace_refill_kernel(const __grid_constant__ TraceParams P, uint64_t total) {
+    DenseSampler<INTERP> sample{P};
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const unsigned lt_mask = (1u << lane) - 1u;
+    const F3 zero = f3(0.0f, 0.0f, 0.0f);
+
+    // warp-uniform local batch of path ids
+    unsigned long long q_base = 0;
+    int q_left = 0;
+
+    bool has = false, exhausted = false;
+    Rng rng;
+    F3 x = zero, w = zero, color = zero, xp = zero, nw = zero;
+    float d = 0.0f, dp = 0.0f, trans = 1.0f, ts = 1.0f, weight = 0.0f;
+    int mode = kModePrimary, bounces = 0;
+    bool ev = false;
+    uint32_t steps = 0;
+    size_t pix = 0;
+    uint32_t lookups = 0, paths = 0;
+    bool guard_hit = false;
+
+    while (true) {
+        // ---- refill lanes without a path ----
+        const bool need = !has && !exhausted;
+        const unsigned m = __ballot_sync(FULL, need);
+        if (m) {
+            const int n = __popc(m);
+            const int r = __popc(m & lt_mask);
+            unsigned long long fresh = 0;
+            if (n > q_left) {
+                unsigned long long b = 0;
+                if (lane == 0) b = atomicAdd(reinterpret_cast<unsigned long long*>(P.work_counter),
+                                             (unsigned long long)kRefillBatch);
+                fresh = __shfl_sync(FULL, b, 0);
+            }
+            if (need) {
+                unsigned long long p = r < q_left ? q_base + (unsigned long long)r
+                                                  : fresh + (unsigned long long)(r - q_left);
+                uint32_t frame;
+                int px, py;
+                if (p >= total) {
+                    exhausted = true;
+                } else if (decode_path(P, p, frame, px, py)) {
+                    const uint32_t w_u = (uint32_t)P.width, h_u = (uint32_t)P.height;
+                    uint32_t seed = (P.global_frame + frame) * w_u * h_u + (uint32_t)px + (uint32_t)py * w_u;
+                    seed += P.seed_offset;
+                    rng = rng_init(seed);
+                    float rx = rng_next(rng);
+                    float ry = rng_next(rng);
+                    float sx = (2.0f * ((float)px + rx)) / (float)P.width - 1.0f;
+                    float sy = (2.0f * ((float)py + ry)) / (float)P.height - 1.0f;
+                    camera_ray(P, sx, sy, x, w);
+                    pix = (size_t)py * P.width + px;
+                    paths++;
+                    steps = 0;
+                    bounces = 0;
+                    trans = 1.0f;
+                    color = zero;
+                    ev = false;
+                    mode = kModePrimary;
+                    float tmin, tmax;
+                    has = true;
+                    if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
+                        x = x + w * tmin;
+                        d = tmax - tmin;
+                    } else {
+                        F3 L = sky_and_sun(P, w);
+                        refill_finish<TRACKER>(P, pix, L, has);
+                    }
+                }
+            }
+            if (n > q_left) {
+                q_base = fresh + (unsigned long long)(n - q_left);
+                q_left = kRefillBatch - (n - q_left);
+            } else {
+                q_base += (unsigned long long)n;
+                q_left -= n;
+            }
+        }
+        if (!__any_sync(FULL, has)) {
+            if (__all_sync(FULL, exhausted)) break;
+            continue;
+        }
+        if (!has) continue;
+
+        // ---- one tentative collision ----
+        if (++steps > P.max_steps) {
+            guard_hit = true;
+            refill_finish<TRACKER>(P, pix, TRACKER == kNextEvent ? color : zero, has);
+            continue;
+        }
+        const float t = free_path(rng, P.inv_extinction);
+        const bool escape = t > d;
+        float density = 0.0f;
+        if (!escape) {
+            F3 xn = x + w * t;
+            density = sample(xn, rng);
+            lookups++;
+            x = xn;
+        }
+        if (TRACKER == kNextEvent && mode == kModeShadow) {
+            if (!escape) {
+                ts *= 1.0f - density;
+                d -= t;
+                continue;
+            }
+            end_shadow(P, color, x, w, d, xp, nw, dp, weight, ts, mode);
+            continue;
+        }
+        if (escape) {
+            F3 L;
+            if (TRACKER == kNextEvent) L = ev ? color : color + sky_and_sun(P, w);
+            else if (TRACKER == kRatio) L = sky_and_sun(P, w) * trans;
+            else L = sky_and_sun(P, w);
+            refill_finish<TRACKER>(P, pix, L, has);
+            continue;
+        }
+        const float xi = rng_next(rng);
+        if (TRACKER != kRatio && xi < P.absorb_albedo * density) {
+            refill_finish<TRACKER>(P, pix, TRACKER == kNextEvent ? color : zero, has);
+            continue;
+        }
+        if (xi < density) {
+            if (P.max_bounces > 0 && ++bounces > P.max_bounces) {
+                refill_finish<TRACKER>(P, pix, TRACKER == kNextEvent ? color : zero, has);
+                continue;
+            }
+            float tmin, tmax;
+            if (TRACKER == kNextEvent) {
+                nw = sample_phase(rng, P.g, w);
+                ev = true;
+                float pdf_light;
+                F3 dir = importance_sample_sky(P, rng, pdf_light);
+                weight = evaluate_phase(P.g, w, dir) / pdf_light;
+                xp = x;
+                dp = d;
+                w = dir;
+                ts = 1.0f;
+                mode = kModeShadow;
+                if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
+                    x = x + w * tmin;
+                    d = tmax - tmin;
+                } else {
+                    // no shadow steps (and no random numbers), like calculateTransmittance
+                    end_shadow(P, color, x, w, d, xp, nw, dp, weight, ts, mode);
+                }
+                continue;
+            }
+            if (TRACKER == kRatio) {
+                float pa = P.absorb_albedo * density;
+                float ps = P.albedo * density;
+                trans *= 1.0f - pa / (pa + ps);
+            }
+            w = sample_phase(rng, P.g, w);
+            if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
+                x = x + w * tmin;
+                d = tmax - tmin;
+            }
+        } else {
+            d -= t;
+        }
+    }
+    flush_counters(P, paths, lookups, guard_hit);
+}
+
 uint64_t padded_paths(int width, int height, uint32_t frames) {
     uint64_t tiles = (uint64_t)((width + 15) / 16) * (uint64_t)((height + 15) / 16);
     return tiles * 256ull * frames;
 }
 
 template <int TRACKER, int INTERP>
+static int refill_blocks(int requested) {
+    if (requested > 0) return requested;
+    static int per_sm = 0;
+    if (per_sm == 0) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_refill_kernel<TRACKER, INTERP>, kTraceBlock, 0);
+        if (per_sm <= 0) per_sm = 1;
+    }
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return per_sm * sms;
+}
+
+template <int TRACKER, int INTERP>
 static cudaError_t launch_trace_t(const TraceParams& P, int schedule, int features, int persistent_blocks,
                                   cudaStream_t stream) {
     uint64_t total = padded_paths(P.width, P.height, P.num_frames);
+    constexpr bool kRefillable = TRACKER == kDelta || TRACKER == kRatio || TRACKER == kNextEvent;
+    if (schedule == kScheduleRefill && kRefillable && !features) {
+        if constexpr (kRefillable) {
+            int blocks = refill_blocks<TRACKER, INTERP>(persistent_blocks);
+            cudaMemsetAsync(P.work_counter, 0, sizeof(unsigned long long), stream);
+            trace_refill_kernel<TRACKER, INTERP><<<blocks, kTraceBlock, 0, stream>>>(P, total);
+            count_launches(1);
+            return cudaGetLastError();
+        }
+    }
+    if (schedule == kScheduleRefill) schedule = kSchedulePersistent;
     if (schedule == kScheduleTiles) {
         uint64_t blocks = (total + kTraceBlock - 1) / kTraceBlock;
         trace_tiles_kernel<TRACKER, INTERP><<<(unsigned)blocks, kTraceBlock, 0, stream>>>(P, features);

@@ -8,7 +8,7 @@ namespace vpt {
 
 constexpr int kTraceBlock = 128;
 
-enum Schedule : int { kScheduleTiles = 0, kSchedulePersistent = 1 };
+enum Schedule : int { kScheduleTiles = 0, kSchedulePersistent = 1, kScheduleRefill = 2 };
 
 struct FbmParams {
     int octaves;

@@ -178,7 +178,9 @@ VptStatus vpt_synchronize(VptContext* ctx, void* stream);
 /* vpt.set_use_empty_space_skipping (VolumetricPathTracingPass::setUseEmptySpaceSkipping): NEE shadow
  * rays skip empty 8^3 blocks of the occupancy grid. */
 VptStatus vpt_set_use_empty_space_skipping(VptContext* ctx, int enabled);
-/* Tuning knobs without a reference counterpart: "schedule" (0 = tiles, 1 = persistent),
+/* Tuning knobs without a reference counterpart: "schedule" (0 = one path per thread over pixel
+ * tiles, 1 = persistent warps taking 32-path batches, 2 = persistent with per-lane path refill, the
+ * default; trackers without a refill kernel fall back to 1),
  * "persistent_blocks_per_sm", "max_steps_per_path" (guard on tentative collisions of one path,
  * default 2^24; a path that reaches it stops and vpt_synchronize reports VPT_ERR_ITER_LIMIT),
  * "ess_ref_compat" (1 = empty-space skipping exactly as the reference runs it: every block marked

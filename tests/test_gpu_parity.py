@@ -209,3 +209,19 @@ def test_iteration_guard_reports_error_without_hanging(core):
     core("vpt_reset_stats")
     core("vpt_render_frames", 1, None)
     core("vpt_synchronize", None)
+
+
+@pytest.mark.parametrize("mode", ["delta", "ratio", "nee"])
+def test_schedules_trace_identical_paths(core, mode):
+    """Tile, persistent-batch and per-lane-refill schedules trace the same paths (same film up to the
+    order of the FP64 atomic additions)."""
+    sp = fbm_scene(mode=mode, width=40, height=40)
+    setup_core(core, sp)
+    films = []
+    for sched in (0, 1, 2):
+        core("vpt_set_option", b"schedule", float(sched))
+        s, _ = gpu_render(core, sp, 3, stats=False)
+        films.append(s)
+    core("vpt_set_option", b"schedule", 2.0)
+    assert np.allclose(films[0], films[1], rtol=1e-12, atol=1e-12)
+    assert np.allclose(films[0], films[2], rtol=1e-12, atol=1e-12)
