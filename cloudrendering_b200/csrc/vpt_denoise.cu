@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
+#include <mutex>
 #include "vpt_denoise.h"
 #include "vpt_params.h"
 #include "vpt_kernels.h"
@@ -19,6 +20,7 @@
 
 namespace vpt {
 
+constexpr int kMaxDevices = 64;
 __constant__ float c_eaw_kernel[25];
 
 __device__ __forceinline__ float4 ld4(const float* img, int x, int y, int w, int h) {
@@ -76,17 +78,24 @@ __global__ void eaw_iteration_kernel(const float* __restrict__ color, const floa
     reinterpret_cast<float4*>(out)[(size_t)y * w + x] = make_float4(sum.x / acc, sum.y / acc, sum.z / acc, sum.w / acc);
 }
 
+// The 25 Gaussian tap weights live in constant memory, which is per device: upload once per device.
 static cudaError_t upload_eaw_kernel(cudaStream_t s) {
-    static bool done = false;
-    if (done) return cudaSuccess;
+    static std::mutex mu;
+    static bool done[kMaxDevices] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(mu);
+    if (done[dev]) return cudaSuccess;
     float k[25];
     for (int i = 0; i < 25; i++) {
         int x = i % 5 - 2, y = i / 5 - 2;
         k[i] = expf(-float(x * x + y * y) / 2.0f);
     }
-    cudaError_t e = cudaMemcpyToSymbolAsync(c_eaw_kernel, k, sizeof(k), 0, cudaMemcpyHostToDevice, s);
+    e = cudaMemcpyToSymbolAsync(c_eaw_kernel, k, sizeof(k), 0, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    if (e == cudaSuccess) done = true;
+    if (e == cudaSuccess) done[dev] = true;
     return e;
 }
 
