@@ -81,6 +81,8 @@ SIGNATURES = {
     "vpt_build_environment_pyramid": (c_int, [c_void_p, c_int, c_int, c_int, c_void_p, c_void_p]),
     "vpt_eaw_denoise_rgba": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_float, c_float, c_float,
                                      c_int, c_void_p, c_void_p]),
+    "vpt_eaw_denoise_rgba_noalloc": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_float, c_float,
+                                             c_float, c_int, c_void_p, c_void_p]),
 }
 
 _lib = None

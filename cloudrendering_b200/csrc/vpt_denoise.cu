@@ -569,4 +569,72 @@ cudaError_t feature_to_chw(const float* feat, int n, uint32_t frames, int featur
     return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------------------------
+// EAW without allocation.
+//
+// vpt_eaw_denoise_rgba takes its ping-pong image from the stream-ordered allocator.  Some callers
+// cannot allocate at that point: a frame loop that has already given nearly all device memory to
+// the volume, the film and a framework's caching allocator (an allocation there fails mid-frame or
+// makes the caching allocator release blocks and synchronise), and host engines that keep a fixed
+// device-memory budget and do not let a library touch the allocator inside their render loop.
+// For them, the ping-pong image lives in the fixed array below, which the library reserves on
+// every GPU that loads it, for the life of the process.
+//
+// The array holds one RGBA fp32 image of at most kEawNoAllocMaxPixels pixels (16 MiB).  Every call
+// on a device shares it and it keeps the previous call's contents.  Nothing in it has to start at
+// zero: each a-trous iteration writes every pixel of its target image before the next iteration
+// reads it.  Calls whose work overlaps on the GPU (other streams, other host threads) race on the
+// array.
+constexpr long long kEawNoAllocMaxPixels = 1024LL * 1024LL;
+static __device__ __align__(256) float4 g_eaw_noalloc_scratch[kEawNoAllocMaxPixels];
+
+// Device address of the array on the current device.  In host code the array's name only stands
+// in for the symbol; the address comes from the runtime, once per device.  The first call on a
+// device also uploads the tap weights (a synchronous copy), so it should come before any stream
+// capture.
+static cudaError_t eaw_noalloc_scratch(float** ptr) {
+    static std::mutex mu;
+    static float* addr[kMaxDevices] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!addr[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_eaw_noalloc_scratch);
+        if (e != cudaSuccess) return e;
+        addr[dev] = static_cast<float*>(p);
+    }
+    *ptr = addr[dev];
+    return cudaSuccess;
+}
+
 }  // namespace vpt
+
+extern "C" VptStatus vpt_eaw_denoise_rgba_noalloc(const float* color, const float* position, const float* normal,
+                                                  int width, int height, int iterations, float phi_color,
+                                                  float phi_position, float phi_normal, int ref_compute_quirk,
+                                                  float* out, void* stream) {
+    if (!color || !out || width <= 0 || height <= 0 || iterations < 0) return VPT_ERR_ARG;
+    if ((long long)width * (long long)height > vpt::kEawNoAllocMaxPixels) return VPT_ERR_ARG;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const size_t bytes = (size_t)width * height * 4 * sizeof(float);
+    if (iterations == 0) {
+        return cudaMemcpyAsync(out, color, bytes, cudaMemcpyDeviceToDevice, s) == cudaSuccess ? VPT_OK : VPT_ERR_CUDA;
+    }
+    float* scratch = nullptr;
+    if (vpt::eaw_noalloc_scratch(&scratch) != cudaSuccess) return VPT_ERR_CUDA;
+    vpt::EawSettings st;
+    st.iterations = iterations;
+    st.phi_color = phi_color;
+    st.phi_position = phi_position;
+    st.phi_normal = phi_normal;
+    st.ref_compute_quirk = ref_compute_quirk;
+    // The last iteration lands in `out`: odd counts start there, even counts start in the array.
+    float* ping = (iterations % 2 == 1) ? out : scratch;
+    float* pong = (iterations % 2 == 1) ? scratch : out;
+    float* result = nullptr;
+    cudaError_t e = vpt::eaw_denoise(color, position, normal, width, height, st, ping, pong, &result, s);
+    return e == cudaSuccess ? VPT_OK : VPT_ERR_CUDA;
+}

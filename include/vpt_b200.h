@@ -220,6 +220,18 @@ VptStatus vpt_build_environment_pyramid(const float* rgba, int width, int height
 VptStatus vpt_eaw_denoise_rgba(const float* color, const float* position, const float* normal, int width,
                                int height, int iterations, float phi_color, float phi_position, float phi_normal,
                                int ref_compute_quirk, float* out, void* stream);
+/* No counterpart in the reference.  Same filter and arguments as vpt_eaw_denoise_rgba, for callers
+ * that cannot allocate device memory while they denoise (a frame loop whose device memory is
+ * already spent on the volume, the film and a framework's caching allocator; a host engine with a
+ * fixed memory budget).  It allocates and frees nothing: its ping-pong image is one RGBA fp32 array
+ * of at most 1024*1024 pixels (16 MiB) that the library reserves on every GPU that loads it, for the
+ * life of the process.  width*height above 1048576 returns VPT_ERR_ARG.  The first call on a device
+ * looks up the array's address and uploads the filter's tap weights with a synchronous copy; make
+ * that first call before any stream capture.  All calls on a device share the array, so calls whose
+ * work overlaps on the GPU race; nothing in it needs to start at zero. */
+VptStatus vpt_eaw_denoise_rgba_noalloc(const float* color, const float* position, const float* normal, int width,
+                                       int height, int iterations, float phi_color, float phi_position,
+                                       float phi_normal, int ref_compute_quirk, float* out, void* stream);
 
 #ifdef __cplusplus
 }
