@@ -11,6 +11,7 @@ from ctypes import POINTER, c_char_p, c_double, c_float, c_int, c_uint32, c_uint
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libvpt_b200.so")
+LIB_PATH_DR = os.path.join(_HERE, "libvpt_b200_dr.so")
 
 
 class VptStats(ctypes.Structure):
@@ -85,24 +86,26 @@ SIGNATURES = {
                                              c_float, c_int, c_void_p, c_void_p]),
 }
 
-_lib = None
+_libs: dict = {}
 
 
-def load() -> ctypes.CDLL:
-    """Loads the library (once) and installs the argument types."""
-    global _lib
-    if _lib is not None:
-        return _lib
-    if not os.path.exists(LIB_PATH):
-        raise ImportError(
-            f"{LIB_PATH} is missing: build the CUDA core first (python -m cloudrendering_b200.build)"
-        )
-    lib = ctypes.CDLL(LIB_PATH)
+def load(variant: str = "default") -> ctypes.CDLL:
+    """Loads the library (once per variant) and installs the argument types.
+
+    ``variant="dr"`` loads ``libvpt_b200_dr.so``: the same core with the tracer's transcendental
+    functions evaluated in double precision and rounded once to float (used by the parity tests to
+    compare paths one by one with the CPU oracle in the same mode)."""
+    if variant in _libs:
+        return _libs[variant]
+    path = {"default": LIB_PATH, "dr": LIB_PATH_DR}[variant]
+    if not os.path.exists(path):
+        raise ImportError(f"{path} is missing: build the CUDA core first (python -m cloudrendering_b200.build)")
+    lib = ctypes.CDLL(path)
     for name, (res, args) in SIGNATURES.items():
         fn = getattr(lib, name)
         fn.restype = res
         fn.argtypes = args
-    _lib = lib
+    _libs[variant] = lib
     return lib
 
 
@@ -119,10 +122,10 @@ class VptError(RuntimeError):
         self.status = status
 
 
-def check(status: int, where: str, ctx=None) -> None:
+def check(status: int, where: str, ctx=None, lib=None) -> None:
     if status == 0:
         return
-    lib = load()
+    lib = lib or load()
     msg = lib.vpt_last_error(ctx).decode() if ctx else ""
     if not msg:
         msg = lib.vpt_status_string(status).decode()

@@ -4,6 +4,11 @@ Run ``python -m cloudrendering_b200.build`` (or ``__graft_entry__.build()``).  E
 ``csrc/`` is compiled in parallel; objects go to ``cloudrendering_b200/_build/`` and the shared library
 next to this file, where ``cloudrendering_b200._lib`` loads it.  The CUDA runtime is linked statically,
 so the library only needs the NVIDIA driver at run time.
+
+A second library, ``libvpt_b200_dr.so``, is the same core with the tracer's transcendental functions
+evaluated in double precision and rounded once to float (``-DVPT_DOUBLE_ROUNDED_MATH`` on
+``vpt_kernels.cu``).  The parity tests use it to compare paths one by one with the CPU oracle in the
+same mode; the default library is the product.
 """
 from __future__ import annotations
 
@@ -16,6 +21,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libvpt_b200.so")
+LIB_DR = os.path.join(HERE, "libvpt_b200_dr.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -25,6 +31,8 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", INCLUDE
 PER_FILE = {
     "vpt_kernels.cu": ["--fmad=false"],
 }
+# sources that hold the tracer's transcendental calls (built twice, see above)
+DOUBLE_ROUNDED = {"vpt_kernels.cu"}
 
 
 def _nvcc() -> str:
@@ -51,14 +59,24 @@ def build(verbose: bool = False, force: bool = False) -> str:
     headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
     headers.append(os.path.join(INCLUDE, "vpt_b200.h"))
     jobs = []
-    objs = []
-    for src in _sources():
-        obj = os.path.join(BUILD, src[:-3] + ".o")
-        objs.append(obj)
+    objs, objs_dr = [], []
+
+    def add(src, obj, extra):
         deps = [os.path.join(CSRC, src)] + headers
         if force or _needs_rebuild(obj, deps):
-            cmd = [nvcc, *ARCH, *COMMON, *PER_FILE.get(src, []), "-c", os.path.join(CSRC, src), "-o", obj]
-            jobs.append(cmd)
+            jobs.append([nvcc, *ARCH, *COMMON, *PER_FILE.get(src, []), *extra, "-c", os.path.join(CSRC, src),
+                         "-o", obj])
+
+    for src in _sources():
+        obj = os.path.join(BUILD, src[:-3] + ".o")
+        add(src, obj, [])
+        objs.append(obj)
+        if src in DOUBLE_ROUNDED:
+            obj_dr = os.path.join(BUILD, src[:-3] + "_dr.o")
+            add(src, obj_dr, ["-DVPT_DOUBLE_ROUNDED_MATH"])
+            objs_dr.append(obj_dr)
+        else:
+            objs_dr.append(obj)
 
     def run(cmd):
         if verbose:
@@ -71,8 +89,9 @@ def build(verbose: bool = False, force: bool = False) -> str:
     if jobs:
         with ThreadPoolExecutor(max_workers=min(len(jobs), os.cpu_count() or 4)) as ex:
             list(ex.map(run, jobs))
-    if jobs or not os.path.exists(LIB) or force:
-        run([nvcc, *ARCH, "-shared", "-o", LIB, *objs])
+    for lib, lib_objs in ((LIB, objs), (LIB_DR, objs_dr)):
+        if jobs or not os.path.exists(lib) or force:
+            run([nvcc, *ARCH, "-shared", "-o", lib, *lib_objs])
     return LIB
 
 

@@ -21,6 +21,31 @@ namespace vpt {
 constexpr float kPi = 3.14159265359f;        // VptUtils.glsl:27
 constexpr float kTwoPi = 2.0f * 3.14159265359f;
 
+// Transcendental functions of the tracer.  By default they are CUDA's single-precision functions,
+// which can differ from a CPU C library by an ulp on some arguments.  With VPT_DOUBLE_ROUNDED_MATH
+// (the library variant libvpt_b200_dr.so) each one is evaluated in double precision and rounded
+// once to float.  The CPU oracle has the same mode: both sides then return the correctly rounded
+// float except where the exact result lies within about one double ulp of a float rounding
+// boundary (probability ~2^-29 per call), so paths of thousands of bounces can be compared one by
+// one without an ulp difference flipping a later comparison.
+#ifdef VPT_DOUBLE_ROUNDED_MATH
+VPT_DEV float m_log(float x) { return (float)log((double)x); }
+VPT_DEV float m_exp(float x) { return (float)exp((double)x); }
+VPT_DEV float m_sin(float x) { return (float)sin((double)x); }
+VPT_DEV float m_cos(float x) { return (float)cos((double)x); }
+VPT_DEV float m_pow(float x, float y) { return (float)pow((double)x, (double)y); }
+VPT_DEV float m_atan2(float y, float x) { return (float)atan2((double)y, (double)x); }
+VPT_DEV float m_asin(float x) { return (float)asin((double)x); }
+#else
+VPT_DEV float m_log(float x) { return logf(x); }
+VPT_DEV float m_exp(float x) { return expf(x); }
+VPT_DEV float m_sin(float x) { return sinf(x); }
+VPT_DEV float m_cos(float x) { return cosf(x); }
+VPT_DEV float m_pow(float x, float y) { return powf(x, y); }
+VPT_DEV float m_atan2(float y, float x) { return atan2f(y, x); }
+VPT_DEV float m_asin(float x) { return asinf(x); }
+#endif
+
 VPT_DEV F3 f3(float x, float y, float z) { F3 r; r.x = x; r.y = y; r.z = z; return r; }
 VPT_DEV F3 operator+(F3 a, F3 b) { return f3(a.x + b.x, a.y + b.y, a.z + b.z); }
 VPT_DEV F3 operator-(F3 a, F3 b) { return f3(a.x - b.x, a.y - b.y, a.z - b.z); }
@@ -121,8 +146,8 @@ VPT_DEV F3 random_direction(Rng& rng, F3 d) {
     float sq = r2 * r2;
     float a = kTwoPi * r1;
     float s = sqrtf(1.0f - sq);
-    float x = cosf(a) * s;
-    float y = sinf(a) * s;
+    float x = m_cos(a) * s;
+    float y = m_sin(a) * s;
     F3 t0, t1;
     orthonormal_basis(d, t0, t1);
     return (t0 * x + t1 * y) + d * r2;
@@ -143,22 +168,22 @@ VPT_DEV F3 sample_phase(Rng& rng, float g, F3 d) {
     float sin_t = sqrtf(fmaxf(0.0f, 1.0f - cos_t * cos_t));
     F3 t0, t1;
     orthonormal_basis(d, t0, t1);
-    return (t0 * (sin_t * sinf(phi)) + t1 * (sin_t * cosf(phi))) + d * cos_t;
+    return (t0 * (sin_t * m_sin(phi)) + t1 * (sin_t * m_cos(phi))) + d * cos_t;
 }
 
 VPT_DEV float evaluate_phase(float g, F3 a, F3 b) {
     float c = dot3(normalize3(a), normalize3(b));
-    return ((0.25f / kPi) * (1.0f - g * g)) / powf((1.0f + g * g) - 2.0f * g * c, 1.5f);
+    return ((0.25f / kPi) * (1.0f - g * g)) / m_pow((1.0f + g * g) - 2.0f * g * c, 1.5f);
 }
 
 // ---------------------------------------------------------------------------------------------
 // Sky and sun (VptUtils.glsl:288-389).
 VPT_DEV float srgb_to_linear(float c) {
-    return c <= 0.04045f ? c / 12.92f : powf((c + 0.055f) / 1.055f, 2.4f);
+    return c <= 0.04045f ? c / 12.92f : m_pow((c + 0.055f) / 1.055f, 2.4f);
 }
 
 VPT_DEV float linear_to_srgb(float c) {
-    return c <= 0.0031308f ? c * 12.92f : 1.055f * powf(c, 1.0f / 2.4f) - 0.055f;
+    return c <= 0.0031308f ? c * 12.92f : 1.055f * m_pow(c, 1.0f / 2.4f) - 0.055f;
 }
 
 VPT_DEV F3 sky_default(F3 dir, int linear_rgb) {
@@ -186,7 +211,7 @@ VPT_DEV F3 sky_default(F3 dir, int linear_rgb) {
 // (sampleLight, VptUtils.glsl:370-374).
 VPT_DEV F3 sun_lobe(const TraceParams& P, F3 dir) {
     const float norm = 11.0f / (2.0f * 3.14159f);
-    float p = powf(fmaxf(0.0f, dot3(dir, P.sun_dir)), 10.0f);
+    float p = m_pow(fmaxf(0.0f, dot3(dir, P.sun_dir)), 10.0f);
     return f3((P.sun_intensity.x * p) * norm, (P.sun_intensity.y * p) * norm, (P.sun_intensity.z * p) * norm);
 }
 
@@ -212,8 +237,8 @@ VPT_DEV F3 env_image_fetch(const TraceParams& P, float u, float v) {
 
 // sampleSkybox for an environment image (VptUtils.glsl:303-328; no rotation).
 VPT_DEV F3 sky_image(const TraceParams& P, F3 dir) {
-    float u = atan2f(dir.z, dir.x) / kTwoPi + 0.5f;
-    float v = -asinf(dir.y) / kPi + 0.5f;
+    float u = m_atan2(dir.z, dir.x) / kTwoPi + 0.5f;
+    float v = -m_asin(dir.y) / kPi + 0.5f;
     F3 c = env_image_fetch(P, u, v);
     c.x = fminf(c.x, 100000.0f);
     c.y = fminf(c.y, 100000.0f);
@@ -262,8 +287,8 @@ VPT_DEV F3 octahedral_uv_to_world(float u, float v) {
     if (r == 0.0f) phi = 0.0f;
     float r2 = r * r;
     float s = sqrtf(2.0f - r2);
-    float x = sx * cosf(phi) * r * s;
-    float y = sy * sinf(phi) * r * s;
+    float x = sx * m_cos(phi) * r * s;
+    float y = sy * m_sin(phi) * r * s;
     float z = signf(1.0f - u - v) * (1.0f - r2);
     return f3(x, y, z);
 }
@@ -272,7 +297,7 @@ VPT_DEV void world_to_octahedral_uv(F3 dir, float& u, float& v) {
     dir = normalize3(dir);
     float sx = signf(dir.x), sy = signf(dir.y), sz = signf(dir.z);
     dir = f3(fabsf(dir.x), fabsf(dir.y), fabsf(dir.z));
-    float phi = atan2f(dir.y, dir.x);
+    float phi = m_atan2(dir.y, dir.x);
     float r = sqrtf(1.0f - dir.z);
     float vv = r * 2.0f / kPi * phi;
     float uu = r - vv;

@@ -640,7 +640,7 @@ __global__ void rrt_params_kernel(const float* __restrict__ mn, const float* __r
     if (i >= total) return;
     float mu_min = mn[i] * extinction, mu_max = mx[i] * extinction, mu_avg = avg[i] * extinction;
     float mu_r = fmaxf(mu_max - mu_min, 0.1f);
-    float mu_c = mu_min + mu_r * powf(2.0f, (1.0f / (D * mu_r)) - 1.0f);
+    float mu_c = mu_min + mu_r * m_pow(2.0f, (1.0f / (D * mu_r)) - 1.0f);
     mu_c = fminf(fmaxf(mu_c, mu_min), mu_avg);
     out_pairs[2 * i + 0] = mu_c;
     out_pairs[2 * i + 1] = mu_r;
@@ -698,8 +698,8 @@ __global__ void env_octahedral_level0_kernel(const __grid_constant__ TraceParams
             float u = ((float)x + sxo) / (float)res;
             float v = ((float)y + syo) / (float)res;
             F3 dir = octahedral_uv_to_world(u, v);
-            float tu = atan2f(dir.z, dir.x) / (2.0f * kPi) + 0.5f;
-            float tv = -asinf(dir.y) / kPi + 0.5f;
+            float tu = m_atan2(dir.z, dir.x) / (2.0f * kPi) + 0.5f;
+            float tv = -m_asin(dir.y) / kPi + 0.5f;
             F3 c = env_image_fetch(P, tu, tv);
             c = f3(fminf(c.x, 100000.0f), fminf(c.y, 100000.0f), fminf(c.z, 100000.0f));
             best = fmaxf(best, length3(c));

@@ -31,6 +31,40 @@ constexpr uint32_t kMaxStepsPerPath = 1u << 24;
 
 struct F3 { float x, y, z; };
 
+// A constant region of a sparse grid: a tile of a lower (level 1), upper (level 2) or root (level
+// 3) node, or the background outside every root tile (level 4).  `box` is the index-space bounding
+// box of the node that holds the tile (its active values, inclusive), which the sparse
+// decomposition tracker clips against (DecompositionTracking.glsl:219-240).
+struct SparseTile {
+    float value;
+    int active;
+    int level;
+    int box[6];
+};
+
+// Sparse (NanoVDB-compatible) volume as the tracer reads it.  The tree is flattened into a table
+// with one 32-bit entry per 8^3 brick of the root's bounding box: bit 31 clear = index of a leaf in
+// the leaf pools, bit 31 set = index into `tiles`.  Bricks outside the table are background.
+constexpr uint32_t kSparseTileBit = 0x80000000u;
+struct SparseView {
+    float mat[9];              // index -> world (Map::mMatF, row-major as PNanoVDB applies it)
+    float inv_mat[9];          // world -> index (Map::mInvMatF)
+    float vec[3];              // Map::mVecF
+    F3 grid_min, grid_max;     // world bounding box of the active values (float)
+    int root_min[3], root_max[3];  // index bounding box of the root node (inclusive)
+    int tbl_origin[3];         // first voxel of the brick table (multiple of 8)
+    int tbl_dim[3];            // bricks per axis
+    int lowest_level;          // HDDA cell size of the decomposition tracker: 8 (leaves) or 1 (voxels)
+    int fp16;                  // leaf values stored as IEEE half
+    float background;
+    const uint32_t* table;
+    const float* values;            // 512 floats per leaf, NanoVDB voxel order ((x&7)<<6 | (y&7)<<3 | (z&7))
+    const unsigned short* values_h; // the same as half (fp16 variant)
+    const uint32_t* masks;          // 16 words per leaf: active voxels
+    const int* leaf_bbox_min;       // 3 per leaf: LeafData::mBBoxMin
+    const SparseTile* tiles;
+};
+
 struct TraceParams {
     // camera: inverse(proj * view), column-major like glm (m[col*4 + row])
     float inv_view_proj[16];
@@ -55,6 +89,7 @@ struct TraceParams {
     int interp;                // Interp
     int max_bounces;           // 0 = unlimited
     uint32_t max_steps;        // guard on tentative collisions per path (kMaxStepsPerPath by default)
+    int grid_kind;             // GridKind: dense texture or sparse (NanoVDB) volume
     int ess_ref_compat;        // reproduce the reference's empty-space-skipping shadow loop exactly
 
     // supervoxels (residual ratio / decomposition tracking, occupancy grid)
@@ -88,6 +123,8 @@ struct TraceParams {
     unsigned long long* counters;  // [0] paths, [1] density lookups
     int* error_flags;
     unsigned int* work_counter;    // persistent-kernel path queue
+
+    SparseView sparse;             // valid when grid_kind == kNanoVdb
 };
 
 // Offsets of the per-pixel feature accumulators (floats).

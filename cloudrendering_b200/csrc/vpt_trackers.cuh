@@ -7,6 +7,7 @@
 // so the dense texture and the NanoVDB tree share the trackers.
 #pragma once
 #include "vpt_device.cuh"
+#include "vpt_sparse.cuh"
 
 namespace vpt {
 
@@ -33,7 +34,7 @@ VPT_DEV bool guard(PathCtx& pc) {
 }
 
 VPT_DEV float free_path(Rng& rng, float inv_majorant) {
-    return -logf(fmaxf(0.0000000001f, 1.0f - rng_next(rng))) * inv_majorant;
+    return -m_log(fmaxf(0.0000000001f, 1.0f - rng_next(rng))) * inv_majorant;
 }
 
 VPT_DEV void record_event(FirstEvent& fe, F3 x, float density, float extinction, float depth) {
@@ -189,7 +190,7 @@ VPT_DEV float shadow_transmittance_ess(const TraceParams& P, S& sample, Rng& rng
             float t = 0.0f;
             while (true) {
                 if (guard(pc)) return 0.0f;
-                t -= logf(fmaxf(0.0000000001f, 1.0f - rng_next(rng))) * P.inv_extinction;
+                t -= m_log(fmaxf(0.0000000001f, 1.0f - rng_next(rng))) * P.inv_extinction;
                 if (t >= d_max) {
                     x = (P.ess_ref_compat ? x : x0) + w * d_max;
                     break;
@@ -322,11 +323,11 @@ VPT_DEV F3 track_decomposition(const TraceParams& P, S& sample, Rng& rng, F3 x, 
             } else {
                 float mu_c = fmaxf(0.0000000001f, majorant * smin_d);
                 float mu_r = fmaxf(0.0000000001f, majorant * smax_d - mu_c);
-                float t_c = -logf(fmaxf(0.0000000001f, 1.0f - rng_next(rng))) / mu_c;
+                float t_c = -m_log(fmaxf(0.0000000001f, 1.0f - rng_next(rng))) / mu_c;
                 float t_r = 0.0f;
                 while (true) {
                     if (guard(pc)) return f3(0.0f, 0.0f, 0.0f);
-                    t_r -= logf(fmaxf(0.0000000001f, 1.0f - rng_next(rng))) / mu_r;
+                    t_r -= m_log(fmaxf(0.0000000001f, 1.0f - rng_next(rng))) / mu_r;
                     if (t_c >= d_max && t_r >= d_max) {
                         x = x + w * d_max;
                         break;
@@ -346,7 +347,7 @@ VPT_DEV F3 track_decomposition(const TraceParams& P, S& sample, Rng& rng, F3 x, 
                         if (P.max_bounces > 0 && ++bounces > P.max_bounces) return f3(0.0f, 0.0f, 0.0f);
                         w = sample_phase(rng, P.g, w);
                         t_r = 0.0f;
-                        t_c = -logf(fmaxf(0.0000000001f, 1.0f - rng_next(rng))) / mu_c;
+                        t_c = -m_log(fmaxf(0.0000000001f, 1.0f - rng_next(rng))) / mu_c;
                         ray_box(smin, smax, x, w, tmin_sv, tmax_sv);
                         d_max = tmax_sv - tmin_sv;
                     }
@@ -358,18 +359,105 @@ VPT_DEV F3 track_decomposition(const TraceParams& P, S& sample, Rng& rng, F3 x, 
     return sky_and_sun(P, w);
 }
 
+// Analog decomposition tracking over a sparse grid with the hierarchical DDA
+// (analogDecompositionTracking, DecompositionTracking.glsl:130-360): the HDDA walks the tree at the
+// leaf level (cells of 8^3, coarser in tiles), skips inactive nodes, and inside an active node
+// tracks with a control extinction of 1e-10 and a residual majorant equal to the global majorant
+// (the node min/max are read but unused by the reference).  After a scattering event the node box
+// bounds the next segment and the HDDA restarts behind it.  The node box of a leaf is
+// [LeafData::mBBoxMin, +8), of a tile the bounding box of its node, as in the reference.
+template <class S>
+VPT_DEV F3 track_decomposition_sparse(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, FirstEvent& fe,
+                                      PathCtx& pc) {
+    const SparseView& V = P.sparse;
+    F3 origin = sparse_world_to_index(V, x);
+    F3 direction = sparse_world_to_index_dir(V, w);
+    const float grid_to_world = 1.0f / length3(direction);
+    direction = direction * grid_to_world;
+    float t_min = 0.0f, t_max = 1e10f;
+    const F3 root_lo = f3((float)V.root_min[0], (float)V.root_min[1], (float)V.root_min[2]);
+    const F3 root_hi = f3((float)(V.root_max[0] + 1), (float)(V.root_max[1] + 1), (float)(V.root_max[2] + 1));
+    const bool hits_root = hdda_ray_clip(root_lo, root_hi, origin, t_min, direction, t_max);
+    if (hits_root && t_max < 1e20f) {
+        const float majorant = P.extinction;
+        const int lowest = V.lowest_level;
+        int bounces = 0;
+        Hdda h;
+        hdda_init(h, origin, t_min - 1e-4f, direction, t_max + 1e-4f, lowest);
+        for (int iteration = 0;; iteration++) {
+            if (guard(pc)) return f3(0.0f, 0.0f, 0.0f);
+            if (iteration > 0) {
+                if (!hdda_step(h)) break;
+                const int d = max(sparse_dim(V, h.voxel[0], h.voxel[1], h.voxel[2]), lowest);
+                hdda_update(h, origin, direction, d);
+            }
+            F3 nmin, nmax;
+            if (!sparse_cell_node(V, h.voxel, nmin, nmax)) continue;
+            float t_min_node = 0.0f, t_max_node = 1e10f;
+            const bool hits_node = hdda_ray_clip(nmin, nmax, origin, t_min_node, direction, t_max_node);
+            x = sparse_index_to_world(V, origin + direction * t_min_node);
+            if (!hits_node) continue;
+            float d_max = grid_to_world * (fminf(fminf(h.next[0], h.next[1]), h.next[2]) - h.tmin);
+            const float mu_c = 0.0000000001f;
+            const float mu_r = fmaxf(0.0000000001f, majorant * 1.0f - mu_c);
+            bool direction_changed = false;
+            float t_c = -m_log(fmaxf(0.0000000001f, 1.0f - rng_next(rng))) / mu_c;
+            float t_r = 0.0f;
+            while (true) {
+                if (guard(pc)) return f3(0.0f, 0.0f, 0.0f);
+                t_r -= m_log(fmaxf(0.0000000001f, 1.0f - rng_next(rng))) / mu_r;
+                if (t_c >= d_max && t_r >= d_max) {
+                    x = x + d_max * w;
+                    break;
+                }
+                const F3 xs = x + w * fminf(t_c, t_r);
+                bool collision;
+                if (t_c <= t_r) {
+                    collision = true;
+                } else {
+                    const float density = sample(xs, rng);
+                    pc.lookups++;
+                    collision = rng_next(rng) * mu_r < P.extinction * density - mu_c;
+                }
+                if (collision) {
+                    x = xs;
+                    if (rng_next(rng) < P.absorb_albedo) return f3(0.0f, 0.0f, 0.0f);
+                    if (P.max_bounces > 0 && ++bounces > P.max_bounces) return f3(0.0f, 0.0f, 0.0f);
+                    w = sample_phase(rng, P.g, w);
+                    t_r = 0.0f;
+                    t_c = -m_log(fmaxf(0.0000000001f, 1.0f - rng_next(rng))) / mu_c;
+                    origin = sparse_world_to_index(V, x);
+                    direction = normalize3(sparse_world_to_index_dir(V, w));
+                    float t_min_leaf = 0.0f, t_max_leaf = 1e10f;
+                    ray_box(nmin, nmax, origin, direction, t_min_leaf, t_max_leaf);
+                    hdda_ray_clip(nmin, nmax, origin, t_min_leaf, direction, t_max_leaf);
+                    d_max = grid_to_world * (t_max_leaf - t_min_leaf);
+                    direction_changed = true;
+                }
+            }
+            if (direction_changed) {
+                t_min = 0.0f;
+                t_max = 1e10f;
+                hdda_ray_clip(root_lo, root_hi, origin, t_min, direction, t_max);
+                hdda_init(h, origin, t_min + d_max / grid_to_world + 1e-4f, direction, t_max + 1e-4f, lowest);
+            }
+        }
+    }
+    return sky_and_sun(P, w);
+}
+
 // Per-supervoxel residual ratio tracking estimator with reservoir selection of the next
 // in-scattering distance (residualRatioTrackingEstimator, ResidualRatioTracking.glsl:34-76).
 template <class S>
 VPT_DEV float rrt_estimator(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, float d_start, float d_end,
                             float T, float& wsum, float& res_t, float& res_dist, float mu_c, float mu_r,
                             PathCtx& pc) {
-    float t_c = expf(-mu_c * (d_end - d_start));
+    float t_c = m_exp(-mu_c * (d_end - d_start));
     float t_r = 1.0f;
     float d_trav = d_start;
     while (true) {
         if (guard(pc)) break;
-        float t = -logf(fmaxf(0.0000000001f, 1.0f - rng_next(rng))) / mu_r;
+        float t = -m_log(fmaxf(0.0000000001f, 1.0f - rng_next(rng))) / mu_r;
         x = x + w * t;
         d_trav += t;
         if (d_trav >= d_end) break;
@@ -377,7 +465,7 @@ VPT_DEV float rrt_estimator(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 
         pc.lookups++;
         float mu = P.extinction * density;
         t_r *= 1.0f - (mu - mu_c) / mu_r;
-        float t_c_local = expf(-mu_c * (d_trav - d_start));
+        float t_c_local = m_exp(-mu_c * (d_trav - d_start));
         float t_local = (T * t_r) * t_c_local;
         wsum += t_local;
         float xi = rng_next(rng);

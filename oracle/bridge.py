@@ -64,6 +64,8 @@ def load():
         lib.oracle_eaw.argtypes = [c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_float, c_float, c_float,
                                    c_int, c_void_p]
         lib.oracle_rng_stream.argtypes = [c_uint32, c_int, c_void_p, c_void_p]
+        lib.oracle_set_double_rounded_math.argtypes = [c_int]
+        lib.oracle_set_double_rounded_math.restype = None
         _lib = lib
     return _lib
 
@@ -188,3 +190,19 @@ class Scene:
         out = np.empty((xs.size, 3), np.float32)
         load().oracle_trace_paths(ctypes.byref(self.s), _p(xs), _p(ys), _p(fr), xs.size, _p(out), threads)
         return out
+
+
+class double_rounded_math:
+    """Context manager: the oracle's transcendentals in double precision rounded to float (the mode
+    of the CUDA core's libvpt_b200_dr.so) inside the block."""
+
+    def __init__(self, on: bool = True):
+        self.on = on
+
+    def __enter__(self):
+        load().oracle_set_double_rounded_math(1 if self.on else 0)
+        return self
+
+    def __exit__(self, *exc):
+        load().oracle_set_double_rounded_math(0)
+        return False

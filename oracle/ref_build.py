@@ -6,9 +6,12 @@
    literals -> ``f`` suffix, the RNG state made thread-local, ``main`` renamed); nothing else is
    changed.  One variant per (tracker, interpolation, environment, colour space) define set, as the
    reference's loadShader() would select (VolumetricPathTracingPass.cpp:1558-1782).
-2. ``libref_svgrid.so``: src/PathTracer/SuperVoxelGrid.cpp compiled against stub headers for the
-   GPU-upload parts (the CPU loops are the reference's).
-3. ``libref_pnanovdb.so``: Data/Shaders/VPT/PNanoVDB.glsl compiled as C99 (-DPNANOVDB_C).
+3. ``libref_pnanovdb.so``: Data/Shaders/VPT/PNanoVDB.glsl compiled in its own C99 mode
+   (-DPNANOVDB_C -DPNANOVDB_HDDA) with ``ref_pnanovdb_driver.c``: the reference's NanoVDB read
+   accessor, map and HDDA.
+4. ``libref_nanovdb_builder.so``: the reference's vendored NanoVDB GridBuilder
+   (src/nanovdb/util/GridBuilder.h) driven as CloudData::getSparseDensityField drives it
+   (``ref_nanovdb_builder.cpp``).
 
 The reference tree is read from $VPT_REFERENCE_ROOT or /root/reference; when it is absent the build
 is skipped (the prebuilt libraries under oracle/_ref are used as they are).
@@ -151,11 +154,29 @@ def build_tracer(force=False, verbose=False) -> str:
     return lib
 
 
+def _stale(lib, deps, force):
+    return force or not os.path.exists(lib) or os.path.getmtime(lib) < max(os.path.getmtime(d) for d in deps)
+
+
+def build_nanovdb(force=False, verbose=False) -> None:
+    drv = os.path.join(HERE, "ref_pnanovdb_driver.c")
+    lib = os.path.join(OUT, "libref_pnanovdb.so")
+    if _stale(lib, [drv, __file__], force):
+        _run(["gcc", "-O2", "-std=c99", "-fPIC", "-shared", "-ffp-contract=off", "-w", "-I", SHADERS, "-o", lib, drv,
+              "-lm"], verbose)
+    src = os.path.join(HERE, "ref_nanovdb_builder.cpp")
+    lib = os.path.join(OUT, "libref_nanovdb_builder.so")
+    if _stale(lib, [src, __file__], force):
+        _run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-w", "-I", os.path.join(REF, "src"), "-o", lib, src,
+              "-lpthread"], verbose)
+
+
 def build(force=False, verbose=False) -> None:
     if not os.path.isdir(SHADERS):
         return
     os.makedirs(OUT, exist_ok=True)
     build_tracer(force, verbose)
+    build_nanovdb(force, verbose)
 
 
 if __name__ == "__main__":

@@ -17,6 +17,19 @@ namespace {
 const float PI = 3.14159265359f;  // VptUtils.glsl:27
 const float TWO_PI = 2.0f * 3.14159265359f;
 
+// Transcendentals of the tracer: the C library's float functions, or (oracle_set_double_rounded_math)
+// the double-precision functions rounded once to float, the mode of the CUDA core's
+// libvpt_b200_dr.so.  In that mode both sides return the correctly rounded float except on
+// arguments whose exact result lies within about one double ulp of a float rounding boundary.
+bool g_dr_math = false;
+inline float m_log(float x) { return g_dr_math ? (float)log((double)x) : logf(x); }
+inline float m_exp(float x) { return g_dr_math ? (float)exp((double)x) : expf(x); }
+inline float m_sin(float x) { return g_dr_math ? (float)sin((double)x) : sinf(x); }
+inline float m_cos(float x) { return g_dr_math ? (float)cos((double)x) : cosf(x); }
+inline float m_pow(float x, float y) { return g_dr_math ? (float)pow((double)x, (double)y) : powf(x, y); }
+inline float m_atan2(float y, float x) { return g_dr_math ? (float)atan2((double)y, (double)x) : atan2f(y, x); }
+inline float m_asin(float x) { return g_dr_math ? (float)asin((double)x) : asinf(x); }
+
 struct V3 {
     float x, y, z;
 };
@@ -100,7 +113,7 @@ V3 random_direction(Rng& r, V3 d) {
     float r2 = rnd(r) * 2.0f - 1.0f;
     float s = sqrtf(1.0f - r2 * r2);
     float a = TWO_PI * r1;
-    float x = cosf(a) * s, y = sinf(a) * s;
+    float x = m_cos(a) * s, y = m_sin(a) * s;
     V3 t0, t1;
     basis(d, t0, t1);
     return add(add(mul(t0, x), mul(t1, y)), mul(d, r2));
@@ -114,16 +127,16 @@ V3 sample_phase(Rng& r, float g, V3 d) {
     float sin_t = sqrtf(std::max(0.0f, 1.0f - cos_t * cos_t));
     V3 t0, t1;
     basis(d, t0, t1);
-    return add(add(mul(t0, sin_t * sinf(phi)), mul(t1, sin_t * cosf(phi))), mul(d, cos_t));
+    return add(add(mul(t0, sin_t * m_sin(phi)), mul(t1, sin_t * m_cos(phi))), mul(d, cos_t));
 }
 float eval_phase(float g, V3 a, V3 b) {
     float c = dot(normalize(a), normalize(b));
-    return ((0.25f / PI) * (1.0f - g * g)) / powf((1.0f + g * g) - 2.0f * g * c, 1.5f);
+    return ((0.25f / PI) * (1.0f - g * g)) / m_pow((1.0f + g * g) - 2.0f * g * c, 1.5f);
 }
 
 // ---- sky and sun (VptUtils.glsl:288-389, 125-267) ----
-float srgb_to_lin(float c) { return c <= 0.04045f ? c / 12.92f : powf((c + 0.055f) / 1.055f, 2.4f); }
-float lin_to_srgb(float c) { return c <= 0.0031308f ? c * 12.92f : 1.055f * powf(c, 1.0f / 2.4f) - 0.055f; }
+float srgb_to_lin(float c) { return c <= 0.04045f ? c / 12.92f : m_pow((c + 0.055f) / 1.055f, 2.4f); }
+float lin_to_srgb(float c) { return c <= 0.0031308f ? c * 12.92f : 1.055f * m_pow(c, 1.0f / 2.4f) - 0.055f; }
 
 V3 sky_default(V3 dir, int lin) {
     const float cr[5] = {0.1f, 0.01f, 0.8f, 0.1f, 0.01f};
@@ -142,7 +155,7 @@ V3 sky_default(V3 dir, int lin) {
 }
 V3 sun_lobe(const OracleScene& S, V3 dir) {
     const float norm = 11.0f / (2.0f * 3.14159f);
-    float p = powf(std::max(0.0f, dot(dir, v3(S.sun_dir[0], S.sun_dir[1], S.sun_dir[2]))), 10.0f);
+    float p = m_pow(std::max(0.0f, dot(dir, v3(S.sun_dir[0], S.sun_dir[1], S.sun_dir[2]))), 10.0f);
     return v3((S.sun_intensity[0] * p) * norm, (S.sun_intensity[1] * p) * norm, (S.sun_intensity[2] * p) * norm);
 }
 V3 env_fetch(const OracleScene& S, float u, float v) {
@@ -161,8 +174,8 @@ V3 env_fetch(const OracleScene& S, float u, float v) {
     return v3(o[0], o[1], o[2]);
 }
 V3 sky_image(const OracleScene& S, V3 dir) {
-    float u = atan2f(dir.z, dir.x) / TWO_PI + 0.5f;
-    float v = -asinf(dir.y) / PI + 0.5f;
+    float u = m_atan2(dir.z, dir.x) / TWO_PI + 0.5f;
+    float v = -m_asin(dir.y) / PI + 0.5f;
     V3 c = env_fetch(S, u, v);
     c = v3(std::min(c.x, 100000.0f), std::min(c.y, 100000.0f), std::min(c.z, 100000.0f));
     if (!S.env_image_linear && S.use_linear_rgb) c = v3(srgb_to_lin(c.x), srgb_to_lin(c.y), srgb_to_lin(c.z));
@@ -189,7 +202,7 @@ V3 oct_to_world(float u, float v) {
     float phi = 0.25f * PI * ((v - u) / r + 1.0f);
     if (r == 0.0f) phi = 0.0f;
     float r2 = r * r, s = sqrtf(2.0f - r2);
-    return v3(sx * cosf(phi) * r * s, sy * sinf(phi) * r * s, signf(1.0f - u - v) * (1.0f - r2));
+    return v3(sx * m_cos(phi) * r * s, sy * m_sin(phi) * r * s, signf(1.0f - u - v) * (1.0f - r2));
 }
 
 struct Pyramid {
@@ -285,7 +298,7 @@ struct Tracer {
         }
         return at_vox(ux, uy, uz);
     }
-    float free_path(Rng& r) const { return -logf(std::max(0.0000000001f, 1.0f - rnd(r))) * (1.0f / S.extinction); }
+    float free_path(Rng& r) const { return -m_log(std::max(0.0000000001f, 1.0f - rnd(r))) * (1.0f / S.extinction); }
     bool guard() { return ++steps > (1u << 24); }
     V3 sky(V3 d) const { return sky_and_sun(S, d); }
 
@@ -426,7 +439,7 @@ struct Tracer {
                 float t = 0.0f;
                 while (true) {
                     if (guard()) return 0.0f;
-                    t -= logf(std::max(0.0000000001f, 1.0f - rnd(r))) * (1.0f / S.extinction);
+                    t -= m_log(std::max(0.0000000001f, 1.0f - rnd(r))) * (1.0f / S.extinction);
                     if (t >= dmax) {
                         x = add(S.ess_ref_compat ? x : x0, mul(w, dmax));
                         break;
@@ -528,11 +541,11 @@ struct Tracer {
                 } else {
                     float mu_c = std::max(0.0000000001f, maj * mn);
                     float mu_r = std::max(0.0000000001f, maj * mx - mu_c);
-                    float t_c = -logf(std::max(0.0000000001f, 1.0f - rnd(r))) / mu_c;
+                    float t_c = -m_log(std::max(0.0000000001f, 1.0f - rnd(r))) / mu_c;
                     float t_r = 0.0f;
                     while (true) {
                         if (guard()) return v3(0, 0, 0);
-                        t_r -= logf(std::max(0.0000000001f, 1.0f - rnd(r))) / mu_r;
+                        t_r -= m_log(std::max(0.0000000001f, 1.0f - rnd(r))) / mu_r;
                         if (t_c >= dmax && t_r >= dmax) {
                             x = add(x, mul(w, dmax));
                             break;
@@ -551,7 +564,7 @@ struct Tracer {
                             if (S.max_bounces > 0 && ++bounces > S.max_bounces) return v3(0, 0, 0);
                             w = sample_phase(r, S.g, w);
                             t_r = 0.0f;
-                            t_c = -logf(std::max(0.0000000001f, 1.0f - rnd(r))) / mu_c;
+                            t_c = -m_log(std::max(0.0000000001f, 1.0f - rnd(r))) / mu_c;
                             ray_box(smin, smax, x, w, ts0, ts1);
                             dmax = ts1 - ts0;
                         }
@@ -566,19 +579,19 @@ struct Tracer {
     // residualRatioTrackingEstimator (ResidualRatioTracking.glsl:34-76)
     float rrt_est(V3 x, V3 w, float d0, float d1, float T, float& wsum, float& res_t, float& res_d, float mu_c,
                   float mu_r, Rng& r) {
-        float tc = expf(-mu_c * (d1 - d0));
+        float tc = m_exp(-mu_c * (d1 - d0));
         float tr = 1.0f;
         float dt = d0;
         while (true) {
             if (guard()) break;
-            float t = -logf(std::max(0.0000000001f, 1.0f - rnd(r))) / mu_r;
+            float t = -m_log(std::max(0.0000000001f, 1.0f - rnd(r))) / mu_r;
             x = add(x, mul(w, t));
             dt += t;
             if (dt >= d1) break;
             float dens = sample(x, r);
             float mu = S.extinction * dens;
             tr *= 1.0f - (mu - mu_c) / mu_r;
-            float tcl = expf(-mu_c * (dt - d0));
+            float tcl = m_exp(-mu_c * (dt - d0));
             float tl = (T * tr) * tcl;
             wsum += tl;
             float xi = rnd(r);
@@ -907,7 +920,7 @@ void oracle_rrt_params(const float* mn, const float* mx, const float* avg, int t
     for (int i = 0; i < total; i++) {
         float mu_min = mn[i] * extinction, mu_max = mx[i] * extinction, mu_avg = avg[i] * extinction;
         float mu_r = std::max(mu_max - mu_min, 0.1f);
-        float mu_c = mu_min + mu_r * powf(gamma, (1.0f / (D * mu_r)) - 1.0f);
+        float mu_c = mu_min + mu_r * m_pow(gamma, (1.0f / (D * mu_r)) - 1.0f);
         mu_c = std::min(std::max(mu_c, mu_min), mu_avg);
         out_pairs[2 * i] = mu_c;
         out_pairs[2 * i + 1] = mu_r;
@@ -949,8 +962,8 @@ void oracle_env_pyramid(const float* rgba, int w, int h, int levels, float* pyra
                 for (int j = 0; j < 5; j++) {
                     float syo = 0.1f + 0.2f * (float)j;
                     V3 dir = oct_to_world(((float)x + sxo) / (float)res, ((float)y + syo) / (float)res);
-                    float tu = atan2f(dir.z, dir.x) / (2.0f * PI) + 0.5f;
-                    float tv = -asinf(dir.y) / PI + 0.5f;
+                    float tu = m_atan2(dir.z, dir.x) / (2.0f * PI) + 0.5f;
+                    float tv = -m_asin(dir.y) / PI + 0.5f;
                     V3 c = env_fetch(S, tu, tv);
                     c = v3(std::min(c.x, 100000.0f), std::min(c.y, 100000.0f), std::min(c.z, 100000.0f));
                     best = std::max(best, length(c));
@@ -1031,6 +1044,8 @@ void oracle_eaw(const float* color, const float* pos, const float* nrm, int w, i
     }
     memcpy(out, a.data(), a.size() * sizeof(float));
 }
+
+void oracle_set_double_rounded_math(int on) { g_dr_math = on != 0; }
 
 void oracle_rng_stream(uint32_t seed, int n, float* out, uint32_t* st4) {
     Rng r = rng_init(seed);

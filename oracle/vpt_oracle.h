@@ -72,6 +72,9 @@ void oracle_eaw(const float* color, const float* pos, const float* nrm, int w, i
 
 /* Hybrid Tausworthe stream: n floats after seeding with `seed`. */
 void oracle_rng_stream(uint32_t seed, int n, float* out, uint32_t* out_state4);
+/* 1: evaluate the tracer's transcendentals in double precision, rounded once to float (the mode of
+ * the CUDA core's libvpt_b200_dr.so); 0 (default): the C library's float functions. */
+void oracle_set_double_rounded_math(int on);
 
 #ifdef __cplusplus
 }

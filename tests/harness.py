@@ -40,8 +40,8 @@ def supervoxel_size(nx, ny, nz, s=8):
 class Core:
     """One VptContext."""
 
-    def __init__(self, device=0):
-        self.lib = _lib.load()
+    def __init__(self, device=0, variant="default"):
+        self.lib = _lib.load(variant)
         c = ctypes.c_void_p()
         st = self.lib.vpt_create(ctypes.byref(c), device)
         if st != 0:
@@ -49,7 +49,7 @@ class Core:
         self.ctx = c.value
 
     def __call__(self, name, *args):
-        check(getattr(self.lib, name)(self.ctx, *args), name, self.ctx)
+        check(getattr(self.lib, name)(self.ctx, *args), name, self.ctx, self.lib)
 
     def close(self):
         if self.ctx:
@@ -116,28 +116,68 @@ def gpu_render(core: Core, sp: SceneSpec, frames: int, stats=True):
     return s, sq
 
 
+def _mat_mul(a, b):
+    """Column-major 4x4 product in double, summation order of the core's mat_mul."""
+    r = [0.0] * 16
+    for c in range(4):
+        for rr in range(4):
+            acc = 0.0
+            for k in range(4):
+                acc += a[k * 4 + rr] * b[c * 4 + k]
+            r[c * 4 + rr] = acc
+    return r
+
+
+def _mat_inverse(m):
+    """Gauss-Jordan with partial pivoting, operation for operation as the core's mat_inverse."""
+    a = [[m[c * 4 + r] for c in range(4)] + [1.0 if r == c else 0.0 for c in range(4)] for r in range(4)]
+    for col in range(4):
+        piv = col
+        for r in range(col + 1, 4):
+            if abs(a[r][col]) > abs(a[piv][col]):
+                piv = r
+        if piv != col:
+            a[piv], a[col] = a[col], a[piv]
+        inv = 1.0 / a[col][col]
+        a[col] = [v * inv for v in a[col]]
+        for r in range(4):
+            if r == col:
+                continue
+            f = a[r][col]
+            a[r] = [a[r][c] - f * a[col][c] for c in range(8)]
+    return [a[r][4 + c] for c in range(4) for r in range(4)]
+
+
 def camera_inv_view_proj(sp: SceneSpec):
-    """Same camera model as the core (vpt_set_camera): look-at view, perspective with depth in
-    [0, 1] and y flipped, computed in double, inverse rounded to float."""
-    e = np.array(sp.cam_pos, np.float64)
-    f = np.array(sp.cam_target, np.float64) - e
-    f /= np.linalg.norm(f)
-    s = np.cross(f, np.array([0.0, 1.0, 0.0]))
-    s /= np.linalg.norm(s)
-    u = np.cross(s, f)
-    view = np.array([[s[0], s[1], s[2], -s.dot(e)], [u[0], u[1], u[2], -u.dot(e)],
-                     [-f[0], -f[1], -f[2], f.dot(e)], [0, 0, 0, 1.0]])
-    th = math.tan(sp.fovy / 2.0)
-    aspect = sp.width / sp.height
-    n, fa = sp.near, sp.far
-    proj = np.zeros((4, 4))
-    proj[0, 0] = 1.0 / (aspect * th)
-    proj[1, 1] = -1.0 / th
-    proj[2, 2] = fa / (n - fa)
-    proj[3, 2] = -1.0
-    proj[2, 3] = -(fa * n) / (fa - n)
-    inv = np.linalg.inv(proj @ view)
-    return [float(np.float32(v)) for v in inv.T.reshape(-1)]  # column-major
+    """The core's camera (vpt_set_camera + compute_camera in vpt_context.cu) restated operation for
+    operation in IEEE double from the float32-rounded inputs: look-at view, perspective with depth in
+    [0, 1] and y flipped, Gauss-Jordan inverse, rounded to float.  Bit-identical to
+    vpt_get_camera_matrices for the same SceneSpec."""
+    f32 = lambda v: float(np.float32(v))  # noqa: E731
+    e = [f32(v) for v in sp.cam_pos]
+    t = [f32(v) for v in sp.cam_target]
+    up = [0.0, 1.0, 0.0]
+    f = [t[i] - e[i] for i in range(3)]
+    fl = math.sqrt(f[0] * f[0] + f[1] * f[1] + f[2] * f[2])
+    f = [v / fl for v in f]
+    s = [f[1] * up[2] - f[2] * up[1], f[2] * up[0] - f[0] * up[2], f[0] * up[1] - f[1] * up[0]]
+    sl = math.sqrt(s[0] * s[0] + s[1] * s[1] + s[2] * s[2])
+    s = [v / sl for v in s]
+    u = [s[1] * f[2] - s[2] * f[1], s[2] * f[0] - s[0] * f[2], s[0] * f[1] - s[1] * f[0]]
+    view = [s[0], u[0], -f[0], 0.0, s[1], u[1], -f[1], 0.0, s[2], u[2], -f[2], 0.0,
+            -(s[0] * e[0] + s[1] * e[1] + s[2] * e[2]), -(u[0] * e[0] + u[1] * e[1] + u[2] * e[2]),
+            (f[0] * e[0] + f[1] * e[1] + f[2] * e[2]), 1.0]
+    aspect = float(sp.width) / float(sp.height) if sp.width > 0 and sp.height > 0 else 1.0
+    th = math.tan(f32(sp.fovy) / 2.0)
+    n, fa = f32(sp.near), f32(sp.far)
+    proj = [0.0] * 16
+    proj[0] = 1.0 / (aspect * th)
+    proj[5] = -1.0 / th
+    proj[10] = fa / (n - fa)
+    proj[11] = -1.0
+    proj[14] = -(fa * n) / (fa - n)
+    inv = _mat_inverse(_mat_mul(proj, view))
+    return [f32(v) for v in inv]
 
 
 def oracle_scene(core, sp: SceneSpec, frames: int, frame_count: int = 0) -> bridge.Scene:

@@ -1,5 +1,7 @@
 """CPU tests of the C-ABI boundary: the library loads and exports every declared entry point."""
 import ctypes
+
+import pytest
 import os
 import re
 
@@ -19,8 +21,9 @@ def declared_functions():
     return sorted(set(names))
 
 
-def test_library_exports_every_declared_symbol():
-    lib = ctypes.CDLL(_lib.LIB_PATH)
+@pytest.mark.parametrize("path", [_lib.LIB_PATH, _lib.LIB_PATH_DR])
+def test_library_exports_every_declared_symbol(path):
+    lib = ctypes.CDLL(path)
     names = declared_functions()
     assert len(names) >= 40
     missing = [n for n in names if not hasattr(lib, n)]
