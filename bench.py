@@ -271,6 +271,10 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(lib, ctx, vpt)
 
+    sparse = None
+    if not args.no_sparse:
+        sparse = run_sparse(vpt, lib, ctx, stream, ctypes_stream, barrier, max_over_ranks, world)
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -286,11 +290,77 @@ def run_ours(args):
         }
         if cpu is not None:
             line["cpu_baseline"] = cpu
+        if sparse is not None:
+            line["sparse_nanovdb"] = sparse
         print(json.dumps(line), flush=True)
     vpt.cleanup()
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+# NanoVDB sparse configuration: 2048x1024x1536 virtual voxels, 8^3 leaves with ~12% of the leaf
+# slots active (seeded fBm cumulus, remap contrast 2, values below 0.85 empty), extinction 2000,
+# 1920x1080, max 256 bounces; delta tracking through the sparse volume and HDDA decomposition
+# tracking (the reference's sparse empty-space-skipping tracker), fp32 and fp16 leaf values.
+SPARSE_DIMS = (2048, 1024, 1536)
+SPARSE_RES = (1920, 1080)
+SPARSE_SPP_PER_STEP = 4
+SPARSE_EXTINCTION = 2000.0
+SPARSE_MAX_BOUNCES = 256
+SPARSE_SEED = 3
+
+
+def run_sparse(vpt, lib, ctx, stream, ctypes_stream, barrier, max_over_ranks, world, steps=2):
+    import ctypes
+    import torch
+
+    t0 = time.perf_counter()
+    vpt.set_max_grid_extent(0.5)
+    _lib_check = vpt._lib.check
+    _lib_check(lib.vpt_set_option(ctx, b"fbm_contrast", 2.0), "contrast", ctx)
+    vpt.generate_fbm_cloud(SPARSE_DIMS, seed=SPARSE_SEED, threshold=0.85)
+    _lib_check(lib.vpt_set_option(ctx, b"fbm_contrast", 3.5), "contrast", ctx)
+    vpt.set_use_sparse_grid(True)
+    info = vpt._sparse_info()
+    torch.cuda.synchronize()
+    build_s = time.perf_counter() - t0
+    slots = np.prod([math.ceil(n / 8) for n in SPARSE_DIMS])
+    vpt.set_extinction_scale(SPARSE_EXTINCTION)
+    vpt.set_max_bounces(SPARSE_MAX_BOUNCES)
+    w, h = SPARSE_RES
+    img = torch.zeros((4, h, w), dtype=torch.float32, device="cuda")
+    out = {"workload": f"NanoVDB-layout sparse grid {SPARSE_DIMS[0]}x{SPARSE_DIMS[1]}x{SPARSE_DIMS[2]} virtual voxels, "
+                       f"{w}x{h}, {SPARSE_SPP_PER_STEP} spp/step, extinction {SPARSE_EXTINCTION:g}, "
+                       f"max {SPARSE_MAX_BOUNCES} bounces",
+           "leaves": int(info.leaves), "leaf_occupancy": float(info.leaves) / float(slots),
+           "device_bytes": int(info.device_bytes), "build_s": build_s, "trackers": {}}
+    for fp16 in (False, True):
+        if fp16:
+            vpt.set_sparse_grid_fp16(True)
+            vpt.set_use_sparse_grid(True)
+            out["device_bytes_fp16"] = int(vpt._sparse_info().device_bytes)
+        for name, mode in (("delta", 0), ("decomposition_hdda", 3)):
+            vpt.set_vpt_mode(mode)
+            vpt.render_frame(img, 1)
+            barrier()
+            vpt.reset_stats()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(steps):
+                _lib_check(lib.vpt_render_frames(ctx, SPARSE_SPP_PER_STEP, ctypes_stream), "render", ctx)
+            e1.record(stream)
+            barrier()
+            ms = max_over_ranks(e0.elapsed_time(e1))
+            st = vpt.get_stats()
+            key = name + ("_fp16" if fp16 else "")
+            out["trackers"][key] = {"path_samples_per_s": w * h * SPARSE_SPP_PER_STEP * steps * world / (ms / 1e3),
+                                    "lookups_per_path": st["density_lookups"] / max(1, st["paths"]),
+                                    "lookups_per_s": st["density_lookups"] * world / (ms / 1e3),
+                                    "ms_per_step": ms / steps}
+    vpt.set_sparse_grid_fp16(False)
+    vpt.set_use_sparse_grid(False)
+    return out
 
 
 def cpu_baseline(lib, ctx, vpt, target_s=12.0):
@@ -398,6 +468,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-sparse", action="store_true", help="skip the NanoVDB sparse configuration")
     ap.add_argument("--workload", choices=["full", "small"], default="full",
                     help="small: 384^3 grid, 512^2, 4 spp/step (for ncu captures; not a bench line)")
     args = ap.parse_args()
@@ -407,6 +478,8 @@ def main():
         global GRID, RES, SPP_PER_STEP, TRACKER_SPP
         GRID, RES, SPP_PER_STEP, TRACKER_SPP = 384, 512, 4, 1
         args.no_cpu_baseline = True
+        global SPARSE_DIMS, SPARSE_RES
+        SPARSE_DIMS, SPARSE_RES = (512, 256, 384), (480, 270)
     if args.impl == "reference":
         run_reference(args)
     else:

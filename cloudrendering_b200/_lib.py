@@ -82,9 +82,23 @@ SIGNATURES = {
     "vpt_build_environment_pyramid": (c_int, [c_void_p, c_int, c_int, c_int, c_void_p, c_void_p]),
     "vpt_eaw_denoise_rgba": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_float, c_float, c_float,
                                      c_int, c_void_p, c_void_p]),
+    "vpt_set_use_sparse_grid": (c_int, [c_void_p, c_int]),
+    "vpt_set_nanovdb_grid": (c_int, [c_void_p, c_void_p, ctypes.c_size_t, c_int]),
+    "vpt_get_sparse_grid_info": (c_int, [c_void_p, c_void_p]),
+    "vpt_sparse_query": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p]),
     "vpt_eaw_denoise_rgba_noalloc": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_float, c_float,
                                              c_float, c_int, c_void_p, c_void_p]),
 }
+
+class VptSparseInfo(ctypes.Structure):
+    _fields_ = [("leaves", ctypes.c_uint64), ("tiles", ctypes.c_uint64), ("device_bytes", ctypes.c_uint64),
+                ("table_origin", ctypes.c_int32 * 3), ("table_dim", ctypes.c_int32 * 3),
+                ("root_min", ctypes.c_int32 * 3), ("root_max", ctypes.c_int32 * 3),
+                ("box_min", c_float * 3), ("box_max", c_float * 3),
+                ("world_min", ctypes.c_double * 3), ("world_max", ctypes.c_double * 3),
+                ("voxel_size", ctypes.c_double * 3),
+                ("fp16", ctypes.c_int32), ("lowest_level", ctypes.c_int32)]
+
 
 _libs: dict = {}
 

@@ -15,6 +15,7 @@
 #include "vpt_kernels.h"
 #include "vpt_params.h"
 #include "vpt_denoise.h"
+#include "vpt_sparse.h"
 
 using vpt::F3;
 
@@ -139,6 +140,7 @@ struct VptContext {
     int schedule = vpt::kScheduleRefill;
     int persistent_blocks_per_sm = 0;  // 0 = occupancy calculator (one resident wave)
     uint32_t max_steps = vpt::kMaxStepsPerPath;
+    float fbm_contrast = 3.5f;  // remap of the fBm generator: clamp(0.5 + contrast * fbm, 0, 1)
 
     // dense grid
     int nx = 0, ny = 0, nz = 0;
@@ -146,6 +148,18 @@ struct VptContext {
     float box_min[3] = {0, 0, 0}, box_max[3] = {0, 0, 0};
     DevBuf<float> raw, norm;
     DevBuf<float> minmax;
+
+    // sparse (NanoVDB) volume: built from the dense grid when use_sparse is set
+    // (VolumetricPathTracingPass::setUseSparseGrid -> CloudData::getSparseDensityField) or loaded
+    // from a NanoVDB buffer (CloudData::loadFromNvdbFile)
+    bool use_sparse = false;
+    bool sparse_valid = false;
+    bool sparse_from_dense = true;
+    bool sparse_fp16 = false;
+    int sparse_grid_size[3] = {0, 0, 0};   // gridSizeX/Y/Z of the reference's CloudData
+    float sparse_box_min[3] = {0, 0, 0}, sparse_box_max[3] = {0, 0, 0};
+    vpt::SparseHost sparse_host;
+    vpt::SparseDevice sparse_dev;
 
     // acceleration structures (rebuilt lazily)
     int sv_size = 8, svx = 0, svy = 0, svz = 0;
@@ -269,7 +283,60 @@ VptStatus finish_grid(VptContext* ctx, cudaStream_t s) {
     VPT_CHECK_CUDA(ctx, cudaStreamSynchronize(s));
     compute_bounds(ctx);
     invalidate_accel(ctx);
+    ctx->sparse_valid = false;  // a sparse volume is rebuilt from the new dense grid on demand
+    ctx->sparse_from_dense = true;
     reset_film_state(ctx);
+    return VPT_OK;
+}
+
+// Render box of a sparse volume (CloudData::computeSparseGridMetadata, CloudData.cpp:1289-1357):
+// the grid's world box itself when it was built from the dense grid, otherwise the world box fitted
+// into [-maxGridExtent, maxGridExtent] along its longest side (float arithmetic as glm::vec3).
+void compute_sparse_box(VptContext* ctx) {
+    const vpt::SparseHost& h = ctx->sparse_host;
+    float wmin[3], wmax[3];
+    for (int i = 0; i < 3; i++) {
+        wmin[i] = float(h.world_min[i]);
+        wmax[i] = float(h.world_max[i]);
+    }
+    if (ctx->sparse_from_dense) {
+        for (int i = 0; i < 3; i++) {
+            ctx->sparse_box_min[i] = wmin[i];
+            ctx->sparse_box_max[i] = wmax[i];
+        }
+        return;
+    }
+    float diff[3] = {wmax[0] - wmin[0], wmax[1] - wmin[1], wmax[2] - wmin[2]};
+    float max_dim = std::max(diff[0], std::max(diff[1], diff[2]));
+    float A = 2.0f * ctx->max_grid_extent / max_dim;
+    for (int i = 0; i < 3; i++) {
+        float L = diff[i] / max_dim;
+        float B = ctx->max_grid_extent * L - wmax[i] * A;
+        ctx->sparse_box_min[i] = A * wmin[i] + B;
+        ctx->sparse_box_max[i] = A * wmax[i] + B;
+    }
+}
+
+// Builds the sparse volume from the normalised dense grid as CloudData::getSparseDensityField does
+// (CloudData.cpp:1385-1407): voxel size (boxMax.x - boxMin.x) / gridSizeX, origin boxMin.
+VptStatus ensure_sparse(VptContext* ctx, cudaStream_t s) {
+    if (ctx->sparse_valid) return VPT_OK;
+    if (!ctx->norm.ptr) return fail(ctx, VPT_ERR_STATE, "no volume loaded");
+    const double dx = double(ctx->box_max[0] - ctx->box_min[0]) / double(ctx->nx);
+    const double origin[3] = {ctx->box_min[0], ctx->box_min[1], ctx->box_min[2]};
+    std::string err;
+    cudaError_t e = vpt::build_sparse_from_dense(ctx->norm.ptr, ctx->nx, ctx->ny, ctx->nz, dx, origin,
+                                                 ctx->sparse_fp16, ctx->sparse_host, ctx->sparse_dev, s, err);
+    if (e != cudaSuccess) {
+        if (!err.empty()) return fail(ctx, VPT_ERR_UNSUPPORTED, err);
+        return cuda_fail(ctx, e, "build_sparse_from_dense");
+    }
+    ctx->sparse_valid = true;
+    ctx->sparse_from_dense = true;
+    ctx->sparse_grid_size[0] = ctx->nx;
+    ctx->sparse_grid_size[1] = ctx->ny;
+    ctx->sparse_grid_size[2] = ctx->nz;
+    compute_sparse_box(ctx);
     return VPT_OK;
 }
 
@@ -300,6 +367,12 @@ void supervoxel_dims(VptContext* ctx) {
 float extinction_x(const VptContext* ctx) { return ctx->extinction_base[0] * ctx->extinction_scale; }
 
 VptStatus ensure_accel(VptContext* ctx, int tracker, cudaStream_t s) {
+    if (ctx->use_sparse) {
+        if (tracker == vpt::kResidualRatio || (tracker == vpt::kNextEvent && ctx->use_ess))
+            return fail(ctx, VPT_ERR_UNSUPPORTED,
+                        "residual ratio tracking and empty space skipping need a dense grid (as in the reference)");
+        return ensure_sparse(ctx, s);
+    }
     const bool need_sv = tracker == vpt::kDecomposition || tracker == vpt::kResidualRatio;
     const bool need_occ = tracker == vpt::kNextEvent && ctx->use_ess;
     if (need_sv) {
@@ -451,6 +524,17 @@ VptStatus fill_params(VptContext* ctx, int tracker, int frames, vpt::TraceParams
     P.counters = ctx->counters.ptr;
     P.error_flags = ctx->error_flags.ptr;
     P.work_counter = ctx->work_counter.ptr;
+    P.grid_kind = vpt::kDense;
+    if (ctx->use_sparse && ctx->sparse_valid) {
+        // superVoxelSize 8 (leaf level) unless the grid is smaller than a leaf
+        // (VolumetricPathTracingPass.cpp:2071-2076)
+        const int* gs = ctx->sparse_grid_size;
+        const int lowest = (gs[0] >= 8 && gs[1] >= 8 && gs[2] >= 8) ? 8 : 1;
+        P.grid_kind = vpt::kNanoVdb;
+        P.sparse = vpt::make_sparse_view(ctx->sparse_host, ctx->sparse_dev, lowest);
+        P.box_min = mk(ctx->sparse_box_min[0], ctx->sparse_box_min[1], ctx->sparse_box_min[2]);
+        P.box_max = mk(ctx->sparse_box_max[0], ctx->sparse_box_max[1], ctx->sparse_box_max[2]);
+    }
     (void)tracker;
     return VPT_OK;
 }
@@ -543,6 +627,7 @@ void vpt_destroy(VptContext* ctx) {
     cudaDeviceSynchronize();
     ctx->raw.release();
     ctx->norm.release();
+    ctx->sparse_dev.release();
     ctx->minmax.release();
     ctx->sv_min.release();
     ctx->sv_max.release();
@@ -600,7 +685,7 @@ VptStatus vpt_generate_fbm_grid(VptContext* ctx, int nx, int ny, int nz, uint32_
     fp.gain = gain;
     fp.base_frequency = base_frequency;
     fp.threshold = threshold;
-    fp.contrast = 3.5f;  // 0.5 + 3.5 * fbm, clamped: ~35% of voxels below 0.3 at base frequency 3
+    fp.contrast = ctx->fbm_contrast;  // 0.5 + 3.5 * fbm by default: ~35% of voxels below 0.3 at frequency 3
     fp.inv_max_dim = 1.0f / float(std::max(nx, std::max(ny, nz)));
     VPT_CHECK_CUDA(ctx, vpt::launch_fbm(ctx->raw.ptr, nx, ny, nz, perm, fp, 0));
     ctx->nx = nx;
@@ -638,10 +723,112 @@ VptStatus vpt_set_max_grid_extent(VptContext* ctx, float e) {
 VptStatus vpt_get_render_bounding_box(VptContext* ctx, float out[6]) {
     VPT_CHECK_CTX(ctx);
     if (!out) return VPT_ERR_ARG;
-    for (int i = 0; i < 3; i++) {
-        out[i] = ctx->box_min[i];
-        out[3 + i] = ctx->box_max[i];
+    if (ctx->use_sparse) {
+        VptStatus st = ensure_sparse(ctx, nullptr);
+        if (st != VPT_OK) return st;
     }
+    for (int i = 0; i < 3; i++) {
+        out[i] = ctx->use_sparse ? ctx->sparse_box_min[i] : ctx->box_min[i];
+        out[3 + i] = ctx->use_sparse ? ctx->sparse_box_max[i] : ctx->box_max[i];
+    }
+    return VPT_OK;
+}
+
+VptStatus vpt_set_use_sparse_grid(VptContext* ctx, int use_sparse) {
+    VPT_CHECK_CTX(ctx);
+    bool u = use_sparse != 0;
+    if (!u && ctx->use_sparse && !ctx->norm.ptr)
+        return fail(ctx, VPT_ERR_UNSUPPORTED, "the loaded NanoVDB grid has no dense counterpart in this core");
+    if (u != ctx->use_sparse) reset_film_state(ctx);
+    ctx->use_sparse = u;
+    return VPT_OK;
+}
+
+VptStatus vpt_set_nanovdb_grid(VptContext* ctx, const void* buffer, size_t bytes, int on_device) {
+    VPT_CHECK_CTX(ctx);
+    if (!buffer || bytes == 0) return fail(ctx, VPT_ERR_ARG, "vpt_set_nanovdb_grid: empty buffer");
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = nullptr;
+    std::vector<uint8_t> host;
+    const uint8_t* hb = static_cast<const uint8_t*>(buffer);
+    if (on_device) {
+        host.resize(bytes);
+        VPT_CHECK_CUDA(ctx, cudaMemcpy(host.data(), buffer, bytes, cudaMemcpyDeviceToHost));
+        hb = host.data();
+    }
+    vpt::SparseHost h;
+    std::string err;
+    if (!vpt::parse_nanovdb(hb, bytes, h, err)) return fail(ctx, VPT_ERR_ARG, "vpt_set_nanovdb_grid: " + err);
+    const uint8_t* db = static_cast<const uint8_t*>(buffer);
+    uint8_t* tmp = nullptr;
+    if (!on_device) {
+        VPT_CHECK_CUDA(ctx, cudaMalloc(reinterpret_cast<void**>(&tmp), bytes));
+        cudaError_t e = cudaMemcpy(tmp, buffer, bytes, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) {
+            cudaFree(tmp);
+            return cuda_fail(ctx, e, "vpt_set_nanovdb_grid upload");
+        }
+        db = tmp;
+    }
+    cudaError_t e = vpt::upload_sparse_from_nanovdb(h, db, ctx->sparse_fp16, ctx->sparse_dev, s);
+    if (tmp) cudaFree(tmp);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "upload_sparse_from_nanovdb");
+    ctx->sparse_host = std::move(h);
+    // the NanoVDB grid replaces the dense grid (CloudData::setNanoVdbGridHandle)
+    ctx->raw.release();
+    ctx->norm.release();
+    invalidate_accel(ctx);
+    ctx->use_sparse = true;
+    ctx->sparse_valid = true;
+    ctx->sparse_from_dense = false;
+    for (int i = 0; i < 3; i++) {
+        const int lo = ctx->sparse_host.root_min[i], hi = ctx->sparse_host.root_max[i];
+        ctx->sparse_grid_size[i] = hi >= lo ? hi - lo + 1 : 0;
+    }
+    compute_sparse_box(ctx);
+    reset_film_state(ctx);
+    return VPT_OK;
+}
+
+VptStatus vpt_get_sparse_grid_info(VptContext* ctx, VptSparseInfo* out) {
+    VPT_CHECK_CTX(ctx);
+    if (!out) return VPT_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    VptStatus st = ensure_sparse(ctx, nullptr);
+    if (st != VPT_OK) return st;
+    const vpt::SparseHost& h = ctx->sparse_host;
+    memset(out, 0, sizeof(*out));
+    out->leaves = h.leaf_count();
+    out->tiles = h.tiles.size();
+    out->device_bytes = ctx->sparse_dev.bytes;
+    for (int i = 0; i < 3; i++) {
+        out->table_origin[i] = h.tbl_origin[i];
+        out->table_dim[i] = h.tbl_dim[i];
+        out->root_min[i] = h.root_min[i];
+        out->root_max[i] = h.root_max[i];
+        out->box_min[i] = ctx->sparse_box_min[i];
+        out->box_max[i] = ctx->sparse_box_max[i];
+        out->world_min[i] = h.world_min[i];
+        out->world_max[i] = h.world_max[i];
+        out->voxel_size[i] = h.voxel_size[i];
+    }
+    out->fp16 = ctx->sparse_dev.values_h ? 1 : 0;
+    const int* gs = ctx->sparse_grid_size;
+    out->lowest_level = (gs[0] >= 8 && gs[1] >= 8 && gs[2] >= 8) ? 8 : 1;
+    return VPT_OK;
+}
+
+VptStatus vpt_sparse_query(VptContext* ctx, const int32_t* ijk, int count, float* values, uint32_t* dims,
+                           uint8_t* active, void* stream) {
+    VPT_CHECK_CTX(ctx);
+    if (!ijk || count < 0 || !values || !dims || !active) return VPT_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = as_stream(stream);
+    VptStatus st = ensure_sparse(ctx, s);
+    if (st != VPT_OK) return st;
+    if (count == 0) return VPT_OK;
+    vpt::SparseView v = vpt::make_sparse_view(ctx->sparse_host, ctx->sparse_dev, 8);
+    VPT_CHECK_CUDA(ctx, vpt::launch_sparse_query(v, ijk, count, values, dims, active, s));
     return VPT_OK;
 }
 
@@ -849,7 +1036,7 @@ VptStatus vpt_reset_accumulation(VptContext* ctx) {
 VptStatus vpt_render_frames(VptContext* ctx, int frames, void* stream) {
     VPT_CHECK_CTX(ctx);
     if (frames <= 0) return fail(ctx, VPT_ERR_ARG, "frames must be > 0");
-    if (!ctx->norm.ptr) return fail(ctx, VPT_ERR_STATE, "no volume loaded");
+    if (!ctx->norm.ptr && !(ctx->use_sparse && ctx->sparse_valid)) return fail(ctx, VPT_ERR_STATE, "no volume loaded");
     if (ctx->width <= 0) return fail(ctx, VPT_ERR_STATE, "resolution not set");
     int tracker = tracker_of(ctx->mode);
     if (tracker < 0) return fail(ctx, VPT_ERR_UNSUPPORTED, "VptMode not built in this core");
@@ -1087,6 +1274,14 @@ VptStatus vpt_set_option(VptContext* ctx, const char* key, double value) {
     } else if (k == "max_steps_per_path") {
         if (value < 1 || value > 4294967295.0) return fail(ctx, VPT_ERR_ARG, "max_steps_per_path out of range");
         ctx->max_steps = (uint32_t)value;
+    } else if (k == "fbm_contrast") {
+        if (!(value > 0.0)) return fail(ctx, VPT_ERR_ARG, "fbm_contrast must be > 0");
+        ctx->fbm_contrast = float(value);
+    } else if (k == "sparse_fp16") {
+        bool v = int(value) != 0;
+        if (v != ctx->sparse_fp16 && ctx->sparse_from_dense) ctx->sparse_valid = false;
+        ctx->sparse_fp16 = v;
+        reset_film_state(ctx);
     } else if (k == "ess_ref_compat") {
         ctx->ess_ref_compat = int(value) ? 1 : 0;
         ctx->occ_valid = false;

@@ -21,11 +21,20 @@ static unsigned long long g_launches = 0;
 void count_launches(unsigned n) { __atomic_fetch_add(&g_launches, (unsigned long long)n, __ATOMIC_RELAXED); }
 unsigned long long launch_count() { return __atomic_load_n(&g_launches, __ATOMIC_RELAXED); }
 
-template <int INTERP>
-struct DenseSampler {
+// Density access of the trackers: the dense texture or the sparse (NanoVDB) volume.
+template <int INTERP, int GRID>
+struct Sampler {
     const TraceParams& P;
-    VPT_DEV float operator()(F3 pos, Rng& rng) const { return sample_dense<INTERP>(P, pos, rng); }
-    VPT_DEV F3 normal(F3 pos, Rng& rng) const { return density_normal<INTERP>(P, pos, rng); }
+    static constexpr bool kSparse = GRID == kNanoVdb;
+    VPT_DEV float operator()(F3 pos, Rng& rng) const {
+        if constexpr (GRID == kNanoVdb) return sample_sparse<INTERP>(P, pos, rng);
+        else return sample_dense<INTERP>(P, pos, rng);
+    }
+    VPT_DEV F3 normal(F3 pos, Rng& rng) const {
+        // getCloudFiniteDifference returns 0 for NanoVDB grids (VptUtils.glsl:726-729)
+        if constexpr (GRID == kNanoVdb) return f3(0.0f, 0.0f, 0.0f);
+        else return density_normal<INTERP>(P, pos, rng);
+    }
 };
 
 // Per-path feature accumulation (Clouds.glsl:195-256): position of the first event, depth,
@@ -59,7 +68,10 @@ template <int TRACKER, class S>
 VPT_DEV F3 run_tracker(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, FirstEvent& fe, PathCtx& pc) {
     if (TRACKER == kDelta) return track_delta(P, sample, rng, x, w, fe, pc);
     if (TRACKER == kRatio) return track_ratio(P, sample, rng, x, w, fe, pc);
-    if (TRACKER == kDecomposition) return track_decomposition(P, sample, rng, x, w, fe, pc);
+    if constexpr (TRACKER == kDecomposition) {
+        if constexpr (S::kSparse) return track_decomposition_sparse(P, sample, rng, x, w, fe, pc);
+        else return track_decomposition(P, sample, rng, x, w, fe, pc);
+    }
     if (TRACKER == kResidualRatio) return track_residual_ratio(P, sample, rng, x, w, fe, pc);
     if (TRACKER == kNextEvent + 100) return track_nee<true>(P, sample, rng, x, w, fe, pc);
     return track_nee<false>(P, sample, rng, x, w, fe, pc);
@@ -130,9 +142,9 @@ VPT_DEV void flush_counters(const TraceParams& P, uint32_t paths, uint32_t looku
     if (guard_hit) atomicOr(P.error_flags, kErrIterLimit);
 }
 
-template <int TRACKER, int INTERP>
+template <int TRACKER, int INTERP, int GRID>
 __global__ void __launch_bounds__(kTraceBlock) trace_tiles_kernel(const __grid_constant__ TraceParams P, int features) {
-    DenseSampler<INTERP> sample{P};
+    Sampler<INTERP, GRID> sample{P};
     uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t frame;
     int px, py;
@@ -146,10 +158,10 @@ __global__ void __launch_bounds__(kTraceBlock) trace_tiles_kernel(const __grid_c
     flush_counters(P, paths, lookups, guard_hit);
 }
 
-template <int TRACKER, int INTERP>
+template <int TRACKER, int INTERP, int GRID>
 __global__ void __launch_bounds__(kTraceBlock) trace_persistent_kernel(const __grid_constant__ TraceParams P,
                                                                        int features, uint64_t total) {
-    DenseSampler<INTERP> sample{P};
+    Sampler<INTERP, GRID> sample{P};
     const int lane = threadIdx.x & 31;
     uint32_t lookups = 0, paths = 0;
     bool guard_hit = false;
@@ -215,9 +227,9 @@ VPT_DEV void end_shadow(const TraceParams& P, F3& color, F3& x, F3& w, float& d,
     }
 }
 
-template <int TRACKER, int INTERP>
+template <int TRACKER, int INTERP, int GRID>
 __global__ void __launch_bounds__(kTraceBlock) trace_refill_kernel(const __grid_constant__ TraceParams P, uint64_t total) {
-    DenseSampler<INTERP> sample{P};
+    Sampler<INTERP, GRID> sample{P};
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const unsigned lt_mask = (1u << lane) - 1u;
@@ -387,12 +399,12 @@ uint64_t padded_paths(int width, int height, uint32_t frames) {
     return tiles * 256ull * frames;
 }
 
-template <int TRACKER, int INTERP>
+template <int TRACKER, int INTERP, int GRID>
 static int refill_blocks(int requested) {
     if (requested > 0) return requested;
     static int per_sm = 0;
     if (per_sm == 0) {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_refill_kernel<TRACKER, INTERP>, kTraceBlock, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_refill_kernel<TRACKER, INTERP, GRID>, kTraceBlock, 0);
         if (per_sm <= 0) per_sm = 1;
     }
     int dev = 0, sms = 148;
@@ -401,16 +413,16 @@ static int refill_blocks(int requested) {
     return per_sm * sms;
 }
 
-template <int TRACKER, int INTERP>
+template <int TRACKER, int INTERP, int GRID>
 static cudaError_t launch_trace_t(const TraceParams& P, int schedule, int features, int persistent_blocks,
                                   cudaStream_t stream) {
     uint64_t total = padded_paths(P.width, P.height, P.num_frames);
     constexpr bool kRefillable = TRACKER == kDelta || TRACKER == kRatio || TRACKER == kNextEvent;
     if (schedule == kScheduleRefill && kRefillable && !features) {
         if constexpr (kRefillable) {
-            int blocks = refill_blocks<TRACKER, INTERP>(persistent_blocks);
+            int blocks = refill_blocks<TRACKER, INTERP, GRID>(persistent_blocks);
             cudaMemsetAsync(P.work_counter, 0, sizeof(unsigned long long), stream);
-            trace_refill_kernel<TRACKER, INTERP><<<blocks, kTraceBlock, 0, stream>>>(P, total);
+            trace_refill_kernel<TRACKER, INTERP, GRID><<<blocks, kTraceBlock, 0, stream>>>(P, total);
             count_launches(1);
             return cudaGetLastError();
         }
@@ -418,14 +430,14 @@ static cudaError_t launch_trace_t(const TraceParams& P, int schedule, int featur
     if (schedule == kScheduleRefill) schedule = kSchedulePersistent;
     if (schedule == kScheduleTiles) {
         uint64_t blocks = (total + kTraceBlock - 1) / kTraceBlock;
-        trace_tiles_kernel<TRACKER, INTERP><<<(unsigned)blocks, kTraceBlock, 0, stream>>>(P, features);
+        trace_tiles_kernel<TRACKER, INTERP, GRID><<<(unsigned)blocks, kTraceBlock, 0, stream>>>(P, features);
         count_launches(1);
     } else {
         if (persistent_blocks <= 0) {
             // one wave of resident blocks: SMs x blocks per SM from the occupancy calculator
             static int per_sm = 0;
             if (per_sm == 0) {
-                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_persistent_kernel<TRACKER, INTERP>,
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_persistent_kernel<TRACKER, INTERP, GRID>,
                                                               kTraceBlock, 0);
                 if (per_sm <= 0) per_sm = 1;
             }
@@ -435,33 +447,69 @@ static cudaError_t launch_trace_t(const TraceParams& P, int schedule, int featur
             persistent_blocks = per_sm * sms;
         }
         cudaMemsetAsync(P.work_counter, 0, sizeof(unsigned long long), stream);
-        trace_persistent_kernel<TRACKER, INTERP><<<persistent_blocks, kTraceBlock, 0, stream>>>(P, features, total);
+        trace_persistent_kernel<TRACKER, INTERP, GRID><<<persistent_blocks, kTraceBlock, 0, stream>>>(P, features, total);
         count_launches(1);
     }
     return cudaGetLastError();
 }
 
-template <int TRACKER>
+template <int TRACKER, int GRID>
 static cudaError_t launch_interp(const TraceParams& P, int schedule, int features, int pb, cudaStream_t s) {
     switch (P.interp) {
-        case kNearest: return launch_trace_t<TRACKER, kNearest>(P, schedule, features, pb, s);
-        case kStochastic: return launch_trace_t<TRACKER, kStochastic>(P, schedule, features, pb, s);
-        default: return launch_trace_t<TRACKER, kTrilinear>(P, schedule, features, pb, s);
+        case kNearest: return launch_trace_t<TRACKER, kNearest, GRID>(P, schedule, features, pb, s);
+        case kStochastic: return launch_trace_t<TRACKER, kStochastic, GRID>(P, schedule, features, pb, s);
+        default: return launch_trace_t<TRACKER, kTrilinear, GRID>(P, schedule, features, pb, s);
     }
 }
 
 cudaError_t launch_trace(const TraceParams& P, int tracker, int use_ess, int schedule, int features,
                          int persistent_blocks, cudaStream_t stream) {
+    if (P.grid_kind == kNanoVdb) {
+        // sparse grids: the trackers whose density access goes through sampleCloud, and the HDDA
+        // decomposition tracker; residual ratio tracking and the occupancy grid are dense-only in the
+        // reference (VolumetricPathTracingPass.cpp:1171-1186)
+        switch (tracker) {
+            case kDelta: return launch_interp<kDelta, kNanoVdb>(P, schedule, features, persistent_blocks, stream);
+            case kRatio: return launch_interp<kRatio, kNanoVdb>(P, schedule, features, persistent_blocks, stream);
+            case kDecomposition:
+                return launch_interp<kDecomposition, kNanoVdb>(P, schedule, features, persistent_blocks, stream);
+            case kNextEvent:
+                if (use_ess) return cudaErrorNotSupported;
+                return launch_interp<kNextEvent, kNanoVdb>(P, schedule, features, persistent_blocks, stream);
+            default: return cudaErrorNotSupported;
+        }
+    }
     switch (tracker) {
-        case kDelta: return launch_interp<kDelta>(P, schedule, features, persistent_blocks, stream);
-        case kRatio: return launch_interp<kRatio>(P, schedule, features, persistent_blocks, stream);
-        case kDecomposition: return launch_interp<kDecomposition>(P, schedule, features, persistent_blocks, stream);
-        case kResidualRatio: return launch_interp<kResidualRatio>(P, schedule, features, persistent_blocks, stream);
+        case kDelta: return launch_interp<kDelta, kDense>(P, schedule, features, persistent_blocks, stream);
+        case kRatio: return launch_interp<kRatio, kDense>(P, schedule, features, persistent_blocks, stream);
+        case kDecomposition: return launch_interp<kDecomposition, kDense>(P, schedule, features, persistent_blocks, stream);
+        case kResidualRatio: return launch_interp<kResidualRatio, kDense>(P, schedule, features, persistent_blocks, stream);
         case kNextEvent:
-            if (use_ess) return launch_interp<kNextEvent + 100>(P, schedule, features, persistent_blocks, stream);
-            return launch_interp<kNextEvent>(P, schedule, features, persistent_blocks, stream);
+            if (use_ess) return launch_interp<kNextEvent + 100, kDense>(P, schedule, features, persistent_blocks, stream);
+            return launch_interp<kNextEvent, kDense>(P, schedule, features, persistent_blocks, stream);
         default: return cudaErrorInvalidValue;
     }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Sparse volume queries (accessor checks against the reference's PNanoVDB).
+
+__global__ void sparse_query_kernel(const __grid_constant__ SparseView v, const int* __restrict__ ijk, int count,
+                                    float* __restrict__ values, uint32_t* __restrict__ dims,
+                                    uint8_t* __restrict__ active) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const int x = ijk[3 * i], y = ijk[3 * i + 1], z = ijk[3 * i + 2];
+    values[i] = sparse_value(v, x, y, z);
+    dims[i] = (uint32_t)sparse_dim(v, x, y, z);
+    active[i] = sparse_is_active(v, x, y, z) ? 1 : 0;
+}
+
+cudaError_t launch_sparse_query(const SparseView& v, const int* ijk, int count, float* values, uint32_t* dims,
+                                uint8_t* active, cudaStream_t s) {
+    sparse_query_kernel<<<(count + 255) / 256, 256, 0, s>>>(v, ijk, count, values, dims, active);
+    count_launches(1);
+    return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------------------------------

@@ -34,6 +34,9 @@ cudaError_t launch_supervoxel_stats(const float* dens, int nx, int ny, int nz, i
 cudaError_t launch_rrt_params(const float* mn, const float* mx, const float* avg, int total, float extinction,
                               float D, float* out_pairs, cudaStream_t s);
 cudaError_t launch_interleave(const float* a, const float* b, int total, float* out_pairs, cudaStream_t s);
+// Value, get_dim and is_active of a sparse volume at `count` index-space voxels (device arrays).
+cudaError_t launch_sparse_query(const SparseView& v, const int* ijk, int count, float* values, uint32_t* dims,
+                                uint8_t* active, cudaStream_t s);
 cudaError_t launch_occupancy(const float* dens, int nx, int ny, int nz, int bs, int gx, int gy, int gz, int halo,
                              float threshold, int ref_compat, uint8_t* out, cudaStream_t s);
 cudaError_t launch_env_pyramid(const TraceParams& P, float* pyramid, const uint64_t* level_offsets_host, int levels,

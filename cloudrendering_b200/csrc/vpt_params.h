@@ -46,6 +46,10 @@ struct SparseTile {
 // with one 32-bit entry per 8^3 brick of the root's bounding box: bit 31 clear = index of a leaf in
 // the leaf pools, bit 31 set = index into `tiles`.  Bricks outside the table are background.
 constexpr uint32_t kSparseTileBit = 0x80000000u;
+// Root tiles (4096^3 regions) known to the view, for voxels outside the brick table: inside a root
+// tile with an upper node such a voxel lies in an inactive upper-node tile (dim 128, background
+// value); inside a root tile without child it takes the tile; elsewhere it is background.
+constexpr int kSparseMaxRootTiles = 8;
 struct SparseView {
     float mat[9];              // index -> world (Map::mMatF, row-major as PNanoVDB applies it)
     float inv_mat[9];          // world -> index (Map::mInvMatF)
@@ -57,6 +61,11 @@ struct SparseView {
     int lowest_level;          // HDDA cell size of the decomposition tracker: 8 (leaves) or 1 (voxels)
     int fp16;                  // leaf values stored as IEEE half
     float background;
+    int root_tiles;                                  // entries used below
+    int rt_origin[kSparseMaxRootTiles][3];
+    int rt_child[kSparseMaxRootTiles];               // 1: the tile holds an upper node
+    float rt_value[kSparseMaxRootTiles];
+    int rt_active[kSparseMaxRootTiles];
     const uint32_t* table;
     const float* values;            // 512 floats per leaf, NanoVDB voxel order ((x&7)<<6 | (y&7)<<3 | (z&7))
     const unsigned short* values_h; // the same as half (fp16 variant)

@@ -164,6 +164,7 @@ bool parse_nanovdb(const uint8_t* b, size_t bytes, SparseHost& h, std::string& e
     for (int i = 0; i < 3; i++) {
         h.world_min[i] = rd<double>(b, 560 + 8 * i);
         h.world_max[i] = rd<double>(b, 584 + 8 * i);
+        h.voxel_size[i] = rd<double>(b, 608 + 8 * i);
     }
     const size_t tree = kGridSize;
     const size_t root = tree + rd<uint64_t>(b, tree + 24);
@@ -196,6 +197,8 @@ bool parse_nanovdb(const uint8_t* b, size_t bytes, SparseHost& h, std::string& e
         long long o[3] = {(long long)(int32_t)((uint32_t)((key >> 42) & 0x1FFFFFu) << 12),
                           (long long)(int32_t)((uint32_t)((key >> 21) & 0x1FFFFFu) << 12),
                           (long long)(int32_t)((uint32_t)(key & 0x1FFFFFu) << 12)};
+        h.root_tiles.push_back({{(int)o[0], (int)o[1], (int)o[2]}, child != 0 ? 1 : 0, rd<float>(b, tile + 20),
+                                rd<uint32_t>(b, tile + 16) != 0u ? 1 : 0});
         if (!as.intersects(o, 4096)) continue;
         if (child == 0) {
             as.fill(o, 4096, as.tile(make_tile(rd<float>(b, tile + 20), rd<uint32_t>(b, tile + 16) != 0u, 3, root_box)));
@@ -457,7 +460,10 @@ cudaError_t build_sparse_from_dense(const float* dense, int nx, int ny, int nz, 
         h.mat[i] = (i % 4 == 0) ? (float)dx : 0.0f;
         h.inv_mat[i] = (i % 4 == 0) ? (float)(1.0 / dx) : 0.0f;
     }
-    for (int i = 0; i < 3; i++) h.vec[i] = (float)origin[i];
+    for (int i = 0; i < 3; i++) {
+        h.vec[i] = (float)origin[i];
+        h.voxel_size[i] = dx;
+    }
     h.background = 0.0f;
 
     // Node hierarchy.  Lower nodes are 16^3 bricks, upper nodes 32^3 lower nodes.
@@ -590,6 +596,8 @@ cudaError_t build_sparse_from_dense(const float* dense, int nx, int ny, int nz, 
                 const size_t ui = ((size_t)z * uy + y) * ux + x;
                 if (!upper_exists[ui]) continue;
                 const long long uo[3] = {x * 4096LL, y * 4096LL, z * 4096LL};
+                h.root_tiles.push_back({{(int)uo[0], (int)uo[1], (int)uo[2]}, upper_pruned[ui] ? 0 : 1,
+                                        upper_pruned[ui] ? upper_value[ui] : 0.0f, upper_pruned[ui] ? 1 : 0});
                 if (upper_pruned[ui]) {
                     as.fill(uo, 4096, as.tile(make_tile(upper_value[ui], true, 3, root_b)));
                     continue;
@@ -675,6 +683,13 @@ SparseView make_sparse_view(const SparseHost& h, const SparseDevice& d, int lowe
     v.lowest_level = lowest_level;
     v.fp16 = d.values_h != nullptr;
     v.background = h.background;
+    v.root_tiles = (int)std::min<size_t>(h.root_tiles.size(), kSparseMaxRootTiles);
+    for (int t = 0; t < v.root_tiles; t++) {
+        for (int i = 0; i < 3; i++) v.rt_origin[t][i] = h.root_tiles[t].origin[i];
+        v.rt_child[t] = h.root_tiles[t].child;
+        v.rt_value[t] = h.root_tiles[t].value;
+        v.rt_active[t] = h.root_tiles[t].active;
+    }
     v.table = d.table;
     v.values = d.values;
     v.values_h = d.values_h;

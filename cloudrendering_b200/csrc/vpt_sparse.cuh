@@ -44,6 +44,14 @@ VPT_DEV bool sparse_entry(const SparseView& S, int x, int y, int z, uint32_t& e)
     return true;
 }
 
+// Root tile holding a voxel outside the brick table (-1: none).
+VPT_DEV int sparse_root_tile(const SparseView& S, int x, int y, int z) {
+    const int ox = x & ~4095, oy = y & ~4095, oz = z & ~4095;
+    for (int t = 0; t < S.root_tiles; t++)
+        if (S.rt_origin[t][0] == ox && S.rt_origin[t][1] == oy && S.rt_origin[t][2] == oz) return t;
+    return -1;
+}
+
 VPT_DEV uint32_t sparse_leaf_offset(int x, int y, int z) {
     return ((uint32_t)(x & 7) << 6) | ((uint32_t)(y & 7) << 3) | (uint32_t)(z & 7);
 }
@@ -51,7 +59,10 @@ VPT_DEV uint32_t sparse_leaf_offset(int x, int y, int z) {
 // pnanovdb_readaccessor_get_value_address + pnanovdb_read_float.
 VPT_DEV float sparse_value(const SparseView& S, int x, int y, int z) {
     uint32_t e;
-    if (!sparse_entry(S, x, y, z, e)) return S.background;
+    if (!sparse_entry(S, x, y, z, e)) {
+        const int t = sparse_root_tile(S, x, y, z);
+        return (t >= 0 && !S.rt_child[t]) ? S.rt_value[t] : S.background;
+    }
     if (e & kSparseTileBit) return S.tiles[e & ~kSparseTileBit].value;
     const size_t i = (size_t)e * 512u + sparse_leaf_offset(x, y, z);
     return S.fp16 ? __half2float(__ushort_as_half(__ldg(S.values_h + i))) : __ldg(S.values + i);
@@ -61,7 +72,10 @@ VPT_DEV float sparse_value(const SparseView& S, int x, int y, int z) {
 // the background.
 VPT_DEV int sparse_dim(const SparseView& S, int x, int y, int z) {
     uint32_t e;
-    if (!sparse_entry(S, x, y, z, e)) return 4096;
+    if (!sparse_entry(S, x, y, z, e)) {
+        const int t = sparse_root_tile(S, x, y, z);
+        return (t >= 0 && S.rt_child[t]) ? 128 : 4096;
+    }
     if (!(e & kSparseTileBit)) return 1;
     const int level = S.tiles[e & ~kSparseTileBit].level;
     return level == 1 ? 8 : (level == 2 ? 128 : 4096);
@@ -70,7 +84,10 @@ VPT_DEV int sparse_dim(const SparseView& S, int x, int y, int z) {
 // pnanovdb_readaccessor_is_active.
 VPT_DEV bool sparse_is_active(const SparseView& S, int x, int y, int z) {
     uint32_t e;
-    if (!sparse_entry(S, x, y, z, e)) return false;
+    if (!sparse_entry(S, x, y, z, e)) {
+        const int t = sparse_root_tile(S, x, y, z);
+        return t >= 0 && !S.rt_child[t] && S.rt_active[t];
+    }
     if (e & kSparseTileBit) return S.tiles[e & ~kSparseTileBit].active != 0;
     const uint32_t n = sparse_leaf_offset(x, y, z);
     return (__ldg(S.masks + (size_t)e * 16u + (n >> 5)) >> (n & 31u)) & 1u;
@@ -203,7 +220,13 @@ VPT_DEV bool sparse_cell_node(const SparseView& S, const int v[3], F3& bmin, F3&
         return sparse_is_active(S, v[0], v[1], v[2]);
     }
     uint32_t e;
-    if (!sparse_entry(S, v[0], v[1], v[2], e)) return false;
+    if (!sparse_entry(S, v[0], v[1], v[2], e)) {
+        const int t = sparse_root_tile(S, v[0], v[1], v[2]);
+        if (t < 0 || S.rt_child[t] || !S.rt_active[t]) return false;
+        bmin = f3((float)S.root_min[0], (float)S.root_min[1], (float)S.root_min[2]);
+        bmax = f3((float)S.root_max[0], (float)S.root_max[1], (float)S.root_max[2]);
+        return true;
+    }
     if (!(e & kSparseTileBit)) {
         const int* b = S.leaf_bbox_min + (size_t)e * 3u;
         bmin = f3((float)b[0], (float)b[1], (float)b[2]);

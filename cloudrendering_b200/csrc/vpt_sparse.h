@@ -25,11 +25,19 @@ namespace vpt {
 struct SparseHost {
     float mat[9] = {0}, inv_mat[9] = {0}, vec[3] = {0};
     double world_min[3] = {0}, world_max[3] = {0};  // GridData::mWorldBBox
+    double voxel_size[3] = {0};                      // GridData::mVoxelSize
     int root_min[3] = {0}, root_max[3] = {-1, -1, -1};
     float background = 0.0f;
     int tbl_origin[3] = {0}, tbl_dim[3] = {0};
     std::vector<uint32_t> table;
     std::vector<SparseTile> tiles;
+    struct RootTile {
+        int origin[3];
+        int child;
+        float value;
+        int active;
+    };
+    std::vector<RootTile> root_tiles;  // in the order of the root's tile table
     std::vector<int> leaf_bbox_min;  // 3 per leaf
     std::vector<uint64_t> leaf_src;  // per leaf: byte offset of the LeafNode in the source buffer, or the
                                      // linear index of the source brick (dense build)

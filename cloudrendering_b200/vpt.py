@@ -9,7 +9,9 @@ Differences, all documented supersets:
 * ``render_frame`` on CUDA returns a fresh tensor instead of a view of an internal buffer that the
   next call overwrites (Module.cpp:687-692).
 * extra entry points: ``set_density_field`` (CloudData::setDensityField), ``generate_fbm_cloud``,
-  ``set_grid_interpolation``, ``set_max_bounces``, ``set_sun``, ``set_sky_color``, ``get_stats``.
+  ``set_grid_interpolation``, ``set_max_bounces``, ``set_sun``, ``set_sky_color``, ``get_stats``,
+  ``set_use_sparse_grid`` (the C++ pass's setUseSparseGrid), ``set_sparse_grid_fp16``,
+  ``load_nanovdb_grid``.
 * the builtin environment map list gains "Constant Sky + Sun" (constant sky plus the reference's
   Phong sun lobe, visible to every tracker).
 """
@@ -148,10 +150,42 @@ def generate_fbm_cloud(size, seed: int = 1, octaves: int = 6, lacunarity: float 
     S.grid_size = (nx, ny, nz)
 
 
+_NANOVDB_MAGIC = b"NanoVDB0"
+
+
+def _nanovdb_grid_from_file(buf: bytes) -> bytes:
+    """First grid of an uncompressed NanoVDB file: the file header and the grid data both start
+    with the magic number; the grid's byte size is GridData::mGridSize (offset 32)."""
+    if not buf.startswith(_NANOVDB_MAGIC):
+        raise RuntimeError("Error in CloudData::loadFromNvdbFile: not a NanoVDB file.")
+    start = buf.find(_NANOVDB_MAGIC, 8)
+    if start < 0:
+        raise RuntimeError("Error in CloudData::loadFromNvdbFile: no uncompressed grid found (compressed "
+                           "NanoVDB files are not supported).")
+    size = struct.unpack_from("<Q", buf, start + 32)[0]
+    if start + size > len(buf):
+        raise RuntimeError("Error in CloudData::loadFromNvdbFile: truncated grid.")
+    return buf[start:start + size]
+
+
+def load_nanovdb_grid(grid: bytes) -> None:
+    """A NanoVDB float grid buffer (CloudData::setNanoVdbGridHandle): it replaces the dense grid and
+    is rendered through the sparse path."""
+    arr = np.frombuffer(grid, dtype=np.uint8)
+    _c("vpt_set_nanovdb_grid", arr.ctypes.data_as(ctypes.c_void_p), arr.nbytes, 0)
+    info = _sparse_info()
+    S.grid_size = tuple(int(info.root_max[i] - info.root_min[i] + 1) for i in range(3))
+
+
 def load_cloud_file(filename: str) -> None:
-    """Loads a dense .xyz grid (CloudData::loadFromXyzFile, CloudData.cpp:236-317)."""
+    """Loads a dense .xyz grid (CloudData::loadFromXyzFile, CloudData.cpp:236-317) or an
+    uncompressed .nvdb NanoVDB file (CloudData::loadFromNvdbFile, CloudData.cpp:1360-1365)."""
     if not os.path.exists(filename):
         raise RuntimeError(f"Error in CloudData::loadFromFile: The file \"{filename}\" does not exist.")
+    if filename.endswith(".nvdb"):
+        with open(filename, "rb") as f:
+            load_nanovdb_grid(_nanovdb_grid_from_file(f.read()))
+        return
     if not filename.endswith(".xyz"):
         raise RuntimeError(f"Error in CloudData::loadFromFile: unsupported file format \"{filename}\".")
     with open(filename, "rb") as f:
@@ -180,6 +214,39 @@ def get_render_bounding_box() -> List[float]:
     out = (ctypes.c_float * 6)()
     _c("vpt_get_render_bounding_box", out)
     return [out[0], out[3], out[1], out[4], out[2], out[5]]
+
+
+# ---- sparse grids (VolumetricPathTracingPass::setUseSparseGrid; Module.cpp:1390-1400) ----
+def set_use_sparse_grid(use_sparse: bool) -> None:
+    """Render through a NanoVDB-style sparse volume built from the dense grid (the C++ pass's
+    setUseSparseGrid; not exposed by the reference's Python module)."""
+    _c("vpt_set_use_sparse_grid", 1 if use_sparse else 0)
+
+
+def set_sparse_grid_fp16(use_fp16: bool) -> None:
+    """Store the leaf values of the next sparse volume as IEEE half (no reference counterpart)."""
+    _c("vpt_set_option", b"sparse_fp16", 1.0 if use_fp16 else 0.0)
+
+
+def _sparse_info():
+    info = _lib.VptSparseInfo()
+    _c("vpt_get_sparse_grid_info", ctypes.byref(info))
+    return info
+
+
+def get_vdb_world_bounding_box() -> List[float]:
+    i = _sparse_info()
+    return [i.world_min[0], i.world_max[0], i.world_min[1], i.world_max[1], i.world_min[2], i.world_max[2]]
+
+
+def get_vdb_index_bounding_box() -> List[int]:
+    i = _sparse_info()
+    return [i.root_min[0], i.root_max[0], i.root_min[1], i.root_max[1], i.root_min[2], i.root_max[2]]
+
+
+def get_vdb_voxel_size() -> List[float]:
+    i = _sparse_info()
+    return [i.voxel_size[0], i.voxel_size[1], i.voxel_size[2]]
 
 
 def get_volume_voxel_size() -> List[int]:

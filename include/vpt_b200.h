@@ -185,7 +185,9 @@ VptStatus vpt_set_use_empty_space_skipping(VptContext* ctx, int enabled);
  * default 2^24; a path that reaches it stops and vpt_synchronize reports VPT_ERR_ITER_LIMIT),
  * "ess_ref_compat" (1 = empty-space skipping exactly as the reference runs it: every block marked
  * occupied, ComputeOccupancyGrid.glsl:108-109, and shadow samples stepped from the moving point,
- * NeeTransmittance.glsl:173-228). */
+ * NeeTransmittance.glsl:173-228), "sparse_fp16" (1 = leaf values of the next sparse volume stored as
+ * IEEE half), "fbm_contrast" (remap clamp(0.5 + contrast * fbm, 0, 1) of vpt_generate_fbm_grid,
+ * default 3.5). */
 VptStatus vpt_set_option(VptContext* ctx, const char* key, double value);
 
 /* ---- denoisers (VolumetricPathTracingPass.cpp:2287-2311) ---- */
@@ -214,6 +216,48 @@ VptStatus vpt_build_occupancy_grid(const float* density, int nx, int ny, int nz,
  * of an equirectangular RGBA image (OctahedralMapper.glsl:65-85 + mip reduction). */
 VptStatus vpt_build_environment_pyramid(const float* rgba, int width, int height, int levels, float* out_pyramid,
                                         void* stream);
+/* ---- sparse (NanoVDB) volumes ---- */
+
+typedef struct VptSparseInfo {
+    uint64_t leaves;          /* 8^3 leaf nodes */
+    uint64_t tiles;           /* distinct constant tiles referenced by the brick table */
+    uint64_t device_bytes;    /* device memory of the sparse volume */
+    int32_t table_origin[3];  /* first voxel of the brick table */
+    int32_t table_dim[3];     /* bricks per axis */
+    int32_t root_min[3];      /* index bounding box of the active values (inclusive) */
+    int32_t root_max[3];
+    float box_min[3];         /* render box (world) */
+    float box_max[3];
+    double world_min[3];      /* GridData::mWorldBBox */
+    double world_max[3];
+    double voxel_size[3];     /* GridData::mVoxelSize */
+    int32_t fp16;             /* leaf values stored as half */
+    int32_t lowest_level;     /* HDDA cell of the sparse decomposition tracker: 8 or 1 */
+} VptSparseInfo;
+
+/* Render through a sparse volume (VolumetricPathTracingPass::setUseSparseGrid,
+ * src/PathTracer/VolumetricPathTracingPass.cpp:863-869).  With a dense grid loaded, the sparse
+ * volume is built from it on the next render as CloudData::getSparseDensityField does
+ * (src/CloudData.cpp:1385-1407: GridBuilder, background 0, voxel size boxExtent.x / nx).  Delta,
+ * ratio, NEE (without empty space skipping) and HDDA decomposition tracking run on sparse grids;
+ * residual ratio tracking needs the dense grid, as in the reference. */
+VptStatus vpt_set_use_sparse_grid(VptContext* ctx, int use_sparse);
+/* Loads a NanoVDB float grid (version 32; CloudData::loadFromNvdbFile / setNanoVdbGridHandle,
+ * src/CloudData.cpp:169-172, 1360-1365) from host or device memory; it replaces the dense grid and
+ * is fitted into [-maxGridExtent, maxGridExtent] (CloudData::computeSparseGridMetadata,
+ * src/CloudData.cpp:1289-1357).  vpt_set_option(ctx, "sparse_fp16", 1) before loading stores the
+ * leaf values as IEEE half. */
+VptStatus vpt_set_nanovdb_grid(VptContext* ctx, const void* buffer, size_t bytes, int on_device);
+/* Sparse volume description (builds it from the dense grid first if needed, as
+ * CloudData::getVDBWorldBoundingBox does, src/CloudData.cpp:1440-1491). */
+VptStatus vpt_get_sparse_grid_info(VptContext* ctx, VptSparseInfo* out);
+/* Value, dim and active state of the sparse volume at `count` voxels (device arrays: 3 int32 per voxel
+ * in, float / uint32 / uint8 out), as pnanovdb_readaccessor_get_value_address + read_float,
+ * pnanovdb_readaccessor_get_dim and pnanovdb_readaccessor_is_active return them
+ * (Data/Shaders/VPT/PNanoVDB.glsl:1800-1990). */
+VptStatus vpt_sparse_query(VptContext* ctx, const int32_t* ijk, int count, float* values, uint32_t* dims,
+                           uint8_t* active, void* stream);
+
 /* EAW a-trous chain (EAWBlitPass::_renderCompute, src/Denoiser/EAWDenoiser.cpp:345-391; weights of
  * EAWDenoise.glsl) on RGBA images; position/normal may be NULL.  Allocates its ping-pong images
  * on `stream` with the stream-ordered allocator and frees them before returning. */

@@ -34,6 +34,8 @@ class OracleScene(ctypes.Structure):
         ("env_w", c_int), ("env_h", c_int), ("env_levels", c_int),
         ("density", c_void_p), ("sv_data", c_void_p), ("occupancy", c_void_p),
         ("env_rgba", c_void_p), ("env_pyramid", c_void_p),
+        ("nanovdb", c_void_p), ("grid_min", c_float * 3), ("grid_max", c_float * 3),
+        ("sparse_lowest_level", c_int), ("sparse_fp16", c_int),
     ]
 
 
@@ -64,6 +66,10 @@ def load():
         lib.oracle_eaw.argtypes = [c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_float, c_float, c_float,
                                    c_int, c_void_p]
         lib.oracle_rng_stream.argtypes = [c_uint32, c_int, c_void_p, c_void_p]
+        lib.oracle_nanovdb_query.argtypes = [c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p]
+        lib.oracle_nanovdb_hdda_walk.restype = c_int
+        lib.oracle_nanovdb_hdda_walk.argtypes = [c_void_p, c_void_p, c_void_p, c_int, c_int, c_void_p, c_void_p,
+                                                 c_void_p, c_void_p, c_void_p, c_void_p]
         lib.oracle_set_double_rounded_math.argtypes = [c_int]
         lib.oracle_set_double_rounded_math.restype = None
         _lib = lib
@@ -158,7 +164,7 @@ class Scene:
             self.set(k, v)
 
     def set(self, k, v):
-        if k in ("density", "sv_data", "occupancy", "env_rgba", "env_pyramid"):
+        if k in ("density", "sv_data", "occupancy", "env_rgba", "env_pyramid", "nanovdb"):
             arr = None if v is None else np.ascontiguousarray(v)
             self._keep[k] = arr
             setattr(self.s, k, None if arr is None else arr.ctypes.data_as(c_void_p).value)
@@ -206,3 +212,30 @@ class double_rounded_math:
     def __exit__(self, *exc):
         load().oracle_set_double_rounded_math(0)
         return False
+
+
+def nanovdb_query(buf: np.ndarray, ijk: np.ndarray):
+    """The oracle's restatement of PNanoVDB's accessor: value, dim, active at each voxel."""
+    c = np.ascontiguousarray(ijk, np.int32).reshape(-1, 3)
+    n = c.shape[0]
+    val = np.empty(n, np.float32)
+    dim = np.empty(n, np.uint32)
+    act = np.empty(n, np.uint8)
+    load().oracle_nanovdb_query(_p(buf), n, _p(c), _p(val), _p(dim), _p(act))
+    return val, dim, act
+
+
+def nanovdb_hdda_walk(buf: np.ndarray, origin, direction, lowest_level: int = 8, max_visits: int = 4096):
+    o = np.asarray(origin, np.float32)
+    d = np.asarray(direction, np.float32)
+    vox = np.zeros((max_visits, 3), np.int32)
+    dim = np.zeros(max_visits, np.int32)
+    act = np.zeros(max_visits, np.uint8)
+    lvl = np.zeros(max_visits, np.int32)
+    box = np.zeros((max_visits, 6), np.float32)
+    t = np.zeros((max_visits, 3), np.float32)
+    n = load().oracle_nanovdb_hdda_walk(_p(buf), _p(o), _p(d), lowest_level, max_visits, _p(vox), _p(dim), _p(act),
+                                        _p(lvl), _p(box), _p(t))
+    if n < 0:
+        return None
+    return dict(voxel=vox[:n], dim=dim[:n], active=act[:n], level=lvl[:n], box=box[:n], t=t[:n])

@@ -247,6 +247,239 @@ V3 sample_env_image(const OracleScene& S, const size_t* off, Rng& r, float& pdf)
     return oct_to_world(((float)px + rx) * inv, ((float)py + ry) * inv);
 }
 
+// ---- NanoVDB float grids: the read path of PNanoVDB.glsl restated ----
+// Layout of a version-32 float grid (PNanoVDB.glsl:712-1171): map at 296 (mMatF, mInvMatF, mVecF),
+// tree at 672 (root offset at +24), root: bbox at 0/12, tile count 24, background 28, 32-byte tiles
+// from 64 (key, child, state, value); upper: value mask 32, child mask 4128, 8-byte table 8256;
+// lower: masks 32 / 544, table 1088; leaf: bbox min 0, value mask 16, values 96.
+template <class T>
+T rdv(const uint8_t* b, size_t off) {
+    T v;
+    memcpy(&v, b + off, sizeof(T));
+    return v;
+}
+
+struct Nano {
+    const uint8_t* b = nullptr;
+    size_t root = 0;
+    uint32_t tiles = 0;
+    float background = 0.0f;
+    float mat[9], inv[9], vec[3];
+    int rmin[3], rmax[3];
+    bool fp16 = false;
+
+    void init(const uint8_t* buf, bool half) {
+        b = buf;
+        fp16 = half;
+        for (int i = 0; i < 9; i++) {
+            mat[i] = rdv<float>(b, 296 + 4 * i);
+            inv[i] = rdv<float>(b, 332 + 4 * i);
+        }
+        for (int i = 0; i < 3; i++) vec[i] = rdv<float>(b, 368 + 4 * i);
+        root = 672 + rdv<uint64_t>(b, 672 + 24);
+        for (int i = 0; i < 3; i++) {
+            rmin[i] = rdv<int32_t>(b, root + 4 * i);
+            rmax[i] = rdv<int32_t>(b, root + 12 + 4 * i);
+        }
+        tiles = rdv<uint32_t>(b, root + 24);
+        background = rdv<float>(b, root + 28);
+    }
+    bool bit(size_t mask, uint32_t n) const { return (rdv<uint32_t>(b, mask + 4 * (n >> 5)) >> (n & 31u)) & 1u; }
+    static uint64_t key(int x, int y, int z) {
+        return (uint64_t)((uint32_t)z >> 12) | ((uint64_t)((uint32_t)y >> 12) << 21) |
+               ((uint64_t)((uint32_t)x >> 12) << 42);
+    }
+    static uint32_t upper_off(int x, int y, int z) {
+        return (((uint32_t)(x & 4095) >> 7) << 10) | (((uint32_t)(y & 4095) >> 7) << 5) | ((uint32_t)(z & 4095) >> 7);
+    }
+    static uint32_t lower_off(int x, int y, int z) {
+        return (((uint32_t)(x & 127) >> 3) << 8) | (((uint32_t)(y & 127) >> 3) << 4) | ((uint32_t)(z & 127) >> 3);
+    }
+    static uint32_t leaf_off(int x, int y, int z) {
+        return ((uint32_t)(x & 7) << 6) | ((uint32_t)(y & 7) << 3) | (uint32_t)(z & 7);
+    }
+    // pnanovdb_root_find_tile: linear search over the root tiles; 0 when absent
+    size_t find_tile(int x, int y, int z) const {
+        const uint64_t k = key(x, y, z);
+        for (uint32_t t = 0; t < tiles; t++) {
+            size_t tile = root + 64 + 32 * (size_t)t;
+            if (rdv<uint64_t>(b, tile) == k) return tile;
+        }
+        return 0;
+    }
+    // Node holding (x, y, z): level 0 leaf, 1 lower tile, 2 upper tile, 3 root tile, 4 background.
+    struct Where {
+        int level;
+        size_t tile, upper, lower, leaf;
+        uint32_t un, ln;
+    };
+    Where where(int x, int y, int z) const {
+        Where w{4, 0, 0, 0, 0, 0, 0};
+        w.tile = find_tile(x, y, z);
+        if (!w.tile) return w;
+        int64_t child = rdv<int64_t>(b, w.tile + 8);
+        if (child == 0) {
+            w.level = 3;
+            return w;
+        }
+        w.upper = root + (size_t)child;
+        w.un = upper_off(x, y, z);
+        if (!bit(w.upper + 4128, w.un)) {
+            w.level = 2;
+            return w;
+        }
+        w.lower = w.upper + (size_t)rdv<int64_t>(b, w.upper + 8256 + 8 * (size_t)w.un);
+        w.ln = lower_off(x, y, z);
+        if (!bit(w.lower + 544, w.ln)) {
+            w.level = 1;
+            return w;
+        }
+        w.leaf = w.lower + (size_t)rdv<int64_t>(b, w.lower + 1088 + 8 * (size_t)w.ln);
+        w.level = 0;
+        return w;
+    }
+    float leaf_value(size_t leaf, uint32_t off) const {
+        float v = rdv<float>(b, leaf + 96 + 4 * (size_t)off);
+        if (fp16) v = (float)(_Float16)v;
+        return v;
+    }
+    float value(int x, int y, int z) const {
+        Where w = where(x, y, z);
+        switch (w.level) {
+            case 0: return leaf_value(w.leaf, leaf_off(x, y, z));
+            case 1: return rdv<float>(b, w.lower + 1088 + 8 * (size_t)w.ln);
+            case 2: return rdv<float>(b, w.upper + 8256 + 8 * (size_t)w.un);
+            case 3: return rdv<float>(b, w.tile + 20);
+            default: return background;
+        }
+    }
+    int dim(int x, int y, int z) const {
+        static const int d[5] = {1, 8, 128, 4096, 4096};
+        return d[where(x, y, z).level];
+    }
+    bool active(int x, int y, int z) const {
+        Where w = where(x, y, z);
+        switch (w.level) {
+            case 0: return bit(w.leaf + 16, leaf_off(x, y, z));
+            case 1: return bit(w.lower + 32, w.ln);
+            case 2: return bit(w.upper + 32, w.un);
+            case 3: return rdv<uint32_t>(b, w.tile + 16) != 0u;
+            default: return false;
+        }
+    }
+    // Cell classification of the sparse decomposition tracker at the leaf level
+    // (DecompositionTracking.glsl:178-248); returns the level and writes the node box.
+    int cell(int x, int y, int z, bool& is_active, V3& bmin, V3& bmax) const {
+        Where w = where(x, y, z);
+        is_active = false;
+        auto box = [&](size_t node) {
+            bmin = v3((float)rdv<int32_t>(b, node), (float)rdv<int32_t>(b, node + 4), (float)rdv<int32_t>(b, node + 8));
+            bmax = v3((float)rdv<int32_t>(b, node + 12), (float)rdv<int32_t>(b, node + 16),
+                      (float)rdv<int32_t>(b, node + 20));
+        };
+        switch (w.level) {
+            case 0: {
+                is_active = true;
+                int bx = rdv<int32_t>(b, w.leaf), by = rdv<int32_t>(b, w.leaf + 4), bz = rdv<int32_t>(b, w.leaf + 8);
+                bmin = v3((float)bx, (float)by, (float)bz);
+                bmax = v3((float)(bx + 8), (float)(by + 8), (float)(bz + 8));
+                break;
+            }
+            case 1: is_active = bit(w.lower + 32, w.ln); box(w.lower); break;
+            case 2: is_active = bit(w.upper + 32, w.un); box(w.upper); break;
+            case 3: is_active = rdv<uint32_t>(b, w.tile + 16) != 0u; box(root); break;
+            default: break;
+        }
+        return w.level;
+    }
+    // pnanovdb_map_apply_inverse / _inverse_jacobi / _apply (PNanoVDB.glsl:1996-2040)
+    V3 world_to_index(V3 p) const {
+        float sx = p.x - vec[0], sy = p.y - vec[1], sz = p.z - vec[2];
+        return v3((sx * inv[0] + sy * inv[1]) + sz * inv[2], (sx * inv[3] + sy * inv[4]) + sz * inv[5],
+                  (sx * inv[6] + sy * inv[7]) + sz * inv[8]);
+    }
+    V3 world_to_index_dir(V3 d) const {
+        return v3((d.x * inv[0] + d.y * inv[1]) + d.z * inv[2], (d.x * inv[3] + d.y * inv[4]) + d.z * inv[5],
+                  (d.x * inv[6] + d.y * inv[7]) + d.z * inv[8]);
+    }
+    V3 index_to_world(V3 p) const {
+        return v3(((p.x * mat[0] + p.y * mat[1]) + p.z * mat[2]) + vec[0],
+                  ((p.x * mat[3] + p.y * mat[4]) + p.z * mat[5]) + vec[1],
+                  ((p.x * mat[6] + p.y * mat[7]) + p.z * mat[8]) + vec[2]);
+    }
+};
+
+// ---- hierarchical DDA (pnanovdb_hdda_*, PNanoVDB.glsl:2233-2452) ----
+inline float pmin(float a, float b) { return a < b ? a : b; }
+inline float pmax(float a, float b) { return a > b ? a : b; }
+
+struct HddaState {
+    int dim;
+    float tmin, tmax;
+    int voxel[3], step[3];
+    float delta[3], next[3];
+};
+
+bool hdda_clip(V3 bmin, V3 bmax, V3 o, float& tmin, V3 d, float& tmax) {
+    float ix = 1.0f / d.x, iy = 1.0f / d.y, iz = 1.0f / d.z;
+    float t0x = (bmin.x - o.x) * ix, t0y = (bmin.y - o.y) * iy, t0z = (bmin.z - o.z) * iz;
+    float t1x = (bmax.x - o.x) * ix, t1y = (bmax.y - o.y) * iy, t1z = (bmax.z - o.z) * iz;
+    float tnear = pmax(pmin(t0x, t1x), pmax(pmin(t0y, t1y), pmin(t0z, t1z)));
+    float tfar = pmin(pmax(t0x, t1x), pmin(pmax(t0y, t1y), pmax(t0z, t1z)));
+    bool hit = tnear <= tfar;
+    tmin = pmax(tmin, tnear);
+    tmax = pmin(tmax, tfar);
+    return hit;
+}
+
+void hdda_start(HddaState& h, V3 o, float tmin, V3 d, float tmax, int dim) {
+    h.dim = dim;
+    h.tmin = tmin;
+    h.tmax = tmax;
+    float pos[3] = {d.x * tmin + o.x, d.y * tmin + o.y, d.z * tmin + o.z};
+    float dd[3] = {d.x, d.y, d.z};
+    for (int a = 0; a < 3; a++) h.voxel[a] = (int)floorf(pos[a]) & ~(dim - 1);
+    for (int a = 0; a < 3; a++) {
+        float inv = 1.0f / dd[a];
+        if (dd[a] == 0.0f) {
+            h.next[a] = 1e38f;
+            h.step[a] = 0;
+            h.delta[a] = 0.0f;
+        } else if (inv > 0.0f) {
+            h.step[a] = 1;
+            h.next[a] = h.tmin + ((float)(h.voxel[a] + dim) - pos[a]) * inv;
+            h.delta[a] = inv;
+        } else {
+            h.step[a] = -1;
+            h.next[a] = h.tmin + ((float)h.voxel[a] - pos[a]) * inv;
+            h.delta[a] = -inv;
+        }
+    }
+}
+
+void hdda_set_dim(HddaState& h, V3 o, V3 d, int dim) {
+    if (h.dim == dim) return;
+    h.dim = dim;
+    float pos[3] = {d.x * h.tmin + o.x, d.y * h.tmin + o.y, d.z * h.tmin + o.z};
+    float inv[3] = {1.0f / d.x, 1.0f / d.y, 1.0f / d.z};
+    for (int a = 0; a < 3; a++) h.voxel[a] = (int)floorf(pos[a]) & ~(dim - 1);
+    for (int a = 0; a < 3; a++) {
+        if (h.step[a] != 0) {
+            h.next[a] = h.tmin + ((float)h.voxel[a] - pos[a]) * inv[a];
+            if (h.step[a] > 0) h.next[a] += (float)dim * inv[a];
+        }
+    }
+}
+
+bool hdda_advance(HddaState& h) {
+    int a = (h.next[0] < h.next[1] && h.next[0] < h.next[2]) ? 0 : (h.next[1] < h.next[2] ? 1 : 2);
+    if (h.next[a] <= h.tmin) h.next[a] += (h.tmin - 0.999999f * h.next[a]) + 1.0e-6f;
+    h.tmin = h.next[a];
+    h.next[a] += (float)h.dim * h.delta[a];
+    h.voxel[a] += h.dim * h.step[a];
+    return h.tmin <= h.tmax;
+}
+
 // ---- density lookup (VptUtils.glsl:583-591, 674-683; CLAMP_TO_BORDER) ----
 struct Tracer {
     const OracleScene& S;
@@ -254,7 +487,10 @@ struct Tracer {
     uint64_t lookups = 0;
     uint32_t steps = 0;
 
+    Nano nano;
+
     explicit Tracer(const OracleScene& s) : S(s) {
+        if (S.nanovdb) nano.init(S.nanovdb, S.sparse_fp16 != 0);
         if (S.env_kind == 4) {
             size_t o = 0;
             for (int l = 0; l < S.env_levels; l++) {
@@ -285,8 +521,32 @@ struct Tracer {
                         mixf(texel(x0, y0 + 1, z0 + 1), texel(x0 + 1, y0 + 1, z0 + 1), ax), ay);
         return mixf(f0, f1, az);
     }
+    // sampleCloud (VptUtils.glsl:674-683) + sampleCloudRaw for NanoVDB (VptUtils.glsl:517-581)
+    float sample_sparse(V3 pos, Rng& r) {
+        V3 c;
+        c.x = ((pos.x - S.box_min[0]) / (S.box_max[0] - S.box_min[0])) * (S.grid_max[0] - S.grid_min[0]) + S.grid_min[0];
+        c.y = ((pos.y - S.box_min[1]) / (S.box_max[1] - S.box_min[1])) * (S.grid_max[1] - S.grid_min[1]) + S.grid_min[1];
+        c.z = ((pos.z - S.box_min[2]) / (S.box_max[2] - S.box_min[2])) * (S.grid_max[2] - S.grid_min[2]) + S.grid_min[2];
+        V3 p = nano.world_to_index(c);
+        if (S.interp == 0) return nano.value((int)floorf(p.x), (int)floorf(p.y), (int)floorf(p.z));
+        if (S.interp == 1) {
+            float jx = rnd(r) - 0.5f, jy = rnd(r) - 0.5f, jz = rnd(r) - 0.5f;
+            return nano.value((int)floorf(p.x + jx), (int)floorf(p.y + jy), (int)floorf(p.z + jz));
+        }
+        p = v3(p.x - 0.5f, p.y - 0.5f, p.z - 0.5f);
+        int ix = (int)floorf(p.x), iy = (int)floorf(p.y), iz = (int)floorf(p.z);
+        float fx = p.x - (float)ix, fy = p.y - (float)iy, fz = p.z - (float)iz;
+        float f00 = mixf(nano.value(ix, iy, iz), nano.value(ix + 1, iy, iz), fx);
+        float f10 = mixf(nano.value(ix, iy + 1, iz), nano.value(ix + 1, iy + 1, iz), fx);
+        float f0 = mixf(f00, f10, fy);
+        float f01 = mixf(nano.value(ix, iy, iz + 1), nano.value(ix + 1, iy, iz + 1), fx);
+        float f11 = mixf(nano.value(ix, iy + 1, iz + 1), nano.value(ix + 1, iy + 1, iz + 1), fx);
+        float f1 = mixf(f01, f11, fy);
+        return mixf(f0, f1, fz);
+    }
     float sample(V3 pos, Rng& r) {
         lookups++;
+        if (S.nanovdb) return sample_sparse(pos, r);
         float ux = (pos.x - S.box_min[0]) * S.vox_per_unit[0];
         float uy = (pos.y - S.box_min[1]) * S.vox_per_unit[1];
         float uz = (pos.z - S.box_min[2]) * S.vox_per_unit[2];
@@ -507,6 +767,93 @@ struct Tracer {
         return color;
     }
 
+    // analogDecompositionTracking over a NanoVDB grid with the HDDA
+    // (DecompositionTracking.glsl:130-360)
+    V3 decomposition_sparse(V3 x, V3 w, Rng& r) {
+        V3 origin = nano.world_to_index(x);
+        V3 dir = nano.world_to_index_dir(w);
+        float scale = 1.0f / length(dir);
+        dir = mul(dir, scale);
+        float tmin = 0.0f, tmax = 1e10f;
+        V3 rlo = v3((float)nano.rmin[0], (float)nano.rmin[1], (float)nano.rmin[2]);
+        V3 rhi = v3((float)(nano.rmax[0] + 1), (float)(nano.rmax[1] + 1), (float)(nano.rmax[2] + 1));
+        bool hit = hdda_clip(rlo, rhi, origin, tmin, dir, tmax);
+        if (hit && tmax < 1e20f) {
+            const float majorant = S.extinction;
+            const float absorb = 1.0f - S.albedo;
+            const int lowest = S.sparse_lowest_level;
+            int bounces = 0;
+            HddaState h;
+            hdda_start(h, origin, tmin - 1e-4f, dir, tmax + 1e-4f, lowest);
+            for (int iteration = 0;; iteration++) {
+                if (guard()) return v3(0, 0, 0);
+                if (iteration > 0) {
+                    if (!hdda_advance(h)) break;
+                    int d = std::max(nano.dim(h.voxel[0], h.voxel[1], h.voxel[2]), lowest);
+                    hdda_set_dim(h, origin, dir, d);
+                }
+                bool active = false;
+                V3 nmin = v3(0, 0, 0), nmax = v3(0, 0, 0);
+                if (lowest == 8) {
+                    nano.cell(h.voxel[0], h.voxel[1], h.voxel[2], active, nmin, nmax);
+                } else {
+                    active = nano.active(h.voxel[0], h.voxel[1], h.voxel[2]);
+                    nmin = v3((float)h.voxel[0], (float)h.voxel[1], (float)h.voxel[2]);
+                    nmax = v3((float)(h.voxel[0] + 1), (float)(h.voxel[1] + 1), (float)(h.voxel[2] + 1));
+                }
+                if (!active) continue;
+                float tn0 = 0.0f, tn1 = 1e10f;
+                bool hits_node = hdda_clip(nmin, nmax, origin, tn0, dir, tn1);
+                x = nano.index_to_world(add(origin, mul(dir, tn0)));
+                if (!hits_node) continue;
+                float d_max = scale * (std::min(std::min(h.next[0], h.next[1]), h.next[2]) - h.tmin);
+                const float mu_c = 0.0000000001f;
+                const float mu_r = std::max(0.0000000001f, majorant * 1.0f - mu_c);
+                bool changed = false;
+                float t_c = -m_log(std::max(0.0000000001f, 1.0f - rnd(r))) / mu_c;
+                float t_r = 0.0f;
+                while (true) {
+                    if (guard()) return v3(0, 0, 0);
+                    t_r -= m_log(std::max(0.0000000001f, 1.0f - rnd(r))) / mu_r;
+                    if (t_c >= d_max && t_r >= d_max) {
+                        x = add(x, mul(w, d_max));
+                        break;
+                    }
+                    V3 xs = add(x, mul(w, std::min(t_c, t_r)));
+                    bool collision;
+                    if (t_c <= t_r) {
+                        collision = true;
+                    } else {
+                        float dens = sample(xs, r);
+                        collision = rnd(r) * mu_r < S.extinction * dens - mu_c;
+                    }
+                    if (collision) {
+                        x = xs;
+                        if (rnd(r) < absorb) return v3(0, 0, 0);
+                        if (S.max_bounces > 0 && ++bounces > S.max_bounces) return v3(0, 0, 0);
+                        w = sample_phase(r, S.g, w);
+                        t_r = 0.0f;
+                        t_c = -m_log(std::max(0.0000000001f, 1.0f - rnd(r))) / mu_c;
+                        origin = nano.world_to_index(x);
+                        dir = normalize(nano.world_to_index_dir(w));
+                        float tl0 = 0.0f, tl1 = 1e10f;
+                        ray_box(nmin, nmax, origin, dir, tl0, tl1);
+                        hdda_clip(nmin, nmax, origin, tl0, dir, tl1);
+                        d_max = scale * (tl1 - tl0);
+                        changed = true;
+                    }
+                }
+                if (changed) {
+                    tmin = 0.0f;
+                    tmax = 1e10f;
+                    hdda_clip(rlo, rhi, origin, tmin, dir, tmax);
+                    hdda_start(h, origin, tmin + d_max / scale + 1e-4f, dir, tmax + 1e-4f, lowest);
+                }
+            }
+        }
+        return sky(w);
+    }
+
     // analogDecompositionTracking, dense (DecompositionTracking.glsl:35-123)
     V3 decomposition(V3 x, V3 w, Rng& r) {
         V3 eps = v3(1e-6f, 1e-6f, 1e-6f);
@@ -694,7 +1041,7 @@ struct Tracer {
         switch (S.mode) {
             case 0: return delta(x, w, r, ev);
             case 2: return ratio(x, w, r, ev);
-            case 3: return decomposition(x, w, r);
+            case 3: return S.nanovdb ? decomposition_sparse(x, w, r) : decomposition(x, w, r);
             case 4: return rrt(x, w, r);
             default: return nee(x, w, r, ev);
         }
@@ -1046,6 +1393,70 @@ void oracle_eaw(const float* color, const float* pos, const float* nrm, int w, i
 }
 
 void oracle_set_double_rounded_math(int on) { g_dr_math = on != 0; }
+
+void oracle_nanovdb_query(const uint8_t* buf, int n, const int32_t* ijk, float* value, uint32_t* dim,
+                          uint8_t* active) {
+    Nano g;
+    g.init(buf, false);
+    for (int i = 0; i < n; i++) {
+        int x = ijk[3 * i], y = ijk[3 * i + 1], z = ijk[3 * i + 2];
+        value[i] = g.value(x, y, z);
+        dim[i] = (uint32_t)g.dim(x, y, z);
+        active[i] = g.active(x, y, z) ? 1 : 0;
+    }
+}
+
+int oracle_nanovdb_hdda_walk(const uint8_t* buf, const float world_origin[3], const float world_dir[3],
+                             int lowest_level, int max_visits, int32_t* out_voxel, int32_t* out_dim,
+                             uint8_t* out_active, int32_t* out_level, float* out_box, float* out_t) {
+    Nano g;
+    g.init(buf, false);
+    V3 origin = g.world_to_index(v3(world_origin[0], world_origin[1], world_origin[2]));
+    V3 dir = g.world_to_index_dir(v3(world_dir[0], world_dir[1], world_dir[2]));
+    float scale = 1.0f / length(dir);
+    dir = mul(dir, scale);
+    float tmin = 0.0f, tmax = 1e10f;
+    V3 rlo = v3((float)g.rmin[0], (float)g.rmin[1], (float)g.rmin[2]);
+    V3 rhi = v3((float)(g.rmax[0] + 1), (float)(g.rmax[1] + 1), (float)(g.rmax[2] + 1));
+    if (!(hdda_clip(rlo, rhi, origin, tmin, dir, tmax) && tmax < 1e20f)) return -1;
+    HddaState h;
+    hdda_start(h, origin, tmin - 1e-4f, dir, tmax + 1e-4f, lowest_level);
+    int visits = 0;
+    for (int iteration = 0; visits < max_visits; iteration++) {
+        if (iteration > 0) {
+            if (!hdda_advance(h)) break;
+            hdda_set_dim(h, origin, dir, std::max(g.dim(h.voxel[0], h.voxel[1], h.voxel[2]), lowest_level));
+        }
+        bool active = false;
+        int level = -1;
+        V3 nmin = v3(0, 0, 0), nmax = v3(0, 0, 0);
+        if (lowest_level == 8) {
+            level = g.cell(h.voxel[0], h.voxel[1], h.voxel[2], active, nmin, nmax);
+        } else {
+            active = g.active(h.voxel[0], h.voxel[1], h.voxel[2]);
+            nmin = v3((float)h.voxel[0], (float)h.voxel[1], (float)h.voxel[2]);
+            nmax = v3((float)(h.voxel[0] + 1), (float)(h.voxel[1] + 1), (float)(h.voxel[2] + 1));
+        }
+        for (int a = 0; a < 3; a++) out_voxel[3 * visits + a] = h.voxel[a];
+        out_dim[visits] = h.dim;
+        out_active[visits] = active ? 1 : 0;
+        out_level[visits] = level;
+        float tn0 = 0.0f, tn1 = 1e10f;
+        float* bx = out_box + 6 * visits;
+        if (active) {
+            bx[0] = nmin.x; bx[1] = nmin.y; bx[2] = nmin.z;
+            bx[3] = nmax.x; bx[4] = nmax.y; bx[5] = nmax.z;
+            hdda_clip(nmin, nmax, origin, tn0, dir, tn1);
+        } else {
+            for (int k = 0; k < 6; k++) bx[k] = 0.0f;
+        }
+        out_t[3 * visits] = h.tmin;
+        out_t[3 * visits + 1] = pmin(pmin(h.next[0], h.next[1]), h.next[2]);
+        out_t[3 * visits + 2] = tn0;
+        visits++;
+    }
+    return visits;
+}
 
 void oracle_rng_stream(uint32_t seed, int n, float* out, uint32_t* st4) {
     Rng r = rng_init(seed);

@@ -43,6 +43,12 @@ typedef struct OracleScene {
     const uint8_t* occupancy;
     const float* env_rgba;
     const float* env_pyramid; /* levels concatenated, level 0 first */
+    /* sparse grid: when `nanovdb` is set, densities come from this NanoVDB float grid buffer
+     * (version 32) through a restatement of PNanoVDB's read accessor */
+    const uint8_t* nanovdb;
+    float grid_min[3], grid_max[3];  /* world box of the grid: sampleCloud maps box -> grid box */
+    int sparse_lowest_level;         /* HDDA cell of sparse decomposition tracking: 8 or 1 */
+    int sparse_fp16;                 /* leaf values rounded to IEEE half (fp16 variant) */
 } OracleScene;
 
 /* Renders width*height*num_frames paths; adds radiance (and its square) per pixel (3 doubles). */
@@ -69,6 +75,15 @@ void oracle_env_pyramid(const float* rgba, int w, int h, int levels, float* pyra
 /* EAW a-trous chain on RGBA images (position/normal may be NULL). */
 void oracle_eaw(const float* color, const float* pos, const float* nrm, int w, int h, int iterations,
                 float phi_c, float phi_p, float phi_n, int quirk, float* out);
+
+/* PNanoVDB accessor restated on a NanoVDB float grid: value, dim and active state of n voxels. */
+void oracle_nanovdb_query(const uint8_t* buf, int n, const int32_t* ijk, float* value, uint32_t* dim,
+                          uint8_t* active);
+/* The sparse decomposition tracker's node walk for a straight ray (same record layout as the
+ * reference driver's refvdb_hdda_walk). */
+int oracle_nanovdb_hdda_walk(const uint8_t* buf, const float world_origin[3], const float world_dir[3],
+                             int lowest_level, int max_visits, int32_t* out_voxel, int32_t* out_dim,
+                             uint8_t* out_active, int32_t* out_level, float* out_box, float* out_t);
 
 /* Hybrid Tausworthe stream: n floats after seeding with `seed`. */
 void oracle_rng_stream(uint32_t seed, int n, float* out, uint32_t* out_state4);

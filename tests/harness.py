@@ -324,3 +324,56 @@ def golden_cases():
         sp = SceneSpec(**kw)
         out[name] = (sp, list(z[name + "__inv_view_proj"]), z[name + "__paths"], z[name + "__mean8"])
     return out
+
+
+# ---------------------------------------------------------------------------------------------
+# Sparse (NanoVDB) grids
+
+SPARSE_GOLDEN = __import__("os").path.join(__import__("os").path.dirname(__import__("os").path.abspath(__file__)),
+                                           "golden", "sparse_grids.npz")
+SPARSE_GRIDS = ["fbm24", "block8b", "block1", "ragged", "saturated40", "tiles256"]
+
+
+def sparse_grid(name: str) -> np.ndarray:
+    """Normalised dense grids [nz, ny, nx] of the sparse fixtures (as CloudData::getSparseDensityField
+    reads them through getDataFloatAtNorm)."""
+    if name == "fbm24":
+        g = bridge.fbm(24, 2, base_frequency=3.0, contrast=3.5)
+    elif name == "block8b":
+        g = cloud_block(8, 8, 8, empty_boundary=True)
+    elif name == "block1":
+        g = cloud_block(1, 1, 1)
+    elif name == "ragged":
+        g = bridge.fbm((40, 24, 33), 7, base_frequency=3.0, contrast=3.5)
+    elif name == "saturated40":
+        # high contrast: many leaves whose 512 voxels are all 1.0 become active lower-node tiles
+        g = bridge.fbm(40, 3, base_frequency=2.0, contrast=12.0)
+    elif name == "tiles256":
+        # a 128^3 constant region aligned to a lower node (pruned to an upper-node tile), a constant
+        # 8^3 leaf (pruned to a lower-node tile) and an fBm block with ragged leaves
+        g = np.zeros((256, 256, 256), np.float32)
+        g[0:128, 0:128, 0:128] = 0.7
+        g[0:8, 0:8, 136:144] = 0.5
+        g[16:80, 160:224, 160:224] = bridge.fbm(64, 5, base_frequency=3.0, contrast=3.5)
+    else:
+        raise KeyError(name)
+    vmin, vmax = bridge.minmax(g)
+    return bridge.normalize(g, vmin, vmax)
+
+
+def sparse_golden():
+    """name -> dict(buf, ijk, value, dim, active, walks=[(origin, dir, lowest level, walk records)], meta)."""
+    import json
+
+    z = np.load(SPARSE_GOLDEN)
+    meta = json.loads(str(z["meta"]))
+    out = {}
+    for name, m in meta.items():
+        walks = []
+        index, od = z[f"{name}__walk_index"], z[f"{name}__walk_od"]
+        parts = {f: z[f"{name}__walk_{f}"] for f in ("voxel", "dim", "active", "level", "box", "t")}
+        for (lv, start, n), ray in zip(index, od):
+            walks.append((ray[:3], ray[3:], int(lv), {f: a[start:start + n] for f, a in parts.items()}))
+        out[name] = dict(buf=z[f"{name}__buf"], ijk=z[f"{name}__ijk"], value=z[f"{name}__value"],
+                         dim=z[f"{name}__dim"], active=z[f"{name}__active"], walks=walks, meta=m)
+    return out

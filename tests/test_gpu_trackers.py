@@ -23,15 +23,19 @@ def core():
     c.close()
 
 
-def mean_image(core, sp, frames=SPP):
+def mean_image(core, sp, frames=SPP, sparse=False):
     setup_core(core, sp)
+    if sparse:
+        core("vpt_set_use_sparse_grid", 1)
     s, sq = gpu_render(core, sp, frames)
+    if sparse:
+        core("vpt_set_use_sparse_grid", 0)
     return s, sq
 
 
-def assert_equal_mean(core, sp0, sp1, eps=EPS, frames=SPP):
+def assert_equal_mean(core, sp0, sp1, eps=EPS, frames=SPP, sparse1=False):
     s0, _ = mean_image(core, sp0, frames)
-    s1, _ = mean_image(core, sp1, frames)
+    s1, _ = mean_image(core, sp1, frames, sparse=sparse1)
     m0 = (s0 / frames).mean(axis=(0, 1))
     m1 = (s1 / frames).mean(axis=(0, 1))
     print("means", m0, m1)
@@ -66,6 +70,13 @@ def test_delta_decomposition_equal_mean_boundary_layer(core):
 def test_delta_nee_equal_mean(core):
     g = cloud_block(8, 8, 8, empty_boundary=True)
     assert_equal_mean(core, spec(g, "delta"), spec(g, "nee"))
+
+
+@pytest.mark.parametrize("size", [1, 8])
+def test_delta_dense_sparse_equal_mean(core, size):
+    """DeltaTrackingGridTypesGrid1Test / Grid8Test (TestVolumetricPathTracing.cpp:176-196)."""
+    g = cloud_block(size, size, size)
+    assert_equal_mean(core, spec(g, "delta"), spec(g, "delta"), sparse1=True)
 
 
 # ---- beyond the reference's suite ----
