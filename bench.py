@@ -274,6 +274,9 @@ def run_ours(args):
     sparse = None
     if not args.no_sparse:
         sparse = run_sparse(vpt, lib, ctx, stream, ctypes_stream, barrier, max_over_ranks, world)
+    batch = None
+    if not args.no_batch:
+        batch = run_batch(lib, stream, ctypes_stream, barrier, max_over_ranks, world)
 
     if rank == 0:
         line = {
@@ -292,6 +295,8 @@ def run_ours(args):
             line["cpu_baseline"] = cpu
         if sparse is not None:
             line["sparse_nanovdb"] = sparse
+        if batch is not None:
+            line["batched_scenes"] = batch
         print(json.dumps(line), flush=True)
     vpt.cleanup()
     if world > 1:
@@ -361,6 +366,104 @@ def run_sparse(vpt, lib, ctx, stream, ctypes_stream, barrier, max_over_ranks, wo
     vpt.set_sparse_grid_fp16(False)
     vpt.set_use_sparse_grid(False)
     return out
+
+
+# Batched configuration: 64 independent scenes in one persistent launch (captured CUDA graph,
+# autotuned blocks per SM), delta tracking: grids log-uniform 64^3..512^3 (fBm, seed 1000 + i),
+# extinction log-uniform 100..2000, g uniform 0.6..0.9, images log-uniform 128^2..1024^2, spp uniform
+# 1..64, per-scene sun direction and camera pose.
+BATCH_SCENES = 64
+
+
+def batch_specs(n=None):
+    n = n or BATCH_SCENES
+    rng = np.random.default_rng(1000)
+    specs = []
+    for i in range(n):
+        grid = int(round(math.exp(rng.uniform(math.log(64), math.log(512)))))
+        res = int(round(math.exp(rng.uniform(math.log(128), math.log(1024)))))
+        specs.append(dict(seed=1000 + i, grid=grid, res=res, spp=int(rng.integers(1, 65)),
+                          extinction=float(math.exp(rng.uniform(math.log(100.0), math.log(2000.0)))),
+                          g=float(rng.uniform(0.6, 0.9)), sun=sun_dir(1000 + i), cam=camera_pos(1000 + i)))
+    return specs
+
+
+def run_batch(lib, stream, ctypes_stream, barrier, max_over_ranks, world, steps=3):
+    import ctypes
+    import torch
+    from cloudrendering_b200 import _lib
+
+    specs = batch_specs()
+    ctxs = []
+    t0 = time.perf_counter()
+    best = ctypes.c_int()
+    try:
+        for sp in specs:
+            c = ctypes.c_void_p()
+            _lib.check(lib.vpt_create(ctypes.byref(c), torch.cuda.current_device()), "create")
+            ctxs.append(c.value)
+            h = ctxs[-1]
+
+            def chk(st, what, h=h):
+                _lib.check(st, what, h)
+
+            chk(lib.vpt_set_max_grid_extent(h, 0.5), "extent")
+            chk(lib.vpt_generate_fbm_grid(h, sp["grid"], sp["grid"], sp["grid"], sp["seed"], 6, 2.0, 0.5, 3.0, 0.3),
+                "fbm")
+            chk(lib.vpt_set_vpt_mode(h, 0), "mode")
+            chk(lib.vpt_set_extinction_scale(h, sp["extinction"]), "extinction")
+            chk(lib.vpt_set_scattering_albedo(h, _lib.farr([0.99] * 3)), "albedo")
+            chk(lib.vpt_set_phase_g(h, sp["g"]), "g")
+            chk(lib.vpt_set_builtin_environment_map(h, 3), "env")
+            chk(lib.vpt_set_sky_color(h, _lib.farr([0.2] * 3)), "sky")
+            chk(lib.vpt_set_sun(h, _lib.farr(sp["sun"]), _lib.farr([5.0] * 3)), "sun")
+            chk(lib.vpt_set_camera(h, _lib.farr(sp["cam"]), _lib.farr([0, 0, 0]), _lib.farr([0, 1, 0]),
+                                   math.radians(60.0), 1.0 / 512.0, 80.0), "camera")
+            chk(lib.vpt_set_max_bounces(h, MAX_BOUNCES), "bounces")
+            chk(lib.vpt_set_resolution(h, sp["res"], sp["res"]), "resolution")
+            chk(lib.vpt_set_denoiser(h, 0), "denoiser")
+        torch.cuda.synchronize()
+        setup_s = time.perf_counter() - t0
+        paths_per_step = sum(sp["res"] * sp["res"] * sp["spp"] for sp in specs)
+        frames = (ctypes.c_int * len(specs))(*[sp["spp"] for sp in specs])
+        arr = (ctypes.c_void_p * len(ctxs))(*ctxs)
+        b = ctypes.c_void_p()
+        _lib.check(lib.vpt_batch_create(ctypes.byref(b), arr, len(ctxs)), "batch")
+        try:
+            if lib.vpt_batch_autotune(b, frames, ctypes_stream, ctypes.byref(best)) != 0:
+                raise RuntimeError(lib.vpt_batch_last_error(b).decode())
+            if lib.vpt_batch_render(b, frames, ctypes_stream) != 0:  # captures the graph
+                raise RuntimeError(lib.vpt_batch_last_error(b).decode())
+            barrier()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(steps):
+                if lib.vpt_batch_render(b, frames, ctypes_stream) != 0:
+                    raise RuntimeError(lib.vpt_batch_last_error(b).decode())
+            e1.record(stream)
+            barrier()
+            ms_batch = max_over_ranks(e0.elapsed_time(e1)) / steps
+        finally:
+            lib.vpt_batch_destroy(b)
+        # the same frames as one launch per scene
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for c, sp in zip(ctxs, specs):
+            _lib.check(lib.vpt_render_frames(c, sp["spp"], ctypes_stream), "render", c)
+        e1.record(stream)
+        barrier()
+        ms_seq = max_over_ranks(e0.elapsed_time(e1))
+    finally:
+        for c in ctxs:
+            lib.vpt_destroy(c)
+    return {"workload": f"{len(specs)} independent scenes (grids 64^3..512^3, images 128^2..1024^2, 1..64 spp, "
+                        "extinction 100..2000, g 0.6..0.9), delta tracking, one persistent launch per step "
+                        "(CUDA graph, autotuned blocks per SM)",
+            "scenes": len(specs), "paths_per_step": paths_per_step, "setup_s": setup_s,
+            "autotuned_blocks_per_sm": best.value,
+            "batched_path_samples_per_s": paths_per_step * world / (ms_batch / 1e3), "ms_per_step": ms_batch,
+            "one_launch_per_scene_path_samples_per_s": paths_per_step * world / (ms_seq / 1e3)}
 
 
 def cpu_baseline(lib, ctx, vpt, target_s=12.0):
@@ -469,6 +572,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-sparse", action="store_true", help="skip the NanoVDB sparse configuration")
+    ap.add_argument("--no-batch", action="store_true", help="skip the 64-scene batched configuration")
     ap.add_argument("--workload", choices=["full", "small"], default="full",
                     help="small: 384^3 grid, 512^2, 4 spp/step (for ncu captures; not a bench line)")
     args = ap.parse_args()
@@ -478,8 +582,9 @@ def main():
         global GRID, RES, SPP_PER_STEP, TRACKER_SPP
         GRID, RES, SPP_PER_STEP, TRACKER_SPP = 384, 512, 4, 1
         args.no_cpu_baseline = True
-        global SPARSE_DIMS, SPARSE_RES
+        global SPARSE_DIMS, SPARSE_RES, BATCH_SCENES
         SPARSE_DIMS, SPARSE_RES = (512, 256, 384), (480, 270)
+        BATCH_SCENES = 8
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -82,10 +82,30 @@ SIGNATURES = {
     "vpt_build_environment_pyramid": (c_int, [c_void_p, c_int, c_int, c_int, c_void_p, c_void_p]),
     "vpt_eaw_denoise_rgba": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_float, c_float, c_float,
                                      c_int, c_void_p, c_void_p]),
+    "vpt_batch_create": (c_int, [c_void_p, c_void_p, c_int]),
+    "vpt_batch_destroy": (None, [c_void_p]),
+    "vpt_batch_last_error": (c_char_p, [c_void_p]),
+    "vpt_batch_set_option": (c_int, [c_void_p, c_char_p, c_double]),
+    "vpt_batch_render": (c_int, [c_void_p, c_void_p, c_void_p]),
+    "vpt_batch_autotune": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    "vpt_batch_get_stats": (c_int, [c_void_p, c_void_p]),
+    "vpt_batch_reset_stats": (c_int, [c_void_p]),
+    "vpt_set_use_lights": (c_int, [c_void_p, c_int]),
+    "vpt_clear_lights": (c_int, [c_void_p]),
+    "vpt_add_light": (c_int, [c_void_p, c_void_p]),
+    "vpt_remove_light": (c_int, [c_void_p, c_int]),
+    "vpt_get_light_count": (c_int, [c_void_p, c_void_p]),
+    "vpt_set_light_property": (c_int, [c_void_p, c_int, c_char_p, c_char_p]),
     "vpt_set_use_sparse_grid": (c_int, [c_void_p, c_int]),
     "vpt_set_nanovdb_grid": (c_int, [c_void_p, c_void_p, ctypes.c_size_t, c_int]),
     "vpt_get_sparse_grid_info": (c_int, [c_void_p, c_void_p]),
     "vpt_sparse_query": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "vpt_kpn_apply": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_int, c_int, c_int, c_int, c_void_p,
+                              c_void_p]),
+    "vpt_kpn_inv_iter": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_int,
+                                 c_int, c_int, c_int, c_int, c_int, c_void_p, c_void_p]),
+    "vpt_kpn_avg_pool2": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_void_p, c_void_p]),
+    "vpt_kpn_reproject": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_int, c_int, c_void_p, c_void_p]),
     "vpt_eaw_denoise_rgba_noalloc": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_float, c_float,
                                              c_float, c_int, c_void_p, c_void_p]),
 }

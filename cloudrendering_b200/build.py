@@ -30,6 +30,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", INCLUDE
 # operation by operation (see the conventions at the top of vpt_device.cuh).
 PER_FILE = {
     "vpt_kernels.cu": ["--fmad=false"],
+    "vpt_kpn.cu": ["--fmad=false"],
 }
 # sources that hold the tracer's transcendental calls (built twice, see above)
 DOUBLE_ROUNDED = {"vpt_kernels.cu"}

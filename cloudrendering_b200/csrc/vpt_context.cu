@@ -179,6 +179,10 @@ struct VptContext {
     DevBuf<uint64_t> env_offsets;
     std::vector<uint64_t> env_offsets_host;
 
+    // lights of the light editor (LightEditorWidget), used by NEE when use_lights is set
+    bool use_lights = false;
+    std::vector<vpt::LightParams> lights;
+
     // camera (VolumetricPathTracingModuleRenderer.cpp:124-131)
     float cam_pos[3] = {0.0f, 0.0f, 0.8f};
     float cam_target[3] = {0.0f, 0.0f, 0.0f};
@@ -524,6 +528,14 @@ VptStatus fill_params(VptContext* ctx, int tracker, int frames, vpt::TraceParams
     P.counters = ctx->counters.ptr;
     P.error_flags = ctx->error_flags.ptr;
     P.work_counter = ctx->work_counter.ptr;
+    {
+        double view[16], iv[16];
+        compute_view(ctx, view);
+        mat_inverse(view, iv);
+        for (int i = 0; i < 16; i++) P.inv_view[i] = float(iv[i]);
+    }
+    P.num_lights = ctx->use_lights ? (int)ctx->lights.size() : 0;
+    for (int i = 0; i < P.num_lights; i++) P.lights[i] = ctx->lights[i];
     P.grid_kind = vpt::kDense;
     if (ctx->use_sparse && ctx->sparse_valid) {
         // superVoxelSize 8 (leaf level) unless the grid is smaller than a leaf
@@ -573,6 +585,159 @@ bool parse_float(const char* v, float& out) {
     char* end = nullptr;
     out = strtof(v, &end);
     return end && end != v;
+}
+
+}  // namespace
+
+namespace {
+
+vpt::LightParams default_light() {
+    // struct Light defaults (LightEditorWidget.hpp:69-85)
+    vpt::LightParams l{};
+    l.type = vpt::kLightPoint;
+    l.space = vpt::kLightSpaceView;
+    l.spot_total_width = 0.0981747704f;
+    l.spot_falloff_start = 0.0245436926f;
+    l.color = mk(1.0f, 0.961538462f, 0.884615385f);
+    l.intensity = 0.5f;
+    l.position = mk(0.0f, 0.0f, 0.0f);
+    l.use_distance = 1;
+    l.spot_direction = mk(0.0f, 0.0f, -1.0f);
+    return l;
+}
+
+bool parse_vec3(const char* v, F3& out) {
+    float a[3];
+    const char* p = v;
+    for (int i = 0; i < 3; i++) {
+        char* end = nullptr;
+        a[i] = strtof(p, &end);
+        if (end == p) return false;
+        p = end;
+    }
+    while (*p == ' ' || *p == '\t' || *p == '\n') p++;
+    if (*p != '\0') return false;
+    out = mk(a[0], a[1], a[2]);
+    return true;
+}
+
+}  // namespace
+
+struct VptBatch {
+    std::vector<VptContext*> ctxs;
+    int device = 0;
+    int num_sms = 148;
+    vpt::TraceParams* h_params = nullptr;     // pinned staging, read by the launch's first copy
+    unsigned long long* h_offsets = nullptr;  // pinned staging
+    vpt::TraceParams* d_params = nullptr;
+    unsigned long long* d_offsets = nullptr;
+    unsigned long long* d_counters = nullptr; // [0] work counter, [1] paths, [2] lookups
+    int* d_err = nullptr;
+    int blocks_per_sm = 0;                    // 0: occupancy calculator; set by vpt_batch_autotune
+    bool use_graph = true;
+    cudaStream_t capture_stream = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int exec_key[4] = {-1, -1, -1, -1};       // tracker, interp, grid kind, blocks of the captured launch
+    cudaEvent_t done = nullptr;               // after the last launch (guards the pinned staging)
+    bool launched = false;
+    std::string last_error;
+};
+
+namespace {
+
+VptStatus batch_fail(VptBatch* b, VptStatus st, const std::string& msg) {
+    if (b) b->last_error = msg;
+    return st;
+}
+
+void batch_release(VptBatch* b) {
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->capture_stream) cudaStreamDestroy(b->capture_stream);
+    if (b->done) cudaEventDestroy(b->done);
+    cudaFreeHost(b->h_params);
+    cudaFreeHost(b->h_offsets);
+    cudaFree(b->d_params);
+    cudaFree(b->d_offsets);
+    cudaFree(b->d_counters);
+    cudaFree(b->d_err);
+}
+
+// Prepares every context (acceleration structures, film) and stages the launch parameters.
+VptStatus batch_prepare(VptBatch* b, const int* frames, cudaStream_t s, vpt::BatchLaunch& L) {
+    const int n = (int)b->ctxs.size();
+    if (b->launched && cudaEventSynchronize(b->done) != cudaSuccess)
+        return batch_fail(b, VPT_ERR_CUDA, "previous batch launch failed");
+    int tracker = -1, interp = -1, grid_kind = -1;
+    b->h_offsets[0] = 0;
+    for (int i = 0; i < n; i++) {
+        VptContext* ctx = b->ctxs[i];
+        if (frames[i] < 0) return batch_fail(b, VPT_ERR_ARG, "frames must be >= 0");
+        if (!ctx->norm.ptr && !(ctx->use_sparse && ctx->sparse_valid))
+            return batch_fail(b, VPT_ERR_STATE, "a context has no volume loaded");
+        if (ctx->width <= 0) return batch_fail(b, VPT_ERR_STATE, "a context has no resolution");
+        const int t = tracker_of(ctx->mode);
+        const int gk = ctx->use_sparse ? vpt::kNanoVdb : vpt::kDense;
+        if (i == 0) {
+            tracker = t;
+            interp = ctx->interp;
+            grid_kind = gk;
+        } else if (t != tracker || ctx->interp != interp || gk != grid_kind) {
+            return batch_fail(b, VPT_ERR_UNSUPPORTED,
+                              "all contexts of a batch need the same tracker, interpolation and grid kind");
+        }
+        if (!(t == vpt::kDelta || t == vpt::kRatio || (t == vpt::kNextEvent && !ctx->use_ess)))
+            return batch_fail(b, VPT_ERR_UNSUPPORTED,
+                              "batched rendering supports delta, ratio and NEE (without empty space skipping)");
+        if (features_needed(ctx)) return batch_fail(b, VPT_ERR_UNSUPPORTED, "batched rendering writes no feature maps");
+        if (ctx->env_kind == VPT_ENV_IMAGE && !ctx->env_pyramid.ptr)
+            return batch_fail(b, VPT_ERR_STATE, "environment image not loaded");
+        VptStatus st = ensure_accel(ctx, t, s);
+        if (st == VPT_OK) st = ensure_film(ctx, s);
+        if (st != VPT_OK) return batch_fail(b, st, ctx->last_error);
+        fill_params(ctx, t, frames[i], b->h_params[i]);
+        b->h_offsets[i + 1] = b->h_offsets[i] + vpt::padded_paths(ctx->width, ctx->height, (uint32_t)frames[i]);
+    }
+    int per_sm = b->blocks_per_sm;
+    if (per_sm <= 0) {
+        vpt::BatchLaunch q{};
+        q.tracker = tracker;
+        q.interp = interp;
+        q.grid_kind = grid_kind;
+        q.blocks_per_sm_out = &per_sm;
+        if (vpt::launch_trace_batch(q, s) != cudaSuccess) return batch_fail(b, VPT_ERR_CUDA, "occupancy query failed");
+    }
+    L = vpt::BatchLaunch{};
+    L.scenes = b->d_params;
+    L.offsets = b->d_offsets;
+    L.num = n;
+    L.tracker = tracker;
+    L.interp = interp;
+    L.grid_kind = grid_kind;
+    L.blocks = per_sm * b->num_sms;
+    L.work_counter = b->d_counters;
+    L.counters = b->d_counters + 1;
+    L.error_flags = b->d_err;
+    return VPT_OK;
+}
+
+// copy parameters -> zero the work counter -> trace, on stream s
+cudaError_t batch_enqueue(VptBatch* b, const vpt::BatchLaunch& L, cudaStream_t s) {
+    const int n = (int)b->ctxs.size();
+    cudaError_t e = cudaMemcpyAsync(b->d_params, b->h_params, sizeof(vpt::TraceParams) * n, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(b->d_offsets, b->h_offsets, sizeof(unsigned long long) * (n + 1), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(b->d_counters, 0, sizeof(unsigned long long), s);
+    if (e == cudaSuccess) e = vpt::launch_trace_batch(L, s);
+    return e;
+}
+
+void batch_commit(VptBatch* b, const int* frames) {
+    for (size_t i = 0; i < b->ctxs.size(); i++) {
+        VptContext* ctx = b->ctxs[i];
+        ctx->frame_count += (uint32_t)frames[i];
+        ctx->film_frames += (uint32_t)frames[i];
+        ctx->frames_total += (uint64_t)frames[i];
+    }
 }
 
 }  // namespace
@@ -1256,6 +1421,258 @@ VptStatus vpt_set_denoiser_property(VptContext* ctx, const char* key, const char
 VptStatus vpt_set_use_empty_space_skipping(VptContext* ctx, int enabled) {
     VPT_CHECK_CTX(ctx);
     ctx->use_ess = enabled ? 1 : 0;
+    reset_film_state(ctx);
+    return VPT_OK;
+}
+
+// ---- batched rendering: many contexts in one persistent launch ----
+
+VptStatus vpt_batch_create(VptBatch** out, VptContext* const* ctxs, int count) {
+    if (!out || !ctxs || count <= 0) return VPT_ERR_ARG;
+    *out = nullptr;
+    for (int i = 0; i < count; i++) {
+        if (!ctxs[i]) return VPT_ERR_ARG;
+        if (ctxs[i]->device != ctxs[0]->device) return VPT_ERR_ARG;
+    }
+    VptBatch* b = new VptBatch();
+    b->ctxs.assign(ctxs, ctxs + count);
+    b->device = ctxs[0]->device;
+    b->num_sms = ctxs[0]->num_sms;
+    cudaSetDevice(b->device);
+    cudaError_t e = cudaMallocHost(reinterpret_cast<void**>(&b->h_params), sizeof(vpt::TraceParams) * count);
+    if (e == cudaSuccess)
+        e = cudaMallocHost(reinterpret_cast<void**>(&b->h_offsets), sizeof(unsigned long long) * (count + 1));
+    if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&b->d_params), sizeof(vpt::TraceParams) * count);
+    if (e == cudaSuccess)
+        e = cudaMalloc(reinterpret_cast<void**>(&b->d_offsets), sizeof(unsigned long long) * (count + 1));
+    if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&b->d_counters), sizeof(unsigned long long) * 3);
+    if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&b->d_err), sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(b->d_counters, 0, sizeof(unsigned long long) * 3);
+    if (e == cudaSuccess) e = cudaMemset(b->d_err, 0, sizeof(int));
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->capture_stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming);
+    if (e != cudaSuccess) {
+        batch_release(b);
+        delete b;
+        return e == cudaErrorMemoryAllocation ? VPT_ERR_OOM : VPT_ERR_CUDA;
+    }
+    *out = b;
+    return VPT_OK;
+}
+
+void vpt_batch_destroy(VptBatch* b) {
+    if (!b) return;
+    cudaSetDevice(b->device);
+    cudaDeviceSynchronize();
+    batch_release(b);
+    delete b;
+}
+
+const char* vpt_batch_last_error(VptBatch* b) { return b ? b->last_error.c_str() : ""; }
+
+VptStatus vpt_batch_set_option(VptBatch* b, const char* key, double value) {
+    if (!b || !key) return VPT_ERR_ARG;
+    std::string k(key);
+    if (k == "use_graph") {
+        b->use_graph = value != 0.0;
+    } else if (k == "blocks_per_sm") {
+        if (value < 0 || value > 64) return batch_fail(b, VPT_ERR_ARG, "blocks_per_sm out of range");
+        b->blocks_per_sm = int(value);
+    } else {
+        return batch_fail(b, VPT_ERR_ARG, "unknown batch option " + k);
+    }
+    return VPT_OK;
+}
+
+VptStatus vpt_batch_render(VptBatch* b, const int* frames, void* stream) {
+    if (!b || !frames) return VPT_ERR_ARG;
+    cudaSetDevice(b->device);
+    cudaStream_t s = as_stream(stream);
+    vpt::BatchLaunch L;
+    VptStatus st = batch_prepare(b, frames, s, L);
+    if (st != VPT_OK) return st;
+    cudaError_t e = cudaSuccess;
+    if (b->use_graph) {
+        const int key[4] = {L.tracker, L.interp, L.grid_kind, L.blocks};
+        if (!b->exec || memcmp(key, b->exec_key, sizeof(key)) != 0) {
+            if (b->exec) {
+                cudaGraphExecDestroy(b->exec);
+                b->exec = nullptr;
+            }
+            cudaGraph_t g = nullptr;
+            e = cudaStreamBeginCapture(b->capture_stream, cudaStreamCaptureModeThreadLocal);
+            if (e == cudaSuccess) {
+                vpt::BatchLaunch Lc = L;
+                Lc.counted = false;  // counted when the graph is launched
+                cudaError_t e2 = batch_enqueue(b, Lc, b->capture_stream);
+                e = cudaStreamEndCapture(b->capture_stream, &g);
+                if (e == cudaSuccess) e = e2;
+            }
+            if (e == cudaSuccess) e = cudaGraphInstantiate(&b->exec, g, 0);
+            if (g) cudaGraphDestroy(g);
+            if (e != cudaSuccess)
+                return batch_fail(b, VPT_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+            memcpy(b->exec_key, key, sizeof(key));
+        }
+        e = cudaGraphLaunch(b->exec, s);
+        if (e == cudaSuccess) vpt::count_launches(1);
+    } else {
+        e = batch_enqueue(b, L, s);
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(b->done, s);
+    if (e != cudaSuccess) return batch_fail(b, VPT_ERR_CUDA, std::string("batch launch: ") + cudaGetErrorString(e));
+    b->launched = true;
+    batch_commit(b, frames);
+    return VPT_OK;
+}
+
+VptStatus vpt_batch_autotune(VptBatch* b, const int* frames, void* stream, int* out_blocks_per_sm) {
+    if (!b || !frames) return VPT_ERR_ARG;
+    cudaSetDevice(b->device);
+    cudaStream_t s = as_stream(stream);
+    const int saved = b->blocks_per_sm;
+    const bool saved_graph = b->use_graph;
+    b->blocks_per_sm = 0;
+    b->use_graph = false;
+    vpt::BatchLaunch L;
+    VptStatus st = batch_prepare(b, frames, s, L);  // occupancy limit
+    if (st != VPT_OK) {
+        b->blocks_per_sm = saved;
+        b->use_graph = saved_graph;
+        return st;
+    }
+    const int max_per_sm = L.blocks / b->num_sms;
+    const int cands[4] = {max_per_sm, (3 * max_per_sm) / 4, max_per_sm / 2, max_per_sm / 4};
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    float best_ms = 1e30f;
+    int best = max_per_sm;
+    for (int c = 0; c < 5 && st == VPT_OK; c++) {
+        const int per_sm = c == 0 ? max_per_sm : cands[c - 1];  // the first run warms up
+        if (per_sm <= 0) continue;
+        b->blocks_per_sm = per_sm;
+        cudaEventRecord(e0, s);
+        st = vpt_batch_render(b, frames, stream);
+        cudaEventRecord(e1, s);
+        if (st != VPT_OK) break;
+        if (cudaEventSynchronize(e1) != cudaSuccess) {
+            st = batch_fail(b, VPT_ERR_CUDA, "autotune launch failed");
+            break;
+        }
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (c > 0 && ms < best_ms) {
+            best_ms = ms;
+            best = per_sm;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    // the calibration renders went into the films: start the accumulation over
+    for (VptContext* ctx : b->ctxs) reset_film_state(ctx);
+    b->use_graph = saved_graph;
+    b->blocks_per_sm = st == VPT_OK ? best : saved;
+    if (out_blocks_per_sm) *out_blocks_per_sm = b->blocks_per_sm;
+    return st;
+}
+
+VptStatus vpt_batch_get_stats(VptBatch* b, VptStats* out) {
+    if (!b || !out) return VPT_ERR_ARG;
+    cudaSetDevice(b->device);
+    unsigned long long c[3];
+    int err = 0;
+    if (cudaMemcpy(c, b->d_counters, sizeof(c), cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(&err, b->d_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return batch_fail(b, VPT_ERR_CUDA, "reading batch counters failed");
+    memset(out, 0, sizeof(*out));
+    out->paths = c[1];
+    out->density_lookups = c[2];
+    out->error_flags = err;
+    return VPT_OK;
+}
+
+VptStatus vpt_batch_reset_stats(VptBatch* b) {
+    if (!b) return VPT_ERR_ARG;
+    cudaSetDevice(b->device);
+    if (cudaMemset(b->d_counters, 0, sizeof(unsigned long long) * 3) != cudaSuccess ||
+        cudaMemset(b->d_err, 0, sizeof(int)) != cudaSuccess)
+        return batch_fail(b, VPT_ERR_CUDA, "resetting batch counters failed");
+    return VPT_OK;
+}
+
+// ---- lights (LightEditorWidget, src/PathTracer/LightEditorWidget.cpp:89-103, 286-320) ----
+
+VptStatus vpt_set_use_lights(VptContext* ctx, int use_lights) {
+    VPT_CHECK_CTX(ctx);
+    if ((use_lights != 0) != ctx->use_lights) reset_film_state(ctx);
+    ctx->use_lights = use_lights != 0;
+    return VPT_OK;
+}
+
+VptStatus vpt_clear_lights(VptContext* ctx) {
+    VPT_CHECK_CTX(ctx);
+    ctx->lights.clear();
+    reset_film_state(ctx);
+    return VPT_OK;
+}
+
+VptStatus vpt_add_light(VptContext* ctx, int* out_index) {
+    VPT_CHECK_CTX(ctx);
+    if ((int)ctx->lights.size() >= vpt::kMaxLights)
+        return fail(ctx, VPT_ERR_UNSUPPORTED, "too many lights (at most 16)");
+    ctx->lights.push_back(default_light());
+    if (out_index) *out_index = (int)ctx->lights.size() - 1;
+    reset_film_state(ctx);
+    return VPT_OK;
+}
+
+VptStatus vpt_remove_light(VptContext* ctx, int index) {
+    VPT_CHECK_CTX(ctx);
+    if (index >= 0 && index < (int)ctx->lights.size()) ctx->lights.erase(ctx->lights.begin() + index);
+    reset_film_state(ctx);
+    return VPT_OK;
+}
+
+VptStatus vpt_get_light_count(VptContext* ctx, int* out_count) {
+    VPT_CHECK_CTX(ctx);
+    if (!out_count) return VPT_ERR_ARG;
+    *out_count = (int)ctx->lights.size();
+    return VPT_OK;
+}
+
+VptStatus vpt_set_light_property(VptContext* ctx, int index, const char* key, const char* value) {
+    VPT_CHECK_CTX(ctx);
+    if (!key || !value) return VPT_ERR_ARG;
+    if (index < 0 || index >= (int)ctx->lights.size())
+        return fail(ctx, VPT_ERR_ARG, "Error in LightEditorWidget::setLightProperty: Invalid light index.");
+    vpt::LightParams& l = ctx->lights[index];
+    std::string k(key), v(value);
+    static const char* kTypes[] = {"Point Light", "Spotlight", "Directional Light"};
+    static const char* kSpaces[] = {"World", "View", "View Orientation"};
+    F3 vec;
+    float f;
+    if (k == "type") {
+        for (int i = 0; i < 3; i++)
+            if (v == kTypes[i]) l.type = i;
+    } else if (k == "space") {
+        for (int i = 0; i < 3; i++)
+            if (v == kSpaces[i]) l.space = i;
+    } else if (k == "color" || k == "position" || k == "direction" || k == "spot_direction") {
+        if (!parse_vec3(value, vec)) return fail(ctx, VPT_ERR_ARG, "Error in stringToVec3: Invalid number of entries.");
+        if (k == "color") l.color = vec;
+        else if (k == "spot_direction") l.spot_direction = vec;
+        else l.position = vec;
+    } else if (k == "intensity" || k == "spot_total_width" || k == "spot_falloff_start") {
+        if (!parse_float(value, f)) return fail(ctx, VPT_ERR_ARG, "invalid number for light property " + k);
+        if (k == "intensity") l.intensity = f;
+        else if (k == "spot_total_width") l.spot_total_width = f;
+        else l.spot_falloff_start = f;
+    } else if (k == "use_distance") {
+        // the reference writes this flag into the intensity (LightEditorWidget.cpp:305-306); here it
+        // sets the distance falloff, as the property's name says
+        l.use_distance = (v == "1" || v == "true" || v == "True") ? 1 : 0;
+    }
     reset_film_state(ctx);
     return VPT_OK;
 }

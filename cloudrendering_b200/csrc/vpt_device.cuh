@@ -118,6 +118,61 @@ VPT_DEV void camera_ray(const TraceParams& P, float sx, float sy, F3& x, F3& w) 
     w = normalize3(vt - vp);
 }
 
+// ---------------------------------------------------------------------------------------------
+// Lights of the light editor (VptUtils.glsl:394-453), sampled by next event tracking.
+
+// (m * vec4(v, w)).xyz for a column-major mat4, summed column by column.
+VPT_DEV F3 mat4_mul_xyz(const float* m, F3 v, float w) {
+    return f3(((m[0] * v.x + m[4] * v.y) + m[8] * v.z) + m[12] * w,
+              ((m[1] * v.x + m[5] * v.y) + m[9] * v.z) + m[13] * w,
+              ((m[2] * v.x + m[6] * v.y) + m[10] * v.z) + m[14] * w);
+}
+
+VPT_DEV F3 light_position(const TraceParams& P, const LightParams& L) {
+    if (L.space == kLightSpaceView || L.space == kLightSpaceViewOrientation) {
+        const float hom = (L.type == kLightDirectional || L.space == kLightSpaceViewOrientation) ? 0.0f : 1.0f;
+        return mat4_mul_xyz(P.inv_view, L.position, hom);
+    }
+    return L.position;
+}
+
+// getHeadlightDirection: picks a light uniformly when there are several (one random number),
+// returns the unit direction to it and its distance.
+VPT_DEV F3 light_direction(const TraceParams& P, F3 pos, Rng& rng, int& idx, float& prob_factor, float& dist) {
+    if (P.num_lights > 1) {
+        const uint32_t k = (uint32_t)(rng_next(rng) * (float)P.num_lights);
+        idx = (int)min(k, (uint32_t)P.num_lights - 1u);
+        prob_factor *= (float)P.num_lights;
+    }
+    const LightParams& L = P.lights[idx];
+    const F3 lp = light_position(P, L);
+    const F3 dir = (L.type == kLightPoint || L.type == kLightSpot) ? lp - pos : lp;
+    dist = length3(dir);
+    const float s = dist + 1e-5f;
+    return f3(dir.x / s, dir.y / s, dir.z / s);
+}
+
+// sampleHeadlight: radiance of light `idx` seen from `pos` (distance falloff, spot cone).
+VPT_DEV F3 light_radiance(const TraceParams& P, F3 pos, int idx) {
+    const LightParams& L = P.lights[idx];
+    const F3 lp = light_position(P, L);
+    float f = L.intensity;
+    if ((L.type == kLightPoint || L.type == kLightSpot) && L.use_distance != 0) {
+        const F3 diff = lp - pos;
+        f /= fmaxf(dot3(diff, diff), 1e-3f);
+    }
+    if (L.type == kLightSpot) {
+        const float total = m_cos(L.spot_total_width);
+        const float falloff = L.spot_total_width > L.spot_falloff_start ? m_cos(L.spot_falloff_start) : total;
+        const F3 p = pos - lp;
+        F3 z = normalize3(L.spot_direction);
+        if (L.space == kLightSpaceView || L.space == kLightSpaceViewOrientation) z = mat4_mul_xyz(P.inv_view, z, 0.0f);
+        const float cos_theta = dot3(z, p) / (length3(z) * length3(p));
+        f *= smoothstepf(total, falloff, cos_theta);
+    }
+    return f3(f * L.color.x, f * L.color.y, f * L.color.z);
+}
+
 // Slab test with a 1e-6 clamp of near-zero direction components (rayBoxIntersect,
 // VptUtils.glsl:763-801; the clip plane is not supported).
 VPT_DEV bool ray_box(F3 bmin, F3 bmax, F3 p, F3 d, float& tmin, float& tmax) {

@@ -209,12 +209,13 @@ VPT_DEV void refill_finish(const TraceParams& P, size_t pix, F3 L, bool& has) {
     has = false;
 }
 
-// Shadow ray done: add the light sample (f = pdf_phase / pdf_light * T, NextEventTracking.glsl:367-369)
+// Shadow ray done: add the light sample (f = weight * T with weight = pdf_phase / pdf_light for the
+// sky, or the light probability factor times pdf_phase for a light; NextEventTracking.glsl:348-369)
 // and resume the primary path at the scatter point with the sampled direction.
 VPT_DEV void end_shadow(const TraceParams& P, F3& color, F3& x, F3& w, float& d, F3 xp, F3 nw, float dp,
-                        float weight, float ts, int& mode) {
+                        float weight, float ts, int light, int& mode) {
     const float f = weight * ts;
-    const F3 l = sky_and_sun(P, w);
+    const F3 l = light >= 0 ? light_radiance(P, xp, light) : sky_and_sun(P, w);
     color = color + f3(f * l.x, f * l.y, f * l.z);
     x = xp;
     w = nw;
@@ -227,9 +228,50 @@ VPT_DEV void end_shadow(const TraceParams& P, F3& color, F3& x, F3& w, float& d,
     }
 }
 
-template <int TRACKER, int INTERP, int GRID>
-__global__ void __launch_bounds__(kTraceBlock) trace_refill_kernel(const __grid_constant__ TraceParams P, uint64_t total) {
-    Sampler<INTERP, GRID> sample{P};
+// Where the parameters of a path come from: one scene (the kernel's constant parameter block) or a
+// batch of scenes in global memory whose path ids are concatenated scene after scene.
+struct OneScene {
+    const TraceParams& P;
+    VPT_DEV const TraceParams& scene(int) const { return P; }
+    VPT_DEV int locate(unsigned long long&) const { return 0; }
+};
+struct SceneBatch {
+    const TraceParams* scenes;
+    const unsigned long long* offsets;  // num + 1 prefix sums of the scenes' path counts
+    int num;
+    VPT_DEV const TraceParams& scene(int s) const { return scenes[s]; }
+    // scene of global path id p (binary search); p becomes the scene-local id
+    VPT_DEV int locate(unsigned long long& p) const {
+        int lo = 0, hi = num - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (__ldg(offsets + mid) <= p) lo = mid;
+            else hi = mid - 1;
+        }
+        p -= __ldg(offsets + lo);
+        return lo;
+    }
+};
+
+VPT_DEV void flush_counters_to(unsigned long long* counters, int* error_flags, uint32_t paths, uint32_t lookups,
+                               bool guard_hit) {
+    unsigned long long l = lookups;
+    unsigned long long n = paths;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        l += __shfl_xor_sync(0xffffffffu, l, o);
+        n += __shfl_xor_sync(0xffffffffu, n, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(counters + 0, n);
+        atomicAdd(counters + 1, l);
+    }
+    if (guard_hit) atomicOr(error_flags, kErrIterLimit);
+}
+
+template <int TRACKER, int INTERP, int GRID, class SRC>
+VPT_DEV void refill_loop(const SRC& src, uint64_t total, unsigned long long* work_counter,
+                         unsigned long long* counters, int* error_flags) {
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const unsigned lt_mask = (1u << lane) - 1u;
@@ -243,8 +285,10 @@ __global__ void __launch_bounds__(kTraceBlock) trace_refill_kernel(const __grid_
     Rng rng;
     F3 x = zero, w = zero, color = zero, xp = zero, nw = zero;
     float d = 0.0f, dp = 0.0f, trans = 1.0f, ts = 1.0f, weight = 0.0f;
-    int mode = kModePrimary, bounces = 0;
+    float shadow_dist = 0.0f, shadow_max = 0.0f;  // distance walked / light distance (light shadow rays)
+    int mode = kModePrimary, bounces = 0, light = -1;
     bool ev = false;
+    int scene = 0;
     uint32_t steps = 0;
     size_t pix = 0;
     uint32_t lookups = 0, paths = 0;
@@ -260,8 +304,7 @@ __global__ void __launch_bounds__(kTraceBlock) trace_refill_kernel(const __grid_
             unsigned long long fresh = 0;
             if (n > q_left) {
                 unsigned long long b = 0;
-                if (lane == 0) b = atomicAdd(reinterpret_cast<unsigned long long*>(P.work_counter),
-                                             (unsigned long long)kRefillBatch);
+                if (lane == 0) b = atomicAdd(work_counter, (unsigned long long)kRefillBatch);
                 fresh = __shfl_sync(FULL, b, 0);
             }
             if (need) {
@@ -269,9 +312,14 @@ __global__ void __launch_bounds__(kTraceBlock) trace_refill_kernel(const __grid_
                                                   : fresh + (unsigned long long)(r - q_left);
                 uint32_t frame;
                 int px, py;
-                if (p >= total) {
+                const bool done = p >= total;
+                int s = 0;
+                if (!done) s = src.locate(p);
+                const TraceParams& P = src.scene(s);
+                if (done) {
                     exhausted = true;
                 } else if (decode_path(P, p, frame, px, py)) {
+                    scene = s;
                     const uint32_t w_u = (uint32_t)P.width, h_u = (uint32_t)P.height;
                     uint32_t seed = (P.global_frame + frame) * w_u * h_u + (uint32_t)px + (uint32_t)py * w_u;
                     seed += P.seed_offset;
@@ -315,13 +363,19 @@ __global__ void __launch_bounds__(kTraceBlock) trace_refill_kernel(const __grid_
         if (!has) continue;
 
         // ---- one tentative collision ----
+        const TraceParams& P = src.scene(scene);
+        Sampler<INTERP, GRID> sample{P};
         if (++steps > P.max_steps) {
             guard_hit = true;
             refill_finish<TRACKER>(P, pix, TRACKER == kNextEvent ? color : zero, has);
             continue;
         }
         const float t = free_path(rng, P.inv_extinction);
-        const bool escape = t > d;
+        bool escape = t > d;
+        if (TRACKER == kNextEvent && mode == kModeShadow && light >= 0) {
+            shadow_dist += t;
+            escape = escape || shadow_dist > shadow_max;
+        }
         float density = 0.0f;
         if (!escape) {
             F3 xn = x + w * t;
@@ -335,7 +389,7 @@ __global__ void __launch_bounds__(kTraceBlock) trace_refill_kernel(const __grid_
                 d -= t;
                 continue;
             }
-            end_shadow(P, color, x, w, d, xp, nw, dp, weight, ts, mode);
+            end_shadow(P, color, x, w, d, xp, nw, dp, weight, ts, light, mode);
             continue;
         }
         if (escape) {
@@ -360,9 +414,21 @@ __global__ void __launch_bounds__(kTraceBlock) trace_refill_kernel(const __grid_
             if (TRACKER == kNextEvent) {
                 nw = sample_phase(rng, P.g, w);
                 ev = true;
-                float pdf_light;
-                F3 dir = importance_sample_sky(P, rng, pdf_light);
-                weight = evaluate_phase(P.g, w, dir) / pdf_light;
+                bool to_light = false;
+                float prob_factor = 1.0f, pdf_light = 0.0f, light_dist = 0.0f;
+                int light_idx = 0;
+                if (P.num_lights > 0) {
+                    to_light = P.env_is_black ? true : (rng_next(rng) > 0.5f);
+                    prob_factor = P.env_is_black ? 1.0f : 2.0f;
+                }
+                F3 dir;
+                if (to_light) dir = light_direction(P, x, rng, light_idx, prob_factor, light_dist);
+                else dir = importance_sample_sky(P, rng, pdf_light);
+                const float pdf_phase = evaluate_phase(P.g, w, dir);
+                if (P.num_lights > 0) weight = to_light ? prob_factor * pdf_phase : (prob_factor * pdf_phase) / pdf_light;
+                else weight = pdf_phase / pdf_light;
+                light = to_light ? light_idx : -1;
+                shadow_max = light_dist;
                 xp = x;
                 dp = d;
                 w = dir;
@@ -371,9 +437,10 @@ __global__ void __launch_bounds__(kTraceBlock) trace_refill_kernel(const __grid_
                 if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
                     x = x + w * tmin;
                     d = tmax - tmin;
+                    shadow_dist = tmin;
                 } else {
                     // no shadow steps (and no random numbers), like calculateTransmittance
-                    end_shadow(P, color, x, w, d, xp, nw, dp, weight, ts, mode);
+                    end_shadow(P, color, x, w, d, xp, nw, dp, weight, ts, light, mode);
                 }
                 continue;
             }
@@ -391,7 +458,64 @@ __global__ void __launch_bounds__(kTraceBlock) trace_refill_kernel(const __grid_
             d -= t;
         }
     }
-    flush_counters(P, paths, lookups, guard_hit);
+    flush_counters_to(counters, error_flags, paths, lookups, guard_hit);
+}
+
+template <int TRACKER, int INTERP, int GRID>
+__global__ void __launch_bounds__(kTraceBlock) trace_refill_kernel(const __grid_constant__ TraceParams P, uint64_t total) {
+    refill_loop<TRACKER, INTERP, GRID>(OneScene{P}, total, reinterpret_cast<unsigned long long*>(P.work_counter),
+                                       P.counters, P.error_flags);
+}
+
+// Many independent scenes (own grid, camera, image size, spp, medium) traced by one persistent
+// launch: lanes refill from one id space that concatenates the scenes' paths.  The total path count
+// is read from offsets[num], so a captured launch serves any frame counts.
+template <int TRACKER, int INTERP, int GRID>
+__global__ void __launch_bounds__(kTraceBlock) trace_batch_kernel(const TraceParams* __restrict__ scenes,
+                                                                  const unsigned long long* __restrict__ offsets,
+                                                                  int num, unsigned long long* work_counter,
+                                                                  unsigned long long* counters, int* error_flags) {
+    refill_loop<TRACKER, INTERP, GRID>(SceneBatch{scenes, offsets, num}, __ldg(offsets + num), work_counter, counters,
+                                       error_flags);
+}
+
+template <int TRACKER, int INTERP, int GRID>
+static cudaError_t batch_t(const BatchLaunch& b, cudaStream_t s) {
+    if (b.blocks_per_sm_out) {
+        int per_sm = 0;
+        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_batch_kernel<TRACKER, INTERP, GRID>,
+                                                                      kTraceBlock, 0);
+        *b.blocks_per_sm_out = per_sm > 0 ? per_sm : 1;
+        return e;
+    }
+    trace_batch_kernel<TRACKER, INTERP, GRID><<<b.blocks, kTraceBlock, 0, s>>>(b.scenes, b.offsets, b.num,
+                                                                              b.work_counter, b.counters,
+                                                                              b.error_flags);
+    if (b.counted) count_launches(1);
+    return cudaGetLastError();
+}
+
+template <int TRACKER, int GRID>
+static cudaError_t batch_interp(const BatchLaunch& b, cudaStream_t s) {
+    switch (b.interp) {
+        case kNearest: return batch_t<TRACKER, kNearest, GRID>(b, s);
+        case kStochastic: return batch_t<TRACKER, kStochastic, GRID>(b, s);
+        default: return batch_t<TRACKER, kTrilinear, GRID>(b, s);
+    }
+}
+
+template <int GRID>
+static cudaError_t batch_tracker(const BatchLaunch& b, cudaStream_t s) {
+    switch (b.tracker) {
+        case kDelta: return batch_interp<kDelta, GRID>(b, s);
+        case kRatio: return batch_interp<kRatio, GRID>(b, s);
+        case kNextEvent: return batch_interp<kNextEvent, GRID>(b, s);
+        default: return cudaErrorNotSupported;
+    }
+}
+
+cudaError_t launch_trace_batch(const BatchLaunch& b, cudaStream_t s) {
+    return b.grid_kind == kNanoVdb ? batch_tracker<kNanoVdb>(b, s) : batch_tracker<kDense>(b, s);
 }
 
 uint64_t padded_paths(int width, int height, uint32_t frames) {

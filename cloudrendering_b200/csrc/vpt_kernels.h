@@ -34,6 +34,22 @@ cudaError_t launch_supervoxel_stats(const float* dens, int nx, int ny, int nz, i
 cudaError_t launch_rrt_params(const float* mn, const float* mx, const float* avg, int total, float extinction,
                               float D, float* out_pairs, cudaStream_t s);
 cudaError_t launch_interleave(const float* a, const float* b, int total, float* out_pairs, cudaStream_t s);
+// One persistent launch over many scenes (see trace_batch_kernel).  With blocks_per_sm_out set, only
+// reports the kernel's resident blocks per SM (occupancy calculator) and launches nothing.
+struct BatchLaunch {
+    const TraceParams* scenes;           // device array, num entries
+    const unsigned long long* offsets;   // device array, num + 1 prefix sums of padded path counts
+    int num;
+    int tracker, interp, grid_kind;      // common to every scene of the batch
+    int blocks;
+    unsigned long long* work_counter;    // zeroed before the launch
+    unsigned long long* counters;        // [0] paths, [1] density lookups (accumulated)
+    int* error_flags;
+    int* blocks_per_sm_out;
+    bool counted = true;                 // add the launch to the launch counter (not while capturing)
+};
+cudaError_t launch_trace_batch(const BatchLaunch& b, cudaStream_t s);
+
 // Value, get_dim and is_active of a sparse volume at `count` index-space voxels (device arrays).
 cudaError_t launch_sparse_query(const SparseView& v, const int* ijk, int count, float* values, uint32_t* dims,
                                 uint8_t* active, cudaStream_t s);

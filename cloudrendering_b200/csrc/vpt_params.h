@@ -74,9 +74,27 @@ struct SparseView {
     const SparseTile* tiles;
 };
 
+// A light of the reference's light editor (struct Light, VptHeader.glsl:233-248; defaults of
+// LightEditorWidget.hpp:69-85), sampled by next event tracking only.
+enum LightType : int { kLightPoint = 0, kLightSpot = 1, kLightDirectional = 2 };
+enum LightSpace : int { kLightSpaceWorld = 0, kLightSpaceView = 1, kLightSpaceViewOrientation = 2 };
+constexpr int kMaxLights = 16;
+struct LightParams {
+    int type;                 // LightType
+    int space;                // LightSpace
+    float spot_total_width;   // radians
+    float spot_falloff_start; // radians
+    F3 color;
+    float intensity;
+    F3 position;              // point / spot position; direction (times distance) of a directional light
+    int use_distance;         // 1/d^2 falloff for point and spot lights
+    F3 spot_direction;
+};
+
 struct TraceParams {
     // camera: inverse(proj * view), column-major like glm (m[col*4 + row])
     float inv_view_proj[16];
+    float inv_view[16];        // inverse(view): view-space lights to world space
     float prev_view_proj[16];
     int width, height;
     uint32_t frame_count;      // FrameInfo::frameCount of the first frame in this launch
@@ -134,6 +152,9 @@ struct TraceParams {
     unsigned int* work_counter;    // persistent-kernel path queue
 
     SparseView sparse;             // valid when grid_kind == kNanoVdb
+
+    int num_lights;                // NUM_LIGHTS of the reference (0 when lights are off)
+    LightParams lights[kMaxLights];
 };
 
 // Offsets of the per-pixel feature accumulators (floats).

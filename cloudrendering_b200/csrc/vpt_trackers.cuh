@@ -151,6 +151,35 @@ VPT_DEV float shadow_transmittance(const TraceParams& P, S& sample, Rng& rng, F3
     return trans;
 }
 
+// Ratio-tracking transmittance toward a light at distance `max_dist`
+// (calculateTransmittanceDistance, NeeTransmittance.glsl:264-381, without isosurfaces): the walk
+// stops at the box exit or when the accumulated distance passes the light.
+template <class S>
+VPT_DEV float shadow_transmittance_distance(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, float max_dist,
+                                            PathCtx& pc) {
+    float trans = 1.0f;
+    float tmin, tmax;
+    float cur = 0.0f;
+    if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
+        x = x + w * tmin;
+        cur += tmin;
+        float d = tmax - tmin;
+        while (true) {
+            if (guard(pc)) return 0.0f;
+            float t = free_path(rng, P.inv_extinction);
+            cur += t;
+            if (t > d || cur > max_dist) break;
+            F3 xn = x + w * t;
+            float density = sample(xn, rng);
+            pc.lookups++;
+            x = xn;
+            trans *= 1.0f - density;
+            d -= t;
+        }
+    }
+    return trans;
+}
+
 // Ratio-tracking transmittance with empty-space skipping over the occupancy grid
 // (calculateTransmittance with USE_OCCUPANCY_GRID, NeeTransmittance.glsl:121-259).
 template <class S>
@@ -244,15 +273,41 @@ VPT_DEV F3 track_nee(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, Firs
                 if (P.max_bounces > 0 && ++bounces > P.max_bounces) return color;
                 F3 next_w = sample_phase(rng, P.g, w);
                 record_event(fe, x, density, P.extinction, tmax - d + t);
-                float pdf_light;
-                F3 dir_light = importance_sample_sky(P, rng, pdf_light);
+                // with lights: the light list or the sky with probability 1/2 each (all lights when the
+                // environment is black), NextEventTracking.glsl:335-364
+                bool to_light = false;
+                float prob_factor = 1.0f, light_dist = 0.0f, pdf_light = 0.0f;
+                int light_idx = 0;
+                F3 dir_light;
+                if (P.num_lights > 0) {
+                    to_light = P.env_is_black ? true : (rng_next(rng) > 0.5f);
+                    prob_factor = P.env_is_black ? 1.0f : 2.0f;
+                }
+                if (to_light) dir_light = light_direction(P, x, rng, light_idx, prob_factor, light_dist);
+                else dir_light = importance_sample_sky(P, rng, pdf_light);
                 float pdf_phase = evaluate_phase(P.g, w, dir_light);
                 w = next_w;
-                float tr = ESS ? shadow_transmittance_ess(P, sample, rng, x, dir_light, pc)
-                               : shadow_transmittance(P, sample, rng, x, dir_light, pc);
-                float f = (pdf_phase / pdf_light) * tr;
-                F3 l = sky_and_sun(P, dir_light);
-                color = color + f3(f * l.x, f * l.y, f * l.z);
+                if (P.num_lights > 0) {
+                    const float common = prob_factor * pdf_phase;
+                    if (to_light) {
+                        float tr = shadow_transmittance_distance(P, sample, rng, x, dir_light, light_dist, pc);
+                        float f = common * tr;
+                        F3 l = light_radiance(P, x, light_idx);
+                        color = color + f3(f * l.x, f * l.y, f * l.z);
+                    } else {
+                        float tr = ESS ? shadow_transmittance_ess(P, sample, rng, x, dir_light, pc)
+                                       : shadow_transmittance(P, sample, rng, x, dir_light, pc);
+                        float f = (common / pdf_light) * tr;
+                        F3 l = sky_and_sun(P, dir_light);
+                        color = color + f3(f * l.x, f * l.y, f * l.z);
+                    }
+                } else {
+                    float tr = ESS ? shadow_transmittance_ess(P, sample, rng, x, dir_light, pc)
+                                   : shadow_transmittance(P, sample, rng, x, dir_light, pc);
+                    float f = (pdf_phase / pdf_light) * tr;
+                    F3 l = sky_and_sun(P, dir_light);
+                    color = color + f3(f * l.x, f * l.y, f * l.z);
+                }
                 if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
                     x = x + w * tmin;
                     d = tmax - tmin;

@@ -216,6 +216,87 @@ def get_render_bounding_box() -> List[float]:
     return [out[0], out[3], out[1], out[4], out[2], out[5]]
 
 
+# ---- lights (Module.cpp:1088-1160, LightEditorWidget.cpp:89-103, 286-430) ----
+LIGHT_TYPE_NAMES = ["Point Light", "Spotlight", "Directional Light"]
+LIGHT_SPACE_NAMES = ["World", "View", "View Orientation"]
+
+
+def set_use_lights(_use_lights: bool) -> None:
+    _c("vpt_set_use_lights", 1 if _use_lights else 0)
+
+
+def clear_lights() -> None:
+    _c("vpt_clear_lights")
+
+
+def add_light() -> None:
+    _c("vpt_add_light", None)
+
+
+def remove_light(light_idx: int) -> None:
+    _c("vpt_remove_light", int(light_idx))
+
+
+def set_light_property(light_idx: int, key: str, value: str) -> None:
+    _c("vpt_set_light_property", int(light_idx), key.encode(), str(value).encode())
+
+
+def load_lights_from_file(file_path: str) -> None:
+    """The light editor's JSON format: {"lights": [{"type", "color": {r,g,b}, "intensity", "use_distance",
+    "position": {x,y,z}, "space", "spot_total_width", "spot_falloff_start", "spot_direction": {x,y,z}}]}."""
+    import json
+
+    with open(file_path) as f:
+        root = json.load(f)
+    clear_lights()
+    for i, node in enumerate(root.get("lights", [])):
+        add_light()
+        if "type" in node:
+            set_light_property(i, "type", node["type"])
+        if "color" in node:
+            c = node["color"]
+            set_light_property(i, "color", f"{c['r']!r} {c['g']!r} {c['b']!r}")
+        if "intensity" in node:
+            set_light_property(i, "intensity", repr(float(node["intensity"])))
+        if "use_distance" in node:
+            set_light_property(i, "use_distance", "1" if node["use_distance"] else "0")
+        if "position" in node:
+            p = node["position"]
+            set_light_property(i, "position", f"{p['x']!r} {p['y']!r} {p['z']!r}")
+        if "space" in node:
+            set_light_property(i, "space", node["space"])
+        for k in ("spot_total_width", "spot_falloff_start"):
+            if k in node:
+                set_light_property(i, k, repr(float(node[k])))
+        if "spot_direction" in node:
+            d = node["spot_direction"]
+            set_light_property(i, "spot_direction", f"{d['x']!r} {d['y']!r} {d['z']!r}")
+
+
+def set_use_headlight(_use_headlight: bool) -> None:
+    """One view-space point light at the camera (Module.cpp:1131-1141)."""
+    set_use_lights(_use_headlight)
+    if _use_headlight:
+        clear_lights()
+        add_light()
+        set_light_property(0, "space", "View")
+        set_light_property(0, "position", "0 0 0")
+        set_light_property(0, "use_distance", "1")
+
+
+def set_use_headlight_distance(_use_headlight_distance: bool) -> None:
+    set_light_property(0, "use_distance", "1" if _use_headlight_distance else "0")
+
+
+def set_headlight_color(_headlight_color: List[float]) -> None:
+    c = _vec3(_headlight_color, "set_headlight_color")
+    set_light_property(0, "color", f"{c[0]!r} {c[1]!r} {c[2]!r}")
+
+
+def set_headlight_intensity(_headlight_intensity: float) -> None:
+    set_light_property(0, "intensity", repr(float(_headlight_intensity)))
+
+
 # ---- sparse grids (VolumetricPathTracingPass::setUseSparseGrid; Module.cpp:1390-1400) ----
 def set_use_sparse_grid(use_sparse: bool) -> None:
     """Render through a NanoVDB-style sparse volume built from the dense grid (the C++ pass's

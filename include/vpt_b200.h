@@ -24,6 +24,7 @@ extern "C" {
 #define VPT_B200_ABI_VERSION 1
 
 typedef struct VptContext VptContext;
+typedef struct VptBatch VptBatch;
 
 typedef enum VptStatus {
     VPT_OK = 0,
@@ -216,6 +217,43 @@ VptStatus vpt_build_occupancy_grid(const float* density, int nx, int ny, int nz,
  * of an equirectangular RGBA image (OctahedralMapper.glsl:65-85 + mip reduction). */
 VptStatus vpt_build_environment_pyramid(const float* rgba, int width, int height, int levels, float* out_pyramid,
                                         void* stream);
+/* ---- batched rendering (no counterpart in the reference; the many-scene configuration) ----
+ * A batch renders several contexts in ONE persistent launch: each context keeps its own grid,
+ * camera, resolution, medium, seeds and film, and frames[i] 1-spp frames are traced for context i
+ * (0 skips it).  All contexts live on one device and share the tracker (delta, ratio or NEE without
+ * empty space skipping), the interpolation and the grid kind; feature maps and SVGF are not
+ * written.  The launch (parameter upload from pinned memory, counter reset, trace) is captured in a
+ * CUDA graph on first use and replayed afterwards ("use_graph", default 1).  Results are read per
+ * context with vpt_read_result / vpt_read_statistics. */
+VptStatus vpt_batch_create(VptBatch** out_batch, VptContext* const* contexts, int count);
+void vpt_batch_destroy(VptBatch* batch);
+const char* vpt_batch_last_error(VptBatch* batch);
+/* "use_graph" (0/1), "blocks_per_sm" (0 = occupancy calculator). */
+VptStatus vpt_batch_set_option(VptBatch* batch, const char* key, double value);
+VptStatus vpt_batch_render(VptBatch* batch, const int* frames, void* stream);
+/* Times the batch at 1, 3/4, 1/2 and 1/4 of the resident blocks per SM and keeps the fastest; the
+ * calibration frames are rendered into the contexts' films, whose accumulation is then reset. */
+VptStatus vpt_batch_autotune(VptBatch* batch, const int* frames, void* stream, int* out_blocks_per_sm);
+VptStatus vpt_batch_get_stats(VptBatch* batch, VptStats* stats);
+VptStatus vpt_batch_reset_stats(VptBatch* batch);
+
+/* ---- lights (NEE only; struct Light, Data/Shaders/VPT/VptHeader.glsl:233-248) ---- */
+
+/* vpt.set_use_lights (Module.cpp:1088-1092): NEE samples the lights (NUM_LIGHTS > 0) when set. */
+VptStatus vpt_set_use_lights(VptContext* ctx, int use_lights);
+/* vpt.clear_lights / add_light / remove_light (Module.cpp:1094-1113, LightEditorWidget.cpp:89-103).
+ * add_light appends a light with the defaults of LightEditorWidget.hpp:69-85 (point light in view
+ * space at the camera, intensity 0.5); at most 16 lights. */
+VptStatus vpt_clear_lights(VptContext* ctx);
+VptStatus vpt_add_light(VptContext* ctx, int* out_index);
+VptStatus vpt_remove_light(VptContext* ctx, int index);
+VptStatus vpt_get_light_count(VptContext* ctx, int* out_count);
+/* vpt.set_light_property (LightEditorWidget::setLightProperty, LightEditorWidget.cpp:286-320): keys
+ * "type" ("Point Light", "Spotlight", "Directional Light"), "space" ("World", "View",
+ * "View Orientation"), "color", "position" / "direction", "spot_direction" (three numbers separated by
+ * white space), "intensity", "spot_total_width", "spot_falloff_start", "use_distance" ("0"/"1"). */
+VptStatus vpt_set_light_property(VptContext* ctx, int index, const char* key, const char* value);
+
 /* ---- sparse (NanoVDB) volumes ---- */
 
 typedef struct VptSparseInfo {
@@ -257,6 +295,27 @@ VptStatus vpt_get_sparse_grid_info(VptContext* ctx, VptSparseInfo* out);
  * (Data/Shaders/VPT/PNanoVDB.glsl:1800-1990). */
 VptStatus vpt_sparse_query(VptContext* ctx, const int32_t* ijk, int count, float* values, uint32_t* dims,
                            uint8_t* active, void* stream);
+
+/* ---- kernel-predicting denoiser (modules/kpn_module/src/Kernel.cu; PyTorchDenoiser.cpp:174-179,
+ * 411-440).  Device arrays, NCHW float, at most 4 channels, odd kernel size up to 7. ---- */
+
+/* perPixelKernelCuda (Kernel.cu:38-135): out[n,c,y,x] = sum over the k*k taps of
+ * w[n,t,y,x] * image[n,c,y+dy,x+dx], taps outside the output size skipped; output size
+ * min(image, weights).  softmax = 1 applies torch::softmax over the taps first (fused). */
+VptStatus vpt_kpn_apply(const float* image, const float* weights, int n, int c, int h, int w, int weights_h,
+                        int weights_w, int kernel_size, int softmax, float* out, void* stream);
+/* inv_iter_kernel (PyTorchDenoiser.cpp:174-179 with getInvIterBaseKernel, Kernel.cu:138-186): the
+ * sigmoid-gated blend of the low-resolution prediction, the high-frequency detail and (use_prev)
+ * the reprojected previous frame, followed by the softmaxed per-pixel kernel of fused_weights'
+ * first k*k channels.  fused_weights has k*k + 3 channels; x_lo / pred_lo are low_h x low_w. */
+VptStatus vpt_kpn_inv_iter(const float* x_hi, const float* pred_lo, const float* x_lo, const float* prev,
+                           const float* fused_weights, int n, int c, int h, int w, int low_h, int low_w, int weights_h,
+                           int weights_w, int kernel_size, int use_prev, float* out, void* stream);
+/* torch::avg_pool2d(x, 2, 2). */
+VptStatus vpt_kpn_avg_pool2(const float* in, int n, int c, int h, int w, float* out, void* stream);
+/* torch::grid_sampler_2d(prev, uv * 2 - 1, bilinear, zeros, align_corners = false), uv N x 2 x h x w. */
+VptStatus vpt_kpn_reproject(const float* prev, const float* uv, int n, int c, int prev_h, int prev_w, int h, int w,
+                            float* out, void* stream);
 
 /* EAW a-trous chain (EAWBlitPass::_renderCompute, src/Denoiser/EAWDenoiser.cpp:345-391; weights of
  * EAWDenoise.glsl) on RGBA images; position/normal may be NULL.  Allocates its ping-pong images

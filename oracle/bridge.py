@@ -36,6 +36,7 @@ class OracleScene(ctypes.Structure):
         ("env_rgba", c_void_p), ("env_pyramid", c_void_p),
         ("nanovdb", c_void_p), ("grid_min", c_float * 3), ("grid_max", c_float * 3),
         ("sparse_lowest_level", c_int), ("sparse_fp16", c_int),
+        ("inv_view", c_float * 16), ("num_lights", c_int), ("env_is_black", c_int), ("lights", c_float * 256),
     ]
 
 
@@ -70,6 +71,12 @@ def load():
         lib.oracle_nanovdb_hdda_walk.restype = c_int
         lib.oracle_nanovdb_hdda_walk.argtypes = [c_void_p, c_void_p, c_void_p, c_int, c_int, c_void_p, c_void_p,
                                                  c_void_p, c_void_p, c_void_p, c_void_p]
+        lib.oracle_softmax_channels.argtypes = [c_void_p, c_int, c_int, c_int, c_int, c_void_p]
+        lib.oracle_kpn_apply.argtypes = [c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_int, c_int, c_int, c_void_p]
+        lib.oracle_kpn_inv_iter_base.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int, c_int,
+                                                 c_int, c_int, c_int, c_int, c_int, c_int, c_int, c_void_p]
+        lib.oracle_avg_pool2.argtypes = [c_void_p, c_int, c_int, c_int, c_void_p]
+        lib.oracle_grid_sample.argtypes = [c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_int, c_int, c_void_p]
         lib.oracle_set_double_rounded_math.argtypes = [c_int]
         lib.oracle_set_double_rounded_math.restype = None
         _lib = lib
@@ -239,3 +246,59 @@ def nanovdb_hdda_walk(buf: np.ndarray, origin, direction, lowest_level: int = 8,
     if n < 0:
         return None
     return dict(voxel=vox[:n], dim=dim[:n], active=act[:n], level=lvl[:n], box=box[:n], t=t[:n])
+
+
+# ---- kernel-predicting denoiser (modules/kpn_module/src/Kernel.cu + the libtorch ops around it) ----
+
+def _f(a):
+    return np.ascontiguousarray(a, np.float32)
+
+
+def softmax_channels(x):
+    x = _f(x)
+    out = np.empty_like(x)
+    n, k, h, w = x.shape
+    load().oracle_softmax_channels(_p(x), n, k, h, w, _p(out))
+    return out
+
+
+def kpn_apply(image, weights, k, softmax=False):
+    image, weights = _f(image), _f(weights)
+    if softmax:
+        weights = softmax_channels(weights)
+    n, c, h, w = image.shape
+    wh, ww = weights.shape[2:]
+    out = np.zeros((n, c, min(h, wh), min(w, ww)), np.float32)
+    load().oracle_kpn_apply(_p(image), _p(weights), n, c, h, w, wh, ww, k, _p(out))
+    return out
+
+
+def kpn_inv_iter(x_hi, pred_lo, x_lo, prev, fused, k, use_prev):
+    """inv_iter_kernel (PyTorchDenoiser.cpp:174-179): base image, softmax of the first k*k fused
+    channels, per-pixel kernel."""
+    x_hi, pred_lo, x_lo, fused = _f(x_hi), _f(pred_lo), _f(x_lo), _f(fused)
+    prev = _f(prev) if prev is not None else np.zeros_like(x_hi)
+    n, c, h, w = x_hi.shape
+    lh, lw = x_lo.shape[2:]
+    wh, ww = fused.shape[2:]
+    base = np.zeros((n, c, min(h, wh), min(w, ww)), np.float32)
+    load().oracle_kpn_inv_iter_base(_p(x_hi), _p(pred_lo), _p(x_lo), _p(prev), _p(fused), n, c, h, w, lh, lw, wh, ww,
+                                    k, 1 if use_prev else 0, _p(base))
+    return kpn_apply(base, np.ascontiguousarray(fused[:, :k * k]), k, softmax=True)
+
+
+def avg_pool2(x):
+    x = _f(x)
+    n, c, h, w = x.shape
+    out = np.empty((n, c, h // 2, w // 2), np.float32)
+    load().oracle_avg_pool2(_p(x), n * c, h, w, _p(out))
+    return out
+
+
+def grid_sample(prev, uv):
+    prev, uv = _f(prev), _f(uv)
+    n, c, ph, pw = prev.shape
+    h, w = uv.shape[2:]
+    out = np.empty((n, c, h, w), np.float32)
+    load().oracle_grid_sample(_p(prev), _p(uv), n, c, ph, pw, h, w, _p(out))
+    return out

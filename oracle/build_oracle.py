@@ -28,11 +28,10 @@ def build(force: bool = False, verbose: bool = False) -> str:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"oracle build failed:\n{r.stdout}\n{r.stderr}")
-    try:
-        from oracle import ref_build  # noqa: F401  (optional: needs the reference tree)
-        ref_build.build(force=force, verbose=verbose)
-    except ImportError:
-        pass
+    # the reference's own code for the CPU (optional: needs the reference tree; a no-op without it)
+    sys.path.insert(0, os.path.dirname(HERE))
+    from oracle import ref_build
+    ref_build.build(force=force, verbose=verbose)
     return LIB
 
 

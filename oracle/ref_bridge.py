@@ -25,6 +25,7 @@ class RefScene(ctypes.Structure):
         ("occupancy", c_void_p), ("ox", c_int), ("oy", c_int), ("oz", c_int), ("occ_block", c_int),
         ("env_rgba", c_void_p), ("env_w", c_int), ("env_h", c_int),
         ("env_pyramid", c_void_p), ("env_levels", c_int), ("is_env_black", c_int), ("far_dist", c_float),
+        ("inv_view", c_float * 16), ("lights", c_float * 256),
     ]
 
 

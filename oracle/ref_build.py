@@ -51,12 +51,20 @@ ENVS = {
 }
 
 
+# NEE with lights (NUM_LIGHTS > 0): stochastic lookups, default and black environments
+LIGHT_VARIANTS = {"nee_l1": 1, "nee_l2": 2}
+
+
 def variants():
+    """(name, defines, NUM_LIGHTS)"""
     out = []
     for t, tdefs in TRACKERS.items():
         for i, idef in INTERPS.items():
             for e, edefs in ENVS.items():
-                out.append((f"{t}__{i}__{e}", tdefs + [idef] + edefs))
+                out.append((f"{t}__{i}__{e}", tdefs + [idef] + edefs, 0))
+    for t, n in LIGHT_VARIANTS.items():
+        for e in ("default__linear", "black__linear"):
+            out.append((f"{t}__stochastic__{e}", TRACKERS["nee"] + [INTERPS["stochastic"]] + ENVS[e], n))
     return out
 
 
@@ -130,19 +138,19 @@ def build_tracer(force=False, verbose=False) -> str:
     objs, jobs = [], []
     vs = variants()
     flags = ["g++", "-O2", "-std=c++20", "-fPIC", "-fopenmp", "-ffp-contract=off", "-w", "-I", GEN, "-I", HERE]
-    for idx, (name, defs) in enumerate(vs):
+    for idx, (name, defs, nlights) in enumerate(vs):
         obj = os.path.join(GEN, f"v_{name}.o")
         objs.append(obj)
-        dflags = [f"-D{d}" for d in defs] + [f"-DREF_VARIANT_NS=v_{name}", "-DNUM_LIGHTS=0",
+        dflags = [f"-D{d}" for d in defs] + [f"-DREF_VARIANT_NS=v_{name}", f"-DNUM_LIGHTS={nlights}",
                                              "-DCUSTOM_SEED_OFFSET=ref_seed_offset", "-DREF_VARIANT_BODY"]
         jobs.append(flags + dflags + ["-c", driver, "-o", obj])
     reg = os.path.join(GEN, "registry.cpp")
     with open(reg, "w") as fh:
         fh.write('#include "ref_shim.h"\n#include "ref_driver_api.h"\n')
-        for name, _ in vs:
+        for name, _, _ in vs:
             fh.write(f"namespace glslref {{ namespace v_{name} {{ void run_pixel(int x, int y); }} }}\n")
         fh.write("const RefVariant ref_variants[] = {\n")
-        for name, _ in vs:
+        for name, _, _ in vs:
             fh.write(f'    {{"{name}", &glslref::v_{name}::run_pixel}},\n')
         fh.write("};\nconst int ref_num_variants = %d;\n" % len(vs))
     jobs.append(flags + ["-c", reg, "-o", os.path.join(GEN, "registry.o")])

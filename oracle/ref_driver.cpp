@@ -24,6 +24,7 @@ static sampler2D& environmentMapOctahedralTexture = g_ref.envocta;
 static uimage3D& occupancyGridImage = g_ref.occ;
 static image2D& resultImage = g_ref.result;
 static image2D& accImage = g_ref.acc;
+static Light* const lights = g_ref.lights;
 #define gl_GlobalInvocationID gl_global_invocation_id
 #define main glsl_main
 #include "Clouds.glsl.inc"
@@ -68,6 +69,8 @@ typedef struct RefScene {
     int env_levels;
     int is_env_black;
     float far_dist;
+    float inv_view[16];       /* parameters.inverseViewMatrix, column-major */
+    float lights[16 * 16];    /* 16 floats per light (see oracle/vpt_oracle.h) */
 } RefScene;
 
 int ref_variant_count(void) { return ref_num_variants; }
@@ -111,6 +114,23 @@ int ref_render(int variant, const RefScene* s, float* out_rgba, int threads) {
     p.isEnvMapBlack = (uint)s->is_env_black;
     p.voxelTexelSize = vec3(1.0f / float(s->nx - 1), 1.0f / float(s->ny - 1), 1.0f / float(s->nz - 1));
     p.farDistance = s->far_dist;
+    for (int c = 0; c < 4; c++)
+        p.inverseViewMatrix.c[c] = vec4(s->inv_view[c * 4 + 0], s->inv_view[c * 4 + 1], s->inv_view[c * 4 + 2],
+                                        s->inv_view[c * 4 + 3]);
+    for (int i = 0; i < 16; i++) {
+        const float* L = s->lights + 16 * i;
+        Light& l = g_ref.lights[i];
+        l.lightType = (uint)L[0];
+        l.lightSpace = (uint)L[1];
+        l.spotTotalWidth = L[2];
+        l.spotFalloffStart = L[3];
+        l.color = vec3(L[4], L[5], L[6]);
+        l.intensity = L[7];
+        l.position = vec3(L[8], L[9], L[10]);
+        l.useDistance = (uint)L[11];
+        l.spotDirection = vec3(L[12], L[13], L[14]);
+        l.padding = 0.0f;
+    }
 
     g_ref.grid.data = s->grid;
     g_ref.grid.w = s->nx;

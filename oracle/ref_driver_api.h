@@ -13,6 +13,7 @@ struct RefState {
     sampler2D envocta;    // environmentMapOctahedralTexture (mip chain)
     uimage3D occ;         // occupancyGridImage
     image2D result, acc;  // resultImage, accImage
+    Light lights[16];     // LightsBuffer
 };
 extern RefState g_ref;
 extern thread_local uvec3 gl_global_invocation_id;

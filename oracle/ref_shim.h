@@ -421,5 +421,24 @@ struct Parameters {
 struct FrameInfo {
     uint frameCount, globalFrameNumber;
 };
+// the LightsBuffer UBO (VptHeader.glsl:226-251)
+const uint LIGHT_TYPE_POINT = 0u;
+const uint LIGHT_TYPE_SPOT = 1u;
+const uint LIGHT_TYPE_DIRECTIONAL = 2u;
+const uint LIGHT_SPACE_WORLD = 0u;
+const uint LIGHT_SPACE_VIEW = 1u;
+const uint LIGHT_SPACE_VIEW_ORIENTATION = 2u;
+struct Light {
+    uint lightType;
+    uint lightSpace;
+    float spotTotalWidth;
+    float spotFalloffStart;
+    vec3 color;
+    float intensity;
+    vec3 position;
+    uint useDistance;
+    vec3 spotDirection;
+    float padding;
+};
 
 }  // namespace glslref

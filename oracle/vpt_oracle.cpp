@@ -722,6 +722,78 @@ struct Tracer {
     }
 
     // nextEventTracking (NextEventTracking.glsl:224-393)
+    // ---- lights (VptUtils.glsl:394-453) ----
+    const float* light(int i) const { return S.lights + 16 * i; }
+    V3 inv_view_xyz(V3 v, float wv) const {
+        const float* m = S.inv_view;
+        return v3(((m[0] * v.x + m[4] * v.y) + m[8] * v.z) + m[12] * wv,
+                  ((m[1] * v.x + m[5] * v.y) + m[9] * v.z) + m[13] * wv,
+                  ((m[2] * v.x + m[6] * v.y) + m[10] * v.z) + m[14] * wv);
+    }
+    V3 light_pos(int i) const {
+        const float* L = light(i);
+        int type = (int)L[0], space = (int)L[1];
+        V3 p = v3(L[8], L[9], L[10]);
+        if (space == 1 || space == 2) p = inv_view_xyz(p, (type == 2 || space == 2) ? 0.0f : 1.0f);
+        return p;
+    }
+    // getHeadlightDirection
+    V3 light_dir(V3 pos, Rng& r, int& idx, float& factor, float& dist) const {
+        if (S.num_lights > 1) {
+            uint32_t k = (uint32_t)(rnd(r) * (float)S.num_lights);
+            idx = (int)std::min(k, (uint32_t)S.num_lights - 1u);
+            factor *= (float)S.num_lights;
+        }
+        int type = (int)light(idx)[0];
+        V3 lp = light_pos(idx);
+        V3 dir = (type == 0 || type == 1) ? sub(lp, pos) : lp;
+        dist = length(dir);
+        float s = dist + 1e-5f;
+        return v3(dir.x / s, dir.y / s, dir.z / s);
+    }
+    // sampleHeadlight
+    V3 light_rad(V3 pos, int idx) const {
+        const float* L = light(idx);
+        int type = (int)L[0], space = (int)L[1];
+        V3 lp = light_pos(idx);
+        float f = L[7];
+        if ((type == 0 || type == 1) && L[11] != 0.0f) {
+            V3 diff = sub(lp, pos);
+            f /= std::max(dot(diff, diff), 1e-3f);
+        }
+        if (type == 1) {
+            float total = m_cos(L[2]);
+            float falloff = L[2] > L[3] ? m_cos(L[3]) : total;
+            V3 p = sub(pos, lp);
+            V3 z = normalize(v3(L[12], L[13], L[14]));
+            if (space == 1 || space == 2) z = inv_view_xyz(z, 0.0f);
+            float ct = dot(z, p) / (length(z) * length(p));
+            f *= smoothstepf(total, falloff, ct);
+        }
+        return v3(f * L[4], f * L[5], f * L[6]);
+    }
+    // calculateTransmittanceDistance (NeeTransmittance.glsl:264-381), ratio tracking
+    float transmittance_distance(V3 x, V3 w, float max_dist, Rng& r) {
+        float trans = 1.0f, tmin, tmax, cur = 0.0f;
+        if (ray_box(bmin(), bmax(), x, w, tmin, tmax)) {
+            x = add(x, mul(w, tmin));
+            cur += tmin;
+            float d = tmax - tmin;
+            while (true) {
+                if (guard()) return 0.0f;
+                float t = free_path(r);
+                cur += t;
+                if (t > d || cur > max_dist) break;
+                V3 xn = add(x, mul(w, t));
+                float dens = sample(xn, r);
+                x = xn;
+                trans *= 1.0f - dens;
+                d -= t;
+            }
+        }
+        return trans;
+    }
+
     V3 nee(V3 x, V3 w, Rng& r, bool& ev) {
         V3 color = v3(0, 0, 0);
         float tmin, tmax;
@@ -746,14 +818,37 @@ struct Tracer {
                     if (S.max_bounces > 0 && ++bounces > S.max_bounces) return color;
                     V3 nw = sample_phase(r, S.g, w);
                     ev = true;
-                    float pdf_l;
-                    V3 dl = importance_sky(r, pdf_l);
+                    // NextEventTracking.glsl:335-369: lights or sky, 1/2 each (lights only when the
+                    // environment is black)
+                    bool to_light = false;
+                    float factor = 1.0f, ldist = 0.0f, pdf_l = 0.0f;
+                    int lidx = 0;
+                    if (S.num_lights > 0) {
+                        to_light = S.env_is_black ? true : (rnd(r) > 0.5f);
+                        factor = S.env_is_black ? 1.0f : 2.0f;
+                    }
+                    V3 dl = to_light ? light_dir(x, r, lidx, factor, ldist) : importance_sky(r, pdf_l);
                     float pdf_p = eval_phase(S.g, w, dl);
                     w = nw;
-                    float tr = S.use_ess ? transmittance_ess(x, dl, r) : transmittance(x, dl, r);
-                    float f = (pdf_p / pdf_l) * tr;
-                    V3 l = sky(dl);
-                    color = add(color, v3(f * l.x, f * l.y, f * l.z));
+                    if (S.num_lights > 0) {
+                        float common = factor * pdf_p;
+                        if (to_light) {
+                            float tr = transmittance_distance(x, dl, ldist, r);
+                            float f = common * tr;
+                            V3 l = light_rad(x, lidx);
+                            color = add(color, v3(f * l.x, f * l.y, f * l.z));
+                        } else {
+                            float tr = S.use_ess ? transmittance_ess(x, dl, r) : transmittance(x, dl, r);
+                            float f = (common / pdf_l) * tr;
+                            V3 l = sky(dl);
+                            color = add(color, v3(f * l.x, f * l.y, f * l.z));
+                        }
+                    } else {
+                        float tr = S.use_ess ? transmittance_ess(x, dl, r) : transmittance(x, dl, r);
+                        float f = (pdf_p / pdf_l) * tr;
+                        V3 l = sky(dl);
+                        color = add(color, v3(f * l.x, f * l.y, f * l.z));
+                    }
                     if (ray_box(bmin(), bmax(), x, w, tmin, tmax)) {
                         x = add(x, mul(w, tmin));
                         d = tmax - tmin;
@@ -1393,6 +1488,120 @@ void oracle_eaw(const float* color, const float* pos, const float* nrm, int w, i
 }
 
 void oracle_set_double_rounded_math(int on) { g_dr_math = on != 0; }
+
+// ---- kernel-predicting denoiser (modules/kpn_module/src/Kernel.cu) ----
+
+// torch::softmax(x, 1): exp(x - max) / sum over the channel dimension, per pixel
+void oracle_softmax_channels(const float* in, int n, int k, int h, int w, float* out) {
+    const size_t plane = (size_t)h * w;
+    for (int b = 0; b < n; b++)
+        for (size_t i = 0; i < plane; i++) {
+            const float* x = in + (size_t)b * k * plane + i;
+            float* y = out + (size_t)b * k * plane + i;
+            float m = -INFINITY;
+            for (int t = 0; t < k; t++) m = std::max(m, x[(size_t)t * plane]);
+            float s = 0.0f;
+            for (int t = 0; t < k; t++) {
+                y[(size_t)t * plane] = expf(x[(size_t)t * plane] - m);
+                s += y[(size_t)t * plane];
+            }
+            for (int t = 0; t < k; t++) y[(size_t)t * plane] = y[(size_t)t * plane] / s;
+        }
+}
+
+// perPixelKernelForwardKernel (Kernel.cu:38-81): output size min(image, weights), taps outside it skipped
+void oracle_kpn_apply(const float* image, const float* weights, int n, int c, int h, int w, int wh, int ww, int k,
+                      float* out) {
+    const int ho = std::min(h, wh), wo = std::min(w, ww);
+    const int K = k * k;
+    for (int b = 0; b < n; b++)
+        for (int y = 0; y < ho; y++)
+            for (int x = 0; x < wo; x++) {
+                float acc[4] = {0, 0, 0, 0};
+                int t = 0;
+                for (int dy = -k / 2; dy <= k / 2; dy++) {
+                    int ky = y + dy;
+                    for (int dx = -k / 2; dx <= k / 2; dx++, t++) {
+                        int kx = x + dx;
+                        if (kx >= 0 && kx < wo && ky >= 0 && ky < ho) {
+                            float wt = weights[(size_t)b * ww * wh * K + (size_t)t * ww * wh + (size_t)y * ww + x];
+                            for (int ch = 0; ch < c; ch++)
+                                acc[ch] += wt * image[(size_t)b * w * h * c + (size_t)ch * w * h + (size_t)ky * w + kx];
+                        }
+                    }
+                }
+                for (int ch = 0; ch < c; ch++) out[(size_t)b * wo * ho * c + (size_t)ch * wo * ho + (size_t)y * wo + x] = acc[ch];
+            }
+}
+
+// getInvIterBaseKernel (Kernel.cu:138-186); pixels whose low-resolution texel is out of range stay 0
+void oracle_kpn_inv_iter_base(const float* x_hi, const float* pred_lo, const float* x_lo, const float* prev,
+                              const float* fused, int n, int c, int h, int w, int lh, int lw, int wh, int ww, int k,
+                              int use_prev, float* out) {
+    const int ho = std::min(h, wh), wo = std::min(w, ww);
+    const int K = k * k;
+    const size_t plane = (size_t)wh * ww;
+    for (size_t i = 0; i < (size_t)n * c * ho * wo; i++) out[i] = 0.0f;
+    for (int b = 0; b < n; b++)
+        for (int y = 0; y < ho; y++)
+            for (int x = 0; x < wo; x++) {
+                int lx = x / 2, ly = y / 2;
+                if (lx >= lw || ly >= lh) continue;
+                for (int ch = 0; ch < c; ch++) {
+                    const float* wb = fused + (size_t)b * (K + 3) * plane + (size_t)y * ww + x;
+                    float lf_w = 1.0f / (1.0f + expf(-wb[(size_t)K * plane]));
+                    float hf_w = 1.0f / (1.0f + expf(-wb[(size_t)(K + 1) * plane]));
+                    float pv_w = 1.0f / (1.0f + expf(-wb[(size_t)(K + 2) * plane]));
+                    float xh = x_hi[((size_t)b * c + ch) * h * w + (size_t)y * w + x];
+                    float xl = x_lo[((size_t)b * c + ch) * lh * lw + (size_t)ly * lw + lx];
+                    float pl = pred_lo[((size_t)b * c + ch) * lh * lw + (size_t)ly * lw + lx];
+                    float lf = lf_w * pl + (1.0f - lf_w) * xl;
+                    if (use_prev) {
+                        float pr = prev[((size_t)b * c + ch) * h * w + (size_t)y * w + x];
+                        lf = lf * (1.0 - pv_w) + pr * pv_w;  // double literal, as in the reference
+                    }
+                    out[((size_t)b * c + ch) * ho * wo + (size_t)y * wo + x] = hf_w * (xh - xl + lf) + (1.0f - hf_w) * lf;
+                }
+            }
+}
+
+// torch::avg_pool2d(x, 2, 2)
+void oracle_avg_pool2(const float* in, int nc, int h, int w, float* out) {
+    const int ho = h / 2, wo = w / 2;
+    for (int i = 0; i < nc; i++)
+        for (int y = 0; y < ho; y++)
+            for (int x = 0; x < wo; x++) {
+                const float* b = in + ((size_t)i * h + 2 * y) * w + 2 * x;
+                out[((size_t)i * ho + y) * wo + x] = (((b[0] + b[1]) + b[w]) + b[w + 1]) / 4.0f;
+            }
+}
+
+// torch::grid_sampler_2d(prev, uv * 2 - 1, bilinear, zeros, align_corners = false)
+void oracle_grid_sample(const float* prev, const float* uv, int n, int c, int ph, int pw, int h, int w, float* out) {
+    const size_t plane = (size_t)h * w;
+    for (int b = 0; b < n; b++)
+        for (int y = 0; y < h; y++)
+            for (int x = 0; x < w; x++) {
+                float gx = uv[((size_t)b * 2 + 0) * plane + (size_t)y * w + x] * 2.0f - 1.0f;
+                float gy = uv[((size_t)b * 2 + 1) * plane + (size_t)y * w + x] * 2.0f - 1.0f;
+                float ix = ((gx + 1.0f) * (float)pw - 1.0f) / 2.0f;
+                float iy = ((gy + 1.0f) * (float)ph - 1.0f) / 2.0f;
+                float x0 = floorf(ix), y0 = floorf(iy), x1 = x0 + 1.0f, y1 = y0 + 1.0f;
+                float nw = (x1 - ix) * (y1 - iy), ne = (ix - x0) * (y1 - iy);
+                float sw = (x1 - ix) * (iy - y0), se = (ix - x0) * (iy - y0);
+                int xi0 = (int)x0, yi0 = (int)y0, xi1 = xi0 + 1, yi1 = yi0 + 1;
+                auto in = [&](int xx, int yy) { return xx >= 0 && xx < pw && yy >= 0 && yy < ph; };
+                for (int ch = 0; ch < c; ch++) {
+                    const float* src = prev + ((size_t)b * c + ch) * ph * pw;
+                    float v = 0.0f;
+                    if (in(xi0, yi0)) v += src[(size_t)yi0 * pw + xi0] * nw;
+                    if (in(xi1, yi0)) v += src[(size_t)yi0 * pw + xi1] * ne;
+                    if (in(xi0, yi1)) v += src[(size_t)yi1 * pw + xi0] * sw;
+                    if (in(xi1, yi1)) v += src[(size_t)yi1 * pw + xi1] * se;
+                    out[((size_t)b * c + ch) * plane + (size_t)y * w + x] = v;
+                }
+            }
+}
 
 void oracle_nanovdb_query(const uint8_t* buf, int n, const int32_t* ijk, float* value, uint32_t* dim,
                           uint8_t* active) {

@@ -49,6 +49,12 @@ typedef struct OracleScene {
     float grid_min[3], grid_max[3];  /* world box of the grid: sampleCloud maps box -> grid box */
     int sparse_lowest_level;         /* HDDA cell of sparse decomposition tracking: 8 or 1 */
     int sparse_fp16;                 /* leaf values rounded to IEEE half (fp16 variant) */
+    /* lights (NEE only): 16 floats per light: type, space, spot total width, spot falloff start,
+     * color rgb, intensity, position xyz, use_distance, spot direction xyz, unused */
+    float inv_view[16];              /* inverse view matrix, column-major (view-space lights) */
+    int num_lights;
+    int env_is_black;                /* parameters.isEnvMapBlack */
+    float lights[16 * 16];
 } OracleScene;
 
 /* Renders width*height*num_frames paths; adds radiance (and its square) per pixel (3 doubles). */
@@ -84,6 +90,19 @@ void oracle_nanovdb_query(const uint8_t* buf, int n, const int32_t* ijk, float* 
 int oracle_nanovdb_hdda_walk(const uint8_t* buf, const float world_origin[3], const float world_dir[3],
                              int lowest_level, int max_visits, int32_t* out_voxel, int32_t* out_dim,
                              uint8_t* out_active, int32_t* out_level, float* out_box, float* out_t);
+
+/* Kernel-predicting denoiser, restated from modules/kpn_module/src/Kernel.cu and the libtorch ops it
+ * is composed with (softmax over channels, avg_pool2d(2, 2), grid_sampler_2d bilinear/zeros/
+ * align_corners=false).  NCHW float arrays. */
+void oracle_softmax_channels(const float* in, int n, int k, int h, int w, float* out);
+void oracle_kpn_apply(const float* image, const float* weights, int n, int c, int h, int w, int wh, int ww, int k,
+                      float* out);
+/* getInvIterBaseKernel; fused has k*k + 3 channels (batch stride (k*k + 3) * wh * ww) */
+void oracle_kpn_inv_iter_base(const float* x_hi, const float* pred_lo, const float* x_lo, const float* prev,
+                              const float* fused, int n, int c, int h, int w, int lh, int lw, int wh, int ww, int k,
+                              int use_prev, float* out);
+void oracle_avg_pool2(const float* in, int nc, int h, int w, float* out);
+void oracle_grid_sample(const float* prev, const float* uv, int n, int c, int ph, int pw, int h, int w, float* out);
 
 /* Hybrid Tausworthe stream: n floats after seeding with `seed`. */
 void oracle_rng_stream(uint32_t seed, int n, float* out, uint32_t* out_state4);

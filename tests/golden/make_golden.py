@@ -48,7 +48,17 @@ def cases():
                      "decomposition": dict(mode="decomposition"), "rrt": dict(mode="rrt"),
                      "nee_env_image": dict(mode="nee", env="image", env_rgba=env_image()),
                      "delta_black": dict(mode="delta", env="black"),
-                     "delta_single_color": dict(mode="delta", env="single")}.items():
+                     "delta_single_color": dict(mode="delta", env="single"),
+                     # lights of the light editor (NEE only): a spot light in view space beside the
+                     # camera plus a world-space point light; a directional light alone under a black sky
+                     "nee_lights2": dict(mode="nee", lights=[
+                         dict(type="Spotlight", space="View", position=(0.05, 0.1, 0.0), spot_direction=(0.0, -0.1, -1.0),
+                              spot_total_width=0.6, spot_falloff_start=0.3, intensity=3.0),
+                         dict(type="Point Light", space="World", position=(0.6, 0.8, 0.3), intensity=0.8,
+                              color=(1.0, 0.8, 0.6))]),
+                     "nee_light_directional_black": dict(mode="nee", env="black", lights=[
+                         dict(type="Directional Light", space="World", position=(0.4, 0.9, 0.2), intensity=2.0,
+                              use_distance=0)])}.items():
         kw2 = dict(base)
         kw2.update(kw)
         out["fbm_" + name] = SceneSpec(grid=fbm, **kw2)
@@ -57,7 +67,7 @@ def cases():
 
 FIELDS = ["mode", "interp", "extinction", "albedo", "g", "width", "height", "seed_offset", "env", "linear_rgb",
           "sun_dir", "sun_intensity", "cam_pos", "cam_target", "fovy", "near", "far", "max_grid_extent", "use_ess",
-          "env_intensity", "max_bounces", "ess_ref_compat"]
+          "env_intensity", "max_bounces", "ess_ref_compat", "lights"]
 
 
 def main():

@@ -66,9 +66,43 @@ class SceneSpec:
                  sun_dir=(0.5826, 0.7660, 0.2717), sun_intensity=(2.6, 2.6 * 0.961538462, 2.6 * 0.884615385),
                  sky_color=(1.0, 1.0, 1.0), cam_pos=(0.0, 0.0, 0.8), cam_target=(0.0, 0.0, 0.0),
                  fovy=2.0 * math.atan(0.5), near=0.01, far=100.0, max_grid_extent=0.25, env_rgba=None,
-                 use_ess=False, env_intensity=(1.0, 1.0, 1.0), ess_ref_compat=False):
+                 use_ess=False, env_intensity=(1.0, 1.0, 1.0), ess_ref_compat=False, lights=None):
         self.__dict__.update(locals())
         del self.__dict__["self"]
+
+
+LIGHT_TYPES = ["Point Light", "Spotlight", "Directional Light"]
+LIGHT_SPACES = ["World", "View", "View Orientation"]
+LIGHT_DEFAULTS = dict(type="Point Light", space="View", spot_total_width=0.0981747704, spot_falloff_start=0.0245436926,
+                      color=(1.0, 0.961538462, 0.884615385), intensity=0.5, position=(0.0, 0.0, 0.0), use_distance=1,
+                      spot_direction=(0.0, 0.0, -1.0))
+
+
+def _f32s(v):
+    return repr(float(np.float32(v)))
+
+
+def light_properties(light: dict):
+    """(key, value) strings of vpt_set_light_property for a light dict (defaults of LightEditorWidget)."""
+    L = dict(LIGHT_DEFAULTS)
+    L.update(light)
+    vec = lambda v: " ".join(_f32s(x) for x in v)  # noqa: E731
+    return [("type", L["type"]), ("space", L["space"]), ("color", vec(L["color"])), ("intensity", _f32s(L["intensity"])),
+            ("position", vec(L["position"])), ("use_distance", "1" if L["use_distance"] else "0"),
+            ("spot_direction", vec(L["spot_direction"])), ("spot_total_width", _f32s(L["spot_total_width"])),
+            ("spot_falloff_start", _f32s(L["spot_falloff_start"]))]
+
+
+def light_floats(lights):
+    """16 floats per light for the oracle and the reference driver."""
+    out = np.zeros(256, np.float32)
+    for i, light in enumerate(lights or []):
+        L = dict(LIGHT_DEFAULTS)
+        L.update(light)
+        out[16 * i:16 * i + 15] = [LIGHT_TYPES.index(L["type"]), LIGHT_SPACES.index(L["space"]), L["spot_total_width"],
+                                   L["spot_falloff_start"], *L["color"], L["intensity"], *L["position"],
+                                   1.0 if L["use_distance"] else 0.0, *L["spot_direction"]]
+    return [float(v) for v in out]
 
 
 def setup_core(core: Core, sp: SceneSpec):
@@ -95,6 +129,12 @@ def setup_core(core: Core, sp: SceneSpec):
         core("vpt_set_builtin_environment_map", ENV[sp.env])
     core("vpt_set_use_empty_space_skipping", 1 if sp.use_ess else 0)
     core("vpt_set_camera", farr(sp.cam_pos), farr(sp.cam_target), farr([0, 1, 0]), sp.fovy, sp.near, sp.far)
+    core("vpt_clear_lights")
+    core("vpt_set_use_lights", 1 if sp.lights else 0)
+    for i, light in enumerate(sp.lights or []):
+        core("vpt_add_light", None)
+        for k, v in light_properties(light):
+            core("vpt_set_light_property", i, k.encode(), v.encode())
     core("vpt_set_resolution", sp.width, sp.height)
     core("vpt_set_denoiser", 0)
 
@@ -148,11 +188,7 @@ def _mat_inverse(m):
     return [a[r][4 + c] for c in range(4) for r in range(4)]
 
 
-def camera_inv_view_proj(sp: SceneSpec):
-    """The core's camera (vpt_set_camera + compute_camera in vpt_context.cu) restated operation for
-    operation in IEEE double from the float32-rounded inputs: look-at view, perspective with depth in
-    [0, 1] and y flipped, Gauss-Jordan inverse, rounded to float.  Bit-identical to
-    vpt_get_camera_matrices for the same SceneSpec."""
+def _view_matrix(sp: SceneSpec):
     f32 = lambda v: float(np.float32(v))  # noqa: E731
     e = [f32(v) for v in sp.cam_pos]
     t = [f32(v) for v in sp.cam_target]
@@ -164,9 +200,23 @@ def camera_inv_view_proj(sp: SceneSpec):
     sl = math.sqrt(s[0] * s[0] + s[1] * s[1] + s[2] * s[2])
     s = [v / sl for v in s]
     u = [s[1] * f[2] - s[2] * f[1], s[2] * f[0] - s[0] * f[2], s[0] * f[1] - s[1] * f[0]]
-    view = [s[0], u[0], -f[0], 0.0, s[1], u[1], -f[1], 0.0, s[2], u[2], -f[2], 0.0,
+    return [s[0], u[0], -f[0], 0.0, s[1], u[1], -f[1], 0.0, s[2], u[2], -f[2], 0.0,
             -(s[0] * e[0] + s[1] * e[1] + s[2] * e[2]), -(u[0] * e[0] + u[1] * e[1] + u[2] * e[2]),
             (f[0] * e[0] + f[1] * e[1] + f[2] * e[2]), 1.0]
+
+
+def camera_inv_view(sp: SceneSpec):
+    """inverse(view) as the core computes it for view-space lights (double, rounded to float)."""
+    return [float(np.float32(v)) for v in _mat_inverse(_view_matrix(sp))]
+
+
+def camera_inv_view_proj(sp: SceneSpec):
+    """The core's camera (vpt_set_camera + compute_camera in vpt_context.cu) restated operation for
+    operation in IEEE double from the float32-rounded inputs: look-at view, perspective with depth in
+    [0, 1] and y flipped, Gauss-Jordan inverse, rounded to float.  Bit-identical to
+    vpt_get_camera_matrices for the same SceneSpec."""
+    f32 = lambda v: float(np.float32(v))  # noqa: E731
+    view = _view_matrix(sp)
     aspect = float(sp.width) / float(sp.height) if sp.width > 0 and sp.height > 0 else 1.0
     th = math.tan(f32(sp.fovy) / 2.0)
     n, fa = f32(sp.near), f32(sp.far)
@@ -202,6 +252,10 @@ def oracle_scene(core, sp: SceneSpec, frames: int, frame_count: int = 0) -> brid
         border_density=float(border), extinction=float(f32(sp.extinction)), albedo=float(f32(sp.albedo)),
         g=float(f32(sp.g)), env_kind=ENV[sp.env], use_linear_rgb=sp.linear_rgb, env_image_linear=1,
         sun_intensity=sp.sun_intensity, sky_color=sp.sky_color, env_intensity=sp.env_intensity, density=dens)
+    sc.set("inv_view", camera_inv_view(sp))
+    sc.set("num_lights", len(sp.lights or []))
+    sc.set("env_is_black", 1 if sp.env == "black" else 0)
+    sc.set("lights", light_floats(sp.lights))
     # sun direction normalised exactly like vpt_set_sun (float ops in order)
     d = np.array(sp.sun_dir, np.float32)
     dl = np.sqrt(np.float32(np.float32(d[0] * d[0]) + np.float32(d[1] * d[1])) + np.float32(d[2] * d[2]), dtype=np.float32)
@@ -275,7 +329,8 @@ def reference_scene(sp: SceneSpec, frames: int, frame_start: int = 0, inv=None):
         linear_filter=1 if sp.interp == "trilinear" else 0, voxel_value_min=vmin, voxel_value_max=vmax,
         extinction=[sp.extinction] * 3, albedo=[sp.albedo] * 3, g=sp.g,
         sun_dir=[float(np.float32(d[i] / dl)) for i in range(3)], sun_intensity=sp.sun_intensity,
-        env_intensity=sp.env_intensity, is_env_black=1 if sp.env == "black" else 0, far_dist=sp.far)
+        env_intensity=sp.env_intensity, is_env_black=1 if sp.env == "black" else 0, far_dist=sp.far,
+        inv_view=camera_inv_view(sp), lights=light_floats(sp.lights))
     if sp.mode in ("decomposition", "rrt"):
         svs = supervoxel_size(nx, ny, nz)
         halo = 0 if sp.interp == "nearest" else 1
@@ -299,6 +354,8 @@ def reference_scene(sp: SceneSpec, frames: int, frame_start: int = 0, inv=None):
         sc.set("env_pyramid", bridge.env_pyramid(rgba, 12))
     tracker = {"delta": "delta", "ratio": "ratio", "decomposition": "decomposition", "rrt": "rrt",
                "nee": "nee_ess" if sp.use_ess else "nee"}[sp.mode]
+    if sp.lights:
+        tracker = f"nee_l{len(sp.lights)}"
     env = {"default": "default", "black": "black", "single": "single", "image": "image"}[sp.env]
     colour = "linear" if (sp.linear_rgb or env != "default") else "srgb"
     return sc, f"{tracker}__{sp.interp}__{env}__{colour}"

@@ -135,6 +135,14 @@ PATH_CASES = {
     "rrt": dict(mode="rrt"),
     "delta_default_sky": dict(mode="delta", env="default", linear_rgb=0),
     "nee_default_sky_g0": dict(mode="nee", env="default", g=0.0),
+    # lights of the light editor: a view-space spot light and a world-space point light; a
+    # directional light under a black sky (all NEE samples go to the light)
+    "nee_lights": dict(mode="nee", lights=[
+        dict(type="Spotlight", space="View", position=(0.05, 0.1, 0.0), spot_direction=(0.0, -0.1, -1.0),
+             spot_total_width=0.6, spot_falloff_start=0.3, intensity=3.0),
+        dict(type="Point Light", space="World", position=(0.6, 0.8, 0.3), intensity=0.8, color=(1.0, 0.8, 0.6))]),
+    "nee_light_directional_black": dict(mode="nee", env="black", lights=[
+        dict(type="Directional Light", space="View Orientation", position=(0.4, 0.9, 0.2), intensity=2.0)]),
     # escape radiance depends on the direction and paths are not capped: a diverged path shows
     "delta_default_sky_linear_uncapped": dict(mode="delta", env="default", linear_rgb=1, max_bounces=0),
     "decomposition_default_sky_uncapped": dict(mode="decomposition", env="default", linear_rgb=1, max_bounces=0),
@@ -228,11 +236,12 @@ def test_iteration_guard_reports_error_without_hanging(core):
     core("vpt_synchronize", None)
 
 
-@pytest.mark.parametrize("mode", ["delta", "ratio", "nee"])
+@pytest.mark.parametrize("mode", ["delta", "ratio", "nee", "nee_lights"])
 def test_schedules_trace_identical_paths(core, mode):
     """Tile, persistent-batch and per-lane-refill schedules trace the same paths (same film up to the
     order of the FP64 atomic additions)."""
-    sp = fbm_scene(mode=mode, width=40, height=40)
+    kw = PATH_CASES["nee_lights"] if mode == "nee_lights" else dict(mode=mode)
+    sp = fbm_scene(width=40, height=40, **kw)
     setup_core(core, sp)
     films = []
     for sched in (0, 1, 2):
