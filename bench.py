@@ -8,7 +8,7 @@ tracking; the other trackers are timed for a few steps each (per_tracker).  The 
 larger than L2, so no flush is needed between steps.
 
 `python bench.py --gpus N --steps K --warmup W` prints one JSON line (rank 0).  Under torchrun each
-rank renders its own frames (disjoint seeds; weak scaling, no collective on the data path).
+rank renders its own frame range of the image (weak scaling, no collective on the data path).
 `--impl reference` times the CPU oracle on this host (bounded sample of the same workload).
 """
 from __future__ import annotations
@@ -146,8 +146,9 @@ def setup_scene(vpt, rank):
     vpt.set_max_bounces(MAX_BOUNCES)
     vpt.set_grid_interpolation("Stochastic")
     vpt.set_denoiser("None")
-    # disjoint frame seeds per rank: the whole job renders rank-strided spp of one image
-    vpt.set_seed_offset((rank * 0x9E3779B1) & 0xFFFFFFFF)
+    # disjoint frame ranges per rank (frames [rank * 2^24, ...)): the whole job traces distinct
+    # paths of one image, the same paths one GPU would trace over all ranks' frames
+    vpt.set_frame_index(rank << 24)
 
 
 def run_ours(args):

@@ -60,6 +60,7 @@ SIGNATURES = {
     "vpt_get_camera_matrices": (c_int, [VptCtxP, F3, F3]),
     "vpt_set_resolution": (c_int, [VptCtxP, c_int, c_int]),
     "vpt_reset_accumulation": (c_int, [VptCtxP]),
+    "vpt_set_frame_index": (c_int, [VptCtxP, c_uint32]),
     "vpt_render_frames": (c_int, [VptCtxP, c_int, c_void_p]),
     "vpt_read_result": (c_int, [VptCtxP, c_void_p, c_int, c_int, c_void_p]),
     "vpt_render_frame": (c_int, [VptCtxP, c_int, c_void_p, c_int, c_int, c_void_p]),

@@ -195,6 +195,7 @@ struct VptContext {
     // film
     int width = 0, height = 0;
     uint32_t frame_count = 0;      // FrameInfo::frameCount: seeds and accumulation
+    uint32_t frame_origin = 0;     // frame index a cleared film starts from (frame sharding)
     uint32_t film_frames = 0;      // frames held in the film (1 for SVGF, which wants 1-spp input)
     DevBuf<double> film, film_sq;
     bool collect_stats = false;
@@ -248,7 +249,7 @@ cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 bool features_needed(const VptContext* ctx);
 
 void reset_film_state(VptContext* ctx) {
-    ctx->frame_count = 0;
+    ctx->frame_count = ctx->frame_origin;
     ctx->film_frames = 0;
 }
 
@@ -1194,6 +1195,13 @@ VptStatus vpt_set_resolution(VptContext* ctx, int width, int height) {
 
 VptStatus vpt_reset_accumulation(VptContext* ctx) {
     VPT_CHECK_CTX(ctx);
+    reset_film_state(ctx);
+    return VPT_OK;
+}
+
+VptStatus vpt_set_frame_index(VptContext* ctx, uint32_t first_frame) {
+    VPT_CHECK_CTX(ctx);
+    ctx->frame_origin = first_frame;
     reset_film_state(ctx);
     return VPT_OK;
 }

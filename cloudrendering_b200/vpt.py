@@ -570,6 +570,20 @@ def render_frame(input_tensor: torch.Tensor, frame_count: int) -> torch.Tensor:
     return _read(input_tensor, c, "vpt_read_result")
 
 
+def set_frame_index(first_frame: int) -> None:
+    """Clears the accumulation and makes `first_frame` the seed frame index every cleared film starts
+    from (frame sharding across GPUs; no reference counterpart)."""
+    _c("vpt_set_frame_index", int(first_frame) & 0xFFFFFFFF)
+
+
+def get_film_sum(width: int, height: int) -> torch.Tensor:
+    """The FP64 film: the sum of the radiance of every accumulated frame, [3, H, W] float64 on the host."""
+    _c("vpt_set_resolution", int(width), int(height))
+    out = np.zeros(width * height * 3, np.float64)
+    _c("vpt_read_statistics", out.ctypes.data_as(ctypes.c_void_p), None, 0, None)
+    return torch.from_numpy(out.reshape(height, width, 3).transpose(2, 0, 1).copy())
+
+
 def get_stats() -> dict:
     st = _lib.VptStats()
     _c("vpt_get_stats", ctypes.byref(st))

@@ -154,6 +154,12 @@ VptStatus vpt_get_camera_matrices(VptContext* ctx, float inv_view_proj[16], floa
 VptStatus vpt_set_resolution(VptContext* ctx, int width, int height);
 /* Clears the film: next frame index is 0 (onHasMoved, VolumetricPathTracingPass.cpp:1150-1162). */
 VptStatus vpt_reset_accumulation(VptContext* ctx);
+/* Clears the film and makes `first_frame` the frame index (seed, Clouds.glsl:80-84) that every
+ * cleared film starts from, until set again (default 0; a parameter change clears the film back to
+ * it).  Ranks that render disjoint frame ranges of one image this way trace exactly the paths of a
+ * single run over all frames, so the sum of their FP64 films is that run's film (no counterpart in
+ * the reference, which renders on one GPU). */
+VptStatus vpt_set_frame_index(VptContext* ctx, uint32_t first_frame);
 /* Traces `frames` 1-spp frames into the FP64 film on `stream` (enqueued, not synchronised). */
 VptStatus vpt_render_frames(VptContext* ctx, int frames, void* stream);
 /* Writes the accumulated mean (denoised when a denoiser is set) as channels x H x W fp32
