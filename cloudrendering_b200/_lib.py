@@ -109,6 +109,28 @@ SIGNATURES = {
     "vpt_kpn_reproject": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_int, c_int, c_void_p, c_void_p]),
     "vpt_eaw_denoise_rgba_noalloc": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_float, c_float,
                                              c_float, c_int, c_void_p, c_void_p]),
+    # learned denoiser network (csrc/vpt_unet.cu)
+    "vpt_unet_conv3x3": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_int,
+                                 c_int, c_int, c_void_p, c_void_p]),
+    "vpt_unet_conv3x3_wgrad": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_int, c_int,
+                                       c_void_p, c_void_p]),
+    "vpt_unet_wgrad_rows": (c_int, [c_int]),
+    "vpt_unet_rotate_weights": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p]),
+    "vpt_unet_pool2": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_void_p]),
+    "vpt_unet_upcat": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_int, c_void_p]),
+    "vpt_unet_upcat_grad_lo": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_int, c_void_p]),
+    "vpt_unet_encoder_grad": (c_int, [c_void_p, c_int, c_int, c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_int,
+                                      c_void_p]),
+    "vpt_unet_bias_grad": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_void_p]),
+    "vpt_unet_reduce_grads": (c_int, [c_void_p, c_int, c_int, c_int, c_void_p, c_int, c_void_p, c_void_p, c_void_p]),
+    "vpt_unet_adam": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, ctypes.c_long, c_float, c_float,
+                              c_float, c_float, c_int, c_float, c_void_p]),
+    "vpt_unet_to_bf16": (c_int, [c_void_p, c_void_p, ctypes.c_long, c_void_p]),
+    "vpt_unet_pack_input": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int, c_int,
+                                    c_void_p]),
+    "vpt_unet_head_blocks": (c_int, [c_int, c_int, c_int]),
+    "vpt_unet_kpn_head": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int, c_int,
+                                  c_float, c_void_p]),
 }
 
 class VptSparseInfo(ctypes.Structure):

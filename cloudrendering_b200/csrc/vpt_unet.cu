@@ -1,0 +1,927 @@
+// vpt_unet.cu - the learned denoiser's network kernels: a U-Net of 3x3 convolutions that predicts
+// per-pixel 5x5 kernels (a kernel-predicting denoiser), trained on the GPU by these kernels.
+//
+// The reference runs its learned denoiser through libtorch (src/Denoiser/PyTorchDenoiser.cpp:637-800,
+// a TorchScript forward).  It has no training code and no network of its own; this file is new.
+//
+// Tensors are NHWC bf16 ("pixels x channels", P = N*H*W rows, channels contiguous, every channel
+// count a multiple of 16); accumulation is fp32.  A 3x3 convolution (stride 1, zero padding 1) is an
+// implicit GEMM with K = 9 * Cin, k = tap * Cin + ci, tap = (dy + 1) * 3 + (dx + 1):
+//
+//   forward       y[p][co]  = act(bias[co] + sum_k x[p + off(tap)][ci] * w[co][k])       M = pixels
+//   input grad    dx[p][ci] = sum_k' dy[p + off(tap')][co] * wrot[ci][k'],  wrot[ci][t'][co]
+//                 = w[co][8 - t'][ci] (the same kernel, rotated weights)                   M = pixels
+//   weight grad   dw[co][k] = sum_p dy[p][co] * x[p + off(tap)][ci]                      M = k, K = pixels
+//
+// Tensor-core path (sm_100a tcgen05): one CTA computes a 128 x N tile (N <= 256 output channels) of
+// D = A * B^T with the fp32 accumulator in tensor memory (TMEM).  All 128 threads gather the A / B
+// tiles of the next K-stages with 16-byte cp.async copies (zero-filled outside the image) into a
+// 4-stage shared-memory ring laid out in the UMMA no-swizzle canonical form (8-row x 16-byte core
+// matrices); one thread issues tcgen05.mma (kind::f16, bf16 x bf16 -> fp32) per 16-wide K step and
+// tcgen05.commit signals a per-stage mbarrier when the stage's MMAs have read their operands, which
+// frees the slot for the next gather.  The epilogue reads the accumulator with tcgen05.ld (each warp
+// its 32 TMEM lanes = 32 tile rows) and fuses bias, ReLU, the ReLU-derivative mask of the backward
+// pass and the bf16 / fp32 store.  Forward and input-gradient tiles have K-major operands (k
+// contiguous: channels of one pixel); the weight-gradient tile has MN-major operands (channels
+// contiguous, pixels along K) and writes per-split fp32 partial sums that the optimiser reduces in a
+// fixed order (deterministic).
+//
+// Every mbarrier wait is bounded: on expiry the kernel records VPT_ERR_ITER_LIMIT in *err, waits
+// (bounded) for the MMAs it issued, frees its TMEM and returns.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+#include "../../include/vpt_b200.h"
+#include "vpt_kernels.h"
+
+namespace vpt {
+namespace unet {
+
+typedef __nv_bfloat16 bf16;
+
+constexpr int kBM = 128;      // tile rows (TMEM lanes)
+constexpr int kBK = 64;       // K elements per pipeline stage (4 MMAs of K = 16)
+constexpr int kStages = 4;    // shared-memory ring depth
+constexpr int kThreads = 128;
+constexpr uint32_t kWaitLimit = 1u << 22;  // bounded mbarrier waits (error flag on expiry)
+
+// ---------------------------------------------------------------------------------------------
+// PTX helpers
+// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, bool valid) {
+    const int n = valid ? 16 : 0;  // n = 0 writes 16 zero bytes and reads nothing
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src), "r"(n) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+// make this thread's generic-proxy shared-memory writes visible to the tensor core (async proxy)
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+// waits until the phase with the given parity has completed; false after kWaitLimit polls
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+    for (uint32_t i = 0; i < kWaitLimit; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
+
+// whole warp: allocate `cols` TMEM columns (power of two >= 32), address written to shared memory
+__device__ __forceinline__ void tmem_alloc(uint32_t dst, uint32_t cols) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(dst), "r"(cols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t cols) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(taddr), "r"(cols) : "memory");
+}
+
+// Shared-memory matrix descriptor, no swizzle: start address, leading-dimension byte offset (between
+// core matrices adjacent along K), stride-dimension byte offset (between core matrices adjacent
+// along M/N), all in 16-byte units; bits 46-47 = 1 (descriptor version of sm_100).
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    uint64_t d = (uint64_t)((addr >> 4) & 0x3FFFu);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+    d |= (uint64_t)1 << 46;
+    return d;
+}
+// Instruction descriptor of kind::f16: D fp32 (bits 4-5 = 1), A and B bf16 (bits 7-9, 10-12 = 1),
+// A / B major (bit 15 / 16: 0 = K-major, 1 = MN-major), N >> 3 (bits 17-22), M >> 4 (bits 24-28).
+__host__ __device__ constexpr uint32_t instr_desc(int m, int n, int a_mn, int b_mn) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)a_mn << 15) | ((uint32_t)b_mn << 16) |
+           ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
+}
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\ntcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(
+            tmem_d),
+        "l"(da), "l"(db), "r"(idesc), "r"(acc)
+        : "memory");
+}
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(bar)
+                 : "memory");
+}
+// 32 lanes x 16 consecutive 32-bit columns: lane i of the warp gets TMEM lane (base + i)
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// ---------------------------------------------------------------------------------------------
+// the implicit-GEMM convolution tile
+// ---------------------------------------------------------------------------------------------
+enum Mode : int { kConv = 0, kWgrad = 1 };
+
+struct ConvArgs {
+    const bf16* x;       // conv: input [P][cin]; wgrad: forward input [P][cin]
+    const bf16* w;       // conv: weights [cout][9][cin]; wgrad: output gradient dy [P][cout]
+    const float* bias;   // conv: [cout] or null
+    const bf16* mask;    // conv: [P][cout]; output multiplied by (mask > 0) (ReLU derivative) or null
+    void* y;             // conv: [P][cout] bf16 or fp32; wgrad: fp32 partials [splits][m_pad][cout]
+    int* err;            // device error word (VPT_ERR_ITER_LIMIT on an expired wait) or null
+    int n, h, w_;        // batch and image size (pixels P = n * h * w_)
+    int cin, cout;       // channel counts (multiples of 16)
+    int n_tile;          // output columns per CTA (multiple of 16, <= 256)
+    int tmem_cols;       // power of two >= n_tile, >= 32
+    int relu, out_f32;   // conv epilogue
+    int pix_per_split;   // wgrad: pixels (K) per CTA, multiple of kBK
+    int m_pad;           // wgrad: rows of a partial (multiple of kBM)
+};
+
+__device__ __forceinline__ void pixel_coords(int p, int h, int w, int& n, int& y, int& x) {
+    x = p % w;
+    const int t = p / w;
+    y = t % h;
+    n = t / h;
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kThreads) conv_tile_kernel(const ConvArgs a) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    __shared__ uint64_t bars[kStages];
+    __shared__ uint32_t tmem_slot;
+
+    const int tid = threadIdx.x;
+    const int P = a.n * a.h * a.w_;
+    const int n_tile = a.n_tile;
+    const uint32_t a_bytes = kBM * kBK * 2;
+    const uint32_t b_bytes = (uint32_t)n_tile * kBK * 2;
+    const uint32_t stage_bytes = a_bytes + b_bytes;
+    const uint32_t sbase = smem_u32(smem);
+    const int n0 = blockIdx.y * n_tile;
+
+    // K extent and tile origin
+    int K, m0, kbeg = 0, kend = 0;
+    if (MODE == kConv) {
+        K = 9 * a.cin;
+        m0 = blockIdx.x * kBM;
+    } else {
+        m0 = blockIdx.x * kBM;  // rows m = tap * cin + ci
+        kbeg = blockIdx.z * a.pix_per_split;
+        kend = min(P, kbeg + a.pix_per_split);
+        K = kend - kbeg;
+    }
+    const int M = (MODE == kConv) ? P : 9 * a.cin;
+    const int nk = (K + kBK - 1) / kBK;
+
+    if (tid == 0) {
+        for (int s = 0; s < kStages; ++s) mbar_init(smem_u32(&bars[s]), 1);
+        fence_mbar_init();
+    }
+    if (tid < 32) tmem_alloc(smem_u32(&tmem_slot), (uint32_t)a.tmem_cols);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_slot;
+
+    // per-thread gather state
+    int pn = 0, py = 0, px = 0;
+    bool p_ok = false;
+    int wg_tap = 0, wg_ci = 0;
+    bool wg_m_ok = false;
+    if (MODE == kConv) {
+        const int p = m0 + tid;  // this thread's A row
+        p_ok = p < P;
+        if (p_ok) pixel_coords(p, a.h, a.w_, pn, py, px);
+    } else {
+        const int m = m0 + ((tid >> 3) & 15) * 8;  // this thread's 8 A rows
+        wg_m_ok = m < M;
+        if (wg_m_ok) {
+            wg_tap = m / a.cin;
+            wg_ci = m - wg_tap * a.cin;
+        }
+    }
+
+    auto load_stage = [&](int slot, int s) {
+        const uint32_t sA = sbase + slot * stage_bytes;
+        const uint32_t sB = sA + a_bytes;
+        if (MODE == kConv) {
+            const int k0 = s * kBK;
+            // A: row tid, 8 chunks of 8 channels; unit (r, kc) at kc * kBM * 16 + r * 16
+#pragma unroll
+            for (int kc = 0; kc < 8; ++kc) {
+                const int kk = k0 + kc * 8;
+                const bf16* src = a.x;
+                bool v = false;
+                if (p_ok && kk < K) {
+                    const int tap = kk / a.cin, ci = kk - tap * a.cin;
+                    const int yy = py + tap / 3 - 1, xx = px + tap % 3 - 1;
+                    if (yy >= 0 && yy < a.h && xx >= 0 && xx < a.w_) {
+                        v = true;
+                        src = a.x + ((size_t)(pn * a.h + yy) * a.w_ + xx) * a.cin + ci;
+                    }
+                }
+                cp_async16(sA + kc * (kBM * 16) + tid * 16, src, v);
+            }
+            // B: weight rows n0 .. n0 + n_tile; unit (r, kc) at kc * n_tile * 16 + r * 16
+            for (int q = tid; q < n_tile * 8; q += kThreads) {
+                const int r = q % n_tile, kc = q / n_tile;
+                const int kk = k0 + kc * 8, co = n0 + r;
+                const bool v = co < a.cout && kk < K;
+                cp_async16(sB + kc * (n_tile * 16) + r * 16, v ? a.w + (size_t)co * K + kk : a.w, v);
+            }
+        } else {
+            const int pbase = kbeg + s * kBK;
+            // A (MN-major): unit (mc, kp) at (kp / 8) * 2048 + mc * 128 + (kp % 8) * 16 = 16 * q
+            const int kp_lo = tid & 7;
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                const int p = pbase + i * 8 + kp_lo;
+                const bf16* src = a.x;
+                bool v = false;
+                if (wg_m_ok && p < kend) {
+                    int qn, qy, qx;
+                    pixel_coords(p, a.h, a.w_, qn, qy, qx);
+                    const int yy = qy + wg_tap / 3 - 1, xx = qx + wg_tap % 3 - 1;
+                    if (yy >= 0 && yy < a.h && xx >= 0 && xx < a.w_) {
+                        v = true;
+                        src = a.x + ((size_t)(qn * a.h + yy) * a.w_ + xx) * a.cin + wg_ci;
+                    }
+                }
+                cp_async16(sA + (i * kThreads + tid) * 16, src, v);
+            }
+            // B (MN-major): dy rows; unit (nc, kp) at (kp / 8) * n_tile * 16 + nc * 128 + (kp % 8) * 16
+            const int nch = n_tile / 8;
+            for (int q = tid; q < n_tile * 8; q += kThreads) {
+                const int lo = q & 7, rest = q >> 3;
+                const int nc = rest % nch, kp = (rest / nch) * 8 + lo;
+                const int p = pbase + kp, co = n0 + nc * 8;
+                const bool v = p < kend && co < a.cout;
+                cp_async16(sB + q * 16, v ? a.w + (size_t)p * a.cout + co : a.w, v);
+            }
+        }
+    };
+
+    const uint32_t idesc = (MODE == kConv) ? instr_desc(kBM, n_tile, 0, 0) : instr_desc(kBM, n_tile, 1, 1);
+    const uint32_t a_lbo = (MODE == kConv) ? kBM * 16 : (kBM / 8) * 128;
+    const uint32_t b_lbo = (uint32_t)n_tile * 16;
+
+    for (int s = 0; s < kStages - 1; ++s) {
+        if (s < nk) load_stage(s, s);
+        cp_async_commit();
+    }
+    int aborted = 0;
+    int issued = -1;  // last stage whose MMAs were committed
+    for (int s = 0; s < nk; ++s) {
+        const int slot = s % kStages;
+        cp_async_wait<kStages - 2>();
+        fence_proxy_async();
+        if (__syncthreads_or(aborted)) break;
+        if (tid == 0) {
+            tc_fence_after();
+            const uint32_t sA = sbase + slot * stage_bytes;
+            const uint32_t sB = sA + a_bytes;
+            const int steps = min(kBK / 16, (K - s * kBK + 15) / 16);
+            for (int j = 0; j < steps; ++j) {
+                const uint64_t da = smem_desc(sA + j * 2 * a_lbo, a_lbo, 128);
+                const uint64_t db = smem_desc(sB + j * 2 * b_lbo, b_lbo, 128);
+                mma_bf16(tmem, da, db, idesc, (s > 0 || j > 0) ? 1u : 0u);
+            }
+            mma_commit(smem_u32(&bars[slot]));
+        }
+        issued = s;
+        const int nxt = s + kStages - 1;
+        if (nxt < nk) {
+            bool ok = true;
+            if (s >= 1) {  // the slot of stage s - 1 is refilled: its MMAs must have read it
+                const int ps = s - 1;
+                ok = mbar_wait(smem_u32(&bars[ps % kStages]), (uint32_t)((ps / kStages) & 1));
+            }
+            if (ok) load_stage(nxt % kStages, nxt);
+            else aborted = 1;
+        }
+        cp_async_commit();
+    }
+    cp_async_wait<0>();
+    // the last commit tracks every MMA this CTA issued
+    bool done = true;
+    if (issued >= 0) done = mbar_wait(smem_u32(&bars[issued % kStages]), (uint32_t)((issued / kStages) & 1));
+    const bool fail = __syncthreads_or(aborted || !done || (issued != nk - 1 && nk > 0));
+    tc_fence_after();
+
+    if (!fail && nk > 0) {
+        const int warp = tid >> 5, lane = tid & 31;
+        const int r = warp * 32 + lane;
+        const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+        for (int c0 = 0; c0 < n_tile; c0 += 16) {
+            float v[16];
+            tmem_ld16(trow + (uint32_t)c0, v);  // whole warp, uniform
+            const int co = n0 + c0;
+            if (co >= a.cout) continue;
+            if (MODE == kConv) {
+                const int p = m0 + r;
+                if (p >= P) continue;
+                if (a.bias) {
+#pragma unroll
+                    for (int i = 0; i < 16; ++i) v[i] += a.bias[co + i];
+                }
+                if (a.relu) {
+#pragma unroll
+                    for (int i = 0; i < 16; ++i) v[i] = fmaxf(v[i], 0.0f);
+                }
+                if (a.mask) {
+                    const uint4* mp = reinterpret_cast<const uint4*>(a.mask + (size_t)p * a.cout + co);
+                    const uint4 m4[2] = {mp[0], mp[1]};
+                    const bf16* mb = reinterpret_cast<const bf16*>(m4);
+#pragma unroll
+                    for (int i = 0; i < 16; ++i) v[i] = __bfloat162float(mb[i]) > 0.0f ? v[i] : 0.0f;
+                }
+                if (a.out_f32) {
+                    float4* dst = reinterpret_cast<float4*>(static_cast<float*>(a.y) + (size_t)p * a.cout + co);
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) dst[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+                } else {
+                    uint4 o[2];
+                    __nv_bfloat162* ob = reinterpret_cast<__nv_bfloat162*>(o);
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) ob[i] = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
+                    uint4* dst = reinterpret_cast<uint4*>(static_cast<bf16*>(a.y) + (size_t)p * a.cout + co);
+                    dst[0] = o[0];
+                    dst[1] = o[1];
+                }
+            } else {
+                const int m = m0 + r;
+                if (m >= M) continue;
+                float4* dst = reinterpret_cast<float4*>(static_cast<float*>(a.y) +
+                                                        ((size_t)blockIdx.z * a.m_pad + m) * a.cout + co);
+#pragma unroll
+                for (int i = 0; i < 4; ++i) dst[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+            }
+        }
+    }
+    if (fail && tid == 0 && a.err) atomicExch(a.err, (int)VPT_ERR_ITER_LIMIT);
+    tc_fence_before();
+    __syncthreads();
+    if (tid < 32) {
+        tc_fence_after();
+        tmem_dealloc(tmem, (uint32_t)a.tmem_cols);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// small kernels around the convolutions (NHWC bf16, 8 channels = 16 bytes per thread)
+// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ void load8(const bf16* p, float (&f)[8]) {
+    const uint4 u = *reinterpret_cast<const uint4*>(p);
+    const __nv_bfloat162* b = reinterpret_cast<const __nv_bfloat162*>(&u);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const float2 t = __bfloat1622float2(b[i]);
+        f[2 * i] = t.x;
+        f[2 * i + 1] = t.y;
+    }
+}
+__device__ __forceinline__ void store8(bf16* p, const float (&f)[8]) {
+    uint4 u;
+    __nv_bfloat162* b = reinterpret_cast<__nv_bfloat162*>(&u);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) b[i] = __floats2bfloat162_rn(f[2 * i], f[2 * i + 1]);
+    *reinterpret_cast<uint4*>(p) = u;
+}
+
+// wrot[ci][t][co] = w[co][8 - t][ci]
+__global__ void rotate_weights_kernel(const bf16* __restrict__ w, bf16* __restrict__ wrot, int cin, int cout) {
+    const int total = cout * 9 * cin;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+        const int ci = i % cin, t = (i / cin) % 9, co = i / (9 * cin);
+        wrot[((size_t)ci * 9 + (8 - t)) * cout + co] = w[i];
+    }
+}
+
+// 2x2 average pooling, [n][h][w][c] -> [n][h/2][w/2][c]
+__global__ void pool2_kernel(const bf16* __restrict__ in, bf16* __restrict__ out, int n, int h, int w, int c) {
+    const int ho = h / 2, wo = w / 2, c8 = c / 8;
+    const long total = (long)n * ho * wo * c8;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+        const int cc = (int)(i % c8) * 8;
+        const long pix = i / c8;
+        const int x = (int)(pix % wo), y = (int)((pix / wo) % ho), b = (int)(pix / ((long)wo * ho));
+        float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        for (int dy = 0; dy < 2; ++dy)
+            for (int dx = 0; dx < 2; ++dx) {
+                float f[8];
+                load8(in + (((size_t)b * h + 2 * y + dy) * w + 2 * x + dx) * c + cc, f);
+#pragma unroll
+                for (int k = 0; k < 8; ++k) acc[k] += f[k];
+            }
+#pragma unroll
+        for (int k = 0; k < 8; ++k) acc[k] *= 0.25f;
+        store8(out + pix * c + cc, acc);
+    }
+}
+
+// out[n][y][x] = (lo[n][y/2][x/2] (ca channels), skip[n][y][x] (cs channels)): nearest upsampling
+// of the coarser level concatenated with the skip connection
+__global__ void upcat_kernel(const bf16* __restrict__ lo, const bf16* __restrict__ skip, bf16* __restrict__ out,
+                             int n, int h, int w, int ca, int cs) {
+    const int c = ca + cs, c8 = c / 8;
+    const long total = (long)n * h * w * c8;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+        const int cc = (int)(i % c8) * 8;
+        const long pix = i / c8;
+        const int x = (int)(pix % w), y = (int)((pix / w) % h), b = (int)(pix / ((long)w * h));
+        const uint4* src;
+        if (cc < ca)
+            src = reinterpret_cast<const uint4*>(lo + (((size_t)b * (h / 2) + y / 2) * (w / 2) + x / 2) * ca + cc);
+        else
+            src = reinterpret_cast<const uint4*>(skip + (size_t)pix * cs + (cc - ca));
+        *reinterpret_cast<uint4*>(out + (size_t)pix * c + cc) = *src;
+    }
+}
+
+// backward of upcat for the coarse part: dlo[n][y][x][k] = (lo > 0) * sum of the 2x2 children's
+// gradient d[.][k] (k < ca); lo is the coarse level's ReLU output
+__global__ void upcat_grad_lo_kernel(const bf16* __restrict__ d, const bf16* __restrict__ lo, bf16* __restrict__ dlo,
+                                     int n, int h, int w, int ca, int cs) {
+    const int ho = h / 2, wo = w / 2, c = ca + cs, c8 = ca / 8;
+    const long total = (long)n * ho * wo * c8;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+        const int cc = (int)(i % c8) * 8;
+        const long pix = i / c8;
+        const int x = (int)(pix % wo), y = (int)((pix / wo) % ho), b = (int)(pix / ((long)wo * ho));
+        float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        for (int dy = 0; dy < 2; ++dy)
+            for (int dx = 0; dx < 2; ++dx) {
+                float f[8];
+                load8(d + (((size_t)b * h + 2 * y + dy) * w + 2 * x + dx) * c + cc, f);
+#pragma unroll
+                for (int k = 0; k < 8; ++k) acc[k] += f[k];
+            }
+        float m[8];
+        load8(lo + pix * ca + cc, m);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) acc[k] = m[k] > 0.0f ? acc[k] : 0.0f;
+        store8(dlo + pix * ca + cc, acc);
+    }
+}
+
+// gradient at an encoder level's ReLU output e (c channels): the skip part of the decoder's
+// concatenated gradient (d_cat[p][cat_off + k], row stride cat_c; may be null) plus the pooled
+// branch's gradient d_pool[n][y/2][x/2][k] / 4 (may be null), times (e > 0)
+__global__ void encoder_grad_kernel(const bf16* __restrict__ d_cat, int cat_c, int cat_off,
+                                    const bf16* __restrict__ d_pool, const bf16* __restrict__ e,
+                                    bf16* __restrict__ out, int n, int h, int w, int c) {
+    const int c8 = c / 8;
+    const long total = (long)n * h * w * c8;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+        const int cc = (int)(i % c8) * 8;
+        const long pix = i / c8;
+        const int x = (int)(pix % w), y = (int)((pix / w) % h), b = (int)(pix / ((long)w * h));
+        float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0}, f[8];
+        if (d_cat) {
+            load8(d_cat + (size_t)pix * cat_c + cat_off + cc, f);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) acc[k] += f[k];
+        }
+        if (d_pool) {
+            load8(d_pool + (((size_t)b * (h / 2) + y / 2) * (w / 2) + x / 2) * c + cc, f);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) acc[k] += 0.25f * f[k];
+        }
+        load8(e + (size_t)pix * c + cc, f);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) acc[k] = f[k] > 0.0f ? acc[k] : 0.0f;
+        store8(out + (size_t)pix * c + cc, acc);
+    }
+}
+
+// per-block column sums of dy [P][c] (bias gradient, first pass): partial[block][c]
+__global__ void bias_grad_kernel(const bf16* __restrict__ dy, float* __restrict__ partial, int P, int c) {
+    extern __shared__ float red[];  // [blockDim.x / c8 groups][c]
+    const int c8 = c / 8;
+    const int lane_c = threadIdx.x % c8, group = threadIdx.x / c8, groups = blockDim.x / c8;
+    float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    if (group < groups) {
+        for (long p = (long)blockIdx.x * groups + group; p < P; p += (long)gridDim.x * groups) {
+            float f[8];
+            load8(dy + p * c + lane_c * 8, f);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) acc[k] += f[k];
+        }
+#pragma unroll
+        for (int k = 0; k < 8; ++k) red[group * c + lane_c * 8 + k] = acc[k];
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < c; j += blockDim.x) {
+        float s = 0.0f;
+        for (int g = 0; g < groups; ++g) s += red[g * c + j];
+        partial[(size_t)blockIdx.x * c + j] = s;
+    }
+}
+
+// gradient of one layer into the flat fp32 gradient: g[co][t][ci] = sum_s wpart[s][t*cin+ci][co]
+// (fixed order over the splits) and gb[co] = sum_b bpart[b][co]
+__global__ void reduce_grads_kernel(const float* __restrict__ wpart, int splits, int m_pad, int cin, int cout,
+                                    const float* __restrict__ bpart, int bblocks, float* __restrict__ gw,
+                                    float* __restrict__ gb) {
+    const int nw = cout * 9 * cin;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nw + cout; i += gridDim.x * blockDim.x) {
+        float s = 0.0f;
+        if (i < nw) {
+            const int ci = i % cin, t = (i / cin) % 9, co = i / (9 * cin);
+            const size_t off = (size_t)(t * cin + ci) * cout + co;
+            for (int k = 0; k < splits; ++k) s += wpart[(size_t)k * m_pad * cout + off];
+            gw[i] = s;
+        } else {
+            const int co = i - nw;
+            if (bpart)
+                for (int k = 0; k < bblocks; ++k) s += bpart[(size_t)k * cout + co];
+            gb[co] = s;
+        }
+    }
+}
+
+// Adam (Kingma & Ba 2015, Algorithm 1) on the flat fp32 master parameters; the bf16 copy the
+// convolutions read is written in the same pass
+__global__ void adam_kernel(float* __restrict__ param, bf16* __restrict__ param_bf16, float* __restrict__ m1,
+                            float* __restrict__ m2, const float* __restrict__ grad, long count, float lr, float beta1,
+                            float beta2, float eps, float bias1, float bias2, float grad_scale) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < count; i += (long)gridDim.x * blockDim.x) {
+        const float g = grad[i] * grad_scale;
+        const float a = beta1 * m1[i] + (1.0f - beta1) * g;
+        const float b = beta2 * m2[i] + (1.0f - beta2) * g * g;
+        m1[i] = a;
+        m2[i] = b;
+        const float mhat = a / bias1, vhat = b / bias2;
+        const float p = param[i] - lr * mhat / (sqrtf(vhat) + eps);
+        param[i] = p;
+        if (param_bf16) param_bf16[i] = __float2bfloat16_rn(p);
+    }
+}
+
+__global__ void f32_to_bf16_kernel(const float* __restrict__ in, bf16* __restrict__ out, long count) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < count; i += (long)gridDim.x * blockDim.x)
+        out[i] = __float2bfloat16_rn(in[i]);
+}
+
+// ---------------------------------------------------------------------------------------------
+// network input and the kernel-prediction head
+// ---------------------------------------------------------------------------------------------
+constexpr int kInputChannels = 16;  // 11 used: log radiance 3, albedo 3, normal 3, depth 1, transmittance 1
+constexpr int kHeadChannels = 32;   // 25 used: 5 x 5 kernel logits
+constexpr int kTaps = 25;
+
+// planes: [n][3][h][w] radiance (mean of the frames rendered so far), albedo [n][3][h][w], normal
+// [n][3][h][w], depth [n][h][w], transmittance [n][h][w] (each may be null -> zeros)
+__global__ void pack_input_kernel(const float* __restrict__ radiance, const float* __restrict__ albedo,
+                                  const float* __restrict__ normal, const float* __restrict__ depth,
+                                  const float* __restrict__ transmittance, bf16* __restrict__ out, int n, int h,
+                                  int w) {
+    const long plane = (long)h * w, total = (long)n * plane;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+        const long b = i / plane, q = i % plane;
+        float f[16] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+        for (int c = 0; c < 3; ++c) {
+            const float r = radiance[(b * 3 + c) * plane + q];
+            f[c] = log1pf(fmaxf(r, 0.0f));
+            if (albedo) f[3 + c] = albedo[(b * 3 + c) * plane + q];
+            if (normal) f[6 + c] = normal[(b * 3 + c) * plane + q];
+        }
+        if (depth) f[9] = depth[b * plane + q];
+        if (transmittance) f[10] = transmittance[b * plane + q];
+        float lo[8], hi[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            lo[k] = f[k];
+            hi[k] = f[8 + k];
+        }
+        store8(out + i * kInputChannels, lo);
+        store8(out + i * kInputChannels + 8, hi);
+    }
+}
+
+// Per-pixel 5x5 kernel application with the tap softmax fused, and (target != null) the relative
+// MSE loss and its gradient with respect to the logits:
+//   s = softmax(logits[p][0..24]);  d[c][p] = sum_j s_j x[c][p + off_j]  (taps outside skipped)
+//   loss = sum_{p,c} (d - t)^2 / (t^2 + eps) * inv_count
+//   dL/dlogit_j = s_j (g . x_j - g . d),  g_c = 2 (d_c - t_c) / (t_c^2 + eps) * inv_count
+// logits: [P][32] fp32 (NHWC, channels 25..31 unused); x, t, out: [n][3][h][w] fp32.
+__global__ void kpn_head_kernel(const float* __restrict__ logits, const float* __restrict__ x,
+                                const float* __restrict__ target, float* __restrict__ out, bf16* __restrict__ dlogits,
+                                float* __restrict__ loss_partial, int n, int h, int w, float eps, float inv_count) {
+    const long plane = (long)h * w, total = (long)n * plane;
+    float local = 0.0f;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+        const long b = i / plane, q = i % plane;
+        const int y = (int)(q / w), xx = (int)(q % w);
+        float s[kTaps];
+        float mx = -INFINITY;
+        const float4* lp = reinterpret_cast<const float4*>(logits + i * kHeadChannels);
+#pragma unroll
+        for (int k = 0; k < 7; ++k) {
+            const float4 u = lp[k];
+            const float vals[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+            for (int e = 0; e < 4; ++e)
+                if (4 * k + e < kTaps) s[4 * k + e] = vals[e];
+        }
+#pragma unroll
+        for (int j = 0; j < kTaps; ++j) mx = fmaxf(mx, s[j]);
+        float sum = 0.0f;
+#pragma unroll
+        for (int j = 0; j < kTaps; ++j) {
+            s[j] = __expf(s[j] - mx);
+            sum += s[j];
+        }
+        const float inv = 1.0f / sum;
+        float d[3] = {0.0f, 0.0f, 0.0f};
+        const float* xb = x + b * 3 * plane;
+#pragma unroll
+        for (int j = 0; j < kTaps; ++j) {
+            s[j] *= inv;
+            const int yy = y + j / 5 - 2, xq = xx + j % 5 - 2;
+            if (yy < 0 || yy >= h || xq < 0 || xq >= w) continue;
+            const long o = (long)yy * w + xq;
+            d[0] += s[j] * xb[o];
+            d[1] += s[j] * xb[plane + o];
+            d[2] += s[j] * xb[2 * plane + o];
+        }
+        if (out) {
+            for (int c = 0; c < 3; ++c) out[(b * 3 + c) * plane + q] = d[c];
+        }
+        if (target) {
+            float g[3];
+            for (int c = 0; c < 3; ++c) {
+                const float t = target[(b * 3 + c) * plane + q];
+                const float den = t * t + eps;
+                const float e = d[c] - t;
+                local += e * e / den * inv_count;
+                g[c] = 2.0f * e / den * inv_count;
+            }
+            const float gd = g[0] * d[0] + g[1] * d[1] + g[2] * d[2];
+            float gl[kHeadChannels];
+#pragma unroll
+            for (int j = 0; j < kHeadChannels; ++j) gl[j] = 0.0f;
+#pragma unroll
+            for (int j = 0; j < kTaps; ++j) {
+                const int yy = y + j / 5 - 2, xq = xx + j % 5 - 2;
+                float gx = 0.0f;
+                if (yy >= 0 && yy < h && xq >= 0 && xq < w) {
+                    const long o = (long)yy * w + xq;
+                    gx = g[0] * xb[o] + g[1] * xb[plane + o] + g[2] * xb[2 * plane + o];
+                }
+                gl[j] = s[j] * (gx - gd);
+            }
+#pragma unroll
+            for (int k = 0; k < kHeadChannels / 8; ++k) {
+                float f[8];
+#pragma unroll
+                for (int e = 0; e < 8; ++e) f[e] = gl[8 * k + e];
+                store8(dlogits + i * kHeadChannels + 8 * k, f);
+            }
+        }
+    }
+    if (loss_partial) {
+        // block reduction (fixed order)
+        __shared__ float red[256];
+        red[threadIdx.x] = local;
+        __syncthreads();
+        for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+            if ((int)threadIdx.x < st) red[threadIdx.x] += red[threadIdx.x + st];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) loss_partial[blockIdx.x] = red[0];
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------------------------
+inline int grid_for(long work, int threads) {
+    long b = (work + threads - 1) / threads;
+    if (b < 1) b = 1;
+    if (b > 148L * 16) b = 148L * 16;
+    return (int)b;
+}
+
+inline int pow2_cols(int n) {
+    int c = 32;
+    while (c < n) c <<= 1;
+    return c;
+}
+
+template <int MODE>
+cudaError_t launch_tile(const ConvArgs& a, dim3 grid, cudaStream_t s) {
+    const size_t smem = (size_t)kStages * (kBM * kBK * 2 + (size_t)a.n_tile * kBK * 2);
+    cudaError_t e = cudaFuncSetAttribute(conv_tile_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+    conv_tile_kernel<MODE><<<grid, kThreads, smem, s>>>(a);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+inline bool chan_ok(int c) { return c > 0 && c % 16 == 0; }
+
+}  // namespace unet
+}  // namespace vpt
+
+using namespace vpt::unet;
+
+extern "C" {
+
+VptStatus vpt_unet_conv3x3(const void* x, const void* w, const float* bias, const void* mask, void* y, int n, int h,
+                           int width, int cin, int cout, int relu, int out_f32, int* err, void* stream) {
+    if (!x || !w || !y || n <= 0 || h <= 0 || width <= 0 || !chan_ok(cin) || !chan_ok(cout) || cout > 4096 ||
+        (long)n * h * width > (1L << 30))
+        return VPT_ERR_ARG;
+    ConvArgs a{};
+    a.x = static_cast<const bf16*>(x);
+    a.w = static_cast<const bf16*>(w);
+    a.bias = bias;
+    a.mask = static_cast<const bf16*>(mask);
+    a.y = y;
+    a.err = err;
+    a.n = n;
+    a.h = h;
+    a.w_ = width;
+    a.cin = cin;
+    a.cout = cout;
+    const int ntiles = (cout + 255) / 256;
+    a.n_tile = ((cout + ntiles - 1) / ntiles + 15) / 16 * 16;
+    a.tmem_cols = pow2_cols(a.n_tile);
+    a.relu = relu;
+    a.out_f32 = out_f32;
+    const long P = (long)n * h * width;
+    const dim3 grid((unsigned)((P + kBM - 1) / kBM), (unsigned)((cout + a.n_tile - 1) / a.n_tile), 1);
+    return launch_tile<kConv>(a, grid, static_cast<cudaStream_t>(stream)) == cudaSuccess ? VPT_OK : VPT_ERR_CUDA;
+}
+
+VptStatus vpt_unet_conv3x3_wgrad(const void* x, const void* dy, float* partial, int n, int h, int width, int cin,
+                                 int cout, int pixels_per_split, int* err, void* stream) {
+    if (!x || !dy || !partial || n <= 0 || h <= 0 || width <= 0 || !chan_ok(cin) || !chan_ok(cout) ||
+        cout > 4096 || pixels_per_split <= 0 || pixels_per_split % kBK != 0 || (long)n * h * width > (1L << 30))
+        return VPT_ERR_ARG;
+    ConvArgs a{};
+    a.x = static_cast<const bf16*>(x);
+    a.w = static_cast<const bf16*>(dy);
+    a.y = partial;
+    a.err = err;
+    a.n = n;
+    a.h = h;
+    a.w_ = width;
+    a.cin = cin;
+    a.cout = cout;
+    const int ntiles = (cout + 255) / 256;
+    a.n_tile = ((cout + ntiles - 1) / ntiles + 15) / 16 * 16;
+    a.tmem_cols = pow2_cols(a.n_tile);
+    a.pix_per_split = pixels_per_split;
+    const int mtiles = (9 * cin + kBM - 1) / kBM;
+    a.m_pad = mtiles * kBM;
+    const long P = (long)n * h * width;
+    const dim3 grid((unsigned)mtiles, (unsigned)((cout + a.n_tile - 1) / a.n_tile),
+                    (unsigned)((P + pixels_per_split - 1) / pixels_per_split));
+    return launch_tile<kWgrad>(a, grid, static_cast<cudaStream_t>(stream)) == cudaSuccess ? VPT_OK : VPT_ERR_CUDA;
+}
+
+int vpt_unet_wgrad_rows(int cin) { return (9 * cin + kBM - 1) / kBM * kBM; }
+
+VptStatus vpt_unet_rotate_weights(const void* w, void* wrot, int cin, int cout, void* stream) {
+    if (!w || !wrot || !chan_ok(cin) || !chan_ok(cout)) return VPT_ERR_ARG;
+    rotate_weights_kernel<<<grid_for((long)cout * 9 * cin, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        static_cast<const bf16*>(w), static_cast<bf16*>(wrot), cin, cout);
+    vpt::count_launches(1);
+    return cudaGetLastError() == cudaSuccess ? VPT_OK : VPT_ERR_CUDA;
+}
+
+VptStatus vpt_unet_pool2(const void* in, void* out, int n, int h, int w, int c, void* stream) {
+    if (!in || !out || n <= 0 || h <= 1 || w <= 1 || h % 2 || w % 2 || c <= 0 || c % 8) return VPT_ERR_ARG;
+    pool2_kernel<<<grid_for((long)n * (h / 2) * (w / 2) * (c / 8), 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        static_cast<const bf16*>(in), static_cast<bf16*>(out), n, h, w, c);
+    vpt::count_launches(1);
+    return cudaGetLastError() == cudaSuccess ? VPT_OK : VPT_ERR_CUDA;
+}
+
+VptStatus vpt_unet_upcat(const void* lo, const void* skip, void* out, int n, int h, int w, int ca, int cs,
+                         void* stream) {
+    if (!lo || !skip || !out || n <= 0 || h <= 1 || w <= 1 || h % 2 || w % 2 || ca <= 0 || ca % 8 || cs <= 0 ||
+        cs % 8)
+        return VPT_ERR_ARG;
+    upcat_kernel<<<grid_for((long)n * h * w * ((ca + cs) / 8), 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        static_cast<const bf16*>(lo), static_cast<const bf16*>(skip), static_cast<bf16*>(out), n, h, w, ca, cs);
+    vpt::count_launches(1);
+    return cudaGetLastError() == cudaSuccess ? VPT_OK : VPT_ERR_CUDA;
+}
+
+VptStatus vpt_unet_upcat_grad_lo(const void* d, const void* lo, void* dlo, int n, int h, int w, int ca, int cs,
+                                 void* stream) {
+    if (!d || !lo || !dlo || n <= 0 || h <= 1 || w <= 1 || h % 2 || w % 2 || ca <= 0 || ca % 8 || cs <= 0 ||
+        cs % 8)
+        return VPT_ERR_ARG;
+    upcat_grad_lo_kernel<<<grid_for((long)n * (h / 2) * (w / 2) * (ca / 8), 256), 256, 0,
+                           static_cast<cudaStream_t>(stream)>>>(static_cast<const bf16*>(d),
+                                                                static_cast<const bf16*>(lo), static_cast<bf16*>(dlo),
+                                                                n, h, w, ca, cs);
+    vpt::count_launches(1);
+    return cudaGetLastError() == cudaSuccess ? VPT_OK : VPT_ERR_CUDA;
+}
+
+VptStatus vpt_unet_encoder_grad(const void* d_cat, int cat_c, int cat_off, const void* d_pool, const void* e,
+                                void* out, int n, int h, int w, int c, void* stream) {
+    if (!e || !out || n <= 0 || h <= 0 || w <= 0 || c <= 0 || c % 8 || (d_cat && (cat_off % 8 || cat_c % 8)) ||
+        (d_pool && (h % 2 || w % 2)))
+        return VPT_ERR_ARG;
+    encoder_grad_kernel<<<grid_for((long)n * h * w * (c / 8), 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        static_cast<const bf16*>(d_cat), cat_c, cat_off, static_cast<const bf16*>(d_pool),
+        static_cast<const bf16*>(e), static_cast<bf16*>(out), n, h, w, c);
+    vpt::count_launches(1);
+    return cudaGetLastError() == cudaSuccess ? VPT_OK : VPT_ERR_CUDA;
+}
+
+VptStatus vpt_unet_bias_grad(const void* dy, float* partial, int pixels, int c, int blocks, void* stream) {
+    if (!dy || !partial || pixels <= 0 || c <= 0 || c % 8 || c > 2048 || blocks <= 0) return VPT_ERR_ARG;
+    const int c8 = c / 8;
+    int threads = 256 / c8 * c8;
+    if (threads < c8) threads = c8;
+    const size_t smem = (size_t)(threads / c8) * c * sizeof(float);
+    bias_grad_kernel<<<blocks, threads, smem, static_cast<cudaStream_t>(stream)>>>(static_cast<const bf16*>(dy),
+                                                                                   partial, pixels, c);
+    vpt::count_launches(1);
+    return cudaGetLastError() == cudaSuccess ? VPT_OK : VPT_ERR_CUDA;
+}
+
+VptStatus vpt_unet_reduce_grads(const float* wpartial, int splits, int cin, int cout, const float* bpartial,
+                                int bblocks, float* grad_w, float* grad_b, void* stream) {
+    if (!wpartial || !grad_w || !grad_b || splits <= 0 || !chan_ok(cin) || !chan_ok(cout) ||
+        (bpartial && bblocks <= 0))
+        return VPT_ERR_ARG;
+    const int m_pad = (9 * cin + kBM - 1) / kBM * kBM;
+    reduce_grads_kernel<<<grid_for((long)cout * 9 * cin + cout, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        wpartial, splits, m_pad, cin, cout, bpartial, bblocks, grad_w, grad_b);
+    vpt::count_launches(1);
+    return cudaGetLastError() == cudaSuccess ? VPT_OK : VPT_ERR_CUDA;
+}
+
+VptStatus vpt_unet_adam(float* param, void* param_bf16, float* m1, float* m2, const float* grad, long count, float lr,
+                        float beta1, float beta2, float eps, int step, float grad_scale, void* stream) {
+    if (!param || !m1 || !m2 || !grad || count <= 0 || step <= 0) return VPT_ERR_ARG;
+    const float bias1 = 1.0f - powf(beta1, (float)step), bias2 = 1.0f - powf(beta2, (float)step);
+    adam_kernel<<<grid_for(count, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        param, static_cast<bf16*>(param_bf16), m1, m2, grad, count, lr, beta1, beta2, eps, bias1, bias2, grad_scale);
+    vpt::count_launches(1);
+    return cudaGetLastError() == cudaSuccess ? VPT_OK : VPT_ERR_CUDA;
+}
+
+VptStatus vpt_unet_to_bf16(const float* in, void* out, long count, void* stream) {
+    if (!in || !out || count <= 0) return VPT_ERR_ARG;
+    f32_to_bf16_kernel<<<grid_for(count, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        in, static_cast<bf16*>(out), count);
+    vpt::count_launches(1);
+    return cudaGetLastError() == cudaSuccess ? VPT_OK : VPT_ERR_CUDA;
+}
+
+VptStatus vpt_unet_pack_input(const float* radiance, const float* albedo, const float* normal, const float* depth,
+                              const float* transmittance, void* out, int n, int h, int w, void* stream) {
+    if (!radiance || !out || n <= 0 || h <= 0 || w <= 0) return VPT_ERR_ARG;
+    pack_input_kernel<<<grid_for((long)n * h * w, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        radiance, albedo, normal, depth, transmittance, static_cast<bf16*>(out), n, h, w);
+    vpt::count_launches(1);
+    return cudaGetLastError() == cudaSuccess ? VPT_OK : VPT_ERR_CUDA;
+}
+
+int vpt_unet_head_blocks(int n, int h, int w) { return grid_for((long)n * h * w, 256); }
+
+VptStatus vpt_unet_kpn_head(const float* logits, const float* radiance, const float* target, float* out,
+                            void* dlogits, float* loss_partial, int n, int h, int w, float eps, void* stream) {
+    if (!logits || !radiance || n <= 0 || h <= 0 || w <= 0 || (target && !dlogits) || eps <= 0.0f)
+        return VPT_ERR_ARG;
+    const int blocks = grid_for((long)n * h * w, 256);
+    const float inv_count = 1.0f / (3.0f * (float)n * (float)h * (float)w);
+    kpn_head_kernel<<<blocks, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        logits, radiance, target, out, static_cast<bf16*>(dlogits), loss_partial, n, h, w, eps, inv_count);
+    vpt::count_launches(1);
+    return cudaGetLastError() == cudaSuccess ? VPT_OK : VPT_ERR_CUDA;
+}
+
+}  // extern "C"

@@ -342,6 +342,60 @@ VptStatus vpt_eaw_denoise_rgba_noalloc(const float* color, const float* position
                                        int height, int iterations, float phi_color, float phi_position,
                                        float phi_normal, int ref_compute_quirk, float* out, void* stream);
 
+/* ---- learned denoiser network (no reference counterpart: the reference runs a TorchScript model
+ * through libtorch, src/Denoiser/PyTorchDenoiser.cpp:637-800, and has no training code).  A U-Net of
+ * 3x3 convolutions predicting per-pixel 5x5 kernels, forward and backward on tcgen05 tensor cores.
+ * Tensors are device arrays, NHWC bf16 ("pixels x channels", channel counts multiples of 16 for the
+ * convolutions, 8 for the rest); conv weights [cout][9][cin] bf16 with tap = (dy+1)*3 + (dx+1).
+ * `err` (device int, may be NULL) receives VPT_ERR_ITER_LIMIT if a kernel's bounded wait expired. ---- */
+
+/* y[p][co] = act(bias[co] + sum_{t,ci} x[p + off(t)][ci] w[co][t][ci]) (zero padding), act = ReLU if
+ * relu; then times (mask[p][co] > 0) if mask != NULL; y bf16, or fp32 if out_f32.  The input gradient
+ * of a convolution is this call on the output gradient with vpt_unet_rotate_weights' weights and
+ * the forward input as mask (ReLU derivative). */
+VptStatus vpt_unet_conv3x3(const void* x, const void* w, const float* bias, const void* mask, void* y, int n, int h,
+                           int width, int cin, int cout, int relu, int out_f32, int* err, void* stream);
+/* Weight gradient: partial[s][t*cin + ci][co] = sum over pixels p of split s (pixels_per_split each,
+ * a multiple of 64) of dy[p][co] x[p + off(t)][ci]; partial has vpt_unet_wgrad_rows(cin) rows per
+ * split, reduced by vpt_unet_reduce_grads. */
+VptStatus vpt_unet_conv3x3_wgrad(const void* x, const void* dy, float* partial, int n, int h, int width, int cin,
+                                 int cout, int pixels_per_split, int* err, void* stream);
+int vpt_unet_wgrad_rows(int cin);
+/* wrot[ci][t][co] = w[co][8 - t][ci] */
+VptStatus vpt_unet_rotate_weights(const void* w, void* wrot, int cin, int cout, void* stream);
+/* 2x2 average pooling [n][h][w][c] -> [n][h/2][w/2][c] */
+VptStatus vpt_unet_pool2(const void* in, void* out, int n, int h, int w, int c, void* stream);
+/* out[n][y][x] = concat(lo[n][y/2][x/2] (ca channels), skip[n][y][x] (cs channels)) */
+VptStatus vpt_unet_upcat(const void* lo, const void* skip, void* out, int n, int h, int w, int ca, int cs,
+                         void* stream);
+/* gradient at the coarse input of vpt_unet_upcat: (lo > 0) * sum over the 2x2 children of d[..][0:ca] */
+VptStatus vpt_unet_upcat_grad_lo(const void* d, const void* lo, void* dlo, int n, int h, int w, int ca, int cs,
+                                 void* stream);
+/* (e > 0) * (d_cat[p][cat_off .. cat_off + c] + d_pool[n][y/2][x/2] / 4); d_cat / d_pool may be NULL */
+VptStatus vpt_unet_encoder_grad(const void* d_cat, int cat_c, int cat_off, const void* d_pool, const void* e,
+                                void* out, int n, int h, int w, int c, void* stream);
+/* per-block column sums of dy [pixels][c] into partial[blocks][c] (bias gradient, first pass) */
+VptStatus vpt_unet_bias_grad(const void* dy, float* partial, int pixels, int c, int blocks, void* stream);
+/* grad_w[co][t][ci] = sum_s wpartial[s][t*cin+ci][co]; grad_b[co] = sum_b bpartial[b][co] (fixed order) */
+VptStatus vpt_unet_reduce_grads(const float* wpartial, int splits, int cin, int cout, const float* bpartial,
+                                int bblocks, float* grad_w, float* grad_b, void* stream);
+/* one Adam step (Kingma & Ba 2015) on fp32 parameters; param_bf16 (may be NULL) receives the bf16 copy */
+VptStatus vpt_unet_adam(float* param, void* param_bf16, float* m1, float* m2, const float* grad, long count, float lr,
+                        float beta1, float beta2, float eps, int step, float grad_scale, void* stream);
+VptStatus vpt_unet_to_bf16(const float* in, void* out, long count, void* stream);
+/* network input [n][h][w][16] bf16 from planes [n][c][h][w]: log1p(radiance) 3, albedo 3, normal 3,
+ * depth 1, transmittance 1 (NULL planes give zeros) */
+VptStatus vpt_unet_pack_input(const float* radiance, const float* albedo, const float* normal, const float* depth,
+                              const float* transmittance, void* out, int n, int h, int w, void* stream);
+int vpt_unet_head_blocks(int n, int h, int w);
+/* Kernel-prediction head (perPixelKernelCuda semantics, modules/kpn_module/src/Kernel.cu:38-135, with
+ * the tap softmax fused): out[n][c][y][x] = sum_j softmax(logits[p][0..24])_j radiance[n][c][y+dy][x+dx]
+ * (taps outside skipped; logits [p][32] fp32).  With target != NULL also the relative MSE
+ * sum (d-t)^2/(t^2+eps)/(3*n*h*w) as per-block partial sums (vpt_unet_head_blocks of them) and its
+ * gradient dlogits [p][32] bf16.  out may be NULL. */
+VptStatus vpt_unet_kpn_head(const float* logits, const float* radiance, const float* target, float* out,
+                            void* dlogits, float* loss_partial, int n, int h, int w, float eps, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

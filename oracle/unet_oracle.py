@@ -1,0 +1,177 @@
+"""CPU oracle of the learned denoiser's network operations (test infrastructure only).
+
+Restates, in float64 numpy, what the CUDA kernels of cloudrendering_b200/csrc/vpt_unet.cu compute:
+3x3 convolutions (stride 1, zero padding 1) on NHWC tensors with weights [cout][9][cin]
+(tap = (dy + 1) * 3 + (dx + 1)), their input and weight gradients, 2x2 average pooling, nearest
+upsampling + concatenation, the encoder gradient combine, the per-pixel 5x5 kernel head with the
+relative-MSE loss and its logit gradient, and Adam (Kingma & Ba 2015, Algorithm 1).
+
+The reference (chrismile/CloudRendering) has no training code: its learned denoiser is a TorchScript
+forward (src/Denoiser/PyTorchDenoiser.cpp:637-800) and the kernel application of
+modules/kpn_module/src/Kernel.cu:38-135 (softmax over the taps, taps outside the image skipped),
+which kpn_head follows.  The convolution semantics are pinned to torch.nn.functional.conv2d and the
+gradients to torch.autograd in float64 (tests/test_unet_cpu.py).
+
+Inputs the GPU reads as bf16 are rounded to bf16 first (bf16()), so the oracle sees the same values.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def bf16(a) -> np.ndarray:
+    """Round float32 values to bfloat16 (round to nearest even), returned as float32."""
+    a = np.ascontiguousarray(a, np.float32)
+    u = a.view(np.uint32).astype(np.uint64)
+    r = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16) << 16
+    out = r.astype(np.uint32).view(np.float32).copy()
+    nan = np.isnan(a)
+    out[nan] = np.nan
+    return out
+
+
+def _shift(x: np.ndarray, dy: int, dx: int) -> np.ndarray:
+    """x[n, y + dy, x + dx, c] with zeros outside the image."""
+    n, h, w, c = x.shape
+    out = np.zeros_like(x)
+    ys, ye = max(0, -dy), min(h, h - dy)
+    xs, xe = max(0, -dx), min(w, w - dx)
+    if ys < ye and xs < xe:
+        out[:, ys:ye, xs:xe, :] = x[:, ys + dy:ye + dy, xs + dx:xe + dx, :]
+    return out
+
+
+def conv3x3(x, w, bias=None, relu=False, mask=None) -> np.ndarray:
+    """y[p][co] = act(bias[co] + sum_{t,ci} x[p + off(t)][ci] * w[co][t][ci]); x [n,h,w,cin], w [cout,9,cin].
+    mask (same shape as y): y *= (mask > 0)."""
+    x = np.asarray(x, np.float64)
+    w = np.asarray(w, np.float64)
+    n, h, wd, cin = x.shape
+    cout = w.shape[0]
+    y = np.zeros((n, h, wd, cout))
+    for t in range(9):
+        y += _shift(x, t // 3 - 1, t % 3 - 1) @ w[:, t, :].T
+    if bias is not None:
+        y += np.asarray(bias, np.float64)
+    if relu:
+        y = np.maximum(y, 0.0)
+    if mask is not None:
+        y = np.where(np.asarray(mask) > 0, y, 0.0)
+    return y
+
+
+def rotate_weights(w) -> np.ndarray:
+    """wrot[ci][t][co] = w[co][8 - t][ci]."""
+    w = np.asarray(w)
+    return np.ascontiguousarray(w[:, ::-1, :].transpose(2, 1, 0))
+
+
+def conv3x3_input_grad(dy, w, mask=None) -> np.ndarray:
+    """dx[p][ci] = sum_{t,co} dy[p - off(t)][co] * w[co][t][ci], optionally times (mask > 0)."""
+    return conv3x3(dy, rotate_weights(w), mask=mask)
+
+
+def conv3x3_weight_grad(x, dy) -> np.ndarray:
+    """dw[co][t][ci] = sum_p dy[p][co] * x[p + off(t)][ci]."""
+    x = np.asarray(x, np.float64)
+    dy = np.asarray(dy, np.float64)
+    cin, cout = x.shape[-1], dy.shape[-1]
+    d2 = dy.reshape(-1, cout)
+    dw = np.zeros((cout, 9, cin))
+    for t in range(9):
+        dw[:, t, :] = d2.T @ _shift(x, t // 3 - 1, t % 3 - 1).reshape(-1, cin)
+    return dw
+
+
+def bias_grad(dy) -> np.ndarray:
+    dy = np.asarray(dy, np.float64)
+    return dy.reshape(-1, dy.shape[-1]).sum(axis=0)
+
+
+def pool2(x) -> np.ndarray:
+    x = np.asarray(x, np.float64)
+    n, h, w, c = x.shape
+    return x.reshape(n, h // 2, 2, w // 2, 2, c).mean(axis=(2, 4))
+
+
+def upcat(lo, skip) -> np.ndarray:
+    lo = np.asarray(lo, np.float64)
+    up = lo.repeat(2, axis=1).repeat(2, axis=2)
+    return np.concatenate([up, np.asarray(skip, np.float64)], axis=-1)
+
+
+def upcat_grad_lo(d, lo) -> np.ndarray:
+    """Gradient at the coarse ReLU output lo: (lo > 0) * 2x2 sum of d[..., :ca]."""
+    lo = np.asarray(lo)
+    n, h2, w2, ca = lo.shape
+    s = np.asarray(d, np.float64)[..., :ca].reshape(n, h2, 2, w2, 2, ca).sum(axis=(2, 4))
+    return np.where(lo > 0, s, 0.0)
+
+
+def encoder_grad(d_cat, cat_off, d_pool, e) -> np.ndarray:
+    """(e > 0) * (d_cat[..., cat_off:cat_off + c] + upsampled d_pool / 4)."""
+    e = np.asarray(e)
+    c = e.shape[-1]
+    acc = np.zeros(e.shape)
+    if d_cat is not None:
+        acc += np.asarray(d_cat, np.float64)[..., cat_off:cat_off + c]
+    if d_pool is not None:
+        acc += 0.25 * np.asarray(d_pool, np.float64).repeat(2, axis=1).repeat(2, axis=2)
+    return np.where(e > 0, acc, 0.0)
+
+
+def pack_input(radiance, albedo=None, normal=None, depth=None, transmittance=None) -> np.ndarray:
+    """Network input [n,h,w,16]: log1p(max(radiance, 0)) 3, albedo 3, normal 3, depth 1,
+    transmittance 1, zeros 5 (planes [n][c][h][w])."""
+    r = np.asarray(radiance, np.float32)
+    n, _, h, w = r.shape
+    out = np.zeros((n, h, w, 16), np.float32)
+    out[..., 0:3] = np.log1p(np.maximum(r, 0)).transpose(0, 2, 3, 1)
+    if albedo is not None:
+        out[..., 3:6] = np.asarray(albedo, np.float32).transpose(0, 2, 3, 1)
+    if normal is not None:
+        out[..., 6:9] = np.asarray(normal, np.float32).transpose(0, 2, 3, 1)
+    if depth is not None:
+        out[..., 9] = np.asarray(depth, np.float32)
+    if transmittance is not None:
+        out[..., 10] = np.asarray(transmittance, np.float32)
+    return out
+
+
+def kpn_head(logits, x, target=None, eps=1e-2):
+    """Softmax over the 25 logits of each pixel (channels 0..24 of logits [n,h,w,32]), 5x5 kernel
+    applied to x [n,3,h,w] with taps outside the image skipped; with a target, the relative MSE
+    loss sum (d - t)^2 / (t^2 + eps) / count and its gradient with respect to the logits.
+    Returns (d, loss, dlogits)."""
+    lg = np.asarray(logits, np.float64)[..., :25]
+    x = np.asarray(x, np.float64)
+    n, _, h, w = x.shape
+    s = np.exp(lg - lg.max(axis=-1, keepdims=True))
+    s /= s.sum(axis=-1, keepdims=True)
+    xs = []  # x at each tap, [n,3,h,w], zero outside
+    for j in range(25):
+        dy, dx = j // 5 - 2, j % 5 - 2
+        xs.append(_shift(x.transpose(0, 2, 3, 1), dy, dx).transpose(0, 3, 1, 2))
+    xs = np.stack(xs, axis=-1)  # [n,3,h,w,25]
+    d = (xs * s[:, None, :, :, :]).sum(axis=-1)
+    if target is None:
+        return d, None, None
+    t = np.asarray(target, np.float64)
+    count = d.size
+    den = t * t + eps
+    loss = float(((d - t) ** 2 / den).sum() / count)
+    g = 2.0 * (d - t) / den / count  # [n,3,h,w]
+    gx = (g[..., None] * xs).sum(axis=1)  # [n,h,w,25]
+    gd = (g * d).sum(axis=1)[..., None]
+    dl = np.zeros(np.asarray(logits).shape)
+    dl[..., :25] = s * (gx - gd)
+    return d, loss, dl
+
+
+def adam(param, m1, m2, grad, step, lr=1e-4, beta1=0.9, beta2=0.999, eps=1e-8):
+    """One Adam step; returns (param, m1, m2)."""
+    m1 = beta1 * m1 + (1 - beta1) * grad
+    m2 = beta2 * m2 + (1 - beta2) * grad * grad
+    mhat = m1 / (1 - beta1 ** step)
+    vhat = m2 / (1 - beta2 ** step)
+    return param - lr * mhat / (np.sqrt(vhat) + eps), m1, m2
