@@ -126,8 +126,8 @@ SIGNATURES = {
     "vpt_unet_adam": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, ctypes.c_long, c_float, c_float,
                               c_float, c_float, c_int, c_float, c_void_p]),
     "vpt_unet_to_bf16": (c_int, [c_void_p, c_void_p, ctypes.c_long, c_void_p]),
-    "vpt_unet_pack_input": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int, c_int,
-                                    c_void_p]),
+    "vpt_unet_pack_input": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int,
+                                    c_int, c_int, c_void_p]),
     "vpt_unet_head_blocks": (c_int, [c_int, c_int, c_int]),
     "vpt_unet_kpn_head": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int, c_int,
                                   c_float, c_void_p]),

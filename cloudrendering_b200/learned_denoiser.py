@@ -1,0 +1,471 @@
+"""Learned kernel-predicting denoiser, trained and run on the GPU by this package's own kernels.
+
+The reference's learned path (src/Denoiser/PyTorchDenoiser.cpp:637-800) loads a TorchScript model
+and a ``model_info.json`` and runs it through libtorch; it has no network and no training code of its
+own.  Here the network is a 5-level U-Net of 3x3 convolutions (widths 32-64-96-128-160 by default,
+2x2 average pooling down, nearest upsampling + skip concatenation up, ReLU) whose head predicts a
+5x5 kernel per pixel (25 logits, softmaxed); the kernel is applied to the noisy radiance
+(perPixelKernelCuda semantics, modules/kpn_module/src/Kernel.cu:38-135).  Every convolution,
+forward and backward, runs on the tcgen05 tensor cores (csrc/vpt_unet.cu); torch only allocates
+device memory and orders the launches on its current stream.
+
+Training pairs come from the tracer itself: a noisy render of a seeded cloud scene at a few sample
+counts (radiance plus albedo / normal / depth / primary-ray transmittance features averaged over the
+same frames) against a many-sample render of the same scene from a disjoint frame range.  The loss
+is the relative MSE sum (d - t)^2 / (t^2 + 0.01) / count the evaluation uses.
+
+Parameters are saved as ``<dir>/weights.npz`` (fp32) with ``<dir>/model_info.json`` in the
+reference's key style (``input_feature_maps``, ``blend``, ...; see load()).
+"""
+from __future__ import annotations
+
+import ctypes
+import json
+import math
+import os
+import time
+from typing import Dict, List, Optional, Sequence
+
+import numpy as np
+import torch
+
+from . import _lib
+
+WIDTHS = (32, 64, 96, 128, 160)
+IN_CHANNELS = 16
+HEAD_CHANNELS = 32
+KERNEL_SIZE = 5
+LOSS_EPS = 1e-2
+# feature maps the network reads (names of VolumetricPathTracingPass.hpp:74-80, plus the 2D
+# primary-ray transmittance of this package)
+INPUT_FEATURE_MAPS = ["Result", "Albedo", "Normal", "Depth", "Transmittance"]
+
+
+def _p(t: Optional[torch.Tensor], offset_elems: int = 0):
+    if t is None:
+        return None
+    return ctypes.c_void_p(t.data_ptr() + offset_elems * t.element_size())
+
+
+def layer_table(widths: Sequence[int]) -> List[dict]:
+    """Convolution layers in forward order: name, cin, cout, level."""
+    w = list(widths)
+    if len(w) != 5 or any(c % 16 for c in w):
+        raise ValueError("widths: five multiples of 16")
+    t = []
+    for l in range(4):
+        t.append(dict(name=f"enc{l}a", cin=IN_CHANNELS if l == 0 else w[l - 1], cout=w[l], level=l))
+        t.append(dict(name=f"enc{l}b", cin=w[l], cout=w[l], level=l))
+    t.append(dict(name="mida", cin=w[3], cout=w[4], level=4))
+    t.append(dict(name="midb", cin=w[4], cout=w[4], level=4))
+    for l in (3, 2, 1, 0):
+        t.append(dict(name=f"dec{l}a", cin=w[l + 1] + w[l], cout=w[l], level=l))
+        t.append(dict(name=f"dec{l}b", cin=w[l], cout=w[l], level=l))
+    t.append(dict(name="head", cin=w[0], cout=HEAD_CHANNELS, level=0))
+    return t
+
+
+class KpnUNet:
+    """The network, its fp32 master parameters, Adam state and activation buffers (one device)."""
+
+    def __init__(self, widths: Sequence[int] = WIDTHS, seed: int = 0, device: Optional[torch.device] = None):
+        self.lib = _lib.load()
+        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        self.widths = tuple(int(c) for c in widths)
+        self.layers = layer_table(self.widths)
+        self.by_name = {L["name"]: L for L in self.layers}
+        off = 0
+        for L in self.layers:
+            L["w_off"] = off
+            off += L["cout"] * 9 * L["cin"]
+            L["b_off"] = off
+            off += L["cout"]
+        self.count = off
+        self.param = torch.zeros(self.count, dtype=torch.float32, device=self.device)
+        self.param_bf16 = torch.zeros(self.count, dtype=torch.bfloat16, device=self.device)
+        self.m1 = torch.zeros_like(self.param)
+        self.m2 = torch.zeros_like(self.param)
+        self.grad = torch.zeros_like(self.param)
+        self.wrot = {L["name"]: torch.zeros((L["cin"], 9, L["cout"]), dtype=torch.bfloat16, device=self.device)
+                     for L in self.layers}
+        self.err = torch.zeros(1, dtype=torch.int32, device=self.device)
+        self.steps = 0
+        self._buf: Dict[str, torch.Tensor] = {}
+        self.init_parameters(seed)
+
+    # ---- parameters ----
+    def init_parameters(self, seed: int) -> None:
+        """He-normal weights (std sqrt(2 / fan_in), fan_in over the used input channels), zero
+        biases; the head starts small so the first kernels are close to a 5x5 box filter."""
+        g = np.random.default_rng(seed)
+        host = np.zeros(self.count, np.float32)
+        for L in self.layers:
+            cin_used = 12 if L["name"] == "enc0a" else L["cin"]
+            std = math.sqrt(2.0 / (9 * cin_used)) if L["name"] != "head" else 1e-3
+            w = (g.standard_normal((L["cout"], 9, L["cin"])) * std).astype(np.float32)
+            if L["name"] == "enc0a":
+                w[:, :, 12:] = 0.0
+            host[L["w_off"]:L["w_off"] + w.size] = w.reshape(-1)
+        self.set_parameters(host)
+
+    def set_parameters(self, host: np.ndarray) -> None:
+        if host.size != self.count:
+            raise ValueError(f"expected {self.count} parameters, got {host.size}")
+        self.param.copy_(torch.from_numpy(np.ascontiguousarray(host, np.float32)))
+        self._call("vpt_unet_to_bf16", _p(self.param), _p(self.param_bf16), self.count, self._stream())
+        self._rotate_all()
+
+    def parameters_host(self) -> np.ndarray:
+        return self.param.cpu().numpy()
+
+    def _rotate_all(self) -> None:
+        for L in self.layers:
+            self._call("vpt_unet_rotate_weights", _p(self.param_bf16, L["w_off"]), _p(self.wrot[L["name"]]),
+                       L["cin"], L["cout"], self._stream())
+
+    # ---- plumbing ----
+    def _stream(self):
+        return ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
+
+    def _call(self, name: str, *args) -> None:
+        st = getattr(self.lib, name)(*args)
+        if st != 0:
+            raise RuntimeError(f"{name} failed: {self.lib.vpt_status_string(st).decode()}")
+
+    def check_errors(self) -> None:
+        """Raises if a kernel's bounded wait expired since the last check."""
+        e = int(self.err.item())
+        if e:
+            self.err.zero_()
+            raise RuntimeError(f"device error in the denoiser network: {self.lib.vpt_status_string(e).decode()}")
+
+    def buf(self, name: str, shape, dtype=torch.bfloat16) -> torch.Tensor:
+        t = self._buf.get(name)
+        if t is None or tuple(t.shape) != tuple(shape) or t.dtype != dtype:
+            t = torch.empty(shape, dtype=dtype, device=self.device)
+            self._buf[name] = t
+        return t
+
+    def _conv(self, L: dict, x: torch.Tensor, out: torch.Tensor, n: int, h: int, w: int, relu: int,
+              out_f32: int = 0) -> torch.Tensor:
+        self._call("vpt_unet_conv3x3", _p(x), _p(self.param_bf16, L["w_off"]), _p(self.param, L["b_off"]), None,
+                   _p(out), n, h, w, L["cin"], L["cout"], relu, out_f32, _p(self.err), self._stream())
+        return out
+
+    def _input_grad(self, L: dict, dy: torch.Tensor, mask: Optional[torch.Tensor], out: torch.Tensor, n: int, h: int,
+                    w: int) -> torch.Tensor:
+        self._call("vpt_unet_conv3x3", _p(dy), _p(self.wrot[L["name"]]), None, _p(mask), _p(out), n, h, w,
+                   L["cout"], L["cin"], 0, 0, _p(self.err), self._stream())
+        return out
+
+    def _weight_grad(self, L: dict, x: torch.Tensor, dy: torch.Tensor, n: int, h: int, w: int) -> None:
+        P = n * h * w
+        rows = self.lib.vpt_unet_wgrad_rows(L["cin"])
+        mtiles = rows // 128
+        splits = max(1, min((P + 63) // 64, (2 * 148 + mtiles - 1) // mtiles))
+        pps = ((P + splits - 1) // splits + 63) // 64 * 64
+        splits = (P + pps - 1) // pps
+        part = self.buf("wgrad_partial", (splits * rows * L["cout"],), torch.float32)
+        self._call("vpt_unet_conv3x3_wgrad", _p(x), _p(dy), _p(part), n, h, w, L["cin"], L["cout"], pps,
+                   _p(self.err), self._stream())
+        bblocks = max(1, min(296, (P + 255) // 256))
+        bpart = self.buf("bias_partial", (bblocks * L["cout"],), torch.float32)
+        self._call("vpt_unet_bias_grad", _p(dy), _p(bpart), P, L["cout"], bblocks, self._stream())
+        self._call("vpt_unet_reduce_grads", _p(part), splits, L["cin"], L["cout"], _p(bpart), bblocks,
+                   _p(self.grad, L["w_off"]), _p(self.grad, L["b_off"]), self._stream())
+
+    # ---- network ----
+    def forward(self, x0: torch.Tensor) -> torch.Tensor:
+        """x0: packed input [n, h, w, 16] bf16 (h, w multiples of 16).  Returns the head's logits
+        [n, h, w, 32] fp32; the activations stay in this object for backward()."""
+        n, h, w, c = x0.shape
+        if c != IN_CHANNELS or h % 16 or w % 16:
+            raise ValueError("input must be [n, h, w, 16] with h, w multiples of 16")
+        self.shape = (n, h, w)
+        W = self.widths
+        dims = [(h >> l, w >> l) for l in range(5)]
+        cur = x0
+        for l in range(4):
+            hh, ww = dims[l]
+            a = self._conv(self.by_name[f"enc{l}a"], cur, self.buf(f"enc{l}a", (n, hh, ww, W[l])), n, hh, ww, 1)
+            e = self._conv(self.by_name[f"enc{l}b"], a, self.buf(f"enc{l}b", (n, hh, ww, W[l])), n, hh, ww, 1)
+            pooled = self.buf(f"pool{l}", (n, hh // 2, ww // 2, W[l]))
+            self._call("vpt_unet_pool2", _p(e), _p(pooled), n, hh, ww, W[l], self._stream())
+            cur = pooled
+        hh, ww = dims[4]
+        a = self._conv(self.by_name["mida"], cur, self.buf("mida", (n, hh, ww, W[4])), n, hh, ww, 1)
+        cur = self._conv(self.by_name["midb"], a, self.buf("midb", (n, hh, ww, W[4])), n, hh, ww, 1)
+        for l in (3, 2, 1, 0):
+            hh, ww = dims[l]
+            ca, cs = W[l + 1], W[l]
+            u = self.buf(f"cat{l}", (n, hh, ww, ca + cs))
+            self._call("vpt_unet_upcat", _p(cur), _p(self._buf[f"enc{l}b"]), _p(u), n, hh, ww, ca, cs, self._stream())
+            a = self._conv(self.by_name[f"dec{l}a"], u, self.buf(f"dec{l}a", (n, hh, ww, W[l])), n, hh, ww, 1)
+            cur = self._conv(self.by_name[f"dec{l}b"], a, self.buf(f"dec{l}b", (n, hh, ww, W[l])), n, hh, ww, 1)
+        hh, ww = dims[0]
+        self._x0 = x0
+        return self._conv(self.by_name["head"], cur, self.buf("logits", (n, hh, ww, HEAD_CHANNELS), torch.float32),
+                          n, hh, ww, 0, 1)
+
+    def backward(self, dlogits: torch.Tensor) -> None:
+        """dlogits: [n, h, w, 32] bf16 gradient of the loss at the head's output.  Fills self.grad
+        (flat, same layout as the parameters)."""
+        n, h, w = self.shape
+        W = self.widths
+        B = self._buf
+        dims = [(h >> l, w >> l) for l in range(5)]
+        hh, ww = dims[0]
+        L = self.by_name["head"]
+        self._weight_grad(L, B["dec0b"], dlogits, n, hh, ww)
+        g = self._input_grad(L, dlogits, B["dec0b"], self.buf("g0", (n, hh, ww, W[0])), n, hh, ww)
+        dcat = {}
+        for l in (0, 1, 2, 3):
+            hh, ww = dims[l]
+            Lb, La = self.by_name[f"dec{l}b"], self.by_name[f"dec{l}a"]
+            self._weight_grad(Lb, B[f"dec{l}a"], g, n, hh, ww)
+            ga = self._input_grad(Lb, g, B[f"dec{l}a"], self.buf(f"gdec{l}a", (n, hh, ww, W[l])), n, hh, ww)
+            self._weight_grad(La, B[f"cat{l}"], ga, n, hh, ww)
+            ca, cs = W[l + 1], W[l]
+            du = self._input_grad(La, ga, None, self.buf(f"gcat{l}", (n, hh, ww, ca + cs)), n, hh, ww)
+            dcat[l] = du
+            lo = B["midb"] if l == 3 else B[f"dec{l + 1}b"]
+            h2, w2 = dims[l + 1]
+            g = self.buf(f"glo{l + 1}", (n, h2, w2, ca))
+            self._call("vpt_unet_upcat_grad_lo", _p(du), _p(lo), _p(g), n, hh, ww, ca, cs, self._stream())
+        hh, ww = dims[4]
+        self._weight_grad(self.by_name["midb"], B["mida"], g, n, hh, ww)
+        ga = self._input_grad(self.by_name["midb"], g, B["mida"], self.buf("gmida", (n, hh, ww, W[4])), n, hh, ww)
+        self._weight_grad(self.by_name["mida"], B["pool3"], ga, n, hh, ww)
+        dpool = self._input_grad(self.by_name["mida"], ga, None, self.buf("gpool3", (n, hh, ww, W[3])), n, hh, ww)
+        for l in (3, 2, 1, 0):
+            hh, ww = dims[l]
+            ca, cs = W[l + 1], W[l]
+            ge = self.buf(f"genc{l}b", (n, hh, ww, W[l]))
+            self._call("vpt_unet_encoder_grad", _p(dcat[l]), ca + cs, ca, _p(dpool), _p(B[f"enc{l}b"]), _p(ge), n,
+                       hh, ww, W[l], self._stream())
+            Lb, La = self.by_name[f"enc{l}b"], self.by_name[f"enc{l}a"]
+            self._weight_grad(Lb, B[f"enc{l}a"], ge, n, hh, ww)
+            ga = self._input_grad(Lb, ge, B[f"enc{l}a"], self.buf(f"genc{l}a", (n, hh, ww, W[l])), n, hh, ww)
+            xin = self._x0 if l == 0 else B[f"pool{l - 1}"]
+            self._weight_grad(La, xin, ga, n, hh, ww)
+            if l > 0:
+                dpool = self._input_grad(La, ga, None, self.buf(f"gpool{l - 1}", (n, hh, ww, W[l - 1])), n, hh, ww)
+
+    def adam_step(self, lr: float, beta1: float = 0.9, beta2: float = 0.999, eps: float = 1e-8) -> None:
+        self.steps += 1
+        self._call("vpt_unet_adam", _p(self.param), _p(self.param_bf16), _p(self.m1), _p(self.m2), _p(self.grad),
+                   self.count, lr, beta1, beta2, eps, self.steps, 1.0, self._stream())
+        self._rotate_all()
+
+    # ---- the kernel-prediction head ----
+    def pack(self, radiance, albedo=None, normal=None, depth=None, transmittance=None, noise_level=None):
+        n, _, h, w = radiance.shape
+        x0 = self.buf("input", (n, h, w, IN_CHANNELS))
+        self._call("vpt_unet_pack_input", _p(radiance), _p(albedo), _p(normal), _p(depth), _p(transmittance),
+                   _p(noise_level), _p(x0), n, h, w, self._stream())
+        return x0
+
+    def head(self, logits, radiance, target=None, out=None):
+        """Applies the predicted kernels; with a target also the loss (device scalar) and the
+        gradient at the logits (returned as (out, loss, dlogits))."""
+        n, _, h, w = radiance.shape
+        blocks = self.lib.vpt_unet_head_blocks(n, h, w)
+        dl = lp = None
+        if target is not None:
+            dl = self.buf("dlogits", (n, h, w, HEAD_CHANNELS))
+            lp = self.buf("loss_partial", (blocks,), torch.float32)
+        self._call("vpt_unet_kpn_head", _p(logits), _p(radiance), _p(target), _p(out), _p(dl), _p(lp), n, h, w,
+                   LOSS_EPS, self._stream())
+        return out, (lp.sum() if lp is not None else None), dl
+
+    def train_step(self, batch: dict, lr: float) -> torch.Tensor:
+        x0 = self.pack(batch["radiance"], batch.get("albedo"), batch.get("normal"), batch.get("depth"),
+                       batch.get("transmittance"), batch.get("noise_level"))
+        logits = self.forward(x0)
+        _, loss, dl = self.head(logits, batch["radiance"], batch["target"])
+        self.backward(dl)
+        self.adam_step(lr)
+        return loss
+
+    def denoise(self, radiance, albedo=None, normal=None, depth=None, transmittance=None, noise_level=None):
+        """Denoised radiance [n, 3, h, w] fp32 (h, w multiples of 16)."""
+        x0 = self.pack(radiance, albedo, normal, depth, transmittance, noise_level)
+        logits = self.forward(x0)
+        out = torch.empty_like(radiance)
+        self.head(logits, radiance, None, out)
+        return out
+
+    # ---- the model contract ----
+    def save(self, directory: str) -> None:
+        os.makedirs(directory, exist_ok=True)
+        np.savez(os.path.join(directory, "weights.npz"), params=self.parameters_host())
+        info = {"input_feature_maps": INPUT_FEATURE_MAPS, "blend": "kpn", "kernel_size": KERNEL_SIZE,
+                "use_previous_frame": False, "use_batch_dimension": True, "use_fp16": False,
+                "network": "unet", "widths": list(self.widths), "input_channels": IN_CHANNELS,
+                "head_channels": HEAD_CHANNELS, "loss": "relmse", "loss_eps": LOSS_EPS, "steps": self.steps}
+        with open(os.path.join(directory, "model_info.json"), "w") as f:
+            json.dump(info, f, indent=1)
+
+    @classmethod
+    def load(cls, directory: str, device=None) -> "KpnUNet":
+        with open(os.path.join(directory, "model_info.json")) as f:
+            info = json.load(f)
+        if info.get("network") != "unet" or info.get("blend") != "kpn":
+            raise RuntimeError(f"unsupported model_info.json in {directory}: network {info.get('network')}, "
+                               f"blend {info.get('blend')}")
+        net = cls(info["widths"], device=device)
+        net.set_parameters(np.load(os.path.join(directory, "weights.npz"))["params"])
+        net.steps = int(info.get("steps", 0))
+        return net
+
+
+# ---------------------------------------------------------------------------------------------
+# training pairs from the tracer
+# ---------------------------------------------------------------------------------------------
+def relmse(x: torch.Tensor, ref: torch.Tensor, eps: float = LOSS_EPS) -> float:
+    """mean over pixels and channels of (x - ref)^2 / (ref^2 + eps)."""
+    x = x.double()
+    ref = ref.double()
+    return float(((x - ref) ** 2 / (ref * ref + eps)).mean())
+
+
+def sample_scene(seed: int) -> dict:
+    """A seeded cloud scene of the training / evaluation family (fBm cloud, sun + constant sky)."""
+    g = np.random.default_rng(seed)
+    sun = g.normal(size=3)
+    sun[1] = abs(sun[1]) + 0.5
+    a = g.uniform(0, 2 * math.pi)
+    elev = g.uniform(-0.2, 0.8)
+    return dict(seed=int(seed), extinction=float(math.exp(g.uniform(math.log(100.0), math.log(1000.0)))),
+                g=float(g.uniform(0.6, 0.9)), sun=(sun / np.linalg.norm(sun)).tolist(),
+                camera=[2.0 * math.sin(a), elev, 2.0 * math.cos(a)], threshold=float(g.uniform(0.25, 0.4)))
+
+
+def setup_scene(vpt, sc: dict, grid: int = 128, max_bounces: int = 64) -> None:
+    vpt.set_max_grid_extent(0.5)
+    vpt.generate_fbm_cloud(grid, seed=sc["seed"], threshold=sc["threshold"])
+    vpt.set_extinction_scale(sc["extinction"])
+    vpt.set_scattering_albedo([0.99, 0.99, 0.99])
+    vpt.set_phase_g(sc["g"])
+    vpt.set_use_builtin_environment_map("Constant Sky + Sun")
+    vpt.set_sky_color([0.2, 0.2, 0.2])
+    vpt.set_sun(sc["sun"], [5.0, 5.0, 5.0])
+    vpt.set_camera_position(sc["camera"])
+    vpt.set_camera_target([0.0, 0.0, 0.0])
+    vpt.set_camera_fovy(60.0)
+    vpt.set_max_bounces(max_bounces)
+    vpt.set_grid_interpolation("Stochastic")
+    vpt.set_denoiser("None")
+    vpt.set_vpt_mode_from_name("Delta Tracking")
+
+
+def read_features(vpt, img: torch.Tensor) -> dict:
+    """Feature planes of the current accumulation: albedo [3], normal [3], depth [1], transmittance [1]."""
+    return {"albedo": vpt.get_feature_map_from_string(img, "Albedo")[:3].contiguous(),
+            "normal": vpt.get_feature_map_from_string(img, "Normal")[:3].contiguous(),
+            "depth": vpt.get_feature_map_from_string(img, "Depth")[:1].contiguous(),
+            "transmittance": vpt.get_feature_map_from_string(img, "Transmittance")[:1].contiguous()}
+
+
+TARGET_FRAME_ORIGIN = 1 << 24  # targets use frames disjoint from the noisy inputs'
+
+
+def render_scene_levels(vpt, sc: dict, size: int, spp_levels: Sequence[int], target_spp: int, grid: int = 128,
+                        max_bounces: int = 64) -> dict:
+    """Noisy renders of one scene after each sample count in spp_levels (nested: the frames of a
+    level include the previous level's) with their features, and the target (target_spp frames
+    from a disjoint frame range), all on the GPU."""
+    setup_scene(vpt, sc, grid, max_bounces)
+    vpt.set_use_feature_maps(["Albedo", "Normal", "Depth", "Transmittance"])
+    img = torch.zeros((3, size, size), dtype=torch.float32, device="cuda")
+    vpt.set_frame_index(0)
+    levels = []
+    done = 0
+    for spp in spp_levels:
+        rad = vpt.render_frame(img, spp - done).clone()
+        done = spp
+        levels.append(dict(spp=spp, radiance=rad, **read_features(vpt, img)))
+    vpt.set_use_feature_maps([])
+    vpt.set_frame_index(TARGET_FRAME_ORIGIN)
+    left = target_spp
+    tgt = None
+    while left > 0:
+        k = min(left, 256)
+        tgt = vpt.render_frame(img, k)
+        left -= k
+    target = tgt.clone()
+    vpt.set_frame_index(0)
+    return dict(levels=levels, target=target)
+
+
+class TrainingSet:
+    """Tracer-generated training pairs held on the GPU: for each scene and sample count, the noisy
+    radiance and features, and the scene's target."""
+
+    def __init__(self, vpt, num_scenes: int, size: int = 256, spp_levels=(1, 4, 16, 64), target_spp: int = 1024,
+                 seed0: int = 1000, grid: int = 128):
+        t0 = time.perf_counter()
+        self.size = size
+        self.spp_levels = tuple(spp_levels)
+        S, L = num_scenes, len(self.spp_levels)
+        dev = torch.device("cuda")
+        self.radiance = torch.empty((S, L, 3, size, size), device=dev)
+        self.albedo = torch.empty((S, L, 3, size, size), device=dev)
+        self.normal = torch.empty((S, L, 3, size, size), device=dev)
+        self.depth = torch.empty((S, L, 1, size, size), device=dev)
+        self.transmittance = torch.empty((S, L, 1, size, size), device=dev)
+        self.target = torch.empty((S, 3, size, size), device=dev)
+        for s in range(S):
+            r = render_scene_levels(vpt, sample_scene(seed0 + s), size, self.spp_levels, target_spp, grid)
+            for j, lv in enumerate(r["levels"]):
+                self.radiance[s, j] = lv["radiance"]
+                self.albedo[s, j] = lv["albedo"]
+                self.normal[s, j] = lv["normal"]
+                self.depth[s, j] = lv["depth"]
+                self.transmittance[s, j] = lv["transmittance"]
+            self.target[s] = r["target"]
+        torch.cuda.synchronize()
+        self.seconds = time.perf_counter() - t0
+        self.paths = S * size * size * (max(self.spp_levels) + target_spp)
+
+    def batch(self, rng: np.random.Generator, batch_size: int) -> dict:
+        """A random batch of (scene, sample count) pairs with random flips / transposes."""
+        S, L = self.radiance.shape[:2]
+        si = torch.from_numpy(rng.integers(0, S, batch_size)).cuda()
+        li = torch.from_numpy(rng.integers(0, L, batch_size)).cuda()
+        out = {k: getattr(self, k)[si, li] for k in ("radiance", "albedo", "normal", "depth", "transmittance")}
+        out["target"] = self.target[si]
+        out["noise_level"] = (1.0 / torch.tensor(self.spp_levels, dtype=torch.float32, device="cuda")[li].sqrt())
+        flip = rng.integers(0, 8)
+        for k in ("radiance", "albedo", "normal", "depth", "transmittance", "target"):
+            t = out[k]
+            if flip & 1:
+                t = t.flip(-1)
+            if flip & 2:
+                t = t.flip(-2)
+            if flip & 4:
+                t = t.transpose(-1, -2)
+            out[k] = t.contiguous()
+        for k in ("depth", "transmittance"):
+            out[k] = out[k][:, 0].contiguous()
+        return out
+
+
+def train(net: KpnUNet, data: TrainingSet, steps: int, batch_size: int = 8, lr: float = 1e-4, seed: int = 0,
+          log_every: int = 0) -> dict:
+    """Adam training; returns timing and the loss curve (mean loss per logging window)."""
+    rng = np.random.default_rng(seed)
+    losses = []
+    acc = torch.zeros((), dtype=torch.float32, device=net.device)
+    window = max(1, log_every or steps // 10)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for i in range(steps):
+        loss = net.train_step(data.batch(rng, batch_size), lr)
+        acc += loss
+        if (i + 1) % window == 0:
+            losses.append(float(acc.item()) / window)
+            acc.zero_()
+    torch.cuda.synchronize()
+    net.check_errors()
+    return {"steps": steps, "seconds": time.perf_counter() - t0, "loss_curve": losses}

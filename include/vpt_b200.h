@@ -384,9 +384,10 @@ VptStatus vpt_unet_adam(float* param, void* param_bf16, float* m1, float* m2, co
                         float beta1, float beta2, float eps, int step, float grad_scale, void* stream);
 VptStatus vpt_unet_to_bf16(const float* in, void* out, long count, void* stream);
 /* network input [n][h][w][16] bf16 from planes [n][c][h][w]: log1p(radiance) 3, albedo 3, normal 3,
- * depth 1, transmittance 1 (NULL planes give zeros) */
+ * depth 1, transmittance 1, and noise_level[n] (1/sqrt(frames) per image) 1 (NULL gives zeros) */
 VptStatus vpt_unet_pack_input(const float* radiance, const float* albedo, const float* normal, const float* depth,
-                              const float* transmittance, void* out, int n, int h, int w, void* stream);
+                              const float* transmittance, const float* noise_level, void* out, int n, int h, int w,
+                              void* stream);
 int vpt_unet_head_blocks(int n, int h, int w);
 /* Kernel-prediction head (perPixelKernelCuda semantics, modules/kpn_module/src/Kernel.cu:38-135, with
  * the tap softmax fused): out[n][c][y][x] = sum_j softmax(logits[p][0..24])_j radiance[n][c][y+dy][x+dx]

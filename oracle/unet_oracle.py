@@ -120,9 +120,9 @@ def encoder_grad(d_cat, cat_off, d_pool, e) -> np.ndarray:
     return np.where(e > 0, acc, 0.0)
 
 
-def pack_input(radiance, albedo=None, normal=None, depth=None, transmittance=None) -> np.ndarray:
+def pack_input(radiance, albedo=None, normal=None, depth=None, transmittance=None, noise_level=None) -> np.ndarray:
     """Network input [n,h,w,16]: log1p(max(radiance, 0)) 3, albedo 3, normal 3, depth 1,
-    transmittance 1, zeros 5 (planes [n][c][h][w])."""
+    transmittance 1, noise level (per image) 1, zeros 4 (planes [n][c][h][w])."""
     r = np.asarray(radiance, np.float32)
     n, _, h, w = r.shape
     out = np.zeros((n, h, w, 16), np.float32)
@@ -135,6 +135,8 @@ def pack_input(radiance, albedo=None, normal=None, depth=None, transmittance=Non
         out[..., 9] = np.asarray(depth, np.float32)
     if transmittance is not None:
         out[..., 10] = np.asarray(transmittance, np.float32)
+    if noise_level is not None:
+        out[..., 11] = np.asarray(noise_level, np.float32)[:, None, None]
     return out
 
 
@@ -175,3 +177,92 @@ def adam(param, m1, m2, grad, step, lr=1e-4, beta1=0.9, beta2=0.999, eps=1e-8):
     mhat = m1 / (1 - beta1 ** step)
     vhat = m2 / (1 - beta2 ** step)
     return param - lr * mhat / (np.sqrt(vhat) + eps), m1, m2
+
+
+# ---------------------------------------------------------------------------------------------
+# the whole network (cloudrendering_b200/learned_denoiser.py: KpnUNet.forward / backward)
+# ---------------------------------------------------------------------------------------------
+def layer_table(widths):
+    w = list(widths)
+    t = []
+    for l in range(4):
+        t.append((f"enc{l}a", 16 if l == 0 else w[l - 1], w[l]))
+        t.append((f"enc{l}b", w[l], w[l]))
+    t.append(("mida", w[3], w[4]))
+    t.append(("midb", w[4], w[4]))
+    for l in (3, 2, 1, 0):
+        t.append((f"dec{l}a", w[l + 1] + w[l], w[l]))
+        t.append((f"dec{l}b", w[l], w[l]))
+    t.append(("head", w[0], 32))
+    return t
+
+
+def split_params(flat, widths):
+    """Flat parameter vector -> {name: (w [cout][9][cin], b [cout])} (weights then bias per layer)."""
+    out, off = {}, 0
+    for name, cin, cout in layer_table(widths):
+        w = np.asarray(flat[off:off + cout * 9 * cin]).reshape(cout, 9, cin)
+        off += cout * 9 * cin
+        out[name] = (w, np.asarray(flat[off:off + cout]))
+        off += cout
+    return out
+
+
+def network_loss_and_grad(flat, widths, x0, radiance, target, round_bf16=True, eps=1e-2):
+    """Forward, relative-MSE loss of the kernel head and the gradient with respect to every
+    parameter (flat, same layout).  With round_bf16 the weights, activations and backward
+    gradients are rounded to bf16 where the GPU stores them in bf16; without, all float64."""
+    rnd = (lambda a: bf16(np.asarray(a, np.float32)).astype(np.float64)) if round_bf16 else (lambda a: a)
+    P = split_params(flat, widths)
+    Wt = {k: rnd(v[0]) for k, v in P.items()}
+    Bs = {k: np.asarray(v[1], np.float64) for k, v in P.items()}
+    A = {}
+    cur = rnd(x0)
+    for l in range(4):
+        A[f"in{l}"] = cur
+        A[f"enc{l}a"] = rnd(conv3x3(cur, Wt[f"enc{l}a"], Bs[f"enc{l}a"], relu=True))
+        A[f"enc{l}b"] = rnd(conv3x3(A[f"enc{l}a"], Wt[f"enc{l}b"], Bs[f"enc{l}b"], relu=True))
+        cur = rnd(pool2(A[f"enc{l}b"]))
+    A["in4"] = cur
+    A["mida"] = rnd(conv3x3(cur, Wt["mida"], Bs["mida"], relu=True))
+    cur = A["midb"] = rnd(conv3x3(A["mida"], Wt["midb"], Bs["midb"], relu=True))
+    for l in (3, 2, 1, 0):
+        A[f"cat{l}"] = upcat(cur, A[f"enc{l}b"])
+        A[f"dec{l}a"] = rnd(conv3x3(A[f"cat{l}"], Wt[f"dec{l}a"], Bs[f"dec{l}a"], relu=True))
+        cur = A[f"dec{l}b"] = rnd(conv3x3(A[f"dec{l}a"], Wt[f"dec{l}b"], Bs[f"dec{l}b"], relu=True))
+    logits = conv3x3(cur, Wt["head"], Bs["head"])
+    if round_bf16:
+        logits = logits.astype(np.float32).astype(np.float64)
+    d, loss, dl = kpn_head(logits, radiance, target, eps)
+    G = {}
+
+    def grads(name, x, dy):
+        G[name] = (conv3x3_weight_grad(x, dy), bias_grad(dy))
+
+    g = rnd(dl)
+    grads("head", A["dec0b"], g)
+    g = rnd(conv3x3_input_grad(g, Wt["head"], mask=A["dec0b"]))
+    dcat = {}
+    for l in (0, 1, 2, 3):
+        grads(f"dec{l}b", A[f"dec{l}a"], g)
+        ga = rnd(conv3x3_input_grad(g, Wt[f"dec{l}b"], mask=A[f"dec{l}a"]))
+        grads(f"dec{l}a", A[f"cat{l}"], ga)
+        dcat[l] = rnd(conv3x3_input_grad(ga, Wt[f"dec{l}a"]))
+        lo = A["midb"] if l == 3 else A[f"dec{l + 1}b"]
+        g = rnd(upcat_grad_lo(dcat[l], lo))
+    grads("midb", A["mida"], g)
+    ga = rnd(conv3x3_input_grad(g, Wt["midb"], mask=A["mida"]))
+    grads("mida", A["in4"], ga)
+    dpool = rnd(conv3x3_input_grad(ga, Wt["mida"]))
+    w = list(widths)
+    for l in (3, 2, 1, 0):
+        ge = rnd(encoder_grad(dcat[l], w[l + 1], dpool, A[f"enc{l}b"]))
+        grads(f"enc{l}b", A[f"enc{l}a"], ge)
+        ga = rnd(conv3x3_input_grad(ge, Wt[f"enc{l}b"], mask=A[f"enc{l}a"]))
+        grads(f"enc{l}a", A[f"in{l}"], ga)
+        if l > 0:
+            dpool = rnd(conv3x3_input_grad(ga, Wt[f"enc{l}a"]))
+    flat_g = []
+    for name, _, _ in layer_table(widths):
+        flat_g += [G[name][0].reshape(-1), G[name][1]]
+    return loss, np.concatenate(flat_g), logits, d

@@ -183,11 +183,12 @@ def test_pack_input_and_kpn_head(lib):
     nrm = g.standard_normal((n, 3, h, w)).astype(np.float32)
     dep = g.random((n, h, w)).astype(np.float32)
     trn = g.random((n, h, w)).astype(np.float32)
+    noise = np.array([1.0, 0.125], np.float32)
     packed = torch.empty((n, h, w, 16), dtype=torch.bfloat16, device="cuda")
-    t = [dev_f32(a) for a in (rad, alb, nrm, dep, trn)]
+    t = [dev_f32(a) for a in (rad, alb, nrm, dep, trn, noise)]
     assert lib.vpt_unet_pack_input(*[ptr(a) for a in t], ptr(packed), n, h, w, None) == 0
     torch.cuda.synchronize()
-    ref = uo.pack_input(rad, alb, nrm, dep, trn)
+    ref = uo.pack_input(rad, alb, nrm, dep, trn, noise)
     close_bf16(host(packed), ref.astype(np.float64))
 
     logits = rng_data(15, n, h, w, 32, scale=2.0)
@@ -218,7 +219,9 @@ def test_adam(lib):
                              ctypes.c_float(0.9), ctypes.c_float(0.999), ctypes.c_float(1e-8), 7, ctypes.c_float(1.0),
                              None) == 0
     torch.cuda.synchronize()
-    rp, rm1, rm2 = uo.adam(*(a.astype(np.float64) for a in (p, m1, m2, gr)), 7, lr=1e-3)
+    f32 = lambda v: float(np.float32(v))  # the kernel receives float hyperparameters
+    rp, rm1, rm2 = uo.adam(*(a.astype(np.float64) for a in (p, m1, m2, gr)), 7, lr=f32(1e-3), beta1=f32(0.9),
+                           beta2=f32(0.999), eps=f32(1e-8))
     # fp32 arithmetic: a few ulps of each value's scale
     for got, ref in ((host(tp), rp), (host(tm1), rm1), (host(tm2), rm2)):
         assert np.all(np.abs(got - ref) <= 1e-6 * (np.abs(ref) + np.abs(ref).max() * 1e-3))

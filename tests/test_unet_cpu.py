@@ -102,3 +102,33 @@ def test_adam_matches_torch():
         opt.step()
         p, m1, m2 = uo.adam(p, m1, m2, gr, step, lr=1e-3)
     assert np.allclose(p, tp.detach().numpy(), rtol=1e-12, atol=1e-14)
+
+
+def test_oracle_network_gradient_matches_finite_differences():
+    """The oracle's whole-network backward (float64, no rounding) against central differences of
+    its own forward loss."""
+    widths = (16, 16, 16, 16, 32)
+    g = np.random.default_rng(5)
+    table = uo.layer_table(widths)
+    flat = []
+    for name, cin, cout in table:
+        flat += [g.standard_normal(cout * 9 * cin) * np.sqrt(2.0 / (9 * cin)) * (0.3 if name == "head" else 1.0),
+                 g.standard_normal(cout) * 0.05]
+    flat = np.concatenate(flat)
+    n, h, w = 1, 16, 16
+    x0 = np.zeros((n, h, w, 16))
+    x0[..., :12] = g.standard_normal((n, h, w, 12))
+    rad = g.exponential(1.0, (n, 3, h, w))
+    tgt = g.exponential(1.0, (n, 3, h, w))
+    loss, grad, _, _ = uo.network_loss_and_grad(flat, widths, x0, rad, tgt, round_bf16=False)
+    # indices spread over all layers (weights and biases)
+    idx = np.unique(g.integers(0, flat.size, 40))
+    hstep = 1e-6
+    for i in idx:
+        fp, fm = flat.copy(), flat.copy()
+        fp[i] += hstep
+        fm[i] -= hstep
+        lp = uo.network_loss_and_grad(fp, widths, x0, rad, tgt, round_bf16=False)[0]
+        lm = uo.network_loss_and_grad(fm, widths, x0, rad, tgt, round_bf16=False)[0]
+        fd = (lp - lm) / (2 * hstep)
+        assert abs(fd - grad[i]) <= 1e-5 * (abs(fd) + np.abs(grad).max() * 1e-3), (i, fd, grad[i])
