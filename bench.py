@@ -41,6 +41,16 @@ TRACKERS = {"delta": 0, "ratio": 2, "decomposition": 3, "residual_ratio": 4, "ne
 BYTES_PER_LOOKUP = 32  # one 32-byte sector per uncoalesced density gather
 
 
+def tensor_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["bf16_tflops"]), "measured cuBLAS bf16 burst"
+    except (OSError, KeyError, ValueError):
+        return 1590.0, "fallback"
+
+
 def peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -278,6 +288,9 @@ def run_ours(args):
     batch = None
     if not args.no_batch:
         batch = run_batch(lib, stream, ctypes_stream, barrier, max_over_ranks, world)
+    learned = None
+    if not args.no_learned:
+        learned = run_learned(vpt, lib, ctx, args.workload == "small")
 
     if rank == 0:
         line = {
@@ -298,11 +311,179 @@ def run_ours(args):
             line["sparse_nanovdb"] = sparse
         if batch is not None:
             line["batched_scenes"] = batch
+        if learned is not None:
+            line["learned_denoiser"] = learned
         print(json.dumps(line), flush=True)
     vpt.cleanup()
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+# Learned denoiser: a kernel-predicting U-Net (widths 32-64-96-128-160, 13x13 kernels) trained on the
+# GPU by this package's tcgen05 kernels on tracer-generated pairs (32 seeded cloud scenes at 256^2:
+# noisy renders at 1..256 spp with albedo / normal / depth / transmittance features against
+# 2048-spp targets from disjoint frames; Adam, batch 8, 2000 steps), then the time each method needs
+# to reach relMSE <= 1e-3 on a held-out scene (256^3 cloud, 512^2, max 128 bounces) against its
+# FP64-accumulated 16384-spp render: plain accumulation, EAW (iteration count 1..5 chosen per sample
+# count by the lowest error, i.e. tuned with the reference in hand) and the learned denoiser.
+LEARNED = dict(scenes=32, size=256, spp_levels=(1, 2, 4, 8, 16, 64, 256), target_spp=2048, steps=2000, batch=8,
+               lr=3e-4, kernel_size=13, grid=128)
+EVAL = dict(seed=77777, res=512, grid=256, max_bounces=128, ref_spp=16384,
+            levels=(1, 2, 4, 8, 16, 32, 64, 128, 256, 512, 1024, 2048, 4096), target=1e-3)
+
+
+def time_to_target(spp, err, time_of, target, extrapolate):
+    """Samples and time at which err(spp) first reaches target (log-log interpolation between the
+    bracketing levels); for unbiased accumulation beyond the last level, err ~ 1/spp."""
+    for i, (n, r) in enumerate(zip(spp, err)):
+        if r <= target:
+            if i == 0:
+                ns = float(n)
+            else:
+                n0, r0 = spp[i - 1], err[i - 1]
+                t = (math.log(target) - math.log(r0)) / (math.log(r) - math.log(r0))
+                ns = math.exp(math.log(n0) + t * (math.log(n) - math.log(n0)))
+            return {"spp": ns, "ms": time_of(ns), "extrapolated": False}
+    if not extrapolate:
+        return {"spp": None, "ms": None, "extrapolated": False}
+    ns = spp[-1] * err[-1] / target
+    return {"spp": ns, "ms": time_of(ns), "extrapolated": True}
+
+
+def run_learned(vpt, lib, ctx, small):
+    import ctypes
+    import torch
+    from cloudrendering_b200 import learned_denoiser as ld
+
+    cfg, ev = dict(LEARNED), dict(EVAL)
+    if small:
+        cfg.update(scenes=8, size=128, steps=300, target_spp=512)
+        ev.update(res=256, grid=128, ref_spp=4096, levels=(1, 2, 4, 8, 16, 32, 64, 128, 256, 512))
+    stream = torch.cuda.current_stream()
+    cs = ctypes.c_void_p(stream.cuda_stream)
+    data = ld.TrainingSet(vpt, cfg["scenes"], cfg["size"], cfg["spp_levels"], cfg["target_spp"], grid=cfg["grid"])
+    net = ld.KpnUNet(seed=0, kernel_size=cfg["kernel_size"])
+    # training-step throughput (convolutions forward + input gradient + weight gradient)
+    rng = np.random.default_rng(0)
+    b = data.batch(rng, cfg["batch"])
+    for _ in range(3):
+        net.train_step(b, 0.0)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    k0 = lib.vpt_kernel_launch_count()
+    e0.record(stream)
+    for _ in range(10):
+        net.train_step(b, 0.0)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    step_ms = e0.elapsed_time(e1) / 10
+    launches_per_step = (lib.vpt_kernel_launch_count() - k0) / 10
+    P0 = cfg["batch"] * cfg["size"] ** 2
+    conv_flop = sum(2 * 9 * L["cin"] * L["cout"] * (P0 >> (2 * L["level"])) * (2 if L["name"] == "enc0a" else 3)
+                    for L in net.layers)
+    net = ld.KpnUNet(seed=0, kernel_size=cfg["kernel_size"])
+    hist = ld.train(net, data, cfg["steps"], cfg["batch"], cfg["lr"], seed=1)
+
+    # held-out scene: FP64 reference, then the error curves
+    sc = ld.sample_scene(ev["seed"])
+    ld.setup_scene(vpt, sc, grid=ev["grid"], max_bounces=ev["max_bounces"])
+    R = ev["res"]
+    img = torch.zeros((3, R, R), dtype=torch.float32, device="cuda")
+
+    def frame_ms(frames):
+        vpt.render_frame(img, 2)
+        a, c = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        _lib_check(lib.vpt_render_frames(ctx, frames, cs))
+        c.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(c) / frames
+
+    def _lib_check(st):
+        vpt._lib.check(st, "render", ctx)
+
+    t_ref = time.perf_counter()
+    vpt.set_frame_index(ld.TARGET_FRAME_ORIGIN)
+    left = ev["ref_spp"]
+    while left > 0:
+        k = min(256, left)
+        vpt.render_frame(img, k)
+        left -= k
+    ref = vpt.get_film_sum(R, R).cuda() / float(ev["ref_spp"])
+    ref_s = time.perf_counter() - t_ref
+    vpt.set_frame_index(0)
+    ms_plain = frame_ms(64)
+    vpt.set_use_feature_maps(["Albedo", "Normal", "Depth", "Transmittance"])
+    vpt.set_denoiser("Edge-Avoiding À-Trous Wavelet Transform")
+    vpt.set_denoiser_property("iterations", "1")
+    ms_feat = frame_ms(64)
+    vpt.set_frame_index(0)
+
+    def timed(fn):
+        a, c = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        r = fn()
+        c.record(stream)
+        torch.cuda.synchronize()
+        return r, a.elapsed_time(c)
+
+    rows = []
+    done = 0
+    eaw_ms, net_ms = {}, []
+    for n in ev["levels"]:
+        vpt.render_frame(img, n - done)
+        done = n
+        plain = (vpt.get_film_sum(R, R).cuda() / n).float().contiguous()
+        row = {"spp": n, "plain": ld.relmse(plain, ref)}
+        best = None
+        for it in (1, 2, 3, 4, 5):
+            vpt.set_denoiser_property("iterations", str(it))
+            d, ms = timed(lambda: vpt.get_feature_map(img, 0))
+            eaw_ms.setdefault(it, []).append(ms)
+            r = ld.relmse(d, ref)
+            if best is None or r < best[0]:
+                best = (r, it)
+        row["eaw"], row["eaw_iterations"] = best
+
+        def learned_once():
+            f = ld.read_features(vpt, img)
+            return net.denoise(plain[None], f["albedo"][None], f["normal"][None], f["depth"][None],
+                               f["transmittance"][None], torch.full((1,), 1.0 / math.sqrt(n), device="cuda"))[0]
+        den, ms = timed(learned_once)
+        net_ms.append(ms)
+        row["learned"] = ld.relmse(den, ref)
+        rows.append(row)
+    vpt.set_denoiser("None")
+    vpt.set_use_feature_maps([])
+    net.check_errors()
+    spp = [r["spp"] for r in rows]
+    eaw_cost = statistics.median(sum(v) / len(v) for v in eaw_ms.values())
+    net_cost = statistics.median(net_ms)
+    plain_t = time_to_target(spp, [r["plain"] for r in rows], lambda s: s * ms_plain, ev["target"], True)
+    eaw_t = time_to_target(spp, [r["eaw"] for r in rows], lambda s: s * ms_feat + eaw_cost, ev["target"], False)
+    learned_t = time_to_target(spp, [r["learned"] for r in rows], lambda s: s * ms_feat + net_cost, ev["target"],
+                               False)
+    peak, peak_kind = tensor_peak()
+    out = {
+        "workload": (f"KPN U-Net {'-'.join(map(str, net.widths))}, {cfg['kernel_size']}x{cfg['kernel_size']} kernels, "
+                     f"trained {cfg['steps']} steps (batch {cfg['batch']} x {cfg['size']}^2, {cfg['scenes']} scenes, "
+                     f"inputs {cfg['spp_levels']} spp vs {cfg['target_spp']}-spp targets); held-out scene seed "
+                     f"{ev['seed']} {ev['grid']}^3 at {R}^2 vs its FP64 {ev['ref_spp']}-spp render"),
+        "relmse_target": ev["target"], "relmse_eps": ld.LOSS_EPS,
+        "time_to_target_ms": {"plain": plain_t, "eaw_tuned": eaw_t, "learned": learned_t},
+        "speedup_learned_vs_plain": (plain_t["ms"] / learned_t["ms"]) if learned_t["ms"] else None,
+        "speedup_learned_vs_eaw": (eaw_t["ms"] / learned_t["ms"]) if (learned_t["ms"] and eaw_t["ms"]) else None,
+        "ms_per_frame": {"plain": ms_plain, "with_features": ms_feat}, "denoise_ms": {"eaw": eaw_cost,
+                                                                                     "learned": net_cost},
+        "curve": rows, "reference_render_s": ref_s,
+        "training": {"data_s": data.seconds, "data_paths": data.paths, "train_s": hist["seconds"],
+                     "loss_curve": hist["loss_curve"], "step_ms": step_ms, "launches_per_step": launches_per_step,
+                     "conv_gflop_per_step": conv_flop / 1e9,
+                     "roofline": {"bound": "tensor", "achieved": conv_flop / (step_ms / 1e3) / 1e12, "peak": peak,
+                                  "unit": "TFLOP/s", "frac": conv_flop / (step_ms / 1e3) / 1e12 / peak,
+                                  "note": f"convolution flops of a whole training step / step time; peak {peak_kind}"}},
+    }
+    return out
 
 
 # NanoVDB sparse configuration: 2048x1024x1536 virtual voxels, 8^3 leaves with ~12% of the leaf
@@ -574,6 +755,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-sparse", action="store_true", help="skip the NanoVDB sparse configuration")
     ap.add_argument("--no-batch", action="store_true", help="skip the 64-scene batched configuration")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-denoiser configuration")
     ap.add_argument("--workload", choices=["full", "small"], default="full",
                     help="small: 384^3 grid, 512^2, 4 spp/step (for ncu captures; not a bench line)")
     args = ap.parse_args()

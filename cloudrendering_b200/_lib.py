@@ -129,8 +129,8 @@ SIGNATURES = {
     "vpt_unet_pack_input": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int,
                                     c_int, c_int, c_void_p]),
     "vpt_unet_head_blocks": (c_int, [c_int, c_int, c_int]),
-    "vpt_unet_kpn_head": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int, c_int,
-                                  c_float, c_void_p]),
+    "vpt_unet_kpn_head": (c_int, [c_void_p, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int,
+                                  c_int, c_int, c_float, c_void_p]),
 }
 
 class VptSparseInfo(ctypes.Structure):

@@ -590,8 +590,6 @@ __global__ void f32_to_bf16_kernel(const float* __restrict__ in, bf16* __restric
 // ---------------------------------------------------------------------------------------------
 constexpr int kInputChannels = 16;  // 12 used: log radiance 3, albedo 3, normal 3, depth 1, transmittance 1,
                                     // noise level 1
-constexpr int kHeadChannels = 32;   // 25 used: 5 x 5 kernel logits
-constexpr int kTaps = 25;
 
 // planes: [n][3][h][w] radiance (mean of the frames rendered so far), albedo [n][3][h][w], normal
 // [n][3][h][w], depth [n][h][w], transmittance [n][h][w] (each may be null -> zeros); noise_level
@@ -624,52 +622,42 @@ __global__ void pack_input_kernel(const float* __restrict__ radiance, const floa
     }
 }
 
-// Per-pixel 5x5 kernel application with the tap softmax fused, and (target != null) the relative
+// Per-pixel k x k kernel application with the tap softmax fused, and (target != null) the relative
 // MSE loss and its gradient with respect to the logits:
-//   s = softmax(logits[p][0..24]);  d[c][p] = sum_j s_j x[c][p + off_j]  (taps outside skipped)
+//   s = softmax(logits[p][0 .. k*k-1]);  d[c][p] = sum_j s_j x[c][p + off_j]  (taps outside skipped)
 //   loss = sum_{p,c} (d - t)^2 / (t^2 + eps) * inv_count
 //   dL/dlogit_j = s_j (g . x_j - g . d),  g_c = 2 (d_c - t_c) / (t_c^2 + eps) * inv_count
-// logits: [P][32] fp32 (NHWC, channels 25..31 unused); x, t, out: [n][3][h][w] fp32.
-__global__ void kpn_head_kernel(const float* __restrict__ logits, const float* __restrict__ x,
+// logits: [P][hc] fp32 (NHWC, hc >= k*k a multiple of 8, channels k*k.. unused, their gradient 0);
+// x, t, out: [n][3][h][w] fp32.  The softmax is recomputed per pass (no per-tap arrays in registers).
+__global__ void kpn_head_kernel(const float* __restrict__ logits, int hc, int ks, const float* __restrict__ x,
                                 const float* __restrict__ target, float* __restrict__ out, bf16* __restrict__ dlogits,
                                 float* __restrict__ loss_partial, int n, int h, int w, float eps, float inv_count) {
     const long plane = (long)h * w, total = (long)n * plane;
+    const int taps = ks * ks, rad = ks / 2;
     float local = 0.0f;
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
         const long b = i / plane, q = i % plane;
         const int y = (int)(q / w), xx = (int)(q % w);
-        float s[kTaps];
+        const float* lg = logits + i * hc;
         float mx = -INFINITY;
-        const float4* lp = reinterpret_cast<const float4*>(logits + i * kHeadChannels);
-#pragma unroll
-        for (int k = 0; k < 7; ++k) {
-            const float4 u = lp[k];
-            const float vals[4] = {u.x, u.y, u.z, u.w};
-#pragma unroll
-            for (int e = 0; e < 4; ++e)
-                if (4 * k + e < kTaps) s[4 * k + e] = vals[e];
-        }
-#pragma unroll
-        for (int j = 0; j < kTaps; ++j) mx = fmaxf(mx, s[j]);
+        for (int j = 0; j < taps; ++j) mx = fmaxf(mx, lg[j]);
         float sum = 0.0f;
-#pragma unroll
-        for (int j = 0; j < kTaps; ++j) {
-            s[j] = __expf(s[j] - mx);
-            sum += s[j];
-        }
-        const float inv = 1.0f / sum;
         float d[3] = {0.0f, 0.0f, 0.0f};
         const float* xb = x + b * 3 * plane;
-#pragma unroll
-        for (int j = 0; j < kTaps; ++j) {
-            s[j] *= inv;
-            const int yy = y + j / 5 - 2, xq = xx + j % 5 - 2;
+        for (int j = 0; j < taps; ++j) {
+            const float e = __expf(lg[j] - mx);
+            sum += e;
+            const int yy = y + j / ks - rad, xq = xx + j % ks - rad;
             if (yy < 0 || yy >= h || xq < 0 || xq >= w) continue;
             const long o = (long)yy * w + xq;
-            d[0] += s[j] * xb[o];
-            d[1] += s[j] * xb[plane + o];
-            d[2] += s[j] * xb[2 * plane + o];
+            d[0] += e * xb[o];
+            d[1] += e * xb[plane + o];
+            d[2] += e * xb[2 * plane + o];
         }
+        const float inv = 1.0f / sum;
+        d[0] *= inv;
+        d[1] *= inv;
+        d[2] *= inv;
         if (out) {
             for (int c = 0; c < 3; ++c) out[(b * 3 + c) * plane + q] = d[c];
         }
@@ -683,25 +671,24 @@ __global__ void kpn_head_kernel(const float* __restrict__ logits, const float* _
                 g[c] = 2.0f * e / den * inv_count;
             }
             const float gd = g[0] * d[0] + g[1] * d[1] + g[2] * d[2];
-            float gl[kHeadChannels];
-#pragma unroll
-            for (int j = 0; j < kHeadChannels; ++j) gl[j] = 0.0f;
-#pragma unroll
-            for (int j = 0; j < kTaps; ++j) {
-                const int yy = y + j / 5 - 2, xq = xx + j % 5 - 2;
-                float gx = 0.0f;
-                if (yy >= 0 && yy < h && xq >= 0 && xq < w) {
-                    const long o = (long)yy * w + xq;
-                    gx = g[0] * xb[o] + g[1] * xb[plane + o] + g[2] * xb[2 * plane + o];
-                }
-                gl[j] = s[j] * (gx - gd);
-            }
-#pragma unroll
-            for (int k = 0; k < kHeadChannels / 8; ++k) {
+            for (int j0 = 0; j0 < hc; j0 += 8) {
                 float f[8];
 #pragma unroll
-                for (int e = 0; e < 8; ++e) f[e] = gl[8 * k + e];
-                store8(dlogits + i * kHeadChannels + 8 * k, f);
+                for (int k = 0; k < 8; ++k) {
+                    const int j = j0 + k;
+                    f[k] = 0.0f;
+                    if (j < taps) {
+                        const float sj = __expf(lg[j] - mx) * inv;
+                        const int yy = y + j / ks - rad, xq = xx + j % ks - rad;
+                        float gx = 0.0f;
+                        if (yy >= 0 && yy < h && xq >= 0 && xq < w) {
+                            const long o = (long)yy * w + xq;
+                            gx = g[0] * xb[o] + g[1] * xb[plane + o] + g[2] * xb[2 * plane + o];
+                        }
+                        f[k] = sj * (gx - gd);
+                    }
+                }
+                store8(dlogits + i * hc + j0, f);
             }
         }
     }
@@ -916,14 +903,18 @@ VptStatus vpt_unet_pack_input(const float* radiance, const float* albedo, const 
 
 int vpt_unet_head_blocks(int n, int h, int w) { return grid_for((long)n * h * w, 256); }
 
-VptStatus vpt_unet_kpn_head(const float* logits, const float* radiance, const float* target, float* out,
-                            void* dlogits, float* loss_partial, int n, int h, int w, float eps, void* stream) {
-    if (!logits || !radiance || n <= 0 || h <= 0 || w <= 0 || (target && !dlogits) || eps <= 0.0f)
+VptStatus vpt_unet_kpn_head(const float* logits, int head_channels, int kernel_size, const float* radiance,
+                            const float* target, float* out, void* dlogits, float* loss_partial, int n, int h, int w,
+                            float eps, void* stream) {
+    if (!logits || !radiance || n <= 0 || h <= 0 || w <= 0 || (target && !dlogits) || eps <= 0.0f ||
+        kernel_size <= 0 || kernel_size % 2 == 0 || kernel_size > 15 || head_channels % 8 ||
+        head_channels < kernel_size * kernel_size)
         return VPT_ERR_ARG;
     const int blocks = grid_for((long)n * h * w, 256);
     const float inv_count = 1.0f / (3.0f * (float)n * (float)h * (float)w);
     kpn_head_kernel<<<blocks, 256, 0, static_cast<cudaStream_t>(stream)>>>(
-        logits, radiance, target, out, static_cast<bf16*>(dlogits), loss_partial, n, h, w, eps, inv_count);
+        logits, head_channels, kernel_size, radiance, target, out, static_cast<bf16*>(dlogits), loss_partial, n, h, w,
+        eps, inv_count);
     vpt::count_launches(1);
     return cudaGetLastError() == cudaSuccess ? VPT_OK : VPT_ERR_CUDA;
 }

@@ -4,7 +4,7 @@ The reference's learned path (src/Denoiser/PyTorchDenoiser.cpp:637-800) loads a 
 and a ``model_info.json`` and runs it through libtorch; it has no network and no training code of its
 own.  Here the network is a 5-level U-Net of 3x3 convolutions (widths 32-64-96-128-160 by default,
 2x2 average pooling down, nearest upsampling + skip concatenation up, ReLU) whose head predicts a
-5x5 kernel per pixel (25 logits, softmaxed); the kernel is applied to the noisy radiance
+k x k kernel per pixel (k*k logits, softmaxed; k = 13 by default); the kernel is applied to the noisy radiance
 (perPixelKernelCuda semantics, modules/kpn_module/src/Kernel.cu:38-135).  Every convolution,
 forward and backward, runs on the tcgen05 tensor cores (csrc/vpt_unet.cu); torch only allocates
 device memory and orders the launches on its current stream.
@@ -33,8 +33,7 @@ from . import _lib
 
 WIDTHS = (32, 64, 96, 128, 160)
 IN_CHANNELS = 16
-HEAD_CHANNELS = 32
-KERNEL_SIZE = 5
+KERNEL_SIZE = 13
 LOSS_EPS = 1e-2
 # feature maps the network reads (names of VolumetricPathTracingPass.hpp:74-80, plus the 2D
 # primary-ray transmittance of this package)
@@ -47,7 +46,11 @@ def _p(t: Optional[torch.Tensor], offset_elems: int = 0):
     return ctypes.c_void_p(t.data_ptr() + offset_elems * t.element_size())
 
 
-def layer_table(widths: Sequence[int]) -> List[dict]:
+def head_channels(kernel_size: int) -> int:
+    return (kernel_size * kernel_size + 15) // 16 * 16
+
+
+def layer_table(widths: Sequence[int], kernel_size: int = KERNEL_SIZE) -> List[dict]:
     """Convolution layers in forward order: name, cin, cout, level."""
     w = list(widths)
     if len(w) != 5 or any(c % 16 for c in w):
@@ -61,18 +64,23 @@ def layer_table(widths: Sequence[int]) -> List[dict]:
     for l in (3, 2, 1, 0):
         t.append(dict(name=f"dec{l}a", cin=w[l + 1] + w[l], cout=w[l], level=l))
         t.append(dict(name=f"dec{l}b", cin=w[l], cout=w[l], level=l))
-    t.append(dict(name="head", cin=w[0], cout=HEAD_CHANNELS, level=0))
+    t.append(dict(name="head", cin=w[0], cout=head_channels(kernel_size), level=0))
     return t
 
 
 class KpnUNet:
     """The network, its fp32 master parameters, Adam state and activation buffers (one device)."""
 
-    def __init__(self, widths: Sequence[int] = WIDTHS, seed: int = 0, device: Optional[torch.device] = None):
+    def __init__(self, widths: Sequence[int] = WIDTHS, seed: int = 0, device: Optional[torch.device] = None,
+                 kernel_size: int = KERNEL_SIZE):
         self.lib = _lib.load()
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         self.widths = tuple(int(c) for c in widths)
-        self.layers = layer_table(self.widths)
+        if kernel_size % 2 == 0 or not 1 <= kernel_size <= 15:
+            raise ValueError("kernel_size: odd, 1..15")
+        self.kernel_size = int(kernel_size)
+        self.head_channels = head_channels(self.kernel_size)
+        self.layers = layer_table(self.widths, self.kernel_size)
         self.by_name = {L["name"]: L for L in self.layers}
         off = 0
         for L in self.layers:
@@ -96,7 +104,7 @@ class KpnUNet:
     # ---- parameters ----
     def init_parameters(self, seed: int) -> None:
         """He-normal weights (std sqrt(2 / fan_in), fan_in over the used input channels), zero
-        biases; the head starts small so the first kernels are close to a 5x5 box filter."""
+        biases; the head starts small so the first kernels are close to a k x k box filter."""
         g = np.random.default_rng(seed)
         host = np.zeros(self.count, np.float32)
         for L in self.layers:
@@ -177,7 +185,7 @@ class KpnUNet:
     # ---- network ----
     def forward(self, x0: torch.Tensor) -> torch.Tensor:
         """x0: packed input [n, h, w, 16] bf16 (h, w multiples of 16).  Returns the head's logits
-        [n, h, w, 32] fp32; the activations stay in this object for backward()."""
+        [n, h, w, head channels] fp32; the activations stay in this object for backward()."""
         n, h, w, c = x0.shape
         if c != IN_CHANNELS or h % 16 or w % 16:
             raise ValueError("input must be [n, h, w, 16] with h, w multiples of 16")
@@ -204,11 +212,11 @@ class KpnUNet:
             cur = self._conv(self.by_name[f"dec{l}b"], a, self.buf(f"dec{l}b", (n, hh, ww, W[l])), n, hh, ww, 1)
         hh, ww = dims[0]
         self._x0 = x0
-        return self._conv(self.by_name["head"], cur, self.buf("logits", (n, hh, ww, HEAD_CHANNELS), torch.float32),
-                          n, hh, ww, 0, 1)
+        return self._conv(self.by_name["head"], cur,
+                          self.buf("logits", (n, hh, ww, self.head_channels), torch.float32), n, hh, ww, 0, 1)
 
     def backward(self, dlogits: torch.Tensor) -> None:
-        """dlogits: [n, h, w, 32] bf16 gradient of the loss at the head's output.  Fills self.grad
+        """dlogits: [n, h, w, head channels] bf16 gradient of the loss at the head's output.  Fills self.grad
         (flat, same layout as the parameters)."""
         n, h, w = self.shape
         W = self.widths
@@ -272,10 +280,10 @@ class KpnUNet:
         blocks = self.lib.vpt_unet_head_blocks(n, h, w)
         dl = lp = None
         if target is not None:
-            dl = self.buf("dlogits", (n, h, w, HEAD_CHANNELS))
+            dl = self.buf("dlogits", (n, h, w, self.head_channels))
             lp = self.buf("loss_partial", (blocks,), torch.float32)
-        self._call("vpt_unet_kpn_head", _p(logits), _p(radiance), _p(target), _p(out), _p(dl), _p(lp), n, h, w,
-                   LOSS_EPS, self._stream())
+        self._call("vpt_unet_kpn_head", _p(logits), self.head_channels, self.kernel_size, _p(radiance), _p(target),
+                   _p(out), _p(dl), _p(lp), n, h, w, LOSS_EPS, self._stream())
         return out, (lp.sum() if lp is not None else None), dl
 
     def train_step(self, batch: dict, lr: float) -> torch.Tensor:
@@ -299,10 +307,10 @@ class KpnUNet:
     def save(self, directory: str) -> None:
         os.makedirs(directory, exist_ok=True)
         np.savez(os.path.join(directory, "weights.npz"), params=self.parameters_host())
-        info = {"input_feature_maps": INPUT_FEATURE_MAPS, "blend": "kpn", "kernel_size": KERNEL_SIZE,
+        info = {"input_feature_maps": INPUT_FEATURE_MAPS, "blend": "kpn", "kernel_size": self.kernel_size,
                 "use_previous_frame": False, "use_batch_dimension": True, "use_fp16": False,
                 "network": "unet", "widths": list(self.widths), "input_channels": IN_CHANNELS,
-                "head_channels": HEAD_CHANNELS, "loss": "relmse", "loss_eps": LOSS_EPS, "steps": self.steps}
+                "head_channels": self.head_channels, "loss": "relmse", "loss_eps": LOSS_EPS, "steps": self.steps}
         with open(os.path.join(directory, "model_info.json"), "w") as f:
             json.dump(info, f, indent=1)
 
@@ -313,7 +321,7 @@ class KpnUNet:
         if info.get("network") != "unet" or info.get("blend") != "kpn":
             raise RuntimeError(f"unsupported model_info.json in {directory}: network {info.get('network')}, "
                                f"blend {info.get('blend')}")
-        net = cls(info["widths"], device=device)
+        net = cls(info["widths"], device=device, kernel_size=int(info.get("kernel_size", KERNEL_SIZE)))
         net.set_parameters(np.load(os.path.join(directory, "weights.npz"))["params"])
         net.steps = int(info.get("steps", 0))
         return net

@@ -390,12 +390,14 @@ VptStatus vpt_unet_pack_input(const float* radiance, const float* albedo, const 
                               void* stream);
 int vpt_unet_head_blocks(int n, int h, int w);
 /* Kernel-prediction head (perPixelKernelCuda semantics, modules/kpn_module/src/Kernel.cu:38-135, with
- * the tap softmax fused): out[n][c][y][x] = sum_j softmax(logits[p][0..24])_j radiance[n][c][y+dy][x+dx]
- * (taps outside skipped; logits [p][32] fp32).  With target != NULL also the relative MSE
+ * the tap softmax fused): out[n][c][y][x] = sum_j softmax(logits[p][0 .. k*k-1])_j
+ * radiance[n][c][y+dy][x+dx] (k = kernel_size odd <= 15, taps outside skipped; logits [p][head_channels]
+ * fp32, head_channels >= k*k a multiple of 8).  With target != NULL also the relative MSE
  * sum (d-t)^2/(t^2+eps)/(3*n*h*w) as per-block partial sums (vpt_unet_head_blocks of them) and its
- * gradient dlogits [p][32] bf16.  out may be NULL. */
-VptStatus vpt_unet_kpn_head(const float* logits, const float* radiance, const float* target, float* out,
-                            void* dlogits, float* loss_partial, int n, int h, int w, float eps, void* stream);
+ * gradient dlogits [p][head_channels] bf16 (0 beyond k*k).  out may be NULL. */
+VptStatus vpt_unet_kpn_head(const float* logits, int head_channels, int kernel_size, const float* radiance,
+                            const float* target, float* out, void* dlogits, float* loss_partial, int n, int h, int w,
+                            float eps, void* stream);
 
 #ifdef __cplusplus
 }

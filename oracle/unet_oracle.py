@@ -140,21 +140,22 @@ def pack_input(radiance, albedo=None, normal=None, depth=None, transmittance=Non
     return out
 
 
-def kpn_head(logits, x, target=None, eps=1e-2):
-    """Softmax over the 25 logits of each pixel (channels 0..24 of logits [n,h,w,32]), 5x5 kernel
-    applied to x [n,3,h,w] with taps outside the image skipped; with a target, the relative MSE
-    loss sum (d - t)^2 / (t^2 + eps) / count and its gradient with respect to the logits.
-    Returns (d, loss, dlogits)."""
-    lg = np.asarray(logits, np.float64)[..., :25]
+def kpn_head(logits, x, target=None, eps=1e-2, ks=5):
+    """Softmax over the ks*ks logits of each pixel (channels 0..ks*ks-1 of logits [n,h,w,hc]), the
+    ks x ks kernel applied to x [n,3,h,w] with taps outside the image skipped; with a target, the
+    relative MSE loss sum (d - t)^2 / (t^2 + eps) / count and its gradient with respect to the
+    logits.  Returns (d, loss, dlogits)."""
+    taps, rad = ks * ks, ks // 2
+    lg = np.asarray(logits, np.float64)[..., :taps]
     x = np.asarray(x, np.float64)
     n, _, h, w = x.shape
     s = np.exp(lg - lg.max(axis=-1, keepdims=True))
     s /= s.sum(axis=-1, keepdims=True)
     xs = []  # x at each tap, [n,3,h,w], zero outside
-    for j in range(25):
-        dy, dx = j // 5 - 2, j % 5 - 2
+    for j in range(taps):
+        dy, dx = j // ks - rad, j % ks - rad
         xs.append(_shift(x.transpose(0, 2, 3, 1), dy, dx).transpose(0, 3, 1, 2))
-    xs = np.stack(xs, axis=-1)  # [n,3,h,w,25]
+    xs = np.stack(xs, axis=-1)  # [n,3,h,w,taps]
     d = (xs * s[:, None, :, :, :]).sum(axis=-1)
     if target is None:
         return d, None, None
@@ -163,10 +164,10 @@ def kpn_head(logits, x, target=None, eps=1e-2):
     den = t * t + eps
     loss = float(((d - t) ** 2 / den).sum() / count)
     g = 2.0 * (d - t) / den / count  # [n,3,h,w]
-    gx = (g[..., None] * xs).sum(axis=1)  # [n,h,w,25]
+    gx = (g[..., None] * xs).sum(axis=1)  # [n,h,w,taps]
     gd = (g * d).sum(axis=1)[..., None]
     dl = np.zeros(np.asarray(logits).shape)
-    dl[..., :25] = s * (gx - gd)
+    dl[..., :taps] = s * (gx - gd)
     return d, loss, dl
 
 
@@ -182,7 +183,7 @@ def adam(param, m1, m2, grad, step, lr=1e-4, beta1=0.9, beta2=0.999, eps=1e-8):
 # ---------------------------------------------------------------------------------------------
 # the whole network (cloudrendering_b200/learned_denoiser.py: KpnUNet.forward / backward)
 # ---------------------------------------------------------------------------------------------
-def layer_table(widths):
+def layer_table(widths, head_channels=32):
     w = list(widths)
     t = []
     for l in range(4):
@@ -193,14 +194,14 @@ def layer_table(widths):
     for l in (3, 2, 1, 0):
         t.append((f"dec{l}a", w[l + 1] + w[l], w[l]))
         t.append((f"dec{l}b", w[l], w[l]))
-    t.append(("head", w[0], 32))
+    t.append(("head", w[0], head_channels))
     return t
 
 
-def split_params(flat, widths):
+def split_params(flat, widths, head_channels=32):
     """Flat parameter vector -> {name: (w [cout][9][cin], b [cout])} (weights then bias per layer)."""
     out, off = {}, 0
-    for name, cin, cout in layer_table(widths):
+    for name, cin, cout in layer_table(widths, head_channels):
         w = np.asarray(flat[off:off + cout * 9 * cin]).reshape(cout, 9, cin)
         off += cout * 9 * cin
         out[name] = (w, np.asarray(flat[off:off + cout]))
@@ -208,12 +209,13 @@ def split_params(flat, widths):
     return out
 
 
-def network_loss_and_grad(flat, widths, x0, radiance, target, round_bf16=True, eps=1e-2):
+def network_loss_and_grad(flat, widths, x0, radiance, target, round_bf16=True, eps=1e-2, ks=5):
     """Forward, relative-MSE loss of the kernel head and the gradient with respect to every
     parameter (flat, same layout).  With round_bf16 the weights, activations and backward
     gradients are rounded to bf16 where the GPU stores them in bf16; without, all float64."""
     rnd = (lambda a: bf16(np.asarray(a, np.float32)).astype(np.float64)) if round_bf16 else (lambda a: a)
-    P = split_params(flat, widths)
+    hc = (ks * ks + 15) // 16 * 16
+    P = split_params(flat, widths, hc)
     Wt = {k: rnd(v[0]) for k, v in P.items()}
     Bs = {k: np.asarray(v[1], np.float64) for k, v in P.items()}
     A = {}
@@ -233,7 +235,7 @@ def network_loss_and_grad(flat, widths, x0, radiance, target, round_bf16=True, e
     logits = conv3x3(cur, Wt["head"], Bs["head"])
     if round_bf16:
         logits = logits.astype(np.float32).astype(np.float64)
-    d, loss, dl = kpn_head(logits, radiance, target, eps)
+    d, loss, dl = kpn_head(logits, radiance, target, eps, ks)
     G = {}
 
     def grads(name, x, dy):
@@ -263,6 +265,6 @@ def network_loss_and_grad(flat, widths, x0, radiance, target, round_bf16=True, e
         if l > 0:
             dpool = rnd(conv3x3_input_grad(ga, Wt[f"enc{l}a"]))
     flat_g = []
-    for name, _, _ in layer_table(widths):
+    for name, _, _ in layer_table(widths, hc):
         flat_g += [G[name][0].reshape(-1), G[name][1]]
     return loss, np.concatenate(flat_g), logits, d

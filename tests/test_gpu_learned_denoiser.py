@@ -38,7 +38,7 @@ def random_flat(widths, seed, head_scale=0.3):
 
 def test_network_gradient_matches_oracle():
     widths = (16, 32, 32, 48, 64)
-    net = ld.KpnUNet(widths)
+    net = ld.KpnUNet(widths, kernel_size=5)
     flat = random_flat(widths, 1)
     net.set_parameters(flat)
     g = np.random.default_rng(2)

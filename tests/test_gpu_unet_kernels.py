@@ -191,19 +191,20 @@ def test_pack_input_and_kpn_head(lib):
     ref = uo.pack_input(rad, alb, nrm, dep, trn, noise)
     close_bf16(host(packed), ref.astype(np.float64))
 
-    logits = rng_data(15, n, h, w, 32, scale=2.0)
     target = g.exponential(1.0, (n, 3, h, w)).astype(np.float32)
     blocks = lib.vpt_unet_head_blocks(n, h, w)
-    out = torch.empty((n, 3, h, w), dtype=torch.float32, device="cuda")
-    dl = torch.empty((n, h, w, 32), dtype=torch.bfloat16, device="cuda")
-    lp = torch.empty((blocks,), dtype=torch.float32, device="cuda")
-    assert lib.vpt_unet_kpn_head(ptr(dev_f32(logits)), ptr(t[0]), ptr(dev_f32(target)), ptr(out), ptr(dl), ptr(lp),
-                                 n, h, w, ctypes.c_float(1e-2), None) == 0
-    torch.cuda.synchronize()
-    d, loss, dlog = uo.kpn_head(logits, rad, target)
-    close_f32(host(out), d)
-    assert abs(float(lp.double().sum()) - loss) <= 1e-5 * loss
-    close_bf16(host(dl), dlog)
+    for ks, hc in ((5, 32), (9, 96), (11, 128), (3, 16)):
+        logits = rng_data(15 + ks, n, h, w, hc, scale=2.0)
+        out = torch.empty((n, 3, h, w), dtype=torch.float32, device="cuda")
+        dl = torch.empty((n, h, w, hc), dtype=torch.bfloat16, device="cuda")
+        lp = torch.empty((blocks,), dtype=torch.float32, device="cuda")
+        assert lib.vpt_unet_kpn_head(ptr(dev_f32(logits)), hc, ks, ptr(t[0]), ptr(dev_f32(target)), ptr(out), ptr(dl),
+                                     ptr(lp), n, h, w, ctypes.c_float(1e-2), None) == 0
+        torch.cuda.synchronize()
+        d, loss, dlog = uo.kpn_head(logits, rad, target, ks=ks)
+        close_f32(host(out), d)
+        assert abs(float(lp.double().sum()) - loss) <= 1e-5 * loss
+        close_bf16(host(dl), dlog)
 
 
 def test_adam(lib):
@@ -222,7 +223,7 @@ def test_adam(lib):
     f32 = lambda v: float(np.float32(v))  # the kernel receives float hyperparameters
     rp, rm1, rm2 = uo.adam(*(a.astype(np.float64) for a in (p, m1, m2, gr)), 7, lr=f32(1e-3), beta1=f32(0.9),
                            beta2=f32(0.999), eps=f32(1e-8))
-    # fp32 arithmetic: a few ulps of each value's scale
+    # fp32 arithmetic with contracted multiply-adds: a few ulps of the largest term
     for got, ref in ((host(tp), rp), (host(tm1), rm1), (host(tm2), rm2)):
-        assert np.all(np.abs(got - ref) <= 1e-6 * (np.abs(ref) + np.abs(ref).max() * 1e-3))
+        assert np.all(np.abs(got - ref) <= 1e-6 * np.abs(ref) + 4 * 2.0 ** -23 * np.abs(ref).max())
     assert np.array_equal(host(pb), uo.bf16(host(tp).astype(np.float32)))

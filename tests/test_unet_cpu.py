@@ -88,6 +88,19 @@ def test_kpn_head_loss_gradient_matches_autograd():
     assert abs(loss - tloss.item()) <= 1e-12 * abs(loss)
     assert np.allclose(dl[..., :25], tl.grad.numpy(), atol=1e-14)
     assert np.all(dl[..., 25:] == 0)
+    # other kernel sizes: finite differences of the oracle's own loss
+    for ks in (3, 7):
+        lg = g.standard_normal((1, 5, 6, 64))
+        xx = g.exponential(1.0, (1, 3, 5, 6))
+        tt2 = g.exponential(1.0, (1, 3, 5, 6))
+        _, l0, dl2 = uo.kpn_head(lg, xx, tt2, ks=ks)
+        for idx in [(0, 2, 3, 0), (0, 4, 5, ks * ks - 1), (0, 0, 0, ks * ks // 2)]:
+            lp, lm = lg.copy(), lg.copy()
+            lp[idx] += 1e-6
+            lm[idx] -= 1e-6
+            fd = (uo.kpn_head(lp, xx, tt2, ks=ks)[1] - uo.kpn_head(lm, xx, tt2, ks=ks)[1]) / 2e-6
+            assert abs(fd - dl2[idx]) <= 1e-6 * (abs(fd) + 1e-6)
+        assert np.all(dl2[..., ks * ks:] == 0)
 
 
 def test_adam_matches_torch():
