@@ -40,7 +40,8 @@ GRID_INTERPOLATION_TYPE_NAMES = ["Nearest", "Stochastic", "Trilinear"]
 # RenderSettings.hpp:123-125 (+ one addition)
 BUILTIN_ENV_MAP_NAMES = ["Default", "Black", "Single Color", "Constant Sky + Sun"]
 # Denoiser.hpp:63-79 (names of the denoisers built here)
-DENOISER_NAMES = {"None": 0, "Edge-Avoiding À-Trous Wavelet Transform": 1, "SVGF": 2}
+DENOISER_NAMES = {"None": 0, "Edge-Avoiding À-Trous Wavelet Transform": 1, "SVGF": 2,
+                  "PyTorch Denoiser Module": -1}
 # VolumetricPathTracingPass.hpp:74-80 (+ the new 2D transmittance feature)
 VPT_FEATURE_MAP_NAMES = [
     "Result", "First X", "First W", "Normal", "Normal (Length 1)", "Cloud Only", "Depth", "Depth Far",
@@ -66,6 +67,12 @@ class _State:
     view_override: Optional[List[float]] = None
     grid_size = (0, 0, 0)
     env_intensity = 1.0
+    # "PyTorch Denoiser Module" (runs on the host side of the boundary, pytorch_denoiser.py)
+    torch_denoiser_active = False
+    torch_denoiser_path = ""
+    torch_denoiser = None
+    torch_denoiser_loaded = ""
+    user_feature_maps: List[int] = []
 
 
 S = _State()
@@ -500,7 +507,41 @@ def set_view_projection_matrix_as_previous() -> None:
 def set_denoiser(denoiser_name: str) -> None:
     if denoiser_name not in DENOISER_NAMES:
         raise RuntimeError(f"Error in setDenoiser: Invalid denoiser name \"{denoiser_name}\".")
-    _c("vpt_set_denoiser", DENOISER_NAMES[denoiser_name])
+    S.torch_denoiser_active = DENOISER_NAMES[denoiser_name] < 0
+    _c("vpt_set_denoiser", max(0, DENOISER_NAMES[denoiser_name]))
+    if S.torch_denoiser is not None:
+        S.torch_denoiser.reset_previous_frame()
+    _apply_feature_maps()
+
+
+def set_pytorch_denoiser_model_file(denoiser_model_file_path: str) -> None:
+    """Module.cpp:1070 setPyTorchDenoiserModelFile: the model used by "PyTorch Denoiser Module"
+    (loaded at the next rendered frame)."""
+    S.torch_denoiser_path = str(denoiser_model_file_path)
+    _c("vpt_reset_accumulation")
+    if S.torch_denoiser_active:
+        _ensure_torch_denoiser()
+        _apply_feature_maps()
+
+
+def _ensure_torch_denoiser():
+    if not S.torch_denoiser_path:
+        raise RuntimeError("Error: the PyTorch denoiser has no model file (set_pytorch_denoiser_model_file).")
+    if S.torch_denoiser is None or S.torch_denoiser_loaded != S.torch_denoiser_path:
+        from .pytorch_denoiser import PyTorchDenoiser
+        d = PyTorchDenoiser(torch.device("cuda", S.device))
+        d.load_model_from_file(S.torch_denoiser_path)
+        S.torch_denoiser, S.torch_denoiser_loaded = d, S.torch_denoiser_path
+    return S.torch_denoiser
+
+
+def _apply_feature_maps() -> None:
+    ids = list(S.user_feature_maps)
+    if S.torch_denoiser_active and S.torch_denoiser is not None:
+        ids += [_FEATURE_BY_NAME[n] for n in S.torch_denoiser.renderer_feature_maps()]
+    ids = sorted(set(ids))
+    arr = (ctypes.c_int * max(1, len(ids)))(*ids)
+    _c("vpt_set_use_feature_maps", arr, len(ids))
 
 
 def set_denoiser_property(key: str, value: str) -> None:
@@ -509,9 +550,8 @@ def set_denoiser_property(key: str, value: str) -> None:
 
 # ---- feature maps ----
 def set_use_feature_maps(feature_map_names: List[str]) -> None:
-    ids = [_FEATURE_BY_NAME[n] for n in feature_map_names if n in _FEATURE_BY_NAME]
-    arr = (ctypes.c_int * max(1, len(ids)))(*ids)
-    _c("vpt_set_use_feature_maps", arr, len(ids))
+    S.user_feature_maps = [_FEATURE_BY_NAME[n] for n in feature_map_names if n in _FEATURE_BY_NAME]
+    _apply_feature_maps()
 
 
 _FEATURE_CHANNELS = {1: 4, 3: 4, 5: 4, 6: 2, 12: 2, 17: 4, FEATURE_TRANSMITTANCE: 1}
@@ -565,9 +605,17 @@ def render_frame(input_tensor: torch.Tensor, frame_count: int) -> torch.Tensor:
     """Renders `frame_count` 1-spp frames into the running mean and returns it as [C, H, W]."""
     _validate(input_tensor)
     c, h, w = input_tensor.shape
+    if S.torch_denoiser_active:
+        den = _ensure_torch_denoiser()
+        _apply_feature_maps()
     _c("vpt_set_resolution", int(w), int(h))
     _c("vpt_render_frames", int(frame_count), _stream_of(input_tensor))
-    return _read(input_tensor, c, "vpt_read_result")
+    if not S.torch_denoiser_active:
+        return _read(input_tensor, c, "vpt_read_result")
+    probe = torch.empty((4, h, w), dtype=torch.float32, device=torch.device("cuda", S.device))
+    color = _read(probe, 4, "vpt_read_result")
+    out = den.denoise(color, lambda name: get_feature_map_from_string(probe, name))
+    return out[:c].to(input_tensor.device).contiguous()
 
 
 def set_frame_index(first_frame: int) -> None:
