@@ -42,7 +42,6 @@ typedef __nv_bfloat16 bf16;
 
 constexpr int kBM = 128;      // tile rows (TMEM lanes)
 constexpr int kBK = 64;       // K elements per pipeline stage (4 MMAs of K = 16)
-constexpr int kStages = 4;    // shared-memory ring depth
 constexpr int kThreads = 128;
 constexpr uint32_t kWaitLimit = 1u << 22;  // bounded mbarrier waits (error flag on expiry)
 
@@ -166,7 +165,7 @@ __device__ __forceinline__ void pixel_coords(int p, int h, int w, int& n, int& y
     n = t / h;
 }
 
-template <int MODE>
+template <int MODE, int kStages>
 __global__ void __launch_bounds__(kThreads) conv_tile_kernel(const ConvArgs a) {
     extern __shared__ __align__(1024) uint8_t smem[];
     __shared__ uint64_t bars[kStages];
@@ -223,62 +222,95 @@ __global__ void __launch_bounds__(kThreads) conv_tile_kernel(const ConvArgs a) {
         }
     }
 
+    // incremental gather state (stages are loaded in increasing order, so nothing is divided by a
+    // runtime value inside the loop)
+    int ld_tap = 0, ld_ci = 0;                       // conv: (tap, channel) of the next stage's first k
+    int b_r0 = tid % n_tile, b_kc0 = tid / n_tile;   // conv: first B unit of this thread
+    int wq_n = 0, wq_y = 0, wq_x = 0, wq_p = kbeg + (tid & 7);  // wgrad: this thread's next A pixel
+    if (MODE == kWgrad && wq_p < P) pixel_coords(wq_p, a.h, a.w_, wq_n, wq_y, wq_x);
+    const int nch = n_tile / 8;
+    const int wb_rest0 = tid >> 3;
+    const int wb_nc0 = wb_rest0 % nch, wb_kph0 = wb_rest0 / nch;
+
     auto load_stage = [&](int slot, int s) {
         const uint32_t sA = sbase + slot * stage_bytes;
         const uint32_t sB = sA + a_bytes;
         if (MODE == kConv) {
             const int k0 = s * kBK;
             // A: row tid, 8 chunks of 8 channels; unit (r, kc) at kc * kBM * 16 + r * 16
+            int tap = ld_tap, ci = ld_ci;
 #pragma unroll
             for (int kc = 0; kc < 8; ++kc) {
                 const int kk = k0 + kc * 8;
                 const bf16* src = a.x;
                 bool v = false;
                 if (p_ok && kk < K) {
-                    const int tap = kk / a.cin, ci = kk - tap * a.cin;
-                    const int yy = py + tap / 3 - 1, xx = px + tap % 3 - 1;
+                    const int dy = (tap * 11) >> 5, dx = tap - 3 * dy;  // tap / 3, tap % 3 for tap < 9
+                    const int yy = py + dy - 1, xx = px + dx - 1;
                     if (yy >= 0 && yy < a.h && xx >= 0 && xx < a.w_) {
                         v = true;
                         src = a.x + ((size_t)(pn * a.h + yy) * a.w_ + xx) * a.cin + ci;
                     }
                 }
                 cp_async16(sA + kc * (kBM * 16) + tid * 16, src, v);
+                ci += 8;
+                while (ci >= a.cin) {
+                    ci -= a.cin;
+                    ++tap;
+                }
             }
+            ld_tap = tap;
+            ld_ci = ci;
             // B: weight rows n0 .. n0 + n_tile; unit (r, kc) at kc * n_tile * 16 + r * 16
+            int r = b_r0, kc = b_kc0;
             for (int q = tid; q < n_tile * 8; q += kThreads) {
-                const int r = q % n_tile, kc = q / n_tile;
                 const int kk = k0 + kc * 8, co = n0 + r;
                 const bool v = co < a.cout && kk < K;
                 cp_async16(sB + kc * (n_tile * 16) + r * 16, v ? a.w + (size_t)co * K + kk : a.w, v);
+                r += kThreads;
+                while (r >= n_tile) {
+                    r -= n_tile;
+                    ++kc;
+                }
             }
         } else {
             const int pbase = kbeg + s * kBK;
-            // A (MN-major): unit (mc, kp) at (kp / 8) * 2048 + mc * 128 + (kp % 8) * 16 = 16 * q
-            const int kp_lo = tid & 7;
+            // A (MN-major): unit (mc, kp) at (kp / 8) * 2048 + mc * 128 + (kp % 8) * 16 = 16 * q; this
+            // thread's pixels advance by 8 per unit
+            const int tdy = (wg_tap * 11) >> 5, tdx = wg_tap - 3 * tdy;
 #pragma unroll
             for (int i = 0; i < 8; ++i) {
-                const int p = pbase + i * 8 + kp_lo;
                 const bf16* src = a.x;
                 bool v = false;
-                if (wg_m_ok && p < kend) {
-                    int qn, qy, qx;
-                    pixel_coords(p, a.h, a.w_, qn, qy, qx);
-                    const int yy = qy + wg_tap / 3 - 1, xx = qx + wg_tap % 3 - 1;
+                if (wg_m_ok && wq_p < kend) {
+                    const int yy = wq_y + tdy - 1, xx = wq_x + tdx - 1;
                     if (yy >= 0 && yy < a.h && xx >= 0 && xx < a.w_) {
                         v = true;
-                        src = a.x + ((size_t)(qn * a.h + yy) * a.w_ + xx) * a.cin + wg_ci;
+                        src = a.x + ((size_t)(wq_n * a.h + yy) * a.w_ + xx) * a.cin + wg_ci;
                     }
                 }
                 cp_async16(sA + (i * kThreads + tid) * 16, src, v);
+                wq_p += 8;
+                wq_x += 8;
+                while (wq_x >= a.w_) {
+                    wq_x -= a.w_;
+                    if (++wq_y == a.h) {
+                        wq_y = 0;
+                        ++wq_n;
+                    }
+                }
             }
             // B (MN-major): dy rows; unit (nc, kp) at (kp / 8) * n_tile * 16 + nc * 128 + (kp % 8) * 16
-            const int nch = n_tile / 8;
+            int nc = wb_nc0, kph = wb_kph0;
             for (int q = tid; q < n_tile * 8; q += kThreads) {
-                const int lo = q & 7, rest = q >> 3;
-                const int nc = rest % nch, kp = (rest / nch) * 8 + lo;
-                const int p = pbase + kp, co = n0 + nc * 8;
+                const int p = pbase + kph * 8 + (tid & 7), co = n0 + nc * 8;
                 const bool v = p < kend && co < a.cout;
                 cp_async16(sB + q * 16, v ? a.w + (size_t)p * a.cout + co : a.w, v);
+                nc += kThreads / 8;
+                while (nc >= nch) {
+                    nc -= nch;
+                    ++kph;
+                }
             }
         }
     };
@@ -381,6 +413,228 @@ __global__ void __launch_bounds__(kThreads) conv_tile_kernel(const ConvArgs a) {
         }
     }
     if (fail && tid == 0 && a.err) atomicExch(a.err, (int)VPT_ERR_ITER_LIMIT);
+    tc_fence_before();
+    __syncthreads();
+    if (tid < 32) {
+        tc_fence_after();
+        tmem_dealloc(tmem, (uint32_t)a.tmem_cols);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// the row-strip convolution (forward and input gradient on images at least 128 pixels wide)
+// ---------------------------------------------------------------------------------------------
+// A persistent CTA owns segments of consecutive rows of one 128-pixel-wide image column
+// (n, x0 .. x0 + 127).  The output tile of row y needs input rows y-1, y, y+1 at x0-1 .. x0+128: each
+// input row is gathered once into a ring of 5 shared-memory row strips (130 pixels per 8-channel
+// plane, 16 bytes per pixel, planes 2080 bytes apart), so that a row stays resident for the three
+// output rows that use it and the row two ahead is in flight.  In the UMMA K-major no-swizzle layout
+// (8-row core matrices of 16-byte rows, SBO = 128 between 8-pixel groups, LBO = plane stride between
+// 8-channel chunks) the A operand of tap (dy, dx) is the strip of row y+dy with its start address
+// moved by dx * 16 bytes: the three horizontal taps share one gather.  All 9 taps of the weights are
+// resident in shared memory for the CTA's lifetime.  Two TMEM accumulators alternate: the epilogue
+// of tile i-1 (tcgen05.ld, bias, ReLU, mask, store) runs while the tensor core computes tile i.
+constexpr int kStripPix = kBM + 2;          // 130 pixels: x0-1 .. x0+128
+constexpr int kPlane = kStripPix * 16;      // bytes per 8-channel plane of a row strip
+constexpr int kRing = 5;                    // row strips resident
+
+struct StripArgs {
+    const bf16* x;       // [n][h][w][cin]
+    const bf16* w;       // [cout][9][cin]
+    const float* bias;   // [cout] or null
+    const bf16* mask;    // [n][h][w][cout] or null
+    void* y;             // [n][h][w][cout] bf16 / fp32
+    int* err;
+    int n, h, w_, cin, cout;   // cin: input channels of this pass (a group of the tensor's channels)
+    int cin_total, c0;         // channels per pixel of x (and per tap of w); first channel of this pass
+    const float* part_in;      // fp32 [n][h][w][cout] partial sum added before the epilogue, or null
+    float* part_out;           // non-null: store the raw fp32 sum here (an intermediate pass), no epilogue
+    int relu, out_f32;
+    int xtiles;          // ceil(w / 128)
+    int seg_rows;        // rows per segment
+    int segs_per_col;
+    int tmem_cols;
+};
+
+__device__ __forceinline__ void strip_epilogue(const StripArgs& a, uint32_t tacc, int n_img, int yrow, int x0) {
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int x = x0 + warp * 32 + lane;
+    const bool ok = x < a.w_;
+    const size_t p = ((size_t)n_img * a.h + yrow) * a.w_ + (ok ? x : 0);
+    const uint32_t trow = tacc + ((uint32_t)(warp * 32) << 16);
+    for (int c0 = 0; c0 < a.cout; c0 += 16) {
+        float v[16];
+        tmem_ld16(trow + (uint32_t)c0, v);
+        if (!ok) continue;
+        if (a.part_in) {
+            const float4* src = reinterpret_cast<const float4*>(a.part_in + p * a.cout + c0);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const float4 u = src[i];
+                v[4 * i] += u.x;
+                v[4 * i + 1] += u.y;
+                v[4 * i + 2] += u.z;
+                v[4 * i + 3] += u.w;
+            }
+        }
+        if (a.part_out) {
+            float4* dst = reinterpret_cast<float4*>(a.part_out + p * a.cout + c0);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) dst[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+            continue;
+        }
+        if (a.bias) {
+#pragma unroll
+            for (int i = 0; i < 16; ++i) v[i] += a.bias[c0 + i];
+        }
+        if (a.relu) {
+#pragma unroll
+            for (int i = 0; i < 16; ++i) v[i] = fmaxf(v[i], 0.0f);
+        }
+        if (a.mask) {
+            const uint4* mp = reinterpret_cast<const uint4*>(a.mask + p * a.cout + c0);
+            const uint4 m4[2] = {mp[0], mp[1]};
+            const bf16* mb = reinterpret_cast<const bf16*>(m4);
+#pragma unroll
+            for (int i = 0; i < 16; ++i) v[i] = __bfloat162float(mb[i]) > 0.0f ? v[i] : 0.0f;
+        }
+        if (a.out_f32) {
+            float4* dst = reinterpret_cast<float4*>(static_cast<float*>(a.y) + p * a.cout + c0);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) dst[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+        } else {
+            uint4 o[2];
+            __nv_bfloat162* ob = reinterpret_cast<__nv_bfloat162*>(o);
+#pragma unroll
+            for (int i = 0; i < 8; ++i) ob[i] = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
+            uint4* dst = reinterpret_cast<uint4*>(static_cast<bf16*>(a.y) + p * a.cout + c0);
+            dst[0] = o[0];
+            dst[1] = o[1];
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) conv_strip_kernel(const StripArgs a) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    __shared__ uint64_t bars[2];
+    __shared__ uint32_t tmem_slot;
+    const int tid = threadIdx.x;
+    const int nkc = a.cin / 8;
+    const uint32_t w_bytes = 9u * (uint32_t)a.cin * (uint32_t)a.cout * 2u;
+    const uint32_t row_bytes = (uint32_t)nkc * kPlane;
+    const uint32_t sw = smem_u32(smem);
+    const uint32_t sring = sw + ((w_bytes + 127u) & ~127u);
+
+    if (tid == 0) {
+        mbar_init(smem_u32(&bars[0]), 1);
+        mbar_init(smem_u32(&bars[1]), 1);
+        fence_mbar_init();
+    }
+    if (tid < 32) tmem_alloc(smem_u32(&tmem_slot), (uint32_t)a.tmem_cols);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_slot;
+
+    // resident weights: unit (t, kc, co) at ((t * nkc + kc) * cout + co) * 16
+    for (int q = tid; q < 9 * nkc * a.cout; q += kThreads) {
+        const int co = q % a.cout, rest = q / a.cout;
+        const int kc = rest % nkc, t = rest / nkc;
+        cp_async16(sw + (uint32_t)q * 16u, a.w + ((size_t)co * 9 + t) * a.cin_total + a.c0 + kc * 8, true);
+    }
+    cp_async_commit();
+
+    auto load_row = [&](int n_img, int yy, int x0) {
+        const uint32_t base = sring + (uint32_t)(((yy + 1) % kRing + kRing) % kRing) * row_bytes;
+        const bool row_ok = yy >= 0 && yy < a.h;
+        for (int q = tid; q < kStripPix * nkc; q += kThreads) {
+            const int r = q % kStripPix, kc = q / kStripPix;
+            const int xx = x0 - 1 + r;
+            const bool v = row_ok && xx >= 0 && xx < a.w_;
+            const bf16* src = v ? a.x + (((size_t)n_img * a.h + yy) * a.w_ + xx) * a.cin_total + a.c0 + kc * 8 : a.x;
+            cp_async16(base + (uint32_t)kc * kPlane + (uint32_t)r * 16u, src, v);
+        }
+    };
+
+    const uint32_t idesc = instr_desc(kBM, a.cout, 0, 0);
+    const uint32_t b_lbo = (uint32_t)a.cout * 16u;
+    const int total_segs = a.n * a.xtiles * a.segs_per_col;
+    long g = 0;          // tiles computed by this CTA (accumulator index and mbarrier parity)
+    int fail = 0;
+    int pend_n = 0, pend_y = 0, pend_x0 = 0;
+    bool pending = false;  // a tile whose epilogue has not run
+
+    for (int seg = blockIdx.x; seg < total_segs && !fail; seg += gridDim.x) {
+        const int col = seg / a.segs_per_col, part = seg % a.segs_per_col;
+        const int n_img = col / a.xtiles, x0 = (col % a.xtiles) * kBM;
+        const int y0 = part * a.seg_rows, y1 = min(a.h, y0 + a.seg_rows);
+        if (y0 >= y1) continue;
+        // every MMA of the previous segment has finished reading the ring
+        if (pending) {
+            if (!mbar_wait(smem_u32(&bars[(g - 1) & 1]), (uint32_t)(((g - 1) >> 1) & 1))) fail = 1;
+            if (__syncthreads_or(fail)) break;
+            tc_fence_after();
+            strip_epilogue(a, tmem + (uint32_t)(((g - 1) & 1) * a.cout), pend_n, pend_y, pend_x0);
+            pending = false;
+        }
+        load_row(n_img, y0 - 1, x0);
+        load_row(n_img, y0, x0);
+        load_row(n_img, y0 + 1, x0);
+        cp_async_commit();
+        if (y0 + 2 <= y1) load_row(n_img, y0 + 2, x0);
+        cp_async_commit();
+        for (int yrow = y0; yrow < y1; ++yrow, ++g) {
+            cp_async_wait<1>();  // rows yrow-1 .. yrow+1 (and the weights) have landed
+            fence_proxy_async();
+            tc_fence_before();
+            if (__syncthreads_or(fail)) break;
+            const int buf = (int)(g & 1);
+            if (tid == 0) {
+                tc_fence_after();
+                const uint32_t dacc = tmem + (uint32_t)(buf * a.cout);
+                int first = 1;
+                for (int dy = 0; dy < 3; ++dy) {
+                    const uint32_t rb = sring + (uint32_t)((yrow + dy) % kRing) * row_bytes;  // slot of row yrow+dy-1
+                    for (int dx = 0; dx < 3; ++dx) {
+                        const int t = dy * 3 + dx;
+                        for (int j = 0; j < nkc / 2; ++j) {
+                            const uint64_t da = smem_desc(rb + (uint32_t)(2 * j) * kPlane + (uint32_t)dx * 16u, kPlane,
+                                                          128);
+                            const uint64_t db = smem_desc(sw + (uint32_t)((t * nkc + 2 * j) * a.cout) * 16u, b_lbo, 128);
+                            mma_bf16(dacc, da, db, idesc, first ? 0u : 1u);
+                            first = 0;
+                        }
+                    }
+                }
+                mma_commit(smem_u32(&bars[buf]));
+            }
+            if (pending) {  // epilogue of the previous tile while this one computes
+                if (!mbar_wait(smem_u32(&bars[(g - 1) & 1]), (uint32_t)(((g - 1) >> 1) & 1))) fail = 1;
+                if (__syncthreads_or(fail)) break;
+                tc_fence_after();
+                strip_epilogue(a, tmem + (uint32_t)(((g - 1) & 1) * a.cout), pend_n, pend_y, pend_x0);
+            }
+            pending = true;
+            pend_n = n_img;
+            pend_y = yrow;
+            pend_x0 = x0;
+            // the previous tile's MMAs are done: the slot of row yrow-2 is free for row yrow+3
+            if (yrow + 3 <= y1) load_row(n_img, yrow + 3, x0);
+            cp_async_commit();
+        }
+    }
+    cp_async_wait<0>();
+    if (pending && !fail) {
+        if (!mbar_wait(smem_u32(&bars[(g - 1) & 1]), (uint32_t)(((g - 1) >> 1) & 1))) fail = 1;
+        if (!__syncthreads_or(fail)) {
+            tc_fence_after();
+            strip_epilogue(a, tmem + (uint32_t)(((g - 1) & 1) * a.cout), pend_n, pend_y, pend_x0);
+        }
+    } else if (pending) {
+        // bounded wait for the MMAs in flight before the accumulator is freed
+        mbar_wait(smem_u32(&bars[(g - 1) & 1]), (uint32_t)(((g - 1) >> 1) & 1));
+    }
+    if (__syncthreads_or(fail) && tid == 0 && a.err) atomicExch(a.err, (int)VPT_ERR_ITER_LIMIT);
     tc_fence_before();
     __syncthreads();
     if (tid < 32) {
@@ -721,23 +975,128 @@ inline int pow2_cols(int n) {
     return c;
 }
 
-template <int MODE>
-cudaError_t launch_tile(const ConvArgs& a, dim3 grid, cudaStream_t s) {
-    const size_t smem = (size_t)kStages * (kBM * kBK * 2 + (size_t)a.n_tile * kBK * 2);
-    cudaError_t e = cudaFuncSetAttribute(conv_tile_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
+template <int MODE, int STAGES>
+cudaError_t launch_tile_n(const ConvArgs& a, dim3 grid, cudaStream_t s) {
+    const size_t smem = (size_t)STAGES * (kBM * kBK * 2 + (size_t)a.n_tile * kBK * 2);
+    cudaError_t e = cudaFuncSetAttribute(conv_tile_kernel<MODE, STAGES>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    conv_tile_kernel<MODE><<<grid, kThreads, smem, s>>>(a);
+    conv_tile_kernel<MODE, STAGES><<<grid, kThreads, smem, s>>>(a);
     count_launches(1);
     return cudaGetLastError();
 }
 
+static int g_gather_stages = 0;  // 0: 3 stages, except 4 for 64-column convolution tiles (measured)
+
+template <int MODE>
+cudaError_t launch_tile(const ConvArgs& a, dim3 grid, cudaStream_t s) {
+    int st = g_gather_stages;
+    if (st == 0) st = (MODE == kConv && a.n_tile == 64) ? 4 : 3;
+    return st == 3 ? launch_tile_n<MODE, 3>(a, grid, s) : launch_tile_n<MODE, 4>(a, grid, s);
+}
+
 inline bool chan_ok(int c) { return c > 0 && c % 16 == 0; }
+
+inline int sm_count() {
+    int dev = 0, n = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    return n > 0 ? n : 148;
+}
+
+constexpr size_t kStripSmemLimit = 200 * 1024;
+
+inline size_t strip_smem_bytes(int cin, int cout) {
+    return ((9ul * cin * cout * 2 + 127) & ~(size_t)127) + (size_t)kRing * (cin / 8) * kPlane;
+}
+
+// the row-strip kernel serves images at least one tile wide with at most 256 output channels; the
+// input channels are split into groups whose weights and ring fit in shared memory (one pass each,
+// summed through an fp32 partial)
+inline int strip_groups(int width, int cin, int cout) {
+    if (width < kBM || cout > 256) return 0;
+    for (int g = 1; g <= 4; ++g) {
+        const int cg = (cin / 16 + g - 1) / g * 16;
+        // grouped passes re-stream an fp32 partial; they beat the gather kernel only for narrow
+        // outputs (measured: 176 -> 32 faster, 160 -> 64 slower)
+        if (strip_smem_bytes(cg, cout) <= kStripSmemLimit) return (g == 1 || cout <= 32) ? g : 0;
+    }
+    return 0;
+}
+
+cudaError_t launch_strip_pass(StripArgs a, cudaStream_t s) {
+    a.xtiles = (a.w_ + kBM - 1) / kBM;
+    a.tmem_cols = pow2_cols(2 * a.cout);
+    const size_t smem = strip_smem_bytes(a.cin, a.cout);
+    int per_sm = (int)(220 * 1024 / smem);
+    per_sm = per_sm < 1 ? 1 : per_sm;
+    per_sm = min(per_sm, 512 / a.tmem_cols);
+    const int slots = sm_count() * per_sm;
+    const int cols = a.n * a.xtiles;
+    const int want = max(cols, 2 * slots);
+    int spc = (want + cols - 1) / cols;
+    spc = min(spc, max(1, a.h / 4));  // segments of at least 4 rows (2 halo rows per segment)
+    a.seg_rows = (a.h + spc - 1) / spc;
+    a.segs_per_col = (a.h + a.seg_rows - 1) / a.seg_rows;
+    const int total = cols * a.segs_per_col;
+    const int grid = min(total, slots);
+    cudaError_t e = cudaFuncSetAttribute(conv_strip_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    conv_strip_kernel<<<grid, kThreads, smem, s>>>(a);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_strip(const ConvArgs& c, int groups, cudaStream_t s) {
+    StripArgs a{};
+    a.x = c.x;
+    a.w = c.w;
+    a.err = c.err;
+    a.n = c.n;
+    a.h = c.h;
+    a.w_ = c.w_;
+    a.cout = c.cout;
+    a.cin_total = c.cin;
+    if (groups <= 1) {
+        a.cin = c.cin;
+        a.bias = c.bias;
+        a.mask = c.mask;
+        a.y = c.y;
+        a.relu = c.relu;
+        a.out_f32 = c.out_f32;
+        return launch_strip_pass(a, s);
+    }
+    // fp32 partial sum of the earlier groups (stream-ordered scratch)
+    float* part = nullptr;
+    const size_t bytes = (size_t)c.n * c.h * c.w_ * c.cout * sizeof(float);
+    cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(&part), bytes, s);
+    if (e != cudaSuccess) return e;
+    const int cg = (c.cin / 16 + groups - 1) / groups * 16;
+    for (int g = 0, c0 = 0; c0 < c.cin && e == cudaSuccess; ++g, c0 += cg) {
+        const bool last = c0 + cg >= c.cin;
+        StripArgs p = a;
+        p.c0 = c0;
+        p.cin = min(cg, c.cin - c0);
+        p.part_in = g > 0 ? part : nullptr;
+        p.part_out = last ? nullptr : part;
+        if (last) {
+            p.bias = c.bias;
+            p.mask = c.mask;
+            p.y = c.y;
+            p.relu = c.relu;
+            p.out_f32 = c.out_f32;
+        }
+        e = launch_strip_pass(p, s);
+    }
+    const cudaError_t f = cudaFreeAsync(part, s);
+    return e != cudaSuccess ? e : f;
+}
 
 }  // namespace unet
 }  // namespace vpt
 
 using namespace vpt::unet;
+
+static bool g_force_gather = false;
 
 extern "C" {
 
@@ -763,9 +1122,25 @@ VptStatus vpt_unet_conv3x3(const void* x, const void* w, const float* bias, cons
     a.tmem_cols = pow2_cols(a.n_tile);
     a.relu = relu;
     a.out_f32 = out_f32;
+    const int groups = strip_groups(width, cin, cout);
+    if (groups > 0 && !g_force_gather)
+        return launch_strip(a, groups, static_cast<cudaStream_t>(stream)) == cudaSuccess ? VPT_OK : VPT_ERR_CUDA;
     const long P = (long)n * h * width;
     const dim3 grid((unsigned)((P + kBM - 1) / kBM), (unsigned)((cout + a.n_tile - 1) / a.n_tile), 1);
     return launch_tile<kConv>(a, grid, static_cast<cudaStream_t>(stream)) == cudaSuccess ? VPT_OK : VPT_ERR_CUDA;
+}
+
+// 1: every convolution uses the per-tile gather kernel (for comparisons); 0: row strips where eligible
+VptStatus vpt_unet_set_conv_path(int force_gather) {
+    g_force_gather = force_gather != 0;
+    return VPT_OK;
+}
+
+// shared-memory ring depth of the gather kernel (3 or 4; 0 = by shape)
+VptStatus vpt_unet_set_gather_stages(int stages) {
+    if (stages != 0 && stages != 3 && stages != 4) return VPT_ERR_ARG;
+    g_gather_stages = stages;
+    return VPT_OK;
 }
 
 VptStatus vpt_unet_conv3x3_wgrad(const void* x, const void* dy, float* partial, int n, int h, int width, int cin,

@@ -355,6 +355,13 @@ VptStatus vpt_eaw_denoise_rgba_noalloc(const float* color, const float* position
  * the forward input as mask (ReLU derivative). */
 VptStatus vpt_unet_conv3x3(const void* x, const void* w, const float* bias, const void* mask, void* y, int n, int h,
                            int width, int cin, int cout, int relu, int out_f32, int* err, void* stream);
+/* Selects the convolution kernel: 1 = the per-tile gather kernel everywhere, 0 (default) = the
+ * persistent row-strip kernel for images at least 128 pixels wide with at most 256 output channels
+ * (input channels in up to 4 groups that fit in shared memory; groups summed through an fp32 partial
+ * allocated on the stream). */
+VptStatus vpt_unet_set_conv_path(int force_gather);
+/* Shared-memory ring depth of the per-tile gather kernel: 3 or 4 stages, 0 (default) = by shape. */
+VptStatus vpt_unet_set_gather_stages(int stages);
 /* Weight gradient: partial[s][t*cin + ci][co] = sum over pixels p of split s (pixels_per_split each,
  * a multiple of 64) of dy[p][co] x[p + off(t)][ci]; partial has vpt_unet_wgrad_rows(cin) rows per
  * split, reduced by vpt_unet_reduce_grads. */

@@ -118,6 +118,47 @@ def test_conv_input_grad(lib, case):
     close_bf16(host(out_b), uo.conv3x3_input_grad(dy, wt, mask=x))
 
 
+STRIP_CASES = [
+    # n, h, w, cin, cout: images at least 128 pixels wide take the row-strip kernel
+    (1, 5, 130, 32, 32),    # ragged second tile (2 of 128 pixels valid)
+    (2, 9, 256, 16, 32),
+    (1, 3, 128, 96, 32),
+    (1, 4, 200, 32, 176),   # 13x13 kernel head
+    (1, 37, 128, 64, 64),   # many rows: several segments per column
+    (1, 6, 128, 160, 64),   # input channels in two groups (fp32 partial between the passes)
+]
+
+
+@pytest.mark.parametrize("case", STRIP_CASES)
+def test_strip_conv_forward_and_input_grad(lib, case):
+    n, h, w, cin, cout = case
+    x = uo.bf16(rng_data(21, n, h, w, cin))
+    wt = uo.bf16(rng_data(22, cout, 9, cin, scale=1.0 / np.sqrt(9 * cin)))
+    bias = rng_data(23, cout, scale=0.1)
+    dx, dw, b = dev_bf16(x), dev_bf16(wt), dev_f32(bias)
+    y = torch.empty((n, h, w, cout), dtype=torch.float32, device="cuda")
+    run(lib, "vpt_unet_conv3x3", ptr(dx), ptr(dw), ptr(b), None, ptr(y), n, h, w, cin, cout, 0, 1)
+    close_f32(host(y), uo.conv3x3(x, wt, bias=bias))
+    yb = torch.empty((n, h, w, cout), dtype=torch.bfloat16, device="cuda")
+    run(lib, "vpt_unet_conv3x3", ptr(dx), ptr(dw), ptr(b), None, ptr(yb), n, h, w, cin, cout, 1, 0)
+    close_bf16(host(yb), uo.conv3x3(x, wt, bias=bias, relu=True))
+    # the gather kernel gives the same result up to the summation order
+    assert lib.vpt_unet_set_conv_path(1) == 0
+    y2 = torch.empty_like(y)
+    run(lib, "vpt_unet_conv3x3", ptr(dx), ptr(dw), ptr(b), None, ptr(y2), n, h, w, cin, cout, 0, 1)
+    assert lib.vpt_unet_set_conv_path(0) == 0
+    close_f32(host(y2), host(y))
+    # input gradient with the ReLU-derivative mask (rotated weights: cout -> cin; 176 input channels
+    # of the head's gradient take two channel groups)
+    dy = uo.bf16(rng_data(24, n, h, w, cout))
+    wrot = torch.empty((cin, 9, cout), dtype=torch.bfloat16, device="cuda")
+    assert lib.vpt_unet_rotate_weights(ptr(dw), ptr(wrot), cin, cout, None) == 0
+    g = torch.empty((n, h, w, cin), dtype=torch.bfloat16, device="cuda")
+    d_dy = dev_bf16(dy)  # kept alive: a temporary's memory may be reused by the next allocation
+    run(lib, "vpt_unet_conv3x3", ptr(d_dy), ptr(wrot), None, ptr(dx), ptr(g), n, h, w, cout, cin, 0, 0)
+    close_bf16(host(g), uo.conv3x3_input_grad(dy, wt, mask=x))
+
+
 WGRAD_CASES = [
     # n, h, w, cin, cout, pixels per split
     (2, 9, 13, 16, 32, 64),
@@ -198,8 +239,9 @@ def test_pack_input_and_kpn_head(lib):
         out = torch.empty((n, 3, h, w), dtype=torch.float32, device="cuda")
         dl = torch.empty((n, h, w, hc), dtype=torch.bfloat16, device="cuda")
         lp = torch.empty((blocks,), dtype=torch.float32, device="cuda")
-        assert lib.vpt_unet_kpn_head(ptr(dev_f32(logits)), hc, ks, ptr(t[0]), ptr(dev_f32(target)), ptr(out), ptr(dl),
-                                     ptr(lp), n, h, w, ctypes.c_float(1e-2), None) == 0
+        d_logits, d_target = dev_f32(logits), dev_f32(target)
+        assert lib.vpt_unet_kpn_head(ptr(d_logits), hc, ks, ptr(t[0]), ptr(d_target), ptr(out), ptr(dl), ptr(lp), n,
+                                     h, w, ctypes.c_float(1e-2), None) == 0
         torch.cuda.synchronize()
         d, loss, dlog = uo.kpn_head(logits, rad, target, ks=ks)
         close_f32(host(out), d)
