@@ -109,6 +109,7 @@ SIGNATURES = {
     "vpt_kpn_reproject": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_int, c_int, c_void_p, c_void_p]),
     "vpt_eaw_denoise_rgba_noalloc": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_float, c_float,
                                              c_float, c_int, c_void_p, c_void_p]),
+    "vpt_svgf_filter": (c_int, [c_void_p] * 9 + [c_int, c_int, c_float, c_float, c_int, c_void_p, c_void_p]),
     # learned denoiser network (csrc/vpt_unet.cu)
     "vpt_unet_conv3x3": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_int,
                                  c_int, c_int, c_void_p, c_void_p]),

@@ -31,6 +31,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", INCLUDE
 PER_FILE = {
     "vpt_kernels.cu": ["--fmad=false"],
     "vpt_kpn.cu": ["--fmad=false"],
+    "vpt_denoise.cu": ["--fmad=false"],
 }
 # sources that hold the tracer's transcendental calls (built twice, see above)
 DOUBLE_ROUNDED = {"vpt_kernels.cu"}

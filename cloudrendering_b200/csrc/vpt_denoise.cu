@@ -441,6 +441,10 @@ __global__ void svgf_update_history_kernel(SvgfCur c, float4* __restrict__ momen
     depth_hist[i] = c.depth[i];
 }
 
+cudaError_t svgf_filter_passes(SvgfCur c, float4* color_history, float4* moments_history, float4* normal_history,
+                               float* depth_history, int w, int h, const SvgfSettings& s, cudaStream_t stream,
+                               const float4** result);
+
 cudaError_t svgf_denoise_features(const float* color, const float* feat, uint32_t frames, int w, int h,
                                   const SvgfSettings& s, SvgfState& st, float* out_rgba, float** result,
                                   cudaStream_t stream) {
@@ -472,28 +476,41 @@ cudaError_t svgf_denoise_features(const float* color, const float* feat, uint32_
     }
     svgf_prepare_kernel<<<(n + 255) / 256, 256, 0, stream>>>(reinterpret_cast<const float4*>(color), feat, w, h, itv, pvp,
                                                              s.far_dist, c);
+    count_launches(1);
+    const float4* src = nullptr;
+    cudaError_t e = svgf_filter_passes(c, reinterpret_cast<float4*>(st.color_history),
+                                       reinterpret_cast<float4*>(st.moments_history),
+                                       reinterpret_cast<float4*>(st.normal_history), st.depth_history, w, h, s, stream,
+                                       &src);
+    *result = reinterpret_cast<float*>(const_cast<float4*>(src));
+    return e;
+}
+
+// The filter passes of one SVGF frame on prepared maps (c.noisy / normal / depth / fwidth / motion)
+// and scratch (c.moments / temp / ping / pong); the result is c.temp, c.ping or c.pong.
+cudaError_t svgf_filter_passes(SvgfCur c, float4* color_history, float4* moments_history, float4* normal_history,
+                               float* depth_history, int w, int h, const SvgfSettings& s, cudaStream_t stream,
+                               const float4** result) {
+    const int n = w * h;
     dim3 b(16, 16), g((w + 15) / 16, (h + 15) / 16);
-    svgf_reproject_kernel<<<g, b, 0, stream>>>(c, reinterpret_cast<const float4*>(st.color_history),
-                                               reinterpret_cast<const float4*>(st.moments_history),
-                                               reinterpret_cast<const float4*>(st.normal_history), st.depth_history, w,
-                                               h, s.z_threshold, s.normal_threshold);
+    svgf_reproject_kernel<<<g, b, 0, stream>>>(c, color_history, moments_history, normal_history, depth_history, w, h,
+                                               s.z_threshold, s.normal_threshold);
     svgf_filter_moments_kernel<<<g, b, 0, stream>>>(c, c.ping, w, h);
     cudaMemcpyAsync(c.temp, c.ping, (size_t)n * 16, cudaMemcpyDeviceToDevice, stream);
     const float4* src = c.temp;
     float4* bufs[2] = {c.ping, c.pong};
     if (s.atrous_iterations < 1) {
-        cudaMemcpyAsync(st.color_history, c.temp, (size_t)n * 16, cudaMemcpyDeviceToDevice, stream);
+        cudaMemcpyAsync(color_history, c.temp, (size_t)n * 16, cudaMemcpyDeviceToDevice, stream);
     }
     for (int it = 0; it < s.atrous_iterations; it++) {
         float4* dst = bufs[it & 1];
-        svgf_atrous_kernel<<<g, b, 0, stream>>>(src, c, dst, reinterpret_cast<float4*>(st.color_history), w, h, it);
+        svgf_atrous_kernel<<<g, b, 0, stream>>>(src, c, dst, color_history, w, h, it);
         src = dst;
     }
-    svgf_update_history_kernel<<<(n + 255) / 256, 256, 0, stream>>>(c, reinterpret_cast<float4*>(st.moments_history),
-                                                                     reinterpret_cast<float4*>(st.normal_history),
-                                                                     st.depth_history, n);
-    count_launches(5 + (unsigned)s.atrous_iterations);
-    *result = reinterpret_cast<float*>(const_cast<float4*>(src));
+    svgf_update_history_kernel<<<(n + 255) / 256, 256, 0, stream>>>(c, moments_history, normal_history, depth_history,
+                                                                     n);
+    count_launches(4 + (unsigned)s.atrous_iterations);
+    *result = src;
     return cudaGetLastError();
 }
 
@@ -636,5 +653,43 @@ extern "C" VptStatus vpt_eaw_denoise_rgba_noalloc(const float* color, const floa
     float* pong = (iterations % 2 == 1) ? scratch : out;
     float* result = nullptr;
     cudaError_t e = vpt::eaw_denoise(color, position, normal, width, height, st, ping, pong, &result, s);
+    return e == cudaSuccess ? VPT_OK : VPT_ERR_CUDA;
+}
+
+// One SVGF frame on caller-prepared maps and history (see include/vpt_b200.h).
+extern "C" VptStatus vpt_svgf_filter(const float* noisy_rgba, const float* normal_rgba, const float* depth,
+                                     const float* depth_fwidth, const float* motion, float* color_history,
+                                     float* moments_history, float* normal_history, float* depth_history, int width,
+                                     int height, float z_threshold, float normal_threshold, int iterations,
+                                     float* out_rgba, void* stream) {
+    if (!noisy_rgba || !normal_rgba || !depth || !depth_fwidth || !motion || !color_history || !moments_history ||
+        !normal_history || !depth_history || !out_rgba || width <= 0 || height <= 0 || iterations < 0 ||
+        iterations > 10)
+        return VPT_ERR_ARG;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const size_t n = (size_t)width * height;
+    float* scratch = nullptr;
+    if (cudaMallocAsync(reinterpret_cast<void**>(&scratch), n * 16 * 4, s) != cudaSuccess) return VPT_ERR_OOM;
+    vpt::SvgfCur c;
+    c.noisy = reinterpret_cast<float4*>(const_cast<float*>(noisy_rgba));
+    c.normal = reinterpret_cast<float4*>(const_cast<float*>(normal_rgba));
+    c.depth = const_cast<float*>(depth);
+    c.fwidth = const_cast<float*>(depth_fwidth);
+    c.motion = reinterpret_cast<float2*>(const_cast<float*>(motion));
+    c.moments = reinterpret_cast<float4*>(scratch);
+    c.temp = reinterpret_cast<float4*>(scratch + n * 4);
+    c.ping = reinterpret_cast<float4*>(scratch + n * 8);
+    c.pong = reinterpret_cast<float4*>(scratch + n * 12);
+    vpt::SvgfSettings st;
+    st.z_threshold = z_threshold;
+    st.normal_threshold = normal_threshold;
+    st.atrous_iterations = iterations;
+    const float4* res = nullptr;
+    cudaError_t e = vpt::svgf_filter_passes(c, reinterpret_cast<float4*>(color_history),
+                                            reinterpret_cast<float4*>(moments_history),
+                                            reinterpret_cast<float4*>(normal_history), depth_history, width, height, st,
+                                            s, &res);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out_rgba, res, n * 16, cudaMemcpyDeviceToDevice, s);
+    cudaFreeAsync(scratch, s);
     return e == cudaSuccess ? VPT_OK : VPT_ERR_CUDA;
 }

@@ -342,6 +342,16 @@ VptStatus vpt_eaw_denoise_rgba_noalloc(const float* color, const float* position
                                        int height, int iterations, float phi_color, float phi_position,
                                        float phi_normal, int ref_compute_quirk, float* out, void* stream);
 
+/* One frame of SVGF (Data/Shaders/Denoiser/SVGF/SVGF.glsl: reprojection, moments filter, `iterations`
+ * a-trous passes, history update) on caller-prepared maps: noisy and normal rgba (normal.w unused),
+ * depth, depth fwidth and screen-space motion (2 floats per pixel, previous = current - motion), and
+ * the caller's history (colour rgba, moments rgba (mean, second moment, history length), normal
+ * rgba, depth), updated in place.  Device arrays, width*height pixels. */
+VptStatus vpt_svgf_filter(const float* noisy_rgba, const float* normal_rgba, const float* depth,
+                          const float* depth_fwidth, const float* motion, float* color_history,
+                          float* moments_history, float* normal_history, float* depth_history, int width, int height,
+                          float z_threshold, float normal_threshold, int iterations, float* out_rgba, void* stream);
+
 /* ---- learned denoiser network (no reference counterpart: the reference runs a TorchScript model
  * through libtorch, src/Denoiser/PyTorchDenoiser.cpp:637-800, and has no training code).  A U-Net of
  * 3x3 convolutions predicting per-pixel 5x5 kernels, forward and backward on tcgen05 tensor cores.

@@ -64,6 +64,7 @@ def load():
         lib.oracle_rrt_params.argtypes = [c_void_p, c_void_p, c_void_p, c_int, c_float, c_int, c_void_p]
         lib.oracle_occupancy.argtypes = [c_void_p, c_int, c_int, c_int, c_int, c_int, c_float, c_void_p]
         lib.oracle_env_pyramid.argtypes = [c_void_p, c_int, c_int, c_int, c_void_p]
+        lib.oracle_svgf_frame.argtypes = [c_void_p] * 9 + [c_int, c_int, c_float, c_float, c_int, c_void_p]
         lib.oracle_eaw.argtypes = [c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_float, c_float, c_float,
                                    c_int, c_void_p]
         lib.oracle_rng_stream.argtypes = [c_uint32, c_int, c_void_p, c_void_p]
@@ -144,6 +145,21 @@ def env_pyramid(rgba: np.ndarray, levels: int = 12) -> np.ndarray:
     total = sum((1 << (levels - l)) ** 2 for l in range(levels))
     out = np.empty(total, np.float32)
     load().oracle_env_pyramid(_p(np.ascontiguousarray(rgba, np.float32)), w, h, levels, _p(out))
+    return out
+
+
+def svgf_frame(noisy, normal, depth, fwidth, motion, history, z_threshold, normal_threshold, iterations):
+    """One SVGF frame on prepared maps (noisy / normal [h, w, 4], depth / fwidth [h, w], motion [h, w, 2]);
+    history: dict of color [h,w,4], moments [h,w,4], normal [h,w,4], depth [h,w] (float32, updated in
+    place).  Returns the filtered rgba [h, w, 4]."""
+    h, w = depth.shape
+    arrs = [np.ascontiguousarray(a, np.float32) for a in (noisy, normal, depth, fwidth, motion)]
+    for k in ("color", "moments", "normal", "depth"):
+        assert history[k].dtype == np.float32 and history[k].flags["C_CONTIGUOUS"]
+    out = np.zeros((h, w, 4), np.float32)
+    load().oracle_svgf_frame(*[_p(a) for a in arrs], _p(history["color"]), _p(history["moments"]),
+                             _p(history["normal"]), _p(history["depth"]), w, h, z_threshold, normal_threshold,
+                             iterations, _p(out))
     return out
 
 

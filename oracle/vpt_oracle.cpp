@@ -1429,6 +1429,204 @@ void oracle_env_pyramid(const float* rgba, int w, int h, int levels, float* pyra
 }
 
 // EAWDenoise.glsl:216-314 (compute path) / 92-158 (fragment path colour weight)
+// ---- SVGF (Data/Shaders/Denoiser/SVGF/SVGF.glsl; compute_weight svgf_common.glsl:29-41) ----
+// One frame of the filter on prepared maps (all w*h, rgba = 4 floats): the reprojection pass
+// (SVGF.glsl:210-267 with is_reprj_valid :80-94, try_2x2_tap :96-147, try_3x3_bilat :149-193), the
+// moments filter (:286-347), `iterations` a-trous passes (:401-495; iteration 0 refreshes the colour
+// history) and the history update (moments, normal, depth of this frame).  Two choices where the
+// shader's result is not defined: the moments filter reads the pre-filter values of its neighbours
+// (the shader filters temp_accum in place while neighbours read it), and filter_variance clamps its
+// 3x3 reads to the image (the shader's texelFetch may leave it).
+static float svgf_weight_o(float cd, float od, float phi_d, const float* cn, const float* on, float cc, float oc,
+                           float phi_c) {
+    float wn = powf(std::max(0.0f, (cn[0] * on[0] + cn[1] * on[1]) + cn[2] * on[2]), 128.0f);
+    float wz = (phi_d == 0.0f) ? 0.0f : fabsf(cd - od) / phi_d;
+    float wc = fabsf(cc - oc) * 2.0f / phi_c;
+    return expf(0.0f - std::max(wc, 0.0f) - std::max(wz, 0.0f)) * wn;
+}
+
+void oracle_svgf_frame(const float* noisy, const float* normal, const float* depth, const float* fwidth,
+                       const float* motion, float* color_hist, float* moments_hist, float* normal_hist,
+                       float* depth_hist, int w, int h, float zt, float nt, int iterations, float* out) {
+    const size_t n = (size_t)w * h;
+    std::vector<float> moments(n * 4), temp(n * 4), filt(n * 4), a(n * 4), b(n * 4);
+    auto valid = [&](int x, int y, float z, float zp, const float* nn, const float* np) {
+        if (x < 1 || y < 1 || x > w - 1 || y > h - 1) return false;
+        if (fabsf(zp - z) > zt) return false;
+        float dx = np[0] - nn[0], dy = np[1] - nn[1], dz = np[2] - nn[2];
+        return !(sqrtf((dx * dx + dy * dy) + dz * dz) > nt);
+    };
+    for (int y = 0; y < h; y++)
+        for (int x = 0; x < w; x++) {
+            const size_t i = (size_t)y * w + x;
+            const float mvx = motion[2 * i], mvy = motion[2 * i + 1];
+            int pxp = (int)(0.5f + ((float)x - mvx)), pyp = (int)(0.5f + ((float)y - mvy));
+            float pm0 = 0.0f, pm1 = 0.0f, hist_len = 0.0f;
+            bool ok = !(pxp < 0 || pyp < 0 || pxp >= w || pyp >= h);
+            if (ok) {
+                const float* r = moments_hist + ((size_t)pyp * w + pxp) * 4;
+                pm0 = r[0];
+                pm1 = r[1];
+                hist_len = r[2];
+            }
+            const float* col = noisy + i * 4;
+            float last[3] = {color_hist[i * 4], color_hist[i * 4 + 1], color_hist[i * 4 + 2]};
+            if (ok) {
+                float fx = 0.01f + ((float)x - mvx), fy = 0.01f + ((float)y - mvy);
+                int ix = (int)fx, iy = (int)fy;
+                const float d = depth[i];
+                const float* nn = normal + i * 4;
+                const int ox[4] = {0, 0, 1, 1}, oy[4] = {0, 1, 0, 1};
+                bool vs[4], found = false;
+                for (int k = 0; k < 4; k++) {
+                    int qx = ix + ox[k], qy = iy + oy[k];
+                    bool inside = qx >= 0 && qy >= 0 && qx < w && qy < h;
+                    vs[k] = inside && valid(qx, qy, d, depth_hist[(size_t)qy * w + qx], nn,
+                                            normal_hist + ((size_t)qy * w + qx) * 4);
+                    found = found || vs[k];
+                }
+                if (found) {
+                    float ax = fx - floorf(fx), ay = fy - floorf(fy);
+                    const float wk[4] = {(1 - ax) * (1 - ay), ax * (1 - ay), (1 - ax) * ay, ax * ay};
+                    float cb[3] = {0, 0, 0}, mb[2] = {0, 0}, sw = 0.0f;
+                    for (int k = 0; k < 4; k++) {
+                        if (!vs[k]) continue;
+                        const size_t q = (size_t)(iy + oy[k]) * w + (ix + ox[k]);
+                        mb[0] += wk[k] * moments_hist[q * 4];
+                        mb[1] += wk[k] * moments_hist[q * 4 + 1];
+                        for (int c = 0; c < 3; c++) cb[c] += wk[k] * color_hist[q * 4 + c];
+                        sw += wk[k];
+                    }
+                    found = sw >= 0.001f;
+                    if (found) {
+                        for (int c = 0; c < 3; c++) last[c] = cb[c] / sw;
+                        pm0 = mb[0] / sw;
+                        pm1 = mb[1] / sw;
+                    }
+                }
+                if (!found) {
+                    float nv = 0.0f, fc[3] = {0, 0, 0}, fm[2] = {0, 0};
+                    for (int yy = -1; yy <= 1; yy++)
+                        for (int xx = -1; xx <= 1; xx++) {
+                            int qx = ix + xx, qy = iy + yy;
+                            if (qx < 1 || qy < 1 || qx >= w || qy >= h) continue;
+                            const size_t q = (size_t)qy * w + qx;
+                            if (valid(qx, qy, d, depth_hist[q], nn, normal_hist + q * 4)) {
+                                for (int c = 0; c < 3; c++) fc[c] += color_hist[q * 4 + c];
+                                fm[0] += moments_hist[q * 4];
+                                fm[1] += moments_hist[q * 4 + 1];
+                                nv += 1.0f;
+                            }
+                        }
+                    if (nv > 0.0f) {
+                        for (int c = 0; c < 3; c++) last[c] = fc[c] / nv;
+                        pm0 = fm[0] / nv;
+                        pm1 = fm[1] / nv;
+                        found = true;
+                    }
+                }
+                ok = found;
+            }
+            hist_len = std::min(ok ? hist_len + 1.0f : 1.0f, 32.0f);
+            const float a_c = ok ? std::max(0.01f, 1.0f / hist_len) : 1.0f;
+            const float a_m = ok ? std::max(0.2f, 1.0f / hist_len) : 1.0f;
+            float m1 = col[0], m2 = m1 * m1;
+            m1 = pm0 * (1.0f - a_m) + m1 * a_m;
+            m2 = pm1 * (1.0f - a_m) + m2 * a_m;
+            const float var = std::max(0.0f, m2 - m1 * m1);
+            moments[i * 4] = m1;
+            moments[i * 4 + 1] = m2;
+            moments[i * 4 + 2] = hist_len;
+            moments[i * 4 + 3] = 0.0f;
+            for (int c = 0; c < 3; c++) temp[i * 4 + c] = last[c] * (1.0f - a_c) + col[c] * a_c;
+            temp[i * 4 + 3] = var;
+        }
+    // moments filter
+    for (int y = 0; y < h; y++)
+        for (int x = 0; x < w; x++) {
+            const size_t i = (size_t)y * w + x;
+            const float hl = moments[i * 4 + 2];
+            if (hl >= 4.0f) {
+                for (int c = 0; c < 4; c++) filt[i * 4 + c] = temp[i * 4 + c];
+                continue;
+            }
+            const float cd = depth[i], cfw = fwidth[i];
+            const float* cn = normal + i * 4;
+            float sw = 0.0f, sc[3] = {0, 0, 0}, sm[2] = {0, 0};
+            for (int yy = -3; yy <= 3; yy++)
+                for (int xx = -3; xx <= 3; xx++) {
+                    int qx = x + xx, qy = y + yy;
+                    if (qx < 0 || qy < 0 || qx >= w || qy >= h) continue;
+                    const size_t q = (size_t)qy * w + qx;
+                    float wt = svgf_weight_o(cd, depth[q], fabsf(cfw) + 0.0001f, cn, normal + q * 4, temp[i * 4],
+                                             temp[q * 4], 10.0f);
+                    sw += wt;
+                    for (int c = 0; c < 3; c++) sc[c] += wt * temp[q * 4 + c];
+                    sm[0] += wt * moments[q * 4];
+                    sm[1] += wt * moments[q * 4 + 1];
+                }
+            sw = std::max(sw, 1e-6f);
+            for (int c = 0; c < 3; c++) filt[i * 4 + c] = sc[c] / sw;
+            const float m0 = sm[0] / sw, m1v = sm[1] / sw;
+            float var = m1v - m0 * m0;
+            var *= 4.0f / hl;
+            filt[i * 4 + 3] = var;
+        }
+    // a-trous
+    const float* src = filt.data();
+    if (iterations < 1) std::copy(filt.begin(), filt.end(), color_hist);
+    const float kv2[2][2] = {{1.0f / 4.0f, 1.0f / 8.0f}, {1.0f / 8.0f, 1.0f / 16.0f}};
+    const float kvals[3] = {1.0f, 2.0f / 3.0f, 1.0f / 6.0f};
+    for (int it = 0; it < iterations; it++) {
+        float* dst = (it & 1) ? b.data() : a.data();
+        const int step = 1 << it;
+        for (int y = 0; y < h; y++)
+            for (int x = 0; x < w; x++) {
+                const size_t i = (size_t)y * w + x;
+                const float* cc = src + i * 4;
+                float fv = 0.0f;
+                for (int yy = -1; yy <= 1; yy++)
+                    for (int xx = -1; xx <= 1; xx++) {
+                        int qx = std::min(std::max(x + xx, 0), w - 1), qy = std::min(std::max(y + yy, 0), h - 1);
+                        fv += src[((size_t)qy * w + qx) * 4 + 3] * kv2[abs(xx)][abs(yy)];
+                    }
+                const float* cn = normal + i * 4;
+                const float cz = depth[i], cfw = fwidth[i];
+                const float phi_c = sqrtf(std::max(0.0f, 1e-10f + fv));
+                float accw = kvals[0] * kvals[0];
+                float sum[4] = {cc[0] * accw, cc[1] * accw, cc[2] * accw, cc[3] * accw};
+                for (int yy = -2; yy <= 2; yy++)
+                    for (int xx = -2; xx <= 2; xx++) {
+                        int qx = x + xx * step, qy = y + yy * step;
+                        bool inside = qx >= 0 && qy >= 0 && qx < w && qy < h;
+                        if (!inside || (xx == 0 && yy == 0)) continue;
+                        const float kval = kvals[abs(xx)] * kvals[abs(yy)];
+                        const size_t q = (size_t)qy * w + qx;
+                        const float len = sqrtf((float)(xx * xx + yy * yy));
+                        const float wt = svgf_weight_o(cz, depth[q], fabsf(cfw * len * (float)step) + 0.0001f, cn,
+                                                       normal + q * 4, cc[0], src[q * 4], phi_c) *
+                                         kval;
+                        for (int c = 0; c < 3; c++) sum[c] += wt * src[q * 4 + c];
+                        sum[3] += wt * wt * src[q * 4 + 3];
+                        accw += wt;
+                    }
+                for (int c = 0; c < 3; c++) dst[i * 4 + c] = sum[c] / accw;
+                dst[i * 4 + 3] = sum[3] / (accw * accw);
+                if (it == 0)
+                    for (int c = 0; c < 4; c++) color_hist[i * 4 + c] = dst[i * 4 + c];
+            }
+        src = dst;
+    }
+    for (size_t i = 0; i < n; i++) {
+        for (int c = 0; c < 4; c++) {
+            moments_hist[i * 4 + c] = moments[i * 4 + c];
+            normal_hist[i * 4 + c] = normal[i * 4 + c];
+            out[i * 4 + c] = src[i * 4 + c];
+        }
+        depth_hist[i] = depth[i];
+    }
+}
+
 void oracle_eaw(const float* color, const float* pos, const float* nrm, int w, int h, int iterations, float phi_c,
                 float phi_p, float phi_n, int quirk, float* out) {
     std::vector<float> a(color, color + (size_t)w * h * 4), b((size_t)w * h * 4);

@@ -79,6 +79,9 @@ void oracle_occupancy(const float* dens, int nx, int ny, int nz, int bs, int hal
 void oracle_env_pyramid(const float* rgba, int w, int h, int levels, float* pyramid);
 
 /* EAW a-trous chain on RGBA images (position/normal may be NULL). */
+void oracle_svgf_frame(const float* noisy, const float* normal, const float* depth, const float* fwidth,
+                       const float* motion, float* color_hist, float* moments_hist, float* normal_hist,
+                       float* depth_hist, int w, int h, float zt, float nt, int iterations, float* out);
 void oracle_eaw(const float* color, const float* pos, const float* nrm, int w, int h, int iterations,
                 float phi_c, float phi_p, float phi_n, int quirk, float* out);
 
