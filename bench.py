@@ -60,6 +60,39 @@ def peaks():
     return 6650.0, "fallback"
 
 
+def gather_rates(lib, stream):
+    """Random 32-byte-sector gather rates (GB/s of sectors) of this GPU: a 512 MiB buffer (HBM) and a
+    32 MiB buffer (L2), timed with CUDA events after a warm-up launch."""
+    import ctypes
+    import torch
+    out = {}
+    sink = torch.zeros(1, device="cuda")
+    cs = ctypes.c_void_p(stream.cuda_stream)
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    for name, mib in (("hbm", 512), ("l2", 32)):
+        buf = torch.rand(mib * 1024 * 1024 // 4, device="cuda")
+        blocks, loads = sms * 8, 512
+        for _ in range(2):
+            vpt_check(lib.vpt_gather_bench(ctypes.c_void_p(buf.data_ptr()), buf.numel() * 4, blocks, loads, 7,
+                                           ctypes.c_void_p(sink.data_ptr()), cs))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for r in range(5):
+            vpt_check(lib.vpt_gather_bench(ctypes.c_void_p(buf.data_ptr()), buf.numel() * 4, blocks, loads, 11 + r,
+                                           ctypes.c_void_p(sink.data_ptr()), cs))
+        e1.record(stream)
+        torch.cuda.synchronize()
+        sectors = 5.0 * blocks * 256 * loads
+        out[name] = sectors * BYTES_PER_LOOKUP / (e0.elapsed_time(e1) / 1e3) / 1e9
+        del buf
+    return out
+
+
+def vpt_check(st):
+    if st != 0:
+        raise RuntimeError(f"vpt_gather_bench failed with status {st}")
+
+
 def workload_config(n_gpus):
     return {"workload": f"dense {GRID}^3 fBm cloud, {RES}x{RES}, {SPP_PER_STEP} spp/step, delta tracking "
                         f"(+ratio/decomposition/residual-ratio/NEE timed separately)",
@@ -278,6 +311,13 @@ def run_ours(args):
            "h2d_bytes_per_step": GRID ** 3 * 4, "d2h_bytes_per_step": int(res.numel() * 4),
            "path": "vpt.set_density_field(pinned host grid) + vpt.render_frame(cpu tensor)"}
 
+    gather = gather_rates(lib, stream)
+    gather_roofline = {"unit": "GB/s", "achieved": achieved, "hbm_random_sector": gather["hbm"],
+                       "l2_random_sector": gather["l2"], "frac_of_hbm_random_sector": achieved / gather["hbm"],
+                       "frac_of_l2_random_sector": achieved / gather["l2"],
+                       "note": "same achieved bytes as roofline, against this GPU's random 32 B sector gather rate "
+                               "(vpt_gather_bench, measured in this run)"}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(lib, ctx, vpt)
@@ -303,6 +343,7 @@ def run_ours(args):
                          "note": f"algorithmic bytes = density lookups x {BYTES_PER_LOOKUP} B sector; peak {peak_kind}"},
             "lookups_per_s": lookups / (ms_total / 1e3) * world,
             "lookups_per_path": lookups / max(1, st["paths"]),
+            "gather_roofline": gather_roofline,
             "per_tracker": per_tracker, "schedules_delta": schedules, "e2e": e2e, "gpu_launches": int(launches), "clocks": clock_info,
         }
         if cpu is not None:
@@ -321,14 +362,15 @@ def run_ours(args):
 
 
 # Learned denoiser: a kernel-predicting U-Net (widths 32-64-96-128-160, 13x13 kernels) trained on the
-# GPU by this package's tcgen05 kernels on tracer-generated pairs (32 seeded cloud scenes at 256^2:
-# noisy renders at 1..256 spp with albedo / normal / depth / transmittance features against
-# 2048-spp targets from disjoint frames; Adam, batch 8, 2000 steps), then the time each method needs
+# GPU by this package's tcgen05 kernels on tracer-generated pairs (64 seeded cloud scenes at 256^2:
+# noisy renders at 1..256 spp with albedo / normal / depth / transmittance features against 2048-spp
+# targets from disjoint frames; Adam, batch 8, 4000 steps, learning
+# rate cosine-annealed from 5e-4 to 1e-5), then the time each method needs
 # to reach relMSE <= 1e-3 on a held-out scene (256^3 cloud, 512^2, max 128 bounces) against its
 # FP64-accumulated 16384-spp render: plain accumulation, EAW (iteration count 1..5 chosen per sample
 # count by the lowest error, i.e. tuned with the reference in hand) and the learned denoiser.
-LEARNED = dict(scenes=32, size=256, spp_levels=(1, 2, 4, 8, 16, 64, 256), target_spp=2048, steps=2000, batch=8,
-               lr=3e-4, kernel_size=13, grid=128)
+LEARNED = dict(scenes=64, size=256, spp_levels=(1, 2, 4, 8, 16, 64, 256), target_spp=2048, steps=4000, batch=8,
+               lr=5e-4, lr_end=1e-5, kernel_size=13, grid=128)
 EVAL = dict(seed=77777, res=512, grid=256, max_bounces=128, ref_spp=16384,
             levels=(1, 2, 4, 8, 16, 32, 64, 128, 256, 512, 1024, 2048, 4096), target=1e-3)
 
@@ -358,7 +400,7 @@ def run_learned(vpt, lib, ctx, small):
 
     cfg, ev = dict(LEARNED), dict(EVAL)
     if small:
-        cfg.update(scenes=8, size=128, steps=300, target_spp=512)
+        cfg.update(scenes=8, size=128, steps=300, target_spp=512, lr_end=None)
         ev.update(res=256, grid=128, ref_spp=4096, levels=(1, 2, 4, 8, 16, 32, 64, 128, 256, 512))
     stream = torch.cuda.current_stream()
     cs = ctypes.c_void_p(stream.cuda_stream)
@@ -382,7 +424,7 @@ def run_learned(vpt, lib, ctx, small):
     conv_flop = sum(2 * 9 * L["cin"] * L["cout"] * (P0 >> (2 * L["level"])) * (2 if L["name"] == "enc0a" else 3)
                     for L in net.layers)
     net = ld.KpnUNet(seed=0, kernel_size=cfg["kernel_size"])
-    hist = ld.train(net, data, cfg["steps"], cfg["batch"], cfg["lr"], seed=1)
+    hist = ld.train(net, data, cfg["steps"], cfg["batch"], cfg["lr"], seed=1, lr_end=cfg.get("lr_end"))
 
     # held-out scene: FP64 reference, then the error curves
     sc = ld.sample_scene(ev["seed"])
@@ -416,7 +458,7 @@ def run_learned(vpt, lib, ctx, small):
     vpt.set_use_feature_maps(["Albedo", "Normal", "Depth", "Transmittance"])
     vpt.set_denoiser("Edge-Avoiding À-Trous Wavelet Transform")
     vpt.set_denoiser_property("iterations", "1")
-    ms_feat = frame_ms(64)
+    ms_feat = frame_ms(64)  # with the feature maps: the denoised methods' render cost
     vpt.set_frame_index(0)
 
     def timed(fn):

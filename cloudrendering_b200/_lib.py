@@ -109,6 +109,7 @@ SIGNATURES = {
     "vpt_kpn_reproject": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_int, c_int, c_void_p, c_void_p]),
     "vpt_eaw_denoise_rgba_noalloc": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_float, c_float,
                                              c_float, c_int, c_void_p, c_void_p]),
+    "vpt_gather_bench": (c_int, [c_void_p, ctypes.c_size_t, c_int, c_int, c_uint32, c_void_p, c_void_p]),
     "vpt_svgf_filter": (c_int, [c_void_p] * 9 + [c_int, c_int, c_float, c_float, c_int, c_void_p, c_void_p]),
     # learned denoiser network (csrc/vpt_unet.cu)
     "vpt_unet_conv3x3": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_int,
@@ -129,8 +130,8 @@ SIGNATURES = {
     "vpt_unet_adam": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, ctypes.c_long, c_float, c_float,
                               c_float, c_float, c_int, c_float, c_void_p]),
     "vpt_unet_to_bf16": (c_int, [c_void_p, c_void_p, ctypes.c_long, c_void_p]),
-    "vpt_unet_pack_input": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int,
-                                    c_int, c_int, c_void_p]),
+    "vpt_unet_pack_input": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                    c_int, c_int, c_int, c_void_p]),
     "vpt_unet_head_blocks": (c_int, [c_int, c_int, c_int]),
     "vpt_unet_kpn_head": (c_int, [c_void_p, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int,
                                   c_int, c_int, c_float, c_void_p]),

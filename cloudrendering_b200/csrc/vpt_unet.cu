@@ -842,16 +842,19 @@ __global__ void f32_to_bf16_kernel(const float* __restrict__ in, bf16* __restric
 // ---------------------------------------------------------------------------------------------
 // network input and the kernel-prediction head
 // ---------------------------------------------------------------------------------------------
-constexpr int kInputChannels = 16;  // 12 used: log radiance 3, albedo 3, normal 3, depth 1, transmittance 1,
-                                    // noise level 1
+constexpr int kInputChannels = 16;  // 15 used: log radiance 3, albedo 3, normal 3, depth 1, transmittance 1,
+                                    // noise level 1, log standard error of the pixel mean 3
 
 // planes: [n][3][h][w] radiance (mean of the frames rendered so far), albedo [n][3][h][w], normal
 // [n][3][h][w], depth [n][h][w], transmittance [n][h][w] (each may be null -> zeros); noise_level
-// [n] (1 / sqrt(frames) of each image; may be null -> zeros)
+// [n] (1 / sqrt(frames) of each image; may be null -> zeros); second_moment [n][3][h][w] (mean of the
+// squared per-frame radiance; with noise_level gives log1p of the standard error of the pixel mean,
+// sqrt(max(0, m2 - mean^2)) / sqrt(frames); may be null -> zeros)
 __global__ void pack_input_kernel(const float* __restrict__ radiance, const float* __restrict__ albedo,
                                   const float* __restrict__ normal, const float* __restrict__ depth,
                                   const float* __restrict__ transmittance, const float* __restrict__ noise_level,
-                                  bf16* __restrict__ out, int n, int h, int w) {
+                                  const float* __restrict__ second_moment, bf16* __restrict__ out, int n, int h,
+                                  int w) {
     const long plane = (long)h * w, total = (long)n * plane;
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
         const long b = i / plane, q = i % plane;
@@ -864,7 +867,15 @@ __global__ void pack_input_kernel(const float* __restrict__ radiance, const floa
         }
         if (depth) f[9] = depth[b * plane + q];
         if (transmittance) f[10] = transmittance[b * plane + q];
-        if (noise_level) f[11] = noise_level[b];
+        if (noise_level) {
+            f[11] = noise_level[b];
+            if (second_moment)
+                for (int c = 0; c < 3; ++c) {
+                    const float m1 = radiance[(b * 3 + c) * plane + q];
+                    const float m2 = second_moment[(b * 3 + c) * plane + q];
+                    f[12 + c] = log1pf(sqrtf(fmaxf(0.0f, m2 - m1 * m1)) * noise_level[b]);
+                }
+        }
         float lo[8], hi[8];
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
@@ -1267,11 +1278,11 @@ VptStatus vpt_unet_to_bf16(const float* in, void* out, long count, void* stream)
 }
 
 VptStatus vpt_unet_pack_input(const float* radiance, const float* albedo, const float* normal, const float* depth,
-                              const float* transmittance, const float* noise_level, void* out, int n, int h, int w,
-                              void* stream) {
+                              const float* transmittance, const float* noise_level, const float* second_moment,
+                              void* out, int n, int h, int w, void* stream) {
     if (!radiance || !out || n <= 0 || h <= 0 || w <= 0) return VPT_ERR_ARG;
     pack_input_kernel<<<grid_for((long)n * h * w, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
-        radiance, albedo, normal, depth, transmittance, noise_level, static_cast<bf16*>(out), n, h, w);
+        radiance, albedo, normal, depth, transmittance, noise_level, second_moment, static_cast<bf16*>(out), n, h, w);
     vpt::count_launches(1);
     return cudaGetLastError() == cudaSuccess ? VPT_OK : VPT_ERR_CUDA;
 }

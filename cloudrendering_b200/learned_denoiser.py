@@ -11,7 +11,8 @@ device memory and orders the launches on its current stream.
 
 Training pairs come from the tracer itself: a noisy render of a seeded cloud scene at a few sample
 counts (radiance plus albedo / normal / depth / primary-ray transmittance features averaged over the
-same frames) against a many-sample render of the same scene from a disjoint frame range.  The loss
+same frames; optionally the per-pixel second moment of the frames' radiance, from which the network
+input carries the standard error of each pixel's mean) against a many-sample render of the same scene from a disjoint frame range.  The loss
 is the relative MSE sum (d - t)^2 / (t^2 + 0.01) / count the evaluation uses.
 
 Parameters are saved as ``<dir>/weights.npz`` (fp32) with ``<dir>/model_info.json`` in the
@@ -108,11 +109,11 @@ class KpnUNet:
         g = np.random.default_rng(seed)
         host = np.zeros(self.count, np.float32)
         for L in self.layers:
-            cin_used = 12 if L["name"] == "enc0a" else L["cin"]
+            cin_used = 15 if L["name"] == "enc0a" else L["cin"]
             std = math.sqrt(2.0 / (9 * cin_used)) if L["name"] != "head" else 1e-3
             w = (g.standard_normal((L["cout"], 9, L["cin"])) * std).astype(np.float32)
             if L["name"] == "enc0a":
-                w[:, :, 12:] = 0.0
+                w[:, :, 15:] = 0.0
             host[L["w_off"]:L["w_off"] + w.size] = w.reshape(-1)
         self.set_parameters(host)
 
@@ -266,11 +267,12 @@ class KpnUNet:
         self._rotate_all()
 
     # ---- the kernel-prediction head ----
-    def pack(self, radiance, albedo=None, normal=None, depth=None, transmittance=None, noise_level=None):
+    def pack(self, radiance, albedo=None, normal=None, depth=None, transmittance=None, noise_level=None,
+             second_moment=None):
         n, _, h, w = radiance.shape
         x0 = self.buf("input", (n, h, w, IN_CHANNELS))
         self._call("vpt_unet_pack_input", _p(radiance), _p(albedo), _p(normal), _p(depth), _p(transmittance),
-                   _p(noise_level), _p(x0), n, h, w, self._stream())
+                   _p(noise_level), _p(second_moment), _p(x0), n, h, w, self._stream())
         return x0
 
     def head(self, logits, radiance, target=None, out=None):
@@ -288,16 +290,17 @@ class KpnUNet:
 
     def train_step(self, batch: dict, lr: float) -> torch.Tensor:
         x0 = self.pack(batch["radiance"], batch.get("albedo"), batch.get("normal"), batch.get("depth"),
-                       batch.get("transmittance"), batch.get("noise_level"))
+                       batch.get("transmittance"), batch.get("noise_level"), batch.get("second_moment"))
         logits = self.forward(x0)
         _, loss, dl = self.head(logits, batch["radiance"], batch["target"])
         self.backward(dl)
         self.adam_step(lr)
         return loss
 
-    def denoise(self, radiance, albedo=None, normal=None, depth=None, transmittance=None, noise_level=None):
+    def denoise(self, radiance, albedo=None, normal=None, depth=None, transmittance=None, noise_level=None,
+                second_moment=None):
         """Denoised radiance [n, 3, h, w] fp32 (h, w multiples of 16)."""
-        x0 = self.pack(radiance, albedo, normal, depth, transmittance, noise_level)
+        x0 = self.pack(radiance, albedo, normal, depth, transmittance, noise_level, second_moment)
         logits = self.forward(x0)
         out = torch.empty_like(radiance)
         self.head(logits, radiance, None, out)
@@ -379,12 +382,14 @@ TARGET_FRAME_ORIGIN = 1 << 24  # targets use frames disjoint from the noisy inpu
 
 
 def render_scene_levels(vpt, sc: dict, size: int, spp_levels: Sequence[int], target_spp: int, grid: int = 128,
-                        max_bounces: int = 64) -> dict:
+                        max_bounces: int = 64, second_moment: bool = False) -> dict:
     """Noisy renders of one scene after each sample count in spp_levels (nested: the frames of a
-    level include the previous level's) with their features, and the target (target_spp frames
-    from a disjoint frame range), all on the GPU."""
+    level include the previous level's) with their features (and, with second_moment, the mean
+    square of the frames' radiance), and the target (target_spp frames from a disjoint frame
+    range), all on the GPU."""
     setup_scene(vpt, sc, grid, max_bounces)
     vpt.set_use_feature_maps(["Albedo", "Normal", "Depth", "Transmittance"])
+    vpt.set_collect_statistics(second_moment)
     img = torch.zeros((3, size, size), dtype=torch.float32, device="cuda")
     vpt.set_frame_index(0)
     levels = []
@@ -392,8 +397,10 @@ def render_scene_levels(vpt, sc: dict, size: int, spp_levels: Sequence[int], tar
     for spp in spp_levels:
         rad = vpt.render_frame(img, spp - done).clone()
         done = spp
-        levels.append(dict(spp=spp, radiance=rad, **read_features(vpt, img)))
+        m2 = vpt.get_film_moments(size, size, spp)[1] if second_moment else None
+        levels.append(dict(spp=spp, radiance=rad, second_moment=m2, **read_features(vpt, img)))
     vpt.set_use_feature_maps([])
+    vpt.set_collect_statistics(False)
     vpt.set_frame_index(TARGET_FRAME_ORIGIN)
     left = target_spp
     tgt = None
@@ -411,7 +418,7 @@ class TrainingSet:
     radiance and features, and the scene's target."""
 
     def __init__(self, vpt, num_scenes: int, size: int = 256, spp_levels=(1, 4, 16, 64), target_spp: int = 1024,
-                 seed0: int = 1000, grid: int = 128):
+                 seed0: int = 1000, grid: int = 128, second_moment: bool = False):
         t0 = time.perf_counter()
         self.size = size
         self.spp_levels = tuple(spp_levels)
@@ -422,15 +429,19 @@ class TrainingSet:
         self.normal = torch.empty((S, L, 3, size, size), device=dev)
         self.depth = torch.empty((S, L, 1, size, size), device=dev)
         self.transmittance = torch.empty((S, L, 1, size, size), device=dev)
+        self.second_moment = torch.empty((S, L, 3, size, size), device=dev) if second_moment else None
         self.target = torch.empty((S, 3, size, size), device=dev)
         for s in range(S):
-            r = render_scene_levels(vpt, sample_scene(seed0 + s), size, self.spp_levels, target_spp, grid)
+            r = render_scene_levels(vpt, sample_scene(seed0 + s), size, self.spp_levels, target_spp, grid,
+                                    second_moment=second_moment)
             for j, lv in enumerate(r["levels"]):
                 self.radiance[s, j] = lv["radiance"]
                 self.albedo[s, j] = lv["albedo"]
                 self.normal[s, j] = lv["normal"]
                 self.depth[s, j] = lv["depth"]
                 self.transmittance[s, j] = lv["transmittance"]
+                if second_moment:
+                    self.second_moment[s, j] = lv["second_moment"]
             self.target[s] = r["target"]
         torch.cuda.synchronize()
         self.seconds = time.perf_counter() - t0
@@ -441,11 +452,16 @@ class TrainingSet:
         S, L = self.radiance.shape[:2]
         si = torch.from_numpy(rng.integers(0, S, batch_size)).cuda()
         li = torch.from_numpy(rng.integers(0, L, batch_size)).cuda()
-        out = {k: getattr(self, k)[si, li] for k in ("radiance", "albedo", "normal", "depth", "transmittance")}
+        keys = ["radiance", "albedo", "normal", "depth", "transmittance"]
+        if self.second_moment is not None:
+            keys.append("second_moment")
+        out = {k: getattr(self, k)[si, li] for k in keys}
         out["target"] = self.target[si]
         out["noise_level"] = (1.0 / torch.tensor(self.spp_levels, dtype=torch.float32, device="cuda")[li].sqrt())
         flip = rng.integers(0, 8)
-        for k in ("radiance", "albedo", "normal", "depth", "transmittance", "target"):
+        for k in list(out.keys()):
+            if k == "noise_level":
+                continue
             t = out[k]
             if flip & 1:
                 t = t.flip(-1)
@@ -460,8 +476,9 @@ class TrainingSet:
 
 
 def train(net: KpnUNet, data: TrainingSet, steps: int, batch_size: int = 8, lr: float = 1e-4, seed: int = 0,
-          log_every: int = 0) -> dict:
-    """Adam training; returns timing and the loss curve (mean loss per logging window)."""
+          log_every: int = 0, lr_end: Optional[float] = None) -> dict:
+    """Adam training (learning rate constant, or cosine-annealed from lr to lr_end); returns timing and
+    the loss curve (mean loss per logging window)."""
     rng = np.random.default_rng(seed)
     losses = []
     acc = torch.zeros((), dtype=torch.float32, device=net.device)
@@ -469,7 +486,8 @@ def train(net: KpnUNet, data: TrainingSet, steps: int, batch_size: int = 8, lr: 
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for i in range(steps):
-        loss = net.train_step(data.batch(rng, batch_size), lr)
+        step_lr = lr if lr_end is None else lr_end + 0.5 * (lr - lr_end) * (1.0 + math.cos(math.pi * i / steps))
+        loss = net.train_step(data.batch(rng, batch_size), step_lr)
         acc += loss
         if (i + 1) % window == 0:
             losses.append(float(acc.item()) / window)

@@ -624,6 +624,23 @@ def set_frame_index(first_frame: int) -> None:
     _c("vpt_set_frame_index", int(first_frame) & 0xFFFFFFFF)
 
 
+def set_collect_statistics(enabled: bool) -> None:
+    """Accumulates the per-pixel sum of squared frame radiance beside the FP64 film (no reference
+    counterpart; clears the accumulation when the state changes)."""
+    _c("vpt_set_collect_statistics", 1 if enabled else 0)
+
+
+def get_film_moments(width: int, height: int, frames: int):
+    """Mean and mean square of the accumulated frames' radiance, [3, H, W] float32 on the GPU
+    (statistics collection must be on)."""
+    s = torch.empty((height, width, 3), dtype=torch.float64, device=torch.device("cuda", S.device))
+    q = torch.empty_like(s)
+    _c("vpt_read_statistics", ctypes.c_void_p(s.data_ptr()), ctypes.c_void_p(q.data_ptr()), 1,
+       ctypes.c_void_p(torch.cuda.current_stream(s.device).cuda_stream))
+    inv = 1.0 / float(frames)
+    return ((s * inv).float().permute(2, 0, 1).contiguous(), (q * inv).float().permute(2, 0, 1).contiguous())
+
+
 def get_film_sum(width: int, height: int) -> torch.Tensor:
     """The FP64 film: the sum of the radiance of every accumulated frame, [3, H, W] float64 on the host."""
     _c("vpt_set_resolution", int(width), int(height))

@@ -352,6 +352,13 @@ VptStatus vpt_svgf_filter(const float* noisy_rgba, const float* normal_rgba, con
                           float* moments_history, float* normal_history, float* depth_history, int width, int height,
                           float z_threshold, float normal_threshold, int iterations, float* out_rgba, void* stream);
 
+/* Random-sector gather rate (the access of a density lookup): blocks x 256 threads each issue
+ * loads_per_thread (a multiple of 8) 4-byte loads at pseudo-random 32-byte-aligned offsets of
+ * `buffer` (bytes a power of two, non-negative floats).  Time it on `stream`; sectors per second = 
+ * blocks * 256 * (loads_per_thread / 8 * 8) / time. */
+VptStatus vpt_gather_bench(const float* buffer, size_t bytes, int blocks, int loads_per_thread, uint32_t seed,
+                           float* sink, void* stream);
+
 /* ---- learned denoiser network (no reference counterpart: the reference runs a TorchScript model
  * through libtorch, src/Denoiser/PyTorchDenoiser.cpp:637-800, and has no training code).  A U-Net of
  * 3x3 convolutions predicting per-pixel 5x5 kernels, forward and backward on tcgen05 tensor cores.
@@ -401,10 +408,12 @@ VptStatus vpt_unet_adam(float* param, void* param_bf16, float* m1, float* m2, co
                         float beta1, float beta2, float eps, int step, float grad_scale, void* stream);
 VptStatus vpt_unet_to_bf16(const float* in, void* out, long count, void* stream);
 /* network input [n][h][w][16] bf16 from planes [n][c][h][w]: log1p(radiance) 3, albedo 3, normal 3,
- * depth 1, transmittance 1, and noise_level[n] (1/sqrt(frames) per image) 1 (NULL gives zeros) */
+ * depth 1, transmittance 1, noise_level[n] (1/sqrt(frames) per image) 1, and from second_moment (mean
+ * of the squared per-frame radiance, [n][3][h][w]) log1p of the standard error of the pixel mean
+ * sqrt(max(0, m2 - mean^2)) * noise_level 3 (NULL inputs give zeros) */
 VptStatus vpt_unet_pack_input(const float* radiance, const float* albedo, const float* normal, const float* depth,
-                              const float* transmittance, const float* noise_level, void* out, int n, int h, int w,
-                              void* stream);
+                              const float* transmittance, const float* noise_level, const float* second_moment,
+                              void* out, int n, int h, int w, void* stream);
 int vpt_unet_head_blocks(int n, int h, int w);
 /* Kernel-prediction head (perPixelKernelCuda semantics, modules/kpn_module/src/Kernel.cu:38-135, with
  * the tap softmax fused): out[n][c][y][x] = sum_j softmax(logits[p][0 .. k*k-1])_j

@@ -120,9 +120,11 @@ def encoder_grad(d_cat, cat_off, d_pool, e) -> np.ndarray:
     return np.where(e > 0, acc, 0.0)
 
 
-def pack_input(radiance, albedo=None, normal=None, depth=None, transmittance=None, noise_level=None) -> np.ndarray:
+def pack_input(radiance, albedo=None, normal=None, depth=None, transmittance=None, noise_level=None,
+               second_moment=None) -> np.ndarray:
     """Network input [n,h,w,16]: log1p(max(radiance, 0)) 3, albedo 3, normal 3, depth 1,
-    transmittance 1, noise level (per image) 1, zeros 4 (planes [n][c][h][w])."""
+    transmittance 1, noise level (per image) 1, log1p(sqrt(max(0, m2 - mean^2)) * noise level) 3,
+    zero 1 (planes [n][c][h][w])."""
     r = np.asarray(radiance, np.float32)
     n, _, h, w = r.shape
     out = np.zeros((n, h, w, 16), np.float32)
@@ -136,7 +138,12 @@ def pack_input(radiance, albedo=None, normal=None, depth=None, transmittance=Non
     if transmittance is not None:
         out[..., 10] = np.asarray(transmittance, np.float32)
     if noise_level is not None:
-        out[..., 11] = np.asarray(noise_level, np.float32)[:, None, None]
+        nl = np.asarray(noise_level, np.float32)
+        out[..., 11] = nl[:, None, None]
+        if second_moment is not None:
+            m2 = np.asarray(second_moment, np.float32)
+            se = np.sqrt(np.maximum(0, m2 - r * r)) * nl[:, None, None, None]
+            out[..., 12:15] = np.log1p(se).transpose(0, 2, 3, 1)
     return out
 
 

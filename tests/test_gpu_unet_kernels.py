@@ -225,11 +225,12 @@ def test_pack_input_and_kpn_head(lib):
     dep = g.random((n, h, w)).astype(np.float32)
     trn = g.random((n, h, w)).astype(np.float32)
     noise = np.array([1.0, 0.125], np.float32)
+    m2 = (rad * rad * (1.0 + g.random((n, 3, h, w)))).astype(np.float32)
     packed = torch.empty((n, h, w, 16), dtype=torch.bfloat16, device="cuda")
-    t = [dev_f32(a) for a in (rad, alb, nrm, dep, trn, noise)]
+    t = [dev_f32(a) for a in (rad, alb, nrm, dep, trn, noise, m2)]
     assert lib.vpt_unet_pack_input(*[ptr(a) for a in t], ptr(packed), n, h, w, None) == 0
     torch.cuda.synchronize()
-    ref = uo.pack_input(rad, alb, nrm, dep, trn, noise)
+    ref = uo.pack_input(rad, alb, nrm, dep, trn, noise, m2)
     close_bf16(host(packed), ref.astype(np.float64))
 
     target = g.exponential(1.0, (n, 3, h, w)).astype(np.float32)
