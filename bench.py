@@ -458,8 +458,15 @@ def run_learned(vpt, lib, ctx, small):
     vpt.set_use_feature_maps(["Albedo", "Normal", "Depth", "Transmittance"])
     vpt.set_denoiser("Edge-Avoiding À-Trous Wavelet Transform")
     vpt.set_denoiser_property("iterations", "1")
-    ms_feat = frame_ms(64)  # with the feature maps: the denoised methods' render cost
+    ms_feat = frame_ms(64)  # a frame with the feature pass
+    # both denoisers read feature maps accumulated over the first FEATURE_FRAMES frames; later frames
+    # are traced without the feature pass
+    kf = ld.FEATURE_FRAMES
+    vpt.set_feature_frame_limit(kf)
     vpt.set_frame_index(0)
+
+    def render_ms(spp):
+        return min(spp, kf) * ms_feat + max(0.0, spp - kf) * ms_plain
 
     def timed(fn):
         a, c = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -497,13 +504,14 @@ def run_learned(vpt, lib, ctx, small):
         rows.append(row)
     vpt.set_denoiser("None")
     vpt.set_use_feature_maps([])
+    vpt.set_feature_frame_limit(0)
     net.check_errors()
     spp = [r["spp"] for r in rows]
     eaw_cost = statistics.median(sum(v) / len(v) for v in eaw_ms.values())
     net_cost = statistics.median(net_ms)
     plain_t = time_to_target(spp, [r["plain"] for r in rows], lambda s: s * ms_plain, ev["target"], True)
-    eaw_t = time_to_target(spp, [r["eaw"] for r in rows], lambda s: s * ms_feat + eaw_cost, ev["target"], False)
-    learned_t = time_to_target(spp, [r["learned"] for r in rows], lambda s: s * ms_feat + net_cost, ev["target"],
+    eaw_t = time_to_target(spp, [r["eaw"] for r in rows], lambda s: render_ms(s) + eaw_cost, ev["target"], False)
+    learned_t = time_to_target(spp, [r["learned"] for r in rows], lambda s: render_ms(s) + net_cost, ev["target"],
                                False)
     peak, peak_kind = tensor_peak()
     out = {
@@ -515,8 +523,8 @@ def run_learned(vpt, lib, ctx, small):
         "time_to_target_ms": {"plain": plain_t, "eaw_tuned": eaw_t, "learned": learned_t},
         "speedup_learned_vs_plain": (plain_t["ms"] / learned_t["ms"]) if learned_t["ms"] else None,
         "speedup_learned_vs_eaw": (eaw_t["ms"] / learned_t["ms"]) if (learned_t["ms"] and eaw_t["ms"]) else None,
-        "ms_per_frame": {"plain": ms_plain, "with_features": ms_feat}, "denoise_ms": {"eaw": eaw_cost,
-                                                                                     "learned": net_cost},
+        "ms_per_frame": {"plain": ms_plain, "with_features": ms_feat, "feature_frames": kf},
+        "denoise_ms": {"eaw": eaw_cost, "learned": net_cost},
         "curve": rows, "reference_render_s": ref_s,
         "training": {"data_s": data.seconds, "data_paths": data.paths, "train_s": hist["seconds"],
                      "loss_curve": hist["loss_curve"], "step_ms": step_ms, "launches_per_step": launches_per_step,

@@ -133,6 +133,12 @@ SIGNATURES = {
     "vpt_unet_pack_input": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                     c_int, c_int, c_int, c_void_p]),
     "vpt_unet_head_blocks": (c_int, [c_int, c_int, c_int]),
+    "vpt_unet_kpn_combine": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_void_p, c_int, c_int, c_int,
+                                     c_void_p]),
+    "vpt_unet_kpn_level_grad": (c_int, [c_void_p, c_int, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p,
+                                        c_void_p, c_void_p, c_float, c_void_p, c_void_p, c_void_p, c_int, c_int, c_int,
+                                        c_void_p]),
+    "vpt_unet_add": (c_int, [c_void_p, c_void_p, c_void_p, ctypes.c_long, c_void_p]),
     "vpt_unet_kpn_head": (c_int, [c_void_p, c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int,
                                   c_int, c_int, c_float, c_void_p]),
 }

@@ -197,6 +197,8 @@ struct VptContext {
     uint32_t frame_count = 0;      // FrameInfo::frameCount: seeds and accumulation
     uint32_t frame_origin = 0;     // frame index a cleared film starts from (frame sharding)
     uint32_t film_frames = 0;      // frames held in the film (1 for SVGF, which wants 1-spp input)
+    uint32_t feat_frames = 0;      // frames held in the feature accumulators
+    uint32_t feature_frame_limit = 0;  // > 0: feature maps accumulate over the first this many frames only
     DevBuf<double> film, film_sq;
     bool collect_stats = false;
     bool features_on = false;
@@ -248,9 +250,13 @@ cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
 bool features_needed(const VptContext* ctx);
 
+// frames held in the feature accumulators (every film frame unless a feature frame limit applies)
+uint32_t feature_frames(const VptContext* ctx) { return ctx->feat_frames > 0 ? ctx->feat_frames : 1u; }
+
 void reset_film_state(VptContext* ctx) {
     ctx->frame_count = ctx->frame_origin;
     ctx->film_frames = 0;
+    ctx->feat_frames = 0;
 }
 
 // CloudData::computeGridBounds (CloudData.cpp:63-78) with voxel size 1.
@@ -1241,9 +1247,33 @@ VptStatus vpt_render_frames(VptContext* ctx, int frames, void* stream) {
     if (ctx->schedule != vpt::kScheduleTiles && ctx->persistent_blocks_per_sm > 0) {
         pb = ctx->persistent_blocks_per_sm * ctx->num_sms;
     }
-    VPT_CHECK_CUDA(ctx, vpt::launch_trace(P, tracker, ctx->use_ess, ctx->schedule, P.feat ? 1 : 0, pb, s));
+    // With a feature frame limit, the frames beyond it are traced without the feature pass (same
+    // paths: the feature accumulation draws no random numbers).
+    int feat_n = P.feat ? (single ? 1 : frames) : 0;
+    if (P.feat && !single && ctx->feature_frame_limit > 0) {
+        const uint32_t left = ctx->feat_frames < ctx->feature_frame_limit ? ctx->feature_frame_limit - ctx->feat_frames
+                                                                           : 0u;
+        feat_n = (int)std::min<uint32_t>(left, (uint32_t)frames);
+    }
+    const int plain_n = (single ? 1 : frames) - feat_n;
+    if (feat_n > 0) {
+        vpt::TraceParams Pf = P;
+        Pf.num_frames = feat_n;
+        Pf.num_paths = (uint64_t)ctx->width * ctx->height * (uint64_t)feat_n;
+        VPT_CHECK_CUDA(ctx, vpt::launch_trace(Pf, tracker, ctx->use_ess, ctx->schedule, 1, pb, s));
+    }
+    if (plain_n > 0) {
+        vpt::TraceParams Pp = P;
+        Pp.feat = nullptr;
+        Pp.num_frames = plain_n;
+        Pp.num_paths = (uint64_t)ctx->width * ctx->height * (uint64_t)plain_n;
+        Pp.frame_count = P.frame_count + (uint32_t)feat_n;
+        Pp.global_frame = P.global_frame + (uint32_t)feat_n;
+        VPT_CHECK_CUDA(ctx, vpt::launch_trace(Pp, tracker, ctx->use_ess, ctx->schedule, 0, pb, s));
+    }
     ctx->frame_count += (uint32_t)frames;
     ctx->film_frames += single ? 1u : (uint32_t)frames;
+    ctx->feat_frames = single ? 1u : ctx->feat_frames + (uint32_t)feat_n;
     ctx->frames_total += (uint64_t)frames;
     return VPT_OK;
 }
@@ -1275,7 +1305,7 @@ VptStatus vpt_read_result(VptContext* ctx, float* out, int channels, int out_on_
         cudaError_t e;
         if (ctx->denoiser == VPT_DENOISER_EAW) {
             VPT_CHECK_CUDA(ctx, ctx->eaw_maps.alloc((size_t)n * 8));
-            e = vpt::eaw_denoise_features(ctx->rgba_src.ptr, feat, ctx->film_frames, ctx->width, ctx->height, ctx->eaw,
+            e = vpt::eaw_denoise_features(ctx->rgba_src.ptr, feat, feature_frames(ctx), ctx->width, ctx->height, ctx->eaw,
                                           ctx->eaw_maps.ptr, ctx->rgba_a.ptr, ctx->rgba_b.ptr, &result, s);
         } else {
             double vp[16], inv_vp[16];
@@ -1288,7 +1318,7 @@ VptStatus vpt_read_result(VptContext* ctx, float* out, int channels, int out_on_
             for (int i = 0; i < 16; i++)
                 ctx->svgf.prev_view_proj[i] = float(ctx->has_prev_view_proj ? ctx->prev_view_proj[i] : vp[i]);
             ctx->svgf.far_dist = ctx->far_dist;
-            e = vpt::svgf_denoise_features(ctx->rgba_src.ptr, feat, ctx->film_frames, ctx->width, ctx->height, ctx->svgf,
+            e = vpt::svgf_denoise_features(ctx->rgba_src.ptr, feat, feature_frames(ctx), ctx->width, ctx->height, ctx->svgf,
                                            ctx->svgf_state, ctx->rgba_b.ptr, &result, s);
             // setPreviousViewProjMatrix(current) at the end of _render (VolumetricPathTracingPass.cpp:2421)
             memcpy(ctx->prev_view_proj, vp, sizeof(vp));
@@ -1356,7 +1386,7 @@ VptStatus vpt_get_feature_map(VptContext* ctx, int feature, float* out, int chan
         VPT_CHECK_CUDA(ctx, ctx->staging.alloc((size_t)n * 4));
         dst = ctx->staging.ptr;
     }
-    cudaError_t e = vpt::feature_to_chw(ctx->feat.ptr, n, ctx->film_frames, feature, channels, ctx->albedo, dst, s);
+    cudaError_t e = vpt::feature_to_chw(ctx->feat.ptr, n, feature_frames(ctx), feature, channels, ctx->albedo, dst, s);
     if (e == cudaErrorInvalidValue) return fail(ctx, VPT_ERR_ARG, "feature map not supported");
     VPT_CHECK_CUDA(ctx, e);
     if (!out_on_device) {
@@ -1689,7 +1719,11 @@ VptStatus vpt_set_option(VptContext* ctx, const char* key, double value) {
     VPT_CHECK_CTX(ctx);
     if (!key) return VPT_ERR_ARG;
     std::string k(key);
-    if (k == "schedule") {
+    if (k == "feature_frames") {
+        if (value < 0 || value > 1e9) return fail(ctx, VPT_ERR_ARG, "feature_frames out of range");
+        ctx->feature_frame_limit = (uint32_t)value;
+        reset_film_state(ctx);
+    } else if (k == "schedule") {
         int v = int(value);
         if (v < 0 || v > 2) return fail(ctx, VPT_ERR_ARG, "schedule must be 0 (tiles), 1 (persistent) or 2 (refill)");
         ctx->schedule = v;

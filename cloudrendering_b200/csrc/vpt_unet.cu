@@ -971,6 +971,159 @@ __global__ void kpn_head_kernel(const float* __restrict__ logits, int hc, int ks
 }
 
 // ---------------------------------------------------------------------------------------------
+// multi-scale reconstruction
+// ---------------------------------------------------------------------------------------------
+// Level l (l = 0 full resolution) has the noisy input x_l (x_{l+1} = 2x2 average of x_l), its kernel
+// output d_l = apply(x_l, K_l), and the reconstruction
+//     c_l = d_l + a_l * (up(c_{l+1}) - up(pool(d_l))),   a_l = sigmoid(logit_l[alpha channel])
+// (the coarsest level: c = d): the low frequencies of the fine estimate are replaced, in the
+// proportion a, by the coarser level's estimate.  up = nearest (each coarse pixel to its 2x2
+// children), pool = 2x2 average.  Images are planar [n][3][h][w] fp32; logits NHWC [p][hc] fp32.
+__device__ __forceinline__ float sigmoidf_(float v) { return 1.0f / (1.0f + __expf(-v)); }
+
+__global__ void kpn_combine_kernel(const float* __restrict__ d, const float* __restrict__ c_coarse,
+                                   const float* __restrict__ logits, int hc, int alpha_ch, float* __restrict__ c,
+                                   int n, int h, int w) {
+    const long plane = (long)h * w, total = (long)n * plane;
+    const int hh = h / 2, wh = w / 2;
+    const long cplane = (long)hh * wh;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+        const long b = i / plane, q = i % plane;
+        const int y = (int)(q / w), x = (int)(q % w);
+        const int y0 = y & ~1, x0 = x & ~1;
+        const float a = sigmoidf_(logits[i * hc + alpha_ch]);
+        for (int ch = 0; ch < 3; ++ch) {
+            const float* dp = d + (b * 3 + ch) * plane;
+            const float pool = 0.25f * ((dp[(long)y0 * w + x0] + dp[(long)y0 * w + x0 + 1]) +
+                                        (dp[(long)(y0 + 1) * w + x0] + dp[(long)(y0 + 1) * w + x0 + 1]));
+            const float cc = c_coarse[(b * 3 + ch) * cplane + (long)(y / 2) * wh + x / 2];
+            c[(b * 3 + ch) * plane + q] = dp[q] + a * (cc - pool);
+        }
+    }
+}
+
+// Backward of one level.  g = dL/dc_l is read from g_in, or (level 0, target != null) computed here
+// from the relative-MSE loss of c = c_l against the target (whose partial sums go to loss_partial).
+// With a blend (alpha_ch >= 0): dL/dd = g - pool^T(up^T(a g)) (each pixel minus a quarter of its
+// 2x2 family's sum of a g), dL/dc_{l+1} = up^T(a g) (written by the family's first pixel),
+// dL/dlogit_alpha = a (1 - a) g . (up(c_{l+1}) - up(pool(d))); without: dL/dd = g.  Then the kernel
+// application's gradient dL/dlogit_j = s_j (gd . x_j - gd . d) (taps outside skipped), all written
+// to dlogits [p][hc] bf16 (0 in unused channels).
+__global__ void kpn_level_grad_kernel(const float* __restrict__ logits, int hc, int ks, int alpha_ch,
+                                      const float* __restrict__ x, const float* __restrict__ d,
+                                      const float* __restrict__ c_coarse, const float* __restrict__ g_in,
+                                      const float* __restrict__ c_out, const float* __restrict__ target, float eps,
+                                      float inv_count, bf16* __restrict__ dlogits, float* __restrict__ g_coarse,
+                                      float* __restrict__ loss_partial, int n, int h, int w) {
+    const long plane = (long)h * w, total = (long)n * plane;
+    const int taps = ks * ks, rad = ks / 2;
+    const int hh = h / 2, wh = w / 2;
+    const long cplane = (long)hh * wh;
+    float local = 0.0f;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+        const long b = i / plane, q = i % plane;
+        const int y = (int)(q / w), xx = (int)(q % w);
+        // gradient at c for a pixel of this image
+        auto g_at = [&](long qq, int ch) -> float {
+            if (target) {
+                const float t = target[(b * 3 + ch) * plane + qq];
+                return 2.0f * (c_out[(b * 3 + ch) * plane + qq] - t) / (t * t + eps) * inv_count;
+            }
+            return g_in[(b * 3 + ch) * plane + qq];
+        };
+        float g[3], gd[3];
+        for (int ch = 0; ch < 3; ++ch) g[ch] = g_at(q, ch);
+        if (target) {
+            for (int ch = 0; ch < 3; ++ch) {
+                const float t = target[(b * 3 + ch) * plane + q];
+                const float e = c_out[(b * 3 + ch) * plane + q] - t;
+                local += e * e / (t * t + eps) * inv_count;
+            }
+        }
+        float dalpha = 0.0f;
+        bool has_alpha = alpha_ch >= 0;
+        if (has_alpha) {
+            const int y0 = y & ~1, x0 = xx & ~1;
+            const long fam[4] = {(long)y0 * w + x0, (long)y0 * w + x0 + 1, (long)(y0 + 1) * w + x0,
+                                 (long)(y0 + 1) * w + x0 + 1};
+            const long base = i - q;  // first pixel of this image in NHWC order
+            float sag[3] = {0.0f, 0.0f, 0.0f};
+            for (int k = 0; k < 4; ++k) {
+                const float ak = sigmoidf_(logits[(base + fam[k]) * hc + alpha_ch]);
+                for (int ch = 0; ch < 3; ++ch) sag[ch] += ak * g_at(fam[k], ch);
+            }
+            const float a = sigmoidf_(logits[i * hc + alpha_ch]);
+            const long parent = (long)(y / 2) * wh + xx / 2;
+            for (int ch = 0; ch < 3; ++ch) {
+                gd[ch] = g[ch] - 0.25f * sag[ch];
+                const float* dp = d + (b * 3 + ch) * plane;
+                const float pool = 0.25f * ((dp[fam[0]] + dp[fam[1]]) + (dp[fam[2]] + dp[fam[3]]));
+                dalpha += g[ch] * (c_coarse[(b * 3 + ch) * cplane + parent] - pool);
+            }
+            dalpha *= a * (1.0f - a);
+            if (g_coarse && (y & 1) == 0 && (xx & 1) == 0)
+                for (int ch = 0; ch < 3; ++ch) g_coarse[(b * 3 + ch) * cplane + parent] = sag[ch];
+        } else {
+            for (int ch = 0; ch < 3; ++ch) gd[ch] = g[ch];
+        }
+        // kernel application backward
+        const float* lg = logits + i * hc;
+        float mx = -INFINITY;
+        for (int j = 0; j < taps; ++j) mx = fmaxf(mx, lg[j]);
+        float sum = 0.0f;
+        for (int j = 0; j < taps; ++j) sum += __expf(lg[j] - mx);
+        const float inv = 1.0f / sum;
+        const float* xb = x + b * 3 * plane;
+        const float gdd = gd[0] * d[(b * 3 + 0) * plane + q] + gd[1] * d[(b * 3 + 1) * plane + q] +
+                          gd[2] * d[(b * 3 + 2) * plane + q];
+        for (int j0 = 0; j0 < hc; j0 += 8) {
+            float f[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const int j = j0 + k;
+                f[k] = 0.0f;
+                if (j < taps) {
+                    const float sj = __expf(lg[j] - mx) * inv;
+                    const int yy = y + j / ks - rad, xq = xx + j % ks - rad;
+                    float gx = 0.0f;
+                    if (yy >= 0 && yy < h && xq >= 0 && xq < w) {
+                        const long o = (long)yy * w + xq;
+                        gx = gd[0] * xb[o] + gd[1] * xb[plane + o] + gd[2] * xb[2 * plane + o];
+                    }
+                    f[k] = sj * (gx - gdd);
+                } else if (j == alpha_ch) {
+                    f[k] = dalpha;
+                }
+            }
+            store8(dlogits + i * hc + j0, f);
+        }
+    }
+    if (loss_partial) {
+        __shared__ float red[256];
+        red[threadIdx.x] = local;
+        __syncthreads();
+        for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+            if ((int)threadIdx.x < st) red[threadIdx.x] += red[threadIdx.x + st];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) loss_partial[blockIdx.x] = red[0];
+    }
+}
+
+// out = a + b (bf16, count a multiple of 8)
+__global__ void add_bf16_kernel(const bf16* __restrict__ a, const bf16* __restrict__ b, bf16* __restrict__ out,
+                                long count8) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < count8; i += (long)gridDim.x * blockDim.x) {
+        float fa[8], fb[8];
+        load8(a + i * 8, fa);
+        load8(b + i * 8, fb);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) fa[k] += fb[k];
+        store8(out + i * 8, fa);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------------------------
 inline int grid_for(long work, int threads) {
@@ -1301,6 +1454,43 @@ VptStatus vpt_unet_kpn_head(const float* logits, int head_channels, int kernel_s
     kpn_head_kernel<<<blocks, 256, 0, static_cast<cudaStream_t>(stream)>>>(
         logits, head_channels, kernel_size, radiance, target, out, static_cast<bf16*>(dlogits), loss_partial, n, h, w,
         eps, inv_count);
+    vpt::count_launches(1);
+    return cudaGetLastError() == cudaSuccess ? VPT_OK : VPT_ERR_CUDA;
+}
+
+VptStatus vpt_unet_kpn_combine(const float* d, const float* c_coarse, const float* logits, int head_channels,
+                               int alpha_channel, float* c, int n, int h, int w, void* stream) {
+    if (!d || !c_coarse || !logits || !c || n <= 0 || h <= 1 || w <= 1 || h % 2 || w % 2 || alpha_channel < 0 ||
+        alpha_channel >= head_channels)
+        return VPT_ERR_ARG;
+    kpn_combine_kernel<<<grid_for((long)n * h * w, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        d, c_coarse, logits, head_channels, alpha_channel, c, n, h, w);
+    vpt::count_launches(1);
+    return cudaGetLastError() == cudaSuccess ? VPT_OK : VPT_ERR_CUDA;
+}
+
+VptStatus vpt_unet_kpn_level_grad(const float* logits, int head_channels, int kernel_size, int alpha_channel,
+                                  const float* x, const float* d, const float* c_coarse, const float* g_in,
+                                  const float* c_out, const float* target, float eps, void* dlogits, float* g_coarse,
+                                  float* loss_partial, int n, int h, int w, void* stream) {
+    if (!logits || !x || !d || !dlogits || n <= 0 || h <= 0 || w <= 0 || kernel_size <= 0 || kernel_size % 2 == 0 ||
+        kernel_size > 15 || head_channels % 8 || head_channels < kernel_size * kernel_size ||
+        (alpha_channel >= 0 && (alpha_channel < kernel_size * kernel_size || alpha_channel >= head_channels ||
+                                !c_coarse || h % 2 || w % 2)) ||
+        (target ? !c_out : !g_in) || eps <= 0.0f || (loss_partial && !target))
+        return VPT_ERR_ARG;
+    const float inv_count = 1.0f / (3.0f * (float)n * (float)h * (float)w);
+    kpn_level_grad_kernel<<<grid_for((long)n * h * w, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        logits, head_channels, kernel_size, alpha_channel, x, d, c_coarse, g_in, c_out, target, eps, inv_count,
+        static_cast<bf16*>(dlogits), g_coarse, loss_partial, n, h, w);
+    vpt::count_launches(1);
+    return cudaGetLastError() == cudaSuccess ? VPT_OK : VPT_ERR_CUDA;
+}
+
+VptStatus vpt_unet_add(const void* a, const void* b, void* out, long count, void* stream) {
+    if (!a || !b || !out || count <= 0 || count % 8) return VPT_ERR_ARG;
+    add_bf16_kernel<<<grid_for(count / 8, 256), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        static_cast<const bf16*>(a), static_cast<const bf16*>(b), static_cast<bf16*>(out), count / 8);
     vpt::count_launches(1);
     return cudaGetLastError() == cudaSuccess ? VPT_OK : VPT_ERR_CUDA;
 }

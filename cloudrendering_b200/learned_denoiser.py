@@ -35,6 +35,7 @@ from . import _lib
 WIDTHS = (32, 64, 96, 128, 160)
 IN_CHANNELS = 16
 KERNEL_SIZE = 13
+COARSE_KERNELS = ()  # kernel sizes of the half / quarter-resolution heads (multi-scale reconstruction)
 LOSS_EPS = 1e-2
 # feature maps the network reads (names of VolumetricPathTracingPass.hpp:74-80, plus the 2D
 # primary-ray transmittance of this package)
@@ -47,12 +48,15 @@ def _p(t: Optional[torch.Tensor], offset_elems: int = 0):
     return ctypes.c_void_p(t.data_ptr() + offset_elems * t.element_size())
 
 
-def head_channels(kernel_size: int) -> int:
-    return (kernel_size * kernel_size + 15) // 16 * 16
+def head_channels(kernel_size: int, blend: bool = False) -> int:
+    """Channels of a kernel head: k*k tap logits (+ 1 blend logit), rounded up to 16."""
+    return (kernel_size * kernel_size + (1 if blend else 0) + 15) // 16 * 16
 
 
-def layer_table(widths: Sequence[int], kernel_size: int = KERNEL_SIZE) -> List[dict]:
-    """Convolution layers in forward order: name, cin, cout, level."""
+def layer_table(widths: Sequence[int], kernel_size: int = KERNEL_SIZE, coarse_kernels: Sequence[int] = ()) -> List[dict]:
+    """Convolution layers in forward order: name, cin, cout, level.  coarse_kernels: kernel sizes of the
+    half- and quarter-resolution heads of the multi-scale reconstruction (empty: one full-resolution
+    kernel)."""
     w = list(widths)
     if len(w) != 5 or any(c % 16 for c in w):
         raise ValueError("widths: five multiples of 16")
@@ -65,7 +69,10 @@ def layer_table(widths: Sequence[int], kernel_size: int = KERNEL_SIZE) -> List[d
     for l in (3, 2, 1, 0):
         t.append(dict(name=f"dec{l}a", cin=w[l + 1] + w[l], cout=w[l], level=l))
         t.append(dict(name=f"dec{l}b", cin=w[l], cout=w[l], level=l))
-    t.append(dict(name="head", cin=w[0], cout=head_channels(kernel_size), level=0))
+    multi = len(coarse_kernels) > 0
+    t.append(dict(name="head", cin=w[0], cout=head_channels(kernel_size, multi), level=0))
+    for l, k in enumerate(coarse_kernels, start=1):
+        t.append(dict(name=f"head{l}", cin=w[l], cout=head_channels(k, l < len(coarse_kernels)), level=l))
     return t
 
 
@@ -73,15 +80,20 @@ class KpnUNet:
     """The network, its fp32 master parameters, Adam state and activation buffers (one device)."""
 
     def __init__(self, widths: Sequence[int] = WIDTHS, seed: int = 0, device: Optional[torch.device] = None,
-                 kernel_size: int = KERNEL_SIZE):
+                 kernel_size: int = KERNEL_SIZE, coarse_kernels: Sequence[int] = COARSE_KERNELS):
         self.lib = _lib.load()
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         self.widths = tuple(int(c) for c in widths)
-        if kernel_size % 2 == 0 or not 1 <= kernel_size <= 15:
-            raise ValueError("kernel_size: odd, 1..15")
+        for k in (kernel_size, *coarse_kernels):
+            if k % 2 == 0 or not 1 <= k <= 15:
+                raise ValueError("kernel sizes: odd, 1..15")
+        if len(coarse_kernels) > 2:
+            raise ValueError("at most two coarse levels (half and quarter resolution)")
         self.kernel_size = int(kernel_size)
-        self.head_channels = head_channels(self.kernel_size)
-        self.layers = layer_table(self.widths, self.kernel_size)
+        self.coarse_kernels = tuple(int(k) for k in coarse_kernels)
+        self.kernels = (self.kernel_size,) + self.coarse_kernels
+        self.head_channels = head_channels(self.kernel_size, len(self.coarse_kernels) > 0)
+        self.layers = layer_table(self.widths, self.kernel_size, self.coarse_kernels)
         self.by_name = {L["name"]: L for L in self.layers}
         off = 0
         for L in self.layers:
@@ -110,7 +122,7 @@ class KpnUNet:
         host = np.zeros(self.count, np.float32)
         for L in self.layers:
             cin_used = 15 if L["name"] == "enc0a" else L["cin"]
-            std = math.sqrt(2.0 / (9 * cin_used)) if L["name"] != "head" else 1e-3
+            std = math.sqrt(2.0 / (9 * cin_used)) if not L["name"].startswith("head") else 1e-3
             w = (g.standard_normal((L["cout"], 9, L["cin"])) * std).astype(np.float32)
             if L["name"] == "enc0a":
                 w[:, :, 15:] = 0.0
@@ -213,15 +225,23 @@ class KpnUNet:
             cur = self._conv(self.by_name[f"dec{l}b"], a, self.buf(f"dec{l}b", (n, hh, ww, W[l])), n, hh, ww, 1)
         hh, ww = dims[0]
         self._x0 = x0
-        return self._conv(self.by_name["head"], cur,
-                          self.buf("logits", (n, hh, ww, self.head_channels), torch.float32), n, hh, ww, 0, 1)
+        self.logits = [self._conv(self.by_name["head"], cur,
+                                  self.buf("logits", (n, hh, ww, self.head_channels), torch.float32), n, hh, ww, 0, 1)]
+        for l in range(1, len(self.kernels)):
+            L = self.by_name[f"head{l}"]
+            h2, w2 = dims[l]
+            self.logits.append(self._conv(L, self._buf[f"dec{l}b"], self.buf(f"logits{l}", (n, h2, w2, L["cout"]),
+                                                                          torch.float32), n, h2, w2, 0, 1))
+        return self.logits[0]
 
-    def backward(self, dlogits: torch.Tensor) -> None:
-        """dlogits: [n, h, w, head channels] bf16 gradient of the loss at the head's output.  Fills self.grad
-        (flat, same layout as the parameters)."""
+    def backward(self, dlogits) -> None:
+        """dlogits: bf16 gradient of the loss at the heads' outputs, [n, h, w, head channels] (or one per
+        level of the multi-scale reconstruction).  Fills self.grad (flat, same layout as the parameters)."""
         n, h, w = self.shape
         W = self.widths
         B = self._buf
+        dls = list(dlogits) if isinstance(dlogits, (list, tuple)) else [dlogits]
+        dlogits = dls[0]
         dims = [(h >> l, w >> l) for l in range(5)]
         hh, ww = dims[0]
         L = self.by_name["head"]
@@ -241,6 +261,11 @@ class KpnUNet:
             h2, w2 = dims[l + 1]
             g = self.buf(f"glo{l + 1}", (n, h2, w2, ca))
             self._call("vpt_unet_upcat_grad_lo", _p(du), _p(lo), _p(g), n, hh, ww, ca, cs, self._stream())
+            if l + 1 < len(dls):  # the coarse kernel head on this decoder level
+                Lh = self.by_name[f"head{l + 1}"]
+                self._weight_grad(Lh, lo, dls[l + 1], n, h2, w2)
+                hg = self._input_grad(Lh, dls[l + 1], lo, self.buf(f"ghead{l + 1}", (n, h2, w2, ca)), n, h2, w2)
+                self._call("vpt_unet_add", _p(g), _p(hg), _p(g), g.numel(), self._stream())
         hh, ww = dims[4]
         self._weight_grad(self.by_name["midb"], B["mida"], g, n, hh, ww)
         ga = self._input_grad(self.by_name["midb"], g, B["mida"], self.buf("gmida", (n, hh, ww, W[4])), n, hh, ww)
@@ -275,6 +300,58 @@ class KpnUNet:
                    _p(noise_level), _p(second_moment), _p(x0), n, h, w, self._stream())
         return x0
 
+    def reconstruct(self, radiance, target=None, out=None):
+        """Applies the predicted kernels (multi-scale: at full, half and quarter resolution, blended);
+        with a target also the loss (device scalar) and the gradients at the heads' logits.  Returns
+        (out, loss, dlogits per level)."""
+        if len(self.kernels) == 1:
+            o, loss, dl = self.head(self.logits[0], radiance, target, out)
+            return o, loss, [dl]
+        n, _, h, w = radiance.shape
+        L = len(self.kernels)
+        xs, ds, cs = [radiance], [], [None] * L
+        for l in range(1, L):
+            hl, wl = h >> l, w >> l
+            x = self.buf(f"x{l}", (n, 3, hl, wl), torch.float32)
+            self._call("vpt_kpn_avg_pool2", _p(xs[-1]), n, 3, hl * 2, wl * 2, _p(x), self._stream())
+            xs.append(x)
+        for l in range(L):
+            hl, wl = h >> l, w >> l
+            d = self.buf(f"d{l}", (n, 3, hl, wl), torch.float32)
+            hc = self.logits[l].shape[-1]
+            self._call("vpt_unet_kpn_head", _p(self.logits[l]), hc, self.kernels[l], _p(xs[l]), None, _p(d), None,
+                       None, n, hl, wl, LOSS_EPS, self._stream())
+            ds.append(d)
+        cs[L - 1] = ds[L - 1]
+        for l in range(L - 2, -1, -1):
+            hl, wl = h >> l, w >> l
+            c = out if (l == 0 and out is not None) else self.buf(f"c{l}", (n, 3, hl, wl), torch.float32)
+            hc = self.logits[l].shape[-1]
+            k = self.kernels[l]
+            self._call("vpt_unet_kpn_combine", _p(ds[l]), _p(cs[l + 1]), _p(self.logits[l]), hc, k * k, _p(c), n,
+                       hl, wl, self._stream())
+            cs[l] = c
+        if target is None:
+            return cs[0], None, None
+        blocks = self.lib.vpt_unet_head_blocks(n, h, w)
+        lp = self.buf("loss_partial", (blocks,), torch.float32)
+        dls = []
+        g_in = None
+        for l in range(L):
+            hl, wl = h >> l, w >> l
+            hc = self.logits[l].shape[-1]
+            k = self.kernels[l]
+            dl = self.buf(f"dlogits{l}", (n, hl, wl, hc))
+            blend = l < L - 1
+            g_next = self.buf(f"gc{l + 1}", (n, 3, hl // 2, wl // 2), torch.float32) if blend else None
+            self._call("vpt_unet_kpn_level_grad", _p(self.logits[l]), hc, k, k * k if blend else -1, _p(xs[l]),
+                       _p(ds[l]), _p(cs[l + 1]) if blend else None, _p(g_in), _p(cs[0]) if l == 0 else None,
+                       _p(target) if l == 0 else None, LOSS_EPS, _p(dl), _p(g_next), _p(lp) if l == 0 else None, n,
+                       hl, wl, self._stream())
+            dls.append(dl)
+            g_in = g_next
+        return cs[0], lp.sum(), dls
+
     def head(self, logits, radiance, target=None, out=None):
         """Applies the predicted kernels; with a target also the loss (device scalar) and the
         gradient at the logits (returned as (out, loss, dlogits))."""
@@ -291,9 +368,9 @@ class KpnUNet:
     def train_step(self, batch: dict, lr: float) -> torch.Tensor:
         x0 = self.pack(batch["radiance"], batch.get("albedo"), batch.get("normal"), batch.get("depth"),
                        batch.get("transmittance"), batch.get("noise_level"), batch.get("second_moment"))
-        logits = self.forward(x0)
-        _, loss, dl = self.head(logits, batch["radiance"], batch["target"])
-        self.backward(dl)
+        self.forward(x0)
+        _, loss, dls = self.reconstruct(batch["radiance"], batch["target"])
+        self.backward(dls)
         self.adam_step(lr)
         return loss
 
@@ -301,9 +378,9 @@ class KpnUNet:
                 second_moment=None):
         """Denoised radiance [n, 3, h, w] fp32 (h, w multiples of 16)."""
         x0 = self.pack(radiance, albedo, normal, depth, transmittance, noise_level, second_moment)
-        logits = self.forward(x0)
+        self.forward(x0)
         out = torch.empty_like(radiance)
-        self.head(logits, radiance, None, out)
+        self.reconstruct(radiance, None, out)
         return out
 
     # ---- the model contract ----
@@ -311,6 +388,7 @@ class KpnUNet:
         os.makedirs(directory, exist_ok=True)
         np.savez(os.path.join(directory, "weights.npz"), params=self.parameters_host())
         info = {"input_feature_maps": INPUT_FEATURE_MAPS, "blend": "kpn", "kernel_size": self.kernel_size,
+                "coarse_kernel_sizes": list(self.coarse_kernels),
                 "use_previous_frame": False, "use_batch_dimension": True, "use_fp16": False,
                 "network": "unet", "widths": list(self.widths), "input_channels": IN_CHANNELS,
                 "head_channels": self.head_channels, "loss": "relmse", "loss_eps": LOSS_EPS, "steps": self.steps}
@@ -324,7 +402,8 @@ class KpnUNet:
         if info.get("network") != "unet" or info.get("blend") != "kpn":
             raise RuntimeError(f"unsupported model_info.json in {directory}: network {info.get('network')}, "
                                f"blend {info.get('blend')}")
-        net = cls(info["widths"], device=device, kernel_size=int(info.get("kernel_size", KERNEL_SIZE)))
+        net = cls(info["widths"], device=device, kernel_size=int(info.get("kernel_size", KERNEL_SIZE)),
+                  coarse_kernels=tuple(info.get("coarse_kernel_sizes", ())))
         net.set_parameters(np.load(os.path.join(directory, "weights.npz"))["params"])
         net.steps = int(info.get("steps", 0))
         return net
@@ -379,6 +458,7 @@ def read_features(vpt, img: torch.Tensor) -> dict:
 
 
 TARGET_FRAME_ORIGIN = 1 << 24  # targets use frames disjoint from the noisy inputs'
+FEATURE_FRAMES = 4  # feature maps are accumulated over the first 4 frames (first-hit features converge fast)
 
 
 def render_scene_levels(vpt, sc: dict, size: int, spp_levels: Sequence[int], target_spp: int, grid: int = 128,
@@ -389,6 +469,7 @@ def render_scene_levels(vpt, sc: dict, size: int, spp_levels: Sequence[int], tar
     range), all on the GPU."""
     setup_scene(vpt, sc, grid, max_bounces)
     vpt.set_use_feature_maps(["Albedo", "Normal", "Depth", "Transmittance"])
+    vpt.set_feature_frame_limit(FEATURE_FRAMES)
     vpt.set_collect_statistics(second_moment)
     img = torch.zeros((3, size, size), dtype=torch.float32, device="cuda")
     vpt.set_frame_index(0)
@@ -400,6 +481,7 @@ def render_scene_levels(vpt, sc: dict, size: int, spp_levels: Sequence[int], tar
         m2 = vpt.get_film_moments(size, size, spp)[1] if second_moment else None
         levels.append(dict(spp=spp, radiance=rad, second_moment=m2, **read_features(vpt, img)))
     vpt.set_use_feature_maps([])
+    vpt.set_feature_frame_limit(0)
     vpt.set_collect_statistics(False)
     vpt.set_frame_index(TARGET_FRAME_ORIGIN)
     left = target_spp
@@ -495,3 +577,61 @@ def train(net: KpnUNet, data: TrainingSet, steps: int, batch_size: int = 8, lr: 
     torch.cuda.synchronize()
     net.check_errors()
     return {"steps": steps, "seconds": time.perf_counter() - t0, "loss_curve": losses}
+
+
+def layer_timings(net: KpnUNet, batch: int = 8, size: int = 256, reps: int = 20) -> Dict[str, dict]:
+    """Device time of every convolution of a training step at batch x size^2 (forward, input gradient,
+    weight gradient; random activations), with the flops of each."""
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            fn()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps
+
+    out = {}
+    for L in net.layers:
+        hh, ww = size >> L["level"], size >> L["level"]
+        x = torch.randn((batch, hh, ww, L["cin"]), device=net.device).to(torch.bfloat16)
+        y = torch.empty((batch, hh, ww, L["cout"]), dtype=torch.bfloat16, device=net.device)
+        dy = torch.randn((batch, hh, ww, L["cout"]), device=net.device).to(torch.bfloat16)
+        dx = torch.empty_like(x)
+        flop = 2.0 * 9 * L["cin"] * L["cout"] * batch * hh * ww
+        t_f = timed(lambda: net._conv(L, x, y, batch, hh, ww, 1))
+        t_d = timed(lambda: net._input_grad(L, dy, x, dx, batch, hh, ww))
+        t_w = timed(lambda: net._weight_grad(L, x, dy, batch, hh, ww))
+        out[L["name"]] = {"forward_ms": t_f, "input_grad_ms": t_d, "weight_grad_ms": t_w, "gflop": flop / 1e9}
+    net.check_errors()
+    return out
+
+
+if __name__ == "__main__":
+    import argparse
+
+    ap = argparse.ArgumentParser(description="learned denoiser network: kernel timings and profiling launches")
+    ap.add_argument("--layers", action="store_true", help="time every convolution of a training step")
+    ap.add_argument("--profile-launches", action="store_true",
+                    help="one forward and one weight-gradient launch of two level-0 layers (32->32, 96->32) at "
+                         "8x256^2, for a profiler")
+    ap.add_argument("--size", type=int, default=256)
+    ap.add_argument("--batch", type=int, default=8)
+    args = ap.parse_args()
+    net = KpnUNet(seed=0)
+    if args.layers:
+        print(json.dumps(layer_timings(net, args.batch, args.size), indent=1))
+    if args.profile_launches:
+        for name in ("enc0b", "dec0a"):
+            L = net.by_name[name]
+            n, hh, ww = args.batch, args.size, args.size
+            x = torch.randn((n, hh, ww, L["cin"]), device=net.device).to(torch.bfloat16)
+            y = torch.empty((n, hh, ww, L["cout"]), dtype=torch.bfloat16, device=net.device)
+            dy = torch.randn((n, hh, ww, L["cout"]), device=net.device).to(torch.bfloat16)
+            net._conv(L, x, y, n, hh, ww, 1)
+            net._weight_grad(L, x, dy, n, hh, ww)
+        torch.cuda.synchronize()
+        net.check_errors()
+        print("ok")

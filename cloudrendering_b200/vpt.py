@@ -624,6 +624,13 @@ def set_frame_index(first_frame: int) -> None:
     _c("vpt_set_frame_index", int(first_frame) & 0xFFFFFFFF)
 
 
+def set_feature_frame_limit(frames: int) -> None:
+    """Feature maps accumulate over the first `frames` frames of an accumulation only (0: every frame,
+    as the reference does); later frames are traced without the feature pass (no reference
+    counterpart; clears the accumulation)."""
+    _c("vpt_set_option", b"feature_frames", float(frames))
+
+
 def set_collect_statistics(enabled: bool) -> None:
     """Accumulates the per-pixel sum of squared frame radiance beside the FP64 film (no reference
     counterpart; clears the accumulation when the state changes)."""

@@ -425,6 +425,22 @@ VptStatus vpt_unet_kpn_head(const float* logits, int head_channels, int kernel_s
                             const float* target, float* out, void* dlogits, float* loss_partial, int n, int h, int w,
                             float eps, void* stream);
 
+/* Multi-scale reconstruction, level l (planar [n][3][h][w] fp32, h and w even):
+ * c = d + sigmoid(logits[p][alpha_channel]) * (up(c_coarse) - up(pool(d))), c_coarse at h/2 x w/2. */
+VptStatus vpt_unet_kpn_combine(const float* d, const float* c_coarse, const float* logits, int head_channels,
+                               int alpha_channel, float* c, int n, int h, int w, void* stream);
+/* Backward of one level of the reconstruction and of its kernel application (d = apply(x, logits)):
+ * dlogits [p][head_channels] bf16 (tap logits, the blend logit at alpha_channel (< 0: no blend),
+ * 0 elsewhere) and (with a blend) g_coarse = dL/dc_coarse.  The gradient at this level's output
+ * comes from g_in, or with target != NULL from the relative MSE of c_out against the target (its
+ * per-block partial sums to loss_partial, vpt_unet_head_blocks of them). */
+VptStatus vpt_unet_kpn_level_grad(const float* logits, int head_channels, int kernel_size, int alpha_channel,
+                                  const float* x, const float* d, const float* c_coarse, const float* g_in,
+                                  const float* c_out, const float* target, float eps, void* dlogits, float* g_coarse,
+                                  float* loss_partial, int n, int h, int w, void* stream);
+/* out = a + b, bf16, count a multiple of 8 */
+VptStatus vpt_unet_add(const void* a, const void* b, void* out, long count, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

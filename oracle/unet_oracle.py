@@ -190,7 +190,8 @@ def adam(param, m1, m2, grad, step, lr=1e-4, beta1=0.9, beta2=0.999, eps=1e-8):
 # ---------------------------------------------------------------------------------------------
 # the whole network (cloudrendering_b200/learned_denoiser.py: KpnUNet.forward / backward)
 # ---------------------------------------------------------------------------------------------
-def layer_table(widths, head_channels=32):
+def layer_table(widths, head_channels=32, coarse_heads=()):
+    """coarse_heads: head channel counts of the level 1 and 2 kernel heads (multi-scale), or ()."""
     w = list(widths)
     t = []
     for l in range(4):
@@ -202,13 +203,15 @@ def layer_table(widths, head_channels=32):
         t.append((f"dec{l}a", w[l + 1] + w[l], w[l]))
         t.append((f"dec{l}b", w[l], w[l]))
     t.append(("head", w[0], head_channels))
+    for l, hc in enumerate(coarse_heads, start=1):
+        t.append((f"head{l}", w[l], hc))
     return t
 
 
-def split_params(flat, widths, head_channels=32):
+def split_params(flat, widths, head_channels=32, coarse_heads=()):
     """Flat parameter vector -> {name: (w [cout][9][cin], b [cout])} (weights then bias per layer)."""
     out, off = {}, 0
-    for name, cin, cout in layer_table(widths, head_channels):
+    for name, cin, cout in layer_table(widths, head_channels, coarse_heads):
         w = np.asarray(flat[off:off + cout * 9 * cin]).reshape(cout, 9, cin)
         off += cout * 9 * cin
         out[name] = (w, np.asarray(flat[off:off + cout]))
@@ -216,13 +219,19 @@ def split_params(flat, widths, head_channels=32):
     return out
 
 
-def network_loss_and_grad(flat, widths, x0, radiance, target, round_bf16=True, eps=1e-2, ks=5):
+def head_channels_for(ks, blend):
+    return (ks * ks + (1 if blend else 0) + 15) // 16 * 16
+
+
+def network_loss_and_grad(flat, widths, x0, radiance, target, round_bf16=True, eps=1e-2, ks=5, coarse_ks=()):
     """Forward, relative-MSE loss of the kernel head and the gradient with respect to every
     parameter (flat, same layout).  With round_bf16 the weights, activations and backward
     gradients are rounded to bf16 where the GPU stores them in bf16; without, all float64."""
     rnd = (lambda a: bf16(np.asarray(a, np.float32)).astype(np.float64)) if round_bf16 else (lambda a: a)
-    hc = (ks * ks + 15) // 16 * 16
-    P = split_params(flat, widths, hc)
+    multi = len(coarse_ks) > 0
+    hc = head_channels_for(ks, multi)
+    coarse_hc = tuple(head_channels_for(k, l < len(coarse_ks)) for l, k in enumerate(coarse_ks, start=1))
+    P = split_params(flat, widths, hc, coarse_hc)
     Wt = {k: rnd(v[0]) for k, v in P.items()}
     Bs = {k: np.asarray(v[1], np.float64) for k, v in P.items()}
     A = {}
@@ -239,10 +248,15 @@ def network_loss_and_grad(flat, widths, x0, radiance, target, round_bf16=True, e
         A[f"cat{l}"] = upcat(cur, A[f"enc{l}b"])
         A[f"dec{l}a"] = rnd(conv3x3(A[f"cat{l}"], Wt[f"dec{l}a"], Bs[f"dec{l}a"], relu=True))
         cur = A[f"dec{l}b"] = rnd(conv3x3(A[f"dec{l}a"], Wt[f"dec{l}b"], Bs[f"dec{l}b"], relu=True))
-    logits = conv3x3(cur, Wt["head"], Bs["head"])
-    if round_bf16:
-        logits = logits.astype(np.float32).astype(np.float64)
-    d, loss, dl = kpn_head(logits, radiance, target, eps, ks)
+    f32 = (lambda a: a.astype(np.float32).astype(np.float64)) if round_bf16 else (lambda a: a)
+    logits = f32(conv3x3(cur, Wt["head"], Bs["head"]))
+    if multi:
+        lgs = [logits] + [f32(conv3x3(A[f"dec{l}b"], Wt[f"head{l}"], Bs[f"head{l}"]))
+                          for l in range(1, len(coarse_ks) + 1)]
+        loss, dls, d = multiscale_loss_and_grad(lgs, radiance, target, (ks,) + tuple(coarse_ks), eps)
+        dl = dls[0]
+    else:
+        d, loss, dl = kpn_head(logits, radiance, target, eps, ks)
     G = {}
 
     def grads(name, x, dy):
@@ -259,6 +273,11 @@ def network_loss_and_grad(flat, widths, x0, radiance, target, round_bf16=True, e
         dcat[l] = rnd(conv3x3_input_grad(ga, Wt[f"dec{l}a"]))
         lo = A["midb"] if l == 3 else A[f"dec{l + 1}b"]
         g = rnd(upcat_grad_lo(dcat[l], lo))
+        if multi and l + 1 <= len(coarse_ks):
+            hl = f"head{l + 1}"
+            dlh = rnd(dls[l + 1])
+            grads(hl, A[f"dec{l + 1}b"], dlh)
+            g = rnd(g + rnd(conv3x3_input_grad(dlh, Wt[hl], mask=A[f"dec{l + 1}b"])))
     grads("midb", A["mida"], g)
     ga = rnd(conv3x3_input_grad(g, Wt["midb"], mask=A["mida"]))
     grads("mida", A["in4"], ga)
@@ -272,6 +291,82 @@ def network_loss_and_grad(flat, widths, x0, radiance, target, round_bf16=True, e
         if l > 0:
             dpool = rnd(conv3x3_input_grad(ga, Wt[f"enc{l}a"]))
     flat_g = []
-    for name, _, _ in layer_table(widths, hc):
+    for name, _, _ in layer_table(widths, hc, coarse_hc):
         flat_g += [G[name][0].reshape(-1), G[name][1]]
     return loss, np.concatenate(flat_g), logits, d
+
+
+# ---------------------------------------------------------------------------------------------
+# multi-scale reconstruction (cloudrendering_b200/csrc/vpt_unet.cu: kpn_combine_kernel,
+# kpn_level_grad_kernel)
+# ---------------------------------------------------------------------------------------------
+def pool2_planar(x):
+    x = np.asarray(x, np.float64)
+    n, c, h, w = x.shape
+    return x.reshape(n, c, h // 2, 2, w // 2, 2).mean(axis=(3, 5))
+
+
+def up2_planar(x):
+    return np.asarray(x, np.float64).repeat(2, axis=2).repeat(2, axis=3)
+
+
+def _sigmoid(v):
+    return 1.0 / (1.0 + np.exp(-v))
+
+
+def multiscale_reconstruct(logits, x0, ks):
+    """logits: per level l (l = 0 full resolution) NHWC [n, h_l, w_l, hc_l]; ks: kernel size per level.
+    Levels below the coarsest carry a blend logit at channel ks_l^2.  Returns (c0, per-level d, c)."""
+    L = len(logits)
+    xs = [np.asarray(x0, np.float64)]
+    for _ in range(L - 1):
+        xs.append(pool2_planar(xs[-1]))
+    ds = [kpn_head(logits[l], xs[l], ks=ks[l])[0] for l in range(L)]
+    cs = [None] * L
+    cs[L - 1] = ds[L - 1]
+    for l in range(L - 2, -1, -1):
+        a = _sigmoid(np.asarray(logits[l], np.float64)[..., ks[l] * ks[l]])[:, None, :, :]
+        cs[l] = ds[l] + a * (up2_planar(cs[l + 1]) - up2_planar(pool2_planar(ds[l])))
+    return cs[0], xs, ds, cs
+
+
+def multiscale_loss_and_grad(logits, x0, target, ks, eps=1e-2):
+    """Relative-MSE loss of the reconstruction and its gradient with respect to every level's logits."""
+    L = len(logits)
+    c0, xs, ds, cs = multiscale_reconstruct(logits, x0, ks)
+    t = np.asarray(target, np.float64)
+    count = c0.size
+    loss = float(((c0 - t) ** 2 / (t * t + eps)).sum() / count)
+    g = 2.0 * (c0 - t) / (t * t + eps) / count
+    grads = [None] * L
+    for l in range(L):
+        lg = np.asarray(logits[l], np.float64)
+        taps = ks[l] * ks[l]
+        if l < L - 1:
+            a = _sigmoid(lg[..., taps])[:, None, :, :]
+            ag = a * g
+            s = up2_planar(pool2_planar(ag) * 4.0)  # family sums of a g, on each child
+            gd = g - 0.25 * s
+            diff = up2_planar(cs[l + 1]) - up2_planar(pool2_planar(ds[l]))
+            dalpha = (g * diff).sum(axis=1) * (a[:, 0] * (1 - a[:, 0]))
+            g_next = pool2_planar(ag) * 4.0
+        else:
+            gd, dalpha, g_next = g, None, None
+        # kernel application backward (kpn_head's formula with an upstream gradient)
+        taps_lg = lg[..., :taps]
+        sm = np.exp(taps_lg - taps_lg.max(axis=-1, keepdims=True))
+        sm /= sm.sum(axis=-1, keepdims=True)
+        rad = ks[l] // 2
+        xt = xs[l].transpose(0, 2, 3, 1)
+        gx = np.zeros(taps_lg.shape)
+        for j in range(taps):
+            xs_j = _shift(xt, j // ks[l] - rad, j % ks[l] - rad)  # [n,h,w,3]
+            gx[..., j] = (gd.transpose(0, 2, 3, 1) * xs_j).sum(axis=-1)
+        gdd = (gd * ds[l]).sum(axis=1)[..., None]
+        dl = np.zeros(lg.shape)
+        dl[..., :taps] = sm * (gx - gdd)
+        if dalpha is not None:
+            dl[..., taps] = dalpha
+        grads[l] = dl
+        g = g_next
+    return loss, grads, c0

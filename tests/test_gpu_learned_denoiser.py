@@ -27,19 +27,22 @@ def module():
     vpt.cleanup()
 
 
-def random_flat(widths, seed, head_scale=0.3):
+def random_flat(widths, seed, head_scale=0.3, hc=32, coarse_hc=()):
     g = np.random.default_rng(seed)
     flat = []
-    for name, cin, cout in uo.layer_table(widths):
-        std = np.sqrt(2.0 / (9 * cin)) * (head_scale if name == "head" else 1.0)
+    for name, cin, cout in uo.layer_table(widths, hc, coarse_hc):
+        std = np.sqrt(2.0 / (9 * cin)) * (head_scale if name.startswith("head") else 1.0)
         flat += [g.standard_normal(cout * 9 * cin) * std, g.standard_normal(cout) * 0.05]
     return np.concatenate(flat).astype(np.float32)
 
 
-def test_network_gradient_matches_oracle():
+@pytest.mark.parametrize("coarse", [(), (3, 3)])
+def test_network_gradient_matches_oracle(coarse):
     widths = (16, 32, 32, 48, 64)
-    net = ld.KpnUNet(widths, kernel_size=5)
-    flat = random_flat(widths, 1)
+    net = ld.KpnUNet(widths, kernel_size=5, coarse_kernels=coarse)
+    hc = uo.head_channels_for(5, len(coarse) > 0)
+    chc = tuple(uo.head_channels_for(k, l < len(coarse)) for l, k in enumerate(coarse, start=1))
+    flat = random_flat(widths, 1, hc=hc, coarse_hc=chc)
     net.set_parameters(flat)
     g = np.random.default_rng(2)
     n, h, w = 2, 32, 32
@@ -51,11 +54,12 @@ def test_network_gradient_matches_oracle():
     d_x0 = torch.from_numpy(x0).to(torch.bfloat16).cuda()
     d_rad, d_tgt = torch.from_numpy(rad).cuda(), torch.from_numpy(tgt).cuda()
     logits = net.forward(d_x0)
-    _, loss, dl = net.head(logits, d_rad, d_tgt)
-    net.backward(dl)
+    _, loss, dls = net.reconstruct(d_rad, d_tgt)
+    net.backward(dls)
     torch.cuda.synchronize()
     net.check_errors()
-    ref_loss, ref_grad, ref_logits, _ = uo.network_loss_and_grad(flat.astype(np.float64), widths, x0, rad, tgt)
+    ref_loss, ref_grad, ref_logits, _ = uo.network_loss_and_grad(flat.astype(np.float64), widths, x0, rad, tgt,
+                                                                 coarse_ks=coarse)
     got_logits = logits.cpu().numpy().astype(np.float64)
     assert np.abs(got_logits - ref_logits).max() <= 2e-2 * np.abs(ref_logits).max()
     assert abs(float(loss) - ref_loss) <= 1e-3 * ref_loss
@@ -71,7 +75,7 @@ def test_network_gradient_matches_oracle():
 
 def test_training_on_tracer_pairs_beats_the_noisy_input(tmp_path):
     data = ld.TrainingSet(vpt, num_scenes=12, size=64, spp_levels=(1, 4, 16), target_spp=512, seed0=500, grid=64)
-    net = ld.KpnUNet(seed=3)
+    net = ld.KpnUNet(seed=3, coarse_kernels=(5, 5))
     hist = ld.train(net, data, steps=400, batch_size=8, lr=5e-4, seed=4)
     assert np.all(np.isfinite(hist["loss_curve"]))
     # held-out scenes
@@ -93,4 +97,5 @@ def test_training_on_tracer_pairs_beats_the_noisy_input(tmp_path):
     info = json.load(open(tmp_path / "model" / "model_info.json"))
     assert info["input_feature_maps"][0] == "Result" and info["blend"] == "kpn"
     back = ld.KpnUNet.load(str(tmp_path / "model"))
+    assert back.coarse_kernels == (5, 5)
     assert torch.equal(back.param, net.param) and torch.equal(back.param_bf16, net.param_bf16)

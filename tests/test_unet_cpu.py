@@ -145,3 +145,80 @@ def test_oracle_network_gradient_matches_finite_differences():
         lm = uo.network_loss_and_grad(fm, widths, x0, rad, tgt, round_bf16=False)[0]
         fd = (lp - lm) / (2 * hstep)
         assert abs(fd - grad[i]) <= 1e-5 * (abs(fd) + np.abs(grad).max() * 1e-3), (i, fd, grad[i])
+
+
+def test_multiscale_reconstruction_gradient_matches_autograd():
+    g = np.random.default_rng(6)
+    n, h, w = 2, 8, 12
+    ks = (5, 3, 3)
+    hcs = (32, 16, 16)
+    logits = [g.standard_normal((n, h >> l, w >> l, hcs[l])) for l in range(3)]
+    x0 = g.exponential(1.0, (n, 3, h, w))
+    t = g.exponential(1.0, (n, 3, h, w))
+    loss, grads, c0 = uo.multiscale_loss_and_grad(logits, x0, t, ks)
+
+    tl = [t64(lg, True) for lg in logits]
+    xs = [t64(x0)]
+    for _ in range(2):
+        xs.append(F.avg_pool2d(xs[-1], 2))
+
+    def apply(x, lg, k):
+        s = torch.softmax(lg[..., :k * k], dim=-1)
+        hh, ww = x.shape[2], x.shape[3]
+        xp = F.pad(x, (k // 2,) * 4)
+        out = torch.zeros_like(x)
+        for j in range(k * k):
+            out = out + s[..., j][:, None] * xp[:, :, j // k:j // k + hh, j % k:j % k + ww]
+        return out
+
+    ds = [apply(xs[l], tl[l], ks[l]) for l in range(3)]
+    c = ds[2]
+    for l in (1, 0):
+        a = torch.sigmoid(tl[l][..., ks[l] * ks[l]])[:, None]
+        up = lambda v: F.interpolate(v, scale_factor=2, mode="nearest")
+        c = ds[l] + a * (up(c) - up(F.avg_pool2d(ds[l], 2)))
+    tt = t64(t)
+    tloss = ((c - tt) ** 2 / (tt * tt + 1e-2)).sum() / c.numel()
+    tloss.backward()
+    assert np.allclose(c0, c.detach().numpy(), rtol=1e-12, atol=1e-14)
+    assert abs(loss - tloss.item()) <= 1e-12 * loss
+    for l in range(3):
+        used = ks[l] * ks[l] + (1 if l < 2 else 0)
+        assert np.allclose(grads[l][..., :used], tl[l].grad.numpy()[..., :used], atol=1e-14), l
+        assert np.all(grads[l][..., used:] == 0)
+
+
+def test_oracle_multiscale_network_gradient_matches_finite_differences():
+    widths = (16, 16, 16, 16, 32)
+    coarse_ks = (3, 3)
+    g = np.random.default_rng(8)
+    hc0 = uo.head_channels_for(5, True)
+    chc = (uo.head_channels_for(3, True), uo.head_channels_for(3, False))
+    flat = []
+    for name, cin, cout in uo.layer_table(widths, hc0, chc):
+        flat += [g.standard_normal(cout * 9 * cin) * np.sqrt(2.0 / (9 * cin)) * (0.3 if "head" in name else 1.0),
+                 g.standard_normal(cout) * 0.05]
+    flat = np.concatenate(flat)
+    n, h, w = 1, 16, 16
+    x0 = np.zeros((n, h, w, 16))
+    x0[..., :12] = g.standard_normal((n, h, w, 12))
+    rad = g.exponential(1.0, (n, 3, h, w))
+    tgt = g.exponential(1.0, (n, 3, h, w))
+    kw = dict(round_bf16=False, ks=5, coarse_ks=coarse_ks)
+    loss, grad, _, _ = uo.network_loss_and_grad(flat, widths, x0, rad, tgt, **kw)
+    names = [n_ for n_, _, _ in uo.layer_table(widths, hc0, chc)]
+    # indices in the coarse heads and the decoder levels they feed, plus random ones
+    offs, off = {}, 0
+    for name, cin, cout in uo.layer_table(widths, hc0, chc):
+        offs[name] = off
+        off += cout * 9 * cin + cout
+    idx = [offs["head1"] + 5, offs["head2"] + 17, offs["dec1b"] + 3, offs["dec2b"] + 40, offs["head"] + 9]
+    idx += list(g.integers(0, flat.size, 15))
+    for i in idx:
+        fp, fm = flat.copy(), flat.copy()
+        fp[i] += 1e-6
+        fm[i] -= 1e-6
+        fd = (uo.network_loss_and_grad(fp, widths, x0, rad, tgt, **kw)[0] -
+              uo.network_loss_and_grad(fm, widths, x0, rad, tgt, **kw)[0]) / 2e-6
+        assert abs(fd - grad[i]) <= 1e-5 * (abs(fd) + np.abs(grad).max() * 1e-3), (i, fd, grad[i])
+    assert "head2" in names
