@@ -459,11 +459,11 @@ def run_learned(vpt, lib, ctx, small):
     vpt.set_denoiser("Edge-Avoiding À-Trous Wavelet Transform")
     vpt.set_denoiser_property("iterations", "1")
     ms_feat = frame_ms(64)  # a frame with the feature pass
-    # both denoisers read feature maps accumulated over the first FEATURE_FRAMES frames; later frames
-    # are traced without the feature pass
+    # each denoiser with its own best feature setting: EAW's edge-stopping weights want feature maps
+    # accumulated over every frame (as the reference renders them); the learned denoiser reads feature
+    # maps accumulated over the first FEATURE_FRAMES frames (as it was trained), and later frames are
+    # traced without the feature pass
     kf = ld.FEATURE_FRAMES
-    vpt.set_feature_frame_limit(kf)
-    vpt.set_frame_index(0)
 
     def render_ms(spp):
         return min(spp, kf) * ms_feat + max(0.0, spp - kf) * ms_plain
@@ -476,14 +476,17 @@ def run_learned(vpt, lib, ctx, small):
         torch.cuda.synchronize()
         return r, a.elapsed_time(c)
 
-    rows = []
-    done = 0
+    rows = [{"spp": n} for n in ev["levels"]]
     eaw_ms, net_ms = {}, []
-    for n in ev["levels"]:
+    # pass 1: plain accumulation and EAW (features every frame)
+    vpt.set_frame_index(0)
+    done = 0
+    for row in rows:
+        n = row["spp"]
         vpt.render_frame(img, n - done)
         done = n
         plain = (vpt.get_film_sum(R, R).cuda() / n).float().contiguous()
-        row = {"spp": n, "plain": ld.relmse(plain, ref)}
+        row["plain"] = ld.relmse(plain, ref)
         best = None
         for it in (1, 2, 3, 4, 5):
             vpt.set_denoiser_property("iterations", str(it))
@@ -493,6 +496,16 @@ def run_learned(vpt, lib, ctx, small):
             if best is None or r < best[0]:
                 best = (r, it)
         row["eaw"], row["eaw_iterations"] = best
+    # pass 2: the learned denoiser (the same frames: identical film, features over the first kf frames)
+    vpt.set_denoiser("None")
+    vpt.set_feature_frame_limit(kf)
+    vpt.set_frame_index(0)
+    done = 0
+    for row in rows:
+        n = row["spp"]
+        vpt.render_frame(img, n - done)
+        done = n
+        plain = (vpt.get_film_sum(R, R).cuda() / n).float().contiguous()
 
         def learned_once():
             f = ld.read_features(vpt, img)
@@ -501,8 +514,6 @@ def run_learned(vpt, lib, ctx, small):
         den, ms = timed(learned_once)
         net_ms.append(ms)
         row["learned"] = ld.relmse(den, ref)
-        rows.append(row)
-    vpt.set_denoiser("None")
     vpt.set_use_feature_maps([])
     vpt.set_feature_frame_limit(0)
     net.check_errors()
@@ -510,7 +521,7 @@ def run_learned(vpt, lib, ctx, small):
     eaw_cost = statistics.median(sum(v) / len(v) for v in eaw_ms.values())
     net_cost = statistics.median(net_ms)
     plain_t = time_to_target(spp, [r["plain"] for r in rows], lambda s: s * ms_plain, ev["target"], True)
-    eaw_t = time_to_target(spp, [r["eaw"] for r in rows], lambda s: render_ms(s) + eaw_cost, ev["target"], False)
+    eaw_t = time_to_target(spp, [r["eaw"] for r in rows], lambda s: s * ms_feat + eaw_cost, ev["target"], False)
     learned_t = time_to_target(spp, [r["learned"] for r in rows], lambda s: render_ms(s) + net_cost, ev["target"],
                                False)
     peak, peak_kind = tensor_peak()
