@@ -644,6 +644,192 @@ __global__ void __launch_bounds__(kThreads) conv_strip_kernel(const StripArgs a)
 }
 
 // ---------------------------------------------------------------------------------------------
+// the row-strip weight gradient (images at least 128 pixels wide)
+// ---------------------------------------------------------------------------------------------
+// dw[co][t][ci] = sum over pixels p of dy[p][co] * x[p + off(t)][ci].  Per output row y of a 128-pixel
+// column: the 128 pixels are the K dimension; for tap (dy, dx) the x operand is the row strip of
+// input row y+dy-1 shifted by dx pixels (descriptor start + dx * 16 bytes, as in the forward strip
+// kernel), the dy operand is output-gradient row y.  Both operands are MN-major (8-channel planes of
+// 16-byte pixel rows: LBO = 128 between 8-pixel groups, SBO = plane stride between channel groups).
+// ROLE 0: A = x (M = input channels m0 .. m0+ma, zero planes beyond), B = dy (N = output channels);
+// ROLE 1: A = dy (M = output channels m0 .. m0+ma), B = x (N = input channels).  Each tap t of
+// [t0, t1) accumulates in its own TMEM block (columns (t - t0) * N) over every row the CTA owns; the
+// CTA writes its sums to partial[blockIdx.x][t * cin + ci][co] at the end (reduced in fixed order by
+// reduce_grads_kernel).  M = 64 accumulators occupy lanes 0-15 of each 32-lane quarter of TMEM.
+constexpr int kDyRing = 3;
+constexpr int kDyPlane = kBM * 16;  // 2048 bytes: 128 pixels x 16 bytes
+
+struct WgradStripArgs {
+    const bf16* x;      // [n][h][w][cin]
+    const bf16* dy;     // [n][h][w][cout]
+    float* partial;     // [splits][m_pad][cout]
+    int* err;
+    int n, h, w_, cin, cout;
+    int m0, ma;         // A channel range (input channels for role 0, output channels for role 1), ma 64 / 128
+    int t0, t1;         // taps of this pass
+    int xplanes, dyplanes;  // 8-channel planes per x strip / dy row in shared memory
+    int m_pad;
+    int xtiles, seg_rows, segs_per_col, tmem_cols;
+};
+
+template <int ROLE>
+__global__ void __launch_bounds__(kThreads) wgrad_strip_kernel(const WgradStripArgs a) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    __shared__ uint64_t bars[2];
+    __shared__ uint32_t tmem_slot;
+    const int tid = threadIdx.x;
+    const int N = ROLE == 0 ? a.cout : a.cin;
+    const uint32_t xrow = (uint32_t)a.xplanes * kPlane, dyrow = (uint32_t)a.dyplanes * kDyPlane;
+    const uint32_t sx = smem_u32(smem);
+    const uint32_t sdy = sx + kRing * xrow;
+    // channels gathered into the strips: x planes [x_c0, x_c0 + 8 * x_real), dy planes likewise
+    const int x_c0 = ROLE == 0 ? a.m0 : 0;
+    const int x_real = ROLE == 0 ? min(a.ma, a.cin - a.m0) / 8 : a.cin / 8;
+    const int dy_c0 = ROLE == 0 ? 0 : a.m0;
+    const int dy_real = ROLE == 0 ? a.cout / 8 : min(a.ma, a.cout - a.m0) / 8;
+
+    if (tid == 0) {
+        mbar_init(smem_u32(&bars[0]), 1);
+        mbar_init(smem_u32(&bars[1]), 1);
+        fence_mbar_init();
+    }
+    if (tid < 32) tmem_alloc(smem_u32(&tmem_slot), (uint32_t)a.tmem_cols);
+    // zero the padding planes of every ring slot once (the gathers never write them)
+    {
+        uint4* base = reinterpret_cast<uint4*>(smem);
+        const uint4 z = make_uint4(0u, 0u, 0u, 0u);
+        for (int slot = 0; slot < kRing; ++slot)
+            for (int q = tid; q < (a.xplanes - x_real) * kStripPix; q += kThreads)
+                base[(slot * xrow + (uint32_t)(x_real + q / kStripPix) * kPlane) / 16 + q % kStripPix] = z;
+        for (int slot = 0; slot < kDyRing; ++slot)
+            for (int q = tid; q < (a.dyplanes - dy_real) * kBM; q += kThreads)
+                base[(kRing * xrow + slot * dyrow + (uint32_t)(dy_real + q / kBM) * kDyPlane) / 16 + q % kBM] = z;
+    }
+    fence_proxy_async();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_slot;
+
+    auto load_x = [&](int n_img, int yy, int x0) {
+        const uint32_t base = sx + (uint32_t)(((yy + 1) % kRing + kRing) % kRing) * xrow;
+        const bool row_ok = yy >= 0 && yy < a.h;
+        for (int q = tid; q < kStripPix * x_real; q += kThreads) {
+            const int r = q % kStripPix, kc = q / kStripPix;
+            const int xx = x0 - 1 + r;
+            const bool v = row_ok && xx >= 0 && xx < a.w_;
+            const bf16* src = v ? a.x + (((size_t)n_img * a.h + yy) * a.w_ + xx) * a.cin + x_c0 + kc * 8 : a.x;
+            cp_async16(base + (uint32_t)kc * kPlane + (uint32_t)r * 16u, src, v);
+        }
+    };
+    auto load_dy = [&](int n_img, int yy, int x0) {
+        const uint32_t base = sdy + (uint32_t)(yy % kDyRing) * dyrow;
+        for (int q = tid; q < kBM * dy_real; q += kThreads) {
+            const int r = q % kBM, kc = q / kBM;
+            const int xx = x0 + r;
+            const bool v = yy < a.h && xx < a.w_;
+            const bf16* src = v ? a.dy + (((size_t)n_img * a.h + yy) * a.w_ + xx) * a.cout + dy_c0 + kc * 8 : a.dy;
+            cp_async16(base + (uint32_t)kc * kDyPlane + (uint32_t)r * 16u, src, v);
+        }
+    };
+
+    const uint32_t idesc = instr_desc(a.ma, N, 1, 1);
+    const int total_segs = a.n * a.xtiles * a.segs_per_col;
+    long g = 0;
+    int fail = 0;
+    for (int seg = blockIdx.x; seg < total_segs && !fail; seg += gridDim.x) {
+        const int col = seg / a.segs_per_col, part = seg % a.segs_per_col;
+        const int n_img = col / a.xtiles, x0 = (col % a.xtiles) * kBM;
+        const int y0 = part * a.seg_rows, y1 = min(a.h, y0 + a.seg_rows);
+        if (y0 >= y1) continue;
+        if (g > 0) {  // the previous segment's MMAs have read their rows
+            if (!mbar_wait(smem_u32(&bars[(g - 1) & 1]), (uint32_t)(((g - 1) >> 1) & 1))) fail = 1;
+            if (__syncthreads_or(fail)) break;
+        }
+        load_x(n_img, y0 - 1, x0);
+        load_x(n_img, y0, x0);
+        load_x(n_img, y0 + 1, x0);
+        load_dy(n_img, y0, x0);
+        cp_async_commit();
+        if (y0 + 2 <= y1) load_x(n_img, y0 + 2, x0);
+        if (y0 + 1 < y1) load_dy(n_img, y0 + 1, x0);
+        cp_async_commit();
+        for (int yrow = y0; yrow < y1; ++yrow, ++g) {
+            cp_async_wait<1>();
+            fence_proxy_async();
+            tc_fence_before();
+            if (__syncthreads_or(fail)) break;
+            if (tid == 0) {
+                tc_fence_after();
+                const uint32_t drow = sdy + (uint32_t)(yrow % kDyRing) * dyrow;
+                for (int t = a.t0; t < a.t1; ++t) {
+                    const int dyy = t / 3, dxx = t % 3;
+                    const uint32_t xs = sx + (uint32_t)((yrow + dyy) % kRing) * xrow + (uint32_t)dxx * 16u;
+                    const uint32_t dacc = tmem + (uint32_t)((t - a.t0) * N);
+                    for (int j = 0; j < kBM / 16; ++j) {
+                        const uint64_t dx_desc = smem_desc(xs + (uint32_t)j * 256u, 128, kPlane);
+                        const uint64_t dd_desc = smem_desc(drow + (uint32_t)j * 256u, 128, kDyPlane);
+                        const uint64_t da = ROLE == 0 ? dx_desc : dd_desc;
+                        const uint64_t db = ROLE == 0 ? dd_desc : dx_desc;
+                        mma_bf16(dacc, da, db, idesc, (g == 0 && j == 0) ? 0u : 1u);
+                    }
+                }
+                mma_commit(smem_u32(&bars[g & 1]));
+            }
+            if (yrow > y0) {  // the previous row's MMAs are done: its x and dy slots are free
+                if (!mbar_wait(smem_u32(&bars[(g - 1) & 1]), (uint32_t)(((g - 1) >> 1) & 1))) fail = 1;
+                if (__syncthreads_or(fail)) break;
+            }
+            if (yrow + 3 <= y1) load_x(n_img, yrow + 3, x0);
+            if (yrow + 2 < y1) load_dy(n_img, yrow + 2, x0);
+            cp_async_commit();
+        }
+    }
+    cp_async_wait<0>();
+    bool done = true;
+    if (g > 0) done = mbar_wait(smem_u32(&bars[(g - 1) & 1]), (uint32_t)(((g - 1) >> 1) & 1));
+    fail = __syncthreads_or(fail || !done);
+    tc_fence_after();
+    if (!fail) {
+        // accumulator rows: M = 128 -> lane = row; M = 64 -> lanes 0-15 of each warp quarter
+        const int warp = tid >> 5, lane = tid & 31;
+        const int row = a.ma == 128 ? warp * 32 + lane : (lane < 16 ? warp * 16 + lane : -1);
+        const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+        float* part = a.partial + (size_t)blockIdx.x * a.m_pad * a.cout;
+        for (int t = a.t0; t < a.t1; ++t) {
+            for (int c0 = 0; c0 < N; c0 += 16) {
+                float v[16];
+                tmem_ld16(trow + (uint32_t)((t - a.t0) * N + c0), v);
+                if (row < 0) continue;
+                if (g == 0) {
+#pragma unroll
+                    for (int i = 0; i < 16; ++i) v[i] = 0.0f;
+                }
+                if (ROLE == 0) {
+                    const int ci = a.m0 + row;
+                    if (ci >= a.cin) continue;
+                    float4* dst = reinterpret_cast<float4*>(part + (size_t)(t * a.cin + ci) * a.cout + c0);
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) dst[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+                } else {
+                    const int co = a.m0 + row;
+                    if (co >= a.cout) continue;
+#pragma unroll
+                    for (int i = 0; i < 16; ++i) part[(size_t)(t * a.cin + c0 + i) * a.cout + co] = v[i];
+                }
+            }
+        }
+    }
+    if (fail && tid == 0 && a.err) atomicExch(a.err, (int)VPT_ERR_ITER_LIMIT);
+    tc_fence_before();
+    __syncthreads();
+    if (tid < 32) {
+        tc_fence_after();
+        tmem_dealloc(tmem, (uint32_t)a.tmem_cols);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
 // small kernels around the convolutions (NHWC bf16, 8 channels = 16 bytes per thread)
 // ---------------------------------------------------------------------------------------------
 __device__ __forceinline__ void load8(const bf16* p, float (&f)[8]) {
@@ -1176,15 +1362,110 @@ inline size_t strip_smem_bytes(int cin, int cout) {
 // the row-strip kernel serves images at least one tile wide with at most 256 output channels; the
 // input channels are split into groups whose weights and ring fit in shared memory (one pass each,
 // summed through an fp32 partial)
-inline int strip_groups(int width, int cin, int cout) {
+inline int strip_groups(int width, int cin, int cout, bool any = false) {
     if (width < kBM || cout > 256) return 0;
     for (int g = 1; g <= 4; ++g) {
         const int cg = (cin / 16 + g - 1) / g * 16;
         // grouped passes re-stream an fp32 partial; they beat the gather kernel only for narrow
         // outputs (measured: 176 -> 32 faster, 160 -> 64 slower)
-        if (strip_smem_bytes(cg, cout) <= kStripSmemLimit) return (g == 1 || cout <= 32) ? g : 0;
+        if (strip_smem_bytes(cg, cout) <= kStripSmemLimit) return (g == 1 || cout <= 32 || any) ? g : 0;
     }
     return 0;
+}
+
+// Weight-gradient plan on row strips: the role (which tensor is A), the A channel chunks of at most
+// 128 (M = 64 or 128), tap groups so that taps x N <= 512 TMEM columns, and the shared memory of the
+// largest pass; 0 passes = not eligible (the gather kernel serves it).
+struct WgradPlan {
+    int role = 0, chunks = 0, taps_per = 9, groups = 1, passes = 0;
+    size_t smem = 0;
+};
+
+constexpr size_t kWgradSmemLimit = 220 * 1024;
+
+inline WgradPlan wgrad_plan(int width, int cin, int cout, bool any_width = false) {
+    WgradPlan best;
+    if (width < kBM) return best;
+    // with fewer than 64 channels on both sides the per-row MMAs are too small (M = 64, N = 32) to
+    // beat the gather kernel (measured); any_width lifts the rule
+    if (!any_width && cin < 64 && cout < 64) return best;
+    for (int role = 0; role < 2; ++role) {
+        const int mtot = role == 0 ? cin : cout, N = role == 0 ? cout : cin;
+        if (N > 256) continue;
+        WgradPlan p;
+        p.role = role;
+        p.chunks = (mtot + 127) / 128;
+        const int ma = mtot > 64 ? 128 : 64;  // largest chunk
+        p.taps_per = min(9, 512 / N);
+        p.groups = (9 + p.taps_per - 1) / p.taps_per;
+        p.passes = p.chunks * p.groups;
+        const int xplanes = role == 0 ? ma / 8 : cin / 8, dyplanes = role == 0 ? cout / 8 : ma / 8;
+        p.smem = (size_t)kRing * xplanes * kPlane + (size_t)kDyRing * dyplanes * kDyPlane;
+        if (p.smem > kWgradSmemLimit) continue;
+        if (best.passes == 0 || p.passes < best.passes) best = p;
+    }
+    return best;
+}
+
+inline void strip_segments(int n, int h, int w, int slots, int& xtiles, int& seg_rows, int& segs_per_col,
+                           int& total) {
+    xtiles = (w + kBM - 1) / kBM;
+    const int cols = n * xtiles;
+    const int want = max(cols, 2 * slots);
+    int spc = (want + cols - 1) / cols;
+    spc = min(spc, max(1, h / 4));
+    seg_rows = (h + spc - 1) / spc;
+    segs_per_col = (h + seg_rows - 1) / seg_rows;
+    total = cols * segs_per_col;
+}
+
+inline int wgrad_strip_grid(int n, int h, int w) {
+    int xt, sr, spc, total;
+    strip_segments(n, h, w, sm_count(), xt, sr, spc, total);
+    return min(total, sm_count());
+}
+
+cudaError_t launch_wgrad_strip(const bf16* x, const bf16* dy, float* partial, int* err, int n, int h, int w, int cin,
+                               int cout, const WgradPlan& plan, cudaStream_t s) {
+    WgradStripArgs a{};
+    a.x = x;
+    a.dy = dy;
+    a.partial = partial;
+    a.err = err;
+    a.n = n;
+    a.h = h;
+    a.w_ = w;
+    a.cin = cin;
+    a.cout = cout;
+    a.m_pad = (9 * cin + kBM - 1) / kBM * kBM;
+    const int slots = sm_count();
+    int total = 0;
+    strip_segments(n, h, w, slots, a.xtiles, a.seg_rows, a.segs_per_col, total);
+    const int grid = min(total, slots);
+    const int mtot = plan.role == 0 ? cin : cout, N = plan.role == 0 ? cout : cin;
+    cudaError_t e = cudaSuccess;
+    for (int c = 0; c < plan.chunks && e == cudaSuccess; ++c) {
+        a.m0 = c * 128;
+        a.ma = (mtot - a.m0) > 64 ? 128 : 64;
+        a.xplanes = plan.role == 0 ? a.ma / 8 : cin / 8;
+        a.dyplanes = plan.role == 0 ? cout / 8 : a.ma / 8;
+        const size_t smem = (size_t)kRing * a.xplanes * kPlane + (size_t)kDyRing * a.dyplanes * kDyPlane;
+        for (int gidx = 0; gidx < plan.groups && e == cudaSuccess; ++gidx) {
+            a.t0 = gidx * plan.taps_per;
+            a.t1 = min(9, a.t0 + plan.taps_per);
+            a.tmem_cols = pow2_cols((a.t1 - a.t0) * N);
+            if (plan.role == 0) {
+                e = cudaFuncSetAttribute(wgrad_strip_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                if (e == cudaSuccess) wgrad_strip_kernel<0><<<grid, kThreads, smem, s>>>(a);
+            } else {
+                e = cudaFuncSetAttribute(wgrad_strip_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                if (e == cudaSuccess) wgrad_strip_kernel<1><<<grid, kThreads, smem, s>>>(a);
+            }
+            count_launches(1);
+            if (e == cudaSuccess) e = cudaGetLastError();
+        }
+    }
+    return e;
 }
 
 cudaError_t launch_strip_pass(StripArgs a, cudaStream_t s) {
@@ -1260,7 +1541,8 @@ cudaError_t launch_strip(const ConvArgs& c, int groups, cudaStream_t s) {
 
 using namespace vpt::unet;
 
-static bool g_force_gather = false;
+static bool g_force_gather = false;  // conv path 1: the gather kernels everywhere
+static bool g_force_strip = false;   // conv path 2: the strip kernels wherever they apply
 
 extern "C" {
 
@@ -1286,7 +1568,7 @@ VptStatus vpt_unet_conv3x3(const void* x, const void* w, const float* bias, cons
     a.tmem_cols = pow2_cols(a.n_tile);
     a.relu = relu;
     a.out_f32 = out_f32;
-    const int groups = strip_groups(width, cin, cout);
+    const int groups = strip_groups(width, cin, cout, g_force_strip);
     if (groups > 0 && !g_force_gather)
         return launch_strip(a, groups, static_cast<cudaStream_t>(stream)) == cudaSuccess ? VPT_OK : VPT_ERR_CUDA;
     const long P = (long)n * h * width;
@@ -1295,8 +1577,10 @@ VptStatus vpt_unet_conv3x3(const void* x, const void* w, const float* bias, cons
 }
 
 // 1: every convolution uses the per-tile gather kernel (for comparisons); 0: row strips where eligible
-VptStatus vpt_unet_set_conv_path(int force_gather) {
-    g_force_gather = force_gather != 0;
+VptStatus vpt_unet_set_conv_path(int path) {
+    if (path < 0 || path > 2) return VPT_ERR_ARG;
+    g_force_gather = path == 1;
+    g_force_strip = path == 2;
     return VPT_OK;
 }
 
@@ -1328,6 +1612,10 @@ VptStatus vpt_unet_conv3x3_wgrad(const void* x, const void* dy, float* partial, 
     a.pix_per_split = pixels_per_split;
     const int mtiles = (9 * cin + kBM - 1) / kBM;
     a.m_pad = mtiles * kBM;
+    const WgradPlan plan = wgrad_plan(width, cin, cout, g_force_strip);
+    if (plan.passes > 0 && !g_force_gather)
+        return launch_wgrad_strip(a.x, a.w, partial, err, n, h, width, cin, cout, plan,
+                                  static_cast<cudaStream_t>(stream)) == cudaSuccess ? VPT_OK : VPT_ERR_CUDA;
     const long P = (long)n * h * width;
     const dim3 grid((unsigned)mtiles, (unsigned)((cout + a.n_tile - 1) / a.n_tile),
                     (unsigned)((P + pixels_per_split - 1) / pixels_per_split));
@@ -1335,6 +1623,13 @@ VptStatus vpt_unet_conv3x3_wgrad(const void* x, const void* dy, float* partial, 
 }
 
 int vpt_unet_wgrad_rows(int cin) { return (9 * cin + kBM - 1) / kBM * kBM; }
+
+int vpt_unet_wgrad_splits(int n, int h, int width, int cin, int cout, int pixels_per_split) {
+    if (n <= 0 || h <= 0 || width <= 0 || pixels_per_split <= 0) return 0;
+    if (!g_force_gather && wgrad_plan(width, cin, cout, g_force_strip).passes > 0) return wgrad_strip_grid(n, h, width);
+    const long P = (long)n * h * width;
+    return (int)((P + pixels_per_split - 1) / pixels_per_split);
+}
 
 VptStatus vpt_unet_rotate_weights(const void* w, void* wrot, int cin, int cout, void* stream) {
     if (!w || !wrot || !chan_ok(cin) || !chan_ok(cout)) return VPT_ERR_ARG;

@@ -185,7 +185,7 @@ class KpnUNet:
         mtiles = rows // 128
         splits = max(1, min((P + 63) // 64, (2 * 148 + mtiles - 1) // mtiles))
         pps = ((P + splits - 1) // splits + 63) // 64 * 64
-        splits = (P + pps - 1) // pps
+        splits = self.lib.vpt_unet_wgrad_splits(n, h, w, L["cin"], L["cout"], pps)
         part = self.buf("wgrad_partial", (splits * rows * L["cout"],), torch.float32)
         self._call("vpt_unet_conv3x3_wgrad", _p(x), _p(dy), _p(part), n, h, w, L["cin"], L["cout"], pps,
                    _p(self.err), self._stream())

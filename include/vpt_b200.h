@@ -372,19 +372,23 @@ VptStatus vpt_gather_bench(const float* buffer, size_t bytes, int blocks, int lo
  * the forward input as mask (ReLU derivative). */
 VptStatus vpt_unet_conv3x3(const void* x, const void* w, const float* bias, const void* mask, void* y, int n, int h,
                            int width, int cin, int cout, int relu, int out_f32, int* err, void* stream);
-/* Selects the convolution kernel: 1 = the per-tile gather kernel everywhere, 0 (default) = the
- * persistent row-strip kernel for images at least 128 pixels wide with at most 256 output channels
- * (input channels in up to 4 groups that fit in shared memory; groups summed through an fp32 partial
- * allocated on the stream). */
-VptStatus vpt_unet_set_conv_path(int force_gather);
+/* Selects the convolution kernels: 0 (default) = by shape (the persistent row-strip kernels for images
+ * at least 128 pixels wide where they are measured faster; input channels in up to 4 groups through an
+ * fp32 partial allocated on the stream), 1 = the per-tile gather kernels everywhere, 2 = the row-strip
+ * kernels wherever they apply. */
+VptStatus vpt_unet_set_conv_path(int path);
 /* Shared-memory ring depth of the per-tile gather kernel: 3 or 4 stages, 0 (default) = by shape. */
 VptStatus vpt_unet_set_gather_stages(int stages);
-/* Weight gradient: partial[s][t*cin + ci][co] = sum over pixels p of split s (pixels_per_split each,
- * a multiple of 64) of dy[p][co] x[p + off(t)][ci]; partial has vpt_unet_wgrad_rows(cin) rows per
- * split, reduced by vpt_unet_reduce_grads. */
+/* Weight gradient: partial[s][t*cin + ci][co] = sum over the pixels p of split s of
+ * dy[p][co] x[p + off(t)][ci]; vpt_unet_wgrad_splits splits (pixels_per_split a multiple of 64 sizes
+ * them for the gather kernel), vpt_unet_wgrad_rows(cin) rows each, reduced by vpt_unet_reduce_grads. */
 VptStatus vpt_unet_conv3x3_wgrad(const void* x, const void* dy, float* partial, int n, int h, int width, int cin,
                                  int cout, int pixels_per_split, int* err, void* stream);
 int vpt_unet_wgrad_rows(int cin);
+/* Number of partial sums (splits) vpt_unet_conv3x3_wgrad writes for this shape: the row-strip kernel
+ * (images at least 128 pixels wide) writes one per CTA, the gather kernel one per pixels_per_split
+ * pixels. */
+int vpt_unet_wgrad_splits(int n, int h, int width, int cin, int cout, int pixels_per_split);
 /* wrot[ci][t][co] = w[co][8 - t][ci] */
 VptStatus vpt_unet_rotate_weights(const void* w, void* wrot, int cin, int cout, void* stream);
 /* 2x2 average pooling [n][h][w][c] -> [n][h/2][w/2][c] */

@@ -132,6 +132,7 @@ STRIP_CASES = [
 @pytest.mark.parametrize("case", STRIP_CASES)
 def test_strip_conv_forward_and_input_grad(lib, case):
     n, h, w, cin, cout = case
+    assert lib.vpt_unet_set_conv_path(2) == 0
     x = uo.bf16(rng_data(21, n, h, w, cin))
     wt = uo.bf16(rng_data(22, cout, 9, cin, scale=1.0 / np.sqrt(9 * cin)))
     bias = rng_data(23, cout, scale=0.1)
@@ -146,7 +147,7 @@ def test_strip_conv_forward_and_input_grad(lib, case):
     assert lib.vpt_unet_set_conv_path(1) == 0
     y2 = torch.empty_like(y)
     run(lib, "vpt_unet_conv3x3", ptr(dx), ptr(dw), ptr(b), None, ptr(y2), n, h, w, cin, cout, 0, 1)
-    assert lib.vpt_unet_set_conv_path(0) == 0
+    assert lib.vpt_unet_set_conv_path(2) == 0
     close_f32(host(y2), host(y))
     # input gradient with the ReLU-derivative mask (rotated weights: cout -> cin; 176 input channels
     # of the head's gradient take two channel groups)
@@ -157,15 +158,25 @@ def test_strip_conv_forward_and_input_grad(lib, case):
     d_dy = dev_bf16(dy)  # kept alive: a temporary's memory may be reused by the next allocation
     run(lib, "vpt_unet_conv3x3", ptr(d_dy), ptr(wrot), None, ptr(dx), ptr(g), n, h, w, cout, cin, 0, 0)
     close_bf16(host(g), uo.conv3x3_input_grad(dy, wt, mask=x))
+    assert lib.vpt_unet_set_conv_path(0) == 0
 
 
 WGRAD_CASES = [
-    # n, h, w, cin, cout, pixels per split
+    # n, h, w, cin, cout, pixels per split (images narrower than 128 pixels: the gather kernel)
     (2, 9, 13, 16, 32, 64),
     (1, 16, 16, 96, 160, 128),
     (1, 8, 8, 288, 128, 64),
     (2, 6, 10, 32, 288, 192),
     (1, 32, 32, 64, 64, 1024),
+    # row-strip weight gradient (>= 128 pixels wide): input channels as M (padded to 64 / 128),
+    # output channels as M (two chunks), tap groups, several segments per column
+    (1, 5, 130, 32, 32, 64),
+    (2, 7, 256, 16, 32, 64),
+    (1, 4, 128, 96, 32, 64),
+    (1, 5, 200, 32, 176, 64),
+    (1, 6, 128, 64, 64, 64),
+    (1, 4, 128, 160, 64, 64),
+    (1, 37, 128, 32, 32, 64),
 ]
 
 
@@ -175,7 +186,9 @@ def test_conv_weight_grad(lib, case):
     x = uo.bf16(rng_data(8, n, h, w, cin))
     dy = uo.bf16(rng_data(9, n, h, w, cout))
     P = n * h * w
-    splits = (P + pps - 1) // pps
+    assert lib.vpt_unet_set_conv_path(2 if w >= 128 else 0) == 0  # the strip kernel on every wide case
+    splits = lib.vpt_unet_wgrad_splits(n, h, w, cin, cout, pps)
+    assert splits >= 1
     rows = lib.vpt_unet_wgrad_rows(cin)
     assert rows % 128 == 0 and rows >= 9 * cin
     part = torch.full((splits, rows, cout), float("nan"), dtype=torch.float32, device="cuda")
@@ -188,6 +201,7 @@ def test_conv_weight_grad(lib, case):
     gb = torch.empty((cout,), dtype=torch.float32, device="cuda")
     assert lib.vpt_unet_reduce_grads(ptr(part), splits, cin, cout, ptr(bpart), bblocks, ptr(gw), ptr(gb), None) == 0
     torch.cuda.synchronize()
+    assert lib.vpt_unet_set_conv_path(0) == 0
     close_f32(host(gw), uo.conv3x3_weight_grad(x, dy))
     close_f32(host(gb), uo.bias_grad(dy))
 
