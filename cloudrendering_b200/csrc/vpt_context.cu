@@ -199,6 +199,7 @@ struct VptContext {
     uint32_t film_frames = 0;      // frames held in the film (1 for SVGF, which wants 1-spp input)
     uint32_t feat_frames = 0;      // frames held in the feature accumulators
     uint32_t feature_frame_limit = 0;  // > 0: feature maps accumulate over the first this many frames only
+    int sdt_prob = vpt::kSdtPathHistory;  // sdtCollisionProbability (VolumetricPathTracingPass.hpp:250-251)
     DevBuf<double> film, film_sq;
     bool collect_stats = false;
     bool features_on = false;
@@ -358,6 +359,8 @@ int tracker_of(int mode) {
         case VPT_MODE_DECOMPOSITION_TRACKING: return vpt::kDecomposition;
         case VPT_MODE_RESIDUAL_RATIO_TRACKING: return vpt::kResidualRatio;
         case VPT_MODE_NEXT_EVENT_TRACKING: return vpt::kNextEvent;
+        case VPT_MODE_SPECTRAL_DELTA_TRACKING: return vpt::kSpectralDelta;
+        case VPT_MODE_NEXT_EVENT_TRACKING_SPECTRAL: return vpt::kSpectralNextEvent;
         default: return -1;
     }
 }
@@ -379,13 +382,14 @@ float extinction_x(const VptContext* ctx) { return ctx->extinction_base[0] * ctx
 
 VptStatus ensure_accel(VptContext* ctx, int tracker, cudaStream_t s) {
     if (ctx->use_sparse) {
-        if (tracker == vpt::kResidualRatio || (tracker == vpt::kNextEvent && ctx->use_ess))
+        if (tracker == vpt::kResidualRatio ||
+            ((tracker == vpt::kNextEvent || tracker == vpt::kSpectralNextEvent) && ctx->use_ess))
             return fail(ctx, VPT_ERR_UNSUPPORTED,
                         "residual ratio tracking and empty space skipping need a dense grid (as in the reference)");
         return ensure_sparse(ctx, s);
     }
     const bool need_sv = tracker == vpt::kDecomposition || tracker == vpt::kResidualRatio;
-    const bool need_occ = tracker == vpt::kNextEvent && ctx->use_ess;
+    const bool need_occ = (tracker == vpt::kNextEvent || tracker == vpt::kSpectralNextEvent) && ctx->use_ess;
     if (need_sv) {
         // setExtinctionScale does not rebuild the RRT grid in the reference
         // (VolumetricPathTracingPass.cpp:1289-1291); here the grid follows the current extinction.
@@ -494,6 +498,13 @@ VptStatus fill_params(VptContext* ctx, int tracker, int frames, vpt::TraceParams
     P.inv_extinction = 1.0f / P.extinction;
     P.albedo = ctx->albedo[0];
     P.absorb_albedo = 1.0f - ctx->albedo[0];
+    for (int c = 0; c < 3; ++c) {
+        P.ext_rgb[c] = ctx->extinction_base[c] * ctx->extinction_scale;
+        P.albedo_rgb[c] = ctx->albedo[c];
+    }
+    P.sdt_majorant = std::max(P.ext_rgb[0], std::max(P.ext_rgb[1], P.ext_rgb[2]));
+    P.inv_sdt_majorant = 1.0f / P.sdt_majorant;
+    P.sdt_prob = ctx->sdt_prob;
     P.g = ctx->g;
     P.interp = ctx->interp;
     P.max_bounces = ctx->max_bounces;
@@ -1719,7 +1730,12 @@ VptStatus vpt_set_option(VptContext* ctx, const char* key, double value) {
     VPT_CHECK_CTX(ctx);
     if (!key) return VPT_ERR_ARG;
     std::string k(key);
-    if (k == "feature_frames") {
+    if (k == "sdt_collision_probability") {
+        if (value != 0.0 && value != 1.0 && value != 2.0)
+            return fail(ctx, VPT_ERR_ARG, "sdt_collision_probability: 0 (max), 1 (avg) or 2 (path history avg)");
+        ctx->sdt_prob = (int)value;
+        reset_film_state(ctx);
+    } else if (k == "feature_frames") {
         if (value < 0 || value > 1e9) return fail(ctx, VPT_ERR_ARG, "feature_frames out of range");
         ctx->feature_frame_limit = (uint32_t)value;
         reset_film_state(ctx);

@@ -73,6 +73,9 @@ VPT_DEV F3 run_tracker(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, Fi
         else return track_decomposition(P, sample, rng, x, w, fe, pc);
     }
     if (TRACKER == kResidualRatio) return track_residual_ratio(P, sample, rng, x, w, fe, pc);
+    if constexpr (TRACKER == kSpectralDelta) return track_delta_spectral(P, sample, rng, x, w, fe, pc);
+    if constexpr (TRACKER == kSpectralNextEvent) return track_nee_spectral<false>(P, sample, rng, x, w, fe, pc);
+    if constexpr (TRACKER == kSpectralNextEvent + 100) return track_nee_spectral<true>(P, sample, rng, x, w, fe, pc);
     if (TRACKER == kNextEvent + 100) return track_nee<true>(P, sample, rng, x, w, fe, pc);
     return track_nee<false>(P, sample, rng, x, w, fe, pc);
 }
@@ -600,6 +603,11 @@ cudaError_t launch_trace(const TraceParams& P, int tracker, int use_ess, int sch
             case kNextEvent:
                 if (use_ess) return cudaErrorNotSupported;
                 return launch_interp<kNextEvent, kNanoVdb>(P, schedule, features, persistent_blocks, stream);
+            case kSpectralDelta:
+                return launch_interp<kSpectralDelta, kNanoVdb>(P, schedule, features, persistent_blocks, stream);
+            case kSpectralNextEvent:
+                if (use_ess) return cudaErrorNotSupported;
+                return launch_interp<kSpectralNextEvent, kNanoVdb>(P, schedule, features, persistent_blocks, stream);
             default: return cudaErrorNotSupported;
         }
     }
@@ -611,6 +619,11 @@ cudaError_t launch_trace(const TraceParams& P, int tracker, int use_ess, int sch
         case kNextEvent:
             if (use_ess) return launch_interp<kNextEvent + 100, kDense>(P, schedule, features, persistent_blocks, stream);
             return launch_interp<kNextEvent, kDense>(P, schedule, features, persistent_blocks, stream);
+        case kSpectralDelta: return launch_interp<kSpectralDelta, kDense>(P, schedule, features, persistent_blocks, stream);
+        case kSpectralNextEvent:
+            if (use_ess)
+                return launch_interp<kSpectralNextEvent + 100, kDense>(P, schedule, features, persistent_blocks, stream);
+            return launch_interp<kSpectralNextEvent, kDense>(P, schedule, features, persistent_blocks, stream);
         default: return cudaErrorInvalidValue;
     }
 }

@@ -12,11 +12,17 @@ namespace vpt {
 
 enum Tracker : int {
     kDelta = 0,
+    kSpectralDelta = 1,
     kRatio = 2,
     kDecomposition = 3,
     kResidualRatio = 4,
     kNextEvent = 5,
+    kSpectralNextEvent = 6,
 };
+
+// Collision probabilities of spectral tracking (SpectralDeltaTrackingCollisionProbability,
+// src/PathTracer/RenderSettings.hpp:64-69).
+enum SdtProbability : int { kSdtMax = 0, kSdtAvg = 1, kSdtPathHistory = 2 };
 
 enum GridKind : int { kDense = 0, kNanoVdb = 1 };
 enum Interp : int { kNearest = 0, kStochastic = 1, kTrilinear = 2 };
@@ -112,6 +118,11 @@ struct TraceParams {
     float inv_extinction;
     float albedo;              // parameters.scatteringAlbedo.x
     float absorb_albedo;       // 1 - albedo
+    float ext_rgb[3];          // parameters.extinction (spectral trackers)
+    float albedo_rgb[3];       // parameters.scatteringAlbedo (spectral trackers)
+    float sdt_majorant;        // maxComponent(parameters.extinction)
+    float inv_sdt_majorant;
+    int sdt_prob;              // SdtProbability
     float g;                   // Henyey-Greenstein parameter
     int interp;                // Interp
     int max_bounces;           // 0 = unlimited

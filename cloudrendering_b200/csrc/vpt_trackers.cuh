@@ -322,6 +322,184 @@ VPT_DEV F3 track_nee(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, Firs
 }
 
 // ---------------------------------------------------------------------------------------------
+// Spectral tracking (Kutz et al. 2017): chromatic extinction parameters.extinction (rgb) with the
+// majorant maxComponent(extinction); per-channel path weights; the collision probabilities of the
+// three SpectralDeltaTrackingCollisionProbability modes.  Arithmetic in the shader's order.
+struct SdtStep {
+    float pa, ps, pn;  // normalised collision probabilities
+    F3 sa, ss, sn;     // sigma_a, sigma_s, sigma_n
+};
+
+VPT_DEV float max_component(F3 v) { return fmaxf(v.x, fmaxf(v.y, v.z)); }
+VPT_DEV float avg_component(F3 v) { return ((v.x + v.y) + v.z) / 3.0f; }
+
+VPT_DEV SdtStep sdt_probabilities(const TraceParams& P, float density, F3 weights) {
+    const F3 ext = f3(P.ext_rgb[0], P.ext_rgb[1], P.ext_rgb[2]);
+    const F3 alb = f3(P.albedo_rgb[0], P.albedo_rgb[1], P.albedo_rgb[2]);
+    const F3 abs_alb = f3(1.0f - alb.x, 1.0f - alb.y, 1.0f - alb.z);
+    SdtStep s;
+    s.sa = f3((abs_alb.x * ext.x) * density, (abs_alb.y * ext.y) * density, (abs_alb.z * ext.z) * density);
+    s.ss = f3((alb.x * ext.x) * density, (alb.y * ext.y) * density, (alb.z * ext.z) * density);
+    const float m = P.sdt_majorant;
+    s.sn = f3(m - ext.x * density, m - ext.y * density, m - ext.z * density);
+    if (P.sdt_prob == kSdtMax) {
+        s.pa = max_component(s.sa);
+        s.ps = max_component(s.ss);
+        s.pn = max_component(s.sn);
+    } else if (P.sdt_prob == kSdtAvg) {
+        s.pa = avg_component(s.sa);
+        s.ps = avg_component(s.ss);
+        s.pn = avg_component(s.sn);
+    } else {
+        s.pa = avg_component(f3(s.sa.x * weights.x, s.sa.y * weights.y, s.sa.z * weights.z));
+        s.ps = avg_component(f3(s.ss.x * weights.x, s.ss.y * weights.y, s.ss.z * weights.z));
+        s.pn = avg_component(f3(s.sn.x * weights.x, s.sn.y * weights.y, s.sn.z * weights.z));
+    }
+    const float c = (s.pa + s.ps) + s.pn;
+    s.pa /= c;
+    s.ps /= c;
+    s.pn /= c;
+    return s;
+}
+
+// weights *= sigma / (majorant * P)
+VPT_DEV F3 sdt_reweight(F3 weights, F3 sigma, float majorant, float p) {
+    const float den = majorant * p;
+    return f3(weights.x * (sigma.x / den), weights.y * (sigma.y / den), weights.z * (sigma.z / den));
+}
+
+VPT_DEV F3 sdt_clamp(F3 v, float c) { return f3(fminf(v.x, c), fminf(v.y, c), fminf(v.z, c)); }
+
+// VptMode::SPECTRAL_DELTA_TRACKING (deltaTrackingSpectral, DeltaTracking.glsl:33-163).
+template <class S>
+VPT_DEV F3 track_delta_spectral(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, FirstEvent& fe,
+                                PathCtx& pc) {
+    F3 weights = f3(1.0f, 1.0f, 1.0f);
+    float tmin, tmax;
+    if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
+        x = x + w * tmin;
+        float d = tmax - tmin;
+        int bounces = 0;
+        while (true) {
+            if (guard(pc)) return f3(0.0f, 0.0f, 0.0f);
+            float t = free_path(rng, P.inv_sdt_majorant);
+            if (t > d) break;
+            F3 xn = x + w * t;
+            float density = sample(xn, rng);
+            pc.lookups++;
+            x = xn;
+            const SdtStep st = sdt_probabilities(P, density, weights);
+            float xi = rng_next(rng);
+            if (xi < st.pa) {
+                record_event(fe, x, density, P.sdt_majorant, tmax - d + t);
+                return f3(0.0f, 0.0f, 0.0f);
+            }
+            if (xi < st.pa + st.ps) {
+                if (P.max_bounces > 0 && ++bounces > P.max_bounces) return f3(0.0f, 0.0f, 0.0f);
+                w = sample_phase(rng, P.g, w);
+                record_event(fe, x, density, P.sdt_majorant, tmax - d + t);
+                if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
+                    x = x + w * tmin;
+                    d = tmax - tmin;
+                }
+                weights = sdt_reweight(weights, st.ss, P.sdt_majorant, st.ps);
+            } else {
+                d -= t;
+                weights = sdt_reweight(weights, st.sn, P.sdt_majorant, st.pn);
+            }
+            if (P.sdt_prob == kSdtPathHistory) weights = sdt_clamp(weights, 100.0f);
+        }
+    }
+    const F3 wc = sdt_clamp(weights, 100000.0f);
+    const F3 l = sky_and_sun(P, w);
+    return f3(wc.x * l.x, wc.y * l.y, wc.z * l.z);
+}
+
+// VptMode::NEXT_EVENT_TRACKING_SPECTRAL (nextEventTrackingSpectral, NextEventTracking.glsl:31-220):
+// spectral tracking with a next-event estimate at every scatter event (transmittance from the
+// achromatic shadow estimators, NeeTransmittance.glsl, like the reference).
+template <bool ESS, class S>
+VPT_DEV F3 track_nee_spectral(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, FirstEvent& fe, PathCtx& pc) {
+    F3 weights = f3(1.0f, 1.0f, 1.0f);
+    F3 color = f3(0.0f, 0.0f, 0.0f);
+    float tmin, tmax;
+    if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
+        x = x + w * tmin;
+        float d = tmax - tmin;
+        int bounces = 0;
+        while (true) {
+            if (guard(pc)) return color;
+            float t = free_path(rng, P.inv_sdt_majorant);
+            if (t > d) break;
+            F3 xn = x + w * t;
+            float density = sample(xn, rng);
+            pc.lookups++;
+            x = xn;
+            const SdtStep st = sdt_probabilities(P, density, weights);
+            float xi = rng_next(rng);
+            if (xi < st.pa) {
+                record_event(fe, x, density, P.sdt_majorant, tmax - d + t);
+                return color;
+            }
+            if (xi < st.pa + st.ps) {
+                if (P.max_bounces > 0 && ++bounces > P.max_bounces) return color;
+                F3 next_w = sample_phase(rng, P.g, w);
+                record_event(fe, x, density, P.sdt_majorant, tmax - d + t);
+                bool to_light = false;
+                float prob_factor = 1.0f, light_dist = 0.0f, pdf_light = 0.0f;
+                int light_idx = 0;
+                F3 dir_light;
+                if (P.num_lights > 0) {
+                    to_light = P.env_is_black ? true : (rng_next(rng) > 0.5f);
+                    prob_factor = P.env_is_black ? 1.0f : 2.0f;
+                }
+                if (to_light) dir_light = light_direction(P, x, rng, light_idx, prob_factor, light_dist);
+                else dir_light = importance_sample_sky(P, rng, pdf_light);
+                const float pdf_phase = evaluate_phase(P.g, w, dir_light);
+                w = next_w;
+                weights = sdt_reweight(weights, st.ss, P.sdt_majorant, st.ps);
+                const F3 wc = sdt_clamp(weights, 100000.0f);
+                if (P.num_lights > 0) {
+                    const float cf = prob_factor * pdf_phase;
+                    const F3 common = f3(cf * wc.x, cf * wc.y, cf * wc.z);
+                    if (to_light) {
+                        const float tr = shadow_transmittance_distance(P, sample, rng, x, dir_light, light_dist, pc);
+                        const F3 l = light_radiance(P, x, light_idx);
+                        color = color + f3((common.x * tr) * l.x, (common.y * tr) * l.y, (common.z * tr) * l.z);
+                    } else {
+                        const float tr = ESS ? shadow_transmittance_ess(P, sample, rng, x, dir_light, pc)
+                                             : shadow_transmittance(P, sample, rng, x, dir_light, pc);
+                        const F3 l = sky_and_sun(P, dir_light);
+                        color = color + f3(((common.x / pdf_light) * tr) * l.x, ((common.y / pdf_light) * tr) * l.y,
+                                           ((common.z / pdf_light) * tr) * l.z);
+                    }
+                } else {
+                    const float tr = ESS ? shadow_transmittance_ess(P, sample, rng, x, dir_light, pc)
+                                         : shadow_transmittance(P, sample, rng, x, dir_light, pc);
+                    const float f = (pdf_phase / pdf_light) * tr;
+                    const F3 l = sky_and_sun(P, dir_light);
+                    color = color + f3((f * wc.x) * l.x, (f * wc.y) * l.y, (f * wc.z) * l.z);
+                }
+                if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
+                    x = x + w * tmin;
+                    d = tmax - tmin;
+                }
+            } else {
+                d -= t;
+                weights = sdt_reweight(weights, st.sn, P.sdt_majorant, st.pn);
+            }
+            if (P.sdt_prob == kSdtPathHistory) weights = sdt_clamp(weights, 100.0f);
+        }
+    }
+    if (!fe.has) {
+        const F3 wc = sdt_clamp(weights, 100000.0f);
+        const F3 l = sky_and_sun(P, w);
+        color = color + f3((1.0f * wc.x) * l.x, (1.0f * wc.y) * l.y, (1.0f * wc.z) * l.z);
+    }
+    return color;
+}
+
+// ---------------------------------------------------------------------------------------------
 // Supervoxel stepping shared by decomposition tracking and the occupancy-grid shadow ray: after a
 // supervoxel is left, move to the neighbour along the dominant axis of (x + 1e-5 w - centre)
 // (DecompositionTracking.glsl:112-118).

@@ -375,6 +375,18 @@ def set_vpt_mode_from_name(mode_name: str) -> None:
         set_vpt_mode(VPT_MODE_NAMES.index(mode_name))
 
 
+# SPECTRAL_DELTA_TRACKING_COLLISION_PROBABILITY_NAMES (src/PathTracer/RenderSettings.hpp:64-69)
+SDT_COLLISION_PROBABILITY_NAMES = ["Max-based", "Avg-based", "Path History Avg-based"]
+
+
+def set_spectral_delta_tracking_collision_probability(name: str) -> None:
+    """Collision probabilities of the spectral trackers (VolumetricPathTracingPass::sdtCollisionProbability,
+    set in the reference's GUI; default "Path History Avg-based")."""
+    if name not in SDT_COLLISION_PROBABILITY_NAMES:
+        raise RuntimeError(f"Error: invalid spectral delta tracking collision probability \"{name}\".")
+    _c("vpt_set_option", b"sdt_collision_probability", float(SDT_COLLISION_PROBABILITY_NAMES.index(name)))
+
+
 def set_grid_interpolation(name: str) -> None:
     if name not in GRID_INTERPOLATION_TYPE_NAMES:
         raise RuntimeError(f"Unknown grid interpolation type \"{name}\".")

@@ -37,6 +37,7 @@ class OracleScene(ctypes.Structure):
         ("nanovdb", c_void_p), ("grid_min", c_float * 3), ("grid_max", c_float * 3),
         ("sparse_lowest_level", c_int), ("sparse_fp16", c_int),
         ("inv_view", c_float * 16), ("num_lights", c_int), ("env_is_black", c_int), ("lights", c_float * 256),
+        ("ext_rgb", c_float * 3), ("albedo_rgb", c_float * 3), ("sdt_prob", c_int),
     ]
 
 
@@ -82,6 +83,11 @@ def load():
         lib.oracle_set_double_rounded_math.restype = None
         _lib = lib
     return _lib
+
+
+def _ok(status: int) -> None:
+    if status != 0:
+        raise RuntimeError(f"oracle: scene rejected (status {status}): a tracker input is missing")
 
 
 def _p(a: np.ndarray | None):
@@ -203,13 +209,13 @@ class Scene:
         film = np.zeros(n, np.float64)
         sq = np.zeros(n, np.float64) if with_sq else None
         lk = c_uint64(0)
-        load().oracle_render(ctypes.byref(self.s), _p(film), _p(sq), ctypes.byref(lk), threads)
+        _ok(load().oracle_render(ctypes.byref(self.s), _p(film), _p(sq), ctypes.byref(lk), threads))
         return film, sq, lk.value
 
     def render_rows(self, row0, row1, threads=0):
         film = np.zeros(self.s.width * self.s.height * 3, np.float64)
         lk = c_uint64(0)
-        load().oracle_render_rows(ctypes.byref(self.s), row0, row1, _p(film), ctypes.byref(lk), threads)
+        _ok(load().oracle_render_rows(ctypes.byref(self.s), row0, row1, _p(film), ctypes.byref(lk), threads))
         return film, lk.value
 
     def trace_paths(self, xs, ys, frames, threads=0):
@@ -217,7 +223,7 @@ class Scene:
         ys = np.ascontiguousarray(ys, np.int32)
         fr = np.ascontiguousarray(frames, np.uint32)
         out = np.empty((xs.size, 3), np.float32)
-        load().oracle_trace_paths(ctypes.byref(self.s), _p(xs), _p(ys), _p(fr), xs.size, _p(out), threads)
+        _ok(load().oracle_trace_paths(ctypes.byref(self.s), _p(xs), _p(ys), _p(fr), xs.size, _p(out), threads))
         return out
 
 

@@ -53,6 +53,10 @@ ENVS = {
 
 # NEE with lights (NUM_LIGHTS > 0): stochastic lookups, default and black environments
 LIGHT_VARIANTS = {"nee_l1": 1, "nee_l2": 2}
+# spectral trackers, one variant per collision-probability mode (VolumetricPathTracingPass.cpp:1566-1584)
+SDT_PROB = {"max": "MAX_BASED_PROBABILITY", "avg": "AVG_BASED_PROBABILITY",
+            "hist": "PATH_HISTORY_AVG_BASED_PROBABILITY"}
+SPECTRAL = {"sdt": "USE_SPECTRAL_DELTA_TRACKING", "nees": "USE_NEXT_EVENT_TRACKING_SPECTRAL"}
 
 
 def variants():
@@ -65,6 +69,10 @@ def variants():
     for t, n in LIGHT_VARIANTS.items():
         for e in ("default__linear", "black__linear"):
             out.append((f"{t}__stochastic__{e}", TRACKERS["nee"] + [INTERPS["stochastic"]] + ENVS[e], n))
+    for t, tdef in SPECTRAL.items():
+        for p, pdef in SDT_PROB.items():
+            for i in ("stochastic", "trilinear"):
+                out.append((f"{t}_{p}__{i}__default__linear", [tdef, pdef, INTERPS[i]] + ENVS["default__linear"], 0))
     return out
 
 

@@ -862,6 +862,172 @@ struct Tracer {
         return color;
     }
 
+    // ---- spectral tracking (Kutz et al. 2017) ----
+    V3 ext3() const {
+        if (S.ext_rgb[0] == 0.0f && S.ext_rgb[1] == 0.0f && S.ext_rgb[2] == 0.0f)
+            return v3(S.extinction, S.extinction, S.extinction);
+        return v3(S.ext_rgb[0], S.ext_rgb[1], S.ext_rgb[2]);
+    }
+    V3 alb3() const {
+        if (S.ext_rgb[0] == 0.0f && S.ext_rgb[1] == 0.0f && S.ext_rgb[2] == 0.0f)
+            return v3(S.albedo, S.albedo, S.albedo);
+        return v3(S.albedo_rgb[0], S.albedo_rgb[1], S.albedo_rgb[2]);
+    }
+    static float maxc(V3 v) { return std::max(v.x, std::max(v.y, v.z)); }
+    static float avgc(V3 v) { return ((v.x + v.y) + v.z) / 3.0f; }
+    static V3 cmin(V3 v, float c) { return v3(std::min(v.x, c), std::min(v.y, c), std::min(v.z, c)); }
+    static V3 cmul(V3 a, V3 b) { return v3(a.x * b.x, a.y * b.y, a.z * b.z); }
+    // the collision probabilities of one real-or-null collision (DeltaTracking.glsl:90-110)
+    void sdt_step(float dens, V3 weights, float maj, V3& sa, V3& ss, V3& sn, float& pa, float& ps, float& pn) const {
+        const V3 ext = ext3(), alb = alb3();
+        const V3 aa = v3(1.0f - alb.x, 1.0f - alb.y, 1.0f - alb.z);
+        sa = v3((aa.x * ext.x) * dens, (aa.y * ext.y) * dens, (aa.z * ext.z) * dens);
+        ss = v3((alb.x * ext.x) * dens, (alb.y * ext.y) * dens, (alb.z * ext.z) * dens);
+        sn = v3(maj - ext.x * dens, maj - ext.y * dens, maj - ext.z * dens);
+        if (S.sdt_prob == 0) {
+            pa = maxc(sa);
+            ps = maxc(ss);
+            pn = maxc(sn);
+        } else if (S.sdt_prob == 1) {
+            pa = avgc(sa);
+            ps = avgc(ss);
+            pn = avgc(sn);
+        } else {
+            pa = avgc(cmul(sa, weights));
+            ps = avgc(cmul(ss, weights));
+            pn = avgc(cmul(sn, weights));
+        }
+        const float c = (pa + ps) + pn;
+        pa /= c;
+        ps /= c;
+        pn /= c;
+    }
+    static V3 reweight(V3 weights, V3 sigma, float maj, float p) {
+        const float den = maj * p;
+        return v3(weights.x * (sigma.x / den), weights.y * (sigma.y / den), weights.z * (sigma.z / den));
+    }
+
+    // deltaTrackingSpectral (DeltaTracking.glsl:33-163)
+    V3 spectral_delta(V3 x, V3 w, Rng& r, bool& ev) {
+        const float maj = maxc(ext3());
+        V3 weights = v3(1, 1, 1);
+        float tmin, tmax;
+        if (ray_box(bmin(), bmax(), x, w, tmin, tmax)) {
+            x = add(x, mul(w, tmin));
+            float d = tmax - tmin;
+            int bounces = 0;
+            while (true) {
+                if (guard()) return v3(0, 0, 0);
+                float t = -m_log(std::max(0.0000000001f, 1.0f - rnd(r))) * (1.0f / maj);
+                if (t > d) break;
+                V3 xn = add(x, mul(w, t));
+                float dens = sample(xn, r);
+                x = xn;
+                V3 sa, ss, sn;
+                float pa, ps, pn;
+                sdt_step(dens, weights, maj, sa, ss, sn, pa, ps, pn);
+                float xi = rnd(r);
+                if (xi < pa) {
+                    ev = true;
+                    return v3(0, 0, 0);
+                }
+                if (xi < pa + ps) {
+                    if (S.max_bounces > 0 && ++bounces > S.max_bounces) return v3(0, 0, 0);
+                    w = sample_phase(r, S.g, w);
+                    ev = true;
+                    if (ray_box(bmin(), bmax(), x, w, tmin, tmax)) {
+                        x = add(x, mul(w, tmin));
+                        d = tmax - tmin;
+                    }
+                    weights = reweight(weights, ss, maj, ps);
+                } else {
+                    d -= t;
+                    weights = reweight(weights, sn, maj, pn);
+                }
+                if (S.sdt_prob == 2) weights = cmin(weights, 100.0f);
+            }
+        }
+        return cmul(cmin(weights, 100000.0f), sky(w));
+    }
+
+    // nextEventTrackingSpectral (NextEventTracking.glsl:31-220)
+    V3 spectral_nee(V3 x, V3 w, Rng& r, bool& ev) {
+        const float maj = maxc(ext3());
+        V3 weights = v3(1, 1, 1), color = v3(0, 0, 0);
+        float tmin, tmax;
+        if (ray_box(bmin(), bmax(), x, w, tmin, tmax)) {
+            x = add(x, mul(w, tmin));
+            float d = tmax - tmin;
+            int bounces = 0;
+            while (true) {
+                if (guard()) return color;
+                float t = -m_log(std::max(0.0000000001f, 1.0f - rnd(r))) * (1.0f / maj);
+                if (t > d) break;
+                V3 xn = add(x, mul(w, t));
+                float dens = sample(xn, r);
+                x = xn;
+                V3 sa, ss, sn;
+                float pa, ps, pn;
+                sdt_step(dens, weights, maj, sa, ss, sn, pa, ps, pn);
+                float xi = rnd(r);
+                if (xi < pa) {
+                    ev = true;
+                    return color;
+                }
+                if (xi < pa + ps) {
+                    if (S.max_bounces > 0 && ++bounces > S.max_bounces) return color;
+                    V3 nw = sample_phase(r, S.g, w);
+                    ev = true;
+                    bool to_light = false;
+                    float factor = 1.0f, ldist = 0.0f, pdf_l = 0.0f;
+                    int lidx = 0;
+                    if (S.num_lights > 0) {
+                        to_light = S.env_is_black ? true : (rnd(r) > 0.5f);
+                        factor = S.env_is_black ? 1.0f : 2.0f;
+                    }
+                    V3 dl = to_light ? light_dir(x, r, lidx, factor, ldist) : importance_sky(r, pdf_l);
+                    float pdf_p = eval_phase(S.g, w, dl);
+                    w = nw;
+                    weights = reweight(weights, ss, maj, ps);
+                    const V3 wc = cmin(weights, 100000.0f);
+                    if (S.num_lights > 0) {
+                        const float cf = factor * pdf_p;
+                        const V3 common = v3(cf * wc.x, cf * wc.y, cf * wc.z);
+                        if (to_light) {
+                            float tr = transmittance_distance(x, dl, ldist, r);
+                            V3 l = light_rad(x, lidx);
+                            color = add(color, v3((common.x * tr) * l.x, (common.y * tr) * l.y, (common.z * tr) * l.z));
+                        } else {
+                            float tr = S.use_ess ? transmittance_ess(x, dl, r) : transmittance(x, dl, r);
+                            V3 l = sky(dl);
+                            color = add(color, v3(((common.x / pdf_l) * tr) * l.x, ((common.y / pdf_l) * tr) * l.y,
+                                                  ((common.z / pdf_l) * tr) * l.z));
+                        }
+                    } else {
+                        float tr = S.use_ess ? transmittance_ess(x, dl, r) : transmittance(x, dl, r);
+                        float f = (pdf_p / pdf_l) * tr;
+                        V3 l = sky(dl);
+                        color = add(color, v3((f * wc.x) * l.x, (f * wc.y) * l.y, (f * wc.z) * l.z));
+                    }
+                    if (ray_box(bmin(), bmax(), x, w, tmin, tmax)) {
+                        x = add(x, mul(w, tmin));
+                        d = tmax - tmin;
+                    }
+                } else {
+                    d -= t;
+                    weights = reweight(weights, sn, maj, pn);
+                }
+                if (S.sdt_prob == 2) weights = cmin(weights, 100.0f);
+            }
+        }
+        if (!ev) {
+            const V3 wc = cmin(weights, 100000.0f);
+            const V3 l = sky(w);
+            color = add(color, v3((1.0f * wc.x) * l.x, (1.0f * wc.y) * l.y, (1.0f * wc.z) * l.z));
+        }
+        return color;
+    }
+
     // analogDecompositionTracking over a NanoVDB grid with the HDDA
     // (DecompositionTracking.glsl:130-360)
     V3 decomposition_sparse(V3 x, V3 w, Rng& r) {
@@ -1135,6 +1301,8 @@ struct Tracer {
         bool ev = false;
         switch (S.mode) {
             case 0: return delta(x, w, r, ev);
+            case 1: return spectral_delta(x, w, r, ev);
+            case 6: return spectral_nee(x, w, r, ev);
             case 2: return ratio(x, w, r, ev);
             case 3: return S.nanovdb ? decomposition_sparse(x, w, r) : decomposition(x, w, r);
             case 4: return rrt(x, w, r);
@@ -1156,7 +1324,20 @@ int threads_or_default(int t) {
 
 extern "C" {
 
+// inputs a tracker dereferences: the scene is rejected (status 2) rather than read through null
+static bool scene_inputs_ok(const OracleScene* s) {
+    if (!s || (!s->density && !s->nanovdb)) return false;
+    const bool nee = s->mode == 5 || s->mode == 6;
+    if (nee && s->use_ess && !s->occupancy) return false;
+    if ((s->mode == 3 && !s->nanovdb) || s->mode == 4) {
+        if (!s->sv_data) return false;
+    }
+    if (s->env_kind == 4 && (!s->env_rgba || !s->env_pyramid)) return false;
+    return true;
+}
+
 int oracle_render_rows(const OracleScene* s, int row0, int row1, double* film, uint64_t* lookups, int threads) {
+    if (!scene_inputs_ok(s)) return 2;
     const OracleScene& S = *s;
     uint64_t total_lookups = 0;
     int nt = threads_or_default(threads);
@@ -1188,6 +1369,7 @@ int oracle_render_rows(const OracleScene* s, int row0, int row1, double* film, u
 }
 
 int oracle_render(const OracleScene* s, double* film, double* film_sq, uint64_t* lookups, int threads) {
+    if (!scene_inputs_ok(s)) return 2;
     const OracleScene& S = *s;
     uint64_t total_lookups = 0;
     int nt = threads_or_default(threads);
@@ -1222,6 +1404,7 @@ int oracle_render(const OracleScene* s, double* film, double* film_sq, uint64_t*
 
 int oracle_trace_paths(const OracleScene* s, const int* xs, const int* ys, const uint32_t* frames, int n,
                        float* out_rgb, int threads) {
+    if (!scene_inputs_ok(s)) return 2;
     int nt = threads_or_default(threads);
 #pragma omp parallel num_threads(nt)
     {

@@ -55,6 +55,12 @@ typedef struct OracleScene {
     int num_lights;
     int env_is_black;                /* parameters.isEnvMapBlack */
     float lights[16 * 16];
+    /* spectral trackers: parameters.extinction and parameters.scatteringAlbedo (rgb; zero extinction =
+     * extinction on every channel), SpectralDeltaTrackingCollisionProbability (0 max, 1 avg, 2 path
+     * history avg) */
+    float ext_rgb[3];
+    float albedo_rgb[3];
+    int sdt_prob;
 } OracleScene;
 
 /* Renders width*height*num_frames paths; adds radiance (and its square) per pixel (3 doubles). */

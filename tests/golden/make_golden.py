@@ -62,12 +62,24 @@ def cases():
         kw2 = dict(base)
         kw2.update(kw)
         out["fbm_" + name] = SceneSpec(grid=fbm, **kw2)
+    # spectral trackers: chromatic extinction and albedo, each collision-probability mode
+    chroma = dict(extinction_base=(1.0, 0.55, 0.3), albedo_rgb=(0.99, 0.9, 0.8))
+    for name, kw in {"sdt_max": dict(mode="spectral_delta", sdt_prob=0),
+                     "sdt_avg": dict(mode="spectral_delta", sdt_prob=1),
+                     "sdt_hist": dict(mode="spectral_delta", sdt_prob=2),
+                     "sdt_hist_trilinear": dict(mode="spectral_delta", sdt_prob=2, interp="trilinear"),
+                     "nees_max": dict(mode="spectral_nee", sdt_prob=0),
+                     "nees_hist": dict(mode="spectral_nee", sdt_prob=2)}.items():
+        kw2 = dict(base)
+        kw2.update(chroma)
+        kw2.update(kw)
+        out["fbm_" + name] = SceneSpec(grid=fbm, **kw2)
     return out
 
 
 FIELDS = ["mode", "interp", "extinction", "albedo", "g", "width", "height", "seed_offset", "env", "linear_rgb",
           "sun_dir", "sun_intensity", "cam_pos", "cam_target", "fovy", "near", "far", "max_grid_extent", "use_ess",
-          "env_intensity", "max_bounces", "ess_ref_compat", "lights"]
+          "env_intensity", "max_bounces", "ess_ref_compat", "lights", "extinction_base", "albedo_rgb", "sdt_prob"]
 
 
 def main():

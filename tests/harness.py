@@ -15,7 +15,7 @@ from cloudrendering_b200 import _lib
 from cloudrendering_b200._lib import check, farr
 from oracle import bridge
 
-MODE = {"delta": 0, "ratio": 2, "decomposition": 3, "rrt": 4, "nee": 5}
+MODE = {"delta": 0, "spectral_delta": 1, "ratio": 2, "decomposition": 3, "rrt": 4, "nee": 5, "spectral_nee": 6}
 INTERP = {"nearest": 0, "stochastic": 1, "trilinear": 2}
 ENV = {"default": 0, "black": 1, "single": 2, "constant_sun": 3, "image": 4}
 
@@ -66,7 +66,8 @@ class SceneSpec:
                  sun_dir=(0.5826, 0.7660, 0.2717), sun_intensity=(2.6, 2.6 * 0.961538462, 2.6 * 0.884615385),
                  sky_color=(1.0, 1.0, 1.0), cam_pos=(0.0, 0.0, 0.8), cam_target=(0.0, 0.0, 0.0),
                  fovy=2.0 * math.atan(0.5), near=0.01, far=100.0, max_grid_extent=0.25, env_rgba=None,
-                 use_ess=False, env_intensity=(1.0, 1.0, 1.0), ess_ref_compat=False, lights=None):
+                 use_ess=False, env_intensity=(1.0, 1.0, 1.0), ess_ref_compat=False, lights=None,
+                 extinction_base=(1.0, 1.0, 1.0), albedo_rgb=None, sdt_prob=2):
         self.__dict__.update(locals())
         del self.__dict__["self"]
 
@@ -113,8 +114,9 @@ def setup_core(core: Core, sp: SceneSpec):
     core("vpt_set_vpt_mode", MODE[sp.mode])
     core("vpt_set_grid_interpolation", INTERP[sp.interp])
     core("vpt_set_extinction_scale", sp.extinction)
-    core("vpt_set_extinction_base", farr([1, 1, 1]))
-    core("vpt_set_scattering_albedo", farr([sp.albedo] * 3))
+    core("vpt_set_extinction_base", farr(list(sp.extinction_base)))
+    core("vpt_set_scattering_albedo", farr(list(sp.albedo_rgb) if sp.albedo_rgb is not None else [sp.albedo] * 3))
+    core("vpt_set_option", b"sdt_collision_probability", float(sp.sdt_prob))
     core("vpt_set_phase_g", sp.g)
     core("vpt_set_seed_offset", sp.seed_offset)
     core("vpt_set_use_linear_rgb", sp.linear_rgb)
@@ -249,20 +251,25 @@ def oracle_scene(core, sp: SceneSpec, frames: int, frame_count: int = 0) -> brid
         inv_view_proj=list(inv), width=sp.width, height=sp.height, frame_count=frame_count, num_frames=frames,
         seed_offset=sp.seed_offset, mode=MODE[sp.mode], interp=INTERP[sp.interp], max_bounces=sp.max_bounces,
         use_ess=1 if sp.use_ess else 0, box_min=bmin, box_max=bmax, nx=nx, ny=ny, nz=nz, vox_per_unit=vpu,
-        border_density=float(border), extinction=float(f32(sp.extinction)), albedo=float(f32(sp.albedo)),
+        border_density=float(border), extinction=float(f32(f32(sp.extinction_base[0]) * f32(sp.extinction))),
+        albedo=float(f32(sp.albedo_rgb[0] if sp.albedo_rgb is not None else sp.albedo)),
         g=float(f32(sp.g)), env_kind=ENV[sp.env], use_linear_rgb=sp.linear_rgb, env_image_linear=1,
         sun_intensity=sp.sun_intensity, sky_color=sp.sky_color, env_intensity=sp.env_intensity, density=dens)
     sc.set("inv_view", camera_inv_view(sp))
     sc.set("num_lights", len(sp.lights or []))
     sc.set("env_is_black", 1 if sp.env == "black" else 0)
     sc.set("lights", light_floats(sp.lights))
+    sc.set("ext_rgb", [float(f32(f32(b) * f32(sp.extinction))) for b in sp.extinction_base])
+    sc.set("albedo_rgb", [float(f32(a)) for a in (sp.albedo_rgb if sp.albedo_rgb is not None else [sp.albedo] * 3)])
+    sc.set("sdt_prob", int(sp.sdt_prob))
     # sun direction normalised exactly like vpt_set_sun (float ops in order)
     d = np.array(sp.sun_dir, np.float32)
     dl = np.sqrt(np.float32(np.float32(d[0] * d[0]) + np.float32(d[1] * d[1])) + np.float32(d[2] * d[2]), dtype=np.float32)
     sc.set("sun_dir", [float(np.float32(d[i] / dl)) for i in range(3)])
     ext = f32(sp.extinction)
     if sp.mode in ("decomposition", "rrt") or sp.use_ess:
-        svs = 8 if sp.use_ess and sp.mode == "nee" else supervoxel_size(nx, ny, nz)
+        nee_like = sp.mode in ("nee", "spectral_nee")
+        svs = 8 if sp.use_ess and nee_like else supervoxel_size(nx, ny, nz)
         svx, svy, svz = -(-nx // svs), -(-ny // svs), -(-nz // svs)
         delta = [f32(b1) - f32(b0) for b0, b1 in zip(bmin, bmax)]
         svw = [(f32(svs) * dlt) / f32(n) for dlt, n in zip(delta, (nx, ny, nz))]
@@ -272,7 +279,7 @@ def oracle_scene(core, sp: SceneSpec, frames: int, frame_count: int = 0) -> brid
         sc.set("svz", svz)
         sc.set("sv_world", [float(v) for v in svw])
         halo = 0 if sp.interp == "nearest" else 1
-        if sp.mode == "nee":
+        if nee_like:
             if sp.ess_ref_compat:  # the reference marks every block occupied (ComputeOccupancyGrid.glsl:108-109)
                 sc.set("occupancy", np.ones(svx * svy * svz, np.uint8))
                 sc.set("ess_ref_compat", 1)
@@ -327,7 +334,8 @@ def reference_scene(sp: SceneSpec, frames: int, frame_start: int = 0, inv=None):
         inv_view_proj=list(inv), width=sp.width, height=sp.height, frame_start=frame_start, num_frames=frames,
         seed_offset=sp.seed_offset, box_min=bmin, box_max=bmax, grid=g, nx=nx, ny=ny, nz=nz,
         linear_filter=1 if sp.interp == "trilinear" else 0, voxel_value_min=vmin, voxel_value_max=vmax,
-        extinction=[sp.extinction] * 3, albedo=[sp.albedo] * 3, g=sp.g,
+        extinction=[float(np.float32(np.float32(b) * np.float32(sp.extinction))) for b in sp.extinction_base],
+        albedo=list(sp.albedo_rgb) if sp.albedo_rgb is not None else [sp.albedo] * 3, g=sp.g,
         sun_dir=[float(np.float32(d[i] / dl)) for i in range(3)], sun_intensity=sp.sun_intensity,
         env_intensity=sp.env_intensity, is_env_black=1 if sp.env == "black" else 0, far_dist=sp.far,
         inv_view=camera_inv_view(sp), lights=light_floats(sp.lights))
@@ -352,8 +360,10 @@ def reference_scene(sp: SceneSpec, frames: int, frame_start: int = 0, inv=None):
         sc.set("env_h", rgba.shape[0])
         sc.set("env_levels", 12)
         sc.set("env_pyramid", bridge.env_pyramid(rgba, 12))
+    prob = ["max", "avg", "hist"][sp.sdt_prob]
     tracker = {"delta": "delta", "ratio": "ratio", "decomposition": "decomposition", "rrt": "rrt",
-               "nee": "nee_ess" if sp.use_ess else "nee"}[sp.mode]
+               "nee": "nee_ess" if sp.use_ess else "nee", "spectral_delta": f"sdt_{prob}",
+               "spectral_nee": f"nees_{prob}"}[sp.mode]
     if sp.lights:
         tracker = f"nee_l{len(sp.lights)}"
     env = {"default": "default", "black": "black", "single": "single", "image": "image"}[sp.env]

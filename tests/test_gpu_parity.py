@@ -147,6 +147,22 @@ PATH_CASES = {
     "delta_default_sky_linear_uncapped": dict(mode="delta", env="default", linear_rgb=1, max_bounces=0),
     "decomposition_default_sky_uncapped": dict(mode="decomposition", env="default", linear_rgb=1, max_bounces=0),
     "rrt_default_sky_uncapped": dict(mode="rrt", env="default", linear_rgb=1, max_bounces=0),
+    # spectral trackers: chromatic extinction and albedo, each collision-probability mode
+    "spectral_delta_max": dict(mode="spectral_delta", sdt_prob=0, extinction_base=(1.0, 0.55, 0.3),
+                               albedo_rgb=(0.99, 0.9, 0.8)),
+    "spectral_delta_avg": dict(mode="spectral_delta", sdt_prob=1, extinction_base=(1.0, 0.55, 0.3),
+                               albedo_rgb=(0.99, 0.9, 0.8)),
+    "spectral_delta_hist": dict(mode="spectral_delta", sdt_prob=2, extinction_base=(0.4, 1.0, 0.7),
+                                albedo_rgb=(0.95, 0.99, 0.9)),
+    "spectral_delta_hist_trilinear": dict(mode="spectral_delta", sdt_prob=2, interp="trilinear",
+                                          extinction_base=(1.0, 0.55, 0.3), albedo_rgb=(0.99, 0.9, 0.8)),
+    "spectral_nee_hist": dict(mode="spectral_nee", sdt_prob=2, extinction_base=(1.0, 0.55, 0.3),
+                              albedo_rgb=(0.99, 0.9, 0.8)),
+    "spectral_nee_max_ess": dict(mode="spectral_nee", sdt_prob=0, use_ess=True, extinction_base=(1.0, 0.55, 0.3),
+                                 albedo_rgb=(0.99, 0.9, 0.8)),
+    "spectral_nee_lights": dict(mode="spectral_nee", sdt_prob=2, extinction_base=(1.0, 0.55, 0.3),
+                                albedo_rgb=(0.99, 0.9, 0.8), lights=[
+        dict(type="Point Light", space="World", position=(0.6, 0.8, 0.3), intensity=0.8, color=(1.0, 0.8, 0.6))]),
 }
 
 
