@@ -99,3 +99,17 @@ def test_training_on_tracer_pairs_beats_the_noisy_input(tmp_path):
     back = ld.KpnUNet.load(str(tmp_path / "model"))
     assert back.coarse_kernels == (5, 5)
     assert torch.equal(back.param, net.param) and torch.equal(back.param_bf16, net.param_bf16)
+
+
+def test_denoise_graph_equals_eager_denoise():
+    """The captured denoise (one graph launch) gives the eager result for new inputs."""
+    net = ld.KpnUNet(seed=5, coarse_kernels=(5, 5))
+    g = torch.Generator(device="cuda").manual_seed(1)
+    n, h, w = 1, 64, 128
+    mk = lambda c: torch.rand((n, c, h, w), device="cuda", generator=g)  # noqa: E731
+    graph = net.graph(n, h, w)
+    for _ in range(2):
+        args = (mk(3) * 2, mk(3), mk(3), mk(1), mk(1), torch.tensor([0.5], device="cuda"))
+        got = graph(*args).clone()
+        ref = net.denoise(*args)
+        assert torch.allclose(got, ref, rtol=1e-6, atol=1e-6)
