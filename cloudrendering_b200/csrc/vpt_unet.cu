@@ -56,6 +56,13 @@ __device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, bool v
     const int n = valid ? 16 : 0;  // n = 0 writes 16 zero bytes and reads nothing
     asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src), "r"(n) : "memory");
 }
+__device__ __forceinline__ void cp_async16_stream(uint32_t dst, const void* src) {  // L2 only
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async4(uint32_t dst, const void* src, bool valid) {
+    const int n = valid ? 4 : 0;  // n = 0 writes 4 zero bytes and reads nothing
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(dst), "l"(src), "r"(n) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() {
@@ -156,6 +163,8 @@ struct ConvArgs {
     int relu, out_f32;   // conv epilogue
     int pix_per_split;   // wgrad: pixels (K) per CTA, multiple of kBK
     int m_pad;           // wgrad: rows of a partial (multiple of kBM)
+    int ksplit;          // conv: K stages split over blockIdx.z (> 1: raw sums to `partial`)
+    float* partial;      // conv split-K: fp32 [ksplit][P][cout]
 };
 
 __device__ __forceinline__ void pixel_coords(int p, int h, int w, int& n, int& y, int& x) {
@@ -182,6 +191,7 @@ __global__ void __launch_bounds__(kThreads) conv_tile_kernel(const ConvArgs a) {
 
     // K extent and tile origin
     int K, m0, kbeg = 0, kend = 0;
+    int s_first = 0;  // conv split-K: first K stage of this CTA
     if (MODE == kConv) {
         K = 9 * a.cin;
         m0 = blockIdx.x * kBM;
@@ -192,7 +202,12 @@ __global__ void __launch_bounds__(kThreads) conv_tile_kernel(const ConvArgs a) {
         K = kend - kbeg;
     }
     const int M = (MODE == kConv) ? P : 9 * a.cin;
-    const int nk = (K + kBK - 1) / kBK;
+    int nk = (K + kBK - 1) / kBK;
+    if (MODE == kConv && a.ksplit > 1) {
+        const int per = (nk + a.ksplit - 1) / a.ksplit;
+        s_first = blockIdx.z * per;
+        nk = max(0, min(nk, s_first + per) - s_first);
+    }
 
     if (tid == 0) {
         for (int s = 0; s < kStages; ++s) mbar_init(smem_u32(&bars[s]), 1);
@@ -224,7 +239,7 @@ __global__ void __launch_bounds__(kThreads) conv_tile_kernel(const ConvArgs a) {
 
     // incremental gather state (stages are loaded in increasing order, so nothing is divided by a
     // runtime value inside the loop)
-    int ld_tap = 0, ld_ci = 0;                       // conv: (tap, channel) of the next stage's first k
+    int ld_tap = (s_first * kBK) / a.cin, ld_ci = (s_first * kBK) % a.cin;  // conv: next stage's first k
     int b_r0 = tid % n_tile, b_kc0 = tid / n_tile;   // conv: first B unit of this thread
     int wq_n = 0, wq_y = 0, wq_x = 0, wq_p = kbeg + (tid & 7);  // wgrad: this thread's next A pixel
     if (MODE == kWgrad && wq_p < P) pixel_coords(wq_p, a.h, a.w_, wq_n, wq_y, wq_x);
@@ -236,7 +251,7 @@ __global__ void __launch_bounds__(kThreads) conv_tile_kernel(const ConvArgs a) {
         const uint32_t sA = sbase + slot * stage_bytes;
         const uint32_t sB = sA + a_bytes;
         if (MODE == kConv) {
-            const int k0 = s * kBK;
+            const int k0 = (s_first + s) * kBK;
             // A: row tid, 8 chunks of 8 channels; unit (r, kc) at kc * kBM * 16 + r * 16
             int tap = ld_tap, ci = ld_ci;
 #pragma unroll
@@ -334,7 +349,7 @@ __global__ void __launch_bounds__(kThreads) conv_tile_kernel(const ConvArgs a) {
             tc_fence_after();
             const uint32_t sA = sbase + slot * stage_bytes;
             const uint32_t sB = sA + a_bytes;
-            const int steps = min(kBK / 16, (K - s * kBK + 15) / 16);
+            const int steps = min(kBK / 16, (K - (s_first + s) * kBK + 15) / 16);
             for (int j = 0; j < steps; ++j) {
                 const uint64_t da = smem_desc(sA + j * 2 * a_lbo, a_lbo, 128);
                 const uint64_t db = smem_desc(sB + j * 2 * b_lbo, b_lbo, 128);
@@ -362,6 +377,13 @@ __global__ void __launch_bounds__(kThreads) conv_tile_kernel(const ConvArgs a) {
     const bool fail = __syncthreads_or(aborted || !done || (issued != nk - 1 && nk > 0));
     tc_fence_after();
 
+    if (!fail && nk == 0 && MODE == kConv && a.partial) {  // an empty K range contributes zeros
+        const int p = m0 + tid;
+        if (p < P)
+            for (int co = n0; co < min(a.cout, n0 + n_tile); co += 4)
+                *reinterpret_cast<float4*>(a.partial + ((size_t)blockIdx.z * P + p) * a.cout + co) =
+                    make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
     if (!fail && nk > 0) {
         const int warp = tid >> 5, lane = tid & 31;
         const int r = warp * 32 + lane;
@@ -374,6 +396,13 @@ __global__ void __launch_bounds__(kThreads) conv_tile_kernel(const ConvArgs a) {
             if (MODE == kConv) {
                 const int p = m0 + r;
                 if (p >= P) continue;
+                if (a.partial) {  // split-K: raw sums, finished by conv_finalize_kernel
+                    float4* dst = reinterpret_cast<float4*>(a.partial + ((size_t)blockIdx.z * P + p) * a.cout + co);
+#pragma unroll
+                    for (int i = 0; i < 4; ++i)
+                        dst[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+                    continue;
+                }
                 if (a.bias) {
 #pragma unroll
                     for (int i = 0; i < 16; ++i) v[i] += a.bias[co + i];
@@ -418,6 +447,39 @@ __global__ void __launch_bounds__(kThreads) conv_tile_kernel(const ConvArgs a) {
     if (tid < 32) {
         tc_fence_after();
         tmem_dealloc(tmem, (uint32_t)a.tmem_cols);
+    }
+}
+
+// Split-K convolution: y = act(bias + sum over the splits of partial[s]) (fixed order), times the
+// ReLU-derivative mask, stored bf16 or fp32; 4 channels per thread.
+__global__ void conv_finalize_kernel(const float* __restrict__ partial, int ksplit, long P, int cout,
+                                     const float* __restrict__ bias, const bf16* __restrict__ mask, int relu,
+                                     int out_f32, void* __restrict__ y) {
+    const long total = P * (cout / 4);
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+        const long p = i / (cout / 4);
+        const int c = (int)(i % (cout / 4)) * 4;
+        float4 acc = reinterpret_cast<const float4*>(partial + p * cout + c)[0];
+        for (int k = 1; k < ksplit; ++k) {
+            const float4 u = reinterpret_cast<const float4*>(partial + ((size_t)k * P + p) * cout + c)[0];
+            acc.x += u.x;
+            acc.y += u.y;
+            acc.z += u.z;
+            acc.w += u.w;
+        }
+        float v[4] = {acc.x, acc.y, acc.z, acc.w};
+        for (int j = 0; j < 4; ++j) {
+            if (bias) v[j] += bias[c + j];
+            if (relu) v[j] = fmaxf(v[j], 0.0f);
+            if (mask) v[j] = __bfloat162float(mask[p * cout + c + j]) > 0.0f ? v[j] : 0.0f;
+        }
+        if (out_f32) {
+            reinterpret_cast<float4*>(static_cast<float*>(y) + p * cout + c)[0] = make_float4(v[0], v[1], v[2], v[3]);
+        } else {
+            __nv_bfloat162* o = reinterpret_cast<__nv_bfloat162*>(static_cast<bf16*>(y) + p * cout + c);
+            o[0] = __floats2bfloat162_rn(v[0], v[1]);
+            o[1] = __floats2bfloat162_rn(v[2], v[3]);
+        }
     }
 }
 
@@ -1080,66 +1142,140 @@ __global__ void pack_input_kernel(const float* __restrict__ radiance, const floa
 //   dL/dlogit_j = s_j (g . x_j - g . d),  g_c = 2 (d_c - t_c) / (t_c^2 + eps) * inv_count
 // logits: [P][hc] fp32 (NHWC, hc >= k*k a multiple of 8, channels k*k.. unused, their gradient 0);
 // x, t, out: [n][3][h][w] fp32.  The softmax is recomputed per pass (no per-tap arrays in registers).
-__global__ void kpn_head_kernel(const float* __restrict__ logits, int hc, int ks, const float* __restrict__ x,
-                                const float* __restrict__ target, float* __restrict__ out, bf16* __restrict__ dlogits,
-                                float* __restrict__ loss_partial, int n, int h, int w, float eps, float inv_count) {
-    const long plane = (long)h * w, total = (long)n * plane;
-    const int taps = ks * ks, rad = ks / 2;
+// One block per 64-pixel row segment at a time (grid-stride): the segment's logits (contiguous in
+// NHWC) are staged in shared memory by asynchronous copies, a warp per pixel row, at a row stride of
+// hc + 4 floats; the KS x (64 + KS - 1) radiance window likewise, with zeros outside the image (an
+// out-of-image tap adds to the normalisation only).  Four lanes per pixel take the kernel rows
+// sub, sub + 4, ... (columns unrolled: window offsets are immediates) and combine by shuffles.  Bank
+// spread: the logit stride is 4 (mod 8) with an odd quotient, so the warp's 8 pixels start on banks
+// 0, 4, .., 28 and the lanes' rows (KS odd) add 0..3; the window row length is 8 (mod 16), so the
+// lanes' window rows start 8 banks apart.  The logit gradients overwrite the staged logits and leave
+// as coalesced bf16 rows.
+constexpr int kHeadSeg = 64;
+
+__host__ __device__ constexpr int head_window_row(int ks) {  // >= kHeadSeg + ks - 1, = 8 (mod 16)
+    return (kHeadSeg + ks - 1 + 7) / 16 * 16 + 8;
+}
+
+__device__ __forceinline__ float quad_sum(float v) {
+    v += __shfl_xor_sync(0xffffffffu, v, 1);
+    return v + __shfl_xor_sync(0xffffffffu, v, 2);
+}
+
+template <int KS>
+__global__ void __launch_bounds__(256) kpn_head_kernel(const float* __restrict__ logits, int hc,
+                                                       const float* __restrict__ x, const float* __restrict__ target,
+                                                       float* __restrict__ out, bf16* __restrict__ dlogits,
+                                                       float* __restrict__ loss_partial, int n, int h, int w,
+                                                       float eps, float inv_count) {
+    constexpr int RW = head_window_row(KS), WIN = KS * RW, TAPS = KS * KS, RAD = KS / 2;
+    extern __shared__ float hsm[];
+    const int stride = hc + 4;
+    float* lsm = hsm;                       // [kHeadSeg][stride]
+    float* rsm = hsm + kHeadSeg * stride;   // [3][KS][RW]
+    const long plane = (long)h * w;
+    const int segs_w = (w + kHeadSeg - 1) / kHeadSeg;
+    const long nseg = (long)n * h * segs_w;
+    const int t = threadIdx.x, pl = t >> 2, sub = t & 3, warp = t >> 5, lane = t & 31;
+    const int q4 = hc / 4;
     float local = 0.0f;
-    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
-        const long b = i / plane, q = i % plane;
-        const int y = (int)(q / w), xx = (int)(q % w);
-        const float* lg = logits + i * hc;
-        float mx = -INFINITY;
-        for (int j = 0; j < taps; ++j) mx = fmaxf(mx, lg[j]);
-        float sum = 0.0f;
-        float d[3] = {0.0f, 0.0f, 0.0f};
+    for (long sg = blockIdx.x; sg < nseg; sg += gridDim.x) {
+        const int sx = (int)(sg % segs_w);
+        const long row = sg / segs_w;
+        const int y = (int)(row % h);
+        const long b = row / h;
+        const int x0 = sx * kHeadSeg, np = min(kHeadSeg, w - x0);
+        const long p0 = (b * h + y) * w + x0;
+        __syncthreads();  // the previous segment is done with shared memory
+        // asynchronous copies: every copy of the block is in flight before the first wait
+        const float4* lg4 = reinterpret_cast<const float4*>(logits + p0 * hc);
+        for (int p = warp; p < np; p += 8) {
+            const float4* src = lg4 + (long)p * q4;
+            const uint32_t dst = smem_u32(lsm + p * stride);
+            for (int c = lane; c < q4; c += 32) cp_async16_stream(dst + 16 * c, src + c);
+        }
         const float* xb = x + b * 3 * plane;
-        for (int j = 0; j < taps; ++j) {
-            const float e = __expf(lg[j] - mx);
-            sum += e;
-            const int yy = y + j / ks - rad, xq = xx + j % ks - rad;
-            if (yy < 0 || yy >= h || xq < 0 || xq >= w) continue;
-            const long o = (long)yy * w + xq;
-            d[0] += e * xb[o];
-            d[1] += e * xb[plane + o];
-            d[2] += e * xb[2 * plane + o];
+        for (int rr = warp; rr < 3 * KS; rr += 8) {  // window row rr = c * KS + r
+            const int c = rr / KS, r = rr - c * KS;
+            const int yy = y + r - RAD;
+            const bool row_ok = yy >= 0 && yy < h;
+            const float* src = xb + c * plane + (long)(row_ok ? yy : 0) * w;
+            const uint32_t dst = smem_u32(rsm + rr * RW);
+            for (int xx = lane; xx < kHeadSeg + KS - 1; xx += 32) {
+                const int xq = x0 + xx - RAD;
+                const bool v = row_ok && xq >= 0 && xq < w;
+                cp_async4(dst + 4 * xx, v ? src + xq : xb, v);
+            }
         }
+        cp_async_commit();
+        cp_async_wait<0>();
+        __syncthreads();
+        const bool pv = pl < np;
+        const float* lp = lsm + pl * stride;
+        const float* rp = rsm + pl;
+        float mx = -INFINITY;
+        if (pv)
+            for (int r = sub; r < KS; r += 4) {
+#pragma unroll
+                for (int c = 0; c < KS; ++c) mx = fmaxf(mx, lp[r * KS + c]);
+            }
+        mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, 1));
+        mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, 2));
+        float sum = 0.0f, d0 = 0.0f, d1 = 0.0f, d2 = 0.0f;
+        if (pv)
+            for (int r = sub; r < KS; r += 4) {
+                const float* lr = lp + r * KS;
+                const float* xr = rp + r * RW;
+#pragma unroll
+                for (int c = 0; c < KS; ++c) {
+                    const float e = __expf(lr[c] - mx);
+                    sum += e;
+                    d0 += e * xr[c];
+                    d1 += e * xr[WIN + c];
+                    d2 += e * xr[2 * WIN + c];
+                }
+            }
+        sum = quad_sum(sum);
+        d0 = quad_sum(d0);
+        d1 = quad_sum(d1);
+        d2 = quad_sum(d2);
         const float inv = 1.0f / sum;
-        d[0] *= inv;
-        d[1] *= inv;
-        d[2] *= inv;
-        if (out) {
-            for (int c = 0; c < 3; ++c) out[(b * 3 + c) * plane + q] = d[c];
-        }
+        const float d[3] = {d0 * inv, d1 * inv, d2 * inv};
+        const long q = (long)y * w + x0 + pl;
+        if (pv && out && sub < 3) out[(b * 3 + sub) * plane + q] = sub == 0 ? d[0] : (sub == 1 ? d[1] : d[2]);
         if (target) {
-            float g[3];
-            for (int c = 0; c < 3; ++c) {
-                const float t = target[(b * 3 + c) * plane + q];
-                const float den = t * t + eps;
-                const float e = d[c] - t;
-                local += e * e / den * inv_count;
-                g[c] = 2.0f * e / den * inv_count;
+            float g[3] = {0.0f, 0.0f, 0.0f};
+            if (pv) {
+                for (int c = 0; c < 3; ++c) {
+                    const float tg = target[(b * 3 + c) * plane + q];
+                    const float den = tg * tg + eps;
+                    const float e = d[c] - tg;
+                    if (sub == 0) local += e * e / den * inv_count;
+                    g[c] = 2.0f * e / den * inv_count;
+                }
             }
             const float gd = g[0] * d[0] + g[1] * d[1] + g[2] * d[2];
-            for (int j0 = 0; j0 < hc; j0 += 8) {
-                float f[8];
+            float* lw = lsm + pl * stride;
+            for (int r = sub; r < KS; r += 4) {
+                float* lr = lw + r * KS;
+                const float* xr = rp + r * RW;
 #pragma unroll
-                for (int k = 0; k < 8; ++k) {
-                    const int j = j0 + k;
-                    f[k] = 0.0f;
-                    if (j < taps) {
-                        const float sj = __expf(lg[j] - mx) * inv;
-                        const int yy = y + j / ks - rad, xq = xx + j % ks - rad;
-                        float gx = 0.0f;
-                        if (yy >= 0 && yy < h && xq >= 0 && xq < w) {
-                            const long o = (long)yy * w + xq;
-                            gx = g[0] * xb[o] + g[1] * xb[plane + o] + g[2] * xb[2 * plane + o];
-                        }
-                        f[k] = sj * (gx - gd);
-                    }
+                for (int c = 0; c < KS; ++c) {
+                    const float gx = g[0] * xr[c] + g[1] * xr[WIN + c] + g[2] * xr[2 * WIN + c];
+                    lr[c] = pv ? __expf(lr[c] - mx) * inv * (gx - gd) : 0.0f;
                 }
-                store8(dlogits + i * hc + j0, f);
+            }
+            for (int j = TAPS + sub; j < hc; j += 4) lw[j] = 0.0f;
+            __syncthreads();
+            for (int p = warp; p < np; p += 8) {
+                const float* srow = lsm + p * stride;
+                bf16* drow = dlogits + (p0 + p) * hc;
+                for (int c = lane * 8; c < hc; c += 256) {
+                    const float4 u = *reinterpret_cast<const float4*>(srow + c);
+                    const float4 v = *reinterpret_cast<const float4*>(srow + c + 4);
+                    const float f[8] = {u.x, u.y, u.z, u.w, v.x, v.y, v.z, v.w};
+                    store8(drow + c, f);
+                }
             }
         }
     }
@@ -1543,6 +1679,7 @@ using namespace vpt::unet;
 
 static bool g_force_gather = false;  // conv path 1: the gather kernels everywhere
 static bool g_force_strip = false;   // conv path 2: the strip kernels wherever they apply
+static int g_conv_ksplit = 0;        // gather convolution K splits: 0 automatic, 1 none, k > 1 forced
 
 extern "C" {
 
@@ -1572,8 +1709,40 @@ VptStatus vpt_unet_conv3x3(const void* x, const void* w, const float* bias, cons
     if (groups > 0 && !g_force_gather)
         return launch_strip(a, groups, static_cast<cudaStream_t>(stream)) == cudaSuccess ? VPT_OK : VPT_ERR_CUDA;
     const long P = (long)n * h * width;
-    const dim3 grid((unsigned)((P + kBM - 1) / kBM), (unsigned)((cout + a.n_tile - 1) / a.n_tile), 1);
-    return launch_tile<kConv>(a, grid, static_cast<cudaStream_t>(stream)) == cudaSuccess ? VPT_OK : VPT_ERR_CUDA;
+    const unsigned gx = (unsigned)((P + kBM - 1) / kBM), gy = (unsigned)((cout + a.n_tile - 1) / a.n_tile);
+    // small grids (the deep levels): split the K stages over more CTAs, raw fp32 sums finished by
+    // conv_finalize_kernel in a fixed order
+    const int nk = (9 * cin + kBK - 1) / kBK;
+    const int sms = sm_count();
+    const long tiles = (long)gx * gy;
+    int ksplit = 1;
+    if (g_conv_ksplit > 1) ksplit = std::min(g_conv_ksplit, nk);
+    else if (g_conv_ksplit == 0 && 2 * tiles <= sms)  // under half a wave: about two CTAs per SM (measured)
+        ksplit = (int)std::max<long>(1, std::min<long>(std::min<long>(8, (2L * sms + tiles - 1) / tiles), nk / 2));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (ksplit == 1)
+        return launch_tile<kConv>(a, dim3(gx, gy, 1), s) == cudaSuccess ? VPT_OK : VPT_ERR_CUDA;
+    float* part = nullptr;
+    if (cudaMallocAsync(reinterpret_cast<void**>(&part), (size_t)ksplit * P * cout * sizeof(float), s) != cudaSuccess)
+        return VPT_ERR_OOM;
+    a.ksplit = ksplit;
+    a.partial = part;
+    cudaError_t e = launch_tile<kConv>(a, dim3(gx, gy, (unsigned)ksplit), s);
+    if (e == cudaSuccess) {
+        conv_finalize_kernel<<<grid_for(P * (cout / 4), 256), 256, 0, s>>>(part, ksplit, P, cout, bias,
+                                                                          static_cast<const bf16*>(mask), relu,
+                                                                          out_f32, y);
+        e = cudaGetLastError();
+    }
+    const cudaError_t f = cudaFreeAsync(part, s);
+    return (e == cudaSuccess && f == cudaSuccess) ? VPT_OK : VPT_ERR_CUDA;
+}
+
+// K splits of the gather convolution: 0 chosen by grid size, 1 never split, k > 1 always k (tests)
+VptStatus vpt_unet_set_conv_ksplit(int ksplit) {
+    if (ksplit < 0 || ksplit > 64) return VPT_ERR_ARG;
+    g_conv_ksplit = ksplit;
+    return VPT_OK;
 }
 
 // 1: every convolution uses the per-tile gather kernel (for comparisons); 0: row strips where eligible
@@ -1742,13 +1911,37 @@ VptStatus vpt_unet_kpn_head(const float* logits, int head_channels, int kernel_s
                             float eps, void* stream) {
     if (!logits || !radiance || n <= 0 || h <= 0 || w <= 0 || (target && !dlogits) || eps <= 0.0f ||
         kernel_size <= 0 || kernel_size % 2 == 0 || kernel_size > 15 || head_channels % 8 ||
-        head_channels < kernel_size * kernel_size)
+        head_channels < kernel_size * kernel_size || head_channels > 512 || reinterpret_cast<uintptr_t>(logits) % 16)
         return VPT_ERR_ARG;
+    // the loss partials are per block: as many blocks as vpt_unet_head_blocks (never more than the
+    // row segments, which the blocks stride over)
     const int blocks = grid_for((long)n * h * w, 256);
     const float inv_count = 1.0f / (3.0f * (float)n * (float)h * (float)w);
-    kpn_head_kernel<<<blocks, 256, 0, static_cast<cudaStream_t>(stream)>>>(
-        logits, head_channels, kernel_size, radiance, target, out, static_cast<bf16*>(dlogits), loss_partial, n, h, w,
-        eps, inv_count);
+    const size_t smem =
+        ((size_t)kHeadSeg * (head_channels + 4) + 3 * kernel_size * head_window_row(kernel_size)) * sizeof(float);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    bf16* dl = static_cast<bf16*>(dlogits);
+    cudaError_t e = cudaErrorInvalidValue;
+    auto go = [&](auto kernel) {
+        if (smem > 48 * 1024 &&
+            cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+            return cudaErrorInvalidValue;
+        kernel<<<blocks, 256, smem, s>>>(logits, head_channels, radiance, target, out, dl, loss_partial, n, h, w,
+                                         eps, inv_count);
+        return cudaGetLastError();
+    };
+    switch (kernel_size) {
+        case 1: e = go(kpn_head_kernel<1>); break;
+        case 3: e = go(kpn_head_kernel<3>); break;
+        case 5: e = go(kpn_head_kernel<5>); break;
+        case 7: e = go(kpn_head_kernel<7>); break;
+        case 9: e = go(kpn_head_kernel<9>); break;
+        case 11: e = go(kpn_head_kernel<11>); break;
+        case 13: e = go(kpn_head_kernel<13>); break;
+        case 15: e = go(kpn_head_kernel<15>); break;
+        default: return VPT_ERR_ARG;
+    }
+    if (e != cudaSuccess) return VPT_ERR_CUDA;
     vpt::count_launches(1);
     return cudaGetLastError() == cudaSuccess ? VPT_OK : VPT_ERR_CUDA;
 }

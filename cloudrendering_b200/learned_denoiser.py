@@ -624,14 +624,20 @@ def train(net: KpnUNet, data: TrainingSet, steps: int, batch_size: int = 8, lr: 
 
 def layer_timings(net: KpnUNet, batch: int = 8, size: int = 256, reps: int = 20) -> Dict[str, dict]:
     """Device time of every convolution of a training step at batch x size^2 (forward, input gradient,
-    weight gradient; random activations), with the flops of each."""
+    weight gradient; random activations), with the flops of each.  The repetitions are captured in a
+    CUDA graph, so that host-side launch cost does not hide the device time of small layers."""
     def timed(fn):
         fn()
         torch.cuda.synchronize()
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph):
+            for _ in range(reps):
+                fn()
+        graph.replay()
+        torch.cuda.synchronize()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record()
-        for _ in range(reps):
-            fn()
+        graph.replay()
         b.record()
         torch.cuda.synchronize()
         return a.elapsed_time(b) / reps
@@ -660,12 +666,32 @@ if __name__ == "__main__":
     ap.add_argument("--profile-launches", action="store_true",
                     help="one forward and one weight-gradient launch of two level-0 layers (32->32, 96->32) at "
                          "8x256^2, for a profiler")
+    ap.add_argument("--profile-layer", default="",
+                    help="one forward launch of the named layer (e.g. dec3a) at batch x size^2, for a profiler")
+    ap.add_argument("--profile-denoise", action="store_true",
+                    help="one denoise of a batch x size^2 image (every inference launch), for a profiler")
     ap.add_argument("--size", type=int, default=256)
     ap.add_argument("--batch", type=int, default=8)
     args = ap.parse_args()
     net = KpnUNet(seed=0)
     if args.layers:
         print(json.dumps(layer_timings(net, args.batch, args.size), indent=1))
+    if args.profile_layer:
+        L = net.by_name[args.profile_layer]
+        n, hh, ww = args.batch, args.size >> L["level"], args.size >> L["level"]
+        x = torch.randn((n, hh, ww, L["cin"]), device=net.device).to(torch.bfloat16)
+        y = torch.empty((n, hh, ww, L["cout"]), dtype=torch.bfloat16, device=net.device)
+        net._conv(L, x, y, n, hh, ww, 1)
+        torch.cuda.synchronize()
+        net.check_errors()
+        print("ok")
+    if args.profile_denoise:
+        g = torch.Generator(device=net.device).manual_seed(1)
+        mk = lambda c: torch.rand((args.batch, c, args.size, args.size), device=net.device, generator=g)  # noqa: E731
+        out = net.denoise(mk(3) * 2, mk(3), mk(3), mk(1), mk(1), torch.full((args.batch,), 0.5, device=net.device))
+        torch.cuda.synchronize()
+        net.check_errors()
+        print("ok", float(out.mean()))
     if args.profile_launches:
         for name in ("enc0b", "dec0a"):
             L = net.by_name[name]

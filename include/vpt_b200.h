@@ -377,6 +377,10 @@ VptStatus vpt_unet_conv3x3(const void* x, const void* w, const float* bias, cons
  * fp32 partial allocated on the stream), 1 = the per-tile gather kernels everywhere, 2 = the row-strip
  * kernels wherever they apply. */
 VptStatus vpt_unet_set_conv_path(int path);
+/* K splits of the per-tile gather convolution: 0 (default) = by grid size (grids of at most half an SM wave
+ * split their K stages over up to 8 CTAs, whose fp32 sums, allocated on the stream, are added in split
+ * order before the bias / ReLU / mask epilogue), 1 = never, k > 1 = always k (at most the K stages). */
+VptStatus vpt_unet_set_conv_ksplit(int ksplit);
 /* Shared-memory ring depth of the per-tile gather kernel: 3 or 4 stages, 0 (default) = by shape. */
 VptStatus vpt_unet_set_gather_stages(int stages);
 /* Weight gradient: partial[s][t*cin + ci][co] = sum over the pixels p of split s of
@@ -422,7 +426,7 @@ int vpt_unet_head_blocks(int n, int h, int w);
 /* Kernel-prediction head (perPixelKernelCuda semantics, modules/kpn_module/src/Kernel.cu:38-135, with
  * the tap softmax fused): out[n][c][y][x] = sum_j softmax(logits[p][0 .. k*k-1])_j
  * radiance[n][c][y+dy][x+dx] (k = kernel_size odd <= 15, taps outside skipped; logits [p][head_channels]
- * fp32, head_channels >= k*k a multiple of 8).  With target != NULL also the relative MSE
+ * fp32, 16-byte aligned, head_channels >= k*k a multiple of 8, at most 512).  With target != NULL also the relative MSE
  * sum (d-t)^2/(t^2+eps)/(3*n*h*w) as per-block partial sums (vpt_unet_head_blocks of them) and its
  * gradient dlogits [p][head_channels] bf16 (0 beyond k*k).  out may be NULL. */
 VptStatus vpt_unet_kpn_head(const float* logits, int head_channels, int kernel_size, const float* radiance,

@@ -73,9 +73,18 @@ CONV_CASES = [
 ]
 
 
+@pytest.fixture(params=[0, 1, 8], ids=["ksplit_auto", "ksplit_off", "ksplit_8"])
+def ksplit(lib, request):
+    """K splits of the gather convolution: by grid size (most cases here split), none, and 8 forced
+    (more splits than some cases have K stages per split: empty splits contribute zeros)."""
+    assert lib.vpt_unet_set_conv_ksplit(request.param) == 0
+    yield request.param
+    assert lib.vpt_unet_set_conv_ksplit(0) == 0
+
+
 @pytest.mark.parametrize("case", CONV_CASES)
 @pytest.mark.parametrize("epilogue", ["f32", "bias_relu_bf16", "mask_bf16"])
-def test_conv_forward(lib, case, epilogue):
+def test_conv_forward(lib, case, epilogue, ksplit):
     n, h, w, cin, cout = case
     x = uo.bf16(rng_data(1, n, h, w, cin))
     wt = uo.bf16(rng_data(2, cout, 9, cin, scale=1.0 / np.sqrt(9 * cin)))
@@ -99,7 +108,7 @@ def test_conv_forward(lib, case, epilogue):
 
 
 @pytest.mark.parametrize("case", CONV_CASES)
-def test_conv_input_grad(lib, case):
+def test_conv_input_grad(lib, case, ksplit):
     n, h, w, cin, cout = case
     dy = uo.bf16(rng_data(5, n, h, w, cout))
     wt = uo.bf16(rng_data(6, cout, 9, cin, scale=1.0 / np.sqrt(9 * cout)))
@@ -247,21 +256,37 @@ def test_pack_input_and_kpn_head(lib):
     ref = uo.pack_input(rad, alb, nrm, dep, trn, noise, m2)
     close_bf16(host(packed), ref.astype(np.float64))
 
+
+@pytest.mark.parametrize("shape", [(2, 12, 17), (1, 5, 150), (3, 70, 9), (1, 3, 128)],
+                         ids=["narrow", "ragged_segments", "tall", "two_segments"])
+def test_kpn_head(lib, shape):
+    """Kernel application, loss and logit gradient; rows of 64-pixel segments with ragged ends and
+    images narrower than one segment."""
+    n, h, w = shape
+    g = np.random.default_rng(14)
+    rad = (g.exponential(1.0, (n, 3, h, w)) * (g.random((n, 3, h, w)) < 0.7)).astype(np.float32)
     target = g.exponential(1.0, (n, 3, h, w)).astype(np.float32)
+    d_rad, d_target = dev_f32(rad), dev_f32(target)
     blocks = lib.vpt_unet_head_blocks(n, h, w)
-    for ks, hc in ((5, 32), (9, 96), (11, 128), (3, 16)):
+    for ks, hc in ((5, 32), (9, 96), (11, 128), (3, 16), (13, 176), (1, 8), (7, 56), (15, 232)):
         logits = rng_data(15 + ks, n, h, w, hc, scale=2.0)
         out = torch.empty((n, 3, h, w), dtype=torch.float32, device="cuda")
         dl = torch.empty((n, h, w, hc), dtype=torch.bfloat16, device="cuda")
         lp = torch.empty((blocks,), dtype=torch.float32, device="cuda")
-        d_logits, d_target = dev_f32(logits), dev_f32(target)
-        assert lib.vpt_unet_kpn_head(ptr(d_logits), hc, ks, ptr(t[0]), ptr(d_target), ptr(out), ptr(dl), ptr(lp), n,
+        d_logits = dev_f32(logits)
+        assert lib.vpt_unet_kpn_head(ptr(d_logits), hc, ks, ptr(d_rad), ptr(d_target), ptr(out), ptr(dl), ptr(lp), n,
                                      h, w, ctypes.c_float(1e-2), None) == 0
         torch.cuda.synchronize()
         d, loss, dlog = uo.kpn_head(logits, rad, target, ks=ks)
         close_f32(host(out), d)
         assert abs(float(lp.double().sum()) - loss) <= 1e-5 * loss
         close_bf16(host(dl), dlog)
+        # inference: the image alone
+        out2 = torch.full((n, 3, h, w), -1.0, dtype=torch.float32, device="cuda")
+        assert lib.vpt_unet_kpn_head(ptr(d_logits), hc, ks, ptr(d_rad), None, ptr(out2), None, None, n, h, w,
+                                     ctypes.c_float(1e-2), None) == 0
+        torch.cuda.synchronize()
+        assert torch.equal(out2, out)
 
 
 def test_adam(lib):
