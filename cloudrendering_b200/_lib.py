@@ -120,6 +120,7 @@ SIGNATURES = {
     "vpt_unet_wgrad_splits": (c_int, [c_int, c_int, c_int, c_int, c_int, c_int]),
     "vpt_unet_set_conv_path": (c_int, [c_int]),
     "vpt_unet_set_conv_ksplit": (c_int, [c_int]),
+    "vpt_unet_set_strip_kernel": (c_int, [c_int]),
     "vpt_unet_set_gather_stages": (c_int, [c_int]),
     "vpt_unet_rotate_weights": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p]),
     "vpt_unet_pool2": (c_int, [c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_void_p]),

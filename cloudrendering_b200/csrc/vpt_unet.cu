@@ -28,10 +28,12 @@
 //
 // Every mbarrier wait is bounded: on expiry the kernel records VPT_ERR_ITER_LIMIT in *err, waits
 // (bounded) for the MMAs it issued, frees its TMEM and returns.
+#include <cuda.h>  // CUtensorMap (encoded through the runtime's driver entry point)
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
+#include <string.h>
 #include "../../include/vpt_b200.h"
 #include "vpt_kernels.h"
 
@@ -518,12 +520,13 @@ struct StripArgs {
     int tmem_cols;
 };
 
-__device__ __forceinline__ void strip_epilogue(const StripArgs& a, uint32_t tacc, int n_img, int yrow, int x0) {
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int x = x0 + warp * 32 + lane;
+// TMEM lane quarter `quarter` (the warp's index mod 4) holds pixels x0 + 32 quarter .. + 31
+__device__ __forceinline__ void strip_epilogue(const StripArgs& a, uint32_t tacc, int n_img, int yrow, int x0,
+                                               int quarter, int lane) {
+    const int x = x0 + quarter * 32 + lane;
     const bool ok = x < a.w_;
     const size_t p = ((size_t)n_img * a.h + yrow) * a.w_ + (ok ? x : 0);
-    const uint32_t trow = tacc + ((uint32_t)(warp * 32) << 16);
+    const uint32_t trow = tacc + ((uint32_t)(quarter * 32) << 16);
     for (int c0 = 0; c0 < a.cout; c0 += 16) {
         float v[16];
         tmem_ld16(trow + (uint32_t)c0, v);
@@ -636,7 +639,7 @@ __global__ void __launch_bounds__(kThreads) conv_strip_kernel(const StripArgs a)
             if (!mbar_wait(smem_u32(&bars[(g - 1) & 1]), (uint32_t)(((g - 1) >> 1) & 1))) fail = 1;
             if (__syncthreads_or(fail)) break;
             tc_fence_after();
-            strip_epilogue(a, tmem + (uint32_t)(((g - 1) & 1) * a.cout), pend_n, pend_y, pend_x0);
+            strip_epilogue(a, tmem + (uint32_t)(((g - 1) & 1) * a.cout), pend_n, pend_y, pend_x0, tid >> 5, tid & 31);
             pending = false;
         }
         load_row(n_img, y0 - 1, x0);
@@ -674,7 +677,7 @@ __global__ void __launch_bounds__(kThreads) conv_strip_kernel(const StripArgs a)
                 if (!mbar_wait(smem_u32(&bars[(g - 1) & 1]), (uint32_t)(((g - 1) >> 1) & 1))) fail = 1;
                 if (__syncthreads_or(fail)) break;
                 tc_fence_after();
-                strip_epilogue(a, tmem + (uint32_t)(((g - 1) & 1) * a.cout), pend_n, pend_y, pend_x0);
+                strip_epilogue(a, tmem + (uint32_t)(((g - 1) & 1) * a.cout), pend_n, pend_y, pend_x0, tid >> 5, tid & 31);
             }
             pending = true;
             pend_n = n_img;
@@ -690,7 +693,7 @@ __global__ void __launch_bounds__(kThreads) conv_strip_kernel(const StripArgs a)
         if (!mbar_wait(smem_u32(&bars[(g - 1) & 1]), (uint32_t)(((g - 1) >> 1) & 1))) fail = 1;
         if (!__syncthreads_or(fail)) {
             tc_fence_after();
-            strip_epilogue(a, tmem + (uint32_t)(((g - 1) & 1) * a.cout), pend_n, pend_y, pend_x0);
+            strip_epilogue(a, tmem + (uint32_t)(((g - 1) & 1) * a.cout), pend_n, pend_y, pend_x0, tid >> 5, tid & 31);
         }
     } else if (pending) {
         // bounded wait for the MMAs in flight before the accumulator is freed
@@ -700,6 +703,297 @@ __global__ void __launch_bounds__(kThreads) conv_strip_kernel(const StripArgs a)
     tc_fence_before();
     __syncthreads();
     if (tid < 32) {
+        tc_fence_after();
+        tmem_dealloc(tmem, (uint32_t)a.tmem_cols);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// the warp-specialised row-strip convolution (TMA-fed)
+// ---------------------------------------------------------------------------------------------
+// The tiling of conv_strip_kernel (persistent CTAs over segments of consecutive rows of one
+// 128-pixel column; row strips of 130 pixels; A of tap (dy, dx) = the strip of row y+dy-1 with its
+// start moved by dx pixel rows; the weights of all 9 taps resident), with the work split over warps
+// and no CTA-wide barrier after the weights have landed:
+//   warp 0     one lane loads input rows into a ring of `ring` slots with the tensor-memory-access
+//              unit: one box {64 / 32 / 16 channels, 130 pixels} per channel group, written in the
+//              swizzled K-major layout of that line width (pixel rows of 128 / 64 / 32 bytes), rows and
+//              pixels outside the image arriving as zeros; full[s] completes on the bytes, empty[s] is
+//              signalled by the tensor core once the last MMA reading the slot has completed;
+//   warp 1     one lane issues the 9 x cin/16 MMAs of each output row into one of two TMEM
+//              accumulators (acc_full[b] on completion, after acc_empty[b]);
+//   warps 2-5  the epilogue; warp w reads TMEM lane quarter w % 4 (pixels x0 + 32 (w % 4) .. + 31).
+// All roles walk the same segment sequence, so ring and accumulator positions agree without
+// communication.  Every wait is bounded: on expiry the role records the error and stops, and the
+// CTA waits (bounded) for its copies and MMAs in flight before TMEM is released.
+constexpr int kWsThreads = 192;
+constexpr int kWsMaxRing = 8;
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(bar) : "memory");
+}
+// tiled 4-D load (coordinates innermost first) into this CTA's shared memory, completing on `bar`
+__device__ __forceinline__ void tma_load_4d(uint32_t dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
+                                            uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+        "%5}], [%6];\n" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(bar)
+        : "memory");
+}
+
+struct WsSegment {
+    int n_img, x0, y0, y1;
+};
+__device__ __forceinline__ WsSegment ws_segment(const StripArgs& a, int seg) {
+    const int col = seg / a.segs_per_col, part = seg % a.segs_per_col;
+    WsSegment g;
+    g.n_img = col / a.xtiles;
+    g.x0 = (col % a.xtiles) * kBM;
+    g.y0 = part * a.seg_rows;
+    g.y1 = min(a.h, g.y0 + a.seg_rows);
+    return g;
+}
+
+// Channel groups of a row: widths 64 / 32 / 16 channels = lines of 128 / 64 / 32 bytes per pixel in
+// the 128B / 64B / 32B-swizzled K-major layout (what one TMA box of {width, 130 pixels} writes);
+// each group buffer starts on a 1024-byte boundary.
+constexpr int kWsMaxGroups = 4;
+struct WsArgs {
+    StripArgs s;
+    int ngroups;
+    int gc[kWsMaxGroups];    // first channel of the group (within this pass)
+    int gw[kWsMaxGroups];    // channels of the group: 64, 32 or 16
+    int goff[kWsMaxGroups];  // byte offset of the group buffer in a ring slot
+    int row_bytes;           // ring slot size
+    int tx_bytes;            // bytes the boxes of one row deliver
+};
+
+// K-major swizzled shared-memory descriptor: line = 128 / 64 / 32 bytes per row, 8-row groups
+// `8 * line` apart (SBO), LBO unused (1), layout type 2 / 4 / 6 (bits 61-63).  The swizzle acts on
+// absolute shared-memory address bits (as the TMA's does), so a start moved by whole rows (the dx
+// taps) needs no base offset (measured: base offset 0 matches the oracle for every line width).
+__device__ __forceinline__ uint64_t smem_desc_sw(uint32_t addr, uint32_t line) {
+    uint64_t d = (uint64_t)((addr >> 4) & 0x3FFFu);
+    d |= (uint64_t)1 << 16;
+    d |= (uint64_t)(((8u * line) >> 4) & 0x3FFFu) << 32;
+    d |= (uint64_t)1 << 46;
+    const uint64_t layout = line == 128 ? 2 : (line == 64 ? 4 : 6);
+    d |= layout << 61;
+    return d;
+}
+
+// tcgen05.mma from descriptor halves.  No memory clobber: the MMA reads shared memory asynchronously
+// and is ordered by the mbarrier waits, tcgen05 fences and commits around it (which carry clobbers);
+// without one the issuing loop keeps its loop-invariant values in registers.
+__device__ __forceinline__ void mma_bf16_halves(uint32_t tmem_d, uint32_t a_lo, uint32_t a_hi, uint32_t b_lo,
+                                                uint32_t b_hi, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n.reg .pred p;\n.reg .b64 da, db;\nmov.b64 da, {%1, %2};\nmov.b64 db, {%3, %4};\n"
+        "setp.ne.b32 p, %6, 0;\ntcgen05.mma.cta_group::1.kind::f16 [%0], da, db, %5, p;\n}\n" ::"r"(tmem_d),
+        "r"(a_lo), "r"(a_hi), "r"(b_lo), "r"(b_hi), "r"(idesc), "r"(acc));
+}
+
+// high word of smem_desc_sw: SBO = 8 lines, version, layout type of the line width (2 * channels)
+__device__ __forceinline__ uint32_t a_hi_of(int channels) {
+    return (uint32_t)(smem_desc_sw(0, (uint32_t)channels * 2u) >> 32);
+}
+
+__global__ void __launch_bounds__(kWsThreads, 1) conv_ws_kernel(const __grid_constant__ CUtensorMap map64,
+                                                             const __grid_constant__ CUtensorMap map32,
+                                                             const __grid_constant__ CUtensorMap map16,
+                                                             const __grid_constant__ WsArgs wa, int ring) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    __shared__ uint64_t full[kWsMaxRing], empty[kWsMaxRing], acc_full[2], acc_empty[2], done_bar;
+    __shared__ uint32_t tmem_slot;
+    __shared__ int fail_any;
+    const StripArgs& a = wa.s;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int nkc = a.cin / 8;
+    const uint32_t w_bytes = 9u * (uint32_t)a.cin * (uint32_t)a.cout * 2u;
+    const uint32_t row_bytes = (uint32_t)wa.row_bytes;
+    const uint32_t sw = smem_u32(smem);
+    const uint32_t sring = sw + ((w_bytes + 1023u) & ~1023u);
+    const uint32_t acc_cols = (uint32_t)a.tmem_cols / 2;
+    if (tid == 0) {
+        for (int s = 0; s < ring; ++s) {
+            mbar_init(smem_u32(&full[s]), 1);
+            mbar_init(smem_u32(&empty[s]), 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(smem_u32(&acc_full[b]), 1);
+            mbar_init(smem_u32(&acc_empty[b]), 4);  // one arrival per epilogue warp
+        }
+        mbar_init(smem_u32(&done_bar), 1);
+        fail_any = 0;
+        fence_mbar_init();
+    }
+    if (warp == 1) tmem_alloc(smem_u32(&tmem_slot), (uint32_t)a.tmem_cols);
+    // resident weights: unit (t, kc, co) at ((t * nkc + kc) * cout + co) * 16
+    for (int q = tid; q < 9 * nkc * a.cout; q += kWsThreads) {
+        const int co = q % a.cout, rest = q / a.cout;
+        const int kc = rest % nkc, t = rest / nkc;
+        cp_async16(sw + (uint32_t)q * 16u, a.w + ((size_t)co * 9 + t) * a.cin_total + a.c0 + kc * 8, true);
+    }
+    cp_async_commit();
+    cp_async_wait<0>();
+    fence_proxy_async();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_slot;
+    const int total_segs = a.n * a.xtiles * a.segs_per_col;
+    bool fail = false;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            int slot = 0;
+            uint32_t phase = 0;
+            long issued = 0;
+            for (int seg = blockIdx.x; seg < total_segs && !fail; seg += gridDim.x) {
+                const WsSegment g = ws_segment(a, seg);
+                if (g.y0 >= g.y1) continue;
+                for (int yy = g.y0 - 1; yy <= g.y1; ++yy) {
+                    if (!mbar_wait(smem_u32(&empty[slot]), phase ^ 1u)) {
+                        fail = true;
+                        break;
+                    }
+                    const uint32_t dst = sring + (uint32_t)slot * row_bytes;
+                    const uint32_t fb = smem_u32(&full[slot]);
+                    mbar_arrive_expect_tx(fb, (uint32_t)wa.tx_bytes);
+                    for (int k = 0; k < wa.ngroups; ++k) {
+                        const CUtensorMap* m = wa.gw[k] == 64 ? &map64 : (wa.gw[k] == 32 ? &map32 : &map16);
+                        tma_load_4d(dst + (uint32_t)wa.goff[k], m, a.c0 + wa.gc[k], g.x0 - 1, yy, g.n_img, fb);
+                    }
+                    ++issued;
+                    if (++slot == ring) {
+                        slot = 0;
+                        phase ^= 1u;
+                    }
+                }
+            }
+            // the last loads (one per slot at most) have landed before the CTA can exit
+            const long tail = issued < ring ? issued : ring;
+            for (long k = 1; k <= tail; ++k) {
+                int s = slot - (int)k;
+                uint32_t ph = phase;
+                if (s < 0) {
+                    s += ring;
+                    ph ^= 1u;
+                }
+                if (!mbar_wait(smem_u32(&full[s]), ph)) fail = true;
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            const uint32_t idesc = instr_desc(kBM, a.cout, 0, 0);
+            // descriptor words: A (swizzled, start field added per row / group / dx / step; LBO 1),
+            // B (no swizzle, LBO = one 8-channel plane of the weights, SBO 128)
+            const uint64_t bd0 = smem_desc(sw, (uint32_t)a.cout * 16u, 128);
+            const uint32_t b_hi = (uint32_t)(bd0 >> 32), b_lo0 = (uint32_t)bd0;
+            const uint32_t a_lo1 = 1u << 16;  // LBO field of the A descriptors
+            const uint32_t b_step = 2u * (uint32_t)a.cout, b_tap = (uint32_t)(nkc * a.cout), b_row = 3u * b_tap;
+            // per channel group (registers: every index below is a compile-time constant)
+            const int ngroups = wa.ngroups;
+            uint32_t g_ahi[kWsMaxGroups], g_aoff[kWsMaxGroups], g_line[kWsMaxGroups], g_boff[kWsMaxGroups];
+            int g_steps[kWsMaxGroups];
+#pragma unroll
+            for (int k = 0; k < kWsMaxGroups; ++k) {
+                const bool on = k < ngroups;
+                const int gw = on ? wa.gw[k] : 16;
+                g_ahi[k] = a_hi_of(gw);
+                g_aoff[k] = on ? (uint32_t)wa.goff[k] >> 4 : 0u;
+                g_line[k] = (uint32_t)gw >> 3;  // line bytes / 16
+                g_boff[k] = on ? (uint32_t)((wa.gc[k] >> 3) * a.cout) : 0u;
+                g_steps[k] = gw / 16;
+            }
+            int slot = 0;        // ring position of the segment's first row
+            uint32_t phase = 0;
+            long g = 0;          // accumulators used
+            for (int seg = blockIdx.x; seg < total_segs && !fail; seg += gridDim.x) {
+                const WsSegment sgm = ws_segment(a, seg);
+                if (sgm.y0 >= sgm.y1) continue;
+                const int rows = sgm.y1 - sgm.y0;
+                for (int i = 0; i < rows && !fail; ++i, ++g) {
+                    // input rows i, i+1, i+2 of the segment (y-1, y, y+1): wait for the newest (all
+                    // three for the first output row)
+                    for (int k = (i == 0 ? 0 : 2); k <= 2; ++k) {
+                        const int pos = slot + i + k;
+                        const uint32_t ph = phase ^ (uint32_t)((pos / ring) & 1);
+                        if (!mbar_wait(smem_u32(&full[pos % ring]), ph)) fail = true;
+                    }
+                    const int b = (int)(g & 1);
+                    if (!fail && !mbar_wait(smem_u32(&acc_empty[b]), (uint32_t)(((g >> 1) & 1) ^ 1))) fail = true;
+                    if (fail) break;
+                    tc_fence_after();
+                    const uint32_t dacc = tmem + (uint32_t)b * acc_cols;
+                    // descriptors walk affinely: per channel group, A's start advances by one pixel
+                    // row per dx and 32 bytes per 16-channel step, B's by a tap (nkc * cout * 16
+                    // bytes) per dx and two 8-channel planes per step
+                    uint32_t acc = 0;
+#pragma unroll 1
+                    for (int dy = 0; dy < 3; ++dy) {
+                        const uint32_t row16 = (sring + (uint32_t)((slot + i + dy) % ring) * row_bytes) >> 4;
+#pragma unroll
+                        for (int k = 0; k < kWsMaxGroups; ++k) {
+                            if (k >= ngroups) break;
+                            const uint32_t al0 = a_lo1 + row16 + g_aoff[k];
+                            const uint32_t bl0 = b_lo0 + (uint32_t)dy * b_row + g_boff[k];
+#pragma unroll
+                            for (int dx = 0; dx < 3; ++dx) {
+                                const uint32_t al = al0 + (uint32_t)dx * g_line[k], bl = bl0 + (uint32_t)dx * b_tap;
+#pragma unroll
+                                for (int j = 0; j < 4; ++j) {
+                                    if (j >= g_steps[k]) break;
+                                    mma_bf16_halves(dacc, al + 2u * (uint32_t)j, g_ahi[k], bl + (uint32_t)j * b_step,
+                                                    b_hi, idesc, acc);
+                                    acc = 1;
+                                }
+                            }
+                        }
+                    }
+                    mma_commit(smem_u32(&acc_full[b]));
+                    mma_commit(smem_u32(&empty[(slot + i) % ring]));  // input row y-1 is done
+                }
+                if (fail) break;
+                mma_commit(smem_u32(&empty[(slot + rows) % ring]));
+                mma_commit(smem_u32(&empty[(slot + rows + 1) % ring]));
+                const int adv = slot + rows + 2;
+                slot = adv % ring;
+                phase ^= (uint32_t)((adv / ring) & 1);
+            }
+            // every MMA this CTA issued has completed before TMEM is released
+            mma_commit(smem_u32(&done_bar));
+            if (!mbar_wait(smem_u32(&done_bar), 0)) fail = true;
+        }
+    } else {
+        const int quarter = warp & 3;
+        long g = 0;
+        for (int seg = blockIdx.x; seg < total_segs && !fail; seg += gridDim.x) {
+            const WsSegment sgm = ws_segment(a, seg);
+            for (int y = sgm.y0; y < sgm.y1; ++y, ++g) {
+                const int b = (int)(g & 1);
+                const bool ok = mbar_wait(smem_u32(&acc_full[b]), (uint32_t)((g >> 1) & 1));
+                if (!__all_sync(0xffffffffu, ok)) {
+                    fail = true;
+                    break;
+                }
+                tc_fence_after();
+                strip_epilogue(a, tmem + (uint32_t)b * acc_cols, sgm.n_img, y, sgm.x0, quarter, lane);
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(smem_u32(&acc_empty[b]));
+            }
+        }
+    }
+    if (fail) atomicOr(&fail_any, 1);
+    tc_fence_before();
+    __syncthreads();
+    if (fail_any && tid == 0 && a.err) atomicExch(a.err, (int)VPT_ERR_ITER_LIMIT);
+    if (warp == 1) {
         tc_fence_after();
         tmem_dealloc(tmem, (uint32_t)a.tmem_cols);
     }
@@ -1627,6 +1921,146 @@ cudaError_t launch_strip_pass(StripArgs a, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+// ---- the warp-specialised strip kernel ----
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_tiled() {
+    static EncodeTiledFn fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    }
+    return fn;
+}
+
+// NHWC bf16 activation [n][h][w][c] as a 4-D tensor (c, w, h, n) with boxes of `width` channels x
+// 130 pixels, swizzled for lines of 2 * width bytes (the channel coordinate of every load is a
+// multiple of 16 channels, i.e. 32 bytes)
+bool encode_rows(CUtensorMap* map, const bf16* x, int n, int h, int w, int c, int width) {
+    EncodeTiledFn fn = encode_tiled();
+    if (!fn || reinterpret_cast<uintptr_t>(x) % 16) return false;
+    const cuuint64_t dims[4] = {(cuuint64_t)c, (cuuint64_t)w, (cuuint64_t)h, (cuuint64_t)n};
+    const cuuint64_t strides[3] = {(cuuint64_t)c * 2, (cuuint64_t)w * c * 2, (cuuint64_t)h * w * c * 2};
+    const cuuint32_t box[4] = {(cuuint32_t)width, (cuuint32_t)kStripPix, 1, 1};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    const CUtensorMapSwizzle sz = width == 64 ? CU_TENSOR_MAP_SWIZZLE_128B
+                                              : (width == 32 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_32B);
+    return fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<bf16*>(x), dims, strides, box, estr,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, sz, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+constexpr size_t kSmPerSm = 233472;   // shared memory of one SM (bytes)
+constexpr size_t kSmPerCta = 232448;  // largest dynamic shared memory of one CTA
+constexpr size_t kWsStatic = 2048;    // static shared memory + the per-CTA reservation, rounded up
+
+// a pass's channels as groups of 64, then 32, then 16 (each a 1024-byte aligned buffer of 130 lines)
+struct WsGroups {
+    int n = 0, c[kWsMaxGroups] = {}, w[kWsMaxGroups] = {}, off[kWsMaxGroups] = {}, row_bytes = 0, tx = 0;
+};
+inline WsGroups ws_groups_of(int cin) {
+    WsGroups g;
+    int c = 0, off = 0;
+    while (c < cin && g.n < kWsMaxGroups) {
+        const int rem = cin - c, width = rem >= 64 ? 64 : (rem >= 32 ? 32 : 16);
+        g.c[g.n] = c;
+        g.w[g.n] = width;
+        g.off[g.n] = off;
+        off += (kStripPix * width * 2 + 1023) / 1024 * 1024;
+        g.tx += kStripPix * width * 2;
+        c += width;
+        ++g.n;
+    }
+    g.row_bytes = c == cin ? off : 0;  // 0: more groups than supported
+    return g;
+}
+
+inline size_t ws_weight_bytes(int cin, int cout) { return (9ul * cin * cout * 2 + 1023) & ~(size_t)1023; }
+inline size_t ws_row_bytes(int cin) { return (size_t)ws_groups_of(cin).row_bytes; }
+
+// CTAs per SM and ring depth: the most rows in flight per SM (CTAs x (ring - 3)), then more CTAs;
+// TMEM holds two accumulators per CTA.  false when not even one CTA with a 4-slot ring fits.
+bool ws_config(int cin, int cout, int& per_sm, int& ring) {
+    const int acc = pow2_cols(cout);
+    const size_t rb = ws_row_bytes(cin);
+    per_sm = 0;
+    ring = 0;
+    if (rb == 0) return false;
+    int best = -1;
+    for (int occ = 1; occ <= 3 && occ * 2 * acc <= 512; ++occ) {  // 3: the registers of 3 CTAs fit an SM
+        const size_t budget = kSmPerSm / occ - kWsStatic;
+        const size_t wb = ws_weight_bytes(cin, cout);
+        if (budget > kSmPerCta || wb >= budget) continue;
+        const int r = (int)std::min<size_t>(kWsMaxRing, (budget - wb) / rb);
+        if (r < 4) continue;
+        const int score = occ * (r - 3);
+        if (score > best || (score == best && occ > per_sm)) {
+            best = score;
+            per_sm = occ;
+            ring = r;
+        }
+    }
+    return per_sm > 0;
+}
+
+// input-channel passes for the warp-specialised kernel (0 = not eligible).  Several passes re-stream
+// an fp32 partial: measured faster than the gather kernel for up to 64 output channels (176 -> 32,
+// 160 -> 64), slower for 96 -> 96 and 224 -> 96.
+inline int ws_groups(int width, int cin, int cout, bool any = false) {
+    if (width < kBM || cout > 256) return 0;
+    for (int g = 1; g <= 4; ++g) {
+        const int cg = (cin / 16 + g - 1) / g * 16;
+        int occ, ring;
+        if (ws_config(cg, cout, occ, ring)) return (g == 1 || cout <= 64 || any) ? g : 0;
+    }
+    return 0;
+}
+
+cudaError_t launch_ws_pass(StripArgs a, cudaStream_t s) {
+    int per_sm = 0, ring = 0;
+    if (!ws_config(a.cin, a.cout, per_sm, ring)) return cudaErrorInvalidValue;
+    WsArgs wa{};
+    const WsGroups gr = ws_groups_of(a.cin);
+    CUtensorMap maps[3];  // widths 64, 32, 16
+    memset(maps, 0, sizeof(maps));
+    bool have[3] = {false, false, false};
+    for (int k = 0; k < gr.n; ++k) {
+        const int mi = gr.w[k] == 64 ? 0 : (gr.w[k] == 32 ? 1 : 2);
+        if (!have[mi] && !encode_rows(&maps[mi], a.x, a.n, a.h, a.w_, a.cin_total, gr.w[k]))
+            return cudaErrorInvalidValue;
+        have[mi] = true;
+        wa.gc[k] = gr.c[k];
+        wa.gw[k] = gr.w[k];
+        wa.goff[k] = gr.off[k];
+    }
+    wa.ngroups = gr.n;
+    wa.row_bytes = gr.row_bytes;
+    wa.tx_bytes = gr.tx;
+    a.tmem_cols = 2 * pow2_cols(a.cout);
+    const int slots = sm_count() * per_sm;
+    int total = 0;
+    strip_segments(a.n, a.h, a.w_, slots, a.xtiles, a.seg_rows, a.segs_per_col, total);
+    const int grid = min(total, slots);
+    wa.s = a;
+    // at least the shared memory that holds the CTAs per SM to per_sm (TMEM is sized for that many)
+    const size_t need = ws_weight_bytes(a.cin, a.cout) + (size_t)ring * ws_row_bytes(a.cin);
+    const size_t smem = std::max(need, std::min(kSmPerCta, kSmPerSm / (per_sm + 1) - kWsStatic + 1024));
+    cudaError_t e = cudaFuncSetAttribute(conv_ws_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    conv_ws_kernel<<<grid, kWsThreads, smem, s>>>(maps[0], maps[1], maps[2], wa, ring);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+static int g_strip_kernel = 0;  // 0: warp-specialised (TMA) strips, 1: the cp.async strip kernel
+
 cudaError_t launch_strip(const ConvArgs& c, int groups, cudaStream_t s) {
     StripArgs a{};
     a.x = c.x;
@@ -1644,7 +2078,7 @@ cudaError_t launch_strip(const ConvArgs& c, int groups, cudaStream_t s) {
         a.y = c.y;
         a.relu = c.relu;
         a.out_f32 = c.out_f32;
-        return launch_strip_pass(a, s);
+        return g_strip_kernel == 0 ? launch_ws_pass(a, s) : launch_strip_pass(a, s);
     }
     // fp32 partial sum of the earlier groups (stream-ordered scratch)
     float* part = nullptr;
@@ -1666,7 +2100,7 @@ cudaError_t launch_strip(const ConvArgs& c, int groups, cudaStream_t s) {
             p.relu = c.relu;
             p.out_f32 = c.out_f32;
         }
-        e = launch_strip_pass(p, s);
+        e = g_strip_kernel == 0 ? launch_ws_pass(p, s) : launch_strip_pass(p, s);
     }
     const cudaError_t f = cudaFreeAsync(part, s);
     return e != cudaSuccess ? e : f;
@@ -1705,7 +2139,10 @@ VptStatus vpt_unet_conv3x3(const void* x, const void* w, const float* bias, cons
     a.tmem_cols = pow2_cols(a.n_tile);
     a.relu = relu;
     a.out_f32 = out_f32;
-    const int groups = strip_groups(width, cin, cout, g_force_strip);
+    // row strips: the warp-specialised kernel's tensor map wants a 16-byte aligned base
+    const bool aligned = reinterpret_cast<uintptr_t>(x) % 16 == 0;
+    const int groups = g_strip_kernel == 0 ? (aligned ? ws_groups(width, cin, cout, g_force_strip) : 0)
+                                           : strip_groups(width, cin, cout, g_force_strip);
     if (groups > 0 && !g_force_gather)
         return launch_strip(a, groups, static_cast<cudaStream_t>(stream)) == cudaSuccess ? VPT_OK : VPT_ERR_CUDA;
     const long P = (long)n * h * width;
@@ -1736,6 +2173,13 @@ VptStatus vpt_unet_conv3x3(const void* x, const void* w, const float* bias, cons
     }
     const cudaError_t f = cudaFreeAsync(part, s);
     return (e == cudaSuccess && f == cudaSuccess) ? VPT_OK : VPT_ERR_CUDA;
+}
+
+// 0: the warp-specialised (TMA) row-strip kernel, 1: the cp.async row-strip kernel (comparisons)
+VptStatus vpt_unet_set_strip_kernel(int kind) {
+    if (kind < 0 || kind > 1) return VPT_ERR_ARG;
+    g_strip_kernel = kind;
+    return VPT_OK;
 }
 
 // K splits of the gather convolution: 0 chosen by grid size, 1 never split, k > 1 always k (tests)

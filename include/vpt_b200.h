@@ -377,6 +377,10 @@ VptStatus vpt_unet_conv3x3(const void* x, const void* w, const float* bias, cons
  * fp32 partial allocated on the stream), 1 = the per-tile gather kernels everywhere, 2 = the row-strip
  * kernels wherever they apply. */
 VptStatus vpt_unet_set_conv_path(int path);
+/* Row-strip convolution kernel: 0 (default) = warp-specialised (input rows loaded by the tensor-memory-
+ * access unit into a ring, one MMA warp, four epilogue warps, double TMEM accumulators; input
+ * channel groups when the weights and a 4-row ring do not fit), 1 = the cp.async row-strip kernel. */
+VptStatus vpt_unet_set_strip_kernel(int kind);
 /* K splits of the per-tile gather convolution: 0 (default) = by grid size (grids of at most half an SM wave
  * split their K stages over up to 8 CTAs, whose fp32 sums, allocated on the stream, are added in split
  * order before the bias / ReLU / mask epilogue), 1 = never, k > 1 = always k (at most the K stages). */

@@ -135,12 +135,15 @@ STRIP_CASES = [
     (1, 4, 200, 32, 176),   # 13x13 kernel head
     (1, 37, 128, 64, 64),   # many rows: several segments per column
     (1, 6, 128, 160, 64),   # input channels in two groups (fp32 partial between the passes)
+    (3, 20, 384, 32, 32),   # three columns, several segments each: the input ring wraps across segments
 ]
 
 
+@pytest.mark.parametrize("kind", [0, 1], ids=["warp_specialised", "cp_async"])
 @pytest.mark.parametrize("case", STRIP_CASES)
-def test_strip_conv_forward_and_input_grad(lib, case):
+def test_strip_conv_forward_and_input_grad(lib, case, kind):
     n, h, w, cin, cout = case
+    assert lib.vpt_unet_set_strip_kernel(kind) == 0
     assert lib.vpt_unet_set_conv_path(2) == 0
     x = uo.bf16(rng_data(21, n, h, w, cin))
     wt = uo.bf16(rng_data(22, cout, 9, cin, scale=1.0 / np.sqrt(9 * cin)))
@@ -168,6 +171,7 @@ def test_strip_conv_forward_and_input_grad(lib, case):
     run(lib, "vpt_unet_conv3x3", ptr(d_dy), ptr(wrot), None, ptr(dx), ptr(g), n, h, w, cout, cin, 0, 0)
     close_bf16(host(g), uo.conv3x3_input_grad(dy, wt, mask=x))
     assert lib.vpt_unet_set_conv_path(0) == 0
+    assert lib.vpt_unet_set_strip_kernel(0) == 0
 
 
 WGRAD_CASES = [
