@@ -1090,6 +1090,10 @@ __global__ void __launch_bounds__(kThreads) wgrad_strip_kernel(const WgradStripA
     };
 
     const uint32_t idesc = instr_desc(a.ma, N, 1, 1);
+    // MN-major descriptor words (LBO = 128 between 8-pixel groups, SBO = plane stride); start fields 0
+    const uint64_t xd0 = smem_desc(0, 128, kPlane), dd0 = smem_desc(0, 128, kDyPlane);
+    const uint32_t x_lo = (uint32_t)xd0, x_hi = (uint32_t)(xd0 >> 32);
+    const uint32_t d_lo = (uint32_t)dd0, d_hi = (uint32_t)(dd0 >> 32);
     const int total_segs = a.n * a.xtiles * a.segs_per_col;
     long g = 0;
     int fail = 0;
@@ -1117,17 +1121,19 @@ __global__ void __launch_bounds__(kThreads) wgrad_strip_kernel(const WgradStripA
             if (__syncthreads_or(fail)) break;
             if (tid == 0) {
                 tc_fence_after();
-                const uint32_t drow = sdy + (uint32_t)(yrow % kDyRing) * dyrow;
+                // descriptor halves: the start fields walk 256 bytes (16 pixels) per K step; the x
+                // strip of tap (dyy, dxx) starts dxx pixels (16 bytes) into the slot of row yrow+dyy
+                const uint32_t d16 = (sdy + (uint32_t)(yrow % kDyRing) * dyrow) >> 4;
                 for (int t = a.t0; t < a.t1; ++t) {
-                    const int dyy = t / 3, dxx = t % 3;
-                    const uint32_t xs = sx + (uint32_t)((yrow + dyy) % kRing) * xrow + (uint32_t)dxx * 16u;
+                    const int dyy = t / 3, dxx = t - 3 * dyy;
+                    const uint32_t x16 = ((sx + (uint32_t)((yrow + dyy) % kRing) * xrow) >> 4) + (uint32_t)dxx;
                     const uint32_t dacc = tmem + (uint32_t)((t - a.t0) * N);
+#pragma unroll
                     for (int j = 0; j < kBM / 16; ++j) {
-                        const uint64_t dx_desc = smem_desc(xs + (uint32_t)j * 256u, 128, kPlane);
-                        const uint64_t dd_desc = smem_desc(drow + (uint32_t)j * 256u, 128, kDyPlane);
-                        const uint64_t da = ROLE == 0 ? dx_desc : dd_desc;
-                        const uint64_t db = ROLE == 0 ? dd_desc : dx_desc;
-                        mma_bf16(dacc, da, db, idesc, (g == 0 && j == 0) ? 0u : 1u);
+                        const uint32_t xl = x_lo + x16 + 16u * (uint32_t)j, dl = d_lo + d16 + 16u * (uint32_t)j;
+                        const uint32_t acc = (g == 0 && j == 0) ? 0u : 1u;
+                        if (ROLE == 0) mma_bf16_halves(dacc, xl, x_hi, dl, d_hi, idesc, acc);
+                        else mma_bf16_halves(dacc, dl, d_hi, xl, x_hi, idesc, acc);
                     }
                 }
                 mma_commit(smem_u32(&bars[g & 1]));
