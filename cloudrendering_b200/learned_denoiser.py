@@ -573,16 +573,23 @@ class TrainingSet:
         self.paths = S * size * size * (max(self.spp_levels) + target_spp)
 
     def batch(self, rng: np.random.Generator, batch_size: int) -> dict:
-        """A random batch of (scene, sample count) pairs with random flips / transposes."""
+        """A random batch of (scene, sample count) pairs with random flips / transposes.  The pair
+        indices are drawn on the GPU (a generator seeded from rng on first use): no host round trip,
+        so the host queues the next training step while the GPU runs the current one."""
         S, L = self.radiance.shape[:2]
-        si = torch.from_numpy(rng.integers(0, S, batch_size)).cuda()
-        li = torch.from_numpy(rng.integers(0, L, batch_size)).cuda()
+        if getattr(self, "_gen", None) is None:
+            self._gen = torch.Generator(device="cuda")
+            self._gen.manual_seed(int(rng.integers(0, 2**62)))
+        si = torch.randint(0, S, (batch_size,), device="cuda", generator=self._gen)
+        li = torch.randint(0, L, (batch_size,), device="cuda", generator=self._gen)
         keys = ["radiance", "albedo", "normal", "depth", "transmittance"]
         if self.second_moment is not None:
             keys.append("second_moment")
         out = {k: getattr(self, k)[si, li] for k in keys}
         out["target"] = self.target[si]
-        out["noise_level"] = (1.0 / torch.tensor(self.spp_levels, dtype=torch.float32, device="cuda")[li].sqrt())
+        if getattr(self, "_inv_sqrt_spp", None) is None:  # one upload: a copy per batch would wait for the GPU
+            self._inv_sqrt_spp = 1.0 / torch.tensor(self.spp_levels, dtype=torch.float32, device="cuda").sqrt()
+        out["noise_level"] = self._inv_sqrt_spp[li]
         flip = rng.integers(0, 8)
         for k in list(out.keys()):
             if k == "noise_level":
