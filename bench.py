@@ -369,7 +369,7 @@ def run_ours(args):
 # to reach relMSE <= 1e-3 on a held-out scene (256^3 cloud, 512^2, max 128 bounces) against its
 # FP64-accumulated 16384-spp render: plain accumulation, EAW (iteration count 1..5 chosen per sample
 # count by the lowest error, i.e. tuned with the reference in hand) and the learned denoiser.
-LEARNED = dict(scenes=128, size=256, spp_levels=(1, 2, 4, 8, 16, 64, 256), target_spp=2048, steps=6000, batch=8,
+LEARNED = dict(scenes=256, size=256, spp_levels=(1, 2, 4, 8, 16, 64, 256), target_spp=2048, steps=6000, batch=8,
                lr=5e-4, lr_end=1e-5, kernel_size=13, grid=128)
 EVAL = dict(seed=77777, res=512, grid=256, max_bounces=128, ref_spp=16384,
             levels=(1, 2, 4, 8, 16, 32, 64, 128, 256, 512, 1024, 2048, 4096), target=1e-3)
