@@ -509,10 +509,10 @@ def run_learned(vpt, lib, ctx, small):
         done = n
         plain = (vpt.get_film_sum(R, R).cuda() / n).float().contiguous()
 
-        def learned_once():
-            f = ld.read_features(vpt, img)
-            return dgraph(plain[None], f["albedo"][None], f["normal"][None], f["depth"][None],
-                          f["transmittance"][None], torch.full((1,), 1.0 / math.sqrt(n), device="cuda"))[0]
+        noise = torch.full((1,), 1.0 / math.sqrt(n), device="cuda")
+
+        def learned_once():  # the renderer's feature planes go straight into the graph's inputs
+            return dgraph.from_renderer(vpt, plain, noise)[0]
         den, ms = timed(learned_once)
         net_ms.append(ms)
         row["learned"] = ld.relmse(den, ref)

@@ -1407,6 +1407,17 @@ VptStatus vpt_get_feature_map(VptContext* ctx, int feature, float* out, int chan
     return VPT_OK;
 }
 
+VptStatus vpt_get_denoiser_features(VptContext* ctx, float* albedo, float* normal, float* depth, float* transmittance,
+                                    void* stream) {
+    VPT_CHECK_CTX(ctx);
+    if (!features_needed(ctx) || !ctx->feat.ptr || ctx->film_frames == 0)
+        return fail(ctx, VPT_ERR_STATE, "feature maps are not enabled or nothing rendered");
+    if (!albedo && !normal && !depth && !transmittance) return fail(ctx, VPT_ERR_ARG, "no output");
+    VPT_CHECK_CUDA(ctx, vpt::denoiser_features(ctx->feat.ptr, ctx->width * ctx->height, feature_frames(ctx),
+                                               ctx->albedo, albedo, normal, depth, transmittance, as_stream(stream)));
+    return VPT_OK;
+}
+
 VptStatus vpt_get_stats(VptContext* ctx, VptStats* stats) {
     VPT_CHECK_CTX(ctx);
     if (!stats) return VPT_ERR_ARG;

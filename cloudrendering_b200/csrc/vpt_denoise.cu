@@ -586,6 +586,39 @@ cudaError_t feature_to_chw(const float* feat, int n, uint32_t frames, int featur
     return cudaGetLastError();
 }
 
+// The four feature planes a learned denoiser reads, in one pass over the feature accumulation:
+// albedo (3 planes: the medium albedo times the hit fraction), normal (3), depth mean (1),
+// transmittance (1), each output optional; the same values as feature_to_chw's first channels.
+__global__ void denoiser_features_kernel(const float* __restrict__ feat, int n, float inv_frames, float a0, float a1,
+                                         float a2, float* __restrict__ albedo, float* __restrict__ normal,
+                                         float* __restrict__ depth, float* __restrict__ trans) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float* f = feat + (size_t)i * kFeatStride;
+    if (albedo) {
+        const float hit = f[kFeatPos + 3] * inv_frames;
+        albedo[i] = a0 * hit;
+        albedo[(size_t)n + i] = a1 * hit;
+        albedo[2 * (size_t)n + i] = a2 * hit;
+    }
+    if (normal) {
+        normal[i] = f[kFeatNormal] * inv_frames;
+        normal[(size_t)n + i] = f[kFeatNormal + 1] * inv_frames;
+        normal[2 * (size_t)n + i] = f[kFeatNormal + 2] * inv_frames;
+    }
+    if (depth) depth[i] = f[kFeatDepth] * inv_frames;
+    if (trans) trans[i] = f[kFeatTrans] * inv_frames;
+}
+
+cudaError_t denoiser_features(const float* feat, int n, uint32_t frames, const float* albedo_rgb, float* albedo,
+                              float* normal, float* depth, float* trans, cudaStream_t stream) {
+    denoiser_features_kernel<<<(n + 255) / 256, 256, 0, stream>>>(feat, n, 1.0f / float(frames), albedo_rgb[0],
+                                                                  albedo_rgb[1], albedo_rgb[2], albedo, normal, depth,
+                                                                  trans);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
 // ---------------------------------------------------------------------------------------------
 // EAW without allocation.
 //

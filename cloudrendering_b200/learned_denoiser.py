@@ -441,6 +441,17 @@ class DenoiseGraph:
         return self.net.denoise(i["radiance"], i["albedo"], i["normal"], i["depth"], i["transmittance"],
                                 i["noise_level"])
 
+    def from_renderer(self, vpt, radiance, noise_level):
+        """Denoises the renderer's current accumulation: its feature planes are written straight into
+        the graph's inputs (one launch), then the graph is replayed.  radiance [3, H, W] (or [1, 3, H, W]),
+        noise_level [1]; batch 1."""
+        i = self.inputs
+        vpt.read_denoiser_features(i["albedo"], i["normal"], i["depth"], i["transmittance"])
+        i["radiance"].copy_(radiance.reshape(i["radiance"].shape))
+        i["noise_level"].copy_(noise_level.reshape(i["noise_level"].shape))
+        self.graph.replay()
+        return self.out
+
     def __call__(self, radiance, albedo=None, normal=None, depth=None, transmittance=None, noise_level=None):
         for k, v in (("radiance", radiance), ("albedo", albedo), ("normal", normal), ("depth", depth),
                      ("transmittance", transmittance), ("noise_level", noise_level)):
@@ -493,11 +504,13 @@ def setup_scene(vpt, sc: dict, grid: int = 128, max_bounces: int = 64) -> None:
 
 
 def read_features(vpt, img: torch.Tensor) -> dict:
-    """Feature planes of the current accumulation: albedo [3], normal [3], depth [1], transmittance [1]."""
-    return {"albedo": vpt.get_feature_map_from_string(img, "Albedo")[:3].contiguous(),
-            "normal": vpt.get_feature_map_from_string(img, "Normal")[:3].contiguous(),
-            "depth": vpt.get_feature_map_from_string(img, "Depth")[:1].contiguous(),
-            "transmittance": vpt.get_feature_map_from_string(img, "Transmittance")[:1].contiguous()}
+    """Feature planes of the current accumulation: albedo [3], normal [3], depth [1], transmittance [1]
+    (one launch: vpt.read_denoiser_features)."""
+    _, h, w = img.shape
+    f = {"albedo": torch.empty((3, h, w), device=img.device), "normal": torch.empty((3, h, w), device=img.device),
+         "depth": torch.empty((1, h, w), device=img.device), "transmittance": torch.empty((1, h, w), device=img.device)}
+    vpt.read_denoiser_features(f["albedo"], f["normal"], f["depth"], f["transmittance"])
+    return f
 
 
 TARGET_FRAME_ORIGIN = 1 << 24  # targets use frames disjoint from the noisy inputs'

@@ -583,6 +583,26 @@ def get_feature_map_from_string(input_tensor: torch.Tensor, feature_map: str) ->
     return get_feature_map(input_tensor, _FEATURE_BY_NAME[feature_map])
 
 
+def read_denoiser_features(albedo: Optional[torch.Tensor] = None, normal: Optional[torch.Tensor] = None,
+                           depth: Optional[torch.Tensor] = None, transmittance: Optional[torch.Tensor] = None) -> None:
+    """Writes the feature planes a learned denoiser reads (albedo and normal: 3 x H x W; depth mean and
+    transmittance: H x W; leading dimensions of size 1 allowed) into contiguous float32 CUDA tensors of
+    the current image size, in one launch on the current stream; None skips a plane."""
+    if getattr(S, "last_hw", None) is None:
+        raise RuntimeError("Error in readDenoiserFeatures: nothing rendered.")
+    h, w = S.last_hw
+    ptrs = []
+    for t, planes in ((albedo, 3), (normal, 3), (depth, 1), (transmittance, 1)):
+        if t is None:
+            ptrs.append(None)
+            continue
+        if not t.is_cuda or t.dtype != torch.float32 or not t.is_contiguous() or t.numel() != planes * h * w:
+            raise RuntimeError("Error in readDenoiserFeatures: expected a contiguous float32 CUDA tensor of "
+                               f"{planes} x {h} x {w} values.")
+        ptrs.append(ctypes.c_void_p(t.data_ptr()))
+    _c("vpt_get_denoiser_features", *ptrs, ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+
+
 # ---- rendering (Module.cpp:286-317) ----
 def _validate(input_tensor: torch.Tensor):
     if input_tensor.dim() != 3:
@@ -621,6 +641,7 @@ def render_frame(input_tensor: torch.Tensor, frame_count: int) -> torch.Tensor:
         den = _ensure_torch_denoiser()
         _apply_feature_maps()
     _c("vpt_set_resolution", int(w), int(h))
+    S.last_hw = (int(h), int(w))
     _c("vpt_render_frames", int(frame_count), _stream_of(input_tensor))
     if not S.torch_denoiser_active:
         return _read(input_tensor, c, "vpt_read_result")

@@ -177,6 +177,12 @@ VptStatus vpt_read_statistics(VptContext* ctx, double* out_sum, double* out_sum_
 VptStatus vpt_set_use_feature_maps(VptContext* ctx, const int* features, int count);
 VptStatus vpt_get_feature_map(VptContext* ctx, int feature, float* out, int channels, int out_on_device,
                               void* stream);
+/* The feature planes a learned denoiser reads, in one launch on `stream`, into device buffers of the
+ * current image size (any may be NULL): albedo [3][H][W] (medium albedo x hit fraction), normal
+ * [3][H][W], depth mean [H][W], transmittance [H][W]; the first channels of vpt_get_feature_map's
+ * Albedo / Normal / Depth / Transmittance maps. */
+VptStatus vpt_get_denoiser_features(VptContext* ctx, float* albedo, float* normal, float* depth, float* transmittance,
+                                    void* stream);
 VptStatus vpt_get_stats(VptContext* ctx, VptStats* stats);
 VptStatus vpt_reset_stats(VptContext* ctx);
 /* Waits for the context's work on `stream`, then reports sticky device errors. */

@@ -113,3 +113,25 @@ def test_denoise_graph_equals_eager_denoise():
         got = graph(*args).clone()
         ref = net.denoise(*args)
         assert torch.allclose(got, ref, rtol=1e-6, atol=1e-6)
+
+
+def test_fused_feature_read_and_graph_from_renderer():
+    """vpt.read_denoiser_features writes the same planes as the per-map reads (identical arithmetic),
+    and DenoiseGraph.from_renderer gives the eager denoise of those planes."""
+    ld.setup_scene(vpt, ld.sample_scene(4242), grid=64, max_bounces=16)
+    vpt.set_use_feature_maps(["Albedo", "Normal", "Depth", "Transmittance"])
+    img = torch.zeros((3, 48, 64), device="cuda")
+    vpt.set_frame_index(0)
+    out = vpt.render_frame(img, 3)
+    f = ld.read_features(vpt, img)
+    for key, name, planes in (("albedo", "Albedo", 3), ("normal", "Normal", 3), ("depth", "Depth", 1),
+                              ("transmittance", "Transmittance", 1)):
+        assert torch.equal(f[key], vpt.get_feature_map_from_string(img, name)[:planes]), key
+    net = ld.KpnUNet(seed=6)
+    graph = net.graph(1, 48, 64)
+    noise = torch.tensor([0.5], device="cuda")
+    got = graph.from_renderer(vpt, out, noise).clone()
+    ref = net.denoise(out[None], f["albedo"][None], f["normal"][None], f["depth"][None], f["transmittance"][None],
+                      noise)
+    assert torch.allclose(got, ref, rtol=1e-6, atol=1e-6)
+    vpt.set_use_feature_maps([])
