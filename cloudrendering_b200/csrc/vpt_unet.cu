@@ -720,13 +720,15 @@ __global__ void __launch_bounds__(kThreads) conv_strip_kernel(const StripArgs a)
 //              swizzled K-major layout of that line width (pixel rows of 128 / 64 / 32 bytes), rows and
 //              pixels outside the image arriving as zeros; full[s] completes on the bytes, empty[s] is
 //              signalled by the tensor core once the last MMA reading the slot has completed;
-//   warp 1     one lane issues the 9 x cin/16 MMAs of each output row into one of two TMEM
-//              accumulators (acc_full[b] on completion, after acc_empty[b]);
+//   warps 1, 6 one lane each issues the 9 x cin/16 MMAs of every other output row (accumulator
+//              index g: warp 1 the even, warp 6 the odd) into TMEM accumulator g % 2 (acc_full[b] on
+//              completion, after acc_empty[b]): one issuing thread is the bound for small N (about 93
+//              cycles per MMA against the tensor core's 48), two overlap their issue;
 //   warps 2-5  the epilogue; warp w reads TMEM lane quarter w % 4 (pixels x0 + 32 (w % 4) .. + 31).
 // All roles walk the same segment sequence, so ring and accumulator positions agree without
 // communication.  Every wait is bounded: on expiry the role records the error and stops, and the
 // CTA waits (bounded) for its copies and MMAs in flight before TMEM is released.
-constexpr int kWsThreads = 192;
+constexpr int kWsThreads = 224;  // 7 warps: producer, MMA issuer, 4 epilogue warps, second MMA issuer
 constexpr int kWsMaxRing = 8;
 
 __device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t bar, uint32_t bytes) {
@@ -802,12 +804,12 @@ __device__ __forceinline__ uint32_t a_hi_of(int channels) {
     return (uint32_t)(smem_desc_sw(0, (uint32_t)channels * 2u) >> 32);
 }
 
-__global__ void __launch_bounds__(kWsThreads, 1) conv_ws_kernel(const __grid_constant__ CUtensorMap map64,
+__global__ void __launch_bounds__(kWsThreads, 2) conv_ws_kernel(const __grid_constant__ CUtensorMap map64,
                                                              const __grid_constant__ CUtensorMap map32,
                                                              const __grid_constant__ CUtensorMap map16,
                                                              const __grid_constant__ WsArgs wa, int ring) {
     extern __shared__ __align__(1024) uint8_t smem[];
-    __shared__ uint64_t full[kWsMaxRing], empty[kWsMaxRing], acc_full[2], acc_empty[2], done_bar;
+    __shared__ uint64_t full[kWsMaxRing], empty[kWsMaxRing], acc_full[2], acc_empty[2], done_bar[2];
     __shared__ uint32_t tmem_slot;
     __shared__ int fail_any;
     const StripArgs& a = wa.s;
@@ -821,13 +823,13 @@ __global__ void __launch_bounds__(kWsThreads, 1) conv_ws_kernel(const __grid_con
     if (tid == 0) {
         for (int s = 0; s < ring; ++s) {
             mbar_init(smem_u32(&full[s]), 1);
-            mbar_init(smem_u32(&empty[s]), 1);
+            mbar_init(smem_u32(&empty[s]), 2);  // one release per MMA-issuing warp
         }
         for (int b = 0; b < 2; ++b) {
             mbar_init(smem_u32(&acc_full[b]), 1);
             mbar_init(smem_u32(&acc_empty[b]), 4);  // one arrival per epilogue warp
+            mbar_init(smem_u32(&done_bar[b]), 1);
         }
-        mbar_init(smem_u32(&done_bar), 1);
         fail_any = 0;
         fence_mbar_init();
     }
@@ -887,8 +889,9 @@ __global__ void __launch_bounds__(kWsThreads, 1) conv_ws_kernel(const __grid_con
                 if (!mbar_wait(smem_u32(&full[s]), ph)) fail = true;
             }
         }
-    } else if (warp == 1) {
+    } else if (warp == 1 || warp == 6) {
         if (lane == 0) {
+            const int mw = warp == 1 ? 0 : 1;  // this warp's accumulator parity
             const uint32_t idesc = instr_desc(kBM, a.cout, 0, 0);
             // descriptor words: A (swizzled, start field added per row / group / dx / step; LBO 1),
             // B (no swizzle, LBO = one 8-channel plane of the weights, SBO 128)
@@ -912,15 +915,23 @@ __global__ void __launch_bounds__(kWsThreads, 1) conv_ws_kernel(const __grid_con
             }
             int slot = 0;        // ring position of the segment's first row
             uint32_t phase = 0;
-            long g = 0;          // accumulators used
+            long g = 0;          // accumulators used (both warps count every output row)
+            // Ring slots are released by both issuing warps (empty[] counts 2): after output row i
+            // its warp releases input rows i and i+1 (its last uses of them: it also computed row
+            // i-2, the other warp rows i-1 and i+1).  Rows without such a row get the arrival at the
+            // segment's start (input row 0 from the warp of row -1) or end (rows `rows`, `rows`+1).
+            auto own = [&](long gi) { return (int)(gi & 1) == mw; };
+            auto slot_of = [&](int r) { return (uint32_t)((slot + r) % ring); };
             for (int seg = blockIdx.x; seg < total_segs && !fail; seg += gridDim.x) {
                 const WsSegment sgm = ws_segment(a, seg);
                 if (sgm.y0 >= sgm.y1) continue;
                 const int rows = sgm.y1 - sgm.y0;
+                const long g0 = g;
+                if (own(g0 - 1)) mbar_arrive(smem_u32(&empty[slot_of(0)]));
                 for (int i = 0; i < rows && !fail; ++i, ++g) {
-                    // input rows i, i+1, i+2 of the segment (y-1, y, y+1): wait for the newest (all
-                    // three for the first output row)
-                    for (int k = (i == 0 ? 0 : 2); k <= 2; ++k) {
+                    if (!own(g)) continue;
+                    // input rows i, i+1, i+2 of the segment (y-1, y, y+1)
+                    for (int k = 0; k <= 2; ++k) {
                         const int pos = slot + i + k;
                         const uint32_t ph = phase ^ (uint32_t)((pos / ring) & 1);
                         if (!mbar_wait(smem_u32(&full[pos % ring]), ph)) fail = true;
@@ -936,7 +947,7 @@ __global__ void __launch_bounds__(kWsThreads, 1) conv_ws_kernel(const __grid_con
                     uint32_t acc = 0;
 #pragma unroll 1
                     for (int dy = 0; dy < 3; ++dy) {
-                        const uint32_t row16 = (sring + (uint32_t)((slot + i + dy) % ring) * row_bytes) >> 4;
+                        const uint32_t row16 = (sring + slot_of(i + dy) * row_bytes) >> 4;
 #pragma unroll
                         for (int k = 0; k < kWsMaxGroups; ++k) {
                             if (k >= ngroups) break;
@@ -956,20 +967,24 @@ __global__ void __launch_bounds__(kWsThreads, 1) conv_ws_kernel(const __grid_con
                         }
                     }
                     mma_commit(smem_u32(&acc_full[b]));
-                    mma_commit(smem_u32(&empty[(slot + i) % ring]));  // input row y-1 is done
+                    mma_commit(smem_u32(&empty[slot_of(i)]));
+                    mma_commit(smem_u32(&empty[slot_of(i + 1)]));
                 }
                 if (fail) break;
-                mma_commit(smem_u32(&empty[(slot + rows) % ring]));
-                mma_commit(smem_u32(&empty[(slot + rows + 1) % ring]));
+                if (own(g0 + rows - 1)) mma_commit(smem_u32(&empty[slot_of(rows + 1)]));
+                if (own(g0 + rows)) {
+                    mma_commit(smem_u32(&empty[slot_of(rows)]));
+                    mma_commit(smem_u32(&empty[slot_of(rows + 1)]));
+                }
                 const int adv = slot + rows + 2;
                 slot = adv % ring;
                 phase ^= (uint32_t)((adv / ring) & 1);
             }
-            // every MMA this CTA issued has completed before TMEM is released
-            mma_commit(smem_u32(&done_bar));
-            if (!mbar_wait(smem_u32(&done_bar), 0)) fail = true;
+            // every MMA this warp issued has completed before TMEM is released
+            mma_commit(smem_u32(&done_bar[mw]));
+            if (!mbar_wait(smem_u32(&done_bar[mw]), 0)) fail = true;
         }
-    } else {
+    } else if (warp >= 2 && warp <= 5) {
         const int quarter = warp & 3;
         long g = 0;
         for (int seg = blockIdx.x; seg < total_segs && !fail; seg += gridDim.x) {
@@ -2000,7 +2015,7 @@ bool ws_config(int cin, int cout, int& per_sm, int& ring) {
     ring = 0;
     if (rb == 0) return false;
     int best = -1;
-    for (int occ = 1; occ <= 3 && occ * 2 * acc <= 512; ++occ) {  // 3: the registers of 3 CTAs fit an SM
+    for (int occ = 1; occ <= 2 && occ * 2 * acc <= 512; ++occ) {  // 2: the registers of 2 CTAs fit an SM
         const size_t budget = kSmPerSm / occ - kWsStatic;
         const size_t wb = ws_weight_bytes(cin, cout);
         if (budget > kSmPerCta || wb >= budget) continue;
