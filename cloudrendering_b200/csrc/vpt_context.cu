@@ -203,6 +203,7 @@ struct VptContext {
     DevBuf<double> film, film_sq;
     bool collect_stats = false;
     bool features_on = false;
+    bool feat_background = false;  // the Background map was requested (one more accumulator per sample)
     DevBuf<float> feat;
     DevBuf<float> rgba_src, rgba_a, rgba_b;  // denoiser input and ping-pong buffers
     DevBuf<float> eaw_maps;                  // position + normal RGBA for EAW
@@ -543,6 +544,7 @@ VptStatus fill_params(VptContext* ctx, int tracker, int frames, vpt::TraceParams
     P.film = ctx->film.ptr;
     P.film_sq = ctx->collect_stats ? ctx->film_sq.ptr : nullptr;
     P.feat = features_needed(ctx) ? ctx->feat.ptr : nullptr;
+    P.feat_background = ctx->feat_background ? 1 : 0;
     P.counters = ctx->counters.ptr;
     P.error_flags = ctx->error_flags.ptr;
     P.work_counter = ctx->work_counter.ptr;
@@ -1376,11 +1378,14 @@ VptStatus vpt_read_statistics(VptContext* ctx, double* out_sum, double* out_sum_
 
 VptStatus vpt_set_use_feature_maps(VptContext* ctx, const int* features, int count) {
     VPT_CHECK_CTX(ctx);
-    bool on = false;
-    for (int i = 0; i < count; i++)
+    bool on = false, background = false;
+    for (int i = 0; i < count; i++) {
         if (features && features[i] != VPT_FEATURE_RESULT) on = true;
-    if (on != ctx->features_on) reset_film_state(ctx);
+        if (features && features[i] == VPT_FEATURE_BACKGROUND) background = true;
+    }
+    if (on != ctx->features_on || background != ctx->feat_background) reset_film_state(ctx);
     ctx->features_on = on;
+    ctx->feat_background = background;
     return VPT_OK;
 }
 
@@ -1390,6 +1395,8 @@ VptStatus vpt_get_feature_map(VptContext* ctx, int feature, float* out, int chan
     if (!features_needed(ctx) || !ctx->feat.ptr || ctx->film_frames == 0)
         return fail(ctx, VPT_ERR_STATE, "feature maps are not enabled or nothing rendered");
     if (!out || channels < 1 || channels > 4) return fail(ctx, VPT_ERR_ARG, "bad output");
+    if (feature == VPT_FEATURE_BACKGROUND && !ctx->feat_background)
+        return fail(ctx, VPT_ERR_STATE, "the Background map was not requested in set_use_feature_maps");
     cudaStream_t s = as_stream(stream);
     int n = ctx->width * ctx->height;
     float* dst = out;
@@ -1397,7 +1404,8 @@ VptStatus vpt_get_feature_map(VptContext* ctx, int feature, float* out, int chan
         VPT_CHECK_CUDA(ctx, ctx->staging.alloc((size_t)n * 4));
         dst = ctx->staging.ptr;
     }
-    cudaError_t e = vpt::feature_to_chw(ctx->feat.ptr, n, feature_frames(ctx), feature, channels, ctx->albedo, dst, s);
+    cudaError_t e = vpt::feature_to_chw(ctx->feat.ptr, n, feature_frames(ctx), feature, channels, ctx->albedo,
+                                        ctx->far_dist, dst, s);
     if (e == cudaErrorInvalidValue) return fail(ctx, VPT_ERR_ARG, "feature map not supported");
     VPT_CHECK_CUDA(ctx, e);
     if (!out_on_device) {

@@ -516,7 +516,8 @@ cudaError_t svgf_filter_passes(SvgfCur c, float4* color_history, float4* moments
 
 // ---------------------------------------------------------------------------------------------
 __global__ void feature_to_chw_kernel(const float* __restrict__ feat, int n, float inv_frames, int feature,
-                                      int channels, float a0, float a1, float a2, float* __restrict__ out) {
+                                      int channels, float a0, float a1, float a2, float far_distance,
+                                      float* __restrict__ out) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float* f = feat + (size_t)i * kFeatStride;
@@ -533,6 +534,28 @@ __global__ void feature_to_chw_kernel(const float* __restrict__ feat, int n, flo
             v[0] = f[kFeatNormal] * inv_frames;
             v[1] = f[kFeatNormal + 1] * inv_frames;
             v[2] = f[kFeatNormal + 2] * inv_frames;
+            v[3] = 1.0f;
+            break;
+        case VPT_FEATURE_NORMAL_LEN_1: {  // NormalizeNormals.glsl: rgb / length when length > 1e-5
+            v[0] = f[kFeatNormal] * inv_frames;
+            v[1] = f[kFeatNormal + 1] * inv_frames;
+            v[2] = f[kFeatNormal + 2] * inv_frames;
+            const float len = sqrtf(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+            if (len > 1e-5f) {
+                v[0] /= len;
+                v[1] /= len;
+                v[2] /= len;
+            }
+            v[3] = 1.0f;
+            break;
+        }
+        case VPT_FEATURE_DEPTH_FAR:  // Clouds.glsl:219-227: mean of (event ? depth : far distance)
+            v[0] = f[kFeatDepth] * inv_frames + (1.0f - hit) * far_distance;
+            break;
+        case VPT_FEATURE_BACKGROUND:  // Clouds.glsl:162-170 (alpha 1 for every sample)
+            v[0] = f[kFeatBackground] * inv_frames;
+            v[1] = f[kFeatBackground + 1] * inv_frames;
+            v[2] = f[kFeatBackground + 2] * inv_frames;
             v[3] = 1.0f;
             break;
         case VPT_FEATURE_DEPTH: {
@@ -567,10 +590,13 @@ __global__ void feature_to_chw_kernel(const float* __restrict__ feat, int n, flo
 }
 
 cudaError_t feature_to_chw(const float* feat, int n, uint32_t frames, int feature, int channels, const float* albedo,
-                           float* out, cudaStream_t stream) {
+                           float far_distance, float* out, cudaStream_t stream) {
     switch (feature) {
         case VPT_FEATURE_FIRST_X:
         case VPT_FEATURE_NORMAL:
+        case VPT_FEATURE_NORMAL_LEN_1:
+        case VPT_FEATURE_DEPTH_FAR:
+        case VPT_FEATURE_BACKGROUND:
         case VPT_FEATURE_DEPTH:
         case VPT_FEATURE_DENSITY:
         case VPT_FEATURE_CLOUD_ONLY:
@@ -581,7 +607,7 @@ cudaError_t feature_to_chw(const float* feat, int n, uint32_t frames, int featur
             return cudaErrorInvalidValue;
     }
     feature_to_chw_kernel<<<(n + 255) / 256, 256, 0, stream>>>(feat, n, 1.0f / float(frames), feature, channels,
-                                                               albedo[0], albedo[1], albedo[2], out);
+                                                               albedo[0], albedo[1], albedo[2], far_distance, out);
     count_launches(1);
     return cudaGetLastError();
 }

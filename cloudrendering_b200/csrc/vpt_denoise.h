@@ -64,6 +64,6 @@ cudaError_t svgf_denoise_features(const float* color_rgba, const float* feat, ui
 cudaError_t denoiser_features(const float* feat, int n, uint32_t frames, const float* albedo_rgb, float* albedo,
                               float* normal, float* depth, float* trans, cudaStream_t stream);
 cudaError_t feature_to_chw(const float* feat, int n, uint32_t frames, int feature, int channels, const float* albedo,
-                           float* out, cudaStream_t stream);
+                           float far_distance, float* out, cudaStream_t stream);
 
 }  // namespace vpt

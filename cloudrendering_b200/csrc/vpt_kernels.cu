@@ -37,12 +37,20 @@ struct Sampler {
     }
 };
 
-// Per-path feature accumulation (Clouds.glsl:195-256): position of the first event, depth,
-// density, albedo-weighted hit flag, primary-ray transmittance proxy.
+// Per-path feature accumulation (Clouds.glsl:148-256): position of the first event, depth,
+// density, albedo-weighted hit flag, primary-ray transmittance proxy and, when requested, the
+// background (Clouds.glsl:162-170: sampleSkybox of the camera ray for paths with an event, the
+// path's radiance otherwise).
 template <class S>
 VPT_DEV void accumulate_features(const TraceParams& P, S& sample, Rng& rng, size_t pix, const FirstEvent& fe,
-                                 F3 result) {
+                                 F3 result, F3 w_camera) {
     float* f = P.feat + pix * kFeatStride;
+    if (P.feat_background) {
+        const F3 bg = fe.has ? sky_only(P, w_camera) : result;
+        atomicAdd(f + kFeatBackground + 0, bg.x);
+        atomicAdd(f + kFeatBackground + 1, bg.y);
+        atomicAdd(f + kFeatBackground + 2, bg.z);
+    }
     if (fe.has) {
         F3 n = sample.normal(fe.x, rng);
         atomicAdd(f + kFeatNormal + 0, n.x);
@@ -125,7 +133,7 @@ VPT_DEV void trace_one(const TraceParams& P, S& sample, uint32_t frame, int px, 
         atomicAdd(P.film_sq + pix * 3 + 1, (double)L.y * (double)L.y);
         atomicAdd(P.film_sq + pix * 3 + 2, (double)L.z * (double)L.z);
     }
-    if (features) accumulate_features(P, sample, rng, pix, fe, L);
+    if (features) accumulate_features(P, sample, rng, pix, fe, L, w);
     lookups += pc.lookups;
     guard_hit |= pc.guard_hit;
 }

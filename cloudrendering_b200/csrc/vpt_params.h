@@ -157,7 +157,8 @@ struct TraceParams {
     const uint64_t* env_level_offset; // float offset of each level in env_pyramid (indexed by level)
     double* film;                  // 3 doubles per pixel: sum of radiance
     double* film_sq;               // 3 doubles per pixel: sum of squared radiance (optional)
-    float* feat;                   // feature accumulators (optional), 16 floats per pixel
+    float* feat;                   // feature accumulators (optional), kFeatStride floats per pixel
+    int feat_background;           // accumulate the background map (requested by the user)
     unsigned long long* counters;  // [0] paths, [1] density lookups
     int* error_flags;
     unsigned int* work_counter;    // persistent-kernel path queue
@@ -176,8 +177,9 @@ enum FeatureSlot : int {
     kFeatDensity = 9,    // density*0.001, squared
     kFeatCloudOnly = 11, // rgb of paths with an event
     kFeatTrans = 14,     // primary-ray transmittance
-    kFeatBackground = 15,// luminance proxy (unused slot kept for alignment)
-    kFeatStride = 16,
+                         // 15: unused (keeps the background float4-aligned)
+    kFeatBackground = 16,// rgb: skybox of the camera ray for paths with an event, else their radiance
+    kFeatStride = 20,
 };
 
 }  // namespace vpt

@@ -39,8 +39,9 @@ _BY_LOWER = {n.lower(): n for n, _ in DENOISER_FEATURE_MAPS}
 # denoiser feature map -> (renderer feature map name of vpt.VPT_FEATURE_MAP_NAMES, channels taken);
 # "Color" is the accumulated result
 RENDERER_FEATURES = {
-    "Albedo": ("Albedo", 4), "Position": ("First X", 3), "Normal": ("Normal", 3), "Normal (Length 1)": ("Normal", 3),
-    "CloudOnly": ("Cloud Only", 4), "Depth": ("Depth", 2), "Density": ("Density", 2),
+    "Albedo": ("Albedo", 4), "Position": ("First X", 3), "Normal": ("Normal", 3),
+    "Normal (Length 1)": ("Normal (Length 1)", 3), "CloudOnly": ("Cloud Only", 4), "Depth": ("Depth", 2),
+    "Depth Far": ("Depth Far", 1), "Density": ("Density", 2), "Background": ("Background", 4),
 }
 # maps the renderer provides without a feature pass (static camera: no motion between frames)
 SYNTHESISED = {"Flow", "Flow Reverse", "Reproj_UV", "Unused"}
@@ -147,8 +148,6 @@ class PyTorchDenoiser:
                 t = color[:4]
             elif name in RENDERER_FEATURES:
                 t = feature(RENDERER_FEATURES[name][0])[:c]
-                if name == "Normal (Length 1)":
-                    t = t / t.norm(dim=0, keepdim=True).clamp_min(1e-20)
             elif name == "Reproj_UV":  # static camera: each pixel maps to itself
                 ys = (torch.arange(h, device=color.device, dtype=torch.float32) + 0.5) / h
                 xs = (torch.arange(w, device=color.device, dtype=torch.float32) + 0.5) / w

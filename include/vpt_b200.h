@@ -67,8 +67,10 @@ enum {
     VPT_FEATURE_RESULT = 0,
     VPT_FEATURE_FIRST_X = 1,
     VPT_FEATURE_NORMAL = 3,
+    VPT_FEATURE_NORMAL_LEN_1 = 4,  /* Normal with rgb scaled to length 1 (NormalizeNormals.glsl) */
     VPT_FEATURE_CLOUD_ONLY = 5,
     VPT_FEATURE_DEPTH = 6,
+    VPT_FEATURE_DEPTH_FAR = 7,     /* mean of (event ? depth : far distance) */
     VPT_FEATURE_DENSITY = 12,
     VPT_FEATURE_BACKGROUND = 13,
     VPT_FEATURE_ALBEDO = 17,

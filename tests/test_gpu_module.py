@@ -94,3 +94,42 @@ def test_feature_maps_and_eaw():
     s = vpt.render_frame(t, 1)
     assert torch.isfinite(s).all()
     vpt.set_denoiser("None")
+
+
+def test_normal_len1_depth_far_and_background_maps():
+    """Normal (Length 1): the Normal map's rgb scaled to length 1 where longer than 1e-5, alpha 1
+    (NormalizeNormals.glsl); Depth Far: mean of (event ? depth : far distance) (Clouds.glsl:219-227);
+    Background: mean of (event ? skybox of the camera ray : the path's radiance) (Clouds.glsl:162-170),
+    which under a single-colour sky is that colour at every pixel (the radiance of a path without
+    an event is the sky it escapes to)."""
+    vpt.set_vpt_mode_from_name("Delta Tracking")
+    vpt.set_use_builtin_environment_map("Single Color")
+    vpt.set_sun([0.3, 0.8, 0.5], [0.7, 0.5, 0.25])
+    t = torch.zeros((3, 48, 64), dtype=torch.float32, device="cuda")
+    vpt.set_use_feature_maps(["Normal", "First X", "Depth"])
+    vpt.render_frame(t, 2)
+    with pytest.raises(RuntimeError, match="Background"):
+        vpt.get_feature_map_from_string(t, "Background")
+    vpt.set_use_feature_maps(["Normal", "Normal (Length 1)", "First X", "Depth", "Depth Far", "Background"])
+    img = vpt.render_frame(t, 6)
+    normal = vpt.get_feature_map_from_string(t, "Normal")
+    n1 = vpt.get_feature_map_from_string(t, "Normal (Length 1)")
+    assert n1.shape == (4, 48, 64) and torch.all(n1[3] == 1.0)
+    length = normal[:3].norm(dim=0)
+    long_ = length > 1e-5
+    assert torch.allclose(n1[:3][:, long_], (normal[:3] / length)[:, long_], rtol=1e-5, atol=1e-6)
+    assert torch.equal(n1[:3][:, ~long_], normal[:3][:, ~long_])
+    hit = vpt.get_feature_map_from_string(t, "First X")[3]
+    depth = vpt.get_feature_map_from_string(t, "Depth")[0]
+    far = vpt.get_feature_map_from_string(t, "Depth Far")
+    assert far.shape == (1, 48, 64)
+    assert torch.allclose(far[0], depth + (1.0 - hit) * 80.0, rtol=1e-6, atol=1e-5)
+    assert 0.0 < float(hit.mean()) < 1.0  # events and misses both present
+    bg = vpt.get_feature_map_from_string(t, "Background")
+    assert bg.shape == (4, 48, 64) and torch.all(bg[3] == 1.0)
+    miss = hit == 0.0
+    colour = img[:, miss].mean(dim=1)  # pixels without events render the sky colour itself
+    assert torch.allclose(img[:, miss], colour[:, None], rtol=1e-6)
+    assert torch.allclose(bg[:3], colour[:, None, None].expand(3, 48, 64), rtol=1e-5)
+    vpt.set_use_feature_maps([])
+    vpt.set_use_builtin_environment_map("Default")

@@ -65,7 +65,7 @@ def test_model_info_keys_and_defaults(tmp_path):
     ({"input_feature_maps": "Color"}, "'input_feature_maps' is not an array"),
     ({"input_feature_maps": [1]}, "is not a string"),
     ({"input_feature_maps": ["Colour"]}, "Invalid feature map name 'colour'"),
-    ({"input_feature_maps": ["Color", "Background"]}, "'Background' used by"),
+    ({"input_feature_maps": ["Color", "Depth Blended"]}, "'Depth Blended' used by"),
 ])
 def test_model_info_errors(tmp_path, info, message):
     p = str(tmp_path / "m.pt")
@@ -95,8 +95,8 @@ def test_pack_input_order_and_channels(tmp_path):
     d.load_model_from_file(p)
     h, w = 4, 6
     color = torch.arange(4 * h * w, dtype=torch.float32).reshape(4, h, w)
-    feats = {"Normal": torch.full((4, h, w), 2.0), "Depth": torch.full((2, h, w), 7.0),
-             "First X": torch.full((4, h, w), -1.0)}
+    feats = {"Normal (Length 1)": torch.full((4, h, w), 3 ** -0.5), "Depth": torch.full((2, h, w), 7.0),
+             "First X": torch.full((4, h, w), -1.0)}  # the renderer's maps (Normal (Length 1) normalised there)
     x = d.pack_input(color, lambda n: feats[n])
     assert x.shape == (1, 16, h, w)
     assert torch.equal(x[0, :4], color)
