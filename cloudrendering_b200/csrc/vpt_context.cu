@@ -204,6 +204,7 @@ struct VptContext {
     bool collect_stats = false;
     bool features_on = false;
     bool feat_background = false;  // the Background map was requested (one more accumulator per sample)
+    int feat_depth_maps = 0;       // bit 0: Depth Blended, bit 1: Depth Nearest Opaque requested (ray marches)
     DevBuf<float> feat;
     DevBuf<float> rgba_src, rgba_a, rgba_b;  // denoiser input and ping-pong buffers
     DevBuf<float> eaw_maps;                  // position + normal RGBA for EAW
@@ -545,6 +546,7 @@ VptStatus fill_params(VptContext* ctx, int tracker, int frames, vpt::TraceParams
     P.film_sq = ctx->collect_stats ? ctx->film_sq.ptr : nullptr;
     P.feat = features_needed(ctx) ? ctx->feat.ptr : nullptr;
     P.feat_background = ctx->feat_background ? 1 : 0;
+    P.feat_depth_maps = ctx->feat_depth_maps;
     P.counters = ctx->counters.ptr;
     P.error_flags = ctx->error_flags.ptr;
     P.work_counter = ctx->work_counter.ptr;
@@ -1379,13 +1381,18 @@ VptStatus vpt_read_statistics(VptContext* ctx, double* out_sum, double* out_sum_
 VptStatus vpt_set_use_feature_maps(VptContext* ctx, const int* features, int count) {
     VPT_CHECK_CTX(ctx);
     bool on = false, background = false;
+    int depth_maps = 0;
     for (int i = 0; i < count; i++) {
         if (features && features[i] != VPT_FEATURE_RESULT) on = true;
         if (features && features[i] == VPT_FEATURE_BACKGROUND) background = true;
+        if (features && features[i] == VPT_FEATURE_DEPTH_BLENDED) depth_maps |= 1;
+        if (features && features[i] == VPT_FEATURE_DEPTH_NEAREST_OPAQUE) depth_maps |= 2;
     }
-    if (on != ctx->features_on || background != ctx->feat_background) reset_film_state(ctx);
+    if (on != ctx->features_on || background != ctx->feat_background || depth_maps != ctx->feat_depth_maps)
+        reset_film_state(ctx);
     ctx->features_on = on;
     ctx->feat_background = background;
+    ctx->feat_depth_maps = depth_maps;
     return VPT_OK;
 }
 
@@ -1397,6 +1404,9 @@ VptStatus vpt_get_feature_map(VptContext* ctx, int feature, float* out, int chan
     if (!out || channels < 1 || channels > 4) return fail(ctx, VPT_ERR_ARG, "bad output");
     if (feature == VPT_FEATURE_BACKGROUND && !ctx->feat_background)
         return fail(ctx, VPT_ERR_STATE, "the Background map was not requested in set_use_feature_maps");
+    if ((feature == VPT_FEATURE_DEPTH_BLENDED && !(ctx->feat_depth_maps & 1)) ||
+        (feature == VPT_FEATURE_DEPTH_NEAREST_OPAQUE && !(ctx->feat_depth_maps & 2)))
+        return fail(ctx, VPT_ERR_STATE, "the depth map was not requested in set_use_feature_maps");
     cudaStream_t s = as_stream(stream);
     int n = ctx->width * ctx->height;
     float* dst = out;

@@ -552,6 +552,16 @@ __global__ void feature_to_chw_kernel(const float* __restrict__ feat, int n, flo
         case VPT_FEATURE_DEPTH_FAR:  // Clouds.glsl:219-227: mean of (event ? depth : far distance)
             v[0] = f[kFeatDepth] * inv_frames + (1.0f - hit) * far_distance;
             break;
+        case VPT_FEATURE_DEPTH_BLENDED:  // Clouds.glsl:367-374: (depth, alpha, 0, 1)
+            v[0] = f[kFeatDepthBlended] * inv_frames;
+            v[1] = f[kFeatDepthBlended + 1] * inv_frames;
+            v[3] = 1.0f;
+            break;
+        case VPT_FEATURE_DEPTH_NEAREST_OPAQUE:  // Clouds.glsl:376-383
+            v[0] = f[kFeatDepthNearest] * inv_frames;
+            v[1] = f[kFeatDepthNearest + 1] * inv_frames;
+            v[3] = 1.0f;
+            break;
         case VPT_FEATURE_BACKGROUND:  // Clouds.glsl:162-170 (alpha 1 for every sample)
             v[0] = f[kFeatBackground] * inv_frames;
             v[1] = f[kFeatBackground + 1] * inv_frames;
@@ -597,6 +607,8 @@ cudaError_t feature_to_chw(const float* feat, int n, uint32_t frames, int featur
         case VPT_FEATURE_NORMAL_LEN_1:
         case VPT_FEATURE_DEPTH_FAR:
         case VPT_FEATURE_BACKGROUND:
+        case VPT_FEATURE_DEPTH_BLENDED:
+        case VPT_FEATURE_DEPTH_NEAREST_OPAQUE:
         case VPT_FEATURE_DEPTH:
         case VPT_FEATURE_DENSITY:
         case VPT_FEATURE_CLOUD_ONLY:

@@ -37,13 +37,40 @@ struct Sampler {
     }
 };
 
+// Depth Blended (DepthBlended.glsl) / Depth Nearest Opaque (DepthNearestOpaque.glsl): a march along
+// the camera ray in steps of 0.25 / the largest grid dimension (0.001 for NanoVDB grids) with
+// alpha = 1 - exp(-density * extinction * step), stopping past the box or above 0.999 accumulated
+// alpha A.  Blended: (sum of (1 - A) alpha t / max(A, 1e-5), A); nearest: (t of the last step with
+// alpha > 1e-5, times A; A).  Lookups continue the path's random stream (stochastic interpolation).
+template <bool NEAREST, class S>
+VPT_DEV void depth_march(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, float& depth_out, float& alpha_out) {
+    const float step = S::kSparse ? 0.001f : 0.25f / (float)max(P.nx, max(P.ny, P.nz));
+    const float atten = P.extinction * step;
+    float acc_depth = 0.0f, acc_alpha = 0.0f, nearest = 0.0f;
+    float tmin, tmax;
+    if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
+        float t = tmin;
+        while (true) {
+            t += step;
+            if (t > tmax || acc_alpha > 0.999f) break;
+            const float density = sample(x + w * t, rng);
+            const float alpha = 1.0f - expf(-density * atten);
+            if (!NEAREST) acc_depth = acc_depth + (1.0f - acc_alpha) * alpha * t;
+            acc_alpha = acc_alpha + (1.0f - acc_alpha) * alpha;
+            if (NEAREST && alpha > 1e-5f) nearest = t;
+        }
+    }
+    depth_out = NEAREST ? nearest * acc_alpha : acc_depth / fmaxf(acc_alpha, 1e-5f);
+    alpha_out = acc_alpha;
+}
+
 // Per-path feature accumulation (Clouds.glsl:148-256): position of the first event, depth,
 // density, albedo-weighted hit flag, primary-ray transmittance proxy and, when requested, the
 // background (Clouds.glsl:162-170: sampleSkybox of the camera ray for paths with an event, the
 // path's radiance otherwise).
 template <class S>
 VPT_DEV void accumulate_features(const TraceParams& P, S& sample, Rng& rng, size_t pix, const FirstEvent& fe,
-                                 F3 result, F3 w_camera) {
+                                 F3 result, F3 x_camera, F3 w_camera) {
     float* f = P.feat + pix * kFeatStride;
     if (P.feat_background) {
         const F3 bg = fe.has ? sky_only(P, w_camera) : result;
@@ -69,6 +96,19 @@ VPT_DEV void accumulate_features(const TraceParams& P, S& sample, Rng& rng, size
         atomicAdd(f + kFeatCloudOnly + 2, result.z);
     } else {
         atomicAdd(f + kFeatTrans, 1.0f);
+    }
+    // after the normal, in the reference's order (Clouds.glsl:367-383)
+    if (P.feat_depth_maps & 1) {
+        float d, a;
+        depth_march<false>(P, sample, rng, x_camera, w_camera, d, a);
+        atomicAdd(f + kFeatDepthBlended + 0, d);
+        atomicAdd(f + kFeatDepthBlended + 1, a);
+    }
+    if (P.feat_depth_maps & 2) {
+        float d, a;
+        depth_march<true>(P, sample, rng, x_camera, w_camera, d, a);
+        atomicAdd(f + kFeatDepthNearest + 0, d);
+        atomicAdd(f + kFeatDepthNearest + 1, a);
     }
 }
 
@@ -133,7 +173,7 @@ VPT_DEV void trace_one(const TraceParams& P, S& sample, uint32_t frame, int px, 
         atomicAdd(P.film_sq + pix * 3 + 1, (double)L.y * (double)L.y);
         atomicAdd(P.film_sq + pix * 3 + 2, (double)L.z * (double)L.z);
     }
-    if (features) accumulate_features(P, sample, rng, pix, fe, L, w);
+    if (features) accumulate_features(P, sample, rng, pix, fe, L, x, w);
     lookups += pc.lookups;
     guard_hit |= pc.guard_hit;
 }

@@ -159,6 +159,7 @@ struct TraceParams {
     double* film_sq;               // 3 doubles per pixel: sum of squared radiance (optional)
     float* feat;                   // feature accumulators (optional), kFeatStride floats per pixel
     int feat_background;           // accumulate the background map (requested by the user)
+    int feat_depth_maps;           // bit 0: Depth Blended, bit 1: Depth Nearest Opaque (requested)
     unsigned long long* counters;  // [0] paths, [1] density lookups
     int* error_flags;
     unsigned int* work_counter;    // persistent-kernel path queue
@@ -179,7 +180,10 @@ enum FeatureSlot : int {
     kFeatTrans = 14,     // primary-ray transmittance
                          // 15: unused (keeps the background float4-aligned)
     kFeatBackground = 16,// rgb: skybox of the camera ray for paths with an event, else their radiance
-    kFeatStride = 20,
+                         // 19: unused
+    kFeatDepthBlended = 20,  // alpha-blended depth of the camera ray's march, its alpha
+    kFeatDepthNearest = 22,  // depth of the last non-transparent march step times alpha, alpha
+    kFeatStride = 24,
 };
 
 }  // namespace vpt

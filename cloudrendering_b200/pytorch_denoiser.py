@@ -42,6 +42,7 @@ RENDERER_FEATURES = {
     "Albedo": ("Albedo", 4), "Position": ("First X", 3), "Normal": ("Normal", 3),
     "Normal (Length 1)": ("Normal (Length 1)", 3), "CloudOnly": ("Cloud Only", 4), "Depth": ("Depth", 2),
     "Depth Far": ("Depth Far", 1), "Density": ("Density", 2), "Background": ("Background", 4),
+    "Depth Blended": ("Depth Blended", 2), "Depth Nearest Opaque": ("Depth Nearest Opaque", 2),
 }
 # maps the renderer provides without a feature pass (static camera: no motion between frames)
 SYNTHESISED = {"Flow", "Flow Reverse", "Reproj_UV", "Unused"}

@@ -73,6 +73,8 @@ enum {
     VPT_FEATURE_DEPTH_FAR = 7,     /* mean of (event ? depth : far distance) */
     VPT_FEATURE_DENSITY = 12,
     VPT_FEATURE_BACKGROUND = 13,
+    VPT_FEATURE_DEPTH_BLENDED = 15,        /* (alpha-blended depth, alpha, 0, 1) of a march along the camera ray */
+    VPT_FEATURE_DEPTH_NEAREST_OPAQUE = 16, /* (depth of the last non-transparent step x alpha, alpha, 0, 1) */
     VPT_FEATURE_ALBEDO = 17,
     VPT_FEATURE_TRANSMITTANCE = 32 /* new: primary-ray transmittance (no reference counterpart) */
 };

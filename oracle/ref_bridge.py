@@ -47,6 +47,8 @@ def load():
         lib.ref_find_variant.argtypes = [c_char_p]
         lib.ref_render.restype = c_int
         lib.ref_render.argtypes = [c_int, ctypes.POINTER(RefScene), c_void_p, c_int]
+        lib.ref_read_depth_feature.restype = c_int
+        lib.ref_read_depth_feature.argtypes = [c_int, c_void_p]
         _lib = lib
     return _lib
 
@@ -84,4 +86,12 @@ class Scene:
         st = lib.ref_render(idx, ctypes.byref(self.s), out.ctypes.data_as(c_void_p), threads)
         if st != 0:
             raise RuntimeError("ref_render failed")
+        return out
+
+    @staticmethod
+    def depth_feature(which: int, height: int, width: int) -> np.ndarray:
+        """The last render's depthBlendedImage (which 0) or depthNearestOpaqueImage (1), H x W x 4."""
+        out = np.empty((height, width, 4), np.float32)
+        if load().ref_read_depth_feature(which, out.ctypes.data_as(c_void_p)) != 0:
+            raise RuntimeError("ref_read_depth_feature failed")
         return out

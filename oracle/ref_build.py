@@ -57,6 +57,8 @@ LIGHT_VARIANTS = {"nee_l1": 1, "nee_l2": 2}
 SDT_PROB = {"max": "MAX_BASED_PROBABILITY", "avg": "AVG_BASED_PROBABILITY",
             "hist": "PATH_HISTORY_AVG_BASED_PROBABILITY"}
 SPECTRAL = {"sdt": "USE_SPECTRAL_DELTA_TRACKING", "nees": "USE_NEXT_EVENT_TRACKING_SPECTRAL"}
+# the Depth Blended / Depth Nearest Opaque feature maps (Clouds.glsl:367-383), deterministic lookups
+DEPTH_MAPS = ["WRITE_DEPTH_BLENDED_MAP", "WRITE_DEPTH_NEAREST_OPAQUE_MAP"]
 
 
 def variants():
@@ -73,6 +75,9 @@ def variants():
         for p, pdef in SDT_PROB.items():
             for i in ("stochastic", "trilinear"):
                 out.append((f"{t}_{p}__{i}__default__linear", [tdef, pdef, INTERPS[i]] + ENVS["default__linear"], 0))
+    for i in ("nearest", "trilinear"):
+        out.append((f"depthmaps__{i}__default__linear", TRACKERS["delta"] + [INTERPS[i]] + ENVS["default__linear"]
+                    + DEPTH_MAPS, 0))
     return out
 
 

@@ -24,6 +24,8 @@ static sampler2D& environmentMapOctahedralTexture = g_ref.envocta;
 static uimage3D& occupancyGridImage = g_ref.occ;
 static image2D& resultImage = g_ref.result;
 static image2D& accImage = g_ref.acc;
+static image2D& depthBlendedImage = g_ref.dblend;
+static image2D& depthNearestOpaqueImage = g_ref.dnear;
 static Light* const lights = g_ref.lights;
 #define gl_GlobalInvocationID gl_global_invocation_id
 #define main glsl_main
@@ -42,6 +44,7 @@ namespace glslref {
 RefState g_ref;
 thread_local uvec3 gl_global_invocation_id;
 uint ref_seed_offset = 0;
+static std::vector<float> g_dblend, g_dnear;  // the depth feature images of the last ref_render
 }  // namespace glslref
 
 using namespace glslref;
@@ -174,6 +177,14 @@ int ref_render(int variant, const RefScene* s, float* out_rgba, int threads) {
     g_ref.acc.data = acc.data();
     g_ref.acc.w = s->width;
     g_ref.acc.h = s->height;
+    g_dblend.assign((size_t)s->width * s->height * 4, 0.0f);
+    g_dnear.assign((size_t)s->width * s->height * 4, 0.0f);
+    g_ref.dblend.data = g_dblend.data();
+    g_ref.dblend.w = s->width;
+    g_ref.dblend.h = s->height;
+    g_ref.dnear.data = g_dnear.data();
+    g_ref.dnear.w = s->width;
+    g_ref.dnear.h = s->height;
     ref_seed_offset = s->seed_offset;
     int nt = threads;
 #ifdef _OPENMP
@@ -190,6 +201,15 @@ int ref_render(int variant, const RefScene* s, float* out_rgba, int threads) {
             for (int x = 0; x < s->width; x++) run(x, y);
     }
     memcpy(out_rgba, acc.data(), acc.size() * sizeof(float));
+    return 0;
+}
+
+// The depth feature images of the last ref_render (which: 0 = depthBlendedImage, 1 =
+// depthNearestOpaqueImage; W*H*4, the reference's running means), for WRITE_DEPTH_*_MAP variants.
+int ref_read_depth_feature(int which, float* out_rgba) {
+    const std::vector<float>& v = which == 0 ? g_dblend : g_dnear;
+    if (!out_rgba || (which != 0 && which != 1) || v.empty()) return 1;
+    memcpy(out_rgba, v.data(), v.size() * sizeof(float));
     return 0;
 }
 

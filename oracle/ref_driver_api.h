@@ -13,6 +13,7 @@ struct RefState {
     sampler2D envocta;    // environmentMapOctahedralTexture (mip chain)
     uimage3D occ;         // occupancyGridImage
     image2D result, acc;  // resultImage, accImage
+    image2D dblend, dnear;  // depthBlendedImage, depthNearestOpaqueImage (WRITE_DEPTH_*_MAP variants)
     Light lights[16];     // LightsBuffer
 };
 extern RefState g_ref;

@@ -5,7 +5,10 @@ For every case the fixture stores the inputs (grid, scene parameters, camera mat
 reference's output: the radiance of each camera path of frame 0 (1 spp; accImage after one frame is
 the path radiance itself) and the reference's fp32 running mean after 8 frames.
 
-Run in a container that has the reference tree:  python tests/golden/make_golden.py
+With the argument ``depth_maps`` it writes tests/golden/ref_depth_maps.npz instead: the reference's
+Depth Blended and Depth Nearest Opaque images (Clouds.glsl:367-383) after 4 frames.
+
+Run in a container that has the reference tree:  python tests/golden/make_golden.py [depth_maps]
 """
 import json
 import os
@@ -82,6 +85,41 @@ FIELDS = ["mode", "interp", "extinction", "albedo", "g", "width", "height", "see
           "env_intensity", "max_bounces", "ess_ref_compat", "lights", "extinction_base", "albedo_rgb", "sdt_prob"]
 
 
+def depth_map_cases():
+    """Depth Blended / Depth Nearest Opaque (Clouds.glsl:367-383): the fbm cloud, delta tracking,
+    nearest and trilinear lookups (deterministic: the marches consume no random numbers)."""
+    fbm = bridge.fbm(24, 2, base_frequency=3.0, contrast=3.5)
+    base = dict(mode="delta", extinction=120.0, albedo=0.99, g=0.85, width=W, height=H, env="default", linear_rgb=1,
+                cam_pos=(0.3, 0.4, 1.4), max_grid_extent=0.5)
+    return {f"fbm_depthmaps_{i}": SceneSpec(grid=fbm, interp=i, **base) for i in ("nearest", "trilinear")}
+
+
+DEPTH_FRAMES = 4
+
+
+def main_depth_maps():
+    """tests/golden/ref_depth_maps.npz: the reference's depthBlendedImage and depthNearestOpaqueImage
+    (fp32 running means, H x W x 4) after 4 frames."""
+    from oracle import ref_bridge
+
+    data, meta = {}, {}
+    for name, sp in depth_map_cases().items():
+        inv = camera_inv_view_proj(sp)
+        sc, _ = reference_scene(sp, DEPTH_FRAMES, inv=inv)
+        variant = f"depthmaps__{sp.interp}__default__linear"
+        sc.render(variant)
+        data[name + "__blended"] = ref_bridge.Scene.depth_feature(0, sp.height, sp.width)
+        data[name + "__nearest"] = ref_bridge.Scene.depth_feature(1, sp.height, sp.width)
+        data[name + "__grid"] = np.ascontiguousarray(sp.grid, np.float32)
+        meta[name] = {"variant": variant, "frames": DEPTH_FRAMES,
+                      **{f: (list(getattr(sp, f)) if isinstance(getattr(sp, f), tuple) else getattr(sp, f))
+                         for f in FIELDS}}
+        print(name, variant, float(data[name + "__blended"][..., 1].mean()), float(data[name + "__nearest"][..., 0].mean()))
+    out = os.path.join(os.path.dirname(os.path.abspath(__file__)), "ref_depth_maps.npz")
+    np.savez_compressed(out, meta=json.dumps(meta), **data)
+    print("wrote", out, os.path.getsize(out), "bytes")
+
+
 def main():
     ref_build.build()
     data = {}
@@ -113,4 +151,8 @@ def main():
 
 
 if __name__ == "__main__":
+    if len(sys.argv) > 1 and sys.argv[1] == "depth_maps":
+        ref_build.build()
+        main_depth_maps()
+        sys.exit(0)
     main()

@@ -65,7 +65,7 @@ def test_model_info_keys_and_defaults(tmp_path):
     ({"input_feature_maps": "Color"}, "'input_feature_maps' is not an array"),
     ({"input_feature_maps": [1]}, "is not a string"),
     ({"input_feature_maps": ["Colour"]}, "Invalid feature map name 'colour'"),
-    ({"input_feature_maps": ["Color", "Depth Blended"]}, "'Depth Blended' used by"),
+    ({"input_feature_maps": ["Color", "nabla(z)"]}, "'nabla\\(z\\)' used by"),
 ])
 def test_model_info_errors(tmp_path, info, message):
     p = str(tmp_path / "m.pt")
