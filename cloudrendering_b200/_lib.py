@@ -69,6 +69,10 @@ SIGNATURES = {
     "vpt_set_use_feature_maps": (c_int, [VptCtxP, POINTER(c_int), c_int]),
     "vpt_get_feature_map": (c_int, [VptCtxP, c_int, c_void_p, c_int, c_int, c_void_p]),
     "vpt_get_denoiser_features": (c_int, [VptCtxP, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "vpt_set_emission_grid": (c_int, [VptCtxP, c_void_p, c_int, c_int, c_int, c_int]),
+    "vpt_set_use_emission": (c_int, [VptCtxP, c_int]),
+    "vpt_set_emission_cap": (c_int, [VptCtxP, c_float]),
+    "vpt_set_emission_strength": (c_int, [VptCtxP, c_float]),
     "vpt_get_stats": (c_int, [VptCtxP, POINTER(VptStats)]),
     "vpt_reset_stats": (c_int, [VptCtxP]),
     "vpt_synchronize": (c_int, [VptCtxP, c_void_p]),

@@ -147,6 +147,12 @@ struct VptContext {
     float vmin = 0.0f, vmax = 1.0f;
     float box_min[3] = {0, 0, 0}, box_max[3] = {0, 0, 0};
     DevBuf<float> raw, norm;
+    // emission grid (load_emission_file / set_use_emission / set_emission_cap / set_emission_strength;
+    // VolumetricPathTracingPass.hpp:326-328 defaults)
+    DevBuf<float> emission;
+    int enx = 0, eny = 0, enz = 0;
+    bool use_emission = false;
+    float emission_cap = 1.0f, emission_strength = 1.0f;
     DevBuf<float> minmax;
 
     // sparse (NanoVDB) volume: built from the dense grid when use_sparse is set
@@ -496,6 +502,24 @@ VptStatus fill_params(VptContext* ctx, int tracker, int frames, vpt::TraceParams
                         float(double(ctx->ny) / (double(ctx->box_max[1]) - double(ctx->box_min[1]))),
                         float(double(ctx->nz) / (double(ctx->box_max[2]) - double(ctx->box_min[2]))));
     P.border_density = (0.0f - ctx->vmin) / (ctx->vmax - ctx->vmin);
+    P.emission = nullptr;
+    if (ctx->use_emission && ctx->emission.ptr) {
+        // the emission grid's own box (CloudData::computeGridBounds with voxel size 1, centred)
+        const float sx = float(ctx->enx), sy = float(ctx->eny), sz = float(ctx->enz);
+        const float ms = std::max(sx, std::max(sy, sz));
+        const float hx = sx * ctx->max_grid_extent / ms, hy = sy * ctx->max_grid_extent / ms,
+                    hz = sz * ctx->max_grid_extent / ms;
+        P.emission = ctx->emission.ptr;
+        P.enx = ctx->enx;
+        P.eny = ctx->eny;
+        P.enz = ctx->enz;
+        P.emission_box_min = mk(-hx, -hy, -hz);
+        P.emission_vox_per_unit = mk(float(double(ctx->enx) / (2.0 * double(hx))),
+                                     float(double(ctx->eny) / (2.0 * double(hy))),
+                                     float(double(ctx->enz) / (2.0 * double(hz))));
+        P.emission_cap = ctx->emission_cap;
+        P.emission_strength = ctx->emission_strength;
+    }
     P.extinction = extinction_x(ctx);
     P.inv_extinction = 1.0f / P.extinction;
     P.albedo = ctx->albedo[0];
@@ -854,6 +878,42 @@ VptStatus vpt_set_dense_grid(VptContext* ctx, const float* data, int nx, int ny,
     ctx->ny = ny;
     ctx->nz = nz;
     return finish_grid(ctx, 0);
+}
+
+VptStatus vpt_set_emission_grid(VptContext* ctx, const float* data, int nx, int ny, int nz, int data_on_device) {
+    VPT_CHECK_CTX(ctx);
+    if (!data || nx <= 0 || ny <= 0 || nz <= 0) return fail(ctx, VPT_ERR_ARG, "vpt_set_emission_grid: bad grid");
+    cudaSetDevice(ctx->device);
+    const size_t n = (size_t)nx * ny * nz;
+    VPT_CHECK_CUDA(ctx, ctx->emission.alloc(n));
+    VPT_CHECK_CUDA(ctx, cudaMemcpy(ctx->emission.ptr, data, n * sizeof(float),
+                                   data_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice));
+    ctx->enx = nx;
+    ctx->eny = ny;
+    ctx->enz = nz;
+    reset_film_state(ctx);
+    return VPT_OK;
+}
+
+VptStatus vpt_set_use_emission(VptContext* ctx, int use) {
+    VPT_CHECK_CTX(ctx);
+    if ((use != 0) != ctx->use_emission) reset_film_state(ctx);
+    ctx->use_emission = use != 0;
+    return VPT_OK;
+}
+
+VptStatus vpt_set_emission_cap(VptContext* ctx, float cap) {
+    VPT_CHECK_CTX(ctx);
+    ctx->emission_cap = cap;
+    reset_film_state(ctx);
+    return VPT_OK;
+}
+
+VptStatus vpt_set_emission_strength(VptContext* ctx, float strength) {
+    VPT_CHECK_CTX(ctx);
+    ctx->emission_strength = strength;
+    reset_film_state(ctx);
+    return VPT_OK;
 }
 
 VptStatus vpt_generate_fbm_grid(VptContext* ctx, int nx, int ny, int nz, uint32_t seed, int octaves, float lacunarity,

@@ -462,6 +462,50 @@ VPT_DEV float sample_dense(const TraceParams& P, F3 pos, Rng& rng) {
     return sample_dense_vox<INTERP>(P, ux, uy, uz);
 }
 
+// Emission (sampleEmission / sampleEmissionRaw, VptUtils.glsl:604-626): the emission grid at the
+// point (its own world box, the density texture's filter and stochastic jitter, zero outside),
+// t = clamp(value * cap, 0, 1), radiance (t^2, t^4, t^8) * strength.
+VPT_DEV float emission_texel(const TraceParams& P, int ix, int iy, int iz) {
+    if ((unsigned)ix >= (unsigned)P.enx || (unsigned)iy >= (unsigned)P.eny || (unsigned)iz >= (unsigned)P.enz)
+        return 0.0f;
+    return __ldg(P.emission + ((size_t)iz * (size_t)P.eny + (size_t)iy) * (size_t)P.enx + (size_t)ix);
+}
+
+template <int INTERP>
+VPT_DEV F3 sample_emission(const TraceParams& P, F3 pos, Rng& rng) {
+    float ux = (pos.x - P.emission_box_min.x) * P.emission_vox_per_unit.x;
+    float uy = (pos.y - P.emission_box_min.y) * P.emission_vox_per_unit.y;
+    float uz = (pos.z - P.emission_box_min.z) * P.emission_vox_per_unit.z;
+    if (INTERP == kStochastic) {
+        float jx = rng_next(rng) - 0.5f;
+        float jy = rng_next(rng) - 0.5f;
+        float jz = rng_next(rng) - 0.5f;
+        ux = ux + jx;
+        uy = uy + jy;
+        uz = uz + jz;
+    }
+    float v;
+    if (INTERP != kTrilinear) {
+        v = emission_texel(P, (int)floorf(ux), (int)floorf(uy), (int)floorf(uz));
+    } else {
+        ux = ux - 0.5f;
+        uy = uy - 0.5f;
+        uz = uz - 0.5f;
+        const float fx0 = floorf(ux), fy0 = floorf(uy), fz0 = floorf(uz);
+        const float ax = ux - fx0, ay = uy - fy0, az = uz - fz0;
+        const int x0 = (int)fx0, y0 = (int)fy0, z0 = (int)fz0;
+        const float f0 = mixf(mixf(emission_texel(P, x0, y0, z0), emission_texel(P, x0 + 1, y0, z0), ax),
+                              mixf(emission_texel(P, x0, y0 + 1, z0), emission_texel(P, x0 + 1, y0 + 1, z0), ax), ay);
+        const float f1 =
+            mixf(mixf(emission_texel(P, x0, y0, z0 + 1), emission_texel(P, x0 + 1, y0, z0 + 1), ax),
+                 mixf(emission_texel(P, x0, y0 + 1, z0 + 1), emission_texel(P, x0 + 1, y0 + 1, z0 + 1), ax), ay);
+        v = mixf(f0, f1, az);
+    }
+    const float t = fminf(fmaxf(v * P.emission_cap, 0.0f), 1.0f);
+    const float r = t * t, g = r * r, b = g * g;
+    return f3(r * P.emission_strength, g * P.emission_strength, b * P.emission_strength);
+}
+
 // Normal feature: central differences of the density one voxel apart, scaled by 100/dim and
 // normalised when longer than 1e-5 (getCloudFiniteDifference, VptUtils.glsl:726-748).
 template <int INTERP>

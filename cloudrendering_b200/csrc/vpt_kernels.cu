@@ -30,6 +30,8 @@ struct Sampler {
         if constexpr (GRID == kNanoVdb) return sample_sparse<INTERP>(P, pos, rng);
         else return sample_dense<INTERP>(P, pos, rng);
     }
+    // the emission grid is dense whatever the density grid is
+    VPT_DEV F3 emission(F3 pos, Rng& rng) const { return sample_emission<INTERP>(P, pos, rng); }
     VPT_DEV F3 normal(F3 pos, Rng& rng) const {
         // getCloudFiniteDifference returns 0 for NanoVDB grids (VptUtils.glsl:726-729)
         if constexpr (GRID == kNanoVdb) return f3(0.0f, 0.0f, 0.0f);
@@ -453,7 +455,10 @@ VPT_DEV void refill_loop(const SRC& src, uint64_t total, unsigned long long* wor
         }
         const float xi = rng_next(rng);
         if (TRACKER != kRatio && xi < P.absorb_albedo * density) {
-            refill_finish<TRACKER>(P, pix, TRACKER == kNextEvent ? color : zero, has);
+            // USE_EMISSION (NextEventTracking.glsl:296-301): the absorbed NEE path ends with the emission
+            F3 L = zero;
+            if (TRACKER == kNextEvent) L = P.emission ? color + sample.emission(x, rng) : color;
+            refill_finish<TRACKER>(P, pix, L, has);
             continue;
         }
         if (xi < density) {

@@ -160,6 +160,13 @@ struct TraceParams {
     float* feat;                   // feature accumulators (optional), kFeatStride floats per pixel
     int feat_background;           // accumulate the background map (requested by the user)
     int feat_depth_maps;           // bit 0: Depth Blended, bit 1: Depth Nearest Opaque (requested)
+
+    // emission grid (USE_EMISSION): absorptions in next event tracking add sampleEmission(x)
+    const float* emission;         // dense [nz][ny][nx] values, or null (no emission)
+    int enx, eny, enz;
+    F3 emission_box_min;
+    F3 emission_vox_per_unit;
+    float emission_cap, emission_strength;
     unsigned long long* counters;  // [0] paths, [1] density lookups
     int* error_flags;
     unsigned int* work_counter;    // persistent-kernel path queue

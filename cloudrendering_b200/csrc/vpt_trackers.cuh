@@ -267,7 +267,8 @@ VPT_DEV F3 track_nee(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, Firs
             float xi = rng_next(rng);
             if (xi < P.absorb_albedo * density) {
                 record_event(fe, x, density, P.extinction, tmax - d + t);
-                return color;
+                // USE_EMISSION (NextEventTracking.glsl:296-301): the absorbed path ends with the emission
+                return P.emission ? color + sample.emission(x, rng) : color;
             }
             if (xi < density) {
                 if (P.max_bounces > 0 && ++bounces > P.max_bounces) return color;
@@ -439,7 +440,8 @@ VPT_DEV F3 track_nee_spectral(const TraceParams& P, S& sample, Rng& rng, F3 x, F
             float xi = rng_next(rng);
             if (xi < st.pa) {
                 record_event(fe, x, density, P.sdt_majorant, tmax - d + t);
-                return color;
+                // USE_EMISSION (NextEventTracking.glsl:125-131)
+                return P.emission ? color + sample.emission(x, rng) : color;
             }
             if (xi < st.pa + st.ps) {
                 if (P.max_bounces > 0 && ++bounces > P.max_bounces) return color;

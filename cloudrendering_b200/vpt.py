@@ -196,9 +196,21 @@ def load_cloud_file(filename: str) -> None:
     if not filename.endswith(".xyz"):
         raise RuntimeError(f"Error in CloudData::loadFromFile: unsupported file format \"{filename}\".")
     with open(filename, "rb") as f:
+        vx, vy, vz = struct.unpack_from("<3d", f.read(36), 12)
+    grid = _read_xyz(filename)
+    _c("vpt_set_voxel_size", vx, vy, vz)
+    set_density_field(torch.from_numpy(grid))
+
+
+load_volume_file = load_cloud_file
+
+
+def _read_xyz(filename: str) -> np.ndarray:
+    """A .xyz grid (CloudData::loadFromXyzFile, CloudData.cpp:236-317): [nz][ny][nx] float32 with the
+    file's min-max normalisation (minimum at most 0)."""
+    with open(filename, "rb") as f:
         buf = f.read()
     xs, ys, zs = struct.unpack_from("<3I", buf, 0)
-    vx, vy, vz = struct.unpack_from("<3d", buf, 12)
     n = xs * ys * zs
     data = np.frombuffer(buf, dtype="<f4", count=n, offset=36).astype(np.float32)
     grid = data.reshape(xs, ys, zs).transpose(2, 1, 0).copy()  # z-fastest file -> x-fastest
@@ -206,11 +218,40 @@ def load_cloud_file(filename: str) -> None:
     hi = float(grid.max())
     if hi - lo > 1e-6:
         grid = (grid - np.float32(lo)) / np.float32(hi - lo)
-    _c("vpt_set_voxel_size", vx, vy, vz)
-    set_density_field(torch.from_numpy(np.ascontiguousarray(grid, dtype=np.float32)))
+    return np.ascontiguousarray(grid, dtype=np.float32)
 
 
-load_volume_file = load_cloud_file
+# ---- emission (Module.cpp:826-832, 154-156; VolumetricPathTracingPass.cpp:897-906) ----
+def load_emission_file(filename: str) -> None:
+    """Loads the emission grid from a dense .xyz file (a second CloudData, normalised like the
+    density; its box follows the grid's dimensions and the max grid extent)."""
+    if not os.path.exists(filename):
+        raise RuntimeError(f"Error in CloudData::loadFromFile: The file \"{filename}\" does not exist.")
+    if not filename.endswith(".xyz"):
+        raise RuntimeError(f"Error in CloudData::loadFromFile: unsupported emission file format \"{filename}\".")
+    set_emission_field(torch.from_numpy(_read_xyz(filename)))
+
+
+def set_emission_field(emission: torch.Tensor) -> None:
+    """The emission grid as a [nz][ny][nx] float32 tensor (values scaled by the emission cap)."""
+    if emission.dim() != 3:
+        raise RuntimeError("Error in setEmissionField: expected a 3-D tensor.")
+    e = emission.detach().to(torch.float32).contiguous()
+    nz, ny, nx = e.shape
+    on_dev = 1 if e.is_cuda else 0
+    _c("vpt_set_emission_grid", ctypes.c_void_p(e.data_ptr()), int(nx), int(ny), int(nz), on_dev)
+
+
+def set_use_emission(use_emission: bool) -> None:
+    _c("vpt_set_use_emission", 1 if use_emission else 0)
+
+
+def set_emission_cap(emission_cap: float) -> None:
+    _c("vpt_set_emission_cap", float(emission_cap))
+
+
+def set_emission_strength(emission_strength: float) -> None:
+    _c("vpt_set_emission_strength", float(emission_strength))
 
 
 def set_max_grid_extent(max_grid_extent: float) -> None:

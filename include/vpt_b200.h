@@ -106,6 +106,16 @@ const char* vpt_last_error(const VptContext* ctx);
  * Values are normalised on the device by (v - min)/(max - min) (DensityField::getDataFloatAtNorm,
  * src/DensityField.cpp:262-267; min := 0 when min == max, DensityField.cpp:146-150). */
 VptStatus vpt_set_dense_grid(VptContext* ctx, const float* data, int nx, int ny, int nz, int data_on_device);
+/* Emission (Module.cpp load_emission_file / set_use_emission / set_emission_cap / set_emission_strength;
+ * sampleEmission, VptUtils.glsl:604-626): a dense [nz][ny][nx] grid with its own box (centred, largest
+ * side 2 * max_grid_extent), looked up with the density grid's interpolation; with emission on, an
+ * absorption in next event tracking (grey or spectral) ends the path with (t^2, t^4, t^8) * strength,
+ * t = clamp(value * cap, 0, 1).  Defaults: off, cap 1, strength 1.  (The reference's delta-tracking
+ * emission branch returns an undeclared variable and does not compile; delta tracking ignores it.) */
+VptStatus vpt_set_emission_grid(VptContext* ctx, const float* data, int nx, int ny, int nz, int data_on_device);
+VptStatus vpt_set_use_emission(VptContext* ctx, int use);
+VptStatus vpt_set_emission_cap(VptContext* ctx, float cap);
+VptStatus vpt_set_emission_strength(VptContext* ctx, float strength);
 /* Synthetic scene on the device: seeded fBm of improved Perlin noise, remapped to [0, 1], values
  * below `threshold` set to 0.  No reference counterpart (the reference loads files). */
 VptStatus vpt_generate_fbm_grid(VptContext* ctx, int nx, int ny, int nz, uint32_t seed, int octaves,

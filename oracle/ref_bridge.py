@@ -26,6 +26,9 @@ class RefScene(ctypes.Structure):
         ("env_rgba", c_void_p), ("env_w", c_int), ("env_h", c_int),
         ("env_pyramid", c_void_p), ("env_levels", c_int), ("is_env_black", c_int), ("far_dist", c_float),
         ("inv_view", c_float * 16), ("lights", c_float * 256),
+        ("emission", c_void_p), ("enx", c_int), ("eny", c_int), ("enz", c_int),
+        ("emission_box_min", c_float * 3), ("emission_box_max", c_float * 3), ("emission_cap", c_float),
+        ("emission_strength", c_float),
     ]
 
 
@@ -66,7 +69,7 @@ class Scene:
             self.set(k, v)
 
     def set(self, k, v):
-        if k in ("grid", "sv_data", "occupancy", "env_rgba", "env_pyramid"):
+        if k in ("grid", "sv_data", "occupancy", "env_rgba", "env_pyramid", "emission"):
             arr = None if v is None else np.ascontiguousarray(v)
             self._keep[k] = arr
             setattr(self.s, k, None if arr is None else arr.ctypes.data_as(c_void_p).value)

@@ -78,6 +78,12 @@ def variants():
     for i in ("nearest", "trilinear"):
         out.append((f"depthmaps__{i}__default__linear", TRACKERS["delta"] + [INTERPS[i]] + ENVS["default__linear"]
                     + DEPTH_MAPS, 0))
+    # emission grid (USE_EMISSION) with next event tracking, grey and spectral
+    for i in ("stochastic", "trilinear"):
+        out.append((f"nee_emission__{i}__default__linear", TRACKERS["nee"] + [INTERPS[i]] + ENVS["default__linear"]
+                    + ["USE_EMISSION"], 0))
+    out.append(("nees_hist_emission__stochastic__default__linear",
+                [SPECTRAL["nees"], SDT_PROB["hist"], INTERPS["stochastic"], "USE_EMISSION"] + ENVS["default__linear"], 0))
     return out
 
 

@@ -17,6 +17,7 @@ namespace REF_VARIANT_NS {
 static Parameters& parameters = g_ref.params;
 static FrameInfo& frameInfo = g_ref.frame;
 static sampler3D& gridImage = g_ref.grid;
+static sampler3D& emissionImage = g_ref.emission;
 static sampler3D& superVoxelGridImage = g_ref.sv;
 static usampler3D& superVoxelGridOccupancyImage = g_ref.svocc;
 static sampler2D& environmentMapTexture = g_ref.env;
@@ -74,6 +75,9 @@ typedef struct RefScene {
     float far_dist;
     float inv_view[16];       /* parameters.inverseViewMatrix, column-major */
     float lights[16 * 16];    /* 16 floats per light (see oracle/vpt_oracle.h) */
+    const float* emission;    /* emissionImage values [nz][ny][nx] (USE_EMISSION variants) */
+    int enx, eny, enz;
+    float emission_box_min[3], emission_box_max[3], emission_cap, emission_strength;
 } RefScene;
 
 int ref_variant_count(void) { return ref_num_variants; }
@@ -135,6 +139,16 @@ int ref_render(int variant, const RefScene* s, float* out_rgba, int threads) {
         l.padding = 0.0f;
     }
 
+    p.emissionBoxMin = vec3(s->emission_box_min[0], s->emission_box_min[1], s->emission_box_min[2]);
+    p.emissionBoxMax = vec3(s->emission_box_max[0], s->emission_box_max[1], s->emission_box_max[2]);
+    p.emissionCap = s->emission_cap;
+    p.emissionStrength = s->emission_strength;
+    g_ref.emission.data = s->emission;
+    g_ref.emission.w = s->enx;
+    g_ref.emission.h = s->eny;
+    g_ref.emission.d = s->enz;
+    g_ref.emission.channels = 1;
+    g_ref.emission.filter = s->linear_filter ? FILTER_LINEAR : FILTER_NEAREST;
     g_ref.grid.data = s->grid;
     g_ref.grid.w = s->nx;
     g_ref.grid.h = s->ny;

@@ -7,6 +7,7 @@ struct RefState {
     Parameters params;
     FrameInfo frame;
     sampler3D grid;       // gridImage
+    sampler3D emission;   // emissionImage (USE_EMISSION variants)
     sampler3D sv;         // superVoxelGridImage (RG32F)
     usampler3D svocc;     // superVoxelGridOccupancyImage
     sampler2D env;        // environmentMapTexture

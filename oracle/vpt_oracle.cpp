@@ -559,6 +559,42 @@ struct Tracer {
         return at_vox(ux, uy, uz);
     }
     float free_path(Rng& r) const { return -m_log(std::max(0.0000000001f, 1.0f - rnd(r))) * (1.0f / S.extinction); }
+    // sampleEmission (VptUtils.glsl:604-626): the emission grid at pos (the density texture's filter
+    // and stochastic jitter, zero outside its box), t = clamp(value * cap, 0, 1) -> (t^2, t^4, t^8) * strength
+    float emission_texel(int x, int y, int z) const {
+        if (x < 0 || y < 0 || z < 0 || x >= S.enx || y >= S.eny || z >= S.enz) return 0.0f;
+        return S.emission[((size_t)z * S.eny + y) * S.enx + x];
+    }
+    V3 emission(V3 pos, Rng& r) const {
+        float ux = (pos.x - S.emission_box_min[0]) * S.emission_vox_per_unit[0];
+        float uy = (pos.y - S.emission_box_min[1]) * S.emission_vox_per_unit[1];
+        float uz = (pos.z - S.emission_box_min[2]) * S.emission_vox_per_unit[2];
+        if (S.interp == 1) {
+            float jx = rnd(r) - 0.5f, jy = rnd(r) - 0.5f, jz = rnd(r) - 0.5f;
+            ux = ux + jx;
+            uy = uy + jy;
+            uz = uz + jz;
+        }
+        float v;
+        if (S.interp != 2) {
+            v = emission_texel((int)floorf(ux), (int)floorf(uy), (int)floorf(uz));
+        } else {
+            ux = ux - 0.5f;
+            uy = uy - 0.5f;
+            uz = uz - 0.5f;
+            float fx = floorf(ux), fy = floorf(uy), fz = floorf(uz);
+            float ax = ux - fx, ay = uy - fy, az = uz - fz;
+            int x0 = (int)fx, y0 = (int)fy, z0 = (int)fz;
+            float f0 = mixf(mixf(emission_texel(x0, y0, z0), emission_texel(x0 + 1, y0, z0), ax),
+                            mixf(emission_texel(x0, y0 + 1, z0), emission_texel(x0 + 1, y0 + 1, z0), ax), ay);
+            float f1 = mixf(mixf(emission_texel(x0, y0, z0 + 1), emission_texel(x0 + 1, y0, z0 + 1), ax),
+                            mixf(emission_texel(x0, y0 + 1, z0 + 1), emission_texel(x0 + 1, y0 + 1, z0 + 1), ax), ay);
+            v = mixf(f0, f1, az);
+        }
+        const float t = std::min(std::max(v * S.emission_cap, 0.0f), 1.0f);
+        const float rr = t * t, gg = rr * rr, bb = gg * gg;
+        return v3(rr * S.emission_strength, gg * S.emission_strength, bb * S.emission_strength);
+    }
     bool guard() { return ++steps > (1u << 24); }
     V3 sky(V3 d) const { return sky_and_sun(S, d); }
 
@@ -812,7 +848,8 @@ struct Tracer {
                 float xi = rnd(r);
                 if (xi < absorb * dens) {
                     ev = true;
-                    return color;
+                    // USE_EMISSION (NextEventTracking.glsl:296-301)
+                    return S.emission ? add(color, emission(x, r)) : color;
                 }
                 if (xi < dens) {
                     if (S.max_bounces > 0 && ++bounces > S.max_bounces) return color;
@@ -972,7 +1009,8 @@ struct Tracer {
                 float xi = rnd(r);
                 if (xi < pa) {
                     ev = true;
-                    return color;
+                    // USE_EMISSION (NextEventTracking.glsl:125-131)
+                    return S.emission ? add(color, emission(x, r)) : color;
                 }
                 if (xi < pa + ps) {
                     if (S.max_bounces > 0 && ++bounces > S.max_bounces) return color;

@@ -61,6 +61,12 @@ typedef struct OracleScene {
     float ext_rgb[3];
     float albedo_rgb[3];
     int sdt_prob;
+    /* emission grid (USE_EMISSION; next event tracking, grey and spectral): raw values x-fastest, or
+     * NULL; its world box, voxels per world unit, cap and strength */
+    const float* emission;
+    int enx, eny, enz;
+    float emission_box_min[3], emission_vox_per_unit[3];
+    float emission_cap, emission_strength;
 } OracleScene;
 
 /* Renders width*height*num_frames paths; adds radiance (and its square) per pixel (3 doubles). */

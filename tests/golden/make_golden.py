@@ -77,12 +77,21 @@ def cases():
         kw2.update(chroma)
         kw2.update(kw)
         out["fbm_" + name] = SceneSpec(grid=fbm, **kw2)
+    # emission grid (USE_EMISSION, next event tracking): a second fbm field on its own (smaller) box
+    emission = bridge.fbm(20, 7, base_frequency=2.0, contrast=3.0)
+    for name, kw in {"nee_emission": dict(mode="nee"),
+                     "nee_emission_trilinear": dict(mode="nee", interp="trilinear"),
+                     "nees_hist_emission": dict(mode="spectral_nee", sdt_prob=2, **chroma)}.items():
+        kw2 = dict(base)
+        kw2.update(kw)
+        out["fbm_" + name] = SceneSpec(grid=fbm, emission=emission, emission_cap=1.6, emission_strength=3.0, **kw2)
     return out
 
 
 FIELDS = ["mode", "interp", "extinction", "albedo", "g", "width", "height", "seed_offset", "env", "linear_rgb",
           "sun_dir", "sun_intensity", "cam_pos", "cam_target", "fovy", "near", "far", "max_grid_extent", "use_ess",
-          "env_intensity", "max_bounces", "ess_ref_compat", "lights", "extinction_base", "albedo_rgb", "sdt_prob"]
+          "env_intensity", "max_bounces", "ess_ref_compat", "lights", "extinction_base", "albedo_rgb", "sdt_prob",
+          "emission_cap", "emission_strength"]
 
 
 def depth_map_cases():
@@ -142,6 +151,8 @@ def main():
         data[name + "__inv_view_proj"] = np.array(inv, np.float32)
         if sp.env == "image":
             data[name + "__env_rgba"] = np.ascontiguousarray(sp.env_rgba, np.float32)
+        if sp.emission is not None:
+            data[name + "__emission"] = np.ascontiguousarray(sp.emission, np.float32)
         meta[name] = {"variant": variant, "grid": key, **{f: (list(getattr(sp, f)) if isinstance(getattr(sp, f), tuple)
                                                  else getattr(sp, f)) for f in FIELDS}}
         print(name, variant, float(paths.mean()))

@@ -67,7 +67,8 @@ class SceneSpec:
                  sky_color=(1.0, 1.0, 1.0), cam_pos=(0.0, 0.0, 0.8), cam_target=(0.0, 0.0, 0.0),
                  fovy=2.0 * math.atan(0.5), near=0.01, far=100.0, max_grid_extent=0.25, env_rgba=None,
                  use_ess=False, env_intensity=(1.0, 1.0, 1.0), ess_ref_compat=False, lights=None,
-                 extinction_base=(1.0, 1.0, 1.0), albedo_rgb=None, sdt_prob=2):
+                 extinction_base=(1.0, 1.0, 1.0), albedo_rgb=None, sdt_prob=2, emission=None, emission_cap=1.0,
+                 emission_strength=1.0):
         self.__dict__.update(locals())
         del self.__dict__["self"]
 
@@ -137,6 +138,12 @@ def setup_core(core: Core, sp: SceneSpec):
         core("vpt_add_light", None)
         for k, v in light_properties(light):
             core("vpt_set_light_property", i, k.encode(), v.encode())
+    if sp.emission is not None:
+        e = np.ascontiguousarray(sp.emission, np.float32)
+        core("vpt_set_emission_grid", e.ctypes.data_as(ctypes.c_void_p), e.shape[2], e.shape[1], e.shape[0], 0)
+        core("vpt_set_emission_cap", sp.emission_cap)
+        core("vpt_set_emission_strength", sp.emission_strength)
+    core("vpt_set_use_emission", 1 if sp.emission is not None else 0)
     core("vpt_set_resolution", sp.width, sp.height)
     core("vpt_set_denoiser", 0)
 
@@ -262,6 +269,19 @@ def oracle_scene(core, sp: SceneSpec, frames: int, frame_count: int = 0) -> brid
     sc.set("ext_rgb", [float(f32(f32(b) * f32(sp.extinction))) for b in sp.extinction_base])
     sc.set("albedo_rgb", [float(f32(a)) for a in (sp.albedo_rgb if sp.albedo_rgb is not None else [sp.albedo] * 3)])
     sc.set("sdt_prob", int(sp.sdt_prob))
+    if sp.emission is not None:  # the core's emission box and voxel scale (vpt_context.cu fill_params)
+        e = np.ascontiguousarray(sp.emission, np.float32)
+        enz, eny, enx = e.shape
+        ebmin, ebmax = bridge.grid_bounds(enx, eny, enz, sp.max_grid_extent)
+        sc.set("emission", e)
+        sc.set("enx", enx)
+        sc.set("eny", eny)
+        sc.set("enz", enz)
+        sc.set("emission_box_min", ebmin)
+        sc.set("emission_vox_per_unit", [float(np.float32(n / (float(b1) - float(b0))))
+                                         for n, b0, b1 in zip((enx, eny, enz), ebmin, ebmax)])
+        sc.set("emission_cap", float(np.float32(sp.emission_cap)))
+        sc.set("emission_strength", float(np.float32(sp.emission_strength)))
     # sun direction normalised exactly like vpt_set_sun (float ops in order)
     d = np.array(sp.sun_dir, np.float32)
     dl = np.sqrt(np.float32(np.float32(d[0] * d[0]) + np.float32(d[1] * d[1])) + np.float32(d[2] * d[2]), dtype=np.float32)
@@ -360,12 +380,23 @@ def reference_scene(sp: SceneSpec, frames: int, frame_start: int = 0, inv=None):
         sc.set("env_h", rgba.shape[0])
         sc.set("env_levels", 12)
         sc.set("env_pyramid", bridge.env_pyramid(rgba, 12))
+    if sp.emission is not None:
+        e = np.ascontiguousarray(sp.emission, np.float32)
+        enz, eny, enx = e.shape
+        ebmin, ebmax = bridge.grid_bounds(enx, eny, enz, sp.max_grid_extent)
+        sc.set("emission", e)
+        for k, v in (("enx", enx), ("eny", eny), ("enz", enz), ("emission_box_min", ebmin),
+                     ("emission_box_max", ebmax), ("emission_cap", sp.emission_cap),
+                     ("emission_strength", sp.emission_strength)):
+            sc.set(k, v)
     prob = ["max", "avg", "hist"][sp.sdt_prob]
     tracker = {"delta": "delta", "ratio": "ratio", "decomposition": "decomposition", "rrt": "rrt",
                "nee": "nee_ess" if sp.use_ess else "nee", "spectral_delta": f"sdt_{prob}",
                "spectral_nee": f"nees_{prob}"}[sp.mode]
     if sp.lights:
         tracker = f"nee_l{len(sp.lights)}"
+    if sp.emission is not None:
+        tracker += "_emission"
     env = {"default": "default", "black": "black", "single": "single", "image": "image"}[sp.env]
     colour = "linear" if (sp.linear_rgb or env != "default") else "srgb"
     return sc, f"{tracker}__{sp.interp}__{env}__{colour}"
@@ -388,6 +419,8 @@ def golden_cases():
         kw["grid"] = z[m["grid"]]
         if name + "__env_rgba" in z:
             kw["env_rgba"] = z[name + "__env_rgba"]
+        if name + "__emission" in z:
+            kw["emission"] = z[name + "__emission"]
         sp = SceneSpec(**kw)
         out[name] = (sp, list(z[name + "__inv_view_proj"]), z[name + "__paths"], z[name + "__mean8"])
     return out

@@ -133,3 +133,27 @@ def test_normal_len1_depth_far_and_background_maps():
     assert torch.allclose(bg[:3], colour[:, None, None].expand(3, 48, 64), rtol=1e-5)
     vpt.set_use_feature_maps([])
     vpt.set_use_builtin_environment_map("Default")
+
+
+def test_emission_grid_with_next_event_tracking():
+    """set_emission_field / set_use_emission / set_emission_cap / set_emission_strength: under a black
+    sky an absorbed NEE path ends with (t^2, t^4, t^8) * strength, t = clamp(value * cap, 0, 1); a
+    constant field 0.5 with cap 2 gives t = 1, i.e. strength on every channel."""
+    vpt.set_vpt_mode_from_name("Next Event Tracking")
+    vpt.set_use_builtin_environment_map("Black")
+    t = torch.zeros((3, 32, 32), dtype=torch.float32, device="cuda")
+    vpt.set_use_emission(False)
+    vpt.set_seed_offset(0)
+    dark = vpt.render_frame(t, 4).clone()
+    assert float(dark.abs().max()) == 0.0
+    vpt.set_emission_field(torch.full((8, 8, 8), 0.5))
+    vpt.set_emission_cap(2.0)
+    vpt.set_emission_strength(3.0)
+    vpt.set_use_emission(True)
+    lit = vpt.render_frame(t, 4)
+    assert float(lit.mean()) > 0.0
+    assert torch.equal(lit[0], lit[1]) and torch.equal(lit[1], lit[2])
+    frac = lit[0] / 3.0  # fraction of the pixel's paths that were absorbed
+    assert torch.all(frac <= 1.0 + 1e-6) and torch.allclose(frac * 4, torch.round(frac * 4), atol=1e-5)
+    vpt.set_use_emission(False)
+    vpt.set_use_builtin_environment_map("Default")
