@@ -73,6 +73,8 @@ SIGNATURES = {
     "vpt_set_use_emission": (c_int, [VptCtxP, c_int]),
     "vpt_set_emission_cap": (c_int, [VptCtxP, c_float]),
     "vpt_set_emission_strength": (c_int, [VptCtxP, c_float]),
+    "vpt_set_transfer_function": (c_int, [VptCtxP, c_void_p, c_int]),
+    "vpt_set_use_transfer_function": (c_int, [VptCtxP, c_int]),
     "vpt_get_stats": (c_int, [VptCtxP, POINTER(VptStats)]),
     "vpt_reset_stats": (c_int, [VptCtxP]),
     "vpt_synchronize": (c_int, [VptCtxP, c_void_p]),

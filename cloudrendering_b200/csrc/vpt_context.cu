@@ -153,6 +153,10 @@ struct VptContext {
     int enx = 0, eny = 0, enz = 0;
     bool use_emission = false;
     float emission_cap = 1.0f, emission_strength = 1.0f;
+    // transfer function (set_use_transfer_function; the RGBA table of transferFunctionTexture)
+    DevBuf<float> tf;
+    int tf_size = 0;
+    bool use_tf = false;
     DevBuf<float> minmax;
 
     // sparse (NanoVDB) volume: built from the dense grid when use_sparse is set
@@ -503,6 +507,9 @@ VptStatus fill_params(VptContext* ctx, int tracker, int frames, vpt::TraceParams
                         float(double(ctx->nz) / (double(ctx->box_max[2]) - double(ctx->box_min[2]))));
     P.border_density = (0.0f - ctx->vmin) / (ctx->vmax - ctx->vmin);
     P.emission = nullptr;
+    P.emission_strength = ctx->emission_strength;
+    P.tf = (ctx->use_tf && ctx->tf.ptr && ctx->tf_size > 0) ? ctx->tf.ptr : nullptr;
+    P.tf_size = ctx->tf_size;
     if (ctx->use_emission && ctx->emission.ptr) {
         // the emission grid's own box (CloudData::computeGridBounds with voxel size 1, centred)
         const float sx = float(ctx->enx), sy = float(ctx->eny), sz = float(ctx->enz);
@@ -518,7 +525,6 @@ VptStatus fill_params(VptContext* ctx, int tracker, int frames, vpt::TraceParams
                                      float(double(ctx->eny) / (2.0 * double(hy))),
                                      float(double(ctx->enz) / (2.0 * double(hz))));
         P.emission_cap = ctx->emission_cap;
-        P.emission_strength = ctx->emission_strength;
     }
     P.extinction = extinction_x(ctx);
     P.inv_extinction = 1.0f / P.extinction;
@@ -892,6 +898,24 @@ VptStatus vpt_set_emission_grid(VptContext* ctx, const float* data, int nx, int 
     ctx->eny = ny;
     ctx->enz = nz;
     reset_film_state(ctx);
+    return VPT_OK;
+}
+
+VptStatus vpt_set_transfer_function(VptContext* ctx, const float* rgba, int entries) {
+    VPT_CHECK_CTX(ctx);
+    if (!rgba || entries <= 0 || entries > 65536) return fail(ctx, VPT_ERR_ARG, "vpt_set_transfer_function: bad table");
+    cudaSetDevice(ctx->device);
+    VPT_CHECK_CUDA(ctx, ctx->tf.alloc((size_t)entries * 4));
+    VPT_CHECK_CUDA(ctx, cudaMemcpy(ctx->tf.ptr, rgba, (size_t)entries * 4 * sizeof(float), cudaMemcpyHostToDevice));
+    ctx->tf_size = entries;
+    reset_film_state(ctx);
+    return VPT_OK;
+}
+
+VptStatus vpt_set_use_transfer_function(VptContext* ctx, int use) {
+    VPT_CHECK_CTX(ctx);
+    if ((use != 0) != ctx->use_tf) reset_film_state(ctx);
+    ctx->use_tf = use != 0;
     return VPT_OK;
 }
 

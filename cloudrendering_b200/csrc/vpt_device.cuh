@@ -462,6 +462,21 @@ VPT_DEV float sample_dense(const TraceParams& P, F3 pos, Rng& rng) {
     return sample_dense_vox<INTERP>(P, ux, uy, uz);
 }
 
+// Transfer function (sampleCloudDensityEmission, VptUtils.glsl:647-672; transferFunctionTexture, a
+// one-row array texture): linear filtering along the normalised density with clamp to edge.
+VPT_DEV void tf_lookup(const TraceParams& P, float v, F3& rgb, float& alpha) {
+    const float u = v * (float)P.tf_size - 0.5f;
+    const float fu = floorf(u);
+    const float a = u - fu;
+    int x0 = (int)fu, x1 = x0 + 1;
+    x0 = x0 < 0 ? 0 : (x0 >= P.tf_size ? P.tf_size - 1 : x0);
+    x1 = x1 < 0 ? 0 : (x1 >= P.tf_size ? P.tf_size - 1 : x1);
+    const float* c0 = P.tf + 4 * x0;
+    const float* c1 = P.tf + 4 * x1;
+    rgb = f3(mixf(__ldg(c0), __ldg(c1), a), mixf(__ldg(c0 + 1), __ldg(c1 + 1), a), mixf(__ldg(c0 + 2), __ldg(c1 + 2), a));
+    alpha = mixf(__ldg(c0 + 3), __ldg(c1 + 3), a);
+}
+
 // Emission (sampleEmission / sampleEmissionRaw, VptUtils.glsl:604-626): the emission grid at the
 // point (its own world box, the density texture's filter and stochastic jitter, zero outside),
 // t = clamp(value * cap, 0, 1), radiance (t^2, t^4, t^8) * strength.

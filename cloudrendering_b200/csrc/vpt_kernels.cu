@@ -25,10 +25,22 @@ unsigned long long launch_count() { return __atomic_load_n(&g_launches, __ATOMIC
 template <int INTERP, int GRID>
 struct Sampler {
     const TraceParams& P;
+    F3 tf_rgb = {0.0f, 0.0f, 0.0f};  // transfer-function colour of the last lookup
     static constexpr bool kSparse = GRID == kNanoVdb;
-    VPT_DEV float operator()(F3 pos, Rng& rng) const {
-        if constexpr (GRID == kNanoVdb) return sample_sparse<INTERP>(P, pos, rng);
-        else return sample_dense<INTERP>(P, pos, rng);
+    VPT_DEV float operator()(F3 pos, Rng& rng) {
+        float v;
+        if constexpr (GRID == kNanoVdb) v = sample_sparse<INTERP>(P, pos, rng);
+        else v = sample_dense<INTERP>(P, pos, rng);
+        if (P.tf) {  // sampleCloud with USE_TRANSFER_FUNCTION: the table's alpha at the density
+            float a;
+            tf_lookup(P, v, tf_rgb, a);
+            return a;
+        }
+        return v;
+    }
+    // transfer-function emission of the last lookup (parameters.emissionStrength * densityEmission.rgb)
+    VPT_DEV F3 tf_emission() const {
+        return f3(P.emission_strength * tf_rgb.x, P.emission_strength * tf_rgb.y, P.emission_strength * tf_rgb.z);
     }
     // the emission grid is dense whatever the density grid is
     VPT_DEV F3 emission(F3 pos, Rng& rng) const { return sample_emission<INTERP>(P, pos, rng); }
@@ -457,7 +469,11 @@ VPT_DEV void refill_loop(const SRC& src, uint64_t total, unsigned long long* wor
         if (TRACKER != kRatio && xi < P.absorb_albedo * density) {
             // USE_EMISSION (NextEventTracking.glsl:296-301): the absorbed NEE path ends with the emission
             F3 L = zero;
-            if (TRACKER == kNextEvent) L = P.emission ? color + sample.emission(x, rng) : color;
+            if (TRACKER == kNextEvent) {
+                L = P.emission ? color + sample.emission(x, rng) : (P.tf ? color + sample.tf_emission() : color);
+            } else if (P.tf) {  // delta tracking (DeltaTracking.glsl:293-301)
+                L = sample.tf_emission();
+            }
             refill_finish<TRACKER>(P, pix, L, has);
             continue;
         }

@@ -166,7 +166,12 @@ struct TraceParams {
     int enx, eny, enz;
     F3 emission_box_min;
     F3 emission_vox_per_unit;
-    float emission_cap, emission_strength;
+    float emission_cap, emission_strength;  // the strength also scales transfer-function emission
+
+    // transfer function (USE_TRANSFER_FUNCTION): every density lookup becomes the table's alpha at the
+    // normalised density; absorptions emit strength * its rgb
+    const float* tf;               // tf_size RGBA entries, or null
+    int tf_size;
     unsigned long long* counters;  // [0] paths, [1] density lookups
     int* error_flags;
     unsigned int* work_counter;    // persistent-kernel path queue

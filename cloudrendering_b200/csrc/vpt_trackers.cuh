@@ -67,7 +67,8 @@ VPT_DEV F3 track_delta(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, Fi
             float xi = rng_next(rng);
             if (xi < P.absorb_albedo * density) {
                 record_event(fe, x, density, P.extinction, tmax - d + t);
-                return f3(0.0f, 0.0f, 0.0f);
+                // USE_TRANSFER_FUNCTION (DeltaTracking.glsl:293-301): the table's emission
+                return P.tf ? sample.tf_emission() : f3(0.0f, 0.0f, 0.0f);
             }
             if (xi < density) {
                 if (P.max_bounces > 0 && ++bounces > P.max_bounces) return f3(0.0f, 0.0f, 0.0f);
@@ -267,8 +268,9 @@ VPT_DEV F3 track_nee(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, Firs
             float xi = rng_next(rng);
             if (xi < P.absorb_albedo * density) {
                 record_event(fe, x, density, P.extinction, tmax - d + t);
-                // USE_EMISSION (NextEventTracking.glsl:296-301): the absorbed path ends with the emission
-                return P.emission ? color + sample.emission(x, rng) : color;
+                // USE_EMISSION (NextEventTracking.glsl:296-301): the absorbed path ends with the
+                // emission; else USE_TRANSFER_FUNCTION (:303-310) with the table's
+                return P.emission ? color + sample.emission(x, rng) : (P.tf ? color + sample.tf_emission() : color);
             }
             if (xi < density) {
                 if (P.max_bounces > 0 && ++bounces > P.max_bounces) return color;
@@ -393,6 +395,12 @@ VPT_DEV F3 track_delta_spectral(const TraceParams& P, S& sample, Rng& rng, F3 x,
             float xi = rng_next(rng);
             if (xi < st.pa) {
                 record_event(fe, x, density, P.sdt_majorant, tmax - d + t);
+                if (P.tf) {  // USE_TRANSFER_FUNCTION (DeltaTracking.glsl:125-127): weights sigma_a / (maj Pa) L_e
+                    const F3 le = sample.tf_emission();
+                    const float den = P.sdt_majorant * st.pa;
+                    return f3(weights.x * st.sa.x / den * le.x, weights.y * st.sa.y / den * le.y,
+                              weights.z * st.sa.z / den * le.z);
+                }
                 return f3(0.0f, 0.0f, 0.0f);
             }
             if (xi < st.pa + st.ps) {
@@ -433,15 +441,18 @@ VPT_DEV F3 track_nee_spectral(const TraceParams& P, S& sample, Rng& rng, F3 x, F
             float t = free_path(rng, P.inv_sdt_majorant);
             if (t > d) break;
             F3 xn = x + w * t;
-            float density = sample(xn, rng);
+            // with a transfer function the reference looks up the previous point x
+            // (NextEventTracking.glsl:74, sampleCloudDensityEmission(x)); reproduced
+            float density = sample(P.tf ? x : xn, rng);
             pc.lookups++;
             x = xn;
             const SdtStep st = sdt_probabilities(P, density, weights);
             float xi = rng_next(rng);
             if (xi < st.pa) {
                 record_event(fe, x, density, P.sdt_majorant, tmax - d + t);
-                // USE_EMISSION (NextEventTracking.glsl:125-131)
-                return P.emission ? color + sample.emission(x, rng) : color;
+                // USE_EMISSION (NextEventTracking.glsl:125-131); else USE_TRANSFER_FUNCTION (:133-139),
+                // which returns the emission without the NEE colour gathered so far
+                return P.emission ? color + sample.emission(x, rng) : (P.tf ? sample.tf_emission() : color);
             }
             if (xi < st.pa + st.ps) {
                 if (P.max_bounces > 0 && ++bounces > P.max_bounces) return color;

@@ -254,6 +254,26 @@ def set_emission_strength(emission_strength: float) -> None:
     _c("vpt_set_emission_strength", float(emission_strength))
 
 
+# ---- transfer function (Module.cpp:106-112) ----
+def set_use_transfer_function(_use_tf: bool) -> None:
+    _c("vpt_set_use_transfer_function", 1 if _use_tf else 0)
+
+
+def set_transfer_function_table(rgba) -> None:
+    """The transfer-function texture as N x 4 RGBA values over the normalised density [0, 1] (the
+    reference generates this table in sgl's TransferFunctionWindow)."""
+    t = np.ascontiguousarray(np.asarray(rgba, dtype=np.float32))
+    if t.ndim != 2 or t.shape[1] != 4 or t.shape[0] < 1:
+        raise RuntimeError("Error in setTransferFunctionTable: expected an N x 4 RGBA table.")
+    _c("vpt_set_transfer_function", t.ctypes.data_as(ctypes.c_void_p), int(t.shape[0]))
+
+
+def load_transfer_function_file(tf_file_path: str) -> None:
+    raise RuntimeError("Error in loadTransferFunctionFile: transfer-function files are parsed by sgl's "
+                       "TransferFunctionWindow, which this module does not include; pass the table to "
+                       "set_transfer_function_table.")
+
+
 def set_max_grid_extent(max_grid_extent: float) -> None:
     _c("vpt_set_max_grid_extent", float(max_grid_extent))
 

@@ -116,6 +116,14 @@ VptStatus vpt_set_emission_grid(VptContext* ctx, const float* data, int nx, int 
 VptStatus vpt_set_use_emission(VptContext* ctx, int use);
 VptStatus vpt_set_emission_cap(VptContext* ctx, float cap);
 VptStatus vpt_set_emission_strength(VptContext* ctx, float strength);
+/* Transfer-function appearance (Module.cpp set_use_transfer_function; USE_TRANSFER_FUNCTION in
+ * VptUtils.glsl:629-672, DeltaTracking.glsl, NextEventTracking.glsl): with it on, every density lookup
+ * is the table's alpha at the normalised density (linear filtering over `entries` RGBA entries on
+ * [0, 1], clamp to edge, as transferFunctionTexture), and an absorption emits emission_strength times
+ * the table's rgb (delta and next event tracking, grey and spectral).  The table is the caller's:
+ * the reference builds it in sgl's TransferFunctionWindow, which is not part of its source tree. */
+VptStatus vpt_set_transfer_function(VptContext* ctx, const float* rgba, int entries);
+VptStatus vpt_set_use_transfer_function(VptContext* ctx, int use);
 /* Synthetic scene on the device: seeded fBm of improved Perlin noise, remapped to [0, 1], values
  * below `threshold` set to 0.  No reference counterpart (the reference loads files). */
 VptStatus vpt_generate_fbm_grid(VptContext* ctx, int nx, int ny, int nz, uint32_t seed, int octaves,

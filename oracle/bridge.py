@@ -40,7 +40,7 @@ class OracleScene(ctypes.Structure):
         ("ext_rgb", c_float * 3), ("albedo_rgb", c_float * 3), ("sdt_prob", c_int),
         ("emission", c_void_p), ("enx", c_int), ("eny", c_int), ("enz", c_int),
         ("emission_box_min", c_float * 3), ("emission_vox_per_unit", c_float * 3), ("emission_cap", c_float),
-        ("emission_strength", c_float),
+        ("emission_strength", c_float), ("tf", c_void_p), ("tf_size", c_int),
     ]
 
 
@@ -196,7 +196,7 @@ class Scene:
             self.set(k, v)
 
     def set(self, k, v):
-        if k in ("density", "sv_data", "occupancy", "env_rgba", "env_pyramid", "nanovdb", "emission"):
+        if k in ("density", "sv_data", "occupancy", "env_rgba", "env_pyramid", "nanovdb", "emission", "tf"):
             arr = None if v is None else np.ascontiguousarray(v)
             self._keep[k] = arr
             setattr(self.s, k, None if arr is None else arr.ctypes.data_as(c_void_p).value)

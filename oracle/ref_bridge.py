@@ -28,7 +28,7 @@ class RefScene(ctypes.Structure):
         ("inv_view", c_float * 16), ("lights", c_float * 256),
         ("emission", c_void_p), ("enx", c_int), ("eny", c_int), ("enz", c_int),
         ("emission_box_min", c_float * 3), ("emission_box_max", c_float * 3), ("emission_cap", c_float),
-        ("emission_strength", c_float),
+        ("emission_strength", c_float), ("tf", c_void_p), ("tf_size", c_int),
     ]
 
 
@@ -69,7 +69,7 @@ class Scene:
             self.set(k, v)
 
     def set(self, k, v):
-        if k in ("grid", "sv_data", "occupancy", "env_rgba", "env_pyramid", "emission"):
+        if k in ("grid", "sv_data", "occupancy", "env_rgba", "env_pyramid", "emission", "tf"):
             arr = None if v is None else np.ascontiguousarray(v)
             self._keep[k] = arr
             setattr(self.s, k, None if arr is None else arr.ctypes.data_as(c_void_p).value)

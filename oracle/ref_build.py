@@ -84,6 +84,14 @@ def variants():
                     + ["USE_EMISSION"], 0))
     out.append(("nees_hist_emission__stochastic__default__linear",
                 [SPECTRAL["nees"], SDT_PROB["hist"], INTERPS["stochastic"], "USE_EMISSION"] + ENVS["default__linear"], 0))
+    # transfer-function appearance (USE_TRANSFER_FUNCTION): density = TF(value).a, absorption emission
+    for t in ("delta", "nee"):
+        for i in ("stochastic", "trilinear"):
+            out.append((f"{t}_tf__{i}__default__linear", TRACKERS[t] + [INTERPS[i]] + ENVS["default__linear"]
+                        + ["USE_TRANSFER_FUNCTION"], 0))
+    for t, tdef in SPECTRAL.items():
+        out.append((f"{t}_hist_tf__stochastic__default__linear",
+                    [tdef, SDT_PROB["hist"], INTERPS["stochastic"], "USE_TRANSFER_FUNCTION"] + ENVS["default__linear"], 0))
     return out
 
 

@@ -18,6 +18,7 @@ static Parameters& parameters = g_ref.params;
 static FrameInfo& frameInfo = g_ref.frame;
 static sampler3D& gridImage = g_ref.grid;
 static sampler3D& emissionImage = g_ref.emission;
+static sampler1DArray& transferFunctionTexture = g_ref.tf;
 static sampler3D& superVoxelGridImage = g_ref.sv;
 static usampler3D& superVoxelGridOccupancyImage = g_ref.svocc;
 static sampler2D& environmentMapTexture = g_ref.env;
@@ -78,6 +79,8 @@ typedef struct RefScene {
     const float* emission;    /* emissionImage values [nz][ny][nx] (USE_EMISSION variants) */
     int enx, eny, enz;
     float emission_box_min[3], emission_box_max[3], emission_cap, emission_strength;
+    const float* tf;          /* transferFunctionTexture: tf_size RGBA entries (USE_TRANSFER_FUNCTION variants) */
+    int tf_size;
 } RefScene;
 
 int ref_variant_count(void) { return ref_num_variants; }
@@ -143,6 +146,9 @@ int ref_render(int variant, const RefScene* s, float* out_rgba, int threads) {
     p.emissionBoxMax = vec3(s->emission_box_max[0], s->emission_box_max[1], s->emission_box_max[2]);
     p.emissionCap = s->emission_cap;
     p.emissionStrength = s->emission_strength;
+    g_ref.tf.data = s->tf;
+    g_ref.tf.w = s->tf_size;
+    g_ref.tf.layers = 1;
     g_ref.emission.data = s->emission;
     g_ref.emission.w = s->enx;
     g_ref.emission.h = s->eny;

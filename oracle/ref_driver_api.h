@@ -8,6 +8,7 @@ struct RefState {
     FrameInfo frame;
     sampler3D grid;       // gridImage
     sampler3D emission;   // emissionImage (USE_EMISSION variants)
+    sampler1DArray tf;    // transferFunctionTexture (USE_TRANSFER_FUNCTION variants)
     sampler3D sv;         // superVoxelGridImage (RG32F)
     usampler3D svocc;     // superVoxelGridOccupancyImage
     sampler2D env;        // environmentMapTexture

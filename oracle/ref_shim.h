@@ -363,6 +363,26 @@ inline vec4 texture(const sampler2D& s, const vec2& c) {
     int x = (int)fu, y = (int)fv;
     return mix(mix(s.texel(x, y), s.texel(x + 1, y), a), mix(s.texel(x, y + 1), s.texel(x + 1, y + 1), a), b);
 }
+// sampler1DArray (the transfer-function texture): RGBA fp32 rows, one per layer; linear filtering
+// along u with clamp to edge; coordinate (u, layer)
+struct sampler1DArray {
+    const float* data = nullptr;
+    int w = 0, layers = 1;
+    vec4 texel(int x, int layer) const {
+        x = x < 0 ? 0 : (x >= w ? w - 1 : x);
+        const float* q = data + ((size_t)layer * w + x) * 4;
+        return vec4(q[0], q[1], q[2], q[3]);
+    }
+};
+inline vec4 texture(const sampler1DArray& s, const vec2& c) {
+    int layer = (int)floorf(c.y + 0.5f);
+    layer = layer < 0 ? 0 : (layer >= s.layers ? s.layers - 1 : layer);
+    float u = c.x * (float)s.w - 0.5f;
+    float fu = floorf(u);
+    float a = u - fu;
+    int x = (int)fu;
+    return mix(s.texel(x, layer), s.texel(x + 1, layer), a);
+}
 inline vec4 texelFetch(const sampler3D& s, const ivec3& p, int) { return s.texel(p.x, p.y, p.z); }
 inline vec4 texelFetch(const sampler2D& s, const ivec2& p, int lvl) { return s.texel(p.x, p.y, lvl); }
 inline ivec3 textureSize(const sampler3D& s, int) { return ivec3(s.w, s.h, s.d); }

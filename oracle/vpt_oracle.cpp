@@ -544,7 +544,25 @@ struct Tracer {
         float f1 = mixf(f01, f11, fy);
         return mixf(f0, f1, fz);
     }
-    float sample(V3 pos, Rng& r) {
+    // sampleCloud with USE_TRANSFER_FUNCTION (VptUtils.glsl:647-672): the table (a one-row texture,
+    // linear filtering, clamp to edge) at the normalised density; its rgb kept for the absorption
+    V3 tf_rgb = v3(0, 0, 0);
+    float tf_apply(float v) {
+        if (!S.tf) return v;
+        const float u = v * (float)S.tf_size - 0.5f;
+        const float fu = floorf(u);
+        const float a = u - fu;
+        int x0 = (int)fu, x1 = x0 + 1;
+        x0 = x0 < 0 ? 0 : (x0 >= S.tf_size ? S.tf_size - 1 : x0);
+        x1 = x1 < 0 ? 0 : (x1 >= S.tf_size ? S.tf_size - 1 : x1);
+        const float* c0 = S.tf + 4 * x0;
+        const float* c1 = S.tf + 4 * x1;
+        tf_rgb = v3(mixf(c0[0], c1[0], a), mixf(c0[1], c1[1], a), mixf(c0[2], c1[2], a));
+        return mixf(c0[3], c1[3], a);
+    }
+    V3 tf_emission() const { return mul(tf_rgb, S.emission_strength); }
+    float sample(V3 pos, Rng& r) { return tf_apply(sample_raw(pos, r)); }
+    float sample_raw(V3 pos, Rng& r) {
         lookups++;
         if (S.nanovdb) return sample_sparse(pos, r);
         float ux = (pos.x - S.box_min[0]) * S.vox_per_unit[0];
@@ -616,7 +634,8 @@ struct Tracer {
                 float xi = rnd(r);
                 if (xi < absorb * dens) {
                     ev = true;
-                    return v3(0, 0, 0);
+                    // USE_TRANSFER_FUNCTION (DeltaTracking.glsl:293-301)
+                    return S.tf ? tf_emission() : v3(0, 0, 0);
                 }
                 if (xi < dens) {
                     if (S.max_bounces > 0 && ++bounces > S.max_bounces) return v3(0, 0, 0);
@@ -848,8 +867,8 @@ struct Tracer {
                 float xi = rnd(r);
                 if (xi < absorb * dens) {
                     ev = true;
-                    // USE_EMISSION (NextEventTracking.glsl:296-301)
-                    return S.emission ? add(color, emission(x, r)) : color;
+                    // USE_EMISSION (NextEventTracking.glsl:296-301); else USE_TRANSFER_FUNCTION (:303-310)
+                    return S.emission ? add(color, emission(x, r)) : (S.tf ? add(color, tf_emission()) : color);
                 }
                 if (xi < dens) {
                     if (S.max_bounces > 0 && ++bounces > S.max_bounces) return color;
@@ -966,6 +985,12 @@ struct Tracer {
                 float xi = rnd(r);
                 if (xi < pa) {
                     ev = true;
+                    if (S.tf) {  // USE_TRANSFER_FUNCTION (DeltaTracking.glsl:125-127)
+                        const V3 le = tf_emission();
+                        const float den = maj * pa;
+                        return v3(weights.x * sa.x / den * le.x, weights.y * sa.y / den * le.y,
+                                  weights.z * sa.z / den * le.z);
+                    }
                     return v3(0, 0, 0);
                 }
                 if (xi < pa + ps) {
@@ -1001,7 +1026,9 @@ struct Tracer {
                 float t = -m_log(std::max(0.0000000001f, 1.0f - rnd(r))) * (1.0f / maj);
                 if (t > d) break;
                 V3 xn = add(x, mul(w, t));
-                float dens = sample(xn, r);
+                // with a transfer function the reference looks up the previous point x
+                // (NextEventTracking.glsl:74, sampleCloudDensityEmission(x))
+                float dens = sample(S.tf ? x : xn, r);
                 x = xn;
                 V3 sa, ss, sn;
                 float pa, ps, pn;
@@ -1009,8 +1036,8 @@ struct Tracer {
                 float xi = rnd(r);
                 if (xi < pa) {
                     ev = true;
-                    // USE_EMISSION (NextEventTracking.glsl:125-131)
-                    return S.emission ? add(color, emission(x, r)) : color;
+                    // USE_EMISSION (NextEventTracking.glsl:125-131); else USE_TRANSFER_FUNCTION (:133-139)
+                    return S.emission ? add(color, emission(x, r)) : (S.tf ? tf_emission() : color);
                 }
                 if (xi < pa + ps) {
                     if (S.max_bounces > 0 && ++bounces > S.max_bounces) return color;

@@ -67,6 +67,10 @@ typedef struct OracleScene {
     int enx, eny, enz;
     float emission_box_min[3], emission_vox_per_unit[3];
     float emission_cap, emission_strength;
+    /* transfer function (USE_TRANSFER_FUNCTION): tf_size RGBA entries, or NULL; lookups return the
+     * table's alpha at the normalised density, absorptions emit emission_strength * rgb */
+    const float* tf;
+    int tf_size;
 } OracleScene;
 
 /* Renders width*height*num_frames paths; adds radiance (and its square) per pixel (3 doubles). */

@@ -85,7 +85,21 @@ def cases():
         kw2 = dict(base)
         kw2.update(kw)
         out["fbm_" + name] = SceneSpec(grid=fbm, emission=emission, emission_cap=1.6, emission_strength=3.0, **kw2)
+    # transfer function (USE_TRANSFER_FUNCTION): a 64-entry table, transparent below 0.2, a warm ramp
+    for name, kw in {"delta_tf": dict(mode="delta"), "delta_tf_trilinear": dict(mode="delta", interp="trilinear"),
+                     "nee_tf": dict(mode="nee"), "nee_tf_trilinear": dict(mode="nee", interp="trilinear"),
+                     "sdt_hist_tf": dict(mode="spectral_delta", sdt_prob=2, **chroma),
+                     "nees_hist_tf": dict(mode="spectral_nee", sdt_prob=2, **chroma)}.items():
+        kw2 = dict(base)
+        kw2.update(kw)
+        out["fbm_" + name] = SceneSpec(grid=fbm, tf=transfer_function_table(), emission_strength=2.5, **kw2)
     return out
+
+
+def transfer_function_table(n=64):
+    u = (np.arange(n, dtype=np.float64) + 0.5) / n
+    rgba = np.stack([np.clip(1.5 * u, 0, 1), u ** 2, 0.3 * (1 - u), np.clip((u - 0.2) / 0.8, 0, 1) ** 1.5], axis=1)
+    return rgba.astype(np.float32)
 
 
 FIELDS = ["mode", "interp", "extinction", "albedo", "g", "width", "height", "seed_offset", "env", "linear_rgb",
@@ -153,6 +167,8 @@ def main():
             data[name + "__env_rgba"] = np.ascontiguousarray(sp.env_rgba, np.float32)
         if sp.emission is not None:
             data[name + "__emission"] = np.ascontiguousarray(sp.emission, np.float32)
+        if sp.tf is not None:
+            data[name + "__tf"] = np.ascontiguousarray(sp.tf, np.float32)
         meta[name] = {"variant": variant, "grid": key, **{f: (list(getattr(sp, f)) if isinstance(getattr(sp, f), tuple)
                                                  else getattr(sp, f)) for f in FIELDS}}
         print(name, variant, float(paths.mean()))

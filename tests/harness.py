@@ -68,7 +68,7 @@ class SceneSpec:
                  fovy=2.0 * math.atan(0.5), near=0.01, far=100.0, max_grid_extent=0.25, env_rgba=None,
                  use_ess=False, env_intensity=(1.0, 1.0, 1.0), ess_ref_compat=False, lights=None,
                  extinction_base=(1.0, 1.0, 1.0), albedo_rgb=None, sdt_prob=2, emission=None, emission_cap=1.0,
-                 emission_strength=1.0):
+                 emission_strength=1.0, tf=None):
         self.__dict__.update(locals())
         del self.__dict__["self"]
 
@@ -144,6 +144,11 @@ def setup_core(core: Core, sp: SceneSpec):
         core("vpt_set_emission_cap", sp.emission_cap)
         core("vpt_set_emission_strength", sp.emission_strength)
     core("vpt_set_use_emission", 1 if sp.emission is not None else 0)
+    core("vpt_set_emission_strength", sp.emission_strength)
+    if sp.tf is not None:
+        t = np.ascontiguousarray(sp.tf, np.float32)
+        core("vpt_set_transfer_function", t.ctypes.data_as(ctypes.c_void_p), t.shape[0])
+    core("vpt_set_use_transfer_function", 1 if sp.tf is not None else 0)
     core("vpt_set_resolution", sp.width, sp.height)
     core("vpt_set_denoiser", 0)
 
@@ -281,7 +286,11 @@ def oracle_scene(core, sp: SceneSpec, frames: int, frame_count: int = 0) -> brid
         sc.set("emission_vox_per_unit", [float(np.float32(n / (float(b1) - float(b0))))
                                          for n, b0, b1 in zip((enx, eny, enz), ebmin, ebmax)])
         sc.set("emission_cap", float(np.float32(sp.emission_cap)))
-        sc.set("emission_strength", float(np.float32(sp.emission_strength)))
+    sc.set("emission_strength", float(np.float32(sp.emission_strength)))
+    if sp.tf is not None:
+        t = np.ascontiguousarray(sp.tf, np.float32)
+        sc.set("tf", t)
+        sc.set("tf_size", t.shape[0])
     # sun direction normalised exactly like vpt_set_sun (float ops in order)
     d = np.array(sp.sun_dir, np.float32)
     dl = np.sqrt(np.float32(np.float32(d[0] * d[0]) + np.float32(d[1] * d[1])) + np.float32(d[2] * d[2]), dtype=np.float32)
@@ -389,6 +398,11 @@ def reference_scene(sp: SceneSpec, frames: int, frame_start: int = 0, inv=None):
                      ("emission_box_max", ebmax), ("emission_cap", sp.emission_cap),
                      ("emission_strength", sp.emission_strength)):
             sc.set(k, v)
+    sc.set("emission_strength", sp.emission_strength)
+    if sp.tf is not None:
+        t = np.ascontiguousarray(sp.tf, np.float32)
+        sc.set("tf", t)
+        sc.set("tf_size", t.shape[0])
     prob = ["max", "avg", "hist"][sp.sdt_prob]
     tracker = {"delta": "delta", "ratio": "ratio", "decomposition": "decomposition", "rrt": "rrt",
                "nee": "nee_ess" if sp.use_ess else "nee", "spectral_delta": f"sdt_{prob}",
@@ -397,6 +411,8 @@ def reference_scene(sp: SceneSpec, frames: int, frame_start: int = 0, inv=None):
         tracker = f"nee_l{len(sp.lights)}"
     if sp.emission is not None:
         tracker += "_emission"
+    if sp.tf is not None:
+        tracker += "_tf"
     env = {"default": "default", "black": "black", "single": "single", "image": "image"}[sp.env]
     colour = "linear" if (sp.linear_rgb or env != "default") else "srgb"
     return sc, f"{tracker}__{sp.interp}__{env}__{colour}"
@@ -421,6 +437,8 @@ def golden_cases():
             kw["env_rgba"] = z[name + "__env_rgba"]
         if name + "__emission" in z:
             kw["emission"] = z[name + "__emission"]
+        if name + "__tf" in z:
+            kw["tf"] = z[name + "__tf"]
         sp = SceneSpec(**kw)
         out[name] = (sp, list(z[name + "__inv_view_proj"]), z[name + "__paths"], z[name + "__mean8"])
     return out

@@ -157,3 +157,30 @@ def test_emission_grid_with_next_event_tracking():
     assert torch.all(frac <= 1.0 + 1e-6) and torch.allclose(frac * 4, torch.round(frac * 4), atol=1e-5)
     vpt.set_use_emission(False)
     vpt.set_use_builtin_environment_map("Default")
+
+
+def test_transfer_function_table():
+    """set_transfer_function_table / set_use_transfer_function: every density lookup is the table's
+    alpha, so a transparent table under a single-colour sky leaves every delta-tracked path
+    escaping to that colour; load_transfer_function_file names the missing sgl loader."""
+    vpt.set_vpt_mode_from_name("Delta Tracking")
+    vpt.set_use_builtin_environment_map("Single Color")
+    vpt.set_sun([0.3, 0.8, 0.5], [0.6, 0.4, 0.2])
+    t = torch.zeros((3, 32, 32), dtype=torch.float32, device="cuda")
+    vpt.set_use_transfer_function(False)
+    vpt.set_seed_offset(0)
+    cloud = vpt.render_frame(t, 2).clone()
+    table = np.zeros((16, 4), np.float32)
+    table[:, 0] = 1.0
+    vpt.set_transfer_function_table(table)
+    vpt.set_use_transfer_function(True)
+    clear = vpt.render_frame(t, 2)
+    colour = torch.tensor([0.6, 0.4, 0.2], device="cuda")[:, None, None].expand(3, 32, 32)
+    assert torch.allclose(clear, colour, rtol=1e-6)
+    assert not torch.allclose(cloud, colour, rtol=1e-3)
+    with pytest.raises(RuntimeError, match="sgl"):
+        vpt.load_transfer_function_file("any.xml")
+    with pytest.raises(RuntimeError, match="N x 4"):
+        vpt.set_transfer_function_table(np.zeros((4, 3)))
+    vpt.set_use_transfer_function(False)
+    vpt.set_use_builtin_environment_map("Default")
