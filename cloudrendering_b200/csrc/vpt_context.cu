@@ -741,6 +741,8 @@ VptStatus batch_prepare(VptBatch* b, const int* frames, cudaStream_t s, vpt::Bat
             return batch_fail(b, VPT_ERR_UNSUPPORTED,
                               "batched rendering supports delta, ratio and NEE (without empty space skipping)");
         if (features_needed(ctx)) return batch_fail(b, VPT_ERR_UNSUPPORTED, "batched rendering writes no feature maps");
+        if (ctx->use_tf && ctx->tf.ptr)
+            return batch_fail(b, VPT_ERR_UNSUPPORTED, "batched rendering has no transfer-function variant");
         if (ctx->env_kind == VPT_ENV_IMAGE && !ctx->env_pyramid.ptr)
             return batch_fail(b, VPT_ERR_STATE, "environment image not loaded");
         VptStatus st = ensure_accel(ctx, t, s);
@@ -1318,6 +1320,10 @@ VptStatus vpt_render_frames(VptContext* ctx, int frames, void* stream) {
     if (ctx->width <= 0) return fail(ctx, VPT_ERR_STATE, "resolution not set");
     int tracker = tracker_of(ctx->mode);
     if (tracker < 0) return fail(ctx, VPT_ERR_UNSUPPORTED, "VptMode not built in this core");
+    if (ctx->use_tf && ctx->tf.ptr && tracker != vpt::kDelta && tracker != vpt::kNextEvent &&
+        tracker != vpt::kSpectralDelta && tracker != vpt::kSpectralNextEvent)
+        return fail(ctx, VPT_ERR_UNSUPPORTED,
+                    "the transfer function applies to delta, next event and spectral tracking (as in the reference)");
     if (ctx->env_kind == VPT_ENV_IMAGE && !ctx->env_pyramid.ptr)
         return fail(ctx, VPT_ERR_STATE, "environment image not loaded");
     cudaSetDevice(ctx->device);

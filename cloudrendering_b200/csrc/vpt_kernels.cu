@@ -22,7 +22,9 @@ void count_launches(unsigned n) { __atomic_fetch_add(&g_launches, (unsigned long
 unsigned long long launch_count() { return __atomic_load_n(&g_launches, __ATOMIC_RELAXED); }
 
 // Density access of the trackers: the dense texture or the sparse (NanoVDB) volume.
-template <int INTERP, int GRID>
+// TF: transfer-function variant (density = the table's alpha); compiled only where a table is in
+// use, so that the ordinary lookup carries no check of its own
+template <int INTERP, int GRID, bool TF = false>
 struct Sampler {
     const TraceParams& P;
     F3 tf_rgb = {0.0f, 0.0f, 0.0f};  // transfer-function colour of the last lookup
@@ -31,7 +33,7 @@ struct Sampler {
         float v;
         if constexpr (GRID == kNanoVdb) v = sample_sparse<INTERP>(P, pos, rng);
         else v = sample_dense<INTERP>(P, pos, rng);
-        if (P.tf) {  // sampleCloud with USE_TRANSFER_FUNCTION: the table's alpha at the density
+        if constexpr (TF) {  // sampleCloud with USE_TRANSFER_FUNCTION: the table's alpha at the density
             float a;
             tf_lookup(P, v, tf_rgb, a);
             return a;
@@ -207,9 +209,9 @@ VPT_DEV void flush_counters(const TraceParams& P, uint32_t paths, uint32_t looku
     if (guard_hit) atomicOr(P.error_flags, kErrIterLimit);
 }
 
-template <int TRACKER, int INTERP, int GRID>
+template <int TRACKER, int INTERP, int GRID, bool TF>
 __global__ void __launch_bounds__(kTraceBlock) trace_tiles_kernel(const __grid_constant__ TraceParams P, int features) {
-    Sampler<INTERP, GRID> sample{P};
+    Sampler<INTERP, GRID, TF> sample{P};
     uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t frame;
     int px, py;
@@ -223,10 +225,10 @@ __global__ void __launch_bounds__(kTraceBlock) trace_tiles_kernel(const __grid_c
     flush_counters(P, paths, lookups, guard_hit);
 }
 
-template <int TRACKER, int INTERP, int GRID>
+template <int TRACKER, int INTERP, int GRID, bool TF>
 __global__ void __launch_bounds__(kTraceBlock) trace_persistent_kernel(const __grid_constant__ TraceParams P,
                                                                        int features, uint64_t total) {
-    Sampler<INTERP, GRID> sample{P};
+    Sampler<INTERP, GRID, TF> sample{P};
     const int lane = threadIdx.x & 31;
     uint32_t lookups = 0, paths = 0;
     bool guard_hit = false;
@@ -334,7 +336,7 @@ VPT_DEV void flush_counters_to(unsigned long long* counters, int* error_flags, u
     if (guard_hit) atomicOr(error_flags, kErrIterLimit);
 }
 
-template <int TRACKER, int INTERP, int GRID, class SRC>
+template <int TRACKER, int INTERP, int GRID, bool TF, class SRC>
 VPT_DEV void refill_loop(const SRC& src, uint64_t total, unsigned long long* work_counter,
                          unsigned long long* counters, int* error_flags) {
     const unsigned FULL = 0xffffffffu;
@@ -429,7 +431,7 @@ VPT_DEV void refill_loop(const SRC& src, uint64_t total, unsigned long long* wor
 
         // ---- one tentative collision ----
         const TraceParams& P = src.scene(scene);
-        Sampler<INTERP, GRID> sample{P};
+        Sampler<INTERP, GRID, TF> sample{P};
         if (++steps > P.max_steps) {
             guard_hit = true;
             refill_finish<TRACKER>(P, pix, TRACKER == kNextEvent ? color : zero, has);
@@ -533,9 +535,9 @@ VPT_DEV void refill_loop(const SRC& src, uint64_t total, unsigned long long* wor
     flush_counters_to(counters, error_flags, paths, lookups, guard_hit);
 }
 
-template <int TRACKER, int INTERP, int GRID>
+template <int TRACKER, int INTERP, int GRID, bool TF>
 __global__ void __launch_bounds__(kTraceBlock) trace_refill_kernel(const __grid_constant__ TraceParams P, uint64_t total) {
-    refill_loop<TRACKER, INTERP, GRID>(OneScene{P}, total, reinterpret_cast<unsigned long long*>(P.work_counter),
+    refill_loop<TRACKER, INTERP, GRID, TF>(OneScene{P}, total, reinterpret_cast<unsigned long long*>(P.work_counter),
                                        P.counters, P.error_flags);
 }
 
@@ -547,7 +549,7 @@ __global__ void __launch_bounds__(kTraceBlock) trace_batch_kernel(const TracePar
                                                                   const unsigned long long* __restrict__ offsets,
                                                                   int num, unsigned long long* work_counter,
                                                                   unsigned long long* counters, int* error_flags) {
-    refill_loop<TRACKER, INTERP, GRID>(SceneBatch{scenes, offsets, num}, __ldg(offsets + num), work_counter, counters,
+    refill_loop<TRACKER, INTERP, GRID, false>(SceneBatch{scenes, offsets, num}, __ldg(offsets + num), work_counter, counters,
                                        error_flags);
 }
 
@@ -595,12 +597,13 @@ uint64_t padded_paths(int width, int height, uint32_t frames) {
     return tiles * 256ull * frames;
 }
 
-template <int TRACKER, int INTERP, int GRID>
+template <int TRACKER, int INTERP, int GRID, bool TF>
 static int refill_blocks(int requested) {
     if (requested > 0) return requested;
     static int per_sm = 0;
     if (per_sm == 0) {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_refill_kernel<TRACKER, INTERP, GRID>, kTraceBlock, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_refill_kernel<TRACKER, INTERP, GRID, TF>, kTraceBlock,
+                                                      0);
         if (per_sm <= 0) per_sm = 1;
     }
     int dev = 0, sms = 148;
@@ -609,16 +612,16 @@ static int refill_blocks(int requested) {
     return per_sm * sms;
 }
 
-template <int TRACKER, int INTERP, int GRID>
+template <int TRACKER, int INTERP, int GRID, bool TF>
 static cudaError_t launch_trace_t(const TraceParams& P, int schedule, int features, int persistent_blocks,
                                   cudaStream_t stream) {
     uint64_t total = padded_paths(P.width, P.height, P.num_frames);
     constexpr bool kRefillable = TRACKER == kDelta || TRACKER == kRatio || TRACKER == kNextEvent;
     if (schedule == kScheduleRefill && kRefillable && !features) {
         if constexpr (kRefillable) {
-            int blocks = refill_blocks<TRACKER, INTERP, GRID>(persistent_blocks);
+            int blocks = refill_blocks<TRACKER, INTERP, GRID, TF>(persistent_blocks);
             cudaMemsetAsync(P.work_counter, 0, sizeof(unsigned long long), stream);
-            trace_refill_kernel<TRACKER, INTERP, GRID><<<blocks, kTraceBlock, 0, stream>>>(P, total);
+            trace_refill_kernel<TRACKER, INTERP, GRID, TF><<<blocks, kTraceBlock, 0, stream>>>(P, total);
             count_launches(1);
             return cudaGetLastError();
         }
@@ -626,14 +629,14 @@ static cudaError_t launch_trace_t(const TraceParams& P, int schedule, int featur
     if (schedule == kScheduleRefill) schedule = kSchedulePersistent;
     if (schedule == kScheduleTiles) {
         uint64_t blocks = (total + kTraceBlock - 1) / kTraceBlock;
-        trace_tiles_kernel<TRACKER, INTERP, GRID><<<(unsigned)blocks, kTraceBlock, 0, stream>>>(P, features);
+        trace_tiles_kernel<TRACKER, INTERP, GRID, TF><<<(unsigned)blocks, kTraceBlock, 0, stream>>>(P, features);
         count_launches(1);
     } else {
         if (persistent_blocks <= 0) {
             // one wave of resident blocks: SMs x blocks per SM from the occupancy calculator
             static int per_sm = 0;
             if (per_sm == 0) {
-                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_persistent_kernel<TRACKER, INTERP, GRID>,
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_persistent_kernel<TRACKER, INTERP, GRID, TF>,
                                                               kTraceBlock, 0);
                 if (per_sm <= 0) per_sm = 1;
             }
@@ -643,19 +646,34 @@ static cudaError_t launch_trace_t(const TraceParams& P, int schedule, int featur
             persistent_blocks = per_sm * sms;
         }
         cudaMemsetAsync(P.work_counter, 0, sizeof(unsigned long long), stream);
-        trace_persistent_kernel<TRACKER, INTERP, GRID><<<persistent_blocks, kTraceBlock, 0, stream>>>(P, features, total);
+        trace_persistent_kernel<TRACKER, INTERP, GRID, TF><<<persistent_blocks, kTraceBlock, 0, stream>>>(P, features,
+                                                                                                           total);
         count_launches(1);
     }
     return cudaGetLastError();
 }
 
+template <int TRACKER, int GRID, bool TF>
+static cudaError_t launch_interp_tf(const TraceParams& P, int schedule, int features, int pb, cudaStream_t s) {
+    switch (P.interp) {
+        case kNearest: return launch_trace_t<TRACKER, kNearest, GRID, TF>(P, schedule, features, pb, s);
+        case kStochastic: return launch_trace_t<TRACKER, kStochastic, GRID, TF>(P, schedule, features, pb, s);
+        default: return launch_trace_t<TRACKER, kTrilinear, GRID, TF>(P, schedule, features, pb, s);
+    }
+}
+
+// transfer-function variants exist for the trackers whose transfer-function appearance the reference
+// defines (delta, next event and the spectral trackers); the others reject a table
 template <int TRACKER, int GRID>
 static cudaError_t launch_interp(const TraceParams& P, int schedule, int features, int pb, cudaStream_t s) {
-    switch (P.interp) {
-        case kNearest: return launch_trace_t<TRACKER, kNearest, GRID>(P, schedule, features, pb, s);
-        case kStochastic: return launch_trace_t<TRACKER, kStochastic, GRID>(P, schedule, features, pb, s);
-        default: return launch_trace_t<TRACKER, kTrilinear, GRID>(P, schedule, features, pb, s);
+    constexpr int base = TRACKER >= 100 ? TRACKER - 100 : TRACKER;
+    constexpr bool kTfTracker =
+        base == kDelta || base == kNextEvent || base == kSpectralDelta || base == kSpectralNextEvent;
+    if (P.tf) {
+        if constexpr (kTfTracker) return launch_interp_tf<TRACKER, GRID, true>(P, schedule, features, pb, s);
+        else return cudaErrorNotSupported;
     }
+    return launch_interp_tf<TRACKER, GRID, false>(P, schedule, features, pb, s);
 }
 
 cudaError_t launch_trace(const TraceParams& P, int tracker, int use_ess, int schedule, int features,

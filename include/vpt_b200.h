@@ -120,7 +120,8 @@ VptStatus vpt_set_emission_strength(VptContext* ctx, float strength);
  * VptUtils.glsl:629-672, DeltaTracking.glsl, NextEventTracking.glsl): with it on, every density lookup
  * is the table's alpha at the normalised density (linear filtering over `entries` RGBA entries on
  * [0, 1], clamp to edge, as transferFunctionTexture), and an absorption emits emission_strength times
- * the table's rgb (delta and next event tracking, grey and spectral).  The table is the caller's:
+ * the table's rgb (delta and next event tracking, grey and spectral; other trackers and batched
+ * rendering return VPT_ERR_UNSUPPORTED while a table is in use).  The table is the caller's:
  * the reference builds it in sgl's TransferFunctionWindow, which is not part of its source tree. */
 VptStatus vpt_set_transfer_function(VptContext* ctx, const float* rgba, int entries);
 VptStatus vpt_set_use_transfer_function(VptContext* ctx, int use);
