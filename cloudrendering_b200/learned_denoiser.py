@@ -514,7 +514,7 @@ def read_features(vpt, img: torch.Tensor) -> dict:
 
 
 TARGET_FRAME_ORIGIN = 1 << 24  # targets use frames disjoint from the noisy inputs'
-FEATURE_FRAMES = 4  # feature maps are accumulated over the first 4 frames (first-hit features converge fast)
+FEATURE_FRAMES = 2  # feature maps are accumulated over the first 2 frames (first-hit features converge fast)
 
 
 def render_scene_levels(vpt, sc: dict, size: int, spp_levels: Sequence[int], target_spp: int, grid: int = 128,
