@@ -75,6 +75,12 @@ SIGNATURES = {
     "vpt_set_emission_strength": (c_int, [VptCtxP, c_float]),
     "vpt_set_transfer_function": (c_int, [VptCtxP, c_void_p, c_int]),
     "vpt_set_use_transfer_function": (c_int, [VptCtxP, c_int]),
+    "vpt_set_use_isosurfaces": (c_int, [VptCtxP, c_int]),
+    "vpt_set_iso_value": (c_int, [VptCtxP, c_double]),
+    "vpt_set_iso_surface_color": (c_int, [VptCtxP, c_double, c_double, c_double]),
+    "vpt_set_isosurface_type": (c_int, [VptCtxP, c_char_p]),
+    "vpt_set_surface_brdf": (c_int, [VptCtxP, c_char_p]),
+    "vpt_set_num_isosurface_subdivisions": (c_int, [VptCtxP, c_int]),
     "vpt_get_stats": (c_int, [VptCtxP, POINTER(VptStats)]),
     "vpt_reset_stats": (c_int, [VptCtxP]),
     "vpt_synchronize": (c_int, [VptCtxP, c_void_p]),

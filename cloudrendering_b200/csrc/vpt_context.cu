@@ -157,6 +157,11 @@ struct VptContext {
     DevBuf<float> tf;
     int tf_size = 0;
     bool use_tf = false;
+    // isosurfaces (setUseIsosurfaces, setIsoValue, setIsoSurfaceColor; VolumetricPathTracingPass.hpp:382-395)
+    bool use_iso = false;
+    float iso_value = 0.5f;
+    float iso_color[3] = {0.4f, 0.4f, 0.4f};
+    int iso_subdivisions = 2;
     DevBuf<float> minmax;
 
     // sparse (NanoVDB) volume: built from the dense grid when use_sparse is set
@@ -538,7 +543,12 @@ VptStatus fill_params(VptContext* ctx, int tracker, int frames, vpt::TraceParams
     P.inv_sdt_majorant = 1.0f / P.sdt_majorant;
     P.sdt_prob = ctx->sdt_prob;
     P.g = ctx->g;
-    P.interp = ctx->interp;
+    // isosurfaces force trilinear lookups (VolumetricPathTracingPass.cpp:117-120)
+    P.interp = ctx->use_iso ? vpt::kTrilinear : ctx->interp;
+    P.iso = ctx->use_iso ? 1 : 0;
+    P.iso_subdivisions = ctx->iso_subdivisions;
+    P.iso_value = ctx->iso_value;
+    P.iso_color = mk(ctx->iso_color[0], ctx->iso_color[1], ctx->iso_color[2]);
     P.max_bounces = ctx->max_bounces;
     P.max_steps = ctx->max_steps;
     P.ess_ref_compat = ctx->ess_ref_compat;
@@ -743,6 +753,7 @@ VptStatus batch_prepare(VptBatch* b, const int* frames, cudaStream_t s, vpt::Bat
         if (features_needed(ctx)) return batch_fail(b, VPT_ERR_UNSUPPORTED, "batched rendering writes no feature maps");
         if (ctx->use_tf && ctx->tf.ptr)
             return batch_fail(b, VPT_ERR_UNSUPPORTED, "batched rendering has no transfer-function variant");
+        if (ctx->use_iso) return batch_fail(b, VPT_ERR_UNSUPPORTED, "batched rendering has no isosurface variant");
         if (ctx->env_kind == VPT_ENV_IMAGE && !ctx->env_pyramid.ptr)
             return batch_fail(b, VPT_ERR_STATE, "environment image not loaded");
         VptStatus st = ensure_accel(ctx, t, s);
@@ -918,6 +929,55 @@ VptStatus vpt_set_use_transfer_function(VptContext* ctx, int use) {
     VPT_CHECK_CTX(ctx);
     if ((use != 0) != ctx->use_tf) reset_film_state(ctx);
     ctx->use_tf = use != 0;
+    return VPT_OK;
+}
+
+VptStatus vpt_set_use_isosurfaces(VptContext* ctx, int use) {
+    VPT_CHECK_CTX(ctx);
+    if ((use != 0) != ctx->use_iso) reset_film_state(ctx);
+    ctx->use_iso = use != 0;
+    return VPT_OK;
+}
+
+VptStatus vpt_set_iso_value(VptContext* ctx, double value) {
+    VPT_CHECK_CTX(ctx);
+    if (float(value) != ctx->iso_value) reset_film_state(ctx);
+    ctx->iso_value = float(value);
+    return VPT_OK;
+}
+
+VptStatus vpt_set_iso_surface_color(VptContext* ctx, double r, double g, double b) {
+    VPT_CHECK_CTX(ctx);
+    const float c[3] = {float(r), float(g), float(b)};
+    if (c[0] != ctx->iso_color[0] || c[1] != ctx->iso_color[1] || c[2] != ctx->iso_color[2]) reset_film_state(ctx);
+    for (int i = 0; i < 3; ++i) ctx->iso_color[i] = c[i];
+    return VPT_OK;
+}
+
+VptStatus vpt_set_isosurface_type(VptContext* ctx, const char* name) {
+    VPT_CHECK_CTX(ctx);
+    if (!name) return fail(ctx, VPT_ERR_ARG, "null isosurface type");
+    if (strcmp(name, "Density") == 0) return VPT_OK;
+    if (strcmp(name, "Gradient") == 0)
+        return fail(ctx, VPT_ERR_UNSUPPORTED, "gradient-magnitude isosurfaces are not built in this core");
+    return VPT_OK;  // unknown names are ignored, as in the reference
+}
+
+VptStatus vpt_set_surface_brdf(VptContext* ctx, const char* name) {
+    VPT_CHECK_CTX(ctx);
+    if (!name) return fail(ctx, VPT_ERR_ARG, "null surface BRDF");
+    if (strcmp(name, "Lambertian") == 0) return VPT_OK;
+    if (strcmp(name, "Blinn Phong") == 0 || strcmp(name, "Disney (2012)") == 0 || strcmp(name, "Cook Torrance") == 0 ||
+        strcmp(name, "Ambient") == 0)
+        return fail(ctx, VPT_ERR_UNSUPPORTED, "only the Lambertian surface BRDF is built in this core");
+    return VPT_OK;  // unknown names are ignored, as in the reference
+}
+
+VptStatus vpt_set_num_isosurface_subdivisions(VptContext* ctx, int subdivisions) {
+    VPT_CHECK_CTX(ctx);
+    if (subdivisions < 1 || subdivisions > 8) return fail(ctx, VPT_ERR_ARG, "isosurface subdivisions must be in [1, 8]");
+    if (subdivisions != ctx->iso_subdivisions) reset_film_state(ctx);
+    ctx->iso_subdivisions = subdivisions;
     return VPT_OK;
 }
 
@@ -1324,6 +1384,9 @@ VptStatus vpt_render_frames(VptContext* ctx, int frames, void* stream) {
         tracker != vpt::kSpectralDelta && tracker != vpt::kSpectralNextEvent)
         return fail(ctx, VPT_ERR_UNSUPPORTED,
                     "the transfer function applies to delta, next event and spectral tracking (as in the reference)");
+    if (ctx->use_iso && (tracker != vpt::kDelta || ctx->use_sparse || (ctx->use_tf && ctx->tf.ptr)))
+        return fail(ctx, VPT_ERR_UNSUPPORTED,
+                    "isosurfaces are built for delta tracking on dense grids without a transfer function");
     if (ctx->env_kind == VPT_ENV_IMAGE && !ctx->env_pyramid.ptr)
         return fail(ctx, VPT_ERR_STATE, "environment image not loaded");
     cudaSetDevice(ctx->device);

@@ -546,4 +546,92 @@ VPT_DEV F3 density_normal(const TraceParams& P, F3 pos, Rng& rng) {
     return d;
 }
 
+// ---------------------------------------------------------------------------------------------
+// Isosurfaces of the density field (USE_ISOSURFACES with ISOSURFACE_TYPE_DENSITY; dense grids).
+
+// The density texture's linear filter at a normalised texture coordinate (sampleIsoImage,
+// VptUtils.glsl:599; the texels are normalised already).
+VPT_DEV float iso_tex(const TraceParams& P, float cx, float cy, float cz) {
+    return sample_dense_vox<kTrilinear>(P, cx * (float)P.nx, cy * (float)P.ny, cz * (float)P.nz);
+}
+
+// getNearestMultiple (VptUtils.glsl:896-906) with GLSL mod(n, x) = n - x * floor(n / x).
+VPT_DEV float iso_nearest_multiple(float n, float x, bool smaller) {
+    const float rest = n - x * floorf(n / x);
+    if (smaller) return n - rest;
+    if (rest == 0.0f) return n;
+    return x + n - rest;
+}
+
+// trilinearInterpolationDensity (VptUtils.glsl:908-959): the eight lattice points k / (size - 1)
+// around c looked up through the texture filter, blended with the fractions of c * (size - 1).
+VPT_DEV float iso_trilinear(const TraceParams& P, float cx, float cy, float cz) {
+    const float sx = (float)P.nx - 1.0f, sy = (float)P.ny - 1.0f, sz = (float)P.nz - 1.0f;
+    const float dx = 1.0f / sx, dy = 1.0f / sy, dz = 1.0f / sz;
+    const float x0 = iso_nearest_multiple(cx, dx, true), x1 = iso_nearest_multiple(cx, dx, false);
+    const float y0 = iso_nearest_multiple(cy, dy, true), y1 = iso_nearest_multiple(cy, dy, false);
+    const float z0 = iso_nearest_multiple(cz, dz, true), z1 = iso_nearest_multiple(cz, dz, false);
+    const float d000 = iso_tex(P, x0, y0, z0), d100 = iso_tex(P, x1, y0, z0);
+    const float d110 = iso_tex(P, x1, y1, z0), d010 = iso_tex(P, x0, y1, z0);
+    const float d001 = iso_tex(P, x0, y0, z1), d101 = iso_tex(P, x1, y0, z1);
+    const float d111 = iso_tex(P, x1, y1, z1), d011 = iso_tex(P, x0, y1, z1);
+    const float px = cx * sx, py = cy * sy, pz = cz * sz;
+    const float fx = px - floorf(px), fy = py - floorf(py), fz = pz - floorf(pz);
+    const float t00 = mixf(d000, d100, fx), t10 = mixf(d010, d110, fx);
+    const float t01 = mixf(d001, d101, fx), t11 = mixf(d011, d111, fx);
+    return mixf(mixf(t00, t10, fy), mixf(t01, t11, fy), fz);
+}
+
+// Surface normal (computeGradient with DIFFERENCES_NEIGHBOR, VptUtils.glsl:965-984): central
+// differences four lattice spacings apart, (0, 0, 1) when shorter than 1e-3.
+VPT_DEV F3 iso_normal(const TraceParams& P, F3 pos) {
+    const F3 c = (pos - P.box_min) / (P.box_max - P.box_min);
+    const float hx = 4.0f * (1.0f / (float)(P.nx - 1)), hy = 4.0f * (1.0f / (float)(P.ny - 1)),
+                hz = 4.0f * (1.0f / (float)(P.nz - 1));
+    const F3 g = f3(0.5f * (iso_trilinear(P, c.x + hx, c.y, c.z) - iso_trilinear(P, c.x - hx, c.y, c.z)),
+                    0.5f * (iso_trilinear(P, c.x, c.y + hy, c.z) - iso_trilinear(P, c.x, c.y - hy, c.z)),
+                    0.5f * (iso_trilinear(P, c.x, c.y, c.z + hz) - iso_trilinear(P, c.x, c.y, c.z - hz)));
+    const float l = length3(g);
+    if (l < 1e-3f) return f3(0.0f, 0.0f, 1.0f);
+    return f3(g.x / l, g.y / l, g.z / l);
+}
+
+// An opaque Lambertian surface hit (getIsoSurfaceHit, VptUtils.glsl:1151-1334): one random number
+// for the opacity test, the normal turned against the ray, a cosine-weighted direction in the
+// ComputeDefaultBasis frame (RayTracingUtilities.glsl:20-28; Lambertian.glsl is included before
+// UNIFORM_SAMPLING is defined, so the concentric-disk map of VptUtils.glsl:1078-1098 and a pdf factor
+// equal to the cosine), throughput *= color * cos / cos.
+VPT_DEV void iso_scatter(const TraceParams& P, Rng& rng, F3 p, F3& w, F3& weights) {
+    (void)rng_next(rng);  // isoSurfaceOpacity (1) < random() never holds
+    F3 n = iso_normal(P, p);
+    if (dot3(w, n) > 0.0f) n = -n;
+    const float yz = -n.y * n.z;
+    const F3 b = normalize3(fabsf(n.z) > 0.99999f ? f3(-n.x * n.y, 1.0f - n.y * n.y, yz)
+                                                  : f3(-n.x * n.z, yz, 1.0f - n.z * n.z));
+    const F3 t = cross3(b, n);
+    const float xi0 = rng_next(rng);
+    const float xi1 = rng_next(rng);
+    const float ox = 2.0f * xi0 - 1.0f, oy = 2.0f * xi1 - 1.0f;
+    float dx = 0.0f, dy = 0.0f;
+    if (!(ox == 0.0f && oy == 0.0f)) {
+        float rad, th;
+        if (fabsf(ox) > fabsf(oy)) {
+            rad = ox;
+            th = 0.785398185f * (oy / ox);  // pi / 4 in float
+        } else {
+            rad = oy;
+            th = 1.57079637f - 0.785398185f * (ox / oy);  // pi / 2 - pi / 4 * ...
+        }
+        dx = rad * cosf(th);
+        dy = rad * sinf(th);
+    }
+    const float hz = sqrtf(1.0f - dx * dx - dy * dy);
+    const F3 out = f3((t.x * dx + b.x * dy) + n.x * hz, (t.y * dx + b.y * dy) + n.y * hz,
+                      (t.z * dx + b.z * dy) + n.z * hz);
+    const float cosv = dot3(out, n);
+    weights = f3(weights.x * ((P.iso_color.x * cosv) / cosv), weights.y * ((P.iso_color.y * cosv) / cosv),
+                 weights.z * ((P.iso_color.z * cosv) / cosv));
+    w = out;
+}
+
 }  // namespace vpt

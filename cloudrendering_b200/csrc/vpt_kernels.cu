@@ -49,6 +49,8 @@ struct Sampler {
     VPT_DEV F3 normal(F3 pos, Rng& rng) const {
         // getCloudFiniteDifference returns 0 for NanoVDB grids (VptUtils.glsl:726-729)
         if constexpr (GRID == kNanoVdb) return f3(0.0f, 0.0f, 0.0f);
+        // with isosurfaces the normal map is -computeGradient at the first event (Clouds.glsl:274-275)
+        else if (P.iso) return -iso_normal(P, pos);
         else return density_normal<INTERP>(P, pos, rng);
     }
 };
@@ -130,6 +132,7 @@ VPT_DEV void accumulate_features(const TraceParams& P, S& sample, Rng& rng, size
 
 template <int TRACKER, class S>
 VPT_DEV F3 run_tracker(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, FirstEvent& fe, PathCtx& pc) {
+    if constexpr (TRACKER == kDeltaIso) return track_delta_iso(P, sample, rng, x, w, fe, pc);
     if (TRACKER == kDelta) return track_delta(P, sample, rng, x, w, fe, pc);
     if (TRACKER == kRatio) return track_ratio(P, sample, rng, x, w, fe, pc);
     if constexpr (TRACKER == kDecomposition) {
@@ -678,6 +681,11 @@ static cudaError_t launch_interp(const TraceParams& P, int schedule, int feature
 
 cudaError_t launch_trace(const TraceParams& P, int tracker, int use_ess, int schedule, int features,
                          int persistent_blocks, cudaStream_t stream) {
+    if (P.iso) {
+        // isosurfaces: delta tracking on dense grids, trilinear lookups, no transfer function
+        if (tracker != kDelta || P.grid_kind != kDense || P.tf) return cudaErrorNotSupported;
+        return launch_trace_t<kDeltaIso, kTrilinear, kDense, false>(P, schedule, features, persistent_blocks, stream);
+    }
     if (P.grid_kind == kNanoVdb) {
         // sparse grids: the trackers whose density access goes through sampleCloud, and the HDDA
         // decomposition tracker; residual ratio tracking and the occupancy grid are dense-only in the

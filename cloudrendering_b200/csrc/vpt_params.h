@@ -18,6 +18,8 @@ enum Tracker : int {
     kResidualRatio = 4,
     kNextEvent = 5,
     kSpectralNextEvent = 6,
+    // kernel variant, not a VptMode: delta tracking with isosurfaces inside the volume
+    kDeltaIso = 300,
 };
 
 // Collision probabilities of spectral tracking (SpectralDeltaTrackingCollisionProbability,
@@ -172,6 +174,12 @@ struct TraceParams {
     // normalised density; absorptions emit strength * its rgb
     const float* tf;               // tf_size RGBA entries, or null
     int tf_size;
+    // isosurfaces inside the volume (USE_ISOSURFACES with a density field and Lambertian surfaces;
+    // delta tracking with trilinear lookups): surfaces where the normalised density crosses iso_value
+    int iso;
+    int iso_subdivisions;          // checks per free-flight segment (NUM_ISOSURFACE_SUBDIVISIONS)
+    float iso_value;
+    F3 iso_color;
     unsigned long long* counters;  // [0] paths, [1] density lookups
     int* error_flags;
     unsigned int* work_counter;    // persistent-kernel path queue

@@ -86,6 +86,93 @@ VPT_DEV F3 track_delta(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, Fi
     return sky_and_sun(P, w);
 }
 
+// Delta tracking with isosurfaces (DeltaTracking.glsl:168-344 with CheckIsosurfaceHit.glsl): every
+// free-flight segment [x, x_new] is checked at P.iso_subdivisions points for a sign change of
+// density - iso_value against the first point after the last surface event; a crossing is bisected
+// (refineIsoSurfaceHit, VptUtils.glsl:1045-1058, 8 steps), the surface reflects (iso_scatter) and the
+// path restarts from the box boundary; escapes carry the surface throughput; the 1000th loop
+// iteration ends the path with zero.  Trilinear lookups (the reference forces them with isosurfaces).
+template <class S>
+VPT_DEV F3 track_delta_iso(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, FirstEvent& fe, PathCtx& pc) {
+    F3 weights = f3(1.0f, 1.0f, 1.0f);
+    float last_sign = 0.0f;
+    bool first_point = true;
+    const int nsub = P.iso_subdivisions;
+    int it = 0;
+    float tmin, tmax;
+    if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
+        x = x + w * tmin;
+        float d = tmax - tmin;
+        int bounces = 0;
+        while (true) {
+            if (++it == 1000) return f3(0.0f, 0.0f, 0.0f);
+            if (guard(pc)) return f3(0.0f, 0.0f, 0.0f);
+            float t = free_path(rng, P.inv_extinction);
+            if (t > d) break;
+            F3 xn = x + w * t;
+            float density = sample(xn, rng);
+            pc.lookups++;
+            bool hit = false;
+            for (int sub = 0; sub < nsub; ++sub) {
+                const float a0 = (float)sub / (float)nsub, a1 = (float)(sub + 1) / (float)nsub;
+                F3 x0 = x * (1.0f - a0) + xn * a0;
+                F3 x1 = x * (1.0f - a1) + xn * a1;
+                const float v = sample(x1, rng);
+                pc.lookups++;
+                const float v_minus = v - P.iso_value;
+                const float cur_sign = v_minus > 0.0f ? 1.0f : (v_minus < 0.0f ? -1.0f : 0.0f);
+                if (first_point) {
+                    first_point = false;
+                    last_sign = cur_sign;
+                }
+                if (last_sign != cur_sign) {
+                    for (int r = 0; r < 8; ++r) {
+                        const F3 mid = f3((x1.x + x0.x) * 0.5f, (x1.y + x0.y) * 0.5f, (x1.z + x0.z) * 0.5f);
+                        const float vm = sample(mid, rng);
+                        pc.lookups++;
+                        if ((vm - P.iso_value) * cur_sign >= 0.0f) x1 = mid;
+                        else x0 = mid;
+                    }
+                    x = x1;
+                    iso_scatter(P, rng, x, w, weights);
+                    x = x + w * 1e-4f;
+                    first_point = true;
+                    hit = true;
+                    // firstEvent of a surface hit: density = extinction, depth = tMax - d + |x - x1|
+                    record_event(fe, x, 1.0f, P.extinction, tmax - d + length3(x1 - x));
+                    if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
+                        x = x + w * tmin;
+                        d = tmax - tmin;
+                    }
+                    break;
+                }
+            }
+            if (hit) {
+                if (weights.x < 1e-3f && weights.y < 1e-3f && weights.z < 1e-3f) return f3(0.0f, 0.0f, 0.0f);
+                continue;
+            }
+            x = xn;
+            float xi = rng_next(rng);
+            if (xi < P.absorb_albedo * density) {
+                record_event(fe, x, density, P.extinction, tmax - d + t);
+                return f3(0.0f, 0.0f, 0.0f);
+            }
+            if (xi < density) {
+                if (P.max_bounces > 0 && ++bounces > P.max_bounces) return f3(0.0f, 0.0f, 0.0f);
+                w = sample_phase(rng, P.g, w);
+                record_event(fe, x, density, P.extinction, tmax - d + t);
+                if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
+                    x = x + w * tmin;
+                    d = tmax - tmin;
+                }
+            } else {
+                d -= t;
+            }
+        }
+    }
+    return weights * sky_and_sun(P, w);
+}
+
 // VptMode::RATIO_TRACKING: delta tracking that never absorbs and weights each real collision by
 // the single-scattering albedo (ratioTracking, RatioTracking.glsl:26-95).
 template <class S>

@@ -268,6 +268,33 @@ def set_transfer_function_table(rgba) -> None:
     _c("vpt_set_transfer_function", t.ctypes.data_as(ctypes.c_void_p), int(t.shape[0]))
 
 
+# ---- isosurfaces (Module.cpp:1163-1194) ----
+def set_use_isosurfaces(_use_isosurfaces: bool) -> None:
+    _c("vpt_set_use_isosurfaces", 1 if _use_isosurfaces else 0)
+
+
+def set_iso_value(_iso_value: float) -> None:
+    _c("vpt_set_iso_value", float(_iso_value))
+
+
+def set_iso_surface_color(_iso_surface_color) -> None:
+    _c("vpt_set_iso_surface_color", *_vec3(_iso_surface_color, "setIsoSurfaceColor"))
+
+
+def set_isosurface_type(_isosurface_type: str) -> None:
+    """"Density" (the only type built; "Gradient" raises); unknown names are ignored."""
+    _c("vpt_set_isosurface_type", str(_isosurface_type).encode())
+
+
+def set_surface_brdf(_surface_brdf: str) -> None:
+    """"Lambertian" (the only BRDF built; the reference's other names raise); unknown names are ignored."""
+    _c("vpt_set_surface_brdf", str(_surface_brdf).encode())
+
+
+def set_num_isosurface_subdivisions(subdivisions: int) -> None:
+    _c("vpt_set_num_isosurface_subdivisions", int(subdivisions))
+
+
 def load_transfer_function_file(tf_file_path: str) -> None:
     raise RuntimeError("Error in loadTransferFunctionFile: transfer-function files are parsed by sgl's "
                        "TransferFunctionWindow, which this module does not include; pass the table to "

@@ -125,6 +125,22 @@ VptStatus vpt_set_emission_strength(VptContext* ctx, float strength);
  * the reference builds it in sgl's TransferFunctionWindow, which is not part of its source tree. */
 VptStatus vpt_set_transfer_function(VptContext* ctx, const float* rgba, int entries);
 VptStatus vpt_set_use_transfer_function(VptContext* ctx, int use);
+/* Isosurfaces inside the volume (Module.cpp set_use_isosurfaces / set_iso_value / set_iso_surface_color /
+ * set_isosurface_type / set_surface_brdf, src/PyTorch/Module.cpp:1163-1194; USE_ISOSURFACES in
+ * DeltaTracking.glsl and CheckIsosurfaceHit.glsl): the surface where the normalised density crosses
+ * iso_value (default 0.5) is found on every free-flight segment and reflects like an opaque
+ * Lambertian surface of colour iso_surface_color (default 0.4 0.4 0.4); lookups are trilinear while
+ * isosurfaces are on.  Built for delta tracking on dense grids: other trackers, sparse grids, a
+ * transfer function and batched rendering return VPT_ERR_UNSUPPORTED.  Type "Density" and BRDF
+ * "Lambertian" are accepted, "Gradient" and the other BRDF names return VPT_ERR_UNSUPPORTED, unknown
+ * names are ignored (as in the reference).  vpt_set_num_isosurface_subdivisions is the pass's own
+ * setting (VolumetricPathTracingPass.cpp:1028-1033, default 2, 1..8). */
+VptStatus vpt_set_use_isosurfaces(VptContext* ctx, int use);
+VptStatus vpt_set_iso_value(VptContext* ctx, double value);
+VptStatus vpt_set_iso_surface_color(VptContext* ctx, double r, double g, double b);
+VptStatus vpt_set_isosurface_type(VptContext* ctx, const char* name);
+VptStatus vpt_set_surface_brdf(VptContext* ctx, const char* name);
+VptStatus vpt_set_num_isosurface_subdivisions(VptContext* ctx, int subdivisions);
 /* Synthetic scene on the device: seeded fBm of improved Perlin noise, remapped to [0, 1], values
  * below `threshold` set to 0.  No reference counterpart (the reference loads files). */
 VptStatus vpt_generate_fbm_grid(VptContext* ctx, int nx, int ny, int nz, uint32_t seed, int octaves,

@@ -29,6 +29,7 @@ OUT = os.path.join(HERE, "_ref")
 GEN = os.path.join(OUT, "gen")
 REF = os.environ.get("VPT_REFERENCE_ROOT", "/root/reference")
 SHADERS = os.path.join(REF, "Data", "Shaders", "VPT")
+BRDFS = os.path.join(REF, "Data", "Shaders", "BRDF")
 
 # (name, defines) of the tracer variants; the C driver indexes them in this order.
 TRACKERS = {
@@ -59,6 +60,7 @@ SDT_PROB = {"max": "MAX_BASED_PROBABILITY", "avg": "AVG_BASED_PROBABILITY",
 SPECTRAL = {"sdt": "USE_SPECTRAL_DELTA_TRACKING", "nees": "USE_NEXT_EVENT_TRACKING_SPECTRAL"}
 # the Depth Blended / Depth Nearest Opaque feature maps (Clouds.glsl:367-383), deterministic lookups
 DEPTH_MAPS = ["WRITE_DEPTH_BLENDED_MAP", "WRITE_DEPTH_NEAREST_OPAQUE_MAP"]
+ISO = ["USE_ISOSURFACES", "NUM_ISOSURFACE_SUBDIVISIONS=2", "SURFACE_BRDF_LAMBERTIAN", "ISOSURFACE_TYPE_DENSITY"]
 
 
 def variants():
@@ -92,6 +94,11 @@ def variants():
     for t, tdef in SPECTRAL.items():
         out.append((f"{t}_hist_tf__stochastic__default__linear",
                     [tdef, SDT_PROB["hist"], INTERPS["stochastic"], "USE_TRANSFER_FUNCTION"] + ENVS["default__linear"], 0))
+    # isosurfaces inside the volume (USE_ISOSURFACES; VolumetricPathTracingPass.cpp:1737-1768): density
+    # isosurfaces, Lambertian surfaces, 2 subdivisions per free-flight segment, trilinear lookups forced
+    # (VolumetricPathTracingPass.cpp:117-120)
+    out.append(("delta_iso__trilinear__default__linear", TRACKERS["delta"] + [INTERPS["trilinear"]]
+                + ENVS["default__linear"] + ISO, 0))
     return out
 
 
@@ -137,12 +144,14 @@ def transform(text: str) -> str:
 
 def generate() -> None:
     os.makedirs(GEN, exist_ok=True)
-    for f in os.listdir(SHADERS):
-        if f.endswith(".glsl"):
-            with open(os.path.join(SHADERS, f), encoding="utf-8") as fh:
-                text = fh.read()
-            with open(os.path.join(GEN, f + ".inc"), "w") as fh:
-                fh.write(transform(text))
+    # the tracer shaders and the surface BRDFs (Data/Shaders/BRDF, included by the isosurface code)
+    for d in (SHADERS, BRDFS):
+        for f in os.listdir(d):
+            if f.endswith(".glsl"):
+                with open(os.path.join(d, f), encoding="utf-8") as fh:
+                    text = fh.read()
+                with open(os.path.join(GEN, f + ".inc"), "w") as fh:
+                    fh.write(transform(text))
 
 
 def _run(cmd, verbose):

@@ -81,6 +81,8 @@ typedef struct RefScene {
     float emission_box_min[3], emission_box_max[3], emission_cap, emission_strength;
     const float* tf;          /* transferFunctionTexture: tf_size RGBA entries (USE_TRANSFER_FUNCTION variants) */
     int tf_size;
+    float iso_value;          /* parameters.isoValue (USE_ISOSURFACES variants) */
+    float iso_color[3];       /* parameters.isoSurfaceColor */
 } RefScene;
 
 int ref_variant_count(void) { return ref_num_variants; }
@@ -146,6 +148,8 @@ int ref_render(int variant, const RefScene* s, float* out_rgba, int threads) {
     p.emissionBoxMax = vec3(s->emission_box_max[0], s->emission_box_max[1], s->emission_box_max[2]);
     p.emissionCap = s->emission_cap;
     p.emissionStrength = s->emission_strength;
+    p.isoValue = s->iso_value;
+    p.isoSurfaceColor = vec3(s->iso_color[0], s->iso_color[1], s->iso_color[2]);
     g_ref.tf.data = s->tf;
     g_ref.tf.w = s->tf_size;
     g_ref.tf.layers = 1;

@@ -221,6 +221,11 @@ inline bool operator!=(const ivec3& a, const ivec3& b) { return !(a == b); }
 struct mat3 {
     vec3 c[3];
     mat3() {}
+    mat3(const vec3& c0, const vec3& c1, const vec3& c2) {
+        c[0] = c0;
+        c[1] = c1;
+        c[2] = c2;
+    }
 };
 struct mat4 {
     vec4 c[4];
@@ -251,6 +256,8 @@ inline float floor(float v) { return floorf(v); }
 inline vec3 floor(const vec3& v) { return vec3(floorf(v.x), floorf(v.y), floorf(v.z)); }
 inline vec3 ceil(const vec3& v) { return vec3(ceilf(v.x), ceilf(v.y), ceilf(v.z)); }
 inline float fract(float v) { return v - floorf(v); }
+// GLSL mod: x - y * floor(x / y)
+inline float mod(float x, float y) { return x - y * floorf(x / y); }
 inline float min(float a, float b) { return b < a ? b : a; }
 inline float max(float a, float b) { return a < b ? b : a; }
 inline int min(int a, int b) { return b < a ? b : a; }
@@ -356,6 +363,10 @@ inline vec4 texture(const sampler3D& s, const vec3& c) {
                   mix(s.texel(x, y + 1, z + 1), s.texel(x + 1, y + 1, z + 1), a), b);
     return mix(r0, r1, cc);
 }
+// textureOffset: the lookup moved by whole texels
+inline vec4 textureOffset(const sampler3D& s, const vec3& c, const ivec3& o) {
+    return texture(s, vec3(c.x + float(o.x) / float(s.w), c.y + float(o.y) / float(s.h), c.z + float(o.z) / float(s.d)));
+}
 inline vec4 texture(const sampler2D& s, const vec2& c) {
     float u = c.x * (float)s.w - 0.5f, v = c.y * (float)s.h - 0.5f;
     float fu = floorf(u), fv = floorf(v);
@@ -437,6 +448,12 @@ struct Parameters {
     uint isEnvMapBlack;
     vec3 voxelTexelSize;
     float farDistance;
+    // isosurfaces (VptHeader.glsl:88-93)
+    vec3 isoSurfaceColor;
+    float isoValue;
+    float isoStepWidth;
+    float maxAoDist;
+    int numAoSamples;
 };
 struct FrameInfo {
     uint frameCount, globalFrameNumber;

@@ -653,6 +653,169 @@ struct Tracer {
         return sky(w);
     }
 
+    // ---- isosurfaces (USE_ISOSURFACES, ISOSURFACE_TYPE_DENSITY, SURFACE_BRDF_LAMBERTIAN) ----
+    // the isosurface field at a texture coordinate: the density texture's linear filter there
+    // (sampleIsoImage, VptUtils.glsl:599; the texel values are normalised already)
+    float iso_tex(V3 c) const { return at_vox(c.x * (float)S.nx, c.y * (float)S.ny, c.z * (float)S.nz); }
+    // getNearestMultiple (VptUtils.glsl:896-906) with GLSL mod(n, x) = n - x * floor(n / x)
+    static float nearest_multiple(float n, float x, bool smaller) {
+        const float rest = n - x * floorf(n / x);
+        if (smaller) return n - rest;
+        if (rest == 0.0f) return n;
+        return x + n - rest;
+    }
+    // trilinearInterpolationDensity (VptUtils.glsl:908-959): the eight lattice points k / (size - 1)
+    // around c looked up through the texture filter, blended with the fractions of c * (size - 1)
+    float iso_trilinear(V3 c) const {
+        const float dx = 1.0f / ((float)S.nx - 1.0f), dy = 1.0f / ((float)S.ny - 1.0f),
+                    dz = 1.0f / ((float)S.nz - 1.0f);
+        const float x0 = nearest_multiple(c.x, dx, true), x1 = nearest_multiple(c.x, dx, false);
+        const float y0 = nearest_multiple(c.y, dy, true), y1 = nearest_multiple(c.y, dy, false);
+        const float z0 = nearest_multiple(c.z, dz, true), z1 = nearest_multiple(c.z, dz, false);
+        const float d000 = iso_tex(v3(x0, y0, z0)), d100 = iso_tex(v3(x1, y0, z0));
+        const float d110 = iso_tex(v3(x1, y1, z0)), d010 = iso_tex(v3(x0, y1, z0));
+        const float d001 = iso_tex(v3(x0, y0, z1)), d101 = iso_tex(v3(x1, y0, z1));
+        const float d111 = iso_tex(v3(x1, y1, z1)), d011 = iso_tex(v3(x0, y1, z1));
+        const float px = c.x * ((float)S.nx - 1.0f), py = c.y * ((float)S.ny - 1.0f), pz = c.z * ((float)S.nz - 1.0f);
+        const float fx = px - floorf(px), fy = py - floorf(py), fz = pz - floorf(pz);
+        const float t00 = mixf(d000, d100, fx), t10 = mixf(d010, d110, fx);
+        const float t01 = mixf(d001, d101, fx), t11 = mixf(d011, d111, fx);
+        return mixf(mixf(t00, t10, fy), mixf(t01, t11, fy), fz);
+    }
+    // computeGradient with DIFFERENCES_NEIGHBOR (VptUtils.glsl:965-984): central differences four
+    // voxel spacings (1 / (size - 1)) apart, (0, 0, 1) when shorter than 1e-3
+    V3 iso_normal(V3 pos) const {
+        const V3 c = divv(sub(pos, bmin()), sub(bmax(), bmin()));
+        const float hx = 4.0f * (1.0f / (float)(S.nx - 1)), hy = 4.0f * (1.0f / (float)(S.ny - 1)),
+                    hz = 4.0f * (1.0f / (float)(S.nz - 1));
+        const V3 g = v3(0.5f * (iso_trilinear(v3(c.x + hx, c.y, c.z)) - iso_trilinear(v3(c.x - hx, c.y, c.z))),
+                        0.5f * (iso_trilinear(v3(c.x, c.y + hy, c.z)) - iso_trilinear(v3(c.x, c.y - hy, c.z))),
+                        0.5f * (iso_trilinear(v3(c.x, c.y, c.z + hz)) - iso_trilinear(v3(c.x, c.y, c.z - hz))));
+        const float l = length(g);
+        if (l < 1e-3f) return v3(0.0f, 0.0f, 1.0f);
+        return v3(g.x / l, g.y / l, g.z / l);
+    }
+    // refineIsoSurfaceHit (VptUtils.glsl:1045-1058): 8 bisection steps
+    void iso_refine(V3& cur, V3 last, float step_sign, Rng& r) {
+        for (int i = 0; i < 8; i++) {
+            const V3 mid = v3((cur.x + last.x) * 0.5f, (cur.y + last.y) * 0.5f, (cur.z + last.z) * 0.5f);
+            const float v = sample(mid, r);
+            if ((v - S.iso_value) * step_sign >= 0.0f) cur = mid;
+            else last = mid;
+        }
+    }
+    // getIsoSurfaceHit (VptUtils.glsl:1151-1334) for an opaque Lambertian surface: one random number
+    // for the opacity test, normal facing the ray, a direction in the ComputeDefaultBasis frame
+    // (RayTracingUtilities.glsl:20-28), throughput *= color * cos / pdf factor.  Lambertian.glsl is
+    // included (VptUtils.glsl:1121) before UNIFORM_SAMPLING is defined (:1144), so it samples the
+    // cosine-weighted hemisphere through the concentric disk map (VptUtils.glsl:1078-1098) and its
+    // pdf factor is the cosine itself
+    void iso_scatter(V3 p, V3& w, V3& weights, Rng& r) {
+        (void)rnd(r);  // isoSurfaceOpacity (1) < random() never holds
+        V3 n = iso_normal(p);
+        if (dot(w, n) > 0.0f) n = neg(n);
+        const float yz = -n.y * n.z;
+        const V3 b = normalize(fabsf(n.z) > 0.99999f ? v3(-n.x * n.y, 1.0f - n.y * n.y, yz)
+                                                     : v3(-n.x * n.z, yz, 1.0f - n.z * n.z));
+        const V3 t = cross(b, n);
+        const float xi0 = rnd(r), xi1 = rnd(r);
+        const float ox = 2.0f * xi0 - 1.0f, oy = 2.0f * xi1 - 1.0f;
+        float dx = 0.0f, dy = 0.0f;
+        if (!(ox == 0.0f && oy == 0.0f)) {
+            float rad, th;
+            if (fabsf(ox) > fabsf(oy)) {
+                rad = ox;
+                th = 0.785398185f * (oy / ox);  // M_PI / 4 in float
+            } else {
+                rad = oy;
+                th = 1.57079637f - 0.785398185f * (ox / oy);  // M_PI / 2 - M_PI / 4 * ...
+            }
+            dx = rad * cosf(th);
+            dy = rad * sinf(th);
+        }
+        const float hz = sqrtf(1.0f - dx * dx - dy * dy);
+        const V3 out = v3((t.x * dx + b.x * dy) + n.x * hz, (t.y * dx + b.y * dy) + n.y * hz,
+                          (t.z * dx + b.z * dy) + n.z * hz);
+        const float cosv = dot(out, n);
+        weights = v3(weights.x * ((S.iso_color[0] * cosv) / cosv), weights.y * ((S.iso_color[1] * cosv) / cosv),
+                     weights.z * ((S.iso_color[2] * cosv) / cosv));
+        w = out;
+    }
+    // deltaTracking with USE_ISOSURFACES (DeltaTracking.glsl:168-344 with CheckIsosurfaceHit.glsl):
+    // every free-flight segment [x, x_new] is checked at iso_subdivisions points for a sign change of
+    // density - iso_value against the first point after the last surface event; a crossing is
+    // bisected, the surface reflects, the path restarts from the box boundary; escapes carry the
+    // surface throughput; 1000 loop iterations end the path with zero
+    V3 delta_iso(V3 x, V3 w, Rng& r, bool& ev) {
+        float tmin, tmax;
+        const float absorb = 1.0f - S.albedo;
+        V3 weights = v3(1, 1, 1);
+        float last_sign = 0.0f;
+        bool first_point = true;
+        const int nsub = S.iso_subdivisions;
+        int it = 0;
+        if (ray_box(bmin(), bmax(), x, w, tmin, tmax)) {
+            x = add(x, mul(w, tmin));
+            float d = tmax - tmin;
+            int bounces = 0;
+            while (true) {
+                if (++it == 1000) return v3(0, 0, 0);
+                if (guard()) return v3(0, 0, 0);
+                float t = free_path(r);
+                if (t > d) break;
+                V3 xn = add(x, mul(w, t));
+                float dens = sample(xn, r);
+                bool hit = false;
+                for (int sub = 0; sub < nsub; sub++) {
+                    const float a0 = (float)sub / (float)nsub, a1 = (float)(sub + 1) / (float)nsub;
+                    const V3 x0 = add(mul(x, 1.0f - a0), mul(xn, a0));
+                    V3 x1 = add(mul(x, 1.0f - a1), mul(xn, a1));
+                    const float cur_sign = signf(sample(x1, r) - S.iso_value);
+                    if (first_point) {
+                        first_point = false;
+                        last_sign = cur_sign;
+                    }
+                    if (last_sign != cur_sign) {
+                        iso_refine(x1, x0, cur_sign, r);
+                        x = x1;
+                        iso_scatter(x, w, weights, r);
+                        x = add(x, mul(w, 1e-4f));
+                        first_point = true;
+                        hit = true;
+                        ev = true;
+                        if (ray_box(bmin(), bmax(), x, w, tmin, tmax)) {
+                            x = add(x, mul(w, tmin));
+                            d = tmax - tmin;
+                        }
+                        break;
+                    }
+                }
+                if (hit) {
+                    if (weights.x < 1e-3f && weights.y < 1e-3f && weights.z < 1e-3f) return v3(0, 0, 0);
+                    continue;
+                }
+                x = xn;
+                float xi = rnd(r);
+                if (xi < absorb * dens) {
+                    ev = true;
+                    return v3(0, 0, 0);
+                }
+                if (xi < dens) {
+                    if (S.max_bounces > 0 && ++bounces > S.max_bounces) return v3(0, 0, 0);
+                    w = sample_phase(r, S.g, w);
+                    ev = true;
+                    if (ray_box(bmin(), bmax(), x, w, tmin, tmax)) {
+                        x = add(x, mul(w, tmin));
+                        d = tmax - tmin;
+                    }
+                } else {
+                    d -= t;
+                }
+            }
+        }
+        return mulv(weights, sky(w));
+    }
+
     // ratioTracking (RatioTracking.glsl:26-95)
     V3 ratio(V3 x, V3 w, Rng& r, bool& ev) {
         float trans = 1.0f, tmin, tmax;
@@ -1365,7 +1528,7 @@ struct Tracer {
         camera_ray(S, sx, sy, x, w);
         bool ev = false;
         switch (S.mode) {
-            case 0: return delta(x, w, r, ev);
+            case 0: return S.use_iso ? delta_iso(x, w, r, ev) : delta(x, w, r, ev);
             case 1: return spectral_delta(x, w, r, ev);
             case 6: return spectral_nee(x, w, r, ev);
             case 2: return ratio(x, w, r, ev);

@@ -71,6 +71,13 @@ typedef struct OracleScene {
      * table's alpha at the normalised density, absorptions emit emission_strength * rgb */
     const float* tf;
     int tf_size;
+    /* isosurfaces (USE_ISOSURFACES with ISOSURFACE_TYPE_DENSITY and SURFACE_BRDF_LAMBERTIAN; delta
+     * tracking, trilinear lookups): surfaces where the normalised density crosses iso_value, checked
+     * at iso_subdivisions points of every free-flight segment, reflecting with albedo iso_color */
+    int use_iso;
+    float iso_value;
+    float iso_color[3];
+    int iso_subdivisions;
 } OracleScene;
 
 /* Renders width*height*num_frames paths; adds radiance (and its square) per pixel (3 doubles). */

@@ -93,6 +93,14 @@ def cases():
         kw2 = dict(base)
         kw2.update(kw)
         out["fbm_" + name] = SceneSpec(grid=fbm, tf=transfer_function_table(), emission_strength=2.5, **kw2)
+    # isosurfaces inside the volume (USE_ISOSURFACES, density field, Lambertian surfaces, delta tracking
+    # with trilinear lookups): the reference's default surface, and a thinner medium with a coloured one
+    for name, kw in {"delta_iso": dict(iso_value=0.5),
+                     "delta_iso_coloured": dict(iso_value=0.3, iso_color=(0.9, 0.6, 0.3), extinction=40.0,
+                                                albedo=0.9, g=0.2)}.items():
+        kw2 = dict(base)
+        kw2.update(kw)
+        out["fbm_" + name] = SceneSpec(grid=fbm, mode="delta", interp="trilinear", iso=True, **kw2)
     return out
 
 
@@ -105,7 +113,7 @@ def transfer_function_table(n=64):
 FIELDS = ["mode", "interp", "extinction", "albedo", "g", "width", "height", "seed_offset", "env", "linear_rgb",
           "sun_dir", "sun_intensity", "cam_pos", "cam_target", "fovy", "near", "far", "max_grid_extent", "use_ess",
           "env_intensity", "max_bounces", "ess_ref_compat", "lights", "extinction_base", "albedo_rgb", "sdt_prob",
-          "emission_cap", "emission_strength"]
+          "emission_cap", "emission_strength", "iso", "iso_value", "iso_color"]
 
 
 def depth_map_cases():

@@ -68,7 +68,7 @@ class SceneSpec:
                  fovy=2.0 * math.atan(0.5), near=0.01, far=100.0, max_grid_extent=0.25, env_rgba=None,
                  use_ess=False, env_intensity=(1.0, 1.0, 1.0), ess_ref_compat=False, lights=None,
                  extinction_base=(1.0, 1.0, 1.0), albedo_rgb=None, sdt_prob=2, emission=None, emission_cap=1.0,
-                 emission_strength=1.0, tf=None):
+                 emission_strength=1.0, tf=None, iso=False, iso_value=0.5, iso_color=(0.4, 0.4, 0.4)):
         self.__dict__.update(locals())
         del self.__dict__["self"]
 
@@ -149,6 +149,9 @@ def setup_core(core: Core, sp: SceneSpec):
         t = np.ascontiguousarray(sp.tf, np.float32)
         core("vpt_set_transfer_function", t.ctypes.data_as(ctypes.c_void_p), t.shape[0])
     core("vpt_set_use_transfer_function", 1 if sp.tf is not None else 0)
+    core("vpt_set_use_isosurfaces", 1 if sp.iso else 0)
+    core("vpt_set_iso_value", sp.iso_value)
+    core("vpt_set_iso_surface_color", *[float(c) for c in sp.iso_color])
     core("vpt_set_resolution", sp.width, sp.height)
     core("vpt_set_denoiser", 0)
 
@@ -291,6 +294,12 @@ def oracle_scene(core, sp: SceneSpec, frames: int, frame_count: int = 0) -> brid
         t = np.ascontiguousarray(sp.tf, np.float32)
         sc.set("tf", t)
         sc.set("tf_size", t.shape[0])
+    if sp.iso:
+        sc.set("use_iso", 1)
+        sc.set("iso_subdivisions", 2)
+        sc.set("interp", 2)
+    sc.set("iso_value", float(np.float32(sp.iso_value)))
+    sc.set("iso_color", [float(np.float32(c)) for c in sp.iso_color])
     # sun direction normalised exactly like vpt_set_sun (float ops in order)
     d = np.array(sp.sun_dir, np.float32)
     dl = np.sqrt(np.float32(np.float32(d[0] * d[0]) + np.float32(d[1] * d[1])) + np.float32(d[2] * d[2]), dtype=np.float32)
@@ -413,6 +422,10 @@ def reference_scene(sp: SceneSpec, frames: int, frame_start: int = 0, inv=None):
         tracker += "_emission"
     if sp.tf is not None:
         tracker += "_tf"
+    sc.set("iso_value", sp.iso_value)
+    sc.set("iso_color", sp.iso_color)
+    if sp.iso:
+        tracker += "_iso"
     env = {"default": "default", "black": "black", "single": "single", "image": "image"}[sp.env]
     colour = "linear" if (sp.linear_rgb or env != "default") else "srgb"
     return sc, f"{tracker}__{sp.interp}__{env}__{colour}"

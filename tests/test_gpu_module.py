@@ -184,3 +184,43 @@ def test_transfer_function_table():
         vpt.set_transfer_function_table(np.zeros((4, 3)))
     vpt.set_use_transfer_function(False)
     vpt.set_use_builtin_environment_map("Default")
+
+
+def test_isosurfaces():
+    """set_use_isosurfaces and its settings: an iso value above every density finds no surface, so
+    the image equals the trilinear render without isosurfaces bit for bit; a surface inside the cloud
+    changes it; the types, BRDFs and trackers that are not built raise."""
+    vpt.set_vpt_mode_from_name("Delta Tracking")
+    vpt.set_grid_interpolation("Trilinear")
+    vpt.set_extinction_scale(100.0)  # paths well below the 1000-iteration cap of the isosurface loop
+    t = torch.zeros((3, 32, 32), dtype=torch.float32, device="cuda")
+    vpt.set_use_isosurfaces(False)
+    vpt.set_seed_offset(0)
+    plain = vpt.render_frame(t, 2).clone()
+    vpt.set_isosurface_type("Density")
+    vpt.set_surface_brdf("Lambertian")
+    vpt.set_iso_surface_color([0.8, 0.5, 0.3])
+    vpt.set_iso_value(2.0)
+    vpt.set_use_isosurfaces(True)
+    vpt.set_seed_offset(0)
+    none_found = vpt.render_frame(t, 2).clone()
+    assert torch.equal(none_found, plain)
+    vpt.set_iso_value(0.3)
+    vpt.set_seed_offset(0)
+    surf = vpt.render_frame(t, 2).clone()
+    assert torch.isfinite(surf).all()
+    assert not torch.allclose(surf, plain, rtol=1e-3)
+    with pytest.raises(RuntimeError, match="not built"):
+        vpt.set_isosurface_type("Gradient")
+    with pytest.raises(RuntimeError, match="Lambertian"):
+        vpt.set_surface_brdf("Cook Torrance")
+    with pytest.raises(RuntimeError):
+        vpt.set_iso_surface_color([0.1, 0.2])
+    vpt.set_vpt_mode_from_name("Next Event Tracking")
+    with pytest.raises(RuntimeError, match="delta tracking"):
+        vpt.render_frame(t, 1)
+    vpt.set_use_isosurfaces(False)
+    vpt.set_iso_value(0.5)
+    vpt.set_vpt_mode_from_name("Delta Tracking")
+    vpt.set_grid_interpolation("Stochastic")
+    vpt.set_extinction_scale(1024.0)
