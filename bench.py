@@ -260,8 +260,11 @@ def run_ours(args):
 
     # per tracker: one warm-up frame, then 2 steps of TRACKER_SPP frames
     per_tracker = {}
-    for name, mode in TRACKERS.items():
+    # delta tracking with isosurfaces at density 0.5 (Lambertian surfaces, trilinear lookups) last
+    for name, mode in list(TRACKERS.items()) + [("delta_isosurfaces", 0)]:
         vpt.set_vpt_mode(mode)
+        vpt.set_use_isosurfaces(name == "delta_isosurfaces")
+        vpt.set_iso_value(0.5)
         vpt.render_frame(img, 1)
         barrier()
         vpt.reset_stats()
@@ -277,6 +280,7 @@ def run_ours(args):
                              "lookups_per_path": s2["density_lookups"] / max(1, s2["paths"]),
                              "lookups_per_s": s2["density_lookups"] * world / (ms / 1e3),
                              "ms_per_step": ms / 2, "spp_per_step": TRACKER_SPP}
+    vpt.set_use_isosurfaces(False)
 
     # schedule comparison for delta tracking (the reason the refill schedule is the default)
     schedules = {}
