@@ -117,8 +117,13 @@ VPT_DEV F3 track_delta_iso(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w
                 const float a0 = (float)sub / (float)nsub, a1 = (float)(sub + 1) / (float)nsub;
                 F3 x0 = x * (1.0f - a0) + xn * a0;
                 F3 x1 = x * (1.0f - a1) + xn * a1;
-                const float v = sample(x1, rng);
-                pc.lookups++;
+                // the last check point is x_new itself (a1 = 1: x * 0 + x_new): its density was just
+                // looked up, and the trilinear lookup draws no random number, so it is reused
+                float v = density;
+                if (sub != nsub - 1) {
+                    v = sample(x1, rng);
+                    pc.lookups++;
+                }
                 const float v_minus = v - P.iso_value;
                 const float cur_sign = v_minus > 0.0f ? 1.0f : (v_minus < 0.0f ? -1.0f : 0.0f);
                 if (first_point) {
