@@ -358,6 +358,12 @@ VPT_DEV void refill_loop(const SRC& src, uint64_t total, unsigned long long* wor
     float shadow_dist = 0.0f, shadow_max = 0.0f;  // distance walked / light distance (light shadow rays)
     int mode = kModePrimary, bounces = 0, light = -1;
     bool ev = false;
+    // isosurface state (kDeltaIso): surface throughput, sign at the first point after the last event,
+    // loop iterations of the path
+    F3 iw = f3(1.0f, 1.0f, 1.0f);
+    float iso_last = 0.0f;
+    bool iso_first = true;
+    int iso_it = 0;
     int scene = 0;
     uint32_t steps = 0;
     size_t pix = 0;
@@ -407,6 +413,9 @@ VPT_DEV void refill_loop(const SRC& src, uint64_t total, unsigned long long* wor
                     color = zero;
                     ev = false;
                     mode = kModePrimary;
+                    iw = f3(1.0f, 1.0f, 1.0f);
+                    iso_first = true;
+                    iso_it = 0;
                     float tmin, tmax;
                     has = true;
                     if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
@@ -435,6 +444,10 @@ VPT_DEV void refill_loop(const SRC& src, uint64_t total, unsigned long long* wor
         // ---- one tentative collision ----
         const TraceParams& P = src.scene(scene);
         Sampler<INTERP, GRID, TF> sample{P};
+        if (TRACKER == kDeltaIso && ++iso_it == 1000) {
+            refill_finish<TRACKER>(P, pix, zero, has);
+            continue;
+        }
         if (++steps > P.max_steps) {
             guard_hit = true;
             refill_finish<TRACKER>(P, pix, TRACKER == kNextEvent ? color : zero, has);
@@ -451,6 +464,14 @@ VPT_DEV void refill_loop(const SRC& src, uint64_t total, unsigned long long* wor
             F3 xn = x + w * t;
             density = sample(xn, rng);
             lookups++;
+            if constexpr (TRACKER == kDeltaIso) {
+                float tmax_unused = 0.0f;
+                if (iso_segment(P, sample, rng, x, xn, density, w, d, tmax_unused, iw, iso_last, iso_first, lookups,
+                                nullptr)) {
+                    if (iw.x < 1e-3f && iw.y < 1e-3f && iw.z < 1e-3f) refill_finish<TRACKER>(P, pix, zero, has);
+                    continue;
+                }
+            }
             x = xn;
         }
         if (TRACKER == kNextEvent && mode == kModeShadow) {
@@ -466,6 +487,7 @@ VPT_DEV void refill_loop(const SRC& src, uint64_t total, unsigned long long* wor
             F3 L;
             if (TRACKER == kNextEvent) L = ev ? color : color + sky_and_sun(P, w);
             else if (TRACKER == kRatio) L = sky_and_sun(P, w) * trans;
+            else if (TRACKER == kDeltaIso) L = iw * sky_and_sun(P, w);
             else L = sky_and_sun(P, w);
             refill_finish<TRACKER>(P, pix, L, has);
             continue;
@@ -619,7 +641,7 @@ template <int TRACKER, int INTERP, int GRID, bool TF>
 static cudaError_t launch_trace_t(const TraceParams& P, int schedule, int features, int persistent_blocks,
                                   cudaStream_t stream) {
     uint64_t total = padded_paths(P.width, P.height, P.num_frames);
-    constexpr bool kRefillable = TRACKER == kDelta || TRACKER == kRatio || TRACKER == kNextEvent;
+    constexpr bool kRefillable = TRACKER == kDelta || TRACKER == kRatio || TRACKER == kNextEvent || TRACKER == kDeltaIso;
     if (schedule == kScheduleRefill && kRefillable && !features) {
         if constexpr (kRefillable) {
             int blocks = refill_blocks<TRACKER, INTERP, GRID, TF>(persistent_blocks);

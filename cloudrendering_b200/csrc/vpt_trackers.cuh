@@ -86,18 +86,67 @@ VPT_DEV F3 track_delta(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, Fi
     return sky_and_sun(P, w);
 }
 
+// One free-flight segment [x, x_new] of delta tracking with isosurfaces (CheckIsosurfaceHit.glsl):
+// P.iso_subdivisions check points for a sign change of density - iso_value against the first point
+// after the last surface event; a crossing is bisected (refineIsoSurfaceHit, VptUtils.glsl:1045-1058,
+// 8 steps), the surface reflects (iso_scatter), the path moves 1e-4 off it and restarts from the box
+// boundary.  Returns true on a surface event (x, w, d, tmax and weights updated; the first event
+// recorded when `fe` is given).  The last check point is x_new itself (a1 = 1: x * 0 + x_new), whose
+// density was just looked up; trilinear lookups draw no random number, so it is reused.
+template <class S>
+VPT_DEV bool iso_segment(const TraceParams& P, S& sample, Rng& rng, F3& x, F3 xn, float density, F3& w, float& d,
+                         float& tmax, F3& weights, float& last_sign, bool& first_point, uint32_t& lookups,
+                         FirstEvent* fe) {
+    const int nsub = P.iso_subdivisions;
+    for (int sub = 0; sub < nsub; ++sub) {
+        const float a0 = (float)sub / (float)nsub, a1 = (float)(sub + 1) / (float)nsub;
+        F3 x0 = x * (1.0f - a0) + xn * a0;
+        F3 x1 = x * (1.0f - a1) + xn * a1;
+        float v = density;
+        if (sub != nsub - 1) {
+            v = sample(x1, rng);
+            lookups++;
+        }
+        const float v_minus = v - P.iso_value;
+        const float cur_sign = v_minus > 0.0f ? 1.0f : (v_minus < 0.0f ? -1.0f : 0.0f);
+        if (first_point) {
+            first_point = false;
+            last_sign = cur_sign;
+        }
+        if (last_sign != cur_sign) {
+            for (int r = 0; r < 8; ++r) {
+                const F3 mid = f3((x1.x + x0.x) * 0.5f, (x1.y + x0.y) * 0.5f, (x1.z + x0.z) * 0.5f);
+                const float vm = sample(mid, rng);
+                lookups++;
+                if ((vm - P.iso_value) * cur_sign >= 0.0f) x1 = mid;
+                else x0 = mid;
+            }
+            x = x1;
+            iso_scatter(P, rng, x, w, weights);
+            x = x + w * 1e-4f;
+            first_point = true;
+            // firstEvent of a surface hit: density = extinction, depth = tMax - d + |x - x1|
+            if (fe) record_event(*fe, x, 1.0f, P.extinction, tmax - d + length3(x1 - x));
+            float tmin;
+            if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
+                x = x + w * tmin;
+                d = tmax - tmin;
+            }
+            return true;
+        }
+    }
+    return false;
+}
+
 // Delta tracking with isosurfaces (DeltaTracking.glsl:168-344 with CheckIsosurfaceHit.glsl): every
-// free-flight segment [x, x_new] is checked at P.iso_subdivisions points for a sign change of
-// density - iso_value against the first point after the last surface event; a crossing is bisected
-// (refineIsoSurfaceHit, VptUtils.glsl:1045-1058, 8 steps), the surface reflects (iso_scatter) and the
-// path restarts from the box boundary; escapes carry the surface throughput; the 1000th loop
-// iteration ends the path with zero.  Trilinear lookups (the reference forces them with isosurfaces).
+// free-flight segment goes through iso_segment; escapes carry the surface throughput; weights below
+// 1e-3 in every channel end the path after a surface event; the 1000th loop iteration ends the path
+// with zero.  Trilinear lookups (the reference forces them with isosurfaces).
 template <class S>
 VPT_DEV F3 track_delta_iso(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, FirstEvent& fe, PathCtx& pc) {
     F3 weights = f3(1.0f, 1.0f, 1.0f);
     float last_sign = 0.0f;
     bool first_point = true;
-    const int nsub = P.iso_subdivisions;
     int it = 0;
     float tmin, tmax;
     if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
@@ -112,47 +161,8 @@ VPT_DEV F3 track_delta_iso(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w
             F3 xn = x + w * t;
             float density = sample(xn, rng);
             pc.lookups++;
-            bool hit = false;
-            for (int sub = 0; sub < nsub; ++sub) {
-                const float a0 = (float)sub / (float)nsub, a1 = (float)(sub + 1) / (float)nsub;
-                F3 x0 = x * (1.0f - a0) + xn * a0;
-                F3 x1 = x * (1.0f - a1) + xn * a1;
-                // the last check point is x_new itself (a1 = 1: x * 0 + x_new): its density was just
-                // looked up, and the trilinear lookup draws no random number, so it is reused
-                float v = density;
-                if (sub != nsub - 1) {
-                    v = sample(x1, rng);
-                    pc.lookups++;
-                }
-                const float v_minus = v - P.iso_value;
-                const float cur_sign = v_minus > 0.0f ? 1.0f : (v_minus < 0.0f ? -1.0f : 0.0f);
-                if (first_point) {
-                    first_point = false;
-                    last_sign = cur_sign;
-                }
-                if (last_sign != cur_sign) {
-                    for (int r = 0; r < 8; ++r) {
-                        const F3 mid = f3((x1.x + x0.x) * 0.5f, (x1.y + x0.y) * 0.5f, (x1.z + x0.z) * 0.5f);
-                        const float vm = sample(mid, rng);
-                        pc.lookups++;
-                        if ((vm - P.iso_value) * cur_sign >= 0.0f) x1 = mid;
-                        else x0 = mid;
-                    }
-                    x = x1;
-                    iso_scatter(P, rng, x, w, weights);
-                    x = x + w * 1e-4f;
-                    first_point = true;
-                    hit = true;
-                    // firstEvent of a surface hit: density = extinction, depth = tMax - d + |x - x1|
-                    record_event(fe, x, 1.0f, P.extinction, tmax - d + length3(x1 - x));
-                    if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
-                        x = x + w * tmin;
-                        d = tmax - tmin;
-                    }
-                    break;
-                }
-            }
-            if (hit) {
+            if (iso_segment(P, sample, rng, x, xn, density, w, d, tmax, weights, last_sign, first_point, pc.lookups,
+                            &fe)) {
                 if (weights.x < 1e-3f && weights.y < 1e-3f && weights.z < 1e-3f) return f3(0.0f, 0.0f, 0.0f);
                 continue;
             }
