@@ -33,7 +33,6 @@ UNIT = "path samples/s"
 GRID = 512
 RES = 1024
 SPP_PER_STEP = 64
-TRACKER_SPP = 4  # per-tracker rates are measured on 4-spp steps
 MAX_BOUNCES = 128
 EXTINCTION = 1000.0
 SEED = 2
@@ -258,29 +257,10 @@ def run_ours(args):
     achieved = (lookups / args.steps) * BYTES_PER_LOOKUP / (ms_per_launch / 1e3) / 1e9
     peak, peak_kind = peaks()
 
-    # per tracker: one warm-up frame, then 2 steps of TRACKER_SPP frames
-    per_tracker = {}
-    # delta tracking with isosurfaces at density 0.5 (Lambertian surfaces, trilinear lookups) last
-    for name, mode in list(TRACKERS.items()) + [("delta_isosurfaces", 0)]:
-        vpt.set_vpt_mode(mode)
-        vpt.set_use_isosurfaces(name == "delta_isosurfaces")
-        vpt.set_iso_value(0.5)
-        vpt.render_frame(img, 1)
-        barrier()
-        vpt.reset_stats()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(2):
-            _lib.check(lib.vpt_render_frames(ctx, TRACKER_SPP, ctypes_stream), "render", ctx)
-        e1.record(stream)
-        barrier()
-        ms = max_over_ranks(e0.elapsed_time(e1))
-        s2 = vpt.get_stats()
-        per_tracker[name] = {"path_samples_per_s": RES * RES * TRACKER_SPP * 2 * world / (ms / 1e3),
-                             "lookups_per_path": s2["density_lookups"] / max(1, s2["paths"]),
-                             "lookups_per_s": s2["density_lookups"] * world / (ms / 1e3),
-                             "ms_per_step": ms / 2, "spp_per_step": TRACKER_SPP}
-    vpt.set_use_isosurfaces(False)
+    # per tracker: rates on 64-spp steps and the error of each tracker's image against an
+    # FP64-accumulated 16384-spp delta-tracking render of the same scene
+    per_tracker, reference_render = run_trackers(vpt, lib, ctx, img, stream, ctypes_stream, barrier, max_over_ranks,
+                                                 world, args.workload == "small")
 
     # schedule comparison for delta tracking (the reason the refill schedule is the default)
     schedules = {}
@@ -291,11 +271,11 @@ def run_ours(args):
         barrier()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        _lib.check(lib.vpt_render_frames(ctx, TRACKER_SPP, ctypes_stream), "render", ctx)
+        _lib.check(lib.vpt_render_frames(ctx, SPP_PER_STEP, ctypes_stream), "render", ctx)
         e1.record(stream)
         barrier()
         ms = max_over_ranks(e0.elapsed_time(e1))
-        schedules[label] = RES * RES * TRACKER_SPP * world / (ms / 1e3)
+        schedules[label] = RES * RES * SPP_PER_STEP * world / (ms / 1e3)
     _lib.check(lib.vpt_set_option(ctx, b"schedule", 2.0), "schedule", ctx)
 
     # end to end through the public API: host grid -> device, render, result -> host
@@ -348,7 +328,7 @@ def run_ours(args):
             "lookups_per_s": lookups / (ms_total / 1e3) * world,
             "lookups_per_path": lookups / max(1, st["paths"]),
             "gather_roofline": gather_roofline,
-            "per_tracker": per_tracker, "schedules_delta": schedules, "e2e": e2e, "gpu_launches": int(launches), "clocks": clock_info,
+            "per_tracker": per_tracker, "tracker_reference_render": reference_render, "schedules_delta": schedules, "e2e": e2e, "gpu_launches": int(launches), "clocks": clock_info,
         }
         if cpu is not None:
             line["cpu_baseline"] = cpu
@@ -363,6 +343,102 @@ def run_ours(args):
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+TRACKER_STEPS = 4  # 4 steps of SPP_PER_STEP frames: 256 spp per tracker
+REF_SPP = 16384
+REF_FRAME_ORIGIN = 1 << 28  # the reference render's frames are disjoint from the trackers'
+RELMSE_EPS = 1e-2
+
+
+def film_moments_f64(lib, ctx, n, stream):
+    """(sum, sum of squares) of the accumulated frames' radiance, float64 [H*W*3] on the GPU."""
+    import ctypes
+    import torch
+    from cloudrendering_b200 import _lib
+    s = torch.empty(n * 3, dtype=torch.float64, device="cuda")
+    q = torch.empty_like(s)
+    _lib.check(lib.vpt_read_statistics(ctx, ctypes.c_void_p(s.data_ptr()), ctypes.c_void_p(q.data_ptr()), 1,
+                                       ctypes.c_void_p(stream.cuda_stream)), "statistics", ctx)
+    return s, q
+
+
+def run_trackers(vpt, lib, ctx, img, stream, ctypes_stream, barrier, max_over_ranks, world, small):
+    """Each tracker on the bench scene: TRACKER_STEPS timed steps of SPP_PER_STEP frames (path samples/s,
+    density lookups/s), then its image (TRACKER_STEPS * SPP_PER_STEP spp) against the FP64 16384-spp
+    delta-tracking render: relMSE = mean((x - ref)^2 / (ref^2 + RELMSE_EPS)) over pixels and channels,
+    and per-pixel z-scores (x - ref) / sqrt(var_x / n_x + var_ref / n_ref) from each render's own
+    per-pixel sample variance, with the image mean's deviation in standard errors."""
+    import torch
+    from cloudrendering_b200 import _lib
+    ref_spp = 1024 if small else REF_SPP
+    n_pix = RES * RES
+    vpt.set_vpt_mode_from_name("Delta Tracking")
+    vpt.set_use_isosurfaces(False)
+    vpt.set_collect_statistics(True)
+    t0 = time.perf_counter()
+    vpt.set_frame_index(REF_FRAME_ORIGIN)
+    left = ref_spp
+    while left > 0:
+        k = min(256, left)
+        _lib.check(lib.vpt_render_frames(ctx, k, ctypes_stream), "render", ctx)
+        left -= k
+    rs, rq = film_moments_f64(lib, ctx, n_pix, stream)
+    torch.cuda.synchronize()
+    ref_s = time.perf_counter() - t0
+    ref_mean = rs / ref_spp
+    ref_var = torch.clamp(rq / ref_spp - ref_mean * ref_mean, min=0.0) * (ref_spp / (ref_spp - 1))
+    out = {}
+    spp = TRACKER_STEPS * SPP_PER_STEP
+    # delta tracking with isosurfaces at density 0.5 (Lambertian surfaces, trilinear lookups) is a
+    # different image: its rate only
+    for name, mode in list(TRACKERS.items()) + [("delta_isosurfaces", 0)]:
+        iso = name == "delta_isosurfaces"
+        vpt.set_vpt_mode(mode)
+        vpt.set_use_isosurfaces(iso)
+        vpt.set_iso_value(0.5)
+        vpt.set_frame_index(0)
+        _lib.check(lib.vpt_render_frames(ctx, 1, ctypes_stream), "warm-up", ctx)
+        vpt.set_frame_index(0)
+        barrier()
+        vpt.reset_stats()
+        steps = 1 if iso else TRACKER_STEPS
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            _lib.check(lib.vpt_render_frames(ctx, SPP_PER_STEP, ctypes_stream), "render", ctx)
+        e1.record(stream)
+        barrier()
+        ms = max_over_ranks(e0.elapsed_time(e1))
+        st = vpt.get_stats()
+        row = {"path_samples_per_s": n_pix * SPP_PER_STEP * steps * world / (ms / 1e3),
+               "lookups_per_path": st["density_lookups"] / max(1, st["paths"]),
+               "lookups_per_s": st["density_lookups"] * world / (ms / 1e3),
+               "ms_per_step": ms / steps, "spp_per_step": SPP_PER_STEP}
+        if not iso:
+            s, q = film_moments_f64(lib, ctx, n_pix, stream)
+            m = s / spp
+            var = torch.clamp(q / spp - m * m, min=0.0) * (spp / (spp - 1))
+            rel = float(((m - ref_mean) ** 2 / (ref_mean ** 2 + RELMSE_EPS)).mean())
+            se = torch.sqrt(var / spp + ref_var / ref_spp)
+            z = torch.where(se > 0, (m - ref_mean) / torch.where(se > 0, se, torch.ones_like(se)),
+                            torch.zeros_like(se))
+            mc = m.view(-1, 3).mean(dim=0)
+            rc = ref_mean.view(-1, 3).mean(dim=0)
+            se_mean = torch.sqrt(var.view(-1, 3).mean(dim=0) / (spp * n_pix)
+                                 + ref_var.view(-1, 3).mean(dim=0) / (ref_spp * n_pix))
+            row.update({"spp": spp, "relmse_vs_fp64_16k": rel, "relmse_eps": RELMSE_EPS,
+                        "max_abs_z_vs_fp64_16k": float(z.abs().max()),
+                        "image_mean_dev_in_se": float(((mc - rc).abs() / se_mean).max()),
+                        "image_mean": [float(v) for v in mc]})
+        out[name] = row
+    vpt.set_use_isosurfaces(False)
+    vpt.set_collect_statistics(False)
+    vpt.set_frame_index(0)
+    reference = {"tracker": "delta", "spp": ref_spp, "accumulation": "fp64", "seconds": ref_s,
+                 "image_mean": [float(v) for v in ref_mean.view(-1, 3).mean(dim=0)],
+                 "z_bound_note": f"Bonferroni |z| < 6 over {n_pix * 3} pixel-channels"}
+    return out, reference
 
 
 # Learned denoiser: a kernel-predicting U-Net (widths 32-64-96-128-160, 13x13 kernels) trained on the
@@ -744,22 +820,20 @@ def cpu_baseline(lib, ctx, vpt, target_s=12.0):
                       sun_dir=[float(f32(sd[i] / dl)) for i in range(3)], sun_intensity=[5.0] * 3,
                       sky_color=[0.2] * 3, env_intensity=[1.0] * 3, density=dens)
     threads = os.cpu_count() or 1
-    rows = 32
-    row0 = RES // 2 - rows // 2
+    # the whole image (the GPU arm's pixel mix) at as many spp as fit in about target_s
     frames, elapsed, lookups = 1, 0.0, 0
     while True:
         sc.set("num_frames", frames)
         t0 = time.perf_counter()
-        _, lookups = sc.render_rows(row0, row0 + rows, threads)
+        _, _, lookups = sc.render(threads)
         elapsed = time.perf_counter() - t0
         if elapsed >= target_s / 3 or frames >= 4096:
             break
         frames = min(4096, max(frames * 2, int(frames * target_s / max(elapsed, 1e-3))))
-    paths = rows * RES * frames
+    paths = RES * RES * frames
     return {"value": paths / elapsed, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"delta tracking, rows {row0}..{row0 + rows} of the {RES}x{RES} image x {frames} spp "
-                      f"({paths} paths, {elapsed:.1f} s, {lookups / elapsed:.3g} lookups/s)",
-            "lookups_per_path": lookups / paths}
+            "sample": f"delta tracking, the whole {RES}x{RES} image x {frames} spp ({paths} paths, {elapsed:.1f} s)",
+            "lookups_per_s": lookups / elapsed, "lookups_per_path": lookups / paths}
 
 
 def run_reference(args):
@@ -788,20 +862,23 @@ def run_reference(args):
                       env_kind=3, use_linear_rgb=1, env_image_linear=1, sun_dir=sd.tolist(), sun_intensity=[5.0] * 3,
                       sky_color=[0.2] * 3, env_intensity=[1.0] * 3, density=dens)
     threads = os.cpu_count() or 1
-    rows = 8
-    row0 = RES // 2 - rows // 2
-    for _ in range(args.warmup):
-        sc.render_rows(row0, row0 + 2, threads)
+    # each step: the whole image at 1 spp (the GPU arm's pixel mix), frame index = step
+    sc.set("num_frames", 1)
+    for i in range(args.warmup):
+        sc.set("frame_count", 1000 + i)
+        sc.render_rows(RES // 2 - 4, RES // 2 + 4, threads)
     times = []
     lookups = 0
-    for _ in range(args.steps):
+    for i in range(args.steps):
+        sc.set("frame_count", i)
         t0 = time.perf_counter()
-        _, lookups = sc.render_rows(row0, row0 + rows, threads)
+        _, _, lk = sc.render(threads)
         times.append(time.perf_counter() - t0)
+        lookups += lk
     total = sum(times)
-    paths = rows * RES * args.steps
+    paths = RES * RES * args.steps
     value = paths / total
-    sample = f"delta tracking, {rows} rows x {RES} px at 1 spp per step (center band), {threads} threads"
+    sample = f"delta tracking, the whole {RES}x{RES} image at 1 spp per step, {threads} threads"
     print(json.dumps({
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": total / args.steps * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -809,8 +886,32 @@ def run_reference(args):
         "impl": "reference",
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "lookups_per_path": lookups / (rows * RES),
+        "lookups_per_s": lookups / total, "lookups_per_path": lookups / paths,
     }), flush=True)
+
+
+def profile_trace(spp):
+    """Two launches of the delta tracker on the bench scene (1 frame, then `spp` frames) for ncu:
+    `ncu -k regex:trace_refill -s 1 -c 1 ... python bench.py --profile-trace SPP` captures the second."""
+    import torch
+    from cloudrendering_b200 import vpt, _lib
+    torch.cuda.set_device(0)
+    lib = _lib.load()
+    vpt.initialize()
+    ctx = vpt.context_handle()
+    setup_scene(vpt, 0)
+    vpt.set_vpt_mode_from_name("Delta Tracking")
+    _lib.check(lib.vpt_set_resolution(ctx, RES, RES), "resolution", ctx)
+    cs = __import__("ctypes").c_void_p(torch.cuda.current_stream().cuda_stream)
+    for frames in (1, spp):
+        _lib.check(lib.vpt_synchronize(ctx, cs), "sync", ctx)
+        vpt.reset_stats()
+        _lib.check(lib.vpt_render_frames(ctx, frames, cs), "render", ctx)
+    _lib.check(lib.vpt_synchronize(ctx, cs), "sync", ctx)
+    st = vpt.get_stats()
+    print(json.dumps({"profile_trace": {"grid": GRID, "image": RES, "spp": spp, "paths": st["paths"],
+                                        "density_lookups": st["density_lookups"]}}), flush=True)
+    vpt.cleanup()
 
 
 def main():
@@ -823,19 +924,24 @@ def main():
     ap.add_argument("--no-sparse", action="store_true", help="skip the NanoVDB sparse configuration")
     ap.add_argument("--no-batch", action="store_true", help="skip the 64-scene batched configuration")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-denoiser configuration")
+    ap.add_argument("--profile-trace", type=int, default=0, metavar="SPP",
+                    help="profiling entry: set up the bench scene, render one warm-up frame, then one launch of "
+                         "SPP frames of delta tracking, and exit (capture the second trace launch with ncu)")
     ap.add_argument("--workload", choices=["full", "small"], default="full",
                     help="small: 384^3 grid, 512^2, 4 spp/step (for ncu captures; not a bench line)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.workload == "small":
-        global GRID, RES, SPP_PER_STEP, TRACKER_SPP
-        GRID, RES, SPP_PER_STEP, TRACKER_SPP = 384, 512, 4, 1
+        global GRID, RES, SPP_PER_STEP
+        GRID, RES, SPP_PER_STEP = 384, 512, 4
         args.no_cpu_baseline = True
         global SPARSE_DIMS, SPARSE_RES, BATCH_SCENES
         SPARSE_DIMS, SPARSE_RES = (512, 256, 384), (480, 270)
         BATCH_SCENES = 8
-    if args.impl == "reference":
+    if args.profile_trace:
+        profile_trace(args.profile_trace)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

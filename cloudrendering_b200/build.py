@@ -7,7 +7,7 @@ so the library only needs the NVIDIA driver at run time.
 
 A second library, ``libvpt_b200_dr.so``, is the same core with the tracer's transcendental functions
 evaluated in double precision and rounded once to float (``-DVPT_DOUBLE_ROUNDED_MATH`` on
-``vpt_kernels.cu``).  The parity tests use it to compare paths one by one with the CPU oracle in the
+the tracer units ``vpt_kernels.cu`` and ``vpt_trace_*.cu``).  The parity tests use it to compare paths one by one with the CPU oracle in the
 same mode; the default library is the product.
 """
 from __future__ import annotations
@@ -28,13 +28,16 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", INCLUDE, "-I", CSRC]
 # The tracer is compiled without FMA contraction so that its arithmetic matches the CPU oracle
 # operation by operation (see the conventions at the top of vpt_device.cuh).
-PER_FILE = {
-    "vpt_kernels.cu": ["--fmad=false"],
-    "vpt_kpn.cu": ["--fmad=false"],
-    "vpt_denoise.cu": ["--fmad=false"],
-}
-# sources that hold the tracer's transcendental calls (built twice, see above)
-DOUBLE_ROUNDED = {"vpt_kernels.cu"}
+NO_FMA = {"vpt_kernels.cu", "vpt_kpn.cu", "vpt_denoise.cu"}
+
+
+def _is_tracer(src: str) -> bool:
+    """The tracer's units: the launchers and the per-family kernel instantiations (vpt_trace_*.cu)."""
+    return src == "vpt_kernels.cu" or src.startswith("vpt_trace_")
+
+
+def _per_file(src: str) -> list[str]:
+    return ["--fmad=false"] if src in NO_FMA or _is_tracer(src) else []
 
 
 def _nvcc() -> str:
@@ -66,14 +69,14 @@ def build(verbose: bool = False, force: bool = False) -> str:
     def add(src, obj, extra):
         deps = [os.path.join(CSRC, src)] + headers
         if force or _needs_rebuild(obj, deps):
-            jobs.append([nvcc, *ARCH, *COMMON, *PER_FILE.get(src, []), *extra, "-c", os.path.join(CSRC, src),
+            jobs.append([nvcc, *ARCH, *COMMON, *_per_file(src), *extra, "-c", os.path.join(CSRC, src),
                          "-o", obj])
 
     for src in _sources():
         obj = os.path.join(BUILD, src[:-3] + ".o")
         add(src, obj, [])
         objs.append(obj)
-        if src in DOUBLE_ROUNDED:
+        if _is_tracer(src):  # the sources that hold the tracer's transcendental calls (built twice)
             obj_dr = os.path.join(BUILD, src[:-3] + "_dr.o")
             add(src, obj_dr, ["-DVPT_DOUBLE_ROUNDED_MATH"])
             objs_dr.append(obj_dr)

@@ -2000,6 +2000,9 @@ VptStatus vpt_eaw_denoise_rgba(const float* color, const float* position, const 
     if (!color || !out || width <= 0 || height <= 0 || iterations < 0) return VPT_ERR_ARG;
     cudaStream_t s = as_stream(stream);
     size_t bytes = (size_t)width * height * 4 * sizeof(float);
+    if (vpt::image_ranges_overlap(out, color, bytes) || vpt::image_ranges_overlap(out, position, bytes) ||
+        vpt::image_ranges_overlap(out, normal, bytes))
+        return VPT_ERR_ARG;
     if (iterations == 0) {
         return cudaMemcpyAsync(out, color, bytes, cudaMemcpyDeviceToDevice, s) == cudaSuccess ? VPT_OK : VPT_ERR_CUDA;
     }

@@ -708,6 +708,9 @@ extern "C" VptStatus vpt_eaw_denoise_rgba_noalloc(const float* color, const floa
     if ((long long)width * (long long)height > vpt::kEawNoAllocMaxPixels) return VPT_ERR_ARG;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const size_t bytes = (size_t)width * height * 4 * sizeof(float);
+    if (vpt::image_ranges_overlap(out, color, bytes) || vpt::image_ranges_overlap(out, position, bytes) ||
+        vpt::image_ranges_overlap(out, normal, bytes))
+        return VPT_ERR_ARG;
     if (iterations == 0) {
         return cudaMemcpyAsync(out, color, bytes, cudaMemcpyDeviceToDevice, s) == cudaSuccess ? VPT_OK : VPT_ERR_CUDA;
     }

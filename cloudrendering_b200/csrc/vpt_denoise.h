@@ -43,6 +43,15 @@ struct SvgfState {
 
 void svgf_release(SvgfState& s);
 
+// True when the byte ranges [a, a + bytes) and [b, b + bytes) overlap (b may be nullptr).  The EAW
+// entry points reject an output image that overlaps one of their inputs: an odd iteration count
+// writes the first pass into the output while the same launch still reads the inputs.
+inline bool image_ranges_overlap(const void* a, const void* b, size_t bytes) {
+    if (!a || !b) return false;
+    const uintptr_t x = reinterpret_cast<uintptr_t>(a), y = reinterpret_cast<uintptr_t>(b);
+    return x < y + bytes && y < x + bytes;
+}
+
 // One EAW pass chain on an RGBA image.  position/normal are RGBA images or nullptr (weights off).
 cudaError_t eaw_denoise(const float* color_rgba, const float* position_rgba, const float* normal_rgba, int width,
                         int height, const EawSettings& s, float* ping, float* pong, float** result,

@@ -1,0 +1,722 @@
+// vpt_trace.cuh - the tracer kernels and their launch templates, shared by the vpt_trace_*.cu
+// units.  Each unit instantiates the kernels of one tracker family (launch_tracker below), so
+// that the families compile in parallel; vpt_kernels.cu dispatches to them (launch_trace).
+//
+//  * trace kernels: one camera path per thread; TRACKER x INTERP x GRID x TF are template
+//    parameters (the reference selects them with shader #defines, VolumetricPathTracingPass.cpp:
+//    1558-1782).  Three schedules: a plain grid over 16x16 pixel tiles, a persistent grid whose
+//    warps pull 32-path batches from a global counter, and the per-lane refill loop.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "vpt_device.cuh"
+#include "vpt_trackers.cuh"
+#include "vpt_kernels.h"
+
+namespace vpt {
+
+
+// Density access of the trackers: the dense texture or the sparse (NanoVDB) volume.
+// TF: transfer-function variant (density = the table's alpha); compiled only where a table is in
+// use, so that the ordinary lookup carries no check of its own
+template <int INTERP, int GRID, bool TF = false>
+struct Sampler {
+    const TraceParams& P;
+    F3 tf_rgb = {0.0f, 0.0f, 0.0f};  // transfer-function colour of the last lookup
+    static constexpr bool kSparse = GRID == kNanoVdb;
+    // a lookup that draws no random number and reads the density itself (trilinear, dense, no
+    // transfer function): two lookups at one point return the same value
+    static constexpr bool kRepeatable = INTERP == kTrilinear && GRID != kNanoVdb && !TF;
+    VPT_DEV float operator()(F3 pos, Rng& rng) {
+        float v;
+        if constexpr (GRID == kNanoVdb) v = sample_sparse<INTERP>(P, pos, rng);
+        else v = sample_dense<INTERP>(P, pos, rng);
+        if constexpr (TF) {  // sampleCloud with USE_TRANSFER_FUNCTION: the table's alpha at the density
+            float a;
+            tf_lookup(P, v, tf_rgb, a);
+            return a;
+        }
+        return v;
+    }
+    // transfer-function emission of the last lookup (parameters.emissionStrength * densityEmission.rgb)
+    VPT_DEV F3 tf_emission() const {
+        return f3(P.emission_strength * tf_rgb.x, P.emission_strength * tf_rgb.y, P.emission_strength * tf_rgb.z);
+    }
+    // the emission grid is dense whatever the density grid is
+    VPT_DEV F3 emission(F3 pos, Rng& rng) const { return sample_emission<INTERP>(P, pos, rng); }
+    VPT_DEV F3 normal(F3 pos, Rng& rng) const {
+        // getCloudFiniteDifference returns 0 for NanoVDB grids (VptUtils.glsl:726-729)
+        if constexpr (GRID == kNanoVdb) return f3(0.0f, 0.0f, 0.0f);
+        // with isosurfaces the normal map is -computeGradient at the first event (Clouds.glsl:274-275)
+        else if (P.iso) return -iso_normal(P, pos);
+        else return density_normal<INTERP>(P, pos, rng);
+    }
+};
+
+// Depth Blended (DepthBlended.glsl) / Depth Nearest Opaque (DepthNearestOpaque.glsl): a march along
+// the camera ray in steps of 0.25 / the largest grid dimension (0.001 for NanoVDB grids) with
+// alpha = 1 - exp(-density * extinction * step), stopping past the box or above 0.999 accumulated
+// alpha A.  Blended: (sum of (1 - A) alpha t / max(A, 1e-5), A); nearest: (t of the last step with
+// alpha > 1e-5, times A; A).  Lookups continue the path's random stream (stochastic interpolation).
+template <bool NEAREST, class S>
+VPT_DEV void depth_march(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, float& depth_out, float& alpha_out) {
+    const float step = S::kSparse ? 0.001f : 0.25f / (float)max(P.nx, max(P.ny, P.nz));
+    const float atten = P.extinction * step;
+    float acc_depth = 0.0f, acc_alpha = 0.0f, nearest = 0.0f;
+    float tmin, tmax;
+    if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
+        float t = tmin;
+        while (true) {
+            t += step;
+            if (t > tmax || acc_alpha > 0.999f) break;
+            const float density = sample(x + w * t, rng);
+            const float alpha = 1.0f - expf(-density * atten);
+            if (!NEAREST) acc_depth = acc_depth + (1.0f - acc_alpha) * alpha * t;
+            acc_alpha = acc_alpha + (1.0f - acc_alpha) * alpha;
+            if (NEAREST && alpha > 1e-5f) nearest = t;
+        }
+    }
+    depth_out = NEAREST ? nearest * acc_alpha : acc_depth / fmaxf(acc_alpha, 1e-5f);
+    alpha_out = acc_alpha;
+}
+
+// Per-path feature accumulation (Clouds.glsl:148-256): position of the first event, depth,
+// density, albedo-weighted hit flag, primary-ray transmittance proxy and, when requested, the
+// background (Clouds.glsl:162-170: sampleSkybox of the camera ray for paths with an event, the
+// path's radiance otherwise).
+template <class S>
+VPT_DEV void accumulate_features(const TraceParams& P, S& sample, Rng& rng, size_t pix, const FirstEvent& fe,
+                                 F3 result, F3 x_camera, F3 w_camera) {
+    float* f = P.feat + pix * kFeatStride;
+    if (P.feat_background) {
+        const F3 bg = fe.has ? sky_only(P, w_camera) : result;
+        atomicAdd(f + kFeatBackground + 0, bg.x);
+        atomicAdd(f + kFeatBackground + 1, bg.y);
+        atomicAdd(f + kFeatBackground + 2, bg.z);
+    }
+    if (fe.has) {
+        F3 n = sample.normal(fe.x, rng);
+        atomicAdd(f + kFeatNormal + 0, n.x);
+        atomicAdd(f + kFeatNormal + 1, n.y);
+        atomicAdd(f + kFeatNormal + 2, n.z);
+        atomicAdd(f + kFeatPos + 0, fe.x.x);
+        atomicAdd(f + kFeatPos + 1, fe.x.y);
+        atomicAdd(f + kFeatPos + 2, fe.x.z);
+        atomicAdd(f + kFeatPos + 3, 1.0f);
+        atomicAdd(f + kFeatDepth + 0, fe.depth);
+        atomicAdd(f + kFeatDepth + 1, fe.depth * fe.depth);
+        atomicAdd(f + kFeatDensity + 0, fe.density * 0.001f);
+        atomicAdd(f + kFeatDensity + 1, (fe.density * fe.density * 0.001f) * 0.001f);
+        atomicAdd(f + kFeatCloudOnly + 0, result.x);
+        atomicAdd(f + kFeatCloudOnly + 1, result.y);
+        atomicAdd(f + kFeatCloudOnly + 2, result.z);
+    } else {
+        atomicAdd(f + kFeatTrans, 1.0f);
+    }
+    // after the normal, in the reference's order (Clouds.glsl:367-383)
+    if (P.feat_depth_maps & 1) {
+        float d, a;
+        depth_march<false>(P, sample, rng, x_camera, w_camera, d, a);
+        atomicAdd(f + kFeatDepthBlended + 0, d);
+        atomicAdd(f + kFeatDepthBlended + 1, a);
+    }
+    if (P.feat_depth_maps & 2) {
+        float d, a;
+        depth_march<true>(P, sample, rng, x_camera, w_camera, d, a);
+        atomicAdd(f + kFeatDepthNearest + 0, d);
+        atomicAdd(f + kFeatDepthNearest + 1, a);
+    }
+}
+
+template <int TRACKER, class S>
+VPT_DEV F3 run_tracker(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, FirstEvent& fe, PathCtx& pc) {
+    if constexpr (TRACKER == kDeltaIso) return track_delta_iso(P, sample, rng, x, w, fe, pc);
+    if (TRACKER == kDelta) return track_delta(P, sample, rng, x, w, fe, pc);
+    if (TRACKER == kRatio) return track_ratio(P, sample, rng, x, w, fe, pc);
+    if constexpr (TRACKER == kDecomposition) {
+        if constexpr (S::kSparse) return track_decomposition_sparse(P, sample, rng, x, w, fe, pc);
+        else return track_decomposition(P, sample, rng, x, w, fe, pc);
+    }
+    if (TRACKER == kResidualRatio) return track_residual_ratio(P, sample, rng, x, w, fe, pc);
+    if constexpr (TRACKER == kSpectralDelta) return track_delta_spectral(P, sample, rng, x, w, fe, pc);
+    if constexpr (TRACKER == kSpectralNextEvent) return track_nee_spectral<false>(P, sample, rng, x, w, fe, pc);
+    if constexpr (TRACKER == kSpectralNextEvent + 100) return track_nee_spectral<true>(P, sample, rng, x, w, fe, pc);
+    if (TRACKER == kNextEvent + 100) return track_nee<true>(P, sample, rng, x, w, fe, pc);
+    return track_nee<false>(P, sample, rng, x, w, fe, pc);
+}
+
+// Maps a path index to (frame, x, y): 16x16 pixel tiles, tiles row-major, frames outermost, so a
+// warp traces a 16x2 pixel strip of one frame (coherent primary rays).
+VPT_DEV bool decode_path(const TraceParams& P, uint64_t p, uint32_t& frame, int& x, int& y) {
+    const uint32_t tiles_x = (uint32_t)(P.width + 15) >> 4;
+    const uint32_t tiles_y = (uint32_t)(P.height + 15) >> 4;
+    const uint64_t per_frame = (uint64_t)tiles_x * tiles_y * 256u;
+    frame = (uint32_t)(p / per_frame);
+    uint32_t q = (uint32_t)(p - (uint64_t)frame * per_frame);
+    uint32_t tile = q >> 8, within = q & 255u;
+    x = (int)((tile % tiles_x) * 16u + (within & 15u));
+    y = (int)((tile / tiles_x) * 16u + (within >> 4));
+    return frame < P.num_frames && x < P.width && y < P.height;
+}
+
+// One camera path: seed (Clouds.glsl:80-84), jittered NDC (Clouds.glsl:86), tracker, film.
+template <int TRACKER, class S>
+VPT_DEV void trace_one(const TraceParams& P, S& sample, uint32_t frame, int px, int py, bool features,
+                       uint32_t& lookups, bool& guard_hit) {
+    const uint32_t w_u = (uint32_t)P.width, h_u = (uint32_t)P.height;
+    uint32_t seed = (P.global_frame + frame) * w_u * h_u + (uint32_t)px + (uint32_t)py * w_u;
+    seed += P.seed_offset;
+    Rng rng = rng_init(seed);
+    float rx = rng_next(rng);
+    float ry = rng_next(rng);
+    float sx = (2.0f * ((float)px + rx)) / (float)P.width - 1.0f;
+    float sy = (2.0f * ((float)py + ry)) / (float)P.height - 1.0f;
+    F3 x, w;
+    camera_ray(P, sx, sy, x, w);
+    FirstEvent fe;
+    fe.has = false;
+    PathCtx pc;
+    pc.steps = 0;
+    pc.max_steps = P.max_steps;
+    pc.lookups = 0;
+    pc.guard_hit = false;
+    F3 L = run_tracker<TRACKER>(P, sample, rng, x, w, fe, pc);
+    const size_t pix = (size_t)py * P.width + px;
+    atomicAdd(P.film + pix * 3 + 0, (double)L.x);
+    atomicAdd(P.film + pix * 3 + 1, (double)L.y);
+    atomicAdd(P.film + pix * 3 + 2, (double)L.z);
+    if (P.film_sq) {
+        atomicAdd(P.film_sq + pix * 3 + 0, (double)L.x * (double)L.x);
+        atomicAdd(P.film_sq + pix * 3 + 1, (double)L.y * (double)L.y);
+        atomicAdd(P.film_sq + pix * 3 + 2, (double)L.z * (double)L.z);
+    }
+    if (features) accumulate_features(P, sample, rng, pix, fe, L, x, w);
+    lookups += pc.lookups;
+    guard_hit |= pc.guard_hit;
+}
+
+VPT_DEV void flush_counters(const TraceParams& P, uint32_t paths, uint32_t lookups, bool guard_hit) {
+    unsigned long long l = lookups;
+    unsigned long long n = paths;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        l += __shfl_xor_sync(0xffffffffu, l, o);
+        n += __shfl_xor_sync(0xffffffffu, n, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(P.counters + 0, n);
+        atomicAdd(P.counters + 1, l);
+    }
+    if (guard_hit) atomicOr(P.error_flags, kErrIterLimit);
+}
+
+template <int TRACKER, int INTERP, int GRID, bool TF>
+__global__ void __launch_bounds__(kTraceBlock) trace_tiles_kernel(const __grid_constant__ TraceParams P, int features) {
+    Sampler<INTERP, GRID, TF> sample{P};
+    uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t frame;
+    int px, py;
+    uint32_t lookups = 0, paths = 0;
+    bool guard_hit = false;
+    if (decode_path(P, p, frame, px, py)) {
+        trace_one<TRACKER>(P, sample, frame, px, py, features != 0, lookups, guard_hit);
+        paths = 1;
+    }
+    __syncwarp();
+    flush_counters(P, paths, lookups, guard_hit);
+}
+
+template <int TRACKER, int INTERP, int GRID, bool TF>
+__global__ void __launch_bounds__(kTraceBlock) trace_persistent_kernel(const __grid_constant__ TraceParams P,
+                                                                       int features, uint64_t total) {
+    Sampler<INTERP, GRID, TF> sample{P};
+    const int lane = threadIdx.x & 31;
+    uint32_t lookups = 0, paths = 0;
+    bool guard_hit = false;
+    while (true) {
+        unsigned long long base = 0;
+        if (lane == 0) base = atomicAdd(reinterpret_cast<unsigned long long*>(P.work_counter), 32ull);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= total) break;
+        uint64_t p = base + lane;
+        uint32_t frame;
+        int px, py;
+        if (p < total && decode_path(P, p, frame, px, py)) {
+            trace_one<TRACKER>(P, sample, frame, px, py, features != 0, lookups, guard_hit);
+            paths++;
+        }
+        __syncwarp();
+    }
+    flush_counters(P, paths, lookups, guard_hit);
+}
+
+
+// ---------------------------------------------------------------------------------------------
+// Per-lane path refill schedule (delta, ratio and NEE trackers).
+//
+// Each loop iteration advances every live lane by ONE tentative collision.  A lane whose path ends
+// (escape, absorption, bounce cap) writes the film and takes the next path id at the top of the
+// next iteration, so the 32 lanes of a warp keep executing the same step code instead of waiting
+// for the warp's longest path.  NEE shadow rays are a second mode of the same step: the free-path
+// sample and the density lookup are shared code for primary and shadow lanes.  Random numbers are
+// drawn in exactly the order of the recursive trackers (vpt_trackers.cuh), so every path is the same
+// path.  Path ids come from a global counter in warp batches of 64 (one atomic per 64 paths).
+enum : int { kModePrimary = 0, kModeShadow = 1 };
+constexpr int kRefillBatch = 64;
+
+template <int TRACKER>
+VPT_DEV void refill_finish(const TraceParams& P, size_t pix, F3 L, bool& has) {
+    atomicAdd(P.film + pix * 3 + 0, (double)L.x);
+    atomicAdd(P.film + pix * 3 + 1, (double)L.y);
+    atomicAdd(P.film + pix * 3 + 2, (double)L.z);
+    if (P.film_sq) {
+        atomicAdd(P.film_sq + pix * 3 + 0, (double)L.x * (double)L.x);
+        atomicAdd(P.film_sq + pix * 3 + 1, (double)L.y * (double)L.y);
+        atomicAdd(P.film_sq + pix * 3 + 2, (double)L.z * (double)L.z);
+    }
+    has = false;
+}
+
+// Shadow ray done: add the light sample (f = weight * T with weight = pdf_phase / pdf_light for the
+// sky, or the light probability factor times pdf_phase for a light; NextEventTracking.glsl:348-369)
+// and resume the primary path at the scatter point with the sampled direction.
+VPT_DEV void end_shadow(const TraceParams& P, F3& color, F3& x, F3& w, float& d, F3 xp, F3 nw, float dp,
+                        float weight, float ts, int light, int& mode) {
+    const float f = weight * ts;
+    const F3 l = light >= 0 ? light_radiance(P, xp, light) : sky_and_sun(P, w);
+    color = color + f3(f * l.x, f * l.y, f * l.z);
+    x = xp;
+    w = nw;
+    d = dp;
+    mode = kModePrimary;
+    float tmin, tmax;
+    if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
+        x = x + w * tmin;
+        d = tmax - tmin;
+    }
+}
+
+// Where the parameters of a path come from: one scene (the kernel's constant parameter block) or a
+// batch of scenes in global memory whose path ids are concatenated scene after scene.
+struct OneScene {
+    const TraceParams& P;
+    VPT_DEV const TraceParams& scene(int) const { return P; }
+    VPT_DEV int locate(unsigned long long&) const { return 0; }
+};
+struct SceneBatch {
+    const TraceParams* scenes;
+    const unsigned long long* offsets;  // num + 1 prefix sums of the scenes' path counts
+    int num;
+    VPT_DEV const TraceParams& scene(int s) const { return scenes[s]; }
+    // scene of global path id p (binary search); p becomes the scene-local id
+    VPT_DEV int locate(unsigned long long& p) const {
+        int lo = 0, hi = num - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (__ldg(offsets + mid) <= p) lo = mid;
+            else hi = mid - 1;
+        }
+        p -= __ldg(offsets + lo);
+        return lo;
+    }
+};
+
+VPT_DEV void flush_counters_to(unsigned long long* counters, int* error_flags, uint32_t paths, uint32_t lookups,
+                               bool guard_hit) {
+    unsigned long long l = lookups;
+    unsigned long long n = paths;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        l += __shfl_xor_sync(0xffffffffu, l, o);
+        n += __shfl_xor_sync(0xffffffffu, n, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(counters + 0, n);
+        atomicAdd(counters + 1, l);
+    }
+    if (guard_hit) atomicOr(error_flags, kErrIterLimit);
+}
+
+template <int TRACKER, int INTERP, int GRID, bool TF, class SRC>
+VPT_DEV void refill_loop(const SRC& src, uint64_t total, unsigned long long* work_counter,
+                         unsigned long long* counters, int* error_flags) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const unsigned lt_mask = (1u << lane) - 1u;
+    const F3 zero = f3(0.0f, 0.0f, 0.0f);
+
+    // warp-uniform local batch of path ids
+    unsigned long long q_base = 0;
+    int q_left = 0;
+
+    bool has = false, exhausted = false;
+    Rng rng;
+    F3 x = zero, w = zero, color = zero, xp = zero, nw = zero;
+    float d = 0.0f, dp = 0.0f, trans = 1.0f, ts = 1.0f, weight = 0.0f;
+    float shadow_dist = 0.0f, shadow_max = 0.0f;  // distance walked / light distance (light shadow rays)
+    int mode = kModePrimary, bounces = 0, light = -1;
+    bool ev = false;
+    // isosurface state (kDeltaIso): surface throughput, sign at the first point after the last event,
+    // loop iterations of the path
+    F3 iw = f3(1.0f, 1.0f, 1.0f);
+    float iso_last = 0.0f;
+    bool iso_first = true;
+    int iso_it = 0;
+    int scene = 0;
+    uint32_t steps = 0;
+    size_t pix = 0;
+    uint32_t lookups = 0, paths = 0;
+    bool guard_hit = false;
+
+    while (true) {
+        // ---- refill lanes without a path ----
+        const bool need = !has && !exhausted;
+        const unsigned m = __ballot_sync(FULL, need);
+        if (m) {
+            const int n = __popc(m);
+            const int r = __popc(m & lt_mask);
+            unsigned long long fresh = 0;
+            if (n > q_left) {
+                unsigned long long b = 0;
+                if (lane == 0) b = atomicAdd(work_counter, (unsigned long long)kRefillBatch);
+                fresh = __shfl_sync(FULL, b, 0);
+            }
+            if (need) {
+                unsigned long long p = r < q_left ? q_base + (unsigned long long)r
+                                                  : fresh + (unsigned long long)(r - q_left);
+                uint32_t frame;
+                int px, py;
+                const bool done = p >= total;
+                int s = 0;
+                if (!done) s = src.locate(p);
+                const TraceParams& P = src.scene(s);
+                if (done) {
+                    exhausted = true;
+                } else if (decode_path(P, p, frame, px, py)) {
+                    scene = s;
+                    const uint32_t w_u = (uint32_t)P.width, h_u = (uint32_t)P.height;
+                    uint32_t seed = (P.global_frame + frame) * w_u * h_u + (uint32_t)px + (uint32_t)py * w_u;
+                    seed += P.seed_offset;
+                    rng = rng_init(seed);
+                    float rx = rng_next(rng);
+                    float ry = rng_next(rng);
+                    float sx = (2.0f * ((float)px + rx)) / (float)P.width - 1.0f;
+                    float sy = (2.0f * ((float)py + ry)) / (float)P.height - 1.0f;
+                    camera_ray(P, sx, sy, x, w);
+                    pix = (size_t)py * P.width + px;
+                    paths++;
+                    steps = 0;
+                    bounces = 0;
+                    trans = 1.0f;
+                    color = zero;
+                    ev = false;
+                    mode = kModePrimary;
+                    iw = f3(1.0f, 1.0f, 1.0f);
+                    iso_first = true;
+                    iso_it = 0;
+                    float tmin, tmax;
+                    has = true;
+                    if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
+                        x = x + w * tmin;
+                        d = tmax - tmin;
+                    } else {
+                        F3 L = sky_and_sun(P, w);
+                        refill_finish<TRACKER>(P, pix, L, has);
+                    }
+                }
+            }
+            if (n > q_left) {
+                q_base = fresh + (unsigned long long)(n - q_left);
+                q_left = kRefillBatch - (n - q_left);
+            } else {
+                q_base += (unsigned long long)n;
+                q_left -= n;
+            }
+        }
+        if (!__any_sync(FULL, has)) {
+            if (__all_sync(FULL, exhausted)) break;
+            continue;
+        }
+        if (!has) continue;
+
+        // ---- one tentative collision ----
+        const TraceParams& P = src.scene(scene);
+        Sampler<INTERP, GRID, TF> sample{P};
+        if (TRACKER == kDeltaIso && ++iso_it == 1000) {
+            refill_finish<TRACKER>(P, pix, zero, has);
+            continue;
+        }
+        if (++steps > P.max_steps) {
+            guard_hit = true;
+            refill_finish<TRACKER>(P, pix, TRACKER == kNextEvent ? color : zero, has);
+            continue;
+        }
+        const float t = free_path(rng, P.inv_extinction);
+        bool escape = t > d;
+        if (TRACKER == kNextEvent && mode == kModeShadow && light >= 0) {
+            shadow_dist += t;
+            escape = escape || shadow_dist > shadow_max;
+        }
+        float density = 0.0f;
+        if (!escape) {
+            F3 xn = x + w * t;
+            density = sample(xn, rng);
+            lookups++;
+            if constexpr (TRACKER == kDeltaIso) {
+                float tmax_unused = 0.0f;
+                if (iso_segment(P, sample, rng, x, xn, density, w, d, tmax_unused, iw, iso_last, iso_first, lookups,
+                                nullptr)) {
+                    if (iw.x < 1e-3f && iw.y < 1e-3f && iw.z < 1e-3f) refill_finish<TRACKER>(P, pix, zero, has);
+                    continue;
+                }
+            }
+            x = xn;
+        }
+        if (TRACKER == kNextEvent && mode == kModeShadow) {
+            if (!escape) {
+                ts *= 1.0f - density;
+                d -= t;
+                continue;
+            }
+            end_shadow(P, color, x, w, d, xp, nw, dp, weight, ts, light, mode);
+            continue;
+        }
+        if (escape) {
+            F3 L;
+            if (TRACKER == kNextEvent) L = ev ? color : color + sky_and_sun(P, w);
+            else if (TRACKER == kRatio) L = sky_and_sun(P, w) * trans;
+            else if (TRACKER == kDeltaIso) L = iw * sky_and_sun(P, w);
+            else L = sky_and_sun(P, w);
+            refill_finish<TRACKER>(P, pix, L, has);
+            continue;
+        }
+        const float xi = rng_next(rng);
+        if (TRACKER != kRatio && xi < P.absorb_albedo * density) {
+            // USE_EMISSION (NextEventTracking.glsl:296-301): the absorbed NEE path ends with the emission
+            F3 L = zero;
+            if (TRACKER == kNextEvent) {
+                L = P.emission ? color + sample.emission(x, rng) : (P.tf ? color + sample.tf_emission() : color);
+            } else if (P.tf) {  // delta tracking (DeltaTracking.glsl:293-301)
+                L = sample.tf_emission();
+            }
+            refill_finish<TRACKER>(P, pix, L, has);
+            continue;
+        }
+        if (xi < density) {
+            if (P.max_bounces > 0 && ++bounces > P.max_bounces) {
+                refill_finish<TRACKER>(P, pix, TRACKER == kNextEvent ? color : zero, has);
+                continue;
+            }
+            float tmin, tmax;
+            if (TRACKER == kNextEvent) {
+                nw = sample_phase(rng, P.g, w);
+                ev = true;
+                bool to_light = false;
+                float prob_factor = 1.0f, pdf_light = 0.0f, light_dist = 0.0f;
+                int light_idx = 0;
+                if (P.num_lights > 0) {
+                    to_light = P.env_is_black ? true : (rng_next(rng) > 0.5f);
+                    prob_factor = P.env_is_black ? 1.0f : 2.0f;
+                }
+                F3 dir;
+                if (to_light) dir = light_direction(P, x, rng, light_idx, prob_factor, light_dist);
+                else dir = importance_sample_sky(P, rng, pdf_light);
+                const float pdf_phase = evaluate_phase(P.g, w, dir);
+                if (P.num_lights > 0) weight = to_light ? prob_factor * pdf_phase : (prob_factor * pdf_phase) / pdf_light;
+                else weight = pdf_phase / pdf_light;
+                light = to_light ? light_idx : -1;
+                shadow_max = light_dist;
+                xp = x;
+                dp = d;
+                w = dir;
+                ts = 1.0f;
+                mode = kModeShadow;
+                if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
+                    x = x + w * tmin;
+                    d = tmax - tmin;
+                    shadow_dist = tmin;
+                } else {
+                    // no shadow steps (and no random numbers), like calculateTransmittance
+                    end_shadow(P, color, x, w, d, xp, nw, dp, weight, ts, light, mode);
+                }
+                continue;
+            }
+            if (TRACKER == kRatio) {
+                float pa = P.absorb_albedo * density;
+                float ps = P.albedo * density;
+                trans *= 1.0f - pa / (pa + ps);
+            }
+            w = sample_phase(rng, P.g, w);
+            if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
+                x = x + w * tmin;
+                d = tmax - tmin;
+            }
+        } else {
+            d -= t;
+        }
+    }
+    flush_counters_to(counters, error_flags, paths, lookups, guard_hit);
+}
+
+template <int TRACKER, int INTERP, int GRID, bool TF>
+__global__ void __launch_bounds__(kTraceBlock) trace_refill_kernel(const __grid_constant__ TraceParams P, uint64_t total) {
+    refill_loop<TRACKER, INTERP, GRID, TF>(OneScene{P}, total, reinterpret_cast<unsigned long long*>(P.work_counter),
+                                       P.counters, P.error_flags);
+}
+
+// Many independent scenes (own grid, camera, image size, spp, medium) traced by one persistent
+// launch: lanes refill from one id space that concatenates the scenes' paths.  The total path count
+// is read from offsets[num], so a captured launch serves any frame counts.
+template <int TRACKER, int INTERP, int GRID>
+__global__ void __launch_bounds__(kTraceBlock) trace_batch_kernel(const TraceParams* __restrict__ scenes,
+                                                                  const unsigned long long* __restrict__ offsets,
+                                                                  int num, unsigned long long* work_counter,
+                                                                  unsigned long long* counters, int* error_flags) {
+    refill_loop<TRACKER, INTERP, GRID, false>(SceneBatch{scenes, offsets, num}, __ldg(offsets + num), work_counter, counters,
+                                       error_flags);
+}
+
+
+template <int TRACKER, int INTERP, int GRID>
+static cudaError_t batch_t(const BatchLaunch& b, cudaStream_t s) {
+    if (b.blocks_per_sm_out) {
+        int per_sm = 0;
+        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_batch_kernel<TRACKER, INTERP, GRID>,
+                                                                      kTraceBlock, 0);
+        *b.blocks_per_sm_out = per_sm > 0 ? per_sm : 1;
+        return e;
+    }
+    trace_batch_kernel<TRACKER, INTERP, GRID><<<b.blocks, kTraceBlock, 0, s>>>(b.scenes, b.offsets, b.num,
+                                                                              b.work_counter, b.counters,
+                                                                              b.error_flags);
+    if (b.counted) count_launches(1);
+    return cudaGetLastError();
+}
+
+template <int TRACKER, int GRID>
+static cudaError_t batch_interp(const BatchLaunch& b, cudaStream_t s) {
+    switch (b.interp) {
+        case kNearest: return batch_t<TRACKER, kNearest, GRID>(b, s);
+        case kStochastic: return batch_t<TRACKER, kStochastic, GRID>(b, s);
+        default: return batch_t<TRACKER, kTrilinear, GRID>(b, s);
+    }
+}
+
+template <int GRID>
+static cudaError_t batch_tracker(const BatchLaunch& b, cudaStream_t s) {
+    switch (b.tracker) {
+        case kDelta: return batch_interp<kDelta, GRID>(b, s);
+        case kRatio: return batch_interp<kRatio, GRID>(b, s);
+        case kNextEvent: return batch_interp<kNextEvent, GRID>(b, s);
+        default: return cudaErrorNotSupported;
+    }
+}
+template <int TRACKER, int INTERP, int GRID, bool TF>
+static int refill_blocks(int requested) {
+    if (requested > 0) return requested;
+    static int per_sm = 0;
+    if (per_sm == 0) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_refill_kernel<TRACKER, INTERP, GRID, TF>, kTraceBlock,
+                                                      0);
+        if (per_sm <= 0) per_sm = 1;
+    }
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return per_sm * sms;
+}
+
+template <int TRACKER, int INTERP, int GRID, bool TF>
+static cudaError_t launch_trace_t(const TraceParams& P, int schedule, int features, int persistent_blocks,
+                                  cudaStream_t stream) {
+    uint64_t total = padded_paths(P.width, P.height, P.num_frames);
+    constexpr bool kRefillable = TRACKER == kDelta || TRACKER == kRatio || TRACKER == kNextEvent || TRACKER == kDeltaIso;
+    if (schedule == kScheduleRefill && kRefillable && !features) {
+        if constexpr (kRefillable) {
+            int blocks = refill_blocks<TRACKER, INTERP, GRID, TF>(persistent_blocks);
+            cudaMemsetAsync(P.work_counter, 0, sizeof(unsigned long long), stream);
+            trace_refill_kernel<TRACKER, INTERP, GRID, TF><<<blocks, kTraceBlock, 0, stream>>>(P, total);
+            count_launches(1);
+            return cudaGetLastError();
+        }
+    }
+    if (schedule == kScheduleRefill) schedule = kSchedulePersistent;
+    if (schedule == kScheduleTiles) {
+        uint64_t blocks = (total + kTraceBlock - 1) / kTraceBlock;
+        trace_tiles_kernel<TRACKER, INTERP, GRID, TF><<<(unsigned)blocks, kTraceBlock, 0, stream>>>(P, features);
+        count_launches(1);
+    } else {
+        if (persistent_blocks <= 0) {
+            // one wave of resident blocks: SMs x blocks per SM from the occupancy calculator
+            static int per_sm = 0;
+            if (per_sm == 0) {
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_persistent_kernel<TRACKER, INTERP, GRID, TF>,
+                                                              kTraceBlock, 0);
+                if (per_sm <= 0) per_sm = 1;
+            }
+            int dev = 0, sms = 148;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            persistent_blocks = per_sm * sms;
+        }
+        cudaMemsetAsync(P.work_counter, 0, sizeof(unsigned long long), stream);
+        trace_persistent_kernel<TRACKER, INTERP, GRID, TF><<<persistent_blocks, kTraceBlock, 0, stream>>>(P, features,
+                                                                                                           total);
+        count_launches(1);
+    }
+    return cudaGetLastError();
+}
+
+template <int TRACKER, int GRID, bool TF>
+static cudaError_t launch_interp_tf(const TraceParams& P, int schedule, int features, int pb, cudaStream_t s) {
+    switch (P.interp) {
+        case kNearest: return launch_trace_t<TRACKER, kNearest, GRID, TF>(P, schedule, features, pb, s);
+        case kStochastic: return launch_trace_t<TRACKER, kStochastic, GRID, TF>(P, schedule, features, pb, s);
+        default: return launch_trace_t<TRACKER, kTrilinear, GRID, TF>(P, schedule, features, pb, s);
+    }
+}
+
+// transfer-function variants exist for the trackers whose transfer-function appearance the reference
+// defines (delta, next event and the spectral trackers); the others reject a table
+template <int TRACKER, int GRID>
+static cudaError_t launch_interp(const TraceParams& P, int schedule, int features, int pb, cudaStream_t s) {
+    constexpr int base = TRACKER >= 100 ? TRACKER - 100 : TRACKER;
+    constexpr bool kTfTracker =
+        base == kDelta || base == kNextEvent || base == kSpectralDelta || base == kSpectralNextEvent;
+    if (P.tf) {
+        if constexpr (kTfTracker) return launch_interp_tf<TRACKER, GRID, true>(P, schedule, features, pb, s);
+        else return cudaErrorNotSupported;
+    }
+    return launch_interp_tf<TRACKER, GRID, false>(P, schedule, features, pb, s);
+}
+
+// One tracker family on one grid kind: interpolation and transfer-function variants behind it.
+// Defined (explicitly specialised) in the vpt_trace_*.cu unit of the family.
+template <int TRACKER, int GRID>
+cudaError_t launch_tracker(const TraceParams& P, int schedule, int features, int pb, cudaStream_t s);
+
+#define VPT_DECLARE_TRACKER(T, G) \
+    template <>                  \
+    cudaError_t launch_tracker<T, G>(const TraceParams& P, int schedule, int features, int pb, cudaStream_t s)
+#define VPT_DEFINE_TRACKER(T, G) \
+    VPT_DECLARE_TRACKER(T, G) { return launch_interp<T, G>(P, schedule, features, pb, s); }
+
+VPT_DECLARE_TRACKER(kDelta, kDense);
+VPT_DECLARE_TRACKER(kDelta, kNanoVdb);
+VPT_DECLARE_TRACKER(kRatio, kDense);
+VPT_DECLARE_TRACKER(kRatio, kNanoVdb);
+VPT_DECLARE_TRACKER(kDecomposition, kDense);
+VPT_DECLARE_TRACKER(kDecomposition, kNanoVdb);
+VPT_DECLARE_TRACKER(kResidualRatio, kDense);
+VPT_DECLARE_TRACKER(kNextEvent, kDense);
+VPT_DECLARE_TRACKER(kNextEvent + 100, kDense);
+VPT_DECLARE_TRACKER(kNextEvent, kNanoVdb);
+VPT_DECLARE_TRACKER(kSpectralDelta, kDense);
+VPT_DECLARE_TRACKER(kSpectralDelta, kNanoVdb);
+VPT_DECLARE_TRACKER(kSpectralNextEvent, kDense);
+VPT_DECLARE_TRACKER(kSpectralNextEvent + 100, kDense);
+VPT_DECLARE_TRACKER(kSpectralNextEvent, kNanoVdb);
+// delta tracking with isosurfaces: dense grids, trilinear lookups, no transfer function
+cudaError_t launch_tracker_delta_iso(const TraceParams& P, int schedule, int features, int pb, cudaStream_t s);
+
+}  // namespace vpt

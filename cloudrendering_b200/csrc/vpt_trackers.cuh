@@ -92,7 +92,9 @@ VPT_DEV F3 track_delta(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, Fi
 // 8 steps), the surface reflects (iso_scatter), the path moves 1e-4 off it and restarts from the box
 // boundary.  Returns true on a surface event (x, w, d, tmax and weights updated; the first event
 // recorded when `fe` is given).  The last check point is x_new itself (a1 = 1: x * 0 + x_new), whose
-// density was just looked up; trilinear lookups draw no random number, so it is reused.
+// density was just looked up: for a repeatable sampler (trilinear, dense, no transfer function: no
+// random number drawn) that value is reused; any other sampler looks it up again, as the reference
+// does, so that its random stream stays the reference's.
 template <class S>
 VPT_DEV bool iso_segment(const TraceParams& P, S& sample, Rng& rng, F3& x, F3 xn, float density, F3& w, float& d,
                          float& tmax, F3& weights, float& last_sign, bool& first_point, uint32_t& lookups,
@@ -103,7 +105,7 @@ VPT_DEV bool iso_segment(const TraceParams& P, S& sample, Rng& rng, F3& x, F3 xn
         F3 x0 = x * (1.0f - a0) + xn * a0;
         F3 x1 = x * (1.0f - a1) + xn * a1;
         float v = density;
-        if (sub != nsub - 1) {
+        if (sub != nsub - 1 || !S::kRepeatable) {
             v = sample(x1, rng);
             lookups++;
         }

@@ -370,7 +370,8 @@ VptStatus vpt_kpn_reproject(const float* prev, const float* uv, int n, int c, in
 
 /* EAW a-trous chain (EAWBlitPass::_renderCompute, src/Denoiser/EAWDenoiser.cpp:345-391; weights of
  * EAWDenoise.glsl) on RGBA images; position/normal may be NULL.  Allocates its ping-pong images
- * on `stream` with the stream-ordered allocator and frees them before returning. */
+ * on `stream` with the stream-ordered allocator and frees them before returning.  `out` must not
+ * overlap color, position or normal (in-place filtering is rejected with VPT_ERR_ARG). */
 VptStatus vpt_eaw_denoise_rgba(const float* color, const float* position, const float* normal, int width,
                                int height, int iterations, float phi_color, float phi_position, float phi_normal,
                                int ref_compute_quirk, float* out, void* stream);
@@ -382,7 +383,8 @@ VptStatus vpt_eaw_denoise_rgba(const float* color, const float* position, const 
  * life of the process.  width*height above 1048576 returns VPT_ERR_ARG.  The first call on a device
  * looks up the array's address and uploads the filter's tap weights with a synchronous copy; make
  * that first call before any stream capture.  All calls on a device share the array, so calls whose
- * work overlaps on the GPU race; nothing in it needs to start at zero. */
+ * work overlaps on the GPU race; nothing in it needs to start at zero.  As for vpt_eaw_denoise_rgba,
+ * `out` must not overlap color, position or normal (VPT_ERR_ARG). */
 VptStatus vpt_eaw_denoise_rgba_noalloc(const float* color, const float* position, const float* normal, int width,
                                        int height, int iterations, float phi_color, float phi_position,
                                        float phi_normal, int ref_compute_quirk, float* out, void* stream);

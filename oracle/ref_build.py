@@ -13,8 +13,9 @@
    (src/nanovdb/util/GridBuilder.h) driven as CloudData::getSparseDensityField drives it
    (``ref_nanovdb_builder.cpp``).
 
-The reference tree is read from $VPT_REFERENCE_ROOT or /root/reference; when it is absent the build
-is skipped (the prebuilt libraries under oracle/_ref are used as they are).
+The reference tree is read from $VPT_REFERENCE_ROOT, else from a directory named ``reference`` beside
+this repository's root; when it is absent the build is skipped (the prebuilt libraries under
+oracle/_ref are used as they are).
 """
 from __future__ import annotations
 
@@ -27,7 +28,7 @@ from concurrent.futures import ThreadPoolExecutor
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
 GEN = os.path.join(OUT, "gen")
-REF = os.environ.get("VPT_REFERENCE_ROOT", "/root/reference")
+REF = os.environ.get("VPT_REFERENCE_ROOT") or os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference")
 SHADERS = os.path.join(REF, "Data", "Shaders", "VPT")
 BRDFS = os.path.join(REF, "Data", "Shaders", "BRDF")
 

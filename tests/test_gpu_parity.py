@@ -114,6 +114,16 @@ def test_eaw_matches_oracle(core, quirk):
     assert np.allclose(out.cpu().numpy(), ref, rtol=1e-5, atol=1e-6)
 
 
+def test_eaw_rejects_an_output_that_overlaps_an_input(core):
+    h, w = 16, 16
+    imgs = [torch.rand((h, w, 4), device="cuda") for _ in range(3)]
+    for out in (imgs[0], imgs[1], imgs[2], imgs[0][3:]):
+        st = core.lib.vpt_eaw_denoise_rgba(dptr(imgs[0]), dptr(imgs[1]), dptr(imgs[2]), w, h, 3, 5.0, 0.1, 0.1, 0,
+                                           dptr(out), None)
+        assert st == 1  # VPT_ERR_ARG
+    torch.cuda.synchronize()
+
+
 def fbm_scene(**kw):
     g = bridge.fbm(48, 2, base_frequency=3.0, contrast=3.5)
     base = dict(grid=g, extinction=150.0, albedo=0.99, g=0.85, width=64, height=64, env="constant_sun",
@@ -252,11 +262,17 @@ def test_iteration_guard_reports_error_without_hanging(core):
     core("vpt_synchronize", None)
 
 
-@pytest.mark.parametrize("mode", ["delta", "ratio", "nee", "nee_lights"])
+@pytest.mark.parametrize("mode", ["delta", "ratio", "nee", "nee_lights", "delta_isosurfaces"])
 def test_schedules_trace_identical_paths(core, mode):
     """Tile, persistent-batch and per-lane-refill schedules trace the same paths (same film up to the
-    order of the FP64 atomic additions)."""
-    kw = PATH_CASES["nee_lights"] if mode == "nee_lights" else dict(mode=mode)
+    order of the FP64 atomic additions).  The isosurface case covers the refill loop's own surface
+    handling (iteration cap, weight cut-off, per-lane reset of the surface state)."""
+    if mode == "nee_lights":
+        kw = PATH_CASES["nee_lights"]
+    elif mode == "delta_isosurfaces":
+        kw = dict(mode="delta", interp="trilinear", iso=True, iso_value=0.3)
+    else:
+        kw = dict(mode=mode)
     sp = fbm_scene(width=40, height=40, **kw)
     setup_core(core, sp)
     films = []
