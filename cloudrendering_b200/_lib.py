@@ -91,6 +91,10 @@ SIGNATURES = {
     "vpt_build_supervoxel_grid": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_int, c_void_p, c_void_p,
                                           c_void_p, c_void_p, c_void_p]),
     "vpt_build_rrt_params": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_float, c_int, c_void_p, c_void_p]),
+    "vpt_set_env_map_rotation": (c_int, [c_void_p, c_void_p]),
+    "vpt_set_env_map_rotation_camera": (c_int, [c_void_p]),
+    "vpt_set_global_world_bounding_box": (c_int, [c_void_p, c_void_p, c_void_p]),
+    "vpt_build_residual_ratio_grid": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_float, c_int, c_void_p, c_void_p]),
     "vpt_build_occupancy_grid": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_int, c_float, c_void_p,
                                          c_void_p]),
     "vpt_build_environment_pyramid": (c_int, [c_void_p, c_int, c_int, c_int, c_void_p, c_void_p]),

@@ -8,6 +8,7 @@
 #include <stdio.h>
 #include <string.h>
 #include <algorithm>
+#include <cmath>
 #include <string>
 #include <vector>
 
@@ -129,6 +130,10 @@ struct VptContext {
     int env_image_linear = 1;
     int env_image_black = 0;
     float env_intensity[3] = {1.0f, 1.0f, 1.0f};
+    int env_rot_mode = 0;         // 0 off, 1 matrix, 2 camera view (useEnvMapRot, useEnvMapRotCamera)
+    float env_rot_m[9] = {1.0f, 0.0f, 0.0f, 0.0f, 1.0f, 0.0f, 0.0f, 0.0f, 1.0f};
+    int has_global_box = 0;       // setGlobalWorldBoundingBox
+    float global_box_min[3] = {0.0f, 0.0f, 0.0f}, global_box_max[3] = {0.0f, 0.0f, 0.0f};
     float sun_dir[3] = {0.0f, 0.0f, 0.0f};
     float sun_intensity[3] = {2.6f * 1.0f, 2.6f * 0.961538462f, 2.6f * 0.884615385f};
     float sky_color[3] = {1.0f, 1.0f, 1.0f};
@@ -182,6 +187,7 @@ struct VptContext {
     int sv_interp = -1;
     float sv_extinction = -1.0f;
     DevBuf<float> sv_min, sv_max, sv_avg, sv_pairs;
+    DevBuf<float> sv_local;      // unbiased residual ratio tracking: 4 floats per supervoxel
     DevBuf<uint8_t> sv_occ;
     bool occ_valid = false;
     int occ_interp = -1;
@@ -335,12 +341,19 @@ void compute_sparse_box(VptContext* ctx) {
         }
         return;
     }
-    float diff[3] = {wmax[0] - wmin[0], wmax[1] - wmin[1], wmax[2] - wmin[2]};
+    // the global world box, when set, replaces the grid's own box in the normalisation
+    // (CloudData::computeSparseGridMetadata, CloudData.cpp:1320-1344)
+    float gmin[3], gmax[3];
+    for (int i = 0; i < 3; i++) {
+        gmin[i] = ctx->has_global_box ? ctx->global_box_min[i] : wmin[i];
+        gmax[i] = ctx->has_global_box ? ctx->global_box_max[i] : wmax[i];
+    }
+    float diff[3] = {gmax[0] - gmin[0], gmax[1] - gmin[1], gmax[2] - gmin[2]};
     float max_dim = std::max(diff[0], std::max(diff[1], diff[2]));
     float A = 2.0f * ctx->max_grid_extent / max_dim;
     for (int i = 0; i < 3; i++) {
         float L = diff[i] / max_dim;
-        float B = ctx->max_grid_extent * L - wmax[i] * A;
+        float B = ctx->max_grid_extent * L - gmax[i] * A;
         ctx->sparse_box_min[i] = A * wmin[i] + B;
         ctx->sparse_box_max[i] = A * wmax[i] + B;
     }
@@ -378,6 +391,7 @@ int tracker_of(int mode) {
         case VPT_MODE_NEXT_EVENT_TRACKING: return vpt::kNextEvent;
         case VPT_MODE_SPECTRAL_DELTA_TRACKING: return vpt::kSpectralDelta;
         case VPT_MODE_NEXT_EVENT_TRACKING_SPECTRAL: return vpt::kSpectralNextEvent;
+        case VPT_MODE_RESIDUAL_RATIO_TRACKING_UNBIASED: return vpt::kResidualRatioNee;
         default: return -1;
     }
 }
@@ -399,19 +413,21 @@ float extinction_x(const VptContext* ctx) { return ctx->extinction_base[0] * ctx
 
 VptStatus ensure_accel(VptContext* ctx, int tracker, cudaStream_t s) {
     if (ctx->use_sparse) {
-        if (tracker == vpt::kResidualRatio ||
+        if (tracker == vpt::kResidualRatio || tracker == vpt::kResidualRatioNee ||
             ((tracker == vpt::kNextEvent || tracker == vpt::kSpectralNextEvent) && ctx->use_ess))
             return fail(ctx, VPT_ERR_UNSUPPORTED,
                         "residual ratio tracking and empty space skipping need a dense grid (as in the reference)");
         return ensure_sparse(ctx, s);
     }
-    const bool need_sv = tracker == vpt::kDecomposition || tracker == vpt::kResidualRatio;
+    const bool need_sv =
+        tracker == vpt::kDecomposition || tracker == vpt::kResidualRatio || tracker == vpt::kResidualRatioNee;
     const bool need_occ = (tracker == vpt::kNextEvent || tracker == vpt::kSpectralNextEvent) && ctx->use_ess;
     if (need_sv) {
         // setExtinctionScale does not rebuild the RRT grid in the reference
         // (VolumetricPathTracingPass.cpp:1289-1291); here the grid follows the current extinction.
         bool stale = ctx->sv_kind != tracker || ctx->sv_interp != ctx->interp ||
-                     (tracker == vpt::kResidualRatio && ctx->sv_extinction != extinction_x(ctx));
+                     ((tracker == vpt::kResidualRatio || tracker == vpt::kResidualRatioNee) &&
+                      ctx->sv_extinction != extinction_x(ctx));
         if (stale) {
             supervoxel_dims(ctx);
             int total = ctx->svx * ctx->svy * ctx->svz;
@@ -420,11 +436,18 @@ VptStatus ensure_accel(VptContext* ctx, int tracker, cudaStream_t s) {
             VPT_CHECK_CUDA(ctx, ctx->sv_avg.alloc(total));
             VPT_CHECK_CUDA(ctx, ctx->sv_occ.alloc(total));
             VPT_CHECK_CUDA(ctx, ctx->sv_pairs.alloc((size_t)total * 2));
-            int halo = ctx->interp == VPT_INTERP_NEAREST ? 0 : 1;
+            // the unbiased tracker's majorants always include the one-voxel halo (a bound for every
+            // lookup of the supervoxel, whatever the interpolation)
+            int halo = (ctx->interp == VPT_INTERP_NEAREST && tracker != vpt::kResidualRatioNee) ? 0 : 1;
             VPT_CHECK_CUDA(ctx, vpt::launch_supervoxel_stats(ctx->norm.ptr, ctx->nx, ctx->ny, ctx->nz, ctx->sv_size,
                                                              ctx->svx, ctx->svy, ctx->svz, halo, ctx->sv_min.ptr,
                                                              ctx->sv_max.ptr, ctx->sv_avg.ptr, ctx->sv_occ.ptr, s));
-            if (tracker == vpt::kResidualRatio) {
+            if (tracker == vpt::kResidualRatioNee) {
+                float D = sqrtf(3.0f) * float(ctx->sv_size);
+                VPT_CHECK_CUDA(ctx, ctx->sv_local.alloc((size_t)total * 4));
+                VPT_CHECK_CUDA(ctx, vpt::launch_rrt_local(ctx->sv_min.ptr, ctx->sv_max.ptr, ctx->sv_avg.ptr, total,
+                                                          extinction_x(ctx), D, ctx->sv_local.ptr, s));
+            } else if (tracker == vpt::kResidualRatio) {
                 float D = sqrtf(3.0f) * float(ctx->sv_size);
                 VPT_CHECK_CUDA(ctx, vpt::launch_rrt_params(ctx->sv_min.ptr, ctx->sv_max.ptr, ctx->sv_avg.ptr, total,
                                                            extinction_x(ctx), D, ctx->sv_pairs.ptr, s));
@@ -564,6 +587,7 @@ VptStatus fill_params(VptContext* ctx, int tracker, int frames, vpt::TraceParams
         if (a == 1) P.sv_world.y = v;
         if (a == 2) P.sv_world.z = v;
     }
+    P.sv_inv_world = mk(1.0f / P.sv_world.x, 1.0f / P.sv_world.y, 1.0f / P.sv_world.z);
     P.env_kind = ctx->env_kind;
     P.use_linear_rgb = ctx->use_linear_rgb;
     P.env_image_linear = ctx->env_image_linear;
@@ -576,8 +600,19 @@ VptStatus fill_params(VptContext* ctx, int tracker, int frames, vpt::TraceParams
     P.env_h = ctx->env_h;
     P.env_levels = ctx->env_levels;
     P.env_base_res = 1 << ctx->env_levels;
+    P.env_rot = ctx->env_rot_mode != 0 && ctx->env_kind == VPT_ENV_IMAGE;
+    if (ctx->env_rot_mode == 2) {
+        // useEnvMapRotCamera: envMapRot = camera->getViewMatrix() (its upper 3x3, column-major)
+        double view[16];
+        compute_view(ctx, view);
+        for (int c = 0; c < 3; c++)
+            for (int r = 0; r < 3; r++) P.env_rot_m[c * 3 + r] = float(view[c * 4 + r]);
+    } else {
+        for (int i = 0; i < 9; i++) P.env_rot_m[i] = ctx->env_rot_m[i];
+    }
     P.density = ctx->norm.ptr;
     P.sv_data = ctx->sv_pairs.ptr;
+    P.sv_local = ctx->sv_local.ptr;
     P.occupancy = ctx->occupancy.ptr;
     P.env_rgba = ctx->env_rgba.ptr;
     P.env_pyramid = ctx->env_pyramid.ptr;
@@ -863,6 +898,7 @@ void vpt_destroy(VptContext* ctx) {
     ctx->sv_max.release();
     ctx->sv_avg.release();
     ctx->sv_pairs.release();
+    ctx->sv_local.release();
     ctx->sv_occ.release();
     ctx->occupancy.release();
     ctx->env_rgba.release();
@@ -1167,7 +1203,7 @@ VptStatus vpt_sparse_query(VptContext* ctx, const int32_t* ijk, int count, float
 
 VptStatus vpt_set_vpt_mode(VptContext* ctx, int mode) {
     VPT_CHECK_CTX(ctx);
-    if (mode < 0 || mode > VPT_MODE_RAY_MARCHING_EMISSION_ABSORPTION)
+    if (mode < 0 || mode > VPT_MODE_RESIDUAL_RATIO_TRACKING_UNBIASED)
         return fail(ctx, VPT_ERR_ARG, "unknown VptMode");
     if (tracker_of(mode) < 0) return fail(ctx, VPT_ERR_UNSUPPORTED, "VptMode not built in this core");
     if (mode != ctx->mode) reset_film_state(ctx);
@@ -1311,6 +1347,43 @@ VptStatus vpt_load_environment_map_rgba(VptContext* ctx, const float* rgba, int 
     return VPT_OK;
 }
 
+VptStatus vpt_set_env_map_rotation(VptContext* ctx, const float rotation[9]) {
+    VPT_CHECK_CTX(ctx);
+    if (rotation) {
+        for (int i = 0; i < 9; i++) {
+            if (!std::isfinite(rotation[i])) return fail(ctx, VPT_ERR_ARG, "rotation must be finite");
+            ctx->env_rot_m[i] = rotation[i];
+        }
+        ctx->env_rot_mode = 1;
+    } else {
+        ctx->env_rot_mode = 0;
+    }
+    reset_film_state(ctx);
+    return VPT_OK;
+}
+
+VptStatus vpt_set_env_map_rotation_camera(VptContext* ctx) {
+    VPT_CHECK_CTX(ctx);
+    ctx->env_rot_mode = 2;
+    reset_film_state(ctx);
+    return VPT_OK;
+}
+
+VptStatus vpt_set_global_world_bounding_box(VptContext* ctx, const float box_min[3], const float box_max[3]) {
+    VPT_CHECK_CTX(ctx);
+    if (!box_min || !box_max) {
+        ctx->has_global_box = 0;
+        return VPT_OK;
+    }
+    for (int i = 0; i < 3; i++) {
+        if (!(box_max[i] > box_min[i])) return fail(ctx, VPT_ERR_ARG, "global bounding box must have max > min");
+        ctx->global_box_min[i] = box_min[i];
+        ctx->global_box_max[i] = box_max[i];
+    }
+    ctx->has_global_box = 1;
+    return VPT_OK;
+}
+
 VptStatus vpt_set_camera(VptContext* ctx, const float position[3], const float target[3], const float up[3],
                          float fovy_radians, float near_dist, float far_dist) {
     VPT_CHECK_CTX(ctx);
@@ -1405,7 +1478,7 @@ VptStatus vpt_render_frames(VptContext* ctx, int frames, void* stream) {
         P.frame_count = ctx->frame_count + (uint32_t)frames - 1u;
         P.global_frame = P.frame_count;
     }
-    if (tracker == vpt::kDecomposition || tracker == vpt::kResidualRatio) {
+    if (tracker == vpt::kDecomposition || tracker == vpt::kResidualRatio || tracker == vpt::kResidualRatioNee) {
         P.sv_size = ctx->sv_size;
         P.svx = ctx->svx;
         P.svy = ctx->svy;
@@ -1963,6 +2036,14 @@ VptStatus vpt_build_rrt_params(const float* sv_min, const float* sv_max, const f
     if (!sv_min || !sv_max || !sv_avg || !out_pairs || count <= 0 || sv <= 0) return VPT_ERR_ARG;
     float D = sqrtf(3.0f) * float(sv);
     cudaError_t e = vpt::launch_rrt_params(sv_min, sv_max, sv_avg, count, extinction, D, out_pairs, as_stream(stream));
+    return e == cudaSuccess ? VPT_OK : VPT_ERR_CUDA;
+}
+
+VptStatus vpt_build_residual_ratio_grid(const float* sv_min, const float* sv_max, const float* sv_avg, int count,
+                                        float extinction, int sv, float* out4, void* stream) {
+    if (!sv_min || !sv_max || !sv_avg || !out4 || count <= 0 || sv <= 0) return VPT_ERR_ARG;
+    float D = sqrtf(3.0f) * float(sv);
+    cudaError_t e = vpt::launch_rrt_local(sv_min, sv_max, sv_avg, count, extinction, D, out4, as_stream(stream));
     return e == cudaSuccess ? VPT_OK : VPT_ERR_CUDA;
 }
 

@@ -290,8 +290,20 @@ VPT_DEV F3 env_image_fetch(const TraceParams& P, float u, float v) {
     return r;
 }
 
-// sampleSkybox for an environment image (VptUtils.glsl:303-328; no rotation).
+// parameters.envMapDirRot * v and its transpose (invEnvMapDirRot) * v, columns summed in order
+VPT_DEV F3 env_rotate(const float* m, F3 v) {
+    return f3((m[0] * v.x + m[3] * v.y) + m[6] * v.z, (m[1] * v.x + m[4] * v.y) + m[7] * v.z,
+              (m[2] * v.x + m[5] * v.y) + m[8] * v.z);
+}
+VPT_DEV F3 env_rotate_inverse(const float* m, F3 v) {
+    return f3((m[0] * v.x + m[1] * v.y) + m[2] * v.z, (m[3] * v.x + m[4] * v.y) + m[5] * v.z,
+              (m[6] * v.x + m[7] * v.y) + m[8] * v.z);
+}
+
+// sampleSkybox for an environment image (VptUtils.glsl:303-328), with USE_ENV_MAP_ROTATION the
+// direction rotated first.
 VPT_DEV F3 sky_image(const TraceParams& P, F3 dir) {
+    if (P.env_rot) dir = env_rotate(P.env_rot_m, dir);
     float u = m_atan2(dir.z, dir.x) / kTwoPi + 0.5f;
     float v = -m_asin(dir.y) / kPi + 0.5f;
     F3 c = env_image_fetch(P, u, v);
@@ -328,7 +340,7 @@ VPT_DEV F3 sky_only(const TraceParams& P, F3 dir) {
     }
 }
 
-// Octahedral map helpers (VptUtils.glsl:127-170; no rotation).
+// Octahedral map helpers (VptUtils.glsl:127-170, without the rotation; see importance_sample_env_image).
 VPT_DEV float signf(float v) { return v > 0.0f ? 1.0f : (v < 0.0f ? -1.0f : 0.0f); }
 
 VPT_DEV F3 octahedral_uv_to_world(float u, float v) {
@@ -405,7 +417,10 @@ VPT_DEV F3 importance_sample_env_image(const TraceParams& P, Rng& rng, float& pd
         }
     }
     float inv = 1.0f / (float)P.env_base_res;
-    return octahedral_uv_to_world(((float)px + rx) * inv, ((float)py + ry) * inv);
+    // octahedralUVToWorld with USE_ENV_MAP_ROTATION returns invEnvMapDirRot * direction
+    // (VptUtils.glsl:142-146); the pyramid itself is built from unrotated directions
+    const F3 dir = octahedral_uv_to_world(((float)px + rx) * inv, ((float)py + ry) * inv);
+    return P.env_rot ? env_rotate_inverse(P.env_rot_m, dir) : dir;
 }
 
 // Light sample for NEE: environment image -> pyramid, builtin -> uniform sphere.

@@ -54,6 +54,8 @@ cudaError_t launch_trace(const TraceParams& P, int tracker, int use_ess, int sch
         case kRatio: return launch_tracker<kRatio, kDense>(P, schedule, features, persistent_blocks, stream);
         case kDecomposition: return launch_tracker<kDecomposition, kDense>(P, schedule, features, persistent_blocks, stream);
         case kResidualRatio: return launch_tracker<kResidualRatio, kDense>(P, schedule, features, persistent_blocks, stream);
+        case kResidualRatioNee:
+            return launch_tracker<kResidualRatioNee, kDense>(P, schedule, features, persistent_blocks, stream);
         case kNextEvent:
             if (use_ess) return launch_tracker<kNextEvent + 100, kDense>(P, schedule, features, persistent_blocks, stream);
             return launch_tracker<kNextEvent, kDense>(P, schedule, features, persistent_blocks, stream);
@@ -269,6 +271,22 @@ __global__ void rrt_params_kernel(const float* __restrict__ mn, const float* __r
     out_pairs[2 * i + 1] = mu_r;
 }
 
+// Per supervoxel: the residual ratio tracking controls of rrt_params_kernel, then the free-path
+// majorant's reciprocals (0 for a supervoxel whose largest density, halo included, is 0).
+__global__ void rrt_local_kernel(const float* __restrict__ mn, const float* __restrict__ mx,
+                                 const float* __restrict__ avg, int total, float extinction, float D,
+                                 float4* __restrict__ out) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= total) return;
+    const float dmax = mx[i];
+    float mu_min = mn[i] * extinction, mu_max = dmax * extinction, mu_avg = avg[i] * extinction;
+    float mu_r = fmaxf(mu_max - mu_min, 0.1f);
+    float mu_c = mu_min + mu_r * m_pow(2.0f, (1.0f / (D * mu_r)) - 1.0f);
+    mu_c = fminf(fmaxf(mu_c, mu_min), mu_avg);
+    const bool empty = !(dmax > 0.0f) || !(mu_max > 0.0f);
+    out[i] = make_float4(mu_c, mu_r, empty ? 0.0f : 1.0f / dmax, empty ? 0.0f : 1.0f / mu_max);
+}
+
 __global__ void interleave_kernel(const float* __restrict__ a, const float* __restrict__ b, int total,
                                   float* __restrict__ out_pairs) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -414,6 +432,14 @@ cudaError_t launch_supervoxel_stats(const float* dens, int nx, int ny, int nz, i
 cudaError_t launch_rrt_params(const float* mn, const float* mx, const float* avg, int total, float extinction,
                               float D, float* out_pairs, cudaStream_t s) {
     rrt_params_kernel<<<(total + 255) / 256, 256, 0, s>>>(mn, mx, avg, total, extinction, D, out_pairs);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_rrt_local(const float* mn, const float* mx, const float* avg, int total, float extinction,
+                             float D, float* out4, cudaStream_t s) {
+    rrt_local_kernel<<<(total + 255) / 256, 256, 0, s>>>(mn, mx, avg, total, extinction, D,
+                                                        reinterpret_cast<float4*>(out4));
     count_launches(1);
     return cudaGetLastError();
 }

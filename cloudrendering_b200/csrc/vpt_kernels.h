@@ -33,6 +33,9 @@ cudaError_t launch_supervoxel_stats(const float* dens, int nx, int ny, int nz, i
                                     int halo, float* mn, float* mx, float* avg, uint8_t* occ, cudaStream_t s);
 cudaError_t launch_rrt_params(const float* mn, const float* mx, const float* avg, int total, float extinction,
                               float D, float* out_pairs, cudaStream_t s);
+// Unbiased residual ratio tracking grid: per supervoxel (mu_c, mu_r_bar, 1 / max, 1 / (extinction * max)).
+cudaError_t launch_rrt_local(const float* mn, const float* mx, const float* avg, int total, float extinction,
+                             float D, float* out4, cudaStream_t s);
 cudaError_t launch_interleave(const float* a, const float* b, int total, float* out_pairs, cudaStream_t s);
 // One persistent launch over many scenes (see trace_batch_kernel).  With blocks_per_sm_out set, only
 // reports the kernel's resident blocks per SM (occupancy calculator) and launches nothing.

@@ -18,6 +18,9 @@ enum Tracker : int {
     kResidualRatio = 4,
     kNextEvent = 5,
     kSpectralNextEvent = 6,
+    // no reference counterpart: next-event estimation with residual-ratio-tracked shadow rays and
+    // supervoxel-majorant free paths (VPT_MODE_RESIDUAL_RATIO_TRACKING_UNBIASED)
+    kResidualRatioNee = 9,
     // kernel variant, not a VptMode: delta tracking with isosurfaces inside the volume
     kDeltaIso = 300,
 };
@@ -136,6 +139,7 @@ struct TraceParams {
     int sv_size;               // voxels per supervoxel side
     int svx, svy, svz;         // supervoxel grid resolution
     F3 sv_world;               // supervoxel size in world units (superVoxelSize * boxDelta / gridResolution)
+    F3 sv_inv_world;           // 1 / sv_world
 
     // sky and sun
     int env_kind;              // EnvKind
@@ -149,11 +153,16 @@ struct TraceParams {
     int env_w, env_h;          // equirectangular environment image
     int env_levels;            // octahedral pyramid levels (12 in the reference)
     int env_base_res;          // 1 << env_levels
+    // USE_ENV_MAP_ROTATION (VptUtils.glsl:142-153, 303-306): environment-image lookups rotate the
+    // direction by env_rot (mat3, column-major m[col * 3 + row]); importance samples by its transpose
+    int env_rot;
+    float env_rot_m[9];
 
     // device buffers (all owned by the context)
     const float* density;          // normalised density, x-fastest
     const float* sv_data;          // 2 floats per supervoxel: (min, max) or (mu_c, mu_r_bar)
     const uint8_t* occupancy;      // 1 byte per supervoxel
+    const float* sv_local;         // 4 floats per supervoxel: mu_c, mu_r_bar, 1 / max density, 1 / majorant
     const float* env_rgba;         // equirect RGBA fp32
     const float* env_pyramid;      // octahedral max-luminance pyramid, level 0 first
     const uint64_t* env_level_offset; // float offset of each level in env_pyramid (indexed by level)

@@ -138,6 +138,7 @@ VPT_DEV F3 run_tracker(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, Fi
         else return track_decomposition(P, sample, rng, x, w, fe, pc);
     }
     if (TRACKER == kResidualRatio) return track_residual_ratio(P, sample, rng, x, w, fe, pc);
+    if constexpr (TRACKER == kResidualRatioNee) return track_residual_ratio_nee(P, sample, rng, x, w, fe, pc);
     if constexpr (TRACKER == kSpectralDelta) return track_delta_spectral(P, sample, rng, x, w, fe, pc);
     if constexpr (TRACKER == kSpectralNextEvent) return track_nee_spectral<false>(P, sample, rng, x, w, fe, pc);
     if constexpr (TRACKER == kSpectralNextEvent + 100) return track_nee_spectral<true>(P, sample, rng, x, w, fe, pc);
@@ -708,6 +709,7 @@ VPT_DECLARE_TRACKER(kRatio, kNanoVdb);
 VPT_DECLARE_TRACKER(kDecomposition, kDense);
 VPT_DECLARE_TRACKER(kDecomposition, kNanoVdb);
 VPT_DECLARE_TRACKER(kResidualRatio, kDense);
+VPT_DECLARE_TRACKER(kResidualRatioNee, kDense);
 VPT_DECLARE_TRACKER(kNextEvent, kDense);
 VPT_DECLARE_TRACKER(kNextEvent + 100, kDense);
 VPT_DECLARE_TRACKER(kNextEvent, kNanoVdb);

@@ -911,4 +911,195 @@ VPT_DEV F3 track_residual_ratio(const TraceParams& P, S& sample, Rng& rng, F3 x,
     return acc;
 }
 
+
+// ---------------------------------------------------------------------------------------------
+// Residual ratio tracking, unbiased (no reference counterpart; the reference's residual ratio mode
+// is the reservoir estimator above).  Next-event estimation whose shadow transmittance is residual
+// ratio tracking (Novak et al. 2014) with the per-supervoxel control and residual extinctions
+// (mu_c, mu_r_bar) of SuperVoxelGrid.cpp:218-265, and whose free paths are delta tracking with the
+// supervoxel's own majorant: extinction times the largest normalised density of the supervoxel and
+// a one-voxel halo, which bounds every lookup inside it (a stochastic or trilinear lookup reads at
+// most half a voxel beyond its point).  A supervoxel whose majorant is 0 holds no density that a
+// lookup could return, so both walks cross it without drawing a random number.  Supervoxel data:
+// 4 floats (mu_c, mu_r_bar, 1 / max density, 1 / majorant; the last two 0 when empty).
+
+// Amanatides-Woo walk over the supervoxel grid in world units: the ray distance to the next cell
+// boundary of each axis and between boundaries.
+struct SvWalk {
+    int idx[3];
+    int step[3];
+    float next[3];
+    float delta[3];
+};
+
+VPT_DEV void sv_walk_begin(const TraceParams& P, F3 x, F3 w, SvWalk& s) {
+    const float xv[3] = {x.x, x.y, x.z}, wv[3] = {w.x, w.y, w.z};
+    const float bmin[3] = {P.box_min.x, P.box_min.y, P.box_min.z};
+    const float sw[3] = {P.sv_world.x, P.sv_world.y, P.sv_world.z};
+    const float inv[3] = {P.sv_inv_world.x, P.sv_inv_world.y, P.sv_inv_world.z};
+    const int n[3] = {P.svx, P.svy, P.svz};
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        int i = (int)floorf((xv[a] - bmin[a]) * inv[a]);
+        i = min(max(i, 0), n[a] - 1);
+        s.idx[a] = i;
+        if (wv[a] > 0.0f) {
+            s.step[a] = 1;
+            s.next[a] = ((bmin[a] + (float)(i + 1) * sw[a]) - xv[a]) / wv[a];
+            s.delta[a] = sw[a] / wv[a];
+        } else if (wv[a] < 0.0f) {
+            s.step[a] = -1;
+            s.next[a] = ((bmin[a] + (float)i * sw[a]) - xv[a]) / wv[a];
+            s.delta[a] = -sw[a] / wv[a];
+        } else {
+            s.step[a] = 0;
+            s.next[a] = INFINITY;
+            s.delta[a] = INFINITY;
+        }
+    }
+}
+
+// the axis whose cell boundary comes first
+VPT_DEV int sv_walk_axis(const SvWalk& s) {
+    return s.next[0] < s.next[1] ? (s.next[0] < s.next[2] ? 0 : 2) : (s.next[1] < s.next[2] ? 1 : 2);
+}
+
+// steps over the boundary of axis a; false when the walk leaves the grid
+VPT_DEV bool sv_walk_advance(const TraceParams& P, SvWalk& s, int a) {
+    s.idx[a] += s.step[a];
+    s.next[a] += s.delta[a];
+    const int n = a == 0 ? P.svx : (a == 1 ? P.svy : P.svz);
+    return s.idx[a] >= 0 && s.idx[a] < n;
+}
+
+VPT_DEV float4 sv_local_cell(const TraceParams& P, const SvWalk& s) {
+    return __ldg(reinterpret_cast<const float4*>(P.sv_local) + ((size_t)s.idx[2] * P.svy + s.idx[1]) * P.svx +
+                 s.idx[0]);
+}
+
+// Residual ratio tracking transmittance from x along w over at most max_dist (the box exit
+// otherwise): per supervoxel exp(-mu_c * length) times (1 - (mu(x_i) - mu_c) / mu_r_bar) at the
+// points of a Poisson process of rate mu_r_bar.
+template <class S>
+VPT_DEV float shadow_residual_ratio(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, float max_dist,
+                                    PathCtx& pc) {
+    float tmin, tmax;
+    if (!ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) return 1.0f;
+    const float d = fminf(tmax, max_dist) - tmin;
+    if (!(d > 0.0f)) return 1.0f;
+    x = x + w * tmin;
+    SvWalk s;
+    sv_walk_begin(P, x, w, s);
+    float T = 1.0f;
+    float t0 = 0.0f;
+    while (true) {
+        if (guard(pc)) return 0.0f;
+        const int a = sv_walk_axis(s);
+        const float t1 = fminf(s.next[a], d);
+        const float4 c = sv_local_cell(P, s);
+        if (c.w > 0.0f && t1 > t0) {
+            T *= m_exp(-c.x * (t1 - t0));
+            const float inv_mu_r = 1.0f / c.y;
+            float t = t0;
+            while (true) {
+                if (guard(pc)) return 0.0f;
+                t += free_path(rng, inv_mu_r);
+                if (t >= t1) break;
+                const float density = sample(x + w * t, rng);
+                pc.lookups++;
+                T *= 1.0f - (P.extinction * density - c.x) * inv_mu_r;
+            }
+        }
+        if (t1 >= d) break;
+        t0 = fmaxf(t0, t1);
+        if (!sv_walk_advance(P, s, a)) break;
+    }
+    return T;
+}
+
+template <class S>
+VPT_DEV F3 track_residual_ratio_nee(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, FirstEvent& fe,
+                                    PathCtx& pc) {
+    F3 color = f3(0.0f, 0.0f, 0.0f);
+    float tmin, tmax;
+    if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
+        x = x + w * tmin;
+        float d = tmax - tmin;
+        float depth0 = tmin;  // distance of x from the camera while no event has happened
+        int bounces = 0;
+        while (true) {
+            // one free flight from x along w over [0, d)
+            SvWalk s;
+            sv_walk_begin(P, x, w, s);
+            float t0 = 0.0f, t = 0.0f, density = 0.0f;
+            bool collided = false;
+            while (true) {
+                if (guard(pc)) return color;
+                const int a = sv_walk_axis(s);
+                const float t1 = fminf(s.next[a], d);
+                const float4 c = sv_local_cell(P, s);
+                if (c.w > 0.0f && t1 > t0) {
+                    t = t0;
+                    while (true) {
+                        if (guard(pc)) return color;
+                        t += free_path(rng, c.w);
+                        if (t >= t1) break;
+                        density = sample(x + w * t, rng);
+                        pc.lookups++;
+                        const float r = density * c.z;  // density / majorant density
+                        const float xi = rng_next(rng);
+                        if (xi < P.absorb_albedo * r) {
+                            const F3 xa = x + w * t;
+                            record_event(fe, xa, density, P.extinction, depth0 + t);
+                            return P.emission ? color + sample.emission(xa, rng) : color;
+                        }
+                        if (xi < r) {
+                            collided = true;
+                            break;
+                        }
+                    }
+                    if (collided) break;
+                }
+                if (t1 >= d) break;
+                t0 = fmaxf(t0, t1);
+                if (!sv_walk_advance(P, s, a)) break;
+            }
+            if (!collided) break;
+            x = x + w * t;
+            if (P.max_bounces > 0 && ++bounces > P.max_bounces) return color;
+            const F3 next_w = sample_phase(rng, P.g, w);
+            record_event(fe, x, density, P.extinction, depth0 + t);
+            // light selection as in next event tracking (NextEventTracking.glsl:335-364)
+            bool to_light = false;
+            float prob_factor = 1.0f, light_dist = 0.0f, pdf_light = 0.0f;
+            int light_idx = 0;
+            F3 dir_light;
+            if (P.num_lights > 0) {
+                to_light = P.env_is_black ? true : (rng_next(rng) > 0.5f);
+                prob_factor = P.env_is_black ? 1.0f : 2.0f;
+            }
+            if (to_light) dir_light = light_direction(P, x, rng, light_idx, prob_factor, light_dist);
+            else dir_light = importance_sample_sky(P, rng, pdf_light);
+            const float pdf_phase = evaluate_phase(P.g, w, dir_light);
+            w = next_w;
+            if (to_light) {
+                const float tr = shadow_residual_ratio(P, sample, rng, x, dir_light, light_dist, pc);
+                const float f = (prob_factor * pdf_phase) * tr;
+                const F3 l = light_radiance(P, x, light_idx);
+                color = color + f3(f * l.x, f * l.y, f * l.z);
+            } else {
+                const float tr = shadow_residual_ratio(P, sample, rng, x, dir_light, INFINITY, pc);
+                const float f = ((prob_factor * pdf_phase) / pdf_light) * tr;
+                const F3 l = sky_and_sun(P, dir_light);
+                color = color + f3(f * l.x, f * l.y, f * l.z);
+            }
+            if (!ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) break;
+            x = x + w * tmin;
+            d = tmax - tmin;
+        }
+    }
+    if (!fe.has) color = color + sky_and_sun(P, w);
+    return color;
+}
+
 }  // namespace vpt

@@ -513,7 +513,14 @@ def read_features(vpt, img: torch.Tensor) -> dict:
     return f
 
 
-TARGET_FRAME_ORIGIN = 1 << 24  # targets use frames disjoint from the noisy inputs'
+def target_seed_offset(width: int, height: int) -> int:
+    """Seed offset of target renders: the seed of a path is (frame * W * H + pixel + offset) mod 2^32
+    (Clouds.glsl:80-84), so frame indices alone repeat every 2^32 / (W * H) frames.  Half the pixel
+    count is not a multiple of W * H, so the targets' seeds of a pixel (frames 0 .. 2^32 / (W * H) - 1)
+    differ from every seed the noisy inputs use at offset 0."""
+    return (width * height) // 2
+
+
 FEATURE_FRAMES = 2  # feature maps are accumulated over the first 2 frames (first-hit features converge fast)
 
 
@@ -521,8 +528,8 @@ def render_scene_levels(vpt, sc: dict, size: int, spp_levels: Sequence[int], tar
                         max_bounces: int = 64, second_moment: bool = False) -> dict:
     """Noisy renders of one scene after each sample count in spp_levels (nested: the frames of a
     level include the previous level's) with their features (and, with second_moment, the mean
-    square of the frames' radiance), and the target (target_spp frames from a disjoint frame
-    range), all on the GPU."""
+    square of the frames' radiance), and the target (target_spp frames whose seeds differ from the
+    inputs', see target_seed_offset), all on the GPU."""
     setup_scene(vpt, sc, grid, max_bounces)
     vpt.set_use_feature_maps(["Albedo", "Normal", "Depth", "Transmittance"])
     vpt.set_feature_frame_limit(FEATURE_FRAMES)
@@ -539,7 +546,10 @@ def render_scene_levels(vpt, sc: dict, size: int, spp_levels: Sequence[int], tar
     vpt.set_use_feature_maps([])
     vpt.set_feature_frame_limit(0)
     vpt.set_collect_statistics(False)
-    vpt.set_frame_index(TARGET_FRAME_ORIGIN)
+    if target_spp * size * size > (1 << 32):
+        raise ValueError("target_spp exceeds the distinct seeds of one seed offset at this size")
+    vpt.set_seed_offset(target_seed_offset(size, size))
+    vpt.set_frame_index(0)
     left = target_spp
     tgt = None
     while left > 0:
@@ -547,6 +557,7 @@ def render_scene_levels(vpt, sc: dict, size: int, spp_levels: Sequence[int], tar
         tgt = vpt.render_frame(img, k)
         left -= k
     target = tgt.clone()
+    vpt.set_seed_offset(0)
     vpt.set_frame_index(0)
     return dict(levels=levels, target=target)
 

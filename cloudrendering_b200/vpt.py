@@ -34,6 +34,9 @@ VPT_MODE_NAMES = [
     "Delta Tracking", "Delta Tracking (Spectral)", "Ratio Tracking", "Decomposition Tracking",
     "Residual Ratio Tracking", "Next Event Tracking", "Next Event Tracking (Spectral)", "Isosurfaces",
     "Ray Marching (Emission/Absorption)",
+    # no reference counterpart: next-event estimation with residual-ratio-tracked shadow rays and
+    # supervoxel-majorant free paths (the reference's residual ratio mode is a biased estimator)
+    "Residual Ratio Tracking (Unbiased)",
 ]
 # RenderSettings.hpp:56-58
 GRID_INTERPOLATION_TYPE_NAMES = ["Nearest", "Stochastic", "Trilinear"]
@@ -73,6 +76,7 @@ class _State:
     torch_denoiser = None
     torch_denoiser_loaded = ""
     user_feature_maps: List[int] = []
+    feature_map_type: int = 0  # set_feature_map_type: the map render_frame returns (0 = Result)
 
 
 S = _State()
@@ -303,6 +307,15 @@ def load_transfer_function_file(tf_file_path: str) -> None:
 
 def set_max_grid_extent(max_grid_extent: float) -> None:
     _c("vpt_set_max_grid_extent", float(max_grid_extent))
+
+
+def set_global_world_bounding_box(global_bb_vec: List[float]) -> None:
+    """Places NanoVDB grids loaded afterwards by this world box [xmin, xmax, ymin, ymax, zmin, zmax]
+    instead of their own (Module.cpp:1383-1388; CloudData::computeSparseGridMetadata)."""
+    if len(global_bb_vec) != 6:
+        raise RuntimeError("Error in set_global_world_bounding_box: Expected vector of size 6.")
+    b = [float(v) for v in global_bb_vec]
+    _c("vpt_set_global_world_bounding_box", farr([b[0], b[2], b[4]]), farr([b[1], b[3], b[5]]))
 
 
 def get_render_bounding_box() -> List[float]:
@@ -548,6 +561,76 @@ def load_environment_map(filename: str) -> None:
     load_environment_map_from_tensor(torch.from_numpy(arr).permute(2, 0, 1).contiguous())
 
 
+# ---- environment-map rotation (Module.cpp:96-101, 979-1014; VolumetricPathTracingPass.cpp:1218-1284;
+# the matrices of RotationWidget::getMat3, src/Utils/RotationWidget.cpp:62-77) ----
+def _rot_x(a):
+    c, s_ = math.cos(a), math.sin(a)
+    return np.array([[1.0, 0.0, 0.0], [0.0, c, -s_], [0.0, s_, c]])
+
+
+def _rot_y(a):
+    c, s_ = math.cos(a), math.sin(a)
+    return np.array([[c, 0.0, s_], [0.0, 1.0, 0.0], [-s_, 0.0, c]])
+
+
+def _rot_z(a):
+    c, s_ = math.cos(a), math.sin(a)
+    return np.array([[c, -s_, 0.0], [s_, c, 0.0], [0.0, 0.0, 1.0]])
+
+
+def _quat_matrix(x, y, z, w):
+    """Rotation matrix of the quaternion w + xi + yj + zk (glm::toMat3 of a unit quaternion)."""
+    return np.array([[1 - 2 * (y * y + z * z), 2 * (x * y - w * z), 2 * (x * z + w * y)],
+                     [2 * (x * y + w * z), 1 - 2 * (x * x + z * z), 2 * (y * z - w * x)],
+                     [2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y)]])
+
+
+def _set_env_rotation(m) -> None:
+    """m: 3x3 row-major rotation (envMapDirRot); passed column-major to the core."""
+    cm = np.asarray(m, np.float64).T.reshape(-1)
+    _c("vpt_set_env_map_rotation", farr([float(np.float32(v)) for v in cm]))
+
+
+def disable_env_map_rot() -> None:
+    _c("vpt_set_env_map_rotation", None)
+
+
+def set_env_map_rot_camera() -> None:
+    """The environment image rotates with the camera (envMapRot = the view matrix, every frame)."""
+    _c("vpt_set_env_map_rotation_camera")
+
+
+def set_env_map_rot_euler_angles(euler_angles_vec: List[float]) -> None:
+    """glm::eulerAngleYXZ(x, y, z) (radians): rotation about y by x, then x by y, then z by z."""
+    a, b, c = _vec3(euler_angles_vec, "set_env_map_rot_euler_angles")
+    _set_env_rotation(_rot_y(a) @ _rot_x(b) @ _rot_z(c))
+
+
+def set_env_map_rot_yaw_pitch_roll(yaw_pitch_roll_vec: List[float]) -> None:
+    """glm::yawPitchRoll(yaw, pitch, roll) (radians), the same matrix as the YXZ Euler angles."""
+    a, b, c = _vec3(yaw_pitch_roll_vec, "set_env_map_rot_yaw_pitch_roll")
+    _set_env_rotation(_rot_y(a) @ _rot_x(b) @ _rot_z(c))
+
+
+def set_env_map_rot_angle_axis(_axis_vec: List[float], _angle: float) -> None:
+    """glm::toMat3(glm::angleAxis(angle, axis / |axis|)) (the axis is used as given when shorter than 1e-6)."""
+    ax = np.array(_vec3(_axis_vec, "set_env_map_rot_angle_axis"), np.float64)
+    n = float(np.linalg.norm(ax))
+    if n > 1e-6:
+        ax = ax / n
+    h = 0.5 * float(_angle)
+    sh = math.sin(h)
+    _set_env_rotation(_quat_matrix(ax[0] * sh, ax[1] * sh, ax[2] * sh, math.cos(h)))
+
+
+def set_env_map_rot_quaternion(_quaternion_vec: List[float]) -> None:
+    """glm::toMat3 of the quaternion given as (x, y, z, w) (parseQuaternion, Module.cpp:858-868)."""
+    if len(_quaternion_vec) != 4:
+        raise RuntimeError("Error in parseQuaternion: Expected vector of size 4.")
+    x, y, z, w = (float(v) for v in _quaternion_vec)
+    _set_env_rotation(_quat_matrix(x, y, z, w))
+
+
 # ---- camera (VolumetricPathTracingModuleRenderer.cpp:303-324, Module.cpp:1282-1328) ----
 def get_camera_position() -> List[float]:
     return list(S.cam_pos)
@@ -637,6 +720,8 @@ def _ensure_torch_denoiser():
 
 def _apply_feature_maps() -> None:
     ids = list(S.user_feature_maps)
+    if S.feature_map_type != 0:
+        ids.append(S.feature_map_type)
     if S.torch_denoiser_active and S.torch_denoiser is not None:
         ids += [_FEATURE_BY_NAME[n] for n in S.torch_denoiser.renderer_feature_maps()]
     ids = sorted(set(ids))
@@ -649,6 +734,17 @@ def set_denoiser_property(key: str, value: str) -> None:
 
 
 # ---- feature maps ----
+def set_feature_map_type(type: int) -> None:  # noqa: A002 (the reference's argument name)
+    """The feature map that render_frame returns instead of the result (setFeatureMapType,
+    Module.cpp:1078-1081; VolumetricPathTracingPass.cpp:2287-2400 blits it as the scene image).  The
+    map is accumulated while it is selected; 0 (Result) restores the radiance output."""
+    t = int(type)
+    if t != 0 and t not in _FEATURE_CHANNELS:
+        raise RuntimeError(f"Error in setFeatureMapType: feature map {t} is not supported.")
+    S.feature_map_type = t
+    _apply_feature_maps()
+
+
 def set_use_feature_maps(feature_map_names: List[str]) -> None:
     S.user_feature_maps = [_FEATURE_BY_NAME[n] for n in feature_map_names if n in _FEATURE_BY_NAME]
     _apply_feature_maps()
@@ -731,6 +827,17 @@ def render_frame(input_tensor: torch.Tensor, frame_count: int) -> torch.Tensor:
     _c("vpt_set_resolution", int(w), int(h))
     S.last_hw = (int(h), int(w))
     _c("vpt_render_frames", int(frame_count), _stream_of(input_tensor))
+    if S.feature_map_type != 0:
+        # the map blitted into the C-channel scene image: missing colour channels 0, missing alpha 1
+        fm = get_feature_map(input_tensor, S.feature_map_type)
+        k = fm.size(0)
+        if k == c:
+            return fm
+        out = torch.zeros((c, h, w), dtype=torch.float32, device=fm.device)
+        out[:min(k, c)] = fm[:min(k, c)]
+        if c == 4 and k < 4:
+            out[3] = 1.0
+        return out
     if not S.torch_denoiser_active:
         return _read(input_tensor, c, "vpt_read_result")
     probe = torch.empty((4, h, w), dtype=torch.float32, device=torch.device("cuda", S.device))
@@ -791,3 +898,9 @@ def reset_stats() -> None:
 def context_handle() -> int:
     """Raw VptContext* of the module's renderer (for C-ABI level tooling)."""
     return _ctx()
+
+
+# torch.ops.vpt.<name> (the reference's TORCH_LIBRARY(vpt) registrations, Module.cpp:186-280)
+from . import torch_ops as _torch_ops  # noqa: E402
+
+_torch_ops.register(__import__(__name__, fromlist=["_"]))

@@ -46,7 +46,13 @@ enum {
     VPT_MODE_NEXT_EVENT_TRACKING = 5,
     VPT_MODE_NEXT_EVENT_TRACKING_SPECTRAL = 6,
     VPT_MODE_ISOSURFACE_RENDERING = 7,
-    VPT_MODE_RAY_MARCHING_EMISSION_ABSORPTION = 8
+    VPT_MODE_RAY_MARCHING_EMISSION_ABSORPTION = 8,
+    /* No counterpart in the reference, whose residual ratio mode (4) is a biased reservoir estimator
+     * (ResidualRatioTracking.glsl, marked work in progress): next-event estimation with residual ratio
+     * tracking (Novak et al. 2014) for the shadow rays over the supervoxel (mu_c, mu_r_bar) grid of
+     * SuperVoxelGrid.cpp:218-265, and delta tracking with per-supervoxel majorants for the free paths.
+     * Dense grids only. */
+    VPT_MODE_RESIDUAL_RATIO_TRACKING_UNBIASED = 9
 };
 
 /* GridInterpolationType (RenderSettings.hpp:51-55). */
@@ -154,6 +160,11 @@ VptStatus vpt_set_voxel_size(VptContext* ctx, double sx, double sy, double sz);
 VptStatus vpt_set_max_grid_extent(VptContext* ctx, float max_grid_extent);
 /* Returns boxMin (3 floats) then boxMax (3 floats) in world space (vpt.get_render_bounding_box). */
 VptStatus vpt_get_render_bounding_box(VptContext* ctx, float out_min_max[6]);
+/* setGlobalWorldBoundingBox (Module.cpp:1383-1388, CloudData.cpp:1274-1349): NanoVDB grids loaded
+ * afterwards are placed by this world box instead of their own (the largest side of the global box
+ * spans 2 * max grid extent); box_min / box_max NULL clears it.  Grids built from dense data ignore it,
+ * as in the reference. */
+VptStatus vpt_set_global_world_bounding_box(VptContext* ctx, const float box_min[3], const float box_max[3]);
 
 /* ---- settings (VolumetricPathTracingPass setters, .hpp:137-212) ---- */
 VptStatus vpt_set_vpt_mode(VptContext* ctx, int mode);                     /* setVptMode */
@@ -178,6 +189,13 @@ VptStatus vpt_set_sky_color(VptContext* ctx, const float rgb[3]);
  * equirectangular, row-major; builds the 4096^2 octahedral importance pyramid on the device. */
 VptStatus vpt_load_environment_map_rgba(VptContext* ctx, const float* rgba, int width, int height,
                                         int is_linear_rgb, int data_on_device);
+/* Environment-image rotation (USE_ENV_MAP_ROTATION, VptUtils.glsl:142-153, 303-306;
+ * VolumetricPathTracingPass.cpp:1218-1284, 2102-2113): lookups use envMapDirRot * dir, importance
+ * samples invEnvMapDirRot * dir.  `rotation` is a 3x3 matrix, column-major; NULL disables the rotation
+ * (disableEnvMapRot).  Applies to environment images only, as in the reference. */
+VptStatus vpt_set_env_map_rotation(VptContext* ctx, const float rotation[9]);
+/* setEnvMapRotCamera: the rotation follows the camera's view matrix (its upper 3x3) each frame. */
+VptStatus vpt_set_env_map_rotation_camera(VptContext* ctx);
 
 /* ---- camera (VolumetricPathTracingModuleRenderer.cpp:124-131, 303-324) ----
  * Right-handed look-at view, perspective projection with depth in [0, 1] and y flipped so that
@@ -260,6 +278,11 @@ VptStatus vpt_build_supervoxel_grid(const float* density, int nx, int ny, int nz
  * (SuperVoxelGridResidualRatioTracking::recomputeSuperVoxels, SuperVoxelGrid.cpp:218-256). */
 VptStatus vpt_build_rrt_params(const float* sv_min, const float* sv_max, const float* sv_avg, int count,
                                float extinction, int sv, float* out_pairs, void* stream);
+/* No counterpart in the reference: the supervoxel grid of VPT_MODE_RESIDUAL_RATIO_TRACKING_UNBIASED,
+ * 4 floats per supervoxel: (mu_c, mu_r_bar) as vpt_build_rrt_params, then 1 / max and
+ * 1 / (extinction * max) of the supervoxel's largest normalised density (0 when that is 0). */
+VptStatus vpt_build_residual_ratio_grid(const float* sv_min, const float* sv_max, const float* sv_avg, int count,
+                                        float extinction, int sv, float* out4, void* stream);
 /* Occupancy of block^3 blocks: 1 if any voxel (plus `halo` voxels around) exceeds `threshold`
  * (intent of OccupancyGridPass / ComputeOccupancyGrid.glsl:91-143, whose loop never runs). */
 VptStatus vpt_build_occupancy_grid(const float* density, int nx, int ny, int nz, int block, int halo,

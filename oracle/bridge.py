@@ -42,6 +42,8 @@ class OracleScene(ctypes.Structure):
         ("emission_box_min", c_float * 3), ("emission_vox_per_unit", c_float * 3), ("emission_cap", c_float),
         ("emission_strength", c_float), ("tf", c_void_p), ("tf_size", c_int),
         ("use_iso", c_int), ("iso_value", c_float), ("iso_color", c_float * 3), ("iso_subdivisions", c_int),
+        ("sv_inv_world", c_float * 3), ("sv_local", c_void_p),
+        ("env_rot", c_int), ("env_rot_m", c_float * 9),
     ]
 
 
@@ -67,6 +69,7 @@ def load():
         lib.oracle_supervoxel_stats.argtypes = [c_void_p, c_int, c_int, c_int, c_int, c_int, c_void_p, c_void_p,
                                                 c_void_p, c_void_p]
         lib.oracle_rrt_params.argtypes = [c_void_p, c_void_p, c_void_p, c_int, c_float, c_int, c_void_p]
+        lib.oracle_rrt_local.argtypes = [c_void_p, c_void_p, c_void_p, c_int, c_float, c_int, c_void_p]
         lib.oracle_occupancy.argtypes = [c_void_p, c_int, c_int, c_int, c_int, c_int, c_float, c_void_p]
         lib.oracle_env_pyramid.argtypes = [c_void_p, c_int, c_int, c_int, c_void_p]
         lib.oracle_svgf_frame.argtypes = [c_void_p] * 9 + [c_int, c_int, c_float, c_float, c_int, c_void_p]
@@ -142,6 +145,13 @@ def rrt_params(mn, mx, avg, extinction, sv):
     return out
 
 
+def rrt_local(mn, mx, avg, extinction, sv):
+    """Supervoxel grid of the unbiased residual ratio tracker: 4 floats per supervoxel."""
+    out = np.empty(mn.size * 4, np.float32)
+    load().oracle_rrt_local(_p(mn), _p(mx), _p(avg), mn.size, extinction, sv, _p(out))
+    return out
+
+
 def occupancy(dens, bs=8, halo=0, threshold=0.0):
     nz, ny, nx = dens.shape
     gx, gy, gz = -(-nx // bs), -(-ny // bs), -(-nz // bs)
@@ -197,7 +207,8 @@ class Scene:
             self.set(k, v)
 
     def set(self, k, v):
-        if k in ("density", "sv_data", "occupancy", "env_rgba", "env_pyramid", "nanovdb", "emission", "tf"):
+        if k in ("density", "sv_data", "occupancy", "env_rgba", "env_pyramid", "nanovdb", "emission", "tf",
+                 "sv_local"):
             arr = None if v is None else np.ascontiguousarray(v)
             self._keep[k] = arr
             setattr(self.s, k, None if arr is None else arr.ctypes.data_as(c_void_p).value)

@@ -29,7 +29,7 @@ class RefScene(ctypes.Structure):
         ("emission", c_void_p), ("enx", c_int), ("eny", c_int), ("enz", c_int),
         ("emission_box_min", c_float * 3), ("emission_box_max", c_float * 3), ("emission_cap", c_float),
         ("emission_strength", c_float), ("tf", c_void_p), ("tf_size", c_int),
-        ("iso_value", c_float), ("iso_color", c_float * 3),
+        ("iso_value", c_float), ("iso_color", c_float * 3), ("env_rot", c_float * 9),
     ]
 
 

@@ -12,6 +12,9 @@
 4. ``libref_nanovdb_builder.so``: the reference's vendored NanoVDB GridBuilder
    (src/nanovdb/util/GridBuilder.h) driven as CloudData::getSparseDensityField drives it
    (``ref_nanovdb_builder.cpp``).
+5. ``libref_supervoxel.so``: the reference's supervoxel grid builders and density-field normalisation
+   (src/PathTracer/SuperVoxelGrid.cpp, src/DensityField.cpp) compiled unmodified against the small
+   glm / sgl / Vulkan stand-ins of ``ref_cpp_shim/`` (``ref_supervoxel_driver.cpp``).
 
 The reference tree is read from $VPT_REFERENCE_ROOT, else from a directory named ``reference`` beside
 this repository's root; when it is absent the build is skipped (the prebuilt libraries under
@@ -95,6 +98,10 @@ def variants():
     for t, tdef in SPECTRAL.items():
         out.append((f"{t}_hist_tf__stochastic__default__linear",
                     [tdef, SDT_PROB["hist"], INTERPS["stochastic"], "USE_TRANSFER_FUNCTION"] + ENVS["default__linear"], 0))
+    # environment-image rotation (USE_ENV_MAP_ROTATION, VolumetricPathTracingPass.cpp:1708-1710)
+    for t in ("delta", "nee"):
+        out.append((f"{t}_rot__stochastic__image__linear", TRACKERS[t] + [INTERPS["stochastic"]] + ENVS["image__linear"]
+                    + ["USE_ENV_MAP_ROTATION"], 0))
     # isosurfaces inside the volume (USE_ISOSURFACES; VolumetricPathTracingPass.cpp:1737-1768): density
     # isosurfaces, Lambertian surfaces, 2 subdivisions per free-flight segment, trilinear lookups forced
     # (VolumetricPathTracingPass.cpp:117-120)
@@ -216,12 +223,34 @@ def build_nanovdb(force=False, verbose=False) -> None:
               "-lpthread"], verbose)
 
 
+def build_supervoxel(force=False, verbose=False) -> None:
+    """libref_supervoxel.so: src/PathTracer/SuperVoxelGrid.cpp and src/DensityField.cpp copied unmodified
+    into oracle/_ref/gen/cpp (their quoted includes then resolve to oracle/ref_cpp_shim) and compiled
+    with ref_supervoxel_driver.cpp."""
+    srcs = [os.path.join(REF, "src", "PathTracer", "SuperVoxelGrid.cpp"),
+            os.path.join(REF, "src", "PathTracer", "SuperVoxelGrid.hpp"),
+            os.path.join(REF, "src", "DensityField.cpp"), os.path.join(REF, "src", "DensityField.hpp")]
+    drv = os.path.join(HERE, "ref_supervoxel_driver.cpp")
+    shim = os.path.join(HERE, "ref_cpp_shim")
+    lib = os.path.join(OUT, "libref_supervoxel.so")
+    if not _stale(lib, [drv, os.path.join(shim, "ref_cpp_shim.h"), __file__], force):
+        return
+    gen = os.path.join(GEN, "cpp")
+    os.makedirs(gen, exist_ok=True)
+    for src in srcs:
+        with open(src, "rb") as fi, open(os.path.join(gen, os.path.basename(src)), "wb") as fo:
+            fo.write(fi.read())
+    _run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-ffp-contract=off", "-w", "-I", shim, "-I", gen, "-o", lib,
+          os.path.join(gen, "SuperVoxelGrid.cpp"), os.path.join(gen, "DensityField.cpp"), drv], verbose)
+
+
 def build(force=False, verbose=False) -> None:
     if not os.path.isdir(SHADERS):
         return
     os.makedirs(OUT, exist_ok=True)
     build_tracer(force, verbose)
     build_nanovdb(force, verbose)
+    build_supervoxel(force, verbose)
 
 
 if __name__ == "__main__":

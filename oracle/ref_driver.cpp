@@ -83,6 +83,7 @@ typedef struct RefScene {
     int tf_size;
     float iso_value;          /* parameters.isoValue (USE_ISOSURFACES variants) */
     float iso_color[3];       /* parameters.isoSurfaceColor */
+    float env_rot[9];         /* parameters.envMapDirRot, column-major (USE_ENV_MAP_ROTATION variants) */
 } RefScene;
 
 int ref_variant_count(void) { return ref_num_variants; }
@@ -129,6 +130,11 @@ int ref_render(int variant, const RefScene* s, float* out_rgba, int threads) {
     for (int c = 0; c < 4; c++)
         p.inverseViewMatrix.c[c] = vec4(s->inv_view[c * 4 + 0], s->inv_view[c * 4 + 1], s->inv_view[c * 4 + 2],
                                         s->inv_view[c * 4 + 3]);
+    // envMapDirRot and its transpose invEnvMapDirRot (VolumetricPathTracingPass.cpp:2108-2113)
+    for (int c = 0; c < 3; c++) {
+        p.envMapDirRot.c[c] = vec3(s->env_rot[c * 3 + 0], s->env_rot[c * 3 + 1], s->env_rot[c * 3 + 2]);
+        p.invEnvMapDirRot.c[c] = vec3(s->env_rot[0 * 3 + c], s->env_rot[1 * 3 + c], s->env_rot[2 * 3 + c]);
+    }
     for (int i = 0; i < 16; i++) {
         const float* L = s->lights + 16 * i;
         Light& l = g_ref.lights[i];

@@ -173,7 +173,20 @@ V3 env_fetch(const OracleScene& S, float u, float v) {
     for (int c = 0; c < 3; c++) o[c] = mixf(mixf(c00[c], c10[c], ax), mixf(c01[c], c11[c], ax), ay);
     return v3(o[0], o[1], o[2]);
 }
+// USE_ENV_MAP_ROTATION (VptUtils.glsl:142-153, 303-306): parameters.envMapDirRot * v (column-major,
+// columns summed in order) and the transpose invEnvMapDirRot * v
+V3 env_rot(const OracleScene& S, V3 v) {
+    const float* m = S.env_rot_m;
+    return v3((m[0] * v.x + m[3] * v.y) + m[6] * v.z, (m[1] * v.x + m[4] * v.y) + m[7] * v.z,
+              (m[2] * v.x + m[5] * v.y) + m[8] * v.z);
+}
+V3 env_rot_inv(const OracleScene& S, V3 v) {
+    const float* m = S.env_rot_m;
+    return v3((m[0] * v.x + m[1] * v.y) + m[2] * v.z, (m[3] * v.x + m[4] * v.y) + m[5] * v.z,
+              (m[6] * v.x + m[7] * v.y) + m[8] * v.z);
+}
 V3 sky_image(const OracleScene& S, V3 dir) {
+    if (S.env_rot) dir = env_rot(S, dir);
     float u = m_atan2(dir.z, dir.x) / TWO_PI + 0.5f;
     float v = -m_asin(dir.y) / PI + 0.5f;
     V3 c = env_fetch(S, u, v);
@@ -244,7 +257,8 @@ V3 sample_env_image(const OracleScene& S, const size_t* off, Rng& r, float& pdf)
         }
     }
     float inv = 1.0f / (float)(1 << S.env_levels);
-    return oct_to_world(((float)px + rx) * inv, ((float)py + ry) * inv);
+    const V3 dir = oct_to_world(((float)px + rx) * inv, ((float)py + ry) * inv);
+    return S.env_rot ? env_rot_inv(S, dir) : dir;
 }
 
 // ---- NanoVDB float grids: the read path of PNanoVDB.glsl restated ----
@@ -1514,6 +1528,159 @@ struct Tracer {
         return add(acc, v3(l.x * T, l.y * T, l.z * T));
     }
 
+    // ---- unbiased residual ratio tracking (no reference counterpart; the CUDA core's
+    // track_residual_ratio_nee): next-event estimation with residual ratio tracking (Novak et al.
+    // 2014) for the shadow rays over the supervoxel (mu_c, mu_r_bar) of SuperVoxelGrid.cpp:218-265, and
+    // delta tracking with each supervoxel's majorant (extinction * largest density incl. a one-voxel
+    // halo) for the free paths; empty supervoxels are crossed without random numbers.  sv_local: 4
+    // floats per supervoxel (mu_c, mu_r_bar, 1 / max, 1 / majorant).
+    struct Walk {
+        int idx[3], step[3];
+        float next[3], delta[3];
+    };
+    void walk_begin(V3 x, V3 w, Walk& s) const {
+        const float xv[3] = {x.x, x.y, x.z}, wv[3] = {w.x, w.y, w.z};
+        const int n[3] = {S.svx, S.svy, S.svz};
+        for (int a = 0; a < 3; a++) {
+            int i = (int)floorf((xv[a] - S.box_min[a]) * S.sv_inv_world[a]);
+            i = std::min(std::max(i, 0), n[a] - 1);
+            s.idx[a] = i;
+            if (wv[a] > 0.0f) {
+                s.step[a] = 1;
+                s.next[a] = ((S.box_min[a] + (float)(i + 1) * S.sv_world[a]) - xv[a]) / wv[a];
+                s.delta[a] = S.sv_world[a] / wv[a];
+            } else if (wv[a] < 0.0f) {
+                s.step[a] = -1;
+                s.next[a] = ((S.box_min[a] + (float)i * S.sv_world[a]) - xv[a]) / wv[a];
+                s.delta[a] = -S.sv_world[a] / wv[a];
+            } else {
+                s.step[a] = 0;
+                s.next[a] = INFINITY;
+                s.delta[a] = INFINITY;
+            }
+        }
+    }
+    static int walk_axis(const Walk& s) {
+        return s.next[0] < s.next[1] ? (s.next[0] < s.next[2] ? 0 : 2) : (s.next[1] < s.next[2] ? 1 : 2);
+    }
+    bool walk_advance(Walk& s, int a) const {
+        s.idx[a] += s.step[a];
+        s.next[a] += s.delta[a];
+        const int n = a == 0 ? S.svx : (a == 1 ? S.svy : S.svz);
+        return s.idx[a] >= 0 && s.idx[a] < n;
+    }
+    const float* walk_cell(const Walk& s) const {
+        return S.sv_local + 4 * (((size_t)s.idx[2] * S.svy + s.idx[1]) * S.svx + s.idx[0]);
+    }
+    float transmittance_residual_ratio(V3 x, V3 w, float max_dist, Rng& r) {
+        float tmin, tmax;
+        if (!ray_box(bmin(), bmax(), x, w, tmin, tmax)) return 1.0f;
+        const float d = std::min(tmax, max_dist) - tmin;
+        if (!(d > 0.0f)) return 1.0f;
+        x = add(x, mul(w, tmin));
+        Walk s;
+        walk_begin(x, w, s);
+        float T = 1.0f, t0 = 0.0f;
+        while (true) {
+            if (guard()) return 0.0f;
+            const int a = walk_axis(s);
+            const float t1 = std::min(s.next[a], d);
+            const float* c = walk_cell(s);
+            if (c[3] > 0.0f && t1 > t0) {
+                T *= m_exp(-c[0] * (t1 - t0));
+                const float inv_mu_r = 1.0f / c[1];
+                float t = t0;
+                while (true) {
+                    if (guard()) return 0.0f;
+                    t += -m_log(std::max(0.0000000001f, 1.0f - rnd(r))) * inv_mu_r;
+                    if (t >= t1) break;
+                    const float dens = sample(add(x, mul(w, t)), r);
+                    T *= 1.0f - (S.extinction * dens - c[0]) * inv_mu_r;
+                }
+            }
+            if (t1 >= d) break;
+            t0 = std::max(t0, t1);
+            if (!walk_advance(s, a)) break;
+        }
+        return T;
+    }
+    V3 residual_ratio_nee(V3 x, V3 w, Rng& r, bool& ev) {
+        V3 color = v3(0, 0, 0);
+        float tmin, tmax;
+        const float absorb = 1.0f - S.albedo;
+        if (ray_box(bmin(), bmax(), x, w, tmin, tmax)) {
+            x = add(x, mul(w, tmin));
+            float d = tmax - tmin;
+            int bounces = 0;
+            while (true) {
+                Walk s;
+                walk_begin(x, w, s);
+                float t0 = 0.0f, t = 0.0f;
+                bool collided = false;
+                while (true) {
+                    if (guard()) return color;
+                    const int a = walk_axis(s);
+                    const float t1 = std::min(s.next[a], d);
+                    const float* c = walk_cell(s);
+                    if (c[3] > 0.0f && t1 > t0) {
+                        t = t0;
+                        while (true) {
+                            if (guard()) return color;
+                            t += -m_log(std::max(0.0000000001f, 1.0f - rnd(r))) * c[3];
+                            if (t >= t1) break;
+                            const float dens = sample(add(x, mul(w, t)), r);
+                            const float ratio = dens * c[2];
+                            const float xi = rnd(r);
+                            if (xi < absorb * ratio) {
+                                ev = true;
+                                return S.emission ? add(color, emission(add(x, mul(w, t)), r)) : color;
+                            }
+                            if (xi < ratio) {
+                                collided = true;
+                                break;
+                            }
+                        }
+                        if (collided) break;
+                    }
+                    if (t1 >= d) break;
+                    t0 = std::max(t0, t1);
+                    if (!walk_advance(s, a)) break;
+                }
+                if (!collided) break;
+                x = add(x, mul(w, t));
+                if (S.max_bounces > 0 && ++bounces > S.max_bounces) return color;
+                V3 nw = sample_phase(r, S.g, w);
+                ev = true;
+                bool to_light = false;
+                float factor = 1.0f, ldist = 0.0f, pdf_l = 0.0f;
+                int lidx = 0;
+                if (S.num_lights > 0) {
+                    to_light = S.env_is_black ? true : (rnd(r) > 0.5f);
+                    factor = S.env_is_black ? 1.0f : 2.0f;
+                }
+                V3 dl = to_light ? light_dir(x, r, lidx, factor, ldist) : importance_sky(r, pdf_l);
+                float pdf_p = eval_phase(S.g, w, dl);
+                w = nw;
+                if (to_light) {
+                    float tr = transmittance_residual_ratio(x, dl, ldist, r);
+                    float f = (factor * pdf_p) * tr;
+                    V3 l = light_rad(x, lidx);
+                    color = add(color, v3(f * l.x, f * l.y, f * l.z));
+                } else {
+                    float tr = transmittance_residual_ratio(x, dl, INFINITY, r);
+                    float f = ((factor * pdf_p) / pdf_l) * tr;
+                    V3 l = sky(dl);
+                    color = add(color, v3(f * l.x, f * l.y, f * l.z));
+                }
+                if (!ray_box(bmin(), bmax(), x, w, tmin, tmax)) break;
+                x = add(x, mul(w, tmin));
+                d = tmax - tmin;
+            }
+        }
+        if (!ev) color = add(color, sky(w));
+        return color;
+    }
+
     // pathTraceSample (Clouds.glsl:73-141): seed, jittered camera ray, tracker
     V3 path(int px, int py, uint32_t frame) {
         steps = 0;
@@ -1534,6 +1701,7 @@ struct Tracer {
             case 2: return ratio(x, w, r, ev);
             case 3: return S.nanovdb ? decomposition_sparse(x, w, r) : decomposition(x, w, r);
             case 4: return rrt(x, w, r);
+            case 9: return residual_ratio_nee(x, w, r, ev);
             default: return nee(x, w, r, ev);
         }
     }
@@ -1560,6 +1728,7 @@ static bool scene_inputs_ok(const OracleScene* s) {
     if ((s->mode == 3 && !s->nanovdb) || s->mode == 4) {
         if (!s->sv_data) return false;
     }
+    if (s->mode == 9 && (!s->sv_local || s->nanovdb)) return false;
     if (s->env_kind == 4 && (!s->env_rgba || !s->env_pyramid)) return false;
     return true;
 }
@@ -1777,6 +1946,25 @@ void oracle_rrt_params(const float* mn, const float* mx, const float* avg, int t
         mu_c = std::min(std::max(mu_c, mu_min), mu_avg);
         out_pairs[2 * i] = mu_c;
         out_pairs[2 * i + 1] = mu_r;
+    }
+}
+
+// Supervoxel grid of the unbiased residual ratio tracker (the CUDA core's rrt_local_kernel): the
+// (mu_c, mu_r_bar) of oracle_rrt_params, then 1 / max and 1 / (extinction * max) (0 when empty).
+void oracle_rrt_local(const float* mn, const float* mx, const float* avg, int total, float extinction, int sv,
+                      float* out4) {
+    const float D = sqrtf(3.0f) * (float)sv;
+    for (int i = 0; i < total; i++) {
+        const float dmax = mx[i];
+        float mu_min = mn[i] * extinction, mu_max = dmax * extinction, mu_avg = avg[i] * extinction;
+        float mu_r = std::max(mu_max - mu_min, 0.1f);
+        float mu_c = mu_min + mu_r * m_pow(2.0f, (1.0f / (D * mu_r)) - 1.0f);
+        mu_c = std::min(std::max(mu_c, mu_min), mu_avg);
+        const bool empty = !(dmax > 0.0f) || !(mu_max > 0.0f);
+        out4[4 * i + 0] = mu_c;
+        out4[4 * i + 1] = mu_r;
+        out4[4 * i + 2] = empty ? 0.0f : 1.0f / dmax;
+        out4[4 * i + 3] = empty ? 0.0f : 1.0f / mu_max;
     }
 }
 

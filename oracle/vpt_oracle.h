@@ -78,6 +78,13 @@ typedef struct OracleScene {
     float iso_value;
     float iso_color[3];
     int iso_subdivisions;
+    /* unbiased residual ratio tracking (mode 9): 1 / sv_world, and 4 floats per supervoxel (mu_c,
+     * mu_r_bar, 1 / max density, 1 / majorant) */
+    float sv_inv_world[3];
+    const float* sv_local;
+    /* USE_ENV_MAP_ROTATION for environment images: envMapDirRot, 3x3 column-major */
+    int env_rot;
+    float env_rot_m[9];
 } OracleScene;
 
 /* Renders width*height*num_frames paths; adds radiance (and its square) per pixel (3 doubles). */
@@ -98,6 +105,8 @@ void oracle_supervoxel_stats(const float* dens, int nx, int ny, int nz, int sv, 
                              float* out_max, float* out_avg, uint8_t* out_occ);
 void oracle_rrt_params(const float* mn, const float* mx, const float* avg, int total, float extinction, int sv,
                        float* out_pairs);
+void oracle_rrt_local(const float* mn, const float* mx, const float* avg, int total, float extinction, int sv,
+                      float* out4);
 void oracle_occupancy(const float* dens, int nx, int ny, int nz, int bs, int halo, float threshold, uint8_t* out);
 void oracle_env_pyramid(const float* rgba, int w, int h, int levels, float* pyramid);
 

@@ -93,6 +93,12 @@ def cases():
         kw2 = dict(base)
         kw2.update(kw)
         out["fbm_" + name] = SceneSpec(grid=fbm, tf=transfer_function_table(), emission_strength=2.5, **kw2)
+    # environment-image rotation (USE_ENV_MAP_ROTATION): envMapDirRot = glm::eulerAngleYXZ(0.7, -0.4, 0.25)
+    for name, kw in {"delta_env_image_rot": dict(mode="delta"), "nee_env_image_rot": dict(mode="nee")}.items():
+        kw2 = dict(base)
+        kw2.update(kw)
+        kw2.update(env="image", env_rgba=env_image(), env_rot=env_rotation())
+        out["fbm_" + name] = SceneSpec(grid=fbm, **kw2)
     # isosurfaces inside the volume (USE_ISOSURFACES, density field, Lambertian surfaces, delta tracking
     # with trilinear lookups): the reference's default surface, and a thinner medium with a coloured one
     for name, kw in {"delta_iso": dict(iso_value=0.5),
@@ -104,6 +110,21 @@ def cases():
     return out
 
 
+def env_rotation():
+    """glm::eulerAngleYXZ(0.7, -0.4, 0.25) as 9 floats, column-major (R = Ry(0.7) Rx(-0.4) Rz(0.25))."""
+    def ry(a):
+        return np.array([[np.cos(a), 0, np.sin(a)], [0, 1, 0], [-np.sin(a), 0, np.cos(a)]])
+
+    def rx(a):
+        return np.array([[1, 0, 0], [0, np.cos(a), -np.sin(a)], [0, np.sin(a), np.cos(a)]])
+
+    def rz(a):
+        return np.array([[np.cos(a), -np.sin(a), 0], [np.sin(a), np.cos(a), 0], [0, 0, 1]])
+
+    m = ry(0.7) @ rx(-0.4) @ rz(0.25)
+    return tuple(float(v) for v in m.T.reshape(-1).astype(np.float32))
+
+
 def transfer_function_table(n=64):
     u = (np.arange(n, dtype=np.float64) + 0.5) / n
     rgba = np.stack([np.clip(1.5 * u, 0, 1), u ** 2, 0.3 * (1 - u), np.clip((u - 0.2) / 0.8, 0, 1) ** 1.5], axis=1)
@@ -113,7 +134,7 @@ def transfer_function_table(n=64):
 FIELDS = ["mode", "interp", "extinction", "albedo", "g", "width", "height", "seed_offset", "env", "linear_rgb",
           "sun_dir", "sun_intensity", "cam_pos", "cam_target", "fovy", "near", "far", "max_grid_extent", "use_ess",
           "env_intensity", "max_bounces", "ess_ref_compat", "lights", "extinction_base", "albedo_rgb", "sdt_prob",
-          "emission_cap", "emission_strength", "iso", "iso_value", "iso_color"]
+          "emission_cap", "emission_strength", "iso", "iso_value", "iso_color", "env_rot"]
 
 
 def depth_map_cases():

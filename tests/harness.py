@@ -15,7 +15,8 @@ from cloudrendering_b200 import _lib
 from cloudrendering_b200._lib import check, farr
 from oracle import bridge
 
-MODE = {"delta": 0, "spectral_delta": 1, "ratio": 2, "decomposition": 3, "rrt": 4, "nee": 5, "spectral_nee": 6}
+MODE = {"delta": 0, "spectral_delta": 1, "ratio": 2, "decomposition": 3, "rrt": 4, "nee": 5, "spectral_nee": 6,
+        "rrt_unbiased": 9}
 INTERP = {"nearest": 0, "stochastic": 1, "trilinear": 2}
 ENV = {"default": 0, "black": 1, "single": 2, "constant_sun": 3, "image": 4}
 
@@ -68,7 +69,7 @@ class SceneSpec:
                  fovy=2.0 * math.atan(0.5), near=0.01, far=100.0, max_grid_extent=0.25, env_rgba=None,
                  use_ess=False, env_intensity=(1.0, 1.0, 1.0), ess_ref_compat=False, lights=None,
                  extinction_base=(1.0, 1.0, 1.0), albedo_rgb=None, sdt_prob=2, emission=None, emission_cap=1.0,
-                 emission_strength=1.0, tf=None, iso=False, iso_value=0.5, iso_color=(0.4, 0.4, 0.4)):
+                 emission_strength=1.0, tf=None, iso=False, iso_value=0.5, iso_color=(0.4, 0.4, 0.4), env_rot=None):
         self.__dict__.update(locals())
         del self.__dict__["self"]
 
@@ -130,6 +131,7 @@ def setup_core(core: Core, sp: SceneSpec):
         core("vpt_load_environment_map_rgba", rgba.ctypes.data_as(ctypes.c_void_p), rgba.shape[1], rgba.shape[0], 1, 0)
     else:
         core("vpt_set_builtin_environment_map", ENV[sp.env])
+    core("vpt_set_env_map_rotation", farr(list(sp.env_rot)) if sp.env_rot is not None else None)
     core("vpt_set_use_empty_space_skipping", 1 if sp.use_ess else 0)
     core("vpt_set_camera", farr(sp.cam_pos), farr(sp.cam_target), farr([0, 1, 0]), sp.fovy, sp.near, sp.far)
     core("vpt_clear_lights")
@@ -300,12 +302,25 @@ def oracle_scene(core, sp: SceneSpec, frames: int, frame_count: int = 0) -> brid
         sc.set("interp", 2)
     sc.set("iso_value", float(np.float32(sp.iso_value)))
     sc.set("iso_color", [float(np.float32(c)) for c in sp.iso_color])
+    if sp.env_rot is not None and sp.env == "image":
+        sc.set("env_rot", 1)
+        sc.set("env_rot_m", [float(np.float32(v)) for v in sp.env_rot])
     # sun direction normalised exactly like vpt_set_sun (float ops in order)
     d = np.array(sp.sun_dir, np.float32)
     dl = np.sqrt(np.float32(np.float32(d[0] * d[0]) + np.float32(d[1] * d[1])) + np.float32(d[2] * d[2]), dtype=np.float32)
     sc.set("sun_dir", [float(np.float32(d[i] / dl)) for i in range(3)])
     ext = f32(sp.extinction)
-    if sp.mode in ("decomposition", "rrt") or sp.use_ess:
+    if sp.mode == "rrt_unbiased":
+        svs = supervoxel_size(nx, ny, nz)
+        delta = [f32(b1) - f32(b0) for b0, b1 in zip(bmin, bmax)]
+        svw = [(f32(svs) * dlt) / f32(n) for dlt, n in zip(delta, (nx, ny, nz))]
+        for k, v in zip(("sv_size", "svx", "svy", "svz"), (svs, -(-nx // svs), -(-ny // svs), -(-nz // svs))):
+            sc.set(k, v)
+        sc.set("sv_world", [float(v) for v in svw])
+        sc.set("sv_inv_world", [float(f32(1.0) / v) for v in svw])
+        mn, mx, avg, _ = bridge.supervoxel_stats(dens, svs, 1)
+        sc.set("sv_local", bridge.rrt_local(mn, mx, avg, float(ext), svs))
+    elif sp.mode in ("decomposition", "rrt") or sp.use_ess:
         nee_like = sp.mode in ("nee", "spectral_nee")
         svs = 8 if sp.use_ess and nee_like else supervoxel_size(nx, ny, nz)
         svx, svy, svz = -(-nx // svs), -(-ny // svs), -(-nz // svs)
@@ -426,6 +441,9 @@ def reference_scene(sp: SceneSpec, frames: int, frame_start: int = 0, inv=None):
     sc.set("iso_color", sp.iso_color)
     if sp.iso:
         tracker += "_iso"
+    if sp.env_rot is not None:
+        sc.set("env_rot", [float(np.float32(v)) for v in sp.env_rot])
+        tracker += "_rot"
     env = {"default": "default", "black": "black", "single": "single", "image": "image"}[sp.env]
     colour = "linear" if (sp.linear_rgb or env != "default") else "srgb"
     return sc, f"{tracker}__{sp.interp}__{env}__{colour}"
@@ -507,4 +525,25 @@ def sparse_golden():
             walks.append((ray[:3], ray[3:], int(lv), {f: a[start:start + n] for f, a in parts.items()}))
         out[name] = dict(buf=z[f"{name}__buf"], ijk=z[f"{name}__ijk"], value=z[f"{name}__value"],
                          dim=z[f"{name}__dim"], active=z[f"{name}__active"], walks=walks, meta=m)
+    return out
+
+
+# ---------------------------------------------------------------------------------------------
+# Supervoxel grids of the reference's own builders (tests/golden/make_supervoxel_golden.py)
+
+SUPERVOXEL_GOLDEN = __import__("os").path.join(__import__("os").path.dirname(__import__("os").path.abspath(__file__)),
+                                               "golden", "supervoxel_grids.npz")
+
+
+def supervoxel_golden():
+    """key -> dict(raw grid, interp, dims (gx, gy, gz, supervoxel size), extinction, minmax, occ_decomposition,
+    rrt, occ_rrt) from SuperVoxelGrid.cpp compiled unmodified."""
+    import json
+
+    z = np.load(SUPERVOXEL_GOLDEN)
+    meta = json.loads(str(z["meta"]))
+    out = {}
+    for key, m in meta.items():
+        out[key] = dict(raw=z[m["grid"] + "__raw"], interp=m["interp"], dims=m["dims"], extinction=m["extinction"],
+                        **{f: z[f"{key}__{f}"] for f in ("minmax", "occ_decomposition", "rrt", "occ_rrt")})
     return out

@@ -224,3 +224,123 @@ def test_isosurfaces():
     vpt.set_vpt_mode_from_name("Delta Tracking")
     vpt.set_grid_interpolation("Stochastic")
     vpt.set_extinction_scale(1024.0)
+
+
+def test_load_xyz_file_grid_and_bounds(tmp_path):
+    """load_cloud_file with a .xyz file: the normalised x-fastest grid reaches the renderer and the
+    render box follows the header's voxel sizes (CloudData::computeGridBounds: size * voxel size,
+    scaled so that the largest side is 2 * max grid extent, centred)."""
+    import ctypes
+    import struct
+
+    from cloudrendering_b200 import _lib
+    from tests.test_xyz_cpu import reference_grid, write_xyz
+
+    sizes, voxel = (6, 4, 5), (0.5, 1.0, 0.75)
+    values = np.random.default_rng(3).random(int(np.prod(sizes))).astype(np.float32)
+    path = str(tmp_path / "cloud.xyz")
+    write_xyz(path, values, sizes, voxel=voxel)
+    vpt.set_max_grid_extent(0.25)
+    vpt.load_cloud_file(path)
+    lib, ctx = _lib.load(), vpt.context_handle()
+    nx, ny, nz = sizes
+    got = np.empty((nz, ny, nx), np.float32)
+    _lib.check(lib.vpt_get_dense_grid(ctx, got.ctypes.data_as(ctypes.c_void_p), 0), "grid", ctx, lib)
+    assert np.array_equal(got, reference_grid(values, sizes))
+    ext = [np.float32(n) * np.float32(v) for n, v in zip(sizes, voxel)]
+    ms = max(ext)
+    half = [float(e * np.float32(0.25) / ms) for e in ext]
+    box = vpt.get_render_bounding_box()
+    assert np.allclose(box, [-half[0], half[0], -half[1], half[1], -half[2], half[2]], rtol=1e-6, atol=0)
+    out = vpt.render_frame(torch.zeros((3, 16, 16), device="cuda"), 1)
+    assert torch.isfinite(out).all()
+    vpt.set_max_grid_extent(0.5)
+
+
+def _sparse_box(wmin, wmax, gmin, gmax, ext):
+    """CloudData::computeSparseGridMetadata (CloudData.cpp:1336-1344) in float32."""
+    f = np.float32
+    wmin, wmax, gmin, gmax = (np.array(v, f) for v in (wmin, wmax, gmin, gmax))
+    diff = gmax - gmin
+    md = diff.max()
+    L = diff / md
+    A = f(2.0) * f(ext) / md
+    B = f(ext) * L - gmax * A
+    return A * wmin + B, A * wmax + B
+
+
+def test_global_world_bounding_box_places_loaded_nanovdb_grids():
+    from tests.harness import sparse_golden
+
+    buf = bytes(sparse_golden()["fbm24"]["buf"])
+    vpt.set_max_grid_extent(0.5)
+    vpt.load_nanovdb_grid(buf)
+    w = vpt.get_vdb_world_bounding_box()
+    wmin, wmax = [w[0], w[2], w[4]], [w[1], w[3], w[5]]
+    lo, hi = _sparse_box(wmin, wmax, wmin, wmax, 0.5)
+    box = vpt.get_render_bounding_box()
+    assert np.allclose(box, [lo[0], hi[0], lo[1], hi[1], lo[2], hi[2]], rtol=1e-6, atol=1e-7)
+    # a global box twice the grid's size, offset: the grid occupies its part of the unit-extent box
+    g = [wmin[0] - 3.0, wmax[0] + 21.0, wmin[1], wmax[1] + 24.0, wmin[2] - 24.0, wmax[2]]
+    vpt.set_global_world_bounding_box(g)
+    vpt.load_nanovdb_grid(buf)
+    lo, hi = _sparse_box(wmin, wmax, [g[0], g[2], g[4]], [g[1], g[3], g[5]], 0.5)
+    box = vpt.get_render_bounding_box()
+    assert np.allclose(box, [lo[0], hi[0], lo[1], hi[1], lo[2], hi[2]], rtol=1e-6, atol=1e-7)
+    out = vpt.render_frame(torch.zeros((3, 16, 16), device="cuda"), 1)
+    assert torch.isfinite(out).all()
+    from cloudrendering_b200 import _lib
+    _lib.check(_lib.load().vpt_set_global_world_bounding_box(vpt.context_handle(), None, None), "clear")
+    vpt.set_use_sparse_grid(False)
+    vpt.generate_fbm_cloud(32, seed=1)
+
+
+def test_feature_map_type_selects_the_returned_image():
+    vpt.set_max_grid_extent(0.5)
+    vpt.generate_fbm_cloud(32, seed=1)
+    vpt.set_use_builtin_environment_map("Default")
+    t = torch.zeros((4, 24, 32), device="cuda")
+    vpt.set_feature_map_type(6)  # Depth: (mean, standard deviation), blitted into RGBA
+    vpt.set_seed_offset(0)
+    depth_img = vpt.render_frame(t, 3).clone()
+    want = vpt.get_feature_map(t, 6)
+    assert torch.equal(depth_img[:2], want[:2])
+    assert torch.all(depth_img[2] == 0) and torch.all(depth_img[3] == 1)
+    assert float(depth_img[0].max()) > 0.0
+    vpt.set_feature_map_type(0)
+    vpt.set_seed_offset(0)
+    res = vpt.render_frame(t, 3)
+    assert not torch.equal(res[:2], depth_img[:2])
+    vpt.set_use_feature_maps([])
+
+
+def test_torch_ops_render_frame_matches_module():
+    vpt.set_vpt_mode_from_name("Delta Tracking")
+    t = torch.zeros((3, 20, 20), device="cuda")
+    torch.ops.vpt.set_seed_offset(5)
+    a = torch.ops.vpt.render_frame(t, 2).clone()
+    vpt.set_seed_offset(5)
+    b = vpt.render_frame(t, 2)
+    assert torch.equal(a, b)
+
+
+def test_env_map_rotation_identity_and_camera():
+    rgba = torch.rand((4, 32, 64), device="cpu") * 2.0
+    rgba[3] = 1.0
+    vpt.load_environment_map_from_tensor(rgba)
+    vpt.set_vpt_mode_from_name("Next Event Tracking")
+    t = torch.zeros((3, 24, 24), device="cuda")
+    vpt.disable_env_map_rot()
+    a = vpt.render_frame(t, 2).clone()
+    vpt.set_env_map_rot_quaternion([0.0, 0.0, 0.0, 1.0])  # identity: the same paths bit for bit
+    b = vpt.render_frame(t, 2).clone()
+    assert torch.equal(a, b)
+    vpt.set_env_map_rot_euler_angles([1.2, 0.3, -0.5])
+    c = vpt.render_frame(t, 2).clone()
+    assert not torch.equal(a, c) and torch.isfinite(c).all()
+    vpt.set_env_map_rot_camera()
+    d = vpt.render_frame(t, 2)
+    assert torch.isfinite(d).all()
+    vpt.disable_env_map_rot()
+    vpt.set_use_builtin_environment_map("Default")
+    vpt.set_vpt_mode_from_name("Delta Tracking")

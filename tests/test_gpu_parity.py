@@ -71,6 +71,62 @@ def test_supervoxel_grid_bit_exact(core, shape, sv, halo):
     assert np.allclose(got[0::2], ref[0::2], rtol=2e-7, atol=0)
 
 
+@pytest.mark.parametrize("key", sorted(__import__("tests.harness", fromlist=["_"]).supervoxel_golden()))
+def test_supervoxel_grid_matches_reference_builder(core, key):
+    """The core's supervoxel builders against SuperVoxelGrid.cpp compiled unmodified (fixture
+    tests/golden/supervoxel_grids.npz): min / max / occupancy bit for bit, mu_r_bar bit for bit, mu_c to
+    one ulp (powf)."""
+    from tests.harness import supervoxel_golden, supervoxel_size
+
+    g = supervoxel_golden()[key]
+    raw = g["raw"]
+    nz, ny, nx = raw.shape
+    sv = supervoxel_size(nx, ny, nz)
+    vmin, vmax = bridge.minmax(raw)
+    d = torch.from_numpy(bridge.normalize(raw, vmin, vmax)).cuda()
+    n = g["occ_rrt"].size
+    mn, mx, avg = (torch.empty(n, device="cuda") for _ in range(3))
+    occ = torch.empty(n, dtype=torch.uint8, device="cuda")
+    lib = core.lib
+    halo = 0 if g["interp"] == 0 else 1
+    assert lib.vpt_build_supervoxel_grid(dptr(d), nx, ny, nz, sv, halo, dptr(mn), dptr(mx), dptr(avg), dptr(occ),
+                                         None) == 0
+    pairs = torch.empty(2 * n, device="cuda")
+    assert lib.vpt_build_rrt_params(dptr(mn), dptr(mx), dptr(avg), n, g["extinction"], sv, dptr(pairs), None) == 0
+    torch.cuda.synchronize()
+    assert np.array_equal(mn.cpu().numpy().view(np.uint32), g["minmax"][0::2].view(np.uint32))
+    assert np.array_equal(mx.cpu().numpy().view(np.uint32), g["minmax"][1::2].view(np.uint32))
+    assert np.array_equal(occ.cpu().numpy(), g["occ_decomposition"])
+    got = pairs.cpu().numpy()
+    assert np.array_equal(got[1::2].view(np.uint32), g["rrt"][1::2].view(np.uint32))
+    assert np.allclose(got[0::2], g["rrt"][0::2], rtol=2e-7, atol=0)
+
+
+def test_residual_ratio_grid_bit_exact(core):
+    """The unbiased residual ratio tracker's supervoxel grid: (mu_c, mu_r_bar) as the reference's
+    formulas (mu_c through powf: one ulp allowed), the majorant reciprocals bit-exact."""
+    g = bridge.fbm((64, 48, 40), 13, base_frequency=3.0, contrast=3.5)
+    g[:8, :8, :8] = 0.0  # an empty supervoxel (its halo reaches the neighbours: one corner cell)
+    nz, ny, nx = g.shape
+    d = torch.from_numpy(g).cuda()
+    sv = 8
+    n = (-(-nx // sv)) * (-(-ny // sv)) * (-(-nz // sv))
+    mn, mx, avg = (torch.empty(n, device="cuda") for _ in range(3))
+    occ = torch.empty(n, dtype=torch.uint8, device="cuda")
+    lib = core.lib
+    assert lib.vpt_build_supervoxel_grid(dptr(d), nx, ny, nz, sv, 1, dptr(mn), dptr(mx), dptr(avg), dptr(occ),
+                                         None) == 0
+    out = torch.empty(4 * n, device="cuda")
+    assert lib.vpt_build_residual_ratio_grid(dptr(mn), dptr(mx), dptr(avg), n, 700.0, sv, dptr(out), None) == 0
+    torch.cuda.synchronize()
+    rmn, rmx, ravg, _ = bridge.supervoxel_stats(g, sv, 1)
+    ref = bridge.rrt_local(rmn, rmx, ravg, 700.0, sv).reshape(-1, 4)
+    got = out.cpu().numpy().reshape(-1, 4)
+    assert np.array_equal(got[:, 1:].view(np.uint32), ref[:, 1:].view(np.uint32))
+    assert np.allclose(got[:, 0], ref[:, 0], rtol=2e-7, atol=0)
+    assert (got[:, 3] == 0).any() and (got[:, 3] > 0).any()
+
+
 @pytest.mark.parametrize("halo", [0, 1])
 def test_occupancy_grid_bit_exact(core, halo):
     g = bridge.fbm((48, 40, 56), 3, base_frequency=3.0, contrast=3.5)
@@ -143,6 +199,12 @@ PATH_CASES = {
     "decomposition": dict(mode="decomposition"),
     "decomposition_trilinear": dict(mode="decomposition", interp="trilinear"),
     "rrt": dict(mode="rrt"),
+    # the unbiased residual ratio tracker (no reference counterpart): every interpolation, lights
+    "rrt_unbiased": dict(mode="rrt_unbiased"),
+    "rrt_unbiased_nearest": dict(mode="rrt_unbiased", interp="nearest"),
+    "rrt_unbiased_trilinear": dict(mode="rrt_unbiased", interp="trilinear"),
+    "rrt_unbiased_lights": dict(mode="rrt_unbiased", lights=[
+        dict(type="Point Light", space="World", position=(0.6, 0.8, 0.3), intensity=0.8, color=(1.0, 0.8, 0.6))]),
     "delta_default_sky": dict(mode="delta", env="default", linear_rgb=0),
     "nee_default_sky_g0": dict(mode="nee", env="default", g=0.0),
     # lights of the light editor: a view-space spot light and a world-space point light; a
@@ -219,7 +281,7 @@ def test_path_parity_environment_image(core):
     assert agree >= AGREE_MIN
 
 
-@pytest.mark.parametrize("case", ["delta_stochastic", "nee", "decomposition", "rrt"])
+@pytest.mark.parametrize("case", ["delta_stochastic", "nee", "decomposition", "rrt", "rrt_unbiased"])
 def test_image_statistics_match_oracle(core, case):
     sp = fbm_scene(**PATH_CASES[case], width=48, height=48)
     frames = 64

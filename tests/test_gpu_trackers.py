@@ -91,7 +91,10 @@ def fbm_spec(mode, **kw):
 
 
 @pytest.mark.parametrize("mode,kw", [("ratio", {}), ("decomposition", {}), ("nee", {}), ("nee", {"use_ess": True}),
-                                     ("decomposition", {"interp": "trilinear"})])
+                                     ("decomposition", {"interp": "trilinear"}),
+                                     ("rrt_unbiased", {"seed_offset": 0x5BD1E995}),
+                                     ("rrt_unbiased", {"interp": "trilinear", "seed_offset": 0x5BD1E995}),
+                                     ("rrt_unbiased", {"interp": "nearest", "seed_offset": 0x5BD1E995})])
 def test_trackers_agree_with_delta_per_pixel(core, mode, kw):
     """Every unbiased tracker agrees with delta tracking on the fBm cloud: per-pixel z-test and the
     image mean within 5 standard errors (NEE's uniform sky sampling of the sun lobe has a heavy
@@ -151,15 +154,34 @@ def test_spectral_delta_chromatic_extinction_matches_per_channel_delta(core):
         assert abs(m0 - m1[c]) <= 5.0 * se
 
 
-def test_reference_residual_ratio_estimator_deviation_is_reported(core):
+def test_delta_unbiased_residual_ratio_equal_mean(core):
+    """The reference suite's equal-mean check on its 8^3 block with the empty boundary layer (128^2,
+    64 spp) for the unbiased residual ratio tracker.  Its estimate has about ten times delta tracking's
+    standard error on this fixture (one supervoxel holds the block and the empty layer, so the control
+    extinction lies between them and the ratio factors reach 1.42), so the bound is 5 standard errors
+    of the difference instead of 1e-3."""
+    g = cloud_block(8, 8, 8, empty_boundary=True)
+    s0, q0 = mean_image(core, spec(g, "delta"))
+    s1, q1 = mean_image(core, spec(g, "rrt_unbiased", seed_offset=0x5BD1E995))
+    n = RES * RES * SPP
+    m0, m1 = s0.sum(axis=(0, 1)) / n, s1.sum(axis=(0, 1)) / n
+    se = np.sqrt((q0.sum(axis=(0, 1)) / n - m0 * m0) / n + (q1.sum(axis=(0, 1)) / n - m1 * m1) / n)
+    print("delta", m0, "unbiased residual ratio", m1, "se", se)
+    assert np.all(np.abs(m0 - m1) <= 5.0 * se)
+
+
+def test_reference_residual_ratio_estimator_is_biased(core):
     """The reference's residual ratio tracking (ResidualRatioTracking.glsl, marked work in progress
-    upstream) does not estimate the same image as delta tracking; the core reproduces it path for
-    path (test_gpu_parity), and this test records the size of its deviation from delta tracking."""
+    upstream) does not estimate the same image as delta tracking.  The core reproduces it path for
+    path (test_gpu_parity); this test pins the size of the deviation on the fBm scene (the oracle
+    gives -0.064, -9 standard errors: mean 0.208 against 0.272), which the unbiased tracker above
+    does not show."""
     frames = 64
     s0, q0 = mean_image(core, fbm_spec("delta"), frames)
     s1, q1 = mean_image(core, fbm_spec("rrt"), frames)
-    m0 = (s0 / frames).mean(axis=(0, 1))
-    m1 = (s1 / frames).mean(axis=(0, 1))
-    rel = float(np.abs(m1 - m0).max() / np.abs(m0).max())
-    print("residual ratio tracking vs delta: relative image-mean deviation", rel)
-    assert np.all(np.isfinite(m1)) and rel < 1.0
+    n = s0.shape[0] * s0.shape[1] * frames
+    m0, m1 = s0.sum(axis=(0, 1)) / n, s1.sum(axis=(0, 1)) / n
+    se = np.sqrt((q0.sum(axis=(0, 1)) / n - m0 * m0) / n + (q1.sum(axis=(0, 1)) / n - m1 * m1) / n)
+    print("reference residual ratio tracking vs delta:", m1, m0, "se", se)
+    assert np.all(np.isfinite(m1))
+    assert np.all(m0 - m1 > 5.0 * se)
