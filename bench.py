@@ -39,6 +39,9 @@ EXTINCTION = 1000.0
 SEED = 2
 TRACKERS = {"delta": 0, "ratio": 2, "decomposition": 3, "residual_ratio": 4, "nee": 5, "residual_ratio_unbiased": 9}
 BYTES_PER_LOOKUP = 32  # one 32-byte sector per uncoalesced density gather
+# DRAM read + write bytes of one headline launch (64 spp of the 1024^2 image on the 512^3 cloud), from
+# one ncu capture of that launch (profiles/trace_refill_delta_512_1024_64spp.md): 866 B per path
+NCU_DRAM_BYTES_PER_PATH = 58.12e9 / (1024 * 1024 * 64)
 
 
 def tensor_peak():
@@ -330,8 +333,12 @@ def run_ours(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded fBm Perlin cloud)",
             "config": workload_config(world),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None,
-                         "note": f"algorithmic bytes = density lookups x {BYTES_PER_LOOKUP} B sector; peak {peak_kind}"},
+                         "frac": achieved / peak,
+                         "traffic": NCU_DRAM_BYTES_PER_PATH * RES * RES * SPP_PER_STEP if args.workload == "full" else None,
+                         "limiter": "instruction issue at low SIMT efficiency (72 % issue active, 11.4 of 32 lanes per "
+                                    "instruction, DRAM 10 % busy; profiles/trace_refill_delta_512_1024_64spp.md)",
+                         "note": f"algorithmic bytes = density lookups x {BYTES_PER_LOOKUP} B sector; peak {peak_kind} "
+                                 "HBM copy; traffic = ncu dram read + write bytes of this launch"},
             "lookups_per_s": lookups / (ms_total / 1e3) * world,
             "lookups_per_path": lookups / max(1, st["paths"]),
             "gather_roofline": gather_roofline,

@@ -12,6 +12,9 @@
 4. ``libref_nanovdb_builder.so``: the reference's vendored NanoVDB GridBuilder
    (src/nanovdb/util/GridBuilder.h) driven as CloudData::getSparseDensityField drives it
    (``ref_nanovdb_builder.cpp``).
+6. ``libref_kpn.so``: the reference's PyTorch KPN extension (modules/kpn_module/src/Kernel.cu with
+   perPixelKernel.cpp, CUDA for sm_100a) and ``ref_kpn_driver.cpp``; GPU tests load it with
+   torch.ops.load_library and compare the core's KPN kernels with the reference's.
 5. ``libref_supervoxel.so``: the reference's supervoxel grid builders and density-field normalisation
    (src/PathTracer/SuperVoxelGrid.cpp, src/DensityField.cpp) compiled unmodified against the small
    glm / sgl / Vulkan stand-ins of ``ref_cpp_shim/`` (``ref_supervoxel_driver.cpp``).
@@ -150,6 +153,60 @@ def transform(text: str) -> str:
     return "\n".join(lines)
 
 
+UNIFORM_BLOCK = re.compile(r"layout\s*\([^)]*\)\s*uniform\s+\w+\s*\{(.*?)\}\s*;", re.S)
+UNIFORM_VAR = re.compile(r"layout\s*\([^)]*\)\s*uniform\s+(?:writeonly\s+|readonly\s+)?(\w+)\s+(\w+)\s*;")
+LOCAL_SIZE = re.compile(r"layout\s*\([^)]*\)\s*in\s*;")
+
+
+def image_shader_section(path: str, section: str) -> str:
+    """One ``-- <section>`` stage of a shader file, with its resource declarations turned into plain
+    declarations: uniform blocks lose their wrapper (members become variables), samplers and images
+    become variables, the work-group size line and ``shared`` qualifiers are dropped; then the
+    transform of the tracer shaders."""
+    with open(path, encoding="utf-8") as fh:
+        text = fh.read()
+    parts = re.split(r"^-- (.+)$", text, flags=re.M)
+    body = dict(zip(parts[1::2], parts[2::2]))[section]
+    body = strip_comments(body)
+    body = UNIFORM_BLOCK.sub(lambda m: m.group(1), body)
+    body = UNIFORM_VAR.sub(lambda m: f"{m.group(1)} {m.group(2)};", body)
+    body = LOCAL_SIZE.sub("", body)
+    body = re.sub(r"^\s*shared\s+", "", body, flags=re.M)
+    # swizzles that name the whole vector: .rgba of a vec4, .rg of a vec2
+    body = body.replace(".rgba", "")
+    vec2_names = sorted(set(re.findall(r"\bvec2\s+(\w+)", body)))
+    if vec2_names:
+        body = re.sub(r"\b(" + "|".join(vec2_names) + r")\.rg\b", r"\1", body)
+    return transform(body)
+
+
+def build_image_shaders(force=False, verbose=False) -> None:
+    """libref_image.so: OctahedralMapper.glsl, the compute stage of EAWDenoise.glsl and the three compute
+    stages of SVGF.glsl on the CPU (ref_image_driver.cpp)."""
+    drv = os.path.join(HERE, "ref_image_driver.cpp")
+    shim = os.path.join(HERE, "ref_shim.h")
+    lib = os.path.join(OUT, "libref_image.so")
+    if not _stale(lib, [drv, shim, __file__], force):
+        return
+    gen = os.path.join(GEN, "img")
+    os.makedirs(gen, exist_ok=True)
+    den = os.path.join(REF, "Data", "Shaders", "Denoiser")
+    svgf = os.path.join(den, "SVGF", "SVGF.glsl")
+    for src, section, name in (
+            (os.path.join(SHADERS, "OctahedralMapper.glsl"), "Compute", "OctahedralMapper.compute.inc"),
+            (os.path.join(den, "EAWDenoise.glsl"), "Compute", "EAWDenoise.compute.inc"),
+            (svgf, "Compute-Reproject", "SVGF.reproject.inc"),
+            (svgf, "Compute-Filter-Moments", "SVGF.filter_moments.inc"),
+            (svgf, "Compute-ATrous", "SVGF.atrous.inc")):
+        with open(os.path.join(gen, name), "w") as fh:
+            fh.write(image_shader_section(src, section))
+    with open(os.path.join(den, "SVGF", "svgf_common.glsl"), encoding="utf-8") as fi, \
+            open(os.path.join(gen, "svgf_common.glsl.inc"), "w") as fo:
+        fo.write(transform(fi.read()))
+    _run(["g++", "-O2", "-std=c++20", "-fPIC", "-shared", "-ffp-contract=off", "-w", "-I", gen, "-I", HERE, "-o", lib,
+          drv], verbose)
+
+
 def generate() -> None:
     os.makedirs(GEN, exist_ok=True)
     # the tracer shaders and the surface BRDFs (Data/Shaders/BRDF, included by the isosurface code)
@@ -244,6 +301,38 @@ def build_supervoxel(force=False, verbose=False) -> None:
           os.path.join(gen, "SuperVoxelGrid.cpp"), os.path.join(gen, "DensityField.cpp"), drv], verbose)
 
 
+def build_kpn(force=False, verbose=False) -> None:
+    """libref_kpn.so: the reference's PyTorch KPN extension (modules/kpn_module/src/Kernel.cu and
+    perPixelKernel.cpp, unmodified; CUDA kernels for sm_100a) with ref_kpn_driver.cpp.  Loaded with
+    torch.ops.load_library on a GPU, it provides torch.ops.per_pixel_kernel.forward and
+    torch.ops.ref_kpn.inv_iter_base."""
+    import torch
+
+    src = os.path.join(REF, "modules", "kpn_module", "src")
+    drv = os.path.join(HERE, "ref_kpn_driver.cpp")
+    lib = os.path.join(OUT, "libref_kpn.so")
+    if not _stale(lib, [drv, __file__], force):
+        return
+    tdir = os.path.dirname(torch.__file__)
+    inc = ["-I", os.path.join(tdir, "include"), "-I", os.path.join(tdir, "include", "torch", "csrc", "api", "include"),
+           "-I", src, "-I", "/usr/local/cuda/include"]
+    defs = ["-DKPN_MODULE_OP_API=", f"-D_GLIBCXX_USE_CXX11_ABI={int(torch._C._GLIBCXX_USE_CXX11_ABI)}"]
+    gen = os.path.join(GEN, "kpn")
+    os.makedirs(gen, exist_ok=True)
+    objs = [os.path.join(gen, n) for n in ("Kernel.o", "perPixelKernel.o", "driver.o")]
+    nvcc = "/usr/local/cuda/bin/nvcc" if os.path.exists("/usr/local/cuda/bin/nvcc") else "nvcc"
+    jobs = [[nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-O2", "-std=c++17", "-Xcompiler", "-fPIC", "-w",
+             *defs, *inc, "-c", os.path.join(src, "Kernel.cu"), "-o", objs[0]],
+            ["g++", "-O2", "-std=c++17", "-fPIC", "-w", *defs, *inc, "-c", os.path.join(src, "perPixelKernel.cpp"),
+             "-o", objs[1]],
+            ["g++", "-O2", "-std=c++17", "-fPIC", "-w", *defs, *inc, "-c", drv, "-o", objs[2]]]
+    with ThreadPoolExecutor(max_workers=3) as ex:
+        list(ex.map(lambda c: _run(c, verbose), jobs))
+    tlib = os.path.join(tdir, "lib")
+    _run(["g++", "-shared", "-o", lib, *objs, "-L", tlib, "-Wl,-rpath," + tlib, "-ltorch", "-ltorch_cpu", "-ltorch_cuda",
+          "-lc10", "-lc10_cuda", "-L", "/usr/local/cuda/lib64", "-lcudart"], verbose)
+
+
 def build(force=False, verbose=False) -> None:
     if not os.path.isdir(SHADERS):
         return
@@ -251,6 +340,8 @@ def build(force=False, verbose=False) -> None:
     build_tracer(force, verbose)
     build_nanovdb(force, verbose)
     build_supervoxel(force, verbose)
+    build_image_shaders(force, verbose)
+    build_kpn(force, verbose)
 
 
 if __name__ == "__main__":

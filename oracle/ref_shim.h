@@ -28,6 +28,7 @@ template <int A, int B>
 struct Sw2 {
     float v[4];
     operator vec2() const;
+    Sw2& operator=(const vec2& o);
 };
 template <int A, int B, int C>
 struct Sw3 {
@@ -38,7 +39,10 @@ struct Sw3 {
 };
 
 struct vec2 {
-    float x, y;
+    union {
+        struct { float x, y; };
+        struct { float r, g; };
+    };
     vec2() : x(0), y(0) {}
     explicit vec2(float s) : x(s), y(s) {}
     vec2(float a, float b) : x(a), y(b) {}
@@ -97,6 +101,12 @@ struct vec4 {
 
 template <int A, int B>
 Sw2<A, B>::operator vec2() const { return vec2(v[A], v[B]); }
+template <int A, int B>
+Sw2<A, B>& Sw2<A, B>::operator=(const vec2& o) {
+    v[A] = o.x;
+    v[B] = o.y;
+    return *this;
+}
 template <int A, int B, int C>
 Sw3<A, B, C>::operator vec3() const { return vec3(v[A], v[B], v[C]); }
 template <int A, int B, int C>

@@ -547,3 +547,50 @@ def supervoxel_golden():
         out[key] = dict(raw=z[m["grid"] + "__raw"], interp=m["interp"], dims=m["dims"], extinction=m["extinction"],
                         **{f: z[f"{key}__{f}"] for f in ("minmax", "occ_decomposition", "rrt", "occ_rrt")})
     return out
+
+
+IMAGE_GOLDEN = __import__("os").path.join(__import__("os").path.dirname(__import__("os").path.abspath(__file__)),
+                                          "golden", "image_filters.npz")
+
+
+def image_golden():
+    """(octahedral maps, EAW cases) of the reference's image shaders (tests/golden/make_image_golden.py):
+    octa: name -> (env RGBA [h, w, 4], map [res, res]); eaw: key -> (color, position, normal, iterations,
+    phi, output)."""
+    import json
+
+    z = np.load(IMAGE_GOLDEN)
+    meta = json.loads(str(z["meta"]))
+    octa, eaw = {}, {}
+    for key, m in meta.items():
+        if key.startswith("octa_"):
+            octa[key] = (z[key + "__env"], z[key + "__map"])
+        else:
+            i = m["input"]
+            eaw[key] = (z[i + "__color"], z[i + "__position"], z[i + "__normal"], m["iterations"], tuple(m["phi"]),
+                        z[key + "__out"])
+    return octa, eaw
+
+
+SVGF_GOLDEN = __import__("os").path.join(__import__("os").path.dirname(__import__("os").path.abspath(__file__)),
+                                         "golden", "svgf_frames.npz")
+
+
+def svgf_golden():
+    """(meta, inputs [frame] -> (noisy, normal, depth, fwidth, motion), outputs (iterations, frame) -> (out,
+    colour history, moments history)) of the reference's SVGF shaders (tests/golden/make_svgf_golden.py)."""
+    import json
+
+    z = np.load(SVGF_GOLDEN)
+    meta = json.loads(str(z["meta"]))
+    inputs = [tuple(z[f"in{f}__{n}"] for n in ("noisy", "normal", "depth", "fwidth", "motion"))
+              for f in range(meta["frames"])]
+    outputs = {(it, f): (z[f"it{it}_f{f}__out"], z[f"it{it}_f{f}__color"], z[f"it{it}_f{f}__moments"])
+               for it in meta["iterations"] for f in range(meta["frames"])}
+    return meta, inputs, outputs
+
+
+def svgf_close(got, exp):
+    """Fraction of pixels whose every channel agrees to rtol 1e-4 (relative to |exp| + 1e-3)."""
+    close = np.abs(got - exp) <= 1e-4 * (np.abs(exp) + 1e-3)
+    return float(close.reshape(close.shape[0] * close.shape[1], -1).all(axis=1).mean())

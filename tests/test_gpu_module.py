@@ -291,8 +291,8 @@ def test_global_world_bounding_box_places_loaded_nanovdb_grids():
     assert torch.isfinite(out).all()
     from cloudrendering_b200 import _lib
     _lib.check(_lib.load().vpt_set_global_world_bounding_box(vpt.context_handle(), None, None), "clear")
+    vpt.generate_fbm_cloud(32, seed=1)  # a dense grid again, then the dense path
     vpt.set_use_sparse_grid(False)
-    vpt.generate_fbm_cloud(32, seed=1)
 
 
 def test_feature_map_type_selects_the_returned_image():

@@ -345,3 +345,39 @@ def test_schedules_trace_identical_paths(core, mode):
     core("vpt_set_option", b"schedule", 2.0)
     assert np.allclose(films[0], films[1], rtol=1e-12, atol=1e-12)
     assert np.allclose(films[0], films[2], rtol=1e-12, atol=1e-12)
+
+
+def test_environment_map_level0_matches_reference_shader(core):
+    """Level 0 of the core's importance pyramid against OctahedralMapper.glsl run on the CPU
+    (tests/golden/image_filters.npz): rtol 1e-5 (CUDA's atan2f / asinf / sinf / cosf differ from the C
+    library's in the last ulp, which moves the bilinear lookups by that much; the oracle, on the C
+    library, matches the shader bit for bit)."""
+    from tests.harness import image_golden
+
+    octa, _ = image_golden()
+    for key, (env, ref) in sorted(octa.items()):
+        res = ref.shape[0]
+        levels = int(np.log2(res))
+        total = sum((1 << (levels - l)) ** 2 for l in range(levels))
+        d = torch.from_numpy(np.ascontiguousarray(env)).cuda()
+        out = torch.empty(total, device="cuda")
+        assert core.lib.vpt_build_environment_pyramid(dptr(d), env.shape[1], env.shape[0], levels, dptr(out), None) == 0
+        torch.cuda.synchronize()
+        got = out.cpu().numpy()[:res * res].reshape(res, res)
+        assert np.allclose(got, ref, rtol=1e-5, atol=1e-6), key
+
+
+def test_eaw_compute_path_matches_reference_shader(core):
+    """The core's EAW with the compute path's colour weight (ref_compute_quirk) against the compute stage
+    of EAWDenoise.glsl run on the CPU (tests/golden/image_filters.npz); tolerance as in the CPU pin."""
+    from tests.harness import image_golden
+
+    _, eaw = image_golden()
+    for key, (color, pos, nrm, it, phi, ref) in sorted(eaw.items()):
+        h, w = color.shape[:2]
+        dc, dp, dn = (torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (color, pos, nrm))
+        out = torch.empty_like(dc)
+        assert core.lib.vpt_eaw_denoise_rgba(dptr(dc), dptr(dp), dptr(dn), w, h, it, phi[0], phi[1], phi[2], 1,
+                                             dptr(out), None) == 0
+        torch.cuda.synchronize()
+        assert np.allclose(out.cpu().numpy(), ref, rtol=1e-5, atol=2e-5), key

@@ -61,3 +61,30 @@ def test_svgf_frames_match_the_oracle(iterations):
             assert np.abs(got - exp).max() <= 0.05 * (np.abs(exp).max() + 1e-3), (frame, name)
         # the history length grows while reprojection succeeds
         assert hist_o["moments"][..., 2].max() == frame + 1
+
+
+@pytest.mark.parametrize("iterations", [5, 1, 0])
+def test_svgf_frames_match_the_reference_shaders(iterations):
+    """vpt_svgf_filter against the reference's own SVGF compute shaders run on the CPU
+    (tests/golden/svgf_frames.npz), five frames: the image and the colour / moments histories; the same
+    tolerance as against the oracle."""
+    from tests.harness import svgf_close, svgf_golden
+
+    meta, inputs, outputs = svgf_golden()
+    lib = _lib.load()
+    h, w = meta["h"], meta["w"]
+    hist = {"color": torch.zeros((h, w, 4), device="cuda"), "moments": torch.zeros((h, w, 4), device="cuda"),
+            "normal": torch.zeros((h, w, 4), device="cuda"), "depth": torch.zeros((h, w), device="cuda")}
+    p = lambda t: ctypes.c_void_p(t.data_ptr())  # noqa: E731
+    for f, arrs in enumerate(inputs):
+        dev = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in arrs]
+        out = torch.empty((h, w, 4), dtype=torch.float32, device="cuda")
+        st = lib.vpt_svgf_filter(*[p(t) for t in dev], p(hist["color"]), p(hist["moments"]), p(hist["normal"]),
+                                 p(hist["depth"]), w, h, ctypes.c_float(meta["z_threshold"]),
+                                 ctypes.c_float(meta["normal_threshold"]), iterations, p(out), None)
+        assert st == 0
+        torch.cuda.synchronize()
+        ref_out, ref_color, ref_moments = outputs[(iterations, f)]
+        for name, got, exp in (("out", out, ref_out), ("color", hist["color"], ref_color),
+                               ("moments", hist["moments"], ref_moments)):
+            assert svgf_close(got.cpu().numpy(), exp) >= 0.999, (f, name)
