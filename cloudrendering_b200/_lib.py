@@ -92,6 +92,7 @@ SIGNATURES = {
                                           c_void_p, c_void_p, c_void_p]),
     "vpt_build_rrt_params": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_float, c_int, c_void_p, c_void_p]),
     "vpt_set_env_map_rotation": (c_int, [c_void_p, c_void_p]),
+    "vpt_set_previous_view_projection": (c_int, [c_void_p, c_void_p]),
     "vpt_set_env_map_rotation_camera": (c_int, [c_void_p]),
     "vpt_set_global_world_bounding_box": (c_int, [c_void_p, c_void_p, c_void_p]),
     "vpt_build_residual_ratio_grid": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_float, c_int, c_void_p, c_void_p]),

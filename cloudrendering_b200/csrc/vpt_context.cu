@@ -231,6 +231,11 @@ struct VptContext {
     DevBuf<float> eaw_maps;                  // position + normal RGBA for EAW
     double prev_view_proj[16];
     bool has_prev_view_proj = false;
+    // parameters.previousViewProjMatrix of the tracer (Flow, Flow Reverse, Reprojected UV): the matrix
+    // stored by setViewProjectionMatrixAsPrevious, else the current camera's
+    // (VolumetricPathTracingPass.cpp:1985-1989)
+    float trace_prev_vp[16];
+    bool has_trace_prev_vp = false;
     DevBuf<float> staging;         // CHW staging for host outputs
 
     DevBuf<unsigned long long> counters;
@@ -516,7 +521,7 @@ VptStatus fill_params(VptContext* ctx, int tracker, int frames, vpt::TraceParams
     compute_camera(ctx, vp, inv);
     for (int i = 0; i < 16; i++) {
         P.inv_view_proj[i] = float(inv[i]);
-        P.prev_view_proj[i] = float(vp[i]);
+        P.prev_view_proj[i] = ctx->has_trace_prev_vp ? ctx->trace_prev_vp[i] : float(vp[i]);
     }
     P.width = ctx->width;
     P.height = ctx->height;
@@ -1344,6 +1349,19 @@ VptStatus vpt_load_environment_map_rgba(VptContext* ctx, const float* rgba, int 
     VPT_CHECK_CUDA(ctx, vpt::launch_env_pyramid(P, ctx->env_pyramid.ptr, ctx->env_offsets_host.data(), levels, 0));
     VPT_CHECK_CUDA(ctx, cudaDeviceSynchronize());
     reset_film_state(ctx);
+    return VPT_OK;
+}
+
+VptStatus vpt_set_previous_view_projection(VptContext* ctx, const float view_proj[16]) {
+    VPT_CHECK_CTX(ctx);
+    if (view_proj) {
+        for (int i = 0; i < 16; i++) ctx->trace_prev_vp[i] = view_proj[i];
+    } else {
+        double vp[16], inv[16];
+        compute_camera(ctx, vp, inv);
+        for (int i = 0; i < 16; i++) ctx->trace_prev_vp[i] = float(vp[i]);
+    }
+    ctx->has_trace_prev_vp = true;
     return VPT_OK;
 }
 

@@ -592,6 +592,26 @@ __global__ void feature_to_chw_kernel(const float* __restrict__ feat, int n, flo
             v[2] = a2 * hit;
             v[3] = hit;
             break;
+        case VPT_FEATURE_FIRST_W:  // the last frame's values (not accumulated in the reference)
+            v[0] = f[kFeatFirstW];
+            v[1] = f[kFeatFirstW + 1];
+            v[2] = f[kFeatFirstW + 2];
+            v[3] = f[kFeatFirstW + 3];
+            break;
+        case VPT_FEATURE_FLOW:
+            v[0] = f[kFeatFlow];
+            v[1] = f[kFeatFlow + 1];
+            break;
+        case VPT_FEATURE_FLOW_REVERSE:
+            v[0] = f[kFeatFlowReverse];
+            v[1] = f[kFeatFlowReverse + 1];
+            break;
+        case VPT_FEATURE_REPROJ_UV: {  // (-1, -1) until a frame had an event (Clouds.glsl:240)
+            const unsigned long long* key = reinterpret_cast<const unsigned long long*>(f + kFeatReprojUV);
+            v[0] = (key[0] >> 32) != 0 ? __uint_as_float((uint32_t)key[0]) : -1.0f;
+            v[1] = (key[1] >> 32) != 0 ? __uint_as_float((uint32_t)key[1]) : -1.0f;
+            break;
+        }
         default:  // VPT_FEATURE_TRANSMITTANCE
             v[0] = f[kFeatTrans] * inv_frames;
             break;
@@ -614,6 +634,10 @@ cudaError_t feature_to_chw(const float* feat, int n, uint32_t frames, int featur
         case VPT_FEATURE_CLOUD_ONLY:
         case VPT_FEATURE_ALBEDO:
         case VPT_FEATURE_TRANSMITTANCE:
+        case VPT_FEATURE_FIRST_W:
+        case VPT_FEATURE_FLOW:
+        case VPT_FEATURE_FLOW_REVERSE:
+        case VPT_FEATURE_REPROJ_UV:
             break;
         default:
             return cudaErrorInvalidValue;

@@ -2,7 +2,9 @@
 // Henyey-Greenstein sampling, sky/sun models and dense-grid density lookups.
 //
 // Arithmetic conventions (identical in the CPU oracle, so that paths can be compared one by one):
-//  * this translation unit is compiled with --fmad=false: a*b+c is two IEEE-rounded operations;
+//  * the parity build (libvpt_b200_dr.so) is compiled with --fmad=false: a*b+c is two IEEE-rounded
+//    operations, as in the oracle; the product build contracts them into FMAs (a last-ulp difference
+//    per operation, which changes the random decisions of a small fraction of paths only);
 //  * divisions and square roots are IEEE-rounded (-prec-div/-prec-sqrt default true);
 //  * the reference's per-step ratios are written in closed form: with majorant == extinction.x,
 //    Pa = (1 - albedo) * density and 1 - Pn = density (DeltaTracking.glsl:262-268);

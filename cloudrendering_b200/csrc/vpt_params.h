@@ -212,7 +212,16 @@ enum FeatureSlot : int {
                          // 19: unused
     kFeatDepthBlended = 20,  // alpha-blended depth of the camera ray's march, its alpha
     kFeatDepthNearest = 22,  // depth of the last non-transparent march step times alpha, alpha
-    kFeatStride = 24,
+    // maps the reference overwrites every frame (not accumulated): written by the path of the last
+    // frame of a launch
+    kFeatFirstW = 24,        // direction after the first scatter, its phase pdf
+    kFeatFlow = 28,          // pixel - the first event's pixel in the previous view (0 without an event)
+    kFeatFlowReverse = 30,   // the first event's (or the camera direction's) previous pixel - pixel
+    kFeatReprojUV = 32,      // two 64-bit keys (slots 32-33: u, 34-35: v), each (frame + 1) << 32 | float
+                             //   bits: atomicMax keeps the uv of the latest frame with an event in the
+                             //   previous view, whatever order the frames are traced in (0: none yet)
+                             // 35: unused
+    kFeatStride = 36,
 };
 
 }  // namespace vpt

@@ -84,6 +84,55 @@ VPT_DEV void depth_march(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, 
 // density, albedo-weighted hit flag, primary-ray transmittance proxy and, when requested, the
 // background (Clouds.glsl:162-170: sampleSkybox of the camera ray for paths with an event, the
 // path's radiance otherwise).
+// previousViewProjMatrix * (v, vw), column-major, columns summed in order
+VPT_DEV void prev_clip(const TraceParams& P, F3 v, float vw, float out[4]) {
+    const float* m = P.prev_view_proj;
+#pragma unroll
+    for (int r = 0; r < 4; r++) out[r] = ((m[r] * v.x + m[4 + r] * v.y) + m[8 + r] * v.z) + m[12 + r] * vw;
+}
+
+// The maps the reference overwrites every frame (Clouds.glsl:239-246, 300-343), from the path of the
+// frame that is traced last: First W (the direction after the first scatter and its pdf), Flow, Flow
+// Reverse and Reprojected UV (which keeps an earlier frame's value when this frame has no event).
+VPT_DEV void write_last_frame_features(const TraceParams& P, float* f, const FirstEvent& fe, int px, int py,
+                                       F3 w_camera) {
+    f[kFeatFirstW + 0] = fe.has ? fe.w.x : 0.0f;
+    f[kFeatFirstW + 1] = fe.has ? fe.w.y : 0.0f;
+    f[kFeatFirstW + 2] = fe.has ? fe.w.z : 0.0f;
+    f[kFeatFirstW + 3] = fe.has ? fe.pdf_w : 0.0f;
+    const float dw = (float)P.width, dh = (float)P.height;
+    float c[4];
+    float flow_x = 0.0f, flow_y = 0.0f;
+    if (fe.has) {
+        prev_clip(P, fe.x, 1.0f, c);
+        const float nx = c[0] / c[3], ny = c[1] / c[3];
+        flow_x = (float)px - ((0.5f * nx + 0.5f) * dw - 0.5f);
+        flow_y = (float)py - ((0.5f * ny + 0.5f) * dh - 0.5f);
+    }
+    f[kFeatFlow + 0] = flow_x;
+    f[kFeatFlow + 1] = flow_y;
+    if (fe.has) prev_clip(P, fe.x, 1.0f, c);
+    else prev_clip(P, w_camera, 0.0f, c);
+    const float rx = c[0] / c[3], ry = c[1] / c[3];
+    f[kFeatFlowReverse + 0] = ((0.5f * rx + 0.5f) * dw - 0.5f) - (float)px;
+    f[kFeatFlowReverse + 1] = ((0.5f * ry + 0.5f) * dh - 0.5f) - (float)py;
+}
+
+// Reprojected UV (Clouds.glsl:240-246): prevClip.xy / prevClip.w * 0.5 + 0.5 of every frame's first
+// event; the reference keeps the last frame's value, or an earlier one when the last frame has none.
+// Frames of one pixel may run concurrently here, so each coordinate is a 64-bit key whose high word is
+// the frame (+1) and whose low word the coordinate's bits, and atomicMax keeps the latest frame's.
+VPT_DEV void update_reproj_uv(const TraceParams& P, float* f, const FirstEvent& fe, uint32_t global_frame) {
+    float c[4];
+    prev_clip(P, fe.x, 1.0f, c);
+    const float u = (c[0] / c[3]) * 0.5f + 0.5f;
+    const float v = (c[1] / c[3]) * 0.5f + 0.5f;
+    const unsigned long long stamp = (unsigned long long)(global_frame + 1u) << 32;
+    unsigned long long* key = reinterpret_cast<unsigned long long*>(f + kFeatReprojUV);
+    atomicMax(key + 0, stamp | __float_as_uint(u));
+    atomicMax(key + 1, stamp | __float_as_uint(v));
+}
+
 template <class S>
 VPT_DEV void accumulate_features(const TraceParams& P, S& sample, Rng& rng, size_t pix, const FirstEvent& fe,
                                  F3 result, F3 x_camera, F3 w_camera) {
@@ -191,7 +240,11 @@ VPT_DEV void trace_one(const TraceParams& P, S& sample, uint32_t frame, int px, 
         atomicAdd(P.film_sq + pix * 3 + 1, (double)L.y * (double)L.y);
         atomicAdd(P.film_sq + pix * 3 + 2, (double)L.z * (double)L.z);
     }
-    if (features) accumulate_features(P, sample, rng, pix, fe, L, x, w);
+    if (features) {
+        accumulate_features(P, sample, rng, pix, fe, L, x, w);
+        if (fe.has) update_reproj_uv(P, P.feat + pix * kFeatStride, fe, P.global_frame + frame);
+        if (frame + 1 == P.num_frames) write_last_frame_features(P, P.feat + pix * kFeatStride, fe, px, py, w);
+    }
     lookups += pc.lookups;
     guard_hit |= pc.guard_hit;
 }

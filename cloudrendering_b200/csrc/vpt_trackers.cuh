@@ -16,6 +16,8 @@ struct FirstEvent {
     F3 x;
     float depth;
     float density;
+    F3 w;         // direction after the first scatter (0 when the first event is an absorption)
+    float pdf_w;  // phase-function density of that direction (firstEvent.pdf_w)
 };
 
 struct PathCtx {
@@ -43,6 +45,19 @@ VPT_DEV void record_event(FirstEvent& fe, F3 x, float density, float extinction,
         fe.x = x;
         fe.density = density * extinction;
         fe.depth = depth;
+        fe.w = f3(0.0f, 0.0f, 0.0f);
+        fe.pdf_w = 0.0f;
+    }
+}
+
+// A scatter event: records the first event with the scattered direction w_out and its phase-function
+// density (DeltaTracking.glsl:134-141; evaluated for the sampled pair of directions).
+VPT_DEV void record_scatter(FirstEvent& fe, F3 x, float density, float extinction, float depth, F3 w_in, F3 w_out,
+                            float g) {
+    if (!fe.has) {
+        record_event(fe, x, density, extinction, depth);
+        fe.w = w_out;
+        fe.pdf_w = evaluate_phase(g, w_in, w_out);
     }
 }
 
@@ -72,8 +87,9 @@ VPT_DEV F3 track_delta(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, Fi
             }
             if (xi < density) {
                 if (P.max_bounces > 0 && ++bounces > P.max_bounces) return f3(0.0f, 0.0f, 0.0f);
+                const F3 w_in = w;
                 w = sample_phase(rng, P.g, w);
-                record_event(fe, x, density, P.extinction, tmax - d + t);
+                record_scatter(fe, x, density, P.extinction, tmax - d + t, w_in, w, P.g);
                 if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
                     x = x + w * tmin;
                     d = tmax - tmin;
@@ -176,8 +192,9 @@ VPT_DEV F3 track_delta_iso(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w
             }
             if (xi < density) {
                 if (P.max_bounces > 0 && ++bounces > P.max_bounces) return f3(0.0f, 0.0f, 0.0f);
+                const F3 w_in = w;
                 w = sample_phase(rng, P.g, w);
-                record_event(fe, x, density, P.extinction, tmax - d + t);
+                record_scatter(fe, x, density, P.extinction, tmax - d + t, w_in, w, P.g);
                 if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
                     x = x + w * tmin;
                     d = tmax - tmin;
@@ -379,7 +396,7 @@ VPT_DEV F3 track_nee(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, Firs
             if (xi < density) {
                 if (P.max_bounces > 0 && ++bounces > P.max_bounces) return color;
                 F3 next_w = sample_phase(rng, P.g, w);
-                record_event(fe, x, density, P.extinction, tmax - d + t);
+                record_scatter(fe, x, density, P.extinction, tmax - d + t, w, next_w, P.g);
                 // with lights: the light list or the sky with probability 1/2 each (all lights when the
                 // environment is black), NextEventTracking.glsl:335-364
                 bool to_light = false;
@@ -509,8 +526,9 @@ VPT_DEV F3 track_delta_spectral(const TraceParams& P, S& sample, Rng& rng, F3 x,
             }
             if (xi < st.pa + st.ps) {
                 if (P.max_bounces > 0 && ++bounces > P.max_bounces) return f3(0.0f, 0.0f, 0.0f);
+                const F3 w_in = w;
                 w = sample_phase(rng, P.g, w);
-                record_event(fe, x, density, P.sdt_majorant, tmax - d + t);
+                record_scatter(fe, x, density, P.sdt_majorant, tmax - d + t, w_in, w, P.g);
                 if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
                     x = x + w * tmin;
                     d = tmax - tmin;
@@ -561,7 +579,7 @@ VPT_DEV F3 track_nee_spectral(const TraceParams& P, S& sample, Rng& rng, F3 x, F
             if (xi < st.pa + st.ps) {
                 if (P.max_bounces > 0 && ++bounces > P.max_bounces) return color;
                 F3 next_w = sample_phase(rng, P.g, w);
-                record_event(fe, x, density, P.sdt_majorant, tmax - d + t);
+                record_scatter(fe, x, density, P.sdt_majorant, tmax - d + t, w, next_w, P.g);
                 bool to_light = false;
                 float prob_factor = 1.0f, light_dist = 0.0f, pdf_light = 0.0f;
                 int light_idx = 0;
@@ -1068,7 +1086,7 @@ VPT_DEV F3 track_residual_ratio_nee(const TraceParams& P, S& sample, Rng& rng, F
             x = x + w * t;
             if (P.max_bounces > 0 && ++bounces > P.max_bounces) return color;
             const F3 next_w = sample_phase(rng, P.g, w);
-            record_event(fe, x, density, P.extinction, depth0 + t);
+            record_scatter(fe, x, density, P.extinction, depth0 + t, w, next_w, P.g);
             // light selection as in next event tracking (NextEventTracking.glsl:335-364)
             bool to_light = false;
             float prob_factor = 1.0f, light_dist = 0.0f, pdf_light = 0.0f;

@@ -29,6 +29,7 @@ from typing import Dict, List, Optional, Sequence
 
 import numpy as np
 import torch
+import torch.distributed as dist
 
 from . import _lib
 
@@ -365,12 +366,16 @@ class KpnUNet:
                    _p(out), _p(dl), _p(lp), n, h, w, LOSS_EPS, self._stream())
         return out, (lp.sum() if lp is not None else None), dl
 
-    def train_step(self, batch: dict, lr: float) -> torch.Tensor:
+    def train_step(self, batch: dict, lr: float, group=None) -> torch.Tensor:
+        """One Adam step on `batch`.  With a process group (data-parallel training, one rank per GPU),
+        the ranks' gradients are averaged before the step, so every rank's parameters stay equal."""
         x0 = self.pack(batch["radiance"], batch.get("albedo"), batch.get("normal"), batch.get("depth"),
                        batch.get("transmittance"), batch.get("noise_level"), batch.get("second_moment"))
         self.forward(x0)
         _, loss, dls = self.reconstruct(batch["radiance"], batch["target"])
         self.backward(dls)
+        if group is not None:
+            average_gradients(self.grad, group)
         self.adam_step(lr)
         return loss
 
@@ -631,10 +636,24 @@ class TrainingSet:
         return out
 
 
+def average_gradients(grad: torch.Tensor, group=None) -> None:
+    """Data-parallel training: replaces the flat fp32 gradient by the mean over the ranks of `group`
+    (one all_reduce of the whole vector: 7.6 MB for the 1.9 M-parameter network, a few microseconds of
+    NVLink time against a multi-millisecond step)."""
+    world = dist.get_world_size(group)
+    if world > 1:
+        dist.all_reduce(grad, op=dist.ReduceOp.SUM, group=group)
+        grad.div_(float(world))
+
+
 def train(net: KpnUNet, data: TrainingSet, steps: int, batch_size: int = 8, lr: float = 1e-4, seed: int = 0,
-          log_every: int = 0, lr_end: Optional[float] = None) -> dict:
+          log_every: int = 0, lr_end: Optional[float] = None, group=None) -> dict:
     """Adam training (learning rate constant, or cosine-annealed from lr to lr_end); returns timing and
-    the loss curve (mean loss per logging window)."""
+    the loss curve (mean loss per logging window).  With a process group the training is data parallel:
+    each rank draws its own batches (its rank offsets the seed) from its own training set and the
+    gradients are averaged every step (networks built with the same seed start equal and stay equal)."""
+    if group is not None:
+        seed = seed + 7919 * dist.get_rank(group)
     rng = np.random.default_rng(seed)
     losses = []
     acc = torch.zeros((), dtype=torch.float32, device=net.device)
@@ -643,7 +662,7 @@ def train(net: KpnUNet, data: TrainingSet, steps: int, batch_size: int = 8, lr: 
     t0 = time.perf_counter()
     for i in range(steps):
         step_lr = lr if lr_end is None else lr_end + 0.5 * (lr - lr_end) * (1.0 + math.cos(math.pi * i / steps))
-        loss = net.train_step(data.batch(rng, batch_size), step_lr)
+        loss = net.train_step(data.batch(rng, batch_size), step_lr, group)
         acc += loss
         if (i + 1) % window == 0:
             losses.append(float(acc.item()) / window)

@@ -683,7 +683,10 @@ def overwrite_camera_view_matrix(view_matrix_data: List[float]) -> None:
 
 
 def set_view_projection_matrix_as_previous() -> None:
-    """The SVGF history uses the view-projection of the previous render automatically."""
+    """Stores the current camera's view-projection as the previous one (setViewProjectionMatrixAsPrevious,
+    Module.cpp:1339-1341): the Flow, Flow Reverse and Reprojected UV maps reproject into it.  The SVGF
+    history follows the previous render's camera by itself."""
+    _c("vpt_set_previous_view_projection", None)
 
 
 # ---- denoising ----
@@ -750,7 +753,8 @@ def set_use_feature_maps(feature_map_names: List[str]) -> None:
     _apply_feature_maps()
 
 
-_FEATURE_CHANNELS = {1: 4, 3: 4, 4: 4, 5: 4, 6: 2, 7: 1, 12: 2, 13: 4, 15: 4, 16: 4, 17: 4, FEATURE_TRANSMITTANCE: 1}
+_FEATURE_CHANNELS = {1: 4, 2: 4, 3: 4, 4: 4, 5: 4, 6: 2, 7: 1, 8: 2, 9: 2, 12: 2, 13: 4, 14: 2, 15: 4, 16: 4, 17: 4,
+                     FEATURE_TRANSMITTANCE: 1}
 
 
 def get_feature_map(input_tensor: torch.Tensor, feature_map: int) -> torch.Tensor:

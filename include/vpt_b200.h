@@ -72,13 +72,17 @@ enum {
 enum {
     VPT_FEATURE_RESULT = 0,
     VPT_FEATURE_FIRST_X = 1,
+    VPT_FEATURE_FIRST_W = 2,       /* direction after the first scatter and its pdf, of the last frame */
     VPT_FEATURE_NORMAL = 3,
     VPT_FEATURE_NORMAL_LEN_1 = 4,  /* Normal with rgb scaled to length 1 (NormalizeNormals.glsl) */
     VPT_FEATURE_CLOUD_ONLY = 5,
     VPT_FEATURE_DEPTH = 6,
     VPT_FEATURE_DEPTH_FAR = 7,     /* mean of (event ? depth : far distance) */
+    VPT_FEATURE_FLOW = 8,          /* (pixel - previous pixel of the first event, 0, 0), last frame */
+    VPT_FEATURE_FLOW_REVERSE = 9,  /* (previous pixel of the first event or camera direction - pixel), last frame */
     VPT_FEATURE_DENSITY = 12,
     VPT_FEATURE_BACKGROUND = 13,
+    VPT_FEATURE_REPROJ_UV = 14,    /* previous-view uv of the most recent first event, (-1, -1) before one */
     VPT_FEATURE_DEPTH_BLENDED = 15,        /* (alpha-blended depth, alpha, 0, 1) of a march along the camera ray */
     VPT_FEATURE_DEPTH_NEAREST_OPAQUE = 16, /* (depth of the last non-transparent step x alpha, alpha, 0, 1) */
     VPT_FEATURE_ALBEDO = 17,
@@ -204,6 +208,11 @@ VptStatus vpt_set_camera(VptContext* ctx, const float position[3], const float t
                          const float up[3], float fovy_radians, float near_dist, float far_dist);
 /* Overwrites the view matrix (16 floats, column-major) (overwrite_camera_view_matrix). */
 VptStatus vpt_set_view_matrix(VptContext* ctx, const float view[16]);
+/* setViewProjectionMatrixAsPrevious (Module.cpp:1339-1341, VolumetricPathTracingModuleRenderer.cpp:339-341):
+ * the previous view-projection (16 floats, column-major) that the Flow, Flow Reverse and Reprojected
+ * UV feature maps reproject into; NULL stores the current camera's.  Until it is called the current
+ * camera's is used (VolumetricPathTracingPass.cpp:1985-1989). */
+VptStatus vpt_set_previous_view_projection(VptContext* ctx, const float view_proj[16]);
 /* 16 floats each, column-major: inverse(proj * view) for the current resolution, and proj * view. */
 VptStatus vpt_get_camera_matrices(VptContext* ctx, float inv_view_proj[16], float view_proj[16]);
 

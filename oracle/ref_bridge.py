@@ -29,7 +29,7 @@ class RefScene(ctypes.Structure):
         ("emission", c_void_p), ("enx", c_int), ("eny", c_int), ("enz", c_int),
         ("emission_box_min", c_float * 3), ("emission_box_max", c_float * 3), ("emission_cap", c_float),
         ("emission_strength", c_float), ("tf", c_void_p), ("tf_size", c_int),
-        ("iso_value", c_float), ("iso_color", c_float * 3), ("env_rot", c_float * 9),
+        ("iso_value", c_float), ("iso_color", c_float * 3), ("env_rot", c_float * 9), ("prev_view_proj", c_float * 16),
     ]
 
 
@@ -53,6 +53,8 @@ def load():
         lib.ref_render.argtypes = [c_int, ctypes.POINTER(RefScene), c_void_p, c_int]
         lib.ref_read_depth_feature.restype = c_int
         lib.ref_read_depth_feature.argtypes = [c_int, c_void_p]
+        lib.ref_read_last_frame_feature.restype = c_int
+        lib.ref_read_last_frame_feature.argtypes = [c_int, c_void_p]
         _lib = lib
     return _lib
 
@@ -90,6 +92,14 @@ class Scene:
         st = lib.ref_render(idx, ctypes.byref(self.s), out.ctypes.data_as(c_void_p), threads)
         if st != 0:
             raise RuntimeError("ref_render failed")
+        return out
+
+    @staticmethod
+    def last_frame_feature(which: int, height: int, width: int) -> np.ndarray:
+        """The last render's firstW (0), flowImage (1), flowReverseImage (2) or reprojUVImage (3), H x W x 4."""
+        out = np.empty((height, width, 4), np.float32)
+        if load().ref_read_last_frame_feature(which, out.ctypes.data_as(c_void_p)) != 0:
+            raise RuntimeError("ref_read_last_frame_feature failed")
         return out
 
     @staticmethod

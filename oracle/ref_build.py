@@ -67,6 +67,8 @@ SDT_PROB = {"max": "MAX_BASED_PROBABILITY", "avg": "AVG_BASED_PROBABILITY",
 SPECTRAL = {"sdt": "USE_SPECTRAL_DELTA_TRACKING", "nees": "USE_NEXT_EVENT_TRACKING_SPECTRAL"}
 # the Depth Blended / Depth Nearest Opaque feature maps (Clouds.glsl:367-383), deterministic lookups
 DEPTH_MAPS = ["WRITE_DEPTH_BLENDED_MAP", "WRITE_DEPTH_NEAREST_OPAQUE_MAP"]
+# the maps overwritten every frame (Clouds.glsl:239-246, 286-343)
+LAST_FRAME_MAPS = ["WRITE_FIRST_W_MAP", "WRITE_FLOW_MAP", "WRITE_FLOW_REVERSE_MAP", "WRITE_REPROJ_UV_MAP"]
 ISO = ["USE_ISOSURFACES", "NUM_ISOSURFACE_SUBDIVISIONS=2", "SURFACE_BRDF_LAMBERTIAN", "ISOSURFACE_TYPE_DENSITY"]
 
 
@@ -87,6 +89,9 @@ def variants():
     for i in ("nearest", "trilinear"):
         out.append((f"depthmaps__{i}__default__linear", TRACKERS["delta"] + [INTERPS[i]] + ENVS["default__linear"]
                     + DEPTH_MAPS, 0))
+    for t in ("delta", "nee"):
+        out.append((f"lastframe_{t}__stochastic__default__linear", TRACKERS[t] + [INTERPS["stochastic"]]
+                    + ENVS["default__linear"] + LAST_FRAME_MAPS, 0))
     # emission grid (USE_EMISSION) with next event tracking, grey and spectral
     for i in ("stochastic", "trilinear"):
         out.append((f"nee_emission__{i}__default__linear", TRACKERS["nee"] + [INTERPS[i]] + ENVS["default__linear"]

@@ -28,6 +28,10 @@ static image2D& resultImage = g_ref.result;
 static image2D& accImage = g_ref.acc;
 static image2D& depthBlendedImage = g_ref.dblend;
 static image2D& depthNearestOpaqueImage = g_ref.dnear;
+static image2D& firstW = g_ref.firstw;
+static image2D& flowImage = g_ref.flow;
+static image2D& flowReverseImage = g_ref.flowrev;
+static image2D& reprojUVImage = g_ref.reproj;
 static Light* const lights = g_ref.lights;
 #define gl_GlobalInvocationID gl_global_invocation_id
 #define main glsl_main
@@ -47,6 +51,7 @@ RefState g_ref;
 thread_local uvec3 gl_global_invocation_id;
 uint ref_seed_offset = 0;
 static std::vector<float> g_dblend, g_dnear;  // the depth feature images of the last ref_render
+static std::vector<float> g_last[4];          // firstW, flow, flow reverse, reprojected uv images
 }  // namespace glslref
 
 using namespace glslref;
@@ -84,6 +89,7 @@ typedef struct RefScene {
     float iso_value;          /* parameters.isoValue (USE_ISOSURFACES variants) */
     float iso_color[3];       /* parameters.isoSurfaceColor */
     float env_rot[9];         /* parameters.envMapDirRot, column-major (USE_ENV_MAP_ROTATION variants) */
+    float prev_view_proj[16]; /* parameters.previousViewProjMatrix, column-major */
 } RefScene;
 
 int ref_variant_count(void) { return ref_num_variants; }
@@ -215,6 +221,16 @@ int ref_render(int variant, const RefScene* s, float* out_rgba, int threads) {
     g_ref.dnear.data = g_dnear.data();
     g_ref.dnear.w = s->width;
     g_ref.dnear.h = s->height;
+    image2D* last[4] = {&g_ref.firstw, &g_ref.flow, &g_ref.flowrev, &g_ref.reproj};
+    for (int k = 0; k < 4; k++) {
+        g_last[k].assign((size_t)s->width * s->height * 4, 0.0f);
+        last[k]->data = g_last[k].data();
+        last[k]->w = s->width;
+        last[k]->h = s->height;
+    }
+    for (int c = 0; c < 4; c++)
+        p.previousViewProjMatrix.c[c] = vec4(s->prev_view_proj[c * 4 + 0], s->prev_view_proj[c * 4 + 1],
+                                             s->prev_view_proj[c * 4 + 2], s->prev_view_proj[c * 4 + 3]);
     ref_seed_offset = s->seed_offset;
     int nt = threads;
 #ifdef _OPENMP
@@ -231,6 +247,15 @@ int ref_render(int variant, const RefScene* s, float* out_rgba, int threads) {
             for (int x = 0; x < s->width; x++) run(x, y);
     }
     memcpy(out_rgba, acc.data(), acc.size() * sizeof(float));
+    return 0;
+}
+
+// The images the last frame of the last ref_render wrote (which: 0 firstW, 1 flowImage, 2
+// flowReverseImage, 3 reprojUVImage; W*H*4), for the variants with WRITE_FIRST_W_MAP,
+// WRITE_FLOW_MAP, WRITE_FLOW_REVERSE_MAP and WRITE_REPROJ_UV_MAP.
+int ref_read_last_frame_feature(int which, float* out_rgba) {
+    if (!out_rgba || which < 0 || which > 3 || g_last[which].empty()) return 1;
+    memcpy(out_rgba, g_last[which].data(), g_last[which].size() * sizeof(float));
     return 0;
 }
 

@@ -16,6 +16,7 @@ struct RefState {
     uimage3D occ;         // occupancyGridImage
     image2D result, acc;  // resultImage, accImage
     image2D dblend, dnear;  // depthBlendedImage, depthNearestOpaqueImage (WRITE_DEPTH_*_MAP variants)
+    image2D firstw, flow, flowrev, reproj;  // firstW, flowImage, flowReverseImage, reprojUVImage
     Light lights[16];     // LightsBuffer
 };
 extern RefState g_ref;

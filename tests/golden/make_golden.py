@@ -6,7 +6,9 @@ reference's output: the radiance of each camera path of frame 0 (1 spp; accImage
 the path radiance itself) and the reference's fp32 running mean after 8 frames.
 
 With the argument ``depth_maps`` it writes tests/golden/ref_depth_maps.npz instead: the reference's
-Depth Blended and Depth Nearest Opaque images (Clouds.glsl:367-383) after 4 frames.
+Depth Blended and Depth Nearest Opaque images (Clouds.glsl:367-383) after 4 frames; with
+``last_frame_maps``, tests/golden/ref_last_frame_maps.npz: the First W, Flow, Flow Reverse and
+Reprojected UV images, which hold the last frame's values, after 4 frames.
 
 Run in a container that has the reference tree:  python tests/golden/make_golden.py [depth_maps]
 """
@@ -20,7 +22,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)
 sys.path.insert(0, ROOT)
 
 from oracle import bridge, ref_build  # noqa: E402
-from tests.harness import SceneSpec, camera_inv_view_proj, cloud_block, reference_scene  # noqa: E402
+from tests.harness import SceneSpec, camera_inv_view_proj, camera_view_proj, cloud_block, reference_scene  # noqa: E402
 
 W = H = 32
 
@@ -172,6 +174,46 @@ def main_depth_maps():
     print("wrote", out, os.path.getsize(out), "bytes")
 
 
+LAST_FRAMES = 4
+
+
+def last_frame_cases():
+    """First W / Flow / Flow Reverse / Reprojected UV (Clouds.glsl:239-246, 286-343): the fbm cloud seen
+    from cam_pos, the previous view-projection that of a camera a little to the side; delta tracking and
+    next event tracking, stochastic lookups."""
+    fbm = bridge.fbm(24, 2, base_frequency=3.0, contrast=3.5)
+    base = dict(extinction=60.0, albedo=0.99, g=0.85, width=W, height=H, env="default", linear_rgb=1,
+                cam_pos=(0.3, 0.4, 1.4), max_grid_extent=0.5)
+    prev = SceneSpec(grid=fbm, **dict(base, cam_pos=(0.36, 0.37, 1.41)))
+    return {f"fbm_lastframe_{t}": (SceneSpec(grid=fbm, mode=t, **base), camera_view_proj(prev)) for t in ("delta", "nee")}
+
+
+def main_last_frame_maps():
+    """tests/golden/ref_last_frame_maps.npz: the reference's firstW, flowImage, flowReverseImage and
+    reprojUVImage (H x W x 4) after LAST_FRAMES frames, with parameters.previousViewProjMatrix set."""
+    from oracle import ref_bridge
+
+    data, meta = {}, {}
+    for name, (sp, prev_vp) in last_frame_cases().items():
+        inv = camera_inv_view_proj(sp)
+        sc, _ = reference_scene(sp, LAST_FRAMES, inv=inv)
+        sc.set("prev_view_proj", prev_vp)
+        variant = f"lastframe_{sp.mode}__stochastic__default__linear"
+        sc.render(variant)
+        for k, key in enumerate(("first_w", "flow", "flow_reverse", "reproj_uv")):
+            data[f"{name}__{key}"] = ref_bridge.Scene.last_frame_feature(k, sp.height, sp.width)
+        data[name + "__grid"] = np.ascontiguousarray(sp.grid, np.float32)
+        data[name + "__prev_view_proj"] = np.array(prev_vp, np.float32)
+        data[name + "__inv_view_proj"] = np.array(inv, np.float32)
+        meta[name] = {"variant": variant, "frames": LAST_FRAMES,
+                      **{f: (list(getattr(sp, f)) if isinstance(getattr(sp, f), tuple) else getattr(sp, f))
+                         for f in FIELDS}}
+        print(name, variant, float(np.abs(data[name + "__flow"]).mean()), float((data[name + "__reproj_uv"] >= 0).mean()))
+    out = os.path.join(os.path.dirname(os.path.abspath(__file__)), "ref_last_frame_maps.npz")
+    np.savez_compressed(out, meta=json.dumps(meta), **data)
+    print("wrote", out, os.path.getsize(out), "bytes")
+
+
 def main():
     ref_build.build()
     data = {}
@@ -210,5 +252,9 @@ if __name__ == "__main__":
     if len(sys.argv) > 1 and sys.argv[1] == "depth_maps":
         ref_build.build()
         main_depth_maps()
+        sys.exit(0)
+    if len(sys.argv) > 1 and sys.argv[1] == "last_frame_maps":
+        ref_build.build()
+        main_last_frame_maps()
         sys.exit(0)
     main()

@@ -249,6 +249,22 @@ def camera_inv_view_proj(sp: SceneSpec):
     return [f32(v) for v in inv]
 
 
+def camera_view_proj(sp: SceneSpec):
+    """proj * view of the core's camera for `sp` (double, rounded to float; vpt_get_camera_matrices)."""
+    f32 = lambda v: float(np.float32(v))  # noqa: E731
+    view = _view_matrix(sp)
+    aspect = float(sp.width) / float(sp.height) if sp.width > 0 and sp.height > 0 else 1.0
+    th = math.tan(f32(sp.fovy) / 2.0)
+    n, fa = f32(sp.near), f32(sp.far)
+    proj = [0.0] * 16
+    proj[0] = 1.0 / (aspect * th)
+    proj[5] = -1.0 / th
+    proj[10] = fa / (n - fa)
+    proj[11] = -1.0
+    proj[14] = -(fa * n) / (fa - n)
+    return [f32(v) for v in _mat_mul(proj, view)]
+
+
 def oracle_scene(core, sp: SceneSpec, frames: int, frame_count: int = 0) -> bridge.Scene:
     if core is not None:
         inv = (ctypes.c_float * 16)()
@@ -367,6 +383,22 @@ def z_scores(sum_a, sq_a, n_a, sum_b, sq_b, n_b):
     se = np.sqrt(va / n_a + vb / n_b)
     z = np.where(se > 0, (ma - mb) / np.where(se > 0, se, 1.0), np.where(np.abs(ma - mb) > 1e-7, np.inf, 0.0))
     return z
+
+
+def binned_z(sum_a, sq_a, n_a, sum_b, sq_b, n_b, B=8):
+    """Per-pixel radiance is heavy-tailed (rare paths that see the sun lobe: one such path among n
+    samples moves a pixel's z by up to sqrt(n)), so agreement is judged on BxB-pixel bins (n*B*B
+    samples per bin and side).  Returns (max |z| over the bins, fraction of pixels with |z| > 4)."""
+    H, W = sum_a.shape[:2]
+    h, w = H // B * B, W // B * B
+
+    def binsum(x):
+        return x[:h, :w].reshape(h // B, B, w // B, B, -1).sum(axis=(1, 3))
+
+    zb = z_scores(binsum(sum_a), binsum(sq_a), n_a * B * B, binsum(sum_b), binsum(sq_b), n_b * B * B)
+    zpix = z_scores(sum_a, sq_a, n_a, sum_b, sq_b, n_b)
+    zb = np.abs(np.where(np.isfinite(zb), zb, 0.0))
+    return float(zb.max()), float((np.abs(np.where(np.isfinite(zpix), zpix, 0.0)) > 4).mean())
 
 
 def reference_scene(sp: SceneSpec, frames: int, frame_start: int = 0, inv=None):

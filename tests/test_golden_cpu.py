@@ -26,3 +26,32 @@ def test_oracle_matches_reference_shader_paths(name):
     m = film.reshape(paths.shape) / 8.0
     close = np.all(np.abs(m - mean8) <= 1e-5 + 1e-4 * np.abs(mean8), axis=-1)
     assert close.mean() >= 0.99
+
+
+def test_last_frame_maps_fixture_is_consistent():
+    """tests/golden/ref_last_frame_maps.npz (the reference's First W, Flow, Flow Reverse and Reprojected
+    UV images): where the last frame scattered (first W pdf > 0), Flow is the pixel minus the
+    reprojected uv in pixels (Clouds.glsl:240-246 and 319-327 project the same point); where it had no
+    event, Flow and First W are zero."""
+    import json
+    import os
+
+    z = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ref_last_frame_maps.npz"))
+    meta = json.loads(str(z["meta"]))
+    assert set(meta) == {"fbm_lastframe_delta", "fbm_lastframe_nee"}
+    for name, m in meta.items():
+        h, w = m["height"], m["width"]
+        first_w, flow, uv = z[name + "__first_w"], z[name + "__flow"], z[name + "__reproj_uv"]
+        event = first_w[..., 3] > 0
+        assert 0.3 < event.mean() < 1.0
+        ys, xs = np.mgrid[0:h, 0:w]
+        fx = xs - (uv[..., 0] * w - 0.5)
+        fy = ys - (uv[..., 1] * h - 0.5)
+        assert np.allclose(flow[..., 0][event], fx[event], atol=2e-3)
+        assert np.allclose(flow[..., 1][event], fy[event], atol=2e-3)
+        # no event on the last frame: zero flow and zero first W (an absorbed first event has a flow but
+        # no scatter direction, so the converse does not hold)
+        none = np.all(flow[..., :2] == 0.0, axis=-1)
+        assert none.any() and np.all(first_w[none] == 0.0)
+        # unit directions after the first scatter
+        assert np.allclose(np.linalg.norm(first_w[..., :3][event], axis=-1), 1.0, atol=1e-4)
