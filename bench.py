@@ -39,6 +39,9 @@ EXTINCTION = 1000.0
 SEED = 2
 TRACKERS = {"delta": 0, "ratio": 2, "decomposition": 3, "residual_ratio": 4, "nee": 5, "residual_ratio_unbiased": 9}
 BYTES_PER_LOOKUP = 32  # one 32-byte sector per uncoalesced density gather
+# delta tracking reads the density through the grid's 3D texture object (1) or by global loads (0);
+# both read the same texels; the bench's fetch_paths_delta leg times the two
+DENSITY_TEXTURE = 1
 # DRAM read + write bytes of one headline launch (64 spp of the 1024^2 image on the 512^3 cloud), from
 # one ncu capture of that launch (profiles/trace_refill_delta_512_1024_64spp.md): 866 B per path
 NCU_DRAM_BYTES_PER_PATH = 58.12e9 / (1024 * 1024 * 64)
@@ -88,6 +91,67 @@ def gather_rates(lib, stream):
         sectors = 5.0 * blocks * 256 * loads
         out[name] = sectors * BYTES_PER_LOOKUP / (e0.elapsed_time(e1) / 1e3) / 1e9
         del buf
+    return out
+
+
+def run_streaming(lib, stream):
+    """The builders and image filters around the tracer, each on inputs larger than L2, timed with
+    CUDA events (one warm-up call, then the mean of 3): algorithmic bytes (every input read once,
+    every output written once) / time against the measured HBM copy peak."""
+    import ctypes
+    import torch
+    cs = ctypes.c_void_p(stream.cuda_stream)
+    peak, peak_kind = peaks()
+    out = {"peak_gbs": peak, "peak_kind": peak_kind}
+
+    def p(t):
+        return ctypes.c_void_p(t.data_ptr())
+
+    def timed(name, fn, nbytes, work):
+        fn()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(3):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / 3
+        out[name] = {"work": work, "bytes": int(nbytes), "ms": ms, "gbs": nbytes / (ms / 1e3) / 1e9,
+                     "frac_of_hbm_peak": nbytes / (ms / 1e3) / 1e9 / peak}
+
+    n = 512
+    dens = torch.rand(n * n * n, device="cuda")
+    sv = 8
+    g = n // sv
+    smin, smax, savg = (torch.empty(g ** 3, device="cuda") for _ in range(3))
+    socc = torch.empty(g ** 3, dtype=torch.uint8, device="cuda")
+    timed("supervoxel_grid", lambda: vpt_check(lib.vpt_build_supervoxel_grid(
+        p(dens), n, n, n, sv, 1, p(smin), p(smax), p(savg), p(socc), cs)),
+        dens.numel() * 4 + g ** 3 * 13, f"{n}^3 grid, 8^3 supervoxels with halo: min/max/mean/occupancy")
+    occ = torch.empty(g ** 3, dtype=torch.uint8, device="cuda")
+    dens.zero_()  # an empty grid: every block reads all its voxels (an occupied block stops at its first hit)
+    timed("occupancy_grid", lambda: vpt_check(lib.vpt_build_occupancy_grid(
+        p(dens), n, n, n, 8, 1, ctypes.c_float(0.0), p(occ), cs)),
+        dens.numel() * 4 + g ** 3, f"{n}^3 empty grid (the worst case), 8^3 blocks with a one-voxel halo")
+    del dens, smin, smax, savg, socc, occ
+
+    W = H = 2048
+    color, pos, nrm = (torch.rand(H * W * 4, device="cuda") for _ in range(3))
+    dst = torch.empty_like(color)
+    iters = 5
+    timed("eaw", lambda: vpt_check(lib.vpt_eaw_denoise_rgba(
+        p(color), p(pos), p(nrm), W, H, iters, ctypes.c_float(0.5), ctypes.c_float(0.5), ctypes.c_float(0.5), 1,
+        p(dst), cs)),
+        iters * W * H * (3 * 16 + 16), f"{W}x{H} RGBA, {iters} a-trous iterations (colour, position, normal in, "
+                                      "colour out per iteration)")
+    del pos, nrm, dst
+    k = 5
+    logits = torch.rand(1 * k * k * H * W, device="cuda")
+    img = color[:3 * H * W].contiguous()
+    kout = torch.empty(3 * H * W, device="cuda")
+    timed("kpn_apply", lambda: vpt_check(lib.vpt_kpn_apply(
+        p(img), p(logits), 1, 3, H, W, H, W, k, 1, p(kout), cs)),
+        (k * k + 3 + 3) * 4 * H * W, f"{W}x{H}, 3 channels, {k}x{k} per-pixel kernels with the tap softmax fused")
     return out
 
 
@@ -217,6 +281,7 @@ def run_ours(args):
     vpt.initialize()
     ctx = vpt.context_handle()
     setup_scene(vpt, rank)
+    _lib.check(lib.vpt_set_option(ctx, b"density_texture", float(DENSITY_TEXTURE)), "density_texture", ctx)
     stream = torch.cuda.current_stream()
     ctypes_stream = __import__("ctypes").c_void_p(stream.cuda_stream)
     img = torch.zeros((4, RES, RES), dtype=torch.float32, device="cuda")
@@ -288,6 +353,25 @@ def run_ours(args):
         schedules[label] = RES * RES * SPP_PER_STEP * world / (ms / 1e3)
     _lib.check(lib.vpt_set_option(ctx, b"schedule", 2.0), "schedule", ctx)
 
+    # density fetch path for delta tracking: plain global loads of the x-fastest grid against the 3D
+    # texture object (block layout, bounds test in the texture unit); both read the same texels
+    fetch = {}
+    for tex, label in ((0, "global_loads"), (1, "texture_object"), (DENSITY_TEXTURE, "selected")):
+        _lib.check(lib.vpt_set_option(ctx, b"density_texture", float(tex)), "density_texture", ctx)
+        vpt.render_frame(img, 1)
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(3):
+            _lib.check(lib.vpt_render_frames(ctx, SPP_PER_STEP, ctypes_stream), "render", ctx)
+        e1.record(stream)
+        barrier()
+        ms = max_over_ranks(e0.elapsed_time(e1)) / 3
+        fetch[label] = RES * RES * SPP_PER_STEP * world / (ms / 1e3)
+    fetch["selected"] = "texture_object" if DENSITY_TEXTURE else "global_loads"
+    _lib.check(lib.vpt_set_option(ctx, b"density_texture", float(DENSITY_TEXTURE)), "density_texture", ctx)
+
+
     # end to end through the public API: host grid -> device, render, result -> host
     vpt.set_vpt_mode_from_name("Delta Tracking")
     grid_host = torch.empty((GRID, GRID, GRID), dtype=torch.float32).pin_memory()
@@ -306,6 +390,7 @@ def run_ours(args):
            "path": "vpt.set_density_field(pinned host grid) + vpt.render_frame(cpu tensor)"}
 
     gather = gather_rates(lib, stream)
+    streaming = run_streaming(lib, stream) if rank == 0 else None
     gather_roofline = {"unit": "GB/s", "achieved": achieved, "hbm_random_sector": gather["hbm"],
                        "l2_random_sector": gather["l2"], "frac_of_hbm_random_sector": achieved / gather["hbm"],
                        "frac_of_l2_random_sector": achieved / gather["l2"],
@@ -342,7 +427,7 @@ def run_ours(args):
             "lookups_per_s": lookups / (ms_total / 1e3) * world,
             "lookups_per_path": lookups / max(1, st["paths"]),
             "gather_roofline": gather_roofline,
-            "per_tracker": per_tracker, "tracker_reference_render": reference_render, "schedules_delta": schedules, "e2e": e2e, "gpu_launches": int(launches), "clocks": clock_info,
+            "per_tracker": per_tracker, "tracker_reference_render": reference_render, "schedules_delta": schedules, "fetch_paths_delta": fetch, "streaming_kernels": streaming, "e2e": e2e, "gpu_launches": int(launches), "clocks": clock_info,
         }
         if cpu is not None:
             line["cpu_baseline"] = cpu
@@ -657,10 +742,28 @@ def run_learned(vpt, lib, ctx, small):
         den, ms = timed(learned_once)
         net_ms.append(ms)
         row["learned"] = ld.relmse(den, ref)
-    vpt.set_use_feature_maps([])
     vpt.set_feature_frame_limit(0)
+    # pass 3: SVGF as the reference runs it: every call traces one 1-spp frame with its feature maps,
+    # and the filter carries its colour / moments history from call to call (static camera); the error
+    # after n calls is SVGF's estimate from n samples
+    vpt.set_denoiser("SVGF")
+    vpt.set_frame_index(0)
+    svgf_ms = []
+    done = 0
+    for row in rows:
+        n = row["spp"]
+        out = None
+        while done < n:
+            out, ms = timed(lambda: vpt.render_frame(img, 1))
+            svgf_ms.append(ms)
+            done += 1
+        row["svgf"] = ld.relmse(out[:3].float().contiguous(), ref)
+    vpt.set_denoiser("None")
+    vpt.set_use_feature_maps([])
     net.check_errors()
     spp = [r["spp"] for r in rows]
+    svgf_cost = statistics.median(svgf_ms)  # one traced frame with features + the filter
+    svgf_t = time_to_target(spp, [r["svgf"] for r in rows], lambda s: s * svgf_cost, ev["target"], False)
     eaw_cost = statistics.median(sum(v) / len(v) for v in eaw_ms.values())
     net_cost = statistics.median(net_ms)
     plain_t = time_to_target(spp, [r["plain"] for r in rows], lambda s: s * ms_plain, ev["target"], True)
@@ -674,11 +777,13 @@ def run_learned(vpt, lib, ctx, small):
                      f"inputs {cfg['spp_levels']} spp vs {cfg['target_spp']}-spp targets); held-out scene seed "
                      f"{ev['seed']} {ev['grid']}^3 at {R}^2 vs its FP64 {ev['ref_spp']}-spp render"),
         "relmse_target": ev["target"], "relmse_eps": ld.LOSS_EPS,
-        "time_to_target_ms": {"plain": plain_t, "eaw_tuned": eaw_t, "learned": learned_t},
+        "time_to_target_ms": {"plain": plain_t, "eaw_tuned": eaw_t, "svgf": svgf_t, "learned": learned_t},
+        "svgf_best_relmse": min(r["svgf"] for r in rows),
         "speedup_learned_vs_plain": (plain_t["ms"] / learned_t["ms"]) if learned_t["ms"] else None,
         "speedup_learned_vs_eaw": (eaw_t["ms"] / learned_t["ms"]) if (learned_t["ms"] and eaw_t["ms"]) else None,
         "ms_per_frame": {"plain": ms_plain, "with_features": ms_feat, "feature_frames": kf},
         "denoise_ms": {"eaw": eaw_cost, "learned": net_cost},
+        "svgf_ms_per_frame": svgf_cost,
         "curve": rows, "reference_render_s": ref_s,
         "training": {"data_s": data.seconds, "data_paths": data.paths, "train_s": hist["seconds"],
                      "loss_curve": hist["loss_curve"], "step_ms": step_ms, "launches_per_step": launches_per_step,
@@ -970,6 +1075,7 @@ def profile_trace(spp):
     vpt.initialize()
     ctx = vpt.context_handle()
     setup_scene(vpt, 0)
+    _lib.check(lib.vpt_set_option(ctx, b"density_texture", float(DENSITY_TEXTURE)), "density_texture", ctx)
     vpt.set_vpt_mode_from_name("Delta Tracking")
     _lib.check(lib.vpt_set_resolution(ctx, RES, RES), "resolution", ctx)
     cs = __import__("ctypes").c_void_p(torch.cuda.current_stream().cuda_stream)
@@ -985,6 +1091,7 @@ def profile_trace(spp):
 
 
 def main():
+    global DENSITY_TEXTURE
     ap = argparse.ArgumentParser(description=__doc__)
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
@@ -997,9 +1104,14 @@ def main():
     ap.add_argument("--profile-trace", type=int, default=0, metavar="SPP",
                     help="profiling entry: set up the bench scene, render one warm-up frame, then one launch of "
                          "SPP frames of delta tracking, and exit (capture the second trace launch with ncu)")
+    ap.add_argument("--density-texture", type=int, choices=[0, 1], default=None,
+                    help="delta tracking's density fetch: 1 = the grid's 3D texture object, 0 = global loads "
+                         f"(default {DENSITY_TEXTURE})")
     ap.add_argument("--workload", choices=["full", "small"], default="full",
                     help="small: 384^3 grid, 512^2, 4 spp/step (for ncu captures; not a bench line)")
     args = ap.parse_args()
+    if args.density_texture is not None:
+        DENSITY_TEXTURE = args.density_texture
     if args.warmup < 3:
         args.warmup = 3
     if args.workload == "small":

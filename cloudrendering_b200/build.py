@@ -29,6 +29,9 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", INCLUDE
 # The tracer is compiled without FMA contraction so that its arithmetic matches the CPU oracle
 # operation by operation (see the conventions at the top of vpt_device.cuh).
 NO_FMA = {"vpt_kpn.cu", "vpt_denoise.cu"}
+# The product's per-family tracer units use the special-function unit's log / exp / sin / cos / pow
+# and approximate division and square root (VPT_FAST_MATH in vpt_device.cuh).
+FAST_MATH = True
 
 
 def _is_tracer(src: str) -> bool:
@@ -44,6 +47,8 @@ def _per_file(src: str, double_rounded: bool = False) -> list[str]:
     outputs are bit-exact against the oracle and the reference's shaders in both builds."""
     if src in NO_FMA or src == "vpt_kernels.cu" or (double_rounded and _is_tracer(src)):
         return ["--fmad=false"]
+    if FAST_MATH and src.startswith("vpt_trace_"):
+        return ["-DVPT_FAST_MATH", "--prec-div=false", "--prec-sqrt=false"]
     return []
 
 

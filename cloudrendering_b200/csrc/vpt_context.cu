@@ -192,6 +192,12 @@ struct VptContext {
     bool occ_valid = false;
     int occ_interp = -1;
     DevBuf<uint8_t> occupancy;
+    // the normalised dense grid as a 3D texture (option "density_texture"): delta tracking reads it
+    // through the texture unit when the border density is 0
+    int density_texture = 1;
+    cudaArray_t dens_array = nullptr;
+    cudaTextureObject_t dens_tex = 0;
+    bool dens_tex_failed = false;  // no texture for the current grid (size limit or memory)
 
     // environment image
     int env_w = 0, env_h = 0;
@@ -299,9 +305,62 @@ void compute_bounds(VptContext* ctx) {
     for (int i = 0; i < 3; i++) ctx->box_min[i] = -ctx->box_max[i];
 }
 
+void release_density_texture(VptContext* ctx) {
+    if (ctx->dens_tex) cudaDestroyTextureObject(ctx->dens_tex);
+    if (ctx->dens_array) cudaFreeArray(ctx->dens_array);
+    ctx->dens_tex = 0;
+    ctx->dens_array = nullptr;
+}
+
 void invalidate_accel(VptContext* ctx) {
     ctx->sv_kind = -1;
     ctx->occ_valid = false;
+    release_density_texture(ctx);
+    ctx->dens_tex_failed = false;
+}
+
+// The texture over the normalised dense grid: a float 3D array (the driver's block layout) filled by
+// one device-to-device copy, point filtering, unnormalised coordinates, border address mode (0).
+// Returns false (and the kernels read the grid by global loads) when the array cannot be had: a grid
+// beyond the 3D texture size limit, or no device memory left for the second copy.
+bool ensure_density_texture(VptContext* ctx, cudaStream_t s) {
+    if (ctx->dens_tex) return true;
+    if (ctx->dens_tex_failed) return false;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, ctx->device) != cudaSuccess || ctx->nx > prop.maxTexture3D[0] ||
+        ctx->ny > prop.maxTexture3D[1] || ctx->nz > prop.maxTexture3D[2]) {
+        ctx->dens_tex_failed = true;
+        return false;
+    }
+    const cudaChannelFormatDesc fmt = cudaCreateChannelDesc<float>();
+    const cudaExtent ext = make_cudaExtent((size_t)ctx->nx, (size_t)ctx->ny, (size_t)ctx->nz);
+    if (cudaMalloc3DArray(&ctx->dens_array, &fmt, ext) != cudaSuccess) {
+        cudaGetLastError();  // out of memory is not sticky: clear it and read the grid directly
+        ctx->dens_array = nullptr;
+        ctx->dens_tex_failed = true;
+        return false;
+    }
+    cudaMemcpy3DParms cp = {};
+    cp.srcPtr = make_cudaPitchedPtr(ctx->norm.ptr, (size_t)ctx->nx * sizeof(float), (size_t)ctx->nx, (size_t)ctx->ny);
+    cp.dstArray = ctx->dens_array;
+    cp.extent = ext;
+    cp.kind = cudaMemcpyDeviceToDevice;
+    cudaResourceDesc res = {};
+    res.resType = cudaResourceTypeArray;
+    res.res.array.array = ctx->dens_array;
+    cudaTextureDesc td = {};
+    td.addressMode[0] = td.addressMode[1] = td.addressMode[2] = cudaAddressModeBorder;
+    td.filterMode = cudaFilterModePoint;
+    td.readMode = cudaReadModeElementType;
+    td.normalizedCoords = 0;
+    if (cudaMemcpy3DAsync(&cp, s) != cudaSuccess ||
+        cudaCreateTextureObject(&ctx->dens_tex, &res, &td, nullptr) != cudaSuccess) {
+        cudaGetLastError();
+        release_density_texture(ctx);
+        ctx->dens_tex_failed = true;
+        return false;
+    }
+    return true;
 }
 
 VptStatus finish_grid(VptContext* ctx, cudaStream_t s) {
@@ -897,6 +956,7 @@ void vpt_destroy(VptContext* ctx) {
     cudaDeviceSynchronize();
     ctx->raw.release();
     ctx->norm.release();
+    release_density_texture(ctx);
     ctx->sparse_dev.release();
     ctx->minmax.release();
     ctx->sv_min.release();
@@ -1492,6 +1552,10 @@ VptStatus vpt_render_frames(VptContext* ctx, int frames, void* stream) {
     if (st != VPT_OK) return st;
     vpt::TraceParams P;
     fill_params(ctx, tracker, single ? 1 : frames, P);
+    if (ctx->density_texture && (tracker == vpt::kDelta || tracker == vpt::kRatio || tracker == vpt::kNextEvent) &&
+        !ctx->use_sparse && !P.tf && !P.iso && P.border_density == 0.0f && ensure_density_texture(ctx, s)) {
+        P.density_tex = ctx->dens_tex;
+    }
     if (single) {
         P.frame_count = ctx->frame_count + (uint32_t)frames - 1u;
         P.global_frame = P.frame_count;
@@ -1734,6 +1798,7 @@ VptStatus vpt_set_denoiser_property(VptContext* ctx, const char* key, const char
     else if (k == "phi_position" || k == "phiPosition") ctx->eaw.phi_position = f;
     else if (k == "phi_normal" || k == "phiNormal") ctx->eaw.phi_normal = f;
     else if (k == "ref_compute_quirk") ctx->eaw.ref_compute_quirk = int(f);
+    else if (k == "lattice_tiles") ctx->eaw.lattice_tiles = int(f) ? 1 : 0;
     else if (k == "z_threshold") ctx->svgf.z_threshold = f;
     else if (k == "normal_threshold") ctx->svgf.normal_threshold = f;
     else return fail(ctx, VPT_ERR_ARG, std::string("unknown denoiser property: ") + key);
@@ -2016,6 +2081,8 @@ VptStatus vpt_set_option(VptContext* ctx, const char* key, double value) {
         int v = int(value);
         if (v < 0 || v > 2) return fail(ctx, VPT_ERR_ARG, "schedule must be 0 (tiles), 1 (persistent) or 2 (refill)");
         ctx->schedule = v;
+    } else if (k == "density_texture") {
+        ctx->density_texture = int(value) ? 1 : 0;
     } else if (k == "persistent_blocks_per_sm") {
         if (value < 0 || value > 64) return fail(ctx, VPT_ERR_ARG, "persistent_blocks_per_sm out of range");
         ctx->persistent_blocks_per_sm = int(value);

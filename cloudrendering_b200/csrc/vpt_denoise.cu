@@ -78,6 +78,79 @@ __global__ void eaw_iteration_kernel(const float* __restrict__ color, const floa
     reinterpret_cast<float4*>(out)[(size_t)y * w + x] = make_float4(sum.x / acc, sum.y / acc, sum.z / acc, sum.w / acc);
 }
 
+// The same iteration with the taps staged in shared memory.  The 25 taps of pixel (x, y) at step s lie
+// on the lattice (x + i s, y + j s), so a block takes 16 x 16 pixels of ONE residue class (x mod s,
+// y mod s) spaced s apart: their taps all fall on a 20 x 20 patch of that class's lattice, loaded
+// once (16x reuse at every step, where a dense 16 x 16 tile would share few taps at large steps).
+// Lattice points beyond the image are clamped to the edge pixel, as the taps are.  Same arithmetic,
+// tap for tap, as eaw_iteration_kernel.
+constexpr int kEawTile = 16;
+constexpr int kEawPatch = kEawTile + 4;
+
+__global__ void __launch_bounds__(kEawTile* kEawTile)
+    eaw_lattice_kernel(const float* __restrict__ color, const float* __restrict__ pos, const float* __restrict__ nrm,
+                       float* __restrict__ out, int w, int h, int step, int tiles_x, int tiles_y, float phi_c,
+                       float phi_p, float phi_n, int use_c, int use_p, int use_n, int quirk) {
+    __shared__ float4 sc[kEawPatch][kEawPatch];
+    __shared__ float4 sp[kEawPatch][kEawPatch];
+    __shared__ float4 sn[kEawPatch][kEawPatch];
+    // block -> (residue rx, ry; tile tx, ty)
+    int b = blockIdx.x;
+    const int tx = b % tiles_x;
+    b /= tiles_x;
+    const int ty = b % tiles_y;
+    b /= tiles_y;
+    const int rx = b % step, ry = b / step;
+    const int t = threadIdx.y * kEawTile + threadIdx.x;
+    const bool use_pos = use_p && pos, use_nrm = use_n && nrm;
+    for (int k = t; k < kEawPatch * kEawPatch; k += kEawTile * kEawTile) {
+        const int a = k % kEawPatch, c = k / kEawPatch;
+        const int px = min(max((tx * kEawTile + a - 2) * step + rx, 0), w - 1);
+        const int py = min(max((ty * kEawTile + c - 2) * step + ry, 0), h - 1);
+        const size_t o = (size_t)py * w + px;
+        sc[c][a] = __ldg(reinterpret_cast<const float4*>(color) + o);
+        if (use_pos) sp[c][a] = __ldg(reinterpret_cast<const float4*>(pos) + o);
+        if (use_nrm) sn[c][a] = __ldg(reinterpret_cast<const float4*>(nrm) + o);
+    }
+    __syncthreads();
+    const int x = (tx * kEawTile + threadIdx.x) * step + rx;
+    const int y = (ty * kEawTile + threadIdx.y) * step + ry;
+    if (x >= w || y >= h) return;
+    const int cx = threadIdx.x + 2, cy = threadIdx.y + 2;
+    const float4 cc = sc[cy][cx];
+    const float4 cp = use_pos ? sp[cy][cx] : make_float4(0, 0, 0, 0);
+    const float4 cn = use_nrm ? sn[cy][cx] : make_float4(0, 0, 0, 0);
+    float4 sum = make_float4(0, 0, 0, 0);
+    float acc = 0.0f;
+    const float quirk_wc = fminf(expf(-1.0f / phi_c), 1.0f);
+#pragma unroll
+    for (int i = 0; i < 25; i++) {
+        const int ox = i % 5 - 2, oy = i / 5 - 2;
+        const float kv = c_eaw_kernel[i];
+        const float4 oc = sc[cy + oy][cx + ox];
+        float weight = 1.0f;
+        if (use_c) {
+            float4 d = sub4(cc, oc);
+            weight *= quirk ? quirk_wc : fminf(expf(-dot4(d, d) / phi_c), 1.0f);
+        }
+        if (use_pos) {
+            float4 d = sub4(cp, sp[cy + oy][cx + ox]);
+            weight *= fminf(expf(-dot4(d, d) / phi_p), 1.0f);
+        }
+        if (use_nrm) {
+            float4 d = sub4(cn, sn[cy + oy][cx + ox]);
+            weight *= fminf(expf(-dot4(d, d) / phi_n), 1.0f);
+        }
+        float wk = weight * kv;
+        sum.x += oc.x * wk;
+        sum.y += oc.y * wk;
+        sum.z += oc.z * wk;
+        sum.w += oc.w * wk;
+        acc += wk;
+    }
+    reinterpret_cast<float4*>(out)[(size_t)y * w + x] = make_float4(sum.x / acc, sum.y / acc, sum.z / acc, sum.w / acc);
+}
+
 // The 25 Gaussian tap weights live in constant memory, which is per device: upload once per device.
 static cudaError_t upload_eaw_kernel(cudaStream_t s) {
     static std::mutex mu;
@@ -110,9 +183,20 @@ cudaError_t eaw_denoise(const float* color, const float* pos, const float* nrm, 
     float* dst = nullptr;
     for (int i = 0; i < s.iterations; i++) {
         dst = bufs[i & 1];
-        eaw_iteration_kernel<<<g, b, 0, stream>>>(src, pos, nrm, dst, w, h, step, s.phi_color, s.phi_position,
-                                                  s.phi_normal, s.use_color, s.use_position, s.use_normal,
-                                                  s.ref_compute_quirk);
+        if (s.lattice_tiles) {
+            // per residue class: ceil(ceil(w / step) / 16) x ceil(ceil(h / step) / 16) tiles
+            const int tiles_x = ((w + step - 1) / step + kEawTile - 1) / kEawTile;
+            const int tiles_y = ((h + step - 1) / step + kEawTile - 1) / kEawTile;
+            const long long blocks = (long long)tiles_x * tiles_y * step * step;
+            if (blocks > 0x7fffffffLL) return cudaErrorInvalidValue;
+            eaw_lattice_kernel<<<(unsigned)blocks, dim3(kEawTile, kEawTile), 0, stream>>>(
+                src, pos, nrm, dst, w, h, step, tiles_x, tiles_y, s.phi_color, s.phi_position, s.phi_normal,
+                s.use_color, s.use_position, s.use_normal, s.ref_compute_quirk);
+        } else {
+            eaw_iteration_kernel<<<g, b, 0, stream>>>(src, pos, nrm, dst, w, h, step, s.phi_color, s.phi_position,
+                                                      s.phi_normal, s.use_color, s.use_position, s.use_normal,
+                                                      s.ref_compute_quirk);
+        }
         count_launches(1);
         src = dst;
         step *= 2;

@@ -17,6 +17,7 @@ struct EawSettings {
     int use_position = 1;
     int use_normal = 1;
     int ref_compute_quirk = 0;  // EAWDenoise.glsl:269 uses exp(-1/phiColor) instead of exp(-dist/phiColor)
+    int lattice_tiles = 1;      // taps staged in shared memory per residue-class lattice (eaw_lattice_kernel)
 };
 
 // SVGF settings (src/Denoiser/SVGF.hpp:111-112, 159).

@@ -38,6 +38,19 @@ VPT_DEV float m_cos(float x) { return (float)cos((double)x); }
 VPT_DEV float m_pow(float x, float y) { return (float)pow((double)x, (double)y); }
 VPT_DEV float m_atan2(float y, float x) { return (float)atan2((double)y, (double)x); }
 VPT_DEV float m_asin(float x) { return (float)asin((double)x); }
+#elif defined(VPT_FAST_MATH)
+// The product's tracer units (vpt_trace_*.cu): the special-function unit's approximations of log2,
+// exp2, sin and cos (a few ulp; sin and cos to ~2^-21 absolute on the phase angles in [0, 2 pi)), the
+// precision GLSL's log / exp / sin / cos / pow are allowed and get from a GPU driver.  Argument ranges
+// here: log of (0, 1] (free paths), sin / cos of [0, 2 pi) (phase and sphere sampling), pow of
+// non-negative bases.
+VPT_DEV float m_log(float x) { return __logf(x); }
+VPT_DEV float m_exp(float x) { return __expf(x); }
+VPT_DEV float m_sin(float x) { return __sinf(x); }
+VPT_DEV float m_cos(float x) { return __cosf(x); }
+VPT_DEV float m_pow(float x, float y) { return __powf(x, y); }
+VPT_DEV float m_atan2(float y, float x) { return atan2f(y, x); }
+VPT_DEV float m_asin(float x) { return asinf(x); }
 #else
 VPT_DEV float m_log(float x) { return logf(x); }
 VPT_DEV float m_exp(float x) { return expf(x); }
@@ -477,6 +490,43 @@ VPT_DEV float sample_dense(const TraceParams& P, F3 pos, Rng& rng) {
         uz = uz + jz;
     }
     return sample_dense_vox<INTERP>(P, ux, uy, uz);
+}
+
+// The same lookups through the grid's 3D texture object (point filtering, unnormalised coordinates,
+// border colour 0 = the border density when the grid's minimum is 0): the texel index is computed
+// here as in dense_texel and fetched at its centre, so the value is the same texel, bit for bit; the
+// texture unit does the bounds test and the address arithmetic and reads the array's 3D block layout.
+VPT_DEV float tex_texel(const TraceParams& P, float fx, float fy, float fz) {
+    return tex3D<float>((cudaTextureObject_t)P.density_tex, fx + 0.5f, fy + 0.5f, fz + 0.5f);
+}
+
+template <int INTERP>
+VPT_DEV float sample_dense_tex(const TraceParams& P, F3 pos, Rng& rng) {
+    float ux = (pos.x - P.box_min.x) * P.vox_per_unit.x;
+    float uy = (pos.y - P.box_min.y) * P.vox_per_unit.y;
+    float uz = (pos.z - P.box_min.z) * P.vox_per_unit.z;
+    if (INTERP == kStochastic) {
+        float jx = rng_next(rng) - 0.5f;
+        float jy = rng_next(rng) - 0.5f;
+        float jz = rng_next(rng) - 0.5f;
+        ux = ux + jx;
+        uy = uy + jy;
+        uz = uz + jz;
+    }
+    if (INTERP != kTrilinear) return tex_texel(P, floorf(ux), floorf(uy), floorf(uz));
+    ux = ux - 0.5f;
+    uy = uy - 0.5f;
+    uz = uz - 0.5f;
+    const float fx0 = floorf(ux), fy0 = floorf(uy), fz0 = floorf(uz);
+    const float ax = ux - fx0, ay = uy - fy0, az = uz - fz0;
+    const float fx1 = fx0 + 1.0f, fy1 = fy0 + 1.0f, fz1 = fz0 + 1.0f;
+    float f000 = tex_texel(P, fx0, fy0, fz0), f100 = tex_texel(P, fx1, fy0, fz0);
+    float f010 = tex_texel(P, fx0, fy1, fz0), f110 = tex_texel(P, fx1, fy1, fz0);
+    float f001 = tex_texel(P, fx0, fy0, fz1), f101 = tex_texel(P, fx1, fy0, fz1);
+    float f011 = tex_texel(P, fx0, fy1, fz1), f111 = tex_texel(P, fx1, fy1, fz1);
+    float f0 = mixf(mixf(f000, f100, ax), mixf(f010, f110, ax), ay);
+    float f1 = mixf(mixf(f001, f101, ax), mixf(f011, f111, ax), ay);
+    return mixf(f0, f1, az);
 }
 
 // Transfer function (sampleCloudDensityEmission, VptUtils.glsl:647-672; transferFunctionTexture, a

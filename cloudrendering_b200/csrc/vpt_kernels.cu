@@ -50,14 +50,22 @@ cudaError_t launch_trace(const TraceParams& P, int tracker, int use_ess, int sch
         }
     }
     switch (tracker) {
-        case kDelta: return launch_tracker<kDelta, kDense>(P, schedule, features, persistent_blocks, stream);
-        case kRatio: return launch_tracker<kRatio, kDense>(P, schedule, features, persistent_blocks, stream);
+        case kDelta:
+            if (P.density_tex && !P.tf)
+                return launch_tracker<kDelta, kDenseTex>(P, schedule, features, persistent_blocks, stream);
+            return launch_tracker<kDelta, kDense>(P, schedule, features, persistent_blocks, stream);
+        case kRatio:
+            if (P.density_tex && !P.tf)
+                return launch_tracker<kRatio, kDenseTex>(P, schedule, features, persistent_blocks, stream);
+            return launch_tracker<kRatio, kDense>(P, schedule, features, persistent_blocks, stream);
         case kDecomposition: return launch_tracker<kDecomposition, kDense>(P, schedule, features, persistent_blocks, stream);
         case kResidualRatio: return launch_tracker<kResidualRatio, kDense>(P, schedule, features, persistent_blocks, stream);
         case kResidualRatioNee:
             return launch_tracker<kResidualRatioNee, kDense>(P, schedule, features, persistent_blocks, stream);
         case kNextEvent:
             if (use_ess) return launch_tracker<kNextEvent + 100, kDense>(P, schedule, features, persistent_blocks, stream);
+            if (P.density_tex && !P.tf)
+                return launch_tracker<kNextEvent, kDenseTex>(P, schedule, features, persistent_blocks, stream);
             return launch_tracker<kNextEvent, kDense>(P, schedule, features, persistent_blocks, stream);
         case kSpectralDelta: return launch_tracker<kSpectralDelta, kDense>(P, schedule, features, persistent_blocks, stream);
         case kSpectralNextEvent:

@@ -29,7 +29,9 @@ enum Tracker : int {
 // src/PathTracer/RenderSettings.hpp:64-69).
 enum SdtProbability : int { kSdtMax = 0, kSdtAvg = 1, kSdtPathHistory = 2 };
 
-enum GridKind : int { kDense = 0, kNanoVdb = 1 };
+// kDenseTex: the dense grid read through a 3D texture object (point filtering, border colour 0), a
+// kernel variant chosen by the host when the border density is 0; P.grid_kind stays kDense.
+enum GridKind : int { kDense = 0, kNanoVdb = 1, kDenseTex = 2 };
 enum Interp : int { kNearest = 0, kStochastic = 1, kTrilinear = 2 };
 enum EnvKind : int { kEnvDefault = 0, kEnvBlack = 1, kEnvSingleColor = 2, kEnvConstantSun = 3, kEnvImage = 4 };
 
@@ -133,6 +135,7 @@ struct TraceParams {
     int max_bounces;           // 0 = unlimited
     uint32_t max_steps;        // guard on tentative collisions per path (kMaxStepsPerPath by default)
     int grid_kind;             // GridKind: dense texture or sparse (NanoVDB) volume
+    unsigned long long density_tex; // cudaTextureObject_t over `density` (0: none; kDenseTex kernels)
     int ess_ref_compat;        // reproduce the reference's empty-space-skipping shadow loop exactly
 
     // supervoxels (residual ratio / decomposition tracking, occupancy grid)

@@ -30,6 +30,7 @@ struct Sampler {
     VPT_DEV float operator()(F3 pos, Rng& rng) {
         float v;
         if constexpr (GRID == kNanoVdb) v = sample_sparse<INTERP>(P, pos, rng);
+        else if constexpr (GRID == kDenseTex) v = sample_dense_tex<INTERP>(P, pos, rng);
         else v = sample_dense<INTERP>(P, pos, rng);
         if constexpr (TF) {  // sampleCloud with USE_TRANSFER_FUNCTION: the table's alpha at the density
             float a;
@@ -754,16 +755,26 @@ cudaError_t launch_tracker(const TraceParams& P, int schedule, int features, int
     cudaError_t launch_tracker<T, G>(const TraceParams& P, int schedule, int features, int pb, cudaStream_t s)
 #define VPT_DEFINE_TRACKER(T, G) \
     VPT_DECLARE_TRACKER(T, G) { return launch_interp<T, G>(P, schedule, features, pb, s); }
+// The density read through the grid's 3D texture object: no transfer-function variant (the host does
+// not pick these kernels with a transfer function).
+#define VPT_DEFINE_TRACKER_TEX(T)                                                \
+    VPT_DECLARE_TRACKER(T, kDenseTex) {                                          \
+        if (P.tf || !P.density_tex) return cudaErrorNotSupported;                \
+        return launch_interp_tf<T, kDenseTex, false>(P, schedule, features, pb, s); \
+    }
 
 VPT_DECLARE_TRACKER(kDelta, kDense);
+VPT_DECLARE_TRACKER(kDelta, kDenseTex);
 VPT_DECLARE_TRACKER(kDelta, kNanoVdb);
 VPT_DECLARE_TRACKER(kRatio, kDense);
+VPT_DECLARE_TRACKER(kRatio, kDenseTex);
 VPT_DECLARE_TRACKER(kRatio, kNanoVdb);
 VPT_DECLARE_TRACKER(kDecomposition, kDense);
 VPT_DECLARE_TRACKER(kDecomposition, kNanoVdb);
 VPT_DECLARE_TRACKER(kResidualRatio, kDense);
 VPT_DECLARE_TRACKER(kResidualRatioNee, kDense);
 VPT_DECLARE_TRACKER(kNextEvent, kDense);
+VPT_DECLARE_TRACKER(kNextEvent, kDenseTex);
 VPT_DECLARE_TRACKER(kNextEvent + 100, kDense);
 VPT_DECLARE_TRACKER(kNextEvent, kNanoVdb);
 VPT_DECLARE_TRACKER(kSpectralDelta, kDense);

@@ -4,6 +4,7 @@
 namespace vpt {
 
 VPT_DEFINE_TRACKER(kDelta, kDense)
+VPT_DEFINE_TRACKER_TEX(kDelta)
 VPT_DEFINE_TRACKER(kDelta, kNanoVdb)
 
 cudaError_t launch_tracker_delta_iso(const TraceParams& P, int schedule, int features, int pb, cudaStream_t s) {

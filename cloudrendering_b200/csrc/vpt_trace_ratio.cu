@@ -4,6 +4,7 @@
 namespace vpt {
 
 VPT_DEFINE_TRACKER(kRatio, kDense)
+VPT_DEFINE_TRACKER_TEX(kRatio)
 VPT_DEFINE_TRACKER(kRatio, kNanoVdb)
 
 }  // namespace vpt

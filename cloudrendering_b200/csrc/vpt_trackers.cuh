@@ -39,13 +39,18 @@ VPT_DEV float free_path(Rng& rng, float inv_majorant) {
     return -m_log(fmaxf(0.0000000001f, 1.0f - rng_next(rng))) * inv_majorant;
 }
 
-VPT_DEV void record_event(FirstEvent& fe, F3 x, float density, float extinction, float depth) {
+// A first event without a sampled direction: First W is (w_first, 0), the zero vector for absorptions
+// in delta and spectral tracking (DeltaTracking.glsl:118-119, 276-277), the direction of travel for
+// absorptions in next event tracking (NextEventTracking.glsl:290-291) and the reflected direction at an
+// isosurface hit (CheckIsosurfaceHit.glsl:39-40).
+VPT_DEV void record_event(FirstEvent& fe, F3 x, float density, float extinction, float depth,
+                          F3 w_first = F3{0.0f, 0.0f, 0.0f}) {
     if (!fe.has) {
         fe.has = true;
         fe.x = x;
         fe.density = density * extinction;
         fe.depth = depth;
-        fe.w = f3(0.0f, 0.0f, 0.0f);
+        fe.w = w_first;
         fe.pdf_w = 0.0f;
     }
 }
@@ -144,7 +149,7 @@ VPT_DEV bool iso_segment(const TraceParams& P, S& sample, Rng& rng, F3& x, F3 xn
             x = x + w * 1e-4f;
             first_point = true;
             // firstEvent of a surface hit: density = extinction, depth = tMax - d + |x - x1|
-            if (fe) record_event(*fe, x, 1.0f, P.extinction, tmax - d + length3(x1 - x));
+            if (fe) record_event(*fe, x, 1.0f, P.extinction, tmax - d + length3(x1 - x), w);
             float tmin;
             if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
                 x = x + w * tmin;
@@ -230,12 +235,15 @@ VPT_DEV F3 track_ratio(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, Fi
                 float pa = P.absorb_albedo * density;
                 float ps = P.albedo * density;
                 trans *= 1.0f - pa / (pa + ps);
+                const F3 w_in = w;
                 w = sample_phase(rng, P.g, w);
-                if (!fe.has) {
+                if (!fe.has) {  // RatioTracking.glsl:75-81: no density or depth recorded
                     fe.has = true;
                     fe.x = x;
                     fe.density = 0.0f;
                     fe.depth = 0.0f;
+                    fe.w = w;
+                    fe.pdf_w = evaluate_phase(P.g, w_in, w);
                 }
                 if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
                     x = x + w * tmin;
@@ -388,7 +396,7 @@ VPT_DEV F3 track_nee(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, Firs
             x = xn;
             float xi = rng_next(rng);
             if (xi < P.absorb_albedo * density) {
-                record_event(fe, x, density, P.extinction, tmax - d + t);
+                record_event(fe, x, density, P.extinction, tmax - d + t, w);
                 // USE_EMISSION (NextEventTracking.glsl:296-301): the absorbed path ends with the
                 // emission; else USE_TRANSFER_FUNCTION (:303-310) with the table's
                 return P.emission ? color + sample.emission(x, rng) : (P.tf ? color + sample.tf_emission() : color);
@@ -1068,7 +1076,7 @@ VPT_DEV F3 track_residual_ratio_nee(const TraceParams& P, S& sample, Rng& rng, F
                         const float xi = rng_next(rng);
                         if (xi < P.absorb_albedo * r) {
                             const F3 xa = x + w * t;
-                            record_event(fe, xa, density, P.extinction, depth0 + t);
+                            record_event(fe, xa, density, P.extinction, depth0 + t, w);  // as next event tracking
                             return P.emission ? color + sample.emission(xa, rng) : color;
                         }
                         if (xi < r) {

@@ -266,12 +266,18 @@ VptStatus vpt_set_use_empty_space_skipping(VptContext* ctx, int enabled);
  * occupied, ComputeOccupancyGrid.glsl:108-109, and shadow samples stepped from the moving point,
  * NeeTransmittance.glsl:173-228), "sparse_fp16" (1 = leaf values of the next sparse volume stored as
  * IEEE half), "fbm_contrast" (remap clamp(0.5 + contrast * fbm, 0, 1) of vpt_generate_fbm_grid,
- * default 3.5). */
+ * default 3.5), "density_texture" (1, the default: delta, ratio and next event tracking (without
+ * empty-space skipping or a transfer function) on a dense grid whose border density is 0 read the
+ * density through a 3D texture object, the same texels bit for bit, for a second copy of the grid in
+ * device memory; a grid beyond the 3D texture size or without memory for the copy is read directly;
+ * 0 = always read directly). */
 VptStatus vpt_set_option(VptContext* ctx, const char* key, double value);
 
 /* ---- denoisers (VolumetricPathTracingPass.cpp:2287-2311) ---- */
 VptStatus vpt_set_denoiser(VptContext* ctx, int denoiser_type);
-/* EAW keys: "iterations", "phi_color", "phi_position", "phi_normal", "ref_compute_quirk";
+/* EAW keys: "iterations", "phi_color", "phi_position", "phi_normal", "ref_compute_quirk", "lattice_tiles"
+ * (1, the default: each pass stages its taps in shared memory, 16 x 16 pixels of one residue class
+ * modulo the step per block; 0: every tap read from global memory; the same arithmetic either way);
  * SVGF keys: "z_threshold", "normal_threshold" (set_denoiser_property). */
 VptStatus vpt_set_denoiser_property(VptContext* ctx, const char* key, const char* value);
 

