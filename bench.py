@@ -42,9 +42,10 @@ BYTES_PER_LOOKUP = 32  # one 32-byte sector per uncoalesced density gather
 # delta tracking reads the density through the grid's 3D texture object (1) or by global loads (0);
 # both read the same texels; the bench's fetch_paths_delta leg times the two
 DENSITY_TEXTURE = 1
-# DRAM read + write bytes of one headline launch (64 spp of the 1024^2 image on the 512^3 cloud), from
-# one ncu capture of that launch (profiles/trace_refill_delta_512_1024_64spp.md): 866 B per path
-NCU_DRAM_BYTES_PER_PATH = 58.12e9 / (1024 * 1024 * 64)
+# DRAM read + write bytes of one headline launch (64 spp of the 1024^2 image on the 512^3 cloud, density
+# through the texture object), from one ncu capture of that launch
+# (profiles/trace_refill_delta_512_1024_64spp.md): 37.56 GB, 560 B per path
+NCU_DRAM_BYTES_PER_PATH = (35.711e9 + 1.845e9) / (1024 * 1024 * 64)
 
 
 def tensor_peak():
@@ -420,8 +421,8 @@ def run_ours(args):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak,
                          "traffic": NCU_DRAM_BYTES_PER_PATH * RES * RES * SPP_PER_STEP if args.workload == "full" else None,
-                         "limiter": "instruction issue at low SIMT efficiency (72 % issue active, 11.4 of 32 lanes per "
-                                    "instruction, DRAM 10 % busy; profiles/trace_refill_delta_512_1024_64spp.md)",
+                         "limiter": "instruction issue at low SIMT efficiency (71 % issue active, 12.8 of 32 lanes per "
+                                    "instruction, DRAM 9 % busy; profiles/trace_refill_delta_512_1024_64spp.md)",
                          "note": f"algorithmic bytes = density lookups x {BYTES_PER_LOOKUP} B sector; peak {peak_kind} "
                                  "HBM copy; traffic = ncu dram read + write bytes of this launch"},
             "lookups_per_s": lookups / (ms_total / 1e3) * world,
@@ -582,16 +583,16 @@ def run_trackers(vpt, lib, ctx, img, stream, ctypes_stream, barrier, max_over_ra
 
 
 # Learned denoiser: a kernel-predicting U-Net (widths 32-64-96-128-160, 13x13 kernels) trained on the
-# GPU by this package's tcgen05 kernels on tracer-generated pairs (64 seeded cloud scenes at 256^2:
+# GPU by this package's tcgen05 kernels on tracer-generated pairs (512 seeded cloud scenes at 256^2:
 # noisy renders at 1..256 spp with albedo / normal / depth / transmittance features against 2048-spp
-# targets from disjoint frames; Adam, batch 8, 4000 steps, learning
-# rate cosine-annealed from 5e-4 to 1e-5), then the time each method needs
-# to reach relMSE <= 1e-3 on a held-out scene (256^3 cloud, 512^2, max 128 bounces) against its
-# FP64-accumulated 16384-spp render: plain accumulation, EAW (iteration count 1..5 chosen per sample
-# count by the lowest error, i.e. tuned with the reference in hand) and the learned denoiser.
-LEARNED = dict(scenes=256, size=256, spp_levels=(1, 2, 4, 8, 16, 64, 256), target_spp=2048, steps=6000, batch=8,
+# targets from disjoint frames; Adam, batch 8, 6000 steps, learning rate cosine-annealed from 5e-4 to
+# 1e-5), then the time each method needs to reach relMSE <= 1e-3 on held-out scenes (256^3 clouds,
+# 512^2, max 128 bounces) against their FP64-accumulated 16384-spp renders: plain accumulation, EAW
+# (iteration count 1..5 chosen per sample count by the lowest error, i.e. tuned with the reference in
+# hand), SVGF (one 1-spp frame per call, history carried between calls) and the learned denoiser.
+LEARNED = dict(scenes=512, size=256, spp_levels=(1, 2, 4, 8, 16, 64, 256), target_spp=2048, steps=6000, batch=8,
                lr=5e-4, lr_end=1e-5, kernel_size=13, grid=128)
-EVAL = dict(seed=77777, res=512, grid=256, max_bounces=128, ref_spp=16384,
+EVAL = dict(seeds=(77777, 77778, 77779, 77780), res=512, grid=256, max_bounces=128, ref_spp=16384,
             levels=(1, 2, 4, 8, 16, 32, 64, 128, 256, 512, 1024, 2048, 4096), target=1e-3)
 
 
@@ -621,7 +622,7 @@ def run_learned(vpt, lib, ctx, small):
     cfg, ev = dict(LEARNED), dict(EVAL)
     if small:
         cfg.update(scenes=8, size=128, steps=300, target_spp=512, lr_end=None)
-        ev.update(res=256, grid=128, ref_spp=4096, levels=(1, 2, 4, 8, 16, 32, 64, 128, 256, 512))
+        ev.update(seeds=(77777,), res=256, grid=128, ref_spp=4096, levels=(1, 2, 4, 8, 16, 32, 64, 128, 256, 512))
     stream = torch.cuda.current_stream()
     cs = ctypes.c_void_p(stream.cuda_stream)
     data = ld.TrainingSet(vpt, cfg["scenes"], cfg["size"], cfg["spp_levels"], cfg["target_spp"], grid=cfg["grid"])
@@ -646,141 +647,160 @@ def run_learned(vpt, lib, ctx, small):
     net = ld.KpnUNet(seed=0, kernel_size=cfg["kernel_size"])
     hist = ld.train(net, data, cfg["steps"], cfg["batch"], cfg["lr"], seed=1, lr_end=cfg.get("lr_end"))
 
-    # held-out scene: FP64 reference, then the error curves
-    sc = ld.sample_scene(ev["seed"])
-    ld.setup_scene(vpt, sc, grid=ev["grid"], max_bounces=ev["max_bounces"])
-    R = ev["res"]
-    img = torch.zeros((3, R, R), dtype=torch.float32, device="cuda")
+    def eval_scene(seed):
+        """One held-out scene: its FP64 reference, every method's error curve and time to target."""
+        # held-out scene: FP64 reference, then the error curves
+        sc = ld.sample_scene(seed)
+        ld.setup_scene(vpt, sc, grid=ev["grid"], max_bounces=ev["max_bounces"])
+        R = ev["res"]
+        img = torch.zeros((3, R, R), dtype=torch.float32, device="cuda")
 
-    def frame_ms(frames):
-        vpt.render_frame(img, 2)
-        a, c = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        _lib_check(lib.vpt_render_frames(ctx, frames, cs))
-        c.record(stream)
-        torch.cuda.synchronize()
-        return a.elapsed_time(c) / frames
+        def frame_ms(frames):
+            vpt.render_frame(img, 2)
+            a, c = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            _lib_check(lib.vpt_render_frames(ctx, frames, cs))
+            c.record(stream)
+            torch.cuda.synchronize()
+            return a.elapsed_time(c) / frames
 
-    def _lib_check(st):
-        vpt._lib.check(st, "render", ctx)
+        def _lib_check(st):
+            vpt._lib.check(st, "render", ctx)
 
-    t_ref = time.perf_counter()
-    ref = None
-    for offset, frames in independent_passes(R, R, ev["ref_spp"]):
-        vpt.set_seed_offset(offset)
+        t_ref = time.perf_counter()
+        ref = None
+        for offset, frames in independent_passes(R, R, ev["ref_spp"]):
+            vpt.set_seed_offset(offset)
+            vpt.set_frame_index(0)
+            left = frames
+            while left > 0:
+                k = min(256, left)
+                vpt.render_frame(img, k)
+                left -= k
+            part = vpt.get_film_sum(R, R).cuda()
+            ref = part if ref is None else ref + part
+        ref = ref / float(ev["ref_spp"])
+        ref_s = time.perf_counter() - t_ref
+        vpt.set_seed_offset(0)
         vpt.set_frame_index(0)
-        left = frames
-        while left > 0:
-            k = min(256, left)
-            vpt.render_frame(img, k)
-            left -= k
-        part = vpt.get_film_sum(R, R).cuda()
-        ref = part if ref is None else ref + part
-    ref = ref / float(ev["ref_spp"])
-    ref_s = time.perf_counter() - t_ref
-    vpt.set_seed_offset(0)
-    vpt.set_frame_index(0)
-    ms_plain = frame_ms(64)
-    vpt.set_use_feature_maps(["Albedo", "Normal", "Depth", "Transmittance"])
-    vpt.set_denoiser("Edge-Avoiding À-Trous Wavelet Transform")
-    vpt.set_denoiser_property("iterations", "1")
-    ms_feat = frame_ms(64)  # a frame with the feature pass
-    # each denoiser with its own best feature setting: EAW's edge-stopping weights want feature maps
-    # accumulated over every frame (as the reference renders them); the learned denoiser reads feature
-    # maps accumulated over the first FEATURE_FRAMES frames (as it was trained), and later frames are
-    # traced without the feature pass
-    kf = ld.FEATURE_FRAMES
+        ms_plain = frame_ms(64)
+        vpt.set_use_feature_maps(["Albedo", "Normal", "Depth", "Transmittance"])
+        vpt.set_denoiser("Edge-Avoiding À-Trous Wavelet Transform")
+        vpt.set_denoiser_property("iterations", "1")
+        ms_feat = frame_ms(64)  # a frame with the feature pass
+        # each denoiser with its own best feature setting: EAW's edge-stopping weights want feature maps
+        # accumulated over every frame (as the reference renders them); the learned denoiser reads feature
+        # maps accumulated over the first FEATURE_FRAMES frames (as it was trained), and later frames are
+        # traced without the feature pass
+        kf = ld.FEATURE_FRAMES
 
-    def render_ms(spp):
-        return min(spp, kf) * ms_feat + max(0.0, spp - kf) * ms_plain
+        def render_ms(spp):
+            return min(spp, kf) * ms_feat + max(0.0, spp - kf) * ms_plain
 
-    def timed(fn):
-        a, c = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        r = fn()
-        c.record(stream)
-        torch.cuda.synchronize()
-        return r, a.elapsed_time(c)
+        def timed(fn):
+            a, c = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            r = fn()
+            c.record(stream)
+            torch.cuda.synchronize()
+            return r, a.elapsed_time(c)
 
-    rows = [{"spp": n} for n in ev["levels"]]
-    eaw_ms, net_ms = {}, []
-    # pass 1: plain accumulation and EAW (features every frame)
-    vpt.set_frame_index(0)
-    done = 0
-    for row in rows:
-        n = row["spp"]
-        vpt.render_frame(img, n - done)
-        done = n
-        plain = (vpt.get_film_sum(R, R).cuda() / n).float().contiguous()
-        row["plain"] = ld.relmse(plain, ref)
-        best = None
-        for it in (1, 2, 3, 4, 5):
-            vpt.set_denoiser_property("iterations", str(it))
-            d, ms = timed(lambda: vpt.get_feature_map(img, 0))
-            eaw_ms.setdefault(it, []).append(ms)
-            r = ld.relmse(d, ref)
-            if best is None or r < best[0]:
-                best = (r, it)
-        row["eaw"], row["eaw_iterations"] = best
-    # pass 2: the learned denoiser (the same frames: identical film, features over the first kf frames),
-    # replayed from a CUDA graph captured for this image size
-    dgraph = net.graph(1, R, R)
-    vpt.set_denoiser("None")
-    vpt.set_feature_frame_limit(kf)
-    vpt.set_frame_index(0)
-    done = 0
-    for row in rows:
-        n = row["spp"]
-        vpt.render_frame(img, n - done)
-        done = n
-        plain = (vpt.get_film_sum(R, R).cuda() / n).float().contiguous()
+        rows = [{"spp": n} for n in ev["levels"]]
+        eaw_ms, net_ms = {}, []
+        # pass 1: plain accumulation and EAW (features every frame)
+        vpt.set_frame_index(0)
+        done = 0
+        for row in rows:
+            n = row["spp"]
+            vpt.render_frame(img, n - done)
+            done = n
+            plain = (vpt.get_film_sum(R, R).cuda() / n).float().contiguous()
+            row["plain"] = ld.relmse(plain, ref)
+            best = None
+            for it in (1, 2, 3, 4, 5):
+                vpt.set_denoiser_property("iterations", str(it))
+                d, ms = timed(lambda: vpt.get_feature_map(img, 0))
+                eaw_ms.setdefault(it, []).append(ms)
+                r = ld.relmse(d, ref)
+                if best is None or r < best[0]:
+                    best = (r, it)
+            row["eaw"], row["eaw_iterations"] = best
+        # pass 2: the learned denoiser (the same frames: identical film, features over the first kf frames),
+        # replayed from a CUDA graph captured for this image size
+        dgraph = net.graph(1, R, R)
+        vpt.set_denoiser("None")
+        vpt.set_feature_frame_limit(kf)
+        vpt.set_frame_index(0)
+        done = 0
+        for row in rows:
+            n = row["spp"]
+            vpt.render_frame(img, n - done)
+            done = n
+            plain = (vpt.get_film_sum(R, R).cuda() / n).float().contiguous()
 
-        noise = torch.full((1,), 1.0 / math.sqrt(n), device="cuda")
+            noise = torch.full((1,), 1.0 / math.sqrt(n), device="cuda")
 
-        def learned_once():  # the renderer's feature planes go straight into the graph's inputs
-            return dgraph.from_renderer(vpt, plain, noise)[0]
-        den, ms = timed(learned_once)
-        net_ms.append(ms)
-        row["learned"] = ld.relmse(den, ref)
-    vpt.set_feature_frame_limit(0)
-    # pass 3: SVGF as the reference runs it: every call traces one 1-spp frame with its feature maps,
-    # and the filter carries its colour / moments history from call to call (static camera); the error
-    # after n calls is SVGF's estimate from n samples
-    vpt.set_denoiser("SVGF")
-    vpt.set_frame_index(0)
-    svgf_ms = []
-    done = 0
-    for row in rows:
-        n = row["spp"]
-        out = None
-        while done < n:
-            out, ms = timed(lambda: vpt.render_frame(img, 1))
-            svgf_ms.append(ms)
-            done += 1
-        row["svgf"] = ld.relmse(out[:3].float().contiguous(), ref)
-    vpt.set_denoiser("None")
-    vpt.set_use_feature_maps([])
-    net.check_errors()
-    spp = [r["spp"] for r in rows]
-    svgf_cost = statistics.median(svgf_ms)  # one traced frame with features + the filter
-    svgf_t = time_to_target(spp, [r["svgf"] for r in rows], lambda s: s * svgf_cost, ev["target"], False)
-    eaw_cost = statistics.median(sum(v) / len(v) for v in eaw_ms.values())
-    net_cost = statistics.median(net_ms)
-    plain_t = time_to_target(spp, [r["plain"] for r in rows], lambda s: s * ms_plain, ev["target"], True)
-    eaw_t = time_to_target(spp, [r["eaw"] for r in rows], lambda s: s * ms_feat + eaw_cost, ev["target"], False)
-    learned_t = time_to_target(spp, [r["learned"] for r in rows], lambda s: render_ms(s) + net_cost, ev["target"],
-                               False)
+            def learned_once():  # the renderer's feature planes go straight into the graph's inputs
+                return dgraph.from_renderer(vpt, plain, noise)[0]
+            den, ms = timed(learned_once)
+            net_ms.append(ms)
+            row["learned"] = ld.relmse(den, ref)
+        vpt.set_feature_frame_limit(0)
+        # pass 3: SVGF as the reference runs it: every call traces one 1-spp frame with its feature maps,
+        # and the filter carries its colour / moments history from call to call (static camera); the error
+        # after n calls is SVGF's estimate from n samples
+        vpt.set_denoiser("SVGF")
+        vpt.set_frame_index(0)
+        svgf_ms = []
+        done = 0
+        for row in rows:
+            n = row["spp"]
+            out = None
+            while done < n:
+                out, ms = timed(lambda: vpt.render_frame(img, 1))
+                svgf_ms.append(ms)
+                done += 1
+            row["svgf"] = ld.relmse(out[:3].float().contiguous(), ref)
+        vpt.set_denoiser("None")
+        vpt.set_use_feature_maps([])
+        net.check_errors()
+        spp = [r["spp"] for r in rows]
+        svgf_cost = statistics.median(svgf_ms)  # one traced frame with features + the filter
+        svgf_t = time_to_target(spp, [r["svgf"] for r in rows], lambda s: s * svgf_cost, ev["target"], False)
+        eaw_cost = statistics.median(sum(v) / len(v) for v in eaw_ms.values())
+        net_cost = statistics.median(net_ms)
+        plain_t = time_to_target(spp, [r["plain"] for r in rows], lambda s: s * ms_plain, ev["target"], True)
+        eaw_t = time_to_target(spp, [r["eaw"] for r in rows], lambda s: s * ms_feat + eaw_cost, ev["target"], False)
+        learned_t = time_to_target(spp, [r["learned"] for r in rows], lambda s: render_ms(s) + net_cost, ev["target"],
+                                   False)
+        return {"seed": seed, "rows": rows, "plain": plain_t, "eaw_tuned": eaw_t, "svgf": svgf_t,
+                "learned": learned_t, "ms_plain": ms_plain, "ms_feat": ms_feat, "eaw_cost": eaw_cost,
+                "net_cost": net_cost, "svgf_cost": svgf_cost, "ref_s": ref_s, "kf": kf, "R": R}
+
+    scenes = [eval_scene(sd) for sd in ev["seeds"]]
+    speedups = [e["eaw_tuned"]["ms"] / e["learned"]["ms"] for e in scenes
+                if e["learned"]["ms"] and e["eaw_tuned"]["ms"]]
+    first = scenes[0]
+    rows, plain_t, eaw_t, svgf_t, learned_t = (first["rows"], first["plain"], first["eaw_tuned"], first["svgf"],
+                                               first["learned"])
+    ms_plain, ms_feat, kf, R = first["ms_plain"], first["ms_feat"], first["kf"], first["R"]
+    eaw_cost, net_cost, svgf_cost, ref_s = first["eaw_cost"], first["net_cost"], first["svgf_cost"], first["ref_s"]
     peak, peak_kind = tensor_peak()
     out = {
         "workload": (f"KPN U-Net {'-'.join(map(str, net.widths))}, {cfg['kernel_size']}x{cfg['kernel_size']} kernels, "
                      f"trained {cfg['steps']} steps (batch {cfg['batch']} x {cfg['size']}^2, {cfg['scenes']} scenes, "
                      f"inputs {cfg['spp_levels']} spp vs {cfg['target_spp']}-spp targets); held-out scene seed "
-                     f"{ev['seed']} {ev['grid']}^3 at {R}^2 vs its FP64 {ev['ref_spp']}-spp render"),
+                     f"{ev['seeds'][0]} (curves; {len(ev['seeds'])} seeds for the median speed-up) {ev['grid']}^3 at {R}^2 vs its "
+                     f"FP64 {ev['ref_spp']}-spp render"),
         "relmse_target": ev["target"], "relmse_eps": ld.LOSS_EPS,
         "time_to_target_ms": {"plain": plain_t, "eaw_tuned": eaw_t, "svgf": svgf_t, "learned": learned_t},
         "svgf_best_relmse": min(r["svgf"] for r in rows),
         "speedup_learned_vs_plain": (plain_t["ms"] / learned_t["ms"]) if learned_t["ms"] else None,
         "speedup_learned_vs_eaw": (eaw_t["ms"] / learned_t["ms"]) if (learned_t["ms"] and eaw_t["ms"]) else None,
+        "speedup_learned_vs_eaw_median_over_seeds": statistics.median(speedups) if speedups else None,
+        "per_seed": [{"seed": e["seed"], "time_to_target_ms": {k: e[k] for k in ("plain", "eaw_tuned", "svgf", "learned")},
+                      "speedup_learned_vs_eaw": (e["eaw_tuned"]["ms"] / e["learned"]["ms"])
+                      if (e["learned"]["ms"] and e["eaw_tuned"]["ms"]) else None} for e in scenes],
         "ms_per_frame": {"plain": ms_plain, "with_features": ms_feat, "feature_frames": kf},
         "denoise_ms": {"eaw": eaw_cost, "learned": net_cost},
         "svgf_ms_per_frame": svgf_cost,
@@ -801,7 +821,7 @@ def run_learned(vpt, lib, ctx, small):
 # tracking (the reference's sparse empty-space-skipping tracker), fp32 and fp16 leaf values.
 SPARSE_DIMS = (2048, 1024, 1536)
 SPARSE_RES = (1920, 1080)
-SPARSE_SPP_PER_STEP = 4
+SPARSE_SPP_PER_STEP = 128  # the configuration's 128 spp, one step = one full render
 SPARSE_EXTINCTION = 2000.0
 SPARSE_MAX_BOUNCES = 256
 SPARSE_SEED = 3
@@ -1104,6 +1124,8 @@ def main():
     ap.add_argument("--profile-trace", type=int, default=0, metavar="SPP",
                     help="profiling entry: set up the bench scene, render one warm-up frame, then one launch of "
                          "SPP frames of delta tracking, and exit (capture the second trace launch with ncu)")
+    ap.add_argument("--streaming", action="store_true",
+                    help="run only the streaming-kernel leg (builders, EAW, KPN apply) and print its JSON")
     ap.add_argument("--density-texture", type=int, choices=[0, 1], default=None,
                     help="delta tracking's density fetch: 1 = the grid's 3D texture object, 0 = global loads "
                          f"(default {DENSITY_TEXTURE})")
@@ -1121,7 +1143,12 @@ def main():
         global SPARSE_DIMS, SPARSE_RES, BATCH_SCENES
         SPARSE_DIMS, SPARSE_RES = (512, 256, 384), (480, 270)
         BATCH_SCENES = 8
-    if args.profile_trace:
+    if args.streaming:
+        import torch
+        from cloudrendering_b200 import _lib
+        torch.cuda.set_device(0)
+        print(json.dumps({"streaming_kernels": run_streaming(_lib.load(), torch.cuda.current_stream())}), flush=True)
+    elif args.profile_trace:
         profile_trace(args.profile_trace)
     elif args.impl == "reference":
         run_reference(args)

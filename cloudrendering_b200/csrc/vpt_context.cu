@@ -197,6 +197,9 @@ struct VptContext {
     int density_texture = 1;
     cudaArray_t dens_array = nullptr;
     cudaTextureObject_t dens_tex = 0;
+    cudaSurfaceObject_t dens_surf = 0;  // the same array, written by fill_density_array_kernel
+    int dens_dims[3] = {0, 0, 0};
+    bool dens_tex_fresh = false;   // the array holds the current grid
     bool dens_tex_failed = false;  // no texture for the current grid (size limit or memory)
 
     // environment image
@@ -307,59 +310,76 @@ void compute_bounds(VptContext* ctx) {
 
 void release_density_texture(VptContext* ctx) {
     if (ctx->dens_tex) cudaDestroyTextureObject(ctx->dens_tex);
+    if (ctx->dens_surf) cudaDestroySurfaceObject(ctx->dens_surf);
     if (ctx->dens_array) cudaFreeArray(ctx->dens_array);
     ctx->dens_tex = 0;
+    ctx->dens_surf = 0;
     ctx->dens_array = nullptr;
+    ctx->dens_dims[0] = ctx->dens_dims[1] = ctx->dens_dims[2] = 0;
+    ctx->dens_tex_fresh = false;
 }
 
+// A new grid: the texture array is refilled on next use (kept when the dimensions stay the same).
 void invalidate_accel(VptContext* ctx) {
     ctx->sv_kind = -1;
     ctx->occ_valid = false;
-    release_density_texture(ctx);
+    ctx->dens_tex_fresh = false;
     ctx->dens_tex_failed = false;
 }
 
-// The texture over the normalised dense grid: a float 3D array (the driver's block layout) filled by
-// one device-to-device copy, point filtering, unnormalised coordinates, border address mode (0).
-// Returns false (and the kernels read the grid by global loads) when the array cannot be had: a grid
-// beyond the 3D texture size limit, or no device memory left for the second copy.
+// The texture over the normalised dense grid: a float 3D array (the driver's block layout) with a
+// texture object (point filtering, unnormalised coordinates, border address mode: 0) and a surface
+// object through which fill_density_array_kernel copies the grid in (one pass at HBM speed).  The
+// array is kept across grids of the same size.  Returns false (and the kernels read the grid by
+// global loads) when the array cannot be had: a grid beyond the 3D texture size limit, or no device
+// memory left for the second copy.
 bool ensure_density_texture(VptContext* ctx, cudaStream_t s) {
-    if (ctx->dens_tex) return true;
+    if (ctx->dens_tex_fresh) return true;
     if (ctx->dens_tex_failed) return false;
-    cudaDeviceProp prop;
-    if (cudaGetDeviceProperties(&prop, ctx->device) != cudaSuccess || ctx->nx > prop.maxTexture3D[0] ||
-        ctx->ny > prop.maxTexture3D[1] || ctx->nz > prop.maxTexture3D[2]) {
-        ctx->dens_tex_failed = true;
-        return false;
+    if (ctx->dens_array &&
+        (ctx->dens_dims[0] != ctx->nx || ctx->dens_dims[1] != ctx->ny || ctx->dens_dims[2] != ctx->nz))
+        release_density_texture(ctx);
+    if (!ctx->dens_array) {
+        cudaDeviceProp prop;
+        if (cudaGetDeviceProperties(&prop, ctx->device) != cudaSuccess || ctx->nx > prop.maxTexture3D[0] ||
+            ctx->ny > prop.maxTexture3D[1] || ctx->nz > prop.maxTexture3D[2] || ctx->ny > 65535 || ctx->nz > 65535) {
+            ctx->dens_tex_failed = true;
+            return false;
+        }
+        const cudaChannelFormatDesc fmt = cudaCreateChannelDesc<float>();
+        const cudaExtent ext = make_cudaExtent((size_t)ctx->nx, (size_t)ctx->ny, (size_t)ctx->nz);
+        if (cudaMalloc3DArray(&ctx->dens_array, &fmt, ext, cudaArraySurfaceLoadStore) != cudaSuccess) {
+            cudaGetLastError();  // out of memory is not sticky: clear it and read the grid directly
+            ctx->dens_array = nullptr;
+            ctx->dens_tex_failed = true;
+            return false;
+        }
+        cudaResourceDesc res = {};
+        res.resType = cudaResourceTypeArray;
+        res.res.array.array = ctx->dens_array;
+        cudaTextureDesc td = {};
+        td.addressMode[0] = td.addressMode[1] = td.addressMode[2] = cudaAddressModeBorder;
+        td.filterMode = cudaFilterModePoint;
+        td.readMode = cudaReadModeElementType;
+        td.normalizedCoords = 0;
+        if (cudaCreateTextureObject(&ctx->dens_tex, &res, &td, nullptr) != cudaSuccess ||
+            cudaCreateSurfaceObject(&ctx->dens_surf, &res) != cudaSuccess) {
+            cudaGetLastError();
+            release_density_texture(ctx);
+            ctx->dens_tex_failed = true;
+            return false;
+        }
+        ctx->dens_dims[0] = ctx->nx;
+        ctx->dens_dims[1] = ctx->ny;
+        ctx->dens_dims[2] = ctx->nz;
     }
-    const cudaChannelFormatDesc fmt = cudaCreateChannelDesc<float>();
-    const cudaExtent ext = make_cudaExtent((size_t)ctx->nx, (size_t)ctx->ny, (size_t)ctx->nz);
-    if (cudaMalloc3DArray(&ctx->dens_array, &fmt, ext) != cudaSuccess) {
-        cudaGetLastError();  // out of memory is not sticky: clear it and read the grid directly
-        ctx->dens_array = nullptr;
-        ctx->dens_tex_failed = true;
-        return false;
-    }
-    cudaMemcpy3DParms cp = {};
-    cp.srcPtr = make_cudaPitchedPtr(ctx->norm.ptr, (size_t)ctx->nx * sizeof(float), (size_t)ctx->nx, (size_t)ctx->ny);
-    cp.dstArray = ctx->dens_array;
-    cp.extent = ext;
-    cp.kind = cudaMemcpyDeviceToDevice;
-    cudaResourceDesc res = {};
-    res.resType = cudaResourceTypeArray;
-    res.res.array.array = ctx->dens_array;
-    cudaTextureDesc td = {};
-    td.addressMode[0] = td.addressMode[1] = td.addressMode[2] = cudaAddressModeBorder;
-    td.filterMode = cudaFilterModePoint;
-    td.readMode = cudaReadModeElementType;
-    td.normalizedCoords = 0;
-    if (cudaMemcpy3DAsync(&cp, s) != cudaSuccess ||
-        cudaCreateTextureObject(&ctx->dens_tex, &res, &td, nullptr) != cudaSuccess) {
+    if (vpt::launch_fill_density_array(ctx->norm.ptr, ctx->dens_surf, ctx->nx, ctx->ny, ctx->nz, s) != cudaSuccess) {
         cudaGetLastError();
         release_density_texture(ctx);
         ctx->dens_tex_failed = true;
         return false;
     }
+    ctx->dens_tex_fresh = true;
     return true;
 }
 
@@ -1211,6 +1231,7 @@ VptStatus vpt_set_nanovdb_grid(VptContext* ctx, const void* buffer, size_t bytes
     // the NanoVDB grid replaces the dense grid (CloudData::setNanoVdbGridHandle)
     ctx->raw.release();
     ctx->norm.release();
+    release_density_texture(ctx);
     invalidate_accel(ctx);
     ctx->use_sparse = true;
     ctx->sparse_valid = true;

@@ -4,8 +4,8 @@
 // Data/Shaders/Denoiser/EAWDenoise.glsl: 5x5 taps at step 2^i with Gaussian weights exp(-(x^2+y^2)/2),
 // colour / position / normal edge stops min(exp(-|d|^2/phi), 1); taps outside the image are clamped
 // to the edge (sampler address mode of the reference's textures).  One launch per iteration, each
-// thread one pixel; the 25 taps of a warp are contiguous rows, served from L1/L2 (the image chain
-// of 3 RGBA maps stays L2-resident up to 2048^2).
+// thread one pixel; by default a block stages the taps of 16 x 16 pixels of one residue class modulo
+// the step in shared memory (eaw_lattice_kernel), the direct kernel reads every tap through L1.
 //
 // SVGF: Data/Shaders/Denoiser/SVGF/SVGF.glsl (reproject 210-267, filter moments 286-347, a-trous
 // 401-495) with compute_weight from svgf_common.glsl:29-41.
@@ -36,6 +36,13 @@ __device__ __forceinline__ float4 sub4(float4 a, float4 b) {
     return make_float4(a.x - b.x, a.y - b.y, a.z - b.z, a.w - b.w);
 }
 
+// Edge-stopping weight min(exp(-|d|^2 / phi), 1) with the special-function unit's exponential and
+// the reciprocal of phi computed once (a few ulp from the IEEE form; the filter is a normalised
+// weighted mean, so its output moves by about as much).
+__device__ __forceinline__ float eaw_stop(float4 d, float inv_phi) {
+    return fminf(__expf(-dot4(d, d) * inv_phi), 1.0f);
+}
+
 __global__ void eaw_iteration_kernel(const float* __restrict__ color, const float* __restrict__ pos,
                                      const float* __restrict__ nrm, float* __restrict__ out, int w, int h, int step,
                                      float phi_c, float phi_p, float phi_n, int use_c, int use_p, int use_n,
@@ -49,6 +56,7 @@ __global__ void eaw_iteration_kernel(const float* __restrict__ color, const floa
     float4 sum = make_float4(0, 0, 0, 0);
     float acc = 0.0f;
     const float quirk_wc = fminf(expf(-1.0f / phi_c), 1.0f);
+    const float inv_c = 1.0f / phi_c, inv_p = 1.0f / phi_p, inv_n = 1.0f / phi_n;
 #pragma unroll
     for (int i = 0; i < 25; i++) {
         int ox = i % 5 - 2, oy = i / 5 - 2;
@@ -58,15 +66,15 @@ __global__ void eaw_iteration_kernel(const float* __restrict__ color, const floa
         float weight = 1.0f;
         if (use_c) {
             float4 d = sub4(cc, oc);
-            weight *= quirk ? quirk_wc : fminf(expf(-dot4(d, d) / phi_c), 1.0f);
+            weight *= quirk ? quirk_wc : eaw_stop(d, inv_c);
         }
         if (use_p && pos) {
             float4 d = sub4(cp, ld4(pos, sx, sy, w, h));
-            weight *= fminf(expf(-dot4(d, d) / phi_p), 1.0f);
+            weight *= eaw_stop(d, inv_p);
         }
         if (use_n && nrm) {
             float4 d = sub4(cn, ld4(nrm, sx, sy, w, h));
-            weight *= fminf(expf(-dot4(d, d) / phi_n), 1.0f);
+            weight *= eaw_stop(d, inv_n);
         }
         float wk = weight * kv;
         sum.x += oc.x * wk;
@@ -75,7 +83,8 @@ __global__ void eaw_iteration_kernel(const float* __restrict__ color, const floa
         sum.w += oc.w * wk;
         acc += wk;
     }
-    reinterpret_cast<float4*>(out)[(size_t)y * w + x] = make_float4(sum.x / acc, sum.y / acc, sum.z / acc, sum.w / acc);
+    const float ia = 1.0f / acc;
+    reinterpret_cast<float4*>(out)[(size_t)y * w + x] = make_float4(sum.x * ia, sum.y * ia, sum.z * ia, sum.w * ia);
 }
 
 // The same iteration with the taps staged in shared memory.  The 25 taps of pixel (x, y) at step s lie
@@ -123,6 +132,7 @@ __global__ void __launch_bounds__(kEawTile* kEawTile)
     float4 sum = make_float4(0, 0, 0, 0);
     float acc = 0.0f;
     const float quirk_wc = fminf(expf(-1.0f / phi_c), 1.0f);
+    const float inv_c = 1.0f / phi_c, inv_p = 1.0f / phi_p, inv_n = 1.0f / phi_n;
 #pragma unroll
     for (int i = 0; i < 25; i++) {
         const int ox = i % 5 - 2, oy = i / 5 - 2;
@@ -131,15 +141,15 @@ __global__ void __launch_bounds__(kEawTile* kEawTile)
         float weight = 1.0f;
         if (use_c) {
             float4 d = sub4(cc, oc);
-            weight *= quirk ? quirk_wc : fminf(expf(-dot4(d, d) / phi_c), 1.0f);
+            weight *= quirk ? quirk_wc : eaw_stop(d, inv_c);
         }
         if (use_pos) {
             float4 d = sub4(cp, sp[cy + oy][cx + ox]);
-            weight *= fminf(expf(-dot4(d, d) / phi_p), 1.0f);
+            weight *= eaw_stop(d, inv_p);
         }
         if (use_nrm) {
             float4 d = sub4(cn, sn[cy + oy][cx + ox]);
-            weight *= fminf(expf(-dot4(d, d) / phi_n), 1.0f);
+            weight *= eaw_stop(d, inv_n);
         }
         float wk = weight * kv;
         sum.x += oc.x * wk;
@@ -148,7 +158,8 @@ __global__ void __launch_bounds__(kEawTile* kEawTile)
         sum.w += oc.w * wk;
         acc += wk;
     }
-    reinterpret_cast<float4*>(out)[(size_t)y * w + x] = make_float4(sum.x / acc, sum.y / acc, sum.z / acc, sum.w / acc);
+    const float ia = 1.0f / acc;
+    reinterpret_cast<float4*>(out)[(size_t)y * w + x] = make_float4(sum.x * ia, sum.y * ia, sum.z * ia, sum.w * ia);
 }
 
 // The 25 Gaussian tap weights live in constant memory, which is per device: upload once per device.

@@ -319,17 +319,58 @@ __global__ void occupancy_kernel(const float* __restrict__ dens, int nx, int ny,
     }
     int bx = warp % gx, by = (warp / gx) % gy, bz = warp / (gx * gy);
     int ext = bs + 2 * halo;
-    int n = ext * ext * ext;
     bool occ = false;
-    for (int i = lane; i < n && !__any_sync(__activemask(), occ); i += 32) {
-        int ox = i % ext - halo, oy = (i / ext) % ext - halo, oz = i / (ext * ext) - halo;
-        int x = bx * bs + ox, y = by * bs + oy, z = bz * bs + oz;
-        if (x >= 0 && y >= 0 && z >= 0 && x < nx && y < ny && z < nz) {
-            occ |= __ldg(dens + ((size_t)z * ny + y) * nx + x) > threshold;
+    if (ext <= 32) {
+        // the warp reads 32 / ext rows of the block (with its halo) per step, lane (lx, lr) the voxel lx
+        // of row lr; rows advance by (y, z) increments, without divisions in the loop
+        const int per = 32 / ext;
+        const int steps = (ext * ext + per - 1) / per;  // the same trip count on every lane
+        const int lx = lane % ext, lr = lane / ext;
+        int oy = lr % ext, oz = lr / ext;  // row lr of the block
+        const int x = bx * bs + lx - halo;
+        const bool x_in = lr < per && x >= 0 && x < nx;
+        for (int k = 0; k < steps; k++) {
+            if (__any_sync(0xffffffffu, occ)) break;
+            const int y = by * bs + oy - halo, z = bz * bs + oz - halo;
+            if (x_in && oz < ext && y >= 0 && y < ny && z >= 0 && z < nz)
+                occ |= __ldg(dens + ((size_t)z * ny + y) * nx + x) > threshold;
+            oy += per;
+            while (oy >= ext) {
+                oy -= ext;
+                oz++;
+            }
+        }
+    } else {
+        const int n = ext * ext * ext;
+        for (int i = lane; i < n && !__any_sync(__activemask(), occ); i += 32) {
+            int ox = i % ext - halo, oy = (i / ext) % ext - halo, oz = i / (ext * ext) - halo;
+            int x = bx * bs + ox, y = by * bs + oy, z = bz * bs + oz;
+            if (x >= 0 && y >= 0 && z >= 0 && x < nx && y < ny && z < nz) {
+                occ |= __ldg(dens + ((size_t)z * ny + y) * nx + x) > threshold;
+            }
         }
     }
     occ = __any_sync(0xffffffffu, occ);
     if (lane == 0) out[warp] = occ ? 1 : 0;
+}
+
+// ---------------------------------------------------------------------------------------------
+// The grid's texture array: one thread per voxel of a row (x), rows y and slices z on the grid's y and
+// z dimensions; coalesced reads, surface stores into the array's block layout.
+__global__ void fill_density_array_kernel(const float* __restrict__ src, cudaSurfaceObject_t surf, int nx, int ny) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y, z = blockIdx.z;
+    if (x >= nx) return;
+    surf3Dwrite(__ldg(src + ((size_t)z * ny + y) * nx + x), surf, x * (int)sizeof(float), y, z);
+}
+
+cudaError_t launch_fill_density_array(const float* src, unsigned long long surface, int nx, int ny, int nz,
+                                      cudaStream_t s) {
+    if (ny > 65535 || nz > 65535) return cudaErrorInvalidValue;
+    fill_density_array_kernel<<<dim3((unsigned)((nx + 255) / 256), (unsigned)ny, (unsigned)nz), 256, 0, s>>>(
+        src, (cudaSurfaceObject_t)surface, nx, ny);
+    count_launches(1);
+    return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------------------------------

@@ -26,46 +26,56 @@ namespace {
 constexpr int kMaxKpnChannels = 4;
 constexpr int kMaxTaps = 49;  // kernels up to 7 x 7
 
-// softmax over the K logits of pixel (y, x): torch's definition exp(l - max) / sum exp(l - max)
-__device__ __forceinline__ void tap_softmax(const float* __restrict__ wbase, size_t plane, int K, float* p) {
+// softmax over the K logits of pixel (y, x): torch's definition exp(l - max) / sum exp(l - max).
+// K is a compile-time constant so that the K values live in registers.
+template <int K>
+__device__ __forceinline__ void tap_softmax(const float* __restrict__ wbase, size_t plane, float* p) {
     float m = -INFINITY;
+#pragma unroll
     for (int k = 0; k < K; k++) {
         p[k] = __ldg(wbase + (size_t)k * plane);
         m = fmaxf(m, p[k]);
     }
     float s = 0.0f;
+#pragma unroll
     for (int k = 0; k < K; k++) {
         p[k] = expf(p[k] - m);
         s += p[k];
     }
+#pragma unroll
     for (int k = 0; k < K; k++) p[k] = p[k] / s;
 }
 
+template <int KS>
 __global__ void kpn_apply_kernel(const float* __restrict__ image, const float* __restrict__ weights,
                                  float* __restrict__ out, int N, int C, int H, int W, int Hw, int Ww, int h, int w,
-                                 int k, int softmax) {
+                                 int softmax) {
+    constexpr int K = KS * KS;
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     const int n = blockIdx.z;
     if (x >= w || y >= h || n >= N) return;
-    const int K = k * k;
     const size_t plane = (size_t)Hw * Ww;
     const float* wb = weights + (size_t)n * K * plane + (size_t)y * Ww + x;
-    float p[kMaxTaps];
+    float p[K];
     if (softmax) {
-        tap_softmax(wb, plane, K, p);
+        tap_softmax<K>(wb, plane, p);
     } else {
+#pragma unroll
         for (int t = 0; t < K; t++) p[t] = __ldg(wb + (size_t)t * plane);
     }
     float acc[kMaxKpnChannels] = {0.0f, 0.0f, 0.0f, 0.0f};
-    int t = 0;
-    for (int dy = -k / 2; dy <= k / 2; dy++) {
+#pragma unroll
+    for (int dy = -KS / 2; dy <= KS / 2; dy++) {
         const int ky = y + dy;
-        for (int dx = -k / 2; dx <= k / 2; dx++, t++) {
+#pragma unroll
+        for (int dx = -KS / 2; dx <= KS / 2; dx++) {
+            const int t = (dy + KS / 2) * KS + (dx + KS / 2);
             const int kx = x + dx;
             if (kx < 0 || kx >= w || ky < 0 || ky >= h) continue;
-            for (int c = 0; c < C; c++)
-                acc[c] += p[t] * __ldg(image + (((size_t)n * C + c) * H + ky) * W + kx);
+#pragma unroll
+            for (int c = 0; c < kMaxKpnChannels; c++)
+                if (c < C) acc[c] += p[t] * __ldg(image + (((size_t)n * C + c) * H + ky) * W + kx);
         }
     }
     for (int c = 0; c < C; c++) out[(((size_t)n * C + c) * h + y) * w + x] = acc[c];
@@ -107,20 +117,23 @@ __device__ __forceinline__ bool inv_iter_base(const InvIterArgs& a, int n, int c
     return true;
 }
 
+template <int KS>
 __global__ void kpn_inv_iter_kernel(const InvIterArgs a) {
+    constexpr int K = KS * KS;
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     const int n = blockIdx.z;
     if (x >= a.w || y >= a.h || n >= a.N) return;
-    const int K = a.k * a.k;
     const size_t plane = (size_t)a.Hw * a.Ww;
-    float p[kMaxTaps];
-    tap_softmax(a.fused + (size_t)n * (K + 3) * plane + (size_t)y * a.Ww + x, plane, K, p);
+    float p[K];
+    tap_softmax<K>(a.fused + (size_t)n * (K + 3) * plane + (size_t)y * a.Ww + x, plane, p);
     float acc[kMaxKpnChannels] = {0.0f, 0.0f, 0.0f, 0.0f};
-    int t = 0;
-    for (int dy = -a.k / 2; dy <= a.k / 2; dy++) {
+#pragma unroll
+    for (int dy = -KS / 2; dy <= KS / 2; dy++) {
         const int ky = y + dy;
-        for (int dx = -a.k / 2; dx <= a.k / 2; dx++, t++) {
+#pragma unroll
+        for (int dx = -KS / 2; dx <= KS / 2; dx++) {
+            const int t = (dy + KS / 2) * KS + (dx + KS / 2);
             const int kx = x + dx;
             if (kx < 0 || kx >= a.w || ky < 0 || ky >= a.h) continue;
             for (int c = 0; c < a.C; c++) {
@@ -197,8 +210,13 @@ VptStatus vpt_kpn_apply(const float* image, const float* weights, int n, int c, 
         return VPT_ERR_ARG;
     const int ho = h < weights_h ? h : weights_h, wo = w < weights_w ? w : weights_w;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    vpt::kpn_apply_kernel<<<vpt::grid2d(wo, ho, n), dim3(16, 16), 0, s>>>(image, weights, out, n, c, h, w, weights_h,
-                                                                          weights_w, ho, wo, kernel_size, softmax);
+    const dim3 g = vpt::grid2d(wo, ho, n), b(16, 16);
+    switch (kernel_size) {
+        case 1: vpt::kpn_apply_kernel<1><<<g, b, 0, s>>>(image, weights, out, n, c, h, w, weights_h, weights_w, ho, wo, softmax); break;
+        case 3: vpt::kpn_apply_kernel<3><<<g, b, 0, s>>>(image, weights, out, n, c, h, w, weights_h, weights_w, ho, wo, softmax); break;
+        case 5: vpt::kpn_apply_kernel<5><<<g, b, 0, s>>>(image, weights, out, n, c, h, w, weights_h, weights_w, ho, wo, softmax); break;
+        default: vpt::kpn_apply_kernel<7><<<g, b, 0, s>>>(image, weights, out, n, c, h, w, weights_h, weights_w, ho, wo, softmax); break;
+    }
     vpt::count_launches(1);
     return cudaGetLastError() == cudaSuccess ? VPT_OK : VPT_ERR_CUDA;
 }
@@ -230,7 +248,13 @@ VptStatus vpt_kpn_inv_iter(const float* x_hi, const float* pred_lo, const float*
     a.k = kernel_size;
     a.use_prev = use_prev ? 1 : 0;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    vpt::kpn_inv_iter_kernel<<<vpt::grid2d(a.w, a.h, n), dim3(16, 16), 0, s>>>(a);
+    const dim3 g = vpt::grid2d(a.w, a.h, n), b(16, 16);
+    switch (kernel_size) {  // odd and at most 7 (checked above)
+        case 1: vpt::kpn_inv_iter_kernel<1><<<g, b, 0, s>>>(a); break;
+        case 3: vpt::kpn_inv_iter_kernel<3><<<g, b, 0, s>>>(a); break;
+        case 5: vpt::kpn_inv_iter_kernel<5><<<g, b, 0, s>>>(a); break;
+        default: vpt::kpn_inv_iter_kernel<7><<<g, b, 0, s>>>(a); break;
+    }
     vpt::count_launches(1);
     return cudaGetLastError() == cudaSuccess ? VPT_OK : VPT_ERR_CUDA;
 }
