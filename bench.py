@@ -515,10 +515,12 @@ def run_trackers(vpt, lib, ctx, img, stream, ctypes_stream, barrier, max_over_ra
     out = {}
     # delta tracking with isosurfaces at density 0.5 (Lambertian surfaces, trilinear lookups) is a
     # different image: its rate only
-    for name, mode in list(TRACKERS.items()) + [("delta_isosurfaces", 0)]:
+    for name, mode in list(TRACKERS.items()) + [("nee_empty_space_skipping", 5), ("delta_isosurfaces", 0)]:
         iso = name == "delta_isosurfaces"
         vpt.set_vpt_mode(mode)
         vpt.set_use_isosurfaces(iso)
+        # next event tracking whose shadow rays skip the occupancy grid's empty 8^3 blocks
+        vpt.set_use_empty_space_skipping(name == "nee_empty_space_skipping")
         vpt.set_iso_value(0.5)
         vpt.set_frame_index(0)
         _lib.check(lib.vpt_render_frames(ctx, 1, ctypes_stream), "warm-up", ctx)
@@ -571,6 +573,7 @@ def run_trackers(vpt, lib, ctx, img, stream, ctypes_stream, barrier, max_over_ra
                         "image_mean": [float(v) for v in mc]})
         out[name] = row
     vpt.set_use_isosurfaces(False)
+    vpt.set_use_empty_space_skipping(False)
     vpt.set_collect_statistics(False)
     vpt.set_frame_index(0)
     reference = {"tracker": "delta", "spp": ref_spp, "accumulation": "fp64", "seconds": ref_s,

@@ -235,6 +235,8 @@ struct VptContext {
     bool features_on = false;
     bool feat_background = false;  // the Background map was requested (one more accumulator per sample)
     int feat_depth_maps = 0;       // bit 0: Depth Blended, bit 1: Depth Nearest Opaque requested (ray marches)
+    bool feat_depth_deriv = false; // Depth (nabla) or Depth (fwidth) requested (per-frame normals replayed)
+    DevBuf<float> frame_normals;   //   4 floats per pixel and frame of one feature launch
     DevBuf<float> feat;
     DevBuf<float> rgba_src, rgba_a, rgba_b;  // denoiser input and ping-pong buffers
     DevBuf<float> eaw_maps;                  // position + normal RGBA for EAW
@@ -880,6 +882,15 @@ VptStatus batch_prepare(VptBatch* b, const int* frames, cudaStream_t s, vpt::Bat
         if (st != VPT_OK) return batch_fail(b, st, ctx->last_error);
         fill_params(ctx, t, frames[i], b->h_params[i]);
         b->h_offsets[i + 1] = b->h_offsets[i] + vpt::padded_paths(ctx->width, ctx->height, (uint32_t)frames[i]);
+        // the density through each scene's texture object when every scene has one
+        if (gk == vpt::kDense && ctx->density_texture && b->h_params[i].border_density == 0.0f &&
+            ensure_density_texture(ctx, s))
+            b->h_params[i].density_tex = ctx->dens_tex;
+    }
+    if (grid_kind == vpt::kDense) {
+        bool all_tex = true;
+        for (int i = 0; i < n; i++) all_tex = all_tex && b->h_params[i].density_tex != 0;
+        if (all_tex) grid_kind = vpt::kDenseTex;
     }
     int per_sm = b->blocks_per_sm;
     if (per_sm <= 0) {
@@ -1600,11 +1611,36 @@ VptStatus vpt_render_frames(VptContext* ctx, int frames, void* stream) {
         feat_n = (int)std::min<uint32_t>(left, (uint32_t)frames);
     }
     const int plain_n = (single ? 1 : frames) - feat_n;
-    if (feat_n > 0) {
+    if (feat_n > 0 && !ctx->feat_depth_deriv) {
         vpt::TraceParams Pf = P;
         Pf.num_frames = feat_n;
         Pf.num_paths = (uint64_t)ctx->width * ctx->height * (uint64_t)feat_n;
         VPT_CHECK_CUDA(ctx, vpt::launch_trace(Pf, tracker, ctx->use_ess, ctx->schedule, 1, pb, s));
+    } else if (feat_n > 0) {
+        // Depth (nabla) / (fwidth): the feature frames in chunks whose per-frame normals fit 256 MiB, each
+        // followed by the in-order replay of its frames per pixel
+        const size_t npix = (size_t)ctx->width * ctx->height;
+        const int chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)feat_n, (256u << 20) / (npix * 16)));
+        VPT_CHECK_CUDA(ctx, ctx->frame_normals.alloc(npix * 4 * (size_t)chunk));
+        double view[16], iv[16];
+        compute_view(ctx, view);
+        mat_inverse(view, iv);
+        float itv[16];  // transpose(inverse(view)), column-major
+        for (int r = 0; r < 4; r++)
+            for (int c = 0; c < 4; c++) itv[c * 4 + r] = float(iv[r * 4 + c]);
+        const uint32_t film0 = single ? 0u : ctx->film_frames;  // accumulation frame of the call's first frame
+        for (int done = 0; done < feat_n; done += chunk) {
+            const int k = std::min(chunk, feat_n - done);
+            vpt::TraceParams Pf = P;
+            Pf.num_frames = (uint32_t)k;
+            Pf.num_paths = (uint64_t)npix * (uint64_t)k;
+            Pf.frame_count = P.frame_count + (uint32_t)done;
+            Pf.global_frame = P.global_frame + (uint32_t)done;
+            Pf.frame_normals = ctx->frame_normals.ptr;
+            VPT_CHECK_CUDA(ctx, vpt::launch_trace(Pf, tracker, ctx->use_ess, ctx->schedule, 1, pb, s));
+            VPT_CHECK_CUDA(ctx, vpt::launch_depth_deriv(ctx->frame_normals.ptr, k, (int)npix, film0 + (uint32_t)done,
+                                                        itv, ctx->feat.ptr, s));
+        }
     }
     if (plain_n > 0) {
         vpt::TraceParams Pp = P;
@@ -1709,19 +1745,23 @@ VptStatus vpt_read_statistics(VptContext* ctx, double* out_sum, double* out_sum_
 
 VptStatus vpt_set_use_feature_maps(VptContext* ctx, const int* features, int count) {
     VPT_CHECK_CTX(ctx);
-    bool on = false, background = false;
+    bool on = false, background = false, deriv = false;
     int depth_maps = 0;
     for (int i = 0; i < count; i++) {
         if (features && features[i] != VPT_FEATURE_RESULT) on = true;
         if (features && features[i] == VPT_FEATURE_BACKGROUND) background = true;
         if (features && features[i] == VPT_FEATURE_DEPTH_BLENDED) depth_maps |= 1;
         if (features && features[i] == VPT_FEATURE_DEPTH_NEAREST_OPAQUE) depth_maps |= 2;
+        if (features && (features[i] == VPT_FEATURE_DEPTH_NABLA || features[i] == VPT_FEATURE_DEPTH_FWIDTH)) deriv = true;
     }
-    if (on != ctx->features_on || background != ctx->feat_background || depth_maps != ctx->feat_depth_maps)
+    if (on != ctx->features_on || background != ctx->feat_background || depth_maps != ctx->feat_depth_maps ||
+        deriv != ctx->feat_depth_deriv)
         reset_film_state(ctx);
     ctx->features_on = on;
     ctx->feat_background = background;
     ctx->feat_depth_maps = depth_maps;
+    ctx->feat_depth_deriv = deriv;
+    if (!deriv) ctx->frame_normals.release();
     return VPT_OK;
 }
 
@@ -1734,7 +1774,8 @@ VptStatus vpt_get_feature_map(VptContext* ctx, int feature, float* out, int chan
     if (feature == VPT_FEATURE_BACKGROUND && !ctx->feat_background)
         return fail(ctx, VPT_ERR_STATE, "the Background map was not requested in set_use_feature_maps");
     if ((feature == VPT_FEATURE_DEPTH_BLENDED && !(ctx->feat_depth_maps & 1)) ||
-        (feature == VPT_FEATURE_DEPTH_NEAREST_OPAQUE && !(ctx->feat_depth_maps & 2)))
+        (feature == VPT_FEATURE_DEPTH_NEAREST_OPAQUE && !(ctx->feat_depth_maps & 2)) ||
+        ((feature == VPT_FEATURE_DEPTH_NABLA || feature == VPT_FEATURE_DEPTH_FWIDTH) && !ctx->feat_depth_deriv))
         return fail(ctx, VPT_ERR_STATE, "the depth map was not requested in set_use_feature_maps");
     cudaStream_t s = as_stream(stream);
     int n = ctx->width * ctx->height;

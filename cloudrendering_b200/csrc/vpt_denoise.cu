@@ -610,6 +610,80 @@ cudaError_t svgf_filter_passes(SvgfCur c, float4* color_history, float4* moments
 }
 
 // ---------------------------------------------------------------------------------------------
+// Depth (nabla) and Depth (fwidth) (Clouds.glsl:258-297, 344-364).  Each frame f of the reference
+// mixes the normal map (running mean; frames without an event scale it by f / (f + 1)), then, for a
+// frame with an event, projects that running-mean normal with inverseTransposedViewMatrix and takes
+// nabla = (A / sqrt(1 - A^2), B / sqrt(1 - B^2)) of its x and y (0 without an event), whose running
+// means are the two maps (fwidth = |nabla.x| + |nabla.y|).  The frames of a launch run concurrently
+// here, so the trace stores each frame's normal and this kernel replays the frames in order per pixel.
+
+__global__ void depth_deriv_kernel(const float4* __restrict__ frame_normals, int frames, int n, uint32_t f0, Mat4 M,
+                                   float* __restrict__ feat) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float* f = feat + (size_t)i * kFeatStride;
+    float nx = f[kFeatDerivNormal + 0], ny = f[kFeatDerivNormal + 1], nz = f[kFeatDerivNormal + 2];
+    float ax = f[kFeatNabla + 0], ay = f[kFeatNabla + 1], fw = f[kFeatFwidth];
+    for (int j = 0; j < frames; j++) {
+        const uint32_t frame = f0 + (uint32_t)j;
+        const float4 v = frame_normals[(size_t)j * n + i];
+        const float t = 1.0f / float(frame + 1u);
+        float bx = 0.0f, by = 0.0f;
+        if (v.w != 0.0f) {
+            float dx = v.x, dy = v.y, dz = v.z;
+            if (frame != 0u) {  // mix(diffOld, diff, 1 / (frame + 1)); diffOld = 0 at frame 0
+                dx = nx * (1.0f - t) + dx * t;
+                dy = ny * (1.0f - t) + dy * t;
+                dz = nz * (1.0f - t) + dz * t;
+            } else {
+                dx = 0.0f * (1.0f - t) + dx * t;
+                dy = 0.0f * (1.0f - t) + dy * t;
+                dz = 0.0f * (1.0f - t) + dz * t;
+            }
+            nx = dx;
+            ny = dy;
+            nz = dz;
+            // (inverseTransposedViewMatrix * vec4(diff, 0)).xy
+            const float A = ((M.m[0] * dx + M.m[4] * dy) + M.m[8] * dz) + M.m[12] * 0.0f;
+            const float B = ((M.m[1] * dx + M.m[5] * dy) + M.m[9] * dz) + M.m[13] * 0.0f;
+            bx = A / sqrtf(1.0f - A * A);
+            by = B / sqrtf(1.0f - B * B);
+        } else {
+            const float s = frame == 0u ? 0.0f : float(frame) / float(frame + 1u);
+            nx = frame == 0u ? 0.0f : nx * s;
+            ny = frame == 0u ? 0.0f : ny * s;
+            nz = frame == 0u ? 0.0f : nz * s;
+        }
+        const float fv = fabsf(bx) + fabsf(by);
+        if (frame != 0u) {
+            ax = ax * (1.0f - t) + bx * t;
+            ay = ay * (1.0f - t) + by * t;
+            fw = fw * (1.0f - t) + fv * t;
+        } else {
+            ax = bx;
+            ay = by;
+            fw = fv;
+        }
+    }
+    f[kFeatDerivNormal + 0] = nx;
+    f[kFeatDerivNormal + 1] = ny;
+    f[kFeatDerivNormal + 2] = nz;
+    f[kFeatNabla + 0] = ax;
+    f[kFeatNabla + 1] = ay;
+    f[kFeatFwidth] = fw;
+}
+
+cudaError_t launch_depth_deriv(const float* frame_normals, int frames, int n, uint32_t f0,
+                               const float inv_transposed_view[16], float* feat, cudaStream_t s) {
+    Mat4 M;
+    for (int k = 0; k < 16; k++) M.m[k] = inv_transposed_view[k];
+    depth_deriv_kernel<<<(n + 255) / 256, 256, 0, s>>>(reinterpret_cast<const float4*>(frame_normals), frames, n, f0,
+                                                       M, feat);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------------------------
 __global__ void feature_to_chw_kernel(const float* __restrict__ feat, int n, float inv_frames, int feature,
                                       int channels, float a0, float a1, float a2, float far_distance,
                                       float* __restrict__ out) {
@@ -701,6 +775,13 @@ __global__ void feature_to_chw_kernel(const float* __restrict__ feat, int n, flo
             v[0] = f[kFeatFlowReverse];
             v[1] = f[kFeatFlowReverse + 1];
             break;
+        case VPT_FEATURE_DEPTH_NABLA:  // running means written by depth_deriv_kernel (imageStore(vec4(nabla, 0, 0)))
+            v[0] = f[kFeatNabla];
+            v[1] = f[kFeatNabla + 1];
+            break;
+        case VPT_FEATURE_DEPTH_FWIDTH:  // imageStore(depthFwidthImage, vec4(fwidthValue))
+            v[0] = v[1] = v[2] = v[3] = f[kFeatFwidth];
+            break;
         case VPT_FEATURE_REPROJ_UV: {  // (-1, -1) until a frame had an event (Clouds.glsl:240)
             const unsigned long long* key = reinterpret_cast<const unsigned long long*>(f + kFeatReprojUV);
             v[0] = (key[0] >> 32) != 0 ? __uint_as_float((uint32_t)key[0]) : -1.0f;
@@ -733,6 +814,8 @@ cudaError_t feature_to_chw(const float* feat, int n, uint32_t frames, int featur
         case VPT_FEATURE_FLOW:
         case VPT_FEATURE_FLOW_REVERSE:
         case VPT_FEATURE_REPROJ_UV:
+        case VPT_FEATURE_DEPTH_NABLA:
+        case VPT_FEATURE_DEPTH_FWIDTH:
             break;
         default:
             return cudaErrorInvalidValue;

@@ -73,6 +73,11 @@ cudaError_t svgf_denoise_features(const float* color_rgba, const float* feat, ui
 // albedo / normal [3][n], depth / transmittance [n] planes of the feature accumulation (NULL = skip)
 cudaError_t denoiser_features(const float* feat, int n, uint32_t frames, const float* albedo_rgb, float* albedo,
                               float* normal, float* depth, float* trans, cudaStream_t stream);
+// Depth (nabla) / Depth (fwidth): advances each pixel's running-mean normal, nabla and fwidth over the
+// `frames` frames of one feature launch (per-frame normals from the trace, frame-major float4), the
+// first of which is accumulation frame f0; inv_transposed_view is column-major 4 x 4.
+cudaError_t launch_depth_deriv(const float* frame_normals, int frames, int n, uint32_t f0,
+                               const float inv_transposed_view[16], float* feat, cudaStream_t s);
 cudaError_t feature_to_chw(const float* feat, int n, uint32_t frames, int feature, int channels, const float* albedo,
                            float far_distance, float* out, cudaStream_t stream);
 

@@ -136,6 +136,8 @@ struct TraceParams {
     uint32_t max_steps;        // guard on tentative collisions per path (kMaxStepsPerPath by default)
     int grid_kind;             // GridKind: dense texture or sparse (NanoVDB) volume
     unsigned long long density_tex; // cudaTextureObject_t over `density` (0: none; kDenseTex kernels)
+    float* frame_normals;      // Depth (nabla) / (fwidth): 4 floats per frame of the launch and pixel, the
+                               //   first event's normal and 1 (0 0 0 0 without an event), frame-major
     int ess_ref_compat;        // reproduce the reference's empty-space-skipping shadow loop exactly
 
     // supervoxels (residual ratio / decomposition tracking, occupancy grid)
@@ -224,7 +226,10 @@ enum FeatureSlot : int {
                              //   bits: atomicMax keeps the uv of the latest frame with an event in the
                              //   previous view, whatever order the frames are traced in (0: none yet)
                              // 35: unused
-    kFeatStride = 36,
+    kFeatDerivNormal = 36,   // Depth (nabla) / (fwidth): the running-mean normal as Clouds.glsl mixes it,
+    kFeatNabla = 39,         //   the nabla running mean (2)
+    kFeatFwidth = 41,        //   and the fwidth running mean, advanced frame by frame by depth_deriv_kernel
+    kFeatStride = 42,
 };
 
 }  // namespace vpt

@@ -135,9 +135,10 @@ VPT_DEV void update_reproj_uv(const TraceParams& P, float* f, const FirstEvent& 
 }
 
 template <class S>
-VPT_DEV void accumulate_features(const TraceParams& P, S& sample, Rng& rng, size_t pix, const FirstEvent& fe,
-                                 F3 result, F3 x_camera, F3 w_camera) {
+VPT_DEV void accumulate_features(const TraceParams& P, S& sample, Rng& rng, size_t pix, uint32_t frame,
+                                 const FirstEvent& fe, F3 result, F3 x_camera, F3 w_camera) {
     float* f = P.feat + pix * kFeatStride;
+    float4 frame_normal = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     if (P.feat_background) {
         const F3 bg = fe.has ? sky_only(P, w_camera) : result;
         atomicAdd(f + kFeatBackground + 0, bg.x);
@@ -146,6 +147,7 @@ VPT_DEV void accumulate_features(const TraceParams& P, S& sample, Rng& rng, size
     }
     if (fe.has) {
         F3 n = sample.normal(fe.x, rng);
+        frame_normal = make_float4(n.x, n.y, n.z, 1.0f);
         atomicAdd(f + kFeatNormal + 0, n.x);
         atomicAdd(f + kFeatNormal + 1, n.y);
         atomicAdd(f + kFeatNormal + 2, n.z);
@@ -162,6 +164,10 @@ VPT_DEV void accumulate_features(const TraceParams& P, S& sample, Rng& rng, size
         atomicAdd(f + kFeatCloudOnly + 2, result.z);
     } else {
         atomicAdd(f + kFeatTrans, 1.0f);
+    }
+    if (P.frame_normals) {
+        const size_t npix = (size_t)P.width * P.height;
+        reinterpret_cast<float4*>(P.frame_normals)[(size_t)frame * npix + pix] = frame_normal;
     }
     // after the normal, in the reference's order (Clouds.glsl:367-383)
     if (P.feat_depth_maps & 1) {
@@ -242,7 +248,7 @@ VPT_DEV void trace_one(const TraceParams& P, S& sample, uint32_t frame, int px, 
         atomicAdd(P.film_sq + pix * 3 + 2, (double)L.z * (double)L.z);
     }
     if (features) {
-        accumulate_features(P, sample, rng, pix, fe, L, x, w);
+        accumulate_features(P, sample, rng, pix, frame, fe, L, x, w);
         if (fe.has) update_reproj_uv(P, P.feat + pix * kFeatStride, fe, P.global_frame + frame);
         if (frame + 1 == P.num_frames) write_last_frame_features(P, P.feat + pix * kFeatStride, fe, px, py, w);
     }
@@ -316,7 +322,33 @@ __global__ void __launch_bounds__(kTraceBlock) trace_persistent_kernel(const __g
 // sample and the density lookup are shared code for primary and shadow lanes.  Random numbers are
 // drawn in exactly the order of the recursive trackers (vpt_trackers.cuh), so every path is the same
 // path.  Path ids come from a global counter in warp batches of 64 (one atomic per 64 paths).
-enum : int { kModePrimary = 0, kModeShadow = 1 };
+enum : int { kModePrimary = 0, kModeShadow = 1, kModeShadowEss = 2 };
+
+// Block walk of shadow_transmittance_ess (NeeTransmittance.glsl:173-228): the block of the entry
+// point, and the next block from the exit point (the axis of the largest offset from the block centre).
+VPT_DEV void ess_first_block(const TraceParams& P, F3 x, int& bx, int& by, int& bz) {
+    const F3 delta = P.box_max - P.box_min;
+    const F3 sp = (((x - P.box_min) / delta) * f3((float)P.nx, (float)P.ny, (float)P.nz)) /
+                  f3((float)P.sv_size, (float)P.sv_size, (float)P.sv_size);
+    bx = (int)floorf(sp.x);
+    by = (int)floorf(sp.y);
+    bz = (int)floorf(sp.z);
+}
+
+VPT_DEV void ess_next_block(const TraceParams& P, F3 x, F3 w, int& bx, int& by, int& bz) {
+    const F3 smin = P.box_min + f3((float)bx, (float)by, (float)bz) * P.sv_world;
+    const F3 smax = smin + P.sv_world;
+    const F3 center = (smin + smax) * 0.5f;
+    F3 mov = (x + w * 0.00001f) - center;
+    const float sx = signf(mov.x), sy = signf(mov.y), sz = signf(mov.z);
+    mov = f3(mov.x * sx, mov.y * sy, mov.z * sz);
+    const int dx = (mov.x >= mov.y && mov.x >= mov.z) ? 1 : 0;
+    const int dy = (mov.y >= mov.x && mov.y >= mov.z) ? 1 : 0;
+    const int dz = (mov.z >= mov.x && mov.z >= mov.y) ? 1 : 0;
+    bx += dx * (int)sx;
+    by += dy * (int)sy;
+    bz += dz * (int)sz;
+}
 constexpr int kRefillBatch = 64;
 
 template <int TRACKER>
@@ -395,6 +427,9 @@ VPT_DEV void flush_counters_to(unsigned long long* counters, int* error_flags, u
 template <int TRACKER, int INTERP, int GRID, bool TF, class SRC>
 VPT_DEV void refill_loop(const SRC& src, uint64_t total, unsigned long long* work_counter,
                          unsigned long long* counters, int* error_flags) {
+    // next event tracking; kNextEvent + 100: its sky shadow rays skip the occupancy grid's empty blocks
+    constexpr bool kNee = TRACKER == kNextEvent || TRACKER == kNextEvent + 100;
+    constexpr bool kEss = TRACKER == kNextEvent + 100;
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const unsigned lt_mask = (1u << lane) - 1u;
@@ -417,6 +452,13 @@ VPT_DEV void refill_loop(const SRC& src, uint64_t total, unsigned long long* wor
     float iso_last = 0.0f;
     bool iso_first = true;
     int iso_it = 0;
+    // empty-space-skipping shadow ray (kEss), the walk of shadow_transmittance_ess one step per
+    // iteration: current block, the block whose occupancy `empty` holds, inside an occupied block or
+    // at a block boundary, distance sampled so far from the block entry x0, the block's length
+    int bx = 0, by = 0, bz = 0, ox = 0, oy = 0, oz = 0;
+    bool empty = false, in_block = false;
+    float bt = 0.0f, bd = 0.0f;
+    F3 bx0 = zero;
     int scene = 0;
     uint32_t steps = 0;
     size_t pix = 0;
@@ -503,12 +545,56 @@ VPT_DEV void refill_loop(const SRC& src, uint64_t total, unsigned long long* wor
         }
         if (++steps > P.max_steps) {
             guard_hit = true;
-            refill_finish<TRACKER>(P, pix, TRACKER == kNextEvent ? color : zero, has);
+            refill_finish<TRACKER>(P, pix, kNee ? color : zero, has);
             continue;
+        }
+        if constexpr (kEss) {
+            if (mode == kModeShadowEss) {
+                if (!in_block) {  // at a block boundary (or the entry point)
+                    if (bx < 0 || by < 0 || bz < 0 || bx >= P.svx || by >= P.svy || bz >= P.svz) {
+                        end_shadow(P, color, x, w, d, xp, nw, dp, weight, ts, light, mode);
+                        continue;
+                    }
+                    const F3 smin = P.box_min + f3((float)bx, (float)by, (float)bz) * P.sv_world;
+                    const F3 smax = smin + P.sv_world;
+                    float tmin_sv = 0.0f, tmax_sv = 0.0f;
+                    ray_box(smin, smax, x, w, tmin_sv, tmax_sv);
+                    bd = tmax_sv - tmin_sv;
+                    x = x + w * tmin_sv;
+                    if (ox != bx || oy != by || oz != bz) {
+                        empty = __ldg(P.occupancy + ((size_t)bz * P.svy + by) * P.svx + bx) == 0;
+                        ox = bx;
+                        oy = by;
+                        oz = bz;
+                    }
+                    if (empty) {
+                        x = x + w * bd;
+                        ess_next_block(P, x, w, bx, by, bz);
+                    } else {
+                        bx0 = x;
+                        bt = 0.0f;
+                        in_block = true;
+                    }
+                    continue;
+                }
+                bt -= m_log(fmaxf(0.0000000001f, 1.0f - rng_next(rng))) * P.inv_extinction;
+                if (bt >= bd) {
+                    x = (P.ess_ref_compat ? x : bx0) + w * bd;
+                    in_block = false;
+                    ess_next_block(P, x, w, bx, by, bz);
+                    continue;
+                }
+                const F3 xn = (P.ess_ref_compat ? x : bx0) + w * bt;
+                const float dens = sample(xn, rng);
+                lookups++;
+                x = xn;
+                ts *= 1.0f - dens;
+                continue;
+            }
         }
         const float t = free_path(rng, P.inv_extinction);
         bool escape = t > d;
-        if (TRACKER == kNextEvent && mode == kModeShadow && light >= 0) {
+        if (kNee && mode == kModeShadow && light >= 0) {
             shadow_dist += t;
             escape = escape || shadow_dist > shadow_max;
         }
@@ -527,7 +613,7 @@ VPT_DEV void refill_loop(const SRC& src, uint64_t total, unsigned long long* wor
             }
             x = xn;
         }
-        if (TRACKER == kNextEvent && mode == kModeShadow) {
+        if (kNee && mode == kModeShadow) {
             if (!escape) {
                 ts *= 1.0f - density;
                 d -= t;
@@ -538,7 +624,7 @@ VPT_DEV void refill_loop(const SRC& src, uint64_t total, unsigned long long* wor
         }
         if (escape) {
             F3 L;
-            if (TRACKER == kNextEvent) L = ev ? color : color + sky_and_sun(P, w);
+            if (kNee) L = ev ? color : color + sky_and_sun(P, w);
             else if (TRACKER == kRatio) L = sky_and_sun(P, w) * trans;
             else if (TRACKER == kDeltaIso) L = iw * sky_and_sun(P, w);
             else L = sky_and_sun(P, w);
@@ -549,7 +635,7 @@ VPT_DEV void refill_loop(const SRC& src, uint64_t total, unsigned long long* wor
         if (TRACKER != kRatio && xi < P.absorb_albedo * density) {
             // USE_EMISSION (NextEventTracking.glsl:296-301): the absorbed NEE path ends with the emission
             F3 L = zero;
-            if (TRACKER == kNextEvent) {
+            if (kNee) {
                 L = P.emission ? color + sample.emission(x, rng) : (P.tf ? color + sample.tf_emission() : color);
             } else if (P.tf) {  // delta tracking (DeltaTracking.glsl:293-301)
                 L = sample.tf_emission();
@@ -559,11 +645,11 @@ VPT_DEV void refill_loop(const SRC& src, uint64_t total, unsigned long long* wor
         }
         if (xi < density) {
             if (P.max_bounces > 0 && ++bounces > P.max_bounces) {
-                refill_finish<TRACKER>(P, pix, TRACKER == kNextEvent ? color : zero, has);
+                refill_finish<TRACKER>(P, pix, kNee ? color : zero, has);
                 continue;
             }
             float tmin, tmax;
-            if (TRACKER == kNextEvent) {
+            if (kNee) {
                 nw = sample_phase(rng, P.g, w);
                 ev = true;
                 bool to_light = false;
@@ -586,6 +672,24 @@ VPT_DEV void refill_loop(const SRC& src, uint64_t total, unsigned long long* wor
                 w = dir;
                 ts = 1.0f;
                 mode = kModeShadow;
+                if (kEss && !to_light) {
+                    // shadow_transmittance_ess: entry through the box shrunk by 1e-6, the entry block is
+                    // walked as occupied
+                    const F3 eps = f3(1e-6f, 1e-6f, 1e-6f);
+                    if (ray_box(P.box_min + eps, P.box_max - eps, x, w, tmin, tmax)) {
+                        x = x + w * tmin;
+                        ess_first_block(P, x, bx, by, bz);
+                        ox = bx;
+                        oy = by;
+                        oz = bz;
+                        empty = false;
+                        in_block = false;
+                        mode = kModeShadowEss;
+                    } else {
+                        end_shadow(P, color, x, w, d, xp, nw, dp, weight, ts, light, mode);
+                    }
+                    continue;
+                }
                 if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
                     x = x + w * tmin;
                     d = tmax - tmin;
@@ -685,7 +789,8 @@ template <int TRACKER, int INTERP, int GRID, bool TF>
 static cudaError_t launch_trace_t(const TraceParams& P, int schedule, int features, int persistent_blocks,
                                   cudaStream_t stream) {
     uint64_t total = padded_paths(P.width, P.height, P.num_frames);
-    constexpr bool kRefillable = TRACKER == kDelta || TRACKER == kRatio || TRACKER == kNextEvent || TRACKER == kDeltaIso;
+    constexpr bool kRefillable = TRACKER == kDelta || TRACKER == kRatio || TRACKER == kNextEvent ||
+                                 TRACKER == kNextEvent + 100 || TRACKER == kDeltaIso;
     if (schedule == kScheduleRefill && kRefillable && !features) {
         if constexpr (kRefillable) {
             int blocks = refill_blocks<TRACKER, INTERP, GRID, TF>(persistent_blocks);

@@ -4,7 +4,9 @@
 namespace vpt {
 
 cudaError_t launch_trace_batch(const BatchLaunch& b, cudaStream_t s) {
-    return b.grid_kind == kNanoVdb ? batch_tracker<kNanoVdb>(b, s) : batch_tracker<kDense>(b, s);
+    if (b.grid_kind == kNanoVdb) return batch_tracker<kNanoVdb>(b, s);
+    if (b.grid_kind == kDenseTex) return batch_tracker<kDenseTex>(b, s);  // every scene has a texture object
+    return batch_tracker<kDense>(b, s);
 }
 
 }  // namespace vpt

@@ -753,8 +753,8 @@ def set_use_feature_maps(feature_map_names: List[str]) -> None:
     _apply_feature_maps()
 
 
-_FEATURE_CHANNELS = {1: 4, 2: 4, 3: 4, 4: 4, 5: 4, 6: 2, 7: 1, 8: 2, 9: 2, 12: 2, 13: 4, 14: 2, 15: 4, 16: 4, 17: 4,
-                     FEATURE_TRANSMITTANCE: 1}
+_FEATURE_CHANNELS = {1: 4, 2: 4, 3: 4, 4: 4, 5: 4, 6: 2, 7: 1, 8: 2, 9: 2, 10: 2, 11: 1, 12: 2, 13: 4, 14: 2, 15: 4,
+                     16: 4, 17: 4, FEATURE_TRANSMITTANCE: 1}
 
 
 def get_feature_map(input_tensor: torch.Tensor, feature_map: int) -> torch.Tensor:

@@ -80,6 +80,9 @@ enum {
     VPT_FEATURE_DEPTH_FAR = 7,     /* mean of (event ? depth : far distance) */
     VPT_FEATURE_FLOW = 8,          /* (pixel - previous pixel of the first event, 0, 0), last frame */
     VPT_FEATURE_FLOW_REVERSE = 9,  /* (previous pixel of the first event or camera direction - pixel), last frame */
+    VPT_FEATURE_DEPTH_NABLA = 10,  /* running mean over frames of (A / sqrt(1 - A^2), B / sqrt(1 - B^2)), (A, B) the
+                                      view-space x, y of that frame's running-mean normal (0 without an event) */
+    VPT_FEATURE_DEPTH_FWIDTH = 11, /* running mean of |nabla.x| + |nabla.y| (all channels) */
     VPT_FEATURE_DENSITY = 12,
     VPT_FEATURE_BACKGROUND = 13,
     VPT_FEATURE_REPROJ_UV = 14,    /* previous-view uv of the most recent first event, (-1, -1) before one */

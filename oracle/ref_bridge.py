@@ -96,7 +96,8 @@ class Scene:
 
     @staticmethod
     def last_frame_feature(which: int, height: int, width: int) -> np.ndarray:
-        """The last render's firstW (0), flowImage (1), flowReverseImage (2) or reprojUVImage (3), H x W x 4."""
+        """The last render's firstW (0), flowImage (1), flowReverseImage (2), reprojUVImage (3), normalImage
+        (4), depthNablaImage (5) or depthFwidthImage (6), H x W x 4."""
         out = np.empty((height, width, 4), np.float32)
         if load().ref_read_last_frame_feature(which, out.ctypes.data_as(c_void_p)) != 0:
             raise RuntimeError("ref_read_last_frame_feature failed")

@@ -69,6 +69,8 @@ SPECTRAL = {"sdt": "USE_SPECTRAL_DELTA_TRACKING", "nees": "USE_NEXT_EVENT_TRACKI
 DEPTH_MAPS = ["WRITE_DEPTH_BLENDED_MAP", "WRITE_DEPTH_NEAREST_OPAQUE_MAP"]
 # the maps overwritten every frame (Clouds.glsl:239-246, 286-343)
 LAST_FRAME_MAPS = ["WRITE_FIRST_W_MAP", "WRITE_FLOW_MAP", "WRITE_FLOW_REVERSE_MAP", "WRITE_REPROJ_UV_MAP"]
+# the normal map's running mean and the depth derivative maps computed from it (Clouds.glsl:258-297, 344-364)
+DEPTH_DERIV_MAPS = ["WRITE_NORMAL_MAP", "WRITE_DEPTH_NABLA_MAP", "WRITE_DEPTH_FWIDTH_MAP"]
 ISO = ["USE_ISOSURFACES", "NUM_ISOSURFACE_SUBDIVISIONS=2", "SURFACE_BRDF_LAMBERTIAN", "ISOSURFACE_TYPE_DENSITY"]
 
 
@@ -92,6 +94,8 @@ def variants():
     for t in ("delta", "nee"):
         out.append((f"lastframe_{t}__stochastic__default__linear", TRACKERS[t] + [INTERPS["stochastic"]]
                     + ENVS["default__linear"] + LAST_FRAME_MAPS, 0))
+        out.append((f"depthderiv_{t}__stochastic__default__linear", TRACKERS[t] + [INTERPS["stochastic"]]
+                    + ENVS["default__linear"] + DEPTH_DERIV_MAPS, 0))
     # emission grid (USE_EMISSION) with next event tracking, grey and spectral
     for i in ("stochastic", "trilinear"):
         out.append((f"nee_emission__{i}__default__linear", TRACKERS["nee"] + [INTERPS[i]] + ENVS["default__linear"]

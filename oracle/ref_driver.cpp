@@ -32,6 +32,9 @@ static image2D& firstW = g_ref.firstw;
 static image2D& flowImage = g_ref.flow;
 static image2D& flowReverseImage = g_ref.flowrev;
 static image2D& reprojUVImage = g_ref.reproj;
+static image2D& normalImage = g_ref.normal;
+static image2D& depthNablaImage = g_ref.dnabla;
+static image2D& depthFwidthImage = g_ref.dfwidth;
 static Light* const lights = g_ref.lights;
 #define gl_GlobalInvocationID gl_global_invocation_id
 #define main glsl_main
@@ -51,7 +54,7 @@ RefState g_ref;
 thread_local uvec3 gl_global_invocation_id;
 uint ref_seed_offset = 0;
 static std::vector<float> g_dblend, g_dnear;  // the depth feature images of the last ref_render
-static std::vector<float> g_last[4];          // firstW, flow, flow reverse, reprojected uv images
+static std::vector<float> g_last[7];  // firstW, flow, flow reverse, reprojected uv, normal, depth nabla, fwidth
 }  // namespace glslref
 
 using namespace glslref;
@@ -136,6 +139,10 @@ int ref_render(int variant, const RefScene* s, float* out_rgba, int threads) {
     for (int c = 0; c < 4; c++)
         p.inverseViewMatrix.c[c] = vec4(s->inv_view[c * 4 + 0], s->inv_view[c * 4 + 1], s->inv_view[c * 4 + 2],
                                         s->inv_view[c * 4 + 3]);
+    // inverseTransposedViewMatrix = transpose(inverse(view)) (VolumetricPathTracingPass.cpp)
+    for (int c = 0; c < 4; c++)
+        p.inverseTransposedViewMatrix.c[c] = vec4(s->inv_view[0 * 4 + c], s->inv_view[1 * 4 + c],
+                                                  s->inv_view[2 * 4 + c], s->inv_view[3 * 4 + c]);
     // envMapDirRot and its transpose invEnvMapDirRot (VolumetricPathTracingPass.cpp:2108-2113)
     for (int c = 0; c < 3; c++) {
         p.envMapDirRot.c[c] = vec3(s->env_rot[c * 3 + 0], s->env_rot[c * 3 + 1], s->env_rot[c * 3 + 2]);
@@ -221,8 +228,9 @@ int ref_render(int variant, const RefScene* s, float* out_rgba, int threads) {
     g_ref.dnear.data = g_dnear.data();
     g_ref.dnear.w = s->width;
     g_ref.dnear.h = s->height;
-    image2D* last[4] = {&g_ref.firstw, &g_ref.flow, &g_ref.flowrev, &g_ref.reproj};
-    for (int k = 0; k < 4; k++) {
+    image2D* last[7] = {&g_ref.firstw, &g_ref.flow, &g_ref.flowrev, &g_ref.reproj,
+                        &g_ref.normal, &g_ref.dnabla, &g_ref.dfwidth};
+    for (int k = 0; k < 7; k++) {
         g_last[k].assign((size_t)s->width * s->height * 4, 0.0f);
         last[k]->data = g_last[k].data();
         last[k]->w = s->width;
@@ -250,11 +258,12 @@ int ref_render(int variant, const RefScene* s, float* out_rgba, int threads) {
     return 0;
 }
 
-// The images the last frame of the last ref_render wrote (which: 0 firstW, 1 flowImage, 2
-// flowReverseImage, 3 reprojUVImage; W*H*4), for the variants with WRITE_FIRST_W_MAP,
-// WRITE_FLOW_MAP, WRITE_FLOW_REVERSE_MAP and WRITE_REPROJ_UV_MAP.
+// The images of the last ref_render (which: 0 firstW, 1 flowImage, 2 flowReverseImage, 3
+// reprojUVImage, 4 normalImage, 5 depthNablaImage, 6 depthFwidthImage; W*H*4), for the variants with
+// WRITE_FIRST_W_MAP, WRITE_FLOW_MAP, WRITE_FLOW_REVERSE_MAP, WRITE_REPROJ_UV_MAP, WRITE_NORMAL_MAP,
+// WRITE_DEPTH_NABLA_MAP and WRITE_DEPTH_FWIDTH_MAP.
 int ref_read_last_frame_feature(int which, float* out_rgba) {
-    if (!out_rgba || which < 0 || which > 3 || g_last[which].empty()) return 1;
+    if (!out_rgba || which < 0 || which > 6 || g_last[which].empty()) return 1;
     memcpy(out_rgba, g_last[which].data(), g_last[which].size() * sizeof(float));
     return 0;
 }

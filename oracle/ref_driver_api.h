@@ -17,6 +17,7 @@ struct RefState {
     image2D result, acc;  // resultImage, accImage
     image2D dblend, dnear;  // depthBlendedImage, depthNearestOpaqueImage (WRITE_DEPTH_*_MAP variants)
     image2D firstw, flow, flowrev, reproj;  // firstW, flowImage, flowReverseImage, reprojUVImage
+    image2D normal, dnabla, dfwidth;        // normalImage, depthNablaImage, depthFwidthImage
     Light lights[16];     // LightsBuffer
 };
 extern RefState g_ref;

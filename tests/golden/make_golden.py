@@ -8,7 +8,8 @@ the path radiance itself) and the reference's fp32 running mean after 8 frames.
 With the argument ``depth_maps`` it writes tests/golden/ref_depth_maps.npz instead: the reference's
 Depth Blended and Depth Nearest Opaque images (Clouds.glsl:367-383) after 4 frames; with
 ``last_frame_maps``, tests/golden/ref_last_frame_maps.npz: the First W, Flow, Flow Reverse and
-Reprojected UV images, which hold the last frame's values, after 4 frames.
+Reprojected UV images, which hold the last frame's values, after 4 frames; with ``depth_deriv_maps``,
+tests/golden/ref_depth_deriv_maps.npz: the Normal, Depth (nabla) and Depth (fwidth) images after 4 frames.
 
 Run in a container that has the reference tree:  python tests/golden/make_golden.py [depth_maps]
 """
@@ -214,6 +215,36 @@ def main_last_frame_maps():
     print("wrote", out, os.path.getsize(out), "bytes")
 
 
+DERIV_FRAMES = 4
+
+
+def main_depth_deriv_maps():
+    """tests/golden/ref_depth_deriv_maps.npz: the reference's normalImage, depthNablaImage and
+    depthFwidthImage (H x W x 4) after DERIV_FRAMES frames (the last-frame scenes, current camera)."""
+    from oracle import ref_bridge
+
+    data, meta = {}, {}
+    for name, (sp, _) in last_frame_cases().items():
+        name = name.replace("lastframe", "depthderiv")
+        inv = camera_inv_view_proj(sp)
+        sc, _ = reference_scene(sp, DERIV_FRAMES, inv=inv)
+        variant = f"depthderiv_{sp.mode}__stochastic__default__linear"
+        sc.render(variant)
+        for k, key in ((4, "normal"), (5, "nabla"), (6, "fwidth")):
+            data[f"{name}__{key}"] = ref_bridge.Scene.last_frame_feature(k, sp.height, sp.width)
+        data[name + "__grid"] = np.ascontiguousarray(sp.grid, np.float32)
+        data[name + "__inv_view_proj"] = np.array(inv, np.float32)
+        meta[name] = {"variant": variant, "frames": DERIV_FRAMES,
+                      **{f: (list(getattr(sp, f)) if isinstance(getattr(sp, f), tuple) else getattr(sp, f))
+                         for f in FIELDS}}
+        nab = data[name + "__nabla"]
+        print(name, variant, "nan fraction", float(np.isnan(nab[..., 0]).mean()),
+              "mean |nabla|", float(np.nanmean(np.abs(nab[..., :2]))))
+    out = os.path.join(os.path.dirname(os.path.abspath(__file__)), "ref_depth_deriv_maps.npz")
+    np.savez_compressed(out, meta=json.dumps(meta), **data)
+    print("wrote", out, os.path.getsize(out), "bytes")
+
+
 def main():
     ref_build.build()
     data = {}
@@ -256,5 +287,9 @@ if __name__ == "__main__":
     if len(sys.argv) > 1 and sys.argv[1] == "last_frame_maps":
         ref_build.build()
         main_last_frame_maps()
+        sys.exit(0)
+    if len(sys.argv) > 1 and sys.argv[1] == "depth_deriv_maps":
+        ref_build.build()
+        main_depth_deriv_maps()
         sys.exit(0)
     main()

@@ -170,6 +170,37 @@ def test_eaw_matches_oracle(core, quirk):
     assert np.allclose(out.cpu().numpy(), ref, rtol=1e-5, atol=1e-6)
 
 
+def test_density_texture_follows_a_new_grid_and_a_nonzero_border(core_dr):
+    """The texture array is kept for grids of the same size and refilled for each new grid: a second
+    grid rendered on the same context gives the film of a fresh context (the first grid's texels are
+    gone).  A grid whose minimum is above 0 has a non-zero border density, which the texture's border
+    colour cannot represent: it is read by global loads, with the same film as with the option off."""
+    core = core_dr
+    a = fbm_scene(width=32, height=32, mode="delta")
+    b = fbm_scene(width=32, height=32, mode="delta", grid=bridge.fbm(48, 9, base_frequency=2.0, contrast=6.0))
+    setup_core(core, a)
+    gpu_render(core, a, 2, stats=False)
+    setup_core(core, b)  # same 48^3 size: the array is reused
+    s_reused, _ = gpu_render(core, b, 2, stats=False)
+    fresh = Core(0, "dr")
+    try:
+        setup_core(fresh, b)
+        s_fresh, _ = gpu_render(fresh, b, 2, stats=False)
+    finally:
+        fresh.close()
+    assert np.allclose(s_reused, s_fresh, rtol=1e-12, atol=1e-12)
+    # minimum 0.25 everywhere: border density (0 - 0.25) / 0.75 != 0
+    g = (0.25 + 0.75 * np.asarray(b.grid, np.float32)).astype(np.float32)
+    c = fbm_scene(width=32, height=32, mode="delta", grid=g)
+    setup_core(core, c)
+    films = []
+    for tex in (1.0, 0.0):
+        core("vpt_set_option", b"density_texture", tex)
+        films.append(gpu_render(core, c, 2, stats=False)[0])
+    core("vpt_set_option", b"density_texture", 1.0)
+    assert np.allclose(films[0], films[1], rtol=1e-12, atol=1e-12)
+
+
 @pytest.mark.parametrize("size", [(64, 48), (37, 50), (300, 200)])
 def test_eaw_lattice_tiles_equal_direct_taps(core, size):
     """The shared-memory EAW pass (taps of 16 x 16 pixels of one residue class staged per block) gives
@@ -347,7 +378,8 @@ def test_iteration_guard_reports_error_without_hanging(core):
     core("vpt_synchronize", None)
 
 
-@pytest.mark.parametrize("mode", ["delta", "ratio", "nee", "nee_lights", "delta_isosurfaces"])
+@pytest.mark.parametrize("mode", ["delta", "ratio", "nee", "nee_lights", "delta_isosurfaces", "nee_ess",
+                                  "nee_ess_ref_compat"])
 def test_schedules_trace_identical_paths(core_dr, mode):
     """Tile, persistent-batch and per-lane-refill schedules trace the same paths (same film up to the
     order of the FP64 atomic additions).  The isosurface case covers the refill loop's own surface
@@ -359,16 +391,20 @@ def test_schedules_trace_identical_paths(core_dr, mode):
         kw = PATH_CASES["nee_lights"]
     elif mode == "delta_isosurfaces":
         kw = dict(mode="delta", interp="trilinear", iso=True, iso_value=0.3)
+    elif mode.startswith("nee_ess"):  # sky shadow rays skip empty occupancy blocks (the refill loop's own walk)
+        kw = dict(mode="nee", use_ess=True, ess_ref_compat=mode.endswith("compat"))
     else:
         kw = dict(mode=mode)
     sp = fbm_scene(width=40, height=40, **kw)
     setup_core(core, sp)
+    core("vpt_set_option", b"ess_ref_compat", 1.0 if sp.ess_ref_compat else 0.0)
     films = []
     for sched in (0, 1, 2):
         core("vpt_set_option", b"schedule", float(sched))
         s, _ = gpu_render(core, sp, 3, stats=False)
         films.append(s)
     core("vpt_set_option", b"schedule", 2.0)
+    core("vpt_set_option", b"ess_ref_compat", 0.0)
     for f in films[1:]:
         assert np.allclose(films[0], f, rtol=1e-12, atol=1e-12)
 
