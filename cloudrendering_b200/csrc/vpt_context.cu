@@ -235,7 +235,7 @@ struct VptContext {
     bool features_on = false;
     bool feat_background = false;  // the Background map was requested (one more accumulator per sample)
     int feat_depth_maps = 0;       // bit 0: Depth Blended, bit 1: Depth Nearest Opaque requested (ray marches)
-    bool feat_depth_deriv = false; // Depth (nabla) or Depth (fwidth) requested (per-frame normals replayed)
+    int feat_depth_deriv = 0;      // bit 0: Depth (nabla), bit 1: Depth (fwidth) requested (normals replayed)
     DevBuf<float> frame_normals;   //   4 floats per pixel and frame of one feature launch
     DevBuf<float> feat;
     DevBuf<float> rgba_src, rgba_a, rgba_b;  // denoiser input and ping-pong buffers
@@ -1639,7 +1639,7 @@ VptStatus vpt_render_frames(VptContext* ctx, int frames, void* stream) {
             Pf.frame_normals = ctx->frame_normals.ptr;
             VPT_CHECK_CUDA(ctx, vpt::launch_trace(Pf, tracker, ctx->use_ess, ctx->schedule, 1, pb, s));
             VPT_CHECK_CUDA(ctx, vpt::launch_depth_deriv(ctx->frame_normals.ptr, k, (int)npix, film0 + (uint32_t)done,
-                                                        itv, ctx->feat.ptr, s));
+                                                        itv, ctx->feat_depth_deriv & 1, ctx->feat.ptr, s));
         }
     }
     if (plain_n > 0) {
@@ -1745,14 +1745,16 @@ VptStatus vpt_read_statistics(VptContext* ctx, double* out_sum, double* out_sum_
 
 VptStatus vpt_set_use_feature_maps(VptContext* ctx, const int* features, int count) {
     VPT_CHECK_CTX(ctx);
-    bool on = false, background = false, deriv = false;
+    bool on = false, background = false;
+    int deriv = 0;
     int depth_maps = 0;
     for (int i = 0; i < count; i++) {
         if (features && features[i] != VPT_FEATURE_RESULT) on = true;
         if (features && features[i] == VPT_FEATURE_BACKGROUND) background = true;
         if (features && features[i] == VPT_FEATURE_DEPTH_BLENDED) depth_maps |= 1;
         if (features && features[i] == VPT_FEATURE_DEPTH_NEAREST_OPAQUE) depth_maps |= 2;
-        if (features && (features[i] == VPT_FEATURE_DEPTH_NABLA || features[i] == VPT_FEATURE_DEPTH_FWIDTH)) deriv = true;
+        if (features && features[i] == VPT_FEATURE_DEPTH_NABLA) deriv |= 1;
+        if (features && features[i] == VPT_FEATURE_DEPTH_FWIDTH) deriv |= 2;
     }
     if (on != ctx->features_on || background != ctx->feat_background || depth_maps != ctx->feat_depth_maps ||
         deriv != ctx->feat_depth_deriv)
@@ -1775,7 +1777,8 @@ VptStatus vpt_get_feature_map(VptContext* ctx, int feature, float* out, int chan
         return fail(ctx, VPT_ERR_STATE, "the Background map was not requested in set_use_feature_maps");
     if ((feature == VPT_FEATURE_DEPTH_BLENDED && !(ctx->feat_depth_maps & 1)) ||
         (feature == VPT_FEATURE_DEPTH_NEAREST_OPAQUE && !(ctx->feat_depth_maps & 2)) ||
-        ((feature == VPT_FEATURE_DEPTH_NABLA || feature == VPT_FEATURE_DEPTH_FWIDTH) && !ctx->feat_depth_deriv))
+        (feature == VPT_FEATURE_DEPTH_NABLA && !(ctx->feat_depth_deriv & 1)) ||
+        (feature == VPT_FEATURE_DEPTH_FWIDTH && !(ctx->feat_depth_deriv & 2)))
         return fail(ctx, VPT_ERR_STATE, "the depth map was not requested in set_use_feature_maps");
     cudaStream_t s = as_stream(stream);
     int n = ctx->width * ctx->height;

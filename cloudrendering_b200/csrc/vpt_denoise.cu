@@ -618,7 +618,7 @@ cudaError_t svgf_filter_passes(SvgfCur c, float4* color_history, float4* moments
 // here, so the trace stores each frame's normal and this kernel replays the frames in order per pixel.
 
 __global__ void depth_deriv_kernel(const float4* __restrict__ frame_normals, int frames, int n, uint32_t f0, Mat4 M,
-                                   float* __restrict__ feat) {
+                                   int nabla_map, float* __restrict__ feat) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     float* f = feat + (size_t)i * kFeatStride;
@@ -654,16 +654,17 @@ __global__ void depth_deriv_kernel(const float4* __restrict__ frame_normals, int
             ny = frame == 0u ? 0.0f : ny * s;
             nz = frame == 0u ? 0.0f : nz * s;
         }
-        const float fv = fabsf(bx) + fabsf(by);
         if (frame != 0u) {
             ax = ax * (1.0f - t) + bx * t;
             ay = ay * (1.0f - t) + by * t;
-            fw = fw * (1.0f - t) + fv * t;
         } else {
             ax = bx;
             ay = by;
-            fw = fv;
         }
+        // with the nabla map written, the shader's `nabla` already holds its running mean when the
+        // fwidth block reads it (Clouds.glsl:344-357); without it, this frame's nabla
+        const float fv = nabla_map ? fabsf(ax) + fabsf(ay) : fabsf(bx) + fabsf(by);
+        fw = frame != 0u ? fw * (1.0f - t) + fv * t : fv;
     }
     f[kFeatDerivNormal + 0] = nx;
     f[kFeatDerivNormal + 1] = ny;
@@ -674,11 +675,11 @@ __global__ void depth_deriv_kernel(const float4* __restrict__ frame_normals, int
 }
 
 cudaError_t launch_depth_deriv(const float* frame_normals, int frames, int n, uint32_t f0,
-                               const float inv_transposed_view[16], float* feat, cudaStream_t s) {
+                               const float inv_transposed_view[16], int nabla_map, float* feat, cudaStream_t s) {
     Mat4 M;
     for (int k = 0; k < 16; k++) M.m[k] = inv_transposed_view[k];
     depth_deriv_kernel<<<(n + 255) / 256, 256, 0, s>>>(reinterpret_cast<const float4*>(frame_normals), frames, n, f0,
-                                                       M, feat);
+                                                       M, nabla_map, feat);
     count_launches(1);
     return cudaGetLastError();
 }

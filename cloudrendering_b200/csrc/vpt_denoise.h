@@ -75,9 +75,10 @@ cudaError_t denoiser_features(const float* feat, int n, uint32_t frames, const f
                               float* normal, float* depth, float* trans, cudaStream_t stream);
 // Depth (nabla) / Depth (fwidth): advances each pixel's running-mean normal, nabla and fwidth over the
 // `frames` frames of one feature launch (per-frame normals from the trace, frame-major float4), the
-// first of which is accumulation frame f0; inv_transposed_view is column-major 4 x 4.
+// first of which is accumulation frame f0; inv_transposed_view is column-major 4 x 4; nabla_map: the
+// Depth (nabla) map is requested (the fwidth map then follows the running-mean nabla, as in the shader).
 cudaError_t launch_depth_deriv(const float* frame_normals, int frames, int n, uint32_t f0,
-                               const float inv_transposed_view[16], float* feat, cudaStream_t s);
+                               const float inv_transposed_view[16], int nabla_map, float* feat, cudaStream_t s);
 cudaError_t feature_to_chw(const float* feat, int n, uint32_t frames, int feature, int channels, const float* albedo,
                            float far_distance, float* out, cudaStream_t stream);
 

@@ -208,11 +208,19 @@ VPT_DEV bool decode_path(const TraceParams& P, uint64_t p, uint32_t& frame, int&
     const uint32_t tiles_x = (uint32_t)(P.width + 15) >> 4;
     const uint32_t tiles_y = (uint32_t)(P.height + 15) >> 4;
     const uint64_t per_frame = (uint64_t)tiles_x * tiles_y * 256u;
-    frame = (uint32_t)(p / per_frame);
-    uint32_t q = (uint32_t)(p - (uint64_t)frame * per_frame);
-    uint32_t tile = q >> 8, within = q & 255u;
-    x = (int)((tile % tiles_x) * 16u + (within & 15u));
-    y = (int)((tile / tiles_x) * 16u + (within >> 4));
+    uint32_t q;
+    if ((p | per_frame) < 0x100000000ull) {  // 32-bit division (a 64-bit one is a long software routine)
+        const uint32_t p32 = (uint32_t)p, pf = (uint32_t)per_frame;
+        frame = p32 / pf;
+        q = p32 - frame * pf;
+    } else {
+        frame = (uint32_t)(p / per_frame);
+        q = (uint32_t)(p - (uint64_t)frame * per_frame);
+    }
+    const uint32_t tile = q >> 8, within = q & 255u;
+    const uint32_t ty = tile / tiles_x, tx = tile - ty * tiles_x;
+    x = (int)(tx * 16u + (within & 15u));
+    y = (int)(ty * 16u + (within >> 4));
     return frame < P.num_frames && x < P.width && y < P.height;
 }
 

@@ -96,6 +96,9 @@ def variants():
                     + ENVS["default__linear"] + LAST_FRAME_MAPS, 0))
         out.append((f"depthderiv_{t}__stochastic__default__linear", TRACKERS[t] + [INTERPS["stochastic"]]
                     + ENVS["default__linear"] + DEPTH_DERIV_MAPS, 0))
+    # Depth (fwidth) without the nabla map: it then averages each frame's own nabla
+    out.append(("depthfwidth_delta__stochastic__default__linear", TRACKERS["delta"] + [INTERPS["stochastic"]]
+                + ENVS["default__linear"] + ["WRITE_NORMAL_MAP", "WRITE_DEPTH_FWIDTH_MAP"], 0))
     # emission grid (USE_EMISSION) with next event tracking, grey and spectral
     for i in ("stochastic", "trilinear"):
         out.append((f"nee_emission__{i}__default__linear", TRACKERS["nee"] + [INTERPS[i]] + ENVS["default__linear"]

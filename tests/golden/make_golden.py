@@ -232,6 +232,10 @@ def main_depth_deriv_maps():
         sc.render(variant)
         for k, key in ((4, "normal"), (5, "nabla"), (6, "fwidth")):
             data[f"{name}__{key}"] = ref_bridge.Scene.last_frame_feature(k, sp.height, sp.width)
+        if sp.mode == "delta":  # the fwidth map alone (Clouds.glsl:356-364 then reads this frame's nabla)
+            sc2, _ = reference_scene(sp, DERIV_FRAMES, inv=inv)
+            sc2.render("depthfwidth_delta__stochastic__default__linear")
+            data[f"{name}__fwidth_only"] = ref_bridge.Scene.last_frame_feature(6, sp.height, sp.width)
         data[name + "__grid"] = np.ascontiguousarray(sp.grid, np.float32)
         data[name + "__inv_view_proj"] = np.array(inv, np.float32)
         meta[name] = {"variant": variant, "frames": DERIV_FRAMES,
