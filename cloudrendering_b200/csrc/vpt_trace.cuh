@@ -467,6 +467,9 @@ VPT_DEV void refill_loop(const SRC& src, uint64_t total, unsigned long long* wor
     bool empty = false, in_block = false;
     float bt = 0.0f, bd = 0.0f;
     F3 bx0 = zero;
+    // decomposition tracking (the same block walk): the block's normalised min / max density, its
+    // control and residual extinctions and the control clock (bt is the residual clock)
+    float dc_min = 0.0f, dc_max = 0.0f, mu_c = 1.0f, mu_r = 1.0f, t_c = 0.0f;
     int scene = 0;
     uint32_t steps = 0;
     size_t pix = 0;
@@ -521,7 +524,20 @@ VPT_DEV void refill_loop(const SRC& src, uint64_t total, unsigned long long* wor
                     iso_it = 0;
                     float tmin, tmax;
                     has = true;
-                    if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
+                    if constexpr (TRACKER == kDecomposition) {
+                        // analogDecompositionTracking: entry through the box shrunk by 1e-6, then the
+                        // supervoxel walk (its first block's bounds are read)
+                        const F3 eps = f3(1e-6f, 1e-6f, 1e-6f);
+                        if (ray_box(P.box_min + eps, P.box_max - eps, x, w, tmin, tmax)) {
+                            x = x + w * tmin;
+                            ess_first_block(P, x, bx, by, bz);
+                            ox = oy = oz = -1;
+                            in_block = false;
+                        } else {
+                            F3 L = sky_and_sun(P, w);
+                            refill_finish<TRACKER>(P, pix, L, has);
+                        }
+                    } else if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
                         x = x + w * tmin;
                         d = tmax - tmin;
                     } else {
@@ -599,6 +615,78 @@ VPT_DEV void refill_loop(const SRC& src, uint64_t total, unsigned long long* wor
                 ts *= 1.0f - dens;
                 continue;
             }
+        }
+        if constexpr (TRACKER == kDecomposition) {
+            // the supervoxel walk of track_decomposition, one block boundary or one step of the two
+            // competing exponential clocks (control t_c, residual t_r) per iteration
+            if (!in_block) {
+                if (bx < 0 || by < 0 || bz < 0 || bx >= P.svx || by >= P.svy || bz >= P.svz) {
+                    refill_finish<TRACKER>(P, pix, sky_and_sun(P, w), has);
+                    continue;
+                }
+                const F3 smin = P.box_min + f3((float)bx, (float)by, (float)bz) * P.sv_world;
+                const F3 smax = smin + P.sv_world;
+                float tmin_sv = 0.0f, tmax_sv = 0.0f;
+                ray_box(smin, smax, x, w, tmin_sv, tmax_sv);
+                bd = tmax_sv - tmin_sv;
+                x = x + w * tmin_sv;
+                if (ox != bx || oy != by || oz != bz) {
+                    const float2 mm = __ldg(reinterpret_cast<const float2*>(P.sv_data) +
+                                            ((size_t)bz * P.svy + by) * P.svx + bx);
+                    dc_min = mm.x;
+                    dc_max = mm.y;
+                    ox = bx;
+                    oy = by;
+                    oz = bz;
+                }
+                if (dc_max < 1e-5f) {
+                    x = x + w * bd;
+                    sv_step(smin, smax, x, w, bx, by, bz);
+                } else {
+                    mu_c = fmaxf(0.0000000001f, P.extinction * dc_min);
+                    mu_r = fmaxf(0.0000000001f, P.extinction * dc_max - mu_c);
+                    t_c = -m_log(fmaxf(0.0000000001f, 1.0f - rng_next(rng))) / mu_c;
+                    bt = 0.0f;  // t_r
+                    in_block = true;
+                }
+                continue;
+            }
+            bt -= m_log(fmaxf(0.0000000001f, 1.0f - rng_next(rng))) / mu_r;
+            if (t_c >= bd && bt >= bd) {
+                x = x + w * bd;
+                in_block = false;
+                const F3 smin = P.box_min + f3((float)bx, (float)by, (float)bz) * P.sv_world;
+                sv_step(smin, smin + P.sv_world, x, w, bx, by, bz);
+                continue;
+            }
+            const F3 xs = x + w * fminf(t_c, bt);
+            bool collision;
+            if (t_c <= bt) {
+                collision = true;
+            } else {
+                const float dens = sample(xs, rng);
+                lookups++;
+                collision = rng_next(rng) * mu_r < P.extinction * dens - mu_c;
+            }
+            if (collision) {
+                x = xs;
+                if (rng_next(rng) < P.absorb_albedo) {
+                    refill_finish<TRACKER>(P, pix, zero, has);
+                    continue;
+                }
+                if (P.max_bounces > 0 && ++bounces > P.max_bounces) {
+                    refill_finish<TRACKER>(P, pix, zero, has);
+                    continue;
+                }
+                w = sample_phase(rng, P.g, w);
+                bt = 0.0f;
+                t_c = -m_log(fmaxf(0.0000000001f, 1.0f - rng_next(rng))) / mu_c;
+                const F3 smin = P.box_min + f3((float)bx, (float)by, (float)bz) * P.sv_world;
+                float tmin_sv = 0.0f, tmax_sv = 0.0f;
+                ray_box(smin, smin + P.sv_world, x, w, tmin_sv, tmax_sv);
+                bd = tmax_sv - tmin_sv;
+            }
+            continue;
         }
         const float t = free_path(rng, P.inv_extinction);
         bool escape = t > d;
@@ -798,7 +886,8 @@ static cudaError_t launch_trace_t(const TraceParams& P, int schedule, int featur
                                   cudaStream_t stream) {
     uint64_t total = padded_paths(P.width, P.height, P.num_frames);
     constexpr bool kRefillable = TRACKER == kDelta || TRACKER == kRatio || TRACKER == kNextEvent ||
-                                 TRACKER == kNextEvent + 100 || TRACKER == kDeltaIso;
+                                 TRACKER == kNextEvent + 100 || TRACKER == kDeltaIso ||
+                                 (TRACKER == kDecomposition && GRID != kNanoVdb);
     if (schedule == kScheduleRefill && kRefillable && !features) {
         if constexpr (kRefillable) {
             int blocks = refill_blocks<TRACKER, INTERP, GRID, TF>(persistent_blocks);
