@@ -372,6 +372,21 @@ def run_ours(args):
     fetch["selected"] = "texture_object" if DENSITY_TEXTURE else "global_loads"
     _lib.check(lib.vpt_set_option(ctx, b"density_texture", float(DENSITY_TEXTURE)), "density_texture", ctx)
 
+    # refills taken once k lanes of a warp wait (the film is written when each path ends)
+    refill = {}
+    for k in (1, 2, 4, 8):
+        _lib.check(lib.vpt_set_option(ctx, b"refill_min_lanes", float(k)), "refill_min_lanes", ctx)
+        vpt.render_frame(img, 1)
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(3):
+            _lib.check(lib.vpt_render_frames(ctx, SPP_PER_STEP, ctypes_stream), "render", ctx)
+        e1.record(stream)
+        barrier()
+        refill[str(k)] = RES * RES * SPP_PER_STEP * world / (max_over_ranks(e0.elapsed_time(e1)) / 3 / 1e3)
+    _lib.check(lib.vpt_set_option(ctx, b"refill_min_lanes", 1.0), "refill_min_lanes", ctx)
+
 
     # end to end through the public API: host grid -> device, render, result -> host
     vpt.set_vpt_mode_from_name("Delta Tracking")
@@ -428,7 +443,7 @@ def run_ours(args):
             "lookups_per_s": lookups / (ms_total / 1e3) * world,
             "lookups_per_path": lookups / max(1, st["paths"]),
             "gather_roofline": gather_roofline,
-            "per_tracker": per_tracker, "tracker_reference_render": reference_render, "schedules_delta": schedules, "fetch_paths_delta": fetch, "streaming_kernels": streaming, "e2e": e2e, "gpu_launches": int(launches), "clocks": clock_info,
+            "per_tracker": per_tracker, "tracker_reference_render": reference_render, "schedules_delta": schedules, "fetch_paths_delta": fetch, "refill_min_lanes_delta": refill, "streaming_kernels": streaming, "e2e": e2e, "gpu_launches": int(launches), "clocks": clock_info,
         }
         if cpu is not None:
             line["cpu_baseline"] = cpu

@@ -195,6 +195,7 @@ struct VptContext {
     // the normalised dense grid as a 3D texture (option "density_texture"): delta tracking reads it
     // through the texture unit when the border density is 0
     int density_texture = 1;
+    int refill_min = 1;  // option "refill_min_lanes"
     cudaArray_t dens_array = nullptr;
     cudaTextureObject_t dens_tex = 0;
     cudaSurfaceObject_t dens_surf = 0;  // the same array, written by fill_density_array_kernel
@@ -697,6 +698,7 @@ VptStatus fill_params(VptContext* ctx, int tracker, int frames, vpt::TraceParams
         for (int i = 0; i < 9; i++) P.env_rot_m[i] = ctx->env_rot_m[i];
     }
     P.density = ctx->norm.ptr;
+    P.refill_min = ctx->refill_min;
     P.sv_data = ctx->sv_pairs.ptr;
     P.sv_local = ctx->sv_local.ptr;
     P.occupancy = ctx->occupancy.ptr;
@@ -2146,6 +2148,9 @@ VptStatus vpt_set_option(VptContext* ctx, const char* key, double value) {
         int v = int(value);
         if (v < 0 || v > 2) return fail(ctx, VPT_ERR_ARG, "schedule must be 0 (tiles), 1 (persistent) or 2 (refill)");
         ctx->schedule = v;
+    } else if (k == "refill_min_lanes") {
+        if (value < 1 || value > 32) return fail(ctx, VPT_ERR_ARG, "refill_min_lanes must be in 1..32");
+        ctx->refill_min = int(value);
     } else if (k == "density_texture") {
         ctx->density_texture = int(value) ? 1 : 0;
     } else if (k == "persistent_blocks_per_sm") {

@@ -136,6 +136,7 @@ struct TraceParams {
     uint32_t max_steps;        // guard on tentative collisions per path (kMaxStepsPerPath by default)
     int grid_kind;             // GridKind: dense texture or sparse (NanoVDB) volume
     unsigned long long density_tex; // cudaTextureObject_t over `density` (0: none; kDenseTex kernels)
+    int refill_min;            // per-lane refill schedule: a warp refills its empty lanes once this many wait
     float* frame_normals;      // Depth (nabla) / (fwidth): 4 floats per frame of the launch and pixel, the
                                //   first event's normal and 1 (0 0 0 0 without an event), frame-major
     int ess_ref_compat;        // reproduce the reference's empty-space-skipping shadow loop exactly

@@ -434,7 +434,7 @@ VPT_DEV void flush_counters_to(unsigned long long* counters, int* error_flags, u
 
 template <int TRACKER, int INTERP, int GRID, bool TF, class SRC>
 VPT_DEV void refill_loop(const SRC& src, uint64_t total, unsigned long long* work_counter,
-                         unsigned long long* counters, int* error_flags) {
+                         unsigned long long* counters, int* error_flags, int refill_min) {
     // next event tracking; kNextEvent + 100: its sky shadow rays skip the occupancy grid's empty blocks
     constexpr bool kNee = TRACKER == kNextEvent || TRACKER == kNextEvent + 100;
     constexpr bool kEss = TRACKER == kNextEvent + 100;
@@ -480,7 +480,9 @@ VPT_DEV void refill_loop(const SRC& src, uint64_t total, unsigned long long* wor
         // ---- refill lanes without a path ----
         const bool need = !has && !exhausted;
         const unsigned m = __ballot_sync(FULL, need);
-        if (m) {
+        // refill once `refill_min` lanes wait (the refill step is the loop's longest and most divergent
+        // code), or when no lane of the warp holds a path
+        if (m && (refill_min <= 1 || __popc(m) >= refill_min || !__any_sync(FULL, has))) {
             const int n = __popc(m);
             const int r = __popc(m & lt_mask);
             unsigned long long fresh = 0;
@@ -816,7 +818,7 @@ VPT_DEV void refill_loop(const SRC& src, uint64_t total, unsigned long long* wor
 template <int TRACKER, int INTERP, int GRID, bool TF>
 __global__ void __launch_bounds__(kTraceBlock) trace_refill_kernel(const __grid_constant__ TraceParams P, uint64_t total) {
     refill_loop<TRACKER, INTERP, GRID, TF>(OneScene{P}, total, reinterpret_cast<unsigned long long*>(P.work_counter),
-                                       P.counters, P.error_flags);
+                                       P.counters, P.error_flags, P.refill_min);
 }
 
 // Many independent scenes (own grid, camera, image size, spp, medium) traced by one persistent
@@ -828,7 +830,7 @@ __global__ void __launch_bounds__(kTraceBlock) trace_batch_kernel(const TracePar
                                                                   int num, unsigned long long* work_counter,
                                                                   unsigned long long* counters, int* error_flags) {
     refill_loop<TRACKER, INTERP, GRID, false>(SceneBatch{scenes, offsets, num}, __ldg(offsets + num), work_counter, counters,
-                                       error_flags);
+                                       error_flags, 1);
 }
 
 
