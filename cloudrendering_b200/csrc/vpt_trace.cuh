@@ -470,6 +470,13 @@ VPT_DEV void refill_loop(const SRC& src, uint64_t total, unsigned long long* wor
     // decomposition tracking (the same block walk): the block's normalised min / max density, its
     // control and residual extinctions and the control clock (bt is the residual clock)
     float dc_min = 0.0f, dc_max = 0.0f, mu_c = 1.0f, mu_r = 1.0f, t_c = 0.0f;
+    // unbiased residual ratio tracking: the Amanatides-Woo supervoxel walk of the current free flight
+    // or shadow ray (started lazily), its axis and cell, the distance reached, the walk's length
+    SvWalk sw;
+    bool walking = false;
+    int wa = 0;
+    float4 wc = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    float wt0 = 0.0f, wt1 = 0.0f, wlen = 0.0f;
     int scene = 0;
     uint32_t steps = 0;
     size_t pix = 0;
@@ -521,6 +528,8 @@ VPT_DEV void refill_loop(const SRC& src, uint64_t total, unsigned long long* wor
                     color = zero;
                     ev = false;
                     mode = kModePrimary;
+                    walking = false;
+                    in_block = false;
                     iw = f3(1.0f, 1.0f, 1.0f);
                     iso_first = true;
                     iso_it = 0;
@@ -571,7 +580,7 @@ VPT_DEV void refill_loop(const SRC& src, uint64_t total, unsigned long long* wor
         }
         if (++steps > P.max_steps) {
             guard_hit = true;
-            refill_finish<TRACKER>(P, pix, kNee ? color : zero, has);
+            refill_finish<TRACKER>(P, pix, (kNee || TRACKER == kResidualRatioNee) ? color : zero, has);
             continue;
         }
         if constexpr (kEss) {
@@ -617,6 +626,124 @@ VPT_DEV void refill_loop(const SRC& src, uint64_t total, unsigned long long* wor
                 ts *= 1.0f - dens;
                 continue;
             }
+        }
+        if constexpr (TRACKER == kResidualRatioNee) {
+            // track_residual_ratio_nee one step per iteration: a free flight by delta tracking with each
+            // supervoxel's majorant, then at a scatter a shadow ray whose transmittance is residual
+            // ratio tracking over the same walk (shadow_residual_ratio); a cell boundary or one
+            // tentative collision per iteration
+            if (!walking) {
+                if (mode == kModePrimary) {
+                    wlen = d;
+                } else {  // shadow ray from xp along w (x == xp here), up to the light or the box exit
+                    float tmin_s, tmax_s;
+                    float len = -1.0f;
+                    if (ray_box(P.box_min, P.box_max, x, w, tmin_s, tmax_s)) len = fminf(tmax_s, shadow_max) - tmin_s;
+                    if (!(len > 0.0f)) {  // transmittance 1, no random numbers
+                        goto rrt_shadow_done;
+                    }
+                    x = x + w * tmin_s;
+                    wlen = len;
+                }
+                sv_walk_begin(P, x, w, sw);
+                wt0 = 0.0f;
+                in_block = false;
+                walking = true;
+            }
+            if (!in_block) {  // entering a cell
+                wa = sv_walk_axis(sw);
+                wt1 = fminf(sw.next[wa], wlen);
+                wc = sv_local_cell(P, sw);
+                if (wc.w > 0.0f && wt1 > wt0) {
+                    if (mode != kModePrimary) ts *= m_exp(-wc.x * (wt1 - wt0));
+                    bt = wt0;
+                    in_block = true;
+                    continue;
+                }
+            } else {
+                if (mode == kModePrimary) {
+                    bt += free_path(rng, wc.w);
+                    if (bt < wt1) {
+                        const float dens = sample(x + w * bt, rng);
+                        lookups++;
+                        const float r = dens * wc.z;  // density / majorant density
+                        const float xi = rng_next(rng);
+                        if (xi < P.absorb_albedo * r) {
+                            refill_finish<TRACKER>(P, pix, P.emission ? color + sample.emission(x + w * bt, rng) : color,
+                                                   has);
+                            continue;
+                        }
+                        if (xi < r) {  // scatter: next event estimate, then the next free flight
+                            x = x + w * bt;
+                            walking = false;
+                            in_block = false;
+                            if (P.max_bounces > 0 && ++bounces > P.max_bounces) {
+                                refill_finish<TRACKER>(P, pix, color, has);
+                                continue;
+                            }
+                            nw = sample_phase(rng, P.g, w);
+                            ev = true;
+                            bool to_light = false;
+                            float prob_factor = 1.0f, pdf_light = 0.0f, light_dist = 0.0f;
+                            int light_idx = 0;
+                            if (P.num_lights > 0) {
+                                to_light = P.env_is_black ? true : (rng_next(rng) > 0.5f);
+                                prob_factor = P.env_is_black ? 1.0f : 2.0f;
+                            }
+                            F3 dir;
+                            if (to_light) dir = light_direction(P, x, rng, light_idx, prob_factor, light_dist);
+                            else dir = importance_sample_sky(P, rng, pdf_light);
+                            const float pdf_phase = evaluate_phase(P.g, w, dir);
+                            weight = to_light ? prob_factor * pdf_phase : (prob_factor * pdf_phase) / pdf_light;
+                            light = to_light ? light_idx : -1;
+                            shadow_max = to_light ? light_dist : INFINITY;
+                            xp = x;
+                            w = dir;
+                            ts = 1.0f;
+                            mode = kModeShadow;
+                        }
+                        continue;
+                    }
+                } else {
+                    bt += free_path(rng, 1.0f / wc.y);
+                    if (bt < wt1) {
+                        const float dens = sample(x + w * bt, rng);
+                        lookups++;
+                        ts *= 1.0f - (P.extinction * dens - wc.x) * (1.0f / wc.y);
+                        continue;
+                    }
+                }
+                in_block = false;
+            }
+            // leaving the cell [wt0, wt1)
+            if (wt1 < wlen) {
+                wt0 = fmaxf(wt0, wt1);
+                if (sv_walk_advance(P, sw, wa)) continue;
+            }
+            walking = false;
+            if (mode == kModePrimary) {  // the flight left the box without a collision
+                refill_finish<TRACKER>(P, pix, ev ? color : color + sky_and_sun(P, w), has);
+                continue;
+            }
+        rrt_shadow_done:
+            {
+                const float f = weight * ts;
+                const F3 l = light >= 0 ? light_radiance(P, xp, light) : sky_and_sun(P, w);
+                color = color + f3(f * l.x, f * l.y, f * l.z);
+                x = xp;
+                w = nw;
+                mode = kModePrimary;
+                walking = false;
+                in_block = false;
+                float tmin_b, tmax_b;
+                if (!ray_box(P.box_min, P.box_max, x, w, tmin_b, tmax_b)) {
+                    refill_finish<TRACKER>(P, pix, color, has);
+                    continue;
+                }
+                x = x + w * tmin_b;
+                d = tmax_b - tmin_b;
+            }
+            continue;
         }
         if constexpr (TRACKER == kDecomposition) {
             // the supervoxel walk of track_decomposition, one block boundary or one step of the two
@@ -889,7 +1016,7 @@ static cudaError_t launch_trace_t(const TraceParams& P, int schedule, int featur
     uint64_t total = padded_paths(P.width, P.height, P.num_frames);
     constexpr bool kRefillable = TRACKER == kDelta || TRACKER == kRatio || TRACKER == kNextEvent ||
                                  TRACKER == kNextEvent + 100 || TRACKER == kDeltaIso ||
-                                 (TRACKER == kDecomposition && GRID != kNanoVdb);
+                                 ((TRACKER == kDecomposition || TRACKER == kResidualRatioNee) && GRID != kNanoVdb);
     if (schedule == kScheduleRefill && kRefillable && !features) {
         if constexpr (kRefillable) {
             int blocks = refill_blocks<TRACKER, INTERP, GRID, TF>(persistent_blocks);

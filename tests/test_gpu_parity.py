@@ -379,7 +379,8 @@ def test_iteration_guard_reports_error_without_hanging(core):
 
 
 @pytest.mark.parametrize("mode", ["delta", "ratio", "nee", "nee_lights", "delta_isosurfaces", "nee_ess",
-                                  "nee_ess_ref_compat", "decomposition", "decomposition_trilinear"])
+                                  "nee_ess_ref_compat", "decomposition", "decomposition_trilinear", "rrt_unbiased",
+                                  "rrt_unbiased_trilinear", "rrt_unbiased_lights"])
 def test_schedules_trace_identical_paths(core_dr, mode):
     """Tile, persistent-batch and per-lane-refill schedules trace the same paths (same film up to the
     order of the FP64 atomic additions).  The isosurface case covers the refill loop's own surface
@@ -393,6 +394,10 @@ def test_schedules_trace_identical_paths(core_dr, mode):
         kw = dict(mode="delta", interp="trilinear", iso=True, iso_value=0.3)
     elif mode.startswith("nee_ess"):  # sky shadow rays skip empty occupancy blocks (the refill loop's own walk)
         kw = dict(mode="nee", use_ess=True, ess_ref_compat=mode.endswith("compat"))
+    elif mode == "rrt_unbiased_lights":  # free flights and shadow walks of the refill loop, light shadow rays
+        kw = dict(PATH_CASES["nee_lights"], mode="rrt_unbiased")
+    elif mode.startswith("rrt_unbiased"):
+        kw = dict(mode="rrt_unbiased", interp="trilinear" if mode.endswith("trilinear") else "stochastic")
     elif mode.startswith("decomposition"):  # the supervoxel walk with two clocks in the refill loop
         kw = dict(mode="decomposition", interp="trilinear" if mode.endswith("trilinear") else "stochastic")
     else:
