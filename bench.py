@@ -42,6 +42,9 @@ BYTES_PER_LOOKUP = 32  # one 32-byte sector per uncoalesced density gather
 # delta tracking reads the density through the grid's 3D texture object (1) or by global loads (0);
 # both read the same texels; the bench's fetch_paths_delta leg times the two
 DENSITY_TEXTURE = 1
+# per-lane refill schedule: a warp takes new paths once this many of its lanes wait (the library's
+# default; refill_min_lanes_delta times 1, 2, 4 and 8)
+REFILL_MIN_LANES = 4
 # DRAM read + write bytes of one headline launch (64 spp of the 1024^2 image on the 512^3 cloud, density
 # through the texture object), from one ncu capture of that launch
 # (profiles/trace_refill_delta_512_1024_64spp.md): 37.56 GB, 560 B per path
@@ -283,6 +286,7 @@ def run_ours(args):
     ctx = vpt.context_handle()
     setup_scene(vpt, rank)
     _lib.check(lib.vpt_set_option(ctx, b"density_texture", float(DENSITY_TEXTURE)), "density_texture", ctx)
+    _lib.check(lib.vpt_set_option(ctx, b"refill_min_lanes", float(REFILL_MIN_LANES)), "refill_min_lanes", ctx)
     stream = torch.cuda.current_stream()
     ctypes_stream = __import__("ctypes").c_void_p(stream.cuda_stream)
     img = torch.zeros((4, RES, RES), dtype=torch.float32, device="cuda")
@@ -372,7 +376,8 @@ def run_ours(args):
     fetch["selected"] = "texture_object" if DENSITY_TEXTURE else "global_loads"
     _lib.check(lib.vpt_set_option(ctx, b"density_texture", float(DENSITY_TEXTURE)), "density_texture", ctx)
 
-    # refills taken once k lanes of a warp wait (the film is written when each path ends)
+    # refills taken once k lanes of a warp wait (the film is written when each path ends; the paths are
+    # the same for every k)
     refill = {}
     for k in (1, 2, 4, 8):
         _lib.check(lib.vpt_set_option(ctx, b"refill_min_lanes", float(k)), "refill_min_lanes", ctx)
@@ -385,7 +390,8 @@ def run_ours(args):
         e1.record(stream)
         barrier()
         refill[str(k)] = RES * RES * SPP_PER_STEP * world / (max_over_ranks(e0.elapsed_time(e1)) / 3 / 1e3)
-    _lib.check(lib.vpt_set_option(ctx, b"refill_min_lanes", 1.0), "refill_min_lanes", ctx)
+    _lib.check(lib.vpt_set_option(ctx, b"refill_min_lanes", float(REFILL_MIN_LANES)), "refill_min_lanes", ctx)
+    refill["selected"] = REFILL_MIN_LANES
 
 
     # end to end through the public API: host grid -> device, render, result -> host
@@ -1114,6 +1120,7 @@ def profile_trace(spp):
     ctx = vpt.context_handle()
     setup_scene(vpt, 0)
     _lib.check(lib.vpt_set_option(ctx, b"density_texture", float(DENSITY_TEXTURE)), "density_texture", ctx)
+    _lib.check(lib.vpt_set_option(ctx, b"refill_min_lanes", float(REFILL_MIN_LANES)), "refill_min_lanes", ctx)
     vpt.set_vpt_mode_from_name("Delta Tracking")
     _lib.check(lib.vpt_set_resolution(ctx, RES, RES), "resolution", ctx)
     cs = __import__("ctypes").c_void_p(torch.cuda.current_stream().cuda_stream)

@@ -195,7 +195,7 @@ struct VptContext {
     // the normalised dense grid as a 3D texture (option "density_texture"): delta tracking reads it
     // through the texture unit when the border density is 0
     int density_texture = 1;
-    int refill_min = 1;  // option "refill_min_lanes"
+    int refill_min = 4;  // option "refill_min_lanes" (4: measured best of 1, 2, 4, 8 on the headline launch)
     cudaArray_t dens_array = nullptr;
     cudaTextureObject_t dens_tex = 0;
     cudaSurfaceObject_t dens_surf = 0;  // the same array, written by fill_density_array_kernel

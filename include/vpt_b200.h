@@ -273,7 +273,7 @@ VptStatus vpt_set_use_empty_space_skipping(VptContext* ctx, int enabled);
  * empty-space skipping or a transfer function) on a dense grid whose border density is 0 read the
  * density through a 3D texture object, the same texels bit for bit, for a second copy of the grid in
  * device memory; a grid beyond the 3D texture size or without memory for the copy is read directly;
- * 0 = always read directly), "refill_min_lanes" (1..32, default 1: in the per-lane refill schedule a
+ * 0 = always read directly), "refill_min_lanes" (1..32, default 4: in the per-lane refill schedule a
  * warp takes new paths for its empty lanes once this many wait, or when none holds a path; the paths
  * are the same whatever the value). */
 VptStatus vpt_set_option(VptContext* ctx, const char* key, double value);

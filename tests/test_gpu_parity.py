@@ -410,10 +410,11 @@ def test_schedules_trace_identical_paths(core_dr, mode):
         core("vpt_set_option", b"schedule", float(sched))
         s, _ = gpu_render(core, sp, 3, stats=False)
         films.append(s)
-    # refills taken once 8 lanes wait: the same paths
-    core("vpt_set_option", b"refill_min_lanes", 8.0)
-    films.append(gpu_render(core, sp, 3, stats=False)[0])
-    core("vpt_set_option", b"refill_min_lanes", 1.0)
+    # refills taken as soon as one lane waits, or once 8 wait (the default is 4): the same paths
+    for k in (1.0, 8.0):
+        core("vpt_set_option", b"refill_min_lanes", k)
+        films.append(gpu_render(core, sp, 3, stats=False)[0])
+    core("vpt_set_option", b"refill_min_lanes", 4.0)
     core("vpt_set_option", b"schedule", 2.0)
     core("vpt_set_option", b"ess_ref_compat", 0.0)
     for f in films[1:]:
