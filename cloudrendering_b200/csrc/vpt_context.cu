@@ -1586,7 +1586,9 @@ VptStatus vpt_render_frames(VptContext* ctx, int frames, void* stream) {
     if (st != VPT_OK) return st;
     vpt::TraceParams P;
     fill_params(ctx, tracker, single ? 1 : frames, P);
-    if (ctx->density_texture && (tracker == vpt::kDelta || tracker == vpt::kRatio || tracker == vpt::kNextEvent) &&
+    if (ctx->density_texture &&
+        (tracker == vpt::kDelta || tracker == vpt::kRatio || tracker == vpt::kNextEvent ||
+         tracker == vpt::kDecomposition || tracker == vpt::kResidualRatioNee) &&
         !ctx->use_sparse && !P.tf && !P.iso && P.border_density == 0.0f && ensure_density_texture(ctx, s)) {
         P.density_tex = ctx->dens_tex;
     }

@@ -58,11 +58,18 @@ cudaError_t launch_trace(const TraceParams& P, int tracker, int use_ess, int sch
             if (P.density_tex && !P.tf)
                 return launch_tracker<kRatio, kDenseTex>(P, schedule, features, persistent_blocks, stream);
             return launch_tracker<kRatio, kDense>(P, schedule, features, persistent_blocks, stream);
-        case kDecomposition: return launch_tracker<kDecomposition, kDense>(P, schedule, features, persistent_blocks, stream);
+        case kDecomposition:
+            if (P.density_tex && !P.tf)
+                return launch_tracker<kDecomposition, kDenseTex>(P, schedule, features, persistent_blocks, stream);
+            return launch_tracker<kDecomposition, kDense>(P, schedule, features, persistent_blocks, stream);
         case kResidualRatio: return launch_tracker<kResidualRatio, kDense>(P, schedule, features, persistent_blocks, stream);
         case kResidualRatioNee:
+            if (P.density_tex && !P.tf)
+                return launch_tracker<kResidualRatioNee, kDenseTex>(P, schedule, features, persistent_blocks, stream);
             return launch_tracker<kResidualRatioNee, kDense>(P, schedule, features, persistent_blocks, stream);
         case kNextEvent:
+            if (use_ess && P.density_tex && !P.tf)
+                return launch_tracker<kNextEvent + 100, kDenseTex>(P, schedule, features, persistent_blocks, stream);
             if (use_ess) return launch_tracker<kNextEvent + 100, kDense>(P, schedule, features, persistent_blocks, stream);
             if (P.density_tex && !P.tf)
                 return launch_tracker<kNextEvent, kDenseTex>(P, schedule, features, persistent_blocks, stream);

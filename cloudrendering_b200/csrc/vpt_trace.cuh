@@ -1101,12 +1101,15 @@ VPT_DECLARE_TRACKER(kRatio, kDense);
 VPT_DECLARE_TRACKER(kRatio, kDenseTex);
 VPT_DECLARE_TRACKER(kRatio, kNanoVdb);
 VPT_DECLARE_TRACKER(kDecomposition, kDense);
+VPT_DECLARE_TRACKER(kDecomposition, kDenseTex);
 VPT_DECLARE_TRACKER(kDecomposition, kNanoVdb);
 VPT_DECLARE_TRACKER(kResidualRatio, kDense);
 VPT_DECLARE_TRACKER(kResidualRatioNee, kDense);
+VPT_DECLARE_TRACKER(kResidualRatioNee, kDenseTex);
 VPT_DECLARE_TRACKER(kNextEvent, kDense);
 VPT_DECLARE_TRACKER(kNextEvent, kDenseTex);
 VPT_DECLARE_TRACKER(kNextEvent + 100, kDense);
+VPT_DECLARE_TRACKER(kNextEvent + 100, kDenseTex);
 VPT_DECLARE_TRACKER(kNextEvent, kNanoVdb);
 VPT_DECLARE_TRACKER(kSpectralDelta, kDense);
 VPT_DECLARE_TRACKER(kSpectralDelta, kNanoVdb);

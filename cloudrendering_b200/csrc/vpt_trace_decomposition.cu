@@ -4,6 +4,7 @@
 namespace vpt {
 
 VPT_DEFINE_TRACKER(kDecomposition, kDense)
+VPT_DEFINE_TRACKER_TEX(kDecomposition)
 VPT_DEFINE_TRACKER(kDecomposition, kNanoVdb)
 
 }  // namespace vpt

@@ -6,6 +6,7 @@ namespace vpt {
 VPT_DEFINE_TRACKER(kNextEvent, kDense)
 VPT_DEFINE_TRACKER_TEX(kNextEvent)
 VPT_DEFINE_TRACKER(kNextEvent + 100, kDense)
+VPT_DEFINE_TRACKER_TEX(kNextEvent + 100)
 VPT_DEFINE_TRACKER(kNextEvent, kNanoVdb)
 
 }  // namespace vpt

@@ -5,5 +5,6 @@ namespace vpt {
 
 VPT_DEFINE_TRACKER(kResidualRatio, kDense)
 VPT_DEFINE_TRACKER(kResidualRatioNee, kDense)
+VPT_DEFINE_TRACKER_TEX(kResidualRatioNee)
 
 }  // namespace vpt

@@ -269,8 +269,8 @@ VptStatus vpt_set_use_empty_space_skipping(VptContext* ctx, int enabled);
  * occupied, ComputeOccupancyGrid.glsl:108-109, and shadow samples stepped from the moving point,
  * NeeTransmittance.glsl:173-228), "sparse_fp16" (1 = leaf values of the next sparse volume stored as
  * IEEE half), "fbm_contrast" (remap clamp(0.5 + contrast * fbm, 0, 1) of vpt_generate_fbm_grid,
- * default 3.5), "density_texture" (1, the default: delta, ratio and next event tracking (without
- * empty-space skipping or a transfer function) on a dense grid whose border density is 0 read the
+ * default 3.5), "density_texture" (1, the default: delta, ratio, next event, decomposition and unbiased
+ * residual ratio tracking (without a transfer function) on a dense grid whose border density is 0 read the
  * density through a 3D texture object, the same texels bit for bit, for a second copy of the grid in
  * device memory; a grid beyond the 3D texture size or without memory for the copy is read directly;
  * 0 = always read directly), "refill_min_lanes" (1..32, default 4: in the per-lane refill schedule a

@@ -423,7 +423,7 @@ def test_schedules_trace_identical_paths(core_dr, mode):
 
 @pytest.mark.parametrize("interp", ["nearest", "stochastic", "trilinear"])
 @pytest.mark.parametrize("sched", [1, 2])
-@pytest.mark.parametrize("mode", ["delta", "ratio", "nee"])
+@pytest.mark.parametrize("mode", ["delta", "ratio", "nee", "nee_ess", "decomposition", "rrt_unbiased"])
 def test_density_texture_reads_the_same_texels(core_dr, interp, sched, mode):
     """Delta, ratio and next event tracking through the grid's 3D texture object (option
     density_texture) trace the same paths as through global loads: same film (up to the order of the
@@ -431,7 +431,10 @@ def test_density_texture_reads_the_same_texels(core_dr, interp, sched, mode):
     every interpolation, with the camera seeing the box's border (texels outside the grid read the
     border density 0)."""
     core = core_dr
-    sp = fbm_scene(width=40, height=40, mode=mode, interp=interp)
+    if mode == "nee_ess":
+        sp = fbm_scene(width=40, height=40, mode="nee", use_ess=True, interp=interp)
+    else:
+        sp = fbm_scene(width=40, height=40, mode=mode, interp=interp)
     setup_core(core, sp)
     core("vpt_set_option", b"schedule", float(sched))
     feats = (ctypes.c_int * 2)(3, 6)  # normal, depth
