@@ -47,8 +47,8 @@ DENSITY_TEXTURE = 1
 REFILL_MIN_LANES = 4
 # DRAM read + write bytes of one headline launch (64 spp of the 1024^2 image on the 512^3 cloud, density
 # through the texture object), from one ncu capture of that launch
-# (profiles/trace_refill_delta_512_1024_64spp.md): 37.56 GB, 560 B per path
-NCU_DRAM_BYTES_PER_PATH = (35.711e9 + 1.845e9) / (1024 * 1024 * 64)
+# (profiles/trace_refill_delta_512_1024_64spp.md): 37.09 GB, 553 B per path
+NCU_DRAM_BYTES_PER_PATH = (35.250e9 + 1.844e9) / (1024 * 1024 * 64)
 
 
 def tensor_peak():
@@ -442,8 +442,8 @@ def run_ours(args):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak,
                          "traffic": NCU_DRAM_BYTES_PER_PATH * RES * RES * SPP_PER_STEP if args.workload == "full" else None,
-                         "limiter": "instruction issue at low SIMT efficiency (71 % issue active, 12.8 of 32 lanes per "
-                                    "instruction, DRAM 9 % busy; profiles/trace_refill_delta_512_1024_64spp.md)",
+                         "limiter": "instruction issue at low SIMT efficiency (70 % issue active, 13.6 of 32 lanes per "
+                                    "instruction, DRAM 10 % busy; profiles/trace_refill_delta_512_1024_64spp.md)",
                          "note": f"algorithmic bytes = density lookups x {BYTES_PER_LOOKUP} B sector; peak {peak_kind} "
                                  "HBM copy; traffic = ncu dram read + write bytes of this launch"},
             "lookups_per_s": lookups / (ms_total / 1e3) * world,
