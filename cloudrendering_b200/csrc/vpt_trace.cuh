@@ -957,7 +957,7 @@ __global__ void __launch_bounds__(kTraceBlock) trace_batch_kernel(const TracePar
                                                                   int num, unsigned long long* work_counter,
                                                                   unsigned long long* counters, int* error_flags) {
     refill_loop<TRACKER, INTERP, GRID, false>(SceneBatch{scenes, offsets, num}, __ldg(offsets + num), work_counter, counters,
-                                       error_flags, 1);
+                                       error_flags, scenes[0].refill_min);
 }
 
 

@@ -317,8 +317,9 @@ VptStatus vpt_build_environment_pyramid(const float* rgba, int width, int height
  * (0 skips it).  All contexts live on one device and share the tracker (delta, ratio or NEE without
  * empty space skipping), the interpolation and the grid kind; feature maps and SVGF are not
  * written.  The launch (parameter upload from pinned memory, counter reset, trace) is captured in a
- * CUDA graph on first use and replayed afterwards ("use_graph", default 1).  Results are read per
- * context with vpt_read_result / vpt_read_statistics. */
+ * CUDA graph on first use and replayed afterwards ("use_graph", default 1).  The first context's
+ * "refill_min_lanes" and, when every context has one, the density texture apply to the launch.
+ * Results are read per context with vpt_read_result / vpt_read_statistics. */
 VptStatus vpt_batch_create(VptBatch** out_batch, VptContext* const* contexts, int count);
 void vpt_batch_destroy(VptBatch* batch);
 const char* vpt_batch_last_error(VptBatch* batch);
