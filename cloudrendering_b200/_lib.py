@@ -75,6 +75,7 @@ SIGNATURES = {
     "vpt_set_emission_strength": (c_int, [VptCtxP, c_float]),
     "vpt_set_transfer_function": (c_int, [VptCtxP, c_void_p, c_int]),
     "vpt_set_use_transfer_function": (c_int, [VptCtxP, c_int]),
+    "vpt_set_tf_scattering_albedo_strength": (c_int, [VptCtxP, c_float]),
     "vpt_set_use_isosurfaces": (c_int, [VptCtxP, c_int]),
     "vpt_set_iso_value": (c_int, [VptCtxP, c_double]),
     "vpt_set_iso_surface_color": (c_int, [VptCtxP, c_double, c_double, c_double]),

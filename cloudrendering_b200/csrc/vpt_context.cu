@@ -158,6 +158,7 @@ struct VptContext {
     int enx = 0, eny = 0, enz = 0;
     bool use_emission = false;
     float emission_cap = 1.0f, emission_strength = 1.0f;
+    float tf_albedo_strength = 0.0f;  // setTfScatteringAlbedoStrength
     // transfer function (set_use_transfer_function; the RGBA table of transferFunctionTexture)
     DevBuf<float> tf;
     int tf_size = 0;
@@ -623,6 +624,7 @@ VptStatus fill_params(VptContext* ctx, int tracker, int frames, vpt::TraceParams
     P.border_density = (0.0f - ctx->vmin) / (ctx->vmax - ctx->vmin);
     P.emission = nullptr;
     P.emission_strength = ctx->emission_strength;
+    P.tf_albedo_strength = ctx->tf_albedo_strength;
     P.tf = (ctx->use_tf && ctx->tf.ptr && ctx->tf_size > 0) ? ctx->tf.ptr : nullptr;
     P.tf_size = ctx->tf_size;
     if (ctx->use_emission && ctx->emission.ptr) {
@@ -1056,6 +1058,14 @@ VptStatus vpt_set_transfer_function(VptContext* ctx, const float* rgba, int entr
     VPT_CHECK_CUDA(ctx, cudaMemcpy(ctx->tf.ptr, rgba, (size_t)entries * 4 * sizeof(float), cudaMemcpyHostToDevice));
     ctx->tf_size = entries;
     reset_film_state(ctx);
+    return VPT_OK;
+}
+
+VptStatus vpt_set_tf_scattering_albedo_strength(VptContext* ctx, float strength) {
+    VPT_CHECK_CTX(ctx);
+    if (!std::isfinite(strength)) return fail(ctx, VPT_ERR_ARG, "vpt_set_tf_scattering_albedo_strength: not finite");
+    if (strength != ctx->tf_albedo_strength) reset_film_state(ctx);
+    ctx->tf_albedo_strength = strength;
     return VPT_OK;
 }
 

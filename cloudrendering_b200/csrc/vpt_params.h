@@ -184,6 +184,8 @@ struct TraceParams {
     F3 emission_box_min;
     F3 emission_vox_per_unit;
     float emission_cap, emission_strength;  // the strength also scales transfer-function emission
+    float tf_albedo_strength;  // spectral trackers with a transfer function: scattering albedo mixed toward
+                               //   the table's rgb by this weight (0: off; USE_TRANSFER_FUNCTION_SCATTERING_ALBEDO)
 
     // transfer function (USE_TRANSFER_FUNCTION): every density lookup becomes the table's alpha at the
     // normalised density; absorptions emit strength * its rgb

@@ -465,9 +465,20 @@ struct SdtStep {
 VPT_DEV float max_component(F3 v) { return fmaxf(v.x, fmaxf(v.y, v.z)); }
 VPT_DEV float avg_component(F3 v) { return ((v.x + v.y) + v.z) / 3.0f; }
 
-VPT_DEV SdtStep sdt_probabilities(const TraceParams& P, float density, F3 weights) {
-    const F3 ext = f3(P.ext_rgb[0], P.ext_rgb[1], P.ext_rgb[2]);
+// The scattering albedo of a spectral step: parameters.scatteringAlbedo, or with
+// USE_TRANSFER_FUNCTION_SCATTERING_ALBEDO mix(scatteringAlbedo, the table's rgb at the lookup,
+// tfScatteringAlbedoStrength) (DeltaTracking.glsl:76-81, NextEventTracking.glsl:77-82).
+template <class S>
+VPT_DEV F3 sdt_albedo(const TraceParams& P, const S& sample) {
     const F3 alb = f3(P.albedo_rgb[0], P.albedo_rgb[1], P.albedo_rgb[2]);
+    if (!(P.tf && P.tf_albedo_strength > 0.0f)) return alb;
+    const float s = P.tf_albedo_strength;
+    return f3(alb.x * (1.0f - s) + sample.tf_rgb.x * s, alb.y * (1.0f - s) + sample.tf_rgb.y * s,
+              alb.z * (1.0f - s) + sample.tf_rgb.z * s);
+}
+
+VPT_DEV SdtStep sdt_probabilities(const TraceParams& P, float density, F3 weights, F3 alb) {
+    const F3 ext = f3(P.ext_rgb[0], P.ext_rgb[1], P.ext_rgb[2]);
     const F3 abs_alb = f3(1.0f - alb.x, 1.0f - alb.y, 1.0f - alb.z);
     SdtStep s;
     s.sa = f3((abs_alb.x * ext.x) * density, (abs_alb.y * ext.y) * density, (abs_alb.z * ext.z) * density);
@@ -520,7 +531,7 @@ VPT_DEV F3 track_delta_spectral(const TraceParams& P, S& sample, Rng& rng, F3 x,
             float density = sample(xn, rng);
             pc.lookups++;
             x = xn;
-            const SdtStep st = sdt_probabilities(P, density, weights);
+            const SdtStep st = sdt_probabilities(P, density, weights, sdt_albedo(P, sample));
             float xi = rng_next(rng);
             if (xi < st.pa) {
                 record_event(fe, x, density, P.sdt_majorant, tmax - d + t);
@@ -576,7 +587,7 @@ VPT_DEV F3 track_nee_spectral(const TraceParams& P, S& sample, Rng& rng, F3 x, F
             float density = sample(P.tf ? x : xn, rng);
             pc.lookups++;
             x = xn;
-            const SdtStep st = sdt_probabilities(P, density, weights);
+            const SdtStep st = sdt_probabilities(P, density, weights, sdt_albedo(P, sample));
             float xi = rng_next(rng);
             if (xi < st.pa) {
                 record_event(fe, x, density, P.sdt_majorant, tmax - d + t);

@@ -20,6 +20,7 @@ OPS = [
     "set_env_map_rot_angle_axis", "set_env_map_rot_quaternion", "set_scattering_albedo", "set_extinction_base",
     "set_extinction_scale", "set_vpt_mode", "set_vpt_mode_from_name", "set_denoiser", "set_denoiser_property",
     "set_pytorch_denoiser_model_file", "set_use_transfer_function", "load_transfer_function_file",
+    "set_transfer_function_empty", "set_tf_scattering_albedo_strength",
     "get_camera_position", "get_camera_view_matrix", "get_camera_fovy", "set_camera_position", "set_camera_target",
     "overwrite_camera_view_matrix", "set_feature_map_type", "set_use_empty_space_skipping", "set_use_lights",
     "clear_lights", "add_light", "remove_light", "set_light_property", "load_lights_from_file", "set_use_headlight",

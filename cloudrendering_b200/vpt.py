@@ -263,6 +263,17 @@ def set_use_transfer_function(_use_tf: bool) -> None:
     _c("vpt_set_use_transfer_function", 1 if _use_tf else 0)
 
 
+def set_tf_scattering_albedo_strength(strength: float) -> None:
+    """With a transfer function, spectral tracking scatters with mix(albedo, the table's rgb, strength)
+    (Module.cpp:1352-1354; enabled for strength > 0)."""
+    _c("vpt_set_tf_scattering_albedo_strength", float(strength))
+
+
+def set_transfer_function_empty() -> None:
+    """The empty transfer function of Module.cpp:1262-1276: opacity 0 and colour 0 over [0, 1]."""
+    set_transfer_function_table(np.zeros((2, 4), np.float32))
+
+
 def set_transfer_function_table(rgba) -> None:
     """The transfer-function texture as N x 4 RGBA values over the normalised density [0, 1] (the
     reference generates this table in sgl's TransferFunctionWindow)."""
@@ -303,6 +314,27 @@ def load_transfer_function_file(tf_file_path: str) -> None:
     raise RuntimeError("Error in loadTransferFunctionFile: transfer-function files are parsed by sgl's "
                        "TransferFunctionWindow, which this module does not include; pass the table to "
                        "set_transfer_function_table.")
+
+
+def load_transfer_function_file_gradient(tf_file_path: str) -> None:
+    raise RuntimeError("Error in loadTransferFunctionFileGradient: the gradient-magnitude transfer function "
+                       "(gradient isosurfaces) is not built in this module.")
+
+
+def set_transfer_function_range(_min_val: float, _max_val: float) -> None:
+    raise RuntimeError("Error in setTransferFunctionRange: the range mapping is sgl's TransferFunctionWindow's, "
+                       "which this module does not include; resample the table over the range and pass it to "
+                       "set_transfer_function_table.")
+
+
+def set_transfer_function_range_gradient(_min_val: float, _max_val: float) -> None:
+    raise RuntimeError("Error in setTransferFunctionRangeGradient: the gradient-magnitude transfer function "
+                       "(gradient isosurfaces) is not built in this module.")
+
+
+def set_transfer_function_empty_gradient() -> None:
+    raise RuntimeError("Error in setTransferFunctionEmptyGradient: the gradient-magnitude transfer function "
+                       "(gradient isosurfaces) is not built in this module.")
 
 
 def set_max_grid_extent(max_grid_extent: float) -> None:

@@ -138,6 +138,12 @@ VptStatus vpt_set_emission_strength(VptContext* ctx, float strength);
  * the reference builds it in sgl's TransferFunctionWindow, which is not part of its source tree. */
 VptStatus vpt_set_transfer_function(VptContext* ctx, const float* rgba, int entries);
 VptStatus vpt_set_use_transfer_function(VptContext* ctx, int use);
+/* setTfScatteringAlbedoStrength (Module.cpp:1352-1354, VolumetricPathTracingPass.cpp:914-925): with a
+ * transfer function, spectral delta and spectral next event tracking scatter with the albedo
+ * mix(scattering albedo, the table's rgb at the lookup, strength) (USE_TRANSFER_FUNCTION_SCATTERING_ALBEDO,
+ * DeltaTracking.glsl:76-81) when strength > 0, as the reference enables it; 0, the default, leaves the
+ * albedo alone. */
+VptStatus vpt_set_tf_scattering_albedo_strength(VptContext* ctx, float strength);
 /* Isosurfaces inside the volume (Module.cpp set_use_isosurfaces / set_iso_value / set_iso_surface_color /
  * set_isosurface_type / set_surface_brdf, src/PyTorch/Module.cpp:1163-1194; USE_ISOSURFACES in
  * DeltaTracking.glsl and CheckIsosurfaceHit.glsl): the surface where the normalised density crosses

@@ -113,6 +113,10 @@ def variants():
     for t, tdef in SPECTRAL.items():
         out.append((f"{t}_hist_tf__stochastic__default__linear",
                     [tdef, SDT_PROB["hist"], INTERPS["stochastic"], "USE_TRANSFER_FUNCTION"] + ENVS["default__linear"], 0))
+        # the transfer function's colour as scattering albedo (setTfScatteringAlbedoStrength > 0)
+        out.append((f"{t}_hist_tf_albedo__stochastic__default__linear",
+                    [tdef, SDT_PROB["hist"], INTERPS["stochastic"], "USE_TRANSFER_FUNCTION",
+                     "USE_TRANSFER_FUNCTION_SCATTERING_ALBEDO"] + ENVS["default__linear"], 0))
     # environment-image rotation (USE_ENV_MAP_ROTATION, VolumetricPathTracingPass.cpp:1708-1710)
     for t in ("delta", "nee"):
         out.append((f"{t}_rot__stochastic__image__linear", TRACKERS[t] + [INTERPS["stochastic"]] + ENVS["image__linear"]

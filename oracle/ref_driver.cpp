@@ -93,6 +93,7 @@ typedef struct RefScene {
     float iso_color[3];       /* parameters.isoSurfaceColor */
     float env_rot[9];         /* parameters.envMapDirRot, column-major (USE_ENV_MAP_ROTATION variants) */
     float prev_view_proj[16]; /* parameters.previousViewProjMatrix, column-major */
+    float tf_albedo_strength; /* parameters.tfScatteringAlbedoStrength */
 } RefScene;
 
 int ref_variant_count(void) { return ref_num_variants; }
@@ -167,6 +168,7 @@ int ref_render(int variant, const RefScene* s, float* out_rgba, int threads) {
     p.emissionBoxMax = vec3(s->emission_box_max[0], s->emission_box_max[1], s->emission_box_max[2]);
     p.emissionCap = s->emission_cap;
     p.emissionStrength = s->emission_strength;
+    p.tfScatteringAlbedoStrength = s->tf_albedo_strength;
     p.isoValue = s->iso_value;
     p.isoSurfaceColor = vec3(s->iso_color[0], s->iso_color[1], s->iso_color[2]);
     g_ref.tf.data = s->tf;

@@ -1112,7 +1112,13 @@ struct Tracer {
     static V3 cmul(V3 a, V3 b) { return v3(a.x * b.x, a.y * b.y, a.z * b.z); }
     // the collision probabilities of one real-or-null collision (DeltaTracking.glsl:90-110)
     void sdt_step(float dens, V3 weights, float maj, V3& sa, V3& ss, V3& sn, float& pa, float& ps, float& pn) const {
-        const V3 ext = ext3(), alb = alb3();
+        const V3 ext = ext3();
+        V3 alb = alb3();
+        if (S.tf && S.tf_albedo_strength > 0.0f) {  // mix(scatteringAlbedo, TF rgb, strength), DeltaTracking.glsl:76-81
+            const float s = S.tf_albedo_strength;
+            alb = v3(alb.x * (1.0f - s) + tf_rgb.x * s, alb.y * (1.0f - s) + tf_rgb.y * s,
+                     alb.z * (1.0f - s) + tf_rgb.z * s);
+        }
         const V3 aa = v3(1.0f - alb.x, 1.0f - alb.y, 1.0f - alb.z);
         sa = v3((aa.x * ext.x) * dens, (aa.y * ext.y) * dens, (aa.z * ext.z) * dens);
         ss = v3((alb.x * ext.x) * dens, (alb.y * ext.y) * dens, (alb.z * ext.z) * dens);

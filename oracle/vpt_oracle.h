@@ -85,6 +85,9 @@ typedef struct OracleScene {
     /* USE_ENV_MAP_ROTATION for environment images: envMapDirRot, 3x3 column-major */
     int env_rot;
     float env_rot_m[9];
+    /* USE_TRANSFER_FUNCTION_SCATTERING_ALBEDO (spectral trackers with a transfer function): the
+     * scattering albedo is mixed toward the table's rgb by this weight when it is > 0 */
+    float tf_albedo_strength;
 } OracleScene;
 
 /* Renders width*height*num_frames paths; adds radiance (and its square) per pixel (3 doubles). */

@@ -96,6 +96,13 @@ def cases():
         kw2 = dict(base)
         kw2.update(kw)
         out["fbm_" + name] = SceneSpec(grid=fbm, tf=transfer_function_table(), emission_strength=2.5, **kw2)
+    # the table's colour as scattering albedo of spectral tracking (USE_TRANSFER_FUNCTION_SCATTERING_ALBEDO)
+    for name, kw in {"sdt_hist_tf_albedo": dict(mode="spectral_delta", sdt_prob=2, **chroma),
+                     "nees_hist_tf_albedo": dict(mode="spectral_nee", sdt_prob=2, **chroma)}.items():
+        kw2 = dict(base)
+        kw2.update(kw)
+        out["fbm_" + name] = SceneSpec(grid=fbm, tf=transfer_function_table(), emission_strength=2.5,
+                                       tf_albedo_strength=0.6, **kw2)
     # environment-image rotation (USE_ENV_MAP_ROTATION): envMapDirRot = glm::eulerAngleYXZ(0.7, -0.4, 0.25)
     for name, kw in {"delta_env_image_rot": dict(mode="delta"), "nee_env_image_rot": dict(mode="nee")}.items():
         kw2 = dict(base)
@@ -137,7 +144,7 @@ def transfer_function_table(n=64):
 FIELDS = ["mode", "interp", "extinction", "albedo", "g", "width", "height", "seed_offset", "env", "linear_rgb",
           "sun_dir", "sun_intensity", "cam_pos", "cam_target", "fovy", "near", "far", "max_grid_extent", "use_ess",
           "env_intensity", "max_bounces", "ess_ref_compat", "lights", "extinction_base", "albedo_rgb", "sdt_prob",
-          "emission_cap", "emission_strength", "iso", "iso_value", "iso_color", "env_rot"]
+          "emission_cap", "emission_strength", "iso", "iso_value", "iso_color", "env_rot", "tf_albedo_strength"]
 
 
 def depth_map_cases():

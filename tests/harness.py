@@ -69,7 +69,8 @@ class SceneSpec:
                  fovy=2.0 * math.atan(0.5), near=0.01, far=100.0, max_grid_extent=0.25, env_rgba=None,
                  use_ess=False, env_intensity=(1.0, 1.0, 1.0), ess_ref_compat=False, lights=None,
                  extinction_base=(1.0, 1.0, 1.0), albedo_rgb=None, sdt_prob=2, emission=None, emission_cap=1.0,
-                 emission_strength=1.0, tf=None, iso=False, iso_value=0.5, iso_color=(0.4, 0.4, 0.4), env_rot=None):
+                 emission_strength=1.0, tf=None, iso=False, iso_value=0.5, iso_color=(0.4, 0.4, 0.4), env_rot=None,
+                 tf_albedo_strength=0.0):
         self.__dict__.update(locals())
         del self.__dict__["self"]
 
@@ -151,6 +152,7 @@ def setup_core(core: Core, sp: SceneSpec):
         t = np.ascontiguousarray(sp.tf, np.float32)
         core("vpt_set_transfer_function", t.ctypes.data_as(ctypes.c_void_p), t.shape[0])
     core("vpt_set_use_transfer_function", 1 if sp.tf is not None else 0)
+    core("vpt_set_tf_scattering_albedo_strength", float(sp.tf_albedo_strength))
     core("vpt_set_use_isosurfaces", 1 if sp.iso else 0)
     core("vpt_set_iso_value", sp.iso_value)
     core("vpt_set_iso_surface_color", *[float(c) for c in sp.iso_color])
@@ -312,6 +314,7 @@ def oracle_scene(core, sp: SceneSpec, frames: int, frame_count: int = 0) -> brid
         t = np.ascontiguousarray(sp.tf, np.float32)
         sc.set("tf", t)
         sc.set("tf_size", t.shape[0])
+    sc.set("tf_albedo_strength", float(np.float32(sp.tf_albedo_strength)))
     if sp.iso:
         sc.set("use_iso", 1)
         sc.set("iso_subdivisions", 2)
@@ -459,6 +462,7 @@ def reference_scene(sp: SceneSpec, frames: int, frame_start: int = 0, inv=None):
         t = np.ascontiguousarray(sp.tf, np.float32)
         sc.set("tf", t)
         sc.set("tf_size", t.shape[0])
+    sc.set("tf_albedo_strength", float(np.float32(sp.tf_albedo_strength)))
     prob = ["max", "avg", "hist"][sp.sdt_prob]
     tracker = {"delta": "delta", "ratio": "ratio", "decomposition": "decomposition", "rrt": "rrt",
                "nee": "nee_ess" if sp.use_ess else "nee", "spectral_delta": f"sdt_{prob}",
@@ -468,7 +472,7 @@ def reference_scene(sp: SceneSpec, frames: int, frame_start: int = 0, inv=None):
     if sp.emission is not None:
         tracker += "_emission"
     if sp.tf is not None:
-        tracker += "_tf"
+        tracker += "_tf_albedo" if sp.tf_albedo_strength > 0 else "_tf"
     sc.set("iso_value", sp.iso_value)
     sc.set("iso_color", sp.iso_color)
     if sp.iso:

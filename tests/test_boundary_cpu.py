@@ -67,3 +67,22 @@ def test_rotation_matrices_are_orthonormal(captured):
     m = captured["m"]
     assert np.allclose(m @ m.T, np.eye(3), atol=1e-6)
     assert np.allclose(m, Rotation.from_euler("z", math.pi / 3).as_matrix(), atol=1e-6)
+
+
+def test_transfer_function_empty_and_albedo_strength(monkeypatch):
+    """set_transfer_function_empty uploads the reference's empty function (opacity and colour 0 at both
+    ends, Module.cpp:1262-1276); set_tf_scattering_albedo_strength forwards its weight."""
+    seen = []
+
+    def grab(name, *args):
+        if name == "vpt_set_transfer_function":
+            ptr, n = args
+            import ctypes
+            seen.append((name, np.ctypeslib.as_array(ctypes.cast(ptr, ctypes.POINTER(ctypes.c_float)), (n * 4,)).copy()))
+        else:
+            seen.append((name, args))
+    monkeypatch.setattr(vpt, "_c", grab)
+    vpt.set_transfer_function_empty()
+    torch.ops.vpt.set_tf_scattering_albedo_strength(0.75)
+    assert seen[0][0] == "vpt_set_transfer_function" and np.array_equal(seen[0][1], np.zeros(8, np.float32))
+    assert seen[1] == ("vpt_set_tf_scattering_albedo_strength", (0.75,))
