@@ -821,6 +821,7 @@ struct VptBatch {
     unsigned long long* d_counters = nullptr; // [0] work counter, [1] paths, [2] lookups
     int* d_err = nullptr;
     int blocks_per_sm = 0;                    // 0: occupancy calculator; set by vpt_batch_autotune
+    int refill_min = 0;                       // 0: the first context's refill threshold; set by vpt_batch_autotune
     bool use_graph = true;
     cudaStream_t capture_stream = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -891,6 +892,8 @@ VptStatus batch_prepare(VptBatch* b, const int* frames, cudaStream_t s, vpt::Bat
             ensure_density_texture(ctx, s))
             b->h_params[i].density_tex = ctx->dens_tex;
     }
+    if (b->refill_min > 0)
+        for (int i = 0; i < n; i++) b->h_params[i].refill_min = b->refill_min;
     if (grid_kind == vpt::kDense) {
         bool all_tex = true;
         for (int i = 0; i < n; i++) all_tex = all_tex && b->h_params[i].density_tex != 0;
@@ -1944,6 +1947,9 @@ VptStatus vpt_batch_set_option(VptBatch* b, const char* key, double value) {
     } else if (k == "blocks_per_sm") {
         if (value < 0 || value > 64) return batch_fail(b, VPT_ERR_ARG, "blocks_per_sm out of range");
         b->blocks_per_sm = int(value);
+    } else if (k == "refill_min_lanes") {
+        if (value < 0 || value > 32) return batch_fail(b, VPT_ERR_ARG, "refill_min_lanes out of range");
+        b->refill_min = int(value);
     } else {
         return batch_fail(b, VPT_ERR_ARG, "unknown batch option " + k);
     }
@@ -2033,6 +2039,30 @@ VptStatus vpt_batch_autotune(VptBatch* b, const int* frames, void* stream, int* 
             best = per_sm;
         }
     }
+    // then the refill threshold at that block count
+    const int saved_refill = b->refill_min;
+    int best_refill = saved_refill;
+    best_ms = 1e30f;
+    const int refills[4] = {1, 2, 4, 8};
+    for (int c = 0; c < 4 && st == VPT_OK; c++) {
+        b->blocks_per_sm = best;
+        b->refill_min = refills[c];
+        cudaEventRecord(e0, s);
+        st = vpt_batch_render(b, frames, stream);
+        cudaEventRecord(e1, s);
+        if (st != VPT_OK) break;
+        if (cudaEventSynchronize(e1) != cudaSuccess) {
+            st = batch_fail(b, VPT_ERR_CUDA, "autotune launch failed");
+            break;
+        }
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best_ms) {
+            best_ms = ms;
+            best_refill = refills[c];
+        }
+    }
+    b->refill_min = st == VPT_OK ? best_refill : saved_refill;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     // the calibration renders went into the films: start the accumulation over

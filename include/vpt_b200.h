@@ -329,10 +329,12 @@ VptStatus vpt_build_environment_pyramid(const float* rgba, int width, int height
 VptStatus vpt_batch_create(VptBatch** out_batch, VptContext* const* contexts, int count);
 void vpt_batch_destroy(VptBatch* batch);
 const char* vpt_batch_last_error(VptBatch* batch);
-/* "use_graph" (0/1), "blocks_per_sm" (0 = occupancy calculator). */
+/* "use_graph" (0/1), "blocks_per_sm" (0 = occupancy calculator), "refill_min_lanes" (0 = the first
+ * context's). */
 VptStatus vpt_batch_set_option(VptBatch* batch, const char* key, double value);
 VptStatus vpt_batch_render(VptBatch* batch, const int* frames, void* stream);
-/* Times the batch at 1, 3/4, 1/2 and 1/4 of the resident blocks per SM and keeps the fastest; the
+/* Times the batch at 1, 3/4, 1/2 and 1/4 of the resident blocks per SM and keeps the fastest, then at
+ * that block count with refill thresholds of 1, 2, 4 and 8 lanes and keeps the fastest; the
  * calibration frames are rendered into the contexts' films, whose accumulation is then reset. */
 VptStatus vpt_batch_autotune(VptBatch* batch, const int* frames, void* stream, int* out_blocks_per_sm);
 VptStatus vpt_batch_get_stats(VptBatch* batch, VptStats* stats);
