@@ -159,6 +159,7 @@ struct VptContext {
     bool use_emission = false;
     float emission_cap = 1.0f, emission_strength = 1.0f;
     float tf_albedo_strength = 0.0f;  // setTfScatteringAlbedoStrength
+    int iso_brdf = 0;                 // setSurfaceBrdf: 0 Lambertian, 1 Blinn Phong, 2 Ambient
     // transfer function (set_use_transfer_function; the RGBA table of transferFunctionTexture)
     DevBuf<float> tf;
     int tf_size = 0;
@@ -625,6 +626,7 @@ VptStatus fill_params(VptContext* ctx, int tracker, int frames, vpt::TraceParams
     P.emission = nullptr;
     P.emission_strength = ctx->emission_strength;
     P.tf_albedo_strength = ctx->tf_albedo_strength;
+    P.iso_brdf = ctx->iso_brdf;
     P.tf = (ctx->use_tf && ctx->tf.ptr && ctx->tf_size > 0) ? ctx->tf.ptr : nullptr;
     P.tf_size = ctx->tf_size;
     if (ctx->use_emission && ctx->emission.ptr) {
@@ -1113,11 +1115,16 @@ VptStatus vpt_set_isosurface_type(VptContext* ctx, const char* name) {
 VptStatus vpt_set_surface_brdf(VptContext* ctx, const char* name) {
     VPT_CHECK_CTX(ctx);
     if (!name) return fail(ctx, VPT_ERR_ARG, "null surface BRDF");
-    if (strcmp(name, "Lambertian") == 0) return VPT_OK;
-    if (strcmp(name, "Blinn Phong") == 0 || strcmp(name, "Disney (2012)") == 0 || strcmp(name, "Cook Torrance") == 0 ||
-        strcmp(name, "Ambient") == 0)
-        return fail(ctx, VPT_ERR_UNSUPPORTED, "only the Lambertian surface BRDF is built in this core");
-    return VPT_OK;  // unknown names are ignored, as in the reference
+    int brdf = -1;
+    if (strcmp(name, "Lambertian") == 0) brdf = 0;
+    if (strcmp(name, "Blinn Phong") == 0) brdf = 1;
+    if (strcmp(name, "Ambient") == 0) brdf = 2;
+    if (strcmp(name, "Disney (2012)") == 0 || strcmp(name, "Cook Torrance") == 0)
+        return fail(ctx, VPT_ERR_UNSUPPORTED, "the Disney and Cook-Torrance surface BRDFs are not built in this core");
+    if (brdf < 0) return VPT_OK;  // unknown names are ignored, as in the reference
+    if (brdf != ctx->iso_brdf) reset_film_state(ctx);
+    ctx->iso_brdf = brdf;
+    return VPT_OK;
 }
 
 VptStatus vpt_set_num_isosurface_subdivisions(VptContext* ctx, int subdivisions) {

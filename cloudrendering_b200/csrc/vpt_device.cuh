@@ -678,6 +678,32 @@ VPT_DEV void iso_scatter(const TraceParams& P, Rng& rng, F3 p, F3& w, F3& weight
     const F3 t = cross3(b, n);
     const float xi0 = rng_next(rng);
     const float xi1 = rng_next(rng);
+    if (P.iso_brdf != 0) {
+        // BlinnPhong.glsl / ConstantLighting.glsl: a uniformly sampled hemisphere direction
+        // (sampleHemisphere, VptUtils.glsl:1071-1077: phi = 2 pi xi.y, z = xi.x) in the same frame
+        const float pi = 3.14159265358979323846f;  // M_PI as the shader's float
+        const float phi = (2.0f * pi) * xi1;
+        const float r = sqrtf(1.0f - xi0 * xi0);
+        const float lx = m_cos(phi) * r, ly = m_sin(phi) * r;
+        const F3 out = f3((t.x * lx + b.x * ly) + n.x * xi0, (t.y * lx + b.y * ly) + n.y * xi0,
+                          (t.z * lx + b.z * ly) + n.z * xi0);
+        F3 c = P.iso_color;  // ConstantLighting.glsl: the colour, whatever the direction
+        if (P.iso_brdf == 1) {
+            // BlinnPhong.glsl evaluateBrdf: 2 pi colour (n.h)^10 / norm, h = normalize(normalize(-w) + l),
+            // norm = clamp((n + 2) / (4 pi 2^(-n/2)), (n + 2) / (8 pi), (n + 4) / (8 pi)) with n = 10
+            const F3 view = normalize3(f3(-w.x, -w.y, -w.z));
+            const F3 h = normalize3(f3(view.x + out.x, view.y + out.y, view.z + out.z));
+            const float e = 10.0f;
+            const float norm = fminf(fmaxf((e + 2.0f) / ((4.0f * pi) * 0.03125f), (e + 2.0f) / (8.0f * pi)),
+                                     (e + 4.0f) / (8.0f * pi));
+            const float s = m_pow(fmaxf(dot3(n, h), 0.0f), e) / norm;
+            const float k = 2.0f * pi;
+            c = f3((k * P.iso_color.x) * s, (k * P.iso_color.y) * s, (k * P.iso_color.z) * s);
+        }
+        weights = f3(weights.x * c.x, weights.y * c.y, weights.z * c.z);
+        w = out;
+        return;
+    }
     const float ox = 2.0f * xi0 - 1.0f, oy = 2.0f * xi1 - 1.0f;
     float dx = 0.0f, dy = 0.0f;
     if (!(ox == 0.0f && oy == 0.0f)) {

@@ -184,6 +184,7 @@ struct TraceParams {
     F3 emission_box_min;
     F3 emission_vox_per_unit;
     float emission_cap, emission_strength;  // the strength also scales transfer-function emission
+    int iso_brdf;              // surface BRDF of isosurface hits: 0 Lambertian, 1 Blinn-Phong, 2 Ambient
     float tf_albedo_strength;  // spectral trackers with a transfer function: scattering albedo mixed toward
                                //   the table's rgb by this weight (0: off; USE_TRANSFER_FUNCTION_SCATTERING_ALBEDO)
 

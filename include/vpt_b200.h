@@ -147,12 +147,13 @@ VptStatus vpt_set_tf_scattering_albedo_strength(VptContext* ctx, float strength)
 /* Isosurfaces inside the volume (Module.cpp set_use_isosurfaces / set_iso_value / set_iso_surface_color /
  * set_isosurface_type / set_surface_brdf, src/PyTorch/Module.cpp:1163-1194; USE_ISOSURFACES in
  * DeltaTracking.glsl and CheckIsosurfaceHit.glsl): the surface where the normalised density crosses
- * iso_value (default 0.5) is found on every free-flight segment and reflects like an opaque
- * Lambertian surface of colour iso_surface_color (default 0.4 0.4 0.4); lookups are trilinear while
- * isosurfaces are on.  Built for delta tracking on dense grids: other trackers, sparse grids, a
- * transfer function and batched rendering return VPT_ERR_UNSUPPORTED.  Type "Density" and BRDF
- * "Lambertian" are accepted, "Gradient" and the other BRDF names return VPT_ERR_UNSUPPORTED, unknown
- * names are ignored (as in the reference).  vpt_set_num_isosurface_subdivisions is the pass's own
+ * iso_value (default 0.5) is found on every free-flight segment and reflects like an opaque surface
+ * of colour iso_surface_color (default 0.4 0.4 0.4) with the selected BRDF; lookups are trilinear
+ * while isosurfaces are on.  Built for delta tracking on dense grids: other trackers, sparse grids, a
+ * transfer function and batched rendering return VPT_ERR_UNSUPPORTED.  Type "Density" and the BRDFs
+ * "Lambertian" (Lambertian.glsl, the default), "Blinn Phong" (BlinnPhong.glsl) and "Ambient"
+ * (ConstantLighting.glsl) are accepted, "Gradient", "Disney (2012)" and "Cook Torrance" return
+ * VPT_ERR_UNSUPPORTED, unknown names are ignored (as in the reference).  vpt_set_num_isosurface_subdivisions is the pass's own
  * setting (VolumetricPathTracingPass.cpp:1028-1033, default 2, 1..8). */
 VptStatus vpt_set_use_isosurfaces(VptContext* ctx, int use);
 VptStatus vpt_set_iso_value(VptContext* ctx, double value);

@@ -733,6 +733,29 @@ struct Tracer {
                                                      : v3(-n.x * n.z, yz, 1.0f - n.z * n.z));
         const V3 t = cross(b, n);
         const float xi0 = rnd(r), xi1 = rnd(r);
+        if (S.iso_brdf != 0) {
+            // BlinnPhong.glsl / ConstantLighting.glsl: sampleHemisphere (VptUtils.glsl:1071-1077), uniform
+            const float pi = 3.14159265358979323846f;
+            const float phi = (2.0f * pi) * xi1;
+            const float rr = sqrtf(1.0f - xi0 * xi0);
+            const float lx = m_cos(phi) * rr, ly = m_sin(phi) * rr;
+            const V3 out = v3((t.x * lx + b.x * ly) + n.x * xi0, (t.y * lx + b.y * ly) + n.y * xi0,
+                              (t.z * lx + b.z * ly) + n.z * xi0);
+            V3 c = v3(S.iso_color[0], S.iso_color[1], S.iso_color[2]);
+            if (S.iso_brdf == 1) {  // BlinnPhong.glsl evaluateBrdf
+                const V3 view = normalize(neg(w));
+                const V3 h = normalize(add(view, out));
+                const float e = 10.0f;
+                const float norm = std::min(std::max((e + 2.0f) / ((4.0f * pi) * 0.03125f), (e + 2.0f) / (8.0f * pi)),
+                                            (e + 4.0f) / (8.0f * pi));
+                const float s = m_pow(std::max(dot(n, h), 0.0f), e) / norm;
+                const float k = 2.0f * pi;
+                c = v3((k * S.iso_color[0]) * s, (k * S.iso_color[1]) * s, (k * S.iso_color[2]) * s);
+            }
+            weights = v3(weights.x * c.x, weights.y * c.y, weights.z * c.z);
+            w = out;
+            return;
+        }
         const float ox = 2.0f * xi0 - 1.0f, oy = 2.0f * xi1 - 1.0f;
         float dx = 0.0f, dy = 0.0f;
         if (!(ox == 0.0f && oy == 0.0f)) {

@@ -88,6 +88,8 @@ typedef struct OracleScene {
     /* USE_TRANSFER_FUNCTION_SCATTERING_ALBEDO (spectral trackers with a transfer function): the
      * scattering albedo is mixed toward the table's rgb by this weight when it is > 0 */
     float tf_albedo_strength;
+    /* surface BRDF of isosurface hits: 0 Lambertian, 1 Blinn-Phong, 2 Ambient (ConstantLighting) */
+    int iso_brdf;
 } OracleScene;
 
 /* Renders width*height*num_frames paths; adds radiance (and its square) per pixel (3 doubles). */

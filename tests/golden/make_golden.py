@@ -117,6 +117,11 @@ def cases():
         kw2 = dict(base)
         kw2.update(kw)
         out["fbm_" + name] = SceneSpec(grid=fbm, mode="delta", interp="trilinear", iso=True, **kw2)
+    # the other surface BRDFs built here: Blinn-Phong (exponent 10) and constant lighting ("Ambient")
+    for name, brdf in {"delta_iso_blinn": "Blinn Phong", "delta_iso_ambient": "Ambient"}.items():
+        kw2 = dict(base)
+        kw2.update(iso_value=0.3, iso_color=(0.9, 0.6, 0.3), extinction=40.0, albedo=0.9, g=0.2)
+        out["fbm_" + name] = SceneSpec(grid=fbm, mode="delta", interp="trilinear", iso=True, iso_brdf=brdf, **kw2)
     return out
 
 
@@ -144,7 +149,8 @@ def transfer_function_table(n=64):
 FIELDS = ["mode", "interp", "extinction", "albedo", "g", "width", "height", "seed_offset", "env", "linear_rgb",
           "sun_dir", "sun_intensity", "cam_pos", "cam_target", "fovy", "near", "far", "max_grid_extent", "use_ess",
           "env_intensity", "max_bounces", "ess_ref_compat", "lights", "extinction_base", "albedo_rgb", "sdt_prob",
-          "emission_cap", "emission_strength", "iso", "iso_value", "iso_color", "env_rot", "tf_albedo_strength"]
+          "emission_cap", "emission_strength", "iso", "iso_value", "iso_color", "env_rot", "tf_albedo_strength",
+          "iso_brdf"]
 
 
 def depth_map_cases():
