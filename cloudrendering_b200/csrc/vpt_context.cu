@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 #include <algorithm>
 #include <cmath>
@@ -159,7 +160,9 @@ struct VptContext {
     bool use_emission = false;
     float emission_cap = 1.0f, emission_strength = 1.0f;
     float tf_albedo_strength = 0.0f;  // setTfScatteringAlbedoStrength
-    int iso_brdf = 0;                 // setSurfaceBrdf: 0 Lambertian, 1 Blinn Phong, 2 Ambient
+    int iso_brdf = 0;                 // setSurfaceBrdf: 0 Lambertian, 1 Blinn Phong, 2 Ambient, 3 Cook Torrance
+    // setBrdfParameter, in BrdfParam order; defaults of VolumetricPathTracingPass.hpp:410-419
+    float brdf[vpt::kBrdfParamCount] = {0.0f, 0.0f, 0.5f, 0.0f, 0.5f, 0.0f, 0.0f, 0.5f, 0.0f, 1.0f};
     // transfer function (set_use_transfer_function; the RGBA table of transferFunctionTexture)
     DevBuf<float> tf;
     int tf_size = 0;
@@ -627,6 +630,7 @@ VptStatus fill_params(VptContext* ctx, int tracker, int frames, vpt::TraceParams
     P.emission_strength = ctx->emission_strength;
     P.tf_albedo_strength = ctx->tf_albedo_strength;
     P.iso_brdf = ctx->iso_brdf;
+    for (int i = 0; i < vpt::kBrdfParamCount; ++i) P.brdf[i] = ctx->brdf[i];
     P.tf = (ctx->use_tf && ctx->tf.ptr && ctx->tf_size > 0) ? ctx->tf.ptr : nullptr;
     P.tf_size = ctx->tf_size;
     if (ctx->use_emission && ctx->emission.ptr) {
@@ -1119,11 +1123,31 @@ VptStatus vpt_set_surface_brdf(VptContext* ctx, const char* name) {
     if (strcmp(name, "Lambertian") == 0) brdf = 0;
     if (strcmp(name, "Blinn Phong") == 0) brdf = 1;
     if (strcmp(name, "Ambient") == 0) brdf = 2;
-    if (strcmp(name, "Disney (2012)") == 0 || strcmp(name, "Cook Torrance") == 0)
-        return fail(ctx, VPT_ERR_UNSUPPORTED, "the Disney and Cook-Torrance surface BRDFs are not built in this core");
+    if (strcmp(name, "Cook Torrance") == 0) brdf = 3;
+    if (strcmp(name, "Disney (2012)") == 0)
+        return fail(ctx, VPT_ERR_UNSUPPORTED, "the Disney (2012) surface BRDF is not built in this core");
     if (brdf < 0) return VPT_OK;  // unknown names are ignored, as in the reference
     if (brdf != ctx->iso_brdf) reset_film_state(ctx);
     ctx->iso_brdf = brdf;
+    return VPT_OK;
+}
+
+VptStatus vpt_set_brdf_parameter(VptContext* ctx, const char* key, const char* value) {
+    VPT_CHECK_CTX(ctx);
+    if (!key || !value) return fail(ctx, VPT_ERR_ARG, "null BRDF parameter key or value");
+    static const char* const kKeys[vpt::kBrdfParamCount] = {"subsurface", "metallic", "specular", "specular_tint",
+                                                        "roughness", "anisotropic", "sheen", "sheen_tint",
+                                                        "clearcoat", "clearcoat_gloss"};
+    for (int i = 0; i < vpt::kBrdfParamCount; ++i) {
+        if (strcmp(key, kKeys[i]) != 0) continue;
+        char* end = nullptr;
+        const float v = strtof(value, &end);
+        if (end == value) return fail(ctx, VPT_ERR_ARG, "BRDF parameter value is not a number");
+        ctx->brdf[i] = v;
+        break;
+    }
+    // unknown keys are logged and ignored by the reference; the film restarts either way
+    reset_film_state(ctx);
     return VPT_OK;
 }
 

@@ -38,6 +38,8 @@ VPT_DEV float m_cos(float x) { return (float)cos((double)x); }
 VPT_DEV float m_pow(float x, float y) { return (float)pow((double)x, (double)y); }
 VPT_DEV float m_atan2(float y, float x) { return (float)atan2((double)y, (double)x); }
 VPT_DEV float m_asin(float x) { return (float)asin((double)x); }
+VPT_DEV float m_acos(float x) { return (float)acos((double)x); }
+VPT_DEV float m_pow5(float x) { return (float)pow((double)x, 5.0); }
 #elif defined(VPT_FAST_MATH)
 // The product's tracer units (vpt_trace_*.cu): the special-function unit's approximations of log2,
 // exp2, sin and cos (a few ulp; sin and cos to ~2^-21 absolute on the phase angles in [0, 2 pi)), the
@@ -51,6 +53,10 @@ VPT_DEV float m_cos(float x) { return __cosf(x); }
 VPT_DEV float m_pow(float x, float y) { return __powf(x, y); }
 VPT_DEV float m_atan2(float y, float x) { return atan2f(y, x); }
 VPT_DEV float m_asin(float x) { return asinf(x); }
+VPT_DEV float m_acos(float x) { return acosf(x); }
+// pow(x, 5.0) of the Fresnel term: its base 1 - cos can round to a tiny negative value, which the
+// exp2(5 log2 x) form of __powf would turn into NaN
+VPT_DEV float m_pow5(float x) { const float x2 = x * x; return x2 * x2 * x; }
 #else
 VPT_DEV float m_log(float x) { return logf(x); }
 VPT_DEV float m_exp(float x) { return expf(x); }
@@ -59,6 +65,8 @@ VPT_DEV float m_cos(float x) { return cosf(x); }
 VPT_DEV float m_pow(float x, float y) { return powf(x, y); }
 VPT_DEV float m_atan2(float y, float x) { return atan2f(y, x); }
 VPT_DEV float m_asin(float x) { return asinf(x); }
+VPT_DEV float m_acos(float x) { return acosf(x); }
+VPT_DEV float m_pow5(float x) { return powf(x, 5.0f); }
 #endif
 
 VPT_DEV F3 f3(float x, float y, float z) { F3 r; r.x = x; r.y = y; r.z = z; return r; }
@@ -668,6 +676,70 @@ VPT_DEV F3 iso_normal(const TraceParams& P, F3 pos) {
 // ComputeDefaultBasis frame (RayTracingUtilities.glsl:20-28; Lambertian.glsl is included before
 // UNIFORM_SAMPLING is defined, so the concentric-disk map of VptUtils.glsl:1078-1098 and a pdf factor
 // equal to the cosine), throughput *= color * cos / cos.
+// mat3(t, b, n) * (x, y, z), summed in the order of a GLSL matrix-vector product
+VPT_DEV F3 iso_frame(F3 t, F3 b, F3 n, float x, float y, float z) {
+    return f3((t.x * x + b.x * y) + n.x * z, (t.y * x + b.y * y) + n.y * z, (t.z * x + b.z * y) + n.z * z);
+}
+
+// CookTorrance.glsl computeBrdf: sampleBrdf picks the GGX lobe with probability
+// (metallic + (1 - r)(1 + specular)) / (that + 1 - metallic), r = clamp(roughness, 0.05, 1), else its
+// own cosine lobe (theta = asin(sqrt(u))); evaluateBrdf returns the diffuse colour (1 - F)(1 - metallic)
+// plus F G v.h / (n.h v.n) for a GGX sample or F G D v.h sin(theta_h) / v.n for a diffuse one
+// (F Schlick with f0 = mix(0.16 specular^2, colour, metallic), D GGX, G Smith-Schlick with k = r^2 / 2),
+// and the throughput takes that value as it is.  sel, u are the hit's second and third random numbers.
+VPT_DEV void iso_cook_torrance(const TraceParams& P, Rng& rng, F3 n, F3 t, F3 b, float sel, float u, F3& w,
+                               F3& weights) {
+    const float pi = 3.14159265358979323846f;  // M_PI as the shader's float
+    const float v = rng_next(rng);
+    const float metallic = P.brdf[kBrdfMetallic], specular = P.brdf[kBrdfSpecular];
+    const float rough = fminf(fmaxf(P.brdf[kBrdfRoughness], 0.05f), 1.0f);
+    const float specular_w = metallic + (1.0f - rough) * (1.0f + specular);
+    const float diffuse_w = 1.0f - metallic;
+    const float specular_p = specular_w * (1.0f / (specular_w + diffuse_w));
+    const F3 view = normalize3(f3(-w.x, -w.y, -w.z));
+    const float alpha = rough * rough;
+    const float alpha2 = alpha * alpha;
+    const bool specular_hit = sel < specular_p;
+    const float phi = (2.0f * pi) * v;
+    F3 l;
+    if (specular_hit) {  // sample_GGX
+        const float theta = m_acos(sqrtf((1.0f - u) / (u * (alpha2 - 1.0f) + 1.0f)));
+        const float st = m_sin(theta);
+        const F3 h = iso_frame(t, b, n, st * m_cos(phi), st * m_sin(phi), m_cos(theta));
+        const float vh = fabsf(dot3(view, h));
+        const float s = 2.0f * (vh > 0.001f ? vh : 0.001f);  // avoidZero(v.h, 0.001)
+        l = f3(s * h.x - view.x, s * h.y - view.y, s * h.z - view.z);
+    } else {  // sample_Lambertian
+        const float theta = m_asin(sqrtf(u));
+        const float st = m_sin(theta);
+        l = iso_frame(t, b, n, st * m_cos(phi), st * m_sin(phi), m_cos(theta));
+    }
+    const F3 h = normalize3(f3(l.x + view.x, l.y + view.y, l.z + view.z));
+    const float ndoth = dot3(h, n), vdotn = dot3(view, n), ldotn = dot3(l, n), vdoth = dot3(view, h);
+    const float f0s = 0.16f * (specular * specular);
+    const float p5 = m_pow5(1.0f - vdoth);
+    const float k = alpha / 2.0f;
+    const float gl = ldotn < 0.001f ? 0.001f : ldotn, gv = vdotn < 0.001f ? 0.001f : vdotn;
+    const float g = (gl / (gl * (1.0f - k) + k)) * (gv / (gv * (1.0f - k) + k));
+    float d = 0.0f, sth = 0.0f;
+    if (!specular_hit) {
+        const float bq = (ndoth * ndoth) * (alpha2 - 1.0f) + 1.0f;
+        d = ((1.0f / pi) * alpha2) / (bq * bq);
+        sth = sqrtf(1.0f - fminf(ndoth * ndoth, 0.95f));
+    }
+    const float cx[3] = {P.iso_color.x, P.iso_color.y, P.iso_color.z};
+    float o[3];
+    for (int i = 0; i < 3; ++i) {
+        const float f0 = f0s * (1.0f - metallic) + cx[i] * metallic;
+        const float f = f0 + (1.0f - f0) * p5;
+        const float spec = specular_hit ? ((f * g) * vdoth) / (ndoth * vdotn)
+                                        : ((((f * g) * d) * vdoth) * sth) / vdotn;
+        o[i] = (cx[i] * (1.0f - f)) * (1.0f - metallic) + spec;
+    }
+    weights = f3(weights.x * o[0], weights.y * o[1], weights.z * o[2]);
+    w = l;
+}
+
 VPT_DEV void iso_scatter(const TraceParams& P, Rng& rng, F3 p, F3& w, F3& weights) {
     (void)rng_next(rng);  // isoSurfaceOpacity (1) < random() never holds
     F3 n = iso_normal(P, p);
@@ -678,7 +750,11 @@ VPT_DEV void iso_scatter(const TraceParams& P, Rng& rng, F3 p, F3& w, F3& weight
     const F3 t = cross3(b, n);
     const float xi0 = rng_next(rng);
     const float xi1 = rng_next(rng);
-    if (P.iso_brdf != 0) {
+    if (P.iso_brdf == kBrdfCookTorrance) {
+        iso_cook_torrance(P, rng, n, t, b, xi0, xi1, w, weights);
+        return;
+    }
+    if (P.iso_brdf != kBrdfLambertian) {
         // BlinnPhong.glsl / ConstantLighting.glsl: a uniformly sampled hemisphere direction
         // (sampleHemisphere, VptUtils.glsl:1071-1077: phi = 2 pi xi.y, z = xi.x) in the same frame
         const float pi = 3.14159265358979323846f;  // M_PI as the shader's float

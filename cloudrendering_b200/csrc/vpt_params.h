@@ -33,6 +33,13 @@ enum SdtProbability : int { kSdtMax = 0, kSdtAvg = 1, kSdtPathHistory = 2 };
 // kernel variant chosen by the host when the border density is 0; P.grid_kind stays kDense.
 enum GridKind : int { kDense = 0, kNanoVdb = 1, kDenseTex = 2 };
 enum Interp : int { kNearest = 0, kStochastic = 1, kTrilinear = 2 };
+// surface BRDFs of isosurface hits (SurfaceBrdf, RenderSettings.hpp:94-99, without Disney 2012) and
+// the slots of TraceParams::brdf
+enum IsoBrdf : int { kBrdfLambertian = 0, kBrdfBlinnPhong = 1, kBrdfAmbient = 2, kBrdfCookTorrance = 3 };
+enum BrdfParam : int {
+    kBrdfSubsurface = 0, kBrdfMetallic, kBrdfSpecular, kBrdfSpecularTint, kBrdfRoughness,
+    kBrdfAnisotropic, kBrdfSheen, kBrdfSheenTint, kBrdfClearcoat, kBrdfClearcoatGloss, kBrdfParamCount
+};
 enum EnvKind : int { kEnvDefault = 0, kEnvBlack = 1, kEnvSingleColor = 2, kEnvConstantSun = 3, kEnvImage = 4 };
 
 // Error bits written to TraceParams::error_flags (sticky until the host clears them).
@@ -184,7 +191,11 @@ struct TraceParams {
     F3 emission_box_min;
     F3 emission_vox_per_unit;
     float emission_cap, emission_strength;  // the strength also scales transfer-function emission
-    int iso_brdf;              // surface BRDF of isosurface hits: 0 Lambertian, 1 Blinn-Phong, 2 Ambient
+    int iso_brdf;              // surface BRDF of isosurface hits: 0 Lambertian, 1 Blinn-Phong, 2 Ambient,
+                               //   3 Cook-Torrance
+    // setBrdfParameter (VolumetricPathTracingPass.cpp:987-1011): subsurface, metallic, specular,
+    // specular_tint, roughness, anisotropic, sheen, sheen_tint, clearcoat, clearcoat_gloss
+    float brdf[10];
     float tf_albedo_strength;  // spectral trackers with a transfer function: scattering albedo mixed toward
                                //   the table's rgb by this weight (0: off; USE_TRANSFER_FUNCTION_SCATTERING_ALBEDO)
 

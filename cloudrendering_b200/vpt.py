@@ -302,8 +302,16 @@ def set_isosurface_type(_isosurface_type: str) -> None:
 
 
 def set_surface_brdf(_surface_brdf: str) -> None:
-    """"Lambertian" (the only BRDF built; the reference's other names raise); unknown names are ignored."""
+    """"Lambertian", "Blinn Phong", "Cook Torrance" or "Ambient"; "Disney (2012)" raises; unknown names
+    are ignored."""
     _c("vpt_set_surface_brdf", str(_surface_brdf).encode())
+
+
+def set_brdf_parameter(key: str, value: str) -> None:
+    """One BRDF parameter (subsurface, metallic, specular, specular_tint, roughness, anisotropic, sheen,
+    sheen_tint, clearcoat, clearcoat_gloss) from its decimal string; unknown keys are ignored
+    (src/PyTorch/Module.cpp:1196-1199)."""
+    _c("vpt_set_brdf_parameter", str(key).encode(), str(value).encode())
 
 
 def set_num_isosurface_subdivisions(subdivisions: int) -> None:

@@ -44,6 +44,7 @@ class OracleScene(ctypes.Structure):
         ("use_iso", c_int), ("iso_value", c_float), ("iso_color", c_float * 3), ("iso_subdivisions", c_int),
         ("sv_inv_world", c_float * 3), ("sv_local", c_void_p),
         ("env_rot", c_int), ("env_rot_m", c_float * 9), ("tf_albedo_strength", c_float), ("iso_brdf", c_int),
+        ("brdf", c_float * 10),
     ]
 
 

@@ -94,6 +94,8 @@ typedef struct RefScene {
     float env_rot[9];         /* parameters.envMapDirRot, column-major (USE_ENV_MAP_ROTATION variants) */
     float prev_view_proj[16]; /* parameters.previousViewProjMatrix, column-major */
     float tf_albedo_strength; /* parameters.tfScatteringAlbedoStrength */
+    float brdf[10];           /* parameters.subsurface, metallic, specular, specularTint, roughness,
+                                 anisotropic, sheen, sheenTint, clearcoat, clearcoatGloss */
 } RefScene;
 
 int ref_variant_count(void) { return ref_num_variants; }
@@ -169,6 +171,16 @@ int ref_render(int variant, const RefScene* s, float* out_rgba, int threads) {
     p.emissionCap = s->emission_cap;
     p.emissionStrength = s->emission_strength;
     p.tfScatteringAlbedoStrength = s->tf_albedo_strength;
+    p.subsurface = s->brdf[0];
+    p.metallic = s->brdf[1];
+    p.specular = s->brdf[2];
+    p.specularTint = s->brdf[3];
+    p.roughness = s->brdf[4];
+    p.anisotropic = s->brdf[5];
+    p.sheen = s->brdf[6];
+    p.sheenTint = s->brdf[7];
+    p.clearcoat = s->brdf[8];
+    p.clearcoatGloss = s->brdf[9];
     p.isoValue = s->iso_value;
     p.isoSurfaceColor = vec3(s->iso_color[0], s->iso_color[1], s->iso_color[2]);
     g_ref.tf.data = s->tf;

@@ -464,6 +464,10 @@ struct Parameters {
     float isoStepWidth;
     float maxAoDist;
     int numAoSamples;
+    // surface BRDF parameters (VptHeader.glsl:100-111)
+    float subsurface, metallic, specular, specularTint, roughness, anisotropic, sheen, sheenTint;
+    vec3 camForward;
+    float clearcoat, clearcoatGloss;
 };
 struct FrameInfo {
     uint frameCount, globalFrameNumber;

@@ -29,6 +29,8 @@ inline float m_cos(float x) { return g_dr_math ? (float)cos((double)x) : cosf(x)
 inline float m_pow(float x, float y) { return g_dr_math ? (float)pow((double)x, (double)y) : powf(x, y); }
 inline float m_atan2(float y, float x) { return g_dr_math ? (float)atan2((double)y, (double)x) : atan2f(y, x); }
 inline float m_asin(float x) { return g_dr_math ? (float)asin((double)x) : asinf(x); }
+inline float m_acos(float x) { return g_dr_math ? (float)acos((double)x) : acosf(x); }
+inline float m_pow5(float x) { return g_dr_math ? (float)pow((double)x, 5.0) : powf(x, 5.0f); }
 
 struct V3 {
     float x, y, z;
@@ -724,6 +726,63 @@ struct Tracer {
     // included (VptUtils.glsl:1121) before UNIFORM_SAMPLING is defined (:1144), so it samples the
     // cosine-weighted hemisphere through the concentric disk map (VptUtils.glsl:1078-1098) and its
     // pdf factor is the cosine itself
+    // CookTorrance.glsl computeBrdf = sampleBrdf + evaluateBrdf (no division by the lobe probability):
+    // sel picks sample_GGX (theta = acos(sqrt((1 - u) / (u (a^2 - 1) + 1))), reflected about the half
+    // vector) over sample_Lambertian (theta = asin(sqrt(u))); the value is the diffuse colour
+    // (1 - F)(1 - metallic) plus F G v.h / (n.h v.n) (GGX sample) or F G D v.h sin(theta_h) / v.n
+    V3 frame(V3 t, V3 b, V3 n, float x, float y, float z) const {
+        return v3((t.x * x + b.x * y) + n.x * z, (t.y * x + b.y * y) + n.y * z, (t.z * x + b.z * y) + n.z * z);
+    }
+    void cook_torrance(V3 n, V3 t, V3 b, float sel, float u, V3& w, V3& weights, Rng& r) {
+        const float pi = 3.14159265358979323846f;
+        const float v = rnd(r);
+        const float metallic = S.brdf[1], specular = S.brdf[2];
+        const float rough = std::min(std::max(S.brdf[4], 0.05f), 1.0f);
+        const float specular_w = metallic + (1.0f - rough) * (1.0f + specular);
+        const float diffuse_w = 1.0f - metallic;
+        const float specular_p = specular_w * (1.0f / (specular_w + diffuse_w));
+        const V3 view = normalize(neg(w));
+        const float alpha = rough * rough, alpha2 = alpha * alpha;
+        const bool specular_hit = sel < specular_p;
+        const float phi = (2.0f * pi) * v;
+        V3 l;
+        if (specular_hit) {
+            const float theta = m_acos(sqrtf((1.0f - u) / (u * (alpha2 - 1.0f) + 1.0f)));
+            const float st = m_sin(theta);
+            const V3 h = frame(t, b, n, st * m_cos(phi), st * m_sin(phi), m_cos(theta));
+            const float vh = fabsf(dot(view, h));
+            const float s = 2.0f * (vh > 0.001f ? vh : 0.001f);
+            l = v3(s * h.x - view.x, s * h.y - view.y, s * h.z - view.z);
+        } else {
+            const float theta = m_asin(sqrtf(u));
+            const float st = m_sin(theta);
+            l = frame(t, b, n, st * m_cos(phi), st * m_sin(phi), m_cos(theta));
+        }
+        const V3 h = normalize(add(l, view));
+        const float ndoth = dot(h, n), vdotn = dot(view, n), ldotn = dot(l, n), vdoth = dot(view, h);
+        const float f0s = 0.16f * (specular * specular);
+        const float p5 = m_pow5(1.0f - vdoth);
+        const float k = alpha / 2.0f;
+        const float gl = ldotn < 0.001f ? 0.001f : ldotn, gv = vdotn < 0.001f ? 0.001f : vdotn;
+        const float g = (gl / (gl * (1.0f - k) + k)) * (gv / (gv * (1.0f - k) + k));
+        float d = 0.0f, sth = 0.0f;
+        if (!specular_hit) {
+            const float bq = (ndoth * ndoth) * (alpha2 - 1.0f) + 1.0f;
+            d = ((1.0f / pi) * alpha2) / (bq * bq);
+            sth = sqrtf(1.0f - std::min(ndoth * ndoth, 0.95f));
+        }
+        float o[3];
+        for (int i = 0; i < 3; ++i) {
+            const float c = S.iso_color[i];
+            const float f0 = f0s * (1.0f - metallic) + c * metallic;
+            const float f = f0 + (1.0f - f0) * p5;
+            const float spec = specular_hit ? ((f * g) * vdoth) / (ndoth * vdotn)
+                                            : ((((f * g) * d) * vdoth) * sth) / vdotn;
+            o[i] = (c * (1.0f - f)) * (1.0f - metallic) + spec;
+        }
+        weights = v3(weights.x * o[0], weights.y * o[1], weights.z * o[2]);
+        w = l;
+    }
     void iso_scatter(V3 p, V3& w, V3& weights, Rng& r) {
         (void)rnd(r);  // isoSurfaceOpacity (1) < random() never holds
         V3 n = iso_normal(p);
@@ -733,6 +792,10 @@ struct Tracer {
                                                      : v3(-n.x * n.z, yz, 1.0f - n.z * n.z));
         const V3 t = cross(b, n);
         const float xi0 = rnd(r), xi1 = rnd(r);
+        if (S.iso_brdf == 3) {
+            cook_torrance(n, t, b, xi0, xi1, w, weights, r);
+            return;
+        }
         if (S.iso_brdf != 0) {
             // BlinnPhong.glsl / ConstantLighting.glsl: sampleHemisphere (VptUtils.glsl:1071-1077), uniform
             const float pi = 3.14159265358979323846f;

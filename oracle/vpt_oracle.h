@@ -88,8 +88,12 @@ typedef struct OracleScene {
     /* USE_TRANSFER_FUNCTION_SCATTERING_ALBEDO (spectral trackers with a transfer function): the
      * scattering albedo is mixed toward the table's rgb by this weight when it is > 0 */
     float tf_albedo_strength;
-    /* surface BRDF of isosurface hits: 0 Lambertian, 1 Blinn-Phong, 2 Ambient (ConstantLighting) */
+    /* surface BRDF of isosurface hits: 0 Lambertian, 1 Blinn-Phong, 2 Ambient (ConstantLighting),
+     * 3 Cook-Torrance */
     int iso_brdf;
+    /* setBrdfParameter values: subsurface, metallic, specular, specular_tint, roughness, anisotropic,
+     * sheen, sheen_tint, clearcoat, clearcoat_gloss */
+    float brdf[10];
 } OracleScene;
 
 /* Renders width*height*num_frames paths; adds radiance (and its square) per pixel (3 doubles). */

@@ -122,6 +122,13 @@ def cases():
         kw2 = dict(base)
         kw2.update(iso_value=0.3, iso_color=(0.9, 0.6, 0.3), extinction=40.0, albedo=0.9, g=0.2)
         out["fbm_" + name] = SceneSpec(grid=fbm, mode="delta", interp="trilinear", iso=True, iso_brdf=brdf, **kw2)
+    # Cook-Torrance with the pass's default parameters and with a glossier, partly metallic surface
+    for name, params in {"delta_iso_cook": None,
+                         "delta_iso_cook_metal": {"metallic": 0.6, "specular": 0.8, "roughness": 0.25}}.items():
+        kw2 = dict(base)
+        kw2.update(iso_value=0.3, iso_color=(0.9, 0.6, 0.3), extinction=40.0, albedo=0.9, g=0.2)
+        out["fbm_" + name] = SceneSpec(grid=fbm, mode="delta", interp="trilinear", iso=True, iso_brdf="Cook Torrance",
+                                       brdf_params=params, **kw2)
     return out
 
 
@@ -150,7 +157,7 @@ FIELDS = ["mode", "interp", "extinction", "albedo", "g", "width", "height", "see
           "sun_dir", "sun_intensity", "cam_pos", "cam_target", "fovy", "near", "far", "max_grid_extent", "use_ess",
           "env_intensity", "max_bounces", "ess_ref_compat", "lights", "extinction_base", "albedo_rgb", "sdt_prob",
           "emission_cap", "emission_strength", "iso", "iso_value", "iso_color", "env_rot", "tf_albedo_strength",
-          "iso_brdf"]
+          "iso_brdf", "brdf_params"]
 
 
 def depth_map_cases():

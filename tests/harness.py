@@ -70,13 +70,25 @@ class SceneSpec:
                  use_ess=False, env_intensity=(1.0, 1.0, 1.0), ess_ref_compat=False, lights=None,
                  extinction_base=(1.0, 1.0, 1.0), albedo_rgb=None, sdt_prob=2, emission=None, emission_cap=1.0,
                  emission_strength=1.0, tf=None, iso=False, iso_value=0.5, iso_color=(0.4, 0.4, 0.4), env_rot=None,
-                 tf_albedo_strength=0.0, iso_brdf="Lambertian"):
+                 tf_albedo_strength=0.0, iso_brdf="Lambertian", brdf_params=None):
         self.__dict__.update(locals())
         del self.__dict__["self"]
 
 
 LIGHT_TYPES = ["Point Light", "Spotlight", "Directional Light"]
-ISO_BRDFS = {"Lambertian": 0, "Blinn Phong": 1, "Ambient": 2}
+ISO_BRDFS = {"Lambertian": 0, "Blinn Phong": 1, "Ambient": 2, "Cook Torrance": 3}
+# setBrdfParameter keys in slot order, with the pass's defaults (VolumetricPathTracingPass.hpp:410-419)
+BRDF_KEYS = ["subsurface", "metallic", "specular", "specular_tint", "roughness", "anisotropic", "sheen",
+             "sheen_tint", "clearcoat", "clearcoat_gloss"]
+BRDF_DEFAULTS = [0.0, 0.0, 0.5, 0.0, 0.5, 0.0, 0.0, 0.5, 0.0, 1.0]
+
+
+def brdf_values(sp):
+    """The ten BRDF parameters of a SceneSpec as float32 values."""
+    vals = list(BRDF_DEFAULTS)
+    for k, v in (sp.brdf_params or {}).items():
+        vals[BRDF_KEYS.index(k)] = v
+    return [float(np.float32(v)) for v in vals]
 LIGHT_SPACES = ["World", "View", "View Orientation"]
 LIGHT_DEFAULTS = dict(type="Point Light", space="View", spot_total_width=0.0981747704, spot_falloff_start=0.0245436926,
                       color=(1.0, 0.961538462, 0.884615385), intensity=0.5, position=(0.0, 0.0, 0.0), use_distance=1,
@@ -156,6 +168,8 @@ def setup_core(core: Core, sp: SceneSpec):
     core("vpt_set_tf_scattering_albedo_strength", float(sp.tf_albedo_strength))
     core("vpt_set_use_isosurfaces", 1 if sp.iso else 0)
     core("vpt_set_surface_brdf", sp.iso_brdf.encode())
+    for k, v in zip(BRDF_KEYS, brdf_values(sp)):
+        core("vpt_set_brdf_parameter", k.encode(), repr(v).encode())
     core("vpt_set_iso_value", sp.iso_value)
     core("vpt_set_iso_surface_color", *[float(c) for c in sp.iso_color])
     core("vpt_set_resolution", sp.width, sp.height)
@@ -322,6 +336,7 @@ def oracle_scene(core, sp: SceneSpec, frames: int, frame_count: int = 0) -> brid
         sc.set("iso_subdivisions", 2)
         sc.set("interp", 2)
         sc.set("iso_brdf", ISO_BRDFS[sp.iso_brdf])
+        sc.set("brdf", brdf_values(sp))
     sc.set("iso_value", float(np.float32(sp.iso_value)))
     sc.set("iso_color", [float(np.float32(c)) for c in sp.iso_color])
     if sp.env_rot is not None and sp.env == "image":
@@ -479,7 +494,9 @@ def reference_scene(sp: SceneSpec, frames: int, frame_start: int = 0, inv=None):
     sc.set("iso_value", sp.iso_value)
     sc.set("iso_color", sp.iso_color)
     if sp.iso:
-        tracker += {"Lambertian": "_iso", "Blinn Phong": "_iso_blinn", "Ambient": "_iso_ambient"}[sp.iso_brdf]
+        tracker += {"Lambertian": "_iso", "Blinn Phong": "_iso_blinn", "Ambient": "_iso_ambient",
+                    "Cook Torrance": "_iso_cook"}[sp.iso_brdf]
+        sc.set("brdf", brdf_values(sp))
     if sp.env_rot is not None:
         sc.set("env_rot", [float(np.float32(v)) for v in sp.env_rot])
         tracker += "_rot"

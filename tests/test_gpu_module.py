@@ -186,7 +186,7 @@ def test_transfer_function_table():
     vpt.set_use_builtin_environment_map("Default")
 
 
-def test_isosurfaces():
+def _check_isosurfaces():
     """set_use_isosurfaces and its settings: an iso value above every density finds no surface, so
     the image equals the trilinear render without isosurfaces bit for bit; a surface inside the cloud
     changes it; the types, BRDFs and trackers that are not built raise."""
@@ -212,8 +212,17 @@ def test_isosurfaces():
     assert not torch.allclose(surf, plain, rtol=1e-3)
     with pytest.raises(RuntimeError, match="not built"):
         vpt.set_isosurface_type("Gradient")
-    with pytest.raises(RuntimeError, match="Lambertian"):
-        vpt.set_surface_brdf("Cook Torrance")
+    for brdf in ("Blinn Phong", "Cook Torrance", "Ambient", "Lambertian"):
+        vpt.set_surface_brdf(brdf)
+        vpt.set_seed_offset(0)
+        assert torch.isfinite(vpt.render_frame(t, 1)).all()
+    vpt.set_brdf_parameter("roughness", "0.3")
+    vpt.set_brdf_parameter("no_such_key", "1")  # ignored, as in the reference
+    with pytest.raises(RuntimeError, match="number"):
+        vpt.set_brdf_parameter("metallic", "abc")
+    vpt.set_brdf_parameter("roughness", "0.5")
+    with pytest.raises(RuntimeError, match="Disney"):
+        vpt.set_surface_brdf("Disney (2012)")
     with pytest.raises(RuntimeError):
         vpt.set_iso_surface_color([0.1, 0.2])
     vpt.set_vpt_mode_from_name("Next Event Tracking")
@@ -223,7 +232,18 @@ def test_isosurfaces():
     vpt.set_iso_value(0.5)
     vpt.set_vpt_mode_from_name("Delta Tracking")
     vpt.set_grid_interpolation("Stochastic")
-    vpt.set_extinction_scale(1024.0)
+
+
+def test_isosurfaces():
+    try:
+        _check_isosurfaces()
+    finally:  # the module's state outlives the test: leave the defaults behind even after a failure
+        vpt.set_use_isosurfaces(False)
+        vpt.set_surface_brdf("Lambertian")
+        vpt.set_iso_value(0.5)
+        vpt.set_vpt_mode_from_name("Delta Tracking")
+        vpt.set_grid_interpolation("Stochastic")
+        vpt.set_extinction_scale(1024.0)
 
 
 def test_load_xyz_file_grid_and_bounds(tmp_path):
