@@ -160,7 +160,8 @@ struct VptContext {
     bool use_emission = false;
     float emission_cap = 1.0f, emission_strength = 1.0f;
     float tf_albedo_strength = 0.0f;  // setTfScatteringAlbedoStrength
-    int iso_brdf = 0;                 // setSurfaceBrdf: 0 Lambertian, 1 Blinn Phong, 2 Ambient, 3 Cook Torrance
+    int iso_brdf = 0;                 // setSurfaceBrdf: 0 Lambertian, 1 Blinn Phong, 2 Ambient, 3 Cook Torrance,
+                                      //   4 Disney (2012)
     // setBrdfParameter, in BrdfParam order; defaults of VolumetricPathTracingPass.hpp:410-419
     float brdf[vpt::kBrdfParamCount] = {0.0f, 0.0f, 0.5f, 0.0f, 0.5f, 0.0f, 0.0f, 0.5f, 0.0f, 1.0f};
     // transfer function (set_use_transfer_function; the RGBA table of transferFunctionTexture)
@@ -1124,8 +1125,7 @@ VptStatus vpt_set_surface_brdf(VptContext* ctx, const char* name) {
     if (strcmp(name, "Blinn Phong") == 0) brdf = 1;
     if (strcmp(name, "Ambient") == 0) brdf = 2;
     if (strcmp(name, "Cook Torrance") == 0) brdf = 3;
-    if (strcmp(name, "Disney (2012)") == 0)
-        return fail(ctx, VPT_ERR_UNSUPPORTED, "the Disney (2012) surface BRDF is not built in this core");
+    if (strcmp(name, "Disney (2012)") == 0) brdf = 4;
     if (brdf < 0) return VPT_OK;  // unknown names are ignored, as in the reference
     if (brdf != ctx->iso_brdf) reset_film_state(ctx);
     ctx->iso_brdf = brdf;

@@ -39,6 +39,7 @@ VPT_DEV float m_pow(float x, float y) { return (float)pow((double)x, (double)y);
 VPT_DEV float m_atan2(float y, float x) { return (float)atan2((double)y, (double)x); }
 VPT_DEV float m_asin(float x) { return (float)asin((double)x); }
 VPT_DEV float m_acos(float x) { return (float)acos((double)x); }
+VPT_DEV float m_tan(float x) { return (float)tan((double)x); }
 VPT_DEV float m_pow5(float x) { return (float)pow((double)x, 5.0); }
 #elif defined(VPT_FAST_MATH)
 // The product's tracer units (vpt_trace_*.cu): the special-function unit's approximations of log2,
@@ -54,6 +55,7 @@ VPT_DEV float m_pow(float x, float y) { return __powf(x, y); }
 VPT_DEV float m_atan2(float y, float x) { return atan2f(y, x); }
 VPT_DEV float m_asin(float x) { return asinf(x); }
 VPT_DEV float m_acos(float x) { return acosf(x); }
+VPT_DEV float m_tan(float x) { return tanf(x); }  // near its poles (Disney's anisotropic sampling) __tanf is far off
 // pow(x, 5.0) of the Fresnel term: its base 1 - cos can round to a tiny negative value, which the
 // exp2(5 log2 x) form of __powf would turn into NaN
 VPT_DEV float m_pow5(float x) { const float x2 = x * x; return x2 * x2 * x; }
@@ -66,6 +68,7 @@ VPT_DEV float m_pow(float x, float y) { return powf(x, y); }
 VPT_DEV float m_atan2(float y, float x) { return atan2f(y, x); }
 VPT_DEV float m_asin(float x) { return asinf(x); }
 VPT_DEV float m_acos(float x) { return acosf(x); }
+VPT_DEV float m_tan(float x) { return tanf(x); }
 VPT_DEV float m_pow5(float x) { return powf(x, 5.0f); }
 #endif
 
@@ -740,6 +743,129 @@ VPT_DEV void iso_cook_torrance(const TraceParams& P, Rng& rng, F3 n, F3 t, F3 b,
     w = l;
 }
 
+// Disney2012.glsl computeBrdf: sampleBrdf picks the anisotropic specular lobe (weight metallic +
+// (1 + specular)(1 - roughness)), the diffuse lobe ((1 - metallic)(1 + roughness) + subsurface) or the
+// clearcoat lobe (clamp(clearcoat, 0, 1)); evaluateBrdf returns diffuse + specular + clearcoat as the
+// shader writes them (its cos-of-a-cosine Fresnel arguments and its D term included), and the throughput
+// takes that value as it is.  sel, u are the hit's second and third random numbers.
+VPT_DEV void iso_disney(const TraceParams& P, Rng& rng, F3 n, F3 t, F3 b, float sel, float u, F3& w, F3& weights) {
+    const float pi = 3.14159265358979323846f;  // M_PI
+    const float pi_c = 3.14159265359f;         // PI (VptUtils.glsl:27), used by GTR1 and atan2
+    const float* q = P.brdf;
+    const float roughness = q[kBrdfRoughness], metallic = q[kBrdfMetallic];
+    const float aspect = sqrtf(1.0f - q[kBrdfAnisotropic] * 0.9f);
+    const float r2 = roughness * roughness;
+    const float ax0 = r2 / aspect, ay0 = r2 * aspect;
+    const float ax = 0.001f < ax0 ? ax0 : 0.001f, ay = 0.001f < ay0 ? ay0 : 0.001f;
+    // sampleBrdf
+    const float specular_w = metallic + (1.0f + q[kBrdfSpecular]) * (1.0f - roughness);
+    const float diffuse_w = (1.0f - metallic) * (1.0f + roughness) + q[kBrdfSubsurface];
+    const float clearcoat_w = fminf(fmaxf(q[kBrdfClearcoat], 0.0f), 1.0f);
+    const float norm = 1.0f / ((specular_w + diffuse_w) + clearcoat_w);
+    const float specular_p = specular_w * norm, diffuse_p = diffuse_w * norm;
+    const F3 view = normalize3(f3(-w.x, -w.y, -w.z));
+    const float v0 = rng_next(rng);
+    const int lobe = sel < specular_p ? 0 : (sel < specular_p + diffuse_p ? 1 : 2);  // specular, diffuse, clearcoat
+    const bool specular_hit = lobe != 1, clearcoat_hit = lobe == 2;
+    float th;
+    F3 h, l;
+    if (lobe == 0) {  // sample_specular_disney
+        const float us = fminf(fmaxf(u, 0.05f), 0.95f), vs = fminf(fmaxf(v0, 0.05f), 0.95f);
+        const float a = (2.0f * pi) * us;
+        const float y = ay * m_tan(a);
+        // the shader's own atan2 (Disney2012.glsl): atan(y, x) when |x| > |y|, else PI / 2 - atan(x, y)
+        const float phi = fabsf(ax) > fabsf(y) ? m_atan2(y, ax) : pi_c / 2.0f - m_atan2(ax, y);
+        const float cp = m_cos(phi), sp = m_sin(phi);
+        th = m_acos(sqrtf((1.0f - vs) / (1.0f + ((cp * cp) / (ax * ax) + (sp * sp) / (ay * ay)) * vs)));
+        const float sq = sqrtf(vs / (1.0f - vs));
+        const float ca = ax * m_cos(a), sa = ay * m_sin(a);
+        const F3 m = f3(ca * t.x + sa * b.x, ca * t.y + sa * b.y, ca * t.z + sa * b.z);
+        h = normalize3(f3(sq * m.x + n.x, sq * m.y + n.y, sq * m.z + n.z));
+    } else {
+        const float phi = (2.0f * pi) * v0;
+        float cth;
+        if (!clearcoat_hit) {  // sample_diffuse_disney
+            th = m_asin(sqrtf(u));
+            cth = m_cos(th);
+        } else {  // sample_clearcoat_disney with alpha = mix(0.1, 0.001, clearcoatGloss)
+            const float g = q[kBrdfClearcoatGloss];
+            const float alpha = 0.1f * (1.0f - g) + 0.001f * g;
+            const float alpha2 = alpha * alpha;
+            th = m_acos(sqrtf((1.0f - m_pow(alpha2, 1.0f - u)) / (1.0f - alpha2)));
+            cth = m_cos(th);
+        }
+        const float st = m_sin(th);
+        h = iso_frame(t, b, n, st * m_cos(phi), st * m_sin(phi), cth);
+    }
+    if (specular_hit) {
+        const float vh = fabsf(dot3(view, h));
+        const float s = 2.0f * (vh > 0.001f ? vh : 0.001f);  // avoidZero(v.h, 0.001)
+        l = f3(s * h.x - view.x, s * h.y - view.y, s * h.z - view.z);
+    } else {
+        l = h;  // the diffuse lobe samples the direction itself
+    }
+    // evaluateBrdf
+    const F3 hh = normalize3(f3(l.x + view.x, l.y + view.y, l.z + view.z));
+    const float cos_h = dot3(hh, n), cos_d = dot3(l, hh), cos_v = dot3(view, n), cos_l = dot3(l, n);
+    const float vdoth = dot3(view, hh);
+    const float c[3] = {P.iso_color.x, P.iso_color.y, P.iso_color.z};
+    const float lum = (0.3f * c[0] + 0.6f * c[1]) + 0.1f * c[2];
+    const float cd = m_cos(cos_d);
+    const float cd2 = cd * cd;  // pow(x, 2) of a positive x
+    const float f_d90 = 0.5f + (2.0f * roughness) * cd2;
+    const float pl = m_pow5(1.0f - m_cos(cos_l)), pv = m_pow5(1.0f - m_cos(cos_v));
+    const float f_d = (1.0f + (f_d90 - 1.0f) * pl) * (1.0f + (f_d90 - 1.0f) * pv);
+    const float fss90 = roughness * cd2;
+    const float f_ss = (1.0f + (fss90 - 1.0f) * pl) * (1.0f + (fss90 - 1.0f) * pv);
+    const float lv = cos_l + cos_v;
+    const float f_dss = 1.25f * (f_ss * (1.0f / (lv < 0.001f ? 0.001f : lv) - 0.5f) + 0.5f);
+    const float f_h = m_pow5(1.0f - cos_d);
+    const float sub = q[kBrdfSubsurface];
+    const float fd_mix = f_d * (1.0f - sub) + f_dss * sub;
+    const float dx = dot3(t, hh) / ax, dy = dot3(b, hh) / ay;
+    const float dd = dx * dx + dy * dy;
+    const float d_spec = 1.0f / (((pi * ax) * ay) * (dd * dd) + cos_h * cos_h);
+    const float glx = dot3(t, l) * ax, gly = dot3(b, l) * ay, gvx = dot3(t, view) * ax, gvy = dot3(b, view) * ay;
+    float g_spec = 1.0f / (cos_v + sqrtf((glx * glx + gly * gly) + cos_v * cos_v));
+    g_spec = g_spec * (1.0f / (cos_v + sqrtf((gvx * gvx + gvy * gvy) + cos_v * cos_v)));
+    const float sin_th = m_sin(th);
+    const float f_cc = 0.04f * (1.0f - f_h) + 1.0f * f_h;
+    const float gloss = q[kBrdfClearcoatGloss];
+    const float a_cc = 0.1f * (1.0f - gloss) + 0.001f * gloss;
+    float d_cc;  // GTR1(cos_h, a_cc)
+    if (a_cc >= 1.0f) {
+        d_cc = 1.0f / pi_c;
+    } else {
+        const float a2 = a_cc * a_cc;
+        d_cc = (a2 - 1.0f) / ((pi_c * m_log(a2)) * (1.0f + ((a2 - 1.0f) * cos_h) * cos_h));
+    }
+    const float bl = cos_l * cos_l, bv = cos_v * cos_v, ag = 0.25f * 0.25f;
+    const float g_cc = (1.0f / ((cos_l < -0.99f ? -0.99f : cos_l) + sqrtf((ag + bl) - ag * bl))) *
+                       (1.0f / ((cos_v < -0.99f ? -0.99f : cos_v) + sqrtf((ag + bv) - ag * bv)));
+    const float cc = q[kBrdfClearcoat];
+    const float clear = (specular_hit && clearcoat_hit)
+                            ? (((((cc * f_cc) * g_cc) * cos_l) * vdoth) * sin_th) / cos_h
+                            : ((((((cc * f_cc) * d_cc) * g_cc) * cos_l) * vdoth) * sin_th);
+    const float st = q[kBrdfSpecularTint], sh = q[kBrdfSheenTint];
+    const float spec_scale = q[kBrdfSpecular] * 0.08f;
+    float o[3];
+    for (int i = 0; i < 3; ++i) {
+        const float tint = lum > 0.0f ? c[i] / lum : 1.0f;
+        const float spec0 = (spec_scale * (1.0f * (1.0f - st) + tint * st)) * (1.0f - metallic) + c[i] * metallic;
+        const float sheen_c = 1.0f * (1.0f - sh) + tint * sh;
+        const float sheen = (f_h * q[kBrdfSheen]) * sheen_c;
+        float diffuse = (c[i] * fd_mix + sheen) * (1.0f - metallic);
+        if (specular_hit) diffuse = diffuse * (1.0f / pi);
+        const float f_spec = spec0 * (1.0f - f_h) + 1.0f * f_h;
+        const float spec = (specular_hit && !clearcoat_hit)
+                               ? (((((f_spec * g_spec) * 4.0f) * cos_l) * vdoth) * sin_th) / cos_h
+                               : ((((((f_spec * d_spec) * g_spec) * 4.0f) * cos_l) * vdoth) * sin_th);
+        o[i] = (diffuse + spec) + clear;
+    }
+    weights = f3(weights.x * o[0], weights.y * o[1], weights.z * o[2]);
+    w = l;
+}
+
 VPT_DEV void iso_scatter(const TraceParams& P, Rng& rng, F3 p, F3& w, F3& weights) {
     (void)rng_next(rng);  // isoSurfaceOpacity (1) < random() never holds
     F3 n = iso_normal(P, p);
@@ -752,6 +878,10 @@ VPT_DEV void iso_scatter(const TraceParams& P, Rng& rng, F3 p, F3& w, F3& weight
     const float xi1 = rng_next(rng);
     if (P.iso_brdf == kBrdfCookTorrance) {
         iso_cook_torrance(P, rng, n, t, b, xi0, xi1, w, weights);
+        return;
+    }
+    if (P.iso_brdf == kBrdfDisney) {
+        iso_disney(P, rng, n, t, b, xi0, xi1, w, weights);
         return;
     }
     if (P.iso_brdf != kBrdfLambertian) {

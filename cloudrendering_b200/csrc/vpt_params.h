@@ -33,9 +33,11 @@ enum SdtProbability : int { kSdtMax = 0, kSdtAvg = 1, kSdtPathHistory = 2 };
 // kernel variant chosen by the host when the border density is 0; P.grid_kind stays kDense.
 enum GridKind : int { kDense = 0, kNanoVdb = 1, kDenseTex = 2 };
 enum Interp : int { kNearest = 0, kStochastic = 1, kTrilinear = 2 };
-// surface BRDFs of isosurface hits (SurfaceBrdf, RenderSettings.hpp:94-99, without Disney 2012) and
-// the slots of TraceParams::brdf
-enum IsoBrdf : int { kBrdfLambertian = 0, kBrdfBlinnPhong = 1, kBrdfAmbient = 2, kBrdfCookTorrance = 3 };
+// surface BRDFs of isosurface hits (SurfaceBrdf, RenderSettings.hpp:94-99, numbered in this core's
+// order) and the slots of TraceParams::brdf
+enum IsoBrdf : int {
+    kBrdfLambertian = 0, kBrdfBlinnPhong = 1, kBrdfAmbient = 2, kBrdfCookTorrance = 3, kBrdfDisney = 4
+};
 enum BrdfParam : int {
     kBrdfSubsurface = 0, kBrdfMetallic, kBrdfSpecular, kBrdfSpecularTint, kBrdfRoughness,
     kBrdfAnisotropic, kBrdfSheen, kBrdfSheenTint, kBrdfClearcoat, kBrdfClearcoatGloss, kBrdfParamCount
@@ -191,8 +193,7 @@ struct TraceParams {
     F3 emission_box_min;
     F3 emission_vox_per_unit;
     float emission_cap, emission_strength;  // the strength also scales transfer-function emission
-    int iso_brdf;              // surface BRDF of isosurface hits: 0 Lambertian, 1 Blinn-Phong, 2 Ambient,
-                               //   3 Cook-Torrance
+    int iso_brdf;              // surface BRDF of isosurface hits (IsoBrdf)
     // setBrdfParameter (VolumetricPathTracingPass.cpp:987-1011): subsurface, metallic, specular,
     // specular_tint, roughness, anisotropic, sheen, sheen_tint, clearcoat, clearcoat_gloss
     float brdf[10];

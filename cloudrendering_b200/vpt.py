@@ -302,8 +302,8 @@ def set_isosurface_type(_isosurface_type: str) -> None:
 
 
 def set_surface_brdf(_surface_brdf: str) -> None:
-    """"Lambertian", "Blinn Phong", "Cook Torrance" or "Ambient"; "Disney (2012)" raises; unknown names
-    are ignored."""
+    """"Lambertian", "Blinn Phong", "Disney (2012)", "Cook Torrance" or "Ambient"; unknown names are
+    ignored."""
     _c("vpt_set_surface_brdf", str(_surface_brdf).encode())
 
 

@@ -151,9 +151,9 @@ VptStatus vpt_set_tf_scattering_albedo_strength(VptContext* ctx, float strength)
  * of colour iso_surface_color (default 0.4 0.4 0.4) with the selected BRDF; lookups are trilinear
  * while isosurfaces are on.  Built for delta tracking on dense grids: other trackers, sparse grids, a
  * transfer function and batched rendering return VPT_ERR_UNSUPPORTED.  Type "Density" and the BRDFs
- * "Lambertian" (Lambertian.glsl, the default), "Blinn Phong" (BlinnPhong.glsl), "Cook Torrance"
- * (CookTorrance.glsl) and "Ambient" (ConstantLighting.glsl) are accepted, "Gradient" and
- * "Disney (2012)" return VPT_ERR_UNSUPPORTED, unknown names are ignored (as in the reference).
+ * "Lambertian" (Lambertian.glsl, the default), "Blinn Phong" (BlinnPhong.glsl), "Disney (2012)"
+ * (Disney2012.glsl), "Cook Torrance" (CookTorrance.glsl) and "Ambient" (ConstantLighting.glsl) are
+ * accepted, "Gradient" returns VPT_ERR_UNSUPPORTED, unknown names are ignored (as in the reference).
  * vpt_set_num_isosurface_subdivisions is the pass's own setting (VolumetricPathTracingPass.cpp:1028-1033,
  * default 2, 1..8).
  * vpt_set_brdf_parameter replaces set_brdf_parameter (src/PyTorch/Module.cpp:1196-1199,
@@ -161,7 +161,7 @@ VptStatus vpt_set_tf_scattering_albedo_strength(VptContext* ctx, float strength)
  * roughness, anisotropic, sheen, sheen_tint, clearcoat, clearcoat_gloss (defaults 0, 0, 0.5, 0, 0.5, 0,
  * 0, 0.5, 0, 1), value a decimal string; unknown keys are ignored, the film restarts either way, a
  * value that is not a number returns VPT_ERR_ARG.  Cook-Torrance reads metallic, specular and
- * roughness. */
+ * roughness; Disney (2012) reads all ten. */
 VptStatus vpt_set_use_isosurfaces(VptContext* ctx, int use);
 VptStatus vpt_set_iso_value(VptContext* ctx, double value);
 VptStatus vpt_set_iso_surface_color(VptContext* ctx, double r, double g, double b);

@@ -126,10 +126,10 @@ def variants():
     # (VolumetricPathTracingPass.cpp:117-120)
     out.append(("delta_iso__trilinear__default__linear", TRACKERS["delta"] + [INTERPS["trilinear"]]
                 + ENVS["default__linear"] + ISO, 0))
-    # the Blinn-Phong, Cook-Torrance and constant-lighting surface BRDFs (Data/Shaders/BRDF/BlinnPhong.glsl,
-    # CookTorrance.glsl, ConstantLighting.glsl)
+    # the Blinn-Phong, Cook-Torrance, Disney (2012) and constant-lighting surface BRDFs
+    # (Data/Shaders/BRDF/BlinnPhong.glsl, CookTorrance.glsl, Disney2012.glsl, ConstantLighting.glsl)
     for tag, define in (("blinn", "SURFACE_BRDF_BLINN_PHONG"), ("ambient", "SURFACE_BRDF_AMBIENT"),
-                        ("cook", "SURFACE_BRDF_COOK_TORRANCE")):
+                        ("cook", "SURFACE_BRDF_COOK_TORRANCE"), ("disney", "SURFACE_BRDF_DISNEY")):
         out.append((f"delta_iso_{tag}__trilinear__default__linear", TRACKERS["delta"] + [INTERPS["trilinear"]]
                     + ENVS["default__linear"] + [define if d == "SURFACE_BRDF_LAMBERTIAN" else d for d in ISO], 0))
     return out

@@ -30,6 +30,7 @@ inline float m_pow(float x, float y) { return g_dr_math ? (float)pow((double)x, 
 inline float m_atan2(float y, float x) { return g_dr_math ? (float)atan2((double)y, (double)x) : atan2f(y, x); }
 inline float m_asin(float x) { return g_dr_math ? (float)asin((double)x) : asinf(x); }
 inline float m_acos(float x) { return g_dr_math ? (float)acos((double)x) : acosf(x); }
+inline float m_tan(float x) { return g_dr_math ? (float)tan((double)x) : tanf(x); }
 inline float m_pow5(float x) { return g_dr_math ? (float)pow((double)x, 5.0) : powf(x, 5.0f); }
 
 struct V3 {
@@ -783,6 +784,116 @@ struct Tracer {
         weights = v3(weights.x * o[0], weights.y * o[1], weights.z * o[2]);
         w = l;
     }
+    // Disney2012.glsl computeBrdf = sampleBrdf + evaluateBrdf, its terms as the shader writes them:
+    // lobes specular (metallic + (1 + specular)(1 - roughness)), diffuse ((1 - metallic)(1 + roughness)
+    // + subsurface) and clearcoat (clamp(clearcoat, 0, 1)); the value is diffuse + specular + clearcoat
+    void disney(V3 n, V3 t, V3 b, float sel, float u, V3& w, V3& weights, Rng& r) {
+        const float pi = 3.14159265358979323846f, pi_c = 3.14159265359f;
+        const float* q = S.brdf;
+        const float roughness = q[4], metallic = q[1];
+        const float aspect = sqrtf(1.0f - q[5] * 0.9f);
+        const float r2 = roughness * roughness;
+        const float ax0 = r2 / aspect, ay0 = r2 * aspect;
+        const float ax = 0.001f < ax0 ? ax0 : 0.001f, ay = 0.001f < ay0 ? ay0 : 0.001f;
+        const float specular_w = metallic + (1.0f + q[2]) * (1.0f - roughness);
+        const float diffuse_w = (1.0f - metallic) * (1.0f + roughness) + q[0];
+        const float clearcoat_w = std::min(std::max(q[8], 0.0f), 1.0f);
+        const float norm = 1.0f / ((specular_w + diffuse_w) + clearcoat_w);
+        const float specular_p = specular_w * norm, diffuse_p = diffuse_w * norm;
+        const V3 view = normalize(neg(w));
+        const float v0 = rnd(r);
+        const int lobe = sel < specular_p ? 0 : (sel < specular_p + diffuse_p ? 1 : 2);
+        const bool specular_hit = lobe != 1, clearcoat_hit = lobe == 2;
+        float th;
+        V3 h, l;
+        if (lobe == 0) {  // sample_specular_disney
+            const float us = std::min(std::max(u, 0.05f), 0.95f), vs = std::min(std::max(v0, 0.05f), 0.95f);
+            const float a = (2.0f * pi) * us;
+            const float y = ay * m_tan(a);
+            const float phi = fabsf(ax) > fabsf(y) ? m_atan2(y, ax) : pi_c / 2.0f - m_atan2(ax, y);
+            const float cp = m_cos(phi), sp = m_sin(phi);
+            th = m_acos(sqrtf((1.0f - vs) / (1.0f + ((cp * cp) / (ax * ax) + (sp * sp) / (ay * ay)) * vs)));
+            const float sq = sqrtf(vs / (1.0f - vs));
+            const float ca = ax * m_cos(a), sa = ay * m_sin(a);
+            const V3 m = v3(ca * t.x + sa * b.x, ca * t.y + sa * b.y, ca * t.z + sa * b.z);
+            h = normalize(v3(sq * m.x + n.x, sq * m.y + n.y, sq * m.z + n.z));
+        } else {
+            const float phi = (2.0f * pi) * v0;
+            if (!clearcoat_hit) {
+                th = m_asin(sqrtf(u));
+            } else {
+                const float g = q[9];
+                const float alpha = 0.1f * (1.0f - g) + 0.001f * g;
+                const float alpha2 = alpha * alpha;
+                th = m_acos(sqrtf((1.0f - m_pow(alpha2, 1.0f - u)) / (1.0f - alpha2)));
+            }
+            const float st = m_sin(th);
+            h = frame(t, b, n, st * m_cos(phi), st * m_sin(phi), m_cos(th));
+        }
+        if (specular_hit) {
+            const float vh = fabsf(dot(view, h));
+            const float s = 2.0f * (vh > 0.001f ? vh : 0.001f);
+            l = v3(s * h.x - view.x, s * h.y - view.y, s * h.z - view.z);
+        } else {
+            l = h;
+        }
+        const V3 hh = normalize(add(l, view));
+        const float cos_h = dot(hh, n), cos_d = dot(l, hh), cos_v = dot(view, n), cos_l = dot(l, n);
+        const float vdoth = dot(view, hh);
+        const float* c = S.iso_color;
+        const float lum = (0.3f * c[0] + 0.6f * c[1]) + 0.1f * c[2];
+        const float cd = m_cos(cos_d);
+        const float cd2 = cd * cd;
+        const float f_d90 = 0.5f + (2.0f * roughness) * cd2;
+        const float pl = m_pow5(1.0f - m_cos(cos_l)), pv = m_pow5(1.0f - m_cos(cos_v));
+        const float f_d = (1.0f + (f_d90 - 1.0f) * pl) * (1.0f + (f_d90 - 1.0f) * pv);
+        const float fss90 = roughness * cd2;
+        const float f_ss = (1.0f + (fss90 - 1.0f) * pl) * (1.0f + (fss90 - 1.0f) * pv);
+        const float lv = cos_l + cos_v;
+        const float f_dss = 1.25f * (f_ss * (1.0f / (lv < 0.001f ? 0.001f : lv) - 0.5f) + 0.5f);
+        const float f_h = m_pow5(1.0f - cos_d);
+        const float fd_mix = f_d * (1.0f - q[0]) + f_dss * q[0];
+        const float dx = dot(t, hh) / ax, dy = dot(b, hh) / ay;
+        const float dd = dx * dx + dy * dy;
+        const float d_spec = 1.0f / (((pi * ax) * ay) * (dd * dd) + cos_h * cos_h);
+        const float glx = dot(t, l) * ax, gly = dot(b, l) * ay, gvx = dot(t, view) * ax, gvy = dot(b, view) * ay;
+        float g_spec = 1.0f / (cos_v + sqrtf((glx * glx + gly * gly) + cos_v * cos_v));
+        g_spec = g_spec * (1.0f / (cos_v + sqrtf((gvx * gvx + gvy * gvy) + cos_v * cos_v)));
+        const float sin_th = m_sin(th);
+        const float f_cc = 0.04f * (1.0f - f_h) + 1.0f * f_h;
+        const float a_cc = 0.1f * (1.0f - q[9]) + 0.001f * q[9];
+        float d_cc;
+        if (a_cc >= 1.0f) {
+            d_cc = 1.0f / pi_c;
+        } else {
+            const float a2 = a_cc * a_cc;
+            d_cc = (a2 - 1.0f) / ((pi_c * m_log(a2)) * (1.0f + ((a2 - 1.0f) * cos_h) * cos_h));
+        }
+        const float bl = cos_l * cos_l, bv = cos_v * cos_v, ag = 0.25f * 0.25f;
+        const float g_cc = (1.0f / ((cos_l < -0.99f ? -0.99f : cos_l) + sqrtf((ag + bl) - ag * bl))) *
+                           (1.0f / ((cos_v < -0.99f ? -0.99f : cos_v) + sqrtf((ag + bv) - ag * bv)));
+        const float cc = q[8];
+        const float clear = (specular_hit && clearcoat_hit)
+                                ? (((((cc * f_cc) * g_cc) * cos_l) * vdoth) * sin_th) / cos_h
+                                : ((((((cc * f_cc) * d_cc) * g_cc) * cos_l) * vdoth) * sin_th);
+        const float st = q[3], sh = q[7];
+        const float spec_scale = q[2] * 0.08f;
+        float o[3];
+        for (int i = 0; i < 3; ++i) {
+            const float tint = lum > 0.0f ? c[i] / lum : 1.0f;
+            const float spec0 = (spec_scale * (1.0f * (1.0f - st) + tint * st)) * (1.0f - metallic) + c[i] * metallic;
+            const float sheen = (f_h * q[6]) * (1.0f * (1.0f - sh) + tint * sh);
+            float diffuse = (c[i] * fd_mix + sheen) * (1.0f - metallic);
+            if (specular_hit) diffuse = diffuse * (1.0f / pi);
+            const float f_spec = spec0 * (1.0f - f_h) + 1.0f * f_h;
+            const float spec = (specular_hit && !clearcoat_hit)
+                                   ? (((((f_spec * g_spec) * 4.0f) * cos_l) * vdoth) * sin_th) / cos_h
+                                   : ((((((f_spec * d_spec) * g_spec) * 4.0f) * cos_l) * vdoth) * sin_th);
+            o[i] = (diffuse + spec) + clear;
+        }
+        weights = v3(weights.x * o[0], weights.y * o[1], weights.z * o[2]);
+        w = l;
+    }
     void iso_scatter(V3 p, V3& w, V3& weights, Rng& r) {
         (void)rnd(r);  // isoSurfaceOpacity (1) < random() never holds
         V3 n = iso_normal(p);
@@ -794,6 +905,10 @@ struct Tracer {
         const float xi0 = rnd(r), xi1 = rnd(r);
         if (S.iso_brdf == 3) {
             cook_torrance(n, t, b, xi0, xi1, w, weights, r);
+            return;
+        }
+        if (S.iso_brdf == 4) {
+            disney(n, t, b, xi0, xi1, w, weights, r);
             return;
         }
         if (S.iso_brdf != 0) {

@@ -89,7 +89,7 @@ typedef struct OracleScene {
      * scattering albedo is mixed toward the table's rgb by this weight when it is > 0 */
     float tf_albedo_strength;
     /* surface BRDF of isosurface hits: 0 Lambertian, 1 Blinn-Phong, 2 Ambient (ConstantLighting),
-     * 3 Cook-Torrance */
+     * 3 Cook-Torrance, 4 Disney (2012) */
     int iso_brdf;
     /* setBrdfParameter values: subsurface, metallic, specular, specular_tint, roughness, anisotropic,
      * sheen, sheen_tint, clearcoat, clearcoat_gloss */

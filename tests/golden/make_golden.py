@@ -129,6 +129,16 @@ def cases():
         kw2.update(iso_value=0.3, iso_color=(0.9, 0.6, 0.3), extinction=40.0, albedo=0.9, g=0.2)
         out["fbm_" + name] = SceneSpec(grid=fbm, mode="delta", interp="trilinear", iso=True, iso_brdf="Cook Torrance",
                                        brdf_params=params, **kw2)
+    # Disney (2012) with the pass's default parameters and with every lobe and parameter in use
+    for name, params in {"delta_iso_disney": None,
+                         "delta_iso_disney_all": {"subsurface": 0.3, "metallic": 0.3, "specular": 0.7,
+                                                  "specular_tint": 0.4, "roughness": 0.4, "anisotropic": 0.5,
+                                                  "sheen": 0.5, "sheen_tint": 0.3, "clearcoat": 0.7,
+                                                  "clearcoat_gloss": 0.6}}.items():
+        kw2 = dict(base)
+        kw2.update(iso_value=0.3, iso_color=(0.9, 0.6, 0.3), extinction=40.0, albedo=0.9, g=0.2)
+        out["fbm_" + name] = SceneSpec(grid=fbm, mode="delta", interp="trilinear", iso=True, iso_brdf="Disney (2012)",
+                                       brdf_params=params, **kw2)
     return out
 
 

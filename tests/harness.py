@@ -76,7 +76,7 @@ class SceneSpec:
 
 
 LIGHT_TYPES = ["Point Light", "Spotlight", "Directional Light"]
-ISO_BRDFS = {"Lambertian": 0, "Blinn Phong": 1, "Ambient": 2, "Cook Torrance": 3}
+ISO_BRDFS = {"Lambertian": 0, "Blinn Phong": 1, "Ambient": 2, "Cook Torrance": 3, "Disney (2012)": 4}
 # setBrdfParameter keys in slot order, with the pass's defaults (VolumetricPathTracingPass.hpp:410-419)
 BRDF_KEYS = ["subsurface", "metallic", "specular", "specular_tint", "roughness", "anisotropic", "sheen",
              "sheen_tint", "clearcoat", "clearcoat_gloss"]
@@ -495,7 +495,7 @@ def reference_scene(sp: SceneSpec, frames: int, frame_start: int = 0, inv=None):
     sc.set("iso_color", sp.iso_color)
     if sp.iso:
         tracker += {"Lambertian": "_iso", "Blinn Phong": "_iso_blinn", "Ambient": "_iso_ambient",
-                    "Cook Torrance": "_iso_cook"}[sp.iso_brdf]
+                    "Cook Torrance": "_iso_cook", "Disney (2012)": "_iso_disney"}[sp.iso_brdf]
         sc.set("brdf", brdf_values(sp))
     if sp.env_rot is not None:
         sc.set("env_rot", [float(np.float32(v)) for v in sp.env_rot])
