@@ -153,6 +153,8 @@ struct VptContext {
     float vmin = 0.0f, vmax = 1.0f;
     float box_min[3] = {0, 0, 0}, box_max[3] = {0, 0, 0};
     DevBuf<float> raw, norm;
+    DevBuf<float> grad;      // gradient magnitudes of `raw` for gradient isosurfaces, built on demand
+    bool grad_valid = false;
     // emission grid (load_emission_file / set_use_emission / set_emission_cap / set_emission_strength;
     // VolumetricPathTracingPass.hpp:326-328 defaults)
     DevBuf<float> emission;
@@ -170,6 +172,7 @@ struct VptContext {
     bool use_tf = false;
     // isosurfaces (setUseIsosurfaces, setIsoValue, setIsoSurfaceColor; VolumetricPathTracingPass.hpp:382-395)
     bool use_iso = false;
+    int iso_type = 0;  // setIsosurfaceType: 0 Density, 1 Gradient
     float iso_value = 0.5f;
     float iso_color[3] = {0.4f, 0.4f, 0.4f};
     int iso_subdivisions = 2;
@@ -334,6 +337,7 @@ void invalidate_accel(VptContext* ctx) {
     ctx->occ_valid = false;
     ctx->dens_tex_fresh = false;
     ctx->dens_tex_failed = false;
+    ctx->grad_valid = false;
 }
 
 // The texture over the normalised dense grid: a float 3D array (the driver's block layout) with a
@@ -668,6 +672,9 @@ VptStatus fill_params(VptContext* ctx, int tracker, int frames, vpt::TraceParams
     P.iso_subdivisions = ctx->iso_subdivisions;
     P.iso_value = ctx->iso_value;
     P.iso_color = mk(ctx->iso_color[0], ctx->iso_color[1], ctx->iso_color[2]);
+    P.iso_grad = (ctx->use_iso && ctx->iso_type == 1) ? ctx->grad.ptr : nullptr;
+    P.iso_norm_min = ctx->vmin;
+    P.iso_norm_range = ctx->vmax - ctx->vmin;
     P.max_bounces = ctx->max_bounces;
     P.max_steps = ctx->max_steps;
     P.ess_ref_compat = ctx->ess_ref_compat;
@@ -1111,10 +1118,13 @@ VptStatus vpt_set_iso_surface_color(VptContext* ctx, double r, double g, double 
 VptStatus vpt_set_isosurface_type(VptContext* ctx, const char* name) {
     VPT_CHECK_CTX(ctx);
     if (!name) return fail(ctx, VPT_ERR_ARG, "null isosurface type");
-    if (strcmp(name, "Density") == 0) return VPT_OK;
-    if (strcmp(name, "Gradient") == 0)
-        return fail(ctx, VPT_ERR_UNSUPPORTED, "gradient-magnitude isosurfaces are not built in this core");
-    return VPT_OK;  // unknown names are ignored, as in the reference
+    int type = -1;
+    if (strcmp(name, "Density") == 0) type = 0;
+    if (strcmp(name, "Gradient") == 0) type = 1;
+    if (type < 0) return VPT_OK;  // unknown names are ignored, as in the reference
+    if (type != ctx->iso_type) reset_film_state(ctx);
+    ctx->iso_type = type;
+    return VPT_OK;
 }
 
 VptStatus vpt_set_surface_brdf(VptContext* ctx, const char* name) {
@@ -1622,6 +1632,11 @@ VptStatus vpt_render_frames(VptContext* ctx, int frames, void* stream) {
     cudaStream_t s = as_stream(stream);
     VptStatus st = ensure_accel(ctx, tracker, s);
     if (st != VPT_OK) return st;
+    if (ctx->use_iso && ctx->iso_type == 1 && !ctx->grad_valid) {  // VolumetricPathTracingPass.cpp:690-745
+        VPT_CHECK_CUDA(ctx, ctx->grad.alloc((size_t)ctx->nx * ctx->ny * ctx->nz));
+        VPT_CHECK_CUDA(ctx, vpt::launch_gradient_magnitude(ctx->raw.ptr, ctx->grad.ptr, ctx->nx, ctx->ny, ctx->nz, s));
+        ctx->grad_valid = true;
+    }
     // SVGF wants the last 1-spp frame (DISABLE_ACCUMULATION, VolumetricPathTracingPass.cpp:1665-1667):
     // earlier frames of the call only advance the frame counter, so only the last one is traced.
     const bool single = ctx->denoiser == VPT_DENOISER_SVGF;

@@ -625,11 +625,48 @@ VPT_DEV F3 density_normal(const TraceParams& P, F3 pos, Rng& rng) {
 }
 
 // ---------------------------------------------------------------------------------------------
-// Isosurfaces of the density field (USE_ISOSURFACES with ISOSURFACE_TYPE_DENSITY; dense grids).
+// Isosurfaces of the density field or of its gradient magnitude (USE_ISOSURFACES with
+// ISOSURFACE_TYPE_DENSITY / ISOSURFACE_TYPE_GRADIENT; dense grids).
 
-// The density texture's linear filter at a normalised texture coordinate (sampleIsoImage,
-// VptUtils.glsl:599; the texels are normalised already).
+// gradientImage (ISOSURFACE_TYPE_GRADIENT): the raw gradient magnitudes through a linear filter with
+// border 0 (the density texture's sampler), at continuous voxel coordinates u.
+VPT_DEV float grad_texel(const TraceParams& P, int ix, int iy, int iz) {
+    if ((unsigned)ix >= (unsigned)P.nx || (unsigned)iy >= (unsigned)P.ny || (unsigned)iz >= (unsigned)P.nz) {
+        return 0.0f;
+    }
+    return __ldg(P.iso_grad + ((size_t)iz * (size_t)P.ny + (size_t)iy) * (size_t)P.nx + (size_t)ix);
+}
+
+VPT_DEV float grad_filtered(const TraceParams& P, float ux, float uy, float uz) {
+    ux = ux - 0.5f;
+    uy = uy - 0.5f;
+    uz = uz - 0.5f;
+    const float fx0 = floorf(ux), fy0 = floorf(uy), fz0 = floorf(uz);
+    const float ax = ux - fx0, ay = uy - fy0, az = uz - fz0;
+    const int x0 = (int)fx0, y0 = (int)fy0, z0 = (int)fz0;
+    const float f0 = mixf(mixf(grad_texel(P, x0, y0, z0), grad_texel(P, x0 + 1, y0, z0), ax),
+                          mixf(grad_texel(P, x0, y0 + 1, z0), grad_texel(P, x0 + 1, y0 + 1, z0), ax), ay);
+    const float f1 = mixf(mixf(grad_texel(P, x0, y0, z0 + 1), grad_texel(P, x0 + 1, y0, z0 + 1), ax),
+                          mixf(grad_texel(P, x0, y0 + 1, z0 + 1), grad_texel(P, x0 + 1, y0 + 1, z0 + 1), ax), ay);
+    return mixf(f0, f1, az);
+}
+
+// sampleCloudGradient (VptUtils.glsl:687-699): the filtered magnitude at a world position, the value
+// gradient isosurfaces are found in (no random number drawn: lookups are trilinear with isosurfaces);
+// the texture coordinate is formed as the shader forms it, (pos - boxMin) / (boxMax - boxMin)
+VPT_DEV float iso_gradient_at(const TraceParams& P, F3 pos) {
+    const F3 c = (pos - P.box_min) / (P.box_max - P.box_min);
+    return grad_filtered(P, c.x * (float)P.nx, c.y * (float)P.ny, c.z * (float)P.nz);
+}
+
+// The iso image's linear filter at a normalised texture coordinate (sampleIsoImage, VptUtils.glsl:599):
+// the density texture (its texels are normalised already) or, for gradient isosurfaces, gradientImage
+// normalised with the density's min and range as the shader does.
 VPT_DEV float iso_tex(const TraceParams& P, float cx, float cy, float cz) {
+    if (P.iso_grad) {
+        return (grad_filtered(P, cx * (float)P.nx, cy * (float)P.ny, cz * (float)P.nz) - P.iso_norm_min) /
+               P.iso_norm_range;
+    }
     return sample_dense_vox<kTrilinear>(P, cx * (float)P.nx, cy * (float)P.ny, cz * (float)P.nz);
 }
 
@@ -674,11 +711,6 @@ VPT_DEV F3 iso_normal(const TraceParams& P, F3 pos) {
     return f3(g.x / l, g.y / l, g.z / l);
 }
 
-// An opaque Lambertian surface hit (getIsoSurfaceHit, VptUtils.glsl:1151-1334): one random number
-// for the opacity test, the normal turned against the ray, a cosine-weighted direction in the
-// ComputeDefaultBasis frame (RayTracingUtilities.glsl:20-28; Lambertian.glsl is included before
-// UNIFORM_SAMPLING is defined, so the concentric-disk map of VptUtils.glsl:1078-1098 and a pdf factor
-// equal to the cosine), throughput *= color * cos / cos.
 // mat3(t, b, n) * (x, y, z), summed in the order of a GLSL matrix-vector product
 VPT_DEV F3 iso_frame(F3 t, F3 b, F3 n, float x, float y, float z) {
     return f3((t.x * x + b.x * y) + n.x * z, (t.y * x + b.y * y) + n.y * z, (t.z * x + b.z * y) + n.z * z);
@@ -866,6 +898,11 @@ VPT_DEV void iso_disney(const TraceParams& P, Rng& rng, F3 n, F3 t, F3 b, float 
     w = l;
 }
 
+// An opaque surface hit (getIsoSurfaceHit, VptUtils.glsl:1151-1334): one random number for the
+// opacity test, the normal turned against the ray, the ComputeDefaultBasis frame
+// (RayTracingUtilities.glsl:20-28), then the selected BRDF.  Lambertian: a cosine-weighted direction
+// (Lambertian.glsl is included before UNIFORM_SAMPLING is defined, so the concentric-disk map of
+// VptUtils.glsl:1078-1098 and a pdf factor equal to the cosine), throughput *= color * cos / cos.
 VPT_DEV void iso_scatter(const TraceParams& P, Rng& rng, F3 p, F3& w, F3& weights) {
     (void)rng_next(rng);  // isoSurfaceOpacity (1) < random() never holds
     F3 n = iso_normal(P, p);

@@ -169,6 +169,33 @@ __global__ void normalize_kernel(const float* __restrict__ in, float* __restrict
     }
 }
 
+// Gradient magnitude of the raw grid for gradient isosurfaces (VolumetricPathTracingPass.cpp:690-727):
+// central differences between the neighbours clamped to the grid, divided by their index distance
+// (2 inside, 1 at a face), |g| = sqrt(dx^2 + dy^2 + dz^2) in float, x fastest.  A stencil pass at
+// HBM speed: each thread owns one voxel, the six neighbour loads of a warp fall on at most a few
+// cache lines of the x row and of the rows above and below it.
+__global__ void gradient_magnitude_kernel(const float* __restrict__ g, float* __restrict__ out, int nx, int ny,
+                                          int nz) {
+    const size_t n = (size_t)nx * ny * nz;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const int x = (int)(i % (size_t)nx);
+        const size_t yz = i / (size_t)nx;
+        const int y = (int)(yz % (size_t)ny);
+        const int z = (int)(yz / (size_t)ny);
+        const int xl = x > 0 ? x - 1 : 0, xu = x < nx - 1 ? x + 1 : nx - 1;
+        const int yl = y > 0 ? y - 1 : 0, yu = y < ny - 1 ? y + 1 : ny - 1;
+        const int zl = z > 0 ? z - 1 : 0, zu = z < nz - 1 ? z + 1 : nz - 1;
+        const size_t row = (size_t)nx, plane = (size_t)nx * ny;
+        const size_t base = (size_t)z * plane + (size_t)y * row;
+        const float dx = (g[base + xu] - g[base + xl]) / (float)(xu - xl);
+        const float dy = (g[(size_t)z * plane + (size_t)yu * row + x] - g[(size_t)z * plane + (size_t)yl * row + x]) /
+                         (float)(yu - yl);
+        const float dz = (g[(size_t)zu * plane + (size_t)y * row + x] - g[(size_t)zl * plane + (size_t)y * row + x]) /
+                         (float)(zu - zl);
+        out[i] = sqrtf(dx * dx + dy * dy + dz * dz);
+    }
+}
+
 // Improved Perlin noise (K. Perlin, "Improving Noise", SIGGRAPH 2002) with a seeded permutation;
 // only +, -, *, floor, so the CPU oracle reproduces every value bit for bit.
 struct PermTable {
@@ -463,6 +490,13 @@ cudaError_t launch_minmax(const float* v, size_t n, float* out_minmax, cudaStrea
 
 cudaError_t launch_normalize(const float* in, float* out, size_t n, float vmin, float vmax, cudaStream_t s) {
     normalize_kernel<<<grid_for(n, 256), 256, 0, s>>>(in, out, n, vmin, vmax);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gradient_magnitude(const float* grid, float* out, int nx, int ny, int nz, cudaStream_t s) {
+    const size_t n = (size_t)nx * ny * nz;
+    gradient_magnitude_kernel<<<grid_for(n, 256), 256, 0, s>>>(grid, out, nx, ny, nz);
     count_launches(1);
     return cudaGetLastError();
 }

@@ -28,6 +28,7 @@ cudaError_t launch_trace(const TraceParams& P, int tracker, int use_ess, int sch
                          int persistent_blocks, cudaStream_t stream);
 cudaError_t launch_minmax(const float* v, size_t n, float* out_minmax, cudaStream_t s);
 cudaError_t launch_normalize(const float* in, float* out, size_t n, float vmin, float vmax, cudaStream_t s);
+cudaError_t launch_gradient_magnitude(const float* grid, float* out, int nx, int ny, int nz, cudaStream_t s);
 // Copies an x-fastest nx x ny x nz float grid into a 3D array through its surface object (ny, nz <= 65535).
 cudaError_t launch_fill_density_array(const float* src, unsigned long long surface, int nx, int ny, int nz,
                                       cudaStream_t s);

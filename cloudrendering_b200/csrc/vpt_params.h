@@ -210,6 +210,10 @@ struct TraceParams {
     int iso_subdivisions;          // checks per free-flight segment (NUM_ISOSURFACE_SUBDIVISIONS)
     float iso_value;
     F3 iso_color;
+    // ISOSURFACE_TYPE_GRADIENT: the grid's gradient magnitudes [nz][ny][nx] (raw, not normalised), or
+    // null for density isosurfaces; normals read them normalised with the density's min / range
+    const float* iso_grad;
+    float iso_norm_min, iso_norm_range;
     unsigned long long* counters;  // [0] paths, [1] density lookups
     int* error_flags;
     unsigned int* work_counter;    // persistent-kernel path queue

@@ -108,7 +108,8 @@ VPT_DEV F3 track_delta(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, Fi
 }
 
 // One free-flight segment [x, x_new] of delta tracking with isosurfaces (CheckIsosurfaceHit.glsl):
-// P.iso_subdivisions check points for a sign change of density - iso_value against the first point
+// P.iso_subdivisions check points for a sign change of sampleCloudIso - iso_value (the density, or the
+// filtered gradient magnitude for gradient isosurfaces) against the first point
 // after the last surface event; a crossing is bisected (refineIsoSurfaceHit, VptUtils.glsl:1045-1058,
 // 8 steps), the surface reflects (iso_scatter), the path moves 1e-4 off it and restarts from the box
 // boundary.  Returns true on a surface event (x, w, d, tmax and weights updated; the first event
@@ -126,7 +127,10 @@ VPT_DEV bool iso_segment(const TraceParams& P, S& sample, Rng& rng, F3& x, F3 xn
         F3 x0 = x * (1.0f - a0) + xn * a0;
         F3 x1 = x * (1.0f - a1) + xn * a1;
         float v = density;
-        if (sub != nsub - 1 || !S::kRepeatable) {
+        if (P.iso_grad) {
+            v = iso_gradient_at(P, x1);
+            lookups++;
+        } else if (sub != nsub - 1 || !S::kRepeatable) {
             v = sample(x1, rng);
             lookups++;
         }
@@ -139,7 +143,7 @@ VPT_DEV bool iso_segment(const TraceParams& P, S& sample, Rng& rng, F3& x, F3 xn
         if (last_sign != cur_sign) {
             for (int r = 0; r < 8; ++r) {
                 const F3 mid = f3((x1.x + x0.x) * 0.5f, (x1.y + x0.y) * 0.5f, (x1.z + x0.z) * 0.5f);
-                const float vm = sample(mid, rng);
+                const float vm = P.iso_grad ? iso_gradient_at(P, mid) : sample(mid, rng);
                 lookups++;
                 if ((vm - P.iso_value) * cur_sign >= 0.0f) x1 = mid;
                 else x0 = mid;

@@ -297,7 +297,7 @@ def set_iso_surface_color(_iso_surface_color) -> None:
 
 
 def set_isosurface_type(_isosurface_type: str) -> None:
-    """"Density" (the only type built; "Gradient" raises); unknown names are ignored."""
+    """"Density" or "Gradient" (isosurfaces of the gradient magnitude); unknown names are ignored."""
     _c("vpt_set_isosurface_type", str(_isosurface_type).encode())
 
 
@@ -851,7 +851,10 @@ def _stream_of(t: torch.Tensor):
 
 def _read(input_tensor: torch.Tensor, channels: int, fn: str, feature: Optional[int] = None) -> torch.Tensor:
     h, w = input_tensor.size(1), input_tensor.size(2)
-    out = torch.empty((channels, h, w), dtype=torch.float32, device=input_tensor.device)
+    # a host result lands in page-locked memory (torch's caching host allocator): the device-to-host
+    # copy then runs at link speed instead of through a pageable staging copy
+    out = torch.empty((channels, h, w), dtype=torch.float32, device=input_tensor.device,
+                      pin_memory=not input_tensor.is_cuda)
     on_dev = 1 if out.is_cuda else 0
     ptr = ctypes.c_void_p(out.data_ptr())
     if feature is None:

@@ -150,10 +150,13 @@ VptStatus vpt_set_tf_scattering_albedo_strength(VptContext* ctx, float strength)
  * iso_value (default 0.5) is found on every free-flight segment and reflects like an opaque surface
  * of colour iso_surface_color (default 0.4 0.4 0.4) with the selected BRDF; lookups are trilinear
  * while isosurfaces are on.  Built for delta tracking on dense grids: other trackers, sparse grids, a
- * transfer function and batched rendering return VPT_ERR_UNSUPPORTED.  Type "Density" and the BRDFs
+ * transfer function and batched rendering return VPT_ERR_UNSUPPORTED.  Types "Density" and "Gradient"
+ * (the surface where the trilinear-filtered gradient magnitude of the raw grid crosses iso_value:
+ * central differences with clamped neighbours, VolumetricPathTracingPass.cpp:690-745, built on the GPU
+ * at the first render after the grid or the type changed) and the BRDFs
  * "Lambertian" (Lambertian.glsl, the default), "Blinn Phong" (BlinnPhong.glsl), "Disney (2012)"
  * (Disney2012.glsl), "Cook Torrance" (CookTorrance.glsl) and "Ambient" (ConstantLighting.glsl) are
- * accepted, "Gradient" returns VPT_ERR_UNSUPPORTED, unknown names are ignored (as in the reference).
+ * accepted, unknown names are ignored (as in the reference).
  * vpt_set_num_isosurface_subdivisions is the pass's own setting (VolumetricPathTracingPass.cpp:1028-1033,
  * default 2, 1..8).
  * vpt_set_brdf_parameter replaces set_brdf_parameter (src/PyTorch/Module.cpp:1196-1199,

@@ -44,7 +44,7 @@ class OracleScene(ctypes.Structure):
         ("use_iso", c_int), ("iso_value", c_float), ("iso_color", c_float * 3), ("iso_subdivisions", c_int),
         ("sv_inv_world", c_float * 3), ("sv_local", c_void_p),
         ("env_rot", c_int), ("env_rot_m", c_float * 9), ("tf_albedo_strength", c_float), ("iso_brdf", c_int),
-        ("brdf", c_float * 10),
+        ("brdf", c_float * 10), ("iso_grad", c_void_p), ("iso_norm_min", c_float), ("iso_norm_range", c_float),
     ]
 
 
@@ -209,7 +209,7 @@ class Scene:
 
     def set(self, k, v):
         if k in ("density", "sv_data", "occupancy", "env_rgba", "env_pyramid", "nanovdb", "emission", "tf",
-                 "sv_local"):
+                 "sv_local", "iso_grad"):
             arr = None if v is None else np.ascontiguousarray(v)
             self._keep[k] = arr
             setattr(self.s, k, None if arr is None else arr.ctypes.data_as(c_void_p).value)

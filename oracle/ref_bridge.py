@@ -30,7 +30,7 @@ class RefScene(ctypes.Structure):
         ("emission_box_min", c_float * 3), ("emission_box_max", c_float * 3), ("emission_cap", c_float),
         ("emission_strength", c_float), ("tf", c_void_p), ("tf_size", c_int),
         ("iso_value", c_float), ("iso_color", c_float * 3), ("env_rot", c_float * 9), ("prev_view_proj", c_float * 16),
-        ("tf_albedo_strength", c_float), ("brdf", c_float * 10),
+        ("tf_albedo_strength", c_float), ("brdf", c_float * 10), ("gradient", c_void_p),
     ]
 
 
@@ -73,7 +73,7 @@ class Scene:
             self.set(k, v)
 
     def set(self, k, v):
-        if k in ("grid", "sv_data", "occupancy", "env_rgba", "env_pyramid", "emission", "tf"):
+        if k in ("grid", "sv_data", "occupancy", "env_rgba", "env_pyramid", "emission", "tf", "gradient"):
             arr = None if v is None else np.ascontiguousarray(v)
             self._keep[k] = arr
             setattr(self.s, k, None if arr is None else arr.ctypes.data_as(c_void_p).value)

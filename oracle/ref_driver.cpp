@@ -17,6 +17,7 @@ namespace REF_VARIANT_NS {
 static Parameters& parameters = g_ref.params;
 static FrameInfo& frameInfo = g_ref.frame;
 static sampler3D& gridImage = g_ref.grid;
+static sampler3D& gradientImage = g_ref.gradient;
 static sampler3D& emissionImage = g_ref.emission;
 static sampler1DArray& transferFunctionTexture = g_ref.tf;
 static sampler3D& superVoxelGridImage = g_ref.sv;
@@ -96,6 +97,7 @@ typedef struct RefScene {
     float tf_albedo_strength; /* parameters.tfScatteringAlbedoStrength */
     float brdf[10];           /* parameters.subsurface, metallic, specular, specularTint, roughness,
                                  anisotropic, sheen, sheenTint, clearcoat, clearcoatGloss */
+    const float* gradient;    /* gradientImage values [nz][ny][nx] (ISOSURFACE_TYPE_GRADIENT variants) */
 } RefScene;
 
 int ref_variant_count(void) { return ref_num_variants; }
@@ -198,6 +200,8 @@ int ref_render(int variant, const RefScene* s, float* out_rgba, int threads) {
     g_ref.grid.d = s->nz;
     g_ref.grid.channels = 1;
     g_ref.grid.filter = s->linear_filter ? FILTER_LINEAR : FILTER_NEAREST;
+    g_ref.gradient = g_ref.grid;
+    g_ref.gradient.data = s->gradient;
     g_ref.sv.data = s->sv_data;
     g_ref.sv.w = s->svx;
     g_ref.sv.h = s->svy;

@@ -7,6 +7,7 @@ struct RefState {
     Parameters params;
     FrameInfo frame;
     sampler3D grid;       // gridImage
+    sampler3D gradient;   // gradientImage (ISOSURFACE_TYPE_GRADIENT variants)
     sampler3D emission;   // emissionImage (USE_EMISSION variants)
     sampler1DArray tf;    // transferFunctionTexture (USE_TRANSFER_FUNCTION variants)
     sampler3D sv;         // superVoxelGridImage (RG32F)

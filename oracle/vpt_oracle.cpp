@@ -673,7 +673,40 @@ struct Tracer {
     // ---- isosurfaces (USE_ISOSURFACES, ISOSURFACE_TYPE_DENSITY, SURFACE_BRDF_LAMBERTIAN) ----
     // the isosurface field at a texture coordinate: the density texture's linear filter there
     // (sampleIsoImage, VptUtils.glsl:599; the texel values are normalised already)
-    float iso_tex(V3 c) const { return at_vox(c.x * (float)S.nx, c.y * (float)S.ny, c.z * (float)S.nz); }
+    float iso_tex(V3 c) const {
+        if (S.iso_grad) {  // gradientImage normalised with the density's range (sampleIsoImage)
+            return (grad_vox(c.x * (float)S.nx, c.y * (float)S.ny, c.z * (float)S.nz) - S.iso_norm_min) /
+                   S.iso_norm_range;
+        }
+        return at_vox(c.x * (float)S.nx, c.y * (float)S.ny, c.z * (float)S.nz);
+    }
+    // gradientImage (ISOSURFACE_TYPE_GRADIENT): raw magnitudes, linear filter, border 0
+    float grad_texel(int x, int y, int z) const {
+        if (x < 0 || y < 0 || z < 0 || x >= S.nx || y >= S.ny || z >= S.nz) return 0.0f;
+        return S.iso_grad[((size_t)z * S.ny + y) * S.nx + x];
+    }
+    float grad_vox(float ux, float uy, float uz) const {
+        ux = ux - 0.5f;
+        uy = uy - 0.5f;
+        uz = uz - 0.5f;
+        const float fx = floorf(ux), fy = floorf(uy), fz = floorf(uz);
+        const float ax = ux - fx, ay = uy - fy, az = uz - fz;
+        const int x0 = (int)fx, y0 = (int)fy, z0 = (int)fz;
+        const float f0 = mixf(mixf(grad_texel(x0, y0, z0), grad_texel(x0 + 1, y0, z0), ax),
+                              mixf(grad_texel(x0, y0 + 1, z0), grad_texel(x0 + 1, y0 + 1, z0), ax), ay);
+        const float f1 = mixf(mixf(grad_texel(x0, y0, z0 + 1), grad_texel(x0 + 1, y0, z0 + 1), ax),
+                              mixf(grad_texel(x0, y0 + 1, z0 + 1), grad_texel(x0 + 1, y0 + 1, z0 + 1), ax), ay);
+        return mixf(f0, f1, az);
+    }
+    // sampleCloudIso: the density, or the filtered gradient magnitude (sampleCloudGradient,
+    // VptUtils.glsl:687-699) for gradient isosurfaces
+    float iso_value_at(V3 pos, Rng& r) {
+        if (S.iso_grad) {  // the shader's texture coordinate (pos - boxMin) / (boxMax - boxMin)
+            const V3 c = divv(sub(pos, bmin()), sub(bmax(), bmin()));
+            return grad_vox(c.x * (float)S.nx, c.y * (float)S.ny, c.z * (float)S.nz);
+        }
+        return sample(pos, r);
+    }
     // getNearestMultiple (VptUtils.glsl:896-906) with GLSL mod(n, x) = n - x * floor(n / x)
     static float nearest_multiple(float n, float x, bool smaller) {
         const float rest = n - x * floorf(n / x);
@@ -716,7 +749,7 @@ struct Tracer {
     void iso_refine(V3& cur, V3 last, float step_sign, Rng& r) {
         for (int i = 0; i < 8; i++) {
             const V3 mid = v3((cur.x + last.x) * 0.5f, (cur.y + last.y) * 0.5f, (cur.z + last.z) * 0.5f);
-            const float v = sample(mid, r);
+            const float v = iso_value_at(mid, r);
             if ((v - S.iso_value) * step_sign >= 0.0f) cur = mid;
             else last = mid;
         }
@@ -985,7 +1018,7 @@ struct Tracer {
                     const float a0 = (float)sub / (float)nsub, a1 = (float)(sub + 1) / (float)nsub;
                     const V3 x0 = add(mul(x, 1.0f - a0), mul(xn, a0));
                     V3 x1 = add(mul(x, 1.0f - a1), mul(xn, a1));
-                    const float cur_sign = signf(sample(x1, r) - S.iso_value);
+                    const float cur_sign = signf(iso_value_at(x1, r) - S.iso_value);
                     if (first_point) {
                         first_point = false;
                         last_sign = cur_sign;

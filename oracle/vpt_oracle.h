@@ -94,6 +94,10 @@ typedef struct OracleScene {
     /* setBrdfParameter values: subsurface, metallic, specular, specular_tint, roughness, anisotropic,
      * sheen, sheen_tint, clearcoat, clearcoat_gloss */
     float brdf[10];
+    /* ISOSURFACE_TYPE_GRADIENT: the raw grid's gradient magnitudes [nz][ny][nx], or NULL (density
+     * isosurfaces); normals read them as (v - iso_norm_min) / iso_norm_range (the density's range) */
+    const float* iso_grad;
+    float iso_norm_min, iso_norm_range;
 } OracleScene;
 
 /* Renders width*height*num_frames paths; adds radiance (and its square) per pixel (3 doubles). */

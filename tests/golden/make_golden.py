@@ -23,7 +23,8 @@ ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)
 sys.path.insert(0, ROOT)
 
 from oracle import bridge, ref_build  # noqa: E402
-from tests.harness import SceneSpec, camera_inv_view_proj, camera_view_proj, cloud_block, reference_scene  # noqa: E402
+from tests.harness import (SceneSpec, camera_inv_view_proj, camera_view_proj, cloud_block, gradient_magnitude,  # noqa: E402
+                           reference_scene)
 
 W = H = 32
 
@@ -139,6 +140,12 @@ def cases():
         kw2.update(iso_value=0.3, iso_color=(0.9, 0.6, 0.3), extinction=40.0, albedo=0.9, g=0.2)
         out["fbm_" + name] = SceneSpec(grid=fbm, mode="delta", interp="trilinear", iso=True, iso_brdf="Disney (2012)",
                                        brdf_params=params, **kw2)
+    # isosurfaces of the gradient magnitude (ISOSURFACE_TYPE_GRADIENT) at its upper quartile inside the cloud
+    gm = gradient_magnitude(fbm)
+    kw2 = dict(base)
+    kw2.update(iso_value=float(np.float32(np.quantile(gm[gm > 0], 0.75))), iso_color=(0.9, 0.6, 0.3), extinction=40.0,
+               albedo=0.9, g=0.2)
+    out["fbm_delta_isograd"] = SceneSpec(grid=fbm, mode="delta", interp="trilinear", iso=True, iso_type="Gradient", **kw2)
     return out
 
 
@@ -167,7 +174,7 @@ FIELDS = ["mode", "interp", "extinction", "albedo", "g", "width", "height", "see
           "sun_dir", "sun_intensity", "cam_pos", "cam_target", "fovy", "near", "far", "max_grid_extent", "use_ess",
           "env_intensity", "max_bounces", "ess_ref_compat", "lights", "extinction_base", "albedo_rgb", "sdt_prob",
           "emission_cap", "emission_strength", "iso", "iso_value", "iso_color", "env_rot", "tf_albedo_strength",
-          "iso_brdf", "brdf_params"]
+          "iso_brdf", "brdf_params", "iso_type"]
 
 
 def depth_map_cases():

@@ -70,7 +70,7 @@ class SceneSpec:
                  use_ess=False, env_intensity=(1.0, 1.0, 1.0), ess_ref_compat=False, lights=None,
                  extinction_base=(1.0, 1.0, 1.0), albedo_rgb=None, sdt_prob=2, emission=None, emission_cap=1.0,
                  emission_strength=1.0, tf=None, iso=False, iso_value=0.5, iso_color=(0.4, 0.4, 0.4), env_rot=None,
-                 tf_albedo_strength=0.0, iso_brdf="Lambertian", brdf_params=None):
+                 tf_albedo_strength=0.0, iso_brdf="Lambertian", brdf_params=None, iso_type="Density"):
         self.__dict__.update(locals())
         del self.__dict__["self"]
 
@@ -81,6 +81,24 @@ ISO_BRDFS = {"Lambertian": 0, "Blinn Phong": 1, "Ambient": 2, "Cook Torrance": 3
 BRDF_KEYS = ["subsurface", "metallic", "specular", "specular_tint", "roughness", "anisotropic", "sheen",
              "sheen_tint", "clearcoat", "clearcoat_gloss"]
 BRDF_DEFAULTS = [0.0, 0.0, 0.5, 0.0, 0.5, 0.0, 0.0, 0.5, 0.0, 1.0]
+
+
+def gradient_magnitude(grid):
+    """The gradient-magnitude field of gradient isosurfaces (VolumetricPathTracingPass.cpp:690-727) in
+    float32: central differences between neighbours clamped to the grid over their index distance,
+    sqrt(dx^2 + dy^2 + dz^2); grid [z, y, x]."""
+    g = np.ascontiguousarray(grid, np.float32)
+
+    def diff(axis):
+        n = g.shape[axis]
+        idx = np.arange(n)
+        lo, hi = np.maximum(idx - 1, 0), np.minimum(idx + 1, n - 1)
+        shape = [1, 1, 1]
+        shape[axis] = n
+        return (np.take(g, hi, axis=axis) - np.take(g, lo, axis=axis)) / (hi - lo).astype(np.float32).reshape(shape)
+
+    dz, dy, dx = diff(0), diff(1), diff(2)
+    return np.sqrt((dx * dx + dy * dy) + dz * dz).astype(np.float32)
 
 
 def brdf_values(sp):
@@ -168,6 +186,7 @@ def setup_core(core: Core, sp: SceneSpec):
     core("vpt_set_tf_scattering_albedo_strength", float(sp.tf_albedo_strength))
     core("vpt_set_use_isosurfaces", 1 if sp.iso else 0)
     core("vpt_set_surface_brdf", sp.iso_brdf.encode())
+    core("vpt_set_isosurface_type", sp.iso_type.encode())
     for k, v in zip(BRDF_KEYS, brdf_values(sp)):
         core("vpt_set_brdf_parameter", k.encode(), repr(v).encode())
     core("vpt_set_iso_value", sp.iso_value)
@@ -337,6 +356,11 @@ def oracle_scene(core, sp: SceneSpec, frames: int, frame_count: int = 0) -> brid
         sc.set("interp", 2)
         sc.set("iso_brdf", ISO_BRDFS[sp.iso_brdf])
         sc.set("brdf", brdf_values(sp))
+        if sp.iso_type == "Gradient":
+            vmin, vmax = bridge.minmax(g)
+            sc.set("iso_grad", gradient_magnitude(g))
+            sc.set("iso_norm_min", float(np.float32(vmin)))
+            sc.set("iso_norm_range", float(np.float32(np.float32(vmax) - np.float32(vmin))))
     sc.set("iso_value", float(np.float32(sp.iso_value)))
     sc.set("iso_color", [float(np.float32(c)) for c in sp.iso_color])
     if sp.env_rot is not None and sp.env == "image":
@@ -497,6 +521,9 @@ def reference_scene(sp: SceneSpec, frames: int, frame_start: int = 0, inv=None):
         tracker += {"Lambertian": "_iso", "Blinn Phong": "_iso_blinn", "Ambient": "_iso_ambient",
                     "Cook Torrance": "_iso_cook", "Disney (2012)": "_iso_disney"}[sp.iso_brdf]
         sc.set("brdf", brdf_values(sp))
+        if sp.iso_type == "Gradient":
+            tracker = tracker.replace("_iso", "_isograd")
+            sc.set("gradient", gradient_magnitude(g))
     if sp.env_rot is not None:
         sc.set("env_rot", [float(np.float32(v)) for v in sp.env_rot])
         tracker += "_rot"

@@ -210,8 +210,13 @@ def _check_isosurfaces():
     surf = vpt.render_frame(t, 2).clone()
     assert torch.isfinite(surf).all()
     assert not torch.allclose(surf, plain, rtol=1e-3)
-    with pytest.raises(RuntimeError, match="not built"):
-        vpt.set_isosurface_type("Gradient")
+    vpt.set_isosurface_type("Gradient")  # the gradient-magnitude field is built on the first render
+    vpt.set_iso_value(0.02)
+    vpt.set_seed_offset(0)
+    grad = vpt.render_frame(t, 1).clone()
+    assert torch.isfinite(grad).all()
+    vpt.set_isosurface_type("Density")
+    vpt.set_iso_value(0.3)
     for brdf in ("Blinn Phong", "Disney (2012)", "Cook Torrance", "Ambient", "Lambertian"):
         vpt.set_surface_brdf(brdf)
         vpt.set_seed_offset(0)
@@ -237,6 +242,7 @@ def test_isosurfaces():
         _check_isosurfaces()
     finally:  # the module's state outlives the test: leave the defaults behind even after a failure
         vpt.set_use_isosurfaces(False)
+        vpt.set_isosurface_type("Density")
         vpt.set_surface_brdf("Lambertian")
         vpt.set_iso_value(0.5)
         vpt.set_vpt_mode_from_name("Delta Tracking")

@@ -378,7 +378,8 @@ def test_iteration_guard_reports_error_without_hanging(core):
     core("vpt_synchronize", None)
 
 
-@pytest.mark.parametrize("mode", ["delta", "ratio", "nee", "nee_lights", "delta_isosurfaces", "nee_ess",
+@pytest.mark.parametrize("mode", ["delta", "ratio", "nee", "nee_lights", "delta_isosurfaces",
+                                  "delta_isosurfaces_gradient", "delta_isosurfaces_cook_torrance", "nee_ess",
                                   "nee_ess_ref_compat", "decomposition", "decomposition_trilinear", "rrt_unbiased",
                                   "rrt_unbiased_trilinear", "rrt_unbiased_lights"])
 def test_schedules_trace_identical_paths(core_dr, mode):
@@ -392,6 +393,11 @@ def test_schedules_trace_identical_paths(core_dr, mode):
         kw = PATH_CASES["nee_lights"]
     elif mode == "delta_isosurfaces":
         kw = dict(mode="delta", interp="trilinear", iso=True, iso_value=0.3)
+    elif mode == "delta_isosurfaces_gradient":
+        kw = dict(mode="delta", interp="trilinear", iso=True, iso_value=0.02, iso_type="Gradient")
+    elif mode == "delta_isosurfaces_cook_torrance":
+        kw = dict(mode="delta", interp="trilinear", iso=True, iso_value=0.3, iso_brdf="Cook Torrance",
+                  brdf_params={"metallic": 0.5, "roughness": 0.3})
     elif mode.startswith("nee_ess"):  # sky shadow rays skip empty occupancy blocks (the refill loop's own walk)
         kw = dict(mode="nee", use_ess=True, ess_ref_compat=mode.endswith("compat"))
     elif mode == "rrt_unbiased_lights":  # free flights and shadow walks of the refill loop, light shadow rays
