@@ -25,8 +25,12 @@ uint64_t padded_paths(int width, int height, uint32_t frames) {
 cudaError_t launch_trace(const TraceParams& P, int tracker, int use_ess, int schedule, int features,
                          int persistent_blocks, cudaStream_t stream) {
     if (P.iso) {
-        // isosurfaces: delta tracking on dense grids, trilinear lookups, no transfer function
-        if (tracker != kDelta || P.grid_kind != kDense || P.tf) return cudaErrorNotSupported;
+        // isosurfaces: delta and spectral delta tracking on dense grids, trilinear lookups, no transfer
+        // function
+        if ((tracker != kDelta && tracker != kSpectralDelta) || P.grid_kind != kDense || P.tf)
+            return cudaErrorNotSupported;
+        if (tracker == kSpectralDelta)
+            return launch_tracker_spectral_delta_iso(P, schedule, features, persistent_blocks, stream);
         return launch_tracker_delta_iso(P, schedule, features, persistent_blocks, stream);
     }
     if (P.grid_kind == kNanoVdb) {

@@ -195,7 +195,8 @@ VPT_DEV F3 run_tracker(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, Fi
     }
     if (TRACKER == kResidualRatio) return track_residual_ratio(P, sample, rng, x, w, fe, pc);
     if constexpr (TRACKER == kResidualRatioNee) return track_residual_ratio_nee(P, sample, rng, x, w, fe, pc);
-    if constexpr (TRACKER == kSpectralDelta) return track_delta_spectral(P, sample, rng, x, w, fe, pc);
+    if constexpr (TRACKER == kSpectralDelta) return track_delta_spectral<false>(P, sample, rng, x, w, fe, pc);
+    if constexpr (TRACKER == kSpectralDeltaIso) return track_delta_spectral<true>(P, sample, rng, x, w, fe, pc);
     if constexpr (TRACKER == kSpectralNextEvent) return track_nee_spectral<false>(P, sample, rng, x, w, fe, pc);
     if constexpr (TRACKER == kSpectralNextEvent + 100) return track_nee_spectral<true>(P, sample, rng, x, w, fe, pc);
     if (TRACKER == kNextEvent + 100) return track_nee<true>(P, sample, rng, x, w, fe, pc);
@@ -1118,5 +1119,7 @@ VPT_DECLARE_TRACKER(kSpectralNextEvent + 100, kDense);
 VPT_DECLARE_TRACKER(kSpectralNextEvent, kNanoVdb);
 // delta tracking with isosurfaces: dense grids, trilinear lookups, no transfer function
 cudaError_t launch_tracker_delta_iso(const TraceParams& P, int schedule, int features, int pb, cudaStream_t s);
+cudaError_t launch_tracker_spectral_delta_iso(const TraceParams& P, int schedule, int features, int pb,
+                                              cudaStream_t s);
 
 }  // namespace vpt

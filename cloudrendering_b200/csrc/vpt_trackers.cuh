@@ -517,23 +517,37 @@ VPT_DEV F3 sdt_reweight(F3 weights, F3 sigma, float majorant, float p) {
 
 VPT_DEV F3 sdt_clamp(F3 v, float c) { return f3(fminf(v.x, c), fminf(v.y, c), fminf(v.z, c)); }
 
-// VptMode::SPECTRAL_DELTA_TRACKING (deltaTrackingSpectral, DeltaTracking.glsl:33-163).
-template <class S>
+// VptMode::SPECTRAL_DELTA_TRACKING (deltaTrackingSpectral, DeltaTracking.glsl:33-163).  ISO: with
+// isosurfaces (DeltaTracking.glsl:37-63 and the CheckIsosurfaceHit.glsl include): the 1000-iteration
+// cap, iso_segment on every free-flight segment, the surface throughput multiplied into the spectral
+// weights, and the path ended when all three fall below 1e-3 after a surface event.
+template <bool ISO, class S>
 VPT_DEV F3 track_delta_spectral(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, FirstEvent& fe,
                                 PathCtx& pc) {
     F3 weights = f3(1.0f, 1.0f, 1.0f);
+    float last_sign = 0.0f;
+    bool first_point = true;
+    int it = 0;
     float tmin, tmax;
     if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
         x = x + w * tmin;
         float d = tmax - tmin;
         int bounces = 0;
         while (true) {
+            if (ISO && ++it == 1000) return f3(0.0f, 0.0f, 0.0f);
             if (guard(pc)) return f3(0.0f, 0.0f, 0.0f);
             float t = free_path(rng, P.inv_sdt_majorant);
             if (t > d) break;
             F3 xn = x + w * t;
             float density = sample(xn, rng);
             pc.lookups++;
+            if constexpr (ISO) {
+                if (iso_segment(P, sample, rng, x, xn, density, w, d, tmax, weights, last_sign, first_point,
+                                pc.lookups, &fe)) {
+                    if (weights.x < 1e-3f && weights.y < 1e-3f && weights.z < 1e-3f) return f3(0.0f, 0.0f, 0.0f);
+                    continue;
+                }
+            }
             x = xn;
             const SdtStep st = sdt_probabilities(P, density, weights, sdt_albedo(P, sample));
             float xi = rng_next(rng);

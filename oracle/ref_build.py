@@ -132,6 +132,10 @@ def variants():
                         ("cook", "SURFACE_BRDF_COOK_TORRANCE"), ("disney", "SURFACE_BRDF_DISNEY")):
         out.append((f"delta_iso_{tag}__trilinear__default__linear", TRACKERS["delta"] + [INTERPS["trilinear"]]
                     + ENVS["default__linear"] + [define if d == "SURFACE_BRDF_LAMBERTIAN" else d for d in ISO], 0))
+    # spectral delta tracking with isosurfaces (DeltaTracking.glsl:37-63), path-history and max probabilities
+    for p in ("hist", "max"):
+        out.append((f"sdt_{p}_iso__trilinear__default__linear", [SPECTRAL["sdt"], SDT_PROB[p], INTERPS["trilinear"]]
+                    + ENVS["default__linear"] + ISO, 0))
     # isosurfaces of the gradient magnitude (ISOSURFACE_TYPE_GRADIENT: gradientImage, VptUtils.glsl:687-707)
     out.append(("delta_isograd__trilinear__default__linear", TRACKERS["delta"] + [INTERPS["trilinear"]]
                 + ENVS["default__linear"] + ["ISOSURFACE_TYPE_GRADIENT" if d == "ISOSURFACE_TYPE_DENSITY" else d

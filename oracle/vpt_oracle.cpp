@@ -994,13 +994,45 @@ struct Tracer {
     // density - iso_value against the first point after the last surface event; a crossing is
     // bisected, the surface reflects, the path restarts from the box boundary; escapes carry the
     // surface throughput; 1000 loop iterations end the path with zero
+    // CheckIsosurfaceHit.glsl for one free-flight segment [x, xn]: iso_subdivisions check points for a
+    // sign change of sampleCloudIso - iso_value against the first point after the last surface event;
+    // a crossing is bisected, the surface scatters, the path moves 1e-4 off it and restarts from the
+    // box boundary.  Returns true on a surface event.
+    bool iso_check(V3& x, V3 xn, V3& w, float& d, float& tmax, V3& weights, float& last_sign, bool& first_point,
+                   Rng& r, bool& ev) {
+        const int nsub = S.iso_subdivisions;
+        for (int sub = 0; sub < nsub; sub++) {
+            const float a0 = (float)sub / (float)nsub, a1 = (float)(sub + 1) / (float)nsub;
+            const V3 x0 = add(mul(x, 1.0f - a0), mul(xn, a0));
+            V3 x1 = add(mul(x, 1.0f - a1), mul(xn, a1));
+            const float cur_sign = signf(iso_value_at(x1, r) - S.iso_value);
+            if (first_point) {
+                first_point = false;
+                last_sign = cur_sign;
+            }
+            if (last_sign != cur_sign) {
+                iso_refine(x1, x0, cur_sign, r);
+                x = x1;
+                iso_scatter(x, w, weights, r);
+                x = add(x, mul(w, 1e-4f));
+                first_point = true;
+                ev = true;
+                float tmin;
+                if (ray_box(bmin(), bmax(), x, w, tmin, tmax)) {
+                    x = add(x, mul(w, tmin));
+                    d = tmax - tmin;
+                }
+                return true;
+            }
+        }
+        return false;
+    }
     V3 delta_iso(V3 x, V3 w, Rng& r, bool& ev) {
         float tmin, tmax;
         const float absorb = 1.0f - S.albedo;
         V3 weights = v3(1, 1, 1);
         float last_sign = 0.0f;
         bool first_point = true;
-        const int nsub = S.iso_subdivisions;
         int it = 0;
         if (ray_box(bmin(), bmax(), x, w, tmin, tmax)) {
             x = add(x, mul(w, tmin));
@@ -1013,32 +1045,7 @@ struct Tracer {
                 if (t > d) break;
                 V3 xn = add(x, mul(w, t));
                 float dens = sample(xn, r);
-                bool hit = false;
-                for (int sub = 0; sub < nsub; sub++) {
-                    const float a0 = (float)sub / (float)nsub, a1 = (float)(sub + 1) / (float)nsub;
-                    const V3 x0 = add(mul(x, 1.0f - a0), mul(xn, a0));
-                    V3 x1 = add(mul(x, 1.0f - a1), mul(xn, a1));
-                    const float cur_sign = signf(iso_value_at(x1, r) - S.iso_value);
-                    if (first_point) {
-                        first_point = false;
-                        last_sign = cur_sign;
-                    }
-                    if (last_sign != cur_sign) {
-                        iso_refine(x1, x0, cur_sign, r);
-                        x = x1;
-                        iso_scatter(x, w, weights, r);
-                        x = add(x, mul(w, 1e-4f));
-                        first_point = true;
-                        hit = true;
-                        ev = true;
-                        if (ray_box(bmin(), bmax(), x, w, tmin, tmax)) {
-                            x = add(x, mul(w, tmin));
-                            d = tmax - tmin;
-                        }
-                        break;
-                    }
-                }
-                if (hit) {
+                if (iso_check(x, xn, w, d, tmax, weights, last_sign, first_point, r, ev)) {
                     if (weights.x < 1e-3f && weights.y < 1e-3f && weights.z < 1e-3f) return v3(0, 0, 0);
                     continue;
                 }
@@ -1381,20 +1388,30 @@ struct Tracer {
     }
 
     // deltaTrackingSpectral (DeltaTracking.glsl:33-163)
+    // with isosurfaces (USE_ISOSURFACES, DeltaTracking.glsl:37-63 and the CheckIsosurfaceHit.glsl include):
+    // the 1000-iteration cap, the segment check and the surface throughput in the spectral weights
     V3 spectral_delta(V3 x, V3 w, Rng& r, bool& ev) {
         const float maj = maxc(ext3());
         V3 weights = v3(1, 1, 1);
+        float last_sign = 0.0f;
+        bool first_point = true;
+        int it = 0;
         float tmin, tmax;
         if (ray_box(bmin(), bmax(), x, w, tmin, tmax)) {
             x = add(x, mul(w, tmin));
             float d = tmax - tmin;
             int bounces = 0;
             while (true) {
+                if (S.use_iso && ++it == 1000) return v3(0, 0, 0);
                 if (guard()) return v3(0, 0, 0);
                 float t = -m_log(std::max(0.0000000001f, 1.0f - rnd(r))) * (1.0f / maj);
                 if (t > d) break;
                 V3 xn = add(x, mul(w, t));
                 float dens = sample(xn, r);
+                if (S.use_iso && iso_check(x, xn, w, d, tmax, weights, last_sign, first_point, r, ev)) {
+                    if (weights.x < 1e-3f && weights.y < 1e-3f && weights.z < 1e-3f) return v3(0, 0, 0);
+                    continue;
+                }
                 x = xn;
                 V3 sa, ss, sn;
                 float pa, ps, pn;

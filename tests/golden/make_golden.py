@@ -140,6 +140,13 @@ def cases():
         kw2.update(iso_value=0.3, iso_color=(0.9, 0.6, 0.3), extinction=40.0, albedo=0.9, g=0.2)
         out["fbm_" + name] = SceneSpec(grid=fbm, mode="delta", interp="trilinear", iso=True, iso_brdf="Disney (2012)",
                                        brdf_params=params, **kw2)
+    # spectral delta tracking with isosurfaces: a chromatic medium around the coloured density surface
+    for name, prob in {"sdt_hist_iso": 2, "sdt_max_iso": 0}.items():
+        kw2 = dict(base)
+        kw2.update(iso_value=0.3, iso_color=(0.9, 0.6, 0.3), extinction=40.0, g=0.2,
+                   extinction_base=(1.0, 0.7, 0.4), albedo_rgb=(0.95, 0.8, 0.9))
+        out["fbm_" + name] = SceneSpec(grid=fbm, mode="spectral_delta", sdt_prob=prob, interp="trilinear", iso=True,
+                                       **kw2)
     # isosurfaces of the gradient magnitude (ISOSURFACE_TYPE_GRADIENT) at its upper quartile inside the cloud
     gm = gradient_magnitude(fbm)
     kw2 = dict(base)
