@@ -536,10 +536,11 @@ def run_trackers(vpt, lib, ctx, img, stream, ctypes_stream, barrier, max_over_ra
     ref_mean = rs / ref_spp
     ref_var = torch.clamp(rq / ref_spp - ref_mean * ref_mean, min=0.0) * (ref_spp / (ref_spp - 1))
     out = {}
-    # delta tracking with isosurfaces at density 0.5 (Lambertian surfaces, trilinear lookups) is a
-    # different image: its rate only
-    for name, mode in list(TRACKERS.items()) + [("nee_empty_space_skipping", 5), ("delta_isosurfaces", 0)]:
-        iso = name == "delta_isosurfaces"
+    # delta and next event tracking with isosurfaces at density 0.5 (Lambertian surfaces, trilinear
+    # lookups; next event tracking with surface light samples) make a different image: their rates only
+    for name, mode in list(TRACKERS.items()) + [("nee_empty_space_skipping", 5), ("delta_isosurfaces", 0),
+                                                ("nee_isosurfaces", 5)]:
+        iso = name in ("delta_isosurfaces", "nee_isosurfaces")
         vpt.set_vpt_mode(mode)
         vpt.set_use_isosurfaces(iso)
         # next event tracking whose shadow rays skip the occupancy grid's empty 8^3 blocks

@@ -1623,11 +1623,16 @@ VptStatus vpt_render_frames(VptContext* ctx, int frames, void* stream) {
         tracker != vpt::kSpectralDelta && tracker != vpt::kSpectralNextEvent)
         return fail(ctx, VPT_ERR_UNSUPPORTED,
                     "the transfer function applies to delta, next event and spectral tracking (as in the reference)");
-    if (ctx->use_iso && ((tracker != vpt::kDelta && tracker != vpt::kSpectralDelta) || ctx->use_sparse ||
-                         (ctx->use_tf && ctx->tf.ptr)))
+    if (ctx->use_iso && ((tracker != vpt::kDelta && tracker != vpt::kSpectralDelta && tracker != vpt::kNextEvent) ||
+                         ctx->use_sparse || (ctx->use_tf && ctx->tf.ptr)))
         return fail(ctx, VPT_ERR_UNSUPPORTED,
-                    "isosurfaces are built for delta and spectral delta tracking on dense grids without a transfer "
-                    "function");
+                    "isosurfaces are built for delta, spectral delta and next event tracking on dense grids without a "
+                    "transfer function");
+    if (ctx->use_iso && tracker == vpt::kNextEvent &&
+        (ctx->use_ess || (ctx->use_lights && !ctx->lights.empty()) || ctx->env_kind == VPT_ENV_IMAGE))
+        return fail(ctx, VPT_ERR_UNSUPPORTED,
+                    "next event tracking with isosurfaces is built for sky light samples: no lights, no environment "
+                    "image, no empty-space skipping");
     if (ctx->env_kind == VPT_ENV_IMAGE && !ctx->env_pyramid.ptr)
         return fail(ctx, VPT_ERR_STATE, "environment image not loaded");
     cudaSetDevice(ctx->device);

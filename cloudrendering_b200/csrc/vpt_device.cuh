@@ -711,6 +711,20 @@ VPT_DEV F3 iso_normal(const TraceParams& P, F3 pos) {
     return f3(g.x / l, g.y / l, g.z / l);
 }
 
+// The shading frame at a surface hit: the normal turned against the ray, ComputeDefaultBasis's
+// tangent and bitangent (RayTracingUtilities.glsl:20-28), and the direction back along the ray.
+struct IsoFrame {
+    F3 n, t, b, view;
+};
+
+// One BRDF sample at a surface hit (computeBrdf of the selected BRDF file): the new direction, the value
+// the throughput is multiplied by, the lobe flags and the lobe's samplingPDF (read by MIS).
+struct IsoBrdfSample {
+    F3 dir, value;
+    bool specular, clearcoat;
+    float pdf;
+};
+
 // mat3(t, b, n) * (x, y, z), summed in the order of a GLSL matrix-vector product
 VPT_DEV F3 iso_frame(F3 t, F3 b, F3 n, float x, float y, float z) {
     return f3((t.x * x + b.x * y) + n.x * z, (t.y * x + b.y * y) + n.y * z, (t.z * x + b.z * y) + n.z * z);
@@ -722,8 +736,8 @@ VPT_DEV F3 iso_frame(F3 t, F3 b, F3 n, float x, float y, float z) {
 // plus F G v.h / (n.h v.n) for a GGX sample or F G D v.h sin(theta_h) / v.n for a diffuse one
 // (F Schlick with f0 = mix(0.16 specular^2, colour, metallic), D GGX, G Smith-Schlick with k = r^2 / 2),
 // and the throughput takes that value as it is.  sel, u are the hit's second and third random numbers.
-VPT_DEV void iso_cook_torrance(const TraceParams& P, Rng& rng, F3 n, F3 t, F3 b, float sel, float u, F3& w,
-                               F3& weights) {
+VPT_DEV IsoBrdfSample iso_cook_torrance(const TraceParams& P, Rng& rng, const IsoFrame& fr, float sel, float u) {
+    const F3 n = fr.n, t = fr.t, b = fr.b, view = fr.view;
     const float pi = 3.14159265358979323846f;  // M_PI as the shader's float
     const float v = rng_next(rng);
     const float metallic = P.brdf[kBrdfMetallic], specular = P.brdf[kBrdfSpecular];
@@ -731,7 +745,6 @@ VPT_DEV void iso_cook_torrance(const TraceParams& P, Rng& rng, F3 n, F3 t, F3 b,
     const float specular_w = metallic + (1.0f - rough) * (1.0f + specular);
     const float diffuse_w = 1.0f - metallic;
     const float specular_p = specular_w * (1.0f / (specular_w + diffuse_w));
-    const F3 view = normalize3(f3(-w.x, -w.y, -w.z));
     const float alpha = rough * rough;
     const float alpha2 = alpha * alpha;
     const bool specular_hit = sel < specular_p;
@@ -756,12 +769,9 @@ VPT_DEV void iso_cook_torrance(const TraceParams& P, Rng& rng, F3 n, F3 t, F3 b,
     const float k = alpha / 2.0f;
     const float gl = ldotn < 0.001f ? 0.001f : ldotn, gv = vdotn < 0.001f ? 0.001f : vdotn;
     const float g = (gl / (gl * (1.0f - k) + k)) * (gv / (gv * (1.0f - k) + k));
-    float d = 0.0f, sth = 0.0f;
-    if (!specular_hit) {
-        const float bq = (ndoth * ndoth) * (alpha2 - 1.0f) + 1.0f;
-        d = ((1.0f / pi) * alpha2) / (bq * bq);
-        sth = sqrtf(1.0f - fminf(ndoth * ndoth, 0.95f));
-    }
+    const float bq = (ndoth * ndoth) * (alpha2 - 1.0f) + 1.0f;
+    const float d = ((1.0f / pi) * alpha2) / (bq * bq);
+    const float sth = sqrtf(1.0f - fminf(ndoth * ndoth, 0.95f));
     const float cx[3] = {P.iso_color.x, P.iso_color.y, P.iso_color.z};
     float o[3];
     for (int i = 0; i < 3; ++i) {
@@ -771,8 +781,43 @@ VPT_DEV void iso_cook_torrance(const TraceParams& P, Rng& rng, F3 n, F3 t, F3 b,
                                         : ((((f * g) * d) * vdoth) * sth) / vdotn;
         o[i] = (cx[i] * (1.0f - f)) * (1.0f - metallic) + spec;
     }
-    weights = f3(weights.x * o[0], weights.y * o[1], weights.z * o[2]);
-    w = l;
+    IsoBrdfSample r;
+    r.dir = l;
+    r.value = f3(o[0], o[1], o[2]);
+    r.specular = specular_hit;
+    r.clearcoat = false;
+    r.pdf = specular_hit ? d : 1.0f / pi;  // samplingPDF
+    return r;
+}
+
+// CookTorrance.glsl evaluateBrdfPdf at the light direction l: the diffuse-sample form of the value
+// (F G D v.h sin(theta_h) / v.n) plus the diffuse colour / pi
+VPT_DEV F3 cook_torrance_pdf_value(const TraceParams& P, const IsoFrame& fr, F3 l) {
+    const float pi = 3.14159265358979323846f;
+    const float metallic = P.brdf[kBrdfMetallic], specular = P.brdf[kBrdfSpecular];
+    const float rough = fminf(fmaxf(P.brdf[kBrdfRoughness], 0.05f), 1.0f);
+    const float alpha = rough * rough;
+    const float alpha2 = alpha * alpha;
+    const F3 view = fr.view, n = fr.n;
+    const F3 h = normalize3(f3(l.x + view.x, l.y + view.y, l.z + view.z));
+    const float ndoth = dot3(h, n), vdotn = dot3(view, n), ldotn = dot3(l, n), vdoth = dot3(view, h);
+    const float f0s = 0.16f * (specular * specular);
+    const float p5 = m_pow5(1.0f - vdoth);
+    const float k = alpha / 2.0f;
+    const float gl = ldotn < 0.001f ? 0.001f : ldotn, gv = vdotn < 0.001f ? 0.001f : vdotn;
+    const float g = (gl / (gl * (1.0f - k) + k)) * (gv / (gv * (1.0f - k) + k));
+    const float bq = (ndoth * ndoth) * (alpha2 - 1.0f) + 1.0f;
+    const float d = ((1.0f / pi) * alpha2) / (bq * bq);
+    const float sth = sqrtf(1.0f - fminf(ndoth * ndoth, 0.95f));
+    const float cx[3] = {P.iso_color.x, P.iso_color.y, P.iso_color.z};
+    float o[3];
+    for (int i = 0; i < 3; ++i) {
+        const float f0 = f0s * (1.0f - metallic) + cx[i] * metallic;
+        const float f = f0 + (1.0f - f0) * p5;
+        const float spec = ((((f * g) * d) * vdoth) * sth) / vdotn;
+        o[i] = ((cx[i] * (1.0f - f)) * (1.0f - metallic)) * (1.0f / pi) + spec;
+    }
+    return f3(o[0], o[1], o[2]);
 }
 
 // Disney2012.glsl computeBrdf: sampleBrdf picks the anisotropic specular lobe (weight metallic +
@@ -780,7 +825,8 @@ VPT_DEV void iso_cook_torrance(const TraceParams& P, Rng& rng, F3 n, F3 t, F3 b,
 // clearcoat lobe (clamp(clearcoat, 0, 1)); evaluateBrdf returns diffuse + specular + clearcoat as the
 // shader writes them (its cos-of-a-cosine Fresnel arguments and its D term included), and the throughput
 // takes that value as it is.  sel, u are the hit's second and third random numbers.
-VPT_DEV void iso_disney(const TraceParams& P, Rng& rng, F3 n, F3 t, F3 b, float sel, float u, F3& w, F3& weights) {
+VPT_DEV IsoBrdfSample iso_disney(const TraceParams& P, Rng& rng, const IsoFrame& fr, float sel, float u) {
+    const F3 n = fr.n, t = fr.t, b = fr.b, view = fr.view;
     const float pi = 3.14159265358979323846f;  // M_PI
     const float pi_c = 3.14159265359f;         // PI (VptUtils.glsl:27), used by GTR1 and atan2
     const float* q = P.brdf;
@@ -795,7 +841,6 @@ VPT_DEV void iso_disney(const TraceParams& P, Rng& rng, F3 n, F3 t, F3 b, float 
     const float clearcoat_w = fminf(fmaxf(q[kBrdfClearcoat], 0.0f), 1.0f);
     const float norm = 1.0f / ((specular_w + diffuse_w) + clearcoat_w);
     const float specular_p = specular_w * norm, diffuse_p = diffuse_w * norm;
-    const F3 view = normalize3(f3(-w.x, -w.y, -w.z));
     const float v0 = rng_next(rng);
     const int lobe = sel < specular_p ? 0 : (sel < specular_p + diffuse_p ? 1 : 2);  // specular, diffuse, clearcoat
     const bool specular_hit = lobe != 1, clearcoat_hit = lobe == 2;
@@ -894,16 +939,87 @@ VPT_DEV void iso_disney(const TraceParams& P, Rng& rng, F3 n, F3 t, F3 b, float 
                                : ((((((f_spec * d_spec) * g_spec) * 4.0f) * cos_l) * vdoth) * sin_th);
         o[i] = (diffuse + spec) + clear;
     }
-    weights = f3(weights.x * o[0], weights.y * o[1], weights.z * o[2]);
-    w = l;
+    IsoBrdfSample r;
+    r.dir = l;
+    r.value = f3(o[0], o[1], o[2]);
+    r.specular = specular_hit;
+    r.clearcoat = clearcoat_hit;
+    r.pdf = specular_hit ? (clearcoat_hit ? d_cc : d_spec) : 1.0f / pi;  // samplingPDF
+    return r;
+}
+
+// Disney2012.glsl evaluateBrdfPdf at the light direction l: the terms of evaluateBrdf in their
+// non-specular-sample form, the diffuse term always divided by pi, sin(theta_h) from
+// sqrt(1 - min(n.h^2, 0.95)), and 0.01 as the floor of the subsurface denominator
+VPT_DEV F3 disney_pdf_value(const TraceParams& P, const IsoFrame& fr, F3 l) {
+    const float pi = 3.14159265358979323846f, pi_c = 3.14159265359f;
+    const float* q = P.brdf;
+    const float roughness = q[kBrdfRoughness], metallic = q[kBrdfMetallic];
+    const float aspect = sqrtf(1.0f - q[kBrdfAnisotropic] * 0.9f);
+    const float r2 = roughness * roughness;
+    const float ax0 = r2 / aspect, ay0 = r2 * aspect;
+    const float ax = 0.001f < ax0 ? ax0 : 0.001f, ay = 0.001f < ay0 ? ay0 : 0.001f;
+    const F3 view = fr.view, n = fr.n, t = fr.t, b = fr.b;
+    const F3 hh = normalize3(f3(l.x + view.x, l.y + view.y, l.z + view.z));
+    const float cos_h = dot3(hh, n), cos_d = dot3(l, hh), cos_v = dot3(view, n), cos_l = dot3(l, n);
+    const float vdoth = dot3(view, hh);
+    const float c[3] = {P.iso_color.x, P.iso_color.y, P.iso_color.z};
+    const float lum = (0.3f * c[0] + 0.6f * c[1]) + 0.1f * c[2];
+    const float cd = m_cos(cos_d);
+    const float cd2 = cd * cd;
+    const float f_d90 = 0.5f + (2.0f * roughness) * cd2;
+    const float pl = m_pow5(1.0f - m_cos(cos_l)), pv = m_pow5(1.0f - m_cos(cos_v));
+    const float f_d = (1.0f + (f_d90 - 1.0f) * pl) * (1.0f + (f_d90 - 1.0f) * pv);
+    const float fss90 = roughness * cd2;
+    const float f_ss = (1.0f + (fss90 - 1.0f) * pl) * (1.0f + (fss90 - 1.0f) * pv);
+    const float lv = cos_l + cos_v;
+    const float f_dss = 1.25f * (f_ss * (1.0f / (lv < 0.01f ? 0.01f : lv) - 0.5f) + 0.5f);
+    const float f_h = m_pow5(1.0f - cos_d);
+    const float sub = q[kBrdfSubsurface];
+    const float fd_mix = f_d * (1.0f - sub) + f_dss * sub;
+    const float dx = dot3(t, hh) / ax, dy = dot3(b, hh) / ay;
+    const float dd = dx * dx + dy * dy;
+    const float d_spec = 1.0f / (((pi * ax) * ay) * (dd * dd) + cos_h * cos_h);
+    const float glx = dot3(t, l) * ax, gly = dot3(b, l) * ay, gvx = dot3(t, view) * ax, gvy = dot3(b, view) * ay;
+    float g_spec = 1.0f / (cos_v + sqrtf((glx * glx + gly * gly) + cos_v * cos_v));
+    g_spec = g_spec * (1.0f / (cos_v + sqrtf((gvx * gvx + gvy * gvy) + cos_v * cos_v)));
+    const float sth = sqrtf(1.0f - fminf(cos_h * cos_h, 0.95f));
+    const float f_cc = 0.04f * (1.0f - f_h) + 1.0f * f_h;
+    const float gloss = q[kBrdfClearcoatGloss];
+    const float a_cc = 0.1f * (1.0f - gloss) + 0.001f * gloss;
+    float d_cc;
+    if (a_cc >= 1.0f) {
+        d_cc = 1.0f / pi_c;
+    } else {
+        const float a2 = a_cc * a_cc;
+        d_cc = (a2 - 1.0f) / ((pi_c * m_log(a2)) * (1.0f + ((a2 - 1.0f) * cos_h) * cos_h));
+    }
+    const float bl = cos_l * cos_l, bv = cos_v * cos_v, ag = 0.25f * 0.25f;
+    const float g_cc = (1.0f / ((cos_l < -0.99f ? -0.99f : cos_l) + sqrtf((ag + bl) - ag * bl))) *
+                       (1.0f / ((cos_v < -0.99f ? -0.99f : cos_v) + sqrtf((ag + bv) - ag * bv)));
+    const float clear = (((((q[kBrdfClearcoat] * f_cc) * d_cc) * g_cc) * cos_l) * vdoth) * sth;
+    const float st = q[kBrdfSpecularTint], sh = q[kBrdfSheenTint];
+    const float spec_scale = q[kBrdfSpecular] * 0.08f;
+    float o[3];
+    for (int i = 0; i < 3; ++i) {
+        const float tint = lum > 0.0f ? c[i] / lum : 1.0f;
+        const float spec0 = (spec_scale * (1.0f * (1.0f - st) + tint * st)) * (1.0f - metallic) + c[i] * metallic;
+        const float sheen = (f_h * q[kBrdfSheen]) * (1.0f * (1.0f - sh) + tint * sh);
+        const float diffuse = ((c[i] * fd_mix + sheen) * (1.0f - metallic)) * (1.0f / pi);
+        const float f_spec = spec0 * (1.0f - f_h) + 1.0f * f_h;
+        const float spec = ((((((f_spec * d_spec) * g_spec) * 4.0f) * cos_l) * vdoth) * sth);
+        o[i] = (diffuse + spec) + clear;
+    }
+    return f3(o[0], o[1], o[2]);
 }
 
 // An opaque surface hit (getIsoSurfaceHit, VptUtils.glsl:1151-1334): one random number for the
 // opacity test, the normal turned against the ray, the ComputeDefaultBasis frame
 // (RayTracingUtilities.glsl:20-28), then the selected BRDF.  Lambertian: a cosine-weighted direction
 // (Lambertian.glsl is included before UNIFORM_SAMPLING is defined, so the concentric-disk map of
-// VptUtils.glsl:1078-1098 and a pdf factor equal to the cosine), throughput *= color * cos / cos.
-VPT_DEV void iso_scatter(const TraceParams& P, Rng& rng, F3 p, F3& w, F3& weights) {
+// VptUtils.glsl:1078-1098 and a pdf factor equal to the cosine), value color * cos / cos.  This part
+// ends at computeBrdf and returns the frame and the sample.
+VPT_DEV IsoBrdfSample iso_sample(const TraceParams& P, Rng& rng, F3 p, F3 w, IsoFrame& fr) {
     (void)rng_next(rng);  // isoSurfaceOpacity (1) < random() never holds
     F3 n = iso_normal(P, p);
     if (dot3(w, n) > 0.0f) n = -n;
@@ -911,31 +1027,32 @@ VPT_DEV void iso_scatter(const TraceParams& P, Rng& rng, F3 p, F3& w, F3& weight
     const F3 b = normalize3(fabsf(n.z) > 0.99999f ? f3(-n.x * n.y, 1.0f - n.y * n.y, yz)
                                                   : f3(-n.x * n.z, yz, 1.0f - n.z * n.z));
     const F3 t = cross3(b, n);
+    fr.n = n;
+    fr.t = t;
+    fr.b = b;
+    fr.view = normalize3(f3(-w.x, -w.y, -w.z));
     const float xi0 = rng_next(rng);
     const float xi1 = rng_next(rng);
-    if (P.iso_brdf == kBrdfCookTorrance) {
-        iso_cook_torrance(P, rng, n, t, b, xi0, xi1, w, weights);
-        return;
-    }
-    if (P.iso_brdf == kBrdfDisney) {
-        iso_disney(P, rng, n, t, b, xi0, xi1, w, weights);
-        return;
-    }
+    if (P.iso_brdf == kBrdfCookTorrance) return iso_cook_torrance(P, rng, fr, xi0, xi1);
+    if (P.iso_brdf == kBrdfDisney) return iso_disney(P, rng, fr, xi0, xi1);
+    IsoBrdfSample r;
+    r.specular = false;
+    r.clearcoat = false;
+    r.pdf = 0.0f;
     if (P.iso_brdf != kBrdfLambertian) {
         // BlinnPhong.glsl / ConstantLighting.glsl: a uniformly sampled hemisphere direction
         // (sampleHemisphere, VptUtils.glsl:1071-1077: phi = 2 pi xi.y, z = xi.x) in the same frame
         const float pi = 3.14159265358979323846f;  // M_PI as the shader's float
         const float phi = (2.0f * pi) * xi1;
-        const float r = sqrtf(1.0f - xi0 * xi0);
-        const float lx = m_cos(phi) * r, ly = m_sin(phi) * r;
+        const float rr = sqrtf(1.0f - xi0 * xi0);
+        const float lx = m_cos(phi) * rr, ly = m_sin(phi) * rr;
         const F3 out = f3((t.x * lx + b.x * ly) + n.x * xi0, (t.y * lx + b.y * ly) + n.y * xi0,
                           (t.z * lx + b.z * ly) + n.z * xi0);
         F3 c = P.iso_color;  // ConstantLighting.glsl: the colour, whatever the direction
-        if (P.iso_brdf == 1) {
+        if (P.iso_brdf == kBrdfBlinnPhong) {
             // BlinnPhong.glsl evaluateBrdf: 2 pi colour (n.h)^10 / norm, h = normalize(normalize(-w) + l),
             // norm = clamp((n + 2) / (4 pi 2^(-n/2)), (n + 2) / (8 pi), (n + 4) / (8 pi)) with n = 10
-            const F3 view = normalize3(f3(-w.x, -w.y, -w.z));
-            const F3 h = normalize3(f3(view.x + out.x, view.y + out.y, view.z + out.z));
+            const F3 h = normalize3(f3(fr.view.x + out.x, fr.view.y + out.y, fr.view.z + out.z));
             const float e = 10.0f;
             const float norm = fminf(fmaxf((e + 2.0f) / ((4.0f * pi) * 0.03125f), (e + 2.0f) / (8.0f * pi)),
                                      (e + 4.0f) / (8.0f * pi));
@@ -943,9 +1060,9 @@ VPT_DEV void iso_scatter(const TraceParams& P, Rng& rng, F3 p, F3& w, F3& weight
             const float k = 2.0f * pi;
             c = f3((k * P.iso_color.x) * s, (k * P.iso_color.y) * s, (k * P.iso_color.z) * s);
         }
-        weights = f3(weights.x * c.x, weights.y * c.y, weights.z * c.z);
-        w = out;
-        return;
+        r.dir = out;
+        r.value = c;
+        return r;
     }
     const float ox = 2.0f * xi0 - 1.0f, oy = 2.0f * xi1 - 1.0f;
     float dx = 0.0f, dy = 0.0f;
@@ -965,9 +1082,61 @@ VPT_DEV void iso_scatter(const TraceParams& P, Rng& rng, F3 p, F3& w, F3& weight
     const F3 out = f3((t.x * dx + b.x * dy) + n.x * hz, (t.y * dx + b.y * dy) + n.y * hz,
                       (t.z * dx + b.z * dy) + n.z * hz);
     const float cosv = dot3(out, n);
-    weights = f3(weights.x * ((P.iso_color.x * cosv) / cosv), weights.y * ((P.iso_color.y * cosv) / cosv),
-                 weights.z * ((P.iso_color.z * cosv) / cosv));
-    w = out;
+    r.dir = out;
+    r.value = f3((P.iso_color.x * cosv) / cosv, (P.iso_color.y * cosv) / cosv, (P.iso_color.z * cosv) / cosv);
+    return r;
+}
+
+// An opaque surface hit without next-event estimation: throughput *= the BRDF value, w = its direction.
+VPT_DEV void iso_scatter(const TraceParams& P, Rng& rng, F3 p, F3& w, F3& weights) {
+    IsoFrame fr;
+    const IsoBrdfSample s = iso_sample(P, rng, p, w, fr);
+    weights = f3(weights.x * s.value.x, weights.y * s.value.y, weights.z * s.value.z);
+    w = s.dir;
+}
+
+// evaluateBrdfNee of the selected BRDF for the light direction l (USE_ISOSURFACE_NEE): the value the
+// light sample is weighed with, and the sampling pdfs of the BRDF's own direction and of l that MIS
+// reads (the specular BRDFs only).  Lambertian.glsl takes its non-uniform branch (UNIFORM_SAMPLING is
+// defined after it is included): colour / pi * n.l.
+VPT_DEV F3 iso_brdf_nee(const TraceParams& P, const IsoFrame& fr, const IsoBrdfSample& s, F3 l, float& pdf_out,
+                        float& pdf_nee) {
+    const float pi = 3.14159265358979323846f;
+    const F3 c = P.iso_color;
+    pdf_out = 0.0f;
+    pdf_nee = 0.0f;
+    if (P.iso_brdf == kBrdfLambertian) {
+        const float th = dot3(fr.n, l);
+        return f3((c.x / pi) * th, (c.y / pi) * th, (c.z / pi) * th);
+    }
+    if (P.iso_brdf == kBrdfAmbient) {
+        const float k = 2.0f * pi;
+        return f3(c.x / k, c.y / k, c.z / k);
+    }
+    if (P.iso_brdf == kBrdfBlinnPhong) {
+        const float e = 10.0f;
+        const float norm = fminf(fmaxf((e + 2.0f) / ((4.0f * pi) * 0.03125f), (e + 2.0f) / (8.0f * pi)),
+                                 (e + 4.0f) / (8.0f * pi));
+        const F3 h = normalize3(f3(fr.view.x + l.x, fr.view.y + l.y, fr.view.z + l.z));
+        const float v = m_pow(fmaxf(dot3(fr.n, h), 0.0f), e) / norm;
+        return f3(c.x * v, c.y * v, c.z * v);
+    }
+    const F3 h = normalize3(f3(s.dir.x + fr.view.x, s.dir.y + fr.view.y, s.dir.z + fr.view.z));
+    const float cos_h = dot3(h, fr.n);
+    const float sin_h = sqrtf(1.0f / (cos_h * cos_h));  // as the shaders write it
+    const F3 hn = normalize3(f3(l.x + fr.view.x, l.y + fr.view.y, l.z + fr.view.z));
+    const float cos_hn = dot3(hn, fr.n);
+    const float sin_hn = sqrtf(1.0f - fminf(cos_hn * cos_hn, 0.95f));
+    if (P.iso_brdf == kBrdfDisney && s.specular) {
+        pdf_out = s.pdf * cos_h;
+        pdf_nee = s.pdf * cos_hn;
+    } else {
+        pdf_out = (s.pdf * cos_h) * sin_h;
+        pdf_nee = (s.pdf * cos_hn) * sin_hn;
+    }
+    const F3 v = P.iso_brdf == kBrdfDisney ? disney_pdf_value(P, fr, l) : cook_torrance_pdf_value(P, fr, l);
+    const float nl = dot3(l, fr.n);
+    return f3(v.x * nl, v.y * nl, v.z * nl);
 }
 
 }  // namespace vpt

@@ -25,12 +25,18 @@ uint64_t padded_paths(int width, int height, uint32_t frames) {
 cudaError_t launch_trace(const TraceParams& P, int tracker, int use_ess, int schedule, int features,
                          int persistent_blocks, cudaStream_t stream) {
     if (P.iso) {
-        // isosurfaces: delta and spectral delta tracking on dense grids, trilinear lookups, no transfer
-        // function
-        if ((tracker != kDelta && tracker != kSpectralDelta) || P.grid_kind != kDense || P.tf)
+        // isosurfaces: delta, spectral delta and next event tracking on dense grids, trilinear lookups,
+        // no transfer function
+        if ((tracker != kDelta && tracker != kSpectralDelta && tracker != kNextEvent) || P.grid_kind != kDense ||
+            P.tf)
             return cudaErrorNotSupported;
         if (tracker == kSpectralDelta)
             return launch_tracker_spectral_delta_iso(P, schedule, features, persistent_blocks, stream);
+        if (tracker == kNextEvent) {
+            // next event tracking: sky light samples only (no lights, no environment image, no skipping)
+            if (use_ess || P.num_lights > 0 || P.env_kind == kEnvImage) return cudaErrorNotSupported;
+            return launch_tracker_nee_iso(P, schedule, features, persistent_blocks, stream);
+        }
         return launch_tracker_delta_iso(P, schedule, features, persistent_blocks, stream);
     }
     if (P.grid_kind == kNanoVdb) {

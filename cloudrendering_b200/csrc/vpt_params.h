@@ -21,9 +21,11 @@ enum Tracker : int {
     // no reference counterpart: next-event estimation with residual-ratio-tracked shadow rays and
     // supervoxel-majorant free paths (VPT_MODE_RESIDUAL_RATIO_TRACKING_UNBIASED)
     kResidualRatioNee = 9,
-    // kernel variants, not VptModes: delta and spectral delta tracking with isosurfaces inside the volume
+    // kernel variants, not VptModes: delta, spectral delta and next event tracking with isosurfaces inside
+    // the volume
     kDeltaIso = 300,
     kSpectralDeltaIso = 301,
+    kNextEventIso = 302,
 };
 
 // Collision probabilities of spectral tracking (SpectralDeltaTrackingCollisionProbability,

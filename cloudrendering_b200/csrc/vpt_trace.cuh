@@ -197,6 +197,7 @@ VPT_DEV F3 run_tracker(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, Fi
     if constexpr (TRACKER == kResidualRatioNee) return track_residual_ratio_nee(P, sample, rng, x, w, fe, pc);
     if constexpr (TRACKER == kSpectralDelta) return track_delta_spectral<false>(P, sample, rng, x, w, fe, pc);
     if constexpr (TRACKER == kSpectralDeltaIso) return track_delta_spectral<true>(P, sample, rng, x, w, fe, pc);
+    if constexpr (TRACKER == kNextEventIso) return track_nee_iso(P, sample, rng, x, w, fe, pc);
     if constexpr (TRACKER == kSpectralNextEvent) return track_nee_spectral<false>(P, sample, rng, x, w, fe, pc);
     if constexpr (TRACKER == kSpectralNextEvent + 100) return track_nee_spectral<true>(P, sample, rng, x, w, fe, pc);
     if (TRACKER == kNextEvent + 100) return track_nee<true>(P, sample, rng, x, w, fe, pc);
@@ -1121,5 +1122,6 @@ VPT_DECLARE_TRACKER(kSpectralNextEvent, kNanoVdb);
 cudaError_t launch_tracker_delta_iso(const TraceParams& P, int schedule, int features, int pb, cudaStream_t s);
 cudaError_t launch_tracker_spectral_delta_iso(const TraceParams& P, int schedule, int features, int pb,
                                               cudaStream_t s);
+cudaError_t launch_tracker_nee_iso(const TraceParams& P, int schedule, int features, int pb, cudaStream_t s);
 
 }  // namespace vpt

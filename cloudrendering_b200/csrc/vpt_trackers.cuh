@@ -118,9 +118,13 @@ VPT_DEV F3 track_delta(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, Fi
 // random number drawn) that value is reused; any other sampler looks it up again, as the reference
 // does, so that its random stream stays the reference's.
 template <class S>
+VPT_DEV void iso_surface_nee(const TraceParams& P, S& sample, Rng& rng, F3 x, const IsoFrame& fr,
+                             const IsoBrdfSample& bs, F3 thr, F3& color, PathCtx& pc);
+
+template <bool NEE = false, class S>
 VPT_DEV bool iso_segment(const TraceParams& P, S& sample, Rng& rng, F3& x, F3 xn, float density, F3& w, float& d,
                          float& tmax, F3& weights, float& last_sign, bool& first_point, uint32_t& lookups,
-                         FirstEvent* fe) {
+                         FirstEvent* fe, F3* nee_color = nullptr, PathCtx* pc = nullptr) {
     const int nsub = P.iso_subdivisions;
     for (int sub = 0; sub < nsub; ++sub) {
         const float a0 = (float)sub / (float)nsub, a1 = (float)(sub + 1) / (float)nsub;
@@ -149,7 +153,15 @@ VPT_DEV bool iso_segment(const TraceParams& P, S& sample, Rng& rng, F3& x, F3 xn
                 else x0 = mid;
             }
             x = x1;
-            iso_scatter(P, rng, x, w, weights);
+            if constexpr (NEE) {  // USE_ISOSURFACE_NEE: the light sample before the throughput takes the BRDF
+                IsoFrame fr;
+                const IsoBrdfSample bs = iso_sample(P, rng, x, w, fr);
+                iso_surface_nee(P, sample, rng, x, fr, bs, weights, *nee_color, *pc);
+                weights = f3(weights.x * bs.value.x, weights.y * bs.value.y, weights.z * bs.value.z);
+                w = bs.dir;
+            } else {
+                iso_scatter(P, rng, x, w, weights);
+            }
             x = x + w * 1e-4f;
             first_point = true;
             // firstEvent of a surface hit: density = extinction, depth = tMax - d + |x - x1|
@@ -283,6 +295,69 @@ VPT_DEV float shadow_transmittance(const TraceParams& P, S& sample, Rng& rng, F3
         }
     }
     return trans;
+}
+
+// Shadow rays with isosurfaces (calculateTransmittance, NeeTransmittance.glsl:5-119, after the
+// `#define USE_TRANSMITTANCE_DELTA_TRACKING` of its isosurface block): a delta-tracked 0/1 estimate,
+// 0 at the first tentative collision that is real.  The reference also bisects every isosurface
+// crossing on the way; without ISOSURFACE_USE_TF that changes neither the ray nor the random stream
+// (trilinear lookups draw no random number), so the crossings are not looked for here.
+template <class S>
+VPT_DEV float shadow_transmittance_delta(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, PathCtx& pc) {
+    float tmin, tmax;
+    if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
+        x = x + w * tmin;
+        float d = tmax - tmin;
+        while (true) {
+            if (guard(pc)) return 0.0f;
+            float t = free_path(rng, P.inv_extinction);
+            if (t > d) break;
+            F3 xn = x + w * t;
+            float density = sample(xn, rng);
+            pc.lookups++;
+            x = xn;
+            if (rng_next(rng) > 1.0f - density) return 0.0f;
+            d -= t;
+        }
+    }
+    return 1.0f;
+}
+
+// Next-event estimation at a surface hit (getIsoSurfaceHit with USE_ISOSURFACE_NEE, VptUtils.glsl:1213-1325,
+// no lights): a sky direction l from importanceSampleSkybox; when it lies above the surface, the
+// throughput times evaluateBrdfNee / pdf times the shadow ray's transmittance times the sky.  For a
+// specular sample of Cook-Torrance or Disney (MIS), the light sample is weighed with
+// pdf_l / (pdf_l + pdf_nee) and the BRDF's own direction adds its value weighed with
+// pdf_out / (1 / (4 PI) + pdf_out) through a second shadow ray.
+template <class S>
+VPT_DEV void iso_surface_nee(const TraceParams& P, S& sample, Rng& rng, F3 x, const IsoFrame& fr,
+                             const IsoBrdfSample& bs, F3 thr, F3& color, PathCtx& pc) {
+    float pdf_light;
+    const F3 l = importance_sample_sky(P, rng, pdf_light);
+    if (!(dot3(fr.n, l) > 0.0f)) return;
+    float pdf_out, pdf_nee;
+    const F3 rdf = iso_brdf_nee(P, fr, bs, l, pdf_out, pdf_nee);
+    const bool mis = (P.iso_brdf == kBrdfCookTorrance || P.iso_brdf == kBrdfDisney) && bs.specular;
+    if (mis) {
+        const float pdf_light_out = 1.0f / (4.0f * kPi);  // evaluateSkyboxPDF without an environment image
+        const float w_nee = pdf_light / (pdf_light + pdf_nee);
+        const float w_out = pdf_out / (pdf_light_out + pdf_out);
+        const float tr = shadow_transmittance_delta(P, sample, rng, x + l * 1e-4f, l, pc);
+        const F3 sky = sky_and_sun(P, l);
+        color = color + f3(((((thr.x * rdf.x) * w_nee) / pdf_light) * tr) * sky.x,
+                           ((((thr.y * rdf.y) * w_nee) / pdf_light) * tr) * sky.y,
+                           ((((thr.z * rdf.z) * w_nee) / pdf_light) * tr) * sky.z);
+        const float tr2 = shadow_transmittance_delta(P, sample, rng, x + bs.dir * 1e-4f, bs.dir, pc);
+        const F3 sky2 = sky_and_sun(P, bs.dir);
+        color = color + f3((((thr.x * w_out) * bs.value.x) * tr2) * sky2.x,
+                           (((thr.y * w_out) * bs.value.y) * tr2) * sky2.y,
+                           (((thr.z * w_out) * bs.value.z) * tr2) * sky2.z);
+    } else {
+        const float tr = shadow_transmittance_delta(P, sample, rng, x + l * 1e-4f, l, pc);
+        const F3 sky = sky_and_sun(P, l);
+        color = color + f3((((thr.x * rdf.x) / pdf_light) * tr) * sky.x, (((thr.y * rdf.y) / pdf_light) * tr) * sky.y,
+                           (((thr.z * rdf.z) / pdf_light) * tr) * sky.z);
+    }
 }
 
 // Ratio-tracking transmittance toward a light at distance `max_dist`
@@ -444,6 +519,71 @@ VPT_DEV F3 track_nee(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, Firs
                     F3 l = sky_and_sun(P, dir_light);
                     color = color + f3(f * l.x, f * l.y, f * l.z);
                 }
+                if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
+                    x = x + w * tmin;
+                    d = tmax - tmin;
+                }
+            } else {
+                d -= t;
+            }
+        }
+    }
+    if (!fe.has) color = color + sky_and_sun(P, w);
+    return color;
+}
+
+// VptMode::NEXT_EVENT_TRACKING with isosurfaces (NextEventTracking.glsl:224-393 with USE_ISOSURFACES and
+// USE_ISOSURFACE_NEE; no lights): the 1000-iteration cap, iso_segment with next-event estimation at every
+// surface hit, delta-tracked shadow rays (shadow_transmittance_delta), the volume's light samples scaled
+// by the surface throughput, absorption ending the path with color (+ throughput * emission), and the sky
+// added at the end only for a path without any event.
+template <class S>
+VPT_DEV F3 track_nee_iso(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, FirstEvent& fe, PathCtx& pc) {
+    F3 color = f3(0.0f, 0.0f, 0.0f);
+    F3 weights = f3(1.0f, 1.0f, 1.0f);
+    float last_sign = 0.0f;
+    bool first_point = true;
+    int it = 0;
+    float tmin, tmax;
+    if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
+        x = x + w * tmin;
+        float d = tmax - tmin;
+        int bounces = 0;
+        while (true) {
+            if (++it == 1000) return f3(0.0f, 0.0f, 0.0f);
+            if (guard(pc)) return color;
+            float t = free_path(rng, P.inv_extinction);
+            if (t > d) break;
+            F3 xn = x + w * t;
+            float density = sample(xn, rng);
+            pc.lookups++;
+            if (iso_segment<true>(P, sample, rng, x, xn, density, w, d, tmax, weights, last_sign, first_point,
+                                  pc.lookups, &fe, &color, &pc)) {
+                if (weights.x < 1e-3f && weights.y < 1e-3f && weights.z < 1e-3f) return f3(0.0f, 0.0f, 0.0f);
+                continue;
+            }
+            x = xn;
+            float xi = rng_next(rng);
+            if (xi < P.absorb_albedo * density) {
+                record_event(fe, x, density, P.extinction, tmax - d + t, w);
+                if (P.emission) {
+                    const F3 e = sample.emission(x, rng);
+                    return color + f3(weights.x * e.x, weights.y * e.y, weights.z * e.z);
+                }
+                return color;
+            }
+            if (xi < density) {
+                if (P.max_bounces > 0 && ++bounces > P.max_bounces) return color;
+                F3 next_w = sample_phase(rng, P.g, w);
+                record_scatter(fe, x, density, P.extinction, tmax - d + t, w, next_w, P.g);
+                float pdf_light;
+                const F3 dir_light = importance_sample_sky(P, rng, pdf_light);
+                const float pdf_phase = evaluate_phase(P.g, w, dir_light);
+                w = next_w;
+                const float tr = shadow_transmittance_delta(P, sample, rng, x, dir_light, pc);
+                const float f = (pdf_phase / pdf_light) * tr;
+                const F3 l = sky_and_sun(P, dir_light);
+                color = color + f3((f * l.x) * weights.x, (f * l.y) * weights.y, (f * l.z) * weights.z);
                 if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
                     x = x + w * tmin;
                     d = tmax - tmin;

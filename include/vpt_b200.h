@@ -149,8 +149,10 @@ VptStatus vpt_set_tf_scattering_albedo_strength(VptContext* ctx, float strength)
  * DeltaTracking.glsl and CheckIsosurfaceHit.glsl): the surface where the normalised density crosses
  * iso_value (default 0.5) is found on every free-flight segment and reflects like an opaque surface
  * of colour iso_surface_color (default 0.4 0.4 0.4) with the selected BRDF; lookups are trilinear
- * while isosurfaces are on.  Built for delta and spectral delta tracking on dense grids: other trackers,
- * sparse grids, a transfer function and batched rendering return VPT_ERR_UNSUPPORTED.  Types "Density" and "Gradient"
+ * while isosurfaces are on.  Built for delta, spectral delta and next event tracking on dense grids
+ * (next event tracking with surface next-event estimation, USE_ISOSURFACE_NEE, for sky light samples:
+ * with lights, an environment image or empty-space skipping it returns VPT_ERR_UNSUPPORTED); other
+ * trackers, sparse grids, a transfer function and batched rendering return VPT_ERR_UNSUPPORTED.  Types "Density" and "Gradient"
  * (the surface where the trilinear-filtered gradient magnitude of the raw grid crosses iso_value:
  * central differences with clamped neighbours, VolumetricPathTracingPass.cpp:690-745, built on the GPU
  * at the first render after the grid or the type changed) and the BRDFs

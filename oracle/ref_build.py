@@ -132,6 +132,14 @@ def variants():
                         ("cook", "SURFACE_BRDF_COOK_TORRANCE"), ("disney", "SURFACE_BRDF_DISNEY")):
         out.append((f"delta_iso_{tag}__trilinear__default__linear", TRACKERS["delta"] + [INTERPS["trilinear"]]
                     + ENVS["default__linear"] + [define if d == "SURFACE_BRDF_LAMBERTIAN" else d for d in ISO], 0))
+    # next event tracking with isosurfaces (USE_ISOSURFACE_NEE, VolumetricPathTracingPass.cpp:1761-1763) for
+    # every surface BRDF
+    for tag, define in (("", "SURFACE_BRDF_LAMBERTIAN"), ("_blinn", "SURFACE_BRDF_BLINN_PHONG"),
+                        ("_ambient", "SURFACE_BRDF_AMBIENT"), ("_cook", "SURFACE_BRDF_COOK_TORRANCE"),
+                        ("_disney", "SURFACE_BRDF_DISNEY")):
+        out.append((f"nee_iso{tag}__trilinear__default__linear", TRACKERS["nee"] + [INTERPS["trilinear"]]
+                    + ENVS["default__linear"] + [define if d == "SURFACE_BRDF_LAMBERTIAN" else d for d in ISO]
+                    + ["USE_ISOSURFACE_NEE"], 0))
     # spectral delta tracking with isosurfaces (DeltaTracking.glsl:37-63), path-history and max probabilities
     for p in ("hist", "max"):
         out.append((f"sdt_{p}_iso__trilinear__default__linear", [SPECTRAL["sdt"], SDT_PROB[p], INTERPS["trilinear"]]

@@ -767,7 +767,16 @@ struct Tracer {
     V3 frame(V3 t, V3 b, V3 n, float x, float y, float z) const {
         return v3((t.x * x + b.x * y) + n.x * z, (t.y * x + b.y * y) + n.y * z, (t.z * x + b.z * y) + n.z * z);
     }
-    void cook_torrance(V3 n, V3 t, V3 b, float sel, float u, V3& w, V3& weights, Rng& r) {
+    struct Frame {
+        V3 n, t, b, view;
+    };
+    struct BrdfS {  // one computeBrdf sample: direction, value, lobe flags, samplingPDF
+        V3 dir, value;
+        bool spec, cc;
+        float pdf;
+    };
+    BrdfS cook_torrance(const Frame& fr, float sel, float u, Rng& r) {
+        const V3 n = fr.n, t = fr.t, b = fr.b, view = fr.view;
         const float pi = 3.14159265358979323846f;
         const float v = rnd(r);
         const float metallic = S.brdf[1], specular = S.brdf[2];
@@ -775,7 +784,6 @@ struct Tracer {
         const float specular_w = metallic + (1.0f - rough) * (1.0f + specular);
         const float diffuse_w = 1.0f - metallic;
         const float specular_p = specular_w * (1.0f / (specular_w + diffuse_w));
-        const V3 view = normalize(neg(w));
         const float alpha = rough * rough, alpha2 = alpha * alpha;
         const bool specular_hit = sel < specular_p;
         const float phi = (2.0f * pi) * v;
@@ -799,12 +807,9 @@ struct Tracer {
         const float k = alpha / 2.0f;
         const float gl = ldotn < 0.001f ? 0.001f : ldotn, gv = vdotn < 0.001f ? 0.001f : vdotn;
         const float g = (gl / (gl * (1.0f - k) + k)) * (gv / (gv * (1.0f - k) + k));
-        float d = 0.0f, sth = 0.0f;
-        if (!specular_hit) {
-            const float bq = (ndoth * ndoth) * (alpha2 - 1.0f) + 1.0f;
-            d = ((1.0f / pi) * alpha2) / (bq * bq);
-            sth = sqrtf(1.0f - std::min(ndoth * ndoth, 0.95f));
-        }
+        const float bq = (ndoth * ndoth) * (alpha2 - 1.0f) + 1.0f;
+        const float d = ((1.0f / pi) * alpha2) / (bq * bq);
+        const float sth = sqrtf(1.0f - std::min(ndoth * ndoth, 0.95f));
         float o[3];
         for (int i = 0; i < 3; ++i) {
             const float c = S.iso_color[i];
@@ -814,13 +819,39 @@ struct Tracer {
                                             : ((((f * g) * d) * vdoth) * sth) / vdotn;
             o[i] = (c * (1.0f - f)) * (1.0f - metallic) + spec;
         }
-        weights = v3(weights.x * o[0], weights.y * o[1], weights.z * o[2]);
-        w = l;
+        return BrdfS{l, v3(o[0], o[1], o[2]), specular_hit, false, specular_hit ? d : 1.0f / pi};
+    }
+    // CookTorrance.glsl evaluateBrdfPdf at l: the diffuse-sample specular term plus the diffuse colour / pi
+    V3 cook_torrance_pdf_value(const Frame& fr, V3 l) const {
+        const float pi = 3.14159265358979323846f;
+        const float metallic = S.brdf[1], specular = S.brdf[2];
+        const float rough = std::min(std::max(S.brdf[4], 0.05f), 1.0f);
+        const float alpha = rough * rough, alpha2 = alpha * alpha;
+        const V3 view = fr.view, n = fr.n;
+        const V3 h = normalize(add(l, view));
+        const float ndoth = dot(h, n), vdotn = dot(view, n), ldotn = dot(l, n), vdoth = dot(view, h);
+        const float f0s = 0.16f * (specular * specular);
+        const float p5 = m_pow5(1.0f - vdoth);
+        const float k = alpha / 2.0f;
+        const float gl = ldotn < 0.001f ? 0.001f : ldotn, gv = vdotn < 0.001f ? 0.001f : vdotn;
+        const float g = (gl / (gl * (1.0f - k) + k)) * (gv / (gv * (1.0f - k) + k));
+        const float bq = (ndoth * ndoth) * (alpha2 - 1.0f) + 1.0f;
+        const float d = ((1.0f / pi) * alpha2) / (bq * bq);
+        const float sth = sqrtf(1.0f - std::min(ndoth * ndoth, 0.95f));
+        float o[3];
+        for (int i = 0; i < 3; ++i) {
+            const float c = S.iso_color[i];
+            const float f0 = f0s * (1.0f - metallic) + c * metallic;
+            const float f = f0 + (1.0f - f0) * p5;
+            o[i] = ((c * (1.0f - f)) * (1.0f - metallic)) * (1.0f / pi) + ((((f * g) * d) * vdoth) * sth) / vdotn;
+        }
+        return v3(o[0], o[1], o[2]);
     }
     // Disney2012.glsl computeBrdf = sampleBrdf + evaluateBrdf, its terms as the shader writes them:
     // lobes specular (metallic + (1 + specular)(1 - roughness)), diffuse ((1 - metallic)(1 + roughness)
     // + subsurface) and clearcoat (clamp(clearcoat, 0, 1)); the value is diffuse + specular + clearcoat
-    void disney(V3 n, V3 t, V3 b, float sel, float u, V3& w, V3& weights, Rng& r) {
+    BrdfS disney(const Frame& fr, float sel, float u, Rng& r) {
+        const V3 n = fr.n, t = fr.t, b = fr.b, view = fr.view;
         const float pi = 3.14159265358979323846f, pi_c = 3.14159265359f;
         const float* q = S.brdf;
         const float roughness = q[4], metallic = q[1];
@@ -833,7 +864,6 @@ struct Tracer {
         const float clearcoat_w = std::min(std::max(q[8], 0.0f), 1.0f);
         const float norm = 1.0f / ((specular_w + diffuse_w) + clearcoat_w);
         const float specular_p = specular_w * norm, diffuse_p = diffuse_w * norm;
-        const V3 view = normalize(neg(w));
         const float v0 = rnd(r);
         const int lobe = sel < specular_p ? 0 : (sel < specular_p + diffuse_p ? 1 : 2);
         const bool specular_hit = lobe != 1, clearcoat_hit = lobe == 2;
@@ -924,10 +954,76 @@ struct Tracer {
                                    : ((((((f_spec * d_spec) * g_spec) * 4.0f) * cos_l) * vdoth) * sin_th);
             o[i] = (diffuse + spec) + clear;
         }
-        weights = v3(weights.x * o[0], weights.y * o[1], weights.z * o[2]);
-        w = l;
+        return BrdfS{l, v3(o[0], o[1], o[2]), specular_hit, clearcoat_hit,
+                     specular_hit ? (clearcoat_hit ? d_cc : d_spec) : 1.0f / pi};
     }
-    void iso_scatter(V3 p, V3& w, V3& weights, Rng& r) {
+    // Disney2012.glsl evaluateBrdfPdf at l: the non-specular-sample terms, diffuse / pi, sin(theta_h) =
+    // sqrt(1 - min(n.h^2, 0.95)), 0.01 as the floor of the subsurface denominator
+    V3 disney_pdf_value(const Frame& fr, V3 l) const {
+        const float pi = 3.14159265358979323846f, pi_c = 3.14159265359f;
+        const float* q = S.brdf;
+        const float roughness = q[4], metallic = q[1];
+        const float aspect = sqrtf(1.0f - q[5] * 0.9f);
+        const float r2 = roughness * roughness;
+        const float ax0 = r2 / aspect, ay0 = r2 * aspect;
+        const float ax = 0.001f < ax0 ? ax0 : 0.001f, ay = 0.001f < ay0 ? ay0 : 0.001f;
+        const V3 view = fr.view, n = fr.n, t = fr.t, b = fr.b;
+        const V3 hh = normalize(add(l, view));
+        const float cos_h = dot(hh, n), cos_d = dot(l, hh), cos_v = dot(view, n), cos_l = dot(l, n);
+        const float vdoth = dot(view, hh);
+        const float* c = S.iso_color;
+        const float lum = (0.3f * c[0] + 0.6f * c[1]) + 0.1f * c[2];
+        const float cd = m_cos(cos_d);
+        const float cd2 = cd * cd;
+        const float f_d90 = 0.5f + (2.0f * roughness) * cd2;
+        const float pl = m_pow5(1.0f - m_cos(cos_l)), pv = m_pow5(1.0f - m_cos(cos_v));
+        const float f_d = (1.0f + (f_d90 - 1.0f) * pl) * (1.0f + (f_d90 - 1.0f) * pv);
+        const float fss90 = roughness * cd2;
+        const float f_ss = (1.0f + (fss90 - 1.0f) * pl) * (1.0f + (fss90 - 1.0f) * pv);
+        const float lv = cos_l + cos_v;
+        const float f_dss = 1.25f * (f_ss * (1.0f / (lv < 0.01f ? 0.01f : lv) - 0.5f) + 0.5f);
+        const float f_h = m_pow5(1.0f - cos_d);
+        const float fd_mix = f_d * (1.0f - q[0]) + f_dss * q[0];
+        const float dx = dot(t, hh) / ax, dy = dot(b, hh) / ay;
+        const float dd = dx * dx + dy * dy;
+        const float d_spec = 1.0f / (((pi * ax) * ay) * (dd * dd) + cos_h * cos_h);
+        const float glx = dot(t, l) * ax, gly = dot(b, l) * ay, gvx = dot(t, view) * ax, gvy = dot(b, view) * ay;
+        float g_spec = 1.0f / (cos_v + sqrtf((glx * glx + gly * gly) + cos_v * cos_v));
+        g_spec = g_spec * (1.0f / (cos_v + sqrtf((gvx * gvx + gvy * gvy) + cos_v * cos_v)));
+        const float sth = sqrtf(1.0f - std::min(cos_h * cos_h, 0.95f));
+        const float f_cc = 0.04f * (1.0f - f_h) + 1.0f * f_h;
+        const float a_cc = 0.1f * (1.0f - q[9]) + 0.001f * q[9];
+        float d_cc;
+        if (a_cc >= 1.0f) {
+            d_cc = 1.0f / pi_c;
+        } else {
+            const float a2 = a_cc * a_cc;
+            d_cc = (a2 - 1.0f) / ((pi_c * m_log(a2)) * (1.0f + ((a2 - 1.0f) * cos_h) * cos_h));
+        }
+        const float bl = cos_l * cos_l, bv = cos_v * cos_v, ag = 0.25f * 0.25f;
+        const float g_cc = (1.0f / ((cos_l < -0.99f ? -0.99f : cos_l) + sqrtf((ag + bl) - ag * bl))) *
+                           (1.0f / ((cos_v < -0.99f ? -0.99f : cos_v) + sqrtf((ag + bv) - ag * bv)));
+        const float clear = (((((q[8] * f_cc) * d_cc) * g_cc) * cos_l) * vdoth) * sth;
+        const float st = q[3], sh = q[7];
+        const float spec_scale = q[2] * 0.08f;
+        float o[3];
+        for (int i = 0; i < 3; ++i) {
+            const float tint = lum > 0.0f ? c[i] / lum : 1.0f;
+            const float spec0 = (spec_scale * (1.0f * (1.0f - st) + tint * st)) * (1.0f - metallic) + c[i] * metallic;
+            const float sheen = (f_h * q[6]) * (1.0f * (1.0f - sh) + tint * sh);
+            const float diffuse = ((c[i] * fd_mix + sheen) * (1.0f - metallic)) * (1.0f / pi);
+            const float f_spec = spec0 * (1.0f - f_h) + 1.0f * f_h;
+            const float spec = ((((((f_spec * d_spec) * g_spec) * 4.0f) * cos_l) * vdoth) * sth);
+            o[i] = (diffuse + spec) + clear;
+        }
+        return v3(o[0], o[1], o[2]);
+    }
+    // getIsoSurfaceHit (VptUtils.glsl:1151-1334) up to computeBrdf: one random number for the opacity
+    // test, the normal turned against the ray, the ComputeDefaultBasis frame (RayTracingUtilities.glsl:
+    // 20-28), the selected BRDF's sample.  Lambertian.glsl is included (VptUtils.glsl:1121) before
+    // UNIFORM_SAMPLING is defined (:1144), so it samples the cosine-weighted hemisphere through the
+    // concentric disk map (VptUtils.glsl:1078-1098) and its pdf factor is the cosine itself
+    BrdfS iso_sample(V3 p, V3 w, Frame& fr, Rng& r) {
         (void)rnd(r);  // isoSurfaceOpacity (1) < random() never holds
         V3 n = iso_normal(p);
         if (dot(w, n) > 0.0f) n = neg(n);
@@ -935,15 +1031,10 @@ struct Tracer {
         const V3 b = normalize(fabsf(n.z) > 0.99999f ? v3(-n.x * n.y, 1.0f - n.y * n.y, yz)
                                                      : v3(-n.x * n.z, yz, 1.0f - n.z * n.z));
         const V3 t = cross(b, n);
+        fr = Frame{n, t, b, normalize(neg(w))};
         const float xi0 = rnd(r), xi1 = rnd(r);
-        if (S.iso_brdf == 3) {
-            cook_torrance(n, t, b, xi0, xi1, w, weights, r);
-            return;
-        }
-        if (S.iso_brdf == 4) {
-            disney(n, t, b, xi0, xi1, w, weights, r);
-            return;
-        }
+        if (S.iso_brdf == 3) return cook_torrance(fr, xi0, xi1, r);
+        if (S.iso_brdf == 4) return disney(fr, xi0, xi1, r);
         if (S.iso_brdf != 0) {
             // BlinnPhong.glsl / ConstantLighting.glsl: sampleHemisphere (VptUtils.glsl:1071-1077), uniform
             const float pi = 3.14159265358979323846f;
@@ -954,8 +1045,7 @@ struct Tracer {
                               (t.z * lx + b.z * ly) + n.z * xi0);
             V3 c = v3(S.iso_color[0], S.iso_color[1], S.iso_color[2]);
             if (S.iso_brdf == 1) {  // BlinnPhong.glsl evaluateBrdf
-                const V3 view = normalize(neg(w));
-                const V3 h = normalize(add(view, out));
+                const V3 h = normalize(add(fr.view, out));
                 const float e = 10.0f;
                 const float norm = std::min(std::max((e + 2.0f) / ((4.0f * pi) * 0.03125f), (e + 2.0f) / (8.0f * pi)),
                                             (e + 4.0f) / (8.0f * pi));
@@ -963,9 +1053,7 @@ struct Tracer {
                 const float k = 2.0f * pi;
                 c = v3((k * S.iso_color[0]) * s, (k * S.iso_color[1]) * s, (k * S.iso_color[2]) * s);
             }
-            weights = v3(weights.x * c.x, weights.y * c.y, weights.z * c.z);
-            w = out;
-            return;
+            return BrdfS{out, c, false, false, 0.0f};
         }
         const float ox = 2.0f * xi0 - 1.0f, oy = 2.0f * xi1 - 1.0f;
         float dx = 0.0f, dy = 0.0f;
@@ -985,9 +1073,106 @@ struct Tracer {
         const V3 out = v3((t.x * dx + b.x * dy) + n.x * hz, (t.y * dx + b.y * dy) + n.y * hz,
                           (t.z * dx + b.z * dy) + n.z * hz);
         const float cosv = dot(out, n);
-        weights = v3(weights.x * ((S.iso_color[0] * cosv) / cosv), weights.y * ((S.iso_color[1] * cosv) / cosv),
-                     weights.z * ((S.iso_color[2] * cosv) / cosv));
-        w = out;
+        return BrdfS{out,
+                     v3((S.iso_color[0] * cosv) / cosv, (S.iso_color[1] * cosv) / cosv,
+                        (S.iso_color[2] * cosv) / cosv),
+                     false, false, 0.0f};
+    }
+    void iso_scatter(V3 p, V3& w, V3& weights, Rng& r) {
+        Frame fr;
+        const BrdfS bs = iso_sample(p, w, fr, r);
+        weights = v3(weights.x * bs.value.x, weights.y * bs.value.y, weights.z * bs.value.z);
+        w = bs.dir;
+    }
+    // evaluateBrdfNee of each BRDF file (USE_ISOSURFACE_NEE) for the light direction l, with the
+    // sampling pdfs MIS reads (Cook-Torrance, Disney)
+    V3 brdf_nee(const Frame& fr, const BrdfS& bs, V3 l, float& pdf_out, float& pdf_nee) const {
+        const float pi = 3.14159265358979323846f;
+        const float* c = S.iso_color;
+        pdf_out = 0.0f;
+        pdf_nee = 0.0f;
+        if (S.iso_brdf == 0) {  // Lambertian.glsl, non-uniform branch: colour / pi * n.l
+            const float th = dot(fr.n, l);
+            return v3((c[0] / pi) * th, (c[1] / pi) * th, (c[2] / pi) * th);
+        }
+        if (S.iso_brdf == 2) {  // ConstantLighting.glsl: colour / (2 pi)
+            const float k = 2.0f * pi;
+            return v3(c[0] / k, c[1] / k, c[2] / k);
+        }
+        if (S.iso_brdf == 1) {  // BlinnPhong.glsl: colour (n.h)^10 / norm
+            const float e = 10.0f;
+            const float norm = std::min(std::max((e + 2.0f) / ((4.0f * pi) * 0.03125f), (e + 2.0f) / (8.0f * pi)),
+                                        (e + 4.0f) / (8.0f * pi));
+            const V3 h = normalize(add(fr.view, l));
+            const float v = m_pow(std::max(dot(fr.n, h), 0.0f), e) / norm;
+            return v3(c[0] * v, c[1] * v, c[2] * v);
+        }
+        const V3 h = normalize(add(bs.dir, fr.view));
+        const float cos_h = dot(h, fr.n);
+        const float sin_h = sqrtf(1.0f / (cos_h * cos_h));
+        const V3 hn = normalize(add(l, fr.view));
+        const float cos_hn = dot(hn, fr.n);
+        const float sin_hn = sqrtf(1.0f - std::min(cos_hn * cos_hn, 0.95f));
+        if (S.iso_brdf == 4 && bs.spec) {
+            pdf_out = bs.pdf * cos_h;
+            pdf_nee = bs.pdf * cos_hn;
+        } else {
+            pdf_out = (bs.pdf * cos_h) * sin_h;
+            pdf_nee = (bs.pdf * cos_hn) * sin_hn;
+        }
+        const V3 v = S.iso_brdf == 4 ? disney_pdf_value(fr, l) : cook_torrance_pdf_value(fr, l);
+        const float nl = dot(l, fr.n);
+        return v3(v.x * nl, v.y * nl, v.z * nl);
+    }
+    // calculateTransmittance with USE_TRANSMITTANCE_DELTA_TRACKING (defined by the isosurface block of
+    // NeeTransmittance.glsl): 0 at the first real collision, else 1; the bisected crossings on the way
+    // change nothing without ISOSURFACE_USE_TF and are not looked for
+    float transmittance_delta(V3 x, V3 w, Rng& r) {
+        float tmin, tmax;
+        if (ray_box(bmin(), bmax(), x, w, tmin, tmax)) {
+            x = add(x, mul(w, tmin));
+            float d = tmax - tmin;
+            while (true) {
+                if (guard()) return 0.0f;
+                float t = free_path(r);
+                if (t > d) break;
+                V3 xn = add(x, mul(w, t));
+                float dens = sample(xn, r);
+                x = xn;
+                if (rnd(r) > 1.0f - dens) return 0.0f;
+                d -= t;
+            }
+        }
+        return 1.0f;
+    }
+    // getIsoSurfaceHit's next-event estimate (USE_ISOSURFACE_NEE, VptUtils.glsl:1213-1325, no lights)
+    void surface_nee(V3 x, const Frame& fr, const BrdfS& bs, V3 thr, V3& color, Rng& r) {
+        float pdf_l;
+        const V3 l = importance_sky(r, pdf_l);
+        if (!(dot(fr.n, l) > 0.0f)) return;
+        float pdf_out, pdf_nee;
+        const V3 rdf = brdf_nee(fr, bs, l, pdf_out, pdf_nee);
+        const bool mis = (S.iso_brdf == 3 || S.iso_brdf == 4) && bs.spec;
+        if (mis) {
+            const float pdf_l_out = 1.0f / (4.0f * 3.14159265359f);
+            const float w_nee = pdf_l / (pdf_l + pdf_nee);
+            const float w_out = pdf_out / (pdf_l_out + pdf_out);
+            const float tr = transmittance_delta(add(x, mul(l, 1e-4f)), l, r);
+            const V3 sk = sky(l);
+            color = add(color, v3(((((thr.x * rdf.x) * w_nee) / pdf_l) * tr) * sk.x,
+                                  ((((thr.y * rdf.y) * w_nee) / pdf_l) * tr) * sk.y,
+                                  ((((thr.z * rdf.z) * w_nee) / pdf_l) * tr) * sk.z));
+            const float tr2 = transmittance_delta(add(x, mul(bs.dir, 1e-4f)), bs.dir, r);
+            const V3 sk2 = sky(bs.dir);
+            color = add(color, v3((((thr.x * w_out) * bs.value.x) * tr2) * sk2.x,
+                                  (((thr.y * w_out) * bs.value.y) * tr2) * sk2.y,
+                                  (((thr.z * w_out) * bs.value.z) * tr2) * sk2.z));
+        } else {
+            const float tr = transmittance_delta(add(x, mul(l, 1e-4f)), l, r);
+            const V3 sk = sky(l);
+            color = add(color, v3((((thr.x * rdf.x) / pdf_l) * tr) * sk.x, (((thr.y * rdf.y) / pdf_l) * tr) * sk.y,
+                                  (((thr.z * rdf.z) / pdf_l) * tr) * sk.z));
+        }
     }
     // deltaTracking with USE_ISOSURFACES (DeltaTracking.glsl:168-344 with CheckIsosurfaceHit.glsl):
     // every free-flight segment [x, x_new] is checked at iso_subdivisions points for a sign change of
@@ -999,7 +1184,7 @@ struct Tracer {
     // a crossing is bisected, the surface scatters, the path moves 1e-4 off it and restarts from the
     // box boundary.  Returns true on a surface event.
     bool iso_check(V3& x, V3 xn, V3& w, float& d, float& tmax, V3& weights, float& last_sign, bool& first_point,
-                   Rng& r, bool& ev) {
+                   Rng& r, bool& ev, V3* nee_color = nullptr) {
         const int nsub = S.iso_subdivisions;
         for (int sub = 0; sub < nsub; sub++) {
             const float a0 = (float)sub / (float)nsub, a1 = (float)(sub + 1) / (float)nsub;
@@ -1013,7 +1198,15 @@ struct Tracer {
             if (last_sign != cur_sign) {
                 iso_refine(x1, x0, cur_sign, r);
                 x = x1;
-                iso_scatter(x, w, weights, r);
+                if (nee_color) {  // USE_ISOSURFACE_NEE: the light sample before the throughput takes the BRDF
+                    Frame fr;
+                    const BrdfS bs = iso_sample(x, w, fr, r);
+                    surface_nee(x, fr, bs, weights, *nee_color, r);
+                    weights = v3(weights.x * bs.value.x, weights.y * bs.value.y, weights.z * bs.value.z);
+                    w = bs.dir;
+                } else {
+                    iso_scatter(x, w, weights, r);
+                }
                 x = add(x, mul(w, 1e-4f));
                 first_point = true;
                 ev = true;
@@ -1267,6 +1460,66 @@ struct Tracer {
         return trans;
     }
 
+    // nextEventTracking with USE_ISOSURFACES and USE_ISOSURFACE_NEE (NextEventTracking.glsl:224-393; no
+    // lights): the 1000-iteration cap, the segment check with next-event estimation at surface hits,
+    // delta-tracked shadow rays, volume light samples scaled by the surface throughput, the sky at the
+    // end only for a path without any event
+    V3 nee_iso(V3 x, V3 w, Rng& r, bool& ev) {
+        V3 color = v3(0, 0, 0), weights = v3(1, 1, 1);
+        float last_sign = 0.0f;
+        bool first_point = true;
+        int it = 0;
+        float tmin, tmax;
+        const float absorb = 1.0f - S.albedo;
+        if (ray_box(bmin(), bmax(), x, w, tmin, tmax)) {
+            x = add(x, mul(w, tmin));
+            float d = tmax - tmin;
+            int bounces = 0;
+            while (true) {
+                if (++it == 1000) return v3(0, 0, 0);
+                if (guard()) return color;
+                float t = free_path(r);
+                if (t > d) break;
+                V3 xn = add(x, mul(w, t));
+                float dens = sample(xn, r);
+                if (iso_check(x, xn, w, d, tmax, weights, last_sign, first_point, r, ev, &color)) {
+                    if (weights.x < 1e-3f && weights.y < 1e-3f && weights.z < 1e-3f) return v3(0, 0, 0);
+                    continue;
+                }
+                x = xn;
+                float xi = rnd(r);
+                if (xi < absorb * dens) {
+                    ev = true;
+                    if (S.emission) {
+                        const V3 e = emission(x, r);
+                        return add(color, v3(weights.x * e.x, weights.y * e.y, weights.z * e.z));
+                    }
+                    return color;
+                }
+                if (xi < dens) {
+                    if (S.max_bounces > 0 && ++bounces > S.max_bounces) return color;
+                    V3 nw = sample_phase(r, S.g, w);
+                    ev = true;
+                    float pdf_l;
+                    V3 dl = importance_sky(r, pdf_l);
+                    float pdf_p = eval_phase(S.g, w, dl);
+                    w = nw;
+                    float tr = transmittance_delta(x, dl, r);
+                    float f = (pdf_p / pdf_l) * tr;
+                    V3 l = sky(dl);
+                    color = add(color, v3((f * l.x) * weights.x, (f * l.y) * weights.y, (f * l.z) * weights.z));
+                    if (ray_box(bmin(), bmax(), x, w, tmin, tmax)) {
+                        x = add(x, mul(w, tmin));
+                        d = tmax - tmin;
+                    }
+                } else {
+                    d -= t;
+                }
+            }
+        }
+        if (!ev) color = add(color, sky(w));
+        return color;
+    }
     V3 nee(V3 x, V3 w, Rng& r, bool& ev) {
         V3 color = v3(0, 0, 0);
         float tmin, tmax;
@@ -1959,7 +2212,7 @@ struct Tracer {
             case 3: return S.nanovdb ? decomposition_sparse(x, w, r) : decomposition(x, w, r);
             case 4: return rrt(x, w, r);
             case 9: return residual_ratio_nee(x, w, r, ev);
-            default: return nee(x, w, r, ev);
+            default: return S.use_iso ? nee_iso(x, w, r, ev) : nee(x, w, r, ev);
         }
     }
 };

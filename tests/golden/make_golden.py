@@ -140,6 +140,17 @@ def cases():
         kw2.update(iso_value=0.3, iso_color=(0.9, 0.6, 0.3), extinction=40.0, albedo=0.9, g=0.2)
         out["fbm_" + name] = SceneSpec(grid=fbm, mode="delta", interp="trilinear", iso=True, iso_brdf="Disney (2012)",
                                        brdf_params=params, **kw2)
+    # next event tracking with isosurfaces and surface next-event estimation, every BRDF (MIS for the
+    # specular samples of Cook-Torrance and Disney)
+    for name, brdf, params in (("nee_iso", "Lambertian", None), ("nee_iso_blinn", "Blinn Phong", None),
+                               ("nee_iso_ambient", "Ambient", None),
+                               ("nee_iso_cook", "Cook Torrance", {"metallic": 0.6, "specular": 0.8, "roughness": 0.25}),
+                               ("nee_iso_disney", "Disney (2012)", {"metallic": 0.3, "roughness": 0.4,
+                                                                    "clearcoat": 0.7, "sheen": 0.5})):
+        kw2 = dict(base)
+        kw2.update(iso_value=0.3, iso_color=(0.9, 0.6, 0.3), extinction=40.0, albedo=0.9, g=0.2)
+        out["fbm_" + name] = SceneSpec(grid=fbm, mode="nee", interp="trilinear", iso=True, iso_brdf=brdf,
+                                       brdf_params=params, **kw2)
     # spectral delta tracking with isosurfaces: a chromatic medium around the coloured density surface
     for name, prob in {"sdt_hist_iso": 2, "sdt_max_iso": 0}.items():
         kw2 = dict(base)

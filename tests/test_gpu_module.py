@@ -228,8 +228,11 @@ def _check_isosurfaces():
     vpt.set_brdf_parameter("roughness", "0.5")
     with pytest.raises(RuntimeError):
         vpt.set_iso_surface_color([0.1, 0.2])
-    vpt.set_vpt_mode_from_name("Next Event Tracking")
-    with pytest.raises(RuntimeError, match="delta tracking"):
+    vpt.set_vpt_mode_from_name("Next Event Tracking")  # surface next-event estimation (USE_ISOSURFACE_NEE)
+    vpt.set_seed_offset(0)
+    assert torch.isfinite(vpt.render_frame(t, 1)).all()
+    vpt.set_vpt_mode_from_name("Ratio Tracking")
+    with pytest.raises(RuntimeError, match="delta"):
         vpt.render_frame(t, 1)
     vpt.set_use_isosurfaces(False)
     vpt.set_iso_value(0.5)
