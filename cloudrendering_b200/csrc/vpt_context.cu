@@ -173,6 +173,10 @@ struct VptContext {
     // isosurfaces (setUseIsosurfaces, setIsoValue, setIsoSurfaceColor; VolumetricPathTracingPass.hpp:382-395)
     bool use_iso = false;
     int iso_type = 0;  // setIsosurfaceType: 0 Density, 1 Gradient
+    // setUseClipPlane / setClipPlaneNormal / setClipPlaneDistance (VolumetricPathTracingPass.hpp:403-405)
+    bool use_clip = false;
+    float clip_normal[3] = {1.0f, 0.0f, 0.0f};
+    float clip_distance = 0.0f;
     float iso_value = 0.5f;
     float iso_color[3] = {0.4f, 0.4f, 0.4f};
     int iso_subdivisions = 2;
@@ -673,6 +677,13 @@ VptStatus fill_params(VptContext* ctx, int tracker, int frames, vpt::TraceParams
     P.iso_value = ctx->iso_value;
     P.iso_color = mk(ctx->iso_color[0], ctx->iso_color[1], ctx->iso_color[2]);
     P.iso_grad = (ctx->use_iso && ctx->iso_type == 1) ? ctx->grad.ptr : nullptr;
+    P.use_clip = ctx->use_clip ? 1 : 0;
+    {  // the uniform holds glm::normalize(clipPlaneNormal): v * inversesqrt(dot(v, v)) in float
+        const float* v = ctx->clip_normal;
+        const float inv = 1.0f / std::sqrt((v[0] * v[0] + v[1] * v[1]) + v[2] * v[2]);
+        P.clip_n = mk(v[0] * inv, v[1] * inv, v[2] * inv);
+    }
+    P.clip_d = ctx->clip_distance;
     P.iso_norm_min = ctx->vmin;
     P.iso_norm_range = ctx->vmax - ctx->vmin;
     P.max_bounces = ctx->max_bounces;
@@ -1161,6 +1172,34 @@ VptStatus vpt_set_brdf_parameter(VptContext* ctx, const char* key, const char* v
     return VPT_OK;
 }
 
+VptStatus vpt_set_use_clip_plane(VptContext* ctx, int use) {
+    VPT_CHECK_CTX(ctx);
+    if ((use != 0) != ctx->use_clip) reset_film_state(ctx);
+    ctx->use_clip = use != 0;
+    return VPT_OK;
+}
+
+VptStatus vpt_set_clip_plane_normal(VptContext* ctx, double x, double y, double z) {
+    VPT_CHECK_CTX(ctx);
+    const float v[3] = {(float)x, (float)y, (float)z};
+    if (!std::isfinite(v[0]) || !std::isfinite(v[1]) || !std::isfinite(v[2]) ||
+        (v[0] == 0.0f && v[1] == 0.0f && v[2] == 0.0f))
+        return fail(ctx, VPT_ERR_ARG, "vpt_set_clip_plane_normal: the normal must be finite and non-zero");
+    if (v[0] != ctx->clip_normal[0] || v[1] != ctx->clip_normal[1] || v[2] != ctx->clip_normal[2])
+        reset_film_state(ctx);
+    for (int i = 0; i < 3; ++i) ctx->clip_normal[i] = v[i];
+    return VPT_OK;
+}
+
+VptStatus vpt_set_clip_plane_distance(VptContext* ctx, double distance) {
+    VPT_CHECK_CTX(ctx);
+    const float d = (float)distance;
+    if (!std::isfinite(d)) return fail(ctx, VPT_ERR_ARG, "vpt_set_clip_plane_distance: not finite");
+    if (d != ctx->clip_distance) reset_film_state(ctx);
+    ctx->clip_distance = d;
+    return VPT_OK;
+}
+
 VptStatus vpt_set_num_isosurface_subdivisions(VptContext* ctx, int subdivisions) {
     VPT_CHECK_CTX(ctx);
     if (subdivisions < 1 || subdivisions > 8) return fail(ctx, VPT_ERR_ARG, "isosurface subdivisions must be in [1, 8]");
@@ -1623,16 +1662,22 @@ VptStatus vpt_render_frames(VptContext* ctx, int frames, void* stream) {
         tracker != vpt::kSpectralDelta && tracker != vpt::kSpectralNextEvent)
         return fail(ctx, VPT_ERR_UNSUPPORTED,
                     "the transfer function applies to delta, next event and spectral tracking (as in the reference)");
-    if (ctx->use_iso && ((tracker != vpt::kDelta && tracker != vpt::kSpectralDelta && tracker != vpt::kNextEvent) ||
+    if (ctx->use_iso && ((tracker != vpt::kDelta && tracker != vpt::kSpectralDelta && tracker != vpt::kNextEvent &&
+                          tracker != vpt::kSpectralNextEvent) ||
                          ctx->use_sparse || (ctx->use_tf && ctx->tf.ptr)))
         return fail(ctx, VPT_ERR_UNSUPPORTED,
-                    "isosurfaces are built for delta, spectral delta and next event tracking on dense grids without a "
-                    "transfer function");
-    if (ctx->use_iso && tracker == vpt::kNextEvent &&
+                    "isosurfaces are built for delta and next event tracking (plain and spectral) on dense grids "
+                    "without a transfer function");
+    if (ctx->use_iso && (tracker == vpt::kNextEvent || tracker == vpt::kSpectralNextEvent) &&
         (ctx->use_ess || (ctx->use_lights && !ctx->lights.empty()) || ctx->env_kind == VPT_ENV_IMAGE))
         return fail(ctx, VPT_ERR_UNSUPPORTED,
                     "next event tracking with isosurfaces is built for sky light samples: no lights, no environment "
                     "image, no empty-space skipping");
+    if (ctx->use_clip && (tracker == vpt::kDecomposition || tracker == vpt::kResidualRatio ||
+                          tracker == vpt::kResidualRatioNee || ctx->use_ess))
+        return fail(ctx, VPT_ERR_UNSUPPORTED,
+                    "the clip plane is built for delta, ratio and next event tracking (plain and spectral) without "
+                    "empty-space skipping");
     if (ctx->env_kind == VPT_ENV_IMAGE && !ctx->env_pyramid.ptr)
         return fail(ctx, VPT_ERR_STATE, "environment image not loaded");
     cudaSetDevice(ctx->device);

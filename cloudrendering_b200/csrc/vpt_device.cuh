@@ -213,6 +213,26 @@ VPT_DEV bool ray_box(F3 bmin, F3 bmax, F3 p, F3 d, float& tmin, float& tmax) {
     return !(tmax <= tmin || tmax <= 0.0f);
 }
 
+// rayBoxIntersect of the volume box (VptUtils.glsl:763-801): with the clip plane on (USE_CLIP_PLANE,
+// :776-799) the interval is cut to the plane's positive side, using the direction as modified for the
+// box test; a ray parallel to the plane, or meeting it behind its origin, is kept whole or dropped
+// by the side its origin lies on.
+VPT_DEV bool ray_box_p(const TraceParams& P, F3 p, F3 d, float& tmin, float& tmax) {
+    if (!ray_box(P.box_min, P.box_max, p, d, tmin, tmax)) return false;
+    if (!P.use_clip) return true;
+    d.x = fabsf(d.x) <= 0.000001f ? 0.000001f : d.x;
+    d.y = fabsf(d.y) <= 0.000001f ? 0.000001f : d.y;
+    d.z = fabsf(d.z) <= 0.000001f ? 0.000001f : d.z;
+    const float denom = dot3(P.clip_n, d);
+    const float dp = dot3(P.clip_n, p) - P.clip_d;
+    if (fabsf(denom) < 0.001f) return dp > 0.0f;
+    const float t_clip = (P.clip_d - dot3(P.clip_n, p)) / denom;
+    if (t_clip <= 0.0f) return dp > 0.0f;
+    if (dp > 0.0f) tmax = fminf(t_clip, tmax);
+    else tmin = fmaxf(t_clip, tmin);
+    return !(tmax <= tmin || tmax <= 0.0f);
+}
+
 // ---------------------------------------------------------------------------------------------
 // Direction sampling (VptUtils.glsl:67-123).
 VPT_DEV void orthonormal_basis(F3 d, F3& b, F3& t) {

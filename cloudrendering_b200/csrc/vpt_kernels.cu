@@ -27,14 +27,17 @@ cudaError_t launch_trace(const TraceParams& P, int tracker, int use_ess, int sch
     if (P.iso) {
         // isosurfaces: delta, spectral delta and next event tracking on dense grids, trilinear lookups,
         // no transfer function
-        if ((tracker != kDelta && tracker != kSpectralDelta && tracker != kNextEvent) || P.grid_kind != kDense ||
-            P.tf)
+        if ((tracker != kDelta && tracker != kSpectralDelta && tracker != kNextEvent &&
+             tracker != kSpectralNextEvent) ||
+            P.grid_kind != kDense || P.tf)
             return cudaErrorNotSupported;
         if (tracker == kSpectralDelta)
             return launch_tracker_spectral_delta_iso(P, schedule, features, persistent_blocks, stream);
-        if (tracker == kNextEvent) {
+        if (tracker == kNextEvent || tracker == kSpectralNextEvent) {
             // next event tracking: sky light samples only (no lights, no environment image, no skipping)
             if (use_ess || P.num_lights > 0 || P.env_kind == kEnvImage) return cudaErrorNotSupported;
+            if (tracker == kSpectralNextEvent)
+                return launch_tracker_spectral_nee_iso(P, schedule, features, persistent_blocks, stream);
             return launch_tracker_nee_iso(P, schedule, features, persistent_blocks, stream);
         }
         return launch_tracker_delta_iso(P, schedule, features, persistent_blocks, stream);

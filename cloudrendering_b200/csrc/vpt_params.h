@@ -26,6 +26,7 @@ enum Tracker : int {
     kDeltaIso = 300,
     kSpectralDeltaIso = 301,
     kNextEventIso = 302,
+    kSpectralNextEventIso = 303,
 };
 
 // Collision probabilities of spectral tracking (SpectralDeltaTrackingCollisionProbability,
@@ -217,6 +218,11 @@ struct TraceParams {
     // null for density isosurfaces; normals read them normalised with the density's min / range
     const float* iso_grad;
     float iso_norm_min, iso_norm_range;
+    // USE_CLIP_PLANE: the volume box's ray intervals cut to the positive side of the plane
+    // dot(clip_n, x) = clip_d (clip_n normalised)
+    int use_clip;
+    F3 clip_n;
+    float clip_d;
     unsigned long long* counters;  // [0] paths, [1] density lookups
     int* error_flags;
     unsigned int* work_counter;    // persistent-kernel path queue

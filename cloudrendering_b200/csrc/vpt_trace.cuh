@@ -65,7 +65,7 @@ VPT_DEV void depth_march(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, 
     const float atten = P.extinction * step;
     float acc_depth = 0.0f, acc_alpha = 0.0f, nearest = 0.0f;
     float tmin, tmax;
-    if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
+    if (ray_box_p(P, x, w, tmin, tmax)) {
         float t = tmin;
         while (true) {
             t += step;
@@ -198,6 +198,7 @@ VPT_DEV F3 run_tracker(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, Fi
     if constexpr (TRACKER == kSpectralDelta) return track_delta_spectral<false>(P, sample, rng, x, w, fe, pc);
     if constexpr (TRACKER == kSpectralDeltaIso) return track_delta_spectral<true>(P, sample, rng, x, w, fe, pc);
     if constexpr (TRACKER == kNextEventIso) return track_nee_iso(P, sample, rng, x, w, fe, pc);
+    if constexpr (TRACKER == kSpectralNextEventIso) return track_nee_spectral<false, true>(P, sample, rng, x, w, fe, pc);
     if constexpr (TRACKER == kSpectralNextEvent) return track_nee_spectral<false>(P, sample, rng, x, w, fe, pc);
     if constexpr (TRACKER == kSpectralNextEvent + 100) return track_nee_spectral<true>(P, sample, rng, x, w, fe, pc);
     if (TRACKER == kNextEvent + 100) return track_nee<true>(P, sample, rng, x, w, fe, pc);
@@ -387,7 +388,7 @@ VPT_DEV void end_shadow(const TraceParams& P, F3& color, F3& x, F3& w, float& d,
     d = dp;
     mode = kModePrimary;
     float tmin, tmax;
-    if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
+    if (ray_box_p(P, x, w, tmin, tmax)) {
         x = x + w * tmin;
         d = tmax - tmin;
     }
@@ -550,7 +551,7 @@ VPT_DEV void refill_loop(const SRC& src, uint64_t total, unsigned long long* wor
                             F3 L = sky_and_sun(P, w);
                             refill_finish<TRACKER>(P, pix, L, has);
                         }
-                    } else if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
+                    } else if (ray_box_p(P, x, w, tmin, tmax)) {
                         x = x + w * tmin;
                         d = tmax - tmin;
                     } else {
@@ -640,7 +641,7 @@ VPT_DEV void refill_loop(const SRC& src, uint64_t total, unsigned long long* wor
                 } else {  // shadow ray from xp along w (x == xp here), up to the light or the box exit
                     float tmin_s, tmax_s;
                     float len = -1.0f;
-                    if (ray_box(P.box_min, P.box_max, x, w, tmin_s, tmax_s)) len = fminf(tmax_s, shadow_max) - tmin_s;
+                    if (ray_box_p(P, x, w, tmin_s, tmax_s)) len = fminf(tmax_s, shadow_max) - tmin_s;
                     if (!(len > 0.0f)) {  // transmittance 1, no random numbers
                         goto rrt_shadow_done;
                     }
@@ -738,7 +739,7 @@ VPT_DEV void refill_loop(const SRC& src, uint64_t total, unsigned long long* wor
                 walking = false;
                 in_block = false;
                 float tmin_b, tmax_b;
-                if (!ray_box(P.box_min, P.box_max, x, w, tmin_b, tmax_b)) {
+                if (!ray_box_p(P, x, w, tmin_b, tmax_b)) {
                     refill_finish<TRACKER>(P, pix, color, has);
                     continue;
                 }
@@ -917,7 +918,7 @@ VPT_DEV void refill_loop(const SRC& src, uint64_t total, unsigned long long* wor
                     }
                     continue;
                 }
-                if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
+                if (ray_box_p(P, x, w, tmin, tmax)) {
                     x = x + w * tmin;
                     d = tmax - tmin;
                     shadow_dist = tmin;
@@ -933,7 +934,7 @@ VPT_DEV void refill_loop(const SRC& src, uint64_t total, unsigned long long* wor
                 trans *= 1.0f - pa / (pa + ps);
             }
             w = sample_phase(rng, P.g, w);
-            if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
+            if (ray_box_p(P, x, w, tmin, tmax)) {
                 x = x + w * tmin;
                 d = tmax - tmin;
             }
@@ -1123,5 +1124,6 @@ cudaError_t launch_tracker_delta_iso(const TraceParams& P, int schedule, int fea
 cudaError_t launch_tracker_spectral_delta_iso(const TraceParams& P, int schedule, int features, int pb,
                                               cudaStream_t s);
 cudaError_t launch_tracker_nee_iso(const TraceParams& P, int schedule, int features, int pb, cudaStream_t s);
+cudaError_t launch_tracker_spectral_nee_iso(const TraceParams& P, int schedule, int features, int pb, cudaStream_t s);
 
 }  // namespace vpt

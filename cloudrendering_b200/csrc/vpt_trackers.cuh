@@ -72,7 +72,7 @@ VPT_DEV void record_scatter(FirstEvent& fe, F3 x, float density, float extinctio
 template <class S>
 VPT_DEV F3 track_delta(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, FirstEvent& fe, PathCtx& pc) {
     float tmin, tmax;
-    if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
+    if (ray_box_p(P, x, w, tmin, tmax)) {
         x = x + w * tmin;
         float d = tmax - tmin;
         int bounces = 0;
@@ -95,7 +95,7 @@ VPT_DEV F3 track_delta(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, Fi
                 const F3 w_in = w;
                 w = sample_phase(rng, P.g, w);
                 record_scatter(fe, x, density, P.extinction, tmax - d + t, w_in, w, P.g);
-                if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
+                if (ray_box_p(P, x, w, tmin, tmax)) {
                     x = x + w * tmin;
                     d = tmax - tmin;
                 }
@@ -167,7 +167,7 @@ VPT_DEV bool iso_segment(const TraceParams& P, S& sample, Rng& rng, F3& x, F3 xn
             // firstEvent of a surface hit: density = extinction, depth = tMax - d + |x - x1|
             if (fe) record_event(*fe, x, 1.0f, P.extinction, tmax - d + length3(x1 - x), w);
             float tmin;
-            if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
+            if (ray_box_p(P, x, w, tmin, tmax)) {
                 x = x + w * tmin;
                 d = tmax - tmin;
             }
@@ -188,7 +188,7 @@ VPT_DEV F3 track_delta_iso(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w
     bool first_point = true;
     int it = 0;
     float tmin, tmax;
-    if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
+    if (ray_box_p(P, x, w, tmin, tmax)) {
         x = x + w * tmin;
         float d = tmax - tmin;
         int bounces = 0;
@@ -216,7 +216,7 @@ VPT_DEV F3 track_delta_iso(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w
                 const F3 w_in = w;
                 w = sample_phase(rng, P.g, w);
                 record_scatter(fe, x, density, P.extinction, tmax - d + t, w_in, w, P.g);
-                if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
+                if (ray_box_p(P, x, w, tmin, tmax)) {
                     x = x + w * tmin;
                     d = tmax - tmin;
                 }
@@ -234,7 +234,7 @@ template <class S>
 VPT_DEV F3 track_ratio(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, FirstEvent& fe, PathCtx& pc) {
     float trans = 1.0f;
     float tmin, tmax;
-    if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
+    if (ray_box_p(P, x, w, tmin, tmax)) {
         x = x + w * tmin;
         float d = tmax - tmin;
         int bounces = 0;
@@ -261,7 +261,7 @@ VPT_DEV F3 track_ratio(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, Fi
                     fe.w = w;
                     fe.pdf_w = evaluate_phase(P.g, w_in, w);
                 }
-                if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
+                if (ray_box_p(P, x, w, tmin, tmax)) {
                     x = x + w * tmin;
                     d = tmax - tmin;
                 }
@@ -279,7 +279,7 @@ template <class S>
 VPT_DEV float shadow_transmittance(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, PathCtx& pc) {
     float trans = 1.0f;
     float tmin, tmax;
-    if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
+    if (ray_box_p(P, x, w, tmin, tmax)) {
         x = x + w * tmin;
         float d = tmax - tmin;
         while (true) {
@@ -305,7 +305,7 @@ VPT_DEV float shadow_transmittance(const TraceParams& P, S& sample, Rng& rng, F3
 template <class S>
 VPT_DEV float shadow_transmittance_delta(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, PathCtx& pc) {
     float tmin, tmax;
-    if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
+    if (ray_box_p(P, x, w, tmin, tmax)) {
         x = x + w * tmin;
         float d = tmax - tmin;
         while (true) {
@@ -369,7 +369,7 @@ VPT_DEV float shadow_transmittance_distance(const TraceParams& P, S& sample, Rng
     float trans = 1.0f;
     float tmin, tmax;
     float cur = 0.0f;
-    if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
+    if (ray_box_p(P, x, w, tmin, tmax)) {
         x = x + w * tmin;
         cur += tmin;
         float d = tmax - tmin;
@@ -461,7 +461,7 @@ template <bool ESS, class S>
 VPT_DEV F3 track_nee(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, FirstEvent& fe, PathCtx& pc) {
     F3 color = f3(0.0f, 0.0f, 0.0f);
     float tmin, tmax;
-    if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
+    if (ray_box_p(P, x, w, tmin, tmax)) {
         x = x + w * tmin;
         float d = tmax - tmin;
         int bounces = 0;
@@ -519,7 +519,7 @@ VPT_DEV F3 track_nee(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, Firs
                     F3 l = sky_and_sun(P, dir_light);
                     color = color + f3(f * l.x, f * l.y, f * l.z);
                 }
-                if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
+                if (ray_box_p(P, x, w, tmin, tmax)) {
                     x = x + w * tmin;
                     d = tmax - tmin;
                 }
@@ -545,7 +545,7 @@ VPT_DEV F3 track_nee_iso(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, 
     bool first_point = true;
     int it = 0;
     float tmin, tmax;
-    if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
+    if (ray_box_p(P, x, w, tmin, tmax)) {
         x = x + w * tmin;
         float d = tmax - tmin;
         int bounces = 0;
@@ -584,7 +584,7 @@ VPT_DEV F3 track_nee_iso(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, 
                 const float f = (pdf_phase / pdf_light) * tr;
                 const F3 l = sky_and_sun(P, dir_light);
                 color = color + f3((f * l.x) * weights.x, (f * l.y) * weights.y, (f * l.z) * weights.z);
-                if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
+                if (ray_box_p(P, x, w, tmin, tmax)) {
                     x = x + w * tmin;
                     d = tmax - tmin;
                 }
@@ -669,7 +669,7 @@ VPT_DEV F3 track_delta_spectral(const TraceParams& P, S& sample, Rng& rng, F3 x,
     bool first_point = true;
     int it = 0;
     float tmin, tmax;
-    if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
+    if (ray_box_p(P, x, w, tmin, tmax)) {
         x = x + w * tmin;
         float d = tmax - tmin;
         int bounces = 0;
@@ -706,7 +706,7 @@ VPT_DEV F3 track_delta_spectral(const TraceParams& P, S& sample, Rng& rng, F3 x,
                 const F3 w_in = w;
                 w = sample_phase(rng, P.g, w);
                 record_scatter(fe, x, density, P.sdt_majorant, tmax - d + t, w_in, w, P.g);
-                if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
+                if (ray_box_p(P, x, w, tmin, tmax)) {
                     x = x + w * tmin;
                     d = tmax - tmin;
                 }
@@ -725,17 +725,23 @@ VPT_DEV F3 track_delta_spectral(const TraceParams& P, S& sample, Rng& rng, F3 x,
 
 // VptMode::NEXT_EVENT_TRACKING_SPECTRAL (nextEventTrackingSpectral, NextEventTracking.glsl:31-220):
 // spectral tracking with a next-event estimate at every scatter event (transmittance from the
-// achromatic shadow estimators, NeeTransmittance.glsl, like the reference).
-template <bool ESS, class S>
+// achromatic shadow estimators, NeeTransmittance.glsl, like the reference).  ISO: with isosurfaces and
+// USE_ISOSURFACE_NEE (no lights): the 1000-iteration cap, iso_segment with surface next-event
+// estimation, delta-tracked shadow rays, emission scaled by the surface throughput.
+template <bool ESS, bool ISO = false, class S>
 VPT_DEV F3 track_nee_spectral(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, FirstEvent& fe, PathCtx& pc) {
     F3 weights = f3(1.0f, 1.0f, 1.0f);
     F3 color = f3(0.0f, 0.0f, 0.0f);
+    float last_sign = 0.0f;
+    bool first_point = true;
+    int it = 0;
     float tmin, tmax;
-    if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
+    if (ray_box_p(P, x, w, tmin, tmax)) {
         x = x + w * tmin;
         float d = tmax - tmin;
         int bounces = 0;
         while (true) {
+            if (ISO && ++it == 1000) return f3(0.0f, 0.0f, 0.0f);
             if (guard(pc)) return color;
             float t = free_path(rng, P.inv_sdt_majorant);
             if (t > d) break;
@@ -744,6 +750,13 @@ VPT_DEV F3 track_nee_spectral(const TraceParams& P, S& sample, Rng& rng, F3 x, F
             // (NextEventTracking.glsl:74, sampleCloudDensityEmission(x)); reproduced
             float density = sample(P.tf ? x : xn, rng);
             pc.lookups++;
+            if constexpr (ISO) {  // CheckIsosurfaceHit.glsl with surface next-event estimation
+                if (iso_segment<true>(P, sample, rng, x, xn, density, w, d, tmax, weights, last_sign, first_point,
+                                      pc.lookups, &fe, &color, &pc)) {
+                    if (weights.x < 1e-3f && weights.y < 1e-3f && weights.z < 1e-3f) return f3(0.0f, 0.0f, 0.0f);
+                    continue;
+                }
+            }
             x = xn;
             const SdtStep st = sdt_probabilities(P, density, weights, sdt_albedo(P, sample));
             float xi = rng_next(rng);
@@ -751,6 +764,10 @@ VPT_DEV F3 track_nee_spectral(const TraceParams& P, S& sample, Rng& rng, F3 x, F
                 record_event(fe, x, density, P.sdt_majorant, tmax - d + t);
                 // USE_EMISSION (NextEventTracking.glsl:125-131); else USE_TRANSFER_FUNCTION (:133-139),
                 // which returns the emission without the NEE colour gathered so far
+                if (ISO && P.emission) {  // NextEventTracking.glsl:118-124: the surface throughput applies
+                    const F3 e = sample.emission(x, rng);
+                    return color + f3(weights.x * e.x, weights.y * e.y, weights.z * e.z);
+                }
                 return P.emission ? color + sample.emission(x, rng) : (P.tf ? sample.tf_emission() : color);
             }
             if (xi < st.pa + st.ps) {
@@ -786,13 +803,14 @@ VPT_DEV F3 track_nee_spectral(const TraceParams& P, S& sample, Rng& rng, F3 x, F
                                            ((common.z / pdf_light) * tr) * l.z);
                     }
                 } else {
-                    const float tr = ESS ? shadow_transmittance_ess(P, sample, rng, x, dir_light, pc)
-                                         : shadow_transmittance(P, sample, rng, x, dir_light, pc);
+                    const float tr = ISO ? shadow_transmittance_delta(P, sample, rng, x, dir_light, pc)
+                                         : (ESS ? shadow_transmittance_ess(P, sample, rng, x, dir_light, pc)
+                                                : shadow_transmittance(P, sample, rng, x, dir_light, pc));
                     const float f = (pdf_phase / pdf_light) * tr;
                     const F3 l = sky_and_sun(P, dir_light);
                     color = color + f3((f * wc.x) * l.x, (f * wc.y) * l.y, (f * wc.z) * l.z);
                 }
-                if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
+                if (ray_box_p(P, x, w, tmin, tmax)) {
                     x = x + w * tmin;
                     d = tmax - tmin;
                 }
@@ -1179,7 +1197,7 @@ template <class S>
 VPT_DEV float shadow_residual_ratio(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, float max_dist,
                                     PathCtx& pc) {
     float tmin, tmax;
-    if (!ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) return 1.0f;
+    if (!ray_box_p(P, x, w, tmin, tmax)) return 1.0f;
     const float d = fminf(tmax, max_dist) - tmin;
     if (!(d > 0.0f)) return 1.0f;
     x = x + w * tmin;
@@ -1217,7 +1235,7 @@ VPT_DEV F3 track_residual_ratio_nee(const TraceParams& P, S& sample, Rng& rng, F
                                     PathCtx& pc) {
     F3 color = f3(0.0f, 0.0f, 0.0f);
     float tmin, tmax;
-    if (ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) {
+    if (ray_box_p(P, x, w, tmin, tmax)) {
         x = x + w * tmin;
         float d = tmax - tmin;
         float depth0 = tmin;  // distance of x from the camera while no event has happened
@@ -1288,7 +1306,7 @@ VPT_DEV F3 track_residual_ratio_nee(const TraceParams& P, S& sample, Rng& rng, F
                 const F3 l = sky_and_sun(P, dir_light);
                 color = color + f3(f * l.x, f * l.y, f * l.z);
             }
-            if (!ray_box(P.box_min, P.box_max, x, w, tmin, tmax)) break;
+            if (!ray_box_p(P, x, w, tmin, tmax)) break;
             x = x + w * tmin;
             d = tmax - tmin;
         }

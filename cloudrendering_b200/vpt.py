@@ -314,6 +314,21 @@ def set_brdf_parameter(key: str, value: str) -> None:
     _c("vpt_set_brdf_parameter", str(key).encode(), str(value).encode())
 
 
+def set_use_clip_plane(_use_clip_plane: bool) -> None:
+    """Cuts every ray to the positive side of the clip plane (src/PyTorch/Module.cpp:1218-1220)."""
+    _c("vpt_set_use_clip_plane", 1 if _use_clip_plane else 0)
+
+
+def set_clip_plane_normal(_clip_plane_normal) -> None:
+    """The clip plane's normal, three numbers (normalised by the renderer; Module.cpp:1222-1227)."""
+    _c("vpt_set_clip_plane_normal", *_vec3(_clip_plane_normal, "setClipPlaneNormal"))
+
+
+def set_clip_plane_distance(_clip_plane_distance: float) -> None:
+    """The clip plane's distance along its normal (Module.cpp:1229-1231)."""
+    _c("vpt_set_clip_plane_distance", float(_clip_plane_distance))
+
+
 def set_num_isosurface_subdivisions(subdivisions: int) -> None:
     _c("vpt_set_num_isosurface_subdivisions", int(subdivisions))
 

@@ -149,10 +149,10 @@ VptStatus vpt_set_tf_scattering_albedo_strength(VptContext* ctx, float strength)
  * DeltaTracking.glsl and CheckIsosurfaceHit.glsl): the surface where the normalised density crosses
  * iso_value (default 0.5) is found on every free-flight segment and reflects like an opaque surface
  * of colour iso_surface_color (default 0.4 0.4 0.4) with the selected BRDF; lookups are trilinear
- * while isosurfaces are on.  Built for delta, spectral delta and next event tracking on dense grids
- * (next event tracking with surface next-event estimation, USE_ISOSURFACE_NEE, for sky light samples:
- * with lights, an environment image or empty-space skipping it returns VPT_ERR_UNSUPPORTED); other
- * trackers, sparse grids, a transfer function and batched rendering return VPT_ERR_UNSUPPORTED.  Types "Density" and "Gradient"
+ * while isosurfaces are on.  Built for delta and next event tracking, plain and spectral, on dense
+ * grids (next event tracking with surface next-event estimation, USE_ISOSURFACE_NEE, for sky light
+ * samples: with lights, an environment image or empty-space skipping it returns VPT_ERR_UNSUPPORTED);
+ * other trackers, sparse grids, a transfer function and batched rendering return VPT_ERR_UNSUPPORTED.  Types "Density" and "Gradient"
  * (the surface where the trilinear-filtered gradient magnitude of the raw grid crosses iso_value:
  * central differences with clamped neighbours, VolumetricPathTracingPass.cpp:690-745, built on the GPU
  * at the first render after the grid or the type changed) and the BRDFs
@@ -174,6 +174,15 @@ VptStatus vpt_set_isosurface_type(VptContext* ctx, const char* name);
 VptStatus vpt_set_surface_brdf(VptContext* ctx, const char* name);
 VptStatus vpt_set_brdf_parameter(VptContext* ctx, const char* key, const char* value);
 VptStatus vpt_set_num_isosurface_subdivisions(VptContext* ctx, int subdivisions);
+/* The clip plane (set_use_clip_plane / set_clip_plane_normal / set_clip_plane_distance,
+ * src/PyTorch/Module.cpp:1218-1232; USE_CLIP_PLANE in rayBoxIntersect, VptUtils.glsl:776-799): every
+ * ray's interval in the volume box is cut to the side where dot(n, x) > distance, n the normalised
+ * normal (default (1, 0, 0), distance 0, off).  Built for delta, ratio and next event tracking (plain
+ * and spectral; with isosurfaces too); decomposition, residual ratio tracking and empty-space skipping
+ * return VPT_ERR_UNSUPPORTED while it is on.  A zero or non-finite normal returns VPT_ERR_ARG. */
+VptStatus vpt_set_use_clip_plane(VptContext* ctx, int use);
+VptStatus vpt_set_clip_plane_normal(VptContext* ctx, double x, double y, double z);
+VptStatus vpt_set_clip_plane_distance(VptContext* ctx, double distance);
 /* Synthetic scene on the device: seeded fBm of improved Perlin noise, remapped to [0, 1], values
  * below `threshold` set to 0.  No reference counterpart (the reference loads files). */
 VptStatus vpt_generate_fbm_grid(VptContext* ctx, int nx, int ny, int nz, uint32_t seed, int octaves,

@@ -31,6 +31,7 @@ class RefScene(ctypes.Structure):
         ("emission_strength", c_float), ("tf", c_void_p), ("tf_size", c_int),
         ("iso_value", c_float), ("iso_color", c_float * 3), ("env_rot", c_float * 9), ("prev_view_proj", c_float * 16),
         ("tf_albedo_strength", c_float), ("brdf", c_float * 10), ("gradient", c_void_p),
+        ("use_clip", c_int), ("clip", c_float * 4),
     ]
 
 

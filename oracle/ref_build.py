@@ -132,6 +132,12 @@ def variants():
                         ("cook", "SURFACE_BRDF_COOK_TORRANCE"), ("disney", "SURFACE_BRDF_DISNEY")):
         out.append((f"delta_iso_{tag}__trilinear__default__linear", TRACKERS["delta"] + [INTERPS["trilinear"]]
                     + ENVS["default__linear"] + [define if d == "SURFACE_BRDF_LAMBERTIAN" else d for d in ISO], 0))
+    # the clip plane (USE_CLIP_PLANE, VolumetricPathTracingPass.cpp:1774-1776): delta and next event tracking
+    for t in ("delta", "nee"):
+        out.append((f"{t}_clip__stochastic__default__linear", TRACKERS[t] + [INTERPS["stochastic"]]
+                    + ENVS["default__linear"] + ["USE_CLIP_PLANE"], 0))
+    out.append(("sdt_hist_clip__stochastic__default__linear", [SPECTRAL["sdt"], SDT_PROB["hist"],
+                INTERPS["stochastic"]] + ENVS["default__linear"] + ["USE_CLIP_PLANE"], 0))
     # next event tracking with isosurfaces (USE_ISOSURFACE_NEE, VolumetricPathTracingPass.cpp:1761-1763) for
     # every surface BRDF
     for tag, define in (("", "SURFACE_BRDF_LAMBERTIAN"), ("_blinn", "SURFACE_BRDF_BLINN_PHONG"),
@@ -140,6 +146,11 @@ def variants():
         out.append((f"nee_iso{tag}__trilinear__default__linear", TRACKERS["nee"] + [INTERPS["trilinear"]]
                     + ENVS["default__linear"] + [define if d == "SURFACE_BRDF_LAMBERTIAN" else d for d in ISO]
                     + ["USE_ISOSURFACE_NEE"], 0))
+    # spectral next event tracking with isosurfaces and surface next-event estimation (Lambertian, Cook-Torrance)
+    for tag, define in (("", "SURFACE_BRDF_LAMBERTIAN"), ("_cook", "SURFACE_BRDF_COOK_TORRANCE")):
+        out.append((f"nees_hist_iso{tag}__trilinear__default__linear", [SPECTRAL["nees"], SDT_PROB["hist"],
+                    INTERPS["trilinear"]] + ENVS["default__linear"]
+                    + [define if d == "SURFACE_BRDF_LAMBERTIAN" else d for d in ISO] + ["USE_ISOSURFACE_NEE"], 0))
     # spectral delta tracking with isosurfaces (DeltaTracking.glsl:37-63), path-history and max probabilities
     for p in ("hist", "max"):
         out.append((f"sdt_{p}_iso__trilinear__default__linear", [SPECTRAL["sdt"], SDT_PROB[p], INTERPS["trilinear"]]

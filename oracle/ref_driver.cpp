@@ -98,6 +98,8 @@ typedef struct RefScene {
     float brdf[10];           /* parameters.subsurface, metallic, specular, specularTint, roughness,
                                  anisotropic, sheen, sheenTint, clearcoat, clearcoatGloss */
     const float* gradient;    /* gradientImage values [nz][ny][nx] (ISOSURFACE_TYPE_GRADIENT variants) */
+    int use_clip;             /* parameters.useClipPlane (USE_CLIP_PLANE variants) */
+    float clip[4];            /* parameters.clipPlaneNormal (normalised), clipPlaneDistance */
 } RefScene;
 
 int ref_variant_count(void) { return ref_num_variants; }
@@ -173,6 +175,9 @@ int ref_render(int variant, const RefScene* s, float* out_rgba, int threads) {
     p.emissionCap = s->emission_cap;
     p.emissionStrength = s->emission_strength;
     p.tfScatteringAlbedoStrength = s->tf_albedo_strength;
+    p.useClipPlane = s->use_clip;
+    p.clipPlaneNormal = vec3(s->clip[0], s->clip[1], s->clip[2]);
+    p.clipPlaneDistance = s->clip[3];
     p.subsurface = s->brdf[0];
     p.metallic = s->brdf[1];
     p.specular = s->brdf[2];

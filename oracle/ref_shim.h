@@ -464,6 +464,10 @@ struct Parameters {
     float isoStepWidth;
     float maxAoDist;
     int numAoSamples;
+    // clip plane (VptHeader.glsl:95-98)
+    int useClipPlane;
+    vec3 clipPlaneNormal;
+    float clipPlaneDistance;
     // surface BRDF parameters (VptHeader.glsl:100-111)
     float subsurface, metallic, specular, specularTint, roughness, anisotropic, sheen, sheenTint;
     vec3 camForward;

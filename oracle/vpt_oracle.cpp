@@ -93,7 +93,10 @@ void camera_ray(const OracleScene& S, float sx, float sy, V3& x, V3& w) {
     w = normalize(sub(vt, vp));
 }
 
-// ---- rayBoxIntersect (VptUtils.glsl:763-801) ----
+// USE_CLIP_PLANE: the normalised plane normal and distance of the scene being rendered, or null
+static const float* g_clip = nullptr;
+
+// ---- rayBoxIntersect (VptUtils.glsl:763-801), with the clip plane's interval cut when it is on ----
 bool ray_box(V3 bmin, V3 bmax, V3 p, V3 d, float& tmin, float& tmax) {
     d.x = fabsf(d.x) <= 0.000001f ? 0.000001f : d.x;
     d.y = fabsf(d.y) <= 0.000001f ? 0.000001f : d.y;
@@ -102,7 +105,19 @@ bool ray_box(V3 bmin, V3 bmax, V3 p, V3 d, float& tmin, float& tmax) {
     tmin = std::max(std::max(std::min(cmin.x, cmax.x), std::min(cmin.y, cmax.y)), std::min(cmin.z, cmax.z));
     tmin = std::max(0.0f, tmin);
     tmax = std::min(std::min(std::max(cmin.x, cmax.x), std::max(cmin.y, cmax.y)), std::max(cmin.z, cmax.z));
-    return !(tmax <= tmin || tmax <= 0.0f);
+    if (tmax <= tmin || tmax <= 0.0f) return false;
+    if (g_clip) {  // the part of the ray on the plane's positive side (the direction as modified above)
+        const V3 n = v3(g_clip[0], g_clip[1], g_clip[2]);
+        const float denom = dot(n, d);
+        const float dp = dot(n, p) - g_clip[3];
+        if (fabsf(denom) < 0.001f) return dp > 0.0f;
+        const float t_clip = (g_clip[3] - dot(n, p)) / denom;
+        if (t_clip <= 0.0f) return dp > 0.0f;
+        if (dp > 0.0f) tmax = std::min(t_clip, tmax);
+        else tmin = std::max(t_clip, tmin);
+        if (tmax <= tmin || tmax <= 0.0f) return false;
+    }
+    return true;
 }
 
 // ---- directions (VptUtils.glsl:67-123) ----
@@ -1703,12 +1718,16 @@ struct Tracer {
     V3 spectral_nee(V3 x, V3 w, Rng& r, bool& ev) {
         const float maj = maxc(ext3());
         V3 weights = v3(1, 1, 1), color = v3(0, 0, 0);
+        float last_sign = 0.0f;
+        bool first_point = true;
+        int it = 0;
         float tmin, tmax;
         if (ray_box(bmin(), bmax(), x, w, tmin, tmax)) {
             x = add(x, mul(w, tmin));
             float d = tmax - tmin;
             int bounces = 0;
             while (true) {
+                if (S.use_iso && ++it == 1000) return v3(0, 0, 0);
                 if (guard()) return color;
                 float t = -m_log(std::max(0.0000000001f, 1.0f - rnd(r))) * (1.0f / maj);
                 if (t > d) break;
@@ -1716,6 +1735,11 @@ struct Tracer {
                 // with a transfer function the reference looks up the previous point x
                 // (NextEventTracking.glsl:74, sampleCloudDensityEmission(x))
                 float dens = sample(S.tf ? x : xn, r);
+                // isosurfaces (CheckIsosurfaceHit.glsl with USE_ISOSURFACE_NEE)
+                if (S.use_iso && iso_check(x, xn, w, d, tmax, weights, last_sign, first_point, r, ev, &color)) {
+                    if (weights.x < 1e-3f && weights.y < 1e-3f && weights.z < 1e-3f) return v3(0, 0, 0);
+                    continue;
+                }
                 x = xn;
                 V3 sa, ss, sn;
                 float pa, ps, pn;
@@ -1724,6 +1748,10 @@ struct Tracer {
                 if (xi < pa) {
                     ev = true;
                     // USE_EMISSION (NextEventTracking.glsl:125-131); else USE_TRANSFER_FUNCTION (:133-139)
+                    if (S.use_iso && S.emission) {  // the surface throughput applies (NextEventTracking.glsl:118-124)
+                        const V3 e = emission(x, r);
+                        return add(color, v3(weights.x * e.x, weights.y * e.y, weights.z * e.z));
+                    }
                     return S.emission ? add(color, emission(x, r)) : (S.tf ? tf_emission() : color);
                 }
                 if (xi < pa + ps) {
@@ -1756,7 +1784,9 @@ struct Tracer {
                                                   ((common.z / pdf_l) * tr) * l.z));
                         }
                     } else {
-                        float tr = S.use_ess ? transmittance_ess(x, dl, r) : transmittance(x, dl, r);
+                        // with isosurfaces every shadow ray is delta tracked (USE_TRANSMITTANCE_DELTA_TRACKING)
+                        float tr = S.use_iso ? transmittance_delta(x, dl, r)
+                                             : (S.use_ess ? transmittance_ess(x, dl, r) : transmittance(x, dl, r));
                         float f = (pdf_p / pdf_l) * tr;
                         V3 l = sky(dl);
                         color = add(color, v3((f * wc.x) * l.x, (f * wc.y) * l.y, (f * wc.z) * l.z));
@@ -2245,6 +2275,7 @@ static bool scene_inputs_ok(const OracleScene* s) {
 
 int oracle_render_rows(const OracleScene* s, int row0, int row1, double* film, uint64_t* lookups, int threads) {
     if (!scene_inputs_ok(s)) return 2;
+    g_clip = s->use_clip ? s->clip : nullptr;
     const OracleScene& S = *s;
     uint64_t total_lookups = 0;
     int nt = threads_or_default(threads);
@@ -2277,6 +2308,7 @@ int oracle_render_rows(const OracleScene* s, int row0, int row1, double* film, u
 
 int oracle_render(const OracleScene* s, double* film, double* film_sq, uint64_t* lookups, int threads) {
     if (!scene_inputs_ok(s)) return 2;
+    g_clip = s->use_clip ? s->clip : nullptr;
     const OracleScene& S = *s;
     uint64_t total_lookups = 0;
     int nt = threads_or_default(threads);
@@ -2312,6 +2344,7 @@ int oracle_render(const OracleScene* s, double* film, double* film_sq, uint64_t*
 int oracle_trace_paths(const OracleScene* s, const int* xs, const int* ys, const uint32_t* frames, int n,
                        float* out_rgb, int threads) {
     if (!scene_inputs_ok(s)) return 2;
+    g_clip = s->use_clip ? s->clip : nullptr;
     int nt = threads_or_default(threads);
 #pragma omp parallel num_threads(nt)
     {

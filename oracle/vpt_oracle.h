@@ -98,6 +98,10 @@ typedef struct OracleScene {
      * isosurfaces); normals read them as (v - iso_norm_min) / iso_norm_range (the density's range) */
     const float* iso_grad;
     float iso_norm_min, iso_norm_range;
+    /* USE_CLIP_PLANE: every ray-box interval cut to the plane's positive side; clip = normalised
+     * normal (3) and distance */
+    int use_clip;
+    float clip[4];
 } OracleScene;
 
 /* Renders width*height*num_frames paths; adds radiance (and its square) per pixel (3 doubles). */

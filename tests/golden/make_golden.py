@@ -140,6 +140,12 @@ def cases():
         kw2.update(iso_value=0.3, iso_color=(0.9, 0.6, 0.3), extinction=40.0, albedo=0.9, g=0.2)
         out["fbm_" + name] = SceneSpec(grid=fbm, mode="delta", interp="trilinear", iso=True, iso_brdf="Disney (2012)",
                                        brdf_params=params, **kw2)
+    # the clip plane (USE_CLIP_PLANE): an oblique plane through the cloud, camera on its positive side
+    for name, kw in {"delta_clip": dict(mode="delta"), "nee_clip": dict(mode="nee"),
+                     "sdt_hist_clip": dict(mode="spectral_delta", sdt_prob=2, **chroma)}.items():
+        kw2 = dict(base)
+        kw2.update(kw)
+        out["fbm_" + name] = SceneSpec(grid=fbm, clip_plane=(0.3, 0.5, 0.8, -0.02), **kw2)
     # next event tracking with isosurfaces and surface next-event estimation, every BRDF (MIS for the
     # specular samples of Cook-Torrance and Disney)
     for name, brdf, params in (("nee_iso", "Lambertian", None), ("nee_iso_blinn", "Blinn Phong", None),
@@ -151,6 +157,15 @@ def cases():
         kw2.update(iso_value=0.3, iso_color=(0.9, 0.6, 0.3), extinction=40.0, albedo=0.9, g=0.2)
         out["fbm_" + name] = SceneSpec(grid=fbm, mode="nee", interp="trilinear", iso=True, iso_brdf=brdf,
                                        brdf_params=params, **kw2)
+    # spectral next event tracking with isosurfaces (path-history probabilities, chromatic medium)
+    for name, brdf, params in (("nees_hist_iso", "Lambertian", None),
+                               ("nees_hist_iso_cook", "Cook Torrance", {"metallic": 0.6, "specular": 0.8,
+                                                                        "roughness": 0.25})):
+        kw2 = dict(base)
+        kw2.update(iso_value=0.3, iso_color=(0.9, 0.6, 0.3), extinction=40.0, g=0.2,
+                   extinction_base=(1.0, 0.7, 0.4), albedo_rgb=(0.95, 0.8, 0.9))
+        out["fbm_" + name] = SceneSpec(grid=fbm, mode="spectral_nee", sdt_prob=2, interp="trilinear", iso=True,
+                                       iso_brdf=brdf, brdf_params=params, **kw2)
     # spectral delta tracking with isosurfaces: a chromatic medium around the coloured density surface
     for name, prob in {"sdt_hist_iso": 2, "sdt_max_iso": 0}.items():
         kw2 = dict(base)
@@ -192,7 +207,7 @@ FIELDS = ["mode", "interp", "extinction", "albedo", "g", "width", "height", "see
           "sun_dir", "sun_intensity", "cam_pos", "cam_target", "fovy", "near", "far", "max_grid_extent", "use_ess",
           "env_intensity", "max_bounces", "ess_ref_compat", "lights", "extinction_base", "albedo_rgb", "sdt_prob",
           "emission_cap", "emission_strength", "iso", "iso_value", "iso_color", "env_rot", "tf_albedo_strength",
-          "iso_brdf", "brdf_params", "iso_type"]
+          "iso_brdf", "brdf_params", "iso_type", "clip_plane"]
 
 
 def depth_map_cases():

@@ -70,7 +70,8 @@ class SceneSpec:
                  use_ess=False, env_intensity=(1.0, 1.0, 1.0), ess_ref_compat=False, lights=None,
                  extinction_base=(1.0, 1.0, 1.0), albedo_rgb=None, sdt_prob=2, emission=None, emission_cap=1.0,
                  emission_strength=1.0, tf=None, iso=False, iso_value=0.5, iso_color=(0.4, 0.4, 0.4), env_rot=None,
-                 tf_albedo_strength=0.0, iso_brdf="Lambertian", brdf_params=None, iso_type="Density"):
+                 tf_albedo_strength=0.0, iso_brdf="Lambertian", brdf_params=None, iso_type="Density",
+                 clip_plane=None):
         self.__dict__.update(locals())
         del self.__dict__["self"]
 
@@ -99,6 +100,17 @@ def gradient_magnitude(grid):
 
     dz, dy, dx = diff(0), diff(1), diff(2)
     return np.sqrt((dx * dx + dy * dy) + dz * dz).astype(np.float32)
+
+
+def clip_values(sp):
+    """The clip plane's normal as the pass uploads it (glm::normalize: v * inversesqrt(dot(v, v)), in
+    float32) and its distance, or None."""
+    if sp.clip_plane is None:
+        return None
+    v = np.array(sp.clip_plane[:3], np.float32)
+    dd = np.float32(np.float32(v[0] * v[0]) + np.float32(v[1] * v[1])) + np.float32(v[2] * v[2])
+    inv = np.float32(np.float32(1.0) / np.sqrt(np.float32(dd), dtype=np.float32))
+    return [float(np.float32(c * inv)) for c in v] + [float(np.float32(sp.clip_plane[3]))]
 
 
 def brdf_values(sp):
@@ -187,6 +199,10 @@ def setup_core(core: Core, sp: SceneSpec):
     core("vpt_set_use_isosurfaces", 1 if sp.iso else 0)
     core("vpt_set_surface_brdf", sp.iso_brdf.encode())
     core("vpt_set_isosurface_type", sp.iso_type.encode())
+    core("vpt_set_use_clip_plane", 1 if sp.clip_plane is not None else 0)
+    if sp.clip_plane is not None:
+        core("vpt_set_clip_plane_normal", *[float(c) for c in sp.clip_plane[:3]])
+        core("vpt_set_clip_plane_distance", float(sp.clip_plane[3]))
     for k, v in zip(BRDF_KEYS, brdf_values(sp)):
         core("vpt_set_brdf_parameter", k.encode(), repr(v).encode())
     core("vpt_set_iso_value", sp.iso_value)
@@ -361,6 +377,9 @@ def oracle_scene(core, sp: SceneSpec, frames: int, frame_count: int = 0) -> brid
             sc.set("iso_grad", gradient_magnitude(g))
             sc.set("iso_norm_min", float(np.float32(vmin)))
             sc.set("iso_norm_range", float(np.float32(np.float32(vmax) - np.float32(vmin))))
+    if sp.clip_plane is not None:
+        sc.set("use_clip", 1)
+        sc.set("clip", clip_values(sp))
     sc.set("iso_value", float(np.float32(sp.iso_value)))
     sc.set("iso_color", [float(np.float32(c)) for c in sp.iso_color])
     if sp.env_rot is not None and sp.env == "image":
@@ -527,6 +546,10 @@ def reference_scene(sp: SceneSpec, frames: int, frame_start: int = 0, inv=None):
     if sp.env_rot is not None:
         sc.set("env_rot", [float(np.float32(v)) for v in sp.env_rot])
         tracker += "_rot"
+    if sp.clip_plane is not None:
+        sc.set("use_clip", 1)
+        sc.set("clip", clip_values(sp))
+        tracker += "_clip"
     env = {"default": "default", "black": "black", "single": "single", "image": "image"}[sp.env]
     colour = "linear" if (sp.linear_rgb or env != "default") else "srgb"
     return sc, f"{tracker}__{sp.interp}__{env}__{colour}"

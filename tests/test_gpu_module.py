@@ -371,3 +371,33 @@ def test_env_map_rotation_identity_and_camera():
     vpt.disable_env_map_rot()
     vpt.set_use_builtin_environment_map("Default")
     vpt.set_vpt_mode_from_name("Delta Tracking")
+
+
+def test_clip_plane():
+    """set_use_clip_plane / set_clip_plane_normal / set_clip_plane_distance: a plane through the cloud
+    changes the image, the trackers it is not built for raise, and the setters check their arguments
+    (the clipped paths themselves are pinned by the golden cases *_clip)."""
+    t = torch.zeros((3, 32, 32), dtype=torch.float32, device="cuda")
+    try:
+        vpt.set_vpt_mode_from_name("Delta Tracking")
+        vpt.set_seed_offset(0)
+        plain = vpt.render_frame(t, 2).clone()
+        vpt.set_use_clip_plane(True)
+        vpt.set_clip_plane_normal([0.3, 0.5, 0.8])
+        vpt.set_clip_plane_distance(0.0)
+        vpt.set_seed_offset(0)
+        cut = vpt.render_frame(t, 2).clone()
+        assert torch.isfinite(cut).all()
+        assert not torch.allclose(cut, plain, rtol=1e-3)
+        with pytest.raises(RuntimeError, match="size 3"):
+            vpt.set_clip_plane_normal([1.0, 0.0])
+        with pytest.raises(RuntimeError, match="non-zero"):
+            vpt.set_clip_plane_normal([0.0, 0.0, 0.0])
+        vpt.set_vpt_mode_from_name("Decomposition Tracking")
+        with pytest.raises(RuntimeError, match="clip plane"):
+            vpt.render_frame(t, 1)
+    finally:
+        vpt.set_use_clip_plane(False)
+        vpt.set_clip_plane_normal([1.0, 0.0, 0.0])
+        vpt.set_clip_plane_distance(0.0)
+        vpt.set_vpt_mode_from_name("Delta Tracking")
