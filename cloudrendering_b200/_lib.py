@@ -85,6 +85,7 @@ SIGNATURES = {
     "vpt_set_use_clip_plane": (c_int, [VptCtxP, c_int]),
     "vpt_set_clip_plane_normal": (c_int, [VptCtxP, c_double, c_double, c_double]),
     "vpt_set_clip_plane_distance": (c_int, [VptCtxP, c_double]),
+    "vpt_set_close_isosurfaces": (c_int, [VptCtxP, c_int]),
     "vpt_set_num_isosurface_subdivisions": (c_int, [VptCtxP, c_int]),
     "vpt_get_stats": (c_int, [VptCtxP, POINTER(VptStats)]),
     "vpt_reset_stats": (c_int, [VptCtxP]),

@@ -175,6 +175,7 @@ struct VptContext {
     int iso_type = 0;  // setIsosurfaceType: 0 Density, 1 Gradient
     // setUseClipPlane / setClipPlaneNormal / setClipPlaneDistance (VolumetricPathTracingPass.hpp:403-405)
     bool use_clip = false;
+    bool close_iso = false;  // setCloseIsosurfaces: CLOSE_ISOSURFACES with isosurfaces and the clip plane on
     float clip_normal[3] = {1.0f, 0.0f, 0.0f};
     float clip_distance = 0.0f;
     float iso_value = 0.5f;
@@ -678,6 +679,7 @@ VptStatus fill_params(VptContext* ctx, int tracker, int frames, vpt::TraceParams
     P.iso_color = mk(ctx->iso_color[0], ctx->iso_color[1], ctx->iso_color[2]);
     P.iso_grad = (ctx->use_iso && ctx->iso_type == 1) ? ctx->grad.ptr : nullptr;
     P.use_clip = ctx->use_clip ? 1 : 0;
+    P.iso_close = (ctx->use_clip && ctx->use_iso && ctx->close_iso) ? 1 : 0;  // VolumetricPathTracingPass.cpp:1777
     {  // the uniform holds glm::normalize(clipPlaneNormal): v * inversesqrt(dot(v, v)) in float
         const float* v = ctx->clip_normal;
         const float inv = 1.0f / std::sqrt((v[0] * v[0] + v[1] * v[1]) + v[2] * v[2]);
@@ -1188,6 +1190,13 @@ VptStatus vpt_set_clip_plane_normal(VptContext* ctx, double x, double y, double 
     if (v[0] != ctx->clip_normal[0] || v[1] != ctx->clip_normal[1] || v[2] != ctx->clip_normal[2])
         reset_film_state(ctx);
     for (int i = 0; i < 3; ++i) ctx->clip_normal[i] = v[i];
+    return VPT_OK;
+}
+
+VptStatus vpt_set_close_isosurfaces(VptContext* ctx, int close) {
+    VPT_CHECK_CTX(ctx);
+    if ((close != 0) != ctx->close_iso) reset_film_state(ctx);
+    ctx->close_iso = close != 0;
     return VPT_OK;
 }
 

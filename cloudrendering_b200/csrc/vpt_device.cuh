@@ -233,6 +233,44 @@ VPT_DEV bool ray_box_p(const TraceParams& P, F3 p, F3 d, float& tmin, float& tma
     return !(tmax <= tmin || tmax <= 0.0f);
 }
 
+// rayBoxIntersectionNormal (VptUtils.glsl:803-856, CLOSE_ISOSURFACES): the normal of the box face a ray
+// from p enters through, or -clip_n where the clip plane is the entry surface; n stays as it is when the
+// ray misses the box, or when the ray runs parallel to the plane or meets it behind p on its negative side.
+VPT_DEV void ray_box_normal(const TraceParams& P, F3 p, F3 d, F3& n) {
+    d.x = fabsf(d.x) <= 1e-6f ? 1e-6f : d.x;
+    d.y = fabsf(d.y) <= 1e-6f ? 1e-6f : d.y;
+    d.z = fabsf(d.z) <= 1e-6f ? 1e-6f : d.z;
+    const F3 cmin = (P.box_min - p) / d;
+    const F3 cmax = (P.box_max - p) / d;
+    const float mx = fminf(cmin.x, cmax.x), my = fminf(cmin.y, cmax.y), mz = fminf(cmin.z, cmax.z);
+    const float tmin = fmaxf(0.0f, fmaxf(fmaxf(mx, my), mz));
+    const float tmax = fminf(fminf(fmaxf(cmin.x, cmax.x), fmaxf(cmin.y, cmax.y)), fmaxf(cmin.z, cmax.z));
+    if (tmax <= tmin || tmax <= 0.0f) return;
+    auto sgn = [](float v) { return v > 0.0f ? 1.0f : (v < 0.0f ? -1.0f : 0.0f); };
+    F3 nb;
+    if (mx > my && mx > mz) nb = f3(-sgn(d.x), 0.0f, 0.0f);
+    else if (my > mz) nb = f3(0.0f, -sgn(d.y), 0.0f);
+    else nb = f3(0.0f, 0.0f, -sgn(d.z));
+    if (P.use_clip) {
+        const float denom = dot3(P.clip_n, d);
+        const float dp = dot3(P.clip_n, p) - P.clip_d;
+        if (fabsf(denom) < 1e-3f) {
+            if (dp > 0.0f) n = nb;
+            return;
+        }
+        const float t_clip = (P.clip_d - dot3(P.clip_n, p)) / denom;
+        if (t_clip <= 0.0f) {
+            if (dp > 0.0f) n = nb;
+            return;
+        }
+        if (dp <= 0.0f && t_clip >= tmin) {
+            n = f3(-P.clip_n.x, -P.clip_n.y, -P.clip_n.z);
+            return;
+        }
+    }
+    n = nb;
+}
+
 // ---------------------------------------------------------------------------------------------
 // Direction sampling (VptUtils.glsl:67-123).
 VPT_DEV void orthonormal_basis(F3 d, F3& b, F3& t) {
@@ -1039,10 +1077,11 @@ VPT_DEV F3 disney_pdf_value(const TraceParams& P, const IsoFrame& fr, F3 l) {
 // (Lambertian.glsl is included before UNIFORM_SAMPLING is defined, so the concentric-disk map of
 // VptUtils.glsl:1078-1098 and a pdf factor equal to the cosine), value color * cos / cos.  This part
 // ends at computeBrdf and returns the frame and the sample.
-VPT_DEV IsoBrdfSample iso_sample(const TraceParams& P, Rng& rng, F3 p, F3 w, IsoFrame& fr) {
+VPT_DEV IsoBrdfSample iso_sample(const TraceParams& P, Rng& rng, F3 p, F3 w, IsoFrame& fr, const F3* cam = nullptr) {
     (void)rng_next(rng);  // isoSurfaceOpacity (1) < random() never holds
     F3 n = iso_normal(P, p);
-    if (dot3(w, n) > 0.0f) n = -n;
+    if (cam) ray_box_normal(P, *cam, w, n);  // a closing surface (CLOSE_ISOSURFACES): the face entered
+    else if (dot3(w, n) > 0.0f) n = -n;
     const float yz = -n.y * n.z;
     const F3 b = normalize3(fabsf(n.z) > 0.99999f ? f3(-n.x * n.y, 1.0f - n.y * n.y, yz)
                                                   : f3(-n.x * n.z, yz, 1.0f - n.z * n.z));

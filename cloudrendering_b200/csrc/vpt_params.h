@@ -223,6 +223,9 @@ struct TraceParams {
     int use_clip;
     F3 clip_n;
     float clip_d;
+    // CLOSE_ISOSURFACES (isosurfaces with the clip plane on): the box faces and the clip plane close the
+    // isosurfaces, i.e. outside the volume counts as below the iso value on a path's first check point
+    int iso_close;
     unsigned long long* counters;  // [0] paths, [1] density lookups
     int* error_flags;
     unsigned int* work_counter;    // persistent-kernel path queue

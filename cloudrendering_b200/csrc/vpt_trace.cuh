@@ -45,9 +45,11 @@ struct Sampler {
     }
     // the emission grid is dense whatever the density grid is
     VPT_DEV F3 emission(F3 pos, Rng& rng) const { return sample_emission<INTERP>(P, pos, rng); }
-    VPT_DEV F3 normal(F3 pos, Rng& rng) const {
+    VPT_DEV F3 normal(F3 pos, Rng& rng, const FirstEvent* fe = nullptr) const {
         // getCloudFiniteDifference returns 0 for NanoVDB grids (VptUtils.glsl:726-729)
         if constexpr (GRID == kNanoVdb) return f3(0.0f, 0.0f, 0.0f);
+        // CLOSE_ISOSURFACES: a surface hit as the first event writes its own normal (Clouds.glsl:266-272)
+        else if (P.iso && P.iso_close && fe && fe->iso) return fe->n;
         // with isosurfaces the normal map is -computeGradient at the first event (Clouds.glsl:274-275)
         else if (P.iso) return -iso_normal(P, pos);
         else return density_normal<INTERP>(P, pos, rng);
@@ -146,7 +148,7 @@ VPT_DEV void accumulate_features(const TraceParams& P, S& sample, Rng& rng, size
         atomicAdd(f + kFeatBackground + 2, bg.z);
     }
     if (fe.has) {
-        F3 n = sample.normal(fe.x, rng);
+        F3 n = sample.normal(fe.x, rng, &fe);
         frame_normal = make_float4(n.x, n.y, n.z, 1.0f);
         atomicAdd(f + kFeatNormal + 0, n.x);
         atomicAdd(f + kFeatNormal + 1, n.y);
@@ -243,6 +245,7 @@ VPT_DEV void trace_one(const TraceParams& P, S& sample, uint32_t frame, int px, 
     camera_ray(P, sx, sy, x, w);
     FirstEvent fe;
     fe.has = false;
+    fe.iso = false;
     PathCtx pc;
     pc.steps = 0;
     pc.max_steps = P.max_steps;
@@ -1020,7 +1023,8 @@ static cudaError_t launch_trace_t(const TraceParams& P, int schedule, int featur
     constexpr bool kRefillable = TRACKER == kDelta || TRACKER == kRatio || TRACKER == kNextEvent ||
                                  TRACKER == kNextEvent + 100 || TRACKER == kDeltaIso ||
                                  ((TRACKER == kDecomposition || TRACKER == kResidualRatioNee) && GRID != kNanoVdb);
-    if (schedule == kScheduleRefill && kRefillable && !features) {
+    // the refill loop's surface check has no closing surfaces (CLOSE_ISOSURFACES): persistent batches then
+    if (schedule == kScheduleRefill && kRefillable && !features && !P.iso_close) {
         if constexpr (kRefillable) {
             int blocks = refill_blocks<TRACKER, INTERP, GRID, TF>(persistent_blocks);
             cudaMemsetAsync(P.work_counter, 0, sizeof(unsigned long long), stream);

@@ -18,6 +18,8 @@ struct FirstEvent {
     float density;
     F3 w;         // direction after the first scatter (0 when the first event is an absorption)
     float pdf_w;  // phase-function density of that direction (firstEvent.pdf_w)
+    bool iso;     // CLOSE_ISOSURFACES: the first event is a surface hit, whose normal is n
+    F3 n;
 };
 
 struct PathCtx {
@@ -121,10 +123,15 @@ template <class S>
 VPT_DEV void iso_surface_nee(const TraceParams& P, S& sample, Rng& rng, F3 x, const IsoFrame& fr,
                              const IsoBrdfSample& bs, F3 thr, F3& color, PathCtx& pc);
 
+// With CLOSE_ISOSURFACES (`outside` given, true until the path's first check point): on that first point
+// outside the volume counts as sign(-iso_value), so a path entering the box inside a surface meets the
+// closing surface there, whose normal is the face entered from the camera position `cam`
+// (rayBoxIntersectionNormal); the surface normal is kept in the first event for the normal map.
 template <bool NEE = false, class S>
 VPT_DEV bool iso_segment(const TraceParams& P, S& sample, Rng& rng, F3& x, F3 xn, float density, F3& w, float& d,
                          float& tmax, F3& weights, float& last_sign, bool& first_point, uint32_t& lookups,
-                         FirstEvent* fe, F3* nee_color = nullptr, PathCtx* pc = nullptr) {
+                         FirstEvent* fe, F3* nee_color = nullptr, PathCtx* pc = nullptr, bool* outside = nullptr,
+                         F3 cam = F3{0.0f, 0.0f, 0.0f}) {
     const int nsub = P.iso_subdivisions;
     for (int sub = 0; sub < nsub; ++sub) {
         const float a0 = (float)sub / (float)nsub, a1 = (float)(sub + 1) / (float)nsub;
@@ -140,7 +147,11 @@ VPT_DEV bool iso_segment(const TraceParams& P, S& sample, Rng& rng, F3& x, F3 xn
         }
         const float v_minus = v - P.iso_value;
         const float cur_sign = v_minus > 0.0f ? 1.0f : (v_minus < 0.0f ? -1.0f : 0.0f);
-        if (first_point) {
+        const bool from_outside = outside && *outside;
+        if (from_outside) {
+            first_point = false;
+            last_sign = -P.iso_value > 0.0f ? 1.0f : (-P.iso_value < 0.0f ? -1.0f : 0.0f);
+        } else if (first_point) {
             first_point = false;
             last_sign = cur_sign;
         }
@@ -153,19 +164,24 @@ VPT_DEV bool iso_segment(const TraceParams& P, S& sample, Rng& rng, F3& x, F3 xn
                 else x0 = mid;
             }
             x = x1;
+            IsoFrame fr;
+            const IsoBrdfSample bs = iso_sample(P, rng, x, w, fr, from_outside ? &cam : nullptr);
             if constexpr (NEE) {  // USE_ISOSURFACE_NEE: the light sample before the throughput takes the BRDF
-                IsoFrame fr;
-                const IsoBrdfSample bs = iso_sample(P, rng, x, w, fr);
                 iso_surface_nee(P, sample, rng, x, fr, bs, weights, *nee_color, *pc);
-                weights = f3(weights.x * bs.value.x, weights.y * bs.value.y, weights.z * bs.value.z);
-                w = bs.dir;
-            } else {
-                iso_scatter(P, rng, x, w, weights);
             }
+            weights = f3(weights.x * bs.value.x, weights.y * bs.value.y, weights.z * bs.value.z);
+            w = bs.dir;
             x = x + w * 1e-4f;
             first_point = true;
+            if (outside) *outside = false;
             // firstEvent of a surface hit: density = extinction, depth = tMax - d + |x - x1|
-            if (fe) record_event(*fe, x, 1.0f, P.extinction, tmax - d + length3(x1 - x), w);
+            if (fe) {
+                if (!fe->has && outside) {
+                    fe->iso = true;
+                    fe->n = fr.n;
+                }
+                record_event(*fe, x, 1.0f, P.extinction, tmax - d + length3(x1 - x), w);
+            }
             float tmin;
             if (ray_box_p(P, x, w, tmin, tmax)) {
                 x = x + w * tmin;
@@ -173,6 +189,7 @@ VPT_DEV bool iso_segment(const TraceParams& P, S& sample, Rng& rng, F3& x, F3 xn
             }
             return true;
         }
+        if (outside) *outside = false;
     }
     return false;
 }
@@ -183,6 +200,8 @@ VPT_DEV bool iso_segment(const TraceParams& P, S& sample, Rng& rng, F3& x, F3 xn
 // with zero.  Trilinear lookups (the reference forces them with isosurfaces).
 template <class S>
 VPT_DEV F3 track_delta_iso(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, FirstEvent& fe, PathCtx& pc) {
+    const F3 cam = x;  // cameraPosition (Clouds.glsl:99)
+    bool outside = P.iso_close != 0;
     F3 weights = f3(1.0f, 1.0f, 1.0f);
     float last_sign = 0.0f;
     bool first_point = true;
@@ -201,7 +220,7 @@ VPT_DEV F3 track_delta_iso(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w
             float density = sample(xn, rng);
             pc.lookups++;
             if (iso_segment(P, sample, rng, x, xn, density, w, d, tmax, weights, last_sign, first_point, pc.lookups,
-                            &fe)) {
+                            &fe, nullptr, nullptr, P.iso_close ? &outside : nullptr, cam)) {
                 if (weights.x < 1e-3f && weights.y < 1e-3f && weights.z < 1e-3f) return f3(0.0f, 0.0f, 0.0f);
                 continue;
             }
@@ -539,6 +558,8 @@ VPT_DEV F3 track_nee(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, Firs
 // added at the end only for a path without any event.
 template <class S>
 VPT_DEV F3 track_nee_iso(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, FirstEvent& fe, PathCtx& pc) {
+    const F3 cam = x;  // cameraPosition (Clouds.glsl:99)
+    bool outside = P.iso_close != 0;
     F3 color = f3(0.0f, 0.0f, 0.0f);
     F3 weights = f3(1.0f, 1.0f, 1.0f);
     float last_sign = 0.0f;
@@ -558,7 +579,7 @@ VPT_DEV F3 track_nee_iso(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, 
             float density = sample(xn, rng);
             pc.lookups++;
             if (iso_segment<true>(P, sample, rng, x, xn, density, w, d, tmax, weights, last_sign, first_point,
-                                  pc.lookups, &fe, &color, &pc)) {
+                                  pc.lookups, &fe, &color, &pc, P.iso_close ? &outside : nullptr, cam)) {
                 if (weights.x < 1e-3f && weights.y < 1e-3f && weights.z < 1e-3f) return f3(0.0f, 0.0f, 0.0f);
                 continue;
             }
@@ -664,6 +685,8 @@ VPT_DEV F3 sdt_clamp(F3 v, float c) { return f3(fminf(v.x, c), fminf(v.y, c), fm
 template <bool ISO, class S>
 VPT_DEV F3 track_delta_spectral(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, FirstEvent& fe,
                                 PathCtx& pc) {
+    const F3 cam = x;  // cameraPosition (Clouds.glsl:99)
+    bool outside = ISO && P.iso_close != 0;
     F3 weights = f3(1.0f, 1.0f, 1.0f);
     float last_sign = 0.0f;
     bool first_point = true;
@@ -683,7 +706,7 @@ VPT_DEV F3 track_delta_spectral(const TraceParams& P, S& sample, Rng& rng, F3 x,
             pc.lookups++;
             if constexpr (ISO) {
                 if (iso_segment(P, sample, rng, x, xn, density, w, d, tmax, weights, last_sign, first_point,
-                                pc.lookups, &fe)) {
+                                pc.lookups, &fe, nullptr, nullptr, P.iso_close ? &outside : nullptr, cam)) {
                     if (weights.x < 1e-3f && weights.y < 1e-3f && weights.z < 1e-3f) return f3(0.0f, 0.0f, 0.0f);
                     continue;
                 }
@@ -730,6 +753,8 @@ VPT_DEV F3 track_delta_spectral(const TraceParams& P, S& sample, Rng& rng, F3 x,
 // estimation, delta-tracked shadow rays, emission scaled by the surface throughput.
 template <bool ESS, bool ISO = false, class S>
 VPT_DEV F3 track_nee_spectral(const TraceParams& P, S& sample, Rng& rng, F3 x, F3 w, FirstEvent& fe, PathCtx& pc) {
+    const F3 cam = x;  // cameraPosition (Clouds.glsl:99)
+    bool outside = ISO && P.iso_close != 0;
     F3 weights = f3(1.0f, 1.0f, 1.0f);
     F3 color = f3(0.0f, 0.0f, 0.0f);
     float last_sign = 0.0f;
@@ -752,7 +777,7 @@ VPT_DEV F3 track_nee_spectral(const TraceParams& P, S& sample, Rng& rng, F3 x, F
             pc.lookups++;
             if constexpr (ISO) {  // CheckIsosurfaceHit.glsl with surface next-event estimation
                 if (iso_segment<true>(P, sample, rng, x, xn, density, w, d, tmax, weights, last_sign, first_point,
-                                      pc.lookups, &fe, &color, &pc)) {
+                                      pc.lookups, &fe, &color, &pc, P.iso_close ? &outside : nullptr, cam)) {
                     if (weights.x < 1e-3f && weights.y < 1e-3f && weights.z < 1e-3f) return f3(0.0f, 0.0f, 0.0f);
                     continue;
                 }

@@ -26,7 +26,7 @@ OPS = [
     "clear_lights", "add_light", "remove_light", "set_light_property", "load_lights_from_file", "set_use_headlight",
     "set_use_headlight_distance", "set_headlight_color", "set_headlight_intensity", "set_use_isosurfaces",
     "set_iso_value", "set_iso_surface_color", "set_isosurface_type", "set_surface_brdf", "set_brdf_parameter",
-    "set_use_clip_plane", "set_clip_plane_normal", "set_clip_plane_distance",
+    "set_use_clip_plane", "set_clip_plane_normal", "set_clip_plane_distance", "set_close_isosurfaces",
     "set_num_isosurface_subdivisions", "set_seed_offset", "set_use_feature_maps", "get_feature_map",
     "get_feature_map_from_string", "set_phase_g", "set_view_projection_matrix_as_previous", "set_use_emission",
     "set_emission_strength", "set_emission_cap", "get_volume_voxel_size", "get_render_bounding_box",

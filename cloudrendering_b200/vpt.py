@@ -329,6 +329,12 @@ def set_clip_plane_distance(_clip_plane_distance: float) -> None:
     _c("vpt_set_clip_plane_distance", float(_clip_plane_distance))
 
 
+def set_close_isosurfaces(_close_isosurfaces: bool) -> None:
+    """With isosurfaces and the clip plane on, the box faces and the clip plane close the isosurfaces
+    (CLOSE_ISOSURFACES; src/PyTorch/Module.cpp:1209-1211)."""
+    _c("vpt_set_close_isosurfaces", 1 if _close_isosurfaces else 0)
+
+
 def set_num_isosurface_subdivisions(subdivisions: int) -> None:
     _c("vpt_set_num_isosurface_subdivisions", int(subdivisions))
 

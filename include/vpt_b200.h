@@ -183,6 +183,12 @@ VptStatus vpt_set_num_isosurface_subdivisions(VptContext* ctx, int subdivisions)
 VptStatus vpt_set_use_clip_plane(VptContext* ctx, int use);
 VptStatus vpt_set_clip_plane_normal(VptContext* ctx, double x, double y, double z);
 VptStatus vpt_set_clip_plane_distance(VptContext* ctx, double distance);
+/* set_close_isosurfaces (src/PyTorch/Module.cpp:1209-1211; CLOSE_ISOSURFACES, defined while isosurfaces
+ * and the clip plane are both on, VolumetricPathTracingPass.cpp:1777-1779): outside the volume counts as
+ * below the iso value on a path's first check point, so the box faces and the clip plane close the
+ * isosurfaces, with the face's normal (rayBoxIntersectionNormal) and that normal in the normal map.
+ * Off by default; traced on persistent warp batches. */
+VptStatus vpt_set_close_isosurfaces(VptContext* ctx, int close);
 /* Synthetic scene on the device: seeded fBm of improved Perlin noise, remapped to [0, 1], values
  * below `threshold` set to 0.  No reference counterpart (the reference loads files). */
 VptStatus vpt_generate_fbm_grid(VptContext* ctx, int nx, int ny, int nz, uint32_t seed, int octaves,

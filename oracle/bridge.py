@@ -45,7 +45,7 @@ class OracleScene(ctypes.Structure):
         ("sv_inv_world", c_float * 3), ("sv_local", c_void_p),
         ("env_rot", c_int), ("env_rot_m", c_float * 9), ("tf_albedo_strength", c_float), ("iso_brdf", c_int),
         ("brdf", c_float * 10), ("iso_grad", c_void_p), ("iso_norm_min", c_float), ("iso_norm_range", c_float),
-        ("use_clip", c_int), ("clip", c_float * 4),
+        ("use_clip", c_int), ("clip", c_float * 4), ("iso_close", c_int),
     ]
 
 

@@ -138,6 +138,11 @@ def variants():
                     + ENVS["default__linear"] + ["USE_CLIP_PLANE"], 0))
     out.append(("sdt_hist_clip__stochastic__default__linear", [SPECTRAL["sdt"], SDT_PROB["hist"],
                 INTERPS["stochastic"]] + ENVS["default__linear"] + ["USE_CLIP_PLANE"], 0))
+    # isosurfaces closed by the box and the clip plane (CLOSE_ISOSURFACES, VolumetricPathTracingPass.cpp:1777-1779)
+    out.append(("delta_iso_clip_close__trilinear__default__linear", TRACKERS["delta"] + [INTERPS["trilinear"]]
+                + ENVS["default__linear"] + ISO + ["USE_CLIP_PLANE", "CLOSE_ISOSURFACES"], 0))
+    out.append(("nee_iso_clip_close__trilinear__default__linear", TRACKERS["nee"] + [INTERPS["trilinear"]]
+                + ENVS["default__linear"] + ISO + ["USE_ISOSURFACE_NEE", "USE_CLIP_PLANE", "CLOSE_ISOSURFACES"], 0))
     # next event tracking with isosurfaces (USE_ISOSURFACE_NEE, VolumetricPathTracingPass.cpp:1761-1763) for
     # every surface BRDF
     for tag, define in (("", "SURFACE_BRDF_LAMBERTIAN"), ("_blinn", "SURFACE_BRDF_BLINN_PHONG"),

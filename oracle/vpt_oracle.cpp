@@ -120,6 +120,43 @@ bool ray_box(V3 bmin, V3 bmax, V3 p, V3 d, float& tmin, float& tmax) {
     return true;
 }
 
+// rayBoxIntersectionNormal (VptUtils.glsl:803-856, CLOSE_ISOSURFACES): the entered face's normal, or
+// -clip normal where the clip plane is the entry surface; n unchanged in the cases the shader leaves it
+void ray_box_normal(V3 bmin, V3 bmax, V3 p, V3 d, V3& n) {
+    d.x = fabsf(d.x) <= 1e-6f ? 1e-6f : d.x;
+    d.y = fabsf(d.y) <= 1e-6f ? 1e-6f : d.y;
+    d.z = fabsf(d.z) <= 1e-6f ? 1e-6f : d.z;
+    const V3 cmin = divv(sub(bmin, p), d), cmax = divv(sub(bmax, p), d);
+    const float mx = std::min(cmin.x, cmax.x), my = std::min(cmin.y, cmax.y), mz = std::min(cmin.z, cmax.z);
+    const float tmin = std::max(0.0f, std::max(std::max(mx, my), mz));
+    const float tmax = std::min(std::min(std::max(cmin.x, cmax.x), std::max(cmin.y, cmax.y)), std::max(cmin.z, cmax.z));
+    if (tmax <= tmin || tmax <= 0.0f) return;
+    auto sgn = [](float v) { return v > 0.0f ? 1.0f : (v < 0.0f ? -1.0f : 0.0f); };
+    V3 nb;
+    if (mx > my && mx > mz) nb = v3(-sgn(d.x), 0.0f, 0.0f);
+    else if (my > mz) nb = v3(0.0f, -sgn(d.y), 0.0f);
+    else nb = v3(0.0f, 0.0f, -sgn(d.z));
+    if (g_clip) {
+        const V3 cn = v3(g_clip[0], g_clip[1], g_clip[2]);
+        const float denom = dot(cn, d);
+        const float dp = dot(cn, p) - g_clip[3];
+        if (fabsf(denom) < 1e-3f) {
+            if (dp > 0.0f) n = nb;
+            return;
+        }
+        const float t_clip = (g_clip[3] - dot(cn, p)) / denom;
+        if (t_clip <= 0.0f) {
+            if (dp > 0.0f) n = nb;
+            return;
+        }
+        if (dp <= 0.0f && t_clip >= tmin) {
+            n = v3(-cn.x, -cn.y, -cn.z);
+            return;
+        }
+    }
+    n = nb;
+}
+
 // ---- directions (VptUtils.glsl:67-123) ----
 void basis(V3 d, V3& b, V3& t) {
     V3 other = fabsf(d.z) >= 0.9999f ? v3(1, 0, 0) : v3(0, 0, 1);
@@ -1038,10 +1075,11 @@ struct Tracer {
     // 20-28), the selected BRDF's sample.  Lambertian.glsl is included (VptUtils.glsl:1121) before
     // UNIFORM_SAMPLING is defined (:1144), so it samples the cosine-weighted hemisphere through the
     // concentric disk map (VptUtils.glsl:1078-1098) and its pdf factor is the cosine itself
-    BrdfS iso_sample(V3 p, V3 w, Frame& fr, Rng& r) {
+    BrdfS iso_sample(V3 p, V3 w, Frame& fr, Rng& r, const V3* cam = nullptr) {
         (void)rnd(r);  // isoSurfaceOpacity (1) < random() never holds
         V3 n = iso_normal(p);
-        if (dot(w, n) > 0.0f) n = neg(n);
+        if (cam) ray_box_normal(bmin(), bmax(), *cam, w, n);  // a closing surface (CLOSE_ISOSURFACES)
+        else if (dot(w, n) > 0.0f) n = neg(n);
         const float yz = -n.y * n.z;
         const V3 b = normalize(fabsf(n.z) > 0.99999f ? v3(-n.x * n.y, 1.0f - n.y * n.y, yz)
                                                      : v3(-n.x * n.z, yz, 1.0f - n.z * n.z));
@@ -1198,32 +1236,35 @@ struct Tracer {
     // sign change of sampleCloudIso - iso_value against the first point after the last surface event;
     // a crossing is bisected, the surface scatters, the path moves 1e-4 off it and restarts from the
     // box boundary.  Returns true on a surface event.
+    // CLOSE_ISOSURFACES: `outside` is true until the path's first check point, where outside the volume
+    // counts as sign(-iso_value) and a hit takes the face entered from the camera position `cam`
     bool iso_check(V3& x, V3 xn, V3& w, float& d, float& tmax, V3& weights, float& last_sign, bool& first_point,
-                   Rng& r, bool& ev, V3* nee_color = nullptr) {
+                   Rng& r, bool& ev, V3* nee_color = nullptr, bool* outside = nullptr, V3 cam = V3{0, 0, 0}) {
         const int nsub = S.iso_subdivisions;
         for (int sub = 0; sub < nsub; sub++) {
             const float a0 = (float)sub / (float)nsub, a1 = (float)(sub + 1) / (float)nsub;
             const V3 x0 = add(mul(x, 1.0f - a0), mul(xn, a0));
             V3 x1 = add(mul(x, 1.0f - a1), mul(xn, a1));
             const float cur_sign = signf(iso_value_at(x1, r) - S.iso_value);
-            if (first_point) {
+            const bool from_outside = outside && *outside;
+            if (from_outside) {
+                first_point = false;
+                last_sign = signf(-S.iso_value);
+            } else if (first_point) {
                 first_point = false;
                 last_sign = cur_sign;
             }
             if (last_sign != cur_sign) {
                 iso_refine(x1, x0, cur_sign, r);
                 x = x1;
-                if (nee_color) {  // USE_ISOSURFACE_NEE: the light sample before the throughput takes the BRDF
-                    Frame fr;
-                    const BrdfS bs = iso_sample(x, w, fr, r);
-                    surface_nee(x, fr, bs, weights, *nee_color, r);
-                    weights = v3(weights.x * bs.value.x, weights.y * bs.value.y, weights.z * bs.value.z);
-                    w = bs.dir;
-                } else {
-                    iso_scatter(x, w, weights, r);
-                }
+                Frame fr;
+                const BrdfS bs = iso_sample(x, w, fr, r, from_outside ? &cam : nullptr);
+                if (nee_color) surface_nee(x, fr, bs, weights, *nee_color, r);  // USE_ISOSURFACE_NEE
+                weights = v3(weights.x * bs.value.x, weights.y * bs.value.y, weights.z * bs.value.z);
+                w = bs.dir;
                 x = add(x, mul(w, 1e-4f));
                 first_point = true;
+                if (outside) *outside = false;
                 ev = true;
                 float tmin;
                 if (ray_box(bmin(), bmax(), x, w, tmin, tmax)) {
@@ -1232,10 +1273,13 @@ struct Tracer {
                 }
                 return true;
             }
+            if (outside) *outside = false;
         }
         return false;
     }
     V3 delta_iso(V3 x, V3 w, Rng& r, bool& ev) {
+        const V3 cam = x;  // cameraPosition (Clouds.glsl:99)
+        bool outside = S.use_iso && S.iso_close;
         float tmin, tmax;
         const float absorb = 1.0f - S.albedo;
         V3 weights = v3(1, 1, 1);
@@ -1253,7 +1297,7 @@ struct Tracer {
                 if (t > d) break;
                 V3 xn = add(x, mul(w, t));
                 float dens = sample(xn, r);
-                if (iso_check(x, xn, w, d, tmax, weights, last_sign, first_point, r, ev)) {
+                if (iso_check(x, xn, w, d, tmax, weights, last_sign, first_point, r, ev, nullptr, S.iso_close ? &outside : nullptr, cam)) {
                     if (weights.x < 1e-3f && weights.y < 1e-3f && weights.z < 1e-3f) return v3(0, 0, 0);
                     continue;
                 }
@@ -1480,6 +1524,8 @@ struct Tracer {
     // delta-tracked shadow rays, volume light samples scaled by the surface throughput, the sky at the
     // end only for a path without any event
     V3 nee_iso(V3 x, V3 w, Rng& r, bool& ev) {
+        const V3 cam = x;  // cameraPosition (Clouds.glsl:99)
+        bool outside = S.use_iso && S.iso_close;
         V3 color = v3(0, 0, 0), weights = v3(1, 1, 1);
         float last_sign = 0.0f;
         bool first_point = true;
@@ -1497,7 +1543,7 @@ struct Tracer {
                 if (t > d) break;
                 V3 xn = add(x, mul(w, t));
                 float dens = sample(xn, r);
-                if (iso_check(x, xn, w, d, tmax, weights, last_sign, first_point, r, ev, &color)) {
+                if (iso_check(x, xn, w, d, tmax, weights, last_sign, first_point, r, ev, &color, S.iso_close ? &outside : nullptr, cam)) {
                     if (weights.x < 1e-3f && weights.y < 1e-3f && weights.z < 1e-3f) return v3(0, 0, 0);
                     continue;
                 }
@@ -1659,6 +1705,8 @@ struct Tracer {
     // with isosurfaces (USE_ISOSURFACES, DeltaTracking.glsl:37-63 and the CheckIsosurfaceHit.glsl include):
     // the 1000-iteration cap, the segment check and the surface throughput in the spectral weights
     V3 spectral_delta(V3 x, V3 w, Rng& r, bool& ev) {
+        const V3 cam = x;  // cameraPosition (Clouds.glsl:99)
+        bool outside = S.use_iso && S.iso_close;
         const float maj = maxc(ext3());
         V3 weights = v3(1, 1, 1);
         float last_sign = 0.0f;
@@ -1676,7 +1724,7 @@ struct Tracer {
                 if (t > d) break;
                 V3 xn = add(x, mul(w, t));
                 float dens = sample(xn, r);
-                if (S.use_iso && iso_check(x, xn, w, d, tmax, weights, last_sign, first_point, r, ev)) {
+                if (S.use_iso && iso_check(x, xn, w, d, tmax, weights, last_sign, first_point, r, ev, nullptr, S.iso_close ? &outside : nullptr, cam)) {
                     if (weights.x < 1e-3f && weights.y < 1e-3f && weights.z < 1e-3f) return v3(0, 0, 0);
                     continue;
                 }
@@ -1716,6 +1764,8 @@ struct Tracer {
 
     // nextEventTrackingSpectral (NextEventTracking.glsl:31-220)
     V3 spectral_nee(V3 x, V3 w, Rng& r, bool& ev) {
+        const V3 cam = x;  // cameraPosition (Clouds.glsl:99)
+        bool outside = S.use_iso && S.iso_close;
         const float maj = maxc(ext3());
         V3 weights = v3(1, 1, 1), color = v3(0, 0, 0);
         float last_sign = 0.0f;
@@ -1736,7 +1786,7 @@ struct Tracer {
                 // (NextEventTracking.glsl:74, sampleCloudDensityEmission(x))
                 float dens = sample(S.tf ? x : xn, r);
                 // isosurfaces (CheckIsosurfaceHit.glsl with USE_ISOSURFACE_NEE)
-                if (S.use_iso && iso_check(x, xn, w, d, tmax, weights, last_sign, first_point, r, ev, &color)) {
+                if (S.use_iso && iso_check(x, xn, w, d, tmax, weights, last_sign, first_point, r, ev, &color, S.iso_close ? &outside : nullptr, cam)) {
                     if (weights.x < 1e-3f && weights.y < 1e-3f && weights.z < 1e-3f) return v3(0, 0, 0);
                     continue;
                 }

@@ -102,6 +102,9 @@ typedef struct OracleScene {
      * normal (3) and distance */
     int use_clip;
     float clip[4];
+    /* CLOSE_ISOSURFACES (isosurfaces with the clip plane on): outside the volume counts as below the iso
+     * value on a path's first check point; the surface there takes the entered face's normal */
+    int iso_close;
 } OracleScene;
 
 /* Renders width*height*num_frames paths; adds radiance (and its square) per pixel (3 doubles). */

@@ -146,6 +146,13 @@ def cases():
         kw2 = dict(base)
         kw2.update(kw)
         out["fbm_" + name] = SceneSpec(grid=fbm, clip_plane=(0.3, 0.5, 0.8, -0.02), **kw2)
+    # isosurfaces closed by the box faces and the clip plane (CLOSE_ISOSURFACES): a low iso value, so that
+    # many camera rays enter the box inside a surface, and the plane through the cloud
+    for name, mode in (("delta_iso_clip_close", "delta"), ("nee_iso_clip_close", "nee")):
+        kw2 = dict(base)
+        kw2.update(iso_value=0.05, iso_color=(0.9, 0.6, 0.3), extinction=40.0, albedo=0.9, g=0.2)
+        out["fbm_" + name] = SceneSpec(grid=fbm, mode=mode, interp="trilinear", iso=True, clip_plane=(0.3, 0.5, 0.8, -0.02),
+                                       close_iso=True, **kw2)
     # next event tracking with isosurfaces and surface next-event estimation, every BRDF (MIS for the
     # specular samples of Cook-Torrance and Disney)
     for name, brdf, params in (("nee_iso", "Lambertian", None), ("nee_iso_blinn", "Blinn Phong", None),
@@ -207,7 +214,7 @@ FIELDS = ["mode", "interp", "extinction", "albedo", "g", "width", "height", "see
           "sun_dir", "sun_intensity", "cam_pos", "cam_target", "fovy", "near", "far", "max_grid_extent", "use_ess",
           "env_intensity", "max_bounces", "ess_ref_compat", "lights", "extinction_base", "albedo_rgb", "sdt_prob",
           "emission_cap", "emission_strength", "iso", "iso_value", "iso_color", "env_rot", "tf_albedo_strength",
-          "iso_brdf", "brdf_params", "iso_type", "clip_plane"]
+          "iso_brdf", "brdf_params", "iso_type", "clip_plane", "close_iso"]
 
 
 def depth_map_cases():

@@ -71,7 +71,7 @@ class SceneSpec:
                  extinction_base=(1.0, 1.0, 1.0), albedo_rgb=None, sdt_prob=2, emission=None, emission_cap=1.0,
                  emission_strength=1.0, tf=None, iso=False, iso_value=0.5, iso_color=(0.4, 0.4, 0.4), env_rot=None,
                  tf_albedo_strength=0.0, iso_brdf="Lambertian", brdf_params=None, iso_type="Density",
-                 clip_plane=None):
+                 clip_plane=None, close_iso=False):
         self.__dict__.update(locals())
         del self.__dict__["self"]
 
@@ -200,6 +200,7 @@ def setup_core(core: Core, sp: SceneSpec):
     core("vpt_set_surface_brdf", sp.iso_brdf.encode())
     core("vpt_set_isosurface_type", sp.iso_type.encode())
     core("vpt_set_use_clip_plane", 1 if sp.clip_plane is not None else 0)
+    core("vpt_set_close_isosurfaces", 1 if sp.close_iso else 0)
     if sp.clip_plane is not None:
         core("vpt_set_clip_plane_normal", *[float(c) for c in sp.clip_plane[:3]])
         core("vpt_set_clip_plane_distance", float(sp.clip_plane[3]))
@@ -380,6 +381,7 @@ def oracle_scene(core, sp: SceneSpec, frames: int, frame_count: int = 0) -> brid
     if sp.clip_plane is not None:
         sc.set("use_clip", 1)
         sc.set("clip", clip_values(sp))
+        sc.set("iso_close", 1 if (sp.close_iso and sp.iso) else 0)
     sc.set("iso_value", float(np.float32(sp.iso_value)))
     sc.set("iso_color", [float(np.float32(c)) for c in sp.iso_color])
     if sp.env_rot is not None and sp.env == "image":
@@ -550,6 +552,8 @@ def reference_scene(sp: SceneSpec, frames: int, frame_start: int = 0, inv=None):
         sc.set("use_clip", 1)
         sc.set("clip", clip_values(sp))
         tracker += "_clip"
+        if sp.close_iso and sp.iso:
+            tracker += "_close"
     env = {"default": "default", "black": "black", "single": "single", "image": "image"}[sp.env]
     colour = "linear" if (sp.linear_rgb or env != "default") else "srgb"
     return sc, f"{tracker}__{sp.interp}__{env}__{colour}"
